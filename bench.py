@@ -1,0 +1,371 @@
+"""Benchmark: rays/s of one phase-function record on B200 (and the reference CPU arm).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--rays R]
+
+Workload (hex column): circumradius 0.05 mm, length 0.2 mm (length/diameter 2), n = 1.31,
+550 nm, inclination 30 deg (ki = (cos30, -sin30, 0)), identity orientation, seed 12345,
+1e8 rays, at most 12 internal interactions (the residual is reported), 512 x 1024 (u, phi)
+cells, FP32 trace, FP64 histogram flush and CDF.  A step is one record: trace + bin of all
+rays and the stored CDF.  With N ranks (torchrun), every rank traces its own 1e8-ray shard
+of one record (weak scaling), the FP64 histograms are summed with one NCCL all-reduce, and
+rank 0 builds the CDF.
+
+Timing: CUDA events on the library's stream, W untimed warm-up steps, K timed steps, each
+bracketed by barrier + synchronize; an L2 flush (a 256 MiB write) separates timed steps;
+max over ranks.  `value` has inputs resident in HBM; `e2e` goes through the public
+host-buffer entry (icp_hex_generate) with the host<->device copies inside the timed region.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+CFG = dict(R=0.05, L=0.2, ki=(0.8660254037844387, -0.5, 0.0), n=1.31, nt=512, np=1024, hits=12, seed=12345)
+METRIC = "rays/s (hex column record: 1e8 rays traced, binned and stored as a CDF)"
+# Algorithmic FP32 work counted from the trace kernel source (flops per event; div/sqrt/rsqrt
+# and atan2 counted as one op each): entry = RNG-free geometry 20 + Fresnel/Stokes split 150
+# + binning 80; internal interaction = nearest-plane search 66 + split 150 + binning 80.
+FLOP_ENTRY, FLOP_INTERACTION = 250.0, 296.0
+
+
+def _env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    def __init__(self, device: int):
+        self.device, self.rows, self.proc = device, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm = [float(r[0]) for r in self.rows if r and r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if len(r) > 1 and r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 3 + i and r[3 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------- reference arm
+def reference_sample(rays_per_proc: int, procs: int) -> dict:
+    """Reference CPU path (oracle/_ref/ref_hex_harness, built from the reference sources),
+    one process per core over disjoint ray-id slices of the same record."""
+    exe = ROOT / "oracle" / "_ref" / "ref_hex_harness"
+    if not exe.exists():
+        raise FileNotFoundError(exe)
+    c = CFG
+    args = [str(exe), "time", repr(c["R"]), repr(c["L"]), *map(repr, c["ki"]), repr(c["n"]), "1", str(c["nt"]),
+            str(c["np"]), str(c["hits"]), repr(1e-12), str(c["seed"])]
+    t0 = time.perf_counter()
+    ps = [subprocess.Popen(args + [str(i * rays_per_proc), str(rays_per_proc)], stdout=subprocess.PIPE, text=True)
+          for i in range(procs)]
+    outs = [json.loads(p.communicate()[0]) for p in ps]
+    wall = time.perf_counter() - t0
+    rays = sum(o["rays"] for o in outs)
+    return {"rays": rays, "seconds": wall, "rays_per_s": rays / wall, "procs": procs}
+
+
+def run_reference(a) -> None:
+    rank, world, _ = _env_rank()
+    if rank != 0:
+        return
+    procs = os.cpu_count() or 1
+    per = max(1000, int(a.ref_rays) // procs)
+    for _ in range(a.warmup):
+        reference_sample(max(1000, per // 10), procs)
+    vals = [reference_sample(per, procs) for _ in range(a.steps)]
+    v = sum(x["rays"] for x in vals) / sum(x["seconds"] for x in vals)
+    line = {"metric": METRIC, "value": v, "unit": "rays/s", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": 1e3 * sum(x["seconds"] for x in vals) / len(vals), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "hex_column_config3", **_cfg_public()}, "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "rays/s", "cores": procs, "kind": "reference",
+                             "sample": f"{per} rays per process x {procs} processes per step (disjoint ray ids), "
+                                       "reference ice_crystal hex trace + PhaseMassAccumulator"},
+            "e2e": {"value": v, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def _cfg_public() -> dict:
+    c = CFG
+    return {"circumradius_mm": c["R"], "length_mm": c["L"], "ki": list(c["ki"]), "interior_index": c["n"],
+            "wavelength_nm": 550, "cells": [c["nt"], c["np"]], "max_internal_hits": c["hits"], "seed": c["seed"]}
+
+
+# ----------------------------------------------------------------------------- B200 arm
+def run_b200(a) -> None:
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    import ice_crystal_phase_b200 as I
+
+    rank, world, local = _env_rank()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    ctx = I.Context(local)
+    stream = torch.cuda.ExternalStream(I.LIB.icp_context_stream(ctx.handle))
+    torch.cuda.set_stream(stream)
+    c = CFG
+    rays = int(a.rays)
+    grid = I.make_phase_grid(c["nt"], c["np"], c["ki"])
+    g = grid.abi()
+    edges = torch.from_numpy(grid.edges).cuda()
+    mass = torch.zeros(c["nt"] * c["np"], dtype=torch.float64, device="cuda")
+    phi = torch.empty(c["np"] + 1, dtype=torch.float64, device="cuda")
+    theta = torch.empty(c["np"] * (c["nt"] + 1), dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    node = I.HexNode()
+    node.circumradius_mm, node.length_mm = c["R"], c["L"]
+    for i, v in enumerate(I.rotation_from_quaternion(1, 0, 0, 0)):
+        node.rotation[i] = v
+    node.exterior_index, node.interior_index = 1.0, c["n"]
+    node.tail_tolerance, node.balance_tolerance = 1e-12, 1e-5
+    node.seed, node.total_samples = c["seed"], rays * world
+    node.first_sample, node.sample_count = rank * rays, rays
+    node.max_internal_hits, node.batch_size, node.precision = c["hits"], 4096, I.ICP_FP32
+    area = C.c_double()
+    I.check(I.LIB.icp_hex_node_area(C.byref(node), C.byref(g), C.byref(area)))
+    node.area_weight = area.value / float(rays * world)
+    policy = I.CdfPolicy(1e-10, 1e-12, 1.0)
+    pole = torch.zeros(2, dtype=torch.float64, device="cuda")
+
+    def step() -> I.TraceStats:
+        mass.zero_()
+        s = I.TraceStats()
+        I.check(I.LIB.icp_hex_trace_bin(ctx.handle, C.byref(node), C.byref(g), C.c_void_p(edges.data_ptr()),
+                                        C.c_void_p(mass.data_ptr()), C.byref(s), None, None))
+        if world > 1:
+            pole[0], pole[1] = node.area_weight * s.forward_pole, node.area_weight * s.backward_pole
+            dist.all_reduce(mass)
+            dist.all_reduce(pole)
+            fwd, bwd = float(pole[0]), float(pole[1])
+        else:
+            fwd, bwd = node.area_weight * s.forward_pole, node.area_weight * s.backward_pole
+        if rank == 0:
+            rep = I.CdfReport()
+            I.check(I.LIB.icp_phase_cdf_build(ctx.handle, C.c_void_p(mass.data_ptr()), 0, c["nt"], c["np"], fwd, bwd,
+                                              c["nt"], c["np"], C.byref(policy), C.c_void_p(phi.data_ptr()),
+                                              C.c_void_p(theta.data_ptr()), C.byref(rep)))
+        return s
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(a.warmup):
+        stats = step()
+    # timed region: K steps, device events per step, L2 flush between steps (not timed)
+    launches0 = I.kernel_launches()
+    times, stats_all = [], []
+    with ClockSampler(local) as clocks:
+        for _ in range(a.steps):
+            flush.fill_(1.0)
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            stats_all.append(step())
+            e1.record(stream)
+            barrier()
+            times.append(e0.elapsed_time(e1) / 1e3)
+    launches = I.kernel_launches() - launches0
+    t_local = torch.tensor([sum(times)], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t_local, op=dist.ReduceOp.MAX)
+    t_step = float(t_local) / a.steps
+    value = rays * world / t_step
+
+    # dominant kernel alone (trace+bin), for the roofline: events on the same stream
+    s0 = stats_all[-1]
+    mean_hits = s0.encounters / max(1, s0.rays)
+    flops_per_ray = FLOP_ENTRY + FLOP_INTERACTION * mean_hits
+    k_times = []
+    for _ in range(2):
+        flush.fill_(1.0)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        mass.zero_()
+        s = I.TraceStats()
+        e0.record(stream)
+        I.check(I.LIB.icp_hex_trace_bin(ctx.handle, C.byref(node), C.byref(g), C.c_void_p(edges.data_ptr()),
+                                        C.c_void_p(mass.data_ptr()), C.byref(s), None, None))
+        e1.record(stream)
+        barrier()
+        k_times.append(e0.elapsed_time(e1) / 1e3)
+    t_kernel = min(k_times)
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    clk = clocks.summary()
+    mhz = clk["sm_mhz"] or 1965.0
+    fp32_peak = sms * 128 * 2 * mhz * 1e6 / 1e12
+    achieved = rays * flops_per_ray / t_kernel / 1e12
+
+    # CDF kernel alone (HBM bound): read 8*C, write 8*np*(nt+1) + 8*(np+1)
+    cdf_bytes = 8 * c["nt"] * c["np"] + 8 * c["np"] * (c["nt"] + 1) + 8 * (c["np"] + 1)
+    cdf_t = []
+    if rank == 0:
+        for _ in range(3):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            rep = I.CdfReport()
+            e0.record(stream)
+            I.check(I.LIB.icp_phase_cdf_build(ctx.handle, C.c_void_p(mass.data_ptr()), 0, c["nt"], c["np"], 0.0, 0.0,
+                                              c["nt"], c["np"], C.byref(policy), C.c_void_p(phi.data_ptr()),
+                                              C.c_void_p(theta.data_ptr()), C.byref(rep)))
+            e1.record(stream)
+            torch.cuda.synchronize()
+            cdf_t.append(e0.elapsed_time(e1) / 1e3)
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except (OSError, ValueError):
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+
+    # e2e through the host-buffer public entry (N=1) or the sharded Python entry (N>1)
+    e2e_times = []
+    ph = torch.empty(c["np"] + 1, dtype=torch.float64).pin_memory()
+    th = torch.empty(c["np"] * (c["nt"] + 1), dtype=torch.float64).pin_memory()
+    uh = torch.empty(c["nt"] + 1, dtype=torch.float64).pin_memory()
+    if world == 1:
+        rec = I.HexRecordArgs()
+        rec.circumradius_mm, rec.length_mm = c["R"], c["L"]
+        for i in range(3):
+            rec.ki[i] = c["ki"][i]
+        rec.exterior_index, rec.interior_index = 1.0, c["n"]
+        rec.tail_tolerance, rec.balance_tolerance = 1e-12, 1e-5
+        rec.nt, rec.np, rec.ct, rec.cp = c["nt"], c["np"], c["nt"], c["np"]
+        rec.max_internal_hits, rec.batch_size, rec.precision = c["hits"], 4096, I.ICP_FP32
+        rec.policy = policy
+        nodes = (I.Orientation * 1)()
+        nodes[0].quaternion[0] = 1.0
+        nodes[0].weight, nodes[0].samples, nodes[0].seed = 1.0, rays, c["seed"]
+        for i in range(a.steps + 1):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            rr = I.RecordReport()
+            e0.record(stream)
+            I.check(I.LIB.icp_hex_generate(ctx.handle, C.byref(rec), nodes, 1,
+                                           C.cast(C.c_void_p(ph.data_ptr()), I._D),
+                                           C.cast(C.c_void_p(th.data_ptr()), I._D),
+                                           C.cast(C.c_void_p(uh.data_ptr()), I._D), C.byref(rr)))
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if i:
+                e2e_times.append(e0.elapsed_time(e1) / 1e3)
+        e2e_value = rays / (sum(e2e_times) / len(e2e_times))
+    else:
+        e2e_value = None
+    h2d = 8 * (c["nt"] + 1) + 168  # u edges + per-node record arguments
+    d2h = 8 * (c["np"] + 1) + 8 * c["np"] * (c["nt"] + 1) + 200
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        try:
+            procs = os.cpu_count() or 1
+            rb = reference_sample(max(2000, int(a.ref_rays) // procs), procs)
+            cpu = {"value": rb["rays_per_s"], "unit": "rays/s", "cores": procs, "kind": "reference",
+                   "sample": f"{rb['rays']} rays of the same record (disjoint ray ids, {procs} processes), "
+                             "reference hex tracer + PhaseMassAccumulator compiled from its sources"}
+        except (OSError, ValueError) as e:
+            cpu = {"value": None, "unit": "rays/s", "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1e3 * t_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "hex_column_config3", **_cfg_public(), "rays_per_gpu": rays,
+                   "l2": "flushed between timed steps (256 MiB write)", "trace_precision": "fp32",
+                   "parallelism": f"ray shards x{world}, NCCL all-reduce of FP64 histogram" if world > 1 else "1 GPU"},
+        "records_per_s": 1.0 / t_step,
+        "e2e": {"value": e2e_value, "unit": "rays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "roofline": {"kernel": "hex_trace_bin_kernel<float>", "bound": "fp32_simt", "achieved": achieved,
+                     "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+                     "peak_note": f"derived: {sms} SMs x 128 FP32 lanes x 2 x {mhz:.0f} MHz (median SM clock under load)",
+                     "flops_per_ray": flops_per_ray, "kernel_ms": 1e3 * t_kernel,
+                     "mean_interactions_per_ray": mean_hits},
+        "roofline_cdf": ({"kernel": "cdf_build_kernel", "bound": "hbm", "achieved": cdf_bytes / min(cdf_t) / 1e9,
+                          "peak": hbm, "unit": "GB/s", "frac": cdf_bytes / min(cdf_t) / 1e9 / hbm,
+                          "traffic": None, "algorithmic_bytes": cdf_bytes, "kernel_us": 1e6 * min(cdf_t),
+                          "peak_note": "MEASURED_PEAKS.json hbm_gbs (of measured)"} if cdf_t else None),
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "gpu_launches": launches,
+        "trace": {"outputs_per_ray": s0.outputs / max(1, s0.rays), "unresolved_fraction": s0.unresolved / max(1, s0.rays),
+                  "fallback_adds": s0.fallback_adds, "near_edge": s0.near_edge},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    p.add_argument("--rays", type=float, default=1e8)
+    p.add_argument("--ref-rays", type=float, default=1.6e6, help="reference rays per step (all processes)")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    a = p.parse_args()
+    if a.warmup < 3:
+        a.warmup = 3
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_b200(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,524 @@
+"""B200-native phase-function generation: Python mirror of the reference's stage interfaces.
+
+The compute path is the CUDA shared library ``libicp_b200.so`` (C ABI, include/icp_b200.h)
+built for sm_100a.  This module only marshals arguments: there is no CPU fallback, and
+importing it raises if the library is missing.
+
+Mirrored reference interfaces (Somatic-Cell/ice-crystal-phase):
+  make_phase_grid / PhaseGrid      hex_phase/include/ice_crystal/phase_table.hpp:118-127
+  rotation_from_quaternion         hex_phase/src/phase_table.cpp:11-21
+  parse_orientation_plan           hex_phase/src/orientation_plan.cpp:69-120
+  PhaseMassAccumulatorCuda         hex_phase/include/ice_crystal/phase_cuda.hpp:17-35
+    (.add fused with HexPrismTracer.trace, hex_trace/include/ice_crystal/hex_trace_cuda.hpp:18-41)
+  PhaseCdf.build                   include/rainbow/phase_cdf.hpp:50-96
+  generate_hex_record              hex_phase/apps/generate_hex_phase.cpp:79-154 (CUDA branch)
+"""
+from __future__ import annotations
+
+import ctypes as C
+import hashlib
+import math
+import os
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libicp_b200.so"
+
+ICP_OK, ICP_ERR_INVALID_ARGUMENT, ICP_ERR_AUDIT, ICP_ERR_CAPACITY, ICP_ERR_DEVICE, ICP_ERR_TIMEOUT, ICP_ERR_STATE = range(7)
+ICP_FP32, ICP_FP64 = 0, 1
+STATUS_NAMES = ["exhausted", "tail_tolerance_reached", "interaction_limit", "ambiguous_boundary", "invalid_input",
+                "numerical_failure", "output_overflow", "replay_mismatch"]
+
+
+class IcpError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+class InvalidArgument(IcpError, ValueError):
+    pass
+
+
+class AuditError(IcpError):
+    pass
+
+
+class CapacityError(IcpError):
+    pass
+
+
+_ERRORS = {ICP_ERR_INVALID_ARGUMENT: InvalidArgument, ICP_ERR_AUDIT: AuditError, ICP_ERR_CAPACITY: CapacityError}
+
+
+# ---------------------------------------------------------------- ABI structures
+class Grid(C.Structure):
+    _fields_ = [("nt", C.c_uint32), ("np", C.c_uint32), ("ki", C.c_double * 3), ("e0", C.c_double * 3),
+                ("e1", C.c_double * 3)]
+
+
+class TraceStats(C.Structure):
+    _fields_ = [("escaped", C.c_double), ("unresolved", C.c_double), ("point_axial", C.c_double),
+                ("forward_pole", C.c_double), ("backward_pole", C.c_double), ("max_ray_balance", C.c_double),
+                ("max_interface_balance", C.c_double), ("rays", C.c_uint64), ("outputs", C.c_uint64),
+                ("status_counts", C.c_uint64 * 8), ("rejected_rays", C.c_uint64), ("snapped", C.c_uint64),
+                ("near_edge", C.c_uint64), ("fallback_adds", C.c_uint64), ("max_batch_outputs", C.c_uint64),
+                ("invalid", C.c_uint64), ("encounters", C.c_uint64)]
+
+    def as_dict(self) -> dict:
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "status_counts"}
+        d["status_counts"] = {STATUS_NAMES[i]: int(self.status_counts[i]) for i in range(8)}
+        return d
+
+
+class Tuning(C.Structure):
+    _fields_ = [("block_threads", C.c_uint32), ("blocks_per_sm", C.c_uint32), ("hash_slots", C.c_uint32),
+                ("reserved", C.c_uint32)]
+
+
+class HexNode(C.Structure):
+    _fields_ = [("circumradius_mm", C.c_double), ("length_mm", C.c_double), ("rotation", C.c_double * 9),
+                ("exterior_index", C.c_double), ("interior_index", C.c_double), ("tail_tolerance", C.c_double),
+                ("balance_tolerance", C.c_double), ("area_weight", C.c_double), ("seed", C.c_uint64),
+                ("total_samples", C.c_uint64), ("first_sample", C.c_uint64), ("sample_count", C.c_uint64),
+                ("max_internal_hits", C.c_uint32), ("batch_size", C.c_uint32), ("precision", C.c_uint32),
+                ("reserved", C.c_uint32)]
+
+
+class CdfPolicy(C.Structure):
+    _fields_ = [("max_l1_error", C.c_double), ("max_lost_mass", C.c_double), ("max_coarsening_tv", C.c_double)]
+
+
+class CdfReport(C.Structure):
+    _fields_ = [("g_source", C.c_double), ("g_stored", C.c_double), ("coarsening_tv", C.c_double),
+                ("cdf_mass", C.c_double), ("l1_error", C.c_double), ("lost_mass", C.c_double),
+                ("maximum_cell_error", C.c_double), ("aggregation_relative_error", C.c_double),
+                ("fine_mass", C.c_double), ("fine_axial", C.c_double), ("lost_cells", C.c_uint64),
+                ("malformed", C.c_uint64), ("status", C.c_uint32), ("reserved", C.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+class HexRecordArgs(C.Structure):
+    _fields_ = [("circumradius_mm", C.c_double), ("length_mm", C.c_double), ("ki", C.c_double * 3),
+                ("exterior_index", C.c_double), ("interior_index", C.c_double), ("tail_tolerance", C.c_double),
+                ("balance_tolerance", C.c_double), ("nt", C.c_uint32), ("np", C.c_uint32), ("ct", C.c_uint32),
+                ("cp", C.c_uint32), ("max_internal_hits", C.c_uint32), ("batch_size", C.c_uint32),
+                ("max_output_records", C.c_uint64), ("precision", C.c_uint32), ("reserved", C.c_uint32),
+                ("policy", CdfPolicy), ("tuning", Tuning)]
+
+
+class Orientation(C.Structure):
+    _fields_ = [("quaternion", C.c_double * 4), ("weight", C.c_double), ("samples", C.c_uint64), ("seed", C.c_uint64)]
+
+
+class RecordReport(C.Structure):
+    _fields_ = [("trace", TraceStats), ("expected_area_mm2", C.c_double), ("escaped_area_mm2", C.c_double),
+                ("unresolved_area_mm2", C.c_double), ("histogram_mass_mm2", C.c_double),
+                ("histogram_axial_mm2", C.c_double), ("point_mass_mm2", C.c_double), ("point_axial_mm2", C.c_double),
+                ("forward_mass_mm2", C.c_double), ("backward_mass_mm2", C.c_double),
+                ("histogram_relative_error", C.c_double), ("cdf", CdfReport), ("seconds_trace", C.c_double),
+                ("seconds_cdf", C.c_double)]
+
+
+# ---------------------------------------------------------------- library loading
+_P = C.c_void_p
+_D = C.POINTER(C.c_double)
+_FUNCS = {
+    "icp_abi_version": (C.c_uint32, []),
+    "icp_kernel_launches": (C.c_ulonglong, []),
+    "icp_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
+    "icp_context_create": (C.c_int, [C.c_int, C.POINTER(_P)]),
+    "icp_context_destroy": (C.c_int, [_P]),
+    "icp_context_synchronize": (C.c_int, [_P]),
+    "icp_context_stream": (_P, [_P]),
+    "icp_device_alloc": (C.c_int, [_P, C.c_size_t, C.POINTER(_P)]),
+    "icp_device_free": (C.c_int, [_P, _P]),
+    "icp_memcpy_h2d": (C.c_int, [_P, _P, _P, C.c_size_t]),
+    "icp_memcpy_d2h": (C.c_int, [_P, _P, _P, C.c_size_t]),
+    "icp_memset_d": (C.c_int, [_P, _P, C.c_int, C.c_size_t]),
+    "icp_u_edges": (C.c_int, [C.c_uint32, _D]),
+    "icp_hex_node_area": (C.c_int, [C.POINTER(HexNode), C.POINTER(Grid), _D]),
+    "icp_hex_trace_bin": (C.c_int, [_P, C.POINTER(HexNode), C.POINTER(Grid), _P, _P, C.POINTER(TraceStats), _P,
+                                    C.POINTER(Tuning)]),
+    "icp_phase_cdf_build": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_uint32,
+                                      C.c_uint32, C.POINTER(CdfPolicy), _P, _P, C.POINTER(CdfReport)]),
+    "icp_hex_generate": (C.c_int, [_P, C.POINTER(HexRecordArgs), C.POINTER(Orientation), C.c_uint32, _D, _D, _D,
+                                   C.POINTER(RecordReport)]),
+}
+
+
+def _load() -> C.CDLL:
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python ice_crystal_phase_b200/build.py` "
+                          "(there is no CPU fallback)")
+    lib = C.CDLL(str(LIB_PATH))
+    for name, (res, args) in _FUNCS.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+LIB = _load()
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(4096)
+    LIB.icp_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(status: int) -> None:
+    if status != ICP_OK:
+        raise _ERRORS.get(status, IcpError)(status, last_error())
+
+
+def exported_symbols() -> list[str]:
+    return list(_FUNCS)
+
+
+def kernel_launches() -> int:
+    """CUDA kernels launched by libicp_b200 in this process."""
+    return int(LIB.icp_kernel_launches())
+
+
+# ---------------------------------------------------------------- host-side values
+def u_edges(nt: int) -> np.ndarray:
+    e = np.empty(nt + 1)
+    check(LIB.icp_u_edges(nt, e.ctypes.data_as(_D)))
+    return e
+
+
+def _normalize(a):
+    s = max(abs(a[0]), abs(a[1]), abs(a[2]))
+    if not (s > 0) or not math.isfinite(s):
+        raise ValueError("Invalid incident direction.")
+    a = [a[0] / s, a[1] / s, a[2] / s]
+    n = math.sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2])
+    return [a[0] / n, a[1] / n, a[2] / n]
+
+
+def _cross(a, b):
+    return [a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]]
+
+
+def make_frame(k) -> tuple[list, list, list]:
+    """Transverse frame of a direction (hex_trace/include/ice_crystal/math.hpp:61-69)."""
+    k = _normalize([float(x) for x in k])
+    ax, ay, az = abs(k[0]), abs(k[1]), abs(k[2])
+    a = [1.0, 0.0, 0.0] if (ax <= ay and ax <= az) else ([0.0, 1.0, 0.0] if ay <= az else [0.0, 0.0, 1.0])
+    d = k[0] * a[0] + k[1] * a[1] + k[2] * a[2]
+    e0 = _normalize([a[i] - k[i] * d for i in range(3)])
+    e1 = _normalize(_cross(k, e0))
+    return k, e0, e1
+
+
+@dataclass
+class PhaseGrid:
+    nt: int
+    np: int
+    ki: list
+    e0: list
+    e1: list
+    edges: np.ndarray
+
+    def abi(self) -> Grid:
+        g = Grid()
+        g.nt, g.np = self.nt, self.np
+        for i in range(3):
+            g.ki[i], g.e0[i], g.e1[i] = self.ki[i], self.e0[i], self.e1[i]
+        return g
+
+    def sampling_frame_columns(self) -> list:
+        return [[self.e0[r], self.e1[r], self.ki[r]] for r in range(3)]
+
+
+def make_phase_grid(nt: int, np_: int, ki) -> PhaseGrid:
+    if not nt or not np_ or nt * np_ > 0xFFFFFFFF or nt > 32 * 65535 or np_ > 0x7FFFFFFF:
+        raise ValueError("Unsupported phase grid dimensions.")
+    k, e0, e1 = make_frame(ki)
+    return PhaseGrid(nt, np_, k, e0, e1, u_edges(nt))
+
+
+def rotation_from_quaternion(w: float, x: float, y: float, z: float) -> list:
+    """Column-major body->ensemble rotation (hex_phase/src/phase_table.cpp:11-21)."""
+    n = w * w + x * x + y * y + z * z
+    if not math.isfinite(n) or abs(n - 1) > 2e-12:
+        raise ValueError("Quaternion must be unit length (w,x,y,z).")
+    k = 1 / math.sqrt(n)
+    w, x, y, z = w * k, x * k, y * k, z * k
+    return [1 - 2 * (y * y + z * z), 2 * (x * y + w * z), 2 * (x * z - w * y),
+            2 * (x * y - w * z), 1 - 2 * (x * x + z * z), 2 * (y * z + w * x),
+            2 * (x * z + w * y), 2 * (y * z - w * x), 1 - 2 * (x * x + y * y)]
+
+
+@dataclass
+class OrientationNode:
+    quaternion: tuple
+    weight: float
+    samples: int
+    seed: int
+
+
+@dataclass
+class OrientationPlan:
+    nodes: list
+    total_samples: int
+    input_weight_sum: float
+    source_sha256: str
+
+
+def parse_orientation_plan(text: str | bytes) -> OrientationPlan:
+    """qw,qx,qy,qz,weight,samples,seed CSV (hex_phase/src/orientation_plan.cpp:69-120)."""
+    raw = text.encode() if isinstance(text, str) else text
+    sha = hashlib.sha256(raw).hexdigest()
+    nodes, header, total = [], False, 0
+    s, c = 0.0, 0.0
+    for number, line in enumerate(raw.decode().split("\n"), 1):
+        line = line.strip(" \t\r")
+        if not line or line.startswith("#"):
+            continue
+        try:
+            if not header:
+                if line != "qw,qx,qy,qz,weight,samples,seed":
+                    raise ValueError("Expected CSV header qw,qx,qy,qz,weight,samples,seed.")
+                header = True
+                continue
+            cols = line.split(",")
+            if len(cols) != 7:
+                raise ValueError("Expected seven CSV fields.")
+            q = tuple(float(x.strip(" \t\r")) for x in cols[:4])
+            rotation_from_quaternion(*q)
+            weight, samples, seed = float(cols[4]), int(cols[5]), int(cols[6])
+            if not math.isfinite(weight) or not weight > 0 or samples <= 0:
+                raise ValueError("Weights and sample counts must be positive.")
+            if samples > 2 ** 64 - 1 - total or seed < 0 or seed >= 2 ** 64:
+                raise OverflowError("Planned sample count overflows.")
+            total += samples
+            y = weight - c
+            t = s + y
+            c = (t - s) - y
+            s = t
+            nodes.append(OrientationNode(q, weight, samples, seed))
+        except (ValueError, OverflowError) as e:
+            raise ValueError(f"Orientation CSV line {number}: {e}") from None
+    if not header or not nodes or not math.isfinite(s) or abs(s - 1) > 2e-12:
+        raise ValueError("Orientation number-probability weights must sum to one (within 2e-12).")
+    for n in nodes:
+        n.weight /= s
+    return OrientationPlan(nodes, total, s, sha)
+
+
+# ---------------------------------------------------------------- device context
+class Context:
+    """One CUDA device and one non-blocking stream (rainbow::CudaContext, src/cuda_driver.cpp:148-215)."""
+
+    def __init__(self, device: int = 0):
+        h = _P()
+        check(LIB.icp_context_create(device, C.byref(h)))
+        self.handle = h
+
+    def close(self) -> None:
+        if self.handle:
+            LIB.icp_context_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class DeviceArray:
+    """Context-owned device allocation of float64 (or raw bytes) for FFI-style callers."""
+
+    def __init__(self, ctx: Context, count: int, dtype=np.float64):
+        self.ctx, self.dtype, self.count = ctx, np.dtype(dtype), count
+        self.nbytes = max(1, count * self.dtype.itemsize)
+        p = _P()
+        check(LIB.icp_device_alloc(ctx.handle, self.nbytes, C.byref(p)))
+        self.ptr = p
+
+    def upload(self, host: np.ndarray) -> "DeviceArray":
+        a = np.ascontiguousarray(host, dtype=self.dtype)
+        assert a.size == self.count
+        check(LIB.icp_memcpy_h2d(self.ctx.handle, self.ptr, a.ctypes.data_as(_P), a.nbytes))
+        return self
+
+    def download(self) -> np.ndarray:
+        out = np.empty(self.count, dtype=self.dtype)
+        check(LIB.icp_memcpy_d2h(self.ctx.handle, out.ctypes.data_as(_P), self.ptr, out.nbytes))
+        return out
+
+    def zero(self) -> "DeviceArray":
+        check(LIB.icp_memset_d(self.ctx.handle, self.ptr, 0, self.nbytes))
+        return self
+
+    def free(self) -> None:
+        if self.ptr:
+            LIB.icp_device_free(self.ctx.handle, self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class PhaseMassAccumulatorCuda:
+    """FP64 cell-mass histogram fed by the fused hex trace+bin kernel.
+
+    ``add_hex_node`` replaces HexPrismTracer::trace + PhaseMassAccumulatorCuda::add for one
+    orientation node (all its ray batches in one launch); ``masses`` returns the cell masses
+    with the pole caps spread over the end rows (PhaseMassAccumulator::masses).
+    """
+
+    def __init__(self, ctx: Context, grid: PhaseGrid):
+        self.ctx, self.grid = ctx, grid
+        self.edges = DeviceArray(ctx, grid.nt + 1).upload(grid.edges)
+        self.mass = DeviceArray(ctx, grid.nt * grid.np).zero()
+        self.stats = TraceStats()
+        self.forward = 0.0
+        self.backward = 0.0
+        self.escaped_area = 0.0
+        self.unresolved_area = 0.0
+        self.point_axial = 0.0
+
+    def add_hex_node(self, prism: tuple[float, float], quaternion, weight: float, samples: int, seed: int,
+                     interior_index: float, exterior_index: float = 1.0, max_internal_hits: int = 1024,
+                     tail_tolerance: float = 1e-12, precision: int = ICP_FP32, balance_tolerance: float | None = None,
+                     first: int = 0, count: int | None = None, tuning: Tuning | None = None,
+                     batch_size: int = 4096) -> TraceStats:
+        n = HexNode()
+        n.circumradius_mm, n.length_mm = prism
+        for i, v in enumerate(rotation_from_quaternion(*quaternion)):
+            n.rotation[i] = v
+        n.exterior_index, n.interior_index = exterior_index, interior_index
+        n.tail_tolerance = tail_tolerance
+        n.balance_tolerance = balance_tolerance if balance_tolerance is not None else (
+            1e-10 if precision == ICP_FP64 else 1e-5)
+        n.seed, n.total_samples, n.first_sample = seed, samples, first
+        n.sample_count = samples - first if count is None else count
+        n.max_internal_hits, n.batch_size, n.precision = max_internal_hits, batch_size, precision
+        g = self.grid.abi()
+        area = C.c_double()
+        n.area_weight = 1.0
+        check(LIB.icp_hex_node_area(C.byref(n), C.byref(g), C.byref(area)))
+        n.area_weight = weight * area.value / float(samples)
+        s = TraceStats()
+        check(LIB.icp_hex_trace_bin(self.ctx.handle, C.byref(n), C.byref(g), self.edges.ptr, self.mass.ptr, C.byref(s),
+                                    None, C.byref(tuning) if tuning else None))
+        self.forward += n.area_weight * s.forward_pole
+        self.backward += n.area_weight * s.backward_pole
+        self.escaped_area += n.area_weight * s.escaped
+        self.unresolved_area += n.area_weight * s.unresolved
+        self.point_axial += n.area_weight * s.point_axial
+        for k, _ in TraceStats._fields_:
+            if k == "status_counts":
+                for i in range(8):
+                    self.stats.status_counts[i] += s.status_counts[i]
+            elif k.startswith("max_"):
+                setattr(self.stats, k, max(getattr(self.stats, k), getattr(s, k)))
+            else:
+                setattr(self.stats, k, getattr(self.stats, k) + getattr(s, k))
+        return s
+
+    def cell_mass(self) -> np.ndarray:
+        """Raw cell masses (without pole caps), theta-major."""
+        return self.mass.download()
+
+    def masses(self) -> np.ndarray:
+        m = self.cell_mass().reshape(self.grid.nt, self.grid.np)
+        m[0] += self.forward / self.grid.np
+        m[-1] += self.backward / self.grid.np
+        return m.reshape(-1)
+
+
+@dataclass
+class CdfResult:
+    phi: np.ndarray
+    theta: np.ndarray
+    u_edges: np.ndarray
+    report: dict
+
+
+class PhaseCdf:
+    """Stored CDF builder (rainbow::PhaseCdf::build + build_host_cdf arithmetic)."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+
+    def build(self, values, nt: int, np_: int, ct: int | None = None, cp: int | None = None,
+              forward: float = 0.0, backward: float = 0.0, density: bool = False, max_l1_error: float = 1e-10,
+              max_lost_mass: float = 1e-12, max_coarsening_tv: float = 1.0) -> CdfResult:
+        ct, cp = ct or nt, cp or np_
+        if isinstance(values, DeviceArray):
+            dv = values
+        else:
+            dv = DeviceArray(self.ctx, nt * np_).upload(np.asarray(values, dtype=np.float64).reshape(-1))
+        phi = DeviceArray(self.ctx, cp + 1)
+        theta = DeviceArray(self.ctx, cp * (ct + 1))
+        pol = CdfPolicy(max_l1_error, max_lost_mass, max_coarsening_tv)
+        rep = CdfReport()
+        check(LIB.icp_phase_cdf_build(self.ctx.handle, dv.ptr, 1 if density else 0, nt, np_, forward, backward, ct, cp,
+                                      C.byref(pol), phi.ptr, theta.ptr, C.byref(rep)))
+        edges = u_edges(nt)[:: nt // ct].copy()
+        return CdfResult(phi.download(), theta.download().reshape(cp, ct + 1), edges, rep.as_dict())
+
+
+@dataclass
+class HexRecordResult:
+    phi: np.ndarray
+    theta: np.ndarray
+    u_edges: np.ndarray
+    report: RecordReport
+    grid: PhaseGrid
+
+
+def generate_hex_record(ctx: Context, circumradius_mm: float, length_mm: float, ki, interior_index: float,
+                        nt: int, np_: int, plan: OrientationPlan, ct: int | None = None, cp: int | None = None,
+                        exterior_index: float = 1.0, max_internal_hits: int = 1024, tail_tolerance: float = 1e-12,
+                        precision: int = ICP_FP32, balance_tolerance: float | None = None, batch_size: int = 4096,
+                        max_output_records: int = 0, max_l1_error: float = 1e-10, max_lost_mass: float = 1e-12,
+                        max_coarsening_tv: float = 1.0, tuning: Tuning | None = None) -> HexRecordResult:
+    """One hex record through the host-buffer C-ABI entry (icp_hex_generate)."""
+    ct, cp = ct or nt, cp or np_
+    r = HexRecordArgs()
+    r.circumradius_mm, r.length_mm = circumradius_mm, length_mm
+    for i in range(3):
+        r.ki[i] = float(ki[i])
+    r.exterior_index, r.interior_index = exterior_index, interior_index
+    r.tail_tolerance = tail_tolerance
+    r.balance_tolerance = balance_tolerance if balance_tolerance is not None else (
+        1e-10 if precision == ICP_FP64 else 1e-5)
+    r.nt, r.np, r.ct, r.cp = nt, np_, ct, cp
+    r.max_internal_hits, r.batch_size, r.max_output_records = max_internal_hits, batch_size, max_output_records
+    r.precision = precision
+    r.policy = CdfPolicy(max_l1_error, max_lost_mass, max_coarsening_tv)
+    if tuning:
+        r.tuning = tuning
+    nodes = (Orientation * len(plan.nodes))()
+    for i, n in enumerate(plan.nodes):
+        for j in range(4):
+            nodes[i].quaternion[j] = n.quaternion[j]
+        nodes[i].weight, nodes[i].samples, nodes[i].seed = n.weight, n.samples, n.seed
+    phi = np.empty(cp + 1)
+    theta = np.empty(cp * (ct + 1))
+    u = np.empty(ct + 1)
+    rep = RecordReport()
+    check(LIB.icp_hex_generate(ctx.handle, C.byref(r), nodes, len(plan.nodes), phi.ctypes.data_as(_D),
+                               theta.ctypes.data_as(_D), u.ctypes.data_as(_D), C.byref(rep)))
+    return HexRecordResult(phi, theta.reshape(cp, ct + 1), u, rep, make_phase_grid(nt, np_, ki))

@@ -1,0 +1,659 @@
+// icp_capi.cu -- implementation of the C ABI declared in include/icp_b200.h.
+//
+// The context owns one CUDA stream and reusable device scratch (u edges, statistics,
+// CDF partials and counters).  Every entry point validates its arguments, enqueues on the
+// context stream and synchronises before returning, as the reference stage owners do
+// (hex_trace/src/hex_trace_cuda.cpp:127-174, hex_phase/src/phase_cuda.cpp:334-375,
+// src/phase_cdf.cpp:211-223).  Errors are reported as status codes with a per-thread
+// message (icp_last_error); nothing throws across the ABI.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/icp_b200.h"
+#include "../host/icp_host_math.hpp"
+#include "icp_internal.h"
+
+namespace icp {
+int hex_blocks_per_sm_f32(uint32_t slots, uint32_t nt, uint32_t threads);
+int hex_blocks_per_sm_f64(uint32_t slots, uint32_t nt, uint32_t threads);
+}
+
+using namespace icp;
+namespace H = icp::host;
+
+namespace {
+
+thread_local std::string g_error;
+std::atomic<unsigned long long> g_launches{0};
+
+int fail(int status, const char* fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_error = buf;
+    return status;
+}
+int ok()
+{
+    g_error.clear();
+    return ICP_OK;
+}
+
+#define ICP_CUDA(call)                                                                                  \
+    do {                                                                                                \
+        const cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess)                                                                          \
+            return fail(ICP_ERR_DEVICE, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                        __LINE__);                                                                      \
+    } while (0)
+
+// Device buffer that grows on demand and is reused across calls.
+struct Scratch {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t n)
+    {
+        if (n <= bytes) return cudaSuccess;
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        const cudaError_t e = cudaMalloc(&ptr, n);
+        if (e == cudaSuccess) bytes = n;
+        return e;
+    }
+    void release()
+    {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
+
+__global__ void edges_to_float(const double* in, float* out, uint32_t n)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (float)in[i];
+}
+
+} // namespace
+
+struct icp_context {
+    int device = 0;
+    int sms = 0;
+    cudaStream_t stream = nullptr;
+    Scratch stats, edges_f, cdf_partial, cdf_report, cdf_sync, cdf_colsum;
+    Scratch rec_edges, rec_mass, rec_phi, rec_theta, rec_batch;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+extern "C" {
+
+uint32_t icp_abi_version(void) { return ICP_ABI_VERSION; }
+
+unsigned long long icp_kernel_launches(void) { return g_launches.load(); }
+
+size_t icp_last_error(char* buffer, size_t n)
+{
+    if (buffer && n) {
+        const size_t m = std::min(n - 1, g_error.size());
+        std::memcpy(buffer, g_error.data(), m);
+        buffer[m] = '\0';
+    }
+    return g_error.size();
+}
+
+int icp_context_create(int device, icp_context** out)
+{
+    if (!out) return fail(ICP_ERR_INVALID_ARGUMENT, "icp_context_create: null output pointer");
+    *out = nullptr;
+    int count = 0;
+    ICP_CUDA(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count)
+        return fail(ICP_ERR_INVALID_ARGUMENT, "icp_context_create: device %d outside [0,%d)", device, count);
+    ICP_CUDA(cudaSetDevice(device));
+    int major = 0;
+    ICP_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+    if (major < 10)
+        return fail(ICP_ERR_DEVICE, "icp_context_create: device %d is compute capability %d.x; this library targets sm_100a",
+                    device, major);
+    auto* c = new icp_context();
+    c->device = device;
+    cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
+    if (e != cudaSuccess) {
+        icp_context_destroy(c);
+        return fail(ICP_ERR_DEVICE, "icp_context_create: %s", cudaGetErrorString(e));
+    }
+    *out = c;
+    return ok();
+}
+
+int icp_context_destroy(icp_context* c)
+{
+    if (!c) return ok();
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    Scratch* all[] = {&c->stats, &c->edges_f, &c->cdf_partial, &c->cdf_report, &c->cdf_sync, &c->cdf_colsum,
+                      &c->rec_edges, &c->rec_mass, &c->rec_phi, &c->rec_theta, &c->rec_batch};
+    for (Scratch* s : all) s->release();
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return ok();
+}
+
+int icp_context_synchronize(icp_context* c)
+{
+    if (!c) return fail(ICP_ERR_INVALID_ARGUMENT, "null context");
+    ICP_CUDA(cudaSetDevice(c->device));
+    ICP_CUDA(cudaStreamSynchronize(c->stream));
+    return ok();
+}
+
+void* icp_context_stream(icp_context* c) { return c ? (void*)c->stream : nullptr; }
+
+int icp_device_alloc(icp_context* c, size_t bytes, void** out)
+{
+    if (!c || !out) return fail(ICP_ERR_INVALID_ARGUMENT, "icp_device_alloc: null argument");
+    ICP_CUDA(cudaSetDevice(c->device));
+    ICP_CUDA(cudaMalloc(out, bytes ? bytes : 1));
+    return ok();
+}
+int icp_device_free(icp_context* c, void* ptr)
+{
+    if (!c) return fail(ICP_ERR_INVALID_ARGUMENT, "icp_device_free: null context");
+    ICP_CUDA(cudaSetDevice(c->device));
+    ICP_CUDA(cudaStreamSynchronize(c->stream));
+    ICP_CUDA(cudaFree(ptr));
+    return ok();
+}
+int icp_memcpy_h2d(icp_context* c, void* dst, const void* src, size_t bytes)
+{
+    if (!c) return fail(ICP_ERR_INVALID_ARGUMENT, "null context");
+    ICP_CUDA(cudaSetDevice(c->device));
+    ICP_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream));
+    ICP_CUDA(cudaStreamSynchronize(c->stream));
+    return ok();
+}
+int icp_memcpy_d2h(icp_context* c, void* dst, const void* src, size_t bytes)
+{
+    if (!c) return fail(ICP_ERR_INVALID_ARGUMENT, "null context");
+    ICP_CUDA(cudaSetDevice(c->device));
+    ICP_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream));
+    ICP_CUDA(cudaStreamSynchronize(c->stream));
+    return ok();
+}
+int icp_memset_d(icp_context* c, void* dst, int value, size_t bytes)
+{
+    if (!c) return fail(ICP_ERR_INVALID_ARGUMENT, "null context");
+    ICP_CUDA(cudaSetDevice(c->device));
+    ICP_CUDA(cudaMemsetAsync(dst, value, bytes, c->stream));
+    ICP_CUDA(cudaStreamSynchronize(c->stream));
+    return ok();
+}
+
+int icp_u_edges(uint32_t nt, double* out)
+{
+    if (!out || nt == 0) return fail(ICP_ERR_INVALID_ARGUMENT, "icp_u_edges: theta_count must be positive");
+    std::vector<double> e;
+    if (!H::u_edges(nt, e)) return fail(ICP_ERR_INVALID_ARGUMENT, "Angular cells cannot be represented in binary64.");
+    std::memcpy(out, e.data(), e.size() * sizeof(double));
+    return ok();
+}
+
+} // extern "C"
+
+namespace {
+
+bool grid_valid(const icp_grid* g)
+{
+    if (!g || !g->nt || !g->np || (uint64_t)g->nt * g->np > 0xffffffffull) return false;
+    const H::V k{g->ki[0], g->ki[1], g->ki[2]};
+    const H::Frame f{{g->e0[0], g->e0[1], g->e0[2]}, {g->e1[0], g->e1[1], g->e1[2]}};
+    return H::frame_valid(f, k);
+}
+
+struct NodeSetup {
+    H::V k;
+    H::Frame kf;
+    H::FaceTable faces;
+};
+
+int node_setup(const icp_hex_node* n, const icp_grid* g, NodeSetup& s)
+{
+    if (!H::rotation_valid(n->rotation)) return fail(ICP_ERR_INVALID_ARGUMENT, "Invalid orientation rotation.");
+    const H::V gk{g->ki[0], g->ki[1], g->ki[2]};
+    if (!H::normalize(H::rotate_inverse(n->rotation, gk), s.k) || !H::make_frame(s.k, s.kf))
+        return fail(ICP_ERR_INVALID_ARGUMENT, "Incident direction must be finite and nonzero.");
+    const double R = n->circumradius_mm, L = n->length_mm;
+    const double half = 0.5 * (L / R);
+    if (!(H::finite(R) && H::finite(L) && R > 0 && L > 0 && H::finite(half) && half > 0 && R * R > 0 && R * L > 0))
+        return fail(ICP_ERR_INVALID_ARGUMENT, "Invalid hex prism geometry.");
+    s.faces = H::prism_faces(R, L, s.k);
+    if (!(s.faces.area > 0) || !H::finite(s.faces.area)) return fail(ICP_ERR_INVALID_ARGUMENT, "Invalid projected area.");
+    return ICP_OK;
+}
+
+} // namespace
+
+extern "C" int icp_hex_node_area(const icp_hex_node* node, const icp_grid* grid, double* area)
+{
+    if (!node || !grid || !area) return fail(ICP_ERR_INVALID_ARGUMENT, "icp_hex_node_area: null argument");
+    if (!grid_valid(grid)) return fail(ICP_ERR_INVALID_ARGUMENT, "Malformed phase grid.");
+    NodeSetup s;
+    if (const int r = node_setup(node, grid, s)) return r;
+    *area = s.faces.area;
+    return ok();
+}
+
+namespace {
+
+int ensure_float_edges(icp_context* c, const double* d_edges, uint32_t nt)
+{
+    ICP_CUDA(c->edges_f.ensure(sizeof(float) * (nt + 1)));
+    edges_to_float<<<(nt + 1 + 255) / 256, 256, 0, c->stream>>>(d_edges, (float*)c->edges_f.ptr, nt + 1);
+    ++g_launches;
+    ICP_CUDA(cudaGetLastError());
+    return ICP_OK;
+}
+
+void stats_accumulate(const unsigned char* raw, icp_trace_stats* out)
+{
+    // DevStats layout (icp_hex_kernel.cuh)
+    struct Raw {
+        unsigned long long esc[2], unres[2], fwd[2], bwd[2];
+        double axial;
+        unsigned long long max_bal_bits, max_iface_bits;
+        unsigned long long rays, outputs, status[8], rejected, snapped, near_edge, fallback, invalid;
+        unsigned long long encounters;
+    } r;
+    std::memcpy(&r, raw, sizeof r);
+    auto fx = [](const unsigned long long* v) { return (std::ldexp((double)v[1], 64) + (double)v[0]) * 0x1p-44; };
+    out->escaped += fx(r.esc);
+    out->unresolved += fx(r.unres);
+    out->forward_pole += fx(r.fwd);
+    out->backward_pole += fx(r.bwd);
+    out->point_axial += r.axial;
+    double mb, mi;
+    std::memcpy(&mb, &r.max_bal_bits, 8);
+    std::memcpy(&mi, &r.max_iface_bits, 8);
+    out->max_ray_balance = std::max(out->max_ray_balance, mb);
+    out->max_interface_balance = std::max(out->max_interface_balance, mi);
+    out->rays += r.rays;
+    out->outputs += r.outputs;
+    for (int i = 0; i < 8; ++i) out->status_counts[i] += r.status[i];
+    out->rejected_rays += r.rejected;
+    out->snapped += r.snapped;
+    out->near_edge += r.near_edge;
+    out->fallback_adds += r.fallback;
+    out->invalid += r.invalid;
+    out->encounters += r.encounters;
+}
+
+__global__ void max_u32(const uint32_t* v, uint64_t n, unsigned long long* out)
+{
+    unsigned long long m = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        m = v[i] > m ? v[i] : m;
+    for (int o = 16; o; o >>= 1) {
+        const unsigned long long t = __shfl_xor_sync(0xffffffffu, m, o);
+        m = t > m ? t : m;
+    }
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+}
+
+} // namespace
+
+extern "C" int icp_hex_trace_bin(icp_context* c, const icp_hex_node* n, const icp_grid* g, const double* d_edges,
+                                 double* d_mass, icp_trace_stats* stats, uint32_t* d_batch_out, const icp_tuning* tune)
+{
+    if (!c || !n || !g || !d_edges || !d_mass || !stats) return fail(ICP_ERR_INVALID_ARGUMENT, "icp_hex_trace_bin: null argument");
+    if (!grid_valid(g)) return fail(ICP_ERR_INVALID_ARGUMENT, "Malformed phase grid.");
+    NodeSetup s;
+    if (const int r = node_setup(n, g, s)) return r;
+    if (!(n->exterior_index > 0 && n->interior_index > 0 && H::finite(n->exterior_index) && H::finite(n->interior_index)))
+        return fail(ICP_ERR_INVALID_ARGUMENT, "Invalid refractive indices.");
+    if (!(H::finite(n->tail_tolerance) && n->tail_tolerance >= 0 && n->tail_tolerance < 1))
+        return fail(ICP_ERR_INVALID_ARGUMENT, "Invalid tail tolerance.");
+    if (!n->total_samples || !n->max_internal_hits || !n->batch_size)
+        return fail(ICP_ERR_INVALID_ARGUMENT, "Sample count, hit limit and batch size must be positive.");
+    if (n->sample_count == 0) return ok();
+    if (n->first_sample >= n->total_samples || n->sample_count > n->total_samples - n->first_sample)
+        return fail(ICP_ERR_INVALID_ARGUMENT, "Batch is outside the global incident-sample range.");
+    if (!(n->area_weight > 0) || !H::finite(n->area_weight))
+        return fail(ICP_ERR_INVALID_ARGUMENT, "Invalid orientation / area weight.");
+    if (n->precision != ICP_FP32 && n->precision != ICP_FP64) return fail(ICP_ERR_INVALID_ARGUMENT, "Unknown precision.");
+    ICP_CUDA(cudaSetDevice(c->device));
+
+    uint32_t threads = tune && tune->block_threads ? tune->block_threads : 256u;
+    if (threads < 64 || threads > 256 || threads % 32) return fail(ICP_ERR_INVALID_ARGUMENT, "block_threads must be 64..256, multiple of 32");
+    uint32_t slots = 4096u;
+    if (tune && tune->hash_slots) slots = tune->hash_slots == 1 ? 0u : tune->hash_slots;
+    if (slots & (slots - 1)) return fail(ICP_ERR_INVALID_ARGUMENT, "hash_slots must be a power of two");
+    const bool f32 = n->precision == ICP_FP32;
+    int per_sm = f32 ? hex_blocks_per_sm_f32(slots, g->nt, threads) : hex_blocks_per_sm_f64(slots, g->nt, threads);
+    if (per_sm <= 0) return fail(ICP_ERR_DEVICE, "hex trace kernel cannot be resident with %u threads / %u slots", threads, slots);
+    if (tune && tune->blocks_per_sm) per_sm = std::min<int>(per_sm, (int)tune->blocks_per_sm);
+    const uint32_t warps_per_block = threads / 32;
+    // at least 64 rays per warp when the range is small; at most 2^16 per warp per launch
+    uint64_t blocks = (uint64_t)per_sm * c->sms;
+    blocks = std::max<uint64_t>(1, std::min<uint64_t>(blocks, (n->sample_count + 64ull * warps_per_block - 1) / (64ull * warps_per_block)));
+    const uint64_t piece = blocks * warps_per_block * 65536ull;
+
+    ICP_CUDA(c->stats.ensure(hex_stats_bytes()));
+    ICP_CUDA(cudaMemsetAsync(c->stats.ptr, 0, hex_stats_bytes(), c->stream));
+    if (f32)
+        if (const int r = ensure_float_edges(c, d_edges, g->nt)) return r;
+
+    HexLaunch L{};
+    L.half_len = 0.5 * (n->length_mm / n->circumradius_mm);
+    L.k[0] = s.k.x; L.k[1] = s.k.y; L.k[2] = s.k.z;
+    L.ke0[0] = s.kf.e0.x; L.ke0[1] = s.kf.e0.y; L.ke0[2] = s.kf.e0.z;
+    for (int f = 0; f < 8; ++f) L.cum[f] = s.faces.cum[f];
+    L.face_mask = s.faces.mask;
+    L.area = s.faces.area;
+    L.n_ext = n->exterior_index;
+    L.n_int = n->interior_index;
+    L.tail = n->tail_tolerance;
+    L.bal_tol = n->balance_tolerance;
+    L.seed = n->seed;
+    L.total = n->total_samples;
+    L.max_hits = n->max_internal_hits;
+    L.batch_size = n->batch_size;
+    L.batch_out = d_batch_out;
+    std::memcpy(L.rot, n->rotation, sizeof L.rot);
+    std::memcpy(L.ki, g->ki, sizeof L.ki);
+    std::memcpy(L.e0, g->e0, sizeof L.e0);
+    std::memcpy(L.e1, g->e1, sizeof L.e1);
+    L.nt = g->nt;
+    L.np = g->np;
+    L.edges_d = d_edges;
+    L.edges_f = (const float*)c->edges_f.ptr;
+    L.mass = d_mass;
+    L.to_mass = n->area_weight * 0x1p-44;
+    L.stats = c->stats.ptr;
+    L.hash_slots = slots;
+    L.block_threads = threads;
+    L.blocks = (uint32_t)blocks;
+    for (uint64_t off = 0; off < n->sample_count; off += piece) {
+        L.first = n->first_sample + off;
+        L.count = std::min<uint64_t>(piece, n->sample_count - off);
+        const int e = f32 ? launch_hex_f32(L, c->stream) : launch_hex_f64(L, c->stream);
+        ++g_launches;
+        if (e) return fail(ICP_ERR_DEVICE, "hex trace launch failed: %s", cudaGetErrorString((cudaError_t)e));
+    }
+    std::vector<unsigned char> raw(hex_stats_bytes());
+    ICP_CUDA(cudaMemcpyAsync(raw.data(), c->stats.ptr, raw.size(), cudaMemcpyDeviceToHost, c->stream));
+    ICP_CUDA(cudaStreamSynchronize(c->stream));
+    stats_accumulate(raw.data(), stats);
+    return ok();
+}
+
+namespace {
+
+int choose_cw(icp_context* c, uint32_t ct, uint32_t cp, uint32_t& cw)
+{
+    // smallest strip width whose grid fits co-resident, at least ceil(cp / SMs)
+    uint32_t w = std::max<uint32_t>(1u, (cp + c->sms - 1) / c->sms);
+    for (; w <= cp; ++w) {
+        const size_t smem = sizeof(double) * ((size_t)ct * w + w + 1);
+        if (smem > 200 * 1024) break;
+        const uint32_t blocks = (cp + w - 1) / w;
+        if ((int)blocks <= cdf_max_coresident_blocks(smem, c->device)) {
+            cw = w;
+            return ICP_OK;
+        }
+    }
+    return fail(ICP_ERR_CAPACITY, "CDF strip for %u theta rows does not fit shared memory with a co-resident grid", ct);
+}
+
+} // namespace
+
+extern "C" int icp_phase_cdf_build(icp_context* c, const double* d_values, uint32_t kind, uint32_t nt, uint32_t np,
+                                   double fwd, double bwd, uint32_t ct, uint32_t cp, const icp_cdf_policy* policy,
+                                   double* d_phi, double* d_theta, icp_cdf_report* report)
+{
+    if (!c || !d_values || !d_phi || !d_theta || !report || !policy)
+        return fail(ICP_ERR_INVALID_ARGUMENT, "icp_phase_cdf_build: null argument");
+    std::memset(report, 0, sizeof *report);
+    const icp_cdf_policy& p = *policy;
+    if (!(H::finite(p.max_l1_error) && p.max_l1_error >= 0 && p.max_l1_error <= 2 && H::finite(p.max_lost_mass) &&
+          p.max_lost_mass >= 0 && p.max_lost_mass <= 1 && H::finite(p.max_coarsening_tv) && p.max_coarsening_tv >= 0 &&
+          p.max_coarsening_tv <= 1))
+        return fail(ICP_ERR_INVALID_ARGUMENT, "Invalid CDF quality policy.");
+    if (kind > 1) return fail(ICP_ERR_INVALID_ARGUMENT, "Unknown CDF input kind.");
+    if (!nt || !np || (uint64_t)nt * np > 0xffffffffull)
+        return fail(ICP_ERR_INVALID_ARGUMENT, "Unsupported phase grid dimensions.");
+    if (!ct || !cp || ct > nt || cp > np || nt % ct || np % cp)
+        return fail(ICP_ERR_INVALID_ARGUMENT, "Storage dimensions must divide histogram dimensions.");
+    if (!(fwd >= 0) || !(bwd >= 0) || !H::finite(fwd) || !H::finite(bwd))
+        return fail(ICP_ERR_INVALID_ARGUMENT, "Invalid pole masses.");
+    const double fa = fwd / np, ba = bwd / np;
+    if ((fwd > 0 && !(fa > 0)) || (bwd > 0 && !(ba > 0))) return fail(ICP_ERR_AUDIT, "Pole weight underflow.");
+    ICP_CUDA(cudaSetDevice(c->device));
+    std::vector<double> edges;
+    if (!H::u_edges(nt, edges)) return fail(ICP_ERR_INVALID_ARGUMENT, "Angular cells cannot be represented in binary64.");
+    uint32_t cw = 0;
+    if (const int r = choose_cw(c, ct, cp, cw)) return r;
+    const uint32_t blocks = (cp + cw - 1) / cw;
+    ICP_CUDA(c->rec_edges.ensure(sizeof(double) * (nt + 1)));
+    ICP_CUDA(c->cdf_partial.ensure(cdf_partial_bytes() * blocks));
+    ICP_CUDA(c->cdf_report.ensure(sizeof(CdfDeviceReport)));
+    ICP_CUDA(c->cdf_sync.ensure(2 * sizeof(unsigned)));
+    ICP_CUDA(c->cdf_colsum.ensure(sizeof(double) * cp));
+    ICP_CUDA(cudaMemcpyAsync(c->rec_edges.ptr, edges.data(), sizeof(double) * (nt + 1), cudaMemcpyHostToDevice, c->stream));
+    ICP_CUDA(cudaMemsetAsync(c->cdf_sync.ptr, 0, 2 * sizeof(unsigned), c->stream));
+    ICP_CUDA(cudaMemsetAsync(c->cdf_report.ptr, 0, sizeof(CdfDeviceReport), c->stream));
+    CdfLaunch L{};
+    L.values = d_values;
+    L.edges = (const double*)c->rec_edges.ptr;
+    L.phi = d_phi;
+    L.theta = d_theta;
+    L.colsum = (double*)c->cdf_colsum.ptr;
+    L.partial = c->cdf_partial.ptr;
+    L.report = (CdfDeviceReport*)c->cdf_report.ptr;
+    L.sync = (unsigned*)c->cdf_sync.ptr;
+    L.kind = kind;
+    L.nt = nt;
+    L.np = np;
+    L.ct = ct;
+    L.cp = cp;
+    L.cw = cw;
+    L.fwd_add = fa;
+    L.bwd_add = ba;
+    const int e = launch_cdf_build(L, c->stream);
+    ++g_launches;
+    if (e) return fail(ICP_ERR_DEVICE, "CDF launch failed: %s", cudaGetErrorString((cudaError_t)e));
+    CdfDeviceReport r{};
+    ICP_CUDA(cudaMemcpyAsync(&r, c->cdf_report.ptr, sizeof r, cudaMemcpyDeviceToHost, c->stream));
+    ICP_CUDA(cudaStreamSynchronize(c->stream));
+    if (r.timeout) return fail(ICP_ERR_TIMEOUT, "CDF grid barrier gave up waiting (co-residency violated?)");
+    report->fine_mass = r.fine_mass;
+    report->fine_axial = r.fine_axial;
+    report->g_source = r.fine_axial / r.fine_mass;
+    report->aggregation_relative_error = std::fabs(r.stored_mass / r.fine_mass - 1);
+    report->coarsening_tv = r.tv;
+    report->l1_error = r.l1;
+    report->lost_mass = r.lost;
+    report->maximum_cell_error = r.max_err;
+    report->cdf_mass = r.recovered;
+    report->g_stored = r.axial / r.recovered;
+    report->lost_cells = r.lost_cells;
+    report->malformed = r.malformed;
+    // quality gates of build_host_cdf (hex_phase/src/phase_table.cpp:114-185)
+    int status = ICP_OK;
+    if (r.invalid) status = fail(ICP_ERR_INVALID_ARGUMENT, "Negative/nonfinite mass.");
+    else if (!(r.fine_mass > 0) || !H::finite(r.fine_mass) || !H::finite(r.fine_axial))
+        status = fail(ICP_ERR_AUDIT, "Empty/nonfinite histogram.");
+    else if (!H::finite(report->coarsening_tv) || report->coarsening_tv > p.max_coarsening_tv ||
+             report->aggregation_relative_error > 1e-12)
+        status = fail(ICP_ERR_AUDIT, "Conservative coarsening audit failed.");
+    else if (r.underflow) status = fail(ICP_ERR_AUDIT, "CDF weight underflow.");
+    else if (!(r.total > 0) || !H::finite(r.total)) status = fail(ICP_ERR_AUDIT, "Invalid CDF total.");
+    else if (r.malformed) status = fail(ICP_ERR_AUDIT, "Malformed CDF; refusing repair.");
+    else if (report->l1_error > p.max_l1_error || report->lost_mass > p.max_lost_mass ||
+             std::fabs(report->cdf_mass - 1) > 1e-10 || !H::finite(report->g_stored) ||
+             !(report->g_stored > -1 && report->g_stored < 1))
+        status = fail(ICP_ERR_AUDIT, "CDF mass / HG audit failed.");
+    report->status = (uint32_t)status;
+    return status == ICP_OK ? ok() : status;
+}
+
+extern "C" int icp_hex_generate(icp_context* c, const icp_hex_record* rec, const icp_orientation* nodes, uint32_t count,
+                                double* h_phi, double* h_theta, double* h_u, icp_record_report* report)
+{
+    if (!c || !rec || !nodes || !count || !h_phi || !h_theta || !h_u || !report)
+        return fail(ICP_ERR_INVALID_ARGUMENT, "icp_hex_generate: null argument");
+    std::memset(report, 0, sizeof *report);
+    ICP_CUDA(cudaSetDevice(c->device));
+    // grid (make_phase_grid, hex_phase/src/phase_table.cpp:22-29)
+    icp_grid g{};
+    g.nt = rec->nt;
+    g.np = rec->np;
+    H::V k;
+    H::Frame kf;
+    if (!rec->nt || !rec->np || (uint64_t)rec->nt * rec->np > 0xffffffffull || rec->nt > 32u * 65535u || rec->np > 0x7fffffffu)
+        return fail(ICP_ERR_INVALID_ARGUMENT, "Unsupported phase grid dimensions.");
+    if (!H::normalize({rec->ki[0], rec->ki[1], rec->ki[2]}, k) || !H::make_frame(k, kf))
+        return fail(ICP_ERR_INVALID_ARGUMENT, "Invalid incident direction.");
+    g.ki[0] = k.x; g.ki[1] = k.y; g.ki[2] = k.z;
+    g.e0[0] = kf.e0.x; g.e0[1] = kf.e0.y; g.e0[2] = kf.e0.z;
+    g.e1[0] = kf.e1.x; g.e1[1] = kf.e1.y; g.e1[2] = kf.e1.z;
+    std::vector<double> edges;
+    if (!H::u_edges(rec->nt, edges)) return fail(ICP_ERR_INVALID_ARGUMENT, "Angular cells cannot be represented in binary64.");
+    const uint64_t cells = (uint64_t)rec->nt * rec->np;
+    ICP_CUDA(c->rec_edges.ensure(sizeof(double) * (rec->nt + 1)));
+    ICP_CUDA(c->rec_mass.ensure(sizeof(double) * cells));
+    ICP_CUDA(c->rec_phi.ensure(sizeof(double) * (rec->cp + 1)));
+    ICP_CUDA(c->rec_theta.ensure(sizeof(double) * (size_t)rec->cp * (rec->ct + 1)));
+    ICP_CUDA(cudaMemcpyAsync(c->rec_edges.ptr, edges.data(), sizeof(double) * (rec->nt + 1), cudaMemcpyHostToDevice, c->stream));
+    ICP_CUDA(cudaMemsetAsync(c->rec_mass.ptr, 0, sizeof(double) * cells, c->stream));
+    // preflight all nodes (generate_hex_phase.cpp:82-88)
+    std::vector<icp_hex_node> hn(count);
+    H::KahanSum expected;
+    uint64_t max_batches = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        icp_hex_node& n = hn[i];
+        std::memset(&n, 0, sizeof n);
+        const icp_orientation& o = nodes[i];
+        if (!H::rotation(o.quaternion[0], o.quaternion[1], o.quaternion[2], o.quaternion[3], n.rotation))
+            return fail(ICP_ERR_INVALID_ARGUMENT, "Quaternion must be unit length (w,x,y,z).");
+        if (!H::finite(o.weight) || !(o.weight > 0) || !o.samples)
+            return fail(ICP_ERR_INVALID_ARGUMENT, "Invalid orientation node.");
+        n.circumradius_mm = rec->circumradius_mm;
+        n.length_mm = rec->length_mm;
+        n.exterior_index = rec->exterior_index;
+        n.interior_index = rec->interior_index;
+        n.tail_tolerance = rec->tail_tolerance;
+        n.balance_tolerance = rec->balance_tolerance;
+        n.seed = o.seed;
+        n.total_samples = o.samples;
+        n.first_sample = 0;
+        n.sample_count = o.samples;
+        n.max_internal_hits = rec->max_internal_hits;
+        n.batch_size = rec->batch_size ? rec->batch_size : 4096u;
+        n.precision = rec->precision;
+        double area = 0;
+        if (const int r = icp_hex_node_area(&n, &g, &area)) return r;
+        const double weight = o.weight * area;
+        if (!(weight > 0) || !H::finite(weight) || !(weight / double(o.samples) > 0))
+            return fail(ICP_ERR_INVALID_ARGUMENT, "Orientation area weight over/underflow.");
+        expected.add(weight);
+        n.area_weight = o.weight * area / double(o.samples);
+        max_batches = std::max<uint64_t>(max_batches, (o.samples + n.batch_size - 1) / n.batch_size);
+    }
+    report->expected_area_mm2 = expected.value;
+    uint32_t* d_batch = nullptr;
+    unsigned long long* d_max = nullptr;
+    if (rec->max_output_records) {
+        ICP_CUDA(c->rec_batch.ensure(sizeof(uint32_t) * max_batches + 64));
+        d_batch = (uint32_t*)c->rec_batch.ptr;
+        d_max = (unsigned long long*)((char*)c->rec_batch.ptr + ((sizeof(uint32_t) * max_batches + 7) / 8) * 8);
+    }
+    ICP_CUDA(cudaEventRecord(c->ev0, c->stream));
+    H::KahanSum escaped, unresolved;
+    icp_trace_stats& T = report->trace;
+    uint64_t max_batch_out = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        icp_trace_stats s{};
+        if (d_batch) ICP_CUDA(cudaMemsetAsync(d_batch, 0, sizeof(uint32_t) * max_batches + 8, c->stream));
+        if (const int r = icp_hex_trace_bin(c, &hn[i], &g, (const double*)c->rec_edges.ptr, (double*)c->rec_mass.ptr, &s,
+                                            d_batch, &rec->tuning))
+            return r;
+        if (d_batch) {
+            const uint64_t nb = (hn[i].total_samples + hn[i].batch_size - 1) / hn[i].batch_size;
+            max_u32<<<std::max<uint64_t>(1, std::min<uint64_t>(1024, (nb + 255) / 256)), 256, 0, c->stream>>>(d_batch, nb, d_max);
+            ++g_launches;
+            unsigned long long m = 0;
+            ICP_CUDA(cudaMemcpyAsync(&m, d_max, 8, cudaMemcpyDeviceToHost, c->stream));
+            ICP_CUDA(cudaStreamSynchronize(c->stream));
+            max_batch_out = std::max<uint64_t>(max_batch_out, m);
+        }
+        const double w = hn[i].area_weight;
+        escaped.add(w * s.escaped);
+        unresolved.add(w * s.unresolved);
+        report->point_axial_mm2 += w * s.point_axial;
+        report->forward_mass_mm2 += w * s.forward_pole;
+        report->backward_mass_mm2 += w * s.backward_pole;
+        T.escaped += s.escaped;
+        T.unresolved += s.unresolved;
+        T.point_axial += s.point_axial;
+        T.forward_pole += s.forward_pole;
+        T.backward_pole += s.backward_pole;
+        T.max_ray_balance = std::max(T.max_ray_balance, s.max_ray_balance);
+        T.max_interface_balance = std::max(T.max_interface_balance, s.max_interface_balance);
+        T.rays += s.rays;
+        T.outputs += s.outputs;
+        for (int q = 0; q < 8; ++q) T.status_counts[q] += s.status_counts[q];
+        T.rejected_rays += s.rejected_rays;
+        T.snapped += s.snapped;
+        T.near_edge += s.near_edge;
+        T.fallback_adds += s.fallback_adds;
+        T.invalid += s.invalid;
+        T.encounters += s.encounters;
+    }
+    T.max_batch_outputs = max_batch_out;
+    ICP_CUDA(cudaEventRecord(c->ev1, c->stream));
+    report->escaped_area_mm2 = escaped.value;
+    report->unresolved_area_mm2 = unresolved.value;
+    report->point_mass_mm2 = escaped.value;
+    ICP_CUDA(cudaEventSynchronize(c->ev1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    report->seconds_trace = ms * 1e-3;
+    if (rec->max_output_records && max_batch_out > rec->max_output_records)
+        return fail(ICP_ERR_CAPACITY, "Output memory budget exceeded; batch not silently reduced.");
+    ICP_CUDA(cudaEventRecord(c->ev0, c->stream));
+    const int cr = icp_phase_cdf_build(c, (const double*)c->rec_mass.ptr, ICP_CDF_MASS, rec->nt, rec->np,
+                                       report->forward_mass_mm2, report->backward_mass_mm2, rec->ct, rec->cp, &rec->policy,
+                                       (double*)c->rec_phi.ptr, (double*)c->rec_theta.ptr, &report->cdf);
+    ICP_CUDA(cudaEventRecord(c->ev1, c->stream));
+    report->histogram_mass_mm2 = report->cdf.fine_mass;
+    report->histogram_axial_mm2 = report->cdf.fine_axial;
+    if (cr != ICP_OK) return cr;
+    ICP_CUDA(cudaMemcpyAsync(h_phi, c->rec_phi.ptr, sizeof(double) * (rec->cp + 1), cudaMemcpyDeviceToHost, c->stream));
+    ICP_CUDA(cudaMemcpyAsync(h_theta, c->rec_theta.ptr, sizeof(double) * (size_t)rec->cp * (rec->ct + 1),
+                             cudaMemcpyDeviceToHost, c->stream));
+    ICP_CUDA(cudaStreamSynchronize(c->stream));
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    report->seconds_cdf = ms * 1e-3;
+    const uint32_t dt = rec->nt / rec->ct;
+    for (uint32_t i = 0; i <= rec->ct; ++i) h_u[i] = edges[(size_t)i * dt];
+    const double esc = report->escaped_area_mm2;
+    report->histogram_relative_error =
+        std::max(std::fabs(report->histogram_mass_mm2 / esc - 1), std::fabs(report->point_mass_mm2 / esc - 1));
+    return ok();
+}

@@ -1,0 +1,400 @@
+// icp_cdf.cu -- stored-CDF builder for the (u,phi) histogram, one cooperative launch (sm_100a).
+//
+// Replaces the reference's eight host-synchronised stages (check density, reduce, measure,
+// coarsen, make weights / transpose, per-phi serial scan, 1-thread marginal, normalise,
+// audit, measure CDF: device/phase_cdf.cu:93-339 driven by src/phase_cdf.cpp:275-472) and
+// restates the CPU builder's arithmetic (hex_phase/src/phase_table.cpp:111-187):
+//   phase A  each block owns a strip of CW coarse phi columns: reads its fine strip once
+//            (coalesced), adds the pole caps to the end rows, aggregates conservatively
+//            (Kahan, row-major order), keeps the coarse strip in shared memory, and
+//            publishes fine / coarse moments and its maximum;
+//   barrier
+//   phase B  coarsening TV, then per column an ordered binary64 scan in ascending theta of
+//            w = coarse / largest (exact plateaus, monotone prefixes), written unnormalised
+//            to the phi-major output, column sums published;
+//   barrier
+//   phase C  ordered marginal scan over all column sums (every block, identical result),
+//            normalisation (empty column -> the stored u edges), the phi marginal, and the
+//            L1 / lost-mass / malformed audit and stored moments from the written values;
+//   the last block to finish reduces the audits.
+// Grid barriers are counter spins with an iteration limit: on expiry the kernel records
+// ICP_ERR_TIMEOUT and returns without writing further output.
+#include <cooperative_groups.h>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "icp_internal.h"
+
+namespace icp {
+
+struct KSum {
+    double v, c;
+    __device__ __forceinline__ void add(double x)
+    {
+        const double y = x - c, t = v + y;
+        c = (t - v) - y;
+        v = t;
+    }
+};
+
+struct BlockPartial {
+    double fine_mass, fine_axial, stored_mass, stored_axial, largest;
+    double tv, l1, lost, max_err, recovered, axial;
+    unsigned long long invalid, lost_cells, malformed, underflow;
+};
+
+struct CdfParams {
+    const double* values;
+    const double* edges; // fine edges, nt+1
+    double* phi;
+    double* theta;
+    double* colsum;       // cp
+    BlockPartial* partial; // gridDim.x
+    CdfDeviceReport* report;
+    unsigned* sync;       // [0] barrier arrivals, [1] finished-block ticket
+    uint32_t kind, nt, np, ct, cp, dt, dp, cw;
+    double fwd_add, bwd_add;
+};
+
+constexpr unsigned kThreads = 256;
+constexpr unsigned kSpinLimit = 1u << 22;
+
+__device__ __forceinline__ bool grid_wait(unsigned* counter, unsigned target, unsigned* timeout_flag)
+{
+    __syncthreads();
+    __shared__ int ok;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(counter, 1u);
+        unsigned spins = 0;
+        while (*((volatile unsigned*)counter) < target && spins < kSpinLimit) {
+            __nanosleep(64);
+            ++spins;
+        }
+        ok = spins < kSpinLimit;
+        if (!ok) atomicExch(timeout_flag, 1u);
+        __threadfence();
+    }
+    __syncthreads();
+    return ok;
+}
+
+__device__ __forceinline__ double fine_mass_at(const CdfParams& P, uint32_t i, uint32_t j)
+{
+    double m = P.values[(size_t)i * P.np + j];
+    if (P.kind == 1) m = m * (P.edges[i + 1] - P.edges[i]);
+    if (i == 0) m += P.fwd_add;
+    if (i + 1 == P.nt) m += P.bwd_add;
+    return m;
+}
+
+template <class T> __device__ __forceinline__ T block_sum(T x, T* red)
+{
+    for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = x;
+    __syncthreads();
+    T s = T(0);
+    if (threadIdx.x == 0)
+        for (unsigned w = 0; w < blockDim.x / 32; ++w) s += red[w];
+    return s; // valid in thread 0
+}
+__device__ __forceinline__ double block_max(double x, double* red)
+{
+    for (int o = 16; o; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = x;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0)
+        for (unsigned w = 0; w < blockDim.x / 32; ++w) s = fmax(s, red[w]);
+    return s;
+}
+
+__global__ void __launch_bounds__(kThreads) cdf_build_kernel(const CdfParams P)
+{
+    extern __shared__ __align__(16) double strip[]; // ct x CW coarse strip, then phi strip (CW+1)
+    __shared__ double red_d[kThreads / 32];
+    __shared__ unsigned long long red_u[kThreads / 32];
+    __shared__ double s_glob[6];
+    __shared__ int s_last;
+
+    const uint32_t c0 = blockIdx.x * P.cw;
+    const uint32_t c1 = min(P.cp, c0 + P.cw);
+    const uint32_t w = c1 > c0 ? c1 - c0 : 0u; // columns in this strip
+    const uint32_t CW = P.cw;
+    double* sphi = strip + (size_t)P.ct * CW;
+
+    // ------------------------------------------------------------ phase A
+    KSum fm{0, 0}, fa{0, 0}, sm{0, 0}, sa{0, 0};
+    double largest = 0.0;
+    unsigned long long invalid = 0ull;
+    const uint32_t cells = P.ct * w;
+    for (uint32_t q = threadIdx.x; q < cells; q += blockDim.x) {
+        const uint32_t ci = q / w, cl = q % w, cj = c0 + cl;
+        KSum acc{0, 0};
+        for (uint32_t i = ci * P.dt; i < (ci + 1) * P.dt; ++i) {
+            const double mu = 1.0 - P.edges[i] - P.edges[i + 1];
+            for (uint32_t j = cj * P.dp; j < (cj + 1) * P.dp; ++j) {
+                const double m = fine_mass_at(P, i, j);
+                if (!(m >= 0.0) || !(m <= 1.7976931348623157e308)) ++invalid;
+                acc.add(m);
+                fm.add(m);
+                fa.add(m * mu);
+            }
+        }
+        const double c = acc.v;
+        strip[(size_t)ci * CW + cl] = c;
+        const double E0 = P.edges[(size_t)ci * P.dt], E1 = P.edges[(size_t)(ci + 1) * P.dt];
+        sm.add(c);
+        sa.add(c * (1.0 - E0 - E1));
+        largest = fmax(largest, c);
+    }
+    {
+        const double a = block_sum(fm.v + fm.c, red_d);
+        const double b = block_sum(fa.v + fa.c, red_d);
+        const double c = block_sum(sm.v + sm.c, red_d);
+        const double d = block_sum(sa.v + sa.c, red_d);
+        const double e = block_max(largest, red_d);
+        const unsigned long long f = block_sum(invalid, red_u);
+        if (threadIdx.x == 0) {
+            BlockPartial& bp = P.partial[blockIdx.x];
+            bp.fine_mass = a;
+            bp.fine_axial = b;
+            bp.stored_mass = c;
+            bp.stored_axial = d;
+            bp.largest = e;
+            bp.invalid = f;
+        }
+    }
+    if (!grid_wait(&P.sync[0], gridDim.x, &P.report->timeout)) return;
+
+    // ------------------------------------------------------------ phase B
+    if (threadIdx.x == 0) {
+        double a = 0, b = 0, c = 0, d = 0, e = 0;
+        for (unsigned k = 0; k < gridDim.x; ++k) {
+            const volatile BlockPartial* pp = (const volatile BlockPartial*)P.partial + k;
+            a += pp->fine_mass;
+            b += pp->fine_axial;
+            c += pp->stored_mass;
+            d += pp->stored_axial;
+            e = fmax(e, pp->largest);
+        }
+        s_glob[0] = a;
+        s_glob[1] = b;
+        s_glob[2] = c;
+        s_glob[3] = d;
+        s_glob[4] = e;
+    }
+    __syncthreads();
+    const double fine_total = s_glob[0], stored_total = s_glob[2], big = s_glob[4];
+    KSum tv{0, 0};
+    if (P.dt > 1 || P.dp > 1) {
+        const uint32_t fw = w * P.dp;
+        for (uint32_t q = threadIdx.x; q < P.nt * fw; q += blockDim.x) {
+            const uint32_t i = q / fw, j = c0 * P.dp + q % fw;
+            const uint32_t ci = i / P.dt, cl = j / P.dp - c0;
+            const double fraction = (P.edges[i + 1] - P.edges[i]) /
+                                    (P.edges[(size_t)(ci + 1) * P.dt] - P.edges[(size_t)ci * P.dt]) / P.dp;
+            tv.add(fabs(fine_mass_at(P, i, j) / fine_total - strip[(size_t)ci * CW + cl] / stored_total * fraction));
+        }
+    }
+    unsigned long long underflow = 0ull;
+    if (threadIdx.x < w) {
+        // ordered ascending-theta scan of one phi column; unnormalised prefixes to the output
+        const uint32_t cl = threadIdx.x, j = c0 + cl;
+        double* out = P.theta + (size_t)j * (P.ct + 1);
+        double s = 0.0;
+        out[0] = 0.0;
+        for (uint32_t i = 0; i < P.ct; ++i) {
+            const double c = strip[(size_t)i * CW + cl];
+            const double x = c / big;
+            if (c > 0 && !(x > 0)) ++underflow;
+            s += x;
+            out[i + 1] = s;
+        }
+        P.colsum[j] = s;
+    }
+    {
+        const double t = block_sum(tv.v + tv.c, red_d);
+        const unsigned long long u = block_sum(underflow, red_u);
+        if (threadIdx.x == 0) {
+            P.partial[blockIdx.x].tv = 0.5 * t;
+            P.partial[blockIdx.x].underflow = u;
+        }
+    }
+    if (!grid_wait(&P.sync[0], 2u * gridDim.x, &P.report->timeout)) return;
+
+    // ------------------------------------------------------------ phase C
+    if (threadIdx.x == 0) {
+        // ordered marginal scan (phase_table.cpp:154): phi[j+1] = phi[j] + colsum[j]
+        double a = 0.0;
+        const volatile double* cs = P.colsum;
+        for (uint32_t j = 0; j < c0; ++j) a += cs[j];
+        sphi[0] = a;
+        for (uint32_t cl = 0; cl < w; ++cl) {
+            a += cs[c0 + cl];
+            sphi[cl + 1] = a;
+        }
+        for (uint32_t j = c1; j < P.cp; ++j) a += cs[j];
+        s_glob[5] = a;
+    }
+    __syncthreads();
+    const double total = s_glob[5];
+    // normalised marginal for this strip: phi[0] = 0, phi[cp] = 1, interior / total
+    if (threadIdx.x <= w) {
+        const uint32_t j = c0 + threadIdx.x;
+        if (threadIdx.x > 0 || c0 == 0) {
+            double v = sphi[threadIdx.x];
+            if (j == 0) v = 0.0;
+            else if (j == P.cp) v = 1.0;
+            else v = v / total;
+            P.phi[j] = v;
+        }
+    }
+    __syncthreads();
+    for (uint32_t cl = threadIdx.x; cl <= w; cl += blockDim.x) {
+        const uint32_t j = c0 + cl;
+        double v = sphi[cl];
+        sphi[cl] = (j == 0) ? 0.0 : (j == P.cp ? 1.0 : v / total);
+    }
+    __syncthreads();
+    KSum l1{0, 0}, lost{0, 0}, rec{0, 0}, ax{0, 0};
+    double max_err = 0.0;
+    unsigned long long lost_cells = 0ull, malformed = 0ull;
+    const uint32_t stride = P.ct + 1;
+    // this strip's output rows are contiguous: theta[c0*(ct+1) .. c1*(ct+1)).  Each chunk of
+    // blockDim.x elements is read raw (an element and its successor) before any is rewritten.
+    const uint32_t span = w * stride;
+    for (uint32_t base = 0; base < span; base += blockDim.x) {
+        const uint32_t q = base + threadIdx.x;
+        double b0 = 0.0;
+        double* row = nullptr;
+        uint32_t i = 0;
+        if (q < span) {
+            const uint32_t cl = q / stride, j = c0 + cl;
+            i = q % stride;
+            const double cs = P.colsum[j];
+            row = P.theta + (size_t)j * stride;
+            auto norm = [&](uint32_t k, double raw) -> double {
+                if (k == 0) return 0.0;
+                if (k == P.ct) return 1.0;
+                return cs > 0 ? raw / cs : P.edges[(size_t)k * P.dt];
+            };
+            b0 = norm(i, row[i]);
+            if (i < P.ct) {
+                const double b1 = norm(i + 1, row[i + 1]);
+                const double a0 = sphi[cl], a1 = sphi[cl + 1];
+                const double qv = (a1 - a0) * (b1 - b0);
+                const double c = strip[(size_t)i * CW + cl];
+                const double p = c / stored_total;
+                const bool bad = !(qv >= 0.0) || !(qv <= 1.7976931348623157e308) || a1 < a0 || b1 < b0;
+                if (bad) ++malformed;
+                if (c > 0 && !(p > 0)) ++malformed;
+                const double err = fabs(p - qv);
+                l1.add(err);
+                max_err = fmax(max_err, err);
+                if (p > 0 && qv == 0) {
+                    lost.add(p);
+                    ++lost_cells;
+                }
+                rec.add(qv);
+                const double E0 = P.edges[(size_t)i * P.dt], E1 = P.edges[(size_t)(i + 1) * P.dt];
+                ax.add(qv * (1.0 - E0 - E1));
+            }
+        }
+        __syncthreads();
+        if (row) row[i] = b0;
+        __syncthreads();
+    }
+    {
+        const double a = block_sum(l1.v + l1.c, red_d);
+        const double b = block_sum(lost.v + lost.c, red_d);
+        const double c = block_sum(rec.v + rec.c, red_d);
+        const double d = block_sum(ax.v + ax.c, red_d);
+        const double e = block_max(max_err, red_d);
+        const unsigned long long f = block_sum(lost_cells, red_u);
+        const unsigned long long g = block_sum(malformed, red_u);
+        if (threadIdx.x == 0) {
+            BlockPartial& bp = P.partial[blockIdx.x];
+            bp.l1 = a;
+            bp.lost = b;
+            bp.recovered = c;
+            bp.axial = d;
+            bp.max_err = e;
+            bp.lost_cells = f;
+            bp.malformed = g;
+            __threadfence();
+            s_last = (atomicAdd(&P.sync[1], 1u) == gridDim.x - 1);
+        }
+    }
+    __syncthreads();
+    if (!s_last || threadIdx.x != 0) return;
+    __threadfence();
+    CdfDeviceReport r{};
+    const volatile BlockPartial* vp = P.partial;
+    for (unsigned k = 0; k < gridDim.x; ++k) {
+        r.fine_mass += vp[k].fine_mass;
+        r.fine_axial += vp[k].fine_axial;
+        r.stored_mass += vp[k].stored_mass;
+        r.stored_axial += vp[k].stored_axial;
+        r.tv += vp[k].tv;
+        r.l1 += vp[k].l1;
+        r.lost += vp[k].lost;
+        r.recovered += vp[k].recovered;
+        r.axial += vp[k].axial;
+        r.max_err = fmax(r.max_err, vp[k].max_err);
+        r.lost_cells += vp[k].lost_cells;
+        r.malformed += vp[k].malformed;
+        r.invalid += vp[k].invalid;
+        r.underflow += vp[k].underflow;
+    }
+    r.largest = s_glob[4];
+    r.total = total;
+    r.timeout = P.report->timeout;
+    *P.report = r;
+}
+
+// Fine-grid mass with pole caps for an FP64 histogram (used by the report path).
+int launch_cdf_build(const CdfLaunch& L, cudaStream_t stream)
+{
+    CdfParams P;
+    P.values = L.values;
+    P.edges = L.edges;
+    P.phi = L.phi;
+    P.theta = L.theta;
+    P.colsum = L.colsum;
+    P.partial = reinterpret_cast<BlockPartial*>(L.partial);
+    P.report = L.report;
+    P.sync = L.sync;
+    P.kind = L.kind;
+    P.nt = L.nt;
+    P.np = L.np;
+    P.ct = L.ct;
+    P.cp = L.cp;
+    P.dt = L.nt / L.ct;
+    P.dp = L.np / L.cp;
+    P.cw = L.cw;
+    P.fwd_add = L.fwd_add;
+    P.bwd_add = L.bwd_add;
+    const unsigned blocks = (L.cp + L.cw - 1) / L.cw;
+    const size_t smem = sizeof(double) * ((size_t)L.ct * L.cw + L.cw + 1);
+    cudaError_t e = cudaFuncSetAttribute(cdf_build_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return (int)e;
+    void* args[] = {&P};
+    e = cudaLaunchCooperativeKernel((const void*)cdf_build_kernel, dim3(blocks), dim3(kThreads), args, smem, stream);
+    return (int)e;
+}
+
+int cdf_max_coresident_blocks(size_t smem, int device)
+{
+    int per_sm = 0, sms = 0;
+    cudaFuncSetAttribute(cdf_build_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cdf_build_kernel, kThreads, smem) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
+    return per_sm * sms;
+}
+
+size_t cdf_partial_bytes() { return sizeof(BlockPartial); }
+
+} // namespace icp

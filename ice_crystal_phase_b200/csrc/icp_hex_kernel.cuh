@@ -1,0 +1,407 @@
+// icp_hex_kernel.cuh -- fused hexagonal-prism trace + (u,phi) binning kernel (sm_100a).
+//
+// One launch traces one orientation node's ray range [first, first+count) and adds every
+// exit into the FP64 cell-mass histogram.  It replaces the reference's count kernel, serial
+// prefix, replay kernel, 200-byte CSR round trip and FP64 atomic accumulate
+// (hex_trace/device/hex_trace.cu:12-48, hex_phase/device/phase_accumulate.cu:10-28):
+//   * persistent warps, each owning a contiguous slice of ray ids; a lane whose ray ends
+//     takes the next id of its warp's slice in the next step (no warp idles on long rays);
+//   * one event per lane per step: the entry split, or one internal boundary + split; each
+//     event emits at most one exit, which the whole warp bins together;
+//   * exits go to a shared-memory table through match.any warp aggregation, in 2^-44
+//     fixed point; the table is flushed to FP64 once per block.
+// Ray algorithm: hex_trace/include/ice_crystal/hex_trace_core.hpp:190-259 (linear R/T chain),
+// hex_prism.hpp:64-175 (entry sampling, nearest exit plane), flux_interface.hpp:26-88.
+#pragma once
+#include "icp_bin.cuh"
+#include "icp_device.cuh"
+
+namespace icp {
+
+// Accumulators shared by all blocks of one launch (device memory, zeroed by the host).
+// Power sums are exact 128-bit fixed-point integers (lo, hi words) in units of 2^-44.
+struct DevStats {
+    unsigned long long esc[2], unres[2], fwd[2], bwd[2];
+    double axial;
+    unsigned long long max_bal_bits, max_iface_bits; // bit patterns of non-negative doubles
+    unsigned long long rays, outputs, status[8], rejected, snapped, near_edge, fallback, invalid;
+    unsigned long long encounters;
+};
+
+__device__ __forceinline__ void add128(unsigned long long* p, unsigned long long t)
+{
+    if (!t) return;
+    const unsigned long long old = atomicAdd(p, t);
+    if (old + t < old) atomicAdd(p + 1, 1ull);
+}
+
+template <class R> struct HexParams {
+    // geometry in units of the circumradius, body frame (long axis +y)
+    R half_len;
+    V3<R> k, ke0;    // incident direction and its frame vector
+    R cum[8];        // cumulative projected face weights (plain adds in face order)
+    uint32_t face_mask; // faces with positive projected weight
+    R area;          // total projected weight (Kahan sum, as the reference's projected_area)
+    R n_ext, n_int, tail, bal_tol;
+    uint64_t seed, total, first, count;
+    uint32_t max_hits;
+    uint32_t batch_size;
+    uint32_t* batch_out;   // per-batch exit counters or nullptr
+    // binning
+    BinGridF gf;
+    BinGridD gd;
+    const double* edges_d; // nt+1 (global)
+    const float* edges_f;  // nt+1 (global)
+    double* mass;          // nt*np FP64 histogram (global)
+    double to_mass;        // area weight * 2^-44
+    DevStats* stats;
+    uint32_t hash_slots;   // power of two, 0 = no shared table
+    uint32_t smem_edges;   // 1 = stage edges in shared memory
+};
+
+template <class R> __device__ __forceinline__ V3<R> face_normal(unsigned f)
+{
+    const R h = R(0.5), s = R(kSqrt3 / 2);
+    switch (f) {
+    case 0: return v3(R(1), R(0), R(0));
+    case 1: return v3(h, R(0), s);
+    case 2: return v3(-h, R(0), s);
+    case 3: return v3(R(-1), R(0), R(0));
+    case 4: return v3(-h, R(0), -s);
+    case 5: return v3(h, R(0), -s);
+    case 6: return v3(R(0), R(1), R(0));
+    default: return v3(R(0), R(-1), R(0));
+    }
+}
+template <class R> __device__ __forceinline__ V3<R> hex_vertex(unsigned f)
+{
+    const R s = R(kSqrt3 / 2);
+    switch (f % 6u) {
+    case 0: return v3(s, R(0), R(0.5));
+    case 1: return v3(R(0), R(0), R(1));
+    case 2: return v3(-s, R(0), R(0.5));
+    case 3: return v3(-s, R(0), R(-0.5));
+    case 4: return v3(R(0), R(0), R(-1));
+    default: return v3(s, R(0), R(-0.5));
+    }
+}
+template <class R> __device__ __forceinline__ R face_offset(const HexParams<R>& P, unsigned f)
+{
+    return f < 6u ? R(kSqrt3 / 2) : P.half_len;
+}
+
+// hex_prism.hpp:54-57 / 108-120 (FP64 path only): every other face strictly outside tolerance.
+__device__ __forceinline__ bool strict_face_point(const HexParams<double>& P, V3<double> p, unsigned face)
+{
+    const double tol = 128 * Eps<double>::eps * fmax(1.0, fmax(P.half_len, fmax(fabs(p.x), fmax(fabs(p.y), fabs(p.z)))));
+    for (unsigned f = 0; f < 8; ++f) {
+        const double gap = face_offset(P, f) - dot(face_normal<double>(f), p);
+        if (f == face) {
+            if (fabs(gap) > tol) return false;
+        } else if (!(gap > tol)) return false;
+    }
+    return true;
+}
+
+struct Boundary {
+    unsigned face;
+    int status; // 0 regular, 3 ambiguous, 5 numerical
+    bool near_edge;
+};
+
+// Nearest exit plane of the convex prism from a point on `start` (hex_prism.hpp:123-147).
+// FP32: exit t = min over forward-facing planes (no positivity filter, so a point rounded
+// just outside a neighbouring plane exits there at t = 0); near ties are counted only.
+// FP64: the reference rules, ties within geometry tolerance are ambiguous.
+template <class R>
+__device__ __forceinline__ Boundary next_boundary(const HexParams<R>& P, V3<R>& p, V3<R> d, unsigned start, R& t_out)
+{
+    Boundary out{8u, 0, false};
+    R best = R(3.0e38), second = R(3.0e38);
+    if constexpr (sizeof(R) == 8) {
+        best = 1.7976931348623157e308;
+        second = best;
+        if (!strict_face_point(P, p, start)) { out.status = 3; return out; }
+        if (dot(face_normal<R>(start), d) > 128 * Eps<double>::eps) { out.status = 5; return out; }
+    }
+#pragma unroll
+    for (unsigned f = 0; f < 8; ++f) {
+        if (f == start) continue;
+        const V3<R> n = face_normal<R>(f);
+        const R c = dot(n, d);
+        if (!(c > R(0))) continue;
+        const R t = (face_offset(P, f) - dot(n, p)) / c;
+        if constexpr (sizeof(R) == 8) {
+            if (!(t > 0) || !finite_r(t)) continue;
+        }
+        if (t < best) { second = best; best = t; out.face = f; }
+        else if (t < second) second = t;
+    }
+    if (out.face == 8u) { out.status = 5; return out; }
+    if constexpr (sizeof(R) == 4) {
+        const R t = rmax(best, R(0));
+        p = p + d * t;
+        out.near_edge = (second - best) <= R(64) * Eps<float>::eps * rmax(R(1), P.half_len);
+        t_out = t;
+    } else {
+        p = p + d * best;
+        t_out = best;
+        const double tol = 128 * Eps<double>::eps * fmax(1.0, fmax(P.half_len, fmax(fmax(fabs(p.x), fmax(fabs(p.y), fabs(p.z))), fabs(best))));
+        if (second - best <= tol || !strict_face_point(P, p, out.face)) out.status = 3;
+    }
+    return out;
+}
+
+template <class R> struct LaneRay {
+    V3<R> p, d, e;
+    Stokes<R> S;
+    uint64_t id;
+    R esc;
+    uint32_t face, hits;
+    bool live;
+};
+
+template <class R> struct LaneAcc {
+    unsigned long long esc_fx, unres_fx, fwd_fx, bwd_fx, outputs, rays, rejected, snapped, near_edge, fallback, invalid, encounters;
+    double axial, max_bal, max_iface;
+    uint64_t cur_batch;
+    uint32_t cur_batch_out;
+};
+
+template <class R>
+__device__ __forceinline__ void finish_ray(const HexParams<R>& P, LaneRay<R>& L, LaneAcc<R>& A, unsigned* s_status,
+                                           int status, R residual)
+{
+    L.live = false;
+    const R bal = rabs(L.esc + residual - R(1));
+    A.unres_fx += to_fix(residual);
+    A.max_bal = fmax(A.max_bal, (double)bal);
+    A.rays += 1;
+    atomicAdd(&s_status[status], 1u);
+    const bool ok = (status == 0 || status == 1) && bal <= P.bal_tol;
+    if (!ok) A.rejected += 1;
+}
+
+// Ends the ray if the continuing branch is exhausted / below the tail / out of encounters
+// (the top-of-loop and after-loop tests of hex_trace_core.hpp:217-251, applied eagerly).
+template <class R>
+__device__ __forceinline__ void settle(const HexParams<R>& P, LaneRay<R>& L, LaneAcc<R>& A, unsigned* s_status)
+{
+    const R power = L.S.I;
+    if (power == R(0)) finish_ray(P, L, A, s_status, 0, R(0));
+    else if (power <= P.tail) finish_ray(P, L, A, s_status, 1, power);
+    else if (L.hits >= P.max_hits) finish_ray(P, L, A, s_status, 2, power);
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) hex_trace_bin_kernel(const HexParams<R> P)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    unsigned long long* s_vals = reinterpret_cast<unsigned long long*>(smem);
+    uint32_t* s_keys = reinterpret_cast<uint32_t*>(s_vals + P.hash_slots);
+    unsigned* s_status = reinterpret_cast<unsigned*>(s_keys + P.hash_slots);
+    R* s_edges = reinterpret_cast<R*>(s_status + 8);
+
+    const uint32_t nt = P.gf.nt;
+    for (uint32_t s = threadIdx.x; s < P.hash_slots; s += blockDim.x) { s_keys[s] = 0u; s_vals[s] = 0ull; }
+    if (threadIdx.x < 8) s_status[threadIdx.x] = 0u;
+    const R* edges;
+    if (P.smem_edges) {
+        for (uint32_t i = threadIdx.x; i <= nt; i += blockDim.x) {
+            if constexpr (sizeof(R) == 4) s_edges[i] = P.edges_f[i];
+            else s_edges[i] = P.edges_d[i];
+        }
+        edges = s_edges;
+    } else {
+        if constexpr (sizeof(R) == 4) edges = P.edges_f;
+        else edges = P.edges_d;
+    }
+    __syncthreads();
+    SmemHist H{s_keys, s_vals, P.hash_slots ? P.hash_slots - 1u : 0u};
+
+    const unsigned lane = threadIdx.x & 31u;
+    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    const uint64_t warp = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const uint64_t per = (P.count + warps - 1) / warps;
+    uint64_t wnext = P.first + warp * per;
+    const uint64_t wend = min(P.first + P.count, wnext + per);
+
+    LaneRay<R> L;
+    L.live = false;
+    LaneAcc<R> A;
+    A.esc_fx = A.unres_fx = A.fwd_fx = A.bwd_fx = A.outputs = A.rays = A.rejected = 0ull;
+    A.snapped = A.near_edge = A.fallback = A.invalid = A.encounters = 0ull;
+    A.axial = A.max_bal = A.max_iface = 0.0;
+    A.cur_batch = ~0ull;
+    A.cur_batch_out = 0u;
+    const unsigned lt_mask = (1u << lane) - 1u;
+
+    while (true) {
+        // ---- refill idle lanes from the warp's slice
+        const unsigned idle = __ballot_sync(kFull, !L.live);
+        bool fresh = false;
+        if (idle) {
+            if (!L.live) {
+                const uint64_t id = wnext + __popc(idle & lt_mask);
+                if (id < wend) { L.id = id; fresh = true; }
+            }
+            wnext += __popc(idle);
+        }
+        if (!__any_sync(kFull, L.live || fresh)) break;
+
+        bool has = false;
+        V3<R> od;
+        R opow = R(0);
+        if (fresh) {
+            // ---- entry: face in proportion to projected area, point on the face (hex_prism.hpp:64-98)
+            const R u0 = uniform<R>(rng_bits(P.seed, L.id, 0));
+            const R u1 = uniform<R>(rng_bits(P.seed, L.id, 1));
+            const R u2 = uniform<R>(rng_bits(P.seed, L.id, 2));
+            const R target = u0 * P.area;
+            unsigned face = 8u, last = 8u;
+#pragma unroll
+            for (unsigned f = 0; f < 8; ++f) {
+                const bool pos = (P.face_mask >> f) & 1u;
+                if (pos) {
+                    last = f;
+                    if (face == 8u && target < P.cum[f]) face = f;
+                }
+            }
+            if (face == 8u) face = last;
+            V3<R> pos;
+            const V3<R> n = face_normal<R>(face);
+            if (face < 6u) {
+                const V3<R> tangent = v3(-n.z, R(0), n.x);
+                pos = (n * R(kSqrt3 / 2) + tangent * (u1 - R(0.5))) + v3(R(0), (R(2) * u2 - R(1)) * P.half_len, R(0));
+            } else {
+                const R sector = R(6) * u1;
+                const unsigned j = (unsigned)sector;
+                const R r = sqrt_r(sector - (R)j);
+                pos = (hex_vertex<R>(j) * (R(1) - u2) + hex_vertex<R>(j + 1u) * u2) * r;
+                pos.y = (face == 6u ? R(1) : R(-1)) * P.half_len;
+            }
+            L.live = true;
+            L.esc = R(0);
+            L.hits = 0u;
+            bool entry_ok = true;
+            if constexpr (sizeof(R) == 8) {
+                if (!strict_face_point(P, pos, face)) {
+                    finish_ray(P, L, A, s_status, 3, R(1));
+                    entry_ok = false;
+                }
+            }
+            if (entry_ok) {
+                const Stokes<R> S0{R(1), R(0), R(0), R(0)};
+                const Interface<R> sp = split(P.k, P.ke0, S0, n, P.n_ext, P.n_int);
+                A.max_iface = fmax(A.max_iface, (double)sp.balance);
+                if (sp.r.I > R(0)) { has = true; od = sp.dr; opow = sp.r.I; }
+                if (!sp.has_t) {
+                    L.esc += opow;
+                    finish_ray(P, L, A, s_status, 0, R(0));
+                } else {
+                    L.p = pos;
+                    L.d = sp.dt;
+                    L.e = sp.s;
+                    L.S = sp.t;
+                    L.face = face;
+                    L.esc += opow;
+                    settle(P, L, A, s_status);
+                }
+            }
+        } else if (L.live) {
+            // ---- one internal encounter (hex_trace_core.hpp:217-246)
+            R t;
+            const Boundary hit = next_boundary(P, L.p, L.d, L.face, t);
+            if (hit.status) {
+                finish_ray(P, L, A, s_status, hit.status, L.S.I);
+            } else {
+                A.near_edge += hit.near_edge ? 1ull : 0ull;
+                const Interface<R> sp = split(L.d, L.e, L.S, -face_normal<R>(hit.face), P.n_int, P.n_ext);
+                ++L.hits;
+                ++A.encounters;
+                A.max_iface = fmax(A.max_iface, (double)sp.balance);
+                if (sp.has_t && sp.t.I > R(0)) {
+                    has = true;
+                    od = sp.dt;
+                    opow = sp.t.I;
+                    L.esc += opow;
+                }
+                L.d = sp.dr;
+                L.e = sp.s;
+                L.S = sp.r;
+                L.face = hit.face;
+                settle(P, L, A, s_status);
+            }
+        }
+
+        // ---- bin this step's exits (whole warp)
+        uint32_t cell = 0u;
+        bool to_table = false;
+        uint64_t v = 0ull;
+        if (has) {
+            BinResult b;
+            if constexpr (sizeof(R) == 4) b = bin_f32(P.gf, edges, od);
+            else b = bin_f64(P.gd, edges, od);
+            if (!b.valid) {
+                A.invalid += 1;
+            } else {
+                v = to_fix(opow);
+                A.esc_fx += v;
+                A.outputs += 1;
+                A.snapped += b.snapped ? 1ull : 0ull;
+                A.axial += (double)opow * b.mu;
+                if (b.pole > 0) A.fwd_fx += v;
+                else if (b.pole < 0) A.bwd_fx += v;
+                else { to_table = true; cell = b.cell; }
+            }
+        }
+        hist_add(H, P.mass, P.to_mass, to_table, cell, v, A.fallback);
+
+        // ---- per-batch exit counts (capacity audit), flushed when the lane's batch changes
+        if (P.batch_out && (has || fresh)) {
+            const uint64_t bidx = (L.id - 0) / P.batch_size;
+            if (bidx != A.cur_batch) {
+                if (A.cur_batch != ~0ull && A.cur_batch_out) atomicAdd(&P.batch_out[A.cur_batch], A.cur_batch_out);
+                A.cur_batch = bidx;
+                A.cur_batch_out = 0u;
+            }
+            A.cur_batch_out += has ? 1u : 0u;
+        }
+    }
+    if (P.batch_out && A.cur_batch != ~0ull && A.cur_batch_out) atomicAdd(&P.batch_out[A.cur_batch], A.cur_batch_out);
+
+    // ---- block epilogue: flush the table and the lane accumulators
+    __syncthreads();
+    hist_flush(H, P.mass, P.to_mass);
+    DevStats* G = P.stats;
+    // Per-warp sums stay below 2^60 (a warp slice holds at most 2^16 rays of power <= 1).
+    unsigned long long w[12] = {A.esc_fx, A.unres_fx, A.fwd_fx, A.bwd_fx, A.rays, A.outputs, A.rejected,
+                                A.snapped, A.near_edge, A.fallback, A.invalid, A.encounters};
+#pragma unroll
+    for (int q = 0; q < 12; ++q)
+        for (int o = 16; o; o >>= 1) w[q] += __shfl_xor_sync(kFull, w[q], o);
+    double ax = A.axial, mb = A.max_bal, mi = A.max_iface;
+    for (int o = 16; o; o >>= 1) {
+        ax += __shfl_xor_sync(kFull, ax, o);
+        mb = fmax(mb, __shfl_xor_sync(kFull, mb, o));
+        mi = fmax(mi, __shfl_xor_sync(kFull, mi, o));
+    }
+    if (lane == 0) {
+        add128(G->esc, w[0]);
+        add128(G->unres, w[1]);
+        add128(G->fwd, w[2]);
+        add128(G->bwd, w[3]);
+        unsigned long long* counters[8] = {&G->rays, &G->outputs, &G->rejected, &G->snapped,
+                                           &G->near_edge, &G->fallback, &G->invalid, &G->encounters};
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            if (w[4 + q]) atomicAdd(counters[q], w[4 + q]);
+        if (ax != 0.0) atomicAdd(&G->axial, ax);
+        atomicMax(&G->max_bal_bits, (unsigned long long)__double_as_longlong(mb));
+        atomicMax(&G->max_iface_bits, (unsigned long long)__double_as_longlong(mi));
+    }
+    __syncthreads();
+    if (threadIdx.x < 8 && s_status[threadIdx.x]) atomicAdd(&G->status[threadIdx.x], (unsigned long long)s_status[threadIdx.x]);
+}
+
+} // namespace icp

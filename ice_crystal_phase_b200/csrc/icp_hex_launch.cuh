@@ -1,0 +1,87 @@
+// icp_hex_launch.cuh -- host launcher for the hex trace+bin kernel, instantiated once per
+// arithmetic type in icp_hex_f32.cu / icp_hex_f64.cu.
+#pragma once
+#include "icp_hex_kernel.cuh"
+#include "icp_internal.h"
+
+namespace icp {
+
+constexpr uint32_t kEdgeSmemMax = 4097; // stage u edges in shared memory up to this many
+
+template <class R> size_t hex_smem_bytes(uint32_t hash_slots, uint32_t nt)
+{
+    size_t b = (size_t)hash_slots * (8 + 4) + 8 * 4;
+    if (nt + 1 <= kEdgeSmemMax) b += sizeof(R) * (nt + 1);
+    return b;
+}
+
+template <class R> HexParams<R> make_hex_params(const HexLaunch& L)
+{
+    HexParams<R> P;
+    P.half_len = (R)L.half_len;
+    P.k = v3((R)L.k[0], (R)L.k[1], (R)L.k[2]);
+    P.ke0 = v3((R)L.ke0[0], (R)L.ke0[1], (R)L.ke0[2]);
+    for (int f = 0; f < 8; ++f) P.cum[f] = (R)L.cum[f];
+    P.face_mask = L.face_mask;
+    P.area = (R)L.area;
+    P.n_ext = (R)L.n_ext;
+    P.n_int = (R)L.n_int;
+    P.tail = (R)L.tail;
+    P.bal_tol = (R)L.bal_tol;
+    P.seed = L.seed;
+    P.total = L.total;
+    P.first = L.first;
+    P.count = L.count;
+    P.max_hits = L.max_hits;
+    P.batch_size = L.batch_size;
+    P.batch_out = L.batch_out;
+    // FP32 fused transform rows: (e0, e1, ki)^T * rotation
+    const double* r = L.rot; // column c = r[3c..3c+2]
+    const double* rows[3] = {L.e0, L.e1, L.ki};
+    for (int a = 0; a < 3; ++a)
+        for (int c = 0; c < 3; ++c)
+            P.gf.m[3 * a + c] = (float)(rows[a][0] * r[3 * c] + rows[a][1] * r[3 * c + 1] + rows[a][2] * r[3 * c + 2]);
+    P.gf.nt = L.nt;
+    P.gf.np = L.np;
+    P.gf.np_f = (float)L.np;
+    P.gf.theta_scale = (float)((double)L.nt / kPi);
+    for (int i = 0; i < 9; ++i) P.gd.rot[i] = L.rot[i];
+    for (int i = 0; i < 3; ++i) {
+        P.gd.ki[i] = L.ki[i];
+        P.gd.e0[i] = L.e0[i];
+        P.gd.e1[i] = L.e1[i];
+    }
+    P.gd.edges = L.edges_d;
+    P.gd.nt = L.nt;
+    P.gd.np = L.np;
+    P.edges_d = L.edges_d;
+    P.edges_f = L.edges_f;
+    P.mass = L.mass;
+    P.to_mass = L.to_mass;
+    P.stats = reinterpret_cast<DevStats*>(L.stats);
+    P.hash_slots = L.hash_slots;
+    P.smem_edges = (L.nt + 1 <= kEdgeSmemMax) ? 1u : 0u;
+    return P;
+}
+
+template <class R> int launch_hex(const HexLaunch& L, cudaStream_t stream)
+{
+    const HexParams<R> P = make_hex_params<R>(L);
+    const size_t smem = hex_smem_bytes<R>(L.hash_slots, L.nt);
+    cudaError_t e = cudaFuncSetAttribute(hex_trace_bin_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return (int)e;
+    hex_trace_bin_kernel<R><<<L.blocks, L.block_threads, smem, stream>>>(P);
+    return (int)cudaGetLastError();
+}
+
+template <class R> int hex_blocks_per_sm(uint32_t hash_slots, uint32_t nt, uint32_t threads)
+{
+    const size_t smem = hex_smem_bytes<R>(hash_slots, nt);
+    cudaFuncSetAttribute(hex_trace_bin_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hex_trace_bin_kernel<R>, (int)threads, smem) != cudaSuccess)
+        return 0;
+    return per_sm;
+}
+
+} // namespace icp

@@ -1,0 +1,65 @@
+// icp_internal.h -- declarations shared by the CUDA translation units and the C-ABI layer.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace icp {
+
+// Final audit written by the last block of the CDF kernel.
+struct CdfDeviceReport {
+    double fine_mass, fine_axial, stored_mass, stored_axial, tv, l1, lost, recovered, axial, max_err, largest, total;
+    unsigned long long lost_cells, malformed, invalid, underflow;
+    unsigned timeout, pad;
+};
+
+struct CdfLaunch {
+    const double* values;
+    const double* edges;
+    double* phi;
+    double* theta;
+    double* colsum;
+    void* partial;
+    CdfDeviceReport* report;
+    unsigned* sync; // two counters, zeroed before launch
+    uint32_t kind, nt, np, ct, cp, cw;
+    double fwd_add, bwd_add;
+};
+
+int launch_cdf_build(const CdfLaunch& L, cudaStream_t stream);
+int cdf_max_coresident_blocks(size_t smem, int device);
+size_t cdf_partial_bytes();
+
+// Host-side description of one hex trace+bin launch (double precision inputs; the
+// launcher converts to the kernel's arithmetic type).
+struct HexLaunch {
+    double half_len;
+    double k[3], ke0[3];
+    double cum[8];
+    uint32_t face_mask;
+    double area;
+    double n_ext, n_int, tail, bal_tol;
+    uint64_t seed, total, first, count;
+    uint32_t max_hits, batch_size;
+    uint32_t* batch_out;
+    // grid transforms
+    double rot[9];      // column-major body -> ensemble
+    double ki[3], e0[3], e1[3];
+    uint32_t nt, np;
+    const double* edges_d;
+    const float* edges_f;
+    double* mass;
+    double to_mass;
+    void* stats; // DevStats*
+    uint32_t hash_slots;
+    uint32_t block_threads;
+    uint32_t blocks;
+};
+
+size_t hex_stats_bytes();
+int launch_hex_f32(const HexLaunch& L, cudaStream_t stream);
+int launch_hex_f64(const HexLaunch& L, cudaStream_t stream);
+// Largest number of resident blocks for the chosen configuration.
+int hex_max_blocks(int precision, uint32_t hash_slots, uint32_t nt, uint32_t block_threads, int device);
+
+} // namespace icp

@@ -1,0 +1,222 @@
+/*
+ * icp_b200.h -- C ABI of the B200-native phase-function generation path.
+ *
+ * Plain pointers, sizes and POD structs only.  Every function returns an int
+ * status (ICP_OK = 0) and records a message retrievable with icp_last_error().
+ * Calls are synchronous with respect to the context's stream unless stated;
+ * device pointers are borrowed only for the duration of a call.
+ *
+ * Reference interfaces replaced (Somatic-Cell/ice-crystal-phase):
+ *   icp_context_*         rainbow::CudaContext            include/rainbow/cuda_driver.hpp, src/cuda_driver.cpp:148-215
+ *   icp_abi_version       ABI marker kernels              hex_trace/device/hex_trace.cu:6-11,
+ *                                                         hex_phase/device/phase_accumulate.cu:9,
+ *                                                         device/phase_cdf.cu:65
+ *   icp_hex_trace_bin     HexPrismTracer::trace +         hex_trace/include/ice_crystal/hex_trace_cuda.hpp:26-27
+ *                         PhaseMassAccumulatorCuda::add   hex_phase/include/ice_crystal/phase_cuda.hpp:25
+ *   icp_phase_cdf_build   PhaseMassAccumulatorCuda::finish hex_phase/include/ice_crystal/phase_cuda.hpp:26
+ *                         + rainbow::PhaseCdf::build       include/rainbow/phase_cdf.hpp:63-65
+ *   icp_hex_generate      the CUDA branch of ice_generate_phase's record loop
+ *                                                         hex_phase/apps/generate_hex_phase.cpp:92-134
+ *   icp_drop_trace_bin    RaindropTracer::trace_unpolarized + patch/query/optics stages
+ *                                                         include/rainbow/raindrop_tracer.hpp, apps/generate_phase.cpp:431-439
+ *   icp_drop_generate     rainbow_generate's record path   apps/generate_phase.cpp:395-453
+ */
+#ifndef ICP_B200_H
+#define ICP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ICP_ABI_VERSION 0x49435001u /* "ICP" v1 */
+
+enum icp_status {
+    ICP_OK = 0,
+    ICP_ERR_INVALID_ARGUMENT = 1, /* rejected input (reference: std::invalid_argument)        */
+    ICP_ERR_AUDIT = 2,            /* numerical/quality audit failed (reference: runtime_error) */
+    ICP_ERR_CAPACITY = 3,         /* an explicit capacity/size limit was exceeded              */
+    ICP_ERR_DEVICE = 4,           /* CUDA error                                                */
+    ICP_ERR_TIMEOUT = 5,          /* a bounded device-side wait gave up                        */
+    ICP_ERR_STATE = 6             /* call sequence error (reference: std::logic_error)         */
+};
+
+/* Trace arithmetic: FP32 (default fast path) or FP64 (reference-exact tolerances). */
+enum icp_precision { ICP_FP32 = 0, ICP_FP64 = 1 };
+
+/* Ray status codes, identical to the reference TraceStatus (hex_trace_core.hpp:97-102). */
+enum icp_ray_status {
+    ICP_RAY_EXHAUSTED = 0, ICP_RAY_TAIL = 1, ICP_RAY_LIMIT = 2, ICP_RAY_AMBIGUOUS = 3,
+    ICP_RAY_INVALID = 4, ICP_RAY_NUMERICAL = 5, ICP_RAY_OVERFLOW = 6, ICP_RAY_REPLAY = 7
+};
+
+typedef struct icp_context icp_context;
+
+/* ------------------------------------------------------------------ context */
+uint32_t icp_abi_version(void);
+/* Number of CUDA kernels this library has launched in this process (all contexts). */
+unsigned long long icp_kernel_launches(void);
+/* Copies the calling thread's last error message (NUL-terminated, truncated to n). */
+size_t icp_last_error(char* buffer, size_t n);
+/* Creates a context on CUDA device `device` with one non-blocking stream. */
+int icp_context_create(int device, icp_context** out);
+int icp_context_destroy(icp_context* ctx);
+/* Synchronises the context stream. */
+int icp_context_synchronize(icp_context* ctx);
+/* The context's cudaStream_t, for callers that enqueue their own work. */
+void* icp_context_stream(icp_context* ctx);
+/* Device memory owned by the context's caller (thin wrappers for FFI users). */
+int icp_device_alloc(icp_context* ctx, size_t bytes, void** out);
+int icp_device_free(icp_context* ctx, void* ptr);
+int icp_memcpy_h2d(icp_context* ctx, void* dst, const void* src, size_t bytes);
+int icp_memcpy_d2h(icp_context* ctx, void* dst, const void* src, size_t bytes);
+int icp_memset_d(icp_context* ctx, void* dst, int value, size_t bytes);
+
+/* -------------------------------------------------------------- (u,phi) grid */
+/* Ensemble-frame sampling grid: u = (1-cos theta)/2 rows, phi columns.
+ * ki, e0, e1: unit incident axis and its transverse frame (sampling_frame_columns). */
+typedef struct {
+    uint32_t nt, np;
+    double ki[3], e0[3], e1[3];
+} icp_grid;
+
+/* Writes the nt+1 saved u edges (bit-identical to make_phase_u_edges,
+ * include/rainbow/phase_cdf_math.hpp:16-32). Host function, no device use. */
+int icp_u_edges(uint32_t nt, double* edges_out);
+
+/* Statistics of one trace+bin call (raw sums in units of incident power per ray;
+ * multiply by the per-ray area weight to obtain mm^2). */
+typedef struct {
+    double escaped;          /* sum over rays of escaped power                              */
+    double unresolved;       /* sum over rays of residual power left when a ray stopped     */
+    double point_axial;      /* sum of power * cos(scattering angle) over binned exits      */
+    double forward_pole;     /* power within the forward pole cap                           */
+    double backward_pole;    /* power within the backward pole cap                          */
+    double max_ray_balance;  /* max |escaped + residual - 1| over rays                      */
+    double max_interface_balance; /* max relative Fresnel power imbalance at one interface   */
+    uint64_t rays;
+    uint64_t outputs;
+    uint64_t status_counts[8];
+    uint64_t rejected_rays;  /* rays failing the acceptance predicate (status/balance)      */
+    uint64_t snapped;        /* exits assigned to a cell edge by the roundoff snap rule     */
+    uint64_t near_edge;      /* FP32: interactions within rounding distance of a prism edge */
+    uint64_t fallback_adds;  /* exits that bypassed the shared-memory privatised table      */
+    uint64_t max_batch_outputs; /* largest number of exits produced by one batch of rays    */
+    uint64_t invalid;        /* exits that could not be binned (non-finite direction)       */
+    uint64_t encounters;     /* internal boundary interactions traced                       */
+} icp_trace_stats;
+
+/* Histogram privatisation / launch tuning (all zero = autotuned defaults). */
+typedef struct {
+    uint32_t block_threads;  /* 128..1024, multiple of 32                                     */
+    uint32_t blocks_per_sm;  /* resident blocks per SM requested                              */
+    uint32_t hash_slots;     /* shared-memory table slots (power of two; 0 = default; 1 = off) */
+    uint32_t reserved;
+} icp_tuning;
+
+/* ----------------------------------------------------------------- hex prism */
+/* One orientation node of a hexagonal prism (hex_trace/include/ice_crystal/hex_prism.hpp:6-12:
+ * circumradius R and FULL length L in mm, long axis body +y). */
+typedef struct {
+    double circumradius_mm, length_mm;
+    double rotation[9];       /* column-major body->ensemble rotation (active quaternion)  */
+    double exterior_index, interior_index;
+    double tail_tolerance;    /* per-ray residual power at which tracing stops              */
+    double balance_tolerance; /* per-ray |escaped+residual-1| acceptance bound              */
+    double area_weight;       /* mm^2 added to the histogram per unit exit power            */
+    uint64_t seed, total_samples, first_sample, sample_count;
+    uint32_t max_internal_hits;
+    uint32_t batch_size;      /* audit batch size (capacity check granularity)              */
+    uint32_t precision;       /* icp_precision                                              */
+    uint32_t reserved;
+} icp_hex_node;
+
+/* Projected area (mm^2) of the prism along the node's body-frame incident direction,
+ * rotation^T * grid.ki (hex_prism.hpp:37-43). Host function. */
+int icp_hex_node_area(const icp_hex_node* node, const icp_grid* grid, double* area_mm2);
+
+/* Traces sample_count rays of one node and adds area_weight * exit power into
+ * d_cell_mass[nt*np] (FP64, theta-major), pole caps into the stats.
+ * d_edges: nt+1 u edges on the device. d_stats: one icp_trace_stats on the device
+ * (accumulated into, caller zeroes). d_batch_outputs may be NULL or hold
+ * ceil(total_samples/batch_size) uint32 counters (accumulated into). */
+int icp_hex_trace_bin(icp_context* ctx, const icp_hex_node* node, const icp_grid* grid,
+                      const double* d_edges, double* d_cell_mass, icp_trace_stats* d_stats,
+                      uint32_t* d_batch_outputs, const icp_tuning* tuning);
+
+/* --------------------------------------------------------------------- CDF */
+typedef struct {
+    double max_l1_error;      /* 1e-10 */
+    double max_lost_mass;     /* 1e-12 */
+    double max_coarsening_tv; /* 1     */
+} icp_cdf_policy;
+
+typedef struct {
+    double g_source, g_stored, coarsening_tv, cdf_mass;
+    double l1_error, lost_mass, maximum_cell_error, aggregation_relative_error;
+    double fine_mass, fine_axial;
+    uint64_t lost_cells;
+    uint64_t malformed;
+    uint32_t status;          /* icp_status of the audit                                     */
+    uint32_t reserved;
+} icp_cdf_report;
+
+/* Input kinds for icp_phase_cdf_build. */
+enum icp_cdf_input { ICP_CDF_MASS = 0, ICP_CDF_DENSITY = 1 };
+
+/* Builds the stored CDF from a fine theta-major grid d_values[nt*np] (cell masses, or
+ * densities per steradian when input_kind == ICP_CDF_DENSITY).  forward_pole /
+ * backward_pole masses are spread uniformly over the first / last fine row
+ * (hex_phase/src/phase_table.cpp:63-76).  Aggregates conservatively to ct x cp
+ * (ct | nt, cp | np), scans each phi column in ascending theta with ordered binary64
+ * additions, scans the marginal in ascending phi, normalises and audits.
+ * Outputs (device): d_phi[cp+1], d_theta[cp*(ct+1)] (phi-major); the stored u edges are
+ * every (nt/ct)-th fine edge.  The report is written to host memory. */
+int icp_phase_cdf_build(icp_context* ctx, const double* d_values, uint32_t input_kind, uint32_t nt,
+                        uint32_t np, double forward_pole, double backward_pole, uint32_t ct, uint32_t cp,
+                        const icp_cdf_policy* policy, double* d_phi, double* d_theta, icp_cdf_report* report);
+
+/* ----------------------------------------------------- whole hex record (e2e) */
+typedef struct {
+    double circumradius_mm, length_mm;
+    double ki[3];             /* ensemble incident direction (normalised internally)          */
+    double exterior_index, interior_index;
+    double tail_tolerance, balance_tolerance;
+    uint32_t nt, np, ct, cp;  /* histogram and stored CDF dimensions                          */
+    uint32_t max_internal_hits, batch_size;
+    uint64_t max_output_records; /* per batch; 0 = unlimited                                  */
+    uint32_t precision, reserved;
+    icp_cdf_policy policy;
+    icp_tuning tuning;
+} icp_hex_record;
+
+typedef struct {
+    double quaternion[4];     /* w, x, y, z (active Hamilton, body -> ensemble)              */
+    double weight;            /* normalised number probability                               */
+    uint64_t samples, seed;
+} icp_orientation;
+
+typedef struct {
+    icp_trace_stats trace;    /* raw sums over all nodes (escaped/unresolved unweighted)     */
+    double expected_area_mm2, escaped_area_mm2, unresolved_area_mm2;
+    double histogram_mass_mm2, histogram_axial_mm2; /* fine grid (incl. poles), area units  */
+    double point_mass_mm2, point_axial_mm2, forward_mass_mm2, backward_mass_mm2;
+    double histogram_relative_error;
+    icp_cdf_report cdf;
+    double seconds_trace, seconds_cdf;
+} icp_record_report;
+
+/* Host-buffer entry point used by the ice_generate_phase drop-in: traces every node,
+ * bins, builds and audits the CDF, and copies phi[cp+1], theta[cp*(ct+1)], u[ct+1]
+ * to the caller's host arrays. Quality gates are NOT applied here (report only);
+ * the CLI applies them with the reference's tolerances. */
+int icp_hex_generate(icp_context* ctx, const icp_hex_record* record, const icp_orientation* nodes,
+                     uint32_t node_count, double* h_phi, double* h_theta, double* h_u,
+                     icp_record_report* report);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ICP_B200_H */

@@ -1,0 +1,27 @@
+#!/usr/bin/env bash
+# Builds the REFERENCE CPU hex path from its own source files, where they lie under
+# the read-only reference checkout, into oracle/_ref/ (git-ignored; travels with the
+# repository snapshot).  No reference build system is run: g++ compiles the few
+# translation units directly.  Test infrastructure only.
+#
+#   oracle/_ref/ice_generate_phase_cpu   reference CLI (hex_phase/apps/generate_hex_phase.cpp)
+#   oracle/_ref/ref_hex_harness          oracle/ref_hex_harness.cpp over the same sources
+#
+# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+set -euo pipefail
+here="$(cd "$(dirname "$0")" && pwd)"
+ref="${1:-/root/reference}"
+out="$here/_ref"
+if [ ! -d "$ref/hex_phase" ]; then
+    echo "build_ref.sh: reference sources not found at $ref (prebuilt files in $out are used as-is)" >&2
+    exit 0
+fi
+mkdir -p "$out"
+flags=(-std=c++20 -O2 -fno-fast-math -ffp-contract=off
+       -I"$ref/hex_trace/include" -I"$ref/hex_phase/include" -I"$ref/include")
+srcs=("$ref/hex_phase/src/phase_table.cpp" "$ref/hex_phase/src/phase_generate.cpp"
+      "$ref/hex_phase/src/orientation_plan.cpp" "$ref/hex_trace/src/hex_trace.cpp"
+      "$ref/src/npy_writer.cpp")
+g++ "${flags[@]}" "$ref/hex_phase/apps/generate_hex_phase.cpp" "${srcs[@]}" -o "$out/ice_generate_phase_cpu"
+g++ "${flags[@]}" "$here/ref_hex_harness.cpp" "${srcs[@]}" -o "$out/ref_hex_harness"
+echo "built $out/ice_generate_phase_cpu $out/ref_hex_harness"

@@ -1,0 +1,998 @@
+/*
+ * icp_oracle.c -- CPU restatement of the reference phase-function path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA product
+ * path; nothing in the product links, loads or calls it.  Only tests/,
+ * __graft_entry__.smoke() and bench.py's CPU-baseline leg use it.
+ *
+ * It restates, in plain C (binary64, no FMA contraction, same operation
+ * order), the algorithm of the reference hex-prism Monte Carlo path of
+ * Somatic-Cell/ice-crystal-phase:
+ *   counter RNG            hex_trace/include/ice_crystal/math.hpp:136-146
+ *   vectors / frames       hex_trace/include/ice_crystal/math.hpp:23-133
+ *   prism geometry         hex_trace/include/ice_crystal/hex_prism.hpp:10-175
+ *   Fresnel flux split     hex_trace/include/ice_crystal/flux_interface.hpp:13-88
+ *   linear R/T chain       hex_trace/include/ice_crystal/hex_trace_core.hpp:155-259
+ *   (u,phi) binning        hex_phase/include/ice_crystal/phase_math.hpp:37-81
+ *   Kahan mass histogram   hex_phase/src/phase_table.cpp:39-103
+ *   CPU CDF builder        hex_phase/src/phase_table.cpp:104-187
+ *   u edges                include/rainbow/phase_cdf_math.hpp:16-32
+ *   quaternion rotation    hex_phase/src/phase_table.cpp:11-21
+ * Parity is pinned: tests compare this restatement bit-for-bit with the
+ * reference sources compiled from their own files into oracle/_ref
+ * (oracle/build_ref.sh) and with fixtures under tests/golden/.
+ *
+ * Build: oracle/build_oracle.sh (gcc -O2 -ffp-contract=off -fno-fast-math).
+ */
+#include <float.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define ICPO_PI 3.141592653589793238462643383279502884
+#define ICPO_SQRT3 1.732050807568877293527446341505872367
+#define ICPO_EPS DBL_EPSILON
+
+/* ---------------------------------------------------------------- scalars */
+static int fin(double x) { return x >= -DBL_MAX && x <= DBL_MAX; }
+static double mx(double a, double b) { return a > b ? a : b; }
+
+typedef struct { double x, y, z; } v3;
+static v3 v_add(v3 a, v3 b) { v3 r = {a.x + b.x, a.y + b.y, a.z + b.z}; return r; }
+static v3 v_sub(v3 a, v3 b) { v3 r = {a.x - b.x, a.y - b.y, a.z - b.z}; return r; }
+static v3 v_neg(v3 a) { v3 r = {-a.x, -a.y, -a.z}; return r; }
+static v3 v_mul(v3 a, double s) { v3 r = {a.x * s, a.y * s, a.z * s}; return r; }
+static v3 v_div(v3 a, double s) { v3 r = {a.x / s, a.y / s, a.z / s}; return r; }
+static double v_dot(v3 a, v3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static v3 v_cross(v3 a, v3 b)
+{
+    v3 r = {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+    return r;
+}
+static int v_fin(v3 a) { return fin(a.x) && fin(a.y) && fin(a.z); }
+static double v_maxabs(v3 a) { return mx(fabs(a.x), mx(fabs(a.y), fabs(a.z))); }
+
+/* math.hpp:38-47: scale by the largest component first, then divide by the norm. */
+static int v_normalize(v3 a, v3* out)
+{
+    double s = v_maxabs(a), n;
+    if (!(s > 0) || !fin(s)) return 0;
+    a = v_div(a, s);
+    n = sqrt(v_dot(a, a));
+    if (!(n > 0) || !fin(n)) return 0;
+    *out = v_div(a, n);
+    return v_fin(*out);
+}
+static int v_is_unit(v3 a) { return v_fin(a) && fabs(v_dot(a, a) - 1.0) <= 128 * ICPO_EPS; }
+
+typedef struct { v3 e0, e1; } frame_t;
+/* math.hpp:53-59 */
+static int frame_valid(frame_t f, v3 k)
+{
+    return v_is_unit(k) && v_is_unit(f.e0) && v_is_unit(f.e1) &&
+           fabs(v_dot(k, f.e0)) <= 128 * ICPO_EPS && fabs(v_dot(k, f.e1)) <= 128 * ICPO_EPS &&
+           v_maxabs(v_sub(v_cross(k, f.e0), f.e1)) <= 256 * ICPO_EPS;
+}
+/* math.hpp:61-69: helper axis = the coordinate axis least aligned with k. */
+static int make_frame(v3 k, frame_t* f)
+{
+    double ax, ay, az;
+    v3 a;
+    if (!v_is_unit(k)) return 0;
+    ax = fabs(k.x); ay = fabs(k.y); az = fabs(k.z);
+    if (ax <= ay && ax <= az) { a.x = 1; a.y = 0; a.z = 0; }
+    else if (ay <= az) { a.x = 0; a.y = 1; a.z = 0; }
+    else { a.x = 0; a.y = 0; a.z = 1; }
+    if (!v_normalize(v_sub(a, v_mul(k, v_dot(k, a))), &f->e0)) return 0;
+    if (!v_normalize(v_cross(k, f->e0), &f->e1)) return 0;
+    return frame_valid(*f, k);
+}
+
+/* math.hpp:70-78 */
+typedef struct { double re, im; } cplx;
+static cplx c_add(cplx a, cplx b) { cplx r = {a.re + b.re, a.im + b.im}; return r; }
+static cplx c_muld(cplx a, double b) { cplx r = {a.re * b, a.im * b}; return r; }
+static cplx c_mul(cplx a, cplx b)
+{
+    cplx r = {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+    return r;
+}
+static double c_norm2(cplx a) { return a.re * a.re + a.im * a.im; }
+
+/* math.hpp:79-109: two response columns (unit incident fields), rows in the transverse frame. */
+typedef struct { cplx x, y; } field_t;
+typedef struct { field_t col[2]; } jones_t;
+static jones_t jones_identity(void)
+{
+    jones_t j;
+    memset(&j, 0, sizeof j);
+    j.col[0].x.re = 1;
+    j.col[1].y.re = 1;
+    return j;
+}
+static double jones_power(const jones_t* j)
+{
+    return 0.5 * (c_norm2(j->col[0].x) + c_norm2(j->col[0].y) + c_norm2(j->col[1].x) + c_norm2(j->col[1].y));
+}
+static int jones_finite(const jones_t* j)
+{
+    int i;
+    for (i = 0; i < 2; ++i)
+        if (!fin(j->col[i].x.re) || !fin(j->col[i].x.im) || !fin(j->col[i].y.re) || !fin(j->col[i].y.im)) return 0;
+    return 1;
+}
+static int jones_nonzero(const jones_t* j)
+{
+    int i;
+    for (i = 0; i < 2; ++i)
+        if (j->col[i].x.re != 0 || j->col[i].x.im != 0 || j->col[i].y.re != 0 || j->col[i].y.im != 0) return 1;
+    return 0;
+}
+/* math.hpp:110-119 */
+static jones_t change_frame(const jones_t* j, frame_t o, frame_t n)
+{
+    jones_t r;
+    int c;
+    for (c = 0; c < 2; ++c) {
+        r.col[c].x = c_add(c_muld(j->col[c].x, v_dot(o.e0, n.e0)), c_muld(j->col[c].y, v_dot(o.e1, n.e0)));
+        r.col[c].y = c_add(c_muld(j->col[c].x, v_dot(o.e0, n.e1)), c_muld(j->col[c].y, v_dot(o.e1, n.e1)));
+    }
+    return r;
+}
+/* math.hpp:120-124 */
+static jones_t scale_rows(jones_t j, cplx s, cplx p)
+{
+    int c;
+    for (c = 0; c < 2; ++c) {
+        j.col[c].x = c_mul(j.col[c].x, s);
+        j.col[c].y = c_mul(j.col[c].y, p);
+    }
+    return j;
+}
+
+/* math.hpp:125-133: Kahan sum with a separate correction term. */
+typedef struct { double value, correction; } ksum;
+static void ks_add(ksum* s, double x)
+{
+    double y = x - s->correction, t = s->value + y;
+    s->correction = (t - s->value) - y;
+    s->value = t;
+}
+
+/* math.hpp:136-146: SplitMix64 finaliser over a golden-ratio counter; 52-bit midpoints. */
+static uint64_t mix64(uint64_t x)
+{
+    x = (x ^ (x >> 30)) * UINT64_C(0xbf58476d1ce4e5b9);
+    x = (x ^ (x >> 27)) * UINT64_C(0x94d049bb133111eb);
+    return x ^ (x >> 31);
+}
+double icpo_sample_uniform(uint64_t seed, uint64_t id, unsigned dim)
+{
+    uint64_t x = mix64(seed + UINT64_C(0x9e3779b97f4a7c15) * (3 * id + dim + 1));
+    return ((double)(x >> 12) + 0.5) * 0x1p-52;
+}
+
+/* ----------------------------------------------------------- hex prism */
+/* hex_prism.hpp:10-52: circumradius R, full length L, long axis +y; coordinates are x/R. */
+typedef struct { double R, L; } prism_t;
+static double pr_half(prism_t h) { return 0.5 * (h.L / h.R); }
+static int pr_valid(prism_t h)
+{
+    return fin(h.R) && fin(h.L) && h.R > 0 && h.L > 0 && fin(pr_half(h)) && pr_half(h) > 0 &&
+           fin(h.R * h.R) && h.R * h.R > 0 && fin(h.R * h.L) && h.R * h.L > 0;
+}
+static v3 pr_normal(unsigned f)
+{
+    v3 r = {0, 0, 0};
+    switch (f) {
+    case 0: r.x = 1; break;
+    case 1: r.x = 0.5; r.z = ICPO_SQRT3 / 2; break;
+    case 2: r.x = -0.5; r.z = ICPO_SQRT3 / 2; break;
+    case 3: r.x = -1; break;
+    case 4: r.x = -0.5; r.z = -ICPO_SQRT3 / 2; break;
+    case 5: r.x = 0.5; r.z = -ICPO_SQRT3 / 2; break;
+    case 6: r.y = 1; break;
+    case 7: r.y = -1; break;
+    default: break;
+    }
+    return r;
+}
+static v3 pr_vertex(unsigned f)
+{
+    v3 r = {0, 0, 0};
+    switch (f % 6) {
+    case 0: r.x = ICPO_SQRT3 / 2; r.z = 0.5; break;
+    case 1: r.z = 1; break;
+    case 2: r.x = -ICPO_SQRT3 / 2; r.z = 0.5; break;
+    case 3: r.x = -ICPO_SQRT3 / 2; r.z = -0.5; break;
+    case 4: r.z = -1; break;
+    default: r.x = ICPO_SQRT3 / 2; r.z = -0.5; break;
+    }
+    return r;
+}
+static double pr_offset(prism_t h, unsigned f) { return f < 6 ? ICPO_SQRT3 / 2 : pr_half(h); }
+static double pr_face_area(prism_t h, unsigned f) { return f < 6 ? h.R * h.L : (3 * ICPO_SQRT3 / 2) * h.R * h.R; }
+double icpo_hex_projected_area(double R, double L, const double k[3])
+{
+    prism_t h = {R, L};
+    v3 kk = {k[0], k[1], k[2]};
+    ksum a = {0, 0};
+    unsigned f;
+    for (f = 0; f < 8; ++f) ks_add(&a, pr_face_area(h, f) * mx(0, -v_dot(pr_normal(f), kk)));
+    return a.value;
+}
+static double pr_projected(prism_t h, v3 k)
+{
+    double kk[3] = {k.x, k.y, k.z};
+    return icpo_hex_projected_area(h.R, h.L, kk);
+}
+/* hex_prism.hpp:54-57 */
+static double geom_tol(prism_t h, v3 p, double t)
+{
+    return 128 * ICPO_EPS * mx(1, mx(pr_half(h), mx(v_maxabs(p), fabs(t))));
+}
+
+typedef struct { v3 pos; unsigned face; int valid; } entry_t;
+/* hex_prism.hpp:64-98: face chosen in proportion to projected face area. */
+static entry_t sample_entry(prism_t h, v3 k, double u0, double u1, double u2)
+{
+    entry_t s;
+    double a, target, acc = 0;
+    unsigned last = 8, f;
+    memset(&s, 0, sizeof s);
+    s.face = 8;
+    if (!pr_valid(h) || !v_is_unit(k) || !(u0 >= 0 && u0 < 1 && u1 >= 0 && u1 < 1 && u2 >= 0 && u2 < 1)) return s;
+    a = pr_projected(h, k);
+    if (!(a > 0) || !fin(a)) return s;
+    target = u0 * a;
+    for (f = 0; f < 8; ++f) {
+        double w = pr_face_area(h, f) * mx(0, -v_dot(pr_normal(f), k));
+        if (!(w > 0)) continue;
+        last = f;
+        acc += w;
+        if (target < acc) { s.face = f; break; }
+    }
+    if (s.face == 8) s.face = last;
+    if (s.face == 8) return s;
+    if (s.face < 6) {
+        v3 n = pr_normal(s.face), tangent = {-n.z, 0, n.x}, axial = {0, (2 * u2 - 1) * pr_half(h), 0};
+        s.pos = v_add(v_add(v_mul(n, ICPO_SQRT3 / 2), v_mul(tangent, u1 - 0.5)), axial);
+    } else {
+        double sector = 6 * u1, r;
+        unsigned j = (unsigned)sector;
+        r = sqrt(sector - (double)j);
+        s.pos = v_mul(v_add(v_mul(pr_vertex(j), 1 - u2), v_mul(pr_vertex(j + 1), u2)), r);
+        s.pos.y = (s.face == 6 ? 1 : -1) * pr_half(h);
+    }
+    s.valid = v_fin(s.pos);
+    return s;
+}
+
+enum { HIT_REGULAR = 0, HIT_MISS = 1, HIT_AMBIGUOUS = 2, HIT_INVALID = 3 };
+typedef struct { v3 pos; double t; unsigned face; int status; } hit_t;
+/* hex_prism.hpp:108-120 */
+static int strict_face_point(prism_t h, v3 p, unsigned face)
+{
+    double tol;
+    unsigned f;
+    if (face >= 8 || !v_fin(p)) return 0;
+    tol = geom_tol(h, p, 0);
+    for (f = 0; f < 8; ++f) {
+        double gap = pr_offset(h, f) - v_dot(pr_normal(f), p);
+        if (f == face) { if (fabs(gap) > tol) return 0; }
+        else if (!(gap > tol)) return 0;
+    }
+    return 1;
+}
+/* hex_prism.hpp:123-147: nearest exit plane; an edge/vertex tie is reported as ambiguous. */
+static hit_t next_boundary(prism_t h, v3 p, v3 d, unsigned start)
+{
+    hit_t hit;
+    double best = DBL_MAX, second = DBL_MAX, tol;
+    unsigned f;
+    memset(&hit, 0, sizeof hit);
+    hit.face = 8;
+    hit.status = HIT_INVALID;
+    if (!pr_valid(h) || !v_is_unit(d) || start >= 8) return hit;
+    if (!strict_face_point(h, p, start)) { hit.status = HIT_AMBIGUOUS; return hit; }
+    if (v_dot(pr_normal(start), d) > 128 * ICPO_EPS) return hit;
+    for (f = 0; f < 8; ++f) {
+        double cosine, t;
+        if (f == start) continue;
+        cosine = v_dot(pr_normal(f), d);
+        if (!(cosine > 0)) continue;
+        t = (pr_offset(h, f) - v_dot(pr_normal(f), p)) / cosine;
+        if (!(t > 0) || !fin(t)) continue;
+        if (t < best) { second = best; best = t; hit.face = f; }
+        else if (t < second) second = t;
+    }
+    if (hit.face == 8) return hit;
+    hit.t = best;
+    hit.pos = v_add(p, v_mul(d, best));
+    tol = geom_tol(h, hit.pos, best);
+    if (second - best <= tol || !strict_face_point(h, hit.pos, hit.face)) hit.status = HIT_AMBIGUOUS;
+    else hit.status = HIT_REGULAR;
+    return hit;
+}
+
+/* ------------------------------------------------------ Fresnel (flux) */
+typedef struct { v3 d; frame_t fr; jones_t j; } fray_t;
+typedef struct { fray_t refl, trans; double balance; int valid, has_t, tir; } branches_t;
+/* flux_interface.hpp:13-19 */
+static cplx tir_phase(double a, double b)
+{
+    double s = mx(fabs(a), fabs(b)), den;
+    cplx r;
+    a /= s;
+    b /= s;
+    den = a * a + b * b;
+    r.re = (a * a - b * b) / den;
+    r.im = -2 * a * b / den;
+    return r;
+}
+/* flux_interface.hpp:26-88: s/p split in flux normalisation; n points into the incident medium. */
+static branches_t split_flux(const fray_t* ray, v3 n, double ni, double nt)
+{
+    branches_t b;
+    double ci, scale, sine, ns, a, c, eta, st, before, after;
+    v3 s, scaled, pin;
+    jones_t j;
+    frame_t spf;
+    cplx rs = {0, 0}, rp = {0, 0};
+    memset(&b, 0, sizeof b);
+    if (!frame_valid(ray->fr, ray->d) || !v_is_unit(n) || !jones_finite(&ray->j) ||
+        !(ni > 0 && nt > 0 && fin(ni) && fin(nt)))
+        return b;
+    ci = -v_dot(ray->d, n);
+    if (ci < 0 || ci > 1 + 128 * ICPO_EPS) return b;
+    if (ci > 1) ci = 1;
+    if (ni == nt) {
+        b.trans = *ray;
+        b.has_t = 1;
+        b.refl.d = v_add(ray->d, v_mul(n, 2 * ci));
+        if (!v_normalize(b.refl.d, &b.refl.d)) return b;
+        if (!make_frame(b.refl.d, &b.refl.fr)) return b;
+        b.valid = 1;
+        return b;
+    }
+    s = v_cross(ray->d, n);
+    scale = v_maxabs(s);
+    if (scale > 0) scaled = v_div(s, scale);
+    else { scaled.x = 0; scaled.y = 0; scaled.z = 0; }
+    sine = scale * sqrt(v_dot(scaled, scaled));
+    if (sine > 0) { if (!v_normalize(s, &s)) return b; }
+    else s = ray->fr.e0;
+    if (!v_normalize(v_cross(ray->d, s), &pin)) return b;
+    spf.e0 = s;
+    spf.e1 = pin;
+    j = change_frame(&ray->j, ray->fr, spf);
+    ns = mx(ni, nt);
+    a = ni / ns;
+    c = nt / ns;
+    eta = a / c;
+    if (!fin(eta) || !(a > 0 && c > 0)) return b;
+    st = eta * sine;
+    if (!fin(st)) return b;
+    if (!v_normalize(v_add(ray->d, v_mul(n, 2 * ci)), &b.refl.d)) return b;
+    b.refl.fr.e0 = s;
+    if (!v_normalize(v_cross(b.refl.d, s), &b.refl.fr.e1)) return b;
+    if (st > 1) {
+        double inverse = 1 / st, beta = st * sqrt((1 - inverse) * (1 + inverse));
+        rs = tir_phase(a * ci, c * beta);
+        rp = tir_phase(c * ci, a * beta);
+        b.tir = 1;
+    } else {
+        double ct = sqrt((1 - st) * (1 + st)), ds = a * ci + c * ct, dp = c * ci + a * ct, numerator, ts, tp;
+        cplx cts, ctp;
+        if (!(ds > 0 && dp > 0)) return b;
+        rs.re = (a * ci - c * ct) / ds;
+        rp.re = (c * ci - a * ct) / dp;
+        numerator = 2 * sqrt(a * ci) * sqrt(c * ct);
+        ts = numerator / ds;
+        tp = numerator / dp;
+        cts.re = ts; cts.im = 0;
+        ctp.re = tp; ctp.im = 0;
+        b.trans.j = scale_rows(j, cts, ctp);
+        if (!v_normalize(v_sub(v_mul(v_add(ray->d, v_mul(n, ci)), eta), v_mul(n, ct)), &b.trans.d)) return b;
+        b.trans.fr.e0 = s;
+        if (!v_normalize(v_cross(b.trans.d, s), &b.trans.fr.e1)) return b;
+        b.has_t = 1;
+    }
+    b.refl.j = scale_rows(j, rs, rp);
+    before = jones_power(&ray->j);
+    after = jones_power(&b.refl.j) + (b.has_t ? jones_power(&b.trans.j) : 0);
+    b.balance = after - before;
+    b.valid = frame_valid(b.refl.fr, b.refl.d) && jones_finite(&b.refl.j) &&
+              (!b.has_t || (frame_valid(b.trans.fr, b.trans.d) && jones_finite(&b.trans.j))) &&
+              fin(b.balance) && fabs(b.balance) <= 2048 * ICPO_EPS * mx(before, DBL_MIN);
+    return b;
+}
+
+/* ----------------------------------------------------------- ray chain */
+/* Status codes follow hex_trace_core.hpp:97-102. */
+enum {
+    ST_EXHAUSTED = 0, ST_TAIL = 1, ST_LIMIT = 2, ST_AMBIGUOUS = 3,
+    ST_INVALID = 4, ST_NUMERICAL = 5, ST_OVERFLOW = 6, ST_REPLAY = 7
+};
+
+typedef struct {
+    prism_t prism;
+    v3 k;
+    frame_t kf;
+    double n_ext, n_int, tail;
+    uint64_t seed, total;
+    uint32_t max_hits;
+} trace_cfg_t;
+
+/* One emitted exit; the histogram consumes only its direction and power. */
+typedef struct { v3 d; double power; } exit_t;
+
+typedef struct {
+    double escaped, unresolved, balance, max_iface;
+    uint64_t outputs;
+    uint32_t hits, tir;
+    int status;
+} ray_audit_t;
+
+typedef void (*emit_fn)(void* user, v3 d, double power);
+
+/* hex_trace_core.hpp:155-162 */
+static int cfg_valid(const trace_cfg_t* c)
+{
+    double a = pr_projected(c->prism, c->k);
+    return pr_valid(c->prism) && frame_valid(c->kf, c->k) && fin(c->n_ext) && fin(c->n_int) && c->n_ext > 0 &&
+           c->n_int > 0 && fin(c->tail) && c->tail >= 0 && c->tail < 1 && c->total > 0 && c->max_hits > 0 &&
+           fin(a) && a > 0;
+}
+static ray_audit_t finish_audit(ray_audit_t a, const ksum* esc, double residual, int status)
+{
+    a.escaped = esc->value;
+    a.unresolved = residual;
+    a.balance = esc->value + residual - 1;
+    a.status = status;
+    return a;
+}
+/* hex_trace_core.hpp:169-184 */
+static int emit_exit(emit_fn emit, void* user, ray_audit_t* a, ksum* esc, const trace_cfg_t* c, const fray_t* ray, v3 pos)
+{
+    double power = jones_power(&ray->j);
+    v3 pmm;
+    if (!fin(power) || power < 0 || (!power && jones_nonzero(&ray->j))) return ST_NUMERICAL;
+    if (power == 0) return ST_EXHAUSTED;
+    pmm = v_mul(pos, c->prism.R);
+    if (!v_fin(pmm)) return ST_NUMERICAL;
+    if (emit) emit(user, ray->d, power);
+    ks_add(esc, power);
+    ++a->outputs;
+    return ST_EXHAUSTED;
+}
+/* hex_trace_core.hpp:190-252: exterior R once, then T at every internal hit while R continues. */
+static ray_audit_t trace_from_entry(const trace_cfg_t* c, uint64_t id, entry_t e, emit_fn emit, void* user)
+{
+    ray_audit_t a;
+    ksum esc = {0, 0}, length = {0, 0};
+    fray_t inc, ray;
+    branches_t sp;
+    v3 p;
+    unsigned cur, encounter;
+    int em;
+    double remaining;
+    memset(&a, 0, sizeof a);
+    a.unresolved = 1;
+    a.status = ST_INVALID;
+    if (!cfg_valid(c) || id >= c->total || !e.valid || e.face >= 8) return finish_audit(a, &esc, 1, ST_INVALID);
+    if (!strict_face_point(c->prism, e.pos, e.face)) return finish_audit(a, &esc, 1, ST_AMBIGUOUS);
+    if (!(v_dot(pr_normal(e.face), c->k) < 0)) return finish_audit(a, &esc, 1, ST_INVALID);
+    inc.d = c->k;
+    inc.fr = c->kf;
+    inc.j = jones_identity();
+    sp = split_flux(&inc, pr_normal(e.face), c->n_ext, c->n_int);
+    if (!sp.valid) return finish_audit(a, &esc, 1, ST_NUMERICAL);
+    a.max_iface = fabs(sp.balance);
+    em = emit_exit(emit, user, &a, &esc, c, &sp.refl, e.pos);
+    if (em != ST_EXHAUSTED) return finish_audit(a, &esc, 1, em);
+    if (!sp.has_t) { a.tir = 1; return finish_audit(a, &esc, 0, ST_EXHAUSTED); }
+    ray = sp.trans;
+    p = e.pos;
+    cur = e.face;
+    for (encounter = 0; encounter < c->max_hits; ++encounter) {
+        double power = jones_power(&ray.j), segment;
+        hit_t hit;
+        if (!fin(power) || power < 0 || (!power && jones_nonzero(&ray.j))) return finish_audit(a, &esc, power, ST_NUMERICAL);
+        if (power == 0) return finish_audit(a, &esc, 0, ST_EXHAUSTED);
+        if (power <= c->tail) return finish_audit(a, &esc, power, ST_TAIL);
+        hit = next_boundary(c->prism, p, ray.d, cur);
+        if (hit.status != HIT_REGULAR)
+            return finish_audit(a, &esc, power, hit.status == HIT_AMBIGUOUS ? ST_AMBIGUOUS : ST_NUMERICAL);
+        segment = hit.t * c->prism.R;
+        if (!fin(segment) || segment < 0) return finish_audit(a, &esc, power, ST_NUMERICAL);
+        ks_add(&length, segment);
+        if (!fin(length.value)) return finish_audit(a, &esc, power, ST_NUMERICAL);
+        sp = split_flux(&ray, v_neg(pr_normal(hit.face)), c->n_int, c->n_ext);
+        if (!sp.valid) return finish_audit(a, &esc, power, ST_NUMERICAL);
+        ++a.hits;
+        if (sp.tir) ++a.tir;
+        a.max_iface = mx(a.max_iface, fabs(sp.balance));
+        if (sp.has_t) {
+            em = emit_exit(emit, user, &a, &esc, c, &sp.trans, hit.pos);
+            if (em != ST_EXHAUSTED) return finish_audit(a, &esc, power, em);
+        }
+        ray = sp.refl;
+        p = hit.pos;
+        cur = hit.face;
+    }
+    remaining = jones_power(&ray.j);
+    if (!fin(remaining) || remaining < 0 || (!remaining && jones_nonzero(&ray.j)))
+        return finish_audit(a, &esc, remaining, ST_NUMERICAL);
+    return finish_audit(a, &esc, remaining,
+                        remaining == 0 ? ST_EXHAUSTED : (remaining <= c->tail ? ST_TAIL : ST_LIMIT));
+}
+/* hex_trace_core.hpp:253-259 */
+static ray_audit_t trace_sample(const trace_cfg_t* c, uint64_t id, emit_fn emit, void* user)
+{
+    entry_t e = sample_entry(c->prism, c->k, icpo_sample_uniform(c->seed, id, 0), icpo_sample_uniform(c->seed, id, 1),
+                             icpo_sample_uniform(c->seed, id, 2));
+    return trace_from_entry(c, id, e, emit, user);
+}
+
+/* ------------------------------------------------------------- binning */
+typedef struct {
+    const double* edges;
+    v3 ki;
+    frame_t fr;
+    uint32_t nt, np;
+} grid_t;
+typedef struct { uint64_t index; double mu; int pole, valid, snapped; } bin_t;
+
+/* phase_math.hpp:37-81: u row by binary search on the saved edges, phi column via atan2,
+ * canonical half-open assignment within a 64-epsilon roundoff window. */
+static bin_t phase_bin(const grid_t* g, v3 d)
+{
+    bin_t b;
+    double x, y, z, n, mu, s, u, phi, v, index, nearest;
+    uint32_t lo, hi, j;
+    unsigned cand;
+    memset(&b, 0, sizeof b);
+    if (!g->edges || !g->nt || !g->np || !v_is_unit(d)) return b;
+    x = v_dot(g->fr.e0, d);
+    y = v_dot(g->fr.e1, d);
+    z = v_dot(g->ki, d);
+    n = sqrt(x * x + y * y + z * z);
+    if (!(n > 0) || !fin(n) || fabs(n - 1) > 512 * ICPO_EPS) return b;
+    mu = z / n;
+    s = hypot(x, y) / n;
+    b.mu = mu;
+    if (s <= 256 * ICPO_EPS) { b.pole = mu >= 0 ? 1 : -1; b.valid = 1; return b; }
+    u = mu >= 0 ? (0.5 * s * s) / (1 + mu) : 1 - (0.5 * s * s) / (1 - mu);
+    if (!(u >= 0 && u <= 1)) return b;
+    lo = 0;
+    hi = g->nt;
+    while (lo + 1 < hi) {
+        uint32_t mid = lo + (hi - lo) / 2;
+        if (u >= g->edges[mid]) lo = mid; else hi = mid;
+    }
+    for (cand = 0; cand < 2; ++cand) {
+        uint32_t e = lo + cand;
+        double width, tol;
+        if (e == 0 || e >= g->nt) continue;
+        width = fmin(g->edges[e] - g->edges[e - 1], g->edges[e + 1] - g->edges[e]);
+        tol = fmin(64 * ICPO_EPS * fmax(fabs(u), fabs(g->edges[e])), 1e-7 * width);
+        if (fabs(u - g->edges[e]) <= tol) { b.snapped = (u != g->edges[e]); lo = e; break; }
+    }
+    phi = atan2(y, x);
+    if (phi >= ICPO_PI) phi -= 2 * ICPO_PI;
+    v = (phi + ICPO_PI) / (2 * ICPO_PI);
+    index = v * g->np;
+    nearest = floor(index + 0.5);
+    if (fabs(index - nearest) <= fmin(64 * ICPO_EPS * g->np, 1e-7)) {
+        b.snapped = b.snapped || (index != nearest);
+        index = nearest;
+    }
+    j = (uint32_t)index;
+    if (j == g->np) j = 0;
+    if (j >= g->np) return b;
+    b.index = (uint64_t)lo * g->np + j;
+    b.valid = 1;
+    return b;
+}
+
+/* include/rainbow/phase_cdf_math.hpp:16-32: symmetric sin^2 edges with exact endpoints. */
+int icpo_u_edges(uint32_t n, double* edges)
+{
+    uint32_t i;
+    if (n == 0) return -1;
+    edges[0] = 0;
+    edges[n] = 1;
+    for (i = 1; i < n; ++i) {
+        uint32_t k = i < n - i ? i : n - i;
+        double s = sin((0.5 * ICPO_PI) * (double)k / (double)n);
+        edges[i] = i <= n / 2u ? s * s : 1.0 - s * s;
+    }
+    for (i = 0; i < n; ++i)
+        if (!(edges[i + 1] > edges[i])) return -2;
+    return 0;
+}
+
+/* hex_phase/src/phase_table.cpp:11-21: active Hamilton quaternion (w,x,y,z); columns body->ensemble. */
+typedef struct { v3 x, y, z; } rot_t;
+static v3 rot_apply(const rot_t* r, v3 p) { return v_add(v_add(v_mul(r->x, p.x), v_mul(r->y, p.y)), v_mul(r->z, p.z)); }
+static v3 rot_inverse(const rot_t* r, v3 p)
+{
+    v3 o = {v_dot(r->x, p), v_dot(r->y, p), v_dot(r->z, p)};
+    return o;
+}
+static int rot_valid(const rot_t* r)
+{
+    return v_is_unit(r->x) && v_is_unit(r->y) && v_is_unit(r->z) && fabs(v_dot(r->x, r->y)) <= 128 * ICPO_EPS &&
+           v_maxabs(v_sub(v_cross(r->x, r->y), r->z)) <= 256 * ICPO_EPS;
+}
+int icpo_rotation_from_quaternion(double w, double x, double y, double z, double out[9])
+{
+    double n = w * w + x * x + y * y + z * z, k;
+    rot_t r;
+    if (!fin(n) || fabs(n - 1) > 2e-12) return -1;
+    k = 1 / sqrt(n);
+    w *= k; x *= k; y *= k; z *= k;
+    r.x.x = 1 - 2 * (y * y + z * z); r.x.y = 2 * (x * y + w * z); r.x.z = 2 * (x * z - w * y);
+    r.y.x = 2 * (x * y - w * z); r.y.y = 1 - 2 * (x * x + z * z); r.y.z = 2 * (y * z + w * x);
+    r.z.x = 2 * (x * z + w * y); r.z.y = 2 * (y * z - w * x); r.z.z = 1 - 2 * (x * x + y * y);
+    if (!rot_valid(&r)) return -2;
+    /* column-major: out[0..2] = x column, out[3..5] = y column, out[6..8] = z column */
+    out[0] = r.x.x; out[1] = r.x.y; out[2] = r.x.z;
+    out[3] = r.y.x; out[4] = r.y.y; out[5] = r.y.z;
+    out[6] = r.z.x; out[7] = r.z.y; out[8] = r.z.z;
+    return 0;
+}
+
+/* math.hpp:61-69 exported for host-side frame conventions (ki must already be unit). */
+int icpo_make_frame(const double k_in[3], double k_out[3], double e0[3], double e1[3])
+{
+    v3 k = {k_in[0], k_in[1], k_in[2]}, kn;
+    frame_t f;
+    if (!v_normalize(k, &kn)) return -1;
+    if (!make_frame(kn, &f)) return -2;
+    k_out[0] = kn.x; k_out[1] = kn.y; k_out[2] = kn.z;
+    e0[0] = f.e0.x; e0[1] = f.e0.y; e0[2] = f.e0.z;
+    e1[0] = f.e1.x; e1[1] = f.e1.y; e1[2] = f.e1.z;
+    return 0;
+}
+
+/* ---------------------------------------------------- mass histogram */
+/* Accumulator state (phase_table.cpp:39-62); cells are Kahan pairs (value, correction). */
+typedef struct {
+    grid_t grid;
+    ksum* cells;
+    ksum point_mass, point_axial, forward, backward;
+    uint64_t count, snapped;
+    int error;
+    rot_t rot;
+    double scale;
+} hist_t;
+
+static void hist_emit(void* user, v3 d, double power)
+{
+    hist_t* h = (hist_t*)user;
+    double w = h->scale * power;
+    bin_t b;
+    if (h->error) return;
+    if (!(power > 0) || !fin(power) || !(w > 0) || !fin(w)) { h->error = 1; return; }
+    b = phase_bin(&h->grid, rot_apply(&h->rot, d));
+    if (!b.valid) { h->error = 2; return; }
+    ++h->count;
+    h->snapped += b.snapped;
+    ks_add(&h->point_mass, w);
+    ks_add(&h->point_axial, w * b.mu);
+    if (b.pole > 0) ks_add(&h->forward, w);
+    else if (b.pole < 0) ks_add(&h->backward, w);
+    else ks_add(&h->cells[b.index], w);
+}
+
+/*
+ * Public hex entry: trace rays [first, first+count) of one orientation node and
+ * add their exits to an existing Kahan histogram (cells: 2*nt*np doubles).
+ *
+ * node[] layout (doubles): R, L, n_ext, n_int, tail, normalised orientation weight.
+ *   The body-frame incident direction is the grid axis under the inverse rotation and the
+ *   per-ray area weight is weight * Aproj / samples (generate_hex_phase.cpp:101-102).
+ * grid_frame[] layout: ki(3), e0(3), e1(3) of the ensemble grid.
+ * rot[] column-major body->ensemble rotation (9).
+ * stats[] (inout, doubles): point_mass(v,c), point_axial(v,c), forward(v,c), backward(v,c),
+ *   escaped_sum, unresolved_sum, max_balance, max_iface, [14..]=batch escaped kahan value/corr,...
+ * counts[] (inout, uint64): samples, snapped, outputs, rays, status[8]
+ * Audits follow the reference CLI: per batch of batch_size rays a Kahan summary
+ * (hex_trace/src/hex_trace.cpp:72-88) is merged with plain adds (:89-100).
+ */
+static rot_t rot_from(const double* r9)
+{
+    rot_t r;
+    r.x.x = r9[0]; r.x.y = r9[1]; r.x.z = r9[2];
+    r.y.x = r9[3]; r.y.y = r9[4]; r.y.z = r9[5];
+    r.z.x = r9[6]; r.z.y = r9[7]; r.z.z = r9[8];
+    return r;
+}
+/* node_trace_settings + node_area (hex_phase/src/phase_generate.cpp:240-249, hex_trace.cpp:16-24):
+ * the grid axis rotated into the body frame, normalised, its frame and projected area. */
+static int node_setup(double R, double L, const double* r9, const double* grid_ki, v3* k, frame_t* kf, double* area)
+{
+    rot_t r = rot_from(r9);
+    v3 gk = {grid_ki[0], grid_ki[1], grid_ki[2]};
+    prism_t p = {R, L};
+    if (!v_normalize(rot_inverse(&r, gk), k) || !make_frame(*k, kf)) return -1;
+    *area = pr_projected(p, *k);
+    return 0;
+}
+double icpo_hex_node_area(double R, double L, const double* r9, const double* grid_ki)
+{
+    v3 k;
+    frame_t kf;
+    double a;
+    if (node_setup(R, L, r9, grid_ki, &k, &kf, &a)) return -1;
+    return a;
+}
+int icpo_hex_accumulate(const double* node, uint64_t seed, uint64_t total, uint32_t max_hits,
+                        const double* edges, uint32_t nt, uint32_t np, const double* grid_frame,
+                        const double* rot, uint64_t first, uint64_t count, uint64_t batch_size,
+                        double* cells, double* stats, uint64_t* counts, double balance_tol)
+{
+    trace_cfg_t c;
+    hist_t h;
+    double area;
+    uint64_t i, b0;
+    memset(&c, 0, sizeof c);
+    memset(&h, 0, sizeof h);
+    c.prism.R = node[0];
+    c.prism.L = node[1];
+    if (node_setup(node[0], node[1], rot, grid_frame, &c.k, &c.kf, &area)) return -1;
+    c.n_ext = node[2];
+    c.n_int = node[3];
+    c.tail = node[4];
+    c.seed = seed;
+    c.total = total;
+    c.max_hits = max_hits;
+    if (!cfg_valid(&c)) return -2;
+    h.grid.edges = edges;
+    h.grid.nt = nt;
+    h.grid.np = np;
+    h.grid.ki.x = grid_frame[0]; h.grid.ki.y = grid_frame[1]; h.grid.ki.z = grid_frame[2];
+    h.grid.fr.e0.x = grid_frame[3]; h.grid.fr.e0.y = grid_frame[4]; h.grid.fr.e0.z = grid_frame[5];
+    h.grid.fr.e1.x = grid_frame[6]; h.grid.fr.e1.y = grid_frame[7]; h.grid.fr.e1.z = grid_frame[8];
+    h.rot = rot_from(rot);
+    h.scale = node[5] * area / (double)total;
+    h.cells = (ksum*)cells;
+    h.point_mass.value = stats[0]; h.point_mass.correction = stats[1];
+    h.point_axial.value = stats[2]; h.point_axial.correction = stats[3];
+    h.forward.value = stats[4]; h.forward.correction = stats[5];
+    h.backward.value = stats[6]; h.backward.correction = stats[7];
+    h.count = counts[0];
+    h.snapped = counts[1];
+    if (first + count > total || batch_size == 0) return -3;
+    for (b0 = first; b0 < first + count; b0 += batch_size) {
+        uint64_t b1 = b0 + batch_size < first + count ? b0 + batch_size : first + count;
+        ksum esc = {0, 0}, tail = {0, 0};
+        double maxbal = 0, maxif = 0;
+        int accepted = 1;
+        for (i = b0; i < b1; ++i) {
+            ray_audit_t a = trace_sample(&c, i, hist_emit, &h);
+            if (h.error) return -10 - h.error;
+            counts[2] += a.outputs;
+            counts[3] += 1;
+            if ((unsigned)a.status < 8) counts[4 + a.status] += 1;
+            ks_add(&esc, a.escaped);
+            ks_add(&tail, a.unresolved);
+            maxbal = mx(maxbal, fabs(a.balance));
+            maxif = mx(maxif, a.max_iface);
+            accepted = accepted && (a.status == ST_EXHAUSTED || a.status == ST_TAIL) && fin(a.escaped) &&
+                       fin(a.unresolved) && a.escaped >= 0 && a.unresolved >= 0 && fin(a.balance) &&
+                       fabs(a.balance) <= balance_tol && fin(a.max_iface) && a.max_iface >= 0 &&
+                       a.max_iface <= balance_tol;
+        }
+        /* record_batch_audit: scale * batch sum, Kahan over batches (phase_generate.cpp:258-263) */
+        {
+            ksum ea = {stats[14], stats[15]}, ua = {stats[16], stats[17]};
+            ks_add(&ea, h.scale * esc.value);
+            ks_add(&ua, h.scale * tail.value);
+            stats[14] = ea.value; stats[15] = ea.correction;
+            stats[16] = ua.value; stats[17] = ua.correction;
+        }
+        stats[8] += esc.value;
+        stats[9] += tail.value;
+        stats[10] = mx(stats[10], maxbal);
+        stats[11] = mx(stats[11], maxif);
+        if (!accepted) counts[12] += 1;
+    }
+    stats[0] = h.point_mass.value; stats[1] = h.point_mass.correction;
+    stats[2] = h.point_axial.value; stats[3] = h.point_axial.correction;
+    stats[4] = h.forward.value; stats[5] = h.forward.correction;
+    stats[6] = h.backward.value; stats[7] = h.backward.correction;
+    counts[0] = h.count;
+    counts[1] = h.snapped;
+    return 0;
+}
+
+/*
+ * Per-ray dump for kernel-level parity: for each ray, its status, outputs, escaped and
+ * unresolved power, and the first max_out exits (body-frame direction + power).
+ */
+typedef struct { double* out; uint32_t cap, n; } dump_t;
+static void dump_emit(void* user, v3 d, double power)
+{
+    dump_t* q = (dump_t*)user;
+    if (q->n < q->cap) {
+        q->out[4 * q->n + 0] = d.x;
+        q->out[4 * q->n + 1] = d.y;
+        q->out[4 * q->n + 2] = d.z;
+        q->out[4 * q->n + 3] = power;
+    }
+    q->n++;
+}
+int icpo_hex_trace_rays(const double* node, uint64_t seed, uint64_t total, uint32_t max_hits, uint64_t first,
+                        uint64_t count, uint32_t max_out, double* ray_info, double* exits)
+{
+    trace_cfg_t c;
+    v3 kin;
+    uint64_t i;
+    memset(&c, 0, sizeof c);
+    c.prism.R = node[0];
+    c.prism.L = node[1];
+    kin.x = node[2]; kin.y = node[3]; kin.z = node[4];
+    if (!v_normalize(kin, &c.k) || !make_frame(c.k, &c.kf)) return -1;
+    c.n_ext = node[5];
+    c.n_int = node[6];
+    c.tail = node[7];
+    c.seed = seed;
+    c.total = total;
+    c.max_hits = max_hits;
+    for (i = 0; i < count; ++i) {
+        dump_t q;
+        ray_audit_t a;
+        q.out = exits + (size_t)i * max_out * 4;
+        q.cap = max_out;
+        q.n = 0;
+        a = trace_sample(&c, first + i, dump_emit, &q);
+        ray_info[6 * i + 0] = a.status;
+        ray_info[6 * i + 1] = (double)a.outputs;
+        ray_info[6 * i + 2] = a.escaped;
+        ray_info[6 * i + 3] = a.unresolved;
+        ray_info[6 * i + 4] = a.hits;
+        ray_info[6 * i + 5] = a.max_iface;
+    }
+    return 0;
+}
+
+/* PhaseMassAccumulator::masses (phase_table.cpp:63-76): pole mass spread uniformly
+ * over the first / last row, added into the Kahan pair of each cell. */
+int icpo_masses(const double* cells, uint32_t nt, uint32_t np, const double* stats, double* out)
+{
+    double f = stats[4] / np, b = stats[6] / np;
+    size_t k, n = (size_t)nt * np;
+    if ((stats[4] > 0 && !(f > 0)) || (stats[6] > 0 && !(b > 0))) return -1;
+    for (k = 0; k < n; ++k) {
+        ksum s = {cells[2 * k], cells[2 * k + 1]};
+        size_t i = k / np;
+        if (i == 0) ks_add(&s, f);
+        if (i + 1 == nt) ks_add(&s, b);
+        out[k] = s.value;
+    }
+    return 0;
+}
+
+/* measure_mass (phase_table.cpp:79-93) */
+int icpo_measure_mass(const double* edges, uint32_t nt, uint32_t np, const double* mass, double out[2])
+{
+    ksum total = {0, 0}, axial = {0, 0};
+    size_t k, n = (size_t)nt * np;
+    for (k = 0; k < n; ++k) {
+        double w = mass[k];
+        size_t i = k / np;
+        if (!fin(w) || w < 0) return -1;
+        ks_add(&total, w);
+        ks_add(&axial, w * (1 - edges[i] - edges[i + 1]));
+    }
+    if (!(total.value > 0) || !fin(total.value) || !fin(axial.value)) return -2;
+    out[0] = total.value;
+    out[1] = axial.value;
+    return 0;
+}
+
+/*
+ * build_host_cdf (phase_table.cpp:111-187): conservative aggregation of a fine
+ * (nt x np) mass grid into (ct x cp), ordered binary64 column scans, ordered
+ * marginal scan, normalisation with u-edge fallback for empty columns, audits.
+ * report[]: g_source, g_stored, coarsening_tv, cdf_mass, l1, lost_mass,
+ *           max_cell_error, aggregation_relative_error, lost_cells.
+ * Returns 0, or a negative code for the reference's exception sites.
+ */
+int icpo_build_cdf(const double* edges, uint32_t nt, uint32_t np, const double* mass, uint32_t ct, uint32_t cp,
+                   double max_l1, double max_lost, double max_tv, double* phi, double* theta, double* cedges,
+                   double* report)
+{
+    double fine[2], stored[2], largest, total;
+    ksum* sums;
+    double* coarse;
+    double* columns;
+    uint32_t dt, dp, i, j;
+    ksum tv = {0, 0}, l1 = {0, 0}, lost = {0, 0}, recovered = {0, 0}, axial = {0, 0};
+    size_t k;
+    int rc = 0;
+    if (!fin(max_l1) || max_l1 < 0 || max_l1 > 2 || !fin(max_lost) || max_lost < 0 || max_lost > 1 ||
+        !fin(max_tv) || max_tv < 0 || max_tv > 1)
+        return -1;
+    if (icpo_measure_mass(edges, nt, np, mass, fine)) return -2;
+    if (!ct || !cp || ct > nt || cp > np || nt % ct || np % cp) return -3;
+    dt = nt / ct;
+    dp = np / cp;
+    for (i = 0; i <= ct; ++i) cedges[i] = edges[(size_t)i * dt];
+    sums = (ksum*)calloc((size_t)ct * cp, sizeof(ksum));
+    coarse = (double*)malloc(sizeof(double) * (size_t)ct * cp);
+    columns = (double*)malloc(sizeof(double) * cp);
+    if (!sums || !coarse || !columns) { rc = -4; goto done; }
+    for (i = 0; i < nt; ++i)
+        for (j = 0; j < np; ++j) ks_add(&sums[(size_t)(i / dt) * cp + j / dp], mass[(size_t)i * np + j]);
+    for (k = 0; k < (size_t)ct * cp; ++k) coarse[k] = sums[k].value;
+    if (icpo_measure_mass(cedges, ct, cp, coarse, stored)) { rc = -2; goto done; }
+    report[0] = fine[1] / fine[0];
+    report[7] = fabs(stored[0] / fine[0] - 1);
+    for (i = 0; i < nt; ++i)
+        for (j = 0; j < np; ++j) {
+            uint32_t ci = i / dt, cj = j / dp;
+            double fraction = (edges[i + 1] - edges[i]) / (cedges[ci + 1] - cedges[ci]) / dp;
+            ks_add(&tv, fabs(mass[(size_t)i * np + j] / fine[0] - coarse[(size_t)ci * cp + cj] / stored[0] * fraction));
+        }
+    report[2] = 0.5 * tv.value;
+    if (!fin(report[2]) || report[2] > max_tv || report[7] > 1e-12) { rc = -5; goto done; }
+    largest = coarse[0];
+    for (k = 1; k < (size_t)ct * cp; ++k)
+        if (coarse[k] > largest) largest = coarse[k];
+    phi[0] = 0;
+    for (j = 0; j < cp; ++j) {
+        size_t base = (size_t)j * (ct + 1);
+        double s = 0;
+        theta[base] = 0;
+        for (i = 0; i < ct; ++i) {
+            double w = coarse[(size_t)i * cp + j] / largest;
+            if (coarse[(size_t)i * cp + j] > 0 && !(w > 0)) { rc = -6; goto done; }
+            s += w;
+            theta[base + i + 1] = s;
+        }
+        columns[j] = s;
+        phi[j + 1] = phi[j] + s;
+    }
+    total = phi[cp];
+    if (!(total > 0) || !fin(total)) { rc = -7; goto done; }
+    for (j = 0; j < cp; ++j) {
+        size_t base = (size_t)j * (ct + 1);
+        for (i = 1; i < ct; ++i) theta[base + i] = columns[j] > 0 ? theta[base + i] / columns[j] : cedges[i];
+        theta[base + ct] = 1;
+    }
+    for (j = 1; j < cp; ++j) phi[j] /= total;
+    phi[cp] = 1;
+    report[6] = 0;
+    report[8] = 0;
+    for (j = 0; j < cp; ++j)
+        for (i = 0; i < ct; ++i) {
+            size_t base = (size_t)j * (ct + 1) + i;
+            double q = (phi[j + 1] - phi[j]) * (theta[base + 1] - theta[base]);
+            double p = coarse[(size_t)i * cp + j] / stored[0], err;
+            if (!fin(q) || q < 0 || phi[j + 1] < phi[j] || theta[base + 1] < theta[base]) { rc = -8; goto done; }
+            if (coarse[(size_t)i * cp + j] > 0 && !(p > 0)) { rc = -9; goto done; }
+            err = fabs(p - q);
+            ks_add(&l1, err);
+            if (err > report[6]) report[6] = err;
+            if (p > 0 && q == 0) { ks_add(&lost, p); report[8] += 1; }
+            ks_add(&recovered, q);
+            ks_add(&axial, q * (1 - cedges[i] - cedges[i + 1]));
+        }
+    report[4] = l1.value;
+    report[5] = lost.value;
+    report[3] = recovered.value;
+    report[1] = axial.value / recovered.value;
+    if (report[4] > max_l1 || report[5] > max_lost || fabs(report[3] - 1) > 1e-10 || !fin(report[1]) ||
+        !(report[1] > -1 && report[1] < 1))
+        rc = -10;
+done:
+    free(sums);
+    free(coarse);
+    free(columns);
+    return rc;
+}

@@ -1,0 +1,248 @@
+"""Python access to the CPU oracle (oracle/icp_oracle.c) and the reference build (oracle/_ref).
+
+TEST INFRASTRUCTURE ONLY.  Imported by tests/, __graft_entry__.smoke() and the CPU
+baseline leg of bench.py as the checker; the product (ice_crystal_phase_b200) never
+imports it.
+
+The composition below follows the reference CPU CLI
+hex_phase/apps/generate_hex_phase.cpp:79-140 (preflight areas, per-node batches,
+PhaseMassAccumulator, validate_composition, build_host_cdf).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+import subprocess
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "_build" / "libicp_oracle.so"
+REF_DIR = HERE / "_ref"
+
+_D = C.POINTER(C.c_double)
+_U = C.POINTER(C.c_uint64)
+
+
+def build() -> None:
+    subprocess.run([str(HERE / "build_oracle.sh")], check=True, stdout=subprocess.DEVNULL)
+
+
+def _lib() -> C.CDLL:
+    if not LIB_PATH.exists():
+        build()
+    lib = C.CDLL(str(LIB_PATH))
+    lib.icpo_sample_uniform.restype = C.c_double
+    lib.icpo_sample_uniform.argtypes = [C.c_uint64, C.c_uint64, C.c_uint]
+    lib.icpo_hex_projected_area.restype = C.c_double
+    lib.icpo_hex_projected_area.argtypes = [C.c_double, C.c_double, _D]
+    lib.icpo_u_edges.argtypes = [C.c_uint32, _D]
+    lib.icpo_rotation_from_quaternion.argtypes = [C.c_double] * 4 + [_D]
+    lib.icpo_make_frame.argtypes = [_D, _D, _D, _D]
+    lib.icpo_hex_node_area.restype = C.c_double
+    lib.icpo_hex_node_area.argtypes = [C.c_double, C.c_double, _D, _D]
+    lib.icpo_hex_accumulate.argtypes = [_D, C.c_uint64, C.c_uint64, C.c_uint32, _D, C.c_uint32, C.c_uint32, _D, _D,
+                                        C.c_uint64, C.c_uint64, C.c_uint64, _D, _D, _U, C.c_double]
+    lib.icpo_hex_trace_rays.argtypes = [_D, C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint32,
+                                        _D, _D]
+    lib.icpo_masses.argtypes = [_D, C.c_uint32, C.c_uint32, _D, _D]
+    lib.icpo_measure_mass.argtypes = [_D, C.c_uint32, C.c_uint32, _D, _D]
+    lib.icpo_build_cdf.argtypes = [_D, C.c_uint32, C.c_uint32, _D, C.c_uint32, C.c_uint32, C.c_double, C.c_double,
+                                   C.c_double, _D, _D, _D, _D]
+    return lib
+
+
+_LIB: C.CDLL | None = None
+
+
+def lib() -> C.CDLL:
+    global _LIB
+    if _LIB is None:
+        _LIB = _lib()
+    return _LIB
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(_D if a.dtype == np.float64 else _U)
+
+
+def sample_uniform(seed: int, ray: int, dim: int) -> float:
+    return lib().icpo_sample_uniform(seed, ray, dim)
+
+
+def u_edges(n: int) -> np.ndarray:
+    e = np.empty(n + 1)
+    if lib().icpo_u_edges(n, _p(e)):
+        raise ValueError("u edges not representable")
+    return e
+
+
+def make_frame(k) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    kin = np.asarray(k, dtype=np.float64)
+    ko, e0, e1 = np.empty(3), np.empty(3), np.empty(3)
+    if lib().icpo_make_frame(_p(kin), _p(ko), _p(e0), _p(e1)):
+        raise ValueError("invalid incident direction")
+    return ko, e0, e1
+
+
+def rotation_from_quaternion(q) -> np.ndarray:
+    """Columns body->ensemble, returned as a 3x3 matrix M with M[:, c] = column c."""
+    out = np.empty(9)
+    if lib().icpo_rotation_from_quaternion(*map(float, q), _p(out)):
+        raise ValueError("Quaternion must be unit length (w,x,y,z).")
+    return out.reshape(3, 3).T.copy()
+
+
+def hex_projected_area(R: float, L: float, k) -> float:
+    kk = np.asarray(k, dtype=np.float64)
+    return lib().icpo_hex_projected_area(R, L, _p(kk))
+
+
+@dataclass
+class Node:
+    q: tuple[float, float, float, float]
+    weight: float
+    samples: int
+    seed: int
+
+
+def parse_plan(text: str) -> list[Node]:
+    """Orientation CSV (hex_phase/src/orientation_plan.cpp:69-120) without the SHA digest."""
+    nodes, header = [], False
+    for raw in text.splitlines():
+        line = raw.strip(" \t\r")
+        if not line or line.startswith("#"):
+            continue
+        if not header:
+            if line != "qw,qx,qy,qz,weight,samples,seed":
+                raise ValueError("Expected CSV header qw,qx,qy,qz,weight,samples,seed.")
+            header = True
+            continue
+        cols = line.split(",")
+        if len(cols) != 7:
+            raise ValueError("Expected seven CSV fields.")
+        nodes.append(Node(tuple(float(c) for c in cols[:4]), float(cols[4]), int(cols[5]), int(cols[6])))
+    total = math.fsum(n.weight for n in nodes)
+    if not nodes or abs(total - 1) > 2e-12:
+        raise ValueError("Orientation number-probability weights must sum to one (within 2e-12).")
+    # Kahan sum of weights as in the reference (orientation_plan.cpp:286, 295)
+    s, c = 0.0, 0.0
+    for n in nodes:
+        y = n.weight - c
+        t = s + y
+        c = (t - s) - y
+        s = t
+    for n in nodes:
+        n.weight /= s
+    return nodes
+
+
+@dataclass
+class HexRecord:
+    masses: np.ndarray
+    point_mass: float
+    point_axial: float
+    forward: float
+    backward: float
+    expected_area: float
+    escaped_area: float
+    unresolved_area: float
+    max_balance: float
+    max_iface: float
+    counts: dict = field(default_factory=dict)
+
+
+def hex_record(R: float, L: float, ki, n_int: float, n_ext: float, nt: int, np_: int, nodes: list[Node],
+               max_hits: int = 1024, tail: float = 1e-12, batch: int = 4096,
+               balance_tol: float = 1e-10) -> HexRecord:
+    """Cell masses and audits of one record, in the reference CLI's order of operations."""
+    L_ = lib()
+    edges = u_edges(nt)
+    ko, e0, e1 = make_frame(ki)
+    grid_frame = np.concatenate([ko, e0, e1])
+    cells = np.zeros(2 * nt * np_)
+    stats = np.zeros(18)
+    counts = np.zeros(13, dtype=np.uint64)
+    expected_s, expected_c = 0.0, 0.0
+    rots = []
+    for n in nodes:
+        rot = rotation_from_quaternion(n.q).T.reshape(-1).copy()  # column-major body->ensemble
+        area = L_.icpo_hex_node_area(R, L, _p(rot), _p(ko))
+        if not area > 0:
+            raise ValueError("Invalid node geometry")
+        rots.append(rot)
+        y = n.weight * area - expected_c
+        t = expected_s + y
+        expected_c = (t - expected_s) - y
+        expected_s = t
+    for n, rot in zip(nodes, rots):
+        node = np.array([R, L, n_ext, n_int, tail, n.weight])
+        rc = L_.icpo_hex_accumulate(_p(node), n.seed, n.samples, max_hits, _p(edges), nt, np_, _p(grid_frame),
+                                    _p(rot), 0, n.samples, batch, _p(cells), _p(stats), _p(counts), balance_tol)
+        if rc:
+            raise RuntimeError(f"oracle accumulate failed ({rc})")
+    masses = np.empty(nt * np_)
+    if L_.icpo_masses(_p(cells), nt, np_, _p(stats), _p(masses)):
+        raise RuntimeError("Pole weight underflow.")
+    names = ["samples", "snapped", "outputs", "rays"] + [f"status{i}" for i in range(8)] + ["rejected_batches"]
+    return HexRecord(masses, stats[0], stats[2], stats[4], stats[6], expected_s, stats[14], stats[16], stats[10],
+                     stats[11], {k: int(v) for k, v in zip(names, counts)})
+
+
+def hex_trace_rays(R, L, k_body, n_int, n_ext, seed, total, max_hits, tail, first, count, max_out=64):
+    node = np.array([R, L, k_body[0], k_body[1], k_body[2], n_ext, n_int, tail, 1.0])
+    info = np.zeros((count, 6))
+    exits = np.zeros((count, max_out, 4))
+    if lib().icpo_hex_trace_rays(_p(node), seed, total, max_hits, first, count, max_out, _p(info), _p(exits)):
+        raise RuntimeError("invalid trace settings")
+    return info, exits
+
+
+@dataclass
+class Cdf:
+    phi: np.ndarray
+    theta: np.ndarray
+    edges: np.ndarray
+    report: dict
+
+
+def build_cdf(mass: np.ndarray, nt: int, np_: int, ct: int | None = None, cp: int | None = None,
+              max_l1: float = 1e-10, max_lost: float = 1e-12, max_tv: float = 1.0) -> Cdf:
+    ct = ct or nt
+    cp = cp or np_
+    edges = u_edges(nt)
+    m = np.ascontiguousarray(mass, dtype=np.float64)
+    phi = np.zeros(cp + 1)
+    theta = np.zeros(cp * (ct + 1))
+    ced = np.zeros(ct + 1)
+    rep = np.zeros(9)
+    rc = lib().icpo_build_cdf(_p(edges), nt, np_, _p(m), ct, cp, max_l1, max_lost, max_tv, _p(phi), _p(theta),
+                              _p(ced), _p(rep))
+    names = ["g_source", "g_stored", "coarsening_tv", "cdf_mass", "l1_error", "lost_mass", "maximum_cell_error",
+             "aggregation_relative_error", "lost_cells"]
+    report = dict(zip(names, rep.tolist()))
+    report["status"] = rc
+    return Cdf(phi, theta.reshape(cp, ct + 1), ced, report)
+
+
+# ------------------------------------------------------------------ reference (_ref)
+def ref_available() -> bool:
+    return (REF_DIR / "ref_hex_harness").exists()
+
+
+def ref_masses(R, L, ki, n_int, n_ext, nt, np_, plan_csv: Path, max_hits=1024, tail=1e-12, batch=4096,
+               workdir: Path | None = None) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    out = Path(workdir or "/tmp") / f"ref_masses_{os.getpid()}.bin"
+    args = [str(REF_DIR / "ref_hex_harness"), "masses", repr(R), repr(L), *map(repr, map(float, ki)), repr(n_int),
+            repr(n_ext), str(nt), str(np_), str(max_hits), repr(tail), str(plan_csv), str(batch), str(out)]
+    subprocess.run(args, check=True)
+    raw = out.read_bytes()
+    out.unlink()
+    n = nt * np_
+    masses = np.frombuffer(raw[:8 * n], dtype="<f8").copy()
+    d = np.frombuffer(raw[8 * n:8 * n + 72], dtype="<f8").copy()
+    u = np.frombuffer(raw[8 * n + 72:], dtype="<u8").copy()
+    return masses, d, u

@@ -1,0 +1,116 @@
+"""CDF builder on the GPU vs the pinned CPU oracle (same masses in, same arrays out).
+
+The column scans and the marginal scan use the reference's ordered binary64 additions, so
+phi and theta are compared bit for bit; reductions (g, L1) are parallel and compared within
+the reference's own GPU-vs-CPU tolerances (hex_phase/tests/phase_cuda_tests.cpp:18-47:
+L1 2e-10, g 2e-11).  Edge cases follow tests/test_phase_cdf_cuda.cpp:15-71.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+
+def _check_same(ctx, icp, oracle, m, nt, np_, ct=None, cp=None, fwd=0.0, bwd=0.0):
+    full = m.reshape(nt, np_).copy()
+    full[0] += fwd / np_
+    full[-1] += bwd / np_
+    ref = oracle.build_cdf(full.reshape(-1), nt, np_, ct, cp)
+    assert ref.report["status"] == 0
+    out = icp.PhaseCdf(ctx).build(m, nt, np_, ct, cp, forward=fwd, backward=bwd)
+    if fwd == 0 and bwd == 0:
+        assert np.array_equal(out.phi, ref.phi)
+        assert np.array_equal(out.theta, ref.theta)
+    else:  # pole cap added with one rounding on the device instead of the Kahan pair
+        assert np.abs(out.phi - ref.phi).max() <= 1e-15
+        assert np.abs(out.theta - ref.theta).max() <= 1e-15
+    assert np.array_equal(out.u_edges, ref.edges)
+    r = out.report
+    assert abs(r["g_stored"] - ref.report["g_stored"]) <= 2e-11
+    assert abs(r["l1_error"] - ref.report["l1_error"]) <= 2e-10
+    assert abs(r["cdf_mass"] - 1) <= 1e-10
+    assert r["lost_cells"] == ref.report["lost_cells"]
+    return out, ref
+
+
+def test_reference_record_masses(ctx, icp, oracle):
+    g = np.load(GOLDEN / "hex_two_orientations.npz")
+    out, _ = _check_same(ctx, icp, oracle, g["masses"], 72, 144, 36, 72)
+    assert np.array_equal(out.phi, g["phi"]) and np.array_equal(out.theta, g["theta"])
+    assert abs(out.report["g_stored"] - g["meta"][0]) <= 2e-11
+
+
+@pytest.mark.parametrize("nt,np_", [(1, 1), (17, 13), (257, 33), (513, 513), (900, 1800), (512, 1024)])
+def test_synthetic_densities_with_zero_columns(ctx, icp, oracle, nt, np_):
+    rng = np.random.default_rng(nt * 7919 + np_)
+    m = rng.random((nt, np_)) ** 3
+    m[:, ::5] = 0.0  # empty phi columns -> u-edge conditionals
+    m[rng.random((nt, np_)) < 0.2] = 0.0  # plateaus
+    if m.sum() == 0:
+        m[0, 0] = 1.0
+    _check_same(ctx, icp, oracle, m.reshape(-1), nt, np_)
+
+
+def test_coarsening_and_poles(ctx, icp, oracle):
+    rng = np.random.default_rng(3)
+    m = rng.random(96 * 192)
+    _check_same(ctx, icp, oracle, m, 96, 192, 48, 64)
+    _check_same(ctx, icp, oracle, m, 96, 192, 96, 192, fwd=3.0, bwd=1.0)
+
+
+def test_uniform_contract(ctx, icp, oracle):
+    nt, np_ = 64, 128
+    e = oracle.u_edges(nt)
+    m = np.repeat((4 * math.pi / np_) * np.diff(e), np_)
+    out, _ = _check_same(ctx, icp, oracle, m, nt, np_)
+    assert abs(out.report["g_stored"]) <= 1e-15
+    assert np.abs(out.theta - e[None, :]).max() <= 2e-15
+
+
+def test_density_input(ctx, icp, oracle):
+    # scalar density stage (PhaseDensityView::scalar): w = d * du
+    nt, np_ = 36, 72
+    e = oracle.u_edges(nt)
+    rng = np.random.default_rng(5)
+    d = rng.random((nt, np_))
+    out = icp.PhaseCdf(ctx).build(d.reshape(-1), nt, np_, density=True)
+    ref = oracle.build_cdf((d * np.diff(e)[:, None]).reshape(-1), nt, np_)
+    assert np.abs(out.theta - ref.theta).max() <= 1e-15 and np.abs(out.phi - ref.phi).max() <= 1e-15
+
+
+def test_rejections(ctx, icp):
+    cdf = icp.PhaseCdf(ctx)
+    m = np.ones(8 * 16)
+    bad = m.copy()
+    bad[3] = -1
+    with pytest.raises(icp.InvalidArgument):
+        cdf.build(bad, 8, 16)
+    bad[3] = np.nan
+    with pytest.raises(icp.InvalidArgument):
+        cdf.build(bad, 8, 16)
+    with pytest.raises(icp.AuditError):
+        cdf.build(np.zeros(8 * 16), 8, 16)
+    with pytest.raises(icp.InvalidArgument):
+        cdf.build(m, 8, 16, 3, 16)
+    with pytest.raises(icp.AuditError):
+        cdf.build(np.array([1, 1e-20, 1e-20, 1e-20]), 2, 2, max_lost_mass=0)
+    rng = np.random.default_rng(1)
+    with pytest.raises(icp.AuditError):
+        cdf.build(rng.random(48 * 96), 48, 96, 24, 48, max_coarsening_tv=0)
+
+
+def test_full_size_properties(ctx, icp):
+    # 900 x 1800: monotone conditionals with exact endpoints, normalised marginal, mass 1
+    rng = np.random.default_rng(11)
+    m = rng.exponential(size=900 * 1800) * (rng.random(900 * 1800) < 0.3)
+    out = icp.PhaseCdf(ctx).build(m, 900, 1800)
+    t = out.theta
+    assert np.all(np.diff(t, axis=1) >= 0) and np.all(t[:, 0] == 0) and np.all(t[:, -1] == 1)
+    assert out.phi[0] == 0 and out.phi[-1] == 1 and np.all(np.diff(out.phi) >= 0)
+    assert abs(out.report["cdf_mass"] - 1) <= 1e-10

@@ -1,0 +1,137 @@
+"""The CPU oracle is pinned to the reference before it is trusted as a checker.
+
+Fixtures in tests/golden/ were produced by the reference's own code compiled from its
+sources (tests/golden/make_golden.py); where oracle/_ref is built on this host the oracle is
+also compared with freshly run reference binaries.  Known-answer cases follow the
+reference's hex_phase/tests/phase_tests.cpp and phase_cli_test.py.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, TWO_ORIENTATIONS
+
+CFG3_KI = (0.8660254037844387, -0.5, 0.0)
+
+
+def test_rng_midpoints(oracle):
+    # 52-bit midpoints strictly inside (0,1) (hex_trace/include/ice_crystal/math.hpp:142-146)
+    u = [oracle.sample_uniform(12345, i, d) for i in range(200) for d in range(3)]
+    assert all(0 < x < 1 for x in u)
+    assert all((x * 2.0**52 - 0.5) == int(x * 2.0**52 - 0.5) for x in u)
+
+
+def test_two_orientation_masses_bit_exact(oracle):
+    g = np.load(GOLDEN / "hex_two_orientations.npz")
+    rec = oracle.hex_record(0.1, 0.2, [1, -0.4, 0.3], 1.31, 1.0, 72, 144, oracle.parse_plan(TWO_ORIENTATIONS),
+                            batch=512)
+    assert np.array_equal(rec.masses, g["masses"])
+    d = g["stats"]
+    assert (rec.point_mass, rec.point_axial, rec.forward, rec.backward) == tuple(d[:4])
+    assert (rec.expected_area, rec.escaped_area, rec.unresolved_area) == tuple(d[4:7])
+    c = g["counts"]
+    assert rec.counts["outputs"] == c[2] and rec.counts["rays"] == c[3]
+    assert [rec.counts[f"status{i}"] for i in range(8)] == list(c[4:12])
+
+
+def test_two_orientation_cdf_bit_exact(oracle):
+    g = np.load(GOLDEN / "hex_two_orientations.npz")
+    cdf = oracle.build_cdf(g["masses"], 72, 144, 36, 72)
+    assert cdf.report["status"] == 0
+    assert np.array_equal(cdf.phi, g["phi"])
+    assert np.array_equal(cdf.theta, g["theta"])
+    assert np.array_equal(cdf.edges, g["u"])
+    meta = g["meta"]
+    assert cdf.report["g_stored"] == meta[0]
+    assert cdf.report["l1_error"] == meta[1]
+    assert cdf.report["coarsening_tv"] == meta[2]
+
+
+def test_config3_masses_bit_exact(oracle):
+    g = np.load(GOLDEN / "hex_config3_20k.npz")
+    nodes = oracle.parse_plan("qw,qx,qy,qz,weight,samples,seed\n1,0,0,0,1,20000,12345\n")
+    rec = oracle.hex_record(0.05, 0.2, CFG3_KI, 1.31, 1.0, 512, 1024, nodes, max_hits=12)
+    nz = np.flatnonzero(rec.masses)
+    assert np.array_equal(nz, g["index"])
+    assert np.array_equal(rec.masses[nz], g["value"])
+    assert rec.escaped_area == g["stats"][5] and rec.unresolved_area == g["stats"][6]
+
+
+def test_per_ray_trace_bit_exact(oracle):
+    g = np.load(GOLDEN / "hex_rays.npz")
+    info, exits = oracle.hex_trace_rays(0.05, 0.2, CFG3_KI, 1.31, 1.0, 12345, 20000, 1024, 1e-12, 100, 48)
+    assert np.array_equal(info[:, :4], g["info"][:, :4])
+    assert np.array_equal(info[:, 4], g["info"][:, 4])
+    flat = np.concatenate([exits[i, :int(info[i, 1])] for i in range(48)])
+    assert np.array_equal(flat, g["exits"])
+
+
+def test_uniform_measure_contract(oracle):
+    # phase_tests.cpp:57-70: per-solid-angle uniform masses -> u-edge conditionals, g = 0
+    nt, np_ = 64, 128
+    e = oracle.u_edges(nt)
+    m = np.repeat((4 * math.pi / np_) * np.diff(e), np_)
+    c = oracle.build_cdf(m, nt, np_)
+    assert abs(c.report["g_stored"]) <= 1e-15
+    assert np.abs(c.phi - np.arange(np_ + 1) / np_).max() <= 1e-14
+    assert np.abs(c.theta - e[None, :]).max() <= 2e-15
+
+
+def test_sparse_coarsening_and_zero_columns(oracle):
+    # phase_tests.cpp:105-127
+    nt, np_ = 48, 96
+    i, j = np.meshgrid(np.arange(nt), np.arange(np_), indexing="ij")
+    m = np.where(j % 7 == 0, 10.0 ** (-12.0 * ((17 * i + 13 * j) % 97) / 96), 0.0).reshape(-1)
+    c = oracle.build_cdf(m, nt, np_, 24, 48)
+    assert c.report["status"] == 0 and abs(c.report["cdf_mass"] - 1) <= 2e-15 and c.report["l1_error"] < 2e-14
+    full = oracle.build_cdf(m, nt, np_)
+    e = oracle.u_edges(nt)
+    for col in range(np_):
+        if col % 7:
+            assert np.array_equal(full.theta[col], e)
+    assert oracle.build_cdf(m, nt, np_, 24, 48, max_tv=0).report["status"] != 0
+    assert oracle.build_cdf(np.zeros(nt * np_), nt, np_).report["status"] != 0
+    bad = m.copy()
+    bad[0] = -1
+    assert oracle.build_cdf(bad, nt, np_).report["status"] != 0
+    # lost mass is detected, never repaired
+    assert oracle.build_cdf(np.array([1, 1e-20, 1e-20, 1e-20]), 2, 2, max_lost=0).report["status"] != 0
+
+
+def test_pole_caps(oracle):
+    # phase_tests.cpp:71-77: forward mass 3, backward 1 spread over the end rows
+    nt, np_ = 8, 16
+    m = np.zeros(nt * np_)
+    m[:np_] += 3 / np_
+    m[-np_:] += 1 / np_
+    c = oracle.build_cdf(m, nt, np_)
+    e = oracle.u_edges(nt)
+    assert abs(c.report["g_stored"] - 0.5 * (1 - e[1])) <= 5e-16
+    assert np.abs(c.phi - np.arange(np_ + 1) / np_).max() <= 1e-15
+
+
+def test_transparent_limit(oracle):
+    # n = 1: all light in the forward cap (phase_tests.cpp:172-182)
+    nodes = oracle.parse_plan("qw,qx,qy,qz,weight,samples,seed\n1,0,0,0,0.5,17,11\n"
+                              "0.7071067811865476,0,0,0.7071067811865476,0.5,55,22\n")
+    rec = oracle.hex_record(1, 2, [0, -1, 0], 1.0, 1.0, 16, 32, nodes, tail=0)
+    assert abs(rec.expected_area - 0.5 * ((3 * math.sqrt(3) / 2) + 4)) <= 2e-15
+    assert abs(rec.escaped_area - rec.expected_area) <= 4e-15
+    assert abs(rec.forward - rec.expected_area) <= 4e-15
+
+
+@pytest.mark.skipif(not (GOLDEN.parents[1] / "oracle" / "_ref" / "ref_hex_harness").exists(),
+                    reason="reference binaries not built on this host")
+@pytest.mark.parametrize("ki,R,L,n,hits", [((1, -0.4, 0.3), 0.1, 0.2, 1.31, 1024), ((0.2, 0.9, -0.1), 0.07, 0.05, 1.5, 40),
+                                           ((-1, 0, 0), 0.1, 0.3, 1.33, 1024)])
+def test_oracle_matches_reference_binary(oracle, tmp_path, ki, R, L, n, hits):
+    plan = "qw,qx,qy,qz,weight,samples,seed\n1,0,0,0,0.3,700,7\n0.5,0.5,0.5,0.5,0.7,900,99\n"
+    (tmp_path / "p.csv").write_text(plan)
+    m, d, _ = oracle.ref_masses(R, L, ki, n, 1.0, 24, 48, tmp_path / "p.csv", max_hits=hits, batch=333,
+                                workdir=tmp_path)
+    rec = oracle.hex_record(R, L, ki, n, 1.0, 24, 48, oracle.parse_plan(plan), max_hits=hits, batch=333)
+    assert np.array_equal(m, rec.masses)
+    assert rec.escaped_area == d[5] and rec.unresolved_area == d[6]
