@@ -31,7 +31,7 @@ BIN = PKG / "bin"
 
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-COMMON = ["-std=c++17", "-O3", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
+COMMON = ["-std=c++17", "-O3", "-lineinfo", "--Werror", "cross-execution-space-call", *ARCH, "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
           "-I", str(ROOT / "include"), "-I", str(CSRC), "-I", str(HOST)]
 
 UNITS = {

@@ -409,7 +409,7 @@ int choose_cw(icp_context* c, uint32_t ct, uint32_t cp, uint32_t& cw)
     // smallest strip width whose grid fits co-resident, at least ceil(cp / SMs)
     uint32_t w = std::max<uint32_t>(1u, (cp + c->sms - 1) / c->sms);
     for (; w <= cp; ++w) {
-        const size_t smem = sizeof(double) * ((size_t)ct * w + w + 1);
+        const size_t smem = cdf_smem_bytes(ct, cp, w);
         if (smem > 200 * 1024) break;
         const uint32_t blocks = (cp + w - 1) / w;
         if ((int)blocks <= cdf_max_coresident_blocks(smem, c->device)) {

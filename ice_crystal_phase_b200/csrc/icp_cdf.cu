@@ -170,15 +170,26 @@ __global__ void __launch_bounds__(kThreads) cdf_build_kernel(const CdfParams P)
     if (!grid_wait(&P.sync[0], gridDim.x, &P.report->timeout)) return;
 
     // ------------------------------------------------------------ phase B
+    // block partials staged through shared memory (L2 loads in parallel), then summed in
+    // block order by one thread so that every block derives identical totals
+    double* stage = sphi + CW + 1; // scratch: max(14 * gridDim.x, cp) doubles
+    for (unsigned k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
+        const BlockPartial* bp = P.partial + k;
+        stage[5 * k + 0] = __ldcg(&bp->fine_mass);
+        stage[5 * k + 1] = __ldcg(&bp->fine_axial);
+        stage[5 * k + 2] = __ldcg(&bp->stored_mass);
+        stage[5 * k + 3] = __ldcg(&bp->stored_axial);
+        stage[5 * k + 4] = __ldcg(&bp->largest);
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
         double a = 0, b = 0, c = 0, d = 0, e = 0;
         for (unsigned k = 0; k < gridDim.x; ++k) {
-            const volatile BlockPartial* pp = (const volatile BlockPartial*)P.partial + k;
-            a += pp->fine_mass;
-            b += pp->fine_axial;
-            c += pp->stored_mass;
-            d += pp->stored_axial;
-            e = fmax(e, pp->largest);
+            a += stage[5 * k + 0];
+            b += stage[5 * k + 1];
+            c += stage[5 * k + 2];
+            d += stage[5 * k + 3];
+            e = fmax(e, stage[5 * k + 4]);
         }
         s_glob[0] = a;
         s_glob[1] = b;
@@ -226,17 +237,18 @@ __global__ void __launch_bounds__(kThreads) cdf_build_kernel(const CdfParams P)
     if (!grid_wait(&P.sync[0], 2u * gridDim.x, &P.report->timeout)) return;
 
     // ------------------------------------------------------------ phase C
+    for (uint32_t j = threadIdx.x; j < P.cp; j += blockDim.x) stage[j] = __ldcg(P.colsum + j);
+    __syncthreads();
     if (threadIdx.x == 0) {
         // ordered marginal scan (phase_table.cpp:154): phi[j+1] = phi[j] + colsum[j]
         double a = 0.0;
-        const volatile double* cs = P.colsum;
-        for (uint32_t j = 0; j < c0; ++j) a += cs[j];
+        for (uint32_t j = 0; j < c0; ++j) a += stage[j];
         sphi[0] = a;
         for (uint32_t cl = 0; cl < w; ++cl) {
-            a += cs[c0 + cl];
+            a += stage[c0 + cl];
             sphi[cl + 1] = a;
         }
-        for (uint32_t j = c1; j < P.cp; ++j) a += cs[j];
+        for (uint32_t j = c1; j < P.cp; ++j) a += stage[j];
         s_glob[5] = a;
     }
     __syncthreads();
@@ -274,7 +286,7 @@ __global__ void __launch_bounds__(kThreads) cdf_build_kernel(const CdfParams P)
         if (q < span) {
             const uint32_t cl = q / stride, j = c0 + cl;
             i = q % stride;
-            const double cs = P.colsum[j];
+            const double cs = stage[j];
             row = P.theta + (size_t)j * stride;
             auto norm = [&](uint32_t k, double raw) -> double {
                 if (k == 0) return 0.0;
@@ -329,25 +341,47 @@ __global__ void __launch_bounds__(kThreads) cdf_build_kernel(const CdfParams P)
         }
     }
     __syncthreads();
-    if (!s_last || threadIdx.x != 0) return;
+    if (!s_last) return;
     __threadfence();
+    // last block: stage every block's audit partials (parallel L2 loads), sum in block order
+    constexpr unsigned kF = 14;
+    for (unsigned k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
+        const BlockPartial* bp = P.partial + k;
+        double* o = stage + (size_t)kF * k;
+        o[0] = __ldcg(&bp->fine_mass);
+        o[1] = __ldcg(&bp->fine_axial);
+        o[2] = __ldcg(&bp->stored_mass);
+        o[3] = __ldcg(&bp->stored_axial);
+        o[4] = __ldcg(&bp->tv);
+        o[5] = __ldcg(&bp->l1);
+        o[6] = __ldcg(&bp->lost);
+        o[7] = __ldcg(&bp->recovered);
+        o[8] = __ldcg(&bp->axial);
+        o[9] = __ldcg(&bp->max_err);
+        o[10] = __longlong_as_double((long long)__ldcg(&bp->lost_cells));
+        o[13] = __longlong_as_double((long long)__ldcg(&bp->malformed));
+        o[11] = __longlong_as_double((long long)__ldcg(&bp->invalid));
+        o[12] = __longlong_as_double((long long)__ldcg(&bp->underflow));
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
     CdfDeviceReport r{};
-    const volatile BlockPartial* vp = P.partial;
     for (unsigned k = 0; k < gridDim.x; ++k) {
-        r.fine_mass += vp[k].fine_mass;
-        r.fine_axial += vp[k].fine_axial;
-        r.stored_mass += vp[k].stored_mass;
-        r.stored_axial += vp[k].stored_axial;
-        r.tv += vp[k].tv;
-        r.l1 += vp[k].l1;
-        r.lost += vp[k].lost;
-        r.recovered += vp[k].recovered;
-        r.axial += vp[k].axial;
-        r.max_err = fmax(r.max_err, vp[k].max_err);
-        r.lost_cells += vp[k].lost_cells;
-        r.malformed += vp[k].malformed;
-        r.invalid += vp[k].invalid;
-        r.underflow += vp[k].underflow;
+        const double* o = stage + (size_t)kF * k;
+        r.fine_mass += o[0];
+        r.fine_axial += o[1];
+        r.stored_mass += o[2];
+        r.stored_axial += o[3];
+        r.tv += o[4];
+        r.l1 += o[5];
+        r.lost += o[6];
+        r.recovered += o[7];
+        r.axial += o[8];
+        r.max_err = fmax(r.max_err, o[9]);
+        r.invalid += (unsigned long long)__double_as_longlong(o[11]);
+        r.underflow += (unsigned long long)__double_as_longlong(o[12]);
+        r.lost_cells += (unsigned long long)__double_as_longlong(o[10]);
+        r.malformed += (unsigned long long)__double_as_longlong(o[13]);
     }
     r.largest = s_glob[4];
     r.total = total;
@@ -378,12 +412,19 @@ int launch_cdf_build(const CdfLaunch& L, cudaStream_t stream)
     P.fwd_add = L.fwd_add;
     P.bwd_add = L.bwd_add;
     const unsigned blocks = (L.cp + L.cw - 1) / L.cw;
-    const size_t smem = sizeof(double) * ((size_t)L.ct * L.cw + L.cw + 1);
+    const size_t smem = cdf_smem_bytes(L.ct, L.cp, L.cw);
     cudaError_t e = cudaFuncSetAttribute(cdf_build_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return (int)e;
     void* args[] = {&P};
     e = cudaLaunchCooperativeKernel((const void*)cdf_build_kernel, dim3(blocks), dim3(kThreads), args, smem, stream);
     return (int)e;
+}
+
+size_t cdf_smem_bytes(uint32_t ct, uint32_t cp, uint32_t cw)
+{
+    const size_t blocks = (cp + cw - 1) / cw;
+    const size_t stage = blocks * 14 > cp ? blocks * 14 : cp;
+    return sizeof(double) * ((size_t)ct * cw + cw + 1 + stage);
 }
 
 int cdf_max_coresident_blocks(size_t smem, int device)

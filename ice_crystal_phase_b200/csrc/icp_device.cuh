@@ -22,20 +22,20 @@ constexpr unsigned kFull = 0xffffffffu;
 
 template <class R> struct V3 { R x, y, z; };
 
-template <class R> __device__ __forceinline__ V3<R> v3(R x, R y, R z) { return {x, y, z}; }
-template <class R> __device__ __forceinline__ V3<R> operator+(V3<R> a, V3<R> b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
-template <class R> __device__ __forceinline__ V3<R> operator-(V3<R> a, V3<R> b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
-template <class R> __device__ __forceinline__ V3<R> operator-(V3<R> a) { return {-a.x, -a.y, -a.z}; }
-template <class R> __device__ __forceinline__ V3<R> operator*(V3<R> a, R s) { return {a.x * s, a.y * s, a.z * s}; }
-template <class R> __device__ __forceinline__ V3<R> operator/(V3<R> a, R s) { return {a.x / s, a.y / s, a.z / s}; }
-template <class R> __device__ __forceinline__ R dot(V3<R> a, V3<R> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-template <class R> __device__ __forceinline__ V3<R> cross(V3<R> a, V3<R> b)
+template <class R> __host__ __device__ __forceinline__ V3<R> v3(R x, R y, R z) { return {x, y, z}; }
+template <class R> __host__ __device__ __forceinline__ V3<R> operator+(V3<R> a, V3<R> b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+template <class R> __host__ __device__ __forceinline__ V3<R> operator-(V3<R> a, V3<R> b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <class R> __host__ __device__ __forceinline__ V3<R> operator-(V3<R> a) { return {-a.x, -a.y, -a.z}; }
+template <class R> __host__ __device__ __forceinline__ V3<R> operator*(V3<R> a, R s) { return {a.x * s, a.y * s, a.z * s}; }
+template <class R> __host__ __device__ __forceinline__ V3<R> operator/(V3<R> a, R s) { return {a.x / s, a.y / s, a.z / s}; }
+template <class R> __host__ __device__ __forceinline__ R dot(V3<R> a, V3<R> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <class R> __host__ __device__ __forceinline__ V3<R> cross(V3<R> a, V3<R> b)
 {
     return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
 }
-template <class R> __device__ __forceinline__ R rabs(R x) { return x < R(0) ? -x : x; }
-template <class R> __device__ __forceinline__ R rmax(R a, R b) { return a > b ? a : b; }
-template <class R> __device__ __forceinline__ R rmin(R a, R b) { return a < b ? a : b; }
+template <class R> __host__ __device__ __forceinline__ R rabs(R x) { return x < R(0) ? -x : x; }
+template <class R> __host__ __device__ __forceinline__ R rmax(R a, R b) { return a > b ? a : b; }
+template <class R> __host__ __device__ __forceinline__ R rmin(R a, R b) { return a < b ? a : b; }
 __device__ __forceinline__ float rsqrt_r(float x) { return rsqrtf(x); }
 __device__ __forceinline__ double rsqrt_r(double x) { return 1.0 / sqrt(x); }
 __device__ __forceinline__ float sqrt_r(float x) { return sqrtf(x); }
@@ -123,6 +123,19 @@ template <class R>
 __device__ __forceinline__ Interface<R> split(V3<R> d, V3<R> e, Stokes<R> S, V3<R> n, R ni, R nt)
 {
     Interface<R> out;
+    if (ni == nt) {
+        // matched media (flux_interface.hpp:34-41): the ray continues unchanged, no reflection
+        out.s = e;
+        out.dt = d;
+        out.t = S;
+        out.dr = unit(d - n * (R(2) * dot(d, n)));
+        out.r = {R(0), R(0), R(0), R(0)};
+        out.ci = -dot(d, n);
+        out.has_t = true;
+        out.tir = false;
+        out.balance = R(0);
+        return out;
+    }
     R ci = -dot(d, n);
     ci = rmin(R(1), rmax(R(0), ci));
     V3<R> s = cross(d, n);

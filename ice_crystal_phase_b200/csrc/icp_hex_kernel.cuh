@@ -252,8 +252,14 @@ __global__ void __launch_bounds__(256) hex_trace_bin_kernel(const HexParams<R> P
         bool has = false;
         V3<R> od;
         R opow = R(0);
+        // ---- gather the inputs of this step's interface: the entry face of a fresh ray,
+        // or the next exit plane of a live one (one shared split per lane per step)
+        bool do_split = false;
+        V3<R> sd, se, sn;
+        Stokes<R> sS;
+        R sni, snt;
         if (fresh) {
-            // ---- entry: face in proportion to projected area, point on the face (hex_prism.hpp:64-98)
+            // entry: face in proportion to projected area, point on the face (hex_prism.hpp:64-98)
             const R u0 = uniform<R>(rng_bits(P.seed, L.id, 0));
             const R u1 = uniform<R>(rng_bits(P.seed, L.id, 1));
             const R u2 = uniform<R>(rng_bits(P.seed, L.id, 2));
@@ -261,8 +267,7 @@ __global__ void __launch_bounds__(256) hex_trace_bin_kernel(const HexParams<R> P
             unsigned face = 8u, last = 8u;
 #pragma unroll
             for (unsigned f = 0; f < 8; ++f) {
-                const bool pos = (P.face_mask >> f) & 1u;
-                if (pos) {
+                if ((P.face_mask >> f) & 1u) {
                     last = f;
                     if (face == 8u && target < P.cum[f]) face = f;
                 }
@@ -283,53 +288,59 @@ __global__ void __launch_bounds__(256) hex_trace_bin_kernel(const HexParams<R> P
             L.live = true;
             L.esc = R(0);
             L.hits = 0u;
-            bool entry_ok = true;
+            L.p = pos;
+            L.face = face;
+            do_split = true;
             if constexpr (sizeof(R) == 8) {
                 if (!strict_face_point(P, pos, face)) {
                     finish_ray(P, L, A, s_status, 3, R(1));
-                    entry_ok = false;
+                    do_split = false;
                 }
             }
-            if (entry_ok) {
-                const Stokes<R> S0{R(1), R(0), R(0), R(0)};
-                const Interface<R> sp = split(P.k, P.ke0, S0, n, P.n_ext, P.n_int);
-                A.max_iface = fmax(A.max_iface, (double)sp.balance);
-                if (sp.r.I > R(0)) { has = true; od = sp.dr; opow = sp.r.I; }
-                if (!sp.has_t) {
-                    L.esc += opow;
-                    finish_ray(P, L, A, s_status, 0, R(0));
-                } else {
-                    L.p = pos;
-                    L.d = sp.dt;
-                    L.e = sp.s;
-                    L.S = sp.t;
-                    L.face = face;
-                    L.esc += opow;
-                    settle(P, L, A, s_status);
-                }
-            }
+            sd = P.k;
+            se = P.ke0;
+            sS = Stokes<R>{R(1), R(0), R(0), R(0)};
+            sn = n;
+            sni = P.n_ext;
+            snt = P.n_int;
         } else if (L.live) {
-            // ---- one internal encounter (hex_trace_core.hpp:217-246)
+            // one internal encounter (hex_trace_core.hpp:217-246)
             R t;
             const Boundary hit = next_boundary(P, L.p, L.d, L.face, t);
             if (hit.status) {
                 finish_ray(P, L, A, s_status, hit.status, L.S.I);
             } else {
                 A.near_edge += hit.near_edge ? 1ull : 0ull;
-                const Interface<R> sp = split(L.d, L.e, L.S, -face_normal<R>(hit.face), P.n_int, P.n_ext);
+                L.face = hit.face;
                 ++L.hits;
                 ++A.encounters;
-                A.max_iface = fmax(A.max_iface, (double)sp.balance);
-                if (sp.has_t && sp.t.I > R(0)) {
-                    has = true;
-                    od = sp.dt;
-                    opow = sp.t.I;
-                    L.esc += opow;
-                }
-                L.d = sp.dr;
+                do_split = true;
+                sd = L.d;
+                se = L.e;
+                sS = L.S;
+                sn = -face_normal<R>(hit.face);
+                sni = P.n_int;
+                snt = P.n_ext;
+            }
+        }
+        if (do_split) {
+            const Interface<R> sp = split(sd, se, sS, sn, sni, snt);
+            A.max_iface = fmax(A.max_iface, (double)sp.balance);
+            // entry: exterior reflection exits, transmission continues;
+            // internal: transmission exits, reflection continues
+            const R epow = fresh ? sp.r.I : (sp.has_t ? sp.t.I : R(0));
+            if (epow > R(0)) {
+                has = true;
+                od = fresh ? sp.dr : sp.dt;
+                opow = epow;
+                L.esc += opow;
+            }
+            if (fresh && !sp.has_t) {
+                finish_ray(P, L, A, s_status, 0, R(0));
+            } else {
+                L.d = fresh ? sp.dt : sp.dr;
                 L.e = sp.s;
-                L.S = sp.r;
-                L.face = hit.face;
+                L.S = fresh ? sp.t : sp.r;
                 settle(P, L, A, s_status);
             }
         }

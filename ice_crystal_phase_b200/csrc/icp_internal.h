@@ -28,6 +28,7 @@ struct CdfLaunch {
 
 int launch_cdf_build(const CdfLaunch& L, cudaStream_t stream);
 int cdf_max_coresident_blocks(size_t smem, int device);
+size_t cdf_smem_bytes(uint32_t ct, uint32_t cp, uint32_t cw);
 size_t cdf_partial_bytes();
 
 // Host-side description of one hex trace+bin launch (double precision inputs; the
