@@ -42,6 +42,7 @@ UNITS = {
     "icp_cdf.cu": ["-fmad=false"],
     "icp_capi.cu": ["-fmad=false"],
     "icp_capi_drop.cu": ["-fmad=false"],
+    "icp_cdf_static.cu": ["-fmad=false"],
 }
 
 HOST_SOURCES = ["icp_record_io.cpp", "icp_orientation.cpp", "icp_projected_area.cpp", "icp_water.cpp"]

@@ -87,6 +87,10 @@ __global__ void edges_to_float(const double* in, float* out, uint32_t n)
 
 } // namespace
 
+namespace icp {
+void set_last_error(const char* message) { g_error = message; }
+} // namespace icp
+
 struct icp_context {
     int device = 0;
     int sms = 0;

@@ -30,6 +30,8 @@ int launch_cdf_build(const CdfLaunch& L, cudaStream_t stream);
 int cdf_max_coresident_blocks(size_t smem, int device);
 size_t cdf_smem_bytes(uint32_t ct, uint32_t cp, uint32_t cw);
 size_t cdf_partial_bytes();
+// Sets the calling thread's message returned by icp_last_error().
+void set_last_error(const char* message);
 
 // Host-side description of one hex trace+bin launch (double precision inputs; the
 // launcher converts to the kernel's arithmetic type).

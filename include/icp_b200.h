@@ -178,6 +178,23 @@ int icp_phase_cdf_build(icp_context* ctx, const double* d_values, uint32_t input
                         uint32_t np, double forward_pole, double backward_pole, uint32_t ct, uint32_t cp,
                         const icp_cdf_policy* policy, double* d_phi, double* d_theta, icp_cdf_report* report);
 
+/* Static-scratch CDF builder: no counterpart in the reference.  For callers that cannot
+ * allocate device memory themselves or through this library -- an embedding application
+ * whose own allocator already owns the device, or a callback context where allocating is
+ * not allowed.  Same inputs, outputs, gates and report as icp_phase_cdf_build, on the given
+ * cudaStream_t (NULL = legacy default stream, current device), but every scratch buffer
+ * (u edges, block partials, column sums, barrier counters, audit record) lives in one
+ * file-scope device array of about 220 KiB that each GPU holds until the process exits.
+ * Limits: nt <= ICP_STATIC_MAX_THETA, cp <= ICP_STATIC_MAX_PHI (ICP_ERR_CAPACITY beyond).
+ * The first call on a device looks the array's address up (make it before any stream
+ * capture); all calls share the array, so calls that overlap on the GPU race on it. */
+#define ICP_STATIC_MAX_THETA 4096u
+#define ICP_STATIC_MAX_PHI 8192u
+#define ICP_STATIC_MAX_BLOCKS 1024u
+int icp_phase_cdf_build_static(void* stream, const double* d_values, uint32_t input_kind, uint32_t nt, uint32_t np,
+                               double forward_pole, double backward_pole, uint32_t ct, uint32_t cp,
+                               const icp_cdf_policy* policy, double* d_phi, double* d_theta, icp_cdf_report* report);
+
 /* ----------------------------------------------------- whole hex record (e2e) */
 typedef struct {
     double circumradius_mm, length_mm;
