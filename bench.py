@@ -164,7 +164,7 @@ def run_b200(a) -> None:
     for i, v in enumerate(I.rotation_from_quaternion(1, 0, 0, 0)):
         node.rotation[i] = v
     node.exterior_index, node.interior_index = 1.0, c["n"]
-    node.tail_tolerance, node.balance_tolerance = 1e-12, 1e-5
+    node.tail_tolerance, node.balance_tolerance = 1e-12, 1e-10
     node.seed, node.total_samples = c["seed"], rays * world
     node.first_sample, node.sample_count = rank * rays, rays
     node.max_internal_hits, node.batch_size, node.precision = c["hits"], 4096, I.ICP_FP32
@@ -279,7 +279,7 @@ def run_b200(a) -> None:
         for i in range(3):
             rec.ki[i] = c["ki"][i]
         rec.exterior_index, rec.interior_index = 1.0, c["n"]
-        rec.tail_tolerance, rec.balance_tolerance = 1e-12, 1e-5
+        rec.tail_tolerance, rec.balance_tolerance = 1e-12, 1e-10
         rec.nt, rec.np, rec.ct, rec.cp = c["nt"], c["np"], c["nt"], c["np"]
         rec.max_internal_hits, rec.batch_size, rec.precision = c["hits"], 4096, I.ICP_FP32
         rec.policy = policy

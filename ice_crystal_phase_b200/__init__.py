@@ -66,7 +66,7 @@ class TraceStats(C.Structure):
                 ("max_interface_balance", C.c_double), ("rays", C.c_uint64), ("outputs", C.c_uint64),
                 ("status_counts", C.c_uint64 * 8), ("rejected_rays", C.c_uint64), ("snapped", C.c_uint64),
                 ("near_edge", C.c_uint64), ("fallback_adds", C.c_uint64), ("max_batch_outputs", C.c_uint64),
-                ("invalid", C.c_uint64), ("encounters", C.c_uint64)]
+                ("invalid", C.c_uint64), ("encounters", C.c_uint64), ("missed", C.c_uint64)]
 
     def as_dict(self) -> dict:
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "status_counts"}
@@ -408,8 +408,7 @@ class PhaseMassAccumulatorCuda:
             n.rotation[i] = v
         n.exterior_index, n.interior_index = exterior_index, interior_index
         n.tail_tolerance = tail_tolerance
-        n.balance_tolerance = balance_tolerance if balance_tolerance is not None else (
-            1e-10 if precision == ICP_FP64 else 1e-5)
+        n.balance_tolerance = 1e-10 if balance_tolerance is None else balance_tolerance
         n.seed, n.total_samples, n.first_sample = seed, samples, first
         n.sample_count = samples - first if count is None else count
         n.max_internal_hits, n.batch_size, n.precision = max_internal_hits, batch_size, precision
@@ -502,8 +501,7 @@ def generate_hex_record(ctx: Context, circumradius_mm: float, length_mm: float, 
         r.ki[i] = float(ki[i])
     r.exterior_index, r.interior_index = exterior_index, interior_index
     r.tail_tolerance = tail_tolerance
-    r.balance_tolerance = balance_tolerance if balance_tolerance is not None else (
-        1e-10 if precision == ICP_FP64 else 1e-5)
+    r.balance_tolerance = 1e-10 if balance_tolerance is None else balance_tolerance
     r.nt, r.np, r.ct, r.cp = nt, np_, ct, cp
     r.max_internal_hits, r.batch_size, r.max_output_records = max_internal_hits, batch_size, max_output_records
     r.precision = precision

@@ -35,9 +35,9 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "--Werror", "cross-execution-space-c
           "-I", str(ROOT / "include"), "-I", str(CSRC), "-I", str(HOST)]
 
 UNITS = {
-    "icp_hex_f32.cu": ["-fmad=true"],
+    "icp_hex_f32.cu": ["-fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
     "icp_hex_f64.cu": ["-fmad=false"],
-    "icp_drop_f32.cu": ["-fmad=true"],
+    "icp_drop_f32.cu": ["-fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
     "icp_drop_f64.cu": ["-fmad=false"],
     "icp_cdf.cu": ["-fmad=false"],
     "icp_capi.cu": ["-fmad=false"],
@@ -45,7 +45,7 @@ UNITS = {
     "icp_cdf_static.cu": ["-fmad=false"],
 }
 
-HOST_SOURCES = ["icp_record_io.cpp", "icp_orientation.cpp", "icp_projected_area.cpp", "icp_water.cpp"]
+HOST_SOURCES = ["icp_record_io.cpp", "icp_projected_area.cpp", "icp_water.cpp"]
 APP_SOURCES = {"ice_generate_phase": "ice_generate_phase.cpp", "rainbow_generate": "rainbow_generate.cpp"}
 
 
@@ -84,15 +84,6 @@ def build_library(verbose: bool = False, ptxas_info: bool = False) -> Path:
             extra = ["-Xptxas", "-v"] if ptxas_info else []
             _run([NVCC, *COMMON, *flags, *extra, "-c", str(src), "-o", str(obj)], verbose or ptxas_info)
         objs.append(obj)
-    for unit in HOST_SOURCES:
-        src = HOST / unit
-        if not src.exists():
-            continue
-        obj = OUT / (unit + ".o")
-        if _newer(obj, [src, *hdrs]):
-            _run(["g++", "-std=c++20", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-I", str(ROOT / "include"),
-                  "-I", str(HOST), "-c", str(src), "-o", str(obj)], verbose)
-        objs.append(obj)
     if _newer(LIB, objs):
         _run([NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcuda"], verbose)
     return LIB
@@ -106,10 +97,11 @@ def build_apps(verbose: bool = False) -> list[Path]:
         if not s.exists():
             continue
         exe = BIN / name
-        if _newer(exe, [s, LIB, *_headers()]):
+        host = [HOST / h for h in HOST_SOURCES if (HOST / h).exists()]
+        if _newer(exe, [s, LIB, *host, *_headers()]):
             _run(["g++", "-std=c++20", "-O2", "-ffp-contract=off", "-fno-fast-math", "-I", str(ROOT / "include"),
-                  "-I", str(HOST), str(s), "-L", str(PKG), "-licp_b200", f"-Wl,-rpath,$ORIGIN/..", "-o", str(exe)],
-                 verbose)
+                  "-I", str(HOST), str(s), *map(str, host), "-L", str(PKG), "-licp_b200", "-Wl,-rpath,$ORIGIN/..",
+                  "-o", str(exe)], verbose)
         built.append(exe)
     return built
 

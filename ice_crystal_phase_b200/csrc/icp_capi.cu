@@ -20,10 +20,6 @@
 #include "../host/icp_host_math.hpp"
 #include "icp_internal.h"
 
-namespace icp {
-int hex_blocks_per_sm_f32(uint32_t slots, uint32_t nt, uint32_t threads);
-int hex_blocks_per_sm_f64(uint32_t slots, uint32_t nt, uint32_t threads);
-}
 
 using namespace icp;
 namespace H = icp::host;
@@ -282,7 +278,7 @@ void stats_accumulate(const unsigned char* raw, icp_trace_stats* out)
         double axial;
         unsigned long long max_bal_bits, max_iface_bits;
         unsigned long long rays, outputs, status[8], rejected, snapped, near_edge, fallback, invalid;
-        unsigned long long encounters;
+        unsigned long long encounters, missed;
     } r;
     std::memcpy(&r, raw, sizeof r);
     auto fx = [](const unsigned long long* v) { return (std::ldexp((double)v[1], 64) + (double)v[0]) * 0x1p-44; };
@@ -305,6 +301,7 @@ void stats_accumulate(const unsigned char* raw, icp_trace_stats* out)
     out->fallback_adds += r.fallback;
     out->invalid += r.invalid;
     out->encounters += r.encounters;
+    out->missed += r.missed;
 }
 
 __global__ void max_u32(const uint32_t* v, uint64_t n, unsigned long long* out)
@@ -381,7 +378,7 @@ extern "C" int icp_hex_trace_bin(icp_context* c, const icp_hex_node* n, const ic
     std::memcpy(L.rot, n->rotation, sizeof L.rot);
     std::memcpy(L.ki, g->ki, sizeof L.ki);
     std::memcpy(L.e0, g->e0, sizeof L.e0);
-    std::memcpy(L.e1, g->e1, sizeof L.e1);
+    std::memcpy(L.e1g, g->e1, sizeof L.e1g);
     L.nt = g->nt;
     L.np = g->np;
     L.edges_d = d_edges;

@@ -9,9 +9,9 @@
 //            (Kahan, row-major order), keeps the coarse strip in shared memory, and
 //            publishes fine / coarse moments and its maximum;
 //   barrier
-//   phase B  coarsening TV, then per column an ordered binary64 scan in ascending theta of
-//            w = coarse / largest (exact plateaus, monotone prefixes), written unnormalised
-//            to the phi-major output, column sums published;
+//   phase B  coarsening TV, the weights w = coarse / largest (parallel), then per column an
+//            ordered binary64 scan in ascending theta (exact plateaus, monotone prefixes) kept
+//            in shared memory, column sums published;
 //   barrier
 //   phase C  ordered marginal scan over all column sums (every block, identical result),
 //            normalisation (empty column -> the stored u edges), the phi marginal, and the
@@ -86,6 +86,16 @@ __device__ __forceinline__ double fine_mass_at(const CdfParams& P, uint32_t i, u
     if (i == 0) m += P.fwd_add;
     if (i + 1 == P.nt) m += P.bwd_add;
     return m;
+}
+
+// Conservative aggregate of one coarse cell: Kahan sum in row-major fine order
+// (hex_phase/src/phase_table.cpp:122-123).
+__device__ __forceinline__ double coarse_at(const CdfParams& P, uint32_t ci, uint32_t cj)
+{
+    KSum acc{0, 0};
+    for (uint32_t i = ci * P.dt; i < (ci + 1) * P.dt; ++i)
+        for (uint32_t j = cj * P.dp; j < (cj + 1) * P.dp; ++j) acc.add(fine_mass_at(P, i, j));
+    return acc.v;
 }
 
 template <class T> __device__ __forceinline__ T block_sum(T x, T* red)
@@ -210,19 +220,26 @@ __global__ void __launch_bounds__(kThreads) cdf_build_kernel(const CdfParams P)
             tv.add(fabs(fine_mass_at(P, i, j) / fine_total - strip[(size_t)ci * CW + cl] / stored_total * fraction));
         }
     }
+    // weights w = coarse / largest for the whole strip in parallel (the ordered chains below
+    // then carry only additions); the coarse values are recomputed in phase C for the audit
     unsigned long long underflow = 0ull;
+    for (uint32_t q = threadIdx.x; q < P.ct * w; q += blockDim.x) {
+        const uint32_t i = q / w, cl = q % w;
+        const double c = strip[(size_t)i * CW + cl];
+        const double x = c / big;
+        if (c > 0 && !(x > 0)) ++underflow;
+        strip[(size_t)i * CW + cl] = x;
+    }
+    __syncthreads();
     if (threadIdx.x < w) {
-        // ordered ascending-theta scan of one phi column; unnormalised prefixes to the output
+        // ordered ascending-theta scan of one phi column; the unnormalised prefix of row i+1
+        // replaces the weight of row i in place (each column belongs to one thread)
         const uint32_t cl = threadIdx.x, j = c0 + cl;
-        double* out = P.theta + (size_t)j * (P.ct + 1);
         double s = 0.0;
-        out[0] = 0.0;
+#pragma unroll 8
         for (uint32_t i = 0; i < P.ct; ++i) {
-            const double c = strip[(size_t)i * CW + cl];
-            const double x = c / big;
-            if (c > 0 && !(x > 0)) ++underflow;
-            s += x;
-            out[i + 1] = s;
+            s += strip[(size_t)i * CW + cl];
+            strip[(size_t)i * CW + cl] = s;
         }
         P.colsum[j] = s;
     }
@@ -275,49 +292,40 @@ __global__ void __launch_bounds__(kThreads) cdf_build_kernel(const CdfParams P)
     double max_err = 0.0;
     unsigned long long lost_cells = 0ull, malformed = 0ull;
     const uint32_t stride = P.ct + 1;
-    // this strip's output rows are contiguous: theta[c0*(ct+1) .. c1*(ct+1)).  Each chunk of
-    // blockDim.x elements is read raw (an element and its successor) before any is rewritten.
+    // this strip's output rows are contiguous: theta[c0*(ct+1) .. c1*(ct+1)); every element is
+    // written once, from the prefixes kept in shared memory (prefix of row i at strip[i-1])
     const uint32_t span = w * stride;
-    for (uint32_t base = 0; base < span; base += blockDim.x) {
-        const uint32_t q = base + threadIdx.x;
-        double b0 = 0.0;
-        double* row = nullptr;
-        uint32_t i = 0;
-        if (q < span) {
-            const uint32_t cl = q / stride, j = c0 + cl;
-            i = q % stride;
-            const double cs = stage[j];
-            row = P.theta + (size_t)j * stride;
-            auto norm = [&](uint32_t k, double raw) -> double {
-                if (k == 0) return 0.0;
-                if (k == P.ct) return 1.0;
-                return cs > 0 ? raw / cs : P.edges[(size_t)k * P.dt];
-            };
-            b0 = norm(i, row[i]);
-            if (i < P.ct) {
-                const double b1 = norm(i + 1, row[i + 1]);
-                const double a0 = sphi[cl], a1 = sphi[cl + 1];
-                const double qv = (a1 - a0) * (b1 - b0);
-                const double c = strip[(size_t)i * CW + cl];
-                const double p = c / stored_total;
-                const bool bad = !(qv >= 0.0) || !(qv <= 1.7976931348623157e308) || a1 < a0 || b1 < b0;
-                if (bad) ++malformed;
-                if (c > 0 && !(p > 0)) ++malformed;
-                const double err = fabs(p - qv);
-                l1.add(err);
-                max_err = fmax(max_err, err);
-                if (p > 0 && qv == 0) {
-                    lost.add(p);
-                    ++lost_cells;
-                }
-                rec.add(qv);
-                const double E0 = P.edges[(size_t)i * P.dt], E1 = P.edges[(size_t)(i + 1) * P.dt];
-                ax.add(qv * (1.0 - E0 - E1));
+#pragma unroll 2
+    for (uint32_t q = threadIdx.x; q < span; q += blockDim.x) {
+        const uint32_t cl = q / stride, i = q % stride, j = c0 + cl;
+        const double cs = stage[j];
+        auto norm = [&](uint32_t k) -> double {
+            if (k == 0) return 0.0;
+            if (k == P.ct) return 1.0;
+            return cs > 0 ? strip[(size_t)(k - 1) * CW + cl] / cs : P.edges[(size_t)k * P.dt];
+        };
+        const double b0 = norm(i);
+        if (i < P.ct) {
+            const double b1 = norm(i + 1);
+            const double a0 = sphi[cl], a1 = sphi[cl + 1];
+            const double qv = (a1 - a0) * (b1 - b0);
+            const double c = coarse_at(P, i, j);
+            const double p = c / stored_total;
+            const bool bad = !(qv >= 0.0) || !(qv <= 1.7976931348623157e308) || a1 < a0 || b1 < b0;
+            if (bad) ++malformed;
+            if (c > 0 && !(p > 0)) ++malformed;
+            const double err = fabs(p - qv);
+            l1.add(err);
+            max_err = fmax(max_err, err);
+            if (p > 0 && qv == 0) {
+                lost.add(p);
+                ++lost_cells;
             }
+            rec.add(qv);
+            const double E0 = P.edges[(size_t)i * P.dt], E1 = P.edges[(size_t)(i + 1) * P.dt];
+            ax.add(qv * (1.0 - E0 - E1));
         }
-        __syncthreads();
-        if (row) row[i] = b0;
-        __syncthreads();
+        P.theta[(size_t)c0 * stride + q] = b0;
     }
     {
         const double a = block_sum(l1.v + l1.c, red_d);

@@ -115,16 +115,28 @@ template <class R> struct Interface {
     R balance;      // relative power imbalance of this split
 };
 
+// Refraction constants of one oriented interface (incident index ni -> transmitted nt),
+// normalised by the larger index as the reference does (flux_interface.hpp:51).
+template <class R> struct Media {
+    R a, b, eta; // ni/max, nt/max, a/b
+    bool matched; // ni == nt: the ray passes unchanged (flux_interface.hpp:34-41)
+};
+template <class R> __host__ __device__ inline Media<R> make_media(double ni, double nt)
+{
+    const double ns = ni > nt ? ni : nt, a = ni / ns, b = nt / ns;
+    return Media<R>{R(a), R(b), R(a / b), ni == nt};
+}
+
 // Fresnel split in flux normalisation (flux_interface.hpp:26-88).  n points into the incident
-// medium; (ni, nt) are the incident / transmitted indices.  `e` is the ray's current frame
-// vector.  The transmitted flux is 1 - R for each of s and p, so power is conserved to one
-// rounding per interface; its Mueller off-diagonal term is sqrt(Ts*Tp) = ts*tp.
+// medium.  `e` is the ray's current frame vector.  The transmitted flux is 1 - R for each of
+// s and p, so power is conserved to one rounding per interface; its Mueller off-diagonal
+// term is sqrt(Ts*Tp) = ts*tp.  Partial reflection and total internal reflection are both
+// evaluated and selected per lane (no divergent branch between them).
 template <class R>
-__device__ __forceinline__ Interface<R> split(V3<R> d, V3<R> e, Stokes<R> S, V3<R> n, R ni, R nt)
+__device__ __forceinline__ Interface<R> split(V3<R> d, V3<R> e, Stokes<R> S, V3<R> n, const Media<R>& M)
 {
     Interface<R> out;
-    if (ni == nt) {
-        // matched media (flux_interface.hpp:34-41): the ray continues unchanged, no reflection
+    if (M.matched) {
         out.s = e;
         out.dt = d;
         out.t = S;
@@ -149,61 +161,75 @@ __device__ __forceinline__ Interface<R> split(V3<R> d, V3<R> e, Stokes<R> S, V3<
     const R cos2 = c * c - sg * sg, sin2p = R(2) * c * sg;
     const R Q = cos2 * S.Q + sin2p * S.U;
     const R U = -sin2p * S.Q + cos2 * S.U;
-    const R ns = rmax(ni, nt), a = ni / ns, b = nt / ns, eta = a / b;
-    const R st = eta * sine;
+    const R a = M.a, b = M.b;
+    const R st = M.eta * sine;
     out.dr = unit(d + n * (R(2) * ci));
     out.ci = ci;
-    R Rs, Rp, zr, zi;
-    if (st > R(1)) {
-        // total internal reflection: |rs| = |rp| = 1, relative phase exp(i(ds - dp))
-        const R inv = R(1) / st;
-        const R beta = st * sqrt_r((R(1) - inv) * (R(1) + inv));
-        // rs = (x - i y)/(x + i y) with x = a ci, y = b beta; rp with (b ci, a beta)
-        R x1 = a * ci, y1 = b * beta, x2 = b * ci, y2 = a * beta;
-        const R s1 = rmax(rabs(x1), rabs(y1)), s2 = rmax(rabs(x2), rabs(y2));
-        x1 /= s1; y1 /= s1; x2 /= s2; y2 /= s2;
-        const R d1 = x1 * x1 + y1 * y1, d2 = x2 * x2 + y2 * y2;
-        const R rsr = (x1 * x1 - y1 * y1) / d1, rsi = (R(-2) * x1 * y1) / d1;
-        const R rpr = (x2 * x2 - y2 * y2) / d2, rpi = (R(-2) * x2 * y2) / d2;
-        Rs = R(1);
-        Rp = R(1);
-        zr = rsr * rpr + rsi * rpi; // rs * conj(rp)
-        zi = rsi * rpr - rsr * rpi;
-        out.tir = true;
-        out.has_t = false;
+    const bool tir = st > R(1);
+    R Rs, Rp, zr, zi, ct;
+    if constexpr (sizeof(R) == 8) {
+        // reference arithmetic (flux_interface.hpp:59-79)
+        if (tir) {
+            const R inv = R(1) / st;
+            const R beta = st * sqrt_r((R(1) - inv) * (R(1) + inv));
+            R x1 = a * ci, y1 = b * beta, x2 = b * ci, y2 = a * beta;
+            const R s1 = rmax(rabs(x1), rabs(y1)), s2 = rmax(rabs(x2), rabs(y2));
+            x1 /= s1; y1 /= s1; x2 /= s2; y2 /= s2;
+            const R d1 = x1 * x1 + y1 * y1, d2 = x2 * x2 + y2 * y2;
+            const R rsr = (x1 * x1 - y1 * y1) / d1, rsi = (R(-2) * x1 * y1) / d1;
+            const R rpr = (x2 * x2 - y2 * y2) / d2, rpi = (R(-2) * x2 * y2) / d2;
+            Rs = R(1);
+            Rp = R(1);
+            zr = rsr * rpr + rsi * rpi; // rs * conj(rp)
+            zi = rsi * rpr - rsr * rpi;
+            ct = R(0);
+        } else {
+            ct = sqrt_r((R(1) - st) * (R(1) + st));
+            const R ds = a * ci + b * ct, dp = b * ci + a * ct;
+            const R rs = (a * ci - b * ct) / ds, rp = (b * ci - a * ct) / dp;
+            Rs = rs * rs;
+            Rp = rp * rp;
+            zr = rs * rp;
+            zi = R(0);
+        }
     } else {
-        const R ct = sqrt_r((R(1) - st) * (R(1) + st));
+        // binary32: both branches, selected per lane
+        const R k2 = (R(1) - st) * (R(1) + st);
+        ct = sqrt_r(rmax(k2, R(0)));
+        const R beta = sqrt_r(rmax(-k2, R(0)));
+        // partial reflection
         const R ds = a * ci + b * ct, dp = b * ci + a * ct;
         const R rs = (a * ci - b * ct) / ds, rp = (b * ci - a * ct) / dp;
-        Rs = rs * rs;
-        Rp = rp * rp;
-        zr = rs * rp;
-        zi = R(0);
-        out.tir = false;
-        out.has_t = true;
-        out.dt = unit((d + n * ci) * eta - n * ct);
-        const R Ts = R(1) - Rs, Tp = R(1) - Rp;
-        const R zt = sqrt_r(Ts * Tp);
-        const R hs = R(0.5) * (Rs + Rp), hd = R(0.5) * (Rs - Rp);
-        out.r.I = hs * S.I + hd * Q;
-        out.r.Q = hd * S.I + hs * Q;
-        out.t.I = S.I - out.r.I;
-        out.t.Q = Q - out.r.Q;
-        out.t.U = zt * U;
-        out.t.V = zt * S.V;
-        out.r.U = zr * U;
-        out.r.V = zr * S.V;
-        const R after = out.r.I + out.t.I;
-        out.balance = S.I > R(0) ? rabs(after - S.I) / S.I : R(0);
-        return out;
+        // total internal reflection: rs = (x1 - i y1)/(x1 + i y1), rp = (x2 - i y2)/(x2 + i y2)
+        const R x1 = a * ci, y1 = b * beta, x2 = b * ci, y2 = a * beta;
+        const R i1 = R(1) / (x1 * x1 + y1 * y1), i2 = R(1) / (x2 * x2 + y2 * y2);
+        const R rsr = (x1 * x1 - y1 * y1) * i1, rsi = (R(-2) * x1 * y1) * i1;
+        const R rpr = (x2 * x2 - y2 * y2) * i2, rpi = (R(-2) * x2 * y2) * i2;
+        Rs = tir ? R(1) : rs * rs;
+        Rp = tir ? R(1) : rp * rp;
+        zr = tir ? rsr * rpr + rsi * rpi : rs * rp;
+        zi = tir ? rsi * rpr - rsr * rpi : R(0);
     }
+    out.tir = tir;
+    out.has_t = !tir;
     const R hs = R(0.5) * (Rs + Rp), hd = R(0.5) * (Rs - Rp);
     out.r.I = hs * S.I + hd * Q;
     out.r.Q = hd * S.I + hs * Q;
     out.r.U = zr * U - zi * S.V;
     out.r.V = zi * U + zr * S.V;
-    out.t = {R(0), R(0), R(0), R(0)};
-    out.balance = S.I > R(0) ? rabs(out.r.I - S.I) / S.I : R(0);
+    if (!tir) {
+        out.dt = unit((d + n * ci) * M.eta - n * ct);
+        const R zt = sqrt_r((R(1) - Rs) * (R(1) - Rp));
+        out.t.I = S.I - out.r.I;
+        out.t.Q = Q - out.r.Q;
+        out.t.U = zt * U;
+        out.t.V = zt * S.V;
+        out.balance = S.I > R(0) ? rabs(out.r.I + out.t.I - S.I) / S.I : R(0);
+    } else {
+        out.dt = d;
+        out.t = {R(0), R(0), R(0), R(0)};
+        out.balance = S.I > R(0) ? rabs(out.r.I - S.I) / S.I : R(0);
+    }
     return out;
 }
 

@@ -1,0 +1,145 @@
+// icp_drop.cuh -- axisymmetric water-drop geometry for the drop trace kernel (sm_100a).
+//
+// Shape (include/rainbow/raindrop_shape.hpp:11-100): r/a = 1 + sum_{n=0}^{7} c_n T_n(mu), with
+// mu = cos(chi) and chi measured from the particle's -y axis (gravity), coordinates in units
+// of the equal-volume radius a.  R(mu) and dR/dmu use the Chebyshev recurrence, so no acos and
+// no division by sin(chi) is needed at the poles.
+//
+// Intersection: the reference brackets f = |p| - R(mu) with outward-rounded intervals and
+// polishes with safeguarded Newton (raindrop_intersection.hpp:203-382).  Here the drop is a
+// convex body, so its gauge rho(p) = |p| / R(mu(p)) is a convex function along any line.  On a
+// convex function Newton's method started where rho >= 1 moves monotonically towards the
+// nearest root without overshoot: started on the conservative outer sphere it converges to
+// the entry point (from before the body) or to the exit point (from beyond it), and a line
+// that misses the body shows up as rho' >= 0 while rho > 1.  A point that rounding left
+// slightly off the surface does not change which root is reached.  Spheres (c_1..c_7 = 0) use
+// the closed-form quadratic.
+#pragma once
+#include "icp_device.cuh"
+
+namespace icp {
+
+template <class R> struct DropShape {
+    R c[8];
+    R r_out;     // conservative bounding radius (outer sphere)
+    R r_center;  // 1 + c_0 (the sphere radius when c_1..c_7 vanish)
+    bool sphere;
+};
+
+// R(mu) and dR/dmu (raindrop_shape.hpp:70-84).
+template <class R> __device__ __forceinline__ R drop_radius(const DropShape<R>& S, R mu, R& dr)
+{
+    R prev = R(1), cur = mu, dprev = R(0), dcur = R(1);
+    R radius = R(1) + S.c[0] + S.c[1] * mu;
+    R deriv = S.c[1];
+#pragma unroll
+    for (int n = 2; n < 8; ++n) {
+        const R next = R(2) * mu * cur - prev;
+        const R dnext = R(2) * cur + R(2) * mu * dcur - dprev;
+        radius += S.c[n] * next;
+        deriv += S.c[n] * dnext;
+        prev = cur;
+        cur = next;
+        dprev = dcur;
+        dcur = dnext;
+    }
+    dr = deriv;
+    return radius;
+}
+
+// Outward surface normal at p (gradient of |p| - R(mu), raindrop_shape.hpp:92-100), unit.
+template <class R> __device__ __forceinline__ V3<R> drop_normal(const DropShape<R>& S, V3<R> p)
+{
+    if (S.sphere) return unit(p);
+    const R r = sqrt_r(dot(p, p));
+    const V3<R> u = p * (R(1) / r);
+    const R mu = -u.y;
+    R dr;
+    (void)drop_radius(S, mu, dr);
+    const V3<R> g = u - (v3(R(0), R(-1), R(0)) - u * mu) * (dr / r);
+    return unit(g);
+}
+
+// Gauge rho(p + t d) - 1 and its t-derivative.
+template <class R> __device__ __forceinline__ R gauge(const DropShape<R>& S, V3<R> p, V3<R> d, R& dh)
+{
+    const R r = sqrt_r(dot(p, p));
+    const R inv_r = R(1) / r;
+    const R rd = dot(p, d) * inv_r;             // d|p|/dt
+    const R mu = -p.y * inv_r;
+    const R dmu = (-d.y - mu * rd) * inv_r;     // dmu/dt
+    R dR;
+    const R Rm = drop_radius(S, mu, dR);
+    const R invR = R(1) / Rm;
+    dh = (rd - r * invR * dR * dmu) * invR;
+    return r * invR - R(1);
+}
+
+// Roots of |p + t d| = rad (d unit): false when the line misses the sphere.
+template <class R> __device__ __forceinline__ bool sphere_roots(V3<R> p, V3<R> d, R rad, R& t0, R& t1)
+{
+    const R b = dot(p, d);
+    const R c = dot(p, p) - rad * rad;
+    const R disc = b * b - c;
+    if (!(disc >= R(0))) return false;
+    const R q = sqrt_r(disc);
+    t0 = -b - q;
+    t1 = -b + q;
+    return true;
+}
+
+constexpr int kNewtonMax = 40;
+
+// First surface point along the line from an exterior point: t of the entry, false on a miss.
+template <class R> __device__ __forceinline__ bool drop_entry(const DropShape<R>& S, V3<R> o, V3<R> d, R& t)
+{
+    R t0, t1;
+    if (S.sphere) {
+        if (!sphere_roots(o, d, S.r_center, t0, t1)) return false;
+        t = t0;
+        return t0 >= R(0);
+    }
+    if (!sphere_roots(o, d, S.r_out, t0, t1)) return false;
+    t = rmax(t0, R(0));
+    R prev_h = R(1e30);
+    for (int it = 0; it < kNewtonMax; ++it) {
+        R dh;
+        const R h = gauge(S, o + d * t, d, dh);
+        if (h <= R(0)) return true;          // converged from outside to the entry root
+        if (!(dh < R(0))) return false;       // convex and non-decreasing while outside: miss
+        const R step = h / dh;                // negative
+        t -= step;
+        if (t > t1) return false;
+        if (!(h < prev_h) || rabs(step) <= R(4) * Eps<R>::eps * rmax(R(1), rabs(t))) return true;
+        prev_h = h;
+    }
+    return true;
+}
+
+// Exit point along an interior chord that starts on (or rounding-close to) the surface.
+template <class R> __device__ __forceinline__ R drop_exit(const DropShape<R>& S, V3<R> p, V3<R> d)
+{
+    R t0, t1;
+    if (S.sphere) {
+        // larger root of |p + t d| = R; p may be off the sphere by rounding
+        if (!sphere_roots(p, d, S.r_center, t0, t1)) return R(0);
+        return rmax(t1, R(0));
+    }
+    if (!sphere_roots(p, d, S.r_out, t0, t1)) return R(0);
+    R t = rmax(t1, R(0));
+    R prev_h = R(1e30);
+    for (int it = 0; it < kNewtonMax; ++it) {
+        R dh;
+        const R h = gauge(S, p + d * t, d, dh);
+        if (h <= R(0)) break;                 // reached the exit root from beyond it
+        if (!(dh > R(0))) break;              // degenerate tangent chord: stay at t
+        const R step = h / dh;                // positive
+        t -= step;
+        if (t <= R(0)) return R(0);
+        if (!(h < prev_h) || step <= R(4) * Eps<R>::eps * rmax(R(1), t)) break;
+        prev_h = h;
+    }
+    return t;
+}
+
+} // namespace icp

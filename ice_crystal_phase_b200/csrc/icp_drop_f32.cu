@@ -1,0 +1,10 @@
+// icp_drop_f32.cu -- FP32 instantiation of the trace+bin kernel for the axisymmetric drop.
+#include "icp_hex_launch.cuh"
+
+namespace icp {
+int launch_drop_f32(const HexLaunch& L, cudaStream_t s) { return launch_trace(make_drop_params<float>(L), L, s); }
+int drop_blocks_per_sm_f32(uint32_t slots, uint32_t nt, uint32_t threads)
+{
+    return trace_blocks_per_sm<float, DropGeo<float>>(slots, nt, threads);
+}
+} // namespace icp

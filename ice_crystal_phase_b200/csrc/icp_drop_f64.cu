@@ -1,0 +1,10 @@
+// icp_drop_f64.cu -- FP64 instantiation of the trace+bin kernel for the axisymmetric drop.
+#include "icp_hex_launch.cuh"
+
+namespace icp {
+int launch_drop_f64(const HexLaunch& L, cudaStream_t s) { return launch_trace(make_drop_params<double>(L), L, s); }
+int drop_blocks_per_sm_f64(uint32_t slots, uint32_t nt, uint32_t threads)
+{
+    return trace_blocks_per_sm<double, DropGeo<double>>(slots, nt, threads);
+}
+} // namespace icp

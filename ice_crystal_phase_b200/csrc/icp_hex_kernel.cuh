@@ -1,4 +1,5 @@
-// icp_hex_kernel.cuh -- fused hexagonal-prism trace + (u,phi) binning kernel (sm_100a).
+// icp_hex_kernel.cuh -- fused single-particle trace + (u,phi) binning kernel (sm_100a), with
+// two geometries: the hexagonal prism (HexGeo) and the axisymmetric drop (DropGeo).
 //
 // One launch traces one orientation node's ray range [first, first+count) and adds every
 // exit into the FP64 cell-mass histogram.  It replaces the reference's count kernel, serial
@@ -13,8 +14,10 @@
 // Ray algorithm: hex_trace/include/ice_crystal/hex_trace_core.hpp:190-259 (linear R/T chain),
 // hex_prism.hpp:64-175 (entry sampling, nearest exit plane), flux_interface.hpp:26-88.
 #pragma once
+#include <type_traits>
 #include "icp_bin.cuh"
 #include "icp_device.cuh"
+#include "icp_drop.cuh"
 
 namespace icp {
 
@@ -25,7 +28,7 @@ struct DevStats {
     double axial;
     unsigned long long max_bal_bits, max_iface_bits; // bit patterns of non-negative doubles
     unsigned long long rays, outputs, status[8], rejected, snapped, near_edge, fallback, invalid;
-    unsigned long long encounters;
+    unsigned long long encounters, missed;
 };
 
 __device__ __forceinline__ void add128(unsigned long long* p, unsigned long long t)
@@ -35,14 +38,27 @@ __device__ __forceinline__ void add128(unsigned long long* p, unsigned long long
     if (old + t < old) atomicAdd(p + 1, 1ull);
 }
 
-template <class R> struct HexParams {
-    // geometry in units of the circumradius, body frame (long axis +y)
+// Hexagonal prism in units of its circumradius, body frame (long axis +y).
+template <class R> struct HexGeo {
     R half_len;
-    V3<R> k, ke0;    // incident direction and its frame vector
-    R cum[8];        // cumulative projected face weights (plain adds in face order)
+    R cum[8];           // cumulative projected face weights (plain adds in face order)
     uint32_t face_mask; // faces with positive projected weight
-    R area;          // total projected weight (Kahan sum, as the reference's projected_area)
-    R n_ext, n_int, tail, bal_tol;
+    R area;             // total projected weight (Kahan sum, as the reference's projected_area)
+};
+// Axisymmetric drop in units of its equal-volume radius; rays start on a disk of radius
+// `disk` around the axis through the centre, a distance `back` before the centre.
+template <class R> struct DropGeo {
+    DropShape<R> shape;
+    R disk, back;
+    V3<R> e1;           // second transverse axis (k x ke0)
+};
+
+template <class R, class G> struct TraceParams {
+    G geo;
+    V3<R> k, ke0;    // incident direction and its frame vector
+    R tail, bal_tol;
+    unsigned long long tail_fx; // floor(tail * 2^44): the tail test of the fixed-point path
+    Media<R> enter, leave; // n_ext -> n_int at entry, n_int -> n_ext inside
     uint64_t seed, total, first, count;
     uint32_t max_hits;
     uint32_t batch_size;
@@ -85,13 +101,13 @@ template <class R> __device__ __forceinline__ V3<R> hex_vertex(unsigned f)
     default: return v3(s, R(0), R(-0.5));
     }
 }
-template <class R> __device__ __forceinline__ R face_offset(const HexParams<R>& P, unsigned f)
+template <class R> __device__ __forceinline__ R face_offset(const HexGeo<R>& P, unsigned f)
 {
     return f < 6u ? R(kSqrt3 / 2) : P.half_len;
 }
 
 // hex_prism.hpp:54-57 / 108-120 (FP64 path only): every other face strictly outside tolerance.
-__device__ __forceinline__ bool strict_face_point(const HexParams<double>& P, V3<double> p, unsigned face)
+__device__ __forceinline__ bool strict_face_point(const HexGeo<double>& P, V3<double> p, unsigned face)
 {
     const double tol = 128 * Eps<double>::eps * fmax(1.0, fmax(P.half_len, fmax(fabs(p.x), fmax(fabs(p.y), fabs(p.z)))));
     for (unsigned f = 0; f < 8; ++f) {
@@ -114,7 +130,7 @@ struct Boundary {
 // just outside a neighbouring plane exits there at t = 0); near ties are counted only.
 // FP64: the reference rules, ties within geometry tolerance are ambiguous.
 template <class R>
-__device__ __forceinline__ Boundary next_boundary(const HexParams<R>& P, V3<R>& p, V3<R> d, unsigned start, R& t_out)
+__device__ __forceinline__ Boundary next_boundary(const HexGeo<R>& P, V3<R>& p, V3<R> d, unsigned start, R& t_out)
 {
     Boundary out{8u, 0, false};
     R best = R(3.0e38), second = R(3.0e38);
@@ -152,30 +168,122 @@ __device__ __forceinline__ Boundary next_boundary(const HexParams<R>& P, V3<R>& 
     return out;
 }
 
+// Entry of a fresh ray: point on the particle and the outward normal there.
+// Returns 0, ICP_RAY_AMBIGUOUS (3), or -1 when the sampled ray misses the particle.
+template <class R>
+__device__ __forceinline__ int geo_entry(const HexGeo<R>& G, uint64_t seed, uint64_t id, V3<R>& pos, V3<R>& n,
+                                         unsigned& face)
+{
+    // face in proportion to projected area, point on the face (hex_prism.hpp:64-98)
+    const R u0 = uniform<R>(rng_bits(seed, id, 0));
+    const R u1 = uniform<R>(rng_bits(seed, id, 1));
+    const R u2 = uniform<R>(rng_bits(seed, id, 2));
+    const R target = u0 * G.area;
+    unsigned f8 = 8u, last = 8u;
+#pragma unroll
+    for (unsigned f = 0; f < 8; ++f) {
+        if ((G.face_mask >> f) & 1u) {
+            last = f;
+            if (f8 == 8u && target < G.cum[f]) f8 = f;
+        }
+    }
+    if (f8 == 8u) f8 = last;
+    face = f8;
+    n = face_normal<R>(f8);
+    if (f8 < 6u) {
+        const V3<R> tangent = v3(-n.z, R(0), n.x);
+        pos = (n * R(kSqrt3 / 2) + tangent * (u1 - R(0.5))) + v3(R(0), (R(2) * u2 - R(1)) * G.half_len, R(0));
+    } else {
+        const R sector = R(6) * u1;
+        const unsigned j = (unsigned)sector;
+        const R r = sqrt_r(sector - (R)j);
+        pos = (hex_vertex<R>(j) * (R(1) - u2) + hex_vertex<R>(j + 1u) * u2) * r;
+        pos.y = (f8 == 6u ? R(1) : R(-1)) * G.half_len;
+    }
+    if constexpr (sizeof(R) == 8) {
+        if (!strict_face_point(G, pos, f8)) return 3;
+    }
+    return 0;
+}
+// Next exit point of an interior ray: advances p, returns 0 / 3 / 5 and the outward normal.
+template <class R>
+__device__ __forceinline__ int geo_next(const HexGeo<R>& G, V3<R>& p, V3<R> d, unsigned& face, V3<R>& n, bool& near_edge)
+{
+    R t;
+    const Boundary hit = next_boundary(G, p, d, face, t);
+    near_edge = hit.near_edge;
+    if (hit.status) return hit.status;
+    face = hit.face;
+    n = face_normal<R>(hit.face);
+    return 0;
+}
+
+// Drop: uniform point on the sampling disk (radius^2 uniform, angle uniform), then the first
+// surface point along k; the reference's drops use a deterministic vertex grid instead
+// (raindrop_paths.hpp:52-58), so the counter RNG of the prism path is reused here.
+template <class R>
+__device__ __forceinline__ int geo_entry(const DropGeo<R>& G, const V3<R>& k, const V3<R>& e0, uint64_t seed,
+                                         uint64_t id, V3<R>& pos, V3<R>& n)
+{
+    const R u0 = uniform<R>(rng_bits(seed, id, 0));
+    const R u1 = uniform<R>(rng_bits(seed, id, 1));
+    const R rad = G.disk * sqrt_r(u0);
+    R sn, cs;
+    if constexpr (sizeof(R) == 4) sincospif(R(2) * u1, &sn, &cs);
+    else sincospi(R(2) * u1, &sn, &cs);
+    const V3<R> o = (e0 * (rad * cs) + G.e1 * (rad * sn)) - k * G.back;
+    R t;
+    if (!drop_entry(G.shape, o, k, t)) return -1;
+    pos = o + k * t;
+    n = drop_normal(G.shape, pos);
+    return 0;
+}
+template <class R>
+__device__ __forceinline__ int geo_next(const DropGeo<R>& G, V3<R>& p, V3<R> d, unsigned& face, V3<R>& n, bool& near_edge)
+{
+    near_edge = false;
+    face = 0u;
+    const R t = drop_exit(G.shape, p, d);
+    p = p + d * t;
+    n = drop_normal(G.shape, p);
+    return 0;
+}
+
 template <class R> struct LaneRay {
     V3<R> p, d, e;
     Stokes<R> S;
     uint64_t id;
-    R esc;
+    R esc;                       // binary64 path: escaped power of this ray
+    unsigned long long pfx, escfx; // binary32 path: power of the continuing branch and escaped
+                                   // power, exact integers in units of 2^-44 of one ray
     uint32_t face, hits;
     bool live;
 };
 
 template <class R> struct LaneAcc {
-    unsigned long long esc_fx, unres_fx, fwd_fx, bwd_fx, outputs, rays, rejected, snapped, near_edge, fallback, invalid, encounters;
+    unsigned long long esc_fx, unres_fx, fwd_fx, bwd_fx, outputs, rays, rejected, snapped, near_edge, fallback, invalid, encounters,
+        missed;
     double axial, max_bal, max_iface;
     uint64_t cur_batch;
     uint32_t cur_batch_out;
 };
 
-template <class R>
-__device__ __forceinline__ void finish_ray(const HexParams<R>& P, LaneRay<R>& L, LaneAcc<R>& A, unsigned* s_status,
-                                           int status, R residual)
+template <class R, class P_>
+__device__ __forceinline__ void finish_ray(const P_& P, LaneRay<R>& L, LaneAcc<R>& A, unsigned* s_status,
+                                           int status, unsigned long long residual_fx, R residual)
 {
     L.live = false;
-    const R bal = rabs(L.esc + residual - R(1));
-    A.unres_fx += to_fix(residual);
-    A.max_bal = fmax(A.max_bal, (double)bal);
+    double bal;
+    if constexpr (sizeof(R) == 4) {
+        // escaped + residual is one ray's power exactly unless a branch was lost
+        constexpr unsigned long long one = 1ull << kFixBits;
+        const unsigned long long total = L.escfx + residual_fx;
+        bal = (total >= one ? (double)(total - one) : (double)(one - total)) * kFixUnit;
+    } else {
+        bal = fabs((double)L.esc + (double)residual - 1.0);
+    }
+    A.unres_fx += residual_fx;
+    A.max_bal = fmax(A.max_bal, bal);
     A.rays += 1;
     atomicAdd(&s_status[status], 1u);
     const bool ok = (status == 0 || status == 1) && bal <= P.bal_tol;
@@ -184,17 +292,24 @@ __device__ __forceinline__ void finish_ray(const HexParams<R>& P, LaneRay<R>& L,
 
 // Ends the ray if the continuing branch is exhausted / below the tail / out of encounters
 // (the top-of-loop and after-loop tests of hex_trace_core.hpp:217-251, applied eagerly).
-template <class R>
-__device__ __forceinline__ void settle(const HexParams<R>& P, LaneRay<R>& L, LaneAcc<R>& A, unsigned* s_status)
+template <class R, class P_>
+__device__ __forceinline__ void settle(const P_& P, LaneRay<R>& L, LaneAcc<R>& A, unsigned* s_status)
 {
-    const R power = L.S.I;
-    if (power == R(0)) finish_ray(P, L, A, s_status, 0, R(0));
-    else if (power <= P.tail) finish_ray(P, L, A, s_status, 1, power);
-    else if (L.hits >= P.max_hits) finish_ray(P, L, A, s_status, 2, power);
+    if constexpr (sizeof(R) == 4) {
+        const unsigned long long p = L.pfx;
+        if (p == 0ull) finish_ray<R>(P, L, A, s_status, 0, 0ull, R(0));
+        else if (p <= P.tail_fx) finish_ray<R>(P, L, A, s_status, 1, p, R(0));
+        else if (L.hits >= P.max_hits) finish_ray<R>(P, L, A, s_status, 2, p, R(0));
+    } else {
+        const R power = L.S.I;
+        if (power == R(0)) finish_ray<R>(P, L, A, s_status, 0, 0ull, R(0));
+        else if (power <= P.tail) finish_ray<R>(P, L, A, s_status, 1, to_fix(power), power);
+        else if (L.hits >= P.max_hits) finish_ray<R>(P, L, A, s_status, 2, to_fix(power), power);
+    }
 }
 
-template <class R>
-__global__ void __launch_bounds__(256) hex_trace_bin_kernel(const HexParams<R> P)
+template <class R, class G>
+__global__ void __launch_bounds__(256, (sizeof(R) == 4 ? 3 : 1)) trace_bin_kernel(const TraceParams<R, G> P)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned long long* s_vals = reinterpret_cast<unsigned long long*>(smem);
@@ -230,7 +345,7 @@ __global__ void __launch_bounds__(256) hex_trace_bin_kernel(const HexParams<R> P
     L.live = false;
     LaneAcc<R> A;
     A.esc_fx = A.unres_fx = A.fwd_fx = A.bwd_fx = A.outputs = A.rays = A.rejected = 0ull;
-    A.snapped = A.near_edge = A.fallback = A.invalid = A.encounters = 0ull;
+    A.snapped = A.near_edge = A.fallback = A.invalid = A.encounters = A.missed = 0ull;
     A.axial = A.max_bal = A.max_iface = 0.0;
     A.cur_batch = ~0ull;
     A.cur_batch_out = 0u;
@@ -252,96 +367,101 @@ __global__ void __launch_bounds__(256) hex_trace_bin_kernel(const HexParams<R> P
         bool has = false;
         V3<R> od;
         R opow = R(0);
+        unsigned long long efx = 0ull; // fixed-point power of this step's exit
         // ---- gather the inputs of this step's interface: the entry face of a fresh ray,
         // or the next exit plane of a live one (one shared split per lane per step)
         bool do_split = false;
         V3<R> sd, se, sn;
         Stokes<R> sS;
-        R sni, snt;
+        const Media<R>* media = &P.enter;
         if (fresh) {
-            // entry: face in proportion to projected area, point on the face (hex_prism.hpp:64-98)
-            const R u0 = uniform<R>(rng_bits(P.seed, L.id, 0));
-            const R u1 = uniform<R>(rng_bits(P.seed, L.id, 1));
-            const R u2 = uniform<R>(rng_bits(P.seed, L.id, 2));
-            const R target = u0 * P.area;
-            unsigned face = 8u, last = 8u;
-#pragma unroll
-            for (unsigned f = 0; f < 8; ++f) {
-                if ((P.face_mask >> f) & 1u) {
-                    last = f;
-                    if (face == 8u && target < P.cum[f]) face = f;
-                }
-            }
-            if (face == 8u) face = last;
-            V3<R> pos;
-            const V3<R> n = face_normal<R>(face);
-            if (face < 6u) {
-                const V3<R> tangent = v3(-n.z, R(0), n.x);
-                pos = (n * R(kSqrt3 / 2) + tangent * (u1 - R(0.5))) + v3(R(0), (R(2) * u2 - R(1)) * P.half_len, R(0));
+            V3<R> pos, n;
+            unsigned face = 8u;
+            int es;
+            if constexpr (std::is_same_v<G, HexGeo<R>>) es = geo_entry(P.geo, P.seed, L.id, pos, n, face);
+            else es = geo_entry(P.geo, P.k, P.ke0, P.seed, L.id, pos, n);
+            if (es < 0) {
+                // a sampled ray that misses the particle carries no incident power
+                ++A.missed;
+                ++A.rays;
             } else {
-                const R sector = R(6) * u1;
-                const unsigned j = (unsigned)sector;
-                const R r = sqrt_r(sector - (R)j);
-                pos = (hex_vertex<R>(j) * (R(1) - u2) + hex_vertex<R>(j + 1u) * u2) * r;
-                pos.y = (face == 6u ? R(1) : R(-1)) * P.half_len;
-            }
-            L.live = true;
-            L.esc = R(0);
-            L.hits = 0u;
-            L.p = pos;
-            L.face = face;
-            do_split = true;
-            if constexpr (sizeof(R) == 8) {
-                if (!strict_face_point(P, pos, face)) {
-                    finish_ray(P, L, A, s_status, 3, R(1));
+                L.live = true;
+                L.esc = R(0);
+                L.pfx = 1ull << kFixBits;
+                L.escfx = 0ull;
+                L.hits = 0u;
+                L.p = pos;
+                L.face = face;
+                do_split = true;
+                if (es) {
+                    finish_ray<R>(P, L, A, s_status, es, 1ull << kFixBits, R(1));
                     do_split = false;
                 }
+                sd = P.k;
+                se = P.ke0;
+                sS = Stokes<R>{R(1), R(0), R(0), R(0)};
+                sn = n;
+                media = &P.enter;
             }
-            sd = P.k;
-            se = P.ke0;
-            sS = Stokes<R>{R(1), R(0), R(0), R(0)};
-            sn = n;
-            sni = P.n_ext;
-            snt = P.n_int;
         } else if (L.live) {
             // one internal encounter (hex_trace_core.hpp:217-246)
-            R t;
-            const Boundary hit = next_boundary(P, L.p, L.d, L.face, t);
-            if (hit.status) {
-                finish_ray(P, L, A, s_status, hit.status, L.S.I);
+            V3<R> n;
+            bool near_edge = false;
+            const int hs = geo_next(P.geo, L.p, L.d, L.face, n, near_edge);
+            if (hs) {
+                finish_ray<R>(P, L, A, s_status, hs, sizeof(R) == 4 ? L.pfx : to_fix(L.S.I), L.S.I);
             } else {
-                A.near_edge += hit.near_edge ? 1ull : 0ull;
-                L.face = hit.face;
+                A.near_edge += near_edge ? 1ull : 0ull;
                 ++L.hits;
                 ++A.encounters;
                 do_split = true;
                 sd = L.d;
                 se = L.e;
                 sS = L.S;
-                sn = -face_normal<R>(hit.face);
-                sni = P.n_int;
-                snt = P.n_ext;
+                sn = -n;
+                media = &P.leave;
             }
         }
         if (do_split) {
-            const Interface<R> sp = split(sd, se, sS, sn, sni, snt);
+            const Interface<R> sp = split(sd, se, sS, sn, *media);
             A.max_iface = fmax(A.max_iface, (double)sp.balance);
             // entry: exterior reflection exits, transmission continues;
             // internal: transmission exits, reflection continues
-            const R epow = fresh ? sp.r.I : (sp.has_t ? sp.t.I : R(0));
-            if (epow > R(0)) {
-                has = true;
-                od = fresh ? sp.dr : sp.dt;
-                opow = epow;
-                L.esc += opow;
+            unsigned long long cont_fx = 0ull;
+            if constexpr (sizeof(R) == 4) {
+                // the reflected share is rounded once, the transmitted share is the exact rest
+                const unsigned long long rq = to_fix(sp.r.I);
+                const unsigned long long rfx = (sp.tir || rq > L.pfx) ? L.pfx : rq;
+                const unsigned long long tfx = L.pfx - rfx;
+                efx = fresh ? rfx : tfx;
+                cont_fx = fresh ? tfx : rfx;
+                if (efx) {
+                    has = true;
+                    od = fresh ? sp.dr : sp.dt;
+                    opow = (R)efx * R(kFixUnit);
+                    L.escfx += efx;
+                }
+            } else {
+                const R epow = fresh ? sp.r.I : (sp.has_t ? sp.t.I : R(0));
+                if (epow > R(0)) {
+                    has = true;
+                    od = fresh ? sp.dr : sp.dt;
+                    opow = epow;
+                    efx = to_fix(epow);
+                    L.esc += opow;
+                }
             }
             if (fresh && !sp.has_t) {
-                finish_ray(P, L, A, s_status, 0, R(0));
+                finish_ray<R>(P, L, A, s_status, 0, 0ull, R(0));
             } else {
                 L.d = fresh ? sp.dt : sp.dr;
                 L.e = sp.s;
                 L.S = fresh ? sp.t : sp.r;
-                settle(P, L, A, s_status);
+                if constexpr (sizeof(R) == 4) {
+                    L.pfx = cont_fx;
+                    L.S.I = (R)cont_fx * R(kFixUnit);
+                }
+                settle<R>(P, L, A, s_status);
             }
         }
 
@@ -356,7 +476,7 @@ __global__ void __launch_bounds__(256) hex_trace_bin_kernel(const HexParams<R> P
             if (!b.valid) {
                 A.invalid += 1;
             } else {
-                v = to_fix(opow);
+                v = efx;
                 A.esc_fx += v;
                 A.outputs += 1;
                 A.snapped += b.snapped ? 1ull : 0ull;
@@ -384,12 +504,12 @@ __global__ void __launch_bounds__(256) hex_trace_bin_kernel(const HexParams<R> P
     // ---- block epilogue: flush the table and the lane accumulators
     __syncthreads();
     hist_flush(H, P.mass, P.to_mass);
-    DevStats* G = P.stats;
+    DevStats* Gs = P.stats;
     // Per-warp sums stay below 2^60 (a warp slice holds at most 2^16 rays of power <= 1).
-    unsigned long long w[12] = {A.esc_fx, A.unres_fx, A.fwd_fx, A.bwd_fx, A.rays, A.outputs, A.rejected,
-                                A.snapped, A.near_edge, A.fallback, A.invalid, A.encounters};
+    unsigned long long w[13] = {A.esc_fx, A.unres_fx, A.fwd_fx, A.bwd_fx, A.rays, A.outputs, A.rejected,
+                                A.snapped, A.near_edge, A.fallback, A.invalid, A.encounters, A.missed};
 #pragma unroll
-    for (int q = 0; q < 12; ++q)
+    for (int q = 0; q < 13; ++q)
         for (int o = 16; o; o >>= 1) w[q] += __shfl_xor_sync(kFull, w[q], o);
     double ax = A.axial, mb = A.max_bal, mi = A.max_iface;
     for (int o = 16; o; o >>= 1) {
@@ -398,21 +518,21 @@ __global__ void __launch_bounds__(256) hex_trace_bin_kernel(const HexParams<R> P
         mi = fmax(mi, __shfl_xor_sync(kFull, mi, o));
     }
     if (lane == 0) {
-        add128(G->esc, w[0]);
-        add128(G->unres, w[1]);
-        add128(G->fwd, w[2]);
-        add128(G->bwd, w[3]);
-        unsigned long long* counters[8] = {&G->rays, &G->outputs, &G->rejected, &G->snapped,
-                                           &G->near_edge, &G->fallback, &G->invalid, &G->encounters};
+        add128(Gs->esc, w[0]);
+        add128(Gs->unres, w[1]);
+        add128(Gs->fwd, w[2]);
+        add128(Gs->bwd, w[3]);
+        unsigned long long* counters[9] = {&Gs->rays, &Gs->outputs, &Gs->rejected, &Gs->snapped,
+                                           &Gs->near_edge, &Gs->fallback, &Gs->invalid, &Gs->encounters, &Gs->missed};
 #pragma unroll
-        for (int q = 0; q < 8; ++q)
+        for (int q = 0; q < 9; ++q)
             if (w[4 + q]) atomicAdd(counters[q], w[4 + q]);
-        if (ax != 0.0) atomicAdd(&G->axial, ax);
-        atomicMax(&G->max_bal_bits, (unsigned long long)__double_as_longlong(mb));
-        atomicMax(&G->max_iface_bits, (unsigned long long)__double_as_longlong(mi));
+        if (ax != 0.0) atomicAdd(&Gs->axial, ax);
+        atomicMax(&Gs->max_bal_bits, (unsigned long long)__double_as_longlong(mb));
+        atomicMax(&Gs->max_iface_bits, (unsigned long long)__double_as_longlong(mi));
     }
     __syncthreads();
-    if (threadIdx.x < 8 && s_status[threadIdx.x]) atomicAdd(&G->status[threadIdx.x], (unsigned long long)s_status[threadIdx.x]);
+    if (threadIdx.x < 8 && s_status[threadIdx.x]) atomicAdd(&Gs->status[threadIdx.x], (unsigned long long)s_status[threadIdx.x]);
 }
 
 } // namespace icp

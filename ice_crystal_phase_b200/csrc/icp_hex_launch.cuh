@@ -1,6 +1,8 @@
-// icp_hex_launch.cuh -- host launcher for the hex trace+bin kernel, instantiated once per
-// arithmetic type in icp_hex_f32.cu / icp_hex_f64.cu.
+// icp_hex_launch.cuh -- host launcher for the trace+bin kernel, instantiated once per
+// arithmetic type and geometry in icp_hex_f32.cu / icp_hex_f64.cu / icp_drop_f32.cu / icp_drop_f64.cu.
 #pragma once
+#include <cmath>
+
 #include "icp_hex_kernel.cuh"
 #include "icp_internal.h"
 
@@ -8,25 +10,21 @@ namespace icp {
 
 constexpr uint32_t kEdgeSmemMax = 4097; // stage u edges in shared memory up to this many
 
-template <class R> size_t hex_smem_bytes(uint32_t hash_slots, uint32_t nt)
+template <class R> size_t trace_smem_bytes(uint32_t hash_slots, uint32_t nt)
 {
     size_t b = (size_t)hash_slots * (8 + 4) + 8 * 4;
     if (nt + 1 <= kEdgeSmemMax) b += sizeof(R) * (nt + 1);
     return b;
 }
 
-template <class R> HexParams<R> make_hex_params(const HexLaunch& L)
+template <class R, class G> void fill_common(TraceParams<R, G>& P, const HexLaunch& L)
 {
-    HexParams<R> P;
-    P.half_len = (R)L.half_len;
     P.k = v3((R)L.k[0], (R)L.k[1], (R)L.k[2]);
     P.ke0 = v3((R)L.ke0[0], (R)L.ke0[1], (R)L.ke0[2]);
-    for (int f = 0; f < 8; ++f) P.cum[f] = (R)L.cum[f];
-    P.face_mask = L.face_mask;
-    P.area = (R)L.area;
-    P.n_ext = (R)L.n_ext;
-    P.n_int = (R)L.n_int;
+    P.enter = make_media<R>(L.n_ext, L.n_int);
+    P.leave = make_media<R>(L.n_int, L.n_ext);
     P.tail = (R)L.tail;
+    P.tail_fx = (unsigned long long)std::floor(L.tail * 0x1p44);
     P.bal_tol = (R)L.bal_tol;
     P.seed = L.seed;
     P.total = L.total;
@@ -37,7 +35,7 @@ template <class R> HexParams<R> make_hex_params(const HexLaunch& L)
     P.batch_out = L.batch_out;
     // FP32 fused transform rows: (e0, e1, ki)^T * rotation
     const double* r = L.rot; // column c = r[3c..3c+2]
-    const double* rows[3] = {L.e0, L.e1, L.ki};
+    const double* rows[3] = {L.e0, L.e1g, L.ki};
     for (int a = 0; a < 3; ++a)
         for (int c = 0; c < 3; ++c)
             P.gf.m[3 * a + c] = (float)(rows[a][0] * r[3 * c] + rows[a][1] * r[3 * c + 1] + rows[a][2] * r[3 * c + 2]);
@@ -49,7 +47,7 @@ template <class R> HexParams<R> make_hex_params(const HexLaunch& L)
     for (int i = 0; i < 3; ++i) {
         P.gd.ki[i] = L.ki[i];
         P.gd.e0[i] = L.e0[i];
-        P.gd.e1[i] = L.e1[i];
+        P.gd.e1[i] = L.e1g[i];
     }
     P.gd.edges = L.edges_d;
     P.gd.nt = L.nt;
@@ -61,25 +59,48 @@ template <class R> HexParams<R> make_hex_params(const HexLaunch& L)
     P.stats = reinterpret_cast<DevStats*>(L.stats);
     P.hash_slots = L.hash_slots;
     P.smem_edges = (L.nt + 1 <= kEdgeSmemMax) ? 1u : 0u;
+}
+
+template <class R> TraceParams<R, HexGeo<R>> make_hex_params(const HexLaunch& L)
+{
+    TraceParams<R, HexGeo<R>> P;
+    fill_common(P, L);
+    P.geo.half_len = (R)L.half_len;
+    for (int f = 0; f < 8; ++f) P.geo.cum[f] = (R)L.cum[f];
+    P.geo.face_mask = L.face_mask;
+    P.geo.area = (R)L.area;
     return P;
 }
 
-template <class R> int launch_hex(const HexLaunch& L, cudaStream_t stream)
+template <class R> TraceParams<R, DropGeo<R>> make_drop_params(const HexLaunch& L)
 {
-    const HexParams<R> P = make_hex_params<R>(L);
-    const size_t smem = hex_smem_bytes<R>(L.hash_slots, L.nt);
-    cudaError_t e = cudaFuncSetAttribute(hex_trace_bin_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    TraceParams<R, DropGeo<R>> P;
+    fill_common(P, L);
+    for (int n = 0; n < 8; ++n) P.geo.shape.c[n] = (R)L.coeff[n];
+    P.geo.shape.r_out = (R)L.r_out;
+    P.geo.shape.r_center = (R)L.r_center;
+    P.geo.shape.sphere = L.sphere != 0;
+    P.geo.disk = (R)L.disk;
+    P.geo.back = (R)L.back;
+    P.geo.e1 = v3((R)L.e1[0], (R)L.e1[1], (R)L.e1[2]);
+    return P;
+}
+
+template <class R, class G> int launch_trace(const TraceParams<R, G>& P, const HexLaunch& L, cudaStream_t stream)
+{
+    const size_t smem = trace_smem_bytes<R>(L.hash_slots, L.nt);
+    cudaError_t e = cudaFuncSetAttribute(trace_bin_kernel<R, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return (int)e;
-    hex_trace_bin_kernel<R><<<L.blocks, L.block_threads, smem, stream>>>(P);
+    trace_bin_kernel<R, G><<<L.blocks, L.block_threads, smem, stream>>>(P);
     return (int)cudaGetLastError();
 }
 
-template <class R> int hex_blocks_per_sm(uint32_t hash_slots, uint32_t nt, uint32_t threads)
+template <class R, class G> int trace_blocks_per_sm(uint32_t hash_slots, uint32_t nt, uint32_t threads)
 {
-    const size_t smem = hex_smem_bytes<R>(hash_slots, nt);
-    cudaFuncSetAttribute(hex_trace_bin_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const size_t smem = trace_smem_bytes<R>(hash_slots, nt);
+    cudaFuncSetAttribute(trace_bin_kernel<R, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hex_trace_bin_kernel<R>, (int)threads, smem) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_bin_kernel<R, G>, (int)threads, smem) != cudaSuccess)
         return 0;
     return per_sm;
 }

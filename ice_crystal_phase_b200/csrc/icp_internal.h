@@ -33,21 +33,30 @@ size_t cdf_partial_bytes();
 // Sets the calling thread's message returned by icp_last_error().
 void set_last_error(const char* message);
 
-// Host-side description of one hex trace+bin launch (double precision inputs; the
-// launcher converts to the kernel's arithmetic type).
+// Host-side description of one trace+bin launch (double precision inputs; the launcher
+// converts to the kernel's arithmetic type).  geometry: 0 = hexagonal prism, 1 = drop.
 struct HexLaunch {
+    uint32_t geometry;
+    // prism (units of the circumradius)
     double half_len;
-    double k[3], ke0[3];
     double cum[8];
     uint32_t face_mask;
     double area;
+    // drop (units of the equal-volume radius)
+    double coeff[8];
+    double r_out, r_center;
+    uint32_t sphere;
+    double disk, back;
+    double e1[3];
+    // common
+    double k[3], ke0[3];
     double n_ext, n_int, tail, bal_tol;
     uint64_t seed, total, first, count;
     uint32_t max_hits, batch_size;
     uint32_t* batch_out;
     // grid transforms
     double rot[9];      // column-major body -> ensemble
-    double ki[3], e0[3], e1[3];
+    double ki[3], e0[3], e1g[3];
     uint32_t nt, np;
     const double* edges_d;
     const float* edges_f;
@@ -62,7 +71,11 @@ struct HexLaunch {
 size_t hex_stats_bytes();
 int launch_hex_f32(const HexLaunch& L, cudaStream_t stream);
 int launch_hex_f64(const HexLaunch& L, cudaStream_t stream);
-// Largest number of resident blocks for the chosen configuration.
-int hex_max_blocks(int precision, uint32_t hash_slots, uint32_t nt, uint32_t block_threads, int device);
+int launch_drop_f32(const HexLaunch& L, cudaStream_t stream);
+int launch_drop_f64(const HexLaunch& L, cudaStream_t stream);
+int hex_blocks_per_sm_f32(uint32_t slots, uint32_t nt, uint32_t threads);
+int hex_blocks_per_sm_f64(uint32_t slots, uint32_t nt, uint32_t threads);
+int drop_blocks_per_sm_f32(uint32_t slots, uint32_t nt, uint32_t threads);
+int drop_blocks_per_sm_f64(uint32_t slots, uint32_t nt, uint32_t threads);
 
 } // namespace icp

@@ -106,6 +106,7 @@ typedef struct {
     uint64_t max_batch_outputs; /* largest number of exits produced by one batch of rays    */
     uint64_t invalid;        /* exits that could not be binned (non-finite direction)       */
     uint64_t encounters;     /* internal boundary interactions traced                       */
+    uint64_t missed;         /* sampled rays that miss the particle (drops; never prisms)   */
 } icp_trace_stats;
 
 /* Histogram privatisation / launch tuning (all zero = autotuned defaults). */

@@ -4,7 +4,8 @@ FP64 path: cell masses within the reference's own GPU-vs-CPU histogram tolerance
 (2e-11 relative, hex_phase/tests/phase_cuda_tests.cpp:70-107), identical ray and exit
 counts and status histograms, energy balance to 1e-12.
 FP32 path (north-star fast path): total-variation distance of normalised cell mass
-<= 1e-3 against the same-seed FP64 oracle, energy balance to 1e-6.
+<= 1e-3 against the same-seed FP64 oracle; power is carried in exact fixed point, so the
+energy balance holds to binary64 rounding (1e-12) as in the reference's CLI test.
 """
 from __future__ import annotations
 
@@ -72,7 +73,9 @@ def test_fp32_tv_against_oracle(ctx, icp, oracle, hash_slots):
     tv = _tv(acc.masses(), rec.masses)
     assert tv <= 1e-3, tv
     area = rec.expected_area
-    assert abs((acc.escaped_area + acc.unresolved_area) / area - 1) <= 1e-6
+    # binary32 physics, exact fixed-point power bookkeeping: energy balance to binary64 rounding
+    assert abs((acc.escaped_area + acc.unresolved_area) / area - 1) <= 1e-12
+    assert acc.stats.max_ray_balance == 0.0
     assert abs(acc.escaped_area / rec.escaped_area - 1) <= 1e-5
     assert acc.stats.rays == n
 
@@ -82,7 +85,7 @@ def test_fp32_two_orientations(ctx, icp, oracle):
     acc = _accumulate(ctx, icp, plan, 0.1, 0.2, (1, -0.4, 0.3), 1.31, 72, 144, icp.ICP_FP32)
     g = np.load(GOLDEN / "hex_two_orientations.npz")
     assert _tv(acc.masses(), g["masses"]) <= 1e-3
-    assert abs((acc.escaped_area + acc.unresolved_area) / g["stats"][4] - 1) <= 1e-6
+    assert abs((acc.escaped_area + acc.unresolved_area) / g["stats"][4] - 1) <= 1e-12
 
 
 def test_record_entry_fp64_matches_oracle_record(ctx, icp, oracle):
@@ -137,7 +140,7 @@ def test_fp32_full_size_energy(ctx, icp):
     plan = icp.parse_orientation_plan("qw,qx,qy,qz,weight,samples,seed\n1,0,0,0,1,10000000,12345\n")
     out = icp.generate_hex_record(ctx, 0.05, 0.2, CFG3_KI, 1.31, 512, 1024, plan, max_internal_hits=12)
     rep = out.report
-    assert abs((rep.escaped_area_mm2 + rep.unresolved_area_mm2) / rep.expected_area_mm2 - 1) <= 1e-6
+    assert abs((rep.escaped_area_mm2 + rep.unresolved_area_mm2) / rep.expected_area_mm2 - 1) <= 1e-12
     assert rep.histogram_relative_error <= 1e-10
     assert rep.trace.rays == 10_000_000 and rep.trace.invalid == 0
     assert np.all(np.diff(out.theta, axis=1) >= 0) and abs(rep.cdf.cdf_mass - 1) <= 1e-10
