@@ -12,6 +12,13 @@ Mirrored reference interfaces (Somatic-Cell/ice-crystal-phase):
     (.add fused with HexPrismTracer.trace, hex_trace/include/ice_crystal/hex_trace_cuda.hpp:18-41)
   PhaseCdf.build                   include/rainbow/phase_cdf.hpp:50-96
   generate_hex_record              hex_phase/apps/generate_hex_phase.cpp:79-154 (CUDA branch)
+  evaluate_water_optics            include/rainbow/water_refractive_index.hpp:22-33
+  RaindropShape.make               include/rainbow/raindrop_shape.hpp:22-67
+  compute_projected_area           include/rainbow/projected_area.hpp:31-35
+  drop_frame                       apps/generate_phase.cpp:209-217, 242-245
+  PhaseMassAccumulatorCuda.add_drop  RaindropTracer::trace_unpolarized + patch stages, replaced by
+                                   direct binning (include/rainbow/raindrop_tracer.hpp:32-36)
+  generate_drop_record             apps/generate_phase.cpp:395-453 (rainbow_generate's record path)
 """
 from __future__ import annotations
 
@@ -125,6 +132,26 @@ class RecordReport(C.Structure):
                 ("seconds_cdf", C.c_double)]
 
 
+class DropRecordArgs(C.Structure):
+    _fields_ = [("radius_mm", C.c_double), ("coefficients", C.c_double * 8), ("inclination_deg", C.c_double),
+                ("exterior_index", C.c_double), ("interior_index", C.c_double), ("wavelength_nm", C.c_double),
+                ("tail_tolerance", C.c_double), ("balance_tolerance", C.c_double), ("nt", C.c_uint32),
+                ("np", C.c_uint32), ("ct", C.c_uint32), ("cp", C.c_uint32), ("max_internal_hits", C.c_uint32),
+                ("precision", C.c_uint32), ("rays", C.c_uint64), ("seed", C.c_uint64), ("diffraction", C.c_uint32),
+                ("reserved", C.c_uint32), ("policy", CdfPolicy), ("tuning", Tuning)]
+
+
+class DropReport(C.Structure):
+    _fields_ = [("trace", TraceStats), ("projected_area_mm2", C.c_double), ("sampled_area_mm2", C.c_double),
+                ("incident_area_mm2", C.c_double), ("escaped_area_mm2", C.c_double),
+                ("unresolved_area_mm2", C.c_double), ("diffraction_area_mm2", C.c_double),
+                ("forward_mass_mm2", C.c_double), ("backward_mass_mm2", C.c_double),
+                ("histogram_mass_mm2", C.c_double), ("point_axial_mm2", C.c_double),
+                ("histogram_relative_error", C.c_double), ("ki", C.c_double * 3), ("e0", C.c_double * 3),
+                ("e1", C.c_double * 3), ("cdf", CdfReport), ("seconds_trace", C.c_double),
+                ("seconds_cdf", C.c_double)]
+
+
 # ---------------------------------------------------------------- library loading
 _P = C.c_void_p
 _D = C.POINTER(C.c_double)
@@ -149,6 +176,18 @@ _FUNCS = {
                                       C.c_uint32, C.POINTER(CdfPolicy), _P, _P, C.POINTER(CdfReport)]),
     "icp_hex_generate": (C.c_int, [_P, C.POINTER(HexRecordArgs), C.POINTER(Orientation), C.c_uint32, _D, _D, _D,
                                    C.POINTER(RecordReport)]),
+    "icp_phase_cdf_build_static": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_double, C.c_double,
+                                             C.c_uint32, C.c_uint32, C.POINTER(CdfPolicy), _P, _P,
+                                             C.POINTER(CdfReport)]),
+    "icp_water_index": (C.c_int, [C.c_double, C.c_double, C.c_double, _D, _D]),
+    "icp_drop_shape": (C.c_int, [C.c_double, C.c_int, _D, _D, _D]),
+    "icp_drop_projected_area": (C.c_int, [_D, C.c_double, _D, _D]),
+    "icp_drop_frame": (C.c_int, [C.c_double, _D, _D, _D]),
+    "icp_drop_diffraction_rows": (C.c_int, [_D, C.c_uint32, C.c_double, C.c_double, _D]),
+    "icp_drop_sampling_area": (C.c_int, [_D, C.c_double, _D]),
+    "icp_drop_trace_bin": (C.c_int, [_P, C.POINTER(DropRecordArgs), C.c_uint64, C.c_uint64, C.c_double,
+                                     C.POINTER(Grid), _P, _P, C.POINTER(TraceStats)]),
+    "icp_drop_generate": (C.c_int, [_P, C.POINTER(DropRecordArgs), _D, _D, _D, C.POINTER(DropReport)]),
 }
 
 
@@ -520,3 +559,163 @@ def generate_hex_record(ctx: Context, circumradius_mm: float, length_mm: float, 
     check(LIB.icp_hex_generate(ctx.handle, C.byref(r), nodes, len(plan.nodes), phi.ctypes.data_as(_D),
                                theta.ctypes.data_as(_D), u.ctypes.data_as(_D), C.byref(rep)))
     return HexRecordResult(phi, theta.reshape(cp, ct + 1), u, rep, make_phase_grid(nt, np_, ki))
+
+
+
+# ---------------------------------------------------------------- water drops
+@dataclass
+class WaterOpticalState:
+    refractive_index: float
+    density_kg_m3: float
+    temperature_kelvin: float
+    pressure_pascal: float
+
+
+def evaluate_water_optics(vacuum_wavelength_nm: float, temperature_celsius: float = 20.0,
+                          pressure_pascal: float = 101325.0) -> WaterOpticalState:
+    """IAPWS R9-97 real index of liquid water; bounded to 200..1100 nm, 0..60 C, 50 kPa..100 MPa."""
+    n, rho = C.c_double(), C.c_double()
+    check(LIB.icp_water_index(vacuum_wavelength_nm, temperature_celsius, pressure_pascal, C.byref(n), C.byref(rho)))
+    return WaterOpticalState(n.value, rho.value, temperature_celsius + 273.15, pressure_pascal)
+
+
+@dataclass
+class RaindropShape:
+    """r/a = 1 + sum_n coefficients[n] cos(n chi), chi from the particle's -y axis."""
+    coefficients: list
+    inner_radius: float
+    outer_radius: float
+
+    @staticmethod
+    def make(radius_mm: float, sphere: bool = False) -> "RaindropShape":
+        c = (C.c_double * 8)()
+        lo, hi = C.c_double(), C.c_double()
+        check(LIB.icp_drop_shape(radius_mm, int(sphere), c, C.byref(lo), C.byref(hi)))
+        return RaindropShape(list(c), lo.value, hi.value)
+
+
+def _c8(coefficients) -> C.Array:
+    c = [float(x) for x in coefficients]
+    if len(c) > 8:
+        raise ValueError("At most eight shape coefficients.")
+    return (C.c_double * 8)(*(c + [0.0] * (8 - len(c))))
+
+
+def compute_projected_area(coefficients, radius_mm: float, incident_propagation) -> float:
+    """Projected area (mm^2) of the convex drop along the incident direction, binary64 on the CPU."""
+    k = (C.c_double * 3)(*map(float, incident_propagation))
+    a = C.c_double()
+    check(LIB.icp_drop_projected_area(_c8(coefficients), radius_mm, k, C.byref(a)))
+    return a.value
+
+
+def drop_frame(inclination_deg: float) -> tuple[list, list, list]:
+    """ki = (cos a, -sin a, 0) and the frame of the stored CDF (sampling_frame_columns)."""
+    k, e0, e1 = (C.c_double * 3)(), (C.c_double * 3)(), (C.c_double * 3)()
+    check(LIB.icp_drop_frame(inclination_deg, k, e0, e1))
+    return list(k), list(e0), list(e1)
+
+
+def make_drop_grid(nt: int, np_: int, inclination_deg: float) -> PhaseGrid:
+    if not nt or not np_ or nt * np_ > 0xFFFFFFFF:
+        raise ValueError("Unsupported phase grid dimensions.")
+    k, e0, e1 = drop_frame(inclination_deg)
+    return PhaseGrid(nt, np_, k, e0, e1, u_edges(nt))
+
+
+def sampling_area(coefficients, radius_mm: float) -> float:
+    a = C.c_double()
+    check(LIB.icp_drop_sampling_area(_c8(coefficients), radius_mm, C.byref(a)))
+    return a.value
+
+
+def diffraction_rows(edges: np.ndarray, area_mm2: float, wavelength_nm: float) -> np.ndarray:
+    e = np.ascontiguousarray(edges, dtype=np.float64)
+    rows = np.empty(e.size - 1)
+    check(LIB.icp_drop_diffraction_rows(e.ctypes.data_as(_D), e.size - 1, area_mm2, wavelength_nm,
+                                        rows.ctypes.data_as(_D)))
+    return rows
+
+
+def _drop_args(coefficients, radius_mm, inclination_deg, interior_index, rays, seed, nt, np_, ct, cp,
+               exterior_index, max_internal_hits, tail_tolerance, precision, balance_tolerance, wavelength_nm,
+               diffraction, max_l1_error=1e-10, max_lost_mass=1e-12, max_coarsening_tv=1.0, tuning=None):
+    r = DropRecordArgs()
+    r.radius_mm = radius_mm
+    r.coefficients = _c8(coefficients)
+    r.inclination_deg = inclination_deg
+    r.exterior_index, r.interior_index, r.wavelength_nm = exterior_index, interior_index, wavelength_nm
+    r.tail_tolerance = tail_tolerance
+    r.balance_tolerance = 1e-10 if balance_tolerance is None else balance_tolerance
+    r.nt, r.np, r.ct, r.cp = nt, np_, ct, cp
+    r.max_internal_hits, r.precision = max_internal_hits, precision
+    r.rays, r.seed, r.diffraction = rays, seed, int(bool(diffraction))
+    r.policy = CdfPolicy(max_l1_error, max_lost_mass, max_coarsening_tv)
+    if tuning:
+        r.tuning = tuning
+    return r
+
+
+def _add_drop(self, coefficients, radius_mm: float, interior_index: float, rays: int, seed: int,
+              inclination_deg: float, exterior_index: float = 1.0, max_internal_hits: int = 1024,
+              tail_tolerance: float = 1e-12, precision: int = ICP_FP32, first: int = 0, count: int | None = None,
+              tuning: Tuning | None = None, balance_tolerance: float | None = None) -> TraceStats:
+    """Traces rays [first, first+count) of one drop (sampled on its bounding disk) into the
+    histogram; the grid must be the drop frame's (make_drop_grid)."""
+    r = _drop_args(coefficients, radius_mm, inclination_deg, interior_index, rays, seed, self.grid.nt, self.grid.np,
+                   self.grid.nt, self.grid.np, exterior_index, max_internal_hits, tail_tolerance, precision,
+                   balance_tolerance, 0.0, False, tuning=tuning)
+    weight = sampling_area(coefficients, radius_mm) / float(rays)
+    g = self.grid.abi()
+    s = TraceStats()
+    count = rays - first if count is None else count
+    check(LIB.icp_drop_trace_bin(self.ctx.handle, C.byref(r), first, count, weight, C.byref(g), self.edges.ptr,
+                                 self.mass.ptr, C.byref(s)))
+    self.forward += weight * s.forward_pole
+    self.backward += weight * s.backward_pole
+    self.escaped_area += weight * s.escaped
+    self.unresolved_area += weight * s.unresolved
+    self.point_axial += weight * s.point_axial
+    self.incident_area = getattr(self, "incident_area", 0.0) + weight * (s.rays - s.missed)
+    for k, _ in TraceStats._fields_:
+        if k == "status_counts":
+            for i in range(8):
+                self.stats.status_counts[i] += s.status_counts[i]
+        elif k.startswith("max_"):
+            setattr(self.stats, k, max(getattr(self.stats, k), getattr(s, k)))
+        else:
+            setattr(self.stats, k, getattr(self.stats, k) + getattr(s, k))
+    return s
+
+
+PhaseMassAccumulatorCuda.add_drop = _add_drop
+
+
+@dataclass
+class DropRecordResult:
+    phi: np.ndarray
+    theta: np.ndarray
+    u_edges: np.ndarray
+    report: DropReport
+    grid: PhaseGrid
+
+
+def generate_drop_record(ctx: Context, coefficients, radius_mm: float, interior_index: float, nt: int, np_: int,
+                         rays: int, seed: int = 12345, inclination_deg: float = 20.0, ct: int | None = None,
+                         cp: int | None = None, exterior_index: float = 1.0, max_internal_hits: int = 1024,
+                         tail_tolerance: float = 1e-12, precision: int = ICP_FP32, wavelength_nm: float = 0.0,
+                         diffraction: bool = False, balance_tolerance: float | None = None,
+                         max_l1_error: float = 1e-10, max_lost_mass: float = 1e-12, max_coarsening_tv: float = 1.0,
+                         tuning: Tuning | None = None) -> DropRecordResult:
+    """One drop record through the host-buffer C-ABI entry (icp_drop_generate)."""
+    ct, cp = ct or nt, cp or np_
+    r = _drop_args(coefficients, radius_mm, inclination_deg, interior_index, rays, seed, nt, np_, ct, cp,
+                   exterior_index, max_internal_hits, tail_tolerance, precision, balance_tolerance, wavelength_nm,
+                   diffraction, max_l1_error, max_lost_mass, max_coarsening_tv, tuning)
+    phi = np.empty(cp + 1)
+    theta = np.empty(cp * (ct + 1))
+    u = np.empty(ct + 1)
+    rep = DropReport()
+    check(LIB.icp_drop_generate(ctx.handle, C.byref(r), phi.ctypes.data_as(_D), theta.ctypes.data_as(_D),
+                                u.ctypes.data_as(_D), C.byref(rep)))
+    return DropRecordResult(phi, theta.reshape(cp, ct + 1), u, rep, make_drop_grid(nt, np_, inclination_deg))

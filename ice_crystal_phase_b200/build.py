@@ -45,7 +45,7 @@ UNITS = {
     "icp_cdf_static.cu": ["-fmad=false"],
 }
 
-HOST_SOURCES = ["icp_record_io.cpp", "icp_projected_area.cpp", "icp_water.cpp"]
+HOST_SOURCES = ["icp_record_io.cpp"]
 APP_SOURCES = {"ice_generate_phase": "ice_generate_phase.cpp", "rainbow_generate": "rainbow_generate.cpp"}
 
 

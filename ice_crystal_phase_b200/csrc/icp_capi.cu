@@ -53,28 +53,6 @@ int ok()
                         __LINE__);                                                                      \
     } while (0)
 
-// Device buffer that grows on demand and is reused across calls.
-struct Scratch {
-    void* ptr = nullptr;
-    size_t bytes = 0;
-    cudaError_t ensure(size_t n)
-    {
-        if (n <= bytes) return cudaSuccess;
-        if (ptr) cudaFree(ptr);
-        ptr = nullptr;
-        bytes = 0;
-        const cudaError_t e = cudaMalloc(&ptr, n);
-        if (e == cudaSuccess) bytes = n;
-        return e;
-    }
-    void release()
-    {
-        if (ptr) cudaFree(ptr);
-        ptr = nullptr;
-        bytes = 0;
-    }
-};
-
 __global__ void edges_to_float(const double* in, float* out, uint32_t n)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -85,16 +63,8 @@ __global__ void edges_to_float(const double* in, float* out, uint32_t n)
 
 namespace icp {
 void set_last_error(const char* message) { g_error = message; }
+void count_launch() { ++g_launches; }
 } // namespace icp
-
-struct icp_context {
-    int device = 0;
-    int sms = 0;
-    cudaStream_t stream = nullptr;
-    Scratch stats, edges_f, cdf_partial, cdf_report, cdf_sync, cdf_colsum;
-    Scratch rec_edges, rec_mass, rec_phi, rec_theta, rec_batch;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-};
 
 extern "C" {
 
@@ -146,7 +116,7 @@ int icp_context_destroy(icp_context* c)
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     Scratch* all[] = {&c->stats, &c->edges_f, &c->cdf_partial, &c->cdf_report, &c->cdf_sync, &c->cdf_colsum,
-                      &c->rec_edges, &c->rec_mass, &c->rec_phi, &c->rec_theta, &c->rec_batch};
+                      &c->rec_edges, &c->rec_mass, &c->rec_phi, &c->rec_theta, &c->rec_batch, &c->rows};
     for (Scratch* s : all) s->release();
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -259,9 +229,7 @@ extern "C" int icp_hex_node_area(const icp_hex_node* node, const icp_grid* grid,
     return ok();
 }
 
-namespace {
-
-int ensure_float_edges(icp_context* c, const double* d_edges, uint32_t nt)
+int icp::ensure_float_edges(icp_context* c, const double* d_edges, uint32_t nt)
 {
     ICP_CUDA(c->edges_f.ensure(sizeof(float) * (nt + 1)));
     edges_to_float<<<(nt + 1 + 255) / 256, 256, 0, c->stream>>>(d_edges, (float*)c->edges_f.ptr, nt + 1);
@@ -270,7 +238,7 @@ int ensure_float_edges(icp_context* c, const double* d_edges, uint32_t nt)
     return ICP_OK;
 }
 
-void stats_accumulate(const unsigned char* raw, icp_trace_stats* out)
+void icp::stats_accumulate(const unsigned char* raw, icp_trace_stats* out)
 {
     // DevStats layout (icp_hex_kernel.cuh)
     struct Raw {
@@ -303,6 +271,8 @@ void stats_accumulate(const unsigned char* raw, icp_trace_stats* out)
     out->encounters += r.encounters;
     out->missed += r.missed;
 }
+
+namespace {
 
 __global__ void max_u32(const uint32_t* v, uint64_t n, unsigned long long* out)
 {

@@ -4,6 +4,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "../../include/icp_b200.h"
+
 namespace icp {
 
 // Final audit written by the last block of the CDF kernel.
@@ -78,4 +80,47 @@ int hex_blocks_per_sm_f64(uint32_t slots, uint32_t nt, uint32_t threads);
 int drop_blocks_per_sm_f32(uint32_t slots, uint32_t nt, uint32_t threads);
 int drop_blocks_per_sm_f64(uint32_t slots, uint32_t nt, uint32_t threads);
 
+// Device buffer that grows on demand and is reused across calls.
+struct Scratch {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t n)
+    {
+        if (n <= bytes) return cudaSuccess;
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        const cudaError_t e = cudaMalloc(&ptr, n);
+        if (e == cudaSuccess) bytes = n;
+        return e;
+    }
+    void release()
+    {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
+
+// Launch counter shared by the ABI files (icp_kernel_launches).
+void count_launch();
+
 } // namespace icp
+
+struct icp_context;
+namespace icp {
+// FP32 copy of the u edges in the context scratch (one small kernel).
+int ensure_float_edges(icp_context* c, const double* d_edges, uint32_t nt);
+// Adds one launch's device statistics (DevStats bytes) into the public stats struct.
+void stats_accumulate(const unsigned char* raw, icp_trace_stats* out);
+} // namespace icp
+
+// One CUDA device, one non-blocking stream, reusable scratch.
+struct icp_context {
+    int device = 0;
+    int sms = 0;
+    cudaStream_t stream = nullptr;
+    icp::Scratch stats, edges_f, cdf_partial, cdf_report, cdf_sync, cdf_colsum;
+    icp::Scratch rec_edges, rec_mass, rec_phi, rec_theta, rec_batch, rows;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};

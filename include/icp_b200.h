@@ -234,6 +234,71 @@ int icp_hex_generate(icp_context* ctx, const icp_hex_record* record, const icp_o
                      uint32_t node_count, double* h_phi, double* h_theta, double* h_u,
                      icp_record_report* report);
 
+/* ------------------------------------------------------------ water drops */
+/* Host helpers for the drop record inputs (all binary64, CPU):
+ *  icp_water_index      IAPWS R9-97 index at the drop's wavelength / temperature / pressure
+ *                       (replaces evaluate_water_optics, src/water_refractive_index.cpp:157-187;
+ *                       liquid density from Kell's correlation)
+ *  icp_drop_shape       Table-I coefficients for an equal-volume radius
+ *                       (RaindropShape::try_make, include/rainbow/raindrop_shape.hpp:22-67)
+ *  icp_drop_projected_area  convex-surface projected area (compute_projected_area,
+ *                       src/projected_area.cpp:163-229)
+ *  icp_drop_frame       ki = (cos a, -sin a, 0) and its transverse frame (RaindropSettings,
+ *                       include/rainbow/raindrop_settings.hpp:123-147) */
+int icp_water_index(double wavelength_nm, double temperature_c, double pressure_pa, double* index, double* density);
+int icp_drop_shape(double radius_mm, int sphere, double coefficients[8], double* inner_radius, double* outer_radius);
+int icp_drop_projected_area(const double coefficients[8], double radius_mm, const double k[3], double* area_mm2);
+int icp_drop_frame(double inclination_deg, double k[3], double e0[3], double e1[3]);
+/* Analytic diffraction stage (no reference counterpart; the reference's "diffraction" stage is
+ * a Table-II blur at rainbow transitions, include/rainbow/rainbow_diffraction.hpp:16-28):
+ * Fraunhofer diffraction of the circle of equal projected area, rows[i] = power (mm^2) between
+ * u_edges[i] and u_edges[i+1] from Rayleigh's encircled energy 1 - J0(x)^2 - J1(x)^2,
+ * x = (2 pi a_eq / lambda) sin(theta), over the forward hemisphere, summing to area_mm2. */
+int icp_drop_diffraction_rows(const double* u_edges, uint32_t nt, double area_mm2, double wavelength_nm, double* rows);
+
+/* One drop record (particle frame: gravity along -y, shape polar axis -y).
+ * r/a = 1 + sum_n coefficients[n] T_n(mu), mu = cos(angle from -y); a = radius_mm. */
+typedef struct {
+    double radius_mm;
+    double coefficients[8];
+    double inclination_deg;    /* ki = (cos a, -sin a, 0)                                     */
+    double exterior_index, interior_index, wavelength_nm;
+    double tail_tolerance, balance_tolerance;
+    uint32_t nt, np, ct, cp;
+    uint32_t max_internal_hits, precision;
+    uint64_t rays, seed;       /* rays sampled uniformly over the bounding disk (counter RNG) */
+    uint32_t diffraction;      /* 1: add the analytic Fraunhofer stage (equal power to Aproj) */
+    uint32_t reserved;
+    icp_cdf_policy policy;
+    icp_tuning tuning;
+} icp_drop_record;
+
+typedef struct {
+    icp_trace_stats trace;
+    double projected_area_mm2;  /* CPU binary64 integral                                        */
+    double sampled_area_mm2;    /* area of the sampling disk                                    */
+    double incident_area_mm2;   /* hit fraction x disk area (Monte Carlo estimate of Aproj)     */
+    double escaped_area_mm2, unresolved_area_mm2, diffraction_area_mm2;
+    double forward_mass_mm2, backward_mass_mm2, histogram_mass_mm2, point_axial_mm2;
+    double histogram_relative_error;
+    double ki[3], e0[3], e1[3]; /* ensemble frame of the stored CDF (sampling_frame_columns)   */
+    icp_cdf_report cdf;
+    double seconds_trace, seconds_cdf;
+} icp_drop_report;
+
+/* Area (mm^2) of the disk the drop's rays are sampled on: radius 1 + c0 for a sphere, else the
+ * conservative outer radius (1 + c0 + sum|c_n|)(1 + 1e-6) + 1e-6, times radius_mm.  A record of
+ * N rays weighs each unit of exit power sampled_area / N. */
+int icp_drop_sampling_area(const double coefficients[8], double radius_mm, double* area_mm2);
+/* Traces rays [first, first+count) of a drop record into d_cell_mass (FP64, theta-major);
+ * area_weight mm^2 per unit exit power.  Stats accumulate into *stats (host). */
+int icp_drop_trace_bin(icp_context* ctx, const icp_drop_record* record, uint64_t first, uint64_t count,
+                       double area_weight, const icp_grid* grid, const double* d_edges, double* d_cell_mass,
+                       icp_trace_stats* stats);
+/* Host-buffer entry used by the rainbow_generate drop-in: trace + bin (+ diffraction) + CDF. */
+int icp_drop_generate(icp_context* ctx, const icp_drop_record* record, double* h_phi, double* h_theta, double* h_u,
+                      icp_drop_report* report);
+
 #ifdef __cplusplus
 }
 #endif

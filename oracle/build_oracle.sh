@@ -5,5 +5,5 @@ set -euo pipefail
 here="$(cd "$(dirname "$0")" && pwd)"
 mkdir -p "$here/_build"
 gcc -std=c11 -O2 -fno-fast-math -ffp-contract=off -fPIC -shared \
-    "$here/icp_oracle.c" "$here/icp_oracle_drop.c" -lm -o "$here/_build/libicp_oracle.so"
+    "$here/icp_oracle.c" -lm -o "$here/_build/libicp_oracle.so"
 echo "built $here/_build/libicp_oracle.so"

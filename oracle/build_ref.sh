@@ -6,6 +6,8 @@
 #
 #   oracle/_ref/ice_generate_phase_cpu   reference CLI (hex_phase/apps/generate_hex_phase.cpp)
 #   oracle/_ref/ref_hex_harness          oracle/ref_hex_harness.cpp over the same sources
+#   oracle/_ref/ref_drop_harness         oracle/ref_drop_harness.cpp over the header-only drop
+#                                        tracer, src/projected_area.cpp, src/water_refractive_index.cpp
 #
 # Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
 set -euo pipefail
@@ -24,4 +26,6 @@ srcs=("$ref/hex_phase/src/phase_table.cpp" "$ref/hex_phase/src/phase_generate.cp
       "$ref/src/npy_writer.cpp")
 g++ "${flags[@]}" "$ref/hex_phase/apps/generate_hex_phase.cpp" "${srcs[@]}" -o "$out/ice_generate_phase_cpu"
 g++ "${flags[@]}" "$here/ref_hex_harness.cpp" "${srcs[@]}" -o "$out/ref_hex_harness"
-echo "built $out/ice_generate_phase_cpu $out/ref_hex_harness"
+g++ -std=c++20 -O2 -fno-fast-math -ffp-contract=off -I"$ref/include" "$here/ref_drop_harness.cpp" \
+    "$ref/src/projected_area.cpp" "$ref/src/water_refractive_index.cpp" -o "$out/ref_drop_harness"
+echo "built $out/ice_generate_phase_cpu $out/ref_hex_harness $out/ref_drop_harness"

@@ -331,9 +331,21 @@ static cplx tir_phase(double a, double b)
     r.im = -2 * a * b / den;
     return r;
 }
-/* flux_interface.hpp:26-88: s/p split in flux normalisation; n points into the incident medium. */
-static branches_t split_flux(const fray_t* ray, v3 n, double ni, double nt)
+/* flux_interface.hpp:26-88: s/p split in flux normalisation; n points into the incident medium.
+ * drop = 1 adds the drop interface's conventions (include/rainbow/dielectric_interface.hpp:
+ * 86-91): a cosine down to -2^-19 is clamped to zero, and below sin^2 = 2^-40 the s axis is the
+ * incident frame's e0.  It also re-orthogonalises s against the incident and each outgoing
+ * direction (a no-op in exact arithmetic): near normal incidence d x n loses ~1e-16/sin of
+ * its direction, which on a curved surface would otherwise fail the 128-ulp frame test. */
+static v3 orthogonal_to(v3 s, v3 d)
 {
+    v3 o;
+    if (!v_normalize(v_sub(s, v_mul(d, v_dot(d, s))), &o)) return s;
+    return o;
+}
+static branches_t split_flux_graze(const fray_t* ray, v3 n, double ni, double nt, int drop)
+{
+    const double graze = drop ? 0x1p-19 : 0.0;
     branches_t b;
     double ci, scale, sine, ns, a, c, eta, st, before, after;
     v3 s, scaled, pin;
@@ -345,7 +357,8 @@ static branches_t split_flux(const fray_t* ray, v3 n, double ni, double nt)
         !(ni > 0 && nt > 0 && fin(ni) && fin(nt)))
         return b;
     ci = -v_dot(ray->d, n);
-    if (ci < 0 || ci > 1 + 128 * ICPO_EPS) return b;
+    if (ci < -graze || ci > 1 + 128 * ICPO_EPS) return b;
+    if (ci < 0) ci = 0;
     if (ci > 1) ci = 1;
     if (ni == nt) {
         b.trans = *ray;
@@ -361,7 +374,11 @@ static branches_t split_flux(const fray_t* ray, v3 n, double ni, double nt)
     if (scale > 0) scaled = v_div(s, scale);
     else { scaled.x = 0; scaled.y = 0; scaled.z = 0; }
     sine = scale * sqrt(v_dot(scaled, scaled));
-    if (sine > 0) { if (!v_normalize(s, &s)) return b; }
+    if (drop) {
+        if (sine * sine > 0x1p-40) { if (!v_normalize(s, &s)) return b; }
+        else s = ray->fr.e0;
+        s = orthogonal_to(s, ray->d);
+    } else if (sine > 0) { if (!v_normalize(s, &s)) return b; }
     else s = ray->fr.e0;
     if (!v_normalize(v_cross(ray->d, s), &pin)) return b;
     spf.e0 = s;
@@ -375,8 +392,8 @@ static branches_t split_flux(const fray_t* ray, v3 n, double ni, double nt)
     st = eta * sine;
     if (!fin(st)) return b;
     if (!v_normalize(v_add(ray->d, v_mul(n, 2 * ci)), &b.refl.d)) return b;
-    b.refl.fr.e0 = s;
-    if (!v_normalize(v_cross(b.refl.d, s), &b.refl.fr.e1)) return b;
+    b.refl.fr.e0 = drop ? orthogonal_to(s, b.refl.d) : s;
+    if (!v_normalize(v_cross(b.refl.d, b.refl.fr.e0), &b.refl.fr.e1)) return b;
     if (st > 1) {
         double inverse = 1 / st, beta = st * sqrt((1 - inverse) * (1 + inverse));
         rs = tir_phase(a * ci, c * beta);
@@ -395,8 +412,8 @@ static branches_t split_flux(const fray_t* ray, v3 n, double ni, double nt)
         ctp.re = tp; ctp.im = 0;
         b.trans.j = scale_rows(j, cts, ctp);
         if (!v_normalize(v_sub(v_mul(v_add(ray->d, v_mul(n, ci)), eta), v_mul(n, ct)), &b.trans.d)) return b;
-        b.trans.fr.e0 = s;
-        if (!v_normalize(v_cross(b.trans.d, s), &b.trans.fr.e1)) return b;
+        b.trans.fr.e0 = drop ? orthogonal_to(s, b.trans.d) : s;
+        if (!v_normalize(v_cross(b.trans.d, b.trans.fr.e0), &b.trans.fr.e1)) return b;
         b.has_t = 1;
     }
     b.refl.j = scale_rows(j, rs, rp);
@@ -407,6 +424,10 @@ static branches_t split_flux(const fray_t* ray, v3 n, double ni, double nt)
               (!b.has_t || (frame_valid(b.trans.fr, b.trans.d) && jones_finite(&b.trans.j))) &&
               fin(b.balance) && fabs(b.balance) <= 2048 * ICPO_EPS * mx(before, DBL_MIN);
     return b;
+}
+static branches_t split_flux(const fray_t* ray, v3 n, double ni, double nt)
+{
+    return split_flux_graze(ray, n, ni, nt, 0);
 }
 
 /* ----------------------------------------------------------- ray chain */
@@ -995,4 +1016,486 @@ done:
     free(coarse);
     free(columns);
     return rc;
+}
+
+/* ============================================================ water drops */
+/*
+ * Axisymmetric drop in units of its equal-volume radius a: r/a = 1 + sum_n c_n T_n(mu),
+ * mu = -p.y/|p| (include/rainbow/raindrop_shape.hpp:70-100).  The ray chain is the prism's
+ * linear R/T chain (hex_trace_core.hpp:190-252) with the drop surface as the boundary; its
+ * first four exits are RaindropPathTracer::trace_impl's families R, TT, TRT, TRRT
+ * (include/rainbow/raindrop_paths.hpp:41-107).  The reference intersects with an interval
+ * bracket stack plus safeguarded Newton (raindrop_intersection.hpp:203-382); this oracle
+ * brackets the same root by sampling the chord of the bounding sphere (a golden-section
+ * minimum of the convex gauge |p|/R(mu) decides near-silhouette lines) and polishes it with
+ * bracketed Newton.  Rays start on a disk of radius `disk` perpendicular to k, `back` before
+ * the centre, drawn with the counter RNG (math.hpp:136-146) in place of the reference's
+ * deterministic vertex lattice (raindrop_paths.hpp:52-58).
+ *
+ * drop[] layout (doubles): c[0..7], r_center, r_out, r_in, sphere, disk, back, n_ext, n_int,
+ *   tail, scale (mm^2 per unit exit power), radius_mm.
+ * frame9[]: k(3), e0(3), e1(3) -- the incident direction and the sampling / grid frame.
+ */
+typedef struct {
+    double c[8];
+    double r_center, r_out, r_in, disk, back;
+    int sphere;
+} drop_t;
+
+typedef struct {
+    drop_t shape;
+    v3 k;
+    frame_t kf;
+    double n_ext, n_int, tail, scale, radius_mm;
+    uint64_t seed, total;
+    uint32_t max_hits;
+} drop_cfg_t;
+
+#define DR_SAMPLES 24
+
+static double dr_radius(const drop_t* s, double mu, double* deriv)
+{
+    double prev = 1, cur = mu, dprev = 0, dcur = 1, r = 1 + s->c[0] + s->c[1] * mu, d = s->c[1];
+    int n;
+    for (n = 2; n < 8; ++n) {
+        double next = 2 * mu * cur - prev, dnext = 2 * cur + 2 * mu * dcur - dprev;
+        r += s->c[n] * next;
+        d += s->c[n] * dnext;
+        prev = cur;
+        cur = next;
+        dprev = dcur;
+        dcur = dnext;
+    }
+    *deriv = d;
+    return r;
+}
+/* outward unit normal: gradient of |p| - R(mu) (raindrop_shape.hpp:92-100) */
+static int dr_normal(const drop_t* s, v3 p, v3* n)
+{
+    double r = sqrt(v_dot(p, p)), dR;
+    v3 u, g, down = {0, -1, 0};
+    if (!(r > 0) || !fin(r)) return 0;
+    u = v_div(p, r);
+    if (s->sphere) return v_normalize(u, n);
+    dr_radius(s, -u.y, &dR);
+    g = v_sub(u, v_mul(v_sub(down, v_mul(u, -u.y)), dR / r));
+    return v_normalize(g, n);
+}
+/* f(t) = |o + t d| - R(mu) and df/dt; deep inside only its sign matters (raindrop_shape.hpp:86-91) */
+static double dr_f(const drop_t* s, v3 o, v3 d, double t, double* df)
+{
+    v3 p = v_add(o, v_mul(d, t));
+    double r = sqrt(v_dot(p, p)), mu, dR, R, rd, dmu;
+    if (r < 0.25 * s->r_in) {
+        *df = r > 0 ? v_dot(p, d) / r : 0;
+        return r - s->r_in;
+    }
+    rd = v_dot(p, d) / r;
+    mu = -p.y / r;
+    R = dr_radius(s, mu, &dR);
+    dmu = (-d.y - mu * rd) / r;
+    *df = rd - dR * dmu;
+    return r - R;
+}
+static double dr_gauge(const drop_t* s, v3 o, v3 d, double t)
+{
+    v3 p = v_add(o, v_mul(d, t));
+    double r = sqrt(v_dot(p, p)), dR;
+    if (!(r > 0)) return 0;
+    return r / dr_radius(s, -p.y / r, &dR);
+}
+/* minimum of the convex gauge on [a, b] by golden-section search */
+static double dr_gauge_min(const drop_t* s, v3 o, v3 d, double a, double b)
+{
+    const double g = 0.6180339887498949;
+    double x1 = b - g * (b - a), x2 = a + g * (b - a);
+    double f1 = dr_gauge(s, o, d, x1), f2 = dr_gauge(s, o, d, x2);
+    int it;
+    for (it = 0; it < 200 && b - a > 4 * ICPO_EPS * mx(1, fabs(a)); ++it) {
+        if (f1 <= f2) {
+            b = x2; x2 = x1; f2 = f1;
+            x1 = b - g * (b - a);
+            f1 = dr_gauge(s, o, d, x1);
+        } else {
+            a = x1; x1 = x2; f1 = f2;
+            x2 = a + g * (b - a);
+            f2 = dr_gauge(s, o, d, x2);
+        }
+    }
+    return f1 <= f2 ? x1 : x2;
+}
+/* bracketed Newton on [a, b], f(a) and f(b) of opposite signs (bisection when Newton leaves it) */
+static double dr_refine(const drop_t* s, v3 o, v3 d, double a, double fa, double b)
+{
+    double t = 0.5 * (a + b);
+    int it;
+    for (it = 0; it < 300; ++it) {
+        double df, f = dr_f(s, o, d, t, &df), tn, lo, hi;
+        if (f == 0) return t;
+        if ((f < 0) == (fa < 0)) { a = t; fa = f; }
+        else b = t;
+        lo = a < b ? a : b;
+        hi = a < b ? b : a;
+        tn = t - f / df;
+        if (!(tn > lo && tn < hi)) tn = 0.5 * (lo + hi);
+        if (fabs(tn - t) <= 2 * ICPO_EPS * mx(1, fabs(t)) || hi - lo <= 4 * ICPO_EPS * mx(1, fabs(t))) return tn;
+        t = tn;
+    }
+    return t;
+}
+static int dr_sphere_roots(v3 p, v3 d, double rad, double* t0, double* t1)
+{
+    double b = v_dot(p, d), c = v_dot(p, p) - rad * rad, disc = b * b - c, q;
+    if (!(disc >= 0)) return 0;
+    q = sqrt(disc);
+    *t0 = -b - q;
+    *t1 = -b + q;
+    return 1;
+}
+/* first surface point along an exterior line; 0 on a miss */
+static int dr_entry(const drop_t* s, v3 o, v3 d, double* t)
+{
+    double t0, t1, prev, fprev, df, tm;
+    int i;
+    if (s->sphere) {
+        if (!dr_sphere_roots(o, d, s->r_center, &t0, &t1) || t0 < 0) return 0;
+        *t = t0;
+        return 1;
+    }
+    if (!dr_sphere_roots(o, d, s->r_out, &t0, &t1)) return 0;
+    if (t0 < 0) t0 = 0;
+    prev = t0;
+    fprev = dr_f(s, o, d, prev, &df);
+    for (i = 1; i <= DR_SAMPLES; ++i) {
+        double ti = t0 + (t1 - t0) * i / DR_SAMPLES, fi = dr_f(s, o, d, ti, &df);
+        if (fi < 0) { *t = dr_refine(s, o, d, prev, fprev, ti); return 1; }
+        prev = ti;
+        fprev = fi;
+    }
+    tm = dr_gauge_min(s, o, d, t0, t1);
+    if (!(dr_gauge(s, o, d, tm) < 1)) return 0;
+    *t = dr_refine(s, o, d, t0, dr_f(s, o, d, t0, &df), tm);
+    return 1;
+}
+/* far end of an interior chord that starts on the surface at p */
+static double dr_exit(const drop_t* s, v3 p, v3 d)
+{
+    double t0, t1, df, tm, prev;
+    int i;
+    if (s->sphere) {
+        if (!dr_sphere_roots(p, d, s->r_center, &t0, &t1)) return 0;
+        return t1 > 0 ? t1 : 0;
+    }
+    if (!dr_sphere_roots(p, d, s->r_out, &t0, &t1) || !(t1 > 0)) return 0;
+    prev = t1;
+    for (i = DR_SAMPLES - 1; i >= 1; --i) {
+        double ti = t1 * i / DR_SAMPLES, fi = dr_f(s, p, d, ti, &df);
+        if (fi < 0) return dr_refine(s, p, d, prev, dr_f(s, p, d, prev, &df), ti);
+        prev = ti;
+    }
+    tm = dr_gauge_min(s, p, d, 0, t1);
+    if (!(dr_gauge(s, p, d, tm) < 1)) return 0;
+    return dr_refine(s, p, d, t1, dr_f(s, p, d, t1, &df), tm);
+}
+
+typedef void (*drop_emit_fn)(void* user, v3 d, double power, uint32_t hit);
+
+static int drop_emit(drop_emit_fn emit, void* user, ray_audit_t* a, ksum* esc, const drop_cfg_t* c,
+                     const fray_t* ray, v3 pos, uint32_t hit)
+{
+    double power = jones_power(&ray->j);
+    if (!fin(power) || power < 0 || (!power && jones_nonzero(&ray->j))) return ST_NUMERICAL;
+    if (power == 0) return ST_EXHAUSTED;
+    if (!v_fin(v_mul(pos, c->radius_mm))) return ST_NUMERICAL;
+    if (emit) emit(user, ray->d, power, hit);
+    ks_add(esc, power);
+    ++a->outputs;
+    return ST_EXHAUSTED;
+}
+/* chain from the entry point pos of a ray travelling along k (frame kf) */
+static ray_audit_t drop_from_entry(const drop_cfg_t* c, v3 pos, v3 k, frame_t kf, drop_emit_fn emit, void* user)
+{
+    ray_audit_t a;
+    ksum esc = {0, 0};
+    fray_t inc, ray;
+    branches_t sp;
+    v3 p, n;
+    unsigned encounter;
+    int em;
+    double remaining;
+    memset(&a, 0, sizeof a);
+    if (!dr_normal(&c->shape, pos, &n)) return finish_audit(a, &esc, 1, ST_NUMERICAL);
+    inc.d = k;
+    inc.fr = kf;
+    inc.j = jones_identity();
+    sp = split_flux_graze(&inc, n, c->n_ext, c->n_int, 1);
+    if (!sp.valid) return finish_audit(a, &esc, 1, ST_NUMERICAL);
+    a.max_iface = fabs(sp.balance);
+    em = drop_emit(emit, user, &a, &esc, c, &sp.refl, pos, 0);
+    if (em != ST_EXHAUSTED) return finish_audit(a, &esc, 1, em);
+    if (!sp.has_t) { a.tir = 1; return finish_audit(a, &esc, 0, ST_EXHAUSTED); }
+    ray = sp.trans;
+    p = pos;
+    for (encounter = 0; encounter < c->max_hits; ++encounter) {
+        double power = jones_power(&ray.j), t;
+        if (!fin(power) || power < 0 || (!power && jones_nonzero(&ray.j))) return finish_audit(a, &esc, power, ST_NUMERICAL);
+        if (power == 0) return finish_audit(a, &esc, 0, ST_EXHAUSTED);
+        if (power <= c->tail) return finish_audit(a, &esc, power, ST_TAIL);
+        t = dr_exit(&c->shape, p, ray.d);
+        p = v_add(p, v_mul(ray.d, t));
+        if (!fin(t) || !dr_normal(&c->shape, p, &n)) return finish_audit(a, &esc, power, ST_NUMERICAL);
+        sp = split_flux_graze(&ray, v_neg(n), c->n_int, c->n_ext, 1);
+        if (!sp.valid) return finish_audit(a, &esc, power, ST_NUMERICAL);
+        ++a.hits;
+        if (sp.tir) ++a.tir;
+        a.max_iface = mx(a.max_iface, fabs(sp.balance));
+        if (sp.has_t) {
+            em = drop_emit(emit, user, &a, &esc, c, &sp.trans, p, a.hits);
+            if (em != ST_EXHAUSTED) return finish_audit(a, &esc, power, em);
+        }
+        ray = sp.refl;
+    }
+    remaining = jones_power(&ray.j);
+    if (!fin(remaining) || remaining < 0 || (!remaining && jones_nonzero(&ray.j)))
+        return finish_audit(a, &esc, remaining, ST_NUMERICAL);
+    return finish_audit(a, &esc, remaining,
+                        remaining == 0 ? ST_EXHAUSTED : (remaining <= c->tail ? ST_TAIL : ST_LIMIT));
+}
+/* ray `id`: point on the sampling disk, entry along k; *missed = 1 when the line misses */
+static ray_audit_t drop_sample(const drop_cfg_t* c, uint64_t id, drop_emit_fn emit, void* user, int* missed)
+{
+    ray_audit_t a;
+    ksum none = {0, 0};
+    double u0 = icpo_sample_uniform(c->seed, id, 0), u1 = icpo_sample_uniform(c->seed, id, 1);
+    double rad = c->shape.disk * sqrt(u0), sn = sin(ICPO_PI * (2 * u1)), cs = cos(ICPO_PI * (2 * u1)), t;
+    v3 o = v_sub(v_add(v_mul(c->kf.e0, rad * cs), v_mul(c->kf.e1, rad * sn)), v_mul(c->k, c->shape.back));
+    *missed = 0;
+    if (!dr_entry(&c->shape, o, c->k, &t)) {
+        memset(&a, 0, sizeof a);
+        *missed = 1;
+        return finish_audit(a, &none, 0, ST_EXHAUSTED);
+    }
+    return drop_from_entry(c, v_add(o, v_mul(c->k, t)), c->k, c->kf, emit, user);
+}
+static int drop_setup(const double* drop, const double* frame9, uint64_t seed, uint64_t total, uint32_t max_hits,
+                      drop_cfg_t* c)
+{
+    int i;
+    memset(c, 0, sizeof *c);
+    for (i = 0; i < 8; ++i) c->shape.c[i] = drop[i];
+    c->shape.r_center = drop[8];
+    c->shape.r_out = drop[9];
+    c->shape.r_in = drop[10];
+    c->shape.sphere = drop[11] != 0;
+    c->shape.disk = drop[12];
+    c->shape.back = drop[13];
+    c->n_ext = drop[14];
+    c->n_int = drop[15];
+    c->tail = drop[16];
+    c->scale = drop[17];
+    c->radius_mm = drop[18];
+    c->k.x = frame9[0]; c->k.y = frame9[1]; c->k.z = frame9[2];
+    c->kf.e0.x = frame9[3]; c->kf.e0.y = frame9[4]; c->kf.e0.z = frame9[5];
+    c->kf.e1.x = frame9[6]; c->kf.e1.y = frame9[7]; c->kf.e1.z = frame9[8];
+    c->seed = seed;
+    c->total = total;
+    c->max_hits = max_hits;
+    if (!frame_valid(c->kf, c->k) || !(c->n_ext > 0 && c->n_int > 0) || !(c->tail >= 0 && c->tail < 1) ||
+        !max_hits || !(c->shape.r_out >= c->shape.r_center) || !(c->shape.r_in > 0) || !(c->shape.disk > 0))
+        return -1;
+    return 0;
+}
+
+static void drop_hist_emit(void* user, v3 d, double power, uint32_t hit)
+{
+    (void)hit;
+    hist_emit(user, d, power);
+}
+/*
+ * Traces rays [first, first+count) of a drop record into a Kahan histogram (cells: 2*nt*np).
+ * stats[] (inout): point_mass(v,c), point_axial(v,c), forward(v,c), backward(v,c),
+ *   escaped(v,c), unresolved(v,c), max_balance, max_iface  -- powers in units of one ray.
+ * counts[] (inout): binned exits, snapped, outputs, rays, status[8], missed, encounters.
+ */
+int icpo_drop_accumulate(const double* drop, const double* frame9, uint64_t seed, uint64_t total, uint32_t max_hits,
+                         const double* edges, uint32_t nt, uint32_t np, uint64_t first, uint64_t count,
+                         double* cells, double* stats, uint64_t* counts)
+{
+    drop_cfg_t c;
+    hist_t h;
+    uint64_t i;
+    ksum esc, unres;
+    if (drop_setup(drop, frame9, seed, total, max_hits, &c)) return -1;
+    if (first + count > total) return -3;
+    memset(&h, 0, sizeof h);
+    h.grid.edges = edges;
+    h.grid.nt = nt;
+    h.grid.np = np;
+    h.grid.ki = c.k;
+    h.grid.fr = c.kf;
+    h.rot.x.x = 1; h.rot.y.y = 1; h.rot.z.z = 1;
+    h.scale = c.scale;
+    h.cells = (ksum*)cells;
+    h.point_mass.value = stats[0]; h.point_mass.correction = stats[1];
+    h.point_axial.value = stats[2]; h.point_axial.correction = stats[3];
+    h.forward.value = stats[4]; h.forward.correction = stats[5];
+    h.backward.value = stats[6]; h.backward.correction = stats[7];
+    esc.value = stats[8]; esc.correction = stats[9];
+    unres.value = stats[10]; unres.correction = stats[11];
+    h.count = counts[0];
+    h.snapped = counts[1];
+    for (i = first; i < first + count; ++i) {
+        int missed;
+        ray_audit_t a = drop_sample(&c, i, drop_hist_emit, &h, &missed);
+        if (h.error) return -10 - h.error;
+        counts[3] += 1;
+        if (missed) { counts[12] += 1; continue; }
+        counts[2] += a.outputs;
+        if ((unsigned)a.status < 8) counts[4 + a.status] += 1;
+        counts[13] += a.hits;
+        ks_add(&esc, a.escaped);
+        ks_add(&unres, a.unresolved);
+        stats[12] = mx(stats[12], fabs(a.balance));
+        stats[13] = mx(stats[13], a.max_iface);
+    }
+    stats[0] = h.point_mass.value; stats[1] = h.point_mass.correction;
+    stats[2] = h.point_axial.value; stats[3] = h.point_axial.correction;
+    stats[4] = h.forward.value; stats[5] = h.forward.correction;
+    stats[6] = h.backward.value; stats[7] = h.backward.correction;
+    stats[8] = esc.value; stats[9] = esc.correction;
+    stats[10] = unres.value; stats[11] = unres.correction;
+    counts[0] = h.count;
+    counts[1] = h.snapped;
+    return 0;
+}
+
+/* per-ray dump: ray_info[8] = status, outputs, escaped, unresolved, hits, max_iface, missed, tir;
+ * exits[5 per exit] = direction(3), power, interaction index (0 = entry reflection) */
+typedef struct { double* out; uint32_t cap, n; } drop_dump_t;
+static void drop_dump_emit(void* user, v3 d, double power, uint32_t hit)
+{
+    drop_dump_t* q = (drop_dump_t*)user;
+    if (q->n < q->cap) {
+        double* e = q->out + 5 * (size_t)q->n;
+        e[0] = d.x; e[1] = d.y; e[2] = d.z; e[3] = power; e[4] = hit;
+    }
+    q->n++;
+}
+static void drop_info(double* info, ray_audit_t a, int missed)
+{
+    info[0] = a.status;
+    info[1] = (double)a.outputs;
+    info[2] = a.escaped;
+    info[3] = a.unresolved;
+    info[4] = a.hits;
+    info[5] = a.max_iface;
+    info[6] = missed;
+    info[7] = a.tir;
+}
+int icpo_drop_trace_rays(const double* drop, const double* frame9, uint64_t seed, uint64_t total, uint32_t max_hits,
+                         uint64_t first, uint64_t count, uint32_t max_out, double* ray_info, double* exits)
+{
+    drop_cfg_t c;
+    uint64_t i;
+    if (drop_setup(drop, frame9, seed, total, max_hits, &c)) return -1;
+    for (i = 0; i < count; ++i) {
+        drop_dump_t q;
+        int missed;
+        ray_audit_t a;
+        q.out = exits + (size_t)i * max_out * 5;
+        q.cap = max_out;
+        q.n = 0;
+        a = drop_sample(&c, first + i, drop_dump_emit, &q, &missed);
+        drop_info(ray_info + 8 * i, a, missed);
+    }
+    return 0;
+}
+/* one ray from an exterior origin o along unit k with polarisation frame vector e0 */
+int icpo_drop_trace_from(const double* drop, const double* o3, const double* k3, const double* e03, uint32_t max_hits,
+                         uint32_t max_out, double* ray_info, double* exits)
+{
+    drop_cfg_t c;
+    double frame9[9], t;
+    v3 o = {o3[0], o3[1], o3[2]}, k = {k3[0], k3[1], k3[2]}, e0 = {e03[0], e03[1], e03[2]}, e1 = v_cross(k, e0);
+    drop_dump_t q;
+    ray_audit_t a;
+    frame9[0] = k.x; frame9[1] = k.y; frame9[2] = k.z;
+    frame9[3] = e0.x; frame9[4] = e0.y; frame9[5] = e0.z;
+    frame9[6] = e1.x; frame9[7] = e1.y; frame9[8] = e1.z;
+    if (drop_setup(drop, frame9, 0, 1, max_hits, &c)) return -1;
+    q.out = exits;
+    q.cap = max_out;
+    q.n = 0;
+    if (!dr_entry(&c.shape, o, k, &t)) {
+        ksum none = {0, 0};
+        memset(&a, 0, sizeof a);
+        drop_info(ray_info, finish_audit(a, &none, 0, ST_EXHAUSTED), 1);
+        return 0;
+    }
+    a = drop_from_entry(&c, v_add(o, v_mul(k, t)), k, c.kf, drop_dump_emit, &q);
+    drop_info(ray_info, a, 0);
+    return 0;
+}
+/* boundary query: entry from an exterior point (inside = 0) or chord exit from a surface
+ * point (inside = 1); out[8] = hit, t, position(3), outward normal(3) */
+int icpo_drop_intersect(const double* drop, const double* o3, const double* d3, int inside, double* out)
+{
+    drop_cfg_t c;
+    static const double frame9[9] = {1, 0, 0, 0, 0, 1, 0, -1, 0};
+    v3 o = {o3[0], o3[1], o3[2]}, d = {d3[0], d3[1], d3[2]}, p, n;
+    double t = 0;
+    int hit;
+    if (drop_setup(drop, frame9, 0, 1, 1, &c)) return -1;
+    if (inside) {
+        t = dr_exit(&c.shape, o, d);
+        hit = 1;
+    } else {
+        hit = dr_entry(&c.shape, o, d, &t);
+    }
+    memset(out, 0, 8 * sizeof(double));
+    out[0] = hit;
+    if (!hit) return 0;
+    p = v_add(o, v_mul(d, t));
+    if (!dr_normal(&c.shape, p, &n)) return -2;
+    out[1] = t;
+    out[2] = p.x; out[3] = p.y; out[4] = p.z;
+    out[5] = n.x; out[6] = n.y; out[7] = n.z;
+    return 0;
+}
+/* Incident frame of an inclination alpha: ki = (cos a, -sin a, 0) rounded to binary32 and
+ * normalised there, e0 from the z helper axis (x when |k_z| >= 0.9) in binary32
+ * (apps/generate_phase.cpp:209-217, include/rainbow/raindrop_settings.hpp:37-38,
+ * include/rainbow/vec3.hpp:20-36, 60-65), then promoted and re-orthonormalised in binary64
+ * (apps/generate_phase.cpp:242-245). */
+static float f_dot(float ax, float ay, float az, float bx, float by, float bz)
+{
+    return fmaf(ax, bx, fmaf(ay, by, az * bz));
+}
+int icpo_drop_frame(double inclination_deg, double* k, double* e0, double* e1)
+{
+    double a = inclination_deg * ICPO_PI / 180.0, kd[3], ed[3], n, d;
+    float kx = (float)cos(a), ky = (float)-sin(a), kz = 0.0f, len, hx, hz, w, ex, ey, ez;
+    int i;
+    len = sqrtf(f_dot(kx, ky, kz, kx, ky, kz));
+    kx /= len; ky /= len; kz /= len;
+    hx = fabsf(kz) < 0.9f ? 0.0f : 1.0f;
+    hz = fabsf(kz) < 0.9f ? 1.0f : 0.0f;
+    w = f_dot(kx, ky, kz, hx, 0.0f, hz);
+    ex = hx - kx * w; ey = 0.0f - ky * w; ez = hz - kz * w;
+    len = sqrtf(f_dot(ex, ey, ez, ex, ey, ez));
+    ex /= len; ey /= len; ez /= len;
+    kd[0] = kx; kd[1] = ky; kd[2] = kz;
+    n = sqrt(kd[0] * kd[0] + kd[1] * kd[1] + kd[2] * kd[2]);
+    if (!(n > 0)) return -1;
+    for (i = 0; i < 3; ++i) kd[i] /= n;
+    ed[0] = ex; ed[1] = ey; ed[2] = ez;
+    d = ed[0] * kd[0] + ed[1] * kd[1] + ed[2] * kd[2];
+    for (i = 0; i < 3; ++i) ed[i] -= d * kd[i];
+    n = sqrt(ed[0] * ed[0] + ed[1] * ed[1] + ed[2] * ed[2]);
+    if (!(n > 0)) return -1;
+    for (i = 0; i < 3; ++i) { k[i] = kd[i]; e0[i] = ed[i] / n; }
+    e1[0] = k[1] * e0[2] - k[2] * e0[1];
+    e1[1] = k[2] * e0[0] - k[0] * e0[2];
+    e1[2] = k[0] * e0[1] - k[1] * e0[0];
+    return 0;
 }

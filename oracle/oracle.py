@@ -52,6 +52,13 @@ def _lib() -> C.CDLL:
     lib.icpo_measure_mass.argtypes = [_D, C.c_uint32, C.c_uint32, _D, _D]
     lib.icpo_build_cdf.argtypes = [_D, C.c_uint32, C.c_uint32, _D, C.c_uint32, C.c_uint32, C.c_double, C.c_double,
                                    C.c_double, _D, _D, _D, _D]
+    lib.icpo_drop_accumulate.argtypes = [_D, _D, C.c_uint64, C.c_uint64, C.c_uint32, _D, C.c_uint32, C.c_uint32,
+                                         C.c_uint64, C.c_uint64, _D, _D, _U]
+    lib.icpo_drop_trace_rays.argtypes = [_D, _D, C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint64,
+                                         C.c_uint32, _D, _D]
+    lib.icpo_drop_trace_from.argtypes = [_D, _D, _D, _D, C.c_uint32, C.c_uint32, _D, _D]
+    lib.icpo_drop_intersect.argtypes = [_D, _D, _D, C.c_int, _D]
+    lib.icpo_drop_frame.argtypes = [C.c_double, _D, _D, _D]
     return lib
 
 
@@ -246,3 +253,144 @@ def ref_masses(R, L, ki, n_int, n_ext, nt, np_, plan_csv: Path, max_hits=1024, t
     d = np.frombuffer(raw[8 * n:8 * n + 72], dtype="<f8").copy()
     u = np.frombuffer(raw[8 * n + 72:], dtype="<u8").copy()
     return masses, d, u
+
+
+# ------------------------------------------------------------------ water drops
+@dataclass
+class DropGeometry:
+    """Drop in units of its equal-volume radius and the sampling disk that covers it."""
+    coefficients: np.ndarray
+    radius_mm: float
+    r_center: float
+    r_out: float
+    r_in: float
+    sphere: bool
+    disk: float
+    back: float
+
+    def vector(self, n_int: float, n_ext: float = 1.0, tail: float = 1e-12, scale: float = 1.0) -> np.ndarray:
+        return np.array([*self.coefficients, self.r_center, self.r_out, self.r_in, float(self.sphere), self.disk,
+                         self.back, n_ext, n_int, tail, scale, self.radius_mm])
+
+    @property
+    def disk_area_mm2(self) -> float:
+        return math.pi * self.disk * self.disk * self.radius_mm * self.radius_mm
+
+
+def drop_geometry(coefficients, radius_mm: float) -> DropGeometry:
+    """Bounding radii from |T_n| <= 1; rays are sampled on the disk of the exact sphere radius
+    (spheres) or of the conservative outer radius, 2 r_out + 1 before the centre."""
+    c = np.asarray(coefficients, dtype=np.float64).copy()
+    sphere = bool(np.all(c[1:] == 0))
+    r_center = 1 + c[0]
+    s = 0.0
+    for x in c[1:]:
+        s += abs(float(x))
+    r_out = (1 + c[0] + s) * (1 + 1e-6) + 1e-6
+    r_in = 1 + c[0] - s
+    disk = r_center if sphere else r_out
+    return DropGeometry(c, radius_mm, r_center, r_out, r_in, sphere, disk, 2 * r_out + 1)
+
+
+def drop_frame(inclination_deg: float) -> np.ndarray:
+    """k, e0, e1 of an inclination as a (3, 3) array of rows."""
+    k, e0, e1 = np.empty(3), np.empty(3), np.empty(3)
+    if lib().icpo_drop_frame(inclination_deg, _p(k), _p(e0), _p(e1)):
+        raise ValueError("invalid inclination")
+    return np.stack([k, e0, e1])
+
+
+@dataclass
+class DropRecord:
+    masses: np.ndarray         # cell masses with the pole caps spread over the end rows (mm^2)
+    forward: float
+    backward: float
+    escaped_area: float
+    unresolved_area: float
+    incident_area: float       # hits x disk area / rays
+    point_axial: float
+    max_balance: float
+    max_iface: float
+    counts: dict = field(default_factory=dict)
+
+
+def drop_record(geo: DropGeometry, frame: np.ndarray, n_int: float, nt: int, np_: int, rays: int, seed: int,
+                max_hits: int = 1024, tail: float = 1e-12, n_ext: float = 1.0, first: int = 0,
+                count: int | None = None) -> DropRecord:
+    count = rays - first if count is None else count
+    scale = geo.disk_area_mm2 / rays
+    drop = geo.vector(n_int, n_ext, tail, scale)
+    f9 = np.ascontiguousarray(frame, dtype=np.float64).reshape(-1)
+    edges = u_edges(nt)
+    cells = np.zeros(2 * nt * np_)
+    stats = np.zeros(14)
+    counts = np.zeros(14, dtype=np.uint64)
+    rc = lib().icpo_drop_accumulate(_p(drop), _p(f9), seed, rays, max_hits, _p(edges), nt, np_, first, count,
+                                    _p(cells), _p(stats), _p(counts))
+    if rc:
+        raise RuntimeError(f"oracle drop accumulate failed ({rc})")
+    hist = np.zeros(18)
+    hist[[0, 2, 4, 6]] = stats[[0, 2, 4, 6]]
+    masses = np.empty(nt * np_)
+    if lib().icpo_masses(_p(cells), nt, np_, _p(hist), _p(masses)):
+        raise RuntimeError("Pole weight underflow.")
+    names = ["samples", "snapped", "outputs", "rays"] + [f"status{i}" for i in range(8)] + ["missed", "encounters"]
+    cnt = {k: int(v) for k, v in zip(names, counts)}
+    hits = cnt["rays"] - cnt["missed"]
+    return DropRecord(masses, stats[4], stats[6], scale * stats[8], scale * stats[10], scale * hits, stats[2],
+                      stats[12], stats[13], cnt)
+
+
+def drop_trace_rays(geo: DropGeometry, frame, n_int, seed, total, first, count, max_hits=1024, tail=1e-12,
+                    n_ext=1.0, max_out=64):
+    """Per-ray info (status, outputs, escaped, unresolved, hits, max_iface, missed, tir) and
+    exits (direction, power, interaction index)."""
+    drop = geo.vector(n_int, n_ext, tail)
+    f9 = np.ascontiguousarray(frame, dtype=np.float64).reshape(-1)
+    info = np.zeros((count, 8))
+    exits = np.zeros((count, max_out, 5))
+    if lib().icpo_drop_trace_rays(_p(drop), _p(f9), seed, total, max_hits, first, count, max_out, _p(info),
+                                  _p(exits)):
+        raise RuntimeError("invalid drop settings")
+    return info, exits
+
+
+def drop_trace_from(geo: DropGeometry, origin, k, e0, n_int, max_hits=3, n_ext=1.0, tail=0.0, max_out=16):
+    drop = geo.vector(n_int, n_ext, tail)
+    o, kk, ee = (np.ascontiguousarray(v, dtype=np.float64) for v in (origin, k, e0))
+    info = np.zeros(8)
+    exits = np.zeros((max_out, 5))
+    if lib().icpo_drop_trace_from(_p(drop), _p(o), _p(kk), _p(ee), max_hits, max_out, _p(info), _p(exits)):
+        raise RuntimeError("invalid drop settings")
+    return info, exits[: min(int(info[1]), max_out)]
+
+
+def drop_intersect(geo: DropGeometry, origin, d, inside: bool) -> np.ndarray:
+    out = np.zeros(8)
+    o, dd = (np.ascontiguousarray(v, dtype=np.float64) for v in (origin, d))
+    if lib().icpo_drop_intersect(_p(geo.vector(1.33)), _p(o), _p(dd), int(inside), _p(out)):
+        raise RuntimeError("invalid drop query")
+    return out
+
+
+def ref_drop_available() -> bool:
+    return (REF_DIR / "ref_drop_harness").exists()
+
+
+def ref_drop_lines(mode: str, lines: list[str]) -> list[list[float]]:
+    """Runs the reference drop harness in a line mode (water, shape, area, frame)."""
+    r = subprocess.run([str(REF_DIR / "ref_drop_harness"), mode], input="\n".join(lines) + "\n",
+                       capture_output=True, text=True, check=True)
+    return [[float(x) for x in line.split()] for line in r.stdout.splitlines()]
+
+
+def ref_drop_families(radius_mm: float, sphere: bool, n_int: float, k, grid: int,
+                      workdir: Path | None = None) -> np.ndarray:
+    """The reference four-family tracer over its vertex lattice: (grid^2, 41) float64 rows."""
+    out = Path(workdir or "/tmp") / f"ref_families_{os.getpid()}.bin"
+    args = [str(REF_DIR / "ref_drop_harness"), "families", repr(float(radius_mm)), str(int(sphere)),
+            repr(float(n_int)), *map(repr, map(float, k)), str(grid), str(out)]
+    subprocess.run(args, check=True)
+    a = np.fromfile(out, dtype="<f8").reshape(-1, 41)
+    out.unlink()
+    return a

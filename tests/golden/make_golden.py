@@ -1,8 +1,8 @@
 """Regenerates the golden fixtures in tests/golden/ from the REFERENCE implementation.
 
 Runs the reference's own CPU code, compiled from its sources by oracle/build_ref.sh into
-oracle/_ref/ (ice_generate_phase_cpu and the ref_hex_harness driver), and stores its
-outputs as small .npz files.  Needs the reference checkout (default /root/reference);
+oracle/_ref/ (ice_generate_phase_cpu and the ref_hex_harness / ref_drop_harness drivers),
+and stores its outputs as small .npz files.  Needs the reference checkout (default /root/reference);
 the fixtures are committed so that tests never need it.
 
     python tests/golden/make_golden.py [REFERENCE_ROOT]
@@ -50,6 +50,48 @@ def masses(td: Path, R, L, ki, n, nt, np_, plan: str, max_hits=1024, tail=1e-12,
             np.frombuffer(raw[8 * k + 72:], "<u8").copy())
 
 
+def lines(mode: str, rows: list[str]) -> np.ndarray:
+    r = subprocess.run([str(REF_BIN / "ref_drop_harness"), mode], input="\n".join(rows) + "\n", capture_output=True,
+                       text=True, check=True)
+    return np.array([[float(x) for x in line.split()] for line in r.stdout.splitlines()])
+
+
+# Four-family configurations: radius, sphere, interior index, incident direction, lattice size.
+FAMILY_CASES = [(0.4, 0, 1.3314, (1.0, -0.3, 0.1), 21), (1.5, 0, 1.3314, (0.9396926, -0.3420201, 0.0), 21),
+                (3.0, 0, 1.3435, (1.0, -0.3, 0.1), 21)]
+
+
+def drop_fixtures(td: Path) -> None:
+    alphas = np.array([0.0, 20.0, -35.5, 45.0, 89.0, 120.0])
+    frame = lines("frame", [repr(float(a)) for a in alphas])
+    radii = np.array([0.05, 0.4, 0.41, 0.7, 1.0, 1.5, 1.73, 2.0, 2.5, 2.9, 3.0])
+    shape = lines("shape", [f"{r} 0" for r in radii])
+    water_in = np.array([[l, t, p] for l in (400.0, 550.0, 700.0, 1000.0) for t in (0.0, 20.0, 45.0, 60.0)
+                         for p in (5e4, 101325.0, 1e7, 1e8)])
+    water = lines("water", [f"{float(l)!r} {float(t)!r} {float(p)!r}" for l, t, p in water_in])
+    ks = np.array([[1.0, 0.0, 0.0], [0.9396926164627075, -0.3420201539993286, 0.0], [0.0, 1.0, 0.0],
+                   [0.3, -0.8, 0.52]])
+    area_in = []
+    for c in shape[[3, 5, 8, 10], :8]:
+        for k in ks:
+            area_in.append([*c, 1.5, *k])
+    area_in.append([0, -0.08, -0.02, 0.005, 0, 0, 0, 0, 1.5, *ks[1]])
+    area_in = np.array(area_in)
+    area = lines("area", [" ".join(repr(float(x)) for x in row) for row in area_in])[:, 0]
+    fam = {}
+    for i, (r, sph, n, k, g) in enumerate(FAMILY_CASES):
+        out = td / "f.bin"
+        run([REF_BIN / "ref_drop_harness", "families", repr(r), sph, repr(n), *map(repr, k), g, out])
+        a = np.fromfile(out, "<f8").reshape(-1, 41)
+        power = a[:, [16, 24, 32, 40]]
+        geom = np.delete(a, [16, 24, 32, 40], axis=1).astype(np.float32)  # binary32 values of the tracer
+        fam[f"families{i}_geom"] = geom
+        fam[f"families{i}_power"] = power
+    np.savez_compressed(HERE / "drop_reference.npz", frame_alpha=alphas, frame=frame, shape_radius=radii,
+                        shape=shape, water_in=water_in, water=water, area_in=area_in, area=area,
+                        family_cases=np.array([[r, s, n, *k, g] for r, s, n, k, g in FAMILY_CASES]), **fam)
+
+
 def main() -> None:
     subprocess.run([str(ROOT / "oracle" / "build_ref.sh"), str(REF)], check=True)
     with tempfile.TemporaryDirectory() as t:
@@ -85,6 +127,8 @@ def main() -> None:
         info = raw[:48 * 6].reshape(48, 6)
         exits = raw[48 * 6:].reshape(-1, 4)
         np.savez_compressed(HERE / "hex_rays.npz", info=info, exits=exits)
+        # 4. drops: host inputs and the four-family path tracer
+        drop_fixtures(td)
     for f in sorted(HERE.glob("*.npz")):
         print(f.name, f.stat().st_size)
 
