@@ -1,19 +1,25 @@
 """Benchmark: rays/s of one phase-function record on B200 (and the reference CPU arm).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--rays R]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload drop|hex] [--rays R]
 
-Workload (hex column): circumradius 0.05 mm, length 0.2 mm (length/diameter 2), n = 1.31,
-550 nm, inclination 30 deg (ki = (cos30, -sin30, 0)), identity orientation, seed 12345,
-1e8 rays, at most 12 internal interactions (the residual is reported), 512 x 1024 (u, phi)
-cells, FP32 trace, FP64 histogram flush and CDF.  A step is one record: trace + bin of all
-rays and the stored CDF.  With N ranks (torchrun), every rank traces its own 1e8-ray shard
-of one record (weak scaling), the FP64 histograms are summed with one NCCL all-reduce, and
-rank 0 builds the CDF.
+Default workload (drop, the configuration the headline metric is quoted on): an oblate water
+drop of equal-volume radius 1.5 mm with r/a = 1 - 0.08 cos(chi) - 0.02 cos(2 chi) + 0.005 cos(3 chi),
+650 nm, n = IAPWS R9-97 water at 20 C (binary32, as the solver holds it), inclination 20 deg,
+1e8 rays sampled over the drop's bounding disk (seed 12345), at most 10 internal interactions
+(the residual is reported), 900 x 1800 (u, phi) cells, analytic Fraunhofer diffraction stage,
+FP32 trace, FP64 histogram flush and CDF.  A step is one record: projected area (CPU FP64),
+trace + bin of all rays, diffraction rows and the stored CDF.
+Workload hex (--workload hex): the hexagonal ice column (circumradius 0.05 mm, length 0.2 mm,
+n = 1.31, 550 nm, ki = (cos30, -sin30, 0), 1e8 rays, 12 interactions, 512 x 1024 cells).
+
+With N ranks (torchrun) every rank traces its own 1e8-ray shard of one record (weak scaling),
+the FP64 histograms are summed with one NCCL all-reduce, and rank 0 finishes the record.
 
 Timing: CUDA events on the library's stream, W untimed warm-up steps, K timed steps, each
 bracketed by barrier + synchronize; an L2 flush (a 256 MiB write) separates timed steps;
-max over ranks.  `value` has inputs resident in HBM; `e2e` goes through the public
-host-buffer entry (icp_hex_generate) with the host<->device copies inside the timed region.
+max over ranks.  `value` keeps the outputs in HBM (icp_drop_generate_device); `e2e` goes
+through the public host-buffer entry (icp_drop_generate / icp_hex_generate) with the
+host<->device copies inside the timed region.
 """
 from __future__ import annotations
 
@@ -33,11 +39,17 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 CFG = dict(R=0.05, L=0.2, ki=(0.8660254037844387, -0.5, 0.0), n=1.31, nt=512, np=1024, hits=12, seed=12345)
-METRIC = "rays/s (hex column record: 1e8 rays traced, binned and stored as a CDF)"
-# Algorithmic FP32 work counted from the trace kernel source (flops per event; div/sqrt/rsqrt
-# and atan2 counted as one op each): entry = RNG-free geometry 20 + Fresnel/Stokes split 150
-# + binning 80; internal interaction = nearest-plane search 66 + split 150 + binning 80.
+DROP = dict(radius=1.5, coefficients=(0.0, -0.08, -0.02, 0.005, 0.0, 0.0, 0.0, 0.0), wavelength=650.0, incl=20.0,
+            nt=900, np=1800, hits=10, seed=12345)
+METRIC = "rays/s (one phase-function record: rays traced, binned and stored as a CDF)"
+# Algorithmic FP32 work counted from the trace kernel source (flops per event; div/sqrt/rsqrt,
+# sincospi and atan2 counted as one op each).  Prism: entry = geometry 20 + Fresnel/Stokes split
+# 150 + binning 80; internal interaction = nearest-plane search 66 + split 150 + binning 80.
 FLOP_ENTRY, FLOP_INTERACTION = 250.0, 296.0
+# Drop: every sampled ray = disk point 20 + bounding-sphere roots 12; entry of a hit = normal 105
+# + split 150 + binning 80; internal interaction = bounding-sphere roots 12 + normal 105 + split
+# 150 + binning 80; each Newton evaluation of the surface gauge (Chebyshev R, dR/dmu) = 110.
+FLOP_DROP_RAY, FLOP_DROP_ENTRY, FLOP_DROP_INTERACTION, FLOP_DROP_GAUGE = 32.0, 335.0, 347.0, 110.0
 
 
 def _env_rank():
@@ -103,7 +115,7 @@ def reference_sample(rays_per_proc: int, procs: int) -> dict:
     return {"rays": rays, "seconds": wall, "rays_per_s": rays / wall, "procs": procs}
 
 
-def run_reference(a) -> None:
+def run_reference_hex(a) -> None:
     rank, world, _ = _env_rank()
     if rank != 0:
         return
@@ -124,6 +136,78 @@ def run_reference(a) -> None:
     print(json.dumps(line), flush=True)
 
 
+def _drop_reference_inputs() -> dict:
+    """Interior index (the reference's water model at 650 nm, 20 C, as binary32), the incident
+    direction the reference CLI builds, and this record's sampling hit fraction (the reference's
+    projected area over the bounding-disk area)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import numpy as np
+
+    import oracle
+
+    d = DROP
+    n = float(np.float32(oracle.ref_drop_lines("water", ["650.0 20.0 101325.0"])[0][0]))
+    a = math.radians(d["incl"])
+    k = (float(np.float32(math.cos(a))), float(np.float32(-math.sin(a))), 0.0)
+    area = oracle.ref_drop_lines("area", [" ".join(repr(float(x)) for x in (*d["coefficients"], d["radius"],
+                                                                           *oracle.drop_frame(d["incl"])[0]))])[0][0]
+    disk = oracle.drop_geometry(d["coefficients"], d["radius"]).disk_area_mm2
+    return {"n": n, "k": k, "hit_fraction": area / disk}
+
+
+def reference_drop_sample(grid: int, procs: int, inputs: dict) -> dict:
+    """The reference's CPU drop tracer (RaindropPathTracer: R, TT, TRT, TRRT per lattice vertex,
+    binary32, oracle/_ref/ref_drop_harness built from its sources) over a grid x grid lattice,
+    one process per core on disjoint row slices.  Rays/s are its hit rays per second divided by
+    this record's hit fraction, i.e. sampled rays of this record per second at the reference's
+    cost per hit (its misses are cheaper and its chain stops after three internal hits)."""
+    exe = ROOT / "oracle" / "_ref" / "ref_drop_harness"
+    if not exe.exists():
+        raise FileNotFoundError(exe)
+    d = DROP
+    rows = (grid + procs - 1) // procs
+    args = [str(exe), "time", repr(d["radius"]), "0", repr(inputs["n"]), *map(repr, inputs["k"]), str(grid)]
+    t0 = time.perf_counter()
+    ps = [subprocess.Popen(args + [str(i * rows), str(rows), *map(repr, d["coefficients"])], stdout=subprocess.PIPE,
+                           text=True) for i in range(procs) if i * rows < grid]
+    outs = [p.communicate()[0].split() for p in ps]
+    wall = time.perf_counter() - t0
+    vertices = sum(int(o[0]) for o in outs)
+    hits = sum(int(o[1]) for o in outs)
+    return {"vertices": vertices, "hits": hits, "seconds": wall, "procs": len(ps),
+            "rays_per_s": hits / wall / inputs["hit_fraction"]}
+
+
+def _drop_public() -> dict:
+    d = DROP
+    return {"radius_mm": d["radius"], "shape_coefficients": list(d["coefficients"]), "wavelength_nm": d["wavelength"],
+            "inclination_deg": d["incl"], "cells": [d["nt"], d["np"]], "max_internal_hits": d["hits"],
+            "seed": d["seed"], "diffraction": "analytic_fraunhofer", "material": "water_iapws_r9_97_20C"}
+
+
+def run_reference_drop(a) -> None:
+    rank, world, _ = _env_rank()
+    if rank != 0:
+        return
+    procs = os.cpu_count() or 1
+    inputs = _drop_reference_inputs()
+    grid = int(a.ref_grid)
+    for _ in range(a.warmup):
+        reference_drop_sample(max(64, grid // 8), procs, inputs)
+    vals = [reference_drop_sample(grid, procs, inputs) for _ in range(a.steps)]
+    v = sum(x["rays_per_s"] * x["seconds"] for x in vals) / sum(x["seconds"] for x in vals)
+    sample = (f"{grid}x{grid} lattice per step ({vals[0]['hits']} hits), {vals[0]['procs']} processes; reference "
+              f"RaindropPathTracer (R, TT, TRT, TRRT, binary32) compiled from its sources; rays/s = hit rays/s / "
+              f"{inputs['hit_fraction']:.4f} (this record's hit fraction)")
+    line = {"metric": METRIC, "value": v, "unit": "rays/s", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": 1e3 * sum(x["seconds"] for x in vals) / len(vals), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "oblate_drop_config2", **_drop_public()}, "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "rays/s", "cores": procs, "kind": "reference", "sample": sample},
+            "e2e": {"value": v, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 def _cfg_public() -> dict:
     c = CFG
     return {"circumradius_mm": c["R"], "length_mm": c["L"], "ki": list(c["ki"]), "interior_index": c["n"],
@@ -131,7 +215,7 @@ def _cfg_public() -> dict:
 
 
 # ----------------------------------------------------------------------------- B200 arm
-def run_b200(a) -> None:
+def run_b200_hex(a) -> None:
     import ctypes as C
 
     import numpy as np
@@ -349,12 +433,321 @@ def run_b200(a) -> None:
         dist.destroy_process_group()
 
 
+def batch_records(I, count: int = 256, seed: int = 20260101, rays_max: float = 6e7, rays_min: float = 1e6) -> list:
+    """Drop records of the batched workload: radius log-uniform in [0.1, 3] mm, wavelength uniform
+    in [400, 700] nm, inclination uniform in [-90, 90] deg, Table-I shapes, water at 20 C, rays
+    proportional to the projected area (rays_max for the area of a 3 mm disk), clipped."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    specs = []
+    for _ in range(count):
+        radius = float(np.exp(rng.uniform(np.log(0.1), np.log(3.0))))
+        lam = float(rng.uniform(400.0, 700.0))
+        incl = float(rng.uniform(-90.0, 90.0))
+        shape = I.RaindropShape.make(float(np.float32(radius))).coefficients
+        n = float(np.float32(I.evaluate_water_optics(lam).refractive_index))
+        area = I.compute_projected_area(shape, float(np.float32(radius)), I.drop_frame(incl)[0])
+        rays = int(min(rays_max, max(rays_min, round(rays_max * area / (math.pi * 9.0)))))
+        specs.append(I.DropSpec(shape, float(np.float32(radius)), n, rays, seed=int(rng.integers(1, 2**63)),
+                                inclination_deg=incl, wavelength_nm=lam, diffraction=True))
+    return specs
+
+
+def run_batched(I, ctx, stream, a, nt: int, np_: int) -> dict:
+    """Batched records: one autotuned, graph-captured persistent launch per batch (device-resident
+    outputs), timed with CUDA events on the library stream; then the same records through the
+    single-record entry one after another (the plain path) for records/s at equal work."""
+    import ctypes as C
+
+    import torch
+
+    specs = batch_records(I, a.batch_records)
+    rays = sum(sp.rays for sp in specs)
+    s = I.batch_settings(nt, np_, max_internal_hits=DROP["hits"], precision=I.ICP_FP32, use_graph=True)
+    tuned_rate = I.autotune_drop_batch(ctx, specs, s)
+    n = len(specs)
+    phi = torch.empty(n * (np_ + 1), dtype=torch.float64, device="cuda")
+    theta = torch.empty(n * np_ * (nt + 1), dtype=torch.float64, device="cuda")
+    items = I._items(specs)
+    reps = (I.DropReport * n)()
+    launches0 = I.kernel_launches()
+
+    def one_batch():
+        I.check(I.LIB.icp_drop_batch_generate_device(ctx.handle, items, n, C.byref(s), C.c_void_p(phi.data_ptr()),
+                                                     C.c_void_p(theta.data_ptr()), reps))
+
+    one_batch()  # warm-up (captures and instantiates the graph)
+    times = []
+    for _ in range(a.batch_steps):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        one_batch()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1) / 1e3)
+    launches = (I.kernel_launches() - launches0) // (a.batch_steps + 1)
+    t = sum(times) / len(times)
+    tv_ok = all(r.cdf.status == 0 for r in reps)
+    # plain: the same records one by one through the single-record device entry
+    rec_phi = torch.empty(np_ + 1, dtype=torch.float64, device="cuda")
+    rec_theta = torch.empty(np_ * (nt + 1), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for sp in specs:
+        r = I._drop_args(sp.coefficients, sp.radius_mm, sp.inclination_deg, sp.interior_index, sp.rays, sp.seed, nt,
+                         np_, nt, np_, 1.0, DROP["hits"], 1e-12, I.ICP_FP32, 1e-10, sp.wavelength_nm, True)
+        rr = I.DropReport()
+        I.check(I.LIB.icp_drop_generate_device(ctx.handle, C.byref(r), C.c_void_p(rec_phi.data_ptr()),
+                                               C.c_void_p(rec_theta.data_ptr()), None, C.byref(rr)))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_plain = e0.elapsed_time(e1) / 1e3
+    return {"workload": "batched_drop_records_config4", "records": n, "rays": rays, "seed": 20260101,
+            "cells": [nt, np_], "max_internal_hits": DROP["hits"], "diffraction": "analytic_fraunhofer",
+            "ms_per_batch": 1e3 * t, "rays_per_s": rays / t, "records_per_s": n / t,
+            "plain_loop": {"seconds": t_plain, "rays_per_s": rays / t_plain, "records_per_s": n / t_plain},
+            "speedup_vs_plain_loop": t_plain / t, "cuda_graph": True, "kernel_launches_per_batch": launches,
+            "tuned": {"block_threads": s.block_threads, "chunk_rays": s.chunk_rays,
+                      "sample_rays_per_s": tuned_rate}, "all_records_pass_cdf_audits": tv_ok}
+
+
+def _peaks() -> dict:
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except (OSError, ValueError):
+        return {}
+
+
+def run_b200_drop(a) -> None:
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    import ice_crystal_phase_b200 as I
+
+    rank, world, local = _env_rank()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    ctx = I.Context(local)
+    stream = torch.cuda.ExternalStream(I.LIB.icp_context_stream(ctx.handle))
+    torch.cuda.set_stream(stream)
+    d = DROP
+    nt, np_ = d["nt"], d["np"]
+    rays = int(a.rays)
+    n_int = float(np.float32(I.evaluate_water_optics(d["wavelength"]).refractive_index))
+    tuning = I.Tuning(a.block_threads, 0, a.hash_slots, 0)
+    rec = I._drop_args(d["coefficients"], d["radius"], d["incl"], n_int, rays * world, d["seed"], nt, np_, nt, np_,
+                       1.0, d["hits"], 1e-12, I.ICP_FP32, 1e-10, d["wavelength"], True, tuning=tuning)
+    grid = I.make_drop_grid(nt, np_, d["incl"])
+    g = grid.abi()
+    edges = torch.from_numpy(grid.edges).cuda()
+    mass = torch.zeros(nt * np_, dtype=torch.float64, device="cuda")
+    phi = torch.empty(np_ + 1, dtype=torch.float64, device="cuda")
+    theta = torch.empty(np_ * (nt + 1), dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    weight = I.sampling_area(d["coefficients"], d["radius"]) / float(rays * world)
+    pole = torch.zeros(3, dtype=torch.float64, device="cuda")
+    policy = rec.policy
+
+    def step():
+        """One record; returns (trace stats of this rank, record report or None)."""
+        if world == 1:
+            rep = I.DropReport()
+            I.check(I.LIB.icp_drop_generate_device(ctx.handle, C.byref(rec), C.c_void_p(phi.data_ptr()),
+                                                   C.c_void_p(theta.data_ptr()), None, C.byref(rep)))
+            return rep.trace, rep
+        mass.zero_()
+        s = I.TraceStats()
+        I.check(I.LIB.icp_drop_trace_bin(ctx.handle, C.byref(rec), rank * rays, rays, weight, C.byref(g),
+                                         C.c_void_p(edges.data_ptr()), C.c_void_p(mass.data_ptr()), C.byref(s)))
+        pole[0], pole[1] = weight * s.forward_pole, weight * s.backward_pole
+        pole[2] = weight * (s.rays - s.missed)
+        dist.all_reduce(mass)
+        dist.all_reduce(pole)
+        if rank == 0:
+            rows = torch.from_numpy(I.diffraction_rows(grid.edges, float(pole[2]), d["wavelength"])).cuda()
+            mass.view(nt, np_).add_(rows[:, None] / np_)
+            crep = I.CdfReport()
+            I.check(I.LIB.icp_phase_cdf_build(ctx.handle, C.c_void_p(mass.data_ptr()), 0, nt, np_, float(pole[0]),
+                                              float(pole[1]), nt, np_, C.byref(policy), C.c_void_p(phi.data_ptr()),
+                                              C.c_void_p(theta.data_ptr()), C.byref(crep)))
+        return s, None
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(a.warmup):
+        step()
+    launches0 = I.kernel_launches()
+    times, stats_all, reps = [], [], []
+    with ClockSampler(local) as clocks:
+        for _ in range(a.steps):
+            flush.fill_(1.0)
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st, rp = step()
+            e1.record(stream)
+            barrier()
+            times.append(e0.elapsed_time(e1) / 1e3)
+            stats_all.append(st)
+            reps.append(rp)
+    launches = I.kernel_launches() - launches0
+    t_local = torch.tensor([sum(times)], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t_local, op=dist.ReduceOp.MAX)
+    t_step = float(t_local) / a.steps
+    value = rays * world / t_step
+
+    # dominant kernel alone (drop trace+bin, FP32) on the same stream, for the roofline
+    k_times, ks = [], None
+    for _ in range(2):
+        flush.fill_(1.0)
+        barrier()
+        mass.zero_()
+        ks = I.TraceStats()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        I.check(I.LIB.icp_drop_trace_bin(ctx.handle, C.byref(rec), rank * rays, rays, weight, C.byref(g),
+                                         C.c_void_p(edges.data_ptr()), C.c_void_p(mass.data_ptr()), C.byref(ks)))
+        e1.record(stream)
+        barrier()
+        k_times.append(e0.elapsed_time(e1) / 1e3)
+    t_kernel = min(k_times)
+    hits = ks.rays - ks.missed
+    flops = (FLOP_DROP_RAY * ks.rays + FLOP_DROP_ENTRY * hits + FLOP_DROP_INTERACTION * ks.encounters
+             + FLOP_DROP_GAUGE * ks.gauge_evals)
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    clk = clocks.summary()
+    mhz = clk["sm_mhz"] or 1965.0
+    fp32_peak = sms * 128 * 2 * mhz * 1e6 / 1e12
+    achieved = flops / t_kernel / 1e12
+
+    cdf_bytes = 8 * nt * np_ + 8 * np_ * (nt + 1) + 8 * (np_ + 1)
+    cdf_t = []
+    if rank == 0:
+        for _ in range(3):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            crep = I.CdfReport()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            I.check(I.LIB.icp_phase_cdf_build(ctx.handle, C.c_void_p(mass.data_ptr()), 0, nt, np_, 0.0, 0.0, nt, np_,
+                                              C.byref(policy), C.c_void_p(phi.data_ptr()),
+                                              C.c_void_p(theta.data_ptr()), C.byref(crep)))
+            e1.record(stream)
+            torch.cuda.synchronize()
+            cdf_t.append(e0.elapsed_time(e1) / 1e3)
+    hbm = _peaks().get("hbm_gbs", 6650.0)
+
+    # e2e through the public host-buffer entry (one whole record per step, N=1)
+    e2e_value = None
+    ph = torch.empty(np_ + 1, dtype=torch.float64).pin_memory()
+    th = torch.empty(np_ * (nt + 1), dtype=torch.float64).pin_memory()
+    uh = torch.empty(nt + 1, dtype=torch.float64).pin_memory()
+    if world == 1:
+        e2e_times = []
+        for i in range(a.steps + 1):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            rr = I.DropReport()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            I.check(I.LIB.icp_drop_generate(ctx.handle, C.byref(rec), C.cast(C.c_void_p(ph.data_ptr()), I._D),
+                                            C.cast(C.c_void_p(th.data_ptr()), I._D),
+                                            C.cast(C.c_void_p(uh.data_ptr()), I._D), C.byref(rr)))
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if i:
+                e2e_times.append(e0.elapsed_time(e1) / 1e3)
+        e2e_value = rays / (sum(e2e_times) / len(e2e_times))
+    h2d = 8 * (nt + 1) + 8 * nt  # u edges + diffraction rows
+    d2h = 8 * (np_ + 1) + 8 * np_ * (nt + 1) + 256 + 128  # CDF + trace counters + CDF report
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        try:
+            procs = os.cpu_count() or 1
+            inputs = _drop_reference_inputs()
+            rb = reference_drop_sample(int(a.ref_grid), procs, inputs)
+            cpu = {"value": rb["rays_per_s"], "unit": "rays/s", "cores": rb["procs"], "kind": "reference",
+                   "sample": f"{a.ref_grid}x{a.ref_grid} lattice ({rb['hits']} hit rays, {rb['seconds']:.1f} s), "
+                             "reference RaindropPathTracer (R, TT, TRT, TRRT, binary32) compiled from its sources; "
+                             f"rays/s = hit rays/s / {inputs['hit_fraction']:.4f} (this record's hit fraction)"}
+        except (OSError, ValueError, IndexError) as e:
+            cpu = {"value": None, "unit": "rays/s", "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
+
+    batched = None
+    if world == 1 and a.batch_records > 0:
+        batched = run_batched(I, ctx, stream, a, nt, np_)
+
+    s0 = stats_all[-1]
+    r0 = reps[-1]
+    line = {
+        "metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1e3 * t_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "oblate_drop_config2", **_drop_public(), "interior_index": n_int,
+                   "rays_per_gpu": rays, "l2": "flushed between timed steps (256 MiB write)", "trace_precision": "fp32",
+                   "parallelism": f"ray shards x{world}, NCCL all-reduce of FP64 histogram" if world > 1 else "1 GPU"},
+        "records_per_s": 1.0 / t_step,
+        "e2e": {"value": e2e_value, "unit": "rays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "roofline": {"kernel": "trace_bin_kernel<float, DropGeo<float>>", "bound": "fp32_simt", "achieved": achieved,
+                     "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+                     "peak_note": f"derived: {sms} SMs x 128 FP32 lanes x 2 x {mhz:.0f} MHz (median SM clock under load)",
+                     "flops_per_ray": flops / max(1, ks.rays), "kernel_ms": 1e3 * t_kernel,
+                     "interactions_per_hit": ks.encounters / max(1, hits),
+                     "gauge_evaluations_per_hit": ks.gauge_evals / max(1, hits)},
+        "roofline_cdf": ({"kernel": "cdf_build_kernel", "bound": "hbm", "achieved": cdf_bytes / min(cdf_t) / 1e9,
+                          "peak": hbm, "unit": "GB/s", "frac": cdf_bytes / min(cdf_t) / 1e9 / hbm, "traffic": None,
+                          "algorithmic_bytes": cdf_bytes, "kernel_us": 1e6 * min(cdf_t),
+                          "peak_note": "MEASURED_PEAKS.json hbm_gbs (of measured)"} if cdf_t else None),
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "gpu_launches": launches,
+        "trace": {"outputs_per_ray": s0.outputs / max(1, s0.rays), "missed_fraction": s0.missed / max(1, s0.rays),
+                  "unresolved_fraction": s0.unresolved / max(1, s0.rays - s0.missed),
+                  "fallback_adds": s0.fallback_adds},
+    }
+    if batched is not None:
+        line["batched"] = batched
+    if r0 is not None:
+        line["record"] = {"g": r0.cdf.g_stored, "projected_area_mm2": r0.projected_area_mm2,
+                          "incident_area_mm2": r0.incident_area_mm2, "diffraction_mm2": r0.diffraction_area_mm2,
+                          "histogram_relative_error": r0.histogram_relative_error, "cdf_l1": r0.cdf.l1_error,
+                          "trace_s": r0.seconds_trace, "cdf_s": r0.seconds_cdf}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main() -> None:
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    p.add_argument("--workload", choices=["drop", "hex"], default="drop")
+    p.add_argument("--ref-grid", type=int, default=1025, help="reference drop lattice size per step")
+    p.add_argument("--block-threads", type=int, default=0, help="trace block size (0 = library default)")
+    p.add_argument("--batch-records", type=int, default=256, help="records of the batched measurement (0 = skip)")
+    p.add_argument("--batch-steps", type=int, default=3)
+    p.add_argument("--hash-slots", type=int, default=0, help="shared histogram slots (0 = default, 1 = none)")
     p.add_argument("--rays", type=float, default=1e8)
     p.add_argument("--ref-rays", type=float, default=1.6e6, help="reference rays per step (all processes)")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -362,9 +755,9 @@ def main() -> None:
     if a.warmup < 3:
         a.warmup = 3
     if a.impl == "reference":
-        run_reference(a)
+        (run_reference_drop if a.workload == "drop" else run_reference_hex)(a)
     else:
-        run_b200(a)
+        (run_b200_drop if a.workload == "drop" else run_b200_hex)(a)
 
 
 if __name__ == "__main__":

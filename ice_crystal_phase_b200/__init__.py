@@ -73,7 +73,8 @@ class TraceStats(C.Structure):
                 ("max_interface_balance", C.c_double), ("rays", C.c_uint64), ("outputs", C.c_uint64),
                 ("status_counts", C.c_uint64 * 8), ("rejected_rays", C.c_uint64), ("snapped", C.c_uint64),
                 ("near_edge", C.c_uint64), ("fallback_adds", C.c_uint64), ("max_batch_outputs", C.c_uint64),
-                ("invalid", C.c_uint64), ("encounters", C.c_uint64), ("missed", C.c_uint64)]
+                ("invalid", C.c_uint64), ("encounters", C.c_uint64), ("missed", C.c_uint64),
+                ("gauge_evals", C.c_uint64)]
 
     def as_dict(self) -> dict:
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "status_counts"}
@@ -152,6 +153,20 @@ class DropReport(C.Structure):
                 ("seconds_cdf", C.c_double)]
 
 
+class DropItem(C.Structure):
+    _fields_ = [("radius_mm", C.c_double), ("coefficients", C.c_double * 8), ("inclination_deg", C.c_double),
+                ("interior_index", C.c_double), ("wavelength_nm", C.c_double), ("rays", C.c_uint64),
+                ("seed", C.c_uint64), ("diffraction", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class BatchSettings(C.Structure):
+    _fields_ = [("nt", C.c_uint32), ("np", C.c_uint32), ("ct", C.c_uint32), ("cp", C.c_uint32),
+                ("max_internal_hits", C.c_uint32), ("precision", C.c_uint32), ("exterior_index", C.c_double),
+                ("tail_tolerance", C.c_double), ("balance_tolerance", C.c_double), ("policy", CdfPolicy),
+                ("block_threads", C.c_uint32), ("blocks_per_sm", C.c_uint32), ("chunk_rays", C.c_uint32),
+                ("use_graph", C.c_uint32)]
+
+
 # ---------------------------------------------------------------- library loading
 _P = C.c_void_p
 _D = C.POINTER(C.c_double)
@@ -188,6 +203,12 @@ _FUNCS = {
     "icp_drop_trace_bin": (C.c_int, [_P, C.POINTER(DropRecordArgs), C.c_uint64, C.c_uint64, C.c_double,
                                      C.POINTER(Grid), _P, _P, C.POINTER(TraceStats)]),
     "icp_drop_generate": (C.c_int, [_P, C.POINTER(DropRecordArgs), _D, _D, _D, C.POINTER(DropReport)]),
+    "icp_drop_generate_device": (C.c_int, [_P, C.POINTER(DropRecordArgs), _P, _P, _P, C.POINTER(DropReport)]),
+    "icp_drop_batch_generate_device": (C.c_int, [_P, C.POINTER(DropItem), C.c_uint32, C.POINTER(BatchSettings), _P, _P,
+                                                 C.POINTER(DropReport)]),
+    "icp_drop_batch_generate": (C.c_int, [_P, C.POINTER(DropItem), C.c_uint32, C.POINTER(BatchSettings), _D, _D, _D,
+                                          C.POINTER(DropReport)]),
+    "icp_drop_batch_autotune": (C.c_int, [_P, C.POINTER(DropItem), C.c_uint32, C.POINTER(BatchSettings), _D]),
 }
 
 
@@ -719,3 +740,72 @@ def generate_drop_record(ctx: Context, coefficients, radius_mm: float, interior_
     check(LIB.icp_drop_generate(ctx.handle, C.byref(r), phi.ctypes.data_as(_D), theta.ctypes.data_as(_D),
                                 u.ctypes.data_as(_D), C.byref(rep)))
     return DropRecordResult(phi, theta.reshape(cp, ct + 1), u, rep, make_drop_grid(nt, np_, inclination_deg))
+
+
+# ---------------------------------------------------------------- batched drop records
+@dataclass
+class DropSpec:
+    """One record of a batch (the per-record parameters of a rainbow_generate run)."""
+    coefficients: list
+    radius_mm: float
+    interior_index: float
+    rays: int
+    seed: int = 12345
+    inclination_deg: float = 20.0
+    wavelength_nm: float = 0.0
+    diffraction: bool = False
+
+
+def batch_settings(nt: int, np_: int, ct: int | None = None, cp: int | None = None, max_internal_hits: int = 1024,
+                   precision: int = ICP_FP32, exterior_index: float = 1.0, tail_tolerance: float = 1e-12,
+                   balance_tolerance: float = 1e-10, max_l1_error: float = 1e-10, max_lost_mass: float = 1e-12,
+                   max_coarsening_tv: float = 1.0, block_threads: int = 0, blocks_per_sm: int = 0,
+                   chunk_rays: int = 0, use_graph: bool = True) -> BatchSettings:
+    s = BatchSettings()
+    s.nt, s.np, s.ct, s.cp = nt, np_, ct or nt, cp or np_
+    s.max_internal_hits, s.precision = max_internal_hits, precision
+    s.exterior_index, s.tail_tolerance, s.balance_tolerance = exterior_index, tail_tolerance, balance_tolerance
+    s.policy = CdfPolicy(max_l1_error, max_lost_mass, max_coarsening_tv)
+    s.block_threads, s.blocks_per_sm, s.chunk_rays, s.use_graph = block_threads, blocks_per_sm, chunk_rays, int(use_graph)
+    return s
+
+
+def _items(specs) -> C.Array:
+    arr = (DropItem * len(specs))()
+    for i, sp in enumerate(specs):
+        arr[i].radius_mm = sp.radius_mm
+        arr[i].coefficients = _c8(sp.coefficients)
+        arr[i].inclination_deg, arr[i].interior_index = sp.inclination_deg, sp.interior_index
+        arr[i].wavelength_nm, arr[i].rays, arr[i].seed = sp.wavelength_nm, sp.rays, sp.seed
+        arr[i].diffraction = int(bool(sp.diffraction))
+    return arr
+
+
+@dataclass
+class DropBatchResult:
+    phi: np.ndarray          # (records, cp + 1)
+    theta: np.ndarray        # (records, cp, ct + 1)
+    u_edges: np.ndarray
+    reports: list
+
+
+def generate_drop_batch(ctx: Context, specs: list, settings: BatchSettings) -> DropBatchResult:
+    """Many drop records in one persistent launch (icp_drop_batch_generate, host outputs)."""
+    n = len(specs)
+    items = _items(specs)
+    phi = np.empty(n * (settings.cp + 1))
+    theta = np.empty(n * settings.cp * (settings.ct + 1))
+    u = np.empty(settings.ct + 1)
+    reps = (DropReport * n)()
+    check(LIB.icp_drop_batch_generate(ctx.handle, items, n, C.byref(settings), phi.ctypes.data_as(_D),
+                                      theta.ctypes.data_as(_D), u.ctypes.data_as(_D), reps))
+    return DropBatchResult(phi.reshape(n, settings.cp + 1), theta.reshape(n, settings.cp, settings.ct + 1), u,
+                           list(reps))
+
+
+def autotune_drop_batch(ctx: Context, specs: list, settings: BatchSettings) -> float:
+    """Times candidate block and chunk sizes on a bounded sample of the batch; stores the best
+    in ``settings`` (and in the context for later batches).  Returns the best rays/s."""
+    best = C.c_double()
+    check(LIB.icp_drop_batch_autotune(ctx.handle, _items(specs), len(specs), C.byref(settings), C.byref(best)))
+    return best.value

@@ -42,6 +42,8 @@ UNITS = {
     "icp_cdf.cu": ["-fmad=false"],
     "icp_capi.cu": ["-fmad=false"],
     "icp_capi_drop.cu": ["-fmad=false"],
+    "icp_drop_device.cu": ["-fmad=false"],
+    "icp_capi_batch.cu": ["-fmad=false"],
     "icp_cdf_static.cu": ["-fmad=false"],
 }
 

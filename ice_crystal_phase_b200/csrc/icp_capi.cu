@@ -102,6 +102,7 @@ int icp_context_create(int device, icp_context** out)
     cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->ev2);
     if (e != cudaSuccess) {
         icp_context_destroy(c);
         return fail(ICP_ERR_DEVICE, "icp_context_create: %s", cudaGetErrorString(e));
@@ -120,6 +121,7 @@ int icp_context_destroy(icp_context* c)
     for (Scratch* s : all) s->release();
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->ev2) cudaEventDestroy(c->ev2);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return ok();
@@ -246,7 +248,7 @@ void icp::stats_accumulate(const unsigned char* raw, icp_trace_stats* out)
         double axial;
         unsigned long long max_bal_bits, max_iface_bits;
         unsigned long long rays, outputs, status[8], rejected, snapped, near_edge, fallback, invalid;
-        unsigned long long encounters, missed;
+        unsigned long long encounters, missed, gauge_evals;
     } r;
     std::memcpy(&r, raw, sizeof r);
     auto fx = [](const unsigned long long* v) { return (std::ldexp((double)v[1], 64) + (double)v[0]) * 0x1p-44; };
@@ -270,6 +272,7 @@ void icp::stats_accumulate(const unsigned char* raw, icp_trace_stats* out)
     out->invalid += r.invalid;
     out->encounters += r.encounters;
     out->missed += r.missed;
+    out->gauge_evals += r.gauge_evals;
 }
 
 namespace {
@@ -375,7 +378,67 @@ extern "C" int icp_hex_trace_bin(icp_context* c, const icp_hex_node* n, const ic
 
 namespace {
 
-int choose_cw(icp_context* c, uint32_t ct, uint32_t cp, uint32_t& cw)
+int cdf_launch_common(icp_context* c, CdfLaunch& L, uint32_t ct, uint32_t cp)
+{
+    uint32_t cw = 0;
+    if (const int r = icp::choose_cdf_width(c, ct, cp, cw)) return r;
+    const uint32_t blocks = (cp + cw - 1) / cw;
+    ICP_CUDA(c->cdf_partial.ensure(cdf_partial_bytes() * blocks));
+    ICP_CUDA(c->cdf_colsum.ensure(sizeof(double) * cp));
+    ICP_CUDA(cudaMemsetAsync(L.sync, 0, 2 * sizeof(unsigned), c->stream));
+    ICP_CUDA(cudaMemsetAsync(L.report, 0, sizeof(CdfDeviceReport), c->stream));
+    L.colsum = (double*)c->cdf_colsum.ptr;
+    L.partial = c->cdf_partial.ptr;
+    L.cw = cw;
+    const int e = launch_cdf_build(L, c->stream);
+    ++g_launches;
+    if (e) return fail(ICP_ERR_DEVICE, "CDF launch failed: %s", cudaGetErrorString((cudaError_t)e));
+    return ICP_OK;
+}
+
+// Density input (kind 1) with host pole additions: the public entry's path.
+int cdf_enqueue_kind(icp_context* c, const double* d_values, uint32_t kind, uint32_t nt, uint32_t np, uint32_t ct,
+                     uint32_t cp, const double* d_edges, double fa, double ba, double* d_phi, double* d_theta)
+{
+    CdfLaunch L{};
+    L.values = d_values;
+    L.edges = d_edges;
+    L.phi = d_phi;
+    L.theta = d_theta;
+    L.report = (CdfDeviceReport*)c->cdf_report.ptr;
+    L.sync = (unsigned*)c->cdf_sync.ptr;
+    L.kind = kind;
+    L.nt = nt; L.np = np; L.ct = ct; L.cp = cp;
+    L.fwd_add = fa;
+    L.bwd_add = ba;
+    return cdf_launch_common(c, L, ct, cp);
+}
+
+} // namespace
+
+int icp::cdf_enqueue(icp_context* c, const double* d_values, uint32_t nt, uint32_t np, uint32_t ct, uint32_t cp,
+                     const double* d_edges, double fwd_add, double bwd_add, const unsigned long long* pole_fx,
+                     double pole_weight, const double* row_add, double* d_phi, double* d_theta,
+                     CdfDeviceReport* d_report, unsigned* d_sync)
+{
+    CdfLaunch L{};
+    L.values = d_values;
+    L.edges = d_edges;
+    L.phi = d_phi;
+    L.theta = d_theta;
+    L.report = d_report;
+    L.sync = d_sync;
+    L.kind = 0;
+    L.nt = nt; L.np = np; L.ct = ct; L.cp = cp;
+    L.fwd_add = fwd_add;
+    L.bwd_add = bwd_add;
+    L.pole_fx = pole_fx;
+    L.pole_weight = pole_weight;
+    L.row_add = row_add;
+    return cdf_launch_common(c, L, ct, cp);
+}
+
+int icp::choose_cdf_width(icp_context* c, uint32_t ct, uint32_t cp, uint32_t& cw)
 {
     // smallest strip width whose grid fits co-resident, at least ceil(cp / SMs)
     uint32_t w = std::max<uint32_t>(1u, (cp + c->sms - 1) / c->sms);
@@ -390,8 +453,6 @@ int choose_cw(icp_context* c, uint32_t ct, uint32_t cp, uint32_t& cw)
     }
     return fail(ICP_ERR_CAPACITY, "CDF strip for %u theta rows does not fit shared memory with a co-resident grid", ct);
 }
-
-} // namespace
 
 extern "C" int icp_phase_cdf_build(icp_context* c, const double* d_values, uint32_t kind, uint32_t nt, uint32_t np,
                                    double fwd, double bwd, uint32_t ct, uint32_t cp, const icp_cdf_policy* policy,
@@ -417,40 +478,27 @@ extern "C" int icp_phase_cdf_build(icp_context* c, const double* d_values, uint3
     ICP_CUDA(cudaSetDevice(c->device));
     std::vector<double> edges;
     if (!H::u_edges(nt, edges)) return fail(ICP_ERR_INVALID_ARGUMENT, "Angular cells cannot be represented in binary64.");
-    uint32_t cw = 0;
-    if (const int r = choose_cw(c, ct, cp, cw)) return r;
-    const uint32_t blocks = (cp + cw - 1) / cw;
     ICP_CUDA(c->rec_edges.ensure(sizeof(double) * (nt + 1)));
-    ICP_CUDA(c->cdf_partial.ensure(cdf_partial_bytes() * blocks));
     ICP_CUDA(c->cdf_report.ensure(sizeof(CdfDeviceReport)));
     ICP_CUDA(c->cdf_sync.ensure(2 * sizeof(unsigned)));
-    ICP_CUDA(c->cdf_colsum.ensure(sizeof(double) * cp));
     ICP_CUDA(cudaMemcpyAsync(c->rec_edges.ptr, edges.data(), sizeof(double) * (nt + 1), cudaMemcpyHostToDevice, c->stream));
-    ICP_CUDA(cudaMemsetAsync(c->cdf_sync.ptr, 0, 2 * sizeof(unsigned), c->stream));
-    ICP_CUDA(cudaMemsetAsync(c->cdf_report.ptr, 0, sizeof(CdfDeviceReport), c->stream));
-    CdfLaunch L{};
-    L.values = d_values;
-    L.edges = (const double*)c->rec_edges.ptr;
-    L.phi = d_phi;
-    L.theta = d_theta;
-    L.colsum = (double*)c->cdf_colsum.ptr;
-    L.partial = c->cdf_partial.ptr;
-    L.report = (CdfDeviceReport*)c->cdf_report.ptr;
-    L.sync = (unsigned*)c->cdf_sync.ptr;
-    L.kind = kind;
-    L.nt = nt;
-    L.np = np;
-    L.ct = ct;
-    L.cp = cp;
-    L.cw = cw;
-    L.fwd_add = fa;
-    L.bwd_add = ba;
-    const int e = launch_cdf_build(L, c->stream);
-    ++g_launches;
-    if (e) return fail(ICP_ERR_DEVICE, "CDF launch failed: %s", cudaGetErrorString((cudaError_t)e));
+    if (kind == 1) {
+        // density input: the kernel's mass conversion (kind 1) is only reached through here
+        if (const int e = cdf_enqueue_kind(c, d_values, kind, nt, np, ct, cp, (const double*)c->rec_edges.ptr, fa, ba,
+                                           d_phi, d_theta))
+            return e;
+    } else if (const int e = cdf_enqueue(c, d_values, nt, np, ct, cp, (const double*)c->rec_edges.ptr, fa, ba, nullptr, 0.0,
+                                         nullptr, d_phi, d_theta, (CdfDeviceReport*)c->cdf_report.ptr,
+                                         (unsigned*)c->cdf_sync.ptr))
+        return e;
     CdfDeviceReport r{};
     ICP_CUDA(cudaMemcpyAsync(&r, c->cdf_report.ptr, sizeof r, cudaMemcpyDeviceToHost, c->stream));
     ICP_CUDA(cudaStreamSynchronize(c->stream));
+    return icp::cdf_finish(r, p, report);
+}
+
+int icp::cdf_finish(const CdfDeviceReport& r, const icp_cdf_policy& p, icp_cdf_report* report)
+{
     if (r.timeout) return fail(ICP_ERR_TIMEOUT, "CDF grid barrier gave up waiting (co-residency violated?)");
     report->fine_mass = r.fine_mass;
     report->fine_axial = r.fine_axial;

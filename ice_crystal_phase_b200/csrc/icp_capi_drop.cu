@@ -44,22 +44,14 @@ int ok()
         if (e_ != cudaSuccess) return fail(ICP_ERR_DEVICE, "%s failed: %s", #call, cudaGetErrorString(e_)); \
     } while (0)
 
-// Adds rows[i] / np to every cell of row i (analytic diffraction stage).
-__global__ void add_rows(double* mass, const double* rows, uint32_t nt, uint32_t np)
-{
-    const uint64_t n = (uint64_t)nt * np;
-    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x)
-        mass[k] += rows[k / np] / np;
-}
+} // namespace
 
-bool sphere_of(const double c[8])
+bool icp::dropx::sphere_of(const double c[8])
 {
     for (int n = 1; n < 8; ++n)
         if (c[n] != 0) return false;
     return true;
 }
-
-} // namespace
 
 extern "C" int icp_water_index(double wavelength_nm, double temperature_c, double pressure_pa, double* index,
                                double* density)
@@ -125,7 +117,7 @@ extern "C" int icp_drop_diffraction_rows(const double* u_edges, uint32_t nt, dou
     return ok();
 }
 
-namespace {
+namespace icp::dropx {
 
 // Bounding radius of the sampling disk and the conservative outer radius (units of a).
 void drop_bounds(const double c[8], double& r_center, double& r_out)
@@ -153,7 +145,9 @@ int validate_record(const icp_drop_record* r)
     return ICP_OK;
 }
 
-} // namespace
+} // namespace icp::dropx
+
+using namespace icp::dropx;
 
 extern "C" int icp_drop_sampling_area(const double coefficients[8], double radius_mm, double* area_mm2)
 {
@@ -166,34 +160,13 @@ extern "C" int icp_drop_sampling_area(const double coefficients[8], double radiu
     return ok();
 }
 
-extern "C" int icp_drop_trace_bin(icp_context* c, const icp_drop_record* r, uint64_t first, uint64_t count,
-                                  double area_weight, const icp_grid* g, const double* d_edges, double* d_mass,
-                                  icp_trace_stats* stats)
+namespace icp::dropx {
+
+// Kernel description of one drop record (shared by the single-record and batched launches).
+HexLaunch drop_launch(const icp_drop_record* r, const icp_grid* g, const double* d_edges, const float* edges_f,
+                      double* d_mass, void* d_stats, double area_weight, uint32_t slots)
 {
-    if (!c || !r || !g || !d_edges || !d_mass || !stats) return fail(ICP_ERR_INVALID_ARGUMENT, "icp_drop_trace_bin: null argument");
-    if (const int v = validate_record(r)) return v;
-    if (first >= r->rays || count > r->rays - first) return fail(ICP_ERR_INVALID_ARGUMENT, "Batch is outside the ray range.");
-    if (!(area_weight > 0) || !H::finite(area_weight)) return fail(ICP_ERR_INVALID_ARGUMENT, "Invalid area weight.");
-    if (count == 0) return ok();
-    ICP_CUDA(cudaSetDevice(c->device));
     const auto F = H::drop_frame(r->inclination_deg);
-    const bool f32 = r->precision == ICP_FP32;
-    const uint32_t threads = r->tuning.block_threads ? r->tuning.block_threads : 256u;
-    if (threads < 64 || threads > 256 || threads % 32) return fail(ICP_ERR_INVALID_ARGUMENT, "block_threads must be 64..256, multiple of 32");
-    uint32_t slots = 4096u;
-    if (r->tuning.hash_slots) slots = r->tuning.hash_slots == 1 ? 0u : r->tuning.hash_slots;
-    if (slots & (slots - 1)) return fail(ICP_ERR_INVALID_ARGUMENT, "hash_slots must be a power of two");
-    int per_sm = f32 ? drop_blocks_per_sm_f32(slots, g->nt, threads) : drop_blocks_per_sm_f64(slots, g->nt, threads);
-    if (per_sm <= 0) return fail(ICP_ERR_DEVICE, "drop trace kernel cannot be resident");
-    if (r->tuning.blocks_per_sm) per_sm = std::min<int>(per_sm, (int)r->tuning.blocks_per_sm);
-    const uint32_t wpb = threads / 32;
-    uint64_t blocks = (uint64_t)per_sm * c->sms;
-    blocks = std::max<uint64_t>(1, std::min<uint64_t>(blocks, (count + 64ull * wpb - 1) / (64ull * wpb)));
-    const uint64_t piece = blocks * wpb * 65536ull;
-    ICP_CUDA(c->stats.ensure(hex_stats_bytes()));
-    ICP_CUDA(cudaMemsetAsync(c->stats.ptr, 0, hex_stats_bytes(), c->stream));
-    if (f32)
-        if (const int e = ensure_float_edges(c, d_edges, g->nt)) return e;
     HexLaunch L{};
     L.geometry = 1;
     std::memcpy(L.coeff, r->coefficients, sizeof L.coeff);
@@ -216,17 +189,52 @@ extern "C" int icp_drop_trace_bin(icp_context* c, const icp_drop_record* r, uint
     L.bal_tol = r->balance_tolerance;
     L.seed = r->seed;
     L.total = r->rays;
+    L.first = 0;
+    L.count = r->rays;
     L.max_hits = r->max_internal_hits;
     L.batch_size = 1u << 20;
     L.batch_out = nullptr;
     L.nt = g->nt;
     L.np = g->np;
     L.edges_d = d_edges;
-    L.edges_f = (const float*)c->edges_f.ptr;
+    L.edges_f = edges_f;
     L.mass = d_mass;
     L.to_mass = area_weight * 0x1p-44;
-    L.stats = c->stats.ptr;
+    L.stats = d_stats;
     L.hash_slots = slots;
+    return L;
+}
+
+// Drop exits spread continuously over the sphere, so a shared table of a few thousand cells
+// saturates within one block and only adds probes: by default exits go straight to the FP64
+// histogram (fire-and-forget L2 reductions).  A table can still be requested.
+int table_slots(const icp_tuning& t, uint32_t& slots)
+{
+    slots = 0u;
+    if (t.hash_slots) slots = t.hash_slots == 1 ? 0u : t.hash_slots;
+    if (slots & (slots - 1)) return fail(ICP_ERR_INVALID_ARGUMENT, "hash_slots must be a power of two");
+    return ICP_OK;
+}
+
+// Enqueues the trace of rays [first, first+count) into d_mass / d_stats (no synchronisation).
+int drop_trace_enqueue(icp_context* c, const icp_drop_record* r, uint64_t first, uint64_t count, double area_weight,
+                       const icp_grid* g, const double* d_edges, double* d_mass, void* d_stats)
+{
+    const bool f32 = r->precision == ICP_FP32;
+    const uint32_t threads = r->tuning.block_threads ? r->tuning.block_threads : 256u;
+    if (threads < 64 || threads > 256 || threads % 32) return fail(ICP_ERR_INVALID_ARGUMENT, "block_threads must be 64..256, multiple of 32");
+    uint32_t slots;
+    if (const int e = table_slots(r->tuning, slots)) return e;
+    int per_sm = f32 ? drop_blocks_per_sm_f32(slots, g->nt, threads) : drop_blocks_per_sm_f64(slots, g->nt, threads);
+    if (per_sm <= 0) return fail(ICP_ERR_DEVICE, "drop trace kernel cannot be resident");
+    if (r->tuning.blocks_per_sm) per_sm = std::min<int>(per_sm, (int)r->tuning.blocks_per_sm);
+    const uint32_t wpb = threads / 32;
+    uint64_t blocks = (uint64_t)per_sm * c->sms;
+    blocks = std::max<uint64_t>(1, std::min<uint64_t>(blocks, (count + 64ull * wpb - 1) / (64ull * wpb)));
+    const uint64_t piece = blocks * wpb * 65536ull;
+    if (f32)
+        if (const int e = ensure_float_edges(c, d_edges, g->nt)) return e;
+    HexLaunch L = drop_launch(r, g, d_edges, (const float*)c->edges_f.ptr, d_mass, d_stats, area_weight, slots);
     L.block_threads = threads;
     L.blocks = (uint32_t)blocks;
     for (uint64_t off = 0; off < count; off += piece) {
@@ -236,61 +244,45 @@ extern "C" int icp_drop_trace_bin(icp_context* c, const icp_drop_record* r, uint
         count_launch();
         if (e) return fail(ICP_ERR_DEVICE, "drop trace launch failed: %s", cudaGetErrorString((cudaError_t)e));
     }
-    std::vector<unsigned char> raw(hex_stats_bytes());
-    ICP_CUDA(cudaMemcpyAsync(raw.data(), c->stats.ptr, raw.size(), cudaMemcpyDeviceToHost, c->stream));
-    ICP_CUDA(cudaStreamSynchronize(c->stream));
-    stats_accumulate(raw.data(), stats);
-    return ok();
+    return ICP_OK;
 }
 
-extern "C" int icp_drop_generate(icp_context* c, const icp_drop_record* r, double* h_phi, double* h_theta, double* h_u,
-                                 icp_drop_report* rep)
+int grid_of(const icp_drop_record* r, icp_grid& g)
 {
-    if (!c || !r || !h_phi || !h_theta || !h_u || !rep) return fail(ICP_ERR_INVALID_ARGUMENT, "icp_drop_generate: null argument");
-    std::memset(rep, 0, sizeof *rep);
-    if (const int v = validate_record(r)) return v;
-    if (!r->nt || !r->np || (uint64_t)r->nt * r->np > 0xffffffffull || !r->ct || !r->cp || r->ct > r->nt ||
-        r->cp > r->np || r->nt % r->ct || r->np % r->cp)
-        return fail(ICP_ERR_INVALID_ARGUMENT, "CDF dimensions must divide the query dimensions without upsampling.");
-    if (r->diffraction && !(r->wavelength_nm > 0)) return fail(ICP_ERR_INVALID_ARGUMENT, "Diffraction needs a wavelength.");
-    ICP_CUDA(cudaSetDevice(c->device));
     const auto F = H::drop_frame(r->inclination_deg);
-    icp_grid g{};
+    g = icp_grid{};
     g.nt = r->nt;
     g.np = r->np;
     for (int i = 0; i < 3; ++i) {
         g.ki[i] = F.k[i];
         g.e0[i] = F.e0[i];
         g.e1[i] = F.e1[i];
-        rep->ki[i] = F.k[i];
-        rep->e0[i] = F.e0[i];
-        rep->e1[i] = F.e1[i];
     }
-    double area = 0;
-    try {
-        area = H::drop_projected_area(r->coefficients, r->radius_mm, F.k).area_mm2;
-    } catch (const std::exception& e) {
-        return fail(ICP_ERR_INVALID_ARGUMENT, "%s", e.what());
-    }
-    rep->projected_area_mm2 = area;
-    double disk_area = 0;
-    if (const int e = icp_drop_sampling_area(r->coefficients, r->radius_mm, &disk_area)) return e;
-    rep->sampled_area_mm2 = disk_area;
-    const double weight = disk_area / double(r->rays);
-    std::vector<double> edges;
-    if (!H::u_edges(r->nt, edges)) return fail(ICP_ERR_INVALID_ARGUMENT, "Angular cells cannot be represented in binary64.");
-    const uint64_t cells = (uint64_t)r->nt * r->np;
-    ICP_CUDA(c->rec_edges.ensure(sizeof(double) * (r->nt + 1)));
-    ICP_CUDA(c->rec_mass.ensure(sizeof(double) * cells));
-    ICP_CUDA(c->rec_phi.ensure(sizeof(double) * (r->cp + 1)));
-    ICP_CUDA(c->rec_theta.ensure(sizeof(double) * (size_t)r->cp * (r->ct + 1)));
-    ICP_CUDA(cudaMemcpyAsync(c->rec_edges.ptr, edges.data(), sizeof(double) * (r->nt + 1), cudaMemcpyHostToDevice, c->stream));
-    ICP_CUDA(cudaMemsetAsync(c->rec_mass.ptr, 0, sizeof(double) * cells, c->stream));
-    ICP_CUDA(cudaEventRecord(c->ev0, c->stream));
+    return ICP_OK;
+}
+
+int validate_grid(const icp_drop_record* r)
+{
+    if (!r->nt || !r->np || (uint64_t)r->nt * r->np > 0xffffffffull || !r->ct || !r->cp || r->ct > r->nt ||
+        r->cp > r->np || r->nt % r->ct || r->np % r->cp)
+        return fail(ICP_ERR_INVALID_ARGUMENT, "CDF dimensions must divide the query dimensions without upsampling.");
+    if (r->diffraction && !(r->wavelength_nm > 0 && H::finite(r->wavelength_nm)))
+        return fail(ICP_ERR_INVALID_ARGUMENT, "Diffraction needs a wavelength.");
+    const icp_cdf_policy& p = r->policy;
+    if (!(H::finite(p.max_l1_error) && p.max_l1_error >= 0 && p.max_l1_error <= 2 && H::finite(p.max_lost_mass) &&
+          p.max_lost_mass >= 0 && p.max_lost_mass <= 1 && H::finite(p.max_coarsening_tv) && p.max_coarsening_tv >= 0 &&
+          p.max_coarsening_tv <= 1))
+        return fail(ICP_ERR_INVALID_ARGUMENT, "Invalid CDF quality policy.");
+    return ICP_OK;
+}
+
+// Host part of a record's report from its trace counters, CDF report and diffraction power.
+int finish_report(const icp_drop_record* r, const unsigned char* raw_stats, const CdfDeviceReport& cdf, double power,
+                  double weight, icp_drop_report* rep)
+{
     icp_trace_stats& T = rep->trace;
-    if (const int e = icp_drop_trace_bin(c, r, 0, r->rays, weight, &g, (const double*)c->rec_edges.ptr,
-                                         (double*)c->rec_mass.ptr, &T))
-        return e;
+    T = icp_trace_stats{};
+    stats_accumulate(raw_stats, &T);
     const uint64_t hits = T.rays - T.missed;
     rep->incident_area_mm2 = weight * double(hits);
     rep->escaped_area_mm2 = weight * T.escaped;
@@ -298,39 +290,165 @@ extern "C" int icp_drop_generate(icp_context* c, const icp_drop_record* r, doubl
     rep->forward_mass_mm2 = weight * T.forward_pole;
     rep->backward_mass_mm2 = weight * T.backward_pole;
     rep->point_axial_mm2 = weight * T.point_axial;
+    rep->diffraction_area_mm2 = r->diffraction ? power : 0.0;
+    if (!(hits > 0)) return fail(ICP_ERR_AUDIT, "No sampled ray hit the drop.");
+    const int st = cdf_finish(cdf, r->policy, &rep->cdf);
+    rep->histogram_mass_mm2 = rep->cdf.fine_mass;
+    const double expected = rep->escaped_area_mm2 + rep->diffraction_area_mm2;
+    rep->histogram_relative_error = std::fabs(rep->histogram_mass_mm2 / expected - 1);
+    return st;
+}
+
+double projected_area_of(const icp_drop_record* r, int& status)
+{
+    status = ICP_OK;
+    try {
+        const auto F = H::drop_frame(r->inclination_deg);
+        return H::drop_projected_area(r->coefficients, r->radius_mm, F.k).area_mm2;
+    } catch (const std::exception& e) {
+        status = fail(ICP_ERR_INVALID_ARGUMENT, "%s", e.what());
+        return 0;
+    }
+}
+
+} // namespace icp::dropx
+
+extern "C" int icp_drop_trace_bin(icp_context* c, const icp_drop_record* r, uint64_t first, uint64_t count,
+                                  double area_weight, const icp_grid* g, const double* d_edges, double* d_mass,
+                                  icp_trace_stats* stats)
+{
+    if (!c || !r || !g || !d_edges || !d_mass || !stats) return fail(ICP_ERR_INVALID_ARGUMENT, "icp_drop_trace_bin: null argument");
+    if (const int v = validate_record(r)) return v;
+    if (first >= r->rays || count > r->rays - first) return fail(ICP_ERR_INVALID_ARGUMENT, "Batch is outside the ray range.");
+    if (!(area_weight > 0) || !H::finite(area_weight)) return fail(ICP_ERR_INVALID_ARGUMENT, "Invalid area weight.");
+    if (count == 0) return ok();
+    ICP_CUDA(cudaSetDevice(c->device));
+    ICP_CUDA(c->stats.ensure(hex_stats_bytes()));
+    ICP_CUDA(cudaMemsetAsync(c->stats.ptr, 0, hex_stats_bytes(), c->stream));
+    if (const int e = drop_trace_enqueue(c, r, first, count, area_weight, g, d_edges, d_mass, c->stats.ptr)) return e;
+    std::vector<unsigned char> raw(hex_stats_bytes());
+    ICP_CUDA(cudaMemcpyAsync(raw.data(), c->stats.ptr, raw.size(), cudaMemcpyDeviceToHost, c->stream));
+    ICP_CUDA(cudaStreamSynchronize(c->stream));
+    stats_accumulate(raw.data(), stats);
+    return ok();
+}
+
+namespace {
+
+// One record: trace + bin, diffraction rows and the CDF enqueued back to back, one
+// synchronisation.  host = true: phi/theta/u are host arrays (the CDF goes through context
+// scratch and is copied back); host = false: phi/theta/u are caller device arrays written in
+// place (u may be null).
+int drop_record(icp_context* c, const icp_drop_record* r, double* phi_out, double* theta_out, double* u_out, bool host,
+                icp_drop_report* rep)
+{
+    std::memset(rep, 0, sizeof *rep);
+    if (const int v = validate_record(r)) return v;
+    if (const int v = validate_grid(r)) return v;
+    ICP_CUDA(cudaSetDevice(c->device));
+    icp_grid g;
+    grid_of(r, g);
+    for (int i = 0; i < 3; ++i) {
+        rep->ki[i] = g.ki[i];
+        rep->e0[i] = g.e0[i];
+        rep->e1[i] = g.e1[i];
+    }
+    double disk_area = 0;
+    if (const int e = icp_drop_sampling_area(r->coefficients, r->radius_mm, &disk_area)) return e;
+    rep->sampled_area_mm2 = disk_area;
+    const double weight = disk_area / double(r->rays);
+    std::vector<double> edges;
+    if (!H::u_edges(r->nt, edges)) return fail(ICP_ERR_INVALID_ARGUMENT, "Angular cells cannot be represented in binary64.");
+    const uint64_t cells = (uint64_t)r->nt * r->np;
+    const size_t sb = hex_stats_bytes();
+    ICP_CUDA(c->rec_edges.ensure(sizeof(double) * (r->nt + 1)));
+    ICP_CUDA(c->rec_mass.ensure(sizeof(double) * cells));
+    ICP_CUDA(c->stats.ensure(sb));
+    ICP_CUDA(c->rows.ensure(sizeof(double) * (r->nt + 1)));
+    ICP_CUDA(c->dargs.ensure(sizeof(DiffractionArgs)));
+    ICP_CUDA(c->cdf_report.ensure(sizeof(CdfDeviceReport)));
+    ICP_CUDA(c->cdf_sync.ensure(2 * sizeof(unsigned)));
+    if (host) {
+        ICP_CUDA(c->rec_phi.ensure(sizeof(double) * (r->cp + 1)));
+        ICP_CUDA(c->rec_theta.ensure(sizeof(double) * (size_t)r->cp * (r->ct + 1)));
+    }
+    double* d_phi = host ? (double*)c->rec_phi.ptr : phi_out;
+    double* d_theta = host ? (double*)c->rec_theta.ptr : theta_out;
+    double* d_mass = (double*)c->rec_mass.ptr;
+    double* d_rows = (double*)c->rows.ptr;
+    ICP_CUDA(cudaEventRecord(c->ev0, c->stream));
+    ICP_CUDA(cudaMemcpyAsync(c->rec_edges.ptr, edges.data(), sizeof(double) * (r->nt + 1), cudaMemcpyHostToDevice, c->stream));
+    ICP_CUDA(cudaMemsetAsync(d_mass, 0, sizeof(double) * cells, c->stream));
+    ICP_CUDA(cudaMemsetAsync(c->stats.ptr, 0, sb, c->stream));
+    const double* d_edges = (const double*)c->rec_edges.ptr;
+    if (const int e = drop_trace_enqueue(c, r, 0, r->rays, weight, &g, d_edges, d_mass, c->stats.ptr)) return e;
     if (r->diffraction) {
-        // separately reported stage: Fraunhofer lobe carrying as much power as the geometric part
-        const auto rows = H::diffraction_rows(edges, rep->incident_area_mm2, r->wavelength_nm);
-        for (double v : rows) rep->diffraction_area_mm2 += v;
-        ICP_CUDA(c->rows.ensure(sizeof(double) * r->nt));
-        ICP_CUDA(cudaMemcpyAsync(c->rows.ptr, rows.data(), sizeof(double) * r->nt, cudaMemcpyHostToDevice, c->stream));
-        add_rows<<<(unsigned)std::min<uint64_t>(4096, (cells + 255) / 256), 256, 0, c->stream>>>(
-            (double*)c->rec_mass.ptr, (const double*)c->rows.ptr, r->nt, r->np);
+        DiffractionArgs a{};
+        a.edges = d_edges;
+        a.rays = (const unsigned long long*)c->stats.ptr + devstats_rays_word();
+        a.missed_offset = devstats_missed_word() - devstats_rays_word();
+        a.row_add = d_rows;
+        a.power = d_rows + r->nt;
+        a.weight = weight;
+        a.wavelength_nm = r->wavelength_nm;
+        a.nt = r->nt;
+        a.np = r->np;
+        ICP_CUDA(cudaMemcpyAsync(c->dargs.ptr, &a, sizeof a, cudaMemcpyHostToDevice, c->stream));
+        const int e = launch_diffraction_rows((const DiffractionArgs*)c->dargs.ptr, 1, r->nt, c->stream);
         count_launch();
-        ICP_CUDA(cudaGetLastError());
+        if (e) return fail(ICP_ERR_DEVICE, "diffraction launch failed: %s", cudaGetErrorString((cudaError_t)e));
     }
     ICP_CUDA(cudaEventRecord(c->ev1, c->stream));
-    ICP_CUDA(cudaEventSynchronize(c->ev1));
+    if (const int e = cdf_enqueue(c, d_mass, r->nt, r->np, r->ct, r->cp, d_edges, 0.0, 0.0,
+                                  (const unsigned long long*)c->stats.ptr + devstats_fwd_word(), weight,
+                                  r->diffraction ? d_rows : nullptr, d_phi, d_theta,
+                                  (CdfDeviceReport*)c->cdf_report.ptr, (unsigned*)c->cdf_sync.ptr))
+        return e;
+    ICP_CUDA(cudaEventRecord(c->ev2, c->stream));
+    std::vector<unsigned char> raw(sb);
+    CdfDeviceReport cdf{};
+    double power = 0;
+    ICP_CUDA(cudaMemcpyAsync(raw.data(), c->stats.ptr, sb, cudaMemcpyDeviceToHost, c->stream));
+    ICP_CUDA(cudaMemcpyAsync(&cdf, c->cdf_report.ptr, sizeof cdf, cudaMemcpyDeviceToHost, c->stream));
+    if (r->diffraction) ICP_CUDA(cudaMemcpyAsync(&power, d_rows + r->nt, sizeof power, cudaMemcpyDeviceToHost, c->stream));
+    const uint32_t dt = r->nt / r->ct;
+    std::vector<double> coarse(r->ct + 1);
+    for (uint32_t i = 0; i <= r->ct; ++i) coarse[i] = edges[(size_t)i * dt];
+    if (host) {
+        ICP_CUDA(cudaMemcpyAsync(phi_out, d_phi, sizeof(double) * (r->cp + 1), cudaMemcpyDeviceToHost, c->stream));
+        ICP_CUDA(cudaMemcpyAsync(theta_out, d_theta, sizeof(double) * (size_t)r->cp * (r->ct + 1),
+                                 cudaMemcpyDeviceToHost, c->stream));
+        std::memcpy(u_out, coarse.data(), sizeof(double) * (r->ct + 1));
+    } else if (u_out) {
+        ICP_CUDA(cudaMemcpyAsync(u_out, coarse.data(), sizeof(double) * (r->ct + 1), cudaMemcpyHostToDevice, c->stream));
+    }
+    // the projected area (CPU, binary64) overlaps the device work
+    int area_status = ICP_OK;
+    rep->projected_area_mm2 = projected_area_of(r, area_status);
+    ICP_CUDA(cudaStreamSynchronize(c->stream));
     float ms = 0;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
     rep->seconds_trace = ms * 1e-3;
-    if (!(hits > 0)) return fail(ICP_ERR_AUDIT, "No sampled ray hit the drop.");
-    ICP_CUDA(cudaEventRecord(c->ev0, c->stream));
-    const int cr = icp_phase_cdf_build(c, (const double*)c->rec_mass.ptr, ICP_CDF_MASS, r->nt, r->np,
-                                       rep->forward_mass_mm2, rep->backward_mass_mm2, r->ct, r->cp, &r->policy,
-                                       (double*)c->rec_phi.ptr, (double*)c->rec_theta.ptr, &rep->cdf);
-    ICP_CUDA(cudaEventRecord(c->ev1, c->stream));
-    rep->histogram_mass_mm2 = rep->cdf.fine_mass;
-    if (cr != ICP_OK) return cr;
-    ICP_CUDA(cudaMemcpyAsync(h_phi, c->rec_phi.ptr, sizeof(double) * (r->cp + 1), cudaMemcpyDeviceToHost, c->stream));
-    ICP_CUDA(cudaMemcpyAsync(h_theta, c->rec_theta.ptr, sizeof(double) * (size_t)r->cp * (r->ct + 1),
-                             cudaMemcpyDeviceToHost, c->stream));
-    ICP_CUDA(cudaStreamSynchronize(c->stream));
-    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    cudaEventElapsedTime(&ms, c->ev1, c->ev2);
     rep->seconds_cdf = ms * 1e-3;
-    const uint32_t dt = r->nt / r->ct;
-    for (uint32_t i = 0; i <= r->ct; ++i) h_u[i] = edges[(size_t)i * dt];
-    const double expected = rep->escaped_area_mm2 + rep->diffraction_area_mm2;
-    rep->histogram_relative_error = std::fabs(rep->histogram_mass_mm2 / expected - 1);
-    return ok();
+    if (area_status) return area_status;
+    const int st = finish_report(r, raw.data(), cdf, power, weight, rep);
+    return st == ICP_OK ? ok() : st;
+}
+
+} // namespace
+
+extern "C" int icp_drop_generate(icp_context* c, const icp_drop_record* r, double* h_phi, double* h_theta, double* h_u,
+                                 icp_drop_report* rep)
+{
+    if (!c || !r || !h_phi || !h_theta || !h_u || !rep) return fail(ICP_ERR_INVALID_ARGUMENT, "icp_drop_generate: null argument");
+    return drop_record(c, r, h_phi, h_theta, h_u, true, rep);
+}
+
+extern "C" int icp_drop_generate_device(icp_context* c, const icp_drop_record* r, double* d_phi, double* d_theta,
+                                        double* d_u, icp_drop_report* rep)
+{
+    if (!c || !r || !d_phi || !d_theta || !rep)
+        return fail(ICP_ERR_INVALID_ARGUMENT, "icp_drop_generate_device: null argument");
+    return drop_record(c, r, d_phi, d_theta, d_u, false, rep);
 }

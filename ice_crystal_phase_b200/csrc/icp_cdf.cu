@@ -54,7 +54,32 @@ struct CdfParams {
     unsigned* sync;       // [0] barrier arrivals, [1] finished-block ticket
     uint32_t kind, nt, np, ct, cp, dt, dp, cw;
     double fwd_add, bwd_add;
+    const double* row_add;
+    const unsigned long long* pole_fx;
+    double pole_weight;
 };
+
+// Additions to the fine histogram: pole caps on the end rows, an optional per-row term.
+struct CdfAdds {
+    double fwd, bwd;
+    const double* row;
+};
+
+// Pole caps from fixed-point pole sums: the host's arithmetic (stats_accumulate, then
+// weight x pole power, then / np) evaluated on the device.
+__device__ __forceinline__ CdfAdds cdf_adds(const CdfParams& P, unsigned long long* bad)
+{
+    CdfAdds a{P.fwd_add, P.bwd_add, P.row_add};
+    if (P.pole_fx) {
+        const double f = (ldexp((double)P.pole_fx[1], 64) + (double)P.pole_fx[0]) * 0x1p-44;
+        const double b = (ldexp((double)P.pole_fx[3], 64) + (double)P.pole_fx[2]) * 0x1p-44;
+        const double fm = P.pole_weight * f, bm = P.pole_weight * b;
+        a.fwd = fm / P.np;
+        a.bwd = bm / P.np;
+        if ((fm > 0 && !(a.fwd > 0)) || (bm > 0 && !(a.bwd > 0))) ++*bad;
+    }
+    return a;
+}
 
 constexpr unsigned kThreads = 256;
 constexpr unsigned kSpinLimit = 1u << 22;
@@ -79,22 +104,23 @@ __device__ __forceinline__ bool grid_wait(unsigned* counter, unsigned target, un
     return ok;
 }
 
-__device__ __forceinline__ double fine_mass_at(const CdfParams& P, uint32_t i, uint32_t j)
+__device__ __forceinline__ double fine_mass_at(const CdfParams& P, const CdfAdds& A, uint32_t i, uint32_t j)
 {
     double m = P.values[(size_t)i * P.np + j];
     if (P.kind == 1) m = m * (P.edges[i + 1] - P.edges[i]);
-    if (i == 0) m += P.fwd_add;
-    if (i + 1 == P.nt) m += P.bwd_add;
+    if (A.row) m += A.row[i];
+    if (i == 0) m += A.fwd;
+    if (i + 1 == P.nt) m += A.bwd;
     return m;
 }
 
 // Conservative aggregate of one coarse cell: Kahan sum in row-major fine order
 // (hex_phase/src/phase_table.cpp:122-123).
-__device__ __forceinline__ double coarse_at(const CdfParams& P, uint32_t ci, uint32_t cj)
+__device__ __forceinline__ double coarse_at(const CdfParams& P, const CdfAdds& A, uint32_t ci, uint32_t cj)
 {
     KSum acc{0, 0};
     for (uint32_t i = ci * P.dt; i < (ci + 1) * P.dt; ++i)
-        for (uint32_t j = cj * P.dp; j < (cj + 1) * P.dp; ++j) acc.add(fine_mass_at(P, i, j));
+        for (uint32_t j = cj * P.dp; j < (cj + 1) * P.dp; ++j) acc.add(fine_mass_at(P, A, i, j));
     return acc.v;
 }
 
@@ -138,7 +164,9 @@ __global__ void __launch_bounds__(kThreads) cdf_build_kernel(const CdfParams P)
     // ------------------------------------------------------------ phase A
     KSum fm{0, 0}, fa{0, 0}, sm{0, 0}, sa{0, 0};
     double largest = 0.0;
-    unsigned long long invalid = 0ull;
+    unsigned long long invalid = 0ull, pole_bad = 0ull;
+    const CdfAdds adds = cdf_adds(P, &pole_bad);
+    if (threadIdx.x == 0) invalid += pole_bad;
     const uint32_t cells = P.ct * w;
     for (uint32_t q = threadIdx.x; q < cells; q += blockDim.x) {
         const uint32_t ci = q / w, cl = q % w, cj = c0 + cl;
@@ -146,7 +174,7 @@ __global__ void __launch_bounds__(kThreads) cdf_build_kernel(const CdfParams P)
         for (uint32_t i = ci * P.dt; i < (ci + 1) * P.dt; ++i) {
             const double mu = 1.0 - P.edges[i] - P.edges[i + 1];
             for (uint32_t j = cj * P.dp; j < (cj + 1) * P.dp; ++j) {
-                const double m = fine_mass_at(P, i, j);
+                const double m = fine_mass_at(P, adds, i, j);
                 if (!(m >= 0.0) || !(m <= 1.7976931348623157e308)) ++invalid;
                 acc.add(m);
                 fm.add(m);
@@ -217,7 +245,7 @@ __global__ void __launch_bounds__(kThreads) cdf_build_kernel(const CdfParams P)
             const uint32_t ci = i / P.dt, cl = j / P.dp - c0;
             const double fraction = (P.edges[i + 1] - P.edges[i]) /
                                     (P.edges[(size_t)(ci + 1) * P.dt] - P.edges[(size_t)ci * P.dt]) / P.dp;
-            tv.add(fabs(fine_mass_at(P, i, j) / fine_total - strip[(size_t)ci * CW + cl] / stored_total * fraction));
+            tv.add(fabs(fine_mass_at(P, adds, i, j) / fine_total - strip[(size_t)ci * CW + cl] / stored_total * fraction));
         }
     }
     // weights w = coarse / largest for the whole strip in parallel (the ordered chains below
@@ -309,7 +337,7 @@ __global__ void __launch_bounds__(kThreads) cdf_build_kernel(const CdfParams P)
             const double b1 = norm(i + 1);
             const double a0 = sphi[cl], a1 = sphi[cl + 1];
             const double qv = (a1 - a0) * (b1 - b0);
-            const double c = coarse_at(P, i, j);
+            const double c = coarse_at(P, adds, i, j);
             const double p = c / stored_total;
             const bool bad = !(qv >= 0.0) || !(qv <= 1.7976931348623157e308) || a1 < a0 || b1 < b0;
             if (bad) ++malformed;
@@ -419,6 +447,9 @@ int launch_cdf_build(const CdfLaunch& L, cudaStream_t stream)
     P.cw = L.cw;
     P.fwd_add = L.fwd_add;
     P.bwd_add = L.bwd_add;
+    P.row_add = L.row_add;
+    P.pole_fx = L.pole_fx;
+    P.pole_weight = L.pole_weight;
     const unsigned blocks = (L.cp + L.cw - 1) / L.cw;
     const size_t smem = cdf_smem_bytes(L.ct, L.cp, L.cw);
     cudaError_t e = cudaFuncSetAttribute(cdf_build_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -21,14 +21,27 @@ namespace icp {
 
 template <class R> struct DropShape {
     R c[8];
+    R m[8];      // binary32 path: R(mu) = sum_k m_k mu^k (the series in monomial form)
+    R md[7];     //                dR/dmu = sum_k md_k mu^k
     R r_out;     // conservative bounding radius (outer sphere)
     R r_center;  // 1 + c_0 (the sphere radius when c_1..c_7 vanish)
     bool sphere;
 };
 
-// R(mu) and dR/dmu (raindrop_shape.hpp:70-84).
+// R(mu) and dR/dmu.  binary64: the Chebyshev recurrence of the reference (raindrop_shape.hpp:
+// 70-84); binary32: Horner on the monomial form (13 FMAs; the coefficients are converted in
+// binary64 on the host, and |mu| <= 1 keeps the cancellation below the binary32 rounding).
 template <class R> __device__ __forceinline__ R drop_radius(const DropShape<R>& S, R mu, R& dr)
 {
+    if constexpr (sizeof(R) == 4) {
+        R r = S.m[7], d = S.md[6];
+#pragma unroll
+        for (int k = 6; k >= 0; --k) r = fmaf(r, mu, S.m[k]);
+#pragma unroll
+        for (int k = 5; k >= 0; --k) d = fmaf(d, mu, S.md[k]);
+        dr = d;
+        return r;
+    }
     R prev = R(1), cur = mu, dprev = R(0), dcur = R(1);
     R radius = R(1) + S.c[0] + S.c[1] * mu;
     R deriv = S.c[1];
@@ -90,8 +103,49 @@ template <class R> __device__ __forceinline__ bool sphere_roots(V3<R> p, V3<R> d
 
 constexpr int kNewtonMax = 40;
 
+// Intersection of the line q + t w (w unit) with the drop: entering from outside, the first
+// root; leaving from a surface point, the far root.  Both run one Newton loop on the gauge from
+// the bounding sphere (the near root entering, the far root leaving), so lanes entering and
+// leaving the drop execute the same instructions.  False only for an entering line that misses.
+template <class R>
+__device__ __forceinline__ bool drop_intersect(const DropShape<R>& S, V3<R> q, V3<R> w, bool entering, R& t,
+                                               unsigned& iters)
+{
+    R t0, t1;
+    if (!sphere_roots(q, w, S.sphere ? S.r_center : S.r_out, t0, t1)) {
+        t = R(0);
+        return !entering;
+    }
+    if (S.sphere) {
+        t = entering ? t0 : rmax(t1, R(0));
+        return !entering || t0 >= R(0);
+    }
+    t = rmax(entering ? t0 : t1, R(0));
+    const R sgn = entering ? R(-1) : R(1);
+    R prev_h = R(1e30);
+    for (int it = 0; it < kNewtonMax; ++it) {
+        R dh;
+        const R h = gauge(S, q + w * t, w, dh);
+        ++iters;
+        if (h <= R(0)) return true;           // converged onto the root from outside the drop
+        if (!(sgn * dh > R(0))) return !entering; // entering: non-decreasing while outside -> miss;
+                                                  // leaving: degenerate tangent chord, stay at t
+        const R step = h / dh;
+        t -= step;
+        if (entering ? (t > t1) : (t <= R(0))) {
+            if (!entering) t = R(0);
+            return !entering;
+        }
+        if (!(h < prev_h) || rabs(step) <= R(4) * Eps<R>::eps * rmax(R(1), rabs(t))) return true;
+        prev_h = h;
+    }
+    return true;
+}
+
 // First surface point along the line from an exterior point: t of the entry, false on a miss.
-template <class R> __device__ __forceinline__ bool drop_entry(const DropShape<R>& S, V3<R> o, V3<R> d, R& t)
+// `iters` counts the gauge evaluations (the dominant arithmetic of a non-spherical drop).
+template <class R> __device__ __forceinline__ bool drop_entry(const DropShape<R>& S, V3<R> o, V3<R> d, R& t,
+                                                              unsigned& iters)
 {
     R t0, t1;
     if (S.sphere) {
@@ -105,6 +159,7 @@ template <class R> __device__ __forceinline__ bool drop_entry(const DropShape<R>
     for (int it = 0; it < kNewtonMax; ++it) {
         R dh;
         const R h = gauge(S, o + d * t, d, dh);
+        ++iters;
         if (h <= R(0)) return true;          // converged from outside to the entry root
         if (!(dh < R(0))) return false;       // convex and non-decreasing while outside: miss
         const R step = h / dh;                // negative
@@ -117,7 +172,7 @@ template <class R> __device__ __forceinline__ bool drop_entry(const DropShape<R>
 }
 
 // Exit point along an interior chord that starts on (or rounding-close to) the surface.
-template <class R> __device__ __forceinline__ R drop_exit(const DropShape<R>& S, V3<R> p, V3<R> d)
+template <class R> __device__ __forceinline__ R drop_exit(const DropShape<R>& S, V3<R> p, V3<R> d, unsigned& iters)
 {
     R t0, t1;
     if (S.sphere) {
@@ -131,6 +186,7 @@ template <class R> __device__ __forceinline__ R drop_exit(const DropShape<R>& S,
     for (int it = 0; it < kNewtonMax; ++it) {
         R dh;
         const R h = gauge(S, p + d * t, d, dh);
+        ++iters;
         if (h <= R(0)) break;                 // reached the exit root from beyond it
         if (!(dh > R(0))) break;              // degenerate tangent chord: stay at t
         const R step = h / dh;                // positive

@@ -28,7 +28,7 @@ struct DevStats {
     double axial;
     unsigned long long max_bal_bits, max_iface_bits; // bit patterns of non-negative doubles
     unsigned long long rays, outputs, status[8], rejected, snapped, near_edge, fallback, invalid;
-    unsigned long long encounters, missed;
+    unsigned long long encounters, missed, gauge_evals;
 };
 
 __device__ __forceinline__ void add128(unsigned long long* p, unsigned long long t)
@@ -218,12 +218,12 @@ __device__ __forceinline__ int geo_next(const HexGeo<R>& G, V3<R>& p, V3<R> d, u
     return 0;
 }
 
-// Drop: uniform point on the sampling disk (radius^2 uniform, angle uniform), then the first
-// surface point along k; the reference's drops use a deterministic vertex grid instead
+// Drop: uniform point on the sampling disk (radius^2 uniform, angle uniform) a distance `back`
+// before the centre; the reference's drops use a deterministic vertex grid instead
 // (raindrop_paths.hpp:52-58), so the counter RNG of the prism path is reused here.
 template <class R>
-__device__ __forceinline__ int geo_entry(const DropGeo<R>& G, const V3<R>& k, const V3<R>& e0, uint64_t seed,
-                                         uint64_t id, V3<R>& pos, V3<R>& n)
+__device__ __forceinline__ V3<R> drop_origin(const DropGeo<R>& G, const V3<R>& k, const V3<R>& e0, uint64_t seed,
+                                             uint64_t id)
 {
     const R u0 = uniform<R>(rng_bits(seed, id, 0));
     const R u1 = uniform<R>(rng_bits(seed, id, 1));
@@ -231,22 +231,7 @@ __device__ __forceinline__ int geo_entry(const DropGeo<R>& G, const V3<R>& k, co
     R sn, cs;
     if constexpr (sizeof(R) == 4) sincospif(R(2) * u1, &sn, &cs);
     else sincospi(R(2) * u1, &sn, &cs);
-    const V3<R> o = (e0 * (rad * cs) + G.e1 * (rad * sn)) - k * G.back;
-    R t;
-    if (!drop_entry(G.shape, o, k, t)) return -1;
-    pos = o + k * t;
-    n = drop_normal(G.shape, pos);
-    return 0;
-}
-template <class R>
-__device__ __forceinline__ int geo_next(const DropGeo<R>& G, V3<R>& p, V3<R> d, unsigned& face, V3<R>& n, bool& near_edge)
-{
-    near_edge = false;
-    face = 0u;
-    const R t = drop_exit(G.shape, p, d);
-    p = p + d * t;
-    n = drop_normal(G.shape, p);
-    return 0;
+    return (e0 * (rad * cs) + G.e1 * (rad * sn)) - k * G.back;
 }
 
 template <class R> struct LaneRay {
@@ -263,6 +248,7 @@ template <class R> struct LaneRay {
 template <class R> struct LaneAcc {
     unsigned long long esc_fx, unres_fx, fwd_fx, bwd_fx, outputs, rays, rejected, snapped, near_edge, fallback, invalid, encounters,
         missed;
+    unsigned gauge_evals;
     double axial, max_bal, max_iface;
     uint64_t cur_batch;
     uint32_t cur_batch_out;
@@ -308,49 +294,60 @@ __device__ __forceinline__ void settle(const P_& P, LaneRay<R>& L, LaneAcc<R>& A
     }
 }
 
-template <class R, class G>
-__global__ void __launch_bounds__(256, (sizeof(R) == 4 ? 3 : 1)) trace_bin_kernel(const TraceParams<R, G> P)
+// Per-block shared state: the privatised histogram table, the per-status ray counts of the
+// block and (optionally) the u edges.
+template <class R> struct BlockShared {
+    SmemHist H;
+    unsigned* s_status;
+    const R* edges;
+};
+
+template <class R, class P_>
+__device__ __forceinline__ BlockShared<R> block_setup(const P_& P, unsigned char* smem)
 {
-    extern __shared__ __align__(16) unsigned char smem[];
+    BlockShared<R> B;
     unsigned long long* s_vals = reinterpret_cast<unsigned long long*>(smem);
     uint32_t* s_keys = reinterpret_cast<uint32_t*>(s_vals + P.hash_slots);
-    unsigned* s_status = reinterpret_cast<unsigned*>(s_keys + P.hash_slots);
-    R* s_edges = reinterpret_cast<R*>(s_status + 8);
-
+    B.s_status = reinterpret_cast<unsigned*>(s_keys + P.hash_slots);
+    R* s_edges = reinterpret_cast<R*>(B.s_status + 8);
     const uint32_t nt = P.gf.nt;
     for (uint32_t s = threadIdx.x; s < P.hash_slots; s += blockDim.x) { s_keys[s] = 0u; s_vals[s] = 0ull; }
-    if (threadIdx.x < 8) s_status[threadIdx.x] = 0u;
-    const R* edges;
+    if (threadIdx.x < 8) B.s_status[threadIdx.x] = 0u;
     if (P.smem_edges) {
         for (uint32_t i = threadIdx.x; i <= nt; i += blockDim.x) {
             if constexpr (sizeof(R) == 4) s_edges[i] = P.edges_f[i];
             else s_edges[i] = P.edges_d[i];
         }
-        edges = s_edges;
+        B.edges = s_edges;
     } else {
-        if constexpr (sizeof(R) == 4) edges = P.edges_f;
-        else edges = P.edges_d;
+        if constexpr (sizeof(R) == 4) B.edges = P.edges_f;
+        else B.edges = P.edges_d;
     }
-    __syncthreads();
-    SmemHist H{s_keys, s_vals, P.hash_slots ? P.hash_slots - 1u : 0u};
+    B.H = SmemHist{s_keys, s_vals, P.hash_slots ? P.hash_slots - 1u : 0u};
+    return B;
+}
 
-    const unsigned lane = threadIdx.x & 31u;
-    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
-    const uint64_t warp = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const uint64_t per = (P.count + warps - 1) / warps;
-    uint64_t wnext = P.first + warp * per;
-    const uint64_t wend = min(P.first + P.count, wnext + per);
-
-    LaneRay<R> L;
-    L.live = false;
-    LaneAcc<R> A;
+template <class R> __device__ __forceinline__ void lane_acc_clear(LaneAcc<R>& A)
+{
     A.esc_fx = A.unres_fx = A.fwd_fx = A.bwd_fx = A.outputs = A.rays = A.rejected = 0ull;
     A.snapped = A.near_edge = A.fallback = A.invalid = A.encounters = A.missed = 0ull;
+    A.gauge_evals = 0u;
     A.axial = A.max_bal = A.max_iface = 0.0;
     A.cur_batch = ~0ull;
     A.cur_batch_out = 0u;
-    const unsigned lt_mask = (1u << lane) - 1u;
+}
 
+// The rays [wnext, wend) of one warp: persistent lanes, one event per lane per step, every
+// exit binned by the whole warp (hex_trace_core.hpp:190-259 per ray).
+template <class R, class G, class P_>
+__device__ __forceinline__ void trace_slice(const P_& P, const BlockShared<R>& B, uint64_t wnext, const uint64_t wend,
+                                            LaneAcc<R>& A)
+{
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    unsigned* s_status = B.s_status;
+    LaneRay<R> L;
+    L.live = false;
     while (true) {
         // ---- refill idle lanes from the warp's slice
         const unsigned idle = __ballot_sync(kFull, !L.live);
@@ -374,12 +371,60 @@ __global__ void __launch_bounds__(256, (sizeof(R) == 4 ? 3 : 1)) trace_bin_kerne
         V3<R> sd, se, sn;
         Stokes<R> sS;
         const Media<R>* media = &P.enter;
-        if (fresh) {
+        if constexpr (!std::is_same_v<G, HexGeo<R>>) {
+            // drop: every active lane runs one intersection -- entering from its sampling-disk
+            // origin (fresh) or leaving from its current surface point (live)
+            V3<R> q, w, n;
+            if (fresh) {
+                q = drop_origin(P.geo, P.k, P.ke0, P.seed, L.id);
+                w = P.k;
+            } else {
+                q = L.p;
+                w = L.d;
+            }
+            bool hit = false;
+            if (fresh || L.live) {
+                R t;
+                hit = drop_intersect(P.geo.shape, q, w, fresh, t, A.gauge_evals);
+                q = q + w * t;
+                if (hit) n = drop_normal(P.geo.shape, q);
+            }
+            if (fresh) {
+                if (!hit) {
+                    // a sampled ray that misses the particle carries no incident power
+                    ++A.missed;
+                    ++A.rays;
+                } else {
+                    L.live = true;
+                    L.esc = R(0);
+                    L.pfx = 1ull << kFixBits;
+                    L.escfx = 0ull;
+                    L.hits = 0u;
+                    L.p = q;
+                    L.face = 0u;
+                    do_split = true;
+                    sd = P.k;
+                    se = P.ke0;
+                    sS = Stokes<R>{R(1), R(0), R(0), R(0)};
+                    sn = n;
+                    media = &P.enter;
+                }
+            } else if (L.live) {
+                // one internal encounter (hex_trace_core.hpp:217-246)
+                L.p = q;
+                ++L.hits;
+                ++A.encounters;
+                do_split = true;
+                sd = L.d;
+                se = L.e;
+                sS = L.S;
+                sn = -n;
+                media = &P.leave;
+            }
+        } else if (fresh) {
             V3<R> pos, n;
             unsigned face = 8u;
-            int es;
-            if constexpr (std::is_same_v<G, HexGeo<R>>) es = geo_entry(P.geo, P.seed, L.id, pos, n, face);
-            else es = geo_entry(P.geo, P.k, P.ke0, P.seed, L.id, pos, n);
+            const int es = geo_entry(P.geo, P.seed, L.id, pos, n, face);
             if (es < 0) {
                 // a sampled ray that misses the particle carries no incident power
                 ++A.missed;
@@ -471,8 +516,8 @@ __global__ void __launch_bounds__(256, (sizeof(R) == 4 ? 3 : 1)) trace_bin_kerne
         uint64_t v = 0ull;
         if (has) {
             BinResult b;
-            if constexpr (sizeof(R) == 4) b = bin_f32(P.gf, edges, od);
-            else b = bin_f64(P.gd, edges, od);
+            if constexpr (sizeof(R) == 4) b = bin_f32(P.gf, B.edges, od);
+            else b = bin_f64(P.gd, B.edges, od);
             if (!b.valid) {
                 A.invalid += 1;
             } else {
@@ -486,11 +531,11 @@ __global__ void __launch_bounds__(256, (sizeof(R) == 4 ? 3 : 1)) trace_bin_kerne
                 else { to_table = true; cell = b.cell; }
             }
         }
-        hist_add(H, P.mass, P.to_mass, to_table, cell, v, A.fallback);
+        hist_add(B.H, P.mass, P.to_mass, to_table, cell, v, A.fallback);
 
         // ---- per-batch exit counts (capacity audit), flushed when the lane's batch changes
         if (P.batch_out && (has || fresh)) {
-            const uint64_t bidx = (L.id - 0) / P.batch_size;
+            const uint64_t bidx = L.id / P.batch_size;
             if (bidx != A.cur_batch) {
                 if (A.cur_batch != ~0ull && A.cur_batch_out) atomicAdd(&P.batch_out[A.cur_batch], A.cur_batch_out);
                 A.cur_batch = bidx;
@@ -500,16 +545,21 @@ __global__ void __launch_bounds__(256, (sizeof(R) == 4 ? 3 : 1)) trace_bin_kerne
         }
     }
     if (P.batch_out && A.cur_batch != ~0ull && A.cur_batch_out) atomicAdd(&P.batch_out[A.cur_batch], A.cur_batch_out);
+}
 
-    // ---- block epilogue: flush the table and the lane accumulators
+// Block epilogue (all threads): flush the table into P.mass and the lane accumulators and the
+// block's status counts into P.stats; leaves the table and the status counts cleared.
+template <class R, class P_>
+__device__ __forceinline__ void block_flush(const P_& P, const BlockShared<R>& B, const LaneAcc<R>& A)
+{
     __syncthreads();
-    hist_flush(H, P.mass, P.to_mass);
+    hist_flush(B.H, P.mass, P.to_mass);
     DevStats* Gs = P.stats;
     // Per-warp sums stay below 2^60 (a warp slice holds at most 2^16 rays of power <= 1).
-    unsigned long long w[13] = {A.esc_fx, A.unres_fx, A.fwd_fx, A.bwd_fx, A.rays, A.outputs, A.rejected,
-                                A.snapped, A.near_edge, A.fallback, A.invalid, A.encounters, A.missed};
+    unsigned long long w[14] = {A.esc_fx, A.unres_fx, A.fwd_fx, A.bwd_fx, A.rays, A.outputs, A.rejected,
+                                A.snapped, A.near_edge, A.fallback, A.invalid, A.encounters, A.missed, A.gauge_evals};
 #pragma unroll
-    for (int q = 0; q < 13; ++q)
+    for (int q = 0; q < 14; ++q)
         for (int o = 16; o; o >>= 1) w[q] += __shfl_xor_sync(kFull, w[q], o);
     double ax = A.axial, mb = A.max_bal, mi = A.max_iface;
     for (int o = 16; o; o >>= 1) {
@@ -517,22 +567,43 @@ __global__ void __launch_bounds__(256, (sizeof(R) == 4 ? 3 : 1)) trace_bin_kerne
         mb = fmax(mb, __shfl_xor_sync(kFull, mb, o));
         mi = fmax(mi, __shfl_xor_sync(kFull, mi, o));
     }
-    if (lane == 0) {
+    if ((threadIdx.x & 31u) == 0) {
         add128(Gs->esc, w[0]);
         add128(Gs->unres, w[1]);
         add128(Gs->fwd, w[2]);
         add128(Gs->bwd, w[3]);
-        unsigned long long* counters[9] = {&Gs->rays, &Gs->outputs, &Gs->rejected, &Gs->snapped,
-                                           &Gs->near_edge, &Gs->fallback, &Gs->invalid, &Gs->encounters, &Gs->missed};
+        unsigned long long* counters[10] = {&Gs->rays, &Gs->outputs, &Gs->rejected, &Gs->snapped, &Gs->near_edge,
+                                            &Gs->fallback, &Gs->invalid, &Gs->encounters, &Gs->missed, &Gs->gauge_evals};
 #pragma unroll
-        for (int q = 0; q < 9; ++q)
+        for (int q = 0; q < 10; ++q)
             if (w[4 + q]) atomicAdd(counters[q], w[4 + q]);
         if (ax != 0.0) atomicAdd(&Gs->axial, ax);
         atomicMax(&Gs->max_bal_bits, (unsigned long long)__double_as_longlong(mb));
         atomicMax(&Gs->max_iface_bits, (unsigned long long)__double_as_longlong(mi));
     }
     __syncthreads();
-    if (threadIdx.x < 8 && s_status[threadIdx.x]) atomicAdd(&Gs->status[threadIdx.x], (unsigned long long)s_status[threadIdx.x]);
+    if (threadIdx.x < 8) {
+        if (B.s_status[threadIdx.x]) atomicAdd(&Gs->status[threadIdx.x], (unsigned long long)B.s_status[threadIdx.x]);
+        B.s_status[threadIdx.x] = 0u;
+    }
+}
+
+// One record: the ray range [first, first+count) split into contiguous per-warp slices.
+template <class R, class G>
+__global__ void __launch_bounds__(256, (sizeof(R) == 4 ? 3 : 1)) trace_bin_kernel(const TraceParams<R, G> P)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const BlockShared<R> B = block_setup<R>(P, smem);
+    __syncthreads();
+    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    const uint64_t warp = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const uint64_t per = (P.count + warps - 1) / warps;
+    const uint64_t wnext = P.first + warp * per;
+    const uint64_t wend = min(P.first + P.count, wnext + per);
+    LaneAcc<R> A;
+    lane_acc_clear(A);
+    trace_slice<R, G>(P, B, wnext, wend, A);
+    block_flush<R>(P, B, A);
 }
 
 } // namespace icp

@@ -3,6 +3,7 @@
 #pragma once
 #include <cmath>
 
+#include "icp_batch_kernel.cuh"
 #include "icp_hex_kernel.cuh"
 #include "icp_internal.h"
 
@@ -77,6 +78,24 @@ template <class R> TraceParams<R, DropGeo<R>> make_drop_params(const HexLaunch& 
     TraceParams<R, DropGeo<R>> P;
     fill_common(P, L);
     for (int n = 0; n < 8; ++n) P.geo.shape.c[n] = (R)L.coeff[n];
+    // monomial form of 1 + sum_n c_n T_n(mu) in binary64 (T_{n+1} = 2 mu T_n - T_{n-1})
+    double mono[8] = {1.0 + L.coeff[0], 0, 0, 0, 0, 0, 0, 0};
+    double tm1[8] = {1, 0, 0, 0, 0, 0, 0, 0}, tn[8] = {0, 1, 0, 0, 0, 0, 0, 0};
+    for (int k = 0; k < 8; ++k) mono[k] += L.coeff[1] * tn[k];
+    for (int n = 2; n < 8; ++n) {
+        double tp[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int k = 0; k < 8; ++k) {
+            if (k > 0) tp[k] += 2 * tn[k - 1];
+            tp[k] -= tm1[k];
+        }
+        for (int k = 0; k < 8; ++k) {
+            tm1[k] = tn[k];
+            tn[k] = tp[k];
+            mono[k] += L.coeff[n] * tn[k];
+        }
+    }
+    for (int k = 0; k < 8; ++k) P.geo.shape.m[k] = (R)mono[k];
+    for (int k = 0; k < 7; ++k) P.geo.shape.md[k] = (R)((k + 1) * mono[k + 1]);
     P.geo.shape.r_out = (R)L.r_out;
     P.geo.shape.r_center = (R)L.r_center;
     P.geo.shape.sphere = L.sphere != 0;
@@ -101,6 +120,42 @@ template <class R, class G> int trace_blocks_per_sm(uint32_t hash_slots, uint32_
     cudaFuncSetAttribute(trace_bin_kernel<R, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_bin_kernel<R, G>, (int)threads, smem) != cudaSuccess)
+        return 0;
+    return per_sm;
+}
+
+template <class R> int launch_drop_batch(const BatchLaunch& B, cudaStream_t stream)
+{
+    using P_ = TraceParams<R, DropGeo<R>>;
+    P_* table = static_cast<P_*>(B.h_staging);
+    for (uint32_t r = 0; r < B.n_records; ++r) table[r] = make_drop_params<R>(B.recs[r]);
+    cudaError_t e = cudaMemcpyAsync(B.d_table, table, sizeof(P_) * B.n_records, cudaMemcpyHostToDevice, stream);
+    if (e != cudaSuccess) return (int)e;
+    BatchParams<R, DropGeo<R>> Q;
+    Q.recs = static_cast<const P_*>(B.d_table);
+    Q.chunk_begin = B.d_chunk_begin;
+    Q.queue = B.d_queue;
+    Q.total_chunks = B.total_chunks;
+    Q.n_records = B.n_records;
+    Q.chunk_rays = B.chunk_rays;
+    Q.nt = B.nt;
+    Q.smem_edges = (B.nt + 1 <= kEdgeSmemMax) ? 1u : 0u;
+    Q.edges_f = B.edges_f;
+    Q.edges_d = B.edges_d;
+    const size_t smem = batch_smem_bytes<R, DropGeo<R>>(B.threads, B.nt, Q.smem_edges != 0);
+    e = cudaFuncSetAttribute(batch_trace_kernel<R, DropGeo<R>>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return (int)e;
+    batch_trace_kernel<R, DropGeo<R>><<<B.blocks, B.threads, smem, stream>>>(Q);
+    return (int)cudaGetLastError();
+}
+
+template <class R> int drop_batch_blocks(uint32_t threads, uint32_t nt)
+{
+    const size_t smem = batch_smem_bytes<R, DropGeo<R>>(threads, nt, nt + 1 <= kEdgeSmemMax);
+    cudaFuncSetAttribute(batch_trace_kernel<R, DropGeo<R>>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_trace_kernel<R, DropGeo<R>>, (int)threads, smem) !=
+        cudaSuccess)
         return 0;
     return per_sm;
 }

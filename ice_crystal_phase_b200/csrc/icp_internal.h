@@ -2,6 +2,7 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "../../include/icp_b200.h"
@@ -26,6 +27,10 @@ struct CdfLaunch {
     unsigned* sync; // two counters, zeroed before launch
     uint32_t kind, nt, np, ct, cp, cw;
     double fwd_add, bwd_add;
+    // optional device-side inputs of a record launched without a host round trip:
+    const double* row_add;             // nt values added to every cell of row i (or null)
+    const unsigned long long* pole_fx; // fwd[2], bwd[2] fixed-point pole sums (or null: fwd/bwd_add)
+    double pole_weight;                // mm^2 per unit of pole power (with pole_fx)
 };
 
 int launch_cdf_build(const CdfLaunch& L, cudaStream_t stream);
@@ -80,6 +85,27 @@ int hex_blocks_per_sm_f64(uint32_t slots, uint32_t nt, uint32_t threads);
 int drop_blocks_per_sm_f32(uint32_t slots, uint32_t nt, uint32_t threads);
 int drop_blocks_per_sm_f64(uint32_t slots, uint32_t nt, uint32_t threads);
 
+// One persistent launch over many drop records (icp_batch_kernel.cuh).  recs[r] describes
+// record r exactly as for a single-record launch (first = 0, count = total = its rays, its
+// own mass / stats pointers); the launcher writes the per-record parameter table into
+// h_staging (pinned, n_records x drop_batch_param_bytes) and copies it to d_table.
+struct BatchLaunch {
+    const HexLaunch* recs;
+    uint32_t n_records;
+    void* h_staging;
+    void* d_table;
+    const unsigned long long* d_chunk_begin; // n_records + 1
+    unsigned long long* d_queue;             // zeroed by the caller
+    unsigned long long total_chunks;
+    uint32_t chunk_rays, threads, blocks, nt;
+    const double* edges_d;
+    const float* edges_f;
+};
+size_t drop_batch_param_bytes(uint32_t precision);
+int launch_drop_batch_f32(const BatchLaunch& B, cudaStream_t stream);
+int launch_drop_batch_f64(const BatchLaunch& B, cudaStream_t stream);
+int drop_batch_blocks_per_sm(uint32_t precision, uint32_t threads, uint32_t nt);
+
 // Device buffer that grows on demand and is reused across calls.
 struct Scratch {
     void* ptr = nullptr;
@@ -113,6 +139,82 @@ namespace icp {
 int ensure_float_edges(icp_context* c, const double* d_edges, uint32_t nt);
 // Adds one launch's device statistics (DevStats bytes) into the public stats struct.
 void stats_accumulate(const unsigned char* raw, icp_trace_stats* out);
+// Strip width of the cooperative CDF grid for a (ct, cp) storage grid.
+int choose_cdf_width(icp_context* c, uint32_t ct, uint32_t cp, uint32_t& cw);
+// Public CDF report and quality gates (build_host_cdf) from the kernel's device report.
+int cdf_finish(const CdfDeviceReport& r, const icp_cdf_policy& p, icp_cdf_report* report);
+// Enqueues one cooperative CDF build (no host synchronisation); d_sync[2] and d_report are
+// zeroed here.  pole_fx / row_add select the device-side additions (CdfLaunch).
+int cdf_enqueue(icp_context* c, const double* d_values, uint32_t nt, uint32_t np, uint32_t ct, uint32_t cp,
+                const double* d_edges, double fwd_add, double bwd_add, const unsigned long long* pole_fx,
+                double pole_weight, const double* row_add, double* d_phi, double* d_theta, CdfDeviceReport* d_report,
+                unsigned* d_sync);
+
+// Analytic diffraction rows of one record on the device (icp_drop_device.cu).
+struct DiffractionArgs {
+    const double* edges;              // nt + 1 fine u edges
+    const unsigned long long* rays;   // DevStats::rays of the record (missed follows at +missed_offset)
+    double* row_add;                  // out: nt per-cell additions (row power / np)
+    double* power;                    // out: total diffraction power (mm^2)
+    double weight, wavelength_nm;     // mm^2 per traced ray, vacuum wavelength
+    uint32_t nt, np;
+    uint32_t missed_offset;           // words from rays to missed in DevStats
+    uint32_t pad;
+};
+int launch_diffraction_rows(const DiffractionArgs* d_args, uint32_t count, uint32_t nt, cudaStream_t stream);
+// Drop-record helpers shared by the single-record and batched entries (icp_capi_drop.cu).
+namespace dropx {
+bool sphere_of(const double c[8]);
+void drop_bounds(const double c[8], double& r_center, double& r_out);
+int validate_record(const icp_drop_record* r);
+int validate_grid(const icp_drop_record* r);
+int grid_of(const icp_drop_record* r, icp_grid& g);
+int table_slots(const icp_tuning& t, uint32_t& slots);
+HexLaunch drop_launch(const icp_drop_record* r, const icp_grid* g, const double* d_edges, const float* edges_f,
+                      double* d_mass, void* d_stats, double area_weight, uint32_t slots);
+int finish_report(const icp_drop_record* r, const unsigned char* raw_stats, const CdfDeviceReport& cdf, double power,
+                  double weight, icp_drop_report* rep);
+double projected_area_of(const icp_drop_record* r, int& status);
+} // namespace dropx
+// Offsets (in 64-bit words) of fields of the trace kernel's DevStats.
+uint32_t devstats_rays_word();
+uint32_t devstats_missed_word();
+uint32_t devstats_fwd_word();
+} // namespace icp
+
+namespace icp {
+// Page-locked host staging (copies captured into CUDA graphs must not read pageable memory).
+struct Pinned {
+    void* ptr = nullptr;
+    size_t size = 0;
+    cudaError_t ensure(size_t bytes)
+    {
+        if (bytes <= size) return cudaSuccess;
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        size = 0;
+        const cudaError_t e = cudaMallocHost(&ptr, bytes);
+        if (e == cudaSuccess) size = bytes;
+        return e;
+    }
+    ~Pinned()
+    {
+        if (ptr) cudaFreeHost(ptr);
+    }
+};
+// State of the batched-record entries: host staging, the captured graph, tuned launch shapes.
+struct BatchState {
+    Pinned h_table, h_chunks, h_dargs, h_edges, h_stats, h_reports, h_powers;
+    cudaGraphExec_t exec = nullptr;
+    struct Tuned {
+        uint32_t precision, nt, threads, chunk_rays;
+    };
+    std::vector<Tuned> tuned;
+    ~BatchState()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+    }
+};
 } // namespace icp
 
 // One CUDA device, one non-blocking stream, reusable scratch.
@@ -121,6 +223,9 @@ struct icp_context {
     int sms = 0;
     cudaStream_t stream = nullptr;
     icp::Scratch stats, edges_f, cdf_partial, cdf_report, cdf_sync, cdf_colsum;
-    icp::Scratch rec_edges, rec_mass, rec_phi, rec_theta, rec_batch, rows;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    icp::Scratch rec_edges, rec_mass, rec_phi, rec_theta, rec_batch, rows, dargs;
+    // batched records
+    icp::Scratch b_table, b_chunks, b_queue, b_stats, b_mass, b_rows, b_dargs, b_reports, b_sync, b_phi, b_theta;
+    icp::BatchState batch;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
 };

@@ -107,6 +107,7 @@ typedef struct {
     uint64_t invalid;        /* exits that could not be binned (non-finite direction)       */
     uint64_t encounters;     /* internal boundary interactions traced                       */
     uint64_t missed;         /* sampled rays that miss the particle (drops; never prisms)   */
+    uint64_t gauge_evals;    /* Newton evaluations of the drop surface (non-spherical drops) */
 } icp_trace_stats;
 
 /* Histogram privatisation / launch tuning (all zero = autotuned defaults). */
@@ -298,6 +299,53 @@ int icp_drop_trace_bin(icp_context* ctx, const icp_drop_record* record, uint64_t
 /* Host-buffer entry used by the rainbow_generate drop-in: trace + bin (+ diffraction) + CDF. */
 int icp_drop_generate(icp_context* ctx, const icp_drop_record* record, double* h_phi, double* h_theta, double* h_u,
                       icp_drop_report* report);
+/* The same record with the stored CDF left in caller device arrays d_phi[cp+1],
+ * d_theta[cp*(ct+1)] and (unless NULL) d_u[ct+1]: no host copy of the outputs. */
+int icp_drop_generate_device(icp_context* ctx, const icp_drop_record* record, double* d_phi, double* d_theta,
+                             double* d_u, icp_drop_report* report);
+
+/* ------------------------------------------------------------ batched drop records */
+/* Many drop records in one persistent launch fed from a device work queue (no reference
+ * counterpart: the reference runs one rainbow_generate process per record, driven by
+ * tools/generate_phase_dataset.py:296-311).  Every record keeps its own seed and ray ids,
+ * so its result equals the single-record entry's up to FP64 summation order. */
+typedef struct {
+    double radius_mm;
+    double coefficients[8];
+    double inclination_deg;
+    double interior_index;
+    double wavelength_nm;     /* used by the diffraction stage                              */
+    uint64_t rays, seed;
+    uint32_t diffraction;     /* 1: add the analytic Fraunhofer stage                       */
+    uint32_t reserved;
+} icp_drop_item;
+
+typedef struct {
+    uint32_t nt, np, ct, cp;  /* one (u, phi) grid and storage grid for the whole batch      */
+    uint32_t max_internal_hits, precision;
+    double exterior_index, tail_tolerance, balance_tolerance;
+    icp_cdf_policy policy;
+    uint32_t block_threads;   /* 0: autotuned or 256                                        */
+    uint32_t blocks_per_sm;   /* 0: as many as fit                                          */
+    uint32_t chunk_rays;      /* ray ids per work-queue chunk, 0: autotuned or 8192         */
+    uint32_t use_graph;       /* 1: launch the batch as a captured CUDA graph (replayed when
+                                 the next batch has the same shape)                         */
+} icp_batch_settings;
+
+/* Traces, bins and stores `count` records; phi/theta of record r at d_phi + r*(cp+1) and
+ * d_theta + r*cp*(ct+1) (device arrays).  reports[count] on the host. */
+int icp_drop_batch_generate_device(icp_context* ctx, const icp_drop_item* items, uint32_t count,
+                                   const icp_batch_settings* settings, double* d_phi, double* d_theta,
+                                   icp_drop_report* reports);
+/* The same with host output arrays (phi, theta as above; u[ct+1] shared by all records). */
+int icp_drop_batch_generate(icp_context* ctx, const icp_drop_item* items, uint32_t count,
+                            const icp_batch_settings* settings, double* h_phi, double* h_theta, double* h_u,
+                            icp_drop_report* reports);
+/* Autotuner: times the batch kernel on a bounded sample of `items` for each candidate block
+ * size and chunk size and returns the fastest in settings->block_threads / chunk_rays
+ * (cached in the context per precision and grid, and used when those fields are 0). */
+int icp_drop_batch_autotune(icp_context* ctx, const icp_drop_item* items, uint32_t count,
+                            icp_batch_settings* settings, double* best_rays_per_second);
 
 #ifdef __cplusplus
 }

@@ -280,7 +280,11 @@ class DropGeometry:
 def drop_geometry(coefficients, radius_mm: float) -> DropGeometry:
     """Bounding radii from |T_n| <= 1; rays are sampled on the disk of the exact sphere radius
     (spheres) or of the conservative outer radius, 2 r_out + 1 before the centre."""
-    c = np.asarray(coefficients, dtype=np.float64).copy()
+    c = np.zeros(8)
+    given = np.asarray(coefficients, dtype=np.float64).reshape(-1)
+    if given.size > 8:
+        raise ValueError("At most eight shape coefficients.")
+    c[:given.size] = given
     sphere = bool(np.all(c[1:] == 0))
     r_center = 1 + c[0]
     s = 0.0

@@ -32,7 +32,9 @@ def test_struct_layouts_match_c(icp, tmp_path):
     structs = {"icp_grid": icp.Grid, "icp_trace_stats": icp.TraceStats, "icp_tuning": icp.Tuning,
                "icp_hex_node": icp.HexNode, "icp_cdf_policy": icp.CdfPolicy, "icp_cdf_report": icp.CdfReport,
                "icp_hex_record": icp.HexRecordArgs, "icp_orientation": icp.Orientation,
-               "icp_record_report": icp.RecordReport}
+               "icp_record_report": icp.RecordReport, "icp_drop_record": icp.DropRecordArgs,
+               "icp_drop_report": icp.DropReport, "icp_drop_item": icp.DropItem,
+               "icp_batch_settings": icp.BatchSettings}
     src = tmp_path / "sizes.c"
     src.write_text('#include "icp_b200.h"\n#include <stdio.h>\nint main(void){\n' +
                    "".join(f'printf("{k} %zu\\n", sizeof({k}));\n' for k in structs) + "return 0;}\n")
