@@ -1,0 +1,652 @@
+"""Resumable condition-grid dataset generation on the batched B200 drop path.
+
+Drop-in for the reference's orchestrator (tools/generate_phase_dataset.py): the same config
+file (output_root, generator, radius_mm, force_sphere, temperature_c, pressure_pa, wavelengths,
+inclinations, solver, reserve_gib; an optional "b200" object adds rays, seed, precision,
+max_internal_hits, diffraction and batch_records), the same command line, the same on-disk
+contract -- batch_plan.json with a signature, a .batch.lock, records/i####/w#### written through
+<record>.part -> rename, receipts/<job>.json verified on --resume, progress.json, a free-space
+reserve -- and the same refusal to lower precision, skip or delete anything on failure.
+
+What changes: the reference runs one rainbow_generate process per condition, one at a time
+(generate_phase_dataset.py:296-311).  Here the pending conditions go to the GPU in batches of
+`batch_records` through one persistent launch (icp_drop_batch_generate); every record keeps its
+own seed (derived from the condition indices), so a record does not depend on how the run was
+batched, limited or resumed.  Records are written in rainbow_generate's format.
+
+    python -m ice_crystal_phase_b200.dataset --config CONFIG.json [--execute] [--resume] [--limit N]
+"""
+from __future__ import annotations
+
+import argparse
+import ast
+import hashlib
+import json
+import math
+import os
+import shutil
+import struct
+import sys
+import time
+from contextlib import contextmanager
+from decimal import Decimal, InvalidOperation
+from pathlib import Path
+from typing import Any, Iterator
+
+import numpy as np
+
+VERSION = "rainbow.condition_batch.v1"
+GENERATOR_VERSION = "icp_b200.rainbow.v1"
+ARRAYS = ("phi_cdf.npy", "theta_given_phi_cdf.npy", "u_edges.npy")
+B200_DEFAULTS = {"rays": 10_000_000, "seed": 12345, "precision": "fp32", "max_internal_hits": 1024,
+                 "diffraction": False, "batch_records": 32, "max_unresolved_fraction": 1e-4}
+
+
+# ------------------------------------------------------------------ config (reference semantics)
+def fail_constant(value: str) -> None:
+    raise ValueError(f"Nonfinite JSON constant: {value}")
+
+
+def load_json(path: Path, limit: int = 8 << 20) -> dict[str, Any]:
+    if path.stat().st_size > limit:
+        raise ValueError(f"JSON too large: {path}")
+    with path.open("r", encoding="utf-8-sig") as stream:
+        value = json.load(stream, parse_constant=fail_constant)
+    if not isinstance(value, dict):
+        raise ValueError(f"Expected JSON object: {path}")
+    return value
+
+
+def exact(value: Any) -> Decimal:
+    if isinstance(value, bool):
+        raise ValueError("Boolean is not a numerical parameter")
+    try:
+        d = Decimal(str(value))
+    except InvalidOperation as exc:
+        raise ValueError(f"Invalid decimal: {value}") from exc
+    if not d.is_finite():
+        raise ValueError("Nonfinite parameter")
+    return d
+
+
+def scalar(value: Any, low: float, high: float) -> float:
+    d = exact(value)
+    if not Decimal(str(low)) <= d <= Decimal(str(high)):
+        raise ValueError(f"Parameter {value} is outside [{low}, {high}]")
+    return float(d)
+
+
+def integer(value: Any, low: int, high: int) -> int:
+    d = exact(value)
+    if d != d.to_integral_value() or not low <= d <= high:
+        raise ValueError(f"Expected integer in [{low}, {high}]")
+    return int(d)
+
+
+def flag(value: Any) -> bool:
+    if type(value) is not bool:
+        raise ValueError("Expected JSON true or false")
+    return value
+
+
+def fp32(x: float) -> float:
+    return struct.unpack("<f", struct.pack("<f", x))[0]
+
+
+def wavelengths(spec: dict[str, Any]) -> list[str]:
+    """Inclusive exact-step wavelength list (generate_phase_dataset.py:83-99)."""
+    if set(spec) != {"start_nm", "stop_nm", "step_nm"}:
+        raise ValueError("wavelengths needs start_nm, stop_nm, step_nm")
+    start, stop, step = (exact(spec[k]) for k in ("start_nm", "stop_nm", "step_nm"))
+    if not 380 <= start <= stop <= 830 or step <= 0:
+        raise ValueError("Require 380 <= start <= stop <= 830 and positive step")
+    intervals = (stop - start) / step
+    if intervals != intervals.to_integral_value():
+        raise ValueError("The wavelength range must contain an integer number of steps; no silent endpoint truncation")
+    count = int(intervals) + 1
+    if count > 100000:
+        raise ValueError("Too many wavelengths")
+    values = [format(start + step * i, "f") for i in range(count)]
+    if len({fp32(float(v)) for v in values}) != len(values):
+        raise ValueError("Distinct wavelengths collapse to the same FP32 solver value")
+    return values
+
+
+def inclinations(spec: dict[str, Any]) -> list[str]:
+    """Cell-centred inclinations in [min, max] (generate_phase_dataset.py:102-111)."""
+    if set(spec) != {"min_degrees", "max_degrees", "count", "placement"}:
+        raise ValueError("inclinations needs min_degrees, max_degrees, count, placement")
+    if spec["placement"] != "linear_angle_cell_centers":
+        raise ValueError("Only explicit linear_angle_cell_centers is supported")
+    low, high = exact(spec["min_degrees"]), exact(spec["max_degrees"])
+    count = integer(spec["count"], 1, 100000)
+    if not -90 <= low < high <= 90:
+        raise ValueError("Canonical inclination domain is [-90,90], NOT [0,180]")
+    return [format(low + (high - low) * (Decimal(i) + Decimal("0.5")) / count, "f") for i in range(count)]
+
+
+def normalized_config(raw: dict[str, Any]) -> dict[str, Any]:
+    """The reference's config contract (generate_phase_dataset.py:114-152) plus the optional
+    "b200" object.  Stages other than "incoherent" are the reference's wave-optics patch model,
+    which this build does not implement: they are rejected, as rainbow_generate rejects them."""
+    allowed = {"output_root", "generator", "radius_mm", "force_sphere", "temperature_c", "pressure_pa",
+               "wavelengths", "inclinations", "solver", "reserve_gib"}
+    if set(raw) - {"b200"} != allowed:
+        raise ValueError(f"Unexpected/missing config keys: {(set(raw) - {'b200'}) ^ allowed}")
+    s = raw["solver"]
+    sk = {"grid", "query_theta", "query_phi", "cdf_theta", "cdf_phi", "stage", "device", "focal_offsets",
+          "allow_underresolved", "maximum_coarsening_tv", "cdf_max_l1", "cdf_max_lost_mass"}
+    if not isinstance(s, dict) or set(s) != sk:
+        raise ValueError("Invalid solver keys")
+    out = {k: integer(s[k], 2 if k == "grid" else 1, 32767)
+           for k in ("grid", "query_theta", "query_phi", "cdf_theta", "cdf_phi")}
+    if out["grid"] ** 2 * 4 > 0xFFFFFFFF:
+        raise ValueError("Source index range exceeds the existing solver contract")
+    for axis in ("theta", "phi"):
+        if out["query_" + axis] % out["cdf_" + axis] or out["cdf_" + axis] > out["query_" + axis]:
+            raise ValueError("CDF grids must divide query grids")
+    if s["stage"] not in ("diffraction", "focal", "path", "incoherent"):
+        raise ValueError("Unknown stage")
+    if s["stage"] != "incoherent":
+        raise ValueError(f"Stage {s['stage']} is the reference's wave-optics patch model, which this build does not "
+                         "implement; use stage incoherent (optionally with b200.diffraction)")
+    out["stage"] = s["stage"]
+    out["device"] = integer(s["device"], 0, 128)
+    out["allow_underresolved"] = flag(s["allow_underresolved"])
+    out["maximum_coarsening_tv"] = scalar(s["maximum_coarsening_tv"], 0, 1)
+    out["cdf_max_l1"] = scalar(s["cdf_max_l1"], 0, 1)
+    out["cdf_max_lost_mass"] = scalar(s["cdf_max_lost_mass"], 0, 1)
+    offsets = s["focal_offsets"]
+    if not isinstance(offsets, list) or len(offsets) != 4:
+        raise ValueError("Four focal offsets required")
+    out["focal_offsets"] = [integer(v, 0, 3) for v in offsets]
+    b = dict(B200_DEFAULTS)
+    extra = raw.get("b200", {})
+    if not isinstance(extra, dict) or not set(extra) <= set(B200_DEFAULTS):
+        raise ValueError(f"b200 accepts only {sorted(B200_DEFAULTS)}")
+    b.update(extra)
+    b200 = {"rays": integer(b["rays"], 1, 10 ** 12), "seed": integer(b["seed"], 0, 2 ** 62),
+            "max_internal_hits": integer(b["max_internal_hits"], 1, 1 << 20), "diffraction": flag(b["diffraction"]),
+            "batch_records": integer(b["batch_records"], 1, 4096),
+            "max_unresolved_fraction": scalar(b["max_unresolved_fraction"], 0, 0.999999)}
+    if b["precision"] not in ("fp32", "fp64"):
+        raise ValueError("b200.precision must be fp32 or fp64")
+    b200["precision"] = b["precision"]
+    return {"radius_mm": scalar(raw["radius_mm"], 1e-9, 3), "force_sphere": flag(raw["force_sphere"]),
+            "temperature_c": scalar(raw["temperature_c"], 0, 60),
+            "pressure_pa": scalar(raw["pressure_pa"], 50000, 100000000),
+            "wavelength_nm": wavelengths(raw["wavelengths"]),
+            "inclination_degrees": inclinations(raw["inclinations"]),
+            "inclination_placement": "linear_angle_cell_centers", "material": "water", "solver": out, "b200": b200}
+
+
+def condition_seed(base: int, ii: int, ll: int) -> int:
+    """Seed of condition (ii, ll): a SplitMix64 mix of the base seed and the indices."""
+    x = (base + 0x9E3779B97F4A7C15 * (1 + ii * 100003 + ll)) & 0xFFFFFFFFFFFFFFFF
+    x = ((x ^ (x >> 30)) * 0xBF58476D1CE4E5B9) & 0xFFFFFFFFFFFFFFFF
+    x = ((x ^ (x >> 27)) * 0x94D049BB133111EB) & 0xFFFFFFFFFFFFFFFF
+    return x ^ (x >> 31)
+
+
+# ------------------------------------------------------------------ files
+def sha256(path: Path) -> str:
+    h = hashlib.sha256()
+    with path.open("rb") as f:
+        for block in iter(lambda: f.read(1 << 20), b""):
+            h.update(block)
+    return h.hexdigest()
+
+
+def object_hash(value: Any) -> str:
+    return hashlib.sha256(json.dumps(value, sort_keys=True, separators=(",", ":"), allow_nan=False).encode()).hexdigest()
+
+
+def write_json(path: Path, value: Any) -> None:
+    path.parent.mkdir(parents=True, exist_ok=True)
+    tmp = path.with_suffix(path.suffix + ".tmp")
+    with tmp.open("w", encoding="utf-8", newline="\n") as f:
+        json.dump(value, f, indent=2, ensure_ascii=False, allow_nan=False)
+        f.write("\n")
+    tmp.replace(path)
+
+
+@contextmanager
+def batch_lock(root: Path) -> Iterator[None]:
+    lock = root / ".batch.lock"
+    try:
+        with lock.open("x", encoding="ascii") as f:
+            f.write(f"pid={os.getpid()}\n")
+    except FileExistsError as exc:
+        raise RuntimeError("Batch lock exists. Do not run two writers. After verifying that no batch is running, "
+                           "remove the stale .batch.lock manually.") from exc
+    try:
+        yield
+    finally:
+        lock.unlink()
+
+
+def write_npy(path: Path, array: np.ndarray) -> None:
+    """NPY v1, <f8, C order, header padded to a 64-byte boundary, dictionary text as the
+    command-line writers format it (bytes identical to rainbow_generate's files)."""
+    a = np.ascontiguousarray(array, dtype="<f8")
+    header = "{'descr': '<f8', 'fortran_order': False, 'shape': (" + "".join(f"{d}, " for d in a.shape) + "), }"
+    header += " " * ((64 - (10 + len(header) + 1) % 64) % 64) + "\n"
+    with path.open("xb") as f:
+        f.write(b"\x93NUMPY\x01\x00" + struct.pack("<H", len(header)) + header.encode("latin1"))
+        f.write(a.tobytes())
+
+
+def npy_size(path: Path, expected_shape: tuple[int, ...]) -> int:
+    """Header and length validation only (generate_phase_dataset.py:191-218)."""
+    with path.open("rb") as f:
+        if f.read(6) != b"\x93NUMPY":
+            raise ValueError(f"Not NPY: {path}")
+        ver = f.read(2)
+        if ver == b"\x01\x00":
+            raw = f.read(2)
+            if len(raw) != 2:
+                raise ValueError("Truncated NPY")
+            length = struct.unpack("<H", raw)[0]
+        elif ver == b"\x02\x00":
+            raw = f.read(4)
+            if len(raw) != 4:
+                raise ValueError("Truncated NPY")
+            length = struct.unpack("<I", raw)[0]
+        else:
+            raise ValueError("Unsupported NPY version")
+        if not 0 < length <= 65536:
+            raise ValueError("Invalid NPY header size")
+        text = f.read(length)
+        if len(text) != length:
+            raise ValueError("Truncated NPY header")
+        h = ast.literal_eval(text.decode("latin1"))
+        if h.get("descr") != "<f8" or h.get("fortran_order") is not False or h.get("shape") != expected_shape:
+            raise ValueError(f"Wrong NPY layout: {path}")
+        expected = f.tell() + 8 * math.prod(expected_shape)
+    if path.stat().st_size != expected:
+        raise ValueError(f"Truncated or trailing NPY data: {path}")
+    return expected
+
+
+def close(a: Any, b: float, tol: float = 1e-12) -> bool:
+    return type(a) in (int, float) and math.isfinite(a) and abs(a - b) <= tol * max(1.0, abs(b))
+
+
+def verify_record(path: Path, plan: dict[str, Any], ii: int, ll: int) -> dict[str, Any]:
+    """The reference's record verification (generate_phase_dataset.py:227-287) for this
+    generator's records."""
+    c, s = plan["conditions"], plan["conditions"]["solver"]
+    m = load_json(path / "metadata.json", 1 << 20)
+
+    def require(ok: bool, message: str) -> None:
+        if not ok:
+            raise ValueError(f"{path}: {message}")
+
+    expected = {"complete": True, "schema": "rainbow.phase_cdf.numpy.v2", "generator_version": GENERATOR_VERSION,
+                "coordinate_contract_id": "rainbow.phase_cdf.coordinates.v1",
+                "direction_convention": "physical_propagation", "dtype": "<f8", "order": "C",
+                "density_measure": "solid_angle_sr", "cdf_axis_order": ["phi_cell", "theta_edge"],
+                "theta_count": s["cdf_theta"], "phi_count": s["cdf_phi"],
+                "query_grid": [s["query_theta"], s["query_phi"]], "incident_grid": [s["grid"], s["grid"]],
+                "stage": s["stage"], "force_sphere": c["force_sphere"], "focal_quarter_turn_offsets": s["focal_offsets"]}
+    for key, value in expected.items():
+        require(m.get(key) == value, f"mismatched {key}")
+    require(close(m.get("radius_mm"), fp32(c["radius_mm"])), "radius")
+    require(close(m.get("wavelength_nm"), fp32(float(c["wavelength_nm"][ll]))), "wavelength")
+    alpha = float(c["inclination_degrees"][ii])
+    require(close(m.get("incident_inclination_degrees"), alpha), "inclination")
+    material = m.get("material", {})
+    require(material.get("model") == "water_iapws_r9_97", "material")
+    require(close(material.get("temperature_kelvin"), c["temperature_c"] + 273.15), "temperature")
+    require(close(material.get("pressure_pascal"), c["pressure_pa"]), "pressure")
+    mat = m.get("sampling_frame_columns", [])
+    require(isinstance(mat, list) and len(mat) == 3 and all(isinstance(r, list) and len(r) == 3 for r in mat),
+            "frame shape")
+    require(all(type(v) in (int, float) and math.isfinite(v) for r in mat for v in r), "frame values")
+    cols = [[mat[r][j] for r in range(3)] for j in range(3)]
+    for j in range(3):
+        for k in range(3):
+            require(close(sum(cols[j][r] * cols[k][r] for r in range(3)), float(j == k), 2e-12), "frame orthogonality")
+    cross = [cols[0][1] * cols[1][2] - cols[0][2] * cols[1][1], cols[0][2] * cols[1][0] - cols[0][0] * cols[1][2],
+             cols[0][0] * cols[1][1] - cols[0][1] * cols[1][0]]
+    require(sum(cross[r] * cols[2][r] for r in range(3)) > 1 - 2e-12, "frame handedness")
+    angle = math.radians(alpha)
+    ki = [math.cos(angle), -math.sin(angle), 0.0]
+    require(all(abs(cols[2][r] - ki[r]) < 2e-6 for r in range(3)), "incident direction/sign")
+    geometry, cs = m.get("geometry", {}), m.get("cross_sections", {})
+    area = geometry.get("projected_area_mm2")
+    require(type(area) in (int, float) and math.isfinite(area) and area > 0, "projected area")
+    require(geometry.get("projected_area_converged") is True and geometry.get("convexity_verified") is True,
+            "area validation")
+    require(cs.get("model") == "geometric_nonabsorbing" and cs.get("wave_scattering_cross_section_computed") is False,
+            "cross-section model")
+    require(cs.get("scattering_mm2") == area and cs.get("extinction_mm2") == area and cs.get("absorption_mm2") == 0,
+            "cross sections")
+    q = m.get("quality", {})
+    require(q.get("invalid_values") == 0 and q.get("incomplete_directions") == 0, "invalid optical data")
+    require(q.get("allow_underresolved") is s["allow_underresolved"], "underresolution policy")
+    require(s["allow_underresolved"] or q.get("underresolved_directions") == 0, "underresolution not authorized")
+    for key, cfg in (("cdf_l1_mass_error", "cdf_max_l1"), ("cdf_lost_probability_mass", "cdf_max_lost_mass")):
+        value = q.get(key)
+        require(type(value) in (int, float) and math.isfinite(value) and 0 <= value <= s[cfg], key)
+    sp = m.get("storage_processing", {})
+    require(sp.get("additional_filter") == "none", "unexpected global smoothing")
+    tv = sp.get("coarsening_tv")
+    require(type(tv) in (int, float) and math.isfinite(tv) and 0 <= tv <= s["maximum_coarsening_tv"],
+            "coarsening error")
+    hg = m.get("hg", {})
+    require(hg.get("target") == "saved_cdf" and type(hg.get("g")) in (float, int) and -1 < hg["g"] < 1, "HG target")
+    nt, np_ = s["cdf_theta"], s["cdf_phi"]
+    sizes = {name: npy_size(path / name, shape)
+             for name, shape in zip(ARRAYS, ((np_ + 1,), (np_, nt + 1), (nt + 1,)))}
+    return {"metadata_sha256": sha256(path / "metadata.json"), "npy_sizes": sizes, "hg_g": hg["g"],
+            "projected_area_mm2": area, "underresolved_directions": q.get("underresolved_directions"),
+            "coarsening_tv": tv}
+
+
+# ------------------------------------------------------------------ records
+def record_metadata(c: dict, ii: int, ll: int, spec, rep, water) -> dict:
+    """metadata.json in the layout rainbow_generate writes (apps/rainbow_generate.cpp)."""
+    s, b = c["solver"], c["b200"]
+    k, e0, e1 = list(rep.ki), list(rep.e0), list(rep.e1)
+    area = rep.projected_area_mm2
+    coeff = list(spec.coefficients)
+    sphere = all(x == 0 for x in coeff[1:])
+    t = rep.trace
+    statuses = ["exhausted", "tail_tolerance_reached", "interaction_limit", "ambiguous_boundary", "invalid_input",
+                "numerical_failure", "output_overflow", "replay_mismatch"]
+    lam_f = fp32(float(c["wavelength_nm"][ll]))
+    return {
+        "coordinate_contract_id": "rainbow.phase_cdf.coordinates.v1", "direction_convention": "physical_propagation",
+        "particle_frame_handedness": "right", "particle_up_axis": [0, 1, 0], "shape_polar_axis": [0, -1, 0],
+        "sampling_frame_layout": "rows_xyz_columns_e0_e1_k", "sampling_frame_map": "local_column_to_particle_column",
+        "theta_zero": "forward", "theta_pi": "backward", "azimuth_periodic": True,
+        "inclination_definition": "ki=(cos(alpha),-sin(alpha),0); alpha=0 is +x; positive alpha points downward",
+        "geometry": {"projected_area_mm2": area, "projected_area_m2": area * 1e-6,
+                     "projected_area_method": "analytic_sphere" if sphere else
+                     "convex_surface_integral_azimuth_analytic_gauss_legendre",
+                     "projected_area_shape": "solver_shape_coefficients_promoted_to_fp64",
+                     "projected_area_converged": True, "projected_area_error_is_rigorous_bound": False,
+                     "convexity_verified": True,
+                     "convexity_method": "analytic_sphere" if sphere else "dense_curvature_sampling",
+                     "incident_axis_particle_frame": k, "sampled_disk_area_mm2": rep.sampled_area_mm2,
+                     "traced_hit_area_mm2": rep.incident_area_mm2},
+        "cross_sections": {"model": "geometric_nonabsorbing", "scattering_mm2": area, "extinction_mm2": area,
+                           "absorption_mm2": 0, "scattering_m2": area * 1e-6, "extinction_m2": area * 1e-6,
+                           "absorption_m2": 0, "assignment": "Csca=Cext=Aproj; Cabs=0 (transport model assumption)",
+                           "wave_scattering_cross_section_computed": False},
+        "material": {"model": "water_iapws_r9_97", "wavelength_convention": "vacuum_nm",
+                     "wavelength_requested_nm": float(c["wavelength_nm"][ll]), "wavelength_evaluated_nm": lam_f,
+                     "ambient_model": "unit_absolute_index_air_approximation",
+                     "absorption_model": "ignored_k_equals_zero", "interior_index_evaluated_fp64": water.refractive_index,
+                     "interior_index_solver_fp32": spec.interior_index, "exterior_index_solver": 1,
+                     "refractive_index_release": "IAPWS R9-97",
+                     "density_model": "Tanaka2001/Kell1975 at 1 atm with UNESCO-1981 secant bulk modulus",
+                     "temperature_kelvin": c["temperature_c"] + 273.15, "pressure_pascal": c["pressure_pa"],
+                     "density_kg_m3": water.density_kg_m3},
+        "diffraction_policy": {"name": "fraunhofer_equal_area_circle_v1" if spec.diffraction else "none",
+                               "computed": bool(spec.diffraction),
+                               "selected_output_includes_diffraction": bool(spec.diffraction),
+                               "primary_sigma_degrees": None, "secondary_sigma_degrees": None,
+                               "power_mm2": rep.diffraction_area_mm2,
+                               "query_dtheta_degrees": 180.0 / s["query_theta"],
+                               "query_dphi_degrees": 360.0 / s["query_phi"]},
+        "schema": "rainbow.phase_cdf.numpy.v2", "complete": True, "dtype": "<f8", "order": "C",
+        "theta_count": s["cdf_theta"], "phi_count": s["cdf_phi"], "density_measure": "solid_angle_sr",
+        "cell_model": "constant_density_per_spherical_cell", "coordinates": "u=(1-cos(theta))/2; v=(phi+pi)/(2*pi)",
+        "theta_definition": "angle_between_incident_and_outgoing_propagation_directions",
+        "cdf_axis_order": ["phi_cell", "theta_edge"], "phi_range_rad": [-math.pi, math.pi],
+        "normalization": "integral_p_domega_equals_one", "input_polarization": "unpolarized",
+        "incident_total_intensity": 1, "single_scattering_albedo": 1, "collision_model": "geometric_projected_area",
+        "projected_area_storage": "metadata.geometry.projected_area_mm2", "stage": s["stage"],
+        "radius_mm": spec.radius_mm, "wavelength_nm": lam_f, "exterior_index": 1,
+        "interior_index": spec.interior_index, "force_sphere": c["force_sphere"],
+        "incident_grid": [s["grid"], s["grid"]], "incident_grid_used": False,
+        "query_frame_axis": [fp32(x) for x in k], "query_frame_e0": [fp32(x) for x in e0],
+        "sampling_frame_columns": [[e0[r], e1[r], k[r]] for r in range(3)], "shape_coefficients": coeff,
+        "shape_source": "sphere" if c["force_sphere"] else "Sadeghi2012_TableI",
+        "focal_quarter_turn_offsets": s["focal_offsets"], "diffraction_transition_contrast": 0,
+        "generator_version": GENERATOR_VERSION,
+        "backend": f"b200_batched_trace_{b['precision']}_fixed_point_histogram_cooperative_cdf",
+        "sampling": {"generator": "counter_splitmix64_open52_v1", "method": "uniform_disk_covering_silhouette",
+                     "rays": spec.rays, "seed": spec.seed, "missed_rays": t.missed, "outgoing_samples": t.outputs,
+                     "weight": "disk_area / rays * path_power", "trace_precision": b["precision"]},
+        "transport_audit": {"incident_mm2": rep.incident_area_mm2, "escaped_mm2": rep.escaped_area_mm2,
+                            "unresolved_mm2": rep.unresolved_area_mm2,
+                            "unresolved_fraction": rep.unresolved_area_mm2 / rep.incident_area_mm2,
+                            "maximum_balance_error": t.max_ray_balance,
+                            "maximum_interface_balance_error": t.max_interface_balance,
+                            "max_internal_hits": b["max_internal_hits"], "tail_tolerance_per_ray": 1e-12,
+                            "max_unresolved_fraction": b["max_unresolved_fraction"], "internal_encounters": t.encounters,
+                            "status_counts": {statuses[i]: int(t.status_counts[i]) for i in range(8)}},
+        "histogram": {"theta_count": s["query_theta"], "phi_count": s["query_phi"], "mass_mm2": rep.histogram_mass_mm2,
+                      "relative_mass_audit_error": rep.histogram_relative_error,
+                      "forward_axis_mass_mm2": rep.forward_mass_mm2, "backward_axis_mass_mm2": rep.backward_mass_mm2,
+                      "boundary_snapped_samples": t.snapped},
+        "quality": {"source_coverage_certified": False, "angular_convergence_certified": False,
+                    "missing_source_cells": 0, "invalid_values": int(t.invalid), "incomplete_directions": 0,
+                    "underresolved_directions": 0, "allow_underresolved": s["allow_underresolved"],
+                    "cdf_l1_mass_error": rep.cdf.l1_error, "cdf_maximum_cell_mass_error": rep.cdf.maximum_cell_error,
+                    "cdf_lost_positive_cells": int(rep.cdf.lost_cells), "cdf_lost_probability_mass": rep.cdf.lost_mass,
+                    "maximum_accepted_l1_mass_error": s["cdf_max_l1"],
+                    "maximum_accepted_lost_probability_mass": s["cdf_max_lost_mass"]},
+        "incident_inclination_degrees": float(c["inclination_degrees"][ii]),
+        "query_grid": [s["query_theta"], s["query_phi"]],
+        "storage_processing": {"additional_filter": "none", "additional_filter_is_paper_diffraction": False,
+                               "sigma_degrees": 0, "aggregation": "nested_solid_angle_mass_preserving",
+                               "aggregation_integral_relative_change": rep.cdf.aggregation_relative_error,
+                               "coarsening_tv": rep.cdf.coarsening_tv,
+                               "maximum_accepted_coarsening_tv": s["maximum_coarsening_tv"]},
+        "hg": {"g": rep.cdf.g_stored, "method": "first_moment_of_saved_cell_pdf", "target": "saved_cdf",
+               "cosine_convention": "dot(incident_propagation,outgoing_propagation)", "axis_particle_frame": k,
+               "g_source": rep.cdf.g_source, "cdf_mass_check": rep.cdf.cdf_mass},
+        "timing": {"batch_seconds": rep.seconds_trace},
+    }
+
+
+def accept(rep, c: dict) -> None:
+    """rainbow_generate's record gates: statuses other than exhausted / tail / interaction
+    limit, balance, unbinnable exits, the global unresolved budget, the histogram audit."""
+    t = rep.trace
+    if (t.invalid or any(t.status_counts[i] for i in range(3, 8)) or not rep.incident_area_mm2 > 0
+            or not rep.escaped_area_mm2 > 0 or not t.max_ray_balance <= 1e-10):
+        raise RuntimeError("Drop trace is NOT accepted. Inspect per-ray statuses and unresolved power; "
+                           "do not renormalize it away.")
+    if rep.unresolved_area_mm2 / rep.incident_area_mm2 > c["b200"]["max_unresolved_fraction"]:
+        raise RuntimeError("Unresolved light exceeds explicit global budget.")
+    if abs((rep.escaped_area_mm2 + rep.unresolved_area_mm2) / rep.incident_area_mm2 - 1) > 1e-10:
+        raise RuntimeError("Energy balance failed.")
+    if rep.histogram_relative_error > 1e-10:
+        raise RuntimeError("Histogram mass differs from independent escaped-ray audit.")
+
+
+def write_record(path: Path, phi, theta, u, metadata: dict) -> None:
+    part = Path(str(path) + ".part")
+    if path.exists():
+        raise FileExistsError(f"Dataset already exists; refusing to overwrite: {path}")
+    part.mkdir(parents=True, exist_ok=False)
+    write_npy(part / "phi_cdf.npy", phi)
+    write_npy(part / "theta_given_phi_cdf.npy", theta)
+    write_npy(part / "u_edges.npy", u)
+    with (part / "metadata.json").open("x", encoding="utf-8", newline="\n") as f:
+        json.dump(metadata, f, indent=2, allow_nan=False)
+        f.write("\n")
+    part.rename(path)
+
+
+class GpuBackend:
+    """The batched device library: a context for the run and one persistent launch per batch."""
+
+    def __init__(self):
+        import ice_crystal_phase_b200 as icp  # noqa: PLC0415 (only needed to execute)
+
+        self.icp = icp
+
+    def library_sha256(self) -> str:
+        return sha256(self.icp.LIB_PATH)
+
+    def context(self, device: int):
+        return self.icp.Context(device)
+
+    def generate(self, ctx, c: dict, todo: list) -> list:
+        return generate(self.icp, ctx, c, todo)
+
+
+def generate(icp, ctx, c: dict, todo: list) -> list:
+    """One GPU batch: todo = [(ii, ll), ...] -> (spec, water, phi, theta, u, report) per condition."""
+    s, b = c["solver"], c["b200"]
+    radius = fp32(c["radius_mm"])
+    shape = icp.RaindropShape.make(radius, c["force_sphere"]).coefficients
+    specs, waters = [], []
+    for ii, ll in todo:
+        lam = fp32(float(c["wavelength_nm"][ll]))
+        water = icp.evaluate_water_optics(lam, c["temperature_c"], c["pressure_pa"])
+        n = fp32(water.refractive_index)
+        if not 1.0 <= n <= 2.0:
+            raise ValueError("interior_index must be in [1,2]; exterior_index is 1.")
+        specs.append(icp.DropSpec(shape, radius, n, b["rays"], seed=condition_seed(b["seed"], ii, ll),
+                                  inclination_deg=float(c["inclination_degrees"][ii]), wavelength_nm=lam,
+                                  diffraction=b["diffraction"]))
+        waters.append(water)
+    settings = icp.batch_settings(s["query_theta"], s["query_phi"], s["cdf_theta"], s["cdf_phi"],
+                                  max_internal_hits=b["max_internal_hits"],
+                                  precision=icp.ICP_FP64 if b["precision"] == "fp64" else icp.ICP_FP32,
+                                  max_l1_error=s["cdf_max_l1"], max_lost_mass=s["cdf_max_lost_mass"],
+                                  max_coarsening_tv=s["maximum_coarsening_tv"])
+    out = icp.generate_drop_batch(ctx, specs, settings)
+    return [(specs[i], waters[i], out.phi[i], out.theta[i], out.u_edges, out.reports[i]) for i in range(len(todo))]
+
+
+def run(argv: list[str] | None = None, backend=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--config", type=Path, required=True)
+    ap.add_argument("--out-root", type=Path)
+    ap.add_argument("--generator", type=Path, help="accepted for compatibility; the batched library generates")
+    ap.add_argument("--wavelength-range", nargs=3, metavar=("START_NM", "STOP_NM", "STEP_NM"))
+    ap.add_argument("--radius-mm")
+    ap.add_argument("--inclination-count", type=int)
+    ap.add_argument("--allow-underresolved", action="store_true")
+    ap.add_argument("--resume", action="store_true")
+    ap.add_argument("--limit", type=int, help="run at most this many NEW records, without changing the planned dataset")
+    mode = ap.add_mutually_exclusive_group()
+    mode.add_argument("--execute", action="store_true", help="actually start the simulations; default is a dry run")
+    mode.add_argument("--dry-run", action="store_true")
+    args = ap.parse_args(argv)
+    if args.limit is not None and args.limit <= 0:
+        raise ValueError("limit must be positive")
+    raw = load_json(args.config)
+    if args.wavelength_range:
+        raw["wavelengths"] = dict(zip(("start_nm", "stop_nm", "step_nm"), args.wavelength_range))
+    if args.radius_mm is not None:
+        raw["radius_mm"] = args.radius_mm
+    if args.inclination_count is not None:
+        raw["inclinations"]["count"] = args.inclination_count
+    if args.allow_underresolved:
+        raw["solver"]["allow_underresolved"] = True
+    c = normalized_config(raw)
+    root = Path(args.out_root or raw["output_root"])
+    root = (root if root.is_absolute() else Path.cwd() / root).resolve()
+    reserve = int(scalar(raw["reserve_gib"], 0, 1000000) * (1 << 30))
+    nt, np_ = c["solver"]["cdf_theta"], c["solver"]["cdf_phi"]
+    payload = 8 * ((np_ + 1) + np_ * (nt + 1) + (nt + 1))
+    estimate_per_record = payload + (128 << 10)
+    ni, nl = len(c["inclination_degrees"]), len(c["wavelength_nm"])
+    print(f"conditions={ni} x {nl} = {ni * nl}; CDF={nt}x{np_}; array_bytes_per_record={payload}")
+    print(f"array_total_TB={payload * ni * nl / 1e12:.6f}; output={root}")
+    print(f"inclination_centers=[{c['inclination_degrees'][0]}, {c['inclination_degrees'][-1]}] degrees")
+    print(f"wavelengths=[{c['wavelength_nm'][0]}, {c['wavelength_nm'][-1]}] nm; inclusive exact-step endpoints")
+    print(f"Batches of {c['b200']['batch_records']} records per persistent GPU launch; "
+          f"{c['b200']['rays']} rays per record ({c['b200']['precision']}).")
+    if c["solver"]["maximum_coarsening_tv"] == 1:
+        print("WARNING: maximum_coarsening_tv=1 is not an accuracy acceptance threshold.")
+    if not args.execute:
+        print("DRY RUN: no simulations or files written. Add --execute to start.")
+        return 0
+    backend = backend or GpuBackend()
+    spec = {"version": VERSION, "conditions": c, "binary_sha256": {"libicp_b200": backend.library_sha256()}}
+    signature = object_hash(spec)
+    plan = {**spec, "signature": signature, "record_layout": "records/i{incident_index:04d}/w{wavelength_index:04d}"}
+    root.mkdir(parents=True, exist_ok=True)
+    with batch_lock(root):
+        manifest = root / "batch_plan.json"
+        if manifest.exists():
+            if not args.resume:
+                raise FileExistsError("Dataset plan exists; use --resume with identical configuration and binaries")
+            if load_json(manifest) != json.loads(json.dumps(plan)):
+                raise ValueError("Resume rejected: configuration/binaries differ from batch_plan.json")
+        else:
+            if any(p.name != ".batch.lock" for p in root.iterdir()):
+                raise ValueError("Refusing to adopt a nonempty directory without this batch plan")
+            write_json(manifest, plan)
+        plan = load_json(manifest)
+        pending, skipped = [], 0
+        for ii in range(ni):
+            for ll in range(nl):
+                job = f"i{ii:04d}_w{ll:04d}"
+                path = root / f"records/i{ii:04d}/w{ll:04d}"
+                receipt = root / "receipts" / (job + ".json")
+                if Path(str(path) + ".part").exists():
+                    raise ValueError(f"Incomplete .part exists: {path}.part; inspect and move it manually before retrying")
+                if path.exists():
+                    if not args.resume or not receipt.exists():
+                        raise ValueError(f"Existing record without authorized resume/receipt: {path}")
+                    saved = load_json(receipt)
+                    actual = verify_record(path, plan, ii, ll)
+                    if (saved.get("signature") != signature or saved.get("incident_index") != ii
+                            or saved.get("wavelength_index") != ll or saved.get("record") != actual):
+                        raise ValueError(f"Resume receipt/content mismatch: {path}")
+                    skipped += 1
+                else:
+                    if receipt.exists():
+                        raise ValueError(f"Receipt exists but record missing: {path}")
+                    pending.append((ii, ll, job, path, receipt))
+        selected = pending if args.limit is None else pending[:args.limit]
+        needed = len(selected) * estimate_per_record + reserve
+        free = shutil.disk_usage(root).free
+        print(f"verified_existing={skipped}; pending={len(pending)}; this_run={len(selected)}; free_TB={free / 1e12:.3f}")
+        if needed > free:
+            raise RuntimeError(f"Insufficient free space: estimated {needed} bytes including reserve; available {free}")
+        start = time.monotonic()
+        done = 0
+        per = c["b200"]["batch_records"]
+        with backend.context(c["solver"]["device"]) as ctx:
+            for b0 in range(0, len(selected), per):
+                chunk = selected[b0:b0 + per]
+                free = shutil.disk_usage(root).free
+                if free < len(chunk) * estimate_per_record + reserve:
+                    raise RuntimeError("Free-space reserve reached; stopping without lowering precision")
+                results = backend.generate(ctx, c, [(ii, ll) for ii, ll, *_ in chunk])
+                for (ii, ll, job, path, receipt), (sp, water, phi, theta, u, rep) in zip(chunk, results):
+                    accept(rep, c)
+                    path.parent.mkdir(parents=True, exist_ok=True)
+                    write_record(path, phi, theta, u, record_metadata(c, ii, ll, sp, rep, water))
+                    checked = verify_record(path, plan, ii, ll)
+                    write_json(receipt, {"signature": signature, "incident_index": ii, "wavelength_index": ll,
+                                         "record": checked})
+                    done += 1
+                    write_json(root / "progress.json", {"completed": skipped + done, "total": ni * nl,
+                                                        "last_record": job,
+                                                        "elapsed_seconds_this_run": time.monotonic() - start})
+                    print(f"[{skipped + done}/{ni * nl}] {job}: alpha={c['inclination_degrees'][ii]} "
+                          f"lambda={c['wavelength_nm'][ll]} g={checked['hg_g']:.9g} "
+                          f"Aproj_mm2={checked['projected_area_mm2']:.9g}", flush=True)
+        complete = skipped + len(selected) == ni * nl
+        write_json(root / "progress.json", {"completed": skipped + len(selected), "total": ni * nl,
+                                            "complete": complete, "elapsed_seconds_this_run": time.monotonic() - start})
+        print("Dataset complete." if complete else "Requested subset finished. Repeat with --resume to continue the same plan.")
+    return 0
+
+
+def main() -> None:
+    try:
+        raise SystemExit(run())
+    except KeyboardInterrupt:
+        print("Interrupted. No automatic cleanup of records/.part directories.", file=sys.stderr)
+        raise SystemExit(130)
+    except (OSError, ValueError, RuntimeError, KeyError, TypeError, struct.error) as exc:
+        print(f"generate_phase_dataset: {exc}", file=sys.stderr)
+        raise SystemExit(1)
+
+
+if __name__ == "__main__":
+    main()
