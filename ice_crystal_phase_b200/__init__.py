@@ -209,6 +209,7 @@ _FUNCS = {
     "icp_drop_batch_generate": (C.c_int, [_P, C.POINTER(DropItem), C.c_uint32, C.POINTER(BatchSettings), _D, _D, _D,
                                           C.POINTER(DropReport)]),
     "icp_drop_batch_autotune": (C.c_int, [_P, C.POINTER(DropItem), C.c_uint32, C.POINTER(BatchSettings), _D]),
+    "icp_mlp_gemm_bf16": (C.c_int, [_P, _P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _P, C.c_int]),
 }
 
 
@@ -809,3 +810,12 @@ def autotune_drop_batch(ctx: Context, specs: list, settings: BatchSettings) -> f
     best = C.c_double()
     check(LIB.icp_drop_batch_autotune(ctx.handle, _items(specs), len(specs), C.byref(settings), C.byref(best)))
     return best.value
+
+
+# ---------------------------------------------------------------- surrogate building blocks
+def mlp_gemm_bf16(ctx: Context, a_ptr: int, b_ptr: int, m: int, n: int, k: int, c_ptr: int, accumulate: bool = False,
+                  split_k: int = 1) -> None:
+    """C[m x n] (FP32, device) = / += A[m x k] * B[n x k]^T (BF16, device, K contiguous) on the
+    tensor cores (icp_mlp_gemm_bf16)."""
+    check(LIB.icp_mlp_gemm_bf16(ctx.handle, C.c_void_p(a_ptr), C.c_void_p(b_ptr), m, n, k, split_k, C.c_void_p(c_ptr),
+                                int(accumulate)))

@@ -44,6 +44,8 @@ UNITS = {
     "icp_capi_drop.cu": ["-fmad=false"],
     "icp_drop_device.cu": ["-fmad=false"],
     "icp_capi_batch.cu": ["-fmad=false"],
+    "icp_mlp_gemm.cu": [],
+    "icp_capi_mlp.cu": ["-fmad=false"],
     "icp_cdf_static.cu": ["-fmad=false"],
 }
 

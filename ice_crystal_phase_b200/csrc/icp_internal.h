@@ -227,5 +227,7 @@ struct icp_context {
     // batched records
     icp::Scratch b_table, b_chunks, b_queue, b_stats, b_mass, b_rows, b_dargs, b_reports, b_sync, b_phi, b_theta;
     icp::BatchState batch;
+    // surrogate
+    icp::Scratch mlp_error;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
 };

@@ -1,0 +1,52 @@
+"""The surrogate's tensor-core GEMM (tcgen05.mma, TMEM accumulator, TMA-fed, 128-byte swizzled
+K-major tiles) against an FP64 product of the same BF16 values: FP32 accumulation, so the error
+stays at FP32 rounding of the partial sums."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+def _bf16(shape, gen, scale=1.0):
+    return (torch.randn(*shape, generator=gen) * scale).to(torch.bfloat16)
+
+
+@pytest.mark.parametrize("m,n,k", [(128, 64, 64), (256, 128, 320), (384, 256, 1024), (128, 256, 64)])
+def test_gemm_store_matches_fp64(ctx, icp, m, n, k):
+    gen = torch.Generator().manual_seed(m * 7 + n + k)
+    a, b = _bf16((m, k), gen), _bf16((n, k), gen)
+    ref = a.double().numpy() @ b.double().numpy().T
+    da, db = a.cuda(), b.cuda()
+    dc = torch.full((m, n), float("nan"), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    icp.mlp_gemm_bf16(ctx, da.data_ptr(), db.data_ptr(), m, n, k, dc.data_ptr())
+    got = dc.cpu().double().numpy()
+    assert np.isfinite(got).all()
+    err = np.abs(got - ref).max() / np.abs(ref).max()
+    assert err <= 1e-5, err
+
+
+@pytest.mark.parametrize("split", [1, 3, 16])
+def test_gemm_split_k_accumulates(ctx, icp, split):
+    m, n, k = 256, 256, 4096
+    gen = torch.Generator().manual_seed(split)
+    a, b = _bf16((m, k), gen, 0.1), _bf16((n, k), gen, 0.1)
+    base = torch.randn(m, n, generator=gen)
+    ref = base.double().numpy() + a.double().numpy() @ b.double().numpy().T
+    dc = base.cuda()
+    da, db = a.cuda(), b.cuda()
+    torch.cuda.synchronize()
+    icp.mlp_gemm_bf16(ctx, da.data_ptr(), db.data_ptr(), m, n, k, dc.data_ptr(), accumulate=True, split_k=split)
+    got = dc.cpu().double().numpy()
+    assert np.abs(got - ref).max() / np.abs(ref).max() <= 2e-5
+
+
+def test_gemm_rejects_bad_shapes(ctx, icp):
+    d = torch.zeros(256, 256, dtype=torch.bfloat16, device="cuda")
+    c = torch.zeros(256, 256, dtype=torch.float32, device="cuda")
+    for m, n, k in [(100, 64, 64), (128, 96, 64), (128, 64, 100)]:
+        with pytest.raises(icp.InvalidArgument):
+            icp.mlp_gemm_bf16(ctx, d.data_ptr(), d.data_ptr(), m, n, k, c.data_ptr())
