@@ -167,6 +167,19 @@ class BatchSettings(C.Structure):
                 ("use_graph", C.c_uint32)]
 
 
+class SurrogateConfig(C.Structure):
+    _fields_ = [("nt", C.c_uint32), ("np", C.c_uint32), ("hidden", C.c_uint32), ("input_width", C.c_uint32),
+                ("theta_frequencies", C.c_uint32), ("phi_frequencies", C.c_uint32), ("max_records", C.c_uint32),
+                ("reserved", C.c_uint32), ("log_radius_mm", C.c_double * 2), ("wavelength_nm", C.c_double * 2),
+                ("log_wavelength_over_radius", C.c_double * 2), ("index_center", C.c_double),
+                ("index_scale", C.c_double), ("coefficient_scale", C.c_double * 8)]
+
+
+class Adam(C.Structure):
+    _fields_ = [("lr", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float),
+                ("weight_decay", C.c_float), ("step", C.c_uint32)]
+
+
 # ---------------------------------------------------------------- library loading
 _P = C.c_void_p
 _D = C.POINTER(C.c_double)
@@ -210,6 +223,20 @@ _FUNCS = {
                                           C.POINTER(DropReport)]),
     "icp_drop_batch_autotune": (C.c_int, [_P, C.POINTER(DropItem), C.c_uint32, C.POINTER(BatchSettings), _D]),
     "icp_mlp_gemm_bf16": (C.c_int, [_P, _P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _P, C.c_int]),
+    "icp_surrogate_default_config": (C.c_int, [C.POINTER(SurrogateConfig)]),
+    "icp_surrogate_parameter_count": (C.c_uint64, [C.POINTER(SurrogateConfig)]),
+    "icp_surrogate_record_features": (C.c_int, [C.POINTER(SurrogateConfig), C.POINTER(DropItem), C.c_uint32, _P]),
+    "icp_surrogate_cell_features": (C.c_int, [C.POINTER(SurrogateConfig), _P]),
+    "icp_surrogate_create": (C.c_int, [_P, C.POINTER(SurrogateConfig), C.POINTER(_P)]),
+    "icp_surrogate_destroy": (None, [_P]),
+    "icp_surrogate_set_parameters": (C.c_int, [_P, _P, C.c_uint64]),
+    "icp_surrogate_get_parameters": (C.c_int, [_P, _P, C.c_uint64]),
+    "icp_surrogate_gradient": (C.c_int, [_P, C.POINTER(DropItem), C.c_uint32, _P, _P, _D]),
+    "icp_surrogate_train_step": (C.c_int, [_P, C.POINTER(DropItem), C.c_uint32, _P, C.POINTER(Adam), _D]),
+    "icp_surrogate_predict": (C.c_int, [_P, C.POINTER(DropItem), C.c_uint32, _P]),
+    "icp_surrogate_generate": (C.c_int, [_P, C.POINTER(DropItem), C.c_uint32, C.c_uint32, C.c_uint32,
+                                         C.POINTER(CdfPolicy), _P, _P, C.POINTER(CdfReport)]),
+    "icp_surrogate_targets": (C.c_int, [_P, _P, _P, C.c_uint32, _P]),
 }
 
 
@@ -819,3 +846,107 @@ def mlp_gemm_bf16(ctx: Context, a_ptr: int, b_ptr: int, m: int, n: int, k: int, 
     tensor cores (icp_mlp_gemm_bf16)."""
     check(LIB.icp_mlp_gemm_bf16(ctx.handle, C.c_void_p(a_ptr), C.c_void_p(b_ptr), m, n, k, split_k, C.c_void_p(c_ptr),
                                 int(accumulate)))
+
+
+# ---------------------------------------------------------------- learned surrogate
+def surrogate_config(**overrides) -> SurrogateConfig:
+    """Default surrogate configuration (256 x 512 cells, 3 x 256 hidden, input width 128) with
+    field overrides; array fields take sequences."""
+    cfg = SurrogateConfig()
+    check(LIB.icp_surrogate_default_config(C.byref(cfg)))
+    for k, v in overrides.items():
+        if not hasattr(cfg, k):
+            raise ValueError(f"unknown surrogate config field {k!r}")
+        if isinstance(v, (list, tuple)):
+            arr = getattr(cfg, k)
+            for i, x in enumerate(v):
+                arr[i] = x
+        else:
+            setattr(cfg, k, v)
+    return cfg
+
+
+def surrogate_parameter_count(cfg: SurrogateConfig) -> int:
+    n = int(LIB.icp_surrogate_parameter_count(C.byref(cfg)))
+    if n == 0:
+        raise InvalidArgument(ICP_ERR_INVALID_ARGUMENT, "Invalid surrogate configuration.")
+    return n
+
+
+def surrogate_record_features(cfg: SurrogateConfig, specs) -> np.ndarray:
+    """16 BF16 feature bits per record (uint16), computed by the library on the host."""
+    items = _items(specs)
+    out = np.zeros((len(specs), 16), dtype=np.uint16)
+    check(LIB.icp_surrogate_record_features(C.byref(cfg), items, len(specs), C.c_void_p(out.ctypes.data)))
+    return out
+
+
+def surrogate_cell_features(cfg: SurrogateConfig) -> np.ndarray:
+    """The cell table: nt*np rows x (input_width - 16) BF16 bits (uint16), theta-major cells."""
+    out = np.zeros((cfg.nt * cfg.np, cfg.input_width - 16), dtype=np.uint16)
+    check(LIB.icp_surrogate_cell_features(C.byref(cfg), C.c_void_p(out.ctypes.data)))
+    return out
+
+
+class Surrogate:
+    """Handle of one surrogate network on a context (icp_surrogate_*).  Device arrays are passed
+    as integer pointers (e.g. torch's data_ptr())."""
+
+    def __init__(self, ctx: Context, cfg: SurrogateConfig):
+        self.ctx, self.cfg = ctx, cfg
+        self.n_params = surrogate_parameter_count(cfg)
+        self.cells = cfg.nt * cfg.np
+        h = _P()
+        check(LIB.icp_surrogate_create(ctx.handle, C.byref(cfg), C.byref(h)))
+        self.handle = h
+
+    def close(self) -> None:
+        if self.handle:
+            LIB.icp_surrogate_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_parameters(self, params: np.ndarray) -> None:
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        check(LIB.icp_surrogate_set_parameters(self.handle, C.c_void_p(p.ctypes.data), p.size))
+
+    def parameters(self) -> np.ndarray:
+        p = np.zeros(self.n_params, dtype=np.float32)
+        check(LIB.icp_surrogate_get_parameters(self.handle, C.c_void_p(p.ctypes.data), p.size))
+        return p
+
+    def gradient(self, specs, target_ptr: int, with_grad: bool = True) -> tuple[float, np.ndarray | None]:
+        g = np.zeros(self.n_params, dtype=np.float32) if with_grad else None
+        loss = C.c_double()
+        check(LIB.icp_surrogate_gradient(self.handle, _items(specs), len(specs), C.c_void_p(target_ptr),
+                                         C.c_void_p(g.ctypes.data) if with_grad else None, C.byref(loss)))
+        return loss.value, g
+
+    def train_step(self, specs, target_ptr: int, opt: Adam) -> float:
+        loss = C.c_double()
+        check(LIB.icp_surrogate_train_step(self.handle, _items(specs), len(specs), C.c_void_p(target_ptr),
+                                           C.byref(opt), C.byref(loss)))
+        return loss.value
+
+    def predict(self, specs, logits_ptr: int) -> None:
+        check(LIB.icp_surrogate_predict(self.handle, _items(specs), len(specs), C.c_void_p(logits_ptr)))
+
+    def generate(self, specs, ct: int, cp: int, phi_ptr: int, theta_ptr: int, policy: CdfPolicy | None = None,
+                 raise_on_audit: bool = True) -> list:
+        """Records from the prediction (device phi / theta); returns the per-record CDF reports."""
+        pol = policy or CdfPolicy(1e-10, 1e-12, 1.0)
+        reps = (CdfReport * len(specs))()
+        st = LIB.icp_surrogate_generate(self.handle, _items(specs), len(specs), ct, cp, C.byref(pol),
+                                        C.c_void_p(phi_ptr), C.c_void_p(theta_ptr), reps)
+        if st != ICP_OK and (raise_on_audit or st != ICP_ERR_AUDIT):
+            check(st)
+        return list(reps)
+
+    def targets(self, phi_ptr: int, theta_ptr: int, count: int, target_ptr: int) -> None:
+        check(LIB.icp_surrogate_targets(self.handle, C.c_void_p(phi_ptr), C.c_void_p(theta_ptr), count,
+                                        C.c_void_p(target_ptr)))

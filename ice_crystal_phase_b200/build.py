@@ -45,6 +45,7 @@ UNITS = {
     "icp_drop_device.cu": ["-fmad=false"],
     "icp_capi_batch.cu": ["-fmad=false"],
     "icp_mlp_gemm.cu": [],
+    "icp_mlp.cu": [],
     "icp_capi_mlp.cu": ["-fmad=false"],
     "icp_cdf_static.cu": ["-fmad=false"],
 }

@@ -1,0 +1,261 @@
+// icp_mlp.cu -- the surrogate's kernels around the tensor-core GEMMs: input rows, the per-record
+// softmax loss, the head's backward pass, Adam with the BF16 weight copies, and cell probabilities
+// of stored CDF records (the training targets).  All are bandwidth-bound streaming kernels:
+// 16-byte loads / stores along the contiguous dimension, one block per 128-1024 rows.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "icp_mlp.h"
+
+namespace icp::mlp {
+
+namespace {
+
+__device__ __forceinline__ float silu_of(float z) { return z / (1.0f + __expf(-z)); }
+__device__ __forceinline__ float silu_grad_of(float z)
+{
+    const float s = 1.0f / (1.0f + __expf(-z));
+    return s * (1.0f + z * (1.0f - s));
+}
+
+// X rows: thread per 8 BF16 (one uint4) of a row.
+__global__ void features_kernel(const uint4* __restrict__ rec16, const uint4* __restrict__ cells, uint32_t C,
+                                uint32_t q_row, uint64_t total, uint4* __restrict__ X)
+{
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const uint64_t m = t / q_row;
+    const uint32_t q = (uint32_t)(t - m * q_row);
+    const uint32_t r = (uint32_t)(m / C), c = (uint32_t)(m - (uint64_t)r * C);
+    X[t] = q < 2 ? rec16[2u * r + q] : cells[(uint64_t)c * (q_row - 2) + (q - 2)];
+}
+
+// XT[k][m]: thread per 8 consecutive rows m of one column k.
+__global__ void features_t_kernel(const __nv_bfloat16* __restrict__ rec16, const uint4* __restrict__ cellsT, uint32_t C,
+                                  uint32_t K0, uint32_t records, __nv_bfloat16* __restrict__ XT)
+{
+    const uint64_t per_k = (uint64_t)records * C / 8u;
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= per_k * K0) return;
+    const uint32_t k = (uint32_t)(t / per_k);
+    const uint64_t m8 = t - (uint64_t)k * per_k;
+    const uint64_t m = 8u * m8;
+    const uint32_t r = (uint32_t)(m / C), c = (uint32_t)(m - (uint64_t)r * C);
+    uint4 v;
+    if (k < 16) {
+        const __nv_bfloat16 x = rec16[16u * r + k];
+        const uint32_t w = (uint32_t)__bfloat16_as_ushort(x) * 0x10001u;
+        v = make_uint4(w, w, w, w);
+    } else {
+        v = cellsT[((uint64_t)(k - 16) * C + c) / 8u];
+    }
+    reinterpret_cast<uint4*>(XT + (uint64_t)k * records * C)[m8] = v;
+}
+
+__device__ __forceinline__ double block_sum(double v, double* sh)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const uint32_t w = threadIdx.x >> 5, l = threadIdx.x & 31u, nw = blockDim.x >> 5;
+    __syncthreads();
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    double s = 0;
+    for (uint32_t i = 0; i < nw; ++i) s += sh[i];
+    return s;
+}
+__device__ __forceinline__ float block_max(float v, float* sh)
+{
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const uint32_t w = threadIdx.x >> 5, l = threadIdx.x & 31u, nw = blockDim.x >> 5;
+    __syncthreads();
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    float s = sh[0];
+    for (uint32_t i = 1; i < nw; ++i) s = fmaxf(s, sh[i]);
+    return s;
+}
+
+// One block per record: max, log-sum-exp (FP64 sums), KL loss and dy.
+__global__ void __launch_bounds__(1024) softmax_loss_kernel(const float* __restrict__ y, const float* __restrict__ p,
+                                                            uint32_t C, float scale, float* __restrict__ dy,
+                                                            double* __restrict__ loss)
+{
+    __shared__ double shd[32];
+    __shared__ float shf[32];
+    const uint64_t base = (uint64_t)blockIdx.x * C;
+    const float4* y4 = reinterpret_cast<const float4*>(y + base);
+    const float4* p4 = reinterpret_cast<const float4*>(p + base);
+    const uint32_t n4 = C / 4u;
+    float mx = -INFINITY;
+    for (uint32_t i = threadIdx.x; i < n4; i += blockDim.x) {
+        const float4 v = y4[i];
+        mx = fmaxf(mx, fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)));
+    }
+    mx = block_max(mx, shf);
+    double se = 0, py = 0, plp = 0;
+    for (uint32_t i = threadIdx.x; i < n4; i += blockDim.x) {
+        const float4 v = y4[i], q = p4[i];
+        const float ys[4] = {v.x, v.y, v.z, v.w}, ps[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            se += (double)__expf(ys[j] - mx);
+            if (ps[j] > 0.0f) {
+                py += (double)ps[j] * (double)(ys[j] - mx);
+                plp += (double)ps[j] * log((double)ps[j]);
+            }
+        }
+    }
+    se = block_sum(se, shd);
+    py = block_sum(py, shd);
+    plp = block_sum(plp, shd);
+    const double lse = log(se); // relative to mx
+    if (threadIdx.x == 0) loss[blockIdx.x] = plp - py + lse; // sum p = 1
+    const float lsef = (float)lse + mx;
+    float4* d4 = reinterpret_cast<float4*>(dy + base);
+    for (uint32_t i = threadIdx.x; i < n4; i += blockDim.x) {
+        const float4 v = y4[i], q = p4[i];
+        d4[i] = make_float4((__expf(v.x - lsef) - q.x) * scale, (__expf(v.y - lsef) - q.y) * scale,
+                            (__expf(v.z - lsef) - q.z) * scale, (__expf(v.w - lsef) - q.w) * scale);
+    }
+}
+
+// Block = H threads (thread n = column n) over kRows rows: row-major dz3 coalesced across the
+// block, the column-major copy written 8 rows (16 bytes) at a time per thread.
+constexpr uint32_t kHeadRows = 256;
+__global__ void head_backward_kernel(const __nv_bfloat16* __restrict__ z3, const float* __restrict__ dy,
+                                     const float* __restrict__ w4, uint32_t M, uint32_t H, __nv_bfloat16* __restrict__ dz3,
+                                     __nv_bfloat16* __restrict__ dz3T, float* __restrict__ dw4, float* __restrict__ db3)
+{
+    const uint32_t n = threadIdx.x;
+    const uint64_t m0 = (uint64_t)blockIdx.x * kHeadRows;
+    const float w = w4[n];
+    float sw = 0.0f, sb = 0.0f;
+    for (uint32_t r8 = 0; r8 < kHeadRows; r8 += 8) {
+        __align__(16) __nv_bfloat16 col[8];
+#pragma unroll
+        for (uint32_t k = 0; k < 8; ++k) {
+            const uint64_t m = m0 + r8 + k;
+            const float z = __bfloat162float(z3[m * H + n]);
+            const float d = dy[m];
+            const float g = d * w * silu_grad_of(z);
+            sw = fmaf(d, silu_of(z), sw);
+            sb += g;
+            const __nv_bfloat16 gb = __float2bfloat16_rn(g);
+            dz3[m * H + n] = gb;
+            col[k] = gb;
+        }
+        *reinterpret_cast<uint4*>(dz3T + (uint64_t)n * M + m0 + r8) = *reinterpret_cast<const uint4*>(col);
+    }
+    atomicAdd(&dw4[n], sw);
+    atomicAdd(&db3[n], sb);
+}
+
+__global__ void adam_kernel(AdamArgs a)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const float g = a.g[i];
+    const float m = a.beta1 * a.m[i] + (1.0f - a.beta1) * g;
+    const float v = a.beta2 * a.v[i] + (1.0f - a.beta2) * g * g;
+    a.m[i] = m;
+    a.v[i] = v;
+    const float mh = m / a.bias1, vh = v / a.bias2;
+    a.p[i] -= a.lr * (mh / (sqrtf(vh) + a.eps) + a.weight_decay * a.p[i]);
+}
+
+__global__ void weight_copies_kernel(WeightViews w)
+{
+    const uint32_t H = w.H, K0 = w.K0;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t n1 = H * K0, n2 = H * H;
+    if (i < n1) {
+        w.w1b[i] = __float2bfloat16_rn(w.w1[i]);
+    } else if (i < n1 + n2) {
+        const uint32_t j = i - n1, r = j / H, c = j - r * H;
+        const __nv_bfloat16 b = __float2bfloat16_rn(w.w2[j]);
+        w.w2b[j] = b;
+        w.w2t[c * H + r] = b;
+    } else if (i < n1 + 2 * n2) {
+        const uint32_t j = i - n1 - n2, r = j / H, c = j - r * H;
+        const __nv_bfloat16 b = __float2bfloat16_rn(w.w3[j]);
+        w.w3b[j] = b;
+        w.w3t[c * H + r] = b;
+    }
+}
+
+__global__ void cdf_cells_kernel(const double* __restrict__ phi, const double* __restrict__ theta, uint32_t ct,
+                                 uint32_t cp, uint64_t total, float* __restrict__ p)
+{
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const uint64_t cells = (uint64_t)ct * cp;
+    const uint32_t r = (uint32_t)(t / cells);
+    const uint32_t k = (uint32_t)(t - (uint64_t)r * cells);
+    const uint32_t i = k / cp, j = k - i * cp;
+    const double* a = phi + (uint64_t)r * (cp + 1);
+    const double* T = theta + ((uint64_t)r * cp + j) * (ct + 1);
+    p[t] = (float)((a[j + 1] - a[j]) * (T[i + 1] - T[i]));
+}
+
+unsigned blocks_of(uint64_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+} // namespace
+
+int launch_features(const __nv_bfloat16* rec16, const __nv_bfloat16* cells, uint32_t records, uint32_t C, uint32_t K0,
+                    __nv_bfloat16* X, __nv_bfloat16* XT, cudaStream_t st)
+{
+    if (K0 % 64 || C % 128 || !records) return -1;
+    const uint32_t q_row = K0 / 8u;
+    const uint64_t total = (uint64_t)records * C * q_row;
+    features_kernel<<<blocks_of(total, 256), 256, 0, st>>>(reinterpret_cast<const uint4*>(rec16),
+                                                           reinterpret_cast<const uint4*>(cells), C, q_row, total,
+                                                           reinterpret_cast<uint4*>(X));
+    if (XT) {
+        // the column-major cell table follows the row-major one in the same allocation
+        const uint4* cellsT = reinterpret_cast<const uint4*>(cells + (uint64_t)C * (K0 - 16));
+        const uint64_t n = (uint64_t)records * C / 8u * K0;
+        features_t_kernel<<<blocks_of(n, 256), 256, 0, st>>>(rec16, cellsT, C, K0, records, XT);
+    }
+    return (int)cudaGetLastError();
+}
+
+int launch_softmax_loss(const float* y, const float* p, uint32_t records, uint32_t C, float scale, float* dy,
+                        double* loss, cudaStream_t st)
+{
+    if (C % 4 || !records) return -1;
+    softmax_loss_kernel<<<records, 1024, 0, st>>>(y, p, C, scale, dy, loss);
+    return (int)cudaGetLastError();
+}
+
+int launch_head_backward(const __nv_bfloat16* z3, const float* dy, const float* w4, uint32_t M, uint32_t H,
+                         __nv_bfloat16* dz3, __nv_bfloat16* dz3T, float* dw4, float* db3, cudaStream_t st)
+{
+    if (M % kHeadRows || H > 1024 || H % 32) return -1;
+    head_backward_kernel<<<M / kHeadRows, H, 0, st>>>(z3, dy, w4, M, H, dz3, dz3T, dw4, db3);
+    return (int)cudaGetLastError();
+}
+
+int launch_adam(const AdamArgs& a, cudaStream_t st)
+{
+    adam_kernel<<<blocks_of(a.n, 256), 256, 0, st>>>(a);
+    return (int)cudaGetLastError();
+}
+
+int launch_weight_copies(const WeightViews& w, cudaStream_t st)
+{
+    const uint64_t n = (uint64_t)w.H * w.K0 + 2ull * w.H * w.H;
+    weight_copies_kernel<<<blocks_of(n, 256), 256, 0, st>>>(w);
+    return (int)cudaGetLastError();
+}
+
+int launch_cdf_cells(const double* phi, const double* theta, uint32_t records, uint32_t ct, uint32_t cp, float* p,
+                     cudaStream_t st)
+{
+    const uint64_t total = (uint64_t)records * ct * cp;
+    cdf_cells_kernel<<<blocks_of(total, 256), 256, 0, st>>>(phi, theta, ct, cp, total, p);
+    return (int)cudaGetLastError();
+}
+
+} // namespace icp::mlp

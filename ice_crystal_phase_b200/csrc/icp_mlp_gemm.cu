@@ -31,7 +31,8 @@ constexpr uint32_t kA = 128u * 128u; // bytes of one A stage: 128 rows x 64 BF16
 
 template <int N> __host__ __device__ constexpr int stages() { return N <= 128 ? 4 : 3; }
 template <int N> __host__ __device__ constexpr uint32_t stage_bytes() { return kA + (uint32_t)N * 128u; }
-template <int N> constexpr size_t smem_bytes() { return 1024 + (size_t)stages<N>() * stage_bytes<N>() + 256; }
+// 1024 (alignment) + stages + barriers / TMEM slot (256) + column sums of the bias gradient (1024)
+template <int N> constexpr size_t smem_bytes() { return 1024 + (size_t)stages<N>() * stage_bytes<N>() + 256 + 1024; }
 
 __device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
 __device__ __forceinline__ float silu_grad(float z)
@@ -54,6 +55,31 @@ __device__ __forceinline__ void store_bf16x32(__nv_bfloat16* dst, const float (&
         d[q] = make_uint4(w[0], w[1], w[2], w[3]);
     }
 }
+// Column sums of a warp's 32 x 32 block (lane = row, v[i] = column i): a butterfly
+// reduce-scatter in 31 shuffles, after which lane L holds the sum of column L in v[0].
+__device__ __forceinline__ float warp_column_sum(float (&v)[32], uint32_t lane)
+{
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) {
+        const bool upper = (lane & (uint32_t)off) != 0;
+#pragma unroll
+        for (int j = 0; j < off; ++j) {
+            const float send = upper ? v[j] : v[j + off];
+            const float keep = upper ? v[j + off] : v[j];
+            v[j] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+        }
+    }
+    return v[0];
+}
+
+// Column-major copy of a warp's 32 rows x 32 columns: for each column, the 32 lanes write 32
+// consecutive rows (64 contiguous bytes).
+__device__ __forceinline__ void store_bf16x32_t(__nv_bfloat16* dst, uint32_t ld, const float (&v)[32])
+{
+#pragma unroll
+    for (int i = 0; i < 32; ++i) dst[(size_t)i * ld] = __float2bfloat16_rn(v[i]);
+}
+
 __device__ __forceinline__ void load_bf16x32(const __nv_bfloat16* src, float (&v)[32])
 {
     const uint4* s = reinterpret_cast<const uint4*>(src);
@@ -84,7 +110,10 @@ __global__ void __launch_bounds__(128, 1)
     uint64_t* done = empty + S;
     uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
+    float* colsum = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(full) + 256);
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    if constexpr (EPI == kBackprop)
+        for (uint32_t i = threadIdx.x; i < (uint32_t)N; i += blockDim.x) colsum[i] = 0.0f;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < S; ++s) {
@@ -173,6 +202,7 @@ __global__ void __launch_bounds__(128, 1)
 #pragma unroll
                 for (int i = 0; i < 32; ++i) v[i] = silu(v[i]);
                 if (g.out_h) store_bf16x32(g.out_h + (size_t)m * N + c, v);
+                if (g.out_hT) store_bf16x32_t(g.out_hT + (size_t)c * g.ld_t + m, g.ld_t, v);
                 if constexpr (EPI == kHead) {
 #pragma unroll
                     for (int i = 0; i < 32; ++i) yacc = fmaf(v[i], g.head_w[c + i], yacc);
@@ -182,10 +212,21 @@ __global__ void __launch_bounds__(128, 1)
                 load_bf16x32(g.z_prev + (size_t)m * N + c, z);
 #pragma unroll
                 for (int i = 0; i < 32; ++i) v[i] *= silu_grad(z[i]);
-                store_bf16x32(g.out_dz + (size_t)m * N + c, v);
+                if (g.out_dz) store_bf16x32(g.out_dz + (size_t)m * N + c, v);
+                if (g.out_dzT) store_bf16x32_t(g.out_dzT + (size_t)c * g.ld_t + m, g.ld_t, v);
+                if (g.out_db) atomicAdd(&colsum[c + lane], warp_column_sum(v, lane));
             }
         }
-        if constexpr (EPI == kHead) g.out_y[m] = yacc + g.head_b;
+        if constexpr (EPI == kHead) {
+            const float y = yacc + g.head_b;
+            if (g.out_y) g.out_y[m] = y;
+            if (g.out_mass) g.out_mass[m] = exp((double)y);
+        }
+    }
+    if constexpr (EPI == kBackprop) {
+        __syncthreads();
+        if (g.out_db && ready)
+            for (uint32_t i = threadIdx.x; i < (uint32_t)N; i += blockDim.x) atomicAdd(&g.out_db[i], colsum[i]);
     }
     umma::fence_before_sync();
     __syncthreads();

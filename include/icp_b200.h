@@ -356,6 +356,70 @@ int icp_drop_batch_autotune(icp_context* ctx, const icp_drop_item* items, uint32
 int icp_mlp_gemm_bf16(icp_context* ctx, const void* d_a, const void* d_b, uint32_t m, uint32_t n, uint32_t k,
                       uint32_t split_k, float* d_c, int accumulate);
 
+/* A small MLP conditioned on a drop record's parameters that predicts the log cell mass of its
+ * record on an (nt x np) cell grid: input row = 16 record features + cell features (theta,
+ * phi harmonics), three SiLU layers of `hidden` units (BF16 weights and activations, FP32
+ * accumulation on the tensor cores), a linear head to one value y per cell.  Cell probability =
+ * softmax of y over the record's cells.  Trained by the mean per-record KL divergence of the
+ * tracer's cell probabilities from the prediction. */
+typedef struct icp_surrogate icp_surrogate;
+
+typedef struct {
+    uint32_t nt, np;               /* cell grid: theta rows x phi columns, nt * np % 256 == 0   */
+    uint32_t hidden;               /* 128 or 256                                                */
+    uint32_t input_width;          /* 64 or 128: 16 record features, then the cell features     */
+    uint32_t theta_frequencies;    /* sin / cos (k theta), k = 1..F                             */
+    uint32_t phi_frequencies;      /* sin / cos (l phi), l = 1..G; 4 + 2F + 2G <= width - 16   */
+    uint32_t max_records;          /* records per call (sizes the activation buffers)          */
+    uint32_t reserved;
+    double log_radius_mm[2];       /* ranges mapped onto [-1, 1] by the record features         */
+    double wavelength_nm[2];
+    double log_wavelength_over_radius[2]; /* ln(lambda / radius), both in mm                    */
+    double index_center, index_scale;     /* (n - center) / scale                               */
+    double coefficient_scale[8];          /* shape coefficient c_n enters as c_n * scale_n     */
+} icp_surrogate_config;
+
+typedef struct {
+    float lr, beta1, beta2, eps, weight_decay;
+    uint32_t step;                 /* 1-based step number (bias correction)                     */
+} icp_adam;
+
+/* Defaults for the batched-record distribution: 256 x 512 cells, 256 hidden, width 128,
+ * F = 50, G = 4, radius 0.1-3 mm, wavelength 400-700 nm, 16 records per call. */
+int icp_surrogate_default_config(icp_surrogate_config* cfg);
+/* FP32 parameters, in this order: W1[H][K0], b1[H], W2[H][H], b2[H], W3[H][H], b3[H], w4[H],
+ * head bias (1): H*K0 + 2H^2 + 4H + 1. */
+uint64_t icp_surrogate_parameter_count(const icp_surrogate_config* cfg);
+/* Host-side feature rows (no GPU): 16 BF16 values per record, and the cell table of
+ * nt*np rows x (input_width - 16) BF16 values (theta-major cells, as the histogram). */
+int icp_surrogate_record_features(const icp_surrogate_config* cfg, const icp_drop_item* items, uint32_t count,
+                                  uint16_t* out);
+int icp_surrogate_cell_features(const icp_surrogate_config* cfg, uint16_t* out);
+int icp_surrogate_create(icp_context* ctx, const icp_surrogate_config* cfg, icp_surrogate** out);
+void icp_surrogate_destroy(icp_surrogate* s);
+/* Loads the parameters (and their BF16 copies); resets the Adam moments. */
+int icp_surrogate_set_parameters(icp_surrogate* s, const float* h_params, uint64_t count);
+int icp_surrogate_get_parameters(icp_surrogate* s, float* h_params, uint64_t count);
+/* Mean per-record KL divergence of d_target[count][nt*np] (FP32 cell probabilities, device,
+ * each record summing to 1) from the prediction, and (h_grad not NULL) its gradient in the
+ * parameter layout. */
+int icp_surrogate_gradient(icp_surrogate* s, const icp_drop_item* items, uint32_t count, const float* d_target,
+                           float* h_grad, double* loss);
+/* One training step: the gradient above, then Adam on the device. loss may be NULL. */
+int icp_surrogate_train_step(icp_surrogate* s, const icp_drop_item* items, uint32_t count, const float* d_target,
+                             const icp_adam* opt, double* loss);
+/* y of every cell: d_logits[count][nt*np] (device FP32), log cell mass up to a per-record constant. */
+int icp_surrogate_predict(icp_surrogate* s, const icp_drop_item* items, uint32_t count, float* d_logits);
+/* Records from the prediction: cell mass exp(y) through the CDF build at storage grid (ct, cp);
+ * phi / theta of record r at d_phi + r*(cp+1), d_theta + r*cp*(ct+1) (device), one CDF report
+ * per record (host; status = the record's audit result). */
+int icp_surrogate_generate(icp_surrogate* s, const icp_drop_item* items, uint32_t count, uint32_t ct, uint32_t cp,
+                           const icp_cdf_policy* policy, double* d_phi, double* d_theta, icp_cdf_report* reports);
+/* Training targets: cell probabilities of `count` stored records at the surrogate's grid
+ * (ct = nt, cp = np), d_target[count][nt*np] (device FP32). */
+int icp_surrogate_targets(icp_surrogate* s, const double* d_phi, const double* d_theta, uint32_t count,
+                          float* d_target);
+
 #ifdef __cplusplus
 }
 #endif

@@ -34,7 +34,8 @@ def test_struct_layouts_match_c(icp, tmp_path):
                "icp_hex_record": icp.HexRecordArgs, "icp_orientation": icp.Orientation,
                "icp_record_report": icp.RecordReport, "icp_drop_record": icp.DropRecordArgs,
                "icp_drop_report": icp.DropReport, "icp_drop_item": icp.DropItem,
-               "icp_batch_settings": icp.BatchSettings}
+               "icp_batch_settings": icp.BatchSettings, "icp_surrogate_config": icp.SurrogateConfig,
+               "icp_adam": icp.Adam}
     src = tmp_path / "sizes.c"
     src.write_text('#include "icp_b200.h"\n#include <stdio.h>\nint main(void){\n' +
                    "".join(f'printf("{k} %zu\\n", sizeof({k}));\n' for k in structs) + "return 0;}\n")

@@ -1,0 +1,152 @@
+"""The learned surrogate on the GPU (tcgen05 forward / backward GEMMs and their fused
+epilogues, softmax loss, head backward, Adam) against the numpy FP64 oracle with the same BF16
+rounding points; the records it emits; its training targets from tracer records."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from oracle import surrogate_oracle as SO
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+SMALL = {"nt": 32, "np": 64, "input_width": 64, "theta_frequencies": 18, "phi_frequencies": 4, "max_records": 4}
+
+
+def _specs(icp, n, seed):
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        r = float(np.float32(math.exp(rng.uniform(math.log(0.1), math.log(3.0)))))
+        lam = float(rng.uniform(400, 700))
+        out.append(icp.DropSpec(icp.RaindropShape.make(r).coefficients, r,
+                                float(np.float32(icp.evaluate_water_optics(lam).refractive_index)), rays=200_000,
+                                seed=int(rng.integers(1, 2 ** 62)), inclination_deg=float(rng.uniform(-90, 90)),
+                                wavelength_nm=lam, diffraction=True))
+    return out
+
+
+def _setup(icp, over, R, seed):
+    cfg = icp.surrogate_config(**over)
+    oc = SO.Config.of(cfg)
+    specs = _specs(icp, R, seed)
+    rec = SO.from_bits(icp.surrogate_record_features(cfg, specs))
+    X = SO.inputs(oc, rec, SO.from_bits(icp.surrogate_cell_features(cfg)))
+    rng = np.random.default_rng(seed)
+    p = SO.init_parameters(oc, seed)
+    p[oc.hidden * oc.input_width:oc.hidden * oc.input_width + oc.hidden] = rng.normal(0, 0.1, oc.hidden)  # b1
+    C = cfg.nt * cfg.np
+    # a peaked target with empty cells, each record summing to one in FP32
+    t = rng.gamma(0.3, size=(R, C))
+    t[:, rng.choice(C, C // 10, replace=False)] = 0.0
+    t = (t / t.sum(axis=1, keepdims=True)).astype(np.float32)
+    return cfg, oc, specs, X, p, t
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, float) - b) / max(np.linalg.norm(b), 1e-30))
+
+
+@pytest.mark.parametrize("over,R", [(SMALL, 3), ({**SMALL, "hidden": 128, "input_width": 128, "theta_frequencies": 40},
+                                                  2)])
+def test_gradient_matches_oracle(ctx, icp, over, R):
+    cfg, oc, specs, X, p, t = _setup(icp, over, R, 11 + R)
+    with icp.Surrogate(ctx, cfg) as s:
+        s.set_parameters(p)
+        dt = torch.from_numpy(t).cuda()
+        torch.cuda.synchronize()
+        loss, g = s.gradient(specs, dt.data_ptr())
+    want_loss, want = SO.gradient(oc, p, X, t.astype(np.float64), R, emulate=True)
+    assert abs(loss - want_loss) <= 1e-5 * abs(want_loss), (loss, want_loss)
+    gw, ww = SO.unpack(oc, g), SO.unpack(oc, want)
+    for k in ("W1", "b1", "W2", "b2", "W3", "b3", "w4"):
+        assert _rel(gw[k], ww[k]) <= 2e-3, (k, _rel(gw[k], ww[k]))
+    assert gw["hb"][0] == 0.0
+
+
+def test_train_step_applies_adam(ctx, icp):
+    cfg, oc, specs, X, p, t = _setup(icp, SMALL, 2, 21)
+    lr = 1e-3
+    with icp.Surrogate(ctx, cfg) as s:
+        s.set_parameters(p)
+        dt = torch.from_numpy(t).cuda()
+        torch.cuda.synchronize()
+        _, g = s.gradient(specs, dt.data_ptr())
+        l1 = s.train_step(specs, dt.data_ptr(), icp.Adam(lr, 0.9, 0.999, 1e-8, 0.0, 1))
+        p1 = s.parameters()
+        # a few more steps on the same records lower the loss
+        for k in range(2, 30):
+            last = s.train_step(specs, dt.data_ptr(), icp.Adam(lr, 0.9, 0.999, 1e-8, 0.0, k))
+    want, _, _ = SO.adam(p, g, np.zeros(p.size), np.zeros(p.size), 1, lr)
+    d = np.abs(p1.astype(np.float64) - want)
+    # step 1 of Adam moves every parameter by ~lr * sign(g): the GPU and oracle agree except where
+    # |g| is at the level of the FP32 gradient noise
+    assert np.mean(d <= 1e-2 * lr) >= 0.995
+    assert d.max() <= 2.01 * lr
+    assert p1[-1] == p[-1]
+    assert last < 0.9 * l1
+
+
+def test_generated_records_are_the_predicted_softmax(ctx, icp):
+    cfg, oc, specs, X, p, t = _setup(icp, SMALL, 3, 31)
+    ct, cp = 16, 32
+    C = cfg.nt * cfg.np
+    with icp.Surrogate(ctx, cfg) as s:
+        s.set_parameters(p)
+        y = torch.empty(3 * C, dtype=torch.float32, device="cuda")
+        phi = torch.empty(3 * (cp + 1), dtype=torch.float64, device="cuda")
+        theta = torch.empty(3 * cp * (ct + 1), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        s.predict(specs, y.data_ptr())
+        reps = s.generate(specs, ct, cp, phi.data_ptr(), theta.data_ptr())
+    assert all(r.status == 0 for r in reps)
+    yo = SO.forward(oc, p, X, emulate=True)["y"]
+    yd = y.cpu().double().numpy()
+    assert np.abs(yd - yo).max() <= 1e-3 * max(1.0, np.abs(yo).max())
+    a = phi.cpu().numpy().reshape(3, cp + 1)
+    T = theta.cpu().numpy().reshape(3, cp, ct + 1)
+    for r in range(3):
+        q = np.exp(yd[r * C:(r + 1) * C] - yd[r * C:(r + 1) * C].max())
+        q = (q / q.sum()).reshape(cfg.nt, cfg.np)
+        agg = q.reshape(ct, cfg.nt // ct, cp, cfg.np // cp).sum(axis=(1, 3))
+        stored = np.diff(a[r])[None, :] * np.diff(T[r], axis=1).T
+        assert a[r][0] == 0 and a[r][-1] == 1 and np.all(np.diff(a[r]) >= 0)
+        assert np.abs(stored - agg).sum() <= 1e-9
+
+
+def test_targets_are_cell_probabilities_of_records(ctx, icp):
+    cfg = icp.surrogate_config(**SMALL)
+    specs = _specs(icp, 3, 41)
+    nt, np_ = cfg.nt, cfg.np
+    st = icp.batch_settings(nt, np_, max_internal_hits=10, precision=icp.ICP_FP32)
+    res = icp.generate_drop_batch(ctx, specs, st)
+    a = np.asarray(res.phi).reshape(3, np_ + 1)
+    T = np.asarray(res.theta).reshape(3, np_, nt + 1)
+    dphi = torch.from_numpy(a.ravel().copy()).cuda()
+    dth = torch.from_numpy(T.ravel().copy()).cuda()
+    out = torch.empty(3 * nt * np_, dtype=torch.float32, device="cuda")
+    with icp.Surrogate(ctx, cfg) as s:
+        torch.cuda.synchronize()
+        s.targets(dphi.data_ptr(), dth.data_ptr(), 3, out.data_ptr())
+    got = out.cpu().numpy().reshape(3, nt, np_)
+    for r in range(3):
+        want = (np.diff(a[r])[None, :] * np.diff(T[r], axis=1).T).astype(np.float32)
+        assert np.array_equal(got[r], want)
+        assert abs(got[r].astype(np.float64).sum() - 1) <= 1e-5
+
+
+def test_rejects_bad_calls(ctx, icp):
+    cfg = icp.surrogate_config(**SMALL)
+    with icp.Surrogate(ctx, cfg) as s:
+        with pytest.raises(icp.InvalidArgument):
+            s.set_parameters(np.zeros(10, dtype=np.float32))
+        bad = np.zeros(s.n_params, dtype=np.float32)
+        bad[3] = np.nan
+        with pytest.raises(icp.InvalidArgument):
+            s.set_parameters(bad)
+        y = torch.empty(5 * s.cells, dtype=torch.float32, device="cuda")
+        with pytest.raises(icp.InvalidArgument):
+            s.predict(_specs(icp, 5, 1), y.data_ptr())  # more than max_records

@@ -1,0 +1,104 @@
+"""Learned surrogate, host side (no GPU): the library's feature rows equal the oracle's bit for
+bit, the oracle's analytic gradient matches central finite differences, its BF16 emulation only
+rounds, and the library rejects invalid configurations."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from oracle import surrogate_oracle as SO
+
+
+def _specs(icp, n, seed=5):
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        r = float(np.float32(math.exp(rng.uniform(math.log(0.1), math.log(3.0)))))
+        lam = float(rng.uniform(400, 700))
+        out.append(icp.DropSpec(icp.RaindropShape.make(r).coefficients, r,
+                                float(np.float32(icp.evaluate_water_optics(lam).refractive_index)), rays=1000,
+                                seed=1, inclination_deg=float(rng.uniform(-90, 90)), wavelength_nm=lam))
+    return out
+
+
+@pytest.mark.parametrize("over", [{}, {"nt": 32, "np": 64, "input_width": 64, "theta_frequencies": 18,
+                                       "phi_frequencies": 4}])
+def test_feature_rows_match_oracle(icp, over):
+    cfg = icp.surrogate_config(**over)
+    oc = SO.Config.of(cfg)
+    cells = icp.surrogate_cell_features(cfg)
+    assert cells.shape == (cfg.nt * cfg.np, cfg.input_width - 16)
+    assert np.array_equal(cells, SO.bf16_bits(SO.cell_features(oc)))
+    specs = _specs(icp, 9)
+    rec = icp.surrogate_record_features(cfg, specs)
+    want = np.stack([SO.bf16_bits(SO.record_features(oc, s.radius_mm, s.wavelength_nm, s.inclination_deg,
+                                                      s.interior_index, s.coefficients)) for s in specs])
+    assert np.array_equal(rec, want)
+    # every feature stays O(1) over the batched-record ranges
+    assert np.abs(SO.from_bits(rec)).max() <= 4.0 and np.abs(SO.from_bits(cells)).max() <= 1.0
+
+
+def test_bf16_rounding_is_nearest_even():
+    x = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -9, 1.0 + 2 ** -9, -2.5, 3e38, 1e-40])
+    got = SO.bf16(x)
+    assert got[0] == 1.0
+    assert got[1] == 1.0                       # tie: to even (mantissa 0)
+    assert got[3] == 1.0                       # below the tie
+    assert got[2] == 1.0 + 2 ** -7             # above the tie
+    assert got[4] == -2.5
+    assert np.all(np.abs(SO.bf16(got) - got) == 0)  # idempotent
+    r = np.random.default_rng(0).normal(size=10000)
+    assert np.all(np.abs(SO.bf16(r) - r) <= np.abs(r) * 2 ** -8)
+
+
+def test_oracle_gradient_matches_finite_differences():
+    cfg = SO.Config(nt=4, np=8, hidden=8, input_width=64, theta_frequencies=10, phi_frequencies=3)
+    rng = np.random.default_rng(1)
+    R = 2
+    rec = rng.uniform(-1, 1, (R, 16))
+    X = SO.inputs(cfg, rec, SO.cell_features(cfg))
+    p = SO.init_parameters(cfg, 3).astype(np.float64)
+    target = rng.dirichlet(np.ones(cfg.nt * cfg.np), size=R)
+    target[0, :5] = 0.0
+    target[0] /= target[0].sum()
+    loss, g = SO.gradient(cfg, p, X, target, R, emulate=False)
+    assert loss > 0
+    idx = rng.choice(p.size - 1, 60, replace=False)
+    h = 1e-6
+    for i in idx:
+        e = np.zeros_like(p)
+        e[i] = h
+        lp, _ = SO.gradient(cfg, p + e, X, target, R, emulate=False)
+        lm, _ = SO.gradient(cfg, p - e, X, target, R, emulate=False)
+        fd = (lp - lm) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(fd)) + 1e-8, (i, fd, g[i])
+    # the head bias does not change the loss (softmax is shift-invariant)
+    assert abs(g[-1]) == 0.0
+
+
+def test_oracle_emulation_only_rounds():
+    cfg = SO.Config(nt=8, np=16, hidden=16, input_width=64, theta_frequencies=10, phi_frequencies=3)
+    rng = np.random.default_rng(2)
+    X = SO.inputs(cfg, rng.uniform(-1, 1, (1, 16)), SO.cell_features(cfg))
+    p = SO.init_parameters(cfg, 4)
+    target = rng.dirichlet(np.ones(cfg.nt * cfg.np), size=1)
+    l0, g0 = SO.gradient(cfg, p, X, target, 1, emulate=False)
+    l1, g1 = SO.gradient(cfg, p, X, target, 1, emulate=True)
+    assert abs(l1 - l0) <= 2e-2 * abs(l0)
+    assert np.linalg.norm(g1 - g0) <= 5e-2 * np.linalg.norm(g0)
+
+
+def test_config_validation(icp):
+    for bad in [{"hidden": 96}, {"input_width": 96}, {"theta_frequencies": 60}, {"nt": 3, "np": 5},
+                {"max_records": 0}, {"wavelength_nm": (700.0, 400.0)}, {"index_scale": 0.0}]:
+        cfg = icp.surrogate_config(**bad)
+        with pytest.raises(icp.InvalidArgument):
+            icp.surrogate_parameter_count(cfg)
+        with pytest.raises(icp.InvalidArgument):
+            icp.surrogate_cell_features(cfg)
+    cfg = icp.surrogate_config()
+    assert icp.surrogate_parameter_count(cfg) == SO.parameter_count(SO.Config.of(cfg)) == 256 * 128 + 2 * 256 ** 2 + 4 * 256 + 1
+    with pytest.raises(icp.InvalidArgument):
+        icp.surrogate_record_features(cfg, [icp.DropSpec([0] * 8, -1.0, 1.33, rays=1, seed=1)])
