@@ -433,27 +433,6 @@ def run_b200_hex(a) -> None:
         dist.destroy_process_group()
 
 
-def batch_records(I, count: int = 256, seed: int = 20260101, rays_max: float = 6e7, rays_min: float = 1e6) -> list:
-    """Drop records of the batched workload: radius log-uniform in [0.1, 3] mm, wavelength uniform
-    in [400, 700] nm, inclination uniform in [-90, 90] deg, Table-I shapes, water at 20 C, rays
-    proportional to the projected area (rays_max for the area of a 3 mm disk), clipped."""
-    import numpy as np
-
-    rng = np.random.default_rng(seed)
-    specs = []
-    for _ in range(count):
-        radius = float(np.exp(rng.uniform(np.log(0.1), np.log(3.0))))
-        lam = float(rng.uniform(400.0, 700.0))
-        incl = float(rng.uniform(-90.0, 90.0))
-        shape = I.RaindropShape.make(float(np.float32(radius))).coefficients
-        n = float(np.float32(I.evaluate_water_optics(lam).refractive_index))
-        area = I.compute_projected_area(shape, float(np.float32(radius)), I.drop_frame(incl)[0])
-        rays = int(min(rays_max, max(rays_min, round(rays_max * area / (math.pi * 9.0)))))
-        specs.append(I.DropSpec(shape, float(np.float32(radius)), n, rays, seed=int(rng.integers(1, 2**63)),
-                                inclination_deg=incl, wavelength_nm=lam, diffraction=True))
-    return specs
-
-
 def run_batched(I, ctx, stream, a, nt: int, np_: int) -> dict:
     """Batched records: one autotuned, graph-captured persistent launch per batch (device-resident
     outputs), timed with CUDA events on the library stream; then the same records through the
@@ -462,7 +441,7 @@ def run_batched(I, ctx, stream, a, nt: int, np_: int) -> dict:
 
     import torch
 
-    specs = batch_records(I, a.batch_records)
+    specs = I.batched_record_specs(a.batch_records)
     rays = sum(sp.rays for sp in specs)
     s = I.batch_settings(nt, np_, max_internal_hits=DROP["hits"], precision=I.ICP_FP32, use_graph=True)
     tuned_rate = I.autotune_drop_batch(ctx, specs, s)

@@ -831,6 +831,29 @@ def generate_drop_batch(ctx: Context, specs: list, settings: BatchSettings) -> D
                            list(reps))
 
 
+def batched_record_specs(count: int = 256, seed: int = 20260101, rays_max: float = 6e7, rays_min: float = 1e6,
+                         diffraction: bool = True, rays_scale: float = 1.0) -> list:
+    """Drop records of the batched workload: radius log-uniform in [0.1, 3] mm, wavelength uniform
+    in [400, 700] nm, inclination uniform in [-90, 90] deg, Table-I shapes, water at 20 C, rays
+    proportional to the projected area (rays_max for the area of a 3 mm disk), clipped to
+    [rays_min, rays_max] and then multiplied by rays_scale."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for _ in range(count):
+        radius = float(np.exp(rng.uniform(np.log(0.1), np.log(3.0))))
+        lam = float(rng.uniform(400.0, 700.0))
+        incl = float(rng.uniform(-90.0, 90.0))
+        r32 = float(np.float32(radius))
+        shape = RaindropShape.make(r32).coefficients
+        n = float(np.float32(evaluate_water_optics(lam).refractive_index))
+        area = compute_projected_area(shape, r32, drop_frame(incl)[0])
+        rays = int(min(rays_max, max(rays_min, round(rays_max * area / (math.pi * 9.0)))))
+        specs.append(DropSpec(shape, r32, n, max(1, int(round(rays * rays_scale))),
+                              seed=int(rng.integers(1, 2**63)), inclination_deg=incl, wavelength_nm=lam,
+                              diffraction=diffraction))
+    return specs
+
+
 def autotune_drop_batch(ctx: Context, specs: list, settings: BatchSettings) -> float:
     """Times candidate block and chunk sizes on a bounded sample of the batch; stores the best
     in ``settings`` (and in the context for later batches).  Returns the best rays/s."""

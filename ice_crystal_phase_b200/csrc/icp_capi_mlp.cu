@@ -86,7 +86,7 @@ bool config_valid(const icp_surrogate_config* g)
     if (!g || !g->nt || !g->np || ((uint64_t)g->nt * g->np) % 256u || (uint64_t)g->nt * g->np > (1u << 24)) return false;
     if (g->hidden != 128 && g->hidden != 256) return false;
     if (g->input_width != 64 && g->input_width != 128) return false;
-    if (4u + 2u * g->theta_frequencies + 2u * g->phi_frequencies > g->input_width - 16u) return false;
+    if (4u + 2u * g->theta_frequencies + g->phi_frequencies > g->input_width - 16u) return false;
     if (!g->max_records || g->max_records > 256) return false;
     const double* r[3] = {g->log_radius_mm, g->wavelength_nm, g->log_wavelength_over_radius};
     for (auto* x : r)
@@ -354,8 +354,8 @@ int icp_surrogate_default_config(icp_surrogate_config* g)
     g->np = 512;
     g->hidden = 256;
     g->input_width = 128;
-    g->theta_frequencies = 50;
-    g->phi_frequencies = 4;
+    g->theta_frequencies = 48;
+    g->phi_frequencies = 12;
     g->max_records = 16;
     g->log_radius_mm[0] = std::log(0.1);
     g->log_radius_mm[1] = std::log(3.0);
@@ -406,10 +406,9 @@ int icp_surrogate_cell_features(const icp_surrogate_config* g, uint16_t* out)
                 f[4 + 2 * (k - 1)] = std::sin(k * th);
                 f[5 + 2 * (k - 1)] = std::cos(k * th);
             }
-            for (uint32_t l = 1; l <= Gf; ++l) {
-                f[4 + 2 * F + 2 * (l - 1)] = std::sin(l * ph);
-                f[5 + 2 * F + 2 * (l - 1)] = std::cos(l * ph);
-            }
+            // the pattern of a drop whose axis lies in the plane of ki and e1 is even about
+            // phi = pi/2 (the mirror z -> -z maps phi to pi - phi): only cos(l (phi - pi/2))
+            for (uint32_t l = 1; l <= Gf; ++l) f[4 + 2 * F + (l - 1)] = std::cos(l * (ph - 0.5 * H::kPi));
             uint16_t* row = out + ((size_t)i * g->np + j) * kc;
             for (uint32_t k = 0; k < kc; ++k) row[k] = feature(f[k]);
         }

@@ -358,7 +358,8 @@ int icp_mlp_gemm_bf16(icp_context* ctx, const void* d_a, const void* d_b, uint32
 
 /* A small MLP conditioned on a drop record's parameters that predicts the log cell mass of its
  * record on an (nt x np) cell grid: input row = 16 record features + cell features (theta,
- * phi harmonics), three SiLU layers of `hidden` units (BF16 weights and activations, FP32
+ * phi harmonics; the phi harmonics are even about phi = pi/2, the mirror symmetry of a drop
+ * record), three SiLU layers of `hidden` units (BF16 weights and activations, FP32
  * accumulation on the tensor cores), a linear head to one value y per cell.  Cell probability =
  * softmax of y over the record's cells.  Trained by the mean per-record KL divergence of the
  * tracer's cell probabilities from the prediction. */
@@ -369,7 +370,7 @@ typedef struct {
     uint32_t hidden;               /* 128 or 256                                                */
     uint32_t input_width;          /* 64 or 128: 16 record features, then the cell features     */
     uint32_t theta_frequencies;    /* sin / cos (k theta), k = 1..F                             */
-    uint32_t phi_frequencies;      /* sin / cos (l phi), l = 1..G; 4 + 2F + 2G <= width - 16   */
+    uint32_t phi_frequencies;      /* cos (l (phi - pi/2)), l = 1..G; 4 + 2F + G <= width - 16 */
     uint32_t max_records;          /* records per call (sizes the activation buffers)          */
     uint32_t reserved;
     double log_radius_mm[2];       /* ranges mapped onto [-1, 1] by the record features         */
@@ -385,7 +386,7 @@ typedef struct {
 } icp_adam;
 
 /* Defaults for the batched-record distribution: 256 x 512 cells, 256 hidden, width 128,
- * F = 50, G = 4, radius 0.1-3 mm, wavelength 400-700 nm, 16 records per call. */
+ * F = 48, G = 12, radius 0.1-3 mm, wavelength 400-700 nm, 16 records per call. */
 int icp_surrogate_default_config(icp_surrogate_config* cfg);
 /* FP32 parameters, in this order: W1[H][K0], b1[H], W2[H][H], b2[H], W3[H][H], b3[H], w4[H],
  * head bias (1): H*K0 + 2H^2 + 4H + 1. */

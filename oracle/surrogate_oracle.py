@@ -48,8 +48,8 @@ class Config:
     np: int = 512
     hidden: int = 256
     input_width: int = 128
-    theta_frequencies: int = 50
-    phi_frequencies: int = 4
+    theta_frequencies: int = 48
+    phi_frequencies: int = 12
     log_radius_mm: tuple = (math.log(0.1), math.log(3.0))
     wavelength_nm: tuple = (400.0, 700.0)
     log_wavelength_over_radius: tuple = (math.log(400e-6 / 3.0), math.log(700e-6 / 0.1))
@@ -103,8 +103,7 @@ def cell_features(cfg: Config) -> np.ndarray:
         f[:, 4 + 2 * (k - 1)] = np.sin(k * th)
         f[:, 5 + 2 * (k - 1)] = np.cos(k * th)
     for l in range(1, G + 1):
-        f[:, 4 + 2 * F + 2 * (l - 1)] = np.sin(l * ph)
-        f[:, 5 + 2 * F + 2 * (l - 1)] = np.cos(l * ph)
+        f[:, 4 + 2 * F + (l - 1)] = np.cos(l * (ph - 0.5 * math.pi))
     return f
 
 
