@@ -3,15 +3,18 @@
 //
 //   D[M x N] = A[M x K] * B[N x K]^T      A, B: BF16, K-major (row-major with K contiguous)
 //
-// One CTA of 128 threads computes a 128 x N tile (N in {64, 128, 256}) over a range of K chunks
-// of 64: thread 0 streams A and B chunks through a STAGES-deep ring with 2-D TMA loads (128-byte
-// swizzle, completion counted on a "full" mbarrier per stage) and issues four K=16
-// tcgen05.mma per chunk into an FP32 accumulator in tensor memory; each chunk's MMAs commit to the
-// stage's "empty" mbarrier, which gates the refill.  After the last chunk a commit to "done"
-// releases the epilogue: warp w reads TMEM lanes 32w..32w+31 (rows) with tcgen05.ld, 32 columns at
-// a time, and applies one of the fused epilogues below.  Split-K (grid.y > 1) adds partial tiles
-// with FP32 atomics.  Every mbarrier wait is bounded: on expiry the kernel sets the error word,
-// waits (bounded) for its issued MMAs, frees its tensor memory and returns.
+// Two kernels.  The layer GEMMs (K, N = layer widths <= 256, M = the rows of a batch) run
+// persistent and warp-specialised (gemm_persistent_kernel, below).  The weight gradients (M, N =
+// layer widths, K = rows of a batch) run split-K (gemm_kernel): one CTA of 128 threads computes a
+// 128 x N tile (N in {64, 128, 256}) over a range of K chunks of 64: thread 0 streams A and B
+// chunks through a STAGES-deep ring with 2-D TMA loads (128-byte swizzle, completion counted on a
+// "full" mbarrier per stage) and issues four K=16 tcgen05.mma per chunk into an FP32 accumulator
+// in tensor memory; each chunk's MMAs commit to the stage's "empty" mbarrier, which gates the
+// refill.  After the last chunk a commit to "done" releases the epilogue: warp w reads TMEM lanes
+// 32w..32w+31 (rows) with tcgen05.ld, 32 columns at a time, and applies one of the fused
+// epilogues below.  Split-K (grid.y > 1) adds partial tiles with FP32 atomics.  Every mbarrier
+// wait is bounded: on expiry the kernel sets the error word, waits (bounded) for its issued loads
+// and MMAs, frees its tensor memory and returns.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -34,10 +37,12 @@ template <int N> __host__ __device__ constexpr uint32_t stage_bytes() { return k
 // 1024 (alignment) + stages + barriers / TMEM slot (256) + column sums of the bias gradient (1024)
 template <int N> constexpr size_t smem_bytes() { return 1024 + (size_t)stages<N>() * stage_bytes<N>() + 256 + 1024; }
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+// SiLU and its derivative with the fast exponential and division (relative error ~1e-7, far
+// below the BF16 rounding of the stored activations); exp(-z) = inf gives 0 as it should.
+__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
 __device__ __forceinline__ float silu_grad(float z)
 {
-    const float s = 1.0f / (1.0f + __expf(-z));
+    const float s = __fdividef(1.0f, 1.0f + __expf(-z));
     return s * (1.0f + z * (1.0f - s));
 }
 
@@ -73,11 +78,16 @@ __device__ __forceinline__ float warp_column_sum(float (&v)[32], uint32_t lane)
 }
 
 // Column-major copy of a warp's 32 rows x 32 columns: for each column, the 32 lanes write 32
-// consecutive rows (64 contiguous bytes).
+// consecutive rows (64 contiguous bytes).  One running pointer, not 32 precomputed addresses
+// (the persistent kernel's epilogue runs at 168 registers).
 __device__ __forceinline__ void store_bf16x32_t(__nv_bfloat16* dst, uint32_t ld, const float (&v)[32])
 {
+    __nv_bfloat16* p = dst;
 #pragma unroll
-    for (int i = 0; i < 32; ++i) dst[(size_t)i * ld] = __float2bfloat16_rn(v[i]);
+    for (int i = 0; i < 32; ++i) {
+        *p = __float2bfloat16_rn(v[i]);
+        p += ld;
+    }
 }
 
 __device__ __forceinline__ void load_bf16x32(const __nv_bfloat16* src, float (&v)[32])
@@ -97,6 +107,76 @@ __device__ __forceinline__ void load_bf16x32(const __nv_bfloat16* src, float (&v
     }
 }
 
+// Columns [c0, c1) of one row of a 128 x N accumulator tile through the fused epilogue: this
+// thread's TMEM lane starts at taddr (column 0); m is the output row; bias / head_w point at N
+// values (shared or global memory, 16-byte aligned); colsum collects the bias gradient
+// (kBackprop).  Returns the partial head sum of these columns (kHead).
+template <int N, int EPI>
+__device__ __forceinline__ float epilogue_cols(const GemmArgs& g, uint32_t taddr, uint32_t m, uint32_t lane,
+                                              uint32_t c0, uint32_t c1, const float* bias, const float* head_w,
+                                              float* colsum)
+{
+    float yacc = 0.0f;
+#pragma unroll 1
+    for (uint32_t c = c0; c < c1; c += 32u) {
+        float v[32];
+        umma::tmem_ld32(taddr + c, v);
+        if constexpr (EPI == kStoreF32) {
+            float4* d = reinterpret_cast<float4*>(g.out_f32 + (size_t)m * g.ld_out + c);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) d[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+        } else if constexpr (EPI == kAtomicF32) {
+            float* d = g.out_f32 + (size_t)m * g.ld_out + c;
+#pragma unroll
+            for (int i = 0; i < 32; ++i) atomicAdd(d + i, v[i]);
+        } else if constexpr (EPI == kHidden || EPI == kHead) {
+            const float4* b4 = reinterpret_cast<const float4*>(bias + c);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const float4 b = b4[q];
+                v[4 * q] += b.x;
+                v[4 * q + 1] += b.y;
+                v[4 * q + 2] += b.z;
+                v[4 * q + 3] += b.w;
+            }
+            if (g.out_z) store_bf16x32(g.out_z + (size_t)m * N + c, v);
+#pragma unroll
+            for (int i = 0; i < 32; ++i) v[i] = silu(v[i]);
+            if (g.out_h) store_bf16x32(g.out_h + (size_t)m * N + c, v);
+            if (g.out_hT) store_bf16x32_t(g.out_hT + (size_t)c * g.ld_t + m, g.ld_t, v);
+            if constexpr (EPI == kHead) {
+                const float4* w4 = reinterpret_cast<const float4*>(head_w + c);
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const float4 w = w4[q];
+                    yacc = fmaf(v[4 * q], w.x, yacc);
+                    yacc = fmaf(v[4 * q + 1], w.y, yacc);
+                    yacc = fmaf(v[4 * q + 2], w.z, yacc);
+                    yacc = fmaf(v[4 * q + 3], w.w, yacc);
+                }
+            }
+        } else if constexpr (EPI == kBackprop) {
+            float z[32];
+            load_bf16x32(g.z_prev + (size_t)m * N + c, z);
+#pragma unroll
+            for (int i = 0; i < 32; ++i) v[i] *= silu_grad(z[i]);
+            if (g.out_dz) store_bf16x32(g.out_dz + (size_t)m * N + c, v);
+            if (g.out_dzT) store_bf16x32_t(g.out_dzT + (size_t)c * g.ld_t + m, g.ld_t, v);
+            if (g.out_db) atomicAdd(&colsum[c + lane], warp_column_sum(v, lane));
+        }
+    }
+    return yacc;
+}
+
+__device__ __forceinline__ void head_store(const GemmArgs& g, uint32_t m, float yacc)
+{
+    const float y = yacc + g.head_b;
+    if (g.out_y) g.out_y[m] = y;
+    if (g.out_mass) g.out_mass[m] = exp((double)y);
+}
+
+// Split-K GEMM (one 128-row tile and one K range per CTA): the weight gradients, whose K (the
+// rows of a batch) is long and whose M and N are the layer widths.
 template <int N, int EPI>
 __global__ void __launch_bounds__(128, 1)
     gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const GemmArgs g)
@@ -144,14 +224,15 @@ __global__ void __launch_bounds__(128, 1)
             umma::tma_load_2d(a, &tmA, &full[s], (int32_t)((kc0 + kc) * 64u), (int32_t)m0);
             umma::tma_load_2d(a + kA, &tmB, &full[s], (int32_t)((kc0 + kc) * 64u), 0);
         };
-        const uint32_t pre = nk < (uint32_t)S ? nk : (uint32_t)S;
-        for (uint32_t s = 0; s < pre; ++s) load(s, s);
+        uint32_t issued = nk < (uint32_t)S ? nk : (uint32_t)S, consumed = 0;
+        for (uint32_t s = 0; s < issued; ++s) load(s, s);
         for (uint32_t kc = 0; kc < nk && ok; ++kc) {
             const uint32_t s = kc % S, par = (kc / S) & 1u;
             if (!umma::mbar_wait(&full[s], par, kWaitLimit)) {
                 ok = false;
                 break;
             }
+            consumed = kc + 1;
             umma::fence_after_sync();
             const uint32_t a = umma::smem_u32(smem + s * SB), b = a + kA;
 #pragma unroll
@@ -165,12 +246,15 @@ __global__ void __launch_bounds__(128, 1)
                     break;
                 }
                 load(s, kc + S);
+                issued = kc + S + 1;
             }
         }
         if (!ok) {
             *abort_flag = 1;
             if (nk) atomicExch(g.error, 1u);
             __threadfence_block();
+            // loads still in flight land before this CTA's shared memory is released
+            for (uint32_t j = consumed; j < issued; ++j) umma::mbar_wait(&full[j % S], (j / S) & 1u, kWaitLimit);
         }
         umma::mma_commit(done); // arrives once every MMA issued above has completed
     }
@@ -181,47 +265,10 @@ __global__ void __launch_bounds__(128, 1)
     const bool ready = __all_sync(0xffffffffu, mine && !*abort_flag);
     umma::fence_after_sync();
     if (ready) {
-        const uint32_t row = 32u * warp + lane;
-        const uint32_t m = m0 + row;
-        float yacc = 0.0f;
-        for (uint32_t c = 0; c < (uint32_t)N; c += 32u) {
-            float v[32];
-            umma::tmem_ld32(tmem + ((32u * warp) << 16) + c, v);
-            if constexpr (EPI == kStoreF32) {
-                float4* d = reinterpret_cast<float4*>(g.out_f32 + (size_t)m * g.ld_out + c);
-#pragma unroll
-                for (int q = 0; q < 8; ++q) d[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-            } else if constexpr (EPI == kAtomicF32) {
-                float* d = g.out_f32 + (size_t)m * g.ld_out + c;
-#pragma unroll
-                for (int i = 0; i < 32; ++i) atomicAdd(d + i, v[i]);
-            } else if constexpr (EPI == kHidden || EPI == kHead) {
-#pragma unroll
-                for (int i = 0; i < 32; ++i) v[i] += g.bias[c + i];
-                if (g.out_z) store_bf16x32(g.out_z + (size_t)m * N + c, v);
-#pragma unroll
-                for (int i = 0; i < 32; ++i) v[i] = silu(v[i]);
-                if (g.out_h) store_bf16x32(g.out_h + (size_t)m * N + c, v);
-                if (g.out_hT) store_bf16x32_t(g.out_hT + (size_t)c * g.ld_t + m, g.ld_t, v);
-                if constexpr (EPI == kHead) {
-#pragma unroll
-                    for (int i = 0; i < 32; ++i) yacc = fmaf(v[i], g.head_w[c + i], yacc);
-                }
-            } else if constexpr (EPI == kBackprop) {
-                float z[32];
-                load_bf16x32(g.z_prev + (size_t)m * N + c, z);
-#pragma unroll
-                for (int i = 0; i < 32; ++i) v[i] *= silu_grad(z[i]);
-                if (g.out_dz) store_bf16x32(g.out_dz + (size_t)m * N + c, v);
-                if (g.out_dzT) store_bf16x32_t(g.out_dzT + (size_t)c * g.ld_t + m, g.ld_t, v);
-                if (g.out_db) atomicAdd(&colsum[c + lane], warp_column_sum(v, lane));
-            }
-        }
-        if constexpr (EPI == kHead) {
-            const float y = yacc + g.head_b;
-            if (g.out_y) g.out_y[m] = y;
-            if (g.out_mass) g.out_mass[m] = exp((double)y);
-        }
+        const uint32_t m = m0 + 32u * warp + lane;
+        const float y = epilogue_cols<N, EPI>(g, tmem + ((32u * warp) << 16), m, lane, 0u, (uint32_t)N, g.bias,
+                                              g.head_w, colsum);
+        if constexpr (EPI == kHead) head_store(g, m, y);
     }
     if constexpr (EPI == kBackprop) {
         __syncthreads();
@@ -231,6 +278,215 @@ __global__ void __launch_bounds__(128, 1)
     umma::fence_before_sync();
     __syncthreads();
     if (warp == 0) umma::tmem_dealloc(tmem, (uint32_t)N);
+}
+
+// ---------------------------------------------------------------- persistent layer GEMM
+// D[M x N] = A[M x K] * B[N x K]^T for the layers (M = rows of a batch, K, N = layer widths):
+// the whole B (N x K BF16, <= 128 KB) stays in shared memory; one CTA per SM walks the 128-row
+// tiles t = blockIdx.x, blockIdx.x + gridDim.x, ...  Warp 0 streams A chunks through a deep ring
+// with TMA; warp 1 allocates 2 N TMEM columns and one of its threads issues the MMAs into
+// accumulator buffer (tile & 1); the kEpiWarps warps 2.. drain the other buffer through the
+// fused epilogue, so a tile's epilogue overlaps the next tile's MMAs.  Epilogue warp w reads
+// TMEM lanes 32 (w mod 4) .. (the rows its lane quarter may access) and column slice
+// (w - 2) / 4 of kEpiWarps / 4; the head's partial sums of a row meet in shared memory behind
+// a named barrier per lane quarter.  Bias and head weights are staged in shared memory.
+// Barriers: a_full / a_empty per ring stage, b_full, acc_full / acc_empty per accumulator, and
+// drain (all MMAs complete).  Every wait is bounded; a role that gives up raises the abort flag
+// and the error word, the others give up at their next wait, in-flight loads and MMAs are
+// waited for, and the tensor memory is freed.
+constexpr uint32_t kEpiWarps = 8;
+constexpr uint32_t kSlices = kEpiWarps / 4;
+constexpr uint32_t kPThreads = 64 + 32 * kEpiWarps;
+// per-CTA extras after the ring: barriers (1 KB), colsum, bias, head weights (1 KB each), head
+// partial sums (kSlices - 1 slices x 128 floats, rounded up to kSlices)
+constexpr int kPExtra = 1024 + 3 * 1024 + (int)kSlices * 512;
+template <int N, int KC> __host__ __device__ constexpr int pstages()
+{
+    return (232448 - 1024 - N * 128 * KC - kPExtra) / (int)kA > 8 ? 8
+                                                                   : (232448 - 1024 - N * 128 * KC - kPExtra) / (int)kA;
+}
+template <int N, int KC> constexpr size_t psmem_bytes()
+{
+    return 1024 + (size_t)N * 128 * KC + (size_t)pstages<N, KC>() * kA + kPExtra;
+}
+
+__device__ __forceinline__ void named_sync(uint32_t id, uint32_t threads)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+}
+
+template <int N, int KC, int EPI>
+__global__ void __launch_bounds__(kPThreads, 1)
+    gemm_persistent_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                           const GemmArgs g)
+{
+    constexpr int S = pstages<N, KC>();
+    constexpr uint32_t BB = (uint32_t)N * 128u;   // one 64-wide K chunk of B
+    constexpr uint32_t W = (uint32_t)N / kSlices; // columns per epilogue warp
+    static_assert(S >= 2, "ring too shallow");
+    static_assert(W % 32u == 0, "slice width");
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* bres = smem;
+    uint8_t* ring = smem + KC * BB;
+    uint64_t* a_full = reinterpret_cast<uint64_t*>(ring + S * kA);
+    uint64_t* a_empty = a_full + S;
+    uint64_t* b_full = a_empty + S;
+    uint64_t* acc_full = b_full + 1;
+    uint64_t* acc_empty = acc_full + 2;
+    uint64_t* drain = acc_empty + 2;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(drain + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
+    float* colsum = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(a_full) + 1024);
+    float* sbias = colsum + 256;
+    float* shead = sbias + 256;
+    float* ypart = shead + 256; // [kSlices - 1][128]
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t tiles = g.M / 128u;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            umma::mbar_init(&a_full[s], 1);
+            umma::mbar_init(&a_empty[s], 1);
+        }
+        umma::mbar_init(b_full, 1);
+        for (int b = 0; b < 2; ++b) {
+            umma::mbar_init(&acc_full[b], 1);
+            umma::mbar_init(&acc_empty[b], kEpiWarps);
+        }
+        umma::mbar_init(drain, 1);
+        *abort_flag = 0;
+        umma::mbar_fence_init();
+    }
+    for (uint32_t i = threadIdx.x; i < (uint32_t)N; i += blockDim.x) {
+        colsum[i] = 0.0f;
+        if constexpr (EPI == kHidden || EPI == kHead) sbias[i] = g.bias[i];
+        if constexpr (EPI == kHead) shead[i] = g.head_w[i];
+    }
+    if (warp == 1) umma::tmem_alloc(tslot, 2u * N);
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = *tslot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // producer: B once, then the A chunks of every tile of this CTA
+            bool ok = true;
+            umma::mbar_arrive_expect_tx(b_full, KC * BB);
+            for (int kc = 0; kc < KC; ++kc) umma::tma_load_2d(bres + kc * BB, &tmB, b_full, kc * 64, 0);
+            uint32_t it = 0;
+#pragma unroll 1
+            for (uint32_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+                for (int kc = 0; kc < KC; ++kc, ++it) {
+                    const uint32_t s = it % S;
+                    if (it >= (uint32_t)S && !umma::mbar_wait(&a_empty[s], ((it / S) & 1u) ^ 1u, kWaitLimit)) {
+                        ok = false;
+                        break;
+                    }
+                    if (*abort_flag) {
+                        ok = false;
+                        break;
+                    }
+                    umma::mbar_arrive_expect_tx(&a_full[s], kA);
+                    umma::tma_load_2d(ring + s * kA, &tmA, &a_full[s], kc * 64, (int32_t)(t * 128u));
+                }
+            }
+            if (!ok) {
+                *abort_flag = 1;
+                atomicExch(g.error, 3u);
+            }
+            // every issued load lands before the CTA's shared memory is released
+            for (uint32_t j = it > (uint32_t)S ? it - S : 0u; j < it; ++j)
+                umma::mbar_wait(&a_full[j % S], (j / S) & 1u, kWaitLimit);
+            umma::mbar_wait(b_full, 0, kWaitLimit);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // MMA issuer
+            const uint32_t idesc = umma::instr_desc_bf16_f32(128, (uint32_t)N);
+            bool ok = umma::mbar_wait(b_full, 0, kWaitLimit);
+            uint32_t it = 0, i = 0;
+#pragma unroll 1
+            for (uint32_t t = blockIdx.x; t < tiles && ok; t += gridDim.x, ++i) {
+                const uint32_t b = i & 1u;
+                if (i >= 2 && !umma::mbar_wait(&acc_empty[b], ((i >> 1) - 1u) & 1u, kWaitLimit)) {
+                    ok = false;
+                    break;
+                }
+                umma::fence_after_sync();
+                const uint32_t d = tmem + b * (uint32_t)N;
+                for (int kc = 0; kc < KC; ++kc, ++it) {
+                    const uint32_t s = it % S;
+                    if (!umma::mbar_wait(&a_full[s], (it / S) & 1u, kWaitLimit) || *abort_flag) {
+                        ok = false;
+                        break;
+                    }
+                    umma::fence_after_sync();
+                    const uint32_t a = umma::smem_u32(ring + s * kA), bb = umma::smem_u32(bres + kc * BB);
+#pragma unroll
+                    for (uint32_t k = 0; k < 4; ++k)
+                        umma::mma_bf16(d, umma::smem_desc_sw128(a + 32u * k), umma::smem_desc_sw128(bb + 32u * k), idesc,
+                                       kc > 0 || k > 0);
+                    umma::mma_commit(&a_empty[s]);
+                }
+                if (!ok) break;
+                umma::mma_commit(&acc_full[b]);
+            }
+            if (!ok) {
+                *abort_flag = 1;
+                atomicExch(g.error, 4u);
+            }
+            umma::mma_commit(drain);
+            if (!umma::mbar_wait(drain, 0, kWaitLimit)) atomicExch(g.error, 6u);
+        }
+    } else {
+        // epilogue warps
+        const uint32_t q = warp & 3u, slice = (warp - 2u) >> 2;
+        const uint32_t c0 = slice * W;
+        const uint32_t row = 32u * q + lane;
+        uint32_t i = 0;
+        bool live = true;
+#pragma unroll 1
+        for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x, ++i) {
+            const uint32_t b = i & 1u;
+            const bool mine = live && umma::mbar_wait(&acc_full[b], (i >> 1) & 1u, kWaitLimit);
+            if (!__all_sync(0xffffffffu, mine && !*abort_flag)) {
+                if (lane == 0 && live) {
+                    *abort_flag = 1;
+                    atomicExch(g.error, 5u);
+                }
+                live = false;
+            }
+            float y = 0.0f;
+            if (live) {
+                umma::fence_after_sync();
+                y = epilogue_cols<N, EPI>(g, tmem + ((32u * q) << 16) + b * (uint32_t)N, t * 128u + row, lane, c0,
+                                          c0 + W, sbias, shead, colsum);
+                umma::fence_before_sync();
+                __syncwarp();
+                if (lane == 0) umma::mbar_arrive(&acc_empty[b]);
+            }
+            if constexpr (EPI == kHead) {
+                // the slices of a lane quarter meet here every tile (also after an abort, so that
+                // the named barrier never waits for a warp that has left the loop)
+                if (slice) ypart[(slice - 1u) * 128u + row] = y;
+                named_sync(1u + q, 32u * kSlices);
+                if (slice == 0 && live) {
+                    for (uint32_t k = 1; k < kSlices; ++k) y += ypart[(k - 1u) * 128u + row];
+                    head_store(g, t * 128u + row, y);
+                }
+                named_sync(1u + q, 32u * kSlices);
+            }
+        }
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    if constexpr (EPI == kBackprop) {
+        if (g.out_db && !*abort_flag)
+            for (uint32_t k = threadIdx.x; k < (uint32_t)N; k += blockDim.x) atomicAdd(&g.out_db[k], colsum[k]);
+    }
+    if (warp == 1) umma::tmem_dealloc(tmem, 2u * N);
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link-time libcuda).
@@ -287,6 +543,52 @@ template <int EPI> int launch_epi(const void* A, const void* B, const GemmArgs& 
     }
 }
 
+int sm_count()
+{
+    static const int n = [] {
+        int dev = 0, v = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        return v > 0 ? v : 148;
+    }();
+    return n;
+}
+
+template <int N, int KC, int EPI> int launch_p(const void* A, const void* B, const GemmArgs& g, cudaStream_t st)
+{
+    CUtensorMap ta, tb;
+    if (make_map(&ta, A, g.M, g.K, 128u) || make_map(&tb, B, (uint32_t)N, g.K, (uint32_t)N)) return -1;
+    const size_t smem = psmem_bytes<N, KC>();
+    cudaError_t e = cudaFuncSetAttribute(gemm_persistent_kernel<N, KC, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return (int)e;
+    const uint32_t tiles = g.M / 128u;
+    const uint32_t grid = tiles < (uint32_t)sm_count() ? tiles : (uint32_t)sm_count();
+    gemm_persistent_kernel<N, KC, EPI><<<grid, kPThreads, smem, st>>>(ta, tb, g);
+    return (int)cudaGetLastError();
+}
+
+template <int EPI> int launch_pe(const void* A, const void* B, const GemmArgs& g, cudaStream_t st)
+{
+    const uint32_t kc = g.K / 64u;
+    if (g.N == 256) {
+        if (kc == 1) return launch_p<256, 1, EPI>(A, B, g, st);
+        if (kc == 2) return launch_p<256, 2, EPI>(A, B, g, st);
+        if (kc == 4) return launch_p<256, 4, EPI>(A, B, g, st);
+    } else if (g.N == 128) {
+        if (kc == 1) return launch_p<128, 1, EPI>(A, B, g, st);
+        if (kc == 2) return launch_p<128, 2, EPI>(A, B, g, st);
+        if (kc == 4) return launch_p<128, 4, EPI>(A, B, g, st);
+    }
+    return -2;
+}
+
+bool persistent_shape(const GemmArgs& g)
+{
+    const uint32_t kc = g.K / 64u;
+    return (g.N == 128 || g.N == 256) && (kc == 1 || kc == 2 || kc == 4);
+}
+
 } // namespace
 
 int gemm(const void* A, const void* B, GemmArgs g, int epi, uint32_t splits, cudaStream_t st)
@@ -296,6 +598,15 @@ int gemm(const void* A, const void* B, GemmArgs g, int epi, uint32_t splits, cud
     const uint32_t nk = g.K / 64u;
     g.k_chunks = (nk + splits - 1) / splits;
     splits = (nk + g.k_chunks - 1) / g.k_chunks; // every CTA gets at least one chunk
+    if (epi != kAtomicF32 && persistent_shape(g)) {
+        switch (epi) {
+        case kStoreF32: return launch_pe<kStoreF32>(A, B, g, st);
+        case kHidden: return launch_pe<kHidden>(A, B, g, st);
+        case kHead: return launch_pe<kHead>(A, B, g, st);
+        case kBackprop: return launch_pe<kBackprop>(A, B, g, st);
+        default: return -4;
+        }
+    }
     switch (epi) {
     case kStoreF32: return launch_epi<kStoreF32>(A, B, g, splits, st);
     case kAtomicF32: return launch_epi<kAtomicF32>(A, B, g, splits, st);

@@ -14,7 +14,11 @@ def _bf16(shape, gen, scale=1.0):
     return (torch.randn(*shape, generator=gen) * scale).to(torch.bfloat16)
 
 
-@pytest.mark.parametrize("m,n,k", [(128, 64, 64), (256, 128, 320), (384, 256, 1024), (128, 256, 64)])
+# split-K kernel shapes, then the persistent kernel (N in {128, 256}, K in {64, 128, 256}) with
+# fewer tiles than SMs and with several tiles per CTA (ring wrap-around, both accumulators)
+@pytest.mark.parametrize("m,n,k", [(128, 64, 64), (256, 128, 320), (384, 256, 1024), (128, 256, 64),
+                                   (128 * 37, 256, 256), (128 * 400, 256, 256), (128 * 1000, 128, 128),
+                                   (128 * 311, 256, 64), (128 * 297, 128, 256)])
 def test_gemm_store_matches_fp64(ctx, icp, m, n, k):
     gen = torch.Generator().manual_seed(m * 7 + n + k)
     a, b = _bf16((m, k), gen), _bf16((n, k), gen)

@@ -51,7 +51,9 @@ def _rel(a, b):
 
 
 @pytest.mark.parametrize("over,R", [(SMALL, 3), ({**SMALL, "hidden": 128, "input_width": 128, "theta_frequencies": 40},
-                                                  2)])
+                                                  2),
+                                    # more 128-row tiles than SMs: several tiles per persistent CTA
+                                    ({**SMALL, "nt": 64, "np": 128}, 4)])
 def test_gradient_matches_oracle(ctx, icp, over, R):
     cfg, oc, specs, X, p, t = _setup(icp, over, R, 11 + R)
     with icp.Surrogate(ctx, cfg) as s:
