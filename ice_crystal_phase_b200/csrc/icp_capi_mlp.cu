@@ -20,9 +20,12 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <future>
+#include <thread>
 #include <vector>
 
 #include "../../include/icp_b200.h"
+#include "../host/icp_drop_host.hpp"
 #include "../host/icp_host_math.hpp"
 #include "icp_internal.h"
 #include "icp_mlp.h"
@@ -129,11 +132,14 @@ struct icp_surrogate {
     uint32_t o_w1 = 0, o_b1 = 0, o_w2 = 0, o_b2 = 0, o_w3 = 0, o_b3 = 0, o_w4 = 0, o_hb = 0;
     Scratch params, grads, adam_m, adam_v, wbf, cells, edges, rec16, loss;
     Scratch X, XT, z1, h1, h1T, z2, h2, h2T, z3, y, dy, dz3, dz3T, dz2, dz2T, dz1T, mass, reports, sync;
+    Scratch mass_sum, dfrac, drows;
+    std::vector<double> h_edges;
     std::vector<uint16_t> h_rec;
     ~icp_surrogate()
     {
         Scratch* all[] = {&params, &grads, &adam_m, &adam_v, &wbf, &cells, &edges, &rec16, &loss, &X, &XT, &z1, &h1,
-                          &h1T, &z2, &h2, &h2T, &z3, &y, &dy, &dz3, &dz3T, &dz2, &dz2T, &dz1T, &mass, &reports, &sync};
+                          &h1T, &z2, &h2, &h2T, &z3, &y, &dy, &dz3, &dz3T, &dz2, &dz2T, &dz1T, &mass, &reports, &sync,
+                          &mass_sum, &dfrac, &drows};
         for (Scratch* s : all) s->release();
     }
     float* P(uint32_t o) const { return (float*)params.ptr + o; }
@@ -199,7 +205,8 @@ mlp::GemmArgs layer(uint64_t M, uint32_t N, uint32_t K)
 
 // Forward pass.  training: keep z1, z2, z3 and the column-major activations; else the head
 // writes y (logits) or exp(y) (mass).
-int enqueue_forward(icp_surrogate* s, uint32_t count, bool training, float* y_out, double* mass_out)
+int enqueue_forward(icp_surrogate* s, uint32_t count, bool training, float* y_out, double* mass_out,
+                    double* mass_sum = nullptr)
 {
     const uint64_t M = (uint64_t)count * s->C;
     const uint32_t Hn = s->H;
@@ -217,7 +224,8 @@ int enqueue_forward(icp_surrogate* s, uint32_t count, bool training, float* y_ou
         g.out_z = as<__nv_bfloat16>(s->z1);
         g.out_hT = as<__nv_bfloat16>(s->h1T);
     }
-    ICP_TRY(run_gemm(s, s->X.ptr, s->w1b(), g, mlp::kHidden, 1));
+    const int hid = training ? mlp::kHiddenTrain : mlp::kHidden;
+    ICP_TRY(run_gemm(s, s->X.ptr, s->w1b(), g, hid, 1));
     g = layer(M, Hn, Hn);
     g.bias = s->P(s->o_b2);
     g.out_h = as<__nv_bfloat16>(s->h2);
@@ -225,7 +233,7 @@ int enqueue_forward(icp_surrogate* s, uint32_t count, bool training, float* y_ou
         g.out_z = as<__nv_bfloat16>(s->z2);
         g.out_hT = as<__nv_bfloat16>(s->h2T);
     }
-    ICP_TRY(run_gemm(s, s->h1.ptr, s->w2b(), g, mlp::kHidden, 1));
+    ICP_TRY(run_gemm(s, s->h1.ptr, s->w2b(), g, hid, 1));
     g = layer(M, Hn, Hn);
     g.bias = s->P(s->o_b3);
     g.head_w = s->P(s->o_w4);
@@ -233,7 +241,9 @@ int enqueue_forward(icp_surrogate* s, uint32_t count, bool training, float* y_ou
     if (training) g.out_z = as<__nv_bfloat16>(s->z3);
     g.out_y = y_out;
     g.out_mass = mass_out;
-    return run_gemm(s, s->h2.ptr, s->w3b(), g, mlp::kHead, 1);
+    g.out_mass_sum = mass_sum;
+    g.record_rows = s->C;
+    return run_gemm(s, s->h2.ptr, s->w3b(), g, training ? mlp::kHeadTrain : mlp::kHead, 1);
 }
 
 int enqueue_loss(icp_surrogate* s, uint32_t count, const float* d_target)
@@ -340,6 +350,24 @@ int read_loss(icp_surrogate* s, uint32_t count, double* loss)
     if (loss) *loss = sum / count;
     if (!std::isfinite(sum)) return fail(ICP_ERR_AUDIT, "surrogate: non-finite loss");
     return ok();
+}
+
+// Per-cell diffraction fractions of one record: rows[i] / (np * A) for the Fraunhofer rows of
+// the circle of the record's projected area A (CPU FP64), so that the diffraction adds as much
+// power as the geometric part carries; zero without diffraction.
+int diffraction_fractions(const icp_surrogate* s, const icp_drop_item& it, double* out)
+{
+    const uint32_t nt = s->cfg.nt;
+    std::fill(out, out + nt, 0.0);
+    if (!it.diffraction) return ICP_OK;
+    double k[3], e0[3], e1[3], area = 0;
+    if (const int st = icp_drop_frame(it.inclination_deg, k, e0, e1)) return st;
+    if (const int st = icp_drop_projected_area(it.coefficients, it.radius_mm, k, &area)) return st;
+    if (!(it.wavelength_nm > 0)) return fail(ICP_ERR_INVALID_ARGUMENT, "Diffraction needs a positive wavelength.");
+    const std::vector<double> rows = H::diffraction_rows(s->h_edges, area, it.wavelength_nm);
+    const double scale = 1.0 / ((double)s->cfg.np * area);
+    for (uint32_t i = 0; i < nt; ++i) out[i] = rows[i] * scale;
+    return ICP_OK;
 }
 
 } // namespace
@@ -463,6 +491,7 @@ int icp_surrogate_create(icp_context* c, const icp_surrogate_config* g, icp_surr
     if (e == cudaSuccess) e = s->loss.ensure(sizeof(double) * s->R);
     if (e == cudaSuccess) e = cudaMemcpy(s->cells.ptr, both.data(), 2 * both.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(s->edges.ptr, edges.data(), sizeof(double) * edges.size(), cudaMemcpyHostToDevice);
+    s->h_edges = edges;
     for (Scratch* x : p4)
         if (e == cudaSuccess) e = cudaMemset(x->ptr, 0, np4);
     if (e == cudaSuccess) e = cudaMemset(s->wbf.ptr, 0, s->wbf.bytes);
@@ -580,11 +609,41 @@ int icp_surrogate_generate(icp_surrogate* s, const icp_drop_item* items, uint32_
     ICP_CUDA(s->mass.ensure(sizeof(double) * (uint64_t)count * s->C));
     ICP_CUDA(s->reports.ensure(sizeof(CdfDeviceReport) * s->R));
     ICP_CUDA(s->sync.ensure(2 * sizeof(unsigned) * s->R));
+    ICP_CUDA(s->mass_sum.ensure(sizeof(double) * s->R));
+    ICP_CUDA(s->dfrac.ensure(sizeof(double) * s->R * g.nt));
+    ICP_CUDA(s->drows.ensure(sizeof(double) * s->R * g.nt));
+    ICP_CUDA(cudaMemsetAsync(s->mass_sum.ptr, 0, sizeof(double) * count, c->stream));
     ICP_TRY(enqueue_features(s, items, count, false));
-    ICP_TRY(enqueue_forward(s, count, false, nullptr, as<double>(s->mass)));
+    ICP_TRY(enqueue_forward(s, count, false, nullptr, as<double>(s->mass), as<double>(s->mass_sum)));
+    // the analytic diffraction rows on host threads while the device runs the network
+    std::vector<double> frac((size_t)count * g.nt);
+    std::vector<int> fst(count, ICP_OK);
+    {
+        const unsigned workers = std::max(1u, std::min<unsigned>(count, std::thread::hardware_concurrency()));
+        std::vector<std::future<void>> jobs;
+        for (unsigned w = 0; w < workers; ++w)
+            jobs.push_back(std::async(std::launch::async, [&, w]() {
+                for (uint32_t r = w; r < count; r += workers)
+                    fst[r] = diffraction_fractions(s, items[r], frac.data() + (size_t)r * g.nt);
+            }));
+        for (auto& j : jobs) j.get();
+    }
+    for (uint32_t r = 0; r < count; ++r)
+        if (fst[r]) {
+            cudaStreamSynchronize(c->stream);
+            return fail(fst[r], "surrogate: record %u: diffraction rows failed", r);
+        }
+    ICP_CUDA(cudaMemcpyAsync(s->dfrac.ptr, frac.data(), sizeof(double) * frac.size(), cudaMemcpyHostToDevice, c->stream));
+    {
+        const int e = mlp::launch_scale_rows(as<double>(s->dfrac), as<double>(s->mass_sum), count, g.nt,
+                                             as<double>(s->drows), c->stream);
+        count_launch();
+        if (e) return fail(ICP_ERR_DEVICE, "row launch failed (%d)", e);
+    }
     for (uint32_t r = 0; r < count; ++r)
         ICP_TRY(cdf_enqueue(c, as<double>(s->mass) + (uint64_t)r * s->C, g.nt, g.np, ct, cp, as<double>(s->edges), 0.0,
-                            0.0, nullptr, 0.0, nullptr, d_phi + (size_t)(cp + 1) * r, d_theta + (size_t)cp * (ct + 1) * r,
+                            0.0, nullptr, 0.0, items[r].diffraction ? as<double>(s->drows) + (size_t)r * g.nt : nullptr,
+                            d_phi + (size_t)(cp + 1) * r, d_theta + (size_t)cp * (ct + 1) * r,
                             as<CdfDeviceReport>(s->reports) + r, as<unsigned>(s->sync) + 2 * r));
     std::vector<CdfDeviceReport> dev(count);
     ICP_CUDA(cudaMemcpyAsync(dev.data(), s->reports.ptr, sizeof(CdfDeviceReport) * count, cudaMemcpyDeviceToHost,

@@ -185,6 +185,13 @@ __global__ void weight_copies_kernel(WeightViews w)
     }
 }
 
+__global__ void scale_rows_kernel(const double* __restrict__ frac, const double* __restrict__ sums, uint32_t nt,
+                                  uint32_t total, double* __restrict__ rows)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < total) rows[t] = sums[t / nt] * frac[t];
+}
+
 __global__ void cdf_cells_kernel(const double* __restrict__ phi, const double* __restrict__ theta, uint32_t ct,
                                  uint32_t cp, uint64_t total, float* __restrict__ p)
 {
@@ -247,6 +254,14 @@ int launch_weight_copies(const WeightViews& w, cudaStream_t st)
 {
     const uint64_t n = (uint64_t)w.H * w.K0 + 2ull * w.H * w.H;
     weight_copies_kernel<<<blocks_of(n, 256), 256, 0, st>>>(w);
+    return (int)cudaGetLastError();
+}
+
+int launch_scale_rows(const double* frac, const double* sums, uint32_t records, uint32_t nt, double* rows,
+                      cudaStream_t st)
+{
+    const uint32_t total = records * nt;
+    scale_rows_kernel<<<blocks_of(total, 256), 256, 0, st>>>(frac, sums, nt, total, rows);
     return (int)cudaGetLastError();
 }
 

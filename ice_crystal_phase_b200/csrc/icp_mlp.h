@@ -16,7 +16,9 @@ namespace icp::mlp {
 //   kHead       kHidden, and y[m] = sum_n silu(z) * head_w[n] + head_b into out_y (FP32) and / or
 //               out_mass[m] = exp(y) (FP64)                  (the 256 -> 1 head)
 //   kBackprop   dz = D * silu'(z_prev) into out_dz and out_dzT (BF16); out_db[n] += sum_m dz
-enum Epi : int { kStoreF32 = 0, kAtomicF32 = 1, kHidden = 2, kHead = 3, kBackprop = 4 };
+// kHidden / kHead write only out_h / out_y, out_mass (inference); kHiddenTrain / kHeadTrain also
+// out_z and out_hT (a training step keeps them for the backward pass).
+enum Epi : int { kStoreF32 = 0, kAtomicF32 = 1, kHidden = 2, kHead = 3, kBackprop = 4, kHiddenTrain = 5, kHeadTrain = 6 };
 
 struct GemmArgs {
     uint32_t M, N, K;       // M % 128 == 0, N in {64, 128, 256}, K % 64 == 0
@@ -32,6 +34,8 @@ struct GemmArgs {
     float head_b;
     float* out_y;
     double* out_mass;
+    double* out_mass_sum;   // kHead: += sum of out_mass over each record's rows (or null)
+    uint32_t record_rows;   // rows per record (a multiple of 128)
     const __nv_bfloat16* z_prev;
     __nv_bfloat16* out_dz;
     __nv_bfloat16* out_dzT;
@@ -73,6 +77,11 @@ struct WeightViews {
     uint32_t H, K0;
 };
 int launch_weight_copies(const WeightViews& w, cudaStream_t st);
+// Analytic diffraction rows of each record in the units of its predicted cell mass:
+// rows[r][i] = sums[r] * frac[r][i] (frac = the diffraction power of row i per cell and per
+// unit of geometric power, zero for records without diffraction).
+int launch_scale_rows(const double* frac, const double* sums, uint32_t records, uint32_t nt, double* rows,
+                      cudaStream_t st);
 // Cell probabilities from stored CDFs at the histogram resolution: p[r][i * cp + j] =
 // (phi[j+1] - phi[j]) * (theta[j][i+1] - theta[j][i]).
 int launch_cdf_cells(const double* phi, const double* theta, uint32_t records, uint32_t ct, uint32_t cp, float* p,

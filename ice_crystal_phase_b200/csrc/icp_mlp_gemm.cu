@@ -37,12 +37,24 @@ template <int N> __host__ __device__ constexpr uint32_t stage_bytes() { return k
 // 1024 (alignment) + stages + barriers / TMEM slot (256) + column sums of the bias gradient (1024)
 template <int N> constexpr size_t smem_bytes() { return 1024 + (size_t)stages<N>() * stage_bytes<N>() + 256 + 1024; }
 
-// SiLU and its derivative with the fast exponential and division (relative error ~1e-7, far
-// below the BF16 rounding of the stored activations); exp(-z) = inf gives 0 as it should.
-__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
+// Logistic function 1 / (1 + exp(-z)) with the exponential on the special-function unit and
+// the reciprocal on the FMA pipe, so that the two pipes share the epilogue's activation work
+// (one SiLU per output element is the MLP's largest non-tensor cost).  Reciprocal of d >= 1:
+// the exponent-negation seed y0 = 2 bits(1.0) - bits(d) (relative error at most 1/8), then three
+// Newton steps y <- y (2 - d y) (error squares each step: 1/8 -> 1.6e-2 -> 2.4e-4 -> 6e-8).
+// z is clamped at -80 so that d stays finite; the result then is below 2e-35.
+__device__ __forceinline__ float logistic(float z)
+{
+    const float d = 1.0f + __expf(-fmaxf(z, -80.0f));
+    float y = __int_as_float(0x7F000000 - __float_as_int(d));
+#pragma unroll
+    for (int k = 0; k < 3; ++k) y = fmaf(y, fmaf(-d, y, 1.0f), y);
+    return y;
+}
+__device__ __forceinline__ float silu(float z) { return z * logistic(z); }
 __device__ __forceinline__ float silu_grad(float z)
 {
-    const float s = __fdividef(1.0f, 1.0f + __expf(-z));
+    const float s = logistic(z);
     return s * (1.0f + z * (1.0f - s));
 }
 
@@ -83,7 +95,7 @@ __device__ __forceinline__ float warp_column_sum(float (&v)[32], uint32_t lane)
 __device__ __forceinline__ void store_bf16x32_t(__nv_bfloat16* dst, uint32_t ld, const float (&v)[32])
 {
     __nv_bfloat16* p = dst;
-#pragma unroll
+#pragma unroll 8
     for (int i = 0; i < 32; ++i) {
         *p = __float2bfloat16_rn(v[i]);
         p += ld;
@@ -116,6 +128,9 @@ __device__ __forceinline__ float epilogue_cols(const GemmArgs& g, uint32_t taddr
                                               uint32_t c0, uint32_t c1, const float* bias, const float* head_w,
                                               float* colsum)
 {
+    constexpr bool kHeadEpi = EPI == kHead || EPI == kHeadTrain;
+    constexpr bool kTrain = EPI == kHiddenTrain || EPI == kHeadTrain;
+    constexpr bool kLayer = kHeadEpi || EPI == kHidden || EPI == kHiddenTrain;
     float yacc = 0.0f;
 #pragma unroll 1
     for (uint32_t c = c0; c < c1; c += 32u) {
@@ -129,7 +144,7 @@ __device__ __forceinline__ float epilogue_cols(const GemmArgs& g, uint32_t taddr
             float* d = g.out_f32 + (size_t)m * g.ld_out + c;
 #pragma unroll
             for (int i = 0; i < 32; ++i) atomicAdd(d + i, v[i]);
-        } else if constexpr (EPI == kHidden || EPI == kHead) {
+        } else if constexpr (kLayer) {
             const float4* b4 = reinterpret_cast<const float4*>(bias + c);
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
@@ -139,12 +154,14 @@ __device__ __forceinline__ float epilogue_cols(const GemmArgs& g, uint32_t taddr
                 v[4 * q + 2] += b.z;
                 v[4 * q + 3] += b.w;
             }
-            if (g.out_z) store_bf16x32(g.out_z + (size_t)m * N + c, v);
+            if constexpr (kTrain)
+                if (g.out_z) store_bf16x32(g.out_z + (size_t)m * N + c, v);
 #pragma unroll
             for (int i = 0; i < 32; ++i) v[i] = silu(v[i]);
             if (g.out_h) store_bf16x32(g.out_h + (size_t)m * N + c, v);
-            if (g.out_hT) store_bf16x32_t(g.out_hT + (size_t)c * g.ld_t + m, g.ld_t, v);
-            if constexpr (EPI == kHead) {
+            if constexpr (kTrain)
+                if (g.out_hT) store_bf16x32_t(g.out_hT + (size_t)c * g.ld_t + m, g.ld_t, v);
+            if constexpr (kHeadEpi) {
                 const float4* w4 = reinterpret_cast<const float4*>(head_w + c);
 #pragma unroll
                 for (int q = 0; q < 8; ++q) {
@@ -168,11 +185,21 @@ __device__ __forceinline__ float epilogue_cols(const GemmArgs& g, uint32_t taddr
     return yacc;
 }
 
+// The head's output of row m (one lane per row; called by whole warps whose 32 rows belong to
+// one record): y, and the cell mass exp(y) with its per-record sum (one atomic per warp).
 __device__ __forceinline__ void head_store(const GemmArgs& g, uint32_t m, float yacc)
 {
     const float y = yacc + g.head_b;
     if (g.out_y) g.out_y[m] = y;
-    if (g.out_mass) g.out_mass[m] = exp((double)y);
+    if (g.out_mass) {
+        double e = exp((double)y);
+        g.out_mass[m] = e;
+        if (g.out_mass_sum) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+            if ((threadIdx.x & 31u) == 0) atomicAdd(&g.out_mass_sum[m / g.record_rows], e);
+        }
+    }
 }
 
 // Split-K GEMM (one 128-row tile and one K range per CTA): the weight gradients, whose K (the
@@ -268,7 +295,7 @@ __global__ void __launch_bounds__(128, 1)
         const uint32_t m = m0 + 32u * warp + lane;
         const float y = epilogue_cols<N, EPI>(g, tmem + ((32u * warp) << 16), m, lane, 0u, (uint32_t)N, g.bias,
                                               g.head_w, colsum);
-        if constexpr (EPI == kHead) head_store(g, m, y);
+        if constexpr (EPI == kHead || EPI == kHeadTrain) head_store(g, m, y);
     }
     if constexpr (EPI == kBackprop) {
         __syncthreads();
@@ -321,6 +348,7 @@ __global__ void __launch_bounds__(kPThreads, 1)
                            const GemmArgs g)
 {
     constexpr int S = pstages<N, KC>();
+    constexpr bool kHeadEpi = EPI == kHead || EPI == kHeadTrain;
     constexpr uint32_t BB = (uint32_t)N * 128u;   // one 64-wide K chunk of B
     constexpr uint32_t W = (uint32_t)N / kSlices; // columns per epilogue warp
     static_assert(S >= 2, "ring too shallow");
@@ -360,8 +388,8 @@ __global__ void __launch_bounds__(kPThreads, 1)
     }
     for (uint32_t i = threadIdx.x; i < (uint32_t)N; i += blockDim.x) {
         colsum[i] = 0.0f;
-        if constexpr (EPI == kHidden || EPI == kHead) sbias[i] = g.bias[i];
-        if constexpr (EPI == kHead) shead[i] = g.head_w[i];
+        if constexpr (kHeadEpi || EPI == kHidden || EPI == kHiddenTrain) sbias[i] = g.bias[i];
+        if constexpr (kHeadEpi) shead[i] = g.head_w[i];
     }
     if (warp == 1) umma::tmem_alloc(tslot, 2u * N);
     umma::fence_before_sync();
@@ -467,7 +495,7 @@ __global__ void __launch_bounds__(kPThreads, 1)
                 __syncwarp();
                 if (lane == 0) umma::mbar_arrive(&acc_empty[b]);
             }
-            if constexpr (EPI == kHead) {
+            if constexpr (kHeadEpi) {
                 // the slices of a lane quarter meet here every tile (also after an abort, so that
                 // the named barrier never waits for a warp that has left the loop)
                 if (slice) ypart[(slice - 1u) * 128u + row] = y;
@@ -603,6 +631,8 @@ int gemm(const void* A, const void* B, GemmArgs g, int epi, uint32_t splits, cud
         case kStoreF32: return launch_pe<kStoreF32>(A, B, g, st);
         case kHidden: return launch_pe<kHidden>(A, B, g, st);
         case kHead: return launch_pe<kHead>(A, B, g, st);
+        case kHiddenTrain: return launch_pe<kHiddenTrain>(A, B, g, st);
+        case kHeadTrain: return launch_pe<kHeadTrain>(A, B, g, st);
         case kBackprop: return launch_pe<kBackprop>(A, B, g, st);
         default: return -4;
         }
@@ -612,6 +642,8 @@ int gemm(const void* A, const void* B, GemmArgs g, int epi, uint32_t splits, cud
     case kAtomicF32: return launch_epi<kAtomicF32>(A, B, g, splits, st);
     case kHidden: return launch_epi<kHidden>(A, B, g, 1, st);
     case kHead: return launch_epi<kHead>(A, B, g, 1, st);
+    case kHiddenTrain: return launch_epi<kHiddenTrain>(A, B, g, 1, st);
+    case kHeadTrain: return launch_epi<kHeadTrain>(A, B, g, 1, st);
     case kBackprop: return launch_epi<kBackprop>(A, B, g, 1, st);
     default: return -4;
     }

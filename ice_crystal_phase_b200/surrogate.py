@@ -5,8 +5,10 @@ every record with the tracer, one process per record).
 
 1. Training set: records drawn from the batched-record distribution (radius log-uniform
    0.1-3 mm, wavelength 400-700 nm, inclination -90..90 deg, rays proportional to the projected
-   area) traced by the batched tracer at the network's cell grid; the targets are their cell
-   probabilities (icp_surrogate_targets).
+   area) traced by the batched tracer at the network's cell grid without the diffraction stage;
+   the targets are their cell probabilities (icp_surrogate_targets).  The network learns the
+   geometric-optics part only: a record with diffraction gets the analytic Fraunhofer rows of
+   its projected area added by icp_surrogate_generate, with as much power as the geometric part.
 2. Training: Adam with a cosine learning rate over whole records (the loss is the per-record KL
    divergence, which needs every cell of a record), all on the device
    (icp_surrogate_train_step).
@@ -124,16 +126,30 @@ def mean_loss(sur: I.Surrogate, specs: list, targets) -> float:
 
 
 def predicted_cells(sur: I.Surrogate, specs: list):
-    """Softmax of the prediction per record, device float64 [len(specs), nt*np]."""
+    """Cell probabilities of the records the surrogate emits (icp_surrogate_generate at the full
+    cell grid, so that the judged output is the served one: the network's geometric part plus the
+    analytic diffraction rows), device float64 [len(specs), nt*np]."""
     torch = _torch()
-    R, Cn = sur.cfg.max_records, sur.cells
-    y = torch.empty((min(R, len(specs)), Cn), dtype=torch.float32, device="cuda")
+    R, Cn, nt, np_ = sur.cfg.max_records, sur.cells, sur.cfg.nt, sur.cfg.np
+    n = min(R, len(specs))
+    phi = torch.empty(n * (np_ + 1), dtype=torch.float64, device="cuda")
+    theta = torch.empty(n * np_ * (nt + 1), dtype=torch.float64, device="cuda")
+    cells = torch.empty((n, Cn), dtype=torch.float32, device="cuda")
     out = torch.empty((len(specs), Cn), dtype=torch.float64, device="cuda")
     for i in range(0, len(specs), R):
         part = specs[i:i + R]
-        sur.predict(part, y.data_ptr())
-        out[i:i + len(part)] = torch.softmax(y[:len(part)].double(), dim=1)
+        sur.generate(part, nt, np_, phi.data_ptr(), theta.data_ptr(), raise_on_audit=False)
+        sur.targets(phi.data_ptr(), theta.data_ptr(), len(part), cells.data_ptr())
+        out[i:i + len(part)] = cells[:len(part)].double()
     return out
+
+
+def geometric(specs: list) -> list:
+    """The same records without the diffraction stage: the network's training targets (the
+    surrogate adds the analytic diffraction rows itself)."""
+    return [I.DropSpec(sp.coefficients, sp.radius_mm, sp.interior_index, sp.rays, seed=sp.seed,
+                       inclination_deg=sp.inclination_deg, wavelength_nm=sp.wavelength_nm, diffraction=False)
+            for sp in specs]
 
 
 def coarse(p, nt, np_, ct, cp):
@@ -305,8 +321,8 @@ def run_training(ctx: I.Context, s: TrainSettings, cfg_over: dict | None = None,
                                    rays_min=s.rays_min, diffraction=True)
     train_specs, held = specs[:s.records], specs[s.records:]
     t0 = time.perf_counter()
-    targets = trace_cells(ctx, sur, train_specs, hits=s.max_internal_hits)
-    held_targets = trace_cells(ctx, sur, held, hits=s.max_internal_hits)
+    targets = trace_cells(ctx, sur, geometric(train_specs), hits=s.max_internal_hits)
+    held_targets = trace_cells(ctx, sur, geometric(held), hits=s.max_internal_hits)
     torch.cuda.synchronize()
     t_data = time.perf_counter() - t0
     rays = sum(sp.rays for sp in train_specs)

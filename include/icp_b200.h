@@ -362,7 +362,8 @@ int icp_mlp_gemm_bf16(icp_context* ctx, const void* d_a, const void* d_b, uint32
  * record), three SiLU layers of `hidden` units (BF16 weights and activations, FP32
  * accumulation on the tensor cores), a linear head to one value y per cell.  Cell probability =
  * softmax of y over the record's cells.  Trained by the mean per-record KL divergence of the
- * tracer's cell probabilities from the prediction. */
+ * tracer's cell probabilities (records traced without the diffraction stage, which
+ * icp_surrogate_generate adds analytically) from the prediction. */
 typedef struct icp_surrogate icp_surrogate;
 
 typedef struct {
@@ -411,9 +412,12 @@ int icp_surrogate_train_step(icp_surrogate* s, const icp_drop_item* items, uint3
                              const icp_adam* opt, double* loss);
 /* y of every cell: d_logits[count][nt*np] (device FP32), log cell mass up to a per-record constant. */
 int icp_surrogate_predict(icp_surrogate* s, const icp_drop_item* items, uint32_t count, float* d_logits);
-/* Records from the prediction: cell mass exp(y) through the CDF build at storage grid (ct, cp);
- * phi / theta of record r at d_phi + r*(cp+1), d_theta + r*cp*(ct+1) (device), one CDF report
- * per record (host; status = the record's audit result). */
+/* Records from the prediction: the network gives the geometric-optics cell mass exp(y); an item
+ * with diffraction = 1 also gets the analytic Fraunhofer rows of the circle of its projected area
+ * (CPU FP64, on host threads while the device runs the network) carrying the same total power,
+ * as in a traced record.  Then the CDF build at storage grid (ct, cp); phi / theta of record r
+ * at d_phi + r*(cp+1), d_theta + r*cp*(ct+1) (device), one CDF report per record (host; status
+ * = the record's audit result). */
 int icp_surrogate_generate(icp_surrogate* s, const icp_drop_item* items, uint32_t count, uint32_t ct, uint32_t cp,
                            const icp_cdf_policy* policy, double* d_phi, double* d_theta, icp_cdf_report* reports);
 /* Training targets: cell probabilities of `count` stored records at the surrogate's grid

@@ -92,8 +92,13 @@ def test_train_step_applies_adam(ctx, icp):
     assert last < 0.9 * l1
 
 
-def test_generated_records_are_the_predicted_softmax(ctx, icp):
+@pytest.mark.parametrize("diffraction", [False, True])
+def test_generated_records_are_the_predicted_softmax(ctx, icp, diffraction):
+    """Records: the softmax of the prediction (the geometric part) and, with diffraction, the
+    analytic Fraunhofer rows of the projected area carrying the same power."""
     cfg, oc, specs, X, p, t = _setup(icp, SMALL, 3, 31)
+    for sp in specs:
+        sp.diffraction = diffraction
     ct, cp = 16, 32
     C = cfg.nt * cfg.np
     with icp.Surrogate(ctx, cfg) as s:
@@ -110,9 +115,15 @@ def test_generated_records_are_the_predicted_softmax(ctx, icp):
     assert np.abs(yd - yo).max() <= 1e-3 * max(1.0, np.abs(yo).max())
     a = phi.cpu().numpy().reshape(3, cp + 1)
     T = theta.cpu().numpy().reshape(3, cp, ct + 1)
+    edges = icp.u_edges(cfg.nt)
     for r in range(3):
         q = np.exp(yd[r * C:(r + 1) * C] - yd[r * C:(r + 1) * C].max())
         q = (q / q.sum()).reshape(cfg.nt, cfg.np)
+        if diffraction:
+            sp = specs[r]
+            area = icp.compute_projected_area(sp.coefficients, sp.radius_mm, icp.drop_frame(sp.inclination_deg)[0])
+            rows = icp.diffraction_rows(edges, area, sp.wavelength_nm) / area
+            q = 0.5 * q + 0.5 * np.repeat(rows[:, None] / cfg.np, cfg.np, axis=1)
         agg = q.reshape(ct, cfg.nt // ct, cp, cfg.np // cp).sum(axis=(1, 3))
         stored = np.diff(a[r])[None, :] * np.diff(T[r], axis=1).T
         assert a[r][0] == 0 and a[r][-1] == 1 and np.all(np.diff(a[r]) >= 0)
