@@ -493,6 +493,99 @@ def run_batched(I, ctx, stream, a, nt: int, np_: int) -> dict:
                       "sample_rays_per_s": tuned_rate}, "all_records_pass_cdf_audits": tv_ok}
 
 
+
+
+def run_surrogate(I, ctx, stream, a) -> dict:
+    """The learned surrogate on fresh records of the batched distribution (256 x 512 cells, stored
+    at 64 x 128): records/s of serving (surrogate where the fallback gate trusts it, the batched
+    tracer elsewhere) and of the surrogate alone, against the plain single-record tracer entry on
+    the same records; held-out TV of a fresh sample against 1e8-ray tracer records; the forward
+    pass against the measured BF16 tensor peak."""
+    import ctypes as C
+
+    import torch
+
+    import ice_crystal_phase_b200.surrogate as S
+
+    if not S.DEFAULT_MODEL.exists():
+        return {"unavailable": f"{S.DEFAULT_MODEL.name} missing"}
+    R = 32
+    sur, extra = S.load(ctx, S.DEFAULT_MODEL, max_records=R)
+    gate = S.FallbackGate.from_dict(extra["gate"])
+    ct, cp = extra["storage"]
+    nt, np_ = sur.cfg.nt, sur.cfg.np
+    specs = I.batched_record_specs(a.surrogate_records, seed=20260102)
+    n = len(specs)
+    phi = torch.empty(n * (cp + 1), dtype=torch.float64, device="cuda")
+    theta = torch.empty(n * cp * (ct + 1), dtype=torch.float64, device="cuda")
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3, out
+
+    def surrogate_only():
+        for i in range(0, n, R):
+            sur.generate(specs[i:i + R], ct, cp, phi[i * (cp + 1):].data_ptr(), theta[i * cp * (ct + 1):].data_ptr(),
+                         raise_on_audit=False)
+
+    surrogate_only()  # warm-up
+    t_sur = min(timed(surrogate_only)[0] for _ in range(3))
+    launches0 = I.kernel_launches()
+    S.serve(ctx, sur, specs, gate, ct, cp, phi, theta)  # warm-up
+    t_serve, served = timed(lambda: S.serve(ctx, sur, specs, gate, ct, cp, phi, theta))
+    launches = (I.kernel_launches() - launches0) // 2
+    # the plain GPU tracer: the same records one by one through the single-record device entry
+    rec_phi = torch.empty(cp + 1, dtype=torch.float64, device="cuda")
+    rec_theta = torch.empty(cp * (ct + 1), dtype=torch.float64, device="cuda")
+
+    def plain():
+        for sp in specs:
+            r = I._drop_args(sp.coefficients, sp.radius_mm, sp.inclination_deg, sp.interior_index, sp.rays, sp.seed,
+                             nt, np_, ct, cp, 1.0, 10, 1e-12, I.ICP_FP32, 1e-10, sp.wavelength_nm, True)
+            rr = I.DropReport()
+            I.check(I.LIB.icp_drop_generate_device(ctx.handle, C.byref(r), C.c_void_p(rec_phi.data_ptr()),
+                                                   C.c_void_p(rec_theta.data_ptr()), None, C.byref(rr)))
+
+    t_plain, _ = timed(plain)
+    # forward pass of R records on the tensor cores
+    y = torch.empty(R * sur.cells, dtype=torch.float32, device="cuda")
+    sur.predict(specs[:R], y.data_ptr())
+    t_fwd = min(timed(lambda: sur.predict(specs[:R], y.data_ptr()))[0] for _ in range(5))
+    H, K0 = sur.cfg.hidden, sur.cfg.input_width
+    flops = 2.0 * R * sur.cells * (K0 * H + 2 * H * H + H)
+    peaks = _peaks()
+    bf16 = peaks.get("bf16_tflops", 1590.0)
+    # fresh held-out sample judged by the tracer
+    judge_specs = I.batched_record_specs(a.surrogate_judged, seed=20260103)
+    st = S.TrainSettings(judge_rays=1e8, storage=(ct, cp))
+    ev = S.evaluate(ctx, sur, judge_specs, st)
+    sur.close()
+    tv = ev["storage"]["tv"]
+    return {
+        "workload": "learned_surrogate_config5", "model": S.DEFAULT_MODEL.name, "records": n, "cells": [nt, np_],
+        "storage": [ct, cp], "network": {"hidden": H, "layers": 4, "input_width": K0, "dtype": "bf16 weights and "
+                                         "activations, fp32 accumulation (tcgen05, TMEM)"},
+        "surrogate_records_per_s": n / t_sur, "served_records_per_s": n / t_serve,
+        "served_by_surrogate": served["surrogate"], "served_by_tracer": served["tracer"],
+        "plain_tracer_records_per_s": n / t_plain,
+        "speedup_served_vs_plain": t_plain / t_serve, "speedup_surrogate_only_vs_plain": t_plain / t_sur,
+        "kernel_launches_per_serve": launches,
+        "heldout": {"records": len(tv), "judge_rays": 1e8, "tv_storage_mean": ev["storage"]["tv_mean"],
+                    "tv_storage_median": ev["storage"]["tv_median"], "judge_floor_storage": ev["storage"]["floor_mean"],
+                    "tv_cells_mean": ev["cells"]["tv_mean"], "judge_floor_cells": ev["cells"]["floor_mean"],
+                    "pass_fraction_tv_5e-3": ev["pass_fraction"]},
+        "roofline_forward": {"kernel": "gemm_persistent_kernel x3 (forward pass)", "bound": "tensor",
+                             "achieved": flops / t_fwd / 1e12, "peak": bf16, "unit": "TFLOP/s",
+                             "frac": flops / t_fwd / 1e12 / bf16, "records": R, "ms": 1e3 * t_fwd,
+                             "peak_note": "MEASURED_PEAKS.json bf16_tflops (of measured)"},
+    }
+
+
 def _peaks() -> dict:
     try:
         return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
@@ -671,6 +764,9 @@ def run_b200_drop(a) -> None:
     batched = None
     if world == 1 and a.batch_records > 0:
         batched = run_batched(I, ctx, stream, a, nt, np_)
+    surrogate = None
+    if world == 1 and a.surrogate_records > 0:
+        surrogate = run_surrogate(I, ctx, stream, a)
 
     s0 = stats_all[-1]
     r0 = reps[-1]
@@ -702,6 +798,8 @@ def run_b200_drop(a) -> None:
     }
     if batched is not None:
         line["batched"] = batched
+    if surrogate is not None:
+        line["surrogate"] = surrogate
     if r0 is not None:
         line["record"] = {"g": r0.cdf.g_stored, "projected_area_mm2": r0.projected_area_mm2,
                           "incident_area_mm2": r0.incident_area_mm2, "diffraction_mm2": r0.diffraction_area_mm2,
@@ -726,6 +824,8 @@ def main() -> None:
     p.add_argument("--block-threads", type=int, default=0, help="trace block size (0 = library default)")
     p.add_argument("--batch-records", type=int, default=256, help="records of the batched measurement (0 = skip)")
     p.add_argument("--batch-steps", type=int, default=3)
+    p.add_argument("--surrogate-records", type=int, default=256, help="records of the surrogate measurement (0 = skip)")
+    p.add_argument("--surrogate-judged", type=int, default=32, help="fresh records judged by 1e8-ray tracer records")
     p.add_argument("--hash-slots", type=int, default=0, help="shared histogram slots (0 = default, 1 = none)")
     p.add_argument("--rays", type=float, default=1e8)
     p.add_argument("--ref-rays", type=float, default=1.6e6, help="reference rays per step (all processes)")

@@ -832,15 +832,15 @@ def generate_drop_batch(ctx: Context, specs: list, settings: BatchSettings) -> D
 
 
 def batched_record_specs(count: int = 256, seed: int = 20260101, rays_max: float = 6e7, rays_min: float = 1e6,
-                         diffraction: bool = True, rays_scale: float = 1.0) -> list:
-    """Drop records of the batched workload: radius log-uniform in [0.1, 3] mm, wavelength uniform
-    in [400, 700] nm, inclination uniform in [-90, 90] deg, Table-I shapes, water at 20 C, rays
-    proportional to the projected area (rays_max for the area of a 3 mm disk), clipped to
-    [rays_min, rays_max] and then multiplied by rays_scale."""
+                         diffraction: bool = True, rays_scale: float = 1.0, radius_range: tuple = (0.1, 3.0)) -> list:
+    """Drop records of the batched workload: radius log-uniform in [0.1, 3] mm (radius_range),
+    wavelength uniform in [400, 700] nm, inclination uniform in [-90, 90] deg, Table-I shapes,
+    water at 20 C, rays proportional to the projected area (rays_max for the area of a 3 mm
+    disk), clipped to [rays_min, rays_max] and then multiplied by rays_scale."""
     rng = np.random.default_rng(seed)
     specs = []
     for _ in range(count):
-        radius = float(np.exp(rng.uniform(np.log(0.1), np.log(3.0))))
+        radius = float(np.exp(rng.uniform(np.log(radius_range[0]), np.log(radius_range[1]))))
         lam = float(rng.uniform(400.0, 700.0))
         incl = float(rng.uniform(-90.0, 90.0))
         r32 = float(np.float32(radius))

@@ -37,6 +37,10 @@ import numpy as np
 
 import ice_crystal_phase_b200 as I
 
+# The trained network for the batched-record distribution (parameters, configuration, fallback
+# gate), written by `train` and read by bench.py and the tests.
+DEFAULT_MODEL = Path(__file__).resolve().parent / "surrogate_drop.npz"
+
 
 @dataclass
 class TrainSettings:
@@ -56,6 +60,11 @@ class TrainSettings:
     storage: tuple = (64, 128)
     tv_threshold: float = 5e-3
     neighbours: int = 3
+    # extra training records with the radius log-uniform over [large_radius_mm, 3] mm (the
+    # oblate drops, whose patterns are the hardest to learn); the held-out records keep the
+    # batched distribution
+    large_records: int = 0
+    large_radius_mm: float = 0.8
 
 
 def _torch():
@@ -320,6 +329,10 @@ def run_training(ctx: I.Context, s: TrainSettings, cfg_over: dict | None = None,
     specs = I.batched_record_specs(s.records + s.heldout, seed=1000 * s.seed + 1, rays_max=s.rays_max,
                                    rays_min=s.rays_min, diffraction=True)
     train_specs, held = specs[:s.records], specs[s.records:]
+    if s.large_records:
+        train_specs = train_specs + I.batched_record_specs(s.large_records, seed=1000 * s.seed + 2,
+                                                           rays_max=s.rays_max, rays_min=s.rays_min, diffraction=True,
+                                                           radius_range=(s.large_radius_mm, 3.0))
     t0 = time.perf_counter()
     targets = trace_cells(ctx, sur, geometric(train_specs), hits=s.max_internal_hits)
     held_targets = trace_cells(ctx, sur, geometric(held), hits=s.max_internal_hits)
@@ -358,9 +371,10 @@ def main(argv=None) -> int:
     sub = p.add_subparsers(dest="cmd", required=True)
     t = sub.add_parser("train")
     t.add_argument("--out", required=True)
-    for f in ("records", "heldout", "epochs", "batch", "seed", "max_internal_hits", "warmup_steps", "neighbours"):
+    for f in ("records", "heldout", "epochs", "batch", "seed", "max_internal_hits", "warmup_steps", "neighbours",
+              "large_records"):
         t.add_argument("--" + f.replace("_", "-"), type=int, default=getattr(TrainSettings, f))
-    for f in ("lr", "lr_final", "weight_decay", "rays_max", "rays_min", "judge_rays", "tv_threshold"):
+    for f in ("lr", "lr_final", "weight_decay", "rays_max", "rays_min", "judge_rays", "tv_threshold", "large_radius_mm"):
         t.add_argument("--" + f.replace("_", "-"), type=float, default=getattr(TrainSettings, f))
     t.add_argument("--nt", type=int, default=256)
     t.add_argument("--np", type=int, default=512)
