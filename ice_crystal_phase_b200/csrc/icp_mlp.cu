@@ -121,35 +121,71 @@ __global__ void __launch_bounds__(1024) softmax_loss_kernel(const float* __restr
     }
 }
 
-// Block = H threads (thread n = column n) over kRows rows: row-major dz3 coalesced across the
-// block, the column-major copy written 8 rows (16 bytes) at a time per thread.
-constexpr uint32_t kHeadRows = 256;
-__global__ void head_backward_kernel(const __nv_bfloat16* __restrict__ z3, const float* __restrict__ dy,
-                                     const float* __restrict__ w4, uint32_t M, uint32_t H, __nv_bfloat16* __restrict__ dz3,
-                                     __nv_bfloat16* __restrict__ dz3T, float* __restrict__ dw4, float* __restrict__ db3)
+// One block of 256 threads per tile of kHeadRows = 64 rows x H columns (H <= 256, a multiple of
+// 64).  Load: thread t owns the 8 columns 8 (t mod H/8) .. and the rows t / (H/8) + k (256 / (H/8)),
+// reading z3 and writing dz3 as 16-byte vectors (coalesced rows); dz3 also goes into a shared
+// tile.  Transpose: thread t < H writes the 64 rows of column t of the tile to dz3T as eight
+// 16-byte vectors (one contiguous 128-byte run per column).  Column sums of dy h3 (dw4) and of
+// dz3 (db3) are reduced in registers and shared memory, one atomic per column per block.
+constexpr uint32_t kHeadRows = 64;
+__global__ void __launch_bounds__(256) head_backward_kernel(const __nv_bfloat16* __restrict__ z3,
+                                                            const float* __restrict__ dy, const float* __restrict__ w4,
+                                                            uint32_t M, uint32_t H, __nv_bfloat16* __restrict__ dz3,
+                                                            __nv_bfloat16* __restrict__ dz3T, float* __restrict__ dw4,
+                                                            float* __restrict__ db3)
 {
-    const uint32_t n = threadIdx.x;
+    __shared__ __align__(16) __nv_bfloat16 tile[kHeadRows][256 + 8];
+    __shared__ float sw[256], sb[256];
+    const uint32_t t = threadIdx.x, groups = H / 8u, rstep = 256u / groups;
+    const uint32_t g = t % groups, r0 = t / groups, c = 8u * g;
     const uint64_t m0 = (uint64_t)blockIdx.x * kHeadRows;
-    const float w = w4[n];
-    float sw = 0.0f, sb = 0.0f;
-    for (uint32_t r8 = 0; r8 < kHeadRows; r8 += 8) {
-        __align__(16) __nv_bfloat16 col[8];
-#pragma unroll
-        for (uint32_t k = 0; k < 8; ++k) {
-            const uint64_t m = m0 + r8 + k;
-            const float z = __bfloat162float(z3[m * H + n]);
-            const float d = dy[m];
-            const float g = d * w * silu_grad_of(z);
-            sw = fmaf(d, silu_of(z), sw);
-            sb += g;
-            const __nv_bfloat16 gb = __float2bfloat16_rn(g);
-            dz3[m * H + n] = gb;
-            col[k] = gb;
-        }
-        *reinterpret_cast<uint4*>(dz3T + (uint64_t)n * M + m0 + r8) = *reinterpret_cast<const uint4*>(col);
+    for (uint32_t i = t; i < H; i += 256u) {
+        sw[i] = 0.0f;
+        sb[i] = 0.0f;
     }
-    atomicAdd(&dw4[n], sw);
-    atomicAdd(&db3[n], sb);
+    float w[8], aw[8] = {}, ab[8] = {};
+#pragma unroll
+    for (int k = 0; k < 8; ++k) w[k] = w4[c + k];
+    __syncthreads();
+    for (uint32_t r = r0; r < kHeadRows; r += rstep) {
+        const uint64_t m = m0 + r;
+        const float d = dy[m];
+        const uint4 u = *reinterpret_cast<const uint4*>(z3 + m * H + c);
+        const uint32_t zw[4] = {u.x, u.y, u.z, u.w};
+        uint32_t ow[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float2 z = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&zw[q]));
+            const float g0 = d * w[2 * q] * silu_grad_of(z.x), g1 = d * w[2 * q + 1] * silu_grad_of(z.y);
+            aw[2 * q] = fmaf(d, silu_of(z.x), aw[2 * q]);
+            aw[2 * q + 1] = fmaf(d, silu_of(z.y), aw[2 * q + 1]);
+            ab[2 * q] += g0;
+            ab[2 * q + 1] += g1;
+            const __nv_bfloat162 p = __floats2bfloat162_rn(g0, g1);
+            ow[q] = *reinterpret_cast<const uint32_t*>(&p);
+        }
+        const uint4 o = make_uint4(ow[0], ow[1], ow[2], ow[3]);
+        *reinterpret_cast<uint4*>(dz3 + m * H + c) = o;
+        *reinterpret_cast<uint4*>(&tile[r][c]) = o;
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        atomicAdd(&sw[c + k], aw[k]);
+        atomicAdd(&sb[c + k], ab[k]);
+    }
+    __syncthreads();
+    if (t < H) {
+        __nv_bfloat16* dst = dz3T + (uint64_t)t * M + m0;
+#pragma unroll
+        for (uint32_t r8 = 0; r8 < kHeadRows; r8 += 8) {
+            __align__(16) __nv_bfloat16 col[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) col[k] = tile[r8 + k][t];
+            *reinterpret_cast<uint4*>(dst + r8) = *reinterpret_cast<const uint4*>(col);
+        }
+        atomicAdd(&dw4[t], sw[t]);
+        atomicAdd(&db3[t], sb[t]);
+    }
 }
 
 __global__ void adam_kernel(AdamArgs a)
@@ -239,8 +275,8 @@ int launch_softmax_loss(const float* y, const float* p, uint32_t records, uint32
 int launch_head_backward(const __nv_bfloat16* z3, const float* dy, const float* w4, uint32_t M, uint32_t H,
                          __nv_bfloat16* dz3, __nv_bfloat16* dz3T, float* dw4, float* db3, cudaStream_t st)
 {
-    if (M % kHeadRows || H > 1024 || H % 32) return -1;
-    head_backward_kernel<<<M / kHeadRows, H, 0, st>>>(z3, dy, w4, M, H, dz3, dz3T, dw4, db3);
+    if (M % kHeadRows || H > 256 || H % 64) return -1;
+    head_backward_kernel<<<M / kHeadRows, 256, 0, st>>>(z3, dy, w4, M, H, dz3, dz3T, dw4, db3);
     return (int)cudaGetLastError();
 }
 
