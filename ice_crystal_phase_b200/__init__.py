@@ -170,7 +170,7 @@ class BatchSettings(C.Structure):
 class SurrogateConfig(C.Structure):
     _fields_ = [("nt", C.c_uint32), ("np", C.c_uint32), ("hidden", C.c_uint32), ("input_width", C.c_uint32),
                 ("theta_frequencies", C.c_uint32), ("phi_frequencies", C.c_uint32), ("max_records", C.c_uint32),
-                ("reserved", C.c_uint32), ("log_radius_mm", C.c_double * 2), ("wavelength_nm", C.c_double * 2),
+                ("axis_harmonics", C.c_uint32), ("log_radius_mm", C.c_double * 2), ("wavelength_nm", C.c_double * 2),
                 ("log_wavelength_over_radius", C.c_double * 2), ("index_center", C.c_double),
                 ("index_scale", C.c_double), ("coefficient_scale", C.c_double * 8)]
 
@@ -202,6 +202,8 @@ _FUNCS = {
                                     C.POINTER(Tuning)]),
     "icp_phase_cdf_build": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_uint32,
                                       C.c_uint32, C.POINTER(CdfPolicy), _P, _P, C.POINTER(CdfReport)]),
+    "icp_phase_cdf_build_batch": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                            C.POINTER(CdfPolicy), _P, _P, C.POINTER(CdfReport)]),
     "icp_hex_generate": (C.c_int, [_P, C.POINTER(HexRecordArgs), C.POINTER(Orientation), C.c_uint32, _D, _D, _D,
                                    C.POINTER(RecordReport)]),
     "icp_phase_cdf_build_static": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_double, C.c_double,
@@ -227,6 +229,7 @@ _FUNCS = {
     "icp_surrogate_parameter_count": (C.c_uint64, [C.POINTER(SurrogateConfig)]),
     "icp_surrogate_record_features": (C.c_int, [C.POINTER(SurrogateConfig), C.POINTER(DropItem), C.c_uint32, _P]),
     "icp_surrogate_cell_features": (C.c_int, [C.POINTER(SurrogateConfig), _P]),
+    "icp_surrogate_inputs": (C.c_int, [_P, C.POINTER(DropItem), C.c_uint32, _P]),
     "icp_surrogate_create": (C.c_int, [_P, C.POINTER(SurrogateConfig), C.POINTER(_P)]),
     "icp_surrogate_destroy": (None, [_P]),
     "icp_surrogate_set_parameters": (C.c_int, [_P, _P, C.c_uint64]),
@@ -955,6 +958,12 @@ class Surrogate:
         check(LIB.icp_surrogate_train_step(self.handle, _items(specs), len(specs), C.c_void_p(target_ptr),
                                            C.byref(opt), C.byref(loss)))
         return loss.value
+
+    def inputs(self, specs) -> np.ndarray:
+        """The device's input rows for these records: uint16 BF16 bits [len(specs) * cells, width]."""
+        out = np.zeros((len(specs) * self.cells, self.cfg.input_width), dtype=np.uint16)
+        check(LIB.icp_surrogate_inputs(self.handle, _items(specs), len(specs), C.c_void_p(out.ctypes.data)))
+        return out
 
     def predict(self, specs, logits_ptr: int) -> None:
         check(LIB.icp_surrogate_predict(self.handle, _items(specs), len(specs), C.c_void_p(logits_ptr)))

@@ -438,6 +438,65 @@ int icp::cdf_enqueue(icp_context* c, const double* d_values, uint32_t nt, uint32
     return cdf_launch_common(c, L, ct, cp);
 }
 
+int icp::cdf_enqueue_batch(icp_context* c, const CdfBatchInput* in, uint32_t count, uint32_t nt, uint32_t np,
+                           uint32_t ct, uint32_t cp, const double* d_edges, CdfDeviceReport* d_reports, unsigned* d_sync)
+{
+    if (!count) return ICP_OK;
+    const uint32_t cw = std::max(1u, (cp + 15u) / 16u);
+    const uint32_t strips = (cp + cw - 1) / cw;
+    const size_t smem = cdf_smem_bytes(ct, cp, cw);
+    const int cap = smem <= 200 * 1024 ? cdf_max_coresident_blocks(smem, c->device) : 0;
+    const uint32_t per = (uint32_t)std::max(0, cap) / strips;
+    if (!per) {
+        // a record's strips alone do not fit: one launch per record, with its own strip width
+        for (uint32_t r = 0; r < count; ++r)
+            if (const int e = cdf_enqueue(c, in[r].values, nt, np, ct, cp, d_edges, in[r].fwd_add, in[r].bwd_add,
+                                          in[r].pole_fx, in[r].pole_weight, in[r].row_add, in[r].phi, in[r].theta,
+                                          d_reports + r, d_sync + 2 * r))
+                return e;
+        return ICP_OK;
+    }
+    const size_t pb = cdf_partial_bytes() * strips;
+    ICP_CUDA(c->cdfb_partial.ensure(pb * count));
+    ICP_CUDA(c->cdfb_colsum.ensure(sizeof(double) * cp * count));
+    ICP_CUDA(c->cdfb_recs.ensure(sizeof(CdfBatchRecord) * count));
+    ICP_CUDA(cudaMemsetAsync(d_sync, 0, 2 * sizeof(unsigned) * count, c->stream));
+    ICP_CUDA(cudaMemsetAsync(d_reports, 0, sizeof(CdfDeviceReport) * count, c->stream));
+    std::vector<CdfBatchRecord> recs(count);
+    for (uint32_t r = 0; r < count; ++r) {
+        CdfBatchRecord& b = recs[r];
+        b.values = in[r].values;
+        b.phi = in[r].phi;
+        b.theta = in[r].theta;
+        b.colsum = (double*)c->cdfb_colsum.ptr + (size_t)cp * r;
+        b.partial = (unsigned char*)c->cdfb_partial.ptr + pb * r;
+        b.report = d_reports + r;
+        b.sync = d_sync + 2 * r;
+        b.row_add = in[r].row_add;
+        b.pole_fx = in[r].pole_fx;
+        b.pole_weight = in[r].pole_weight;
+        b.fwd_add = in[r].fwd_add;
+        b.bwd_add = in[r].bwd_add;
+    }
+    ICP_CUDA(cudaMemcpyAsync(c->cdfb_recs.ptr, recs.data(), sizeof(CdfBatchRecord) * count, cudaMemcpyHostToDevice,
+                             c->stream));
+    CdfLaunch L{};
+    L.edges = d_edges;
+    L.kind = 0;
+    L.nt = nt;
+    L.np = np;
+    L.ct = ct;
+    L.cp = cp;
+    L.cw = cw;
+    for (uint32_t r0 = 0; r0 < count; r0 += per) {
+        const uint32_t n = std::min(per, count - r0);
+        const int e = launch_cdf_build_batch(L, (const CdfBatchRecord*)c->cdfb_recs.ptr + r0, n, c->stream);
+        ++g_launches;
+        if (e) return fail(ICP_ERR_DEVICE, "batched CDF launch failed: %s", cudaGetErrorString((cudaError_t)e));
+    }
+    return ICP_OK;
+}
+
 int icp::choose_cdf_width(icp_context* c, uint32_t ct, uint32_t cp, uint32_t& cw)
 {
     // smallest strip width whose grid fits co-resident, at least ceil(cp / SMs)
@@ -495,6 +554,54 @@ extern "C" int icp_phase_cdf_build(icp_context* c, const double* d_values, uint3
     ICP_CUDA(cudaMemcpyAsync(&r, c->cdf_report.ptr, sizeof r, cudaMemcpyDeviceToHost, c->stream));
     ICP_CUDA(cudaStreamSynchronize(c->stream));
     return icp::cdf_finish(r, p, report);
+}
+
+extern "C" int icp_phase_cdf_build_batch(icp_context* c, const double* d_values, uint32_t count, uint32_t nt,
+                                         uint32_t np, uint32_t ct, uint32_t cp, const icp_cdf_policy* policy,
+                                         double* d_phi, double* d_theta, icp_cdf_report* reports)
+{
+    if (!c || !d_values || !d_phi || !d_theta || !reports || !policy)
+        return fail(ICP_ERR_INVALID_ARGUMENT, "icp_phase_cdf_build_batch: null argument");
+    if (!count) return fail(ICP_ERR_INVALID_ARGUMENT, "icp_phase_cdf_build_batch: no records");
+    const icp_cdf_policy& p = *policy;
+    if (!(H::finite(p.max_l1_error) && p.max_l1_error >= 0 && p.max_l1_error <= 2 && H::finite(p.max_lost_mass) &&
+          p.max_lost_mass >= 0 && p.max_lost_mass <= 1 && H::finite(p.max_coarsening_tv) && p.max_coarsening_tv >= 0 &&
+          p.max_coarsening_tv <= 1))
+        return fail(ICP_ERR_INVALID_ARGUMENT, "Invalid CDF quality policy.");
+    if (!nt || !np || (uint64_t)nt * np > 0xffffffffull)
+        return fail(ICP_ERR_INVALID_ARGUMENT, "Unsupported phase grid dimensions.");
+    if (!ct || !cp || ct > nt || cp > np || nt % ct || np % cp)
+        return fail(ICP_ERR_INVALID_ARGUMENT, "Storage dimensions must divide histogram dimensions.");
+    ICP_CUDA(cudaSetDevice(c->device));
+    std::vector<double> edges;
+    if (!H::u_edges(nt, edges)) return fail(ICP_ERR_INVALID_ARGUMENT, "Angular cells cannot be represented in binary64.");
+    ICP_CUDA(c->rec_edges.ensure(sizeof(double) * (nt + 1)));
+    ICP_CUDA(c->b_reports.ensure(sizeof(CdfDeviceReport) * count));
+    ICP_CUDA(c->b_sync.ensure(2 * sizeof(unsigned) * count));
+    ICP_CUDA(cudaMemcpyAsync(c->rec_edges.ptr, edges.data(), sizeof(double) * (nt + 1), cudaMemcpyHostToDevice, c->stream));
+    std::vector<CdfBatchInput> in(count);
+    for (uint32_t r = 0; r < count; ++r) {
+        in[r] = CdfBatchInput{};
+        in[r].values = d_values + (size_t)nt * np * r;
+        in[r].phi = d_phi + (size_t)(cp + 1) * r;
+        in[r].theta = d_theta + (size_t)cp * (ct + 1) * r;
+    }
+    if (const int e = cdf_enqueue_batch(c, in.data(), count, nt, np, ct, cp, (const double*)c->rec_edges.ptr,
+                                        (CdfDeviceReport*)c->b_reports.ptr, (unsigned*)c->b_sync.ptr))
+        return e;
+    std::vector<CdfDeviceReport> dev(count);
+    ICP_CUDA(cudaMemcpyAsync(dev.data(), c->b_reports.ptr, sizeof(CdfDeviceReport) * count, cudaMemcpyDeviceToHost,
+                             c->stream));
+    ICP_CUDA(cudaStreamSynchronize(c->stream));
+    int first = ICP_OK;
+    for (uint32_t r = 0; r < count; ++r) {
+        std::memset(&reports[r], 0, sizeof reports[r]);
+        const int e = icp::cdf_finish(dev[r], p, &reports[r]);
+        reports[r].status = (uint32_t)e;
+        if (e && !first) first = e;
+    }
+    if (first) return first;
+    return ok();
 }
 
 int icp::cdf_finish(const CdfDeviceReport& r, const icp_cdf_policy& p, icp_cdf_report* report)

@@ -89,7 +89,8 @@ bool config_valid(const icp_surrogate_config* g)
     if (!g || !g->nt || !g->np || ((uint64_t)g->nt * g->np) % 256u || (uint64_t)g->nt * g->np > (1u << 24)) return false;
     if (g->hidden != 128 && g->hidden != 256) return false;
     if (g->input_width != 64 && g->input_width != 128) return false;
-    if (4u + 2u * g->theta_frequencies + g->phi_frequencies > g->input_width - 16u) return false;
+    if (g->axis_harmonics % 8u) return false;
+    if (4u + 2u * g->theta_frequencies + g->phi_frequencies + g->axis_harmonics > g->input_width - 16u) return false;
     if (!g->max_records || g->max_records > 256) return false;
     const double* r[3] = {g->log_radius_mm, g->wavelength_nm, g->log_wavelength_over_radius};
     for (auto* x : r)
@@ -132,14 +133,15 @@ struct icp_surrogate {
     uint32_t o_w1 = 0, o_b1 = 0, o_w2 = 0, o_b2 = 0, o_w3 = 0, o_b3 = 0, o_w4 = 0, o_hb = 0;
     Scratch params, grads, adam_m, adam_v, wbf, cells, edges, rec16, loss;
     Scratch X, XT, z1, h1, h1T, z2, h2, h2T, z3, y, dy, dz3, dz3T, dz2, dz2T, dz1T, mass, reports, sync;
-    Scratch mass_sum, dfrac, drows;
+    Scratch mass_sum, dfrac, drows, cellgeo, recgeo;
     std::vector<double> h_edges;
     std::vector<uint16_t> h_rec;
+    std::vector<double> h_recgeo;
     ~icp_surrogate()
     {
         Scratch* all[] = {&params, &grads, &adam_m, &adam_v, &wbf, &cells, &edges, &rec16, &loss, &X, &XT, &z1, &h1,
                           &h1T, &z2, &h2, &h2T, &z3, &y, &dy, &dz3, &dz3T, &dz2, &dz2T, &dz1T, &mass, &reports, &sync,
-                          &mass_sum, &dfrac, &drows};
+                          &mass_sum, &dfrac, &drows, &cellgeo, &recgeo};
         for (Scratch* s : all) s->release();
     }
     float* P(uint32_t o) const { return (float*)params.ptr + o; }
@@ -169,13 +171,22 @@ int enqueue_features(icp_surrogate* s, const icp_drop_item* items, uint32_t coun
 {
     icp_context* c = s->c;
     s->h_rec.resize((size_t)16 * count);
-    for (uint32_t i = 0; i < count; ++i) record_row(s->cfg, items[i], s->h_rec.data() + 16 * i);
+    s->h_recgeo.resize((size_t)2 * count);
+    for (uint32_t i = 0; i < count; ++i) {
+        record_row(s->cfg, items[i], s->h_rec.data() + 16 * i);
+        const double deg = items[i].inclination_deg * (H::kPi / 180.0);
+        s->h_recgeo[2 * i] = std::sin(deg);
+        s->h_recgeo[2 * i + 1] = std::cos(deg);
+    }
     const uint64_t M = (uint64_t)count * s->C;
     ICP_CUDA(s->rec16.ensure(32u * s->R));
+    ICP_CUDA(s->recgeo.ensure(16u * s->R));
     ICP_CUDA(s->X.ensure(2 * M * s->K0));
     if (training) ICP_CUDA(s->XT.ensure(2 * M * s->K0));
     ICP_CUDA(cudaMemcpyAsync(s->rec16.ptr, s->h_rec.data(), 32u * count, cudaMemcpyHostToDevice, c->stream));
+    ICP_CUDA(cudaMemcpyAsync(s->recgeo.ptr, s->h_recgeo.data(), 16u * count, cudaMemcpyHostToDevice, c->stream));
     const int e = mlp::launch_features(as<__nv_bfloat16>(s->rec16), as<__nv_bfloat16>(s->cells), count, s->C, s->K0,
+                                       s->cfg.axis_harmonics, as<double>(s->recgeo), as<double>(s->cellgeo),
                                        as<__nv_bfloat16>(s->X), training ? as<__nv_bfloat16>(s->XT) : nullptr,
                                        c->stream);
     count_launch();
@@ -382,8 +393,9 @@ int icp_surrogate_default_config(icp_surrogate_config* g)
     g->np = 512;
     g->hidden = 256;
     g->input_width = 128;
-    g->theta_frequencies = 48;
+    g->theta_frequencies = 40;
     g->phi_frequencies = 12;
+    g->axis_harmonics = 16;
     g->max_records = 16;
     g->log_radius_mm[0] = std::log(0.1);
     g->log_radius_mm[1] = std::log(3.0);
@@ -492,6 +504,17 @@ int icp_surrogate_create(icp_context* c, const icp_surrogate_config* g, icp_surr
     if (e == cudaSuccess) e = cudaMemcpy(s->cells.ptr, both.data(), 2 * both.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(s->edges.ptr, edges.data(), sizeof(double) * edges.size(), cudaMemcpyHostToDevice);
     s->h_edges = edges;
+    // cell geometry of the axis harmonics: cos(theta) and sin(theta) sin(phi), phi the column's
+    // azimuth in [-pi, pi)
+    std::vector<double> geo(2 * (size_t)s->C);
+    for (uint32_t i = 0; i < g->nt; ++i)
+        for (uint32_t j = 0; j < g->np; ++j) {
+            const double th = H::kPi * (i + 0.5) / g->nt, ph = -H::kPi + 2.0 * H::kPi * (j + 0.5) / g->np;
+            geo[2 * ((size_t)i * g->np + j)] = std::cos(th);
+            geo[2 * ((size_t)i * g->np + j) + 1] = std::sin(th) * std::sin(ph);
+        }
+    if (e == cudaSuccess) e = s->cellgeo.ensure(sizeof(double) * geo.size());
+    if (e == cudaSuccess) e = cudaMemcpy(s->cellgeo.ptr, geo.data(), sizeof(double) * geo.size(), cudaMemcpyHostToDevice);
     for (Scratch* x : p4)
         if (e == cudaSuccess) e = cudaMemset(x->ptr, 0, np4);
     if (e == cudaSuccess) e = cudaMemset(s->wbf.ptr, 0, s->wbf.bytes);
@@ -640,11 +663,16 @@ int icp_surrogate_generate(icp_surrogate* s, const icp_drop_item* items, uint32_
         count_launch();
         if (e) return fail(ICP_ERR_DEVICE, "row launch failed (%d)", e);
     }
-    for (uint32_t r = 0; r < count; ++r)
-        ICP_TRY(cdf_enqueue(c, as<double>(s->mass) + (uint64_t)r * s->C, g.nt, g.np, ct, cp, as<double>(s->edges), 0.0,
-                            0.0, nullptr, 0.0, items[r].diffraction ? as<double>(s->drows) + (size_t)r * g.nt : nullptr,
-                            d_phi + (size_t)(cp + 1) * r, d_theta + (size_t)cp * (ct + 1) * r,
-                            as<CdfDeviceReport>(s->reports) + r, as<unsigned>(s->sync) + 2 * r));
+    std::vector<CdfBatchInput> in(count);
+    for (uint32_t r = 0; r < count; ++r) {
+        in[r] = CdfBatchInput{};
+        in[r].values = as<double>(s->mass) + (uint64_t)r * s->C;
+        in[r].phi = d_phi + (size_t)(cp + 1) * r;
+        in[r].theta = d_theta + (size_t)cp * (ct + 1) * r;
+        in[r].row_add = items[r].diffraction ? as<double>(s->drows) + (size_t)r * g.nt : nullptr;
+    }
+    ICP_TRY(cdf_enqueue_batch(c, in.data(), count, g.nt, g.np, ct, cp, as<double>(s->edges),
+                              as<CdfDeviceReport>(s->reports), as<unsigned>(s->sync)));
     std::vector<CdfDeviceReport> dev(count);
     ICP_CUDA(cudaMemcpyAsync(dev.data(), s->reports.ptr, sizeof(CdfDeviceReport) * count, cudaMemcpyDeviceToHost,
                              c->stream));
@@ -658,6 +686,16 @@ int icp_surrogate_generate(icp_surrogate* s, const icp_drop_item* items, uint32_
     }
     if (first) return first;
     return ok();
+}
+
+int icp_surrogate_inputs(icp_surrogate* s, const icp_drop_item* items, uint32_t count, uint16_t* h_out)
+{
+    ICP_TRY(check_call(s, items, count));
+    if (!h_out) return fail(ICP_ERR_INVALID_ARGUMENT, "surrogate: null output");
+    ICP_TRY(begin(s));
+    ICP_TRY(enqueue_features(s, items, count, false));
+    ICP_CUDA(cudaMemcpyAsync(h_out, s->X.ptr, 2 * (size_t)count * s->C * s->K0, cudaMemcpyDeviceToHost, s->c->stream));
+    return finish(s->c, "icp_surrogate_inputs");
 }
 
 int icp_surrogate_targets(icp_surrogate* s, const double* d_phi, const double* d_theta, uint32_t count, float* d_target)

@@ -44,6 +44,8 @@ struct BlockPartial {
 };
 
 struct CdfParams {
+    const CdfBatchRecord* recs; // batched: block b builds strip b % strips of record b / strips
+    uint32_t strips;           // strips per record (0: one record, strips = gridDim.x)
     const double* values;
     const double* edges; // fine edges, nt+1
     double* phi;
@@ -147,7 +149,7 @@ __device__ __forceinline__ double block_max(double x, double* red)
     return s;
 }
 
-__global__ void __launch_bounds__(kThreads) cdf_build_kernel(const CdfParams P)
+__global__ void __launch_bounds__(kThreads) cdf_build_kernel(const CdfParams P0)
 {
     extern __shared__ __align__(16) double strip[]; // ct x CW coarse strip, then phi strip (CW+1)
     __shared__ double red_d[kThreads / 32];
@@ -155,7 +157,25 @@ __global__ void __launch_bounds__(kThreads) cdf_build_kernel(const CdfParams P)
     __shared__ double s_glob[6];
     __shared__ int s_last;
 
-    const uint32_t c0 = blockIdx.x * P.cw;
+    const uint32_t strips = P0.strips ? P0.strips : gridDim.x;
+    const uint32_t sb = P0.strips ? blockIdx.x % strips : blockIdx.x; // this block's strip of its record
+    CdfParams P = P0;
+    if (P0.recs) {
+        const CdfBatchRecord& R = P0.recs[blockIdx.x / strips];
+        P.values = R.values;
+        P.phi = R.phi;
+        P.theta = R.theta;
+        P.colsum = R.colsum;
+        P.partial = reinterpret_cast<BlockPartial*>(R.partial);
+        P.report = R.report;
+        P.sync = R.sync;
+        P.row_add = R.row_add;
+        P.pole_fx = R.pole_fx;
+        P.pole_weight = R.pole_weight;
+        P.fwd_add = R.fwd_add;
+        P.bwd_add = R.bwd_add;
+    }
+    const uint32_t c0 = sb * P.cw;
     const uint32_t c1 = min(P.cp, c0 + P.cw);
     const uint32_t w = c1 > c0 ? c1 - c0 : 0u; // columns in this strip
     const uint32_t CW = P.cw;
@@ -196,7 +216,7 @@ __global__ void __launch_bounds__(kThreads) cdf_build_kernel(const CdfParams P)
         const double e = block_max(largest, red_d);
         const unsigned long long f = block_sum(invalid, red_u);
         if (threadIdx.x == 0) {
-            BlockPartial& bp = P.partial[blockIdx.x];
+            BlockPartial& bp = P.partial[sb];
             bp.fine_mass = a;
             bp.fine_axial = b;
             bp.stored_mass = c;
@@ -205,13 +225,13 @@ __global__ void __launch_bounds__(kThreads) cdf_build_kernel(const CdfParams P)
             bp.invalid = f;
         }
     }
-    if (!grid_wait(&P.sync[0], gridDim.x, &P.report->timeout)) return;
+    if (!grid_wait(&P.sync[0], strips, &P.report->timeout)) return;
 
     // ------------------------------------------------------------ phase B
     // block partials staged through shared memory (L2 loads in parallel), then summed in
     // block order by one thread so that every block derives identical totals
-    double* stage = sphi + CW + 1; // scratch: max(14 * gridDim.x, cp) doubles
-    for (unsigned k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
+    double* stage = sphi + CW + 1; // scratch: max(14 * strips, cp) doubles
+    for (unsigned k = threadIdx.x; k < strips; k += blockDim.x) {
         const BlockPartial* bp = P.partial + k;
         stage[5 * k + 0] = __ldcg(&bp->fine_mass);
         stage[5 * k + 1] = __ldcg(&bp->fine_axial);
@@ -222,7 +242,7 @@ __global__ void __launch_bounds__(kThreads) cdf_build_kernel(const CdfParams P)
     __syncthreads();
     if (threadIdx.x == 0) {
         double a = 0, b = 0, c = 0, d = 0, e = 0;
-        for (unsigned k = 0; k < gridDim.x; ++k) {
+        for (unsigned k = 0; k < strips; ++k) {
             a += stage[5 * k + 0];
             b += stage[5 * k + 1];
             c += stage[5 * k + 2];
@@ -275,11 +295,11 @@ __global__ void __launch_bounds__(kThreads) cdf_build_kernel(const CdfParams P)
         const double t = block_sum(tv.v + tv.c, red_d);
         const unsigned long long u = block_sum(underflow, red_u);
         if (threadIdx.x == 0) {
-            P.partial[blockIdx.x].tv = 0.5 * t;
-            P.partial[blockIdx.x].underflow = u;
+            P.partial[sb].tv = 0.5 * t;
+            P.partial[sb].underflow = u;
         }
     }
-    if (!grid_wait(&P.sync[0], 2u * gridDim.x, &P.report->timeout)) return;
+    if (!grid_wait(&P.sync[0], 2u * strips, &P.report->timeout)) return;
 
     // ------------------------------------------------------------ phase C
     for (uint32_t j = threadIdx.x; j < P.cp; j += blockDim.x) stage[j] = __ldcg(P.colsum + j);
@@ -364,7 +384,7 @@ __global__ void __launch_bounds__(kThreads) cdf_build_kernel(const CdfParams P)
         const unsigned long long f = block_sum(lost_cells, red_u);
         const unsigned long long g = block_sum(malformed, red_u);
         if (threadIdx.x == 0) {
-            BlockPartial& bp = P.partial[blockIdx.x];
+            BlockPartial& bp = P.partial[sb];
             bp.l1 = a;
             bp.lost = b;
             bp.recovered = c;
@@ -373,7 +393,7 @@ __global__ void __launch_bounds__(kThreads) cdf_build_kernel(const CdfParams P)
             bp.lost_cells = f;
             bp.malformed = g;
             __threadfence();
-            s_last = (atomicAdd(&P.sync[1], 1u) == gridDim.x - 1);
+            s_last = (atomicAdd(&P.sync[1], 1u) == strips - 1);
         }
     }
     __syncthreads();
@@ -381,7 +401,7 @@ __global__ void __launch_bounds__(kThreads) cdf_build_kernel(const CdfParams P)
     __threadfence();
     // last block: stage every block's audit partials (parallel L2 loads), sum in block order
     constexpr unsigned kF = 14;
-    for (unsigned k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
+    for (unsigned k = threadIdx.x; k < strips; k += blockDim.x) {
         const BlockPartial* bp = P.partial + k;
         double* o = stage + (size_t)kF * k;
         o[0] = __ldcg(&bp->fine_mass);
@@ -402,7 +422,7 @@ __global__ void __launch_bounds__(kThreads) cdf_build_kernel(const CdfParams P)
     __syncthreads();
     if (threadIdx.x != 0) return;
     CdfDeviceReport r{};
-    for (unsigned k = 0; k < gridDim.x; ++k) {
+    for (unsigned k = 0; k < strips; ++k) {
         const double* o = stage + (size_t)kF * k;
         r.fine_mass += o[0];
         r.fine_axial += o[1];
@@ -428,7 +448,7 @@ __global__ void __launch_bounds__(kThreads) cdf_build_kernel(const CdfParams P)
 // Fine-grid mass with pole caps for an FP64 histogram (used by the report path).
 int launch_cdf_build(const CdfLaunch& L, cudaStream_t stream)
 {
-    CdfParams P;
+    CdfParams P{};
     P.values = L.values;
     P.edges = L.edges;
     P.phi = L.phi;
@@ -464,6 +484,29 @@ size_t cdf_smem_bytes(uint32_t ct, uint32_t cp, uint32_t cw)
     const size_t blocks = (cp + cw - 1) / cw;
     const size_t stage = blocks * 14 > cp ? blocks * 14 : cp;
     return sizeof(double) * ((size_t)ct * cw + cw + 1 + stage);
+}
+
+int launch_cdf_build_batch(const CdfLaunch& L, const CdfBatchRecord* d_recs, uint32_t count, cudaStream_t stream)
+{
+    CdfParams P{};
+    P.recs = d_recs;
+    P.edges = L.edges;
+    P.kind = L.kind;
+    P.nt = L.nt;
+    P.np = L.np;
+    P.ct = L.ct;
+    P.cp = L.cp;
+    P.dt = L.nt / L.ct;
+    P.dp = L.np / L.cp;
+    P.cw = L.cw;
+    P.strips = (L.cp + L.cw - 1) / L.cw;
+    const size_t smem = cdf_smem_bytes(L.ct, L.cp, L.cw);
+    cudaError_t e = cudaFuncSetAttribute(cdf_build_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return (int)e;
+    void* args[] = {&P};
+    e = cudaLaunchCooperativeKernel((const void*)cdf_build_kernel, dim3(P.strips * count), dim3(kThreads), args, smem,
+                                    stream);
+    return (int)e;
 }
 
 int cdf_max_coresident_blocks(size_t smem, int device)

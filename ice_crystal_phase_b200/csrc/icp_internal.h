@@ -34,6 +34,23 @@ struct CdfLaunch {
 };
 
 int launch_cdf_build(const CdfLaunch& L, cudaStream_t stream);
+// One record of a batched CDF build (device array of these; scratch per record: `strips`
+// partials, cp column sums, two zeroed barrier counters, a zeroed report).
+struct CdfBatchRecord {
+    const double* values;
+    double* phi;
+    double* theta;
+    double* colsum;
+    void* partial;
+    CdfDeviceReport* report;
+    unsigned* sync;
+    const double* row_add;
+    const unsigned long long* pole_fx;
+    double pole_weight, fwd_add, bwd_add;
+};
+// Builds `count` records of one grid shape (L: edges, kind, nt, np, ct, cp, cw; its per-record
+// fields unused) in one cooperative launch of count x ceil(cp / cw) blocks.
+int launch_cdf_build_batch(const CdfLaunch& L, const CdfBatchRecord* d_recs, uint32_t count, cudaStream_t stream);
 int cdf_max_coresident_blocks(size_t smem, int device);
 size_t cdf_smem_bytes(uint32_t ct, uint32_t cp, uint32_t cw);
 size_t cdf_partial_bytes();
@@ -150,6 +167,22 @@ int cdf_enqueue(icp_context* c, const double* d_values, uint32_t nt, uint32_t np
                 double pole_weight, const double* row_add, double* d_phi, double* d_theta, CdfDeviceReport* d_report,
                 unsigned* d_sync);
 
+// Inputs of one record of a batched CDF build (see cdf_enqueue).
+struct CdfBatchInput {
+    const double* values;
+    double* phi;
+    double* theta;
+    const double* row_add;
+    const unsigned long long* pole_fx;
+    double pole_weight, fwd_add, bwd_add;
+};
+// Enqueues the CDF builds of `count` records of one grid shape as few cooperative launches
+// (16 strips per record, as many records per launch as stay co-resident; the records' a / T
+// equal those of one cdf_enqueue per record); d_reports[count] and d_sync[2 count] are zeroed
+// here.  Not for use inside a stream capture (the record table is copied from pageable memory).
+int cdf_enqueue_batch(icp_context* c, const CdfBatchInput* in, uint32_t count, uint32_t nt, uint32_t np, uint32_t ct,
+                      uint32_t cp, const double* d_edges, CdfDeviceReport* d_reports, unsigned* d_sync);
+
 // Analytic diffraction rows of one record on the device (icp_drop_device.cu).
 struct DiffractionArgs {
     const double* edges;              // nt + 1 fine u edges
@@ -229,5 +262,7 @@ struct icp_context {
     icp::BatchState batch;
     // surrogate
     icp::Scratch mlp_error;
+    // batched CDF builds
+    icp::Scratch cdfb_partial, cdfb_colsum, cdfb_recs;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
 };

@@ -20,21 +20,54 @@ __device__ __forceinline__ float silu_grad_of(float z)
     return s * (1.0f + z * (1.0f - s));
 }
 
+// cos psi of one (record, cell) and the Chebyshev values T_k(cos psi), k = k0 .. k0+7, rounded
+// to FP32 then BF16.  Uncontracted FP64 arithmetic (the host restatement repeats it exactly).
+__device__ __forceinline__ double cos_psi(const double* recgeo, const double* cellgeo, uint32_t r, uint32_t c)
+{
+    return __dsub_rn(-__dmul_rn(recgeo[2 * r], cellgeo[2 * c]), __dmul_rn(recgeo[2 * r + 1], cellgeo[2 * c + 1]));
+}
+__device__ __forceinline__ void axis_harmonics8(double x, uint32_t k0, __nv_bfloat16 (&out)[8])
+{
+    double tm = 1.0, t = x; // T_0, T_1
+    for (uint32_t k = 1; k < k0; ++k) {
+        const double tn = __dsub_rn(__dmul_rn(__dmul_rn(2.0, x), t), tm);
+        tm = t;
+        t = tn;
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        out[i] = __float2bfloat16_rn(__double2float_rn(t));
+        const double tn = __dsub_rn(__dmul_rn(__dmul_rn(2.0, x), t), tm);
+        tm = t;
+        t = tn;
+    }
+}
+
 // X rows: thread per 8 BF16 (one uint4) of a row.
 __global__ void features_kernel(const uint4* __restrict__ rec16, const uint4* __restrict__ cells, uint32_t C,
-                                uint32_t q_row, uint64_t total, uint4* __restrict__ X)
+                                uint32_t q_row, uint32_t q_axis, uint64_t total, const double* __restrict__ recgeo,
+                                const double* __restrict__ cellgeo, uint4* __restrict__ X)
 {
     const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= total) return;
     const uint64_t m = t / q_row;
     const uint32_t q = (uint32_t)(t - m * q_row);
     const uint32_t r = (uint32_t)(m / C), c = (uint32_t)(m - (uint64_t)r * C);
-    X[t] = q < 2 ? rec16[2u * r + q] : cells[(uint64_t)c * (q_row - 2) + (q - 2)];
+    if (q < 2) {
+        X[t] = rec16[2u * r + q];
+    } else if (q < q_axis) {
+        X[t] = cells[(uint64_t)c * (q_row - 2) + (q - 2)];
+    } else {
+        __align__(16) __nv_bfloat16 h[8];
+        axis_harmonics8(cos_psi(recgeo, cellgeo, r, c), 1u + 8u * (q - q_axis), h);
+        X[t] = *reinterpret_cast<const uint4*>(h);
+    }
 }
 
 // XT[k][m]: thread per 8 consecutive rows m of one column k.
 __global__ void features_t_kernel(const __nv_bfloat16* __restrict__ rec16, const uint4* __restrict__ cellsT, uint32_t C,
-                                  uint32_t K0, uint32_t records, __nv_bfloat16* __restrict__ XT)
+                                  uint32_t K0, uint32_t P, uint32_t records, const double* __restrict__ recgeo,
+                                  const double* __restrict__ cellgeo, __nv_bfloat16* __restrict__ XT)
 {
     const uint64_t per_k = (uint64_t)records * C / 8u;
     const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -48,8 +81,23 @@ __global__ void features_t_kernel(const __nv_bfloat16* __restrict__ rec16, const
         const __nv_bfloat16 x = rec16[16u * r + k];
         const uint32_t w = (uint32_t)__bfloat16_as_ushort(x) * 0x10001u;
         v = make_uint4(w, w, w, w);
-    } else {
+    } else if (k < K0 - P) {
         v = cellsT[((uint64_t)(k - 16) * C + c) / 8u];
+    } else {
+        // harmonic j of 8 consecutive cells of one record (C is a multiple of 8)
+        const uint32_t j = k - (K0 - P) + 1u;
+        __align__(16) __nv_bfloat16 h[8];
+        for (int i = 0; i < 8; ++i) {
+            const double x = cos_psi(recgeo, cellgeo, r, c + (uint32_t)i);
+            double tm = 1.0, tt = x;
+            for (uint32_t n = 1; n < j; ++n) {
+                const double tn = __dsub_rn(__dmul_rn(__dmul_rn(2.0, x), tt), tm);
+                tm = tt;
+                tt = tn;
+            }
+            h[i] = __float2bfloat16_rn(__double2float_rn(tt));
+        }
+        v = *reinterpret_cast<const uint4*>(h);
     }
     reinterpret_cast<uint4*>(XT + (uint64_t)k * records * C)[m8] = v;
 }
@@ -247,19 +295,21 @@ unsigned blocks_of(uint64_t n, unsigned t) { return (unsigned)((n + t - 1) / t);
 } // namespace
 
 int launch_features(const __nv_bfloat16* rec16, const __nv_bfloat16* cells, uint32_t records, uint32_t C, uint32_t K0,
-                    __nv_bfloat16* X, __nv_bfloat16* XT, cudaStream_t st)
+                    uint32_t P, const double* recgeo, const double* cellgeo, __nv_bfloat16* X, __nv_bfloat16* XT,
+                    cudaStream_t st)
 {
-    if (K0 % 64 || C % 128 || !records) return -1;
+    if (K0 % 64 || C % 128 || !records || P % 8 || P + 16 > K0) return -1;
     const uint32_t q_row = K0 / 8u;
     const uint64_t total = (uint64_t)records * C * q_row;
     features_kernel<<<blocks_of(total, 256), 256, 0, st>>>(reinterpret_cast<const uint4*>(rec16),
-                                                           reinterpret_cast<const uint4*>(cells), C, q_row, total,
+                                                           reinterpret_cast<const uint4*>(cells), C, q_row,
+                                                           q_row - P / 8u, total, recgeo, cellgeo,
                                                            reinterpret_cast<uint4*>(X));
     if (XT) {
         // the column-major cell table follows the row-major one in the same allocation
         const uint4* cellsT = reinterpret_cast<const uint4*>(cells + (uint64_t)C * (K0 - 16));
         const uint64_t n = (uint64_t)records * C / 8u * K0;
-        features_t_kernel<<<blocks_of(n, 256), 256, 0, st>>>(rec16, cellsT, C, K0, records, XT);
+        features_t_kernel<<<blocks_of(n, 256), 256, 0, st>>>(rec16, cellsT, C, K0, P, records, recgeo, cellgeo, XT);
     }
     return (int)cudaGetLastError();
 }

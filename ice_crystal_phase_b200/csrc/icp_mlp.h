@@ -49,9 +49,13 @@ int gemm(const void* A, const void* B, GemmArgs g, int epi, uint32_t splits, cud
 
 // ---------------------------------------------------------------- icp_mlp.cu
 // X[m][k] (BF16, [R*C x K0]) and optionally XT[k][m]: record features in columns [0, 16), the
-// cell table (C x (K0-16), row-major) after them; record r owns rows [r*C, (r+1)*C).
+// cell table (C x (K0-16), row-major) after them; record r owns rows [r*C, (r+1)*C).  The last P
+// columns (P % 8 == 0) are the axis harmonics T_1..T_P(cos psi), cos psi = -(sa ct) - (ca sts)
+// from the record's (sa, ca) = (sin, cos) of its inclination (recgeo[2r..]) and the cell's
+// (ct, sts) = (cos theta, sin theta sin phi) (cellgeo[2c..]), in FP64 without contraction.
 int launch_features(const __nv_bfloat16* rec16, const __nv_bfloat16* cells, uint32_t records, uint32_t C, uint32_t K0,
-                    __nv_bfloat16* X, __nv_bfloat16* XT, cudaStream_t st);
+                    uint32_t P, const double* recgeo, const double* cellgeo, __nv_bfloat16* X, __nv_bfloat16* XT,
+                    cudaStream_t st);
 // Per-record softmax of y against target probabilities p: dy = (softmax(y) - p) * scale and
 // loss[r] = sum_p>0 p (log p - log softmax(y)).
 int launch_softmax_loss(const float* y, const float* p, uint32_t records, uint32_t C, float scale, float* dy,

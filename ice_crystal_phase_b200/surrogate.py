@@ -282,7 +282,9 @@ def save(path, sur: I.Surrogate, extra: dict) -> None:
 
 def load(ctx: I.Context, path, max_records: int | None = None) -> tuple[I.Surrogate, dict]:
     z = np.load(path, allow_pickle=False)
-    fields = {k: v for k, v in json.loads(str(z["config"])).items() if k != "reserved"}
+    fields = json.loads(str(z["config"]))
+    if "reserved" in fields:  # written before the axis harmonics existed: none
+        fields["axis_harmonics"] = fields.pop("reserved")
     if max_records:
         fields["max_records"] = max_records
     sur = I.Surrogate(ctx, I.surrogate_config(**fields))
@@ -353,7 +355,7 @@ def run_training(ctx: I.Context, s: TrainSettings, cfg_over: dict | None = None,
     gate = FallbackGate.of(held, ev["passed"], s.neighbours)
     report = {"settings": asdict(s),
               "config": {k: getattr(cfg, k) for k in ("nt", "np", "hidden", "input_width", "theta_frequencies",
-                                                      "phi_frequencies")},
+                                                      "phi_frequencies", "axis_harmonics")},
               "training_set": {"records": len(train_specs), "rays": rays, "seconds": t_data},
               "training": hist, "heldout_kl_before": loss0, "heldout_kl_after": loss1,
               "train_kl_after": train_loss, "head_bias": hb, "judge_seconds": t_judge, "heldout": ev,
@@ -380,12 +382,14 @@ def main(argv=None) -> int:
     t.add_argument("--np", type=int, default=512)
     t.add_argument("--hidden", type=int, default=256)
     t.add_argument("--input-width", type=int, default=128)
-    t.add_argument("--theta-frequencies", type=int, default=48)
+    t.add_argument("--theta-frequencies", type=int, default=40)
     t.add_argument("--phi-frequencies", type=int, default=12)
+    t.add_argument("--axis-harmonics", type=int, default=16)
     a = p.parse_args(argv)
     s = TrainSettings(**{k: getattr(a, k) for k in TrainSettings.__dataclass_fields__ if hasattr(a, k)})
     over = {"nt": a.nt, "np": a.np, "hidden": a.hidden, "input_width": a.input_width,
-            "theta_frequencies": a.theta_frequencies, "phi_frequencies": a.phi_frequencies, "max_records": s.batch}
+            "theta_frequencies": a.theta_frequencies, "phi_frequencies": a.phi_frequencies,
+            "axis_harmonics": a.axis_harmonics, "max_records": s.batch}
     out = Path(a.out)
     out.mkdir(parents=True, exist_ok=True)
     with I.Context(0) as ctx:

@@ -179,6 +179,13 @@ enum icp_cdf_input { ICP_CDF_MASS = 0, ICP_CDF_DENSITY = 1 };
 int icp_phase_cdf_build(icp_context* ctx, const double* d_values, uint32_t input_kind, uint32_t nt,
                         uint32_t np, double forward_pole, double backward_pole, uint32_t ct, uint32_t cp,
                         const icp_cdf_policy* policy, double* d_phi, double* d_theta, icp_cdf_report* report);
+/* The same for `count` histograms of one shape (mass input, no pole caps) at d_values +
+ * r*nt*np, built in few cooperative launches (no reference counterpart; the reference builds one
+ * record per process): phi / theta of record r at d_phi + r*(cp+1), d_theta + r*cp*(ct+1), equal
+ * to icp_phase_cdf_build's; reports[count] on the host (status = the record's audit). */
+int icp_phase_cdf_build_batch(icp_context* ctx, const double* d_values, uint32_t count, uint32_t nt, uint32_t np,
+                              uint32_t ct, uint32_t cp, const icp_cdf_policy* policy, double* d_phi, double* d_theta,
+                              icp_cdf_report* reports);
 
 /* Static-scratch CDF builder: no counterpart in the reference.  For callers that cannot
  * allocate device memory themselves or through this library -- an embedding application
@@ -371,9 +378,11 @@ typedef struct {
     uint32_t hidden;               /* 128 or 256                                                */
     uint32_t input_width;          /* 64 or 128: 16 record features, then the cell features     */
     uint32_t theta_frequencies;    /* sin / cos (k theta), k = 1..F                             */
-    uint32_t phi_frequencies;      /* cos (l (phi - pi/2)), l = 1..G; 4 + 2F + G <= width - 16 */
+    uint32_t phi_frequencies;      /* cos (l (phi - pi/2)), l = 1..G                            */
     uint32_t max_records;          /* records per call (sizes the activation buffers)          */
-    uint32_t reserved;
+    uint32_t axis_harmonics;       /* P: T_k(cos psi), k = 1..P, in the last P input columns;   */
+                                   /* psi = angle of the cell's direction to the drop's axis,   */
+                                   /* P % 8 == 0, 4 + 2F + G + P <= width - 16                  */
     double log_radius_mm[2];       /* ranges mapped onto [-1, 1] by the record features         */
     double wavelength_nm[2];
     double log_wavelength_over_radius[2]; /* ln(lambda / radius), both in mm                    */
@@ -387,7 +396,7 @@ typedef struct {
 } icp_adam;
 
 /* Defaults for the batched-record distribution: 256 x 512 cells, 256 hidden, width 128,
- * F = 48, G = 12, radius 0.1-3 mm, wavelength 400-700 nm, 16 records per call. */
+ * F = 40, G = 12, P = 16, radius 0.1-3 mm, wavelength 400-700 nm, 16 records per call. */
 int icp_surrogate_default_config(icp_surrogate_config* cfg);
 /* FP32 parameters, in this order: W1[H][K0], b1[H], W2[H][H], b2[H], W3[H][H], b3[H], w4[H],
  * head bias (1): H*K0 + 2H^2 + 4H + 1. */
@@ -397,6 +406,12 @@ uint64_t icp_surrogate_parameter_count(const icp_surrogate_config* cfg);
 int icp_surrogate_record_features(const icp_surrogate_config* cfg, const icp_drop_item* items, uint32_t count,
                                   uint16_t* out);
 int icp_surrogate_cell_features(const icp_surrogate_config* cfg, uint16_t* out);
+/* The input rows the device builds for `count` records (count * nt*np rows x input_width BF16
+ * bits, record-major): record features, cell features and the axis harmonics, which depend on
+ * both (cos psi = -sin(a) cos(theta) - cos(a) sin(theta) sin(phi), a = inclination, phi the
+ * column's azimuth in [-pi, pi), each T_k by the Chebyshev recurrence in FP64, then rounded to
+ * FP32 and BF16). */
+int icp_surrogate_inputs(icp_surrogate* s, const icp_drop_item* items, uint32_t count, uint16_t* h_out);
 int icp_surrogate_create(icp_context* ctx, const icp_surrogate_config* cfg, icp_surrogate** out);
 void icp_surrogate_destroy(icp_surrogate* s);
 /* Loads the parameters (and their BF16 copies); resets the Adam moments. */

@@ -48,8 +48,9 @@ class Config:
     np: int = 512
     hidden: int = 256
     input_width: int = 128
-    theta_frequencies: int = 48
+    theta_frequencies: int = 40
     phi_frequencies: int = 12
+    axis_harmonics: int = 16
     log_radius_mm: tuple = (math.log(0.1), math.log(3.0))
     wavelength_nm: tuple = (400.0, 700.0)
     log_wavelength_over_radius: tuple = (math.log(400e-6 / 3.0), math.log(700e-6 / 0.1))
@@ -61,8 +62,9 @@ class Config:
     def of(cfg) -> "Config":
         """From the library's SurrogateConfig structure."""
         return Config(cfg.nt, cfg.np, cfg.hidden, cfg.input_width, cfg.theta_frequencies, cfg.phi_frequencies,
-                      tuple(cfg.log_radius_mm), tuple(cfg.wavelength_nm), tuple(cfg.log_wavelength_over_radius),
-                      cfg.index_center, cfg.index_scale, tuple(cfg.coefficient_scale))
+                      cfg.axis_harmonics, tuple(cfg.log_radius_mm), tuple(cfg.wavelength_nm),
+                      tuple(cfg.log_wavelength_over_radius), cfg.index_center, cfg.index_scale,
+                      tuple(cfg.coefficient_scale))
 
 
 def _unit(x, r):
@@ -86,8 +88,42 @@ def record_features(cfg: Config, radius_mm, wavelength_nm, inclination_deg, inte
     return f
 
 
+def cell_geometry(cfg: Config) -> tuple[np.ndarray, np.ndarray]:
+    """(cos theta, sin theta sin phi) of every cell centre, phi the column's azimuth in [-pi, pi)
+    (the binning's convention), with the C library's cos / sin."""
+    ct = np.empty(cfg.nt * cfg.np)
+    sts = np.empty(cfg.nt * cfg.np)
+    for i in range(cfg.nt):
+        th = math.pi * (i + 0.5) / cfg.nt
+        c, s = math.cos(th), math.sin(th)
+        for j in range(cfg.np):
+            ph = -math.pi + 2.0 * math.pi * (j + 0.5) / cfg.np
+            ct[i * cfg.np + j] = c
+            sts[i * cfg.np + j] = s * math.sin(ph)
+    return ct, sts
+
+
+def axis_features(cfg: Config, inclination_deg, geometry=None) -> np.ndarray:
+    """Axis harmonics [R*C, P]: T_1..T_P(cos psi), cos psi = -(sin a cos theta) -
+    (cos a sin theta sin phi), the cosine of the angle between a cell's direction and the drop's
+    symmetry axis; FP64 without contraction, Chebyshev recurrence T_{k+1} = (2x) T_k - T_{k-1}."""
+    ct, sts = geometry if geometry is not None else cell_geometry(cfg)
+    out = []
+    for a in inclination_deg:
+        deg = a * (math.pi / 180.0)
+        sa, ca = math.sin(deg), math.cos(deg)
+        x = -(sa * ct) - (ca * sts)
+        cols, tm, t = [], np.ones_like(x), x
+        for _ in range(cfg.axis_harmonics):
+            cols.append(t)
+            tm, t = t, 2.0 * x * t - tm
+        out.append(np.stack(cols, axis=1) if cols else np.zeros((x.size, 0)))
+    return np.concatenate(out, axis=0)
+
+
 def cell_features(cfg: Config) -> np.ndarray:
-    """Cell table [nt*np, K0-16] in FP64 (before rounding), theta-major cells."""
+    """Cell table [nt*np, K0-16] in FP64 (before rounding), theta-major cells; the last
+    axis_harmonics columns are zero (they depend on the record: axis_features)."""
     kc = cfg.input_width - 16
     i = np.repeat(np.arange(cfg.nt), cfg.np).astype(np.float64)
     j = np.tile(np.arange(cfg.np), cfg.nt).astype(np.float64)
@@ -149,13 +185,17 @@ def _silu_grad(z):
     return s * (1.0 + z * (1.0 - s))
 
 
-def inputs(cfg: Config, rec: np.ndarray, cells: np.ndarray) -> np.ndarray:
-    """X [R*C, K0]: record row r (16 values) beside every cell row."""
+def inputs(cfg: Config, rec: np.ndarray, cells: np.ndarray, inclination_deg=None) -> np.ndarray:
+    """X [R*C, K0]: record row r (16 values) beside every cell row, the last axis_harmonics
+    columns the record's axis harmonics (rounded to BF16 like the device's)."""
     R, C = rec.shape[0], cells.shape[0]
     X = np.empty((R * C, cfg.input_width))
     for r in range(R):
         X[r * C:(r + 1) * C, :16] = rec[r]
         X[r * C:(r + 1) * C, 16:] = cells
+    P = cfg.axis_harmonics
+    if P:
+        X[:, cfg.input_width - P:] = bf16(axis_features(cfg, inclination_deg))
     return X
 
 

@@ -114,3 +114,39 @@ def test_full_size_properties(ctx, icp):
     assert np.all(np.diff(t, axis=1) >= 0) and np.all(t[:, 0] == 0) and np.all(t[:, -1] == 1)
     assert out.phi[0] == 0 and out.phi[-1] == 1 and np.all(np.diff(out.phi) >= 0)
     assert abs(out.report["cdf_mass"] - 1) <= 1e-10
+
+
+@pytest.mark.parametrize("count,nt,np_,ct,cp", [(5, 72, 144, 36, 72), (100, 256, 512, 64, 128), (3, 900, 1800, 900, 1800),
+                                               (7, 256, 512, 256, 512)])
+def test_batched_build_equals_single_records(ctx, icp, count, nt, np_, ct, cp):
+    """icp_phase_cdf_build_batch (several records per cooperative launch, 16 strips each; 100
+    records need two launches) writes the same phi / theta bits as icp_phase_cdf_build per
+    record, including records with empty columns and one whose mass is all in the pole rows."""
+    import ctypes as C
+
+    import torch
+
+    rng = np.random.default_rng(count + nt)
+    m = rng.gamma(0.4, size=(count, nt, np_))
+    m[:, :, rng.choice(np_, np_ // 7, replace=False)] = 0.0
+    m[0] = 0.0
+    m[0, 0] = 1.0
+    m[0, -1] = 0.5
+    dv = torch.from_numpy(m.reshape(-1).copy()).cuda()
+    phi = torch.empty(count * (cp + 1), dtype=torch.float64, device="cuda")
+    theta = torch.empty(count * cp * (ct + 1), dtype=torch.float64, device="cuda")
+    reps = (icp.CdfReport * count)()
+    policy = icp.CdfPolicy(1e-10, 1e-12, 1.0)
+    torch.cuda.synchronize()
+    icp.check(icp.LIB.icp_phase_cdf_build_batch(ctx.handle, C.c_void_p(dv.data_ptr()), count, nt, np_, ct, cp,
+                                                C.byref(policy), C.c_void_p(phi.data_ptr()),
+                                                C.c_void_p(theta.data_ptr()), reps))
+    bp = phi.cpu().numpy().reshape(count, cp + 1)
+    bt = theta.cpu().numpy().reshape(count, cp, ct + 1)
+    for r in range(count):
+        one = icp.PhaseCdf(ctx).build(m[r].reshape(-1), nt, np_, ct, cp)
+        assert np.array_equal(bp[r], one.phi), r
+        assert np.array_equal(bt[r], one.theta.reshape(cp, ct + 1)), r
+        assert reps[r].status == 0
+        assert abs(reps[r].g_stored - one.report["g_stored"]) <= 1e-13
+        assert abs(reps[r].l1_error - one.report["l1_error"]) <= 1e-13

@@ -13,7 +13,8 @@ from oracle import surrogate_oracle as SO
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
-SMALL = {"nt": 32, "np": 64, "input_width": 64, "theta_frequencies": 18, "phi_frequencies": 4, "max_records": 4}
+SMALL = {"nt": 32, "np": 64, "input_width": 64, "theta_frequencies": 14, "phi_frequencies": 4, "axis_harmonics": 8,
+         "max_records": 4}
 
 
 def _specs(icp, n, seed):
@@ -34,7 +35,7 @@ def _setup(icp, over, R, seed):
     oc = SO.Config.of(cfg)
     specs = _specs(icp, R, seed)
     rec = SO.from_bits(icp.surrogate_record_features(cfg, specs))
-    X = SO.inputs(oc, rec, SO.from_bits(icp.surrogate_cell_features(cfg)))
+    X = SO.inputs(oc, rec, SO.from_bits(icp.surrogate_cell_features(cfg)), [sp.inclination_deg for sp in specs])
     rng = np.random.default_rng(seed)
     p = SO.init_parameters(oc, seed)
     p[oc.hidden * oc.input_width:oc.hidden * oc.input_width + oc.hidden] = rng.normal(0, 0.1, oc.hidden)  # b1
@@ -67,6 +68,21 @@ def test_gradient_matches_oracle(ctx, icp, over, R):
     for k in ("W1", "b1", "W2", "b2", "W3", "b3", "w4"):
         assert _rel(gw[k], ww[k]) <= 2e-3, (k, _rel(gw[k], ww[k]))
     assert gw["hb"][0] == 0.0
+
+
+@pytest.mark.parametrize("over,R", [(SMALL, 3), ({"max_records": 2}, 2)])
+def test_inputs_match_oracle(ctx, icp, over, R):
+    """The device's input rows (record features, cell table and the axis harmonics it computes in
+    FP64) are bit-identical to the oracle's."""
+    cfg = icp.surrogate_config(**over)
+    oc = SO.Config.of(cfg)
+    specs = _specs(icp, R, 5)
+    with icp.Surrogate(ctx, cfg) as s:
+        got = s.inputs(specs)
+    rec = SO.from_bits(icp.surrogate_record_features(cfg, specs))
+    want = SO.bf16_bits(SO.inputs(oc, rec, SO.from_bits(icp.surrogate_cell_features(cfg)),
+                                  [sp.inclination_deg for sp in specs]))
+    assert np.array_equal(got, want), int((got != want).sum())
 
 
 def test_train_step_applies_adam(ctx, icp):
@@ -171,7 +187,8 @@ def test_training_lowers_heldout_loss(ctx, icp):
     untrained network's."""
     import ice_crystal_phase_b200.surrogate as S
 
-    over = {"nt": 32, "np": 64, "input_width": 64, "theta_frequencies": 18, "phi_frequencies": 8, "max_records": 16}
+    over = {"nt": 32, "np": 64, "input_width": 64, "theta_frequencies": 14, "phi_frequencies": 8, "axis_harmonics": 8,
+            "max_records": 16}
     cfg = icp.surrogate_config(**over)
     specs = S.geometric(icp.batched_record_specs(96, seed=11, rays_max=2e6, rays_min=2e5))
     train, held = specs[:80], specs[80:]

@@ -23,8 +23,8 @@ def _specs(icp, n, seed=5):
     return out
 
 
-@pytest.mark.parametrize("over", [{}, {"nt": 32, "np": 64, "input_width": 64, "theta_frequencies": 18,
-                                       "phi_frequencies": 4}])
+@pytest.mark.parametrize("over", [{}, {"nt": 32, "np": 64, "input_width": 64, "theta_frequencies": 14,
+                                       "phi_frequencies": 4, "axis_harmonics": 8}])
 def test_feature_rows_match_oracle(icp, over):
     cfg = icp.surrogate_config(**over)
     oc = SO.Config.of(cfg)
@@ -54,11 +54,11 @@ def test_bf16_rounding_is_nearest_even():
 
 
 def test_oracle_gradient_matches_finite_differences():
-    cfg = SO.Config(nt=4, np=8, hidden=8, input_width=64, theta_frequencies=10, phi_frequencies=3)
+    cfg = SO.Config(nt=4, np=8, hidden=8, input_width=64, theta_frequencies=10, phi_frequencies=3, axis_harmonics=8)
     rng = np.random.default_rng(1)
     R = 2
     rec = rng.uniform(-1, 1, (R, 16))
-    X = SO.inputs(cfg, rec, SO.cell_features(cfg))
+    X = SO.inputs(cfg, rec, SO.cell_features(cfg), [20.0, -63.0])
     p = SO.init_parameters(cfg, 3).astype(np.float64)
     target = rng.dirichlet(np.ones(cfg.nt * cfg.np), size=R)
     target[0, :5] = 0.0
@@ -79,9 +79,9 @@ def test_oracle_gradient_matches_finite_differences():
 
 
 def test_oracle_emulation_only_rounds():
-    cfg = SO.Config(nt=8, np=16, hidden=16, input_width=64, theta_frequencies=10, phi_frequencies=3)
+    cfg = SO.Config(nt=8, np=16, hidden=16, input_width=64, theta_frequencies=10, phi_frequencies=3, axis_harmonics=8)
     rng = np.random.default_rng(2)
-    X = SO.inputs(cfg, rng.uniform(-1, 1, (1, 16)), SO.cell_features(cfg))
+    X = SO.inputs(cfg, rng.uniform(-1, 1, (1, 16)), SO.cell_features(cfg), [35.0])
     p = SO.init_parameters(cfg, 4)
     target = rng.dirichlet(np.ones(cfg.nt * cfg.np), size=1)
     l0, g0 = SO.gradient(cfg, p, X, target, 1, emulate=False)
@@ -92,6 +92,7 @@ def test_oracle_emulation_only_rounds():
 
 def test_config_validation(icp):
     for bad in [{"hidden": 96}, {"input_width": 96}, {"theta_frequencies": 60}, {"nt": 3, "np": 5},
+                {"axis_harmonics": 4}, {"axis_harmonics": 32},
                 {"max_records": 0}, {"wavelength_nm": (700.0, 400.0)}, {"index_scale": 0.0}]:
         cfg = icp.surrogate_config(**bad)
         with pytest.raises(icp.InvalidArgument):
@@ -102,3 +103,25 @@ def test_config_validation(icp):
     assert icp.surrogate_parameter_count(cfg) == SO.parameter_count(SO.Config.of(cfg)) == 256 * 128 + 2 * 256 ** 2 + 4 * 256 + 1
     with pytest.raises(icp.InvalidArgument):
         icp.surrogate_record_features(cfg, [icp.DropSpec([0] * 8, -1.0, 1.33, rays=1, seed=1)])
+
+
+def test_axis_harmonics_are_the_angle_to_the_drop_axis(icp):
+    """cos psi of the axis harmonics is the cosine between a cell's direction (theta from ki,
+    phi from e0 towards e1, the binning's azimuth in [-pi, pi)) and the drop's axis y, and is
+    even about phi = pi/2 like every other feature."""
+    cfg = SO.Config(nt=8, np=16, axis_harmonics=8)
+    ct, sts = SO.cell_geometry(cfg)
+    for a in (0.0, 20.0, -55.0, 89.0):
+        k, e0, e1 = (np.array(v) for v in icp.drop_frame(a))
+        T = SO.axis_features(cfg, [a], (ct, sts))
+        x = T[:, 0]
+        for i in range(cfg.nt):
+            th = math.pi * (i + 0.5) / cfg.nt
+            for j in range(cfg.np):
+                ph = -math.pi + 2 * math.pi * (j + 0.5) / cfg.np
+                w = math.cos(th) * k + math.sin(th) * (math.cos(ph) * e0 + math.sin(ph) * e1)
+                assert abs(x[i * cfg.np + j] - w[1]) <= 1e-6  # the frame is held in binary32
+        assert np.allclose(T[:, 2], 4 * x ** 3 - 3 * x, atol=1e-12)  # T_3
+        # mirror phi -> pi - phi: column j -> np/2 - 1 - j (mod np) of the [-pi, pi) azimuths
+        g = x.reshape(cfg.nt, cfg.np)
+        assert np.allclose(g, g[:, [(cfg.np // 2 - 1 - j) % cfg.np for j in range(cfg.np)]], atol=1e-12)
