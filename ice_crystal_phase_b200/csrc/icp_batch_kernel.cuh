@@ -79,7 +79,7 @@ __device__ __forceinline__ void warp_flush(const P_& P, unsigned* s_status, cons
 }
 
 template <class R, class G>
-__global__ void __launch_bounds__(256, (sizeof(R) == 4 ? 3 : 1)) batch_trace_kernel(const BatchParams<R, G> Q)
+__global__ void __launch_bounds__(256, (sizeof(R) == 4 ? 4 : 1)) batch_trace_kernel(const BatchParams<R, G> Q)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const unsigned warps = blockDim.x >> 5, wib = threadIdx.x >> 5, lane = threadIdx.x & 31u;

@@ -590,7 +590,7 @@ __device__ __forceinline__ void block_flush(const P_& P, const BlockShared<R>& B
 
 // One record: the ray range [first, first+count) split into contiguous per-warp slices.
 template <class R, class G>
-__global__ void __launch_bounds__(256, (sizeof(R) == 4 ? 3 : 1)) trace_bin_kernel(const TraceParams<R, G> P)
+__global__ void __launch_bounds__(256, (sizeof(R) == 4 ? 4 : 1)) trace_bin_kernel(const TraceParams<R, G> P)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const BlockShared<R> B = block_setup<R>(P, smem);

@@ -2,6 +2,7 @@
 // arithmetic type and geometry in icp_hex_f32.cu / icp_hex_f64.cu / icp_drop_f32.cu / icp_drop_f64.cu.
 #pragma once
 #include <cmath>
+#include <vector>
 
 #include "icp_batch_kernel.cuh"
 #include "icp_hex_kernel.cuh"
@@ -98,6 +99,40 @@ template <class R> TraceParams<R, DropGeo<R>> make_drop_params(const HexLaunch& 
     for (int k = 0; k < 7; ++k) P.geo.shape.md[k] = (R)((k + 1) * mono[k + 1]);
     P.geo.shape.r_out = (R)L.r_out;
     P.geo.shape.r_center = (R)L.r_center;
+    {
+        // enclosing spheroid of the surface r = 1 + sum c_n T_n(mu), y = -mu r: centre and
+        // half-axes from the extents, scaled by the largest spheroid gauge over 2049 samples of
+        // mu, then inflated by 1e-5 (far above the binary32 rounding of the roots and above the
+        // sampling error, which is second order in the 9.8e-4 spacing: below 1e-6)
+        const int n = 2048;
+        double ymin = 1e300, ymax = -1e300, hmax = 0;
+        std::vector<double> ys(n + 1), hs(n + 1);
+        for (int i = 0; i <= n; ++i) {
+            const double mu = -1.0 + 2.0 * i / n;
+            double tm = 1, t = mu, r = 1 + L.coeff[0] + L.coeff[1] * mu;
+            for (int k = 2; k < 8; ++k) {
+                const double tn = 2 * mu * t - tm;
+                r += L.coeff[k] * tn;
+                tm = t;
+                t = tn;
+            }
+            ys[i] = -mu * r;
+            hs[i] = std::sqrt(std::fmax(0.0, 1 - mu * mu)) * r;
+            ymin = std::fmin(ymin, ys[i]);
+            ymax = std::fmax(ymax, ys[i]);
+            hmax = std::fmax(hmax, hs[i]);
+        }
+        const double y0 = 0.5 * (ymax + ymin), A = hmax, B = 0.5 * (ymax - ymin);
+        double sc = 0;
+        for (int i = 0; i <= n; ++i) {
+            const double u = hs[i] / A, v = (ys[i] - y0) / B;
+            sc = std::fmax(sc, std::sqrt(u * u + v * v));
+        }
+        const double Ae = A * sc * (1 + 1e-5) + 1e-7, Be = B * sc * (1 + 1e-5) + 1e-7;
+        P.geo.shape.ea_inv = (R)(1.0 / Ae);
+        P.geo.shape.eb_inv = (R)(1.0 / Be);
+        P.geo.shape.ey0 = (R)y0;
+    }
     P.geo.shape.sphere = L.sphere != 0;
     P.geo.disk = (R)L.disk;
     P.geo.back = (R)L.back;
