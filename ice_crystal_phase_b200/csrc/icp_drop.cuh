@@ -119,6 +119,16 @@ template <class R> __device__ __forceinline__ bool spheroid_roots(const DropShap
 
 constexpr int kNewtonMax = 40;
 
+// Newton on the smooth gauge converges quadratically: successive steps s_{k-1}, s_k estimate
+// the constant C = s_k / s_{k-1}^2 of e_{k+1} = C e_k^2, so the error left after applying s_k is
+// about s_k^3 / s_{k-1}^2.  When that is below a sixteenth of the rounding tolerance of t the
+// root is reached without one more gauge evaluation (which would only confirm a step below tol).
+template <class R> __device__ __forceinline__ bool newton_done(R step, R prev_step, R tol)
+{
+    const R a = rabs(step);
+    return prev_step != R(0) && a * a * a <= R(0.0625) * tol * prev_step * prev_step;
+}
+
 // Intersection of the line q + t w (w unit) with the drop: entering from outside, the first
 // root; leaving from a surface point, the far root.  Both run one Newton loop on the gauge from
 // the bounding sphere (the near root entering, the far root leaving), so lanes entering and
@@ -138,7 +148,7 @@ __device__ __forceinline__ bool drop_intersect(const DropShape<R>& S, V3<R> q, V
     }
     t = rmax(entering ? t0 : t1, R(0));
     const R sgn = entering ? R(-1) : R(1);
-    R prev_h = R(1e30);
+    R prev_h = R(1e30), prev_step = R(0);
     for (int it = 0; it < kNewtonMax; ++it) {
         R dh;
         const R h = gauge(S, q + w * t, w, dh);
@@ -152,8 +162,11 @@ __device__ __forceinline__ bool drop_intersect(const DropShape<R>& S, V3<R> q, V
             if (!entering) t = R(0);
             return !entering;
         }
-        if (!(h < prev_h) || rabs(step) <= R(4) * Eps<R>::eps * rmax(R(1), rabs(t))) return true;
+        const R tol = R(4) * Eps<R>::eps * rmax(R(1), rabs(t));
+        if (!(h < prev_h) || rabs(step) <= tol) return true;
+        if (newton_done(step, prev_step, tol)) return true;
         prev_h = h;
+        prev_step = step;
     }
     return true;
 }
@@ -171,7 +184,7 @@ template <class R> __device__ __forceinline__ bool drop_entry(const DropShape<R>
     }
     if (!spheroid_roots(S, o, d, t0, t1)) return false;
     t = rmax(t0, R(0));
-    R prev_h = R(1e30);
+    R prev_h = R(1e30), prev_step = R(0);
     for (int it = 0; it < kNewtonMax; ++it) {
         R dh;
         const R h = gauge(S, o + d * t, d, dh);
@@ -181,7 +194,10 @@ template <class R> __device__ __forceinline__ bool drop_entry(const DropShape<R>
         const R step = h / dh;                // negative
         t -= step;
         if (t > t1) return false;
-        if (!(h < prev_h) || rabs(step) <= R(4) * Eps<R>::eps * rmax(R(1), rabs(t))) return true;
+        const R tol = R(4) * Eps<R>::eps * rmax(R(1), rabs(t));
+        if (!(h < prev_h) || rabs(step) <= tol) return true;
+        if (newton_done(step, prev_step, tol)) return true;
+        prev_step = step;
         prev_h = h;
     }
     return true;
