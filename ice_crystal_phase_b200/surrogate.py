@@ -328,9 +328,12 @@ def run_training(ctx: I.Context, s: TrainSettings, cfg_over: dict | None = None,
     cfg = I.surrogate_config(**{"max_records": s.batch, **(cfg_over or {})})
     sur = I.Surrogate(ctx, cfg)
     sur.set_parameters(init_parameters(cfg, s.seed))
-    specs = I.batched_record_specs(s.records + s.heldout, seed=1000 * s.seed + 1, rays_max=s.rays_max,
-                                   rays_min=s.rays_min, diffraction=True)
-    train_specs, held = specs[:s.records], specs[s.records:]
+    # the held-out records come from their own seed, so that runs with different training sets
+    # are judged on the same records
+    train_specs = I.batched_record_specs(s.records, seed=1000 * s.seed + 1, rays_max=s.rays_max, rays_min=s.rays_min,
+                                         diffraction=True)
+    held = I.batched_record_specs(s.heldout, seed=1000 * s.seed + 3, rays_max=s.rays_max, rays_min=s.rays_min,
+                                  diffraction=True)
     if s.large_records:
         train_specs = train_specs + I.batched_record_specs(s.large_records, seed=1000 * s.seed + 2,
                                                            rays_max=s.rays_max, rays_min=s.rays_min, diffraction=True,
