@@ -15,6 +15,14 @@ n = 1.31, 550 nm, ki = (cos30, -sin30, 0), 1e8 rays, 12 interactions, 512 x 1024
 With N ranks (torchrun) every rank traces its own 1e8-ray shard of one record (weak scaling),
 the FP64 histograms are summed with one NCCL all-reduce, and rank 0 finishes the record.
 
+Two more measurements ride on the same line (N = 1):
+* `batched`: 256 records of the batched distribution in one autotuned, graph-captured launch,
+  against the same records one by one through the plain entry;
+* `surrogate`: the committed learned surrogate on 256 fresh records (256 x 512 cells, stored at
+  64 x 128), alone and with its tracer fallback, against the plain tracer on the same records,
+  with a held-out sample judged by 1e8-ray tracer records and the forward pass against the BF16
+  peak.
+
 Timing: CUDA events on the library's stream, W untimed warm-up steps, K timed steps, each
 bracketed by barrier + synchronize; an L2 flush (a 256 MiB write) separates timed steps;
 max over ranks.  `value` keeps the outputs in HBM (icp_drop_generate_device); `e2e` goes
@@ -67,10 +75,14 @@ class ClockSampler:
                 ["nvidia-smi", "-i", str(self.device), "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                 "--format=csv,noheader,nounits", "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
                 text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # the timed region starts once the sampler is running (nvidia-smi takes a moment)
+            t0 = time.perf_counter()
+            while not self.rows and time.perf_counter() - t0 < 3.0 and self.proc.poll() is None:
+                time.sleep(0.01)
         except OSError:
             self.proc = None
         return self
@@ -816,7 +828,7 @@ def run_b200_drop(a) -> None:
 def main() -> None:
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["b200", "reference"], default="b200")
     p.add_argument("--workload", choices=["drop", "hex"], default="drop")
