@@ -282,7 +282,9 @@ int enqueue_backward(icp_surrogate* s, uint32_t count)
                                       s->G(s->o_b3), c->stream);
     count_launch();
     if (e) return fail(ICP_ERR_DEVICE, "head backward launch failed (%d)", e);
-    const uint32_t splits = std::max<uint32_t>(1u, (uint32_t)c->sms / (Hn / 128u));
+    // the weight-gradient GEMMs have M = H <= 256 rows, which one CTA covers (two row tiles share
+    // each B chunk): one CTA per SM, each over an equal share of the batch's rows
+    const uint32_t splits = std::max<uint32_t>(1u, (uint32_t)c->sms);
     // dW3 = dz3^T h2
     mlp::GemmArgs g = layer(Hn, Hn, (uint32_t)M);
     g.out_f32 = s->G(s->o_w3);

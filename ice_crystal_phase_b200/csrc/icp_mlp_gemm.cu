@@ -32,10 +32,18 @@ namespace {
 constexpr uint32_t kWaitLimit = 1u << 22;
 constexpr uint32_t kA = 128u * 128u; // bytes of one A stage: 128 rows x 64 BF16
 
-template <int N> __host__ __device__ constexpr int stages() { return N <= 128 ? 4 : 3; }
-template <int N> __host__ __device__ constexpr uint32_t stage_bytes() { return kA + (uint32_t)N * 128u; }
+// split-K kernel: MT row tiles of 128 per CTA share each B chunk (MT = 2 for the weight gradients,
+// whose M is 256: B is then read once instead of once per row tile)
+template <int N, int MT = 1> __host__ __device__ constexpr int stages() { return N <= 128 ? 4 : 3; }
+template <int N, int MT = 1> __host__ __device__ constexpr uint32_t stage_bytes()
+{
+    return (uint32_t)MT * kA + (uint32_t)N * 128u;
+}
 // 1024 (alignment) + stages + barriers / TMEM slot (256) + column sums of the bias gradient (1024)
-template <int N> constexpr size_t smem_bytes() { return 1024 + (size_t)stages<N>() * stage_bytes<N>() + 256 + 1024; }
+template <int N, int MT = 1> constexpr size_t smem_bytes()
+{
+    return 1024 + (size_t)stages<N, MT>() * stage_bytes<N, MT>() + 256 + 1024;
+}
 
 // Logistic function 1 / (1 + exp(-z)) with the exponential on the special-function unit and
 // the reciprocal on the FMA pipe, so that the two pipes share the epilogue's activation work
@@ -51,10 +59,16 @@ __device__ __forceinline__ float logistic(float z)
     for (int k = 0; k < 3; ++k) y = fmaf(y, fmaf(-d, y, 1.0f), y);
     return y;
 }
-__device__ __forceinline__ float silu(float z) { return z * logistic(z); }
-__device__ __forceinline__ float silu_grad(float z)
+// The training epilogues (more stores per element, MUFU pipe not the limit) use the
+// special-function reciprocal instead: both forms agree to ~1e-7 relative.
+__device__ __forceinline__ float logistic_mufu(float z) { return __fdividef(1.0f, 1.0f + __expf(-fmaxf(z, -80.0f))); }
+template <bool kFmaRcp> __device__ __forceinline__ float silu(float z)
 {
-    const float s = logistic(z);
+    return z * (kFmaRcp ? logistic(z) : logistic_mufu(z));
+}
+template <bool kFmaRcp> __device__ __forceinline__ float silu_grad(float z)
+{
+    const float s = kFmaRcp ? logistic(z) : logistic_mufu(z);
     return s * (1.0f + z * (1.0f - s));
 }
 
@@ -89,17 +103,35 @@ __device__ __forceinline__ float warp_column_sum(float (&v)[32], uint32_t lane)
     return v[0];
 }
 
-// Column-major copy of a warp's 32 rows x 32 columns: for each column, the 32 lanes write 32
-// consecutive rows (64 contiguous bytes).  One running pointer, not 32 precomputed addresses
-// (the persistent kernel's epilogue runs at 168 registers).
-__device__ __forceinline__ void store_bf16x32_t(__nv_bfloat16* dst, uint32_t ld, const float (&v)[32])
+// Column-major copy of a warp's 32 rows x 32 columns through the warp's shared transpose buffer
+// (32 rows of 40 BF16, 80-byte stride): lane L writes its row, then gathers column L and writes
+// its 32 rows (64 contiguous bytes) to dst_col0 + L * ld with four 16-byte stores.  dst_col0 is
+// the column's first row of this warp (32-row aligned).  Every index is a compile-time constant.
+constexpr uint32_t kTStride = 40; // BF16 per transpose-buffer row
+__device__ __forceinline__ void store_bf16x32_t(__nv_bfloat16* dst_col0, uint32_t ld, const float (&v)[32],
+                                                __nv_bfloat16* tbuf, uint32_t lane)
 {
-    __nv_bfloat16* p = dst;
-#pragma unroll 8
-    for (int i = 0; i < 32; ++i) {
-        *p = __float2bfloat16_rn(v[i]);
-        p += ld;
+    uint4* row = reinterpret_cast<uint4*>(tbuf + lane * kTStride);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        uint32_t w[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const __nv_bfloat162 p = __floats2bfloat162_rn(v[8 * q + 2 * i], v[8 * q + 2 * i + 1]);
+            w[i] = *reinterpret_cast<const uint32_t*>(&p);
+        }
+        row[q] = make_uint4(w[0], w[1], w[2], w[3]);
     }
+    __syncwarp();
+    const uint16_t* col = reinterpret_cast<const uint16_t*>(tbuf) + lane;
+    uint32_t w[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r)
+        w[r] = (uint32_t)col[(2 * r) * kTStride] | ((uint32_t)col[(2 * r + 1) * kTStride] << 16);
+    uint4* d = reinterpret_cast<uint4*>(dst_col0 + (size_t)lane * ld);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) d[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+    __syncwarp();
 }
 
 __device__ __forceinline__ void load_bf16x32(const __nv_bfloat16* src, float (&v)[32])
@@ -126,7 +158,7 @@ __device__ __forceinline__ void load_bf16x32(const __nv_bfloat16* src, float (&v
 template <int N, int EPI>
 __device__ __forceinline__ float epilogue_cols(const GemmArgs& g, uint32_t taddr, uint32_t m, uint32_t lane,
                                               uint32_t c0, uint32_t c1, const float* bias, const float* head_w,
-                                              float* colsum)
+                                              float* colsum, __nv_bfloat16* tbuf)
 {
     constexpr bool kHeadEpi = EPI == kHead || EPI == kHeadTrain;
     constexpr bool kTrain = EPI == kHiddenTrain || EPI == kHeadTrain;
@@ -157,10 +189,10 @@ __device__ __forceinline__ float epilogue_cols(const GemmArgs& g, uint32_t taddr
             if constexpr (kTrain)
                 if (g.out_z) store_bf16x32(g.out_z + (size_t)m * N + c, v);
 #pragma unroll
-            for (int i = 0; i < 32; ++i) v[i] = silu(v[i]);
+            for (int i = 0; i < 32; ++i) v[i] = silu<!kTrain>(v[i]);
             if (g.out_h) store_bf16x32(g.out_h + (size_t)m * N + c, v);
             if constexpr (kTrain)
-                if (g.out_hT) store_bf16x32_t(g.out_hT + (size_t)c * g.ld_t + m, g.ld_t, v);
+                if (g.out_hT) store_bf16x32_t(g.out_hT + (size_t)c * g.ld_t + (m - lane), g.ld_t, v, tbuf, lane);
             if constexpr (kHeadEpi) {
                 const float4* w4 = reinterpret_cast<const float4*>(head_w + c);
 #pragma unroll
@@ -176,9 +208,9 @@ __device__ __forceinline__ float epilogue_cols(const GemmArgs& g, uint32_t taddr
             float z[32];
             load_bf16x32(g.z_prev + (size_t)m * N + c, z);
 #pragma unroll
-            for (int i = 0; i < 32; ++i) v[i] *= silu_grad(z[i]);
+            for (int i = 0; i < 32; ++i) v[i] *= silu_grad<false>(z[i]);
             if (g.out_dz) store_bf16x32(g.out_dz + (size_t)m * N + c, v);
-            if (g.out_dzT) store_bf16x32_t(g.out_dzT + (size_t)c * g.ld_t + m, g.ld_t, v);
+            if (g.out_dzT) store_bf16x32_t(g.out_dzT + (size_t)c * g.ld_t + (m - lane), g.ld_t, v, tbuf, lane);
             if (g.out_db) atomicAdd(&colsum[c + lane], warp_column_sum(v, lane));
         }
     }
@@ -204,12 +236,13 @@ __device__ __forceinline__ void head_store(const GemmArgs& g, uint32_t m, float 
 
 // Split-K GEMM (one 128-row tile and one K range per CTA): the weight gradients, whose K (the
 // rows of a batch) is long and whose M and N are the layer widths.
-template <int N, int EPI>
+template <int N, int EPI, int MT = 1>
 __global__ void __launch_bounds__(128, 1)
     gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const GemmArgs g)
 {
-    constexpr int S = stages<N>();
-    constexpr uint32_t SB = stage_bytes<N>();
+    constexpr int S = stages<N, MT>();
+    constexpr uint32_t SB = stage_bytes<N, MT>();
+    constexpr uint32_t BOFF = (uint32_t)MT * kA; // B chunk after the MT A tiles of a stage
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * SB);
@@ -231,12 +264,12 @@ __global__ void __launch_bounds__(128, 1)
         *abort_flag = 0;
         umma::mbar_fence_init();
     }
-    if (warp == 0) umma::tmem_alloc(tslot, (uint32_t)N);
+    if (warp == 0) umma::tmem_alloc(tslot, (uint32_t)(MT * N));
     umma::fence_before_sync();
     __syncthreads();
     umma::fence_after_sync();
     const uint32_t tmem = *tslot;
-    const uint32_t m0 = blockIdx.x * 128u;
+    const uint32_t m0 = blockIdx.x * 128u * MT;
     const uint32_t nk_total = g.K / 64u;
     const uint32_t kc0 = blockIdx.y * g.k_chunks;
     const uint32_t kc1 = min(nk_total, kc0 + g.k_chunks);
@@ -248,8 +281,10 @@ __global__ void __launch_bounds__(128, 1)
         auto load = [&](uint32_t s, uint32_t kc) {
             uint8_t* a = smem + s * SB;
             umma::mbar_arrive_expect_tx(&full[s], SB);
-            umma::tma_load_2d(a, &tmA, &full[s], (int32_t)((kc0 + kc) * 64u), (int32_t)m0);
-            umma::tma_load_2d(a + kA, &tmB, &full[s], (int32_t)((kc0 + kc) * 64u), 0);
+#pragma unroll
+            for (int mt = 0; mt < MT; ++mt)
+                umma::tma_load_2d(a + mt * kA, &tmA, &full[s], (int32_t)((kc0 + kc) * 64u), (int32_t)(m0 + 128u * mt));
+            umma::tma_load_2d(a + BOFF, &tmB, &full[s], (int32_t)((kc0 + kc) * 64u), 0);
         };
         uint32_t issued = nk < (uint32_t)S ? nk : (uint32_t)S, consumed = 0;
         for (uint32_t s = 0; s < issued; ++s) load(s, s);
@@ -261,11 +296,13 @@ __global__ void __launch_bounds__(128, 1)
             }
             consumed = kc + 1;
             umma::fence_after_sync();
-            const uint32_t a = umma::smem_u32(smem + s * SB), b = a + kA;
+            const uint32_t a = umma::smem_u32(smem + s * SB), b = a + BOFF;
 #pragma unroll
-            for (uint32_t k = 0; k < 4; ++k)
-                umma::mma_bf16(tmem, umma::smem_desc_sw128(a + 32u * k), umma::smem_desc_sw128(b + 32u * k), idesc,
-                               kc > 0 || k > 0);
+            for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+                for (uint32_t k = 0; k < 4; ++k)
+                    umma::mma_bf16(tmem + (uint32_t)(mt * N), umma::smem_desc_sw128(a + mt * kA + 32u * k),
+                                   umma::smem_desc_sw128(b + 32u * k), idesc, kc > 0 || k > 0);
             umma::mma_commit(&empty[s]);
             if (kc + S < nk) {
                 if (!umma::mbar_wait(&empty[s], par, kWaitLimit)) {
@@ -292,10 +329,15 @@ __global__ void __launch_bounds__(128, 1)
     const bool ready = __all_sync(0xffffffffu, mine && !*abort_flag);
     umma::fence_after_sync();
     if (ready) {
-        const uint32_t m = m0 + 32u * warp + lane;
-        const float y = epilogue_cols<N, EPI>(g, tmem + ((32u * warp) << 16), m, lane, 0u, (uint32_t)N, g.bias,
-                                              g.head_w, colsum);
-        if constexpr (EPI == kHead || EPI == kHeadTrain) head_store(g, m, y);
+        // the stages are free once every MMA has completed: one transpose buffer per warp there
+        __nv_bfloat16* tbuf = reinterpret_cast<__nv_bfloat16*>(smem) + (size_t)warp * 32u * kTStride;
+#pragma unroll 1
+        for (int mt = 0; mt < MT; ++mt) {
+            const uint32_t m = m0 + 128u * mt + 32u * warp + lane;
+            const float y = epilogue_cols<N, EPI>(g, tmem + ((32u * warp) << 16) + (uint32_t)(mt * N), m, lane, 0u,
+                                                  (uint32_t)N, g.bias, g.head_w, colsum, tbuf);
+            if constexpr (EPI == kHead || EPI == kHeadTrain) head_store(g, m, y);
+        }
     }
     if constexpr (EPI == kBackprop) {
         __syncthreads();
@@ -304,7 +346,7 @@ __global__ void __launch_bounds__(128, 1)
     }
     umma::fence_before_sync();
     __syncthreads();
-    if (warp == 0) umma::tmem_dealloc(tmem, (uint32_t)N);
+    if (warp == 0) umma::tmem_dealloc(tmem, (uint32_t)(MT * N));
 }
 
 // ---------------------------------------------------------------- persistent layer GEMM
@@ -326,7 +368,7 @@ constexpr uint32_t kSlices = kEpiWarps / 4;
 constexpr uint32_t kPThreads = 64 + 32 * kEpiWarps;
 // per-CTA extras after the ring: barriers (1 KB), colsum, bias, head weights (1 KB each), head
 // partial sums (kSlices - 1 slices x 128 floats, rounded up to kSlices)
-constexpr int kPExtra = 1024 + 3 * 1024 + (int)kSlices * 512;
+constexpr int kPExtra = 1024 + 3 * 1024 + (int)kSlices * 512 + (int)(kEpiWarps * 32u * kTStride * 2u);
 template <int N, int KC> __host__ __device__ constexpr int pstages()
 {
     return (232448 - 1024 - N * 128 * KC - kPExtra) / (int)kA > 8 ? 8
@@ -369,6 +411,7 @@ __global__ void __launch_bounds__(kPThreads, 1)
     float* sbias = colsum + 256;
     float* shead = sbias + 256;
     float* ypart = shead + 256; // [kSlices - 1][128]
+    __nv_bfloat16* tbufs = reinterpret_cast<__nv_bfloat16*>(ypart + kSlices * 128u); // per epilogue warp
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t tiles = g.M / 128u;
 
@@ -490,7 +533,7 @@ __global__ void __launch_bounds__(kPThreads, 1)
             if (live) {
                 umma::fence_after_sync();
                 y = epilogue_cols<N, EPI>(g, tmem + ((32u * q) << 16) + b * (uint32_t)N, t * 128u + row, lane, c0,
-                                          c0 + W, sbias, shead, colsum);
+                                          c0 + W, sbias, shead, colsum, tbufs + (warp - 2u) * 32u * kTStride);
                 umma::fence_before_sync();
                 __syncwarp();
                 if (lane == 0) umma::mbar_arrive(&acc_empty[b]);
@@ -550,19 +593,32 @@ int make_map(CUtensorMap* map, const void* ptr, uint32_t rows, uint32_t cols, ui
     return r == CUDA_SUCCESS ? 0 : (int)r;
 }
 
-template <int N, int EPI> int launch_n(const void* A, const void* B, const GemmArgs& g, uint32_t splits, cudaStream_t st)
+template <int N, int EPI, int MT = 1>
+int launch_n(const void* A, const void* B, const GemmArgs& g, uint32_t splits, cudaStream_t st)
 {
     CUtensorMap ta, tb;
     if (make_map(&ta, A, g.M, g.K, 128u) || make_map(&tb, B, (uint32_t)N, g.K, (uint32_t)N)) return -1;
-    const size_t smem = smem_bytes<N>();
-    cudaError_t e = cudaFuncSetAttribute(gemm_kernel<N, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const size_t smem = smem_bytes<N, MT>();
+    cudaError_t e =
+        cudaFuncSetAttribute(gemm_kernel<N, EPI, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return (int)e;
-    gemm_kernel<N, EPI><<<dim3(g.M / 128u, splits), 128, smem, st>>>(ta, tb, g);
+    gemm_kernel<N, EPI, MT><<<dim3(g.M / (128u * MT), splits), 128, smem, st>>>(ta, tb, g);
     return (int)cudaGetLastError();
 }
 
 template <int EPI> int launch_epi(const void* A, const void* B, const GemmArgs& g, uint32_t splits, cudaStream_t st)
 {
+    if constexpr (EPI == kAtomicF32) {
+        // two row tiles per CTA share each B chunk
+        if (g.M % 256u == 0) {
+            switch (g.N) {
+            case 64: return launch_n<64, EPI, 2>(A, B, g, splits, st);
+            case 128: return launch_n<128, EPI, 2>(A, B, g, splits, st);
+            case 256: return launch_n<256, EPI, 2>(A, B, g, splits, st);
+            default: return -2;
+            }
+        }
+    }
     switch (g.N) {
     case 64: return launch_n<64, EPI>(A, B, g, splits, st);
     case 128: return launch_n<128, EPI>(A, B, g, splits, st);
