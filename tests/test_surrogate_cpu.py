@@ -125,3 +125,51 @@ def test_axis_harmonics_are_the_angle_to_the_drop_axis(icp):
         # mirror phi -> pi - phi: column j -> np/2 - 1 - j (mod np) of the [-pi, pi) azimuths
         g = x.reshape(cfg.nt, cfg.np)
         assert np.allclose(g, g[:, [(cfg.np // 2 - 1 - j) % cfg.np for j in range(cfg.np)]], atol=1e-12)
+
+
+def test_fallback_gate_rules(icp):
+    """The gate trusts a judged record by its own verdict, any other record only when its k
+    nearest judged records (normalised log radius, wavelength, inclination) all passed; it survives
+    the round trip through the model file's JSON."""
+    import json
+
+    import ice_crystal_phase_b200.surrogate as S
+
+    def spec(r, lam, inc):
+        return icp.DropSpec([0.0] * 8, r, 1.33, 1, seed=1, inclination_deg=inc, wavelength_nm=lam)
+
+    judged = [spec(0.2, 500, 0), spec(0.21, 505, 2), spec(0.19, 495, -2), spec(2.5, 600, 40), spec(2.6, 610, 45),
+              spec(2.4, 590, 35)]
+    gate = S.FallbackGate.of(judged, [True, True, True, True, False, True], k=3)
+    assert gate.trusted(judged[0]) and not gate.trusted(judged[4])
+    assert gate.trusted(spec(0.2, 501, 1))          # all three neighbours passed
+    assert not gate.trusted(spec(2.5, 601, 41))     # a failed neighbour among the three
+    back = S.FallbackGate.from_dict(json.loads(json.dumps(gate.as_dict())))
+    assert back.k == 3 and np.array_equal(back.passed, gate.passed) and np.allclose(back.keys, gate.keys)
+
+
+def test_learning_rate_schedule():
+    import ice_crystal_phase_b200.surrogate as S
+
+    s = S.TrainSettings(lr=2e-3, lr_final=2e-5, warmup_steps=10)
+    lrs = [S._lr(s, k, 110) for k in range(110)]
+    assert abs(lrs[0] - 2e-4) < 1e-12 and abs(lrs[9] - 2e-3) < 1e-12      # linear warm-up
+    assert abs(lrs[10] - 2e-3) < 1e-9 and abs(S._lr(s, 110, 110) - 2e-5) < 1e-12  # cosine to lr_final
+    assert all(a >= b for a, b in zip(lrs[10:], lrs[11:]))
+
+
+def test_storage_grid_sums_and_tv():
+    import torch
+
+    import ice_crystal_phase_b200.surrogate as S
+
+    rng = np.random.default_rng(3)
+    p = rng.dirichlet(np.ones(16 * 32), size=2)
+    q = rng.dirichlet(np.ones(16 * 32), size=2)
+    pt, qt = torch.from_numpy(p), torch.from_numpy(q)
+    c = S.coarse(pt, 16, 32, 4, 8).numpy()
+    want = p.reshape(2, 4, 4, 8, 4).sum(axis=(2, 4)).reshape(2, -1)
+    assert np.allclose(c, want, atol=1e-15)
+    assert np.allclose(S.tv(pt, qt).numpy(), 0.5 * np.abs(p - q).sum(axis=1))
+    # aggregation never raises the total variation
+    assert np.all(S.tv(S.coarse(pt, 16, 32, 4, 8), S.coarse(qt, 16, 32, 4, 8)).numpy() <= S.tv(pt, qt).numpy() + 1e-15)
