@@ -20,7 +20,7 @@ Two more measurements ride on the same line (N = 1):
   against the same records one by one through the plain entry;
 * `surrogate`: the committed learned surrogate on 256 fresh records (256 x 512 cells, stored at
   64 x 128), alone and with its tracer fallback, against the plain tracer on the same records,
-  with a held-out sample judged by 1e8-ray tracer records and the forward pass against the BF16
+  with a held-out sample checked by 1e8-ray tracer records and the forward pass against the BF16
   peak.
 
 Timing: CUDA events on the library's stream, W untimed warm-up steps, K timed steps, each
@@ -140,7 +140,7 @@ def run_reference_hex(a) -> None:
     line = {"metric": METRIC, "value": v, "unit": "rays/s", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": 1e3 * sum(x["seconds"] for x in vals) / len(vals), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "hex_column_config3", **_cfg_public()}, "impl": "reference",
+            "config": {"workload": "hex_column_r0.05mm_1e8_rays_512x1024", **_cfg_public()}, "impl": "reference",
             "cpu_baseline": {"value": v, "unit": "rays/s", "cores": procs, "kind": "reference",
                              "sample": f"{per} rays per process x {procs} processes per step (disjoint ray ids), "
                                        "reference ice_crystal hex trace + PhaseMassAccumulator"},
@@ -214,7 +214,7 @@ def run_reference_drop(a) -> None:
     line = {"metric": METRIC, "value": v, "unit": "rays/s", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": 1e3 * sum(x["seconds"] for x in vals) / len(vals), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "oblate_drop_config2", **_drop_public()}, "impl": "reference",
+            "config": {"workload": "oblate_drop_1.5mm_1e8_rays_900x1800", **_drop_public()}, "impl": "reference",
             "cpu_baseline": {"value": v, "unit": "rays/s", "cores": procs, "kind": "reference", "sample": sample},
             "e2e": {"value": v, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -417,7 +417,7 @@ def run_b200_hex(a) -> None:
         "metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": 1e3 * t_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "hex_column_config3", **_cfg_public(), "rays_per_gpu": rays,
+        "config": {"workload": "hex_column_r0.05mm_1e8_rays_512x1024", **_cfg_public(), "rays_per_gpu": rays,
                    "l2": "flushed between timed steps (256 MiB write)", "trace_precision": "fp32",
                    "parallelism": f"ray shards x{world}, NCCL all-reduce of FP64 histogram" if world > 1 else "1 GPU"},
         "records_per_s": 1.0 / t_step,
@@ -496,7 +496,7 @@ def run_batched(I, ctx, stream, a, nt: int, np_: int) -> dict:
     e1.record(stream)
     torch.cuda.synchronize()
     t_plain = e0.elapsed_time(e1) / 1e3
-    return {"workload": "batched_drop_records_config4", "records": n, "rays": rays, "seed": 20260101,
+    return {"workload": "batched_drop_records_256_900x1800", "records": n, "rays": rays, "seed": 20260101,
             "cells": [nt, np_], "max_internal_hits": DROP["hits"], "diffraction": "analytic_fraunhofer",
             "ms_per_batch": 1e3 * t, "rays_per_s": rays / t, "records_per_s": n / t,
             "plain_loop": {"seconds": t_plain, "rays_per_s": rays / t_plain, "records_per_s": n / t_plain},
@@ -572,14 +572,14 @@ def run_surrogate(I, ctx, stream, a) -> dict:
     flops = 2.0 * R * sur.cells * (K0 * H + 2 * H * H + H)
     peaks = _peaks()
     bf16 = peaks.get("bf16_tflops", 1590.0)
-    # fresh held-out sample judged by the tracer
-    judge_specs = I.batched_record_specs(a.surrogate_judged, seed=20260103)
-    st = S.TrainSettings(judge_rays=1e8, storage=(ct, cp))
-    ev = S.evaluate(ctx, sur, judge_specs, st)
+    # fresh held-out sample checked by the tracer
+    truth_specs = I.batched_record_specs(a.surrogate_checked, seed=20260103)
+    st = S.TrainSettings(truth_rays=1e8, storage=(ct, cp))
+    ev = S.evaluate(ctx, sur, truth_specs, st)
     sur.close()
     tv = ev["storage"]["tv"]
     return {
-        "workload": "learned_surrogate_config5", "model": S.DEFAULT_MODEL.name, "records": n, "cells": [nt, np_],
+        "workload": "learned_surrogate_256x512", "model": S.DEFAULT_MODEL.name, "records": n, "cells": [nt, np_],
         "storage": [ct, cp], "network": {"hidden": H, "layers": 4, "input_width": K0, "dtype": "bf16 weights and "
                                          "activations, fp32 accumulation (tcgen05, TMEM)"},
         "surrogate_records_per_s": n / t_sur, "served_records_per_s": n / t_serve,
@@ -587,9 +587,9 @@ def run_surrogate(I, ctx, stream, a) -> dict:
         "plain_tracer_records_per_s": n / t_plain,
         "speedup_served_vs_plain": t_plain / t_serve, "speedup_surrogate_only_vs_plain": t_plain / t_sur,
         "kernel_launches_per_serve": launches,
-        "heldout": {"records": len(tv), "judge_rays": 1e8, "tv_storage_mean": ev["storage"]["tv_mean"],
-                    "tv_storage_median": ev["storage"]["tv_median"], "judge_floor_storage": ev["storage"]["floor_mean"],
-                    "tv_cells_mean": ev["cells"]["tv_mean"], "judge_floor_cells": ev["cells"]["floor_mean"],
+        "heldout": {"records": len(tv), "truth_rays": 1e8, "tv_storage_mean": ev["storage"]["tv_mean"],
+                    "tv_storage_median": ev["storage"]["tv_median"], "truth_floor_storage": ev["storage"]["floor_mean"],
+                    "tv_cells_mean": ev["cells"]["tv_mean"], "truth_floor_cells": ev["cells"]["floor_mean"],
                     "pass_fraction_tv_5e-3": ev["pass_fraction"]},
         "roofline_forward": {"kernel": "gemm_persistent_kernel x3 (forward pass)", "bound": "tensor",
                              "achieved": flops / t_fwd / 1e12, "peak": bf16, "unit": "TFLOP/s",
@@ -786,7 +786,7 @@ def run_b200_drop(a) -> None:
         "metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": 1e3 * t_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "oblate_drop_config2", **_drop_public(), "interior_index": n_int,
+        "config": {"workload": "oblate_drop_1.5mm_1e8_rays_900x1800", **_drop_public(), "interior_index": n_int,
                    "rays_per_gpu": rays, "l2": "flushed between timed steps (256 MiB write)", "trace_precision": "fp32",
                    "parallelism": f"ray shards x{world}, NCCL all-reduce of FP64 histogram" if world > 1 else "1 GPU"},
         "records_per_s": 1.0 / t_step,
@@ -837,7 +837,7 @@ def main() -> None:
     p.add_argument("--batch-records", type=int, default=256, help="records of the batched measurement (0 = skip)")
     p.add_argument("--batch-steps", type=int, default=3)
     p.add_argument("--surrogate-records", type=int, default=256, help="records of the surrogate measurement (0 = skip)")
-    p.add_argument("--surrogate-judged", type=int, default=32, help="fresh records judged by 1e8-ray tracer records")
+    p.add_argument("--surrogate-checked", type=int, default=32, help="fresh records checked by 1e8-ray tracer records")
     p.add_argument("--hash-slots", type=int, default=0, help="shared histogram slots (0 = default, 1 = none)")
     p.add_argument("--rays", type=float, default=1e8)
     p.add_argument("--ref-rays", type=float, default=1.6e6, help="reference rays per step (all processes)")

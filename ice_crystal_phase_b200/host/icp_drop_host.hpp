@@ -1,6 +1,6 @@
 // icp_drop_host.hpp -- host-side binary64 inputs of a drop record: shape coefficients, the
 // projected area, the water index and the incident frame.  All run once per record on the
-// CPU (the north star keeps the projected-area integral on the CPU in FP64).
+// CPU; the projected-area integral stays in binary64 on the CPU by design.
 #pragma once
 #include <algorithm>
 #include <array>

@@ -12,11 +12,11 @@ every record with the tracer, one process per record).
 2. Training: Adam with a cosine learning rate over whole records (the loss is the per-record KL
    divergence, which needs every cell of a record), all on the device
    (icp_surrogate_train_step).
-3. Held-out judging: every held-out record is traced twice at half the judge's ray count with
-   independent seeds; the judge is their mean (a record of the full ray count) and half their
-   total-variation distance estimates the judge's own Monte-Carlo noise.  The surrogate's TV
-   against the judge is reported on the cell grid and on a coarser storage grid.
-4. Fallback: a record is served by the surrogate only when its k nearest judged held-out
+3. Held-out truth: every held-out record is traced twice at half the truth's ray count with
+   independent seeds; the truth is their mean (a record of the full ray count) and half their
+   total-variation distance estimates the truth's own Monte-Carlo noise.  The surrogate's TV
+   against the truth is reported on the cell grid and on a coarser storage grid.
+4. Fallback: a record is served by the surrogate only when its k nearest checked held-out
    records (normalised log radius, wavelength, inclination) all passed the TV threshold;
    otherwise, and for every held-out record that failed, the tracer makes it.
 
@@ -56,7 +56,7 @@ class TrainSettings:
     max_internal_hits: int = 10
     rays_max: float = 6e7
     rays_min: float = 1e6
-    judge_rays: float = 1e8
+    truth_rays: float = 1e8
     storage: tuple = (64, 128)
     tv_threshold: float = 5e-3
     neighbours: int = 3
@@ -136,7 +136,7 @@ def mean_loss(sur: I.Surrogate, specs: list, targets) -> float:
 
 def predicted_cells(sur: I.Surrogate, specs: list):
     """Cell probabilities of the records the surrogate emits (icp_surrogate_generate at the full
-    cell grid, so that the judged output is the served one: the network's geometric part plus the
+    cell grid, so that the checked output is the served one: the network's geometric part plus the
     analytic diffraction rows), device float64 [len(specs), nt*np]."""
     torch = _torch()
     R, Cn, nt, np_ = sur.cfg.max_records, sur.cells, sur.cfg.nt, sur.cfg.np
@@ -170,9 +170,9 @@ def tv(a, b):
     return 0.5 * (a - b).abs().sum(dim=1)
 
 
-def judge_records(ctx: I.Context, sur: I.Surrogate, specs: list, judge_rays: float, hits: int = 10):
-    """Two independent tracer records per spec at judge_rays / 2: (their mean, A, B)."""
-    half = int(judge_rays // 2)
+def truth_records(ctx: I.Context, sur: I.Surrogate, specs: list, truth_rays: float, hits: int = 10):
+    """Two independent tracer records per spec at truth_rays / 2: (their mean, A, B)."""
+    half = int(truth_rays // 2)
 
     def twin(sp, salt):
         return I.DropSpec(sp.coefficients, sp.radius_mm, sp.interior_index, half, seed=sp.seed ^ salt,
@@ -185,16 +185,16 @@ def judge_records(ctx: I.Context, sur: I.Surrogate, specs: list, judge_rays: flo
 
 
 def evaluate(ctx: I.Context, sur: I.Surrogate, specs: list, s: TrainSettings) -> dict:
-    """Held-out judgement of the surrogate against the tracer at judge_rays."""
+    """Held-out check of the surrogate against tracer truth records of truth_rays rays."""
     nt, np_ = sur.cfg.nt, sur.cfg.np
     ct, cp = s.storage
-    judge, pa, pb = judge_records(ctx, sur, specs, s.judge_rays, s.max_internal_hits)
+    truth, pa, pb = truth_records(ctx, sur, specs, s.truth_rays, s.max_internal_hits)
     q = predicted_cells(sur, specs)
-    out = {"cell_grid": [nt, np_], "storage_grid": [ct, cp], "judge_rays": s.judge_rays}
+    out = {"cell_grid": [nt, np_], "storage_grid": [ct, cp], "truth_rays": s.truth_rays}
     for name, f in (("cells", lambda x: x), ("storage", lambda x: coarse(x, nt, np_, ct, cp))):
-        t_sur = tv(f(q), f(judge)).cpu().numpy()
-        floor = (0.5 * tv(f(pa), f(pb))).cpu().numpy()  # judge noise: TV(A, B) / 2
-        out[name] = {"tv": t_sur.tolist(), "judge_floor": floor.tolist(), "tv_mean": float(t_sur.mean()),
+        t_sur = tv(f(q), f(truth)).cpu().numpy()
+        floor = (0.5 * tv(f(pa), f(pb))).cpu().numpy()  # truth noise: TV(A, B) / 2
+        out[name] = {"tv": t_sur.tolist(), "truth_floor": floor.tolist(), "tv_mean": float(t_sur.mean()),
                      "tv_median": float(np.median(t_sur)), "floor_mean": float(floor.mean())}
     t = np.asarray(out["storage"]["tv"])
     out["passed"] = (t <= s.tv_threshold).tolist()
@@ -209,7 +209,7 @@ def _key(sp) -> np.ndarray:
 
 @dataclass
 class FallbackGate:
-    """Serve by the surrogate only where the k nearest judged held-out records all passed."""
+    """Serve by the surrogate only where the k nearest checked held-out records all passed."""
     keys: np.ndarray
     passed: np.ndarray
     k: int = 3
@@ -221,7 +221,7 @@ class FallbackGate:
     def trusted(self, sp) -> bool:
         d = np.linalg.norm(self.keys - _key(sp), axis=1)
         if d.min() == 0.0:
-            return bool(self.passed[np.argmin(d)])  # a judged record itself
+            return bool(self.passed[np.argmin(d)])  # a checked record itself
         return bool(self.passed[np.argsort(d)[:self.k]].all())
 
     def as_dict(self) -> dict:
@@ -322,14 +322,14 @@ def init_parameters(cfg: I.SurrogateConfig, seed: int) -> np.ndarray:
 
 
 def run_training(ctx: I.Context, s: TrainSettings, cfg_over: dict | None = None, log=print):
-    """The whole pipeline: training set, training, held-out judgement, fallback gate.  Returns
+    """The whole pipeline: training set, training, held-out check, fallback gate.  Returns
     (surrogate, gate, held-out specs, report)."""
     torch = _torch()
     cfg = I.surrogate_config(**{"max_records": s.batch, **(cfg_over or {})})
     sur = I.Surrogate(ctx, cfg)
     sur.set_parameters(init_parameters(cfg, s.seed))
     # the held-out records come from their own seed, so that runs with different training sets
-    # are judged on the same records
+    # are checked on the same records
     train_specs = I.batched_record_specs(s.records, seed=1000 * s.seed + 1, rays_max=s.rays_max, rays_min=s.rays_min,
                                          diffraction=True)
     held = I.batched_record_specs(s.heldout, seed=1000 * s.seed + 3, rays_max=s.rays_max, rays_min=s.rays_min,
@@ -354,18 +354,18 @@ def run_training(ctx: I.Context, s: TrainSettings, cfg_over: dict | None = None,
     del targets
     t1 = time.perf_counter()
     ev = evaluate(ctx, sur, held, s)
-    t_judge = time.perf_counter() - t1
+    t_truth = time.perf_counter() - t1
     gate = FallbackGate.of(held, ev["passed"], s.neighbours)
     report = {"settings": asdict(s),
               "config": {k: getattr(cfg, k) for k in ("nt", "np", "hidden", "input_width", "theta_frequencies",
                                                       "phi_frequencies", "axis_harmonics")},
               "training_set": {"records": len(train_specs), "rays": rays, "seconds": t_data},
               "training": hist, "heldout_kl_before": loss0, "heldout_kl_after": loss1,
-              "train_kl_after": train_loss, "head_bias": hb, "judge_seconds": t_judge, "heldout": ev,
+              "train_kl_after": train_loss, "head_bias": hb, "truth_seconds": t_truth, "heldout": ev,
               "gate": gate.as_dict()}
     if log:
         log(f"held-out KL {loss0:.4f} -> {loss1:.4f} (train {train_loss:.4f}); TV cells "
-            f"{ev['cells']['tv_mean']:.4f} (judge floor {ev['cells']['floor_mean']:.4f}), storage "
+            f"{ev['cells']['tv_mean']:.4f} (truth floor {ev['cells']['floor_mean']:.4f}), storage "
             f"{ev['storage']['tv_mean']:.4f} (floor {ev['storage']['floor_mean']:.4f}), "
             f"pass {ev['pass_fraction']:.3f}")
     return sur, gate, held, report
@@ -379,7 +379,7 @@ def main(argv=None) -> int:
     for f in ("records", "heldout", "epochs", "batch", "seed", "max_internal_hits", "warmup_steps", "neighbours",
               "large_records"):
         t.add_argument("--" + f.replace("_", "-"), type=int, default=getattr(TrainSettings, f))
-    for f in ("lr", "lr_final", "weight_decay", "rays_max", "rays_min", "judge_rays", "tv_threshold", "large_radius_mm"):
+    for f in ("lr", "lr_final", "weight_decay", "rays_max", "rays_min", "truth_rays", "tv_threshold", "large_radius_mm"):
         t.add_argument("--" + f.replace("_", "-"), type=float, default=getattr(TrainSettings, f))
     t.add_argument("--nt", type=int, default=256)
     t.add_argument("--np", type=int, default=512)

@@ -246,7 +246,8 @@ int icp_hex_generate(icp_context* ctx, const icp_hex_record* record, const icp_o
 /* Host helpers for the drop record inputs (all binary64, CPU):
  *  icp_water_index      IAPWS R9-97 index at the drop's wavelength / temperature / pressure
  *                       (replaces evaluate_water_optics, src/water_refractive_index.cpp:157-187;
- *                       liquid density from Kell's correlation)
+ *                       liquid density from the Tanaka / Kell correlations with the
+ *                       UNESCO-1981 secant bulk modulus)
  *  icp_drop_shape       Table-I coefficients for an equal-volume radius
  *                       (RaindropShape::try_make, include/rainbow/raindrop_shape.hpp:22-67)
  *  icp_drop_projected_area  convex-surface projected area (compute_projected_area,

@@ -118,7 +118,7 @@ def main() -> None:
         ki = (0.8660254037844387, -0.5, 0.0)
         m, d, u = masses(td, 0.05, 0.2, ki, 1.31, 512, 1024, CONFIG3_PLAN, max_hits=12)
         nz = np.flatnonzero(m)
-        np.savez_compressed(HERE / "hex_config3_20k.npz", index=nz, value=m[nz], stats=d, counts=u)
+        np.savez_compressed(HERE / "hex_column_20k.npz", index=nz, value=m[nz], stats=d, counts=u)
         # 3. per-ray reference audits and exits for 48 rays of the config-3 node
         out = td / "t.bin"
         run([REF_BIN / "ref_hex_harness", "trace", "0.05", "0.2", *map(repr, ki), "1.31", "1", 12345, 20000, 1024,

@@ -3,7 +3,7 @@
 FP64 path: cell masses within the reference's own GPU-vs-CPU histogram tolerance
 (2e-11 relative, hex_phase/tests/phase_cuda_tests.cpp:70-107), identical ray and exit
 counts and status histograms, energy balance to 1e-12.
-FP32 path (north-star fast path): total-variation distance of normalised cell mass
+FP32 path (the fast path): total-variation distance of normalised cell mass
 <= 1e-3 against the same-seed FP64 oracle; power is carried in exact fixed point, so the
 energy balance holds to binary64 rounding (1e-12) as in the reference's CLI test.
 """
@@ -49,8 +49,8 @@ def test_fp64_matches_reference_masses(ctx, icp):
     assert abs(acc.forward - d[2]) <= 1e-12 * d[4]
 
 
-def test_fp64_config3_sparse(ctx, icp):
-    g = np.load(GOLDEN / "hex_config3_20k.npz")
+def test_fp64_hex_column_sparse(ctx, icp):
+    g = np.load(GOLDEN / "hex_column_20k.npz")
     plan = icp.parse_orientation_plan("qw,qx,qy,qz,weight,samples,seed\n1,0,0,0,1,20000,12345\n")
     acc = _accumulate(ctx, icp, plan, 0.05, 0.2, CFG3_KI, 1.31, 512, 1024, icp.ICP_FP64, hits=12)
     m = acc.masses()

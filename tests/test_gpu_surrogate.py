@@ -205,8 +205,8 @@ def test_training_lowers_heldout_loss(ctx, icp):
 
 
 def test_trained_network_gains_over_the_tracer(ctx, icp):
-    """What the trained network gains: on fresh records of the batched distribution judged by
-    1e8-ray tracer records, the surrogate's records are closer to the judge (total variation on
+    """What the trained network gains: on fresh records of the batched distribution checked by
+    1e8-ray tracer records, the surrogate's records are closer to the truth (total variation on
     the 64 x 128 storage grid) than the tracer's own records made in the same device time, and
     far closer than the untrained network's."""
     import ctypes as C
@@ -220,10 +220,10 @@ def test_trained_network_gains_over_the_tracer(ctx, icp):
     ct, cp = extra["storage"]
     nt, np_ = sur.cfg.nt, sur.cfg.np
     specs = icp.batched_record_specs(8, seed=4242)
-    st = S.TrainSettings(judge_rays=1e8, storage=(ct, cp))
-    judge, _, _ = S.judge_records(ctx, sur, specs, st.judge_rays)
+    st = S.TrainSettings(truth_rays=1e8, storage=(ct, cp))
+    truth, _, _ = S.truth_records(ctx, sur, specs, st.truth_rays)
     q = S.predicted_cells(sur, specs)
-    tv_sur = S.tv(S.coarse(q, nt, np_, ct, cp), S.coarse(judge, nt, np_, ct, cp)).cpu().numpy()
+    tv_sur = S.tv(S.coarse(q, nt, np_, ct, cp), S.coarse(truth, nt, np_, ct, cp)).cpu().numpy()
     # device time of the surrogate per record
     phi = torch.empty(8 * (cp + 1), dtype=torch.float64, device="cuda")
     theta = torch.empty(8 * cp * (ct + 1), dtype=torch.float64, device="cuda")
@@ -249,11 +249,11 @@ def test_trained_network_gains_over_the_tracer(ctx, icp):
                        inclination_deg=sp.inclination_deg, wavelength_nm=sp.wavelength_nm, diffraction=True)
           for sp in specs]
     p_eq = S.trace_cells(ctx, sur, eq).double()
-    tv_eq = S.tv(S.coarse(p_eq, nt, np_, ct, cp), S.coarse(judge, nt, np_, ct, cp)).cpu().numpy()
+    tv_eq = S.tv(S.coarse(p_eq, nt, np_, ct, cp), S.coarse(truth, nt, np_, ct, cp)).cpu().numpy()
     # the untrained network (the same architecture before learning)
     sur.set_parameters(S.init_parameters(sur.cfg, 7))
     q0 = S.predicted_cells(sur, specs)
-    tv_untrained = S.tv(S.coarse(q0, nt, np_, ct, cp), S.coarse(judge, nt, np_, ct, cp)).cpu().numpy()
+    tv_untrained = S.tv(S.coarse(q0, nt, np_, ct, cp), S.coarse(truth, nt, np_, ct, cp)).cpu().numpy()
     sur.close()
     assert tv_sur.mean() < tv_eq.mean(), (tv_sur.mean(), tv_eq.mean(), n_eq)
     assert tv_sur.mean() < 0.2 * tv_untrained.mean(), (tv_sur.mean(), tv_untrained.mean())

@@ -50,8 +50,8 @@ def test_two_orientation_cdf_bit_exact(oracle):
     assert cdf.report["coarsening_tv"] == meta[2]
 
 
-def test_config3_masses_bit_exact(oracle):
-    g = np.load(GOLDEN / "hex_config3_20k.npz")
+def test_hex_column_masses_bit_exact(oracle):
+    g = np.load(GOLDEN / "hex_column_20k.npz")
     nodes = oracle.parse_plan("qw,qx,qy,qz,weight,samples,seed\n1,0,0,0,1,20000,12345\n")
     rec = oracle.hex_record(0.05, 0.2, CFG3_KI, 1.31, 1.0, 512, 1024, nodes, max_hits=12)
     nz = np.flatnonzero(rec.masses)

@@ -128,8 +128,8 @@ def test_axis_harmonics_are_the_angle_to_the_drop_axis(icp):
 
 
 def test_fallback_gate_rules(icp):
-    """The gate trusts a judged record by its own verdict, any other record only when its k
-    nearest judged records (normalised log radius, wavelength, inclination) all passed; it survives
+    """The gate trusts a checked record by its own verdict, any other record only when its k
+    nearest checked records (normalised log radius, wavelength, inclination) all passed; it survives
     the round trip through the model file's JSON."""
     import json
 
@@ -138,10 +138,10 @@ def test_fallback_gate_rules(icp):
     def spec(r, lam, inc):
         return icp.DropSpec([0.0] * 8, r, 1.33, 1, seed=1, inclination_deg=inc, wavelength_nm=lam)
 
-    judged = [spec(0.2, 500, 0), spec(0.21, 505, 2), spec(0.19, 495, -2), spec(2.5, 600, 40), spec(2.6, 610, 45),
+    checked = [spec(0.2, 500, 0), spec(0.21, 505, 2), spec(0.19, 495, -2), spec(2.5, 600, 40), spec(2.6, 610, 45),
               spec(2.4, 590, 35)]
-    gate = S.FallbackGate.of(judged, [True, True, True, True, False, True], k=3)
-    assert gate.trusted(judged[0]) and not gate.trusted(judged[4])
+    gate = S.FallbackGate.of(checked, [True, True, True, True, False, True], k=3)
+    assert gate.trusted(checked[0]) and not gate.trusted(checked[4])
     assert gate.trusted(spec(0.2, 501, 1))          # all three neighbours passed
     assert not gate.trusted(spec(2.5, 601, 41))     # a failed neighbour among the three
     back = S.FallbackGate.from_dict(json.loads(json.dumps(gate.as_dict())))
