@@ -92,6 +92,8 @@ bool config_valid(const icp_surrogate_config* g)
     if (g->axis_harmonics % 8u) return false;
     if (4u + 2u * g->theta_frequencies + g->phi_frequencies + g->axis_harmonics > g->input_width - 16u) return false;
     if (!g->max_records || g->max_records > 256) return false;
+    // the rows of a call (records x cells) are 32-bit GEMM sizes and signed 32-bit TMA coordinates
+    if ((uint64_t)g->max_records * g->nt * g->np > (1ull << 31)) return false;
     const double* r[3] = {g->log_radius_mm, g->wavelength_nm, g->log_wavelength_over_radius};
     for (auto* x : r)
         if (!(std::isfinite(x[0]) && std::isfinite(x[1]) && x[1] > x[0])) return false;

@@ -380,7 +380,8 @@ typedef struct {
     uint32_t input_width;          /* 64 or 128: 16 record features, then the cell features     */
     uint32_t theta_frequencies;    /* sin / cos (k theta), k = 1..F                             */
     uint32_t phi_frequencies;      /* cos (l (phi - pi/2)), l = 1..G                            */
-    uint32_t max_records;          /* records per call (sizes the activation buffers)          */
+    uint32_t max_records;          /* records per call (sizes the activation buffers);          */
+                                   /* max_records * nt * np <= 2^31                             */
     uint32_t axis_harmonics;       /* P: T_k(cos psi), k = 1..P, in the last P input columns;   */
                                    /* psi = angle of the cell's direction to the drop's axis,   */
                                    /* P % 8 == 0, 4 + 2F + G + P <= width - 16                  */

@@ -93,7 +93,8 @@ def test_oracle_emulation_only_rounds():
 def test_config_validation(icp):
     for bad in [{"hidden": 96}, {"input_width": 96}, {"theta_frequencies": 60}, {"nt": 3, "np": 5},
                 {"axis_harmonics": 4}, {"axis_harmonics": 32},
-                {"max_records": 0}, {"wavelength_nm": (700.0, 400.0)}, {"index_scale": 0.0}]:
+                {"max_records": 0}, {"wavelength_nm": (700.0, 400.0)}, {"index_scale": 0.0},
+                {"max_records": 256, "nt": 4096, "np": 4096}]:  # 2^32 rows in one call
         cfg = icp.surrogate_config(**bad)
         with pytest.raises(icp.InvalidArgument):
             icp.surrogate_parameter_count(cfg)
