@@ -720,6 +720,8 @@ int icp_mlp_gemm_bf16(icp_context* c, const void* d_a, const void* d_b, uint32_t
     if (!c || !d_a || !d_b || !d_c) return fail(ICP_ERR_INVALID_ARGUMENT, "icp_mlp_gemm_bf16: null argument");
     if (!m || m % 128 || !k || k % 64 || (n != 64 && n != 128 && n != 256))
         return fail(ICP_ERR_INVALID_ARGUMENT, "GEMM shape: M multiple of 128, N in {64,128,256}, K multiple of 64");
+    if (m > (1u << 31) || k > (1u << 31)) // tile coordinates are signed 32-bit
+        return fail(ICP_ERR_INVALID_ARGUMENT, "GEMM shape: M and K at most 2^31");
     if ((reinterpret_cast<uintptr_t>(d_a) | reinterpret_cast<uintptr_t>(d_b)) & 15)
         return fail(ICP_ERR_INVALID_ARGUMENT, "GEMM operands must be 16-byte aligned");
     if (!accumulate && split_k > 1) return fail(ICP_ERR_INVALID_ARGUMENT, "split-K needs accumulate");

@@ -359,7 +359,7 @@ int icp_drop_batch_autotune(icp_context* ctx, const icp_drop_item* items, uint32
 /* Building block of the learned surrogate's dense layers (no reference counterpart): BF16
  * C[m x n] = A[m x k] * B[n x k]^T on the 5th-generation tensor cores with FP32 accumulation in
  * tensor memory (tcgen05.mma, TMA-fed).  A and B row-major (K contiguous), 16-byte aligned;
- * m % 128 == 0, n in {64, 128, 256}, k % 64 == 0.  accumulate = 0: C is written (split_k must
+ * m % 128 == 0, n in {64, 128, 256}, k % 64 == 0, m and k at most 2^31.  accumulate = 0: C is written (split_k must
  * be 1); accumulate = 1: C += A B^T with the K range split over split_k CTAs per row tile. */
 int icp_mlp_gemm_bf16(icp_context* ctx, const void* d_a, const void* d_b, uint32_t m, uint32_t n, uint32_t k,
                       uint32_t split_k, float* d_c, int accumulate);
