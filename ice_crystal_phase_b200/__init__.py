@@ -167,6 +167,11 @@ class BatchSettings(C.Structure):
                 ("use_graph", C.c_uint32)]
 
 
+class IceState(C.Structure):
+    _fields_ = [("wavelength_nm", C.c_double), ("n", C.c_double), ("kappa", C.c_double), ("lower_nm", C.c_double),
+                ("upper_nm", C.c_double), ("log_wavelength_fraction", C.c_double)]
+
+
 class SurrogateConfig(C.Structure):
     _fields_ = [("nt", C.c_uint32), ("np", C.c_uint32), ("hidden", C.c_uint32), ("input_width", C.c_uint32),
                 ("theta_frequencies", C.c_uint32), ("phi_frequencies", C.c_uint32), ("max_records", C.c_uint32),
@@ -197,6 +202,7 @@ _FUNCS = {
     "icp_memcpy_d2h": (C.c_int, [_P, _P, _P, C.c_size_t]),
     "icp_memset_d": (C.c_int, [_P, _P, C.c_int, C.c_size_t]),
     "icp_u_edges": (C.c_int, [C.c_uint32, _D]),
+    "icp_ice_index": (C.c_int, [C.c_double, C.POINTER(IceState)]),
     "icp_hex_node_area": (C.c_int, [C.POINTER(HexNode), C.POINTER(Grid), _D]),
     "icp_hex_trace_bin": (C.c_int, [_P, C.POINTER(HexNode), C.POINTER(Grid), _P, _P, C.POINTER(TraceStats), _P,
                                     C.POINTER(Tuning)]),
@@ -283,6 +289,15 @@ def u_edges(nt: int) -> np.ndarray:
     e = np.empty(nt + 1)
     check(LIB.icp_u_edges(nt, e.ctypes.data_as(_D)))
     return e
+
+
+def evaluate_ice_optics(vacuum_wavelength_nm: float) -> IceState:
+    """Refractive index of ice Ih (Warren & Brandt 2008) at a vacuum wavelength in 200..1100 nm
+    (evaluate_ice_wb2008, hex_atlas/src/ice_optics.cpp:13-30): the interior index of a prism
+    record at that wavelength.  Raises InvalidArgument outside the table."""
+    st = IceState()
+    check(LIB.icp_ice_index(float(vacuum_wavelength_nm), C.byref(st)))
+    return st
 
 
 def _normalize(a):

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/icp_b200.h"
+#include "../host/icp_ice_optics.hpp"
 #include "../host/icp_host_math.hpp"
 #include "icp_internal.h"
 
@@ -174,6 +175,24 @@ int icp_memset_d(icp_context* c, void* dst, int value, size_t bytes)
     ICP_CUDA(cudaSetDevice(c->device));
     ICP_CUDA(cudaMemsetAsync(dst, value, bytes, c->stream));
     ICP_CUDA(cudaStreamSynchronize(c->stream));
+    return ok();
+}
+
+int icp_ice_index(double wavelength_nm, icp_ice_state* out)
+{
+    if (!out) return fail(ICP_ERR_INVALID_ARGUMENT, "icp_ice_index: null argument");
+    std::memset(out, 0, sizeof *out);
+    if (!std::isfinite(wavelength_nm) || wavelength_nm < 200.0 || wavelength_nm > 1100.0)
+        return fail(ICP_ERR_INVALID_ARGUMENT,
+                    "Warren-Brandt 2008 ice: supported vacuum wavelengths are 200..1100 nm; no extrapolation.");
+    H::IceIndex v{};
+    if (!H::ice_index_wb2008(wavelength_nm, v)) return fail(ICP_ERR_AUDIT, "Invalid ice optical state.");
+    out->wavelength_nm = wavelength_nm;
+    out->n = v.n;
+    out->kappa = v.kappa;
+    out->lower_nm = v.lower_nm;
+    out->upper_nm = v.upper_nm;
+    out->log_wavelength_fraction = v.fraction;
     return ok();
 }
 

@@ -86,6 +86,19 @@ typedef struct {
  * include/rainbow/phase_cdf_math.hpp:16-32). Host function, no device use. */
 int icp_u_edges(uint32_t nt, double* edges_out);
 
+/* Refractive index of ice Ih at a vacuum wavelength (replaces evaluate_ice_wb2008,
+ * hex_atlas/src/ice_optics.cpp:13-30): the Warren & Brandt (2008) table, real index linear and
+ * imaginary index log-linear in log(wavelength) between its rows; 200..1100 nm, no
+ * extrapolation (ICP_ERR_INVALID_ARGUMENT outside).  The tracer uses n; kappa is reported, not
+ * applied.  Host function, no device use. */
+typedef struct {
+    double wavelength_nm;
+    double n, kappa;
+    double lower_nm, upper_nm;      /* bracketing table wavelengths (equal at a table row)     */
+    double log_wavelength_fraction; /* ln(lambda / lower) / ln(upper / lower), 0 at a row      */
+} icp_ice_state;
+int icp_ice_index(double wavelength_nm, icp_ice_state* out);
+
 /* Statistics of one trace+bin call (raw sums in units of incident power per ray;
  * multiply by the per-ray area weight to obtain mm^2). */
 typedef struct {

@@ -8,6 +8,7 @@
 #   oracle/_ref/ref_hex_harness          oracle/ref_hex_harness.cpp over the same sources
 #   oracle/_ref/ref_drop_harness         oracle/ref_drop_harness.cpp over the header-only drop
 #                                        tracer, src/projected_area.cpp, src/water_refractive_index.cpp
+#   oracle/_ref/ref_ice_harness          oracle/ref_ice_harness.cpp over hex_atlas/src/ice_optics.cpp
 #
 # Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
 set -euo pipefail
@@ -28,4 +29,8 @@ g++ "${flags[@]}" "$ref/hex_phase/apps/generate_hex_phase.cpp" "${srcs[@]}" -o "
 g++ "${flags[@]}" "$here/ref_hex_harness.cpp" "${srcs[@]}" -o "$out/ref_hex_harness"
 g++ -std=c++20 -O2 -fno-fast-math -ffp-contract=off -I"$ref/include" "$here/ref_drop_harness.cpp" \
     "$ref/src/projected_area.cpp" "$ref/src/water_refractive_index.cpp" -o "$out/ref_drop_harness"
-echo "built $out/ice_generate_phase_cpu $out/ref_hex_harness $out/ref_drop_harness"
+if [ -f "$ref/hex_atlas/src/ice_optics.cpp" ]; then
+    g++ -std=c++20 -O2 -fno-fast-math -ffp-contract=off -I"$ref/hex_atlas/include" "$here/ref_ice_harness.cpp" \
+        "$ref/hex_atlas/src/ice_optics.cpp" -o "$out/ref_ice_harness"
+fi
+echo "built $out/ice_generate_phase_cpu $out/ref_hex_harness $out/ref_drop_harness $out/ref_ice_harness"

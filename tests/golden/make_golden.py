@@ -10,6 +10,7 @@ the fixtures are committed so that tests never need it.
 from __future__ import annotations
 
 import json
+import math
 import subprocess
 import sys
 import tempfile
@@ -28,7 +29,7 @@ TWO_ORIENTATIONS = ("qw,qx,qy,qz,weight,samples,seed\n"
                     "1,0,0,0,0.5,1024,12345\n"
                     "0.7071067811865475244,0,0,0.7071067811865475244,0.5,2048,54321\n")
 # Config-3 geometry: circumradius 0.05 mm, length 0.2 mm, n = 1.31, ki = (cos30, -sin30, 0).
-CONFIG3_PLAN = "qw,qx,qy,qz,weight,samples,seed\n1,0,0,0,1,20000,12345\n"
+COLUMN_PLAN = "qw,qx,qy,qz,weight,samples,seed\n1,0,0,0,1,20000,12345\n"
 
 
 def run(cmd):
@@ -92,6 +93,29 @@ def drop_fixtures(td: Path) -> None:
                         family_cases=np.array([[r, s, n, *k, g] for r, s, n, k, g in FAMILY_CASES]), **fam)
 
 
+def ice_fixtures() -> None:
+    """Ice Ih index (hex_atlas/src/ice_optics.cpp) at every table wavelength in range, the
+    geometric midpoints, 400 seeded random wavelengths and the domain edges, exact."""
+    knots = [199, 201, 201.9, 210, 250, 300, 350, 390, 400] + list(range(410, 1101, 10))
+    wl = [float(k) for k in knots] + [math.sqrt(a * b) for a, b in zip(knots, knots[1:])]
+    wl += [float(x) for x in np.random.default_rng(2008).uniform(200.0, 1100.0, 400)]
+    wl += [200.0, 1100.0, 199.99999, 1100.00001, 0.0, -5.0, math.inf, math.nan, 555.5, 1099.9999999]
+    r = subprocess.run([str(REF_BIN / "ref_ice_harness")], input="\n".join(repr(x) for x in wl) + "\n",
+                       capture_output=True, text=True, check=True)
+    status, vals = [], []
+    for line in r.stdout.splitlines():
+        f = line.split()
+        if f[0] == "ok":
+            status.append(0)
+            vals.append([float.fromhex(x) for x in f[1:]])
+        else:
+            status.append(1 if f[0] == "invalid" else 2)
+            vals.append([math.nan] * 5)
+    assert len(status) == len(wl)
+    np.savez_compressed(HERE / "ice_wb2008.npz", wavelength_nm=np.array(wl), status=np.array(status),
+                        values=np.array(vals))
+
+
 def main() -> None:
     subprocess.run([str(ROOT / "oracle" / "build_ref.sh"), str(REF)], check=True)
     with tempfile.TemporaryDirectory() as t:
@@ -114,12 +138,12 @@ def main() -> None:
                            meta["transport_audit"]["unresolved_mm2"], meta["geometry"]["projected_area_mm2"],
                            meta["histogram"]["mass_mm2"], meta["histogram"]["g_rays"]]),
             sampling_frame_columns=np.array(meta["sampling_frame_columns"]))
-        # 2. config-3 geometry at 512x1024, 20k rays, 12 hits (sparse: the masses are a few hundred deltas)
+        # 2. the hex column (circumradius 0.05 mm, length 0.2 mm) at 512x1024, 20k rays, 12 hits (sparse: the masses are a few hundred deltas)
         ki = (0.8660254037844387, -0.5, 0.0)
-        m, d, u = masses(td, 0.05, 0.2, ki, 1.31, 512, 1024, CONFIG3_PLAN, max_hits=12)
+        m, d, u = masses(td, 0.05, 0.2, ki, 1.31, 512, 1024, COLUMN_PLAN, max_hits=12)
         nz = np.flatnonzero(m)
         np.savez_compressed(HERE / "hex_column_20k.npz", index=nz, value=m[nz], stats=d, counts=u)
-        # 3. per-ray reference audits and exits for 48 rays of the config-3 node
+        # 3. per-ray reference audits and exits for 48 rays of the hex column node
         out = td / "t.bin"
         run([REF_BIN / "ref_hex_harness", "trace", "0.05", "0.2", *map(repr, ki), "1.31", "1", 12345, 20000, 1024,
              repr(1e-12), 100, 48, out])
@@ -129,6 +153,8 @@ def main() -> None:
         np.savez_compressed(HERE / "hex_rays.npz", info=info, exits=exits)
         # 4. drops: host inputs and the four-family path tracer
         drop_fixtures(td)
+        # 5. ice Ih index of the prism records
+        ice_fixtures()
     for f in sorted(HERE.glob("*.npz")):
         print(f.name, f.stat().st_size)
 
