@@ -172,6 +172,35 @@ class IceState(C.Structure):
                 ("upper_nm", C.c_double), ("log_wavelength_fraction", C.c_double)]
 
 
+class AtlasRay(C.Structure):
+    _fields_ = [("face", C.c_uint32), ("reserved", C.c_uint32), ("x", C.c_double), ("y", C.c_double),
+                ("z", C.c_double), ("weight_mm2", C.c_double)]
+
+
+class AtlasIncident(C.Structure):
+    _fields_ = [("theta", C.c_double), ("phi", C.c_double), ("ki", C.c_double * 3), ("e0", C.c_double * 3),
+                ("e1", C.c_double * 3)]
+
+
+class AtlasSettings(C.Structure):
+    _fields_ = [("circumradius_mm", C.c_double), ("length_mm", C.c_double), ("interior_index", C.c_double),
+                ("exterior_index", C.c_double), ("theta_intervals", C.c_uint32), ("phi_intervals", C.c_uint32),
+                ("nt", C.c_uint32), ("np", C.c_uint32), ("subdivisions", C.c_uint32),
+                ("max_internal_hits", C.c_uint32), ("tail_tolerance", C.c_double),
+                ("max_unresolved_fraction", C.c_double), ("max_balance_error", C.c_double)]
+
+
+class AtlasNodeReport(C.Structure):
+    _fields_ = [("projected_area_mm2", C.c_double), ("escaped_mm2", C.c_double), ("unresolved_mm2", C.c_double),
+                ("histogram_mass_mm2", C.c_double), ("histogram_relative_error", C.c_double),
+                ("max_balance_error", C.c_double), ("max_interface_balance_error", C.c_double),
+                ("rays", C.c_uint64), ("outputs", C.c_uint64), ("invalid_bins", C.c_uint64),
+                ("status", C.c_uint64 * 8), ("first_rejected", C.c_int64)]
+
+    def as_dict(self) -> dict:
+        return {k: (list(getattr(self, k)) if k == "status" else getattr(self, k)) for k, _ in self._fields_}
+
+
 class SurrogateConfig(C.Structure):
     _fields_ = [("nt", C.c_uint32), ("np", C.c_uint32), ("hidden", C.c_uint32), ("input_width", C.c_uint32),
                 ("theta_frequencies", C.c_uint32), ("phi_frequencies", C.c_uint32), ("max_records", C.c_uint32),
@@ -246,6 +275,15 @@ _FUNCS = {
     "icp_surrogate_generate": (C.c_int, [_P, C.POINTER(DropItem), C.c_uint32, C.c_uint32, C.c_uint32,
                                          C.POINTER(CdfPolicy), _P, _P, C.POINTER(CdfReport)]),
     "icp_surrogate_targets": (C.c_int, [_P, _P, _P, C.c_uint32, _P]),
+    "icp_atlas_area_rule": (C.c_int, [C.c_double, C.c_double, _D, C.c_uint32, C.POINTER(AtlasRay), C.c_uint64,
+                                      C.POINTER(C.c_uint64)]),
+    "icp_atlas_incident_node": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                          C.POINTER(AtlasIncident)]),
+    "icp_atlas_trace_node": (C.c_int, [_P, C.POINTER(AtlasSettings), C.c_uint32, C.c_uint32, _P,
+                                       C.POINTER(AtlasNodeReport)]),
+    "icp_atlas_coupling": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_double, C.c_double, _D, _P, _P,
+                                     C.c_uint64, _D, C.c_double, C.c_int, _P, _D]),
+    "icp_atlas_compose": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, _P, _P, _P]),
 }
 
 
@@ -298,6 +336,29 @@ def evaluate_ice_optics(vacuum_wavelength_nm: float) -> IceState:
     st = IceState()
     check(LIB.icp_ice_index(float(vacuum_wavelength_nm), C.byref(st)))
     return st
+
+
+def atlas_area_rule(circumradius_mm: float, length_mm: float, ki, subdivisions: int):
+    """Projected-area quadrature of the prism lit from ki (atlas::make_area_rule,
+    hex_atlas/src/atlas.cpp:11-51): (faces[n], points[n][3] in units of the circumradius,
+    weights_mm2[n])."""
+    k = (C.c_double * 3)(*map(float, ki))
+    n = C.c_uint64()
+    check(LIB.icp_atlas_area_rule(float(circumradius_mm), float(length_mm), k, int(subdivisions), None, 0,
+                                  C.byref(n)))
+    rays = (AtlasRay * max(1, n.value))()
+    check(LIB.icp_atlas_area_rule(float(circumradius_mm), float(length_mm), k, int(subdivisions), rays, n.value,
+                                  C.byref(n)))
+    a = np.frombuffer(rays, dtype=np.dtype([("face", "<u4"), ("reserved", "<u4"), ("x", "<f8"), ("y", "<f8"),
+                                            ("z", "<f8"), ("w", "<f8")]), count=n.value)
+    return a["face"].copy(), np.stack([a["x"], a["y"], a["z"]], axis=1), a["w"].copy()
+
+
+def atlas_incident_node(theta_intervals: int, phi_intervals: int, i: int, j: int) -> AtlasIncident:
+    """Incident node (i, j) of the symmetry domain (the frame part of atlas::make_node)."""
+    out = AtlasIncident()
+    check(LIB.icp_atlas_incident_node(int(theta_intervals), int(phi_intervals), int(i), int(j), C.byref(out)))
+    return out
 
 
 def _normalize(a):

@@ -117,8 +117,12 @@ int icp_context_destroy(icp_context* c)
     if (!c) return ok();
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    Scratch* all[] = {&c->stats, &c->edges_f, &c->cdf_partial, &c->cdf_report, &c->cdf_sync, &c->cdf_colsum,
-                      &c->rec_edges, &c->rec_mass, &c->rec_phi, &c->rec_theta, &c->rec_batch, &c->rows};
+    Scratch* all[] = {&c->stats,      &c->edges_f,    &c->cdf_partial,  &c->cdf_report,  &c->cdf_sync,
+                      &c->cdf_colsum, &c->rec_edges,  &c->rec_mass,     &c->rec_phi,     &c->rec_theta,
+                      &c->rec_batch,  &c->rows,       &c->dargs,        &c->b_table,     &c->b_chunks,
+                      &c->b_queue,    &c->b_stats,    &c->b_mass,       &c->b_rows,      &c->b_dargs,
+                      &c->b_reports,  &c->b_sync,     &c->b_phi,        &c->b_theta,     &c->mlp_error,
+                      &c->cdfb_partial, &c->cdfb_colsum, &c->cdfb_recs, &c->atlas_trace, &c->atlas_coupling};
     for (Scratch* s : all) s->release();
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);

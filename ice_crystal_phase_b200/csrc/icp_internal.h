@@ -264,5 +264,7 @@ struct icp_context {
     icp::Scratch mlp_error;
     // batched CDF builds
     icp::Scratch cdfb_partial, cdfb_colsum, cdfb_recs;
+    // deterministic atlas: per-node trace scratch, coupling accumulators
+    icp::Scratch atlas_trace, atlas_coupling;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
 };

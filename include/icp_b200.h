@@ -455,6 +455,105 @@ int icp_surrogate_generate(icp_surrogate* s, const icp_drop_item* items, uint32_
 int icp_surrogate_targets(icp_surrogate* s, const double* d_phi, const double* d_theta, uint32_t count,
                           float* d_target);
 
+/* --------------------------------------------------------------------- deterministic atlas
+ * Fixed-incidence responses of one hexagonal prism on a grid of incident directions in the
+ * symmetry domain (theta in [0, pi/2] from the body +y axis, phi in [0, pi/6]), then reused by
+ * a deterministic orientation composition.  No random numbers anywhere: entry points come
+ * from a projected-area quadrature, orientations from a fixed product rule. */
+
+/* One quadrature ray: entry face, entry point in units of the circumradius (body frame), and
+ * its projected-area weight in mm^2.  40 bytes. */
+typedef struct {
+    uint32_t face;
+    uint32_t reserved;
+    double x, y, z;
+    double weight_mm2;
+} icp_atlas_ray;
+
+/* Projected-area quadrature of the prism lit from unit direction ki (normalised as the
+ * tracer does): S x S equal-area cells per lit side face and per end-cap sector, 2 x 3
+ * Gauss-Legendre points per cell; replaces atlas::make_area_rule
+ * (hex_atlas/include/ice_crystal/atlas.hpp:17, hex_atlas/src/atlas.cpp:11-51).  rays == NULL
+ * returns the count only; otherwise capacity must hold it (ICP_ERR_CAPACITY).  Invalid
+ * geometry or S (S*S > 10^6) -> ICP_ERR_INVALID_ARGUMENT; a point on an ambiguous boundary or
+ * a failed area audit (1e-12) -> ICP_ERR_AUDIT. */
+int icp_atlas_area_rule(double circumradius_mm, double length_mm, const double ki[3], uint32_t subdivisions,
+                        icp_atlas_ray* rays, uint64_t capacity, uint64_t* count);
+
+typedef struct {
+    double theta, phi;  /* node angles (rad) */
+    double ki[3];       /* incident propagation direction of the trace */
+    double e0[3], e1[3];/* its spherical frame: e0 = (cos t cos p, -sin t, cos t sin p), e1 = ki x e0 */
+} icp_atlas_incident;
+
+/* Incident node (i, j) of theta_intervals x phi_intervals (end points included); replaces the
+ * frame part of atlas::make_node (hex_atlas/src/atlas.cpp:76-97). */
+int icp_atlas_incident_node(uint32_t theta_intervals, uint32_t phi_intervals, uint32_t i, uint32_t j,
+                            icp_atlas_incident* out);
+
+typedef struct {
+    double circumradius_mm, length_mm;
+    double interior_index, exterior_index;
+    uint32_t theta_intervals, phi_intervals; /* incident grid, <= 4096 each */
+    uint32_t nt, np;                         /* outgoing cell grid, nt*np <= 10^8 */
+    uint32_t subdivisions;                   /* area quadrature S, S*S <= 10^6 */
+    uint32_t max_internal_hits;              /* 2048 */
+    double tail_tolerance;                   /* 1e-12 */
+    double max_unresolved_fraction;          /* 1e-10 */
+    double max_balance_error;                /* 1e-10 */
+} icp_atlas_settings;
+
+typedef struct {
+    double projected_area_mm2;   /* analytic projected area at the node */
+    double escaped_mm2;          /* sum over rays of weight x escaped power (ray order, Kahan) */
+    double unresolved_mm2;       /* the same for the power left in the chain */
+    double histogram_mass_mm2;   /* sum of the node's cell masses */
+    double histogram_relative_error;
+    double max_balance_error, max_interface_balance_error;
+    uint64_t rays, outputs, invalid_bins;
+    uint64_t status[8];          /* rays per icp_ray_status */
+    int64_t first_rejected;      /* quadrature index of the first rejected ray, -1 if none */
+} icp_atlas_node_report;
+
+/* Traces every quadrature ray of incident node (i, j) on the device (FP64, each ray's linear
+ * R/T chain as the prism tracer) and writes the node's cell masses in mm^2 to
+ * d_mass[nt*np] (device, theta-major; pole exits spread uniformly over the end rows).  The
+ * histogram is accumulated in exact 64-bit fixed point (2^-62 of the node's projected
+ * area), so the result does not depend on thread scheduling; no floating-point atomics.
+ * Replaces atlas::CudaTracer::trace (hex_atlas/include/ice_crystal/atlas_cuda.hpp:15,
+ * hex_atlas/src/atlas_cuda.cpp:30-58) and atlas::trace_cpu (atlas.cpp:140-153), with the
+ * same gates: every ray accepted with interface balance <= max_balance_error
+ * (ICP_ERR_AUDIT naming the first rejected ray), histogram / escaped and
+ * (escaped + unresolved) / area within max_balance_error, unresolved / area <=
+ * max_unresolved_fraction. */
+int icp_atlas_trace_node(icp_context* ctx, const icp_atlas_settings* settings, uint32_t i, uint32_t j,
+                         double* d_mass, icp_atlas_node_report* report);
+
+/* Orientation coupling of one incident direction: for every rotation r (d_rotations[n][9],
+ * row-major body -> ensemble, device) with number weight d_weights[n] (device), the body
+ * direction r^T ki is folded into the symmetry domain by one of the 24 operations of D6h
+ * (reflections included), the node response is interpolated bilinearly in (theta, phi) after
+ * division by the node areas h_node_area[(T+1)*(P+1)] (host), weighted by the exact
+ * projected area at the query and shifted in phi by the (fractional) cell offset of the
+ * folded frame.  Adds fraction x weights into d_coupling[(T+1)(P+1)][2][np] (device,
+ * [node][parity][shift]; parity 1 = phi reflected), after replacing each [node][parity]
+ * row by its mean when orbit_average != 0 (exact average over a uniform world azimuth, used
+ * at vertical incidence).  Accumulation is exact fixed point (order-independent).  Replaces
+ * coupling / coupling_for_rule (hex_atlas/python/atlas_math.py:272-428).  *expected_area =
+ * sum of weight x projected area (mm^2, before the fraction).  A fold outside the domain or
+ * an inconsistent unfolding -> ICP_ERR_AUDIT. */
+int icp_atlas_coupling(icp_context* ctx, uint32_t theta_intervals, uint32_t phi_intervals, uint32_t np,
+                       double circumradius_mm, double length_mm, const double* h_node_area,
+                       const double* d_rotations, const double* d_weights, uint64_t count, const double ki[3],
+                       double fraction, int orbit_average, double* d_coupling, double* expected_area);
+
+/* Composed cell mass d_out[nt*np] (device) = sum over nodes n, parities q and shifts s of
+ * d_coupling[n][q][s] x (the node's cell masses d_mass[n][nt][np], phi-reflected when q = 1,
+ * rolled by s cells in phi): a non-negative direct cyclic convolution in FP64 with a fixed
+ * summation order per cell.  Replaces compose_mass (atlas_math.py:431-447). */
+int icp_atlas_compose(icp_context* ctx, uint32_t nodes, uint32_t nt, uint32_t np, const double* d_mass,
+                      const double* d_coupling, double* d_out);
+
 #ifdef __cplusplus
 }
 #endif

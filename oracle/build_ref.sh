@@ -9,6 +9,8 @@
 #   oracle/_ref/ref_drop_harness         oracle/ref_drop_harness.cpp over the header-only drop
 #                                        tracer, src/projected_area.cpp, src/water_refractive_index.cpp
 #   oracle/_ref/ref_ice_harness          oracle/ref_ice_harness.cpp over hex_atlas/src/ice_optics.cpp
+#   oracle/_ref/ref_atlas_harness        oracle/ref_atlas_harness.cpp over hex_atlas/src/atlas.cpp and
+#                                        hex_trace/src/hex_trace.cpp (area rule, atlas nodes)
 #
 # Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
 set -euo pipefail
@@ -32,5 +34,7 @@ g++ -std=c++20 -O2 -fno-fast-math -ffp-contract=off -I"$ref/include" "$here/ref_
 if [ -f "$ref/hex_atlas/src/ice_optics.cpp" ]; then
     g++ -std=c++20 -O2 -fno-fast-math -ffp-contract=off -I"$ref/hex_atlas/include" "$here/ref_ice_harness.cpp" \
         "$ref/hex_atlas/src/ice_optics.cpp" -o "$out/ref_ice_harness"
+    g++ "${flags[@]}" -I"$ref/hex_atlas/include" "$here/ref_atlas_harness.cpp" "$ref/hex_atlas/src/atlas.cpp" \
+        "$ref/hex_trace/src/hex_trace.cpp" -o "$out/ref_atlas_harness"
 fi
-echo "built $out/ice_generate_phase_cpu $out/ref_hex_harness $out/ref_drop_harness $out/ref_ice_harness"
+echo "built $out/ice_generate_phase_cpu $out/ref_hex_harness $out/ref_drop_harness $out/ref_ice_harness $out/ref_atlas_harness"

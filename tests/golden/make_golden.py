@@ -1,7 +1,8 @@
 """Regenerates the golden fixtures in tests/golden/ from the REFERENCE implementation.
 
 Runs the reference's own CPU code, compiled from its sources by oracle/build_ref.sh into
-oracle/_ref/ (ice_generate_phase_cpu and the ref_hex_harness / ref_drop_harness drivers),
+oracle/_ref/ (ice_generate_phase_cpu and the ref_*_harness drivers), imports the reference's
+Python atlas composition (hex_atlas/python/atlas_math.py),
 and stores its outputs as small .npz files.  Needs the reference checkout (default /root/reference);
 the fixtures are committed so that tests never need it.
 
@@ -28,7 +29,7 @@ REF_BIN = ROOT / "oracle" / "_ref"
 TWO_ORIENTATIONS = ("qw,qx,qy,qz,weight,samples,seed\n"
                     "1,0,0,0,0.5,1024,12345\n"
                     "0.7071067811865475244,0,0,0.7071067811865475244,0.5,2048,54321\n")
-# Config-3 geometry: circumradius 0.05 mm, length 0.2 mm, n = 1.31, ki = (cos30, -sin30, 0).
+# Hex column: circumradius 0.05 mm, length 0.2 mm, n = 1.31, ki = (cos30, -sin30, 0).
 COLUMN_PLAN = "qw,qx,qy,qz,weight,samples,seed\n1,0,0,0,1,20000,12345\n"
 
 
@@ -116,6 +117,94 @@ def ice_fixtures() -> None:
                         values=np.array(vals))
 
 
+# Area quadratures: circumradius, length, incident direction, subdivisions.
+ATLAS_AREA_CASES = [(0.1, 0.7, (1.0, 0.0, 0.0), 3), (0.1, 0.7, (0.0, 1.0, 0.0), 3), (0.1, 0.7, (1.0, 2.0, 3.0), 3),
+                    (0.1, 0.7, (-1.0, -0.001, -0.9), 3), (0.05, 0.2, (0.8660254037844387, -0.5, 0.0), 2),
+                    (0.1, 0.2, (0.3, 0.2, -0.9), 5), (0.1, 0.2, (0.0, 0.0, 1.0), 1)]
+# Atlases: R, L, n_int, n_ext, nm, theta intervals, phi intervals, nt, np, S, max hits, tail.  The
+# first is the reference's own atlas test setting (hex_atlas/tests/atlas_tests.cpp:12-16); the
+# second is the atlas the composition fixtures are built on.
+ATLAS_NODE_CASES = [(0.1, 0.2, 1.31, 1.0, 550.0, 3, 2, 12, 24, 2, 2048, 1e-12),
+                    (0.05, 0.2, 1.31, 1.0, 550.0, 6, 3, 16, 32, 2, 2048, 1e-12)]
+# Orientation models of the composition fixtures (the reference's own model kinds).
+ATLAS_RULES = [
+    {"quadrature": {"azimuth": 8, "tilt": 4, "spin": 3},
+     "components": [{"kind": "horizontal_gaussian", "sigma_deg": 10, "fraction": 0.9},
+                    {"kind": "isotropic", "fraction": 0.1}]},
+    {"quadrature": {"azimuth": 3, "tilt": 5, "spin": 2},
+     "components": [{"kind": "fixed", "fraction": 0.4,
+                     "quaternion_wxyz": [0.9238795325112867, 0.0, 0.3826834323650898, 0.0]},
+                    {"kind": "isotropic", "fraction": 0.6}]},
+]
+ATLAS_INCIDENTS = [(1.0, 0.0, 0.0), (0.8660254037844387, -0.5, 0.0), (0.0, -1.0, 0.0), (1.0, -0.4, 0.3),
+                   (0.7071067811865476, 0.7071067811865476, 0.0)]
+
+
+def atlas_fixtures(td: Path) -> None:
+    """Deterministic atlas: the reference's area rule and traced nodes (hex_atlas/src/atlas.cpp),
+    then its orientation composition (hex_atlas/python/atlas_math.py, imported from the
+    reference checkout) on the second atlas."""
+    out: dict[str, np.ndarray] = {}
+    faces, pos, wts, off = [], [], [], [0]
+    for R, L, k, S in ATLAS_AREA_CASES:
+        r = subprocess.run([str(REF_BIN / "ref_atlas_harness"), "area", repr(R), repr(L), *map(repr, k), str(S)],
+                           capture_output=True, text=True, check=True)
+        rows = [line.split() for line in r.stdout.splitlines()]
+        assert rows and rows[0][0] != "error", r.stdout
+        faces += [int(x[0]) for x in rows]
+        pos += [[float.fromhex(v) for v in x[1:4]] for x in rows]
+        wts += [float.fromhex(x[4]) for x in rows]
+        off.append(len(faces))
+    out.update(area_cases=np.array([[R, L, *k, S] for R, L, k, S in ATLAS_AREA_CASES]), area_offsets=np.array(off),
+               area_face=np.array(faces, np.uint32), area_pos=np.array(pos), area_weight=np.array(wts))
+    atlases = []
+    for c, case in enumerate(ATLAS_NODE_CASES):
+        R, L, n, ne, nm, T, P, nt, np_, S, hits, tail = case
+        f = td / "atlas.bin"
+        run([REF_BIN / "ref_atlas_harness", "nodes", repr(R), repr(L), repr(n), repr(ne), repr(nm), T, P, nt, np_, S,
+             hits, repr(tail), f])
+        raw = np.fromfile(f, "<f8").reshape((T + 1) * (P + 1), 16 + nt * np_)
+        out[f"nodes{c}_case"] = np.array(case, dtype=np.float64)
+        out[f"nodes{c}_head"] = raw[:, :16]
+        out[f"nodes{c}_mass"] = raw[:, 16:].reshape(T + 1, P + 1, nt, np_)
+        atlases.append((case, raw))
+    # composition on the second atlas, through the reference's own Python operator
+    sys.path.insert(0, str(REF / "hex_atlas" / "python"))
+    import atlas_math as am  # noqa: E402  (reference module, test-fixture generation only)
+    from types import SimpleNamespace
+    (R, L, _, _, _, T, P, nt, np_, _, _, _), raw = atlases[1]
+    head = raw[:, :16].reshape(T + 1, P + 1, 16)
+    edges = u_edges_ref(nt)
+    atlas = SimpleNamespace(it=T, ip=P, nt=nt, np=np_, area=head[:, :, 8].copy(), residual=head[:, :, 10].copy(),
+                            mass=raw[:, 16:].reshape(T + 1, P + 1, nt, np_), radius=R, length=L, edges=edges)
+    for ri, rule in enumerate(ATLAS_RULES):
+        rot, w, meta = am.orientation_rule(rule)
+        out[f"rule{ri}_rotations"], out[f"rule{ri}_weights"] = rot, w
+        out[f"rule{ri}_tilts"] = am.gaussian_tilt_nodes(rule["quadrature"]["tilt"], 10) if ri == 0 else np.zeros(0)
+        for ki_index, ki in enumerate(ATLAS_INCIDENTS):
+            c, area, frame, info = am.coupling_for_rule(atlas, rot, w, ki, meta)
+            mass, residual = am.compose_mass(atlas, c)
+            a, b, rep = am.make_cdf(mass, edges)
+            key = f"compose{ri}_{ki_index}"
+            out[key + "_coupling"] = c
+            out[key + "_scalars"] = np.array([area, residual, rep["g"], rep["cdf_l1_mass_error"],
+                                              float(info["method"].startswith("analytic"))])
+            out[key + "_frame"] = frame
+            out[key + "_mass"] = mass
+            out[key + "_phi"] = a
+            out[key + "_theta"] = b
+    out["compose_incidents"] = np.array(ATLAS_INCIDENTS)
+    out["compose_edges"] = edges
+    np.savez_compressed(HERE / "atlas_reference.npz", **out)
+
+
+def u_edges_ref(nt: int) -> np.ndarray:
+    """u edges of the atlas grid as the reference's precompute stores them (make_phase_u_edges)."""
+    r = subprocess.run([str(REF_BIN / "ref_atlas_harness"), "edges", str(nt)], capture_output=True, text=True,
+                       check=True)
+    return np.array([float.fromhex(x) for x in r.stdout.split()])
+
+
 def main() -> None:
     subprocess.run([str(ROOT / "oracle" / "build_ref.sh"), str(REF)], check=True)
     with tempfile.TemporaryDirectory() as t:
@@ -155,6 +244,8 @@ def main() -> None:
         drop_fixtures(td)
         # 5. ice Ih index of the prism records
         ice_fixtures()
+        # 6. deterministic atlas: area rule, traced nodes, orientation composition
+        atlas_fixtures(td)
     for f in sorted(HERE.glob("*.npz")):
         print(f.name, f.stat().st_size)
 

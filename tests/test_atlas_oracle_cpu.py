@@ -1,0 +1,129 @@
+"""Deterministic atlas composition, CPU: the library's orientation rule equals the reference's
+bit for bit, and the oracle (oracle/atlas_oracle.py, written in the device kernel's operation
+order and fixed-point accumulation) reproduces the reference's coupling weights, composed
+masses and CDFs (tests/golden/atlas_reference.npz, from hex_atlas/python/atlas_math.py on a
+traced reference atlas)."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from oracle import atlas_oracle as AO
+
+RULES = [
+    {"quadrature": {"azimuth": 8, "tilt": 4, "spin": 3},
+     "components": [{"kind": "horizontal_gaussian", "sigma_deg": 10, "fraction": 0.9},
+                    {"kind": "isotropic", "fraction": 0.1}]},
+    {"quadrature": {"azimuth": 3, "tilt": 5, "spin": 2},
+     "components": [{"kind": "fixed", "fraction": 0.4,
+                     "quaternion_wxyz": [0.9238795325112867, 0.0, 0.3826834323650898, 0.0]},
+                    {"kind": "isotropic", "fraction": 0.6}]},
+]
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return np.load(GOLDEN / "atlas_reference.npz")
+
+
+@pytest.fixture(scope="module")
+def atlas(gold):
+    case = gold["nodes1_case"]
+    T, P = int(case[5]), int(case[6])
+    head = gold["nodes1_head"].reshape(T + 1, P + 1, 16)
+    return {"R": case[0], "L": case[1], "T": T, "P": P, "area": head[:, :, 8], "residual": head[:, :, 10],
+            "mass": gold["nodes1_mass"]}
+
+
+def test_orientation_rule_matches_reference(gold):
+    from ice_crystal_phase_b200 import atlas as A
+
+    for ri, rule in enumerate(RULES):
+        r, w, meta = A.orientation_rule(rule)
+        assert np.array_equal(r, gold[f"rule{ri}_rotations"]) and np.array_equal(w, gold[f"rule{ri}_weights"])
+        assert meta["randomness"] is False and meta["component_nodes"][-1] == math.prod(rule["quadrature"].values())
+    assert np.array_equal(A.gaussian_tilt_nodes(4, 10), gold["rule0_tilts"])
+    # the reference's own checks of the rule (hex_atlas/tests/test_compose.py:37-62)
+    for sigma in (.1, 3, 10, 90):
+        b = A.gaussian_tilt_nodes(16, sigma)
+        s = math.radians(sigma)
+        e = math.erf(math.pi / (2 * math.sqrt(2) * s))
+        c = np.array([(1 + math.erf((x - math.pi / 2) / (math.sqrt(2) * s)) / e) / 2 for x in b])
+        assert np.allclose(c, (np.arange(16) + .5) / 16, atol=6e-14, rtol=0)
+        assert np.allclose(b + b[::-1], math.pi, atol=2e-15, rtol=0)
+    assert np.array_equal(A.gaussian_tilt_nodes(4, 0), [math.pi / 2] * 4)
+    for sigma in (-1, float("nan")):
+        with pytest.raises(ValueError):
+            A.gaussian_tilt_nodes(10, sigma)
+    with pytest.raises(ValueError):
+        A.orientation_rule({"quadrature": {"azimuth": 2, "tilt": 2, "spin": 2},
+                            "components": [{"kind": "isotropic", "fraction": .5}]})
+
+
+def _oracle_coupling(atlas, gold, ri, ki):
+    """coupling_for_rule in the oracle: the vertical-incidence orbit average per component."""
+    from ice_crystal_phase_b200 import atlas as A
+
+    rule = RULES[ri]
+    k = AO.unit3(ki)
+    vertical = k[0] == 0.0 and k[2] == 0.0
+    eligible = [c["kind"] in ("isotropic", "horizontal_gaussian") for c in rule["components"]]
+    args = (atlas["area"], atlas["T"], atlas["P"], 32, atlas["R"], atlas["L"])
+    if not vertical or not any(eligible):
+        return AO.coupling(*args, gold[f"rule{ri}_rotations"], gold[f"rule{ri}_weights"], ki)
+    w = np.zeros(((atlas["T"] + 1) * (atlas["P"] + 1), 2, 32))
+    areas = []
+    for comp, analytic in zip(rule["components"], eligible):
+        quad = dict(rule["quadrature"])
+        if analytic:
+            quad["azimuth"] = 1
+        r1, w1, _ = A.orientation_rule({"quadrature": quad, "components": [dict(comp, fraction=1.0)]})
+        _, a = AO.coupling(*args, r1, w1, ki, fraction=comp["fraction"], orbit=analytic, out=w)
+        areas.append(comp["fraction"] * a)
+    return w, math.fsum(areas)
+
+
+@pytest.mark.parametrize("ri", [0, 1])
+@pytest.mark.parametrize("ii", range(5))
+def test_oracle_coupling_and_compose_match_reference(gold, atlas, ri, ii):
+    ki = tuple(gold["compose_incidents"][ii])
+    key = f"compose{ri}_{ii}"
+    want_w = gold[key + "_coupling"].reshape(-1, 2, 32)
+    w, area = _oracle_coupling(atlas, gold, ri, ki)
+    area_ref, residual_ref = gold[key + "_scalars"][:2]
+    assert abs(area / area_ref - 1) < 1e-13
+    # weights: same nonzero pattern, values to a few ulps of the largest weight of the row
+    scale = np.abs(want_w).max()
+    assert np.max(np.abs(w - want_w)) <= 1e-13 * scale
+    # composition of the reference's own weights is bit-exact (same order, separate roundings)
+    nodes = atlas["mass"].reshape(-1, 16, 32)
+    mass = AO.compose(nodes, want_w)
+    assert np.array_equal(mass, gold[key + "_mass"])
+    # and of the oracle's weights within the weights' tolerance
+    mass2 = AO.compose(nodes, w)
+    assert np.max(np.abs(mass2 - mass)) <= 1e-12 * mass.max()
+    residual = float(np.sum(np.sum(want_w, axis=(1, 2)) * atlas["residual"].reshape(-1)))
+    assert residual == pytest.approx(residual_ref, rel=1e-12, abs=1e-30)
+    # conservation: composed flux + residual = expected area (compose_atlas.py:171-173)
+    assert abs((math.fsum(mass.flat) + residual) / area_ref - 1) < 2e-10
+    a, b, rep = AO.make_cdf(mass, gold["compose_edges"])
+    assert np.allclose(a, gold[key + "_phi"], rtol=0, atol=1e-15)
+    assert np.allclose(b, gold[key + "_theta"], rtol=0, atol=1e-15)
+    assert rep["g"] == pytest.approx(gold[key + "_scalars"][2], abs=1e-14)
+
+
+def test_oracle_fold_covers_the_sphere():
+    """Every direction folds into t in [0, pi/2], p in [0, pi/6] with q k(t,p) = direction
+    (hex_atlas/tests/test_compose.py:24-30)."""
+    for theta in np.linspace(0, math.pi, 21):
+        for phi in np.linspace(0, 2 * math.pi, 43):
+            k = [math.sin(theta) * math.cos(phi), math.cos(theta), math.sin(theta) * math.sin(phi)]
+            b = AO.unit3(k)
+            t, p, c, s, sy, sz, _ = AO.fold(b)
+            assert 0 <= t <= math.pi / 2 and 0 <= p <= math.pi / 6
+            kc = (math.sin(t) * math.cos(p), math.cos(t), math.sin(t) * math.sin(p))
+            qk = (c * kc[0] + s * sz * kc[2], sy * kc[1], -s * kc[0] + c * sz * kc[2])
+            assert np.allclose(qk, b, atol=2e-14)

@@ -15,7 +15,7 @@ import pytest
 from conftest import GOLDEN, TWO_ORIENTATIONS
 
 pytestmark = pytest.mark.gpu
-CFG3_KI = (0.8660254037844387, -0.5, 0.0)
+COLUMN_KI = (0.8660254037844387, -0.5, 0.0)
 
 
 def _tv(a, b):
@@ -52,7 +52,7 @@ def test_fp64_matches_reference_masses(ctx, icp):
 def test_fp64_hex_column_sparse(ctx, icp):
     g = np.load(GOLDEN / "hex_column_20k.npz")
     plan = icp.parse_orientation_plan("qw,qx,qy,qz,weight,samples,seed\n1,0,0,0,1,20000,12345\n")
-    acc = _accumulate(ctx, icp, plan, 0.05, 0.2, CFG3_KI, 1.31, 512, 1024, icp.ICP_FP64, hits=12)
+    acc = _accumulate(ctx, icp, plan, 0.05, 0.2, COLUMN_KI, 1.31, 512, 1024, icp.ICP_FP64, hits=12)
     m = acc.masses()
     ref = np.zeros_like(m)
     ref[g["index"]] = g["value"]
@@ -63,13 +63,13 @@ def test_fp64_hex_column_sparse(ctx, icp):
 
 @pytest.mark.parametrize("hash_slots", [0, 1, 64])
 def test_fp32_tv_against_oracle(ctx, icp, oracle, hash_slots):
-    # config-3 geometry, 2e5 rays, 12 interactions (unresolved residual reported, not dropped)
+    # the hex column (circumradius 0.05 mm, length 0.2 mm), 2e5 rays, 12 interactions (unresolved residual reported, not dropped)
     n = 200_000
     text = f"qw,qx,qy,qz,weight,samples,seed\n1,0,0,0,1,{n},12345\n"
     plan = icp.parse_orientation_plan(text)
     tuning = icp.Tuning(0, 0, hash_slots, 0)
-    acc = _accumulate(ctx, icp, plan, 0.05, 0.2, CFG3_KI, 1.31, 512, 1024, icp.ICP_FP32, hits=12, tuning=tuning)
-    rec = oracle.hex_record(0.05, 0.2, CFG3_KI, 1.31, 1.0, 512, 1024, oracle.parse_plan(text), max_hits=12)
+    acc = _accumulate(ctx, icp, plan, 0.05, 0.2, COLUMN_KI, 1.31, 512, 1024, icp.ICP_FP32, hits=12, tuning=tuning)
+    rec = oracle.hex_record(0.05, 0.2, COLUMN_KI, 1.31, 1.0, 512, 1024, oracle.parse_plan(text), max_hits=12)
     tv = _tv(acc.masses(), rec.masses)
     assert tv <= 1e-3, tv
     area = rec.expected_area
@@ -138,7 +138,7 @@ def test_transparent_limit_forward_cap(ctx, icp):
 def test_fp32_full_size_energy(ctx, icp):
     # 1e7 rays of the 1e8-ray config (512 x 1024, 12 interactions): size-independent properties
     plan = icp.parse_orientation_plan("qw,qx,qy,qz,weight,samples,seed\n1,0,0,0,1,10000000,12345\n")
-    out = icp.generate_hex_record(ctx, 0.05, 0.2, CFG3_KI, 1.31, 512, 1024, plan, max_internal_hits=12)
+    out = icp.generate_hex_record(ctx, 0.05, 0.2, COLUMN_KI, 1.31, 512, 1024, plan, max_internal_hits=12)
     rep = out.report
     assert abs((rep.escaped_area_mm2 + rep.unresolved_area_mm2) / rep.expected_area_mm2 - 1) <= 1e-12
     assert rep.histogram_relative_error <= 1e-10

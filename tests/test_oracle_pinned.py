@@ -14,7 +14,7 @@ import pytest
 
 from conftest import GOLDEN, TWO_ORIENTATIONS
 
-CFG3_KI = (0.8660254037844387, -0.5, 0.0)
+COLUMN_KI = (0.8660254037844387, -0.5, 0.0)
 
 
 def test_rng_midpoints(oracle):
@@ -53,7 +53,7 @@ def test_two_orientation_cdf_bit_exact(oracle):
 def test_hex_column_masses_bit_exact(oracle):
     g = np.load(GOLDEN / "hex_column_20k.npz")
     nodes = oracle.parse_plan("qw,qx,qy,qz,weight,samples,seed\n1,0,0,0,1,20000,12345\n")
-    rec = oracle.hex_record(0.05, 0.2, CFG3_KI, 1.31, 1.0, 512, 1024, nodes, max_hits=12)
+    rec = oracle.hex_record(0.05, 0.2, COLUMN_KI, 1.31, 1.0, 512, 1024, nodes, max_hits=12)
     nz = np.flatnonzero(rec.masses)
     assert np.array_equal(nz, g["index"])
     assert np.array_equal(rec.masses[nz], g["value"])
@@ -62,7 +62,7 @@ def test_hex_column_masses_bit_exact(oracle):
 
 def test_per_ray_trace_bit_exact(oracle):
     g = np.load(GOLDEN / "hex_rays.npz")
-    info, exits = oracle.hex_trace_rays(0.05, 0.2, CFG3_KI, 1.31, 1.0, 12345, 20000, 1024, 1e-12, 100, 48)
+    info, exits = oracle.hex_trace_rays(0.05, 0.2, COLUMN_KI, 1.31, 1.0, 12345, 20000, 1024, 1e-12, 100, 48)
     assert np.array_equal(info[:, :4], g["info"][:, :4])
     assert np.array_equal(info[:, 4], g["info"][:, 4])
     flat = np.concatenate([exits[i, :int(info[i, 1])] for i in range(48)])

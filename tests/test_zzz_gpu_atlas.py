@@ -1,0 +1,185 @@
+"""Deterministic atlas on the GPU, through the C ABI, against the reference's own atlas and
+composition (tests/golden/atlas_reference.npz).  The file sorts after the record-path GPU
+suites.
+
+* atlas trace: every node of two reference atlases (the reference's own test setting and the
+  composition atlas); cell masses to 1e-12 of the node's flux, the ray-ordered escaped /
+  unresolved sums, determinism, the index-matched delta and the failure gate of
+  hex_atlas/tests/atlas_tests.cpp:43-72.
+* coupling: the reference's rotations through icp_atlas_coupling; the expected area, the
+  weight of every node (summed over the two parities, which a fold that lands exactly on a
+  mirror plane may exchange), and the composed masses.
+* compose: the reference's own weights give the reference's masses bit for bit.
+* end to end: precompute -> Atlas reader -> compose -> records, conservation and CDF audit.
+"""
+from __future__ import annotations
+
+import json
+import math
+from types import SimpleNamespace
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+RULES = [
+    {"quadrature": {"azimuth": 8, "tilt": 4, "spin": 3},
+     "components": [{"kind": "horizontal_gaussian", "sigma_deg": 10, "fraction": 0.9},
+                    {"kind": "isotropic", "fraction": 0.1}]},
+    {"quadrature": {"azimuth": 3, "tilt": 5, "spin": 2},
+     "components": [{"kind": "fixed", "fraction": 0.4,
+                     "quaternion_wxyz": [0.9238795325112867, 0.0, 0.3826834323650898, 0.0]},
+                    {"kind": "isotropic", "fraction": 0.6}]},
+]
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return np.load(GOLDEN / "atlas_reference.npz")
+
+
+def _settings(A, case, **over):
+    R, L, n, ne, _, T, P, nt, np_, S, hits, tail = case
+    kw = dict(exterior_index=ne, max_internal_hits=int(hits), tail_tolerance=tail)
+    kw.update(over)
+    return A.settings(R, L, n, int(T), int(P), int(nt), int(np_), int(S), **kw)
+
+
+@pytest.mark.parametrize("c", [0, 1])
+def test_atlas_nodes_match_reference(ctx, icp, gold, c):
+    from ice_crystal_phase_b200 import atlas as A
+
+    case = gold[f"nodes{c}_case"]
+    s = _settings(A, case)
+    T, P = s.theta_intervals, s.phi_intervals
+    head, want = gold[f"nodes{c}_head"], gold[f"nodes{c}_mass"]
+    launches = icp.kernel_launches()
+    for n in range((T + 1) * (P + 1)):
+        i, j = divmod(n, P + 1)
+        mass, rep = A.trace_node(ctx, s, i, j)
+        ref = want[i, j]
+        assert rep.rays == int(head[n, 12]) and rep.outputs == int(head[n, 13])
+        assert rep.projected_area_mm2 == head[n, 8]
+        assert rep.escaped_mm2 == pytest.approx(head[n, 9], rel=1e-14)
+        assert rep.unresolved_mm2 == pytest.approx(head[n, 10], rel=1e-9, abs=1e-30)
+        assert rep.first_rejected == -1 and rep.invalid_bins == 0
+        assert np.all(mass >= 0)
+        assert np.max(np.abs(mass - ref)) <= 1e-12 * head[n, 9]
+        assert abs(mass.sum() / rep.escaped_mm2 - 1) < 1e-12
+    assert icp.kernel_launches() - launches == 2 * (T + 1) * (P + 1)
+
+
+def test_atlas_trace_is_deterministic_and_index_matched(ctx, icp, gold):
+    from ice_crystal_phase_b200 import atlas as A
+
+    s = _settings(A, gold["nodes0_case"])
+    a, _ = A.trace_node(ctx, s, 1, 1)
+    b, _ = A.trace_node(ctx, s, 1, 1)
+    assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
+    # n = 1: every ray passes straight through into the forward cap (atlas_tests.cpp:50-55)
+    s.interior_index = 1.0
+    m, rep = A.trace_node(ctx, s, 1, 1)
+    want = np.zeros_like(m)
+    want[0, :] = rep.projected_area_mm2 / s.np
+    assert np.max(np.abs(m - want)) < 1e-15
+
+
+def test_atlas_trace_failure_gates(ctx, icp, gold):
+    from ice_crystal_phase_b200 import atlas as A
+
+    s = _settings(A, gold["nodes0_case"], max_internal_hits=1)
+    with pytest.raises(icp.AuditError, match="Deterministic area ray rejected"):
+        A.trace_node(ctx, s, 1, 1)
+    for over in ({"subdivisions": 0}, {"tail_tolerance": 1e-9, "max_unresolved_fraction": 1e-10}):
+        s = _settings(A, gold["nodes0_case"])
+        for k, v in over.items():
+            setattr(s, k, v)
+        with pytest.raises(icp.InvalidArgument):
+            A.trace_node(ctx, s, 0, 0)
+
+
+def _atlas_stub(gold):
+    case = gold["nodes1_case"]
+    T, P, nt, np_ = (int(x) for x in case[5:9])
+    head = gold["nodes1_head"].reshape(T + 1, P + 1, 16)
+    return SimpleNamespace(it=T, ip=P, nt=nt, np=np_, radius=case[0], length=case[1], area=head[:, :, 8].copy(),
+                           residual=head[:, :, 10].copy(), mass=gold["nodes1_mass"], nodes=(T + 1) * (P + 1),
+                           edges=gold["compose_edges"])
+
+
+@pytest.mark.parametrize("ri", [0, 1])
+@pytest.mark.parametrize("ii", range(5))
+def test_coupling_and_compose_match_reference(ctx, icp, gold, ri, ii):
+    from ice_crystal_phase_b200 import atlas as A
+
+    atlas = _atlas_stub(gold)
+    comp = A.Composer(ctx, atlas)
+    rot, w, meta = A.orientation_rule(RULES[ri])
+    ki = gold["compose_incidents"][ii]
+    key = f"compose{ri}_{ii}"
+    wts, area, frame, info = comp.coupling_for_rule(rot, w, ki, meta)
+    want = gold[key + "_coupling"].reshape(atlas.nodes, 2, atlas.np)
+    assert area == pytest.approx(gold[key + "_scalars"][0], rel=1e-13)
+    assert np.allclose(frame, gold[key + "_frame"], rtol=0, atol=1e-15)
+    assert info["method"].startswith("analytic") == bool(gold[key + "_scalars"][4])
+    per_node, per_node_ref = wts.sum(axis=(1, 2)), want.sum(axis=(1, 2))
+    assert np.max(np.abs(per_node - per_node_ref)) <= 1e-12 * per_node_ref.max()
+    mass, residual = comp.compose(atlas, wts)
+    m = mass.download().reshape(atlas.nt, atlas.np)
+    ref = gold[key + "_mass"]
+    assert np.max(np.abs(m - ref)) <= 1e-10 * ref.max()
+    assert residual == pytest.approx(gold[key + "_scalars"][1], rel=1e-9, abs=1e-30)
+    # the reference's own weights: bit for bit
+    comp.coupling.upload(want.reshape(-1))
+    mass, _ = comp.compose(atlas, want)
+    assert np.array_equal(mass.download().reshape(atlas.nt, atlas.np), ref)
+
+
+def test_compose_larger_grid_matches_oracle(ctx, icp):
+    """Sparse and dense weights over a grid wider than one thread strip (np = 2100 > 2048),
+    against the oracle's ordered sum: bit for bit."""
+    from oracle import atlas_oracle as AO
+
+    rng = np.random.default_rng(7)
+    nodes, nt, np_ = 3, 5, 2100
+    mass = rng.random((nodes, nt, np_))
+    w = np.zeros((nodes, 2, np_))
+    w[0, 0, rng.choice(np_, 9, replace=False)] = rng.random(9)
+    w[1, 1, :] = rng.random(np_) * 1e-3
+    w[2, 0, 100:140] = rng.random(40)
+    d_mass = icp.DeviceArray(ctx, mass.size).upload(mass.reshape(-1))
+    d_w = icp.DeviceArray(ctx, w.size).upload(w.reshape(-1))
+    out = icp.DeviceArray(ctx, nt * np_)
+    icp.check(icp.LIB.icp_atlas_compose(ctx.handle, nodes, nt, np_, d_mass.ptr, d_w.ptr, out.ptr))
+    assert np.array_equal(out.download().reshape(nt, np_), AO.compose(mass, w))
+
+
+def test_precompute_and_compose_end_to_end(ctx, icp, tmp_path):
+    from ice_crystal_phase_b200 import atlas as A
+
+    s = A.settings(0.05, 0.2, 0.0, 2, 1, 16, 32, 2)
+    out = A.precompute(ctx, tmp_path / "atlas_550", s, 550.0, log=lambda *_: None)
+    atlas = A.Atlas(out)  # the reader's audits: frames, areas, mass vs escaped, residual
+    assert atlas.meta["material"]["model"] == "ice_ih_warren_brandt_2008_real_only"
+    assert atlas.meta["material"]["interior_index"] == icp.evaluate_ice_optics(550.0).n
+    cfg = tmp_path / "cfg.json"
+    cfg.write_text(json.dumps({"inclinations_deg": [0, 45, 90], "orientation": RULES[0]}))
+    res = A.compose(ctx, [out], cfg, tmp_path / "phase", log=lambda *_: None)
+    plan = json.loads((res / "batch_plan.json").read_text())
+    assert plan["complete"] and len(plan["records"]) == 3
+    for rec in plan["records"]:
+        d = res / rec["path"]
+        meta = json.loads((d / "metadata.json").read_text())
+        phi = np.load(d / "phi_cdf.npy")
+        theta = np.load(d / "theta_given_phi_cdf.npy")
+        assert phi[0] == 0 and phi[-1] == 1 and np.all(np.diff(phi) >= 0)
+        assert np.all(theta[:, 0] == 0) and np.all(theta[:, -1] == 1)
+        assert meta["quality"]["cdf_l1_mass_error"] <= 1e-10
+        assert abs(meta["transport_audit"]["balance_error"]) <= 2e-10
+        assert -1 < meta["hg"]["g"] < 1
+    vertical = json.loads((res / plan["records"][2]["path"] / "metadata.json").read_text())
+    assert vertical["orientation"]["azimuth_integration"]["method"].startswith("analytic")
+    assert math.isclose(vertical["incident_inclination_degrees"], 90.0)
