@@ -63,6 +63,7 @@ int ok()
     } while (0)
 
 constexpr double kFix62 = 0x1p62;
+constexpr uint64_t kAtlasChunk = 1ull << 20; // quadrature rays per trace launch (72 MiB of scratch)
 constexpr double kUnit62 = 0x1p-62;
 
 // ------------------------------------------------------------------ trace
@@ -486,6 +487,7 @@ int icp_atlas_trace_node(icp_context* ctx, const icp_atlas_settings* s, uint32_t
     if (!ctx || !d_mass || !report) return fail(ICP_ERR_INVALID_ARGUMENT, "icp_atlas_trace_node: null argument");
     if (int e = validate_settings(s)) return e;
     if (i > s->theta_intervals || j > s->phi_intervals) return fail(ICP_ERR_INVALID_ARGUMENT, "Incident node index.");
+    ICP_CUDA(cudaSetDevice(ctx->device));
     std::memset(report, 0, sizeof *report);
     report->first_rejected = -1;
     H::AtlasIncident node;
@@ -503,9 +505,10 @@ int icp_atlas_trace_node(icp_context* ctx, const icp_atlas_settings* s, uint32_t
     const uint64_t nr = rays.size(), cells = uint64_t(s->nt) * s->np;
     std::vector<double> edges;
     if (!H::u_edges(s->nt, edges)) return fail(ICP_ERR_INVALID_ARGUMENT, "Invalid u edges.");
-    // scratch: rays | audits | edges | cells | acc[4]
-    const size_t off_a = (nr * sizeof(icp_atlas_ray) + 255) & ~size_t(255);
-    const size_t off_e = off_a + ((nr * sizeof(AtlasAudit) + 255) & ~size_t(255));
+    // scratch: rays | audits (one chunk) | edges | cells | acc[4]
+    const uint64_t chunk = std::min<uint64_t>(nr, kAtlasChunk);
+    const size_t off_a = (chunk * sizeof(icp_atlas_ray) + 255) & ~size_t(255);
+    const size_t off_e = off_a + ((chunk * sizeof(AtlasAudit) + 255) & ~size_t(255));
     const size_t off_c = off_e + (((s->nt + 1) * sizeof(double) + 255) & ~size_t(255));
     const size_t off_x = off_c + cells * sizeof(unsigned long long);
     const size_t bytes = off_x + 4 * sizeof(unsigned long long);
@@ -517,7 +520,6 @@ int icp_atlas_trace_node(icp_context* ctx, const icp_atlas_settings* s, uint32_t
     auto* d_cells = reinterpret_cast<unsigned long long*>(base + off_c);
     auto* d_acc = reinterpret_cast<unsigned long long*>(base + off_x);
     cudaStream_t stream = ctx->stream;
-    ICP_CUDA(cudaMemcpyAsync(d_rays, rays.data(), nr * sizeof(icp_atlas_ray), cudaMemcpyHostToDevice, stream));
     ICP_CUDA(cudaMemcpyAsync(d_edges, edges.data(), edges.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
     ICP_CUDA(cudaMemsetAsync(d_cells, 0, cells * sizeof(unsigned long long) + 4 * sizeof(unsigned long long), stream));
     AtlasTrace P{};
@@ -541,41 +543,53 @@ int icp_atlas_trace_node(icp_context* ctx, const icp_atlas_settings* s, uint32_t
     P.grid.nt = s->nt;
     P.grid.np = s->np;
     P.rays = d_rays;
-    P.count = nr;
     P.scale = kFix62 / total;
     P.cells = d_cells;
     P.acc = d_acc;
     P.audits = d_audit;
-    atlas_trace_kernel<<<(unsigned)((nr + 127) / 128), 128, 0, stream>>>(P);
-    ICP_CUDA(cudaGetLastError());
-    count_launch();
-    const unsigned mblocks = (unsigned)std::min<uint64_t>((cells + 255) / 256, uint64_t(ctx->sms) * 8);
-    atlas_mass_kernel<<<mblocks, 256, 0, stream>>>(d_cells, d_acc, s->nt, s->np, total * kUnit62, d_mass, d_acc + 3);
-    ICP_CUDA(cudaGetLastError());
-    count_launch();
-    std::vector<AtlasAudit> audits(nr);
-    unsigned long long acc[4];
-    ICP_CUDA(cudaMemcpyAsync(audits.data(), d_audit, nr * sizeof(AtlasAudit), cudaMemcpyDeviceToHost, stream));
-    ICP_CUDA(cudaMemcpyAsync(acc, d_acc, sizeof acc, cudaMemcpyDeviceToHost, stream));
-    ICP_CUDA(cudaStreamSynchronize(stream));
     // host gates (atlas.cpp:98-139): every ray accepted, weighted sums in ray order
     H::KahanSum escaped, unresolved;
     report->projected_area_mm2 = area;
     report->rays = nr;
-    report->invalid_bins = acc[2];
-    for (uint64_t r = 0; r < nr; ++r) {
-        const AtlasAudit& a = audits[r];
-        report->outputs += a.outputs;
-        if (a.status < 8) ++report->status[a.status];
-        const double bal = std::fabs(a.escaped + a.residual - 1);
-        report->max_balance_error = std::max(report->max_balance_error, bal);
-        report->max_interface_balance_error = std::max(report->max_interface_balance_error, a.max_iface);
-        const bool accepted = (a.status == ICP_RAY_EXHAUSTED || a.status == ICP_RAY_TAIL) && H::finite(a.max_iface) &&
-                              a.max_iface <= s->max_balance_error && bal <= s->max_balance_error;
-        if (!accepted && report->first_rejected < 0) report->first_rejected = (int64_t)r;
-        escaped.add(rays[r].weight_mm2 * a.escaped);
-        unresolved.add(rays[r].weight_mm2 * a.residual);
+    std::vector<AtlasAudit> audits(chunk);
+    AtlasAudit first_bad{};
+    for (uint64_t first = 0; first < nr; first += chunk) {
+        const uint64_t n = std::min(chunk, nr - first);
+        ICP_CUDA(cudaMemcpyAsync(d_rays, rays.data() + first, n * sizeof(icp_atlas_ray), cudaMemcpyHostToDevice,
+                                 stream));
+        P.count = n;
+        atlas_trace_kernel<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(P);
+        ICP_CUDA(cudaGetLastError());
+        count_launch();
+        ICP_CUDA(cudaMemcpyAsync(audits.data(), d_audit, n * sizeof(AtlasAudit), cudaMemcpyDeviceToHost, stream));
+        ICP_CUDA(cudaStreamSynchronize(stream));
+        for (uint64_t q = 0; q < n; ++q) {
+            const AtlasAudit& a = audits[q];
+            const uint64_t r = first + q;
+            report->outputs += a.outputs;
+            if (a.status < 8) ++report->status[a.status];
+            const double bal = std::fabs(a.escaped + a.residual - 1);
+            report->max_balance_error = std::max(report->max_balance_error, bal);
+            report->max_interface_balance_error = std::max(report->max_interface_balance_error, a.max_iface);
+            const bool accepted = (a.status == ICP_RAY_EXHAUSTED || a.status == ICP_RAY_TAIL) &&
+                                  H::finite(a.max_iface) && a.max_iface <= s->max_balance_error &&
+                                  bal <= s->max_balance_error;
+            if (!accepted && report->first_rejected < 0) {
+                report->first_rejected = (int64_t)r;
+                first_bad = a;
+            }
+            escaped.add(rays[r].weight_mm2 * a.escaped);
+            unresolved.add(rays[r].weight_mm2 * a.residual);
+        }
     }
+    const unsigned mblocks = (unsigned)std::min<uint64_t>((cells + 255) / 256, uint64_t(ctx->sms) * 8);
+    atlas_mass_kernel<<<mblocks, 256, 0, stream>>>(d_cells, d_acc, s->nt, s->np, total * kUnit62, d_mass, d_acc + 3);
+    ICP_CUDA(cudaGetLastError());
+    count_launch();
+    unsigned long long acc[4];
+    ICP_CUDA(cudaMemcpyAsync(acc, d_acc, sizeof acc, cudaMemcpyDeviceToHost, stream));
+    ICP_CUDA(cudaStreamSynchronize(stream));
+    report->invalid_bins = acc[2];
     report->escaped_mm2 = escaped.value;
     report->unresolved_mm2 = unresolved.value;
     report->histogram_mass_mm2 = (double)(acc[3] + acc[0] + acc[1]) * (total * kUnit62);
@@ -585,7 +599,7 @@ int icp_atlas_trace_node(icp_context* ctx, const icp_atlas_settings* s, uint32_t
         return fail(ICP_ERR_AUDIT,
                     "Deterministic area ray rejected: local_id=%llu face=%u status=%s residual=%.17g. No jitter, "
                     "dropped ray, or renormalized omission is applied.",
-                    (unsigned long long)r, rays[r].face, ray_status_name(audits[r].status), audits[r].residual);
+                    (unsigned long long)r, rays[r].face, ray_status_name(first_bad.status), first_bad.residual);
     }
     if (!(report->histogram_mass_mm2 > 0) || !(report->escaped_mm2 > 0))
         return fail(ICP_ERR_AUDIT, "Incomplete atlas node.");
@@ -615,6 +629,7 @@ int icp_atlas_coupling(icp_context* ctx, uint32_t it, uint32_t ip, uint32_t np, 
     H::Frame f;
     if (!H::normalize(H::V{ki[0], ki[1], ki[2]}, k) || !H::make_frame(k, f))
         return fail(ICP_ERR_INVALID_ARGUMENT, "Expected finite nonzero three-vector");
+    ICP_CUDA(cudaSetDevice(ctx->device));
     // upper bound of the projected area: half the surface area of the convex prism
     const double side = R * L, cap = (3 * H::kSqrt3 / 2) * R * R, bound = 3 * side + cap;
     const uint64_t nacc = nodes * 2 * np;
@@ -680,6 +695,7 @@ int icp_atlas_compose(icp_context* ctx, uint32_t nodes, uint32_t nt, uint32_t np
     if (smem > 227u * 1024u)
         return fail(ICP_ERR_CAPACITY, "icp_atlas_compose: %u phi cells need %zu bytes of shared memory (limit 227 KiB)",
                     np, smem);
+    ICP_CUDA(cudaSetDevice(ctx->device));
     ICP_CUDA(cudaFuncSetAttribute(atlas_compose_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const dim3 grid((nt + kTT - 1) / kTT, (np + kComposeThreads * kPT - 1) / (kComposeThreads * kPT));
     atlas_compose_kernel<<<grid, kComposeThreads, smem, ctx->stream>>>(d_mass, d_coupling, nodes, nt, np, d_out);
