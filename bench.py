@@ -599,6 +599,118 @@ def run_surrogate(I, ctx, stream, a) -> dict:
     }
 
 
+def run_atlas(I, ctx, stream, a) -> dict:
+    """Deterministic atlas composition at the record grid: a 28-node atlas of the hex column
+    (6 x 3 incident intervals, 900 x 1800 cells, S = 2 area quadrature, n from the ice table at
+    550 nm) traced on the device, then per incident inclination the coupling of the reference's
+    horizontal_gaussian rule (16 x 8 x 12 nodes, two components), the cyclic composition and the
+    stored CDF, device-resident; the composition kernel against the FP64 pipe; the NumPy
+    composition of the oracle (the reference's algorithm) on the host as the CPU baseline."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from ice_crystal_phase_b200 import atlas as A
+
+    nt, np_ = DROP["nt"], DROP["np"]
+    s = A.settings(0.05, 0.2, I.evaluate_ice_optics(550.0).n, 6, 3, nt, np_, 2)
+    nodes = (s.theta_intervals + 1) * (s.phi_intervals + 1)
+    d_mass = torch.empty(nodes * nt * np_, dtype=torch.float64, device="cuda")
+    area = np.empty(nodes)
+    residual = np.empty(nodes)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for n in range(nodes):
+        i, j = divmod(n, s.phi_intervals + 1)
+        rep = I.AtlasNodeReport()
+        I.check(I.LIB.icp_atlas_trace_node(ctx.handle, C.byref(s), i, j,
+                                           C.c_void_p(d_mass.data_ptr() + 8 * n * nt * np_), C.byref(rep)))
+        area[n], residual[n] = rep.projected_area_mm2, rep.unresolved_mm2
+    t_atlas = time.perf_counter() - t0
+    rule = {"quadrature": {"azimuth": 16, "tilt": 8, "spin": 12},
+            "components": [{"kind": "horizontal_gaussian", "sigma_deg": 10, "fraction": 0.9},
+                           {"kind": "isotropic", "fraction": 0.1}]}
+    rot, w, _ = A.orientation_rule(rule)
+    d_rot = torch.from_numpy(np.ascontiguousarray(rot.reshape(-1, 9))).cuda()
+    d_w = torch.from_numpy(w).cuda()
+    incl = [0.0, 15.0, 30.0, 45.0, 60.0, 75.0][: max(1, a.atlas_incidents)]
+    coupling = torch.empty(nodes * 2 * np_, dtype=torch.float64, device="cuda")
+    out = torch.empty(nt * np_, dtype=torch.float64, device="cuda")
+    phi = torch.empty(np_ + 1, dtype=torch.float64, device="cuda")
+    theta = torch.empty(np_ * (nt + 1), dtype=torch.float64, device="cuda")
+    policy = I.CdfPolicy(1e-10, 1e-12, 1.0)
+    areas = (C.c_double * nodes)(*area)
+    nnz = []
+
+    def record(alpha: float, keep: bool = False) -> None:
+        k = (C.c_double * 3)(math.cos(math.radians(alpha)), -math.sin(math.radians(alpha)), 0.0)
+        coupling.zero_()
+        exp = C.c_double()
+        I.check(I.LIB.icp_atlas_coupling(ctx.handle, s.theta_intervals, s.phi_intervals, np_, s.circumradius_mm,
+                                         s.length_mm, areas, C.c_void_p(d_rot.data_ptr()), C.c_void_p(d_w.data_ptr()),
+                                         len(w), k, 1.0, 0, C.c_void_p(coupling.data_ptr()), C.byref(exp)))
+        if keep:
+            nnz.append(int((coupling > 0).sum()))
+        I.check(I.LIB.icp_atlas_compose(ctx.handle, nodes, nt, np_, C.c_void_p(d_mass.data_ptr()),
+                                        C.c_void_p(coupling.data_ptr()), C.c_void_p(out.data_ptr())))
+        crep = I.CdfReport()
+        I.check(I.LIB.icp_phase_cdf_build(ctx.handle, C.c_void_p(out.data_ptr()), 0, nt, np_, 0.0, 0.0, nt, np_,
+                                          C.byref(policy), C.c_void_p(phi.data_ptr()), C.c_void_p(theta.data_ptr()),
+                                          C.byref(crep)))
+
+    for alpha in incl:
+        record(alpha, keep=True)  # warm-up, nonzero weights per incidence
+    launches0 = I.kernel_launches()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for alpha in incl:
+        record(alpha)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_rec = e0.elapsed_time(e1) / 1e3 / len(incl)
+    launches = (I.kernel_launches() - launches0) // len(incl)
+    # the composition kernel alone, on the last incidence's weights
+    ck = []
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        I.check(I.LIB.icp_atlas_compose(ctx.handle, nodes, nt, np_, C.c_void_p(d_mass.data_ptr()),
+                                        C.c_void_p(coupling.data_ptr()), C.c_void_p(out.data_ptr())))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ck.append(e0.elapsed_time(e1) / 1e3)
+    flops = 2.0 * nnz[-1] * nt * np_
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    fp64_peak = 40.0  # nominal B200 FP64 TFLOP/s (no measured FP64 figure)
+    cpu = None
+    if not a.no_cpu_baseline:
+        from oracle import atlas_oracle as AO  # the reference's NumPy composition, as the CPU arm
+
+        host_mass = d_mass.cpu().numpy().reshape(nodes, nt, np_)
+        host_w = coupling.cpu().numpy().reshape(nodes, 2, np_)
+        # a bounded sample: the first 64 nonzero weights, scaled to all of them
+        sample = np.zeros_like(host_w)
+        idx = np.flatnonzero(host_w)[:64]
+        sample.flat[idx] = host_w.flat[idx]
+        t0 = time.perf_counter()
+        AO.compose(host_mass, sample)
+        t_cpu = (time.perf_counter() - t0) * nnz[-1] / max(1, len(idx))
+        cpu = {"value": 1.0 / t_cpu, "unit": "compositions/s", "cores": 1, "kind": "port",
+               "sample": f"{len(idx)} of {nnz[-1]} nonzero weights of one composition (28 nodes, 900x1800) as NumPy "
+                         "rolls in the reference's order, scaled to all weights"}
+    return {"workload": "hex_column_atlas_28_nodes_900x1800_horizontal_gaussian", "nodes": nodes,
+            "cells": [nt, np_], "rotations": len(w), "incidences": incl, "atlas_trace_s": t_atlas,
+            "ms_per_record": 1e3 * t_rec, "records_per_s": 1.0 / t_rec, "kernel_launches_per_record": launches,
+            "nonzero_weights": nnz,
+            "roofline_compose": {"kernel": "atlas_compose_kernel", "bound": "fp64", "achieved": flops / min(ck) / 1e12,
+                                 "peak": fp64_peak, "unit": "TFLOP/s", "frac": flops / min(ck) / 1e12 / fp64_peak,
+                                 "kernel_ms": 1e3 * min(ck), "sms": sms,
+                                 "peak_note": "nominal FP64 (separate mul and add; no measured FP64 peak)"},
+            "cpu_baseline": cpu}
+
+
 def _peaks() -> dict:
     try:
         return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
@@ -780,6 +892,9 @@ def run_b200_drop(a) -> None:
     surrogate = None
     if world == 1 and a.surrogate_records > 0:
         surrogate = run_surrogate(I, ctx, stream, a)
+    atlas = None
+    if world == 1 and a.atlas_incidents > 0:
+        atlas = run_atlas(I, ctx, stream, a)
 
     s0 = stats_all[-1]
     r0 = reps[-1]
@@ -813,6 +928,8 @@ def run_b200_drop(a) -> None:
         line["batched"] = batched
     if surrogate is not None:
         line["surrogate"] = surrogate
+    if atlas is not None:
+        line["atlas"] = atlas
     if r0 is not None:
         line["record"] = {"g": r0.cdf.g_stored, "projected_area_mm2": r0.projected_area_mm2,
                           "incident_area_mm2": r0.incident_area_mm2, "diffraction_mm2": r0.diffraction_area_mm2,
@@ -840,6 +957,8 @@ def main() -> None:
     p.add_argument("--surrogate-records", type=int, default=256, help="records of the surrogate measurement (0 = skip)")
     p.add_argument("--surrogate-checked", type=int, default=32, help="fresh records checked by 1e8-ray tracer records")
     p.add_argument("--hash-slots", type=int, default=0, help="shared histogram slots (0 = default, 1 = none)")
+    p.add_argument("--atlas-incidents", type=int, default=0,
+                   help="incidences of the deterministic atlas composition measurement (0 = skip)")
     p.add_argument("--rays", type=float, default=1e8)
     p.add_argument("--ref-rays", type=float, default=1.6e6, help="reference rays per step (all processes)")
     p.add_argument("--no-cpu-baseline", action="store_true")
