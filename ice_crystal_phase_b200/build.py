@@ -6,6 +6,7 @@ Produces, in-tree (git-ignored, shipped with the repository snapshot):
     ice_crystal_phase_b200/libicp_b200.so        C ABI of include/icp_b200.h (sm_100a)
     ice_crystal_phase_b200/bin/ice_generate_phase   hex drop-in CLI (C++ host over the C ABI)
     ice_crystal_phase_b200/bin/rainbow_generate     drop drop-in CLI
+    ice_crystal_phase_b200/bin/ice_precompute_atlas deterministic atlas precompute drop-in CLI
 
 Every CUDA translation unit is compiled for sm_100a only
 (-gencode arch=compute_100a,code=sm_100a).  The FP32 trace unit keeps FMA contraction;
@@ -52,7 +53,8 @@ UNITS = {
 }
 
 HOST_SOURCES = ["icp_record_io.cpp"]
-APP_SOURCES = {"ice_generate_phase": "ice_generate_phase.cpp", "rainbow_generate": "rainbow_generate.cpp"}
+APP_SOURCES = {"ice_generate_phase": "ice_generate_phase.cpp", "rainbow_generate": "rainbow_generate.cpp",
+               "ice_precompute_atlas": "ice_precompute_atlas.cpp"}
 
 
 def _newer(target: Path, deps: list[Path]) -> bool:

@@ -155,3 +155,30 @@ def test_incidents_and_cli_argument_checks(tmp_path):
     assert A.main(common + ["--ior", "1.31"]) == 2                       # ice material takes no --ior
     assert A.main(common + ["--material", "constant"]) == 2             # constant material needs --ior
     assert not (tmp_path / "a").exists() and not (tmp_path / "a.part").exists()
+
+
+def test_precompute_cli_arguments(tmp_path):
+    """The C++ drop-in of ice_precompute_atlas: the reference's option rules and exit code 2
+    (hex_atlas/apps/precompute_atlas.cpp:44-98, 142-143), checked before any device is used."""
+    import subprocess
+
+    from conftest import ROOT
+
+    exe = ROOT / "ice_crystal_phase_b200" / "bin" / "ice_precompute_atlas"
+
+    def run(args, code):
+        r = subprocess.run([str(exe), *map(str, args)], capture_output=True, text=True)
+        assert r.returncode == code, (r.returncode, r.stdout, r.stderr)
+        return r
+
+    assert "--material ice" in run(["--help"], 0).stdout
+    base = ["--out", tmp_path / "a", "--radius-mm", "0.1", "--length-mm", "0.2", "--incident-theta-intervals", "2",
+            "--incident-phi-intervals", "1", "--theta", "8", "--phi", "16", "--area-subdivisions", "1"]
+    assert "--wavelength-nm is required" in run(base, 2).stderr
+    assert "--ior requires explicit --material constant" in run(base + ["--wavelength-nm", "550", "--ior", "1.3"], 2).stderr
+    assert "Constant material requires --ior" in run(base + ["--wavelength-nm", "550", "--material", "constant"], 2).stderr
+    assert "200..1100 nm" in run(base + ["--wavelength-nm", "1200"], 2).stderr
+    assert "Duplicate option" in run(base + ["--theta", "8"], 2).stderr
+    assert "Unknown option" in run(base + ["--wavelength-nm", "550", "--bogus", "1"], 2).stderr
+    assert "Invalid number" in run(base + ["--wavelength-nm", "5x0"], 2).stderr
+    assert not (tmp_path / "a").exists() and not (tmp_path / "a.part").exists()

@@ -183,3 +183,25 @@ def test_precompute_and_compose_end_to_end(ctx, icp, tmp_path):
     vertical = json.loads((res / plan["records"][2]["path"] / "metadata.json").read_text())
     assert vertical["orientation"]["azimuth_integration"]["method"].startswith("analytic")
     assert math.isclose(vertical["incident_inclination_degrees"], 90.0)
+
+
+def test_precompute_cli_matches_the_library(ctx, icp, tmp_path):
+    """bin/ice_precompute_atlas writes the same atlas as atlas.precompute (deterministic
+    histograms: equal bits), and the reader's audits accept it."""
+    import subprocess
+
+    from conftest import ROOT
+    from ice_crystal_phase_b200 import atlas as A
+
+    exe = ROOT / "ice_crystal_phase_b200" / "bin" / "ice_precompute_atlas"
+    out = tmp_path / "cli"
+    r = subprocess.run([str(exe), "--out", str(out), "--radius-mm", "0.05", "--length-mm", "0.2", "--wavelength-nm",
+                        "550", "--incident-theta-intervals", "2", "--incident-phi-intervals", "1", "--theta", "16",
+                        "--phi", "32", "--area-subdivisions", "2"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert "atlas_complete nodes=6" in r.stdout
+    lib = A.precompute(ctx, tmp_path / "lib", A.settings(0.05, 0.2, 0.0, 2, 1, 16, 32, 2), 550.0, log=lambda *_: None)
+    a, b = A.Atlas(out), A.Atlas(lib)
+    assert np.array_equal(np.asarray(a.mass).view(np.uint64), np.asarray(b.mass).view(np.uint64))
+    assert np.array_equal(a.area, b.area) and np.array_equal(a.edges, b.edges)
+    assert a.meta["material"]["interior_index"] == b.meta["material"]["interior_index"]
