@@ -19,6 +19,11 @@ No random numbers: entry points come from a quadrature, orientations from a prod
 
     python -m ice_crystal_phase_b200.atlas precompute --out DIR --radius-mm R --length-mm L --wavelength-nm NM ...
     python -m ice_crystal_phase_b200.atlas compose --atlas DIR [DIR ...] --config CONFIG.json --out OUT
+    python -m ice_crystal_phase_b200.atlas spectrum --plan PLAN.json --atlas-root DIR --out OUT [--reuse] [--dry-run]
+
+``spectrum`` replaces hex_atlas/tools/run_spectrum.py: one dispersive-ice atlas per wavelength
+(cached with a job receipt, reused only for an identical request and library build), then one
+composition over all wavelengths.
 """
 from __future__ import annotations
 
@@ -28,6 +33,7 @@ import hashlib
 import json
 import math
 import sys
+import time
 from pathlib import Path
 from typing import Any
 
@@ -639,6 +645,149 @@ def compose(ctx: icp.Context, atlas_paths: list[Path], config_path: Path, out: P
     return Path(out)
 
 
+# ------------------------------------------------------------------ spectral runner
+SPECTRUM_REQUIRED = {"radius_mm", "length_mm", "incident_theta_intervals", "incident_phi_intervals", "theta", "phi",
+                     "area_subdivisions", "batch_rays", "max_work_mib"}
+SPECTRUM_OPTIONAL = {"max_internal_hits", "tail_tolerance", "max_unresolved_fraction", "max_balance_error"}
+SPECTRUM_INTEGERS = {"incident_theta_intervals", "incident_phi_intervals", "theta", "phi", "area_subdivisions",
+                     "batch_rays", "max_work_mib", "max_internal_hits"}
+
+
+def read_spectrum_plan(path: Path) -> dict[str, Any]:
+    """A spectral plan: wavelengths_nm (unique, ascending, 200..1100), precompute settings of one
+    ice prism, and one composition (inclinations and orientation model); everything is
+    validated before any work (run_spectrum.py:29-63).  batch_rays / max_work_mib size the
+    reference's per-ray histogram columns: required and validated, but they limit nothing here
+    (the device histogram is exact fixed point without per-ray columns)."""
+    with Path(path).open(encoding="utf-8") as f:
+        plan = json.load(f)
+    if set(plan) != {"wavelengths_nm", "precompute", "composition"}:
+        raise ValueError("Plan requires only wavelengths_nm, precompute, composition")
+    st = plan["precompute"]
+    if not isinstance(st, dict) or not SPECTRUM_REQUIRED <= set(st) <= SPECTRUM_REQUIRED | SPECTRUM_OPTIONAL:
+        raise ValueError("Missing/unknown precompute parameter")
+    for k, v in st.items():
+        if k in SPECTRUM_INTEGERS:
+            if type(v) is not int or v <= 0:
+                raise ValueError(f"{k} must be a positive integer")
+        elif type(v) not in (int, float) or not math.isfinite(v) or v < 0:
+            raise ValueError(f"{k} must be a finite nonnegative number")
+    if min(st["radius_mm"], st["length_mm"]) <= 0:
+        raise ValueError("Particle dimensions must be positive")
+    waves = plan["wavelengths_nm"]
+    if (not isinstance(waves, list) or not waves or len(set(waves)) != len(waves) or
+            any(type(w) not in (int, float) or not math.isfinite(w) or not 200 <= w <= 1100 for w in waves)):
+        raise ValueError("Unique vacuum wavelengths in 200..1100 nm are required")
+    if sorted(waves) != waves:
+        raise ValueError("Wavelengths must be listed in increasing order (stable w-index)")
+    cfg = plan["composition"]
+    if set(cfg) != {"inclinations_deg", "orientation"}:
+        raise ValueError("This fixed-condition runner requires inclination angles and one orientation model")
+    if len(set(cfg["inclinations_deg"])) != len(incidents(cfg)):
+        raise ValueError("Duplicate incident conditions")
+    orientation_rule(cfg["orientation"])
+    return plan
+
+
+def atlas_name(wavelength: float) -> str:
+    return "lambda_" + format(float(wavelength), ".17g").replace(".", "p") + "_nm"
+
+
+def verify_spectral_atlas(path: Path, wave: float, st: dict[str, Any]) -> dict[str, Any]:
+    """A cached atlas is the requested dispersive-ice calculation (run_spectrum.py:70-95); the
+    Atlas reader then audits every node."""
+    if path.name.endswith(".part"):
+        raise ValueError("Incomplete atlas")
+    m = json.loads((path / "metadata.json").read_text(encoding="utf-8"))
+    if m.get("complete") is not True or m.get("schema") != ATLAS_SCHEMA:
+        raise ValueError("Incomplete/unknown cached atlas")
+    mat = m["material"]
+    if (mat.get("model") != "ice_ih_warren_brandt_2008_real_only" or mat.get("automatic_ice_dispersion") is not True
+            or mat.get("wavelength_nm") != wave or mat.get("exterior_index") != 1):
+        raise ValueError("Cached atlas is not the requested dispersive ice calculation")
+    grid = {"incident_theta_intervals": st["incident_theta_intervals"],
+            "incident_phi_intervals": st["incident_phi_intervals"], "theta_count": st["theta"], "phi_count": st["phi"]}
+    if any(m.get(k) != v for k, v in grid.items()):
+        raise ValueError("Cached angular grid differs from request")
+    if (m["geometry"]["circumradius_mm"] != st["radius_mm"] or m["geometry"]["full_length_mm"] != st["length_mm"]
+            or m["area_quadrature"]["subdivisions"] != st["area_subdivisions"]):
+        raise ValueError("Cached geometry/area quadrature differs from request")
+    for f in ("mass_mm2.npy", "u_edges.npy"):
+        if not (path / f).is_file():
+            raise ValueError("Missing cached atlas array")
+    return m
+
+
+def spectrum(plan_path: Path, atlas_root: Path, out: Path, reuse: bool = False, dry_run: bool = False,
+             device: int = 0, log=print) -> None:
+    """Atlases of every wavelength (ice index from the table), cached under atlas_root with a job
+    receipt each and reused only when the request and the library build match, then one
+    composition over all of them (run_spectrum.py:98-169)."""
+    plan = read_spectrum_plan(plan_path)
+    out, atlas_root = Path(out), Path(atlas_root)
+    if out.exists() or out.with_name(out.name + ".part").exists():
+        raise ValueError("Use a new CDF output directory; existing output/.part is never replaced")
+    st = plan["precompute"]
+    raw = 8 * (st["incident_theta_intervals"] + 1) * (st["incident_phi_intervals"] + 1) * st["theta"] * st["phi"]
+    waves = plan["wavelengths_nm"]
+    log(f"PLAN: {len(waves)} wavelengths x {len(plan['composition']['inclinations_deg'])} incidents")
+    log(f"RAW ATLAS: {raw / 1024 ** 3:.3f} GiB/wavelength; {raw * len(waves) / 1024 ** 3:.3f} GiB total "
+        "(plus headers/metadata/CDFs)")
+    paths = [atlas_root / atlas_name(w) for w in waves]
+    if dry_run:
+        for w, p in zip(waves, paths):
+            log(f"python -m ice_crystal_phase_b200.atlas precompute --material ice --wavelength-nm {w} "
+                f"--radius-mm {st['radius_mm']} --length-mm {st['length_mm']} "
+                f"--incident-theta-intervals {st['incident_theta_intervals']} "
+                f"--incident-phi-intervals {st['incident_phi_intervals']} --theta {st['theta']} --phi {st['phi']} "
+                f"--area-subdivisions {st['area_subdivisions']} --out {p}")
+        log("DRY RUN: no files were created and no data were generated")
+        return
+    build = {"library_sha256": sha256_file(icp.LIB_PATH)}
+    atlas_root.mkdir(parents=True, exist_ok=True)
+    with icp.Context(device) as ctx:
+        for index, (wave, path) in enumerate(zip(waves, paths)):
+            receipt = path.with_name(path.name + ".job.json")
+            expected = {"schema": "ice.spectral_atlas_job.v1", "wavelength_nm": wave, "precompute": st,
+                        "material": "ice", "build": build}
+            if path.exists():
+                if not reuse:
+                    raise FileExistsError("Atlas exists; use --reuse for validated matching jobs: " + str(path))
+                old = json.loads(receipt.read_text(encoding="utf-8"))
+                if old.get("request") != expected or old.get("complete") is not True:
+                    raise ValueError("Cached atlas arguments/build differ; use another atlas-root")
+                if old.get("metadata_sha256") != sha256_file(path / "metadata.json"):
+                    raise ValueError("Cached metadata changed since the recorded job")
+                verify_spectral_atlas(path, wave, st)
+                log(f"REUSE {index + 1}/{len(paths)}: wavelength_nm={wave}")
+                continue
+            if receipt.exists() or path.with_name(path.name + ".part").exists():
+                raise FileExistsError("Unfinished job or stale receipt; inspect it before retrying: " + str(path))
+            s = settings(st["radius_mm"], st["length_mm"], 0.0, st["incident_theta_intervals"],
+                         st["incident_phi_intervals"], st["theta"], st["phi"], st["area_subdivisions"],
+                         max_internal_hits=st.get("max_internal_hits", 2048),
+                         tail_tolerance=st.get("tail_tolerance", 1e-12),
+                         max_unresolved_fraction=st.get("max_unresolved_fraction", 1e-10),
+                         max_balance_error=st.get("max_balance_error", 1e-10))
+            started = time.perf_counter()
+            with path.with_name(path.name + ".log").open("w", encoding="utf-8") as job_log:
+                precompute(ctx, path, s, float(wave), log=lambda line: print(line, file=job_log))
+            verify_spectral_atlas(path, wave, st)
+            _write_json(receipt, {"complete": True, "request": expected,
+                                  "metadata_sha256": sha256_file(path / "metadata.json"),
+                                  "seconds": time.perf_counter() - started})
+            log(f"ATLAS {index + 1}/{len(paths)}: wavelength_nm={wave}; seconds={time.perf_counter() - started:.3f}")
+        payload = json.dumps(plan["composition"], sort_keys=True, ensure_ascii=True, allow_nan=False).encode("ascii")
+        cfg_path = atlas_root / ("composition_" + hashlib.sha256(payload).hexdigest() + ".json")
+        if cfg_path.exists():
+            if json.loads(cfg_path.read_text(encoding="utf-8")) != plan["composition"]:
+                raise ValueError("Composition configuration cache mismatch")
+        else:
+            _write_json(cfg_path, plan["composition"])
+        compose(ctx, paths, cfg_path, out, "rainbow", log=log)
+    log("COMPLETE: " + ascii(str(out)))
+
+
 # ------------------------------------------------------------------ CLI
 def main(argv: list[str] | None = None) -> int:
     p = argparse.ArgumentParser(prog="python -m ice_crystal_phase_b200.atlas", description=__doc__.split("\n\n")[0])
@@ -667,7 +816,21 @@ def main(argv: list[str] | None = None) -> int:
     c.add_argument("--out", type=Path, required=True)
     c.add_argument("--output-contract", choices=["rainbow", "ensemble"], default="rainbow")
     c.add_argument("--device", type=int, default=0)
+    sp = sub.add_parser("spectrum")
+    sp.add_argument("--plan", type=Path, required=True)
+    sp.add_argument("--atlas-root", type=Path, required=True)
+    sp.add_argument("--out", type=Path, required=True)
+    sp.add_argument("--reuse", action="store_true")
+    sp.add_argument("--dry-run", action="store_true")
+    sp.add_argument("--device", type=int, default=0)
     a = p.parse_args(argv)
+    if a.cmd == "spectrum":
+        try:
+            spectrum(a.plan, a.atlas_root, a.out, a.reuse, a.dry_run, a.device)
+        except Exception as e:  # noqa: BLE001
+            print("SPECTRAL GENERATION FAILED: " + ascii(str(e)), file=sys.stderr)
+            return 2
+        return 0
     try:
         if a.cmd == "precompute":
             if a.material == "ice" and a.ior is not None:

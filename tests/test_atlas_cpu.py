@@ -182,3 +182,50 @@ def test_precompute_cli_arguments(tmp_path):
     assert "Unknown option" in run(base + ["--wavelength-nm", "550", "--bogus", "1"], 2).stderr
     assert "Invalid number" in run(base + ["--wavelength-nm", "5x0"], 2).stderr
     assert not (tmp_path / "a").exists() and not (tmp_path / "a.part").exists()
+
+
+SPECTRAL_PLAN = {"wavelengths_nm": [450, 550, 650],
+                 "precompute": {"radius_mm": .1, "length_mm": .2, "incident_theta_intervals": 3,
+                                "incident_phi_intervals": 2, "theta": 12, "phi": 24, "area_subdivisions": 2,
+                                "batch_rays": 8, "max_work_mib": 32},
+                 "composition": {"inclinations_deg": [-90, 0, 35, 90], "orientation": {
+                     "quadrature": {"azimuth": 4, "tilt": 4, "spin": 3},
+                     "components": [{"kind": "horizontal_gaussian", "sigma_deg": 3, "fraction": .9},
+                                    {"kind": "isotropic", "fraction": .1}]}}}
+
+
+def test_spectral_plan_rules_and_dry_run(tmp_path, capsys):
+    """The spectral runner's plan contract (hex_atlas/tools/run_spectrum.py:29-63) and its dry
+    run, which creates nothing (hex_atlas/tests/spectral_cli_test.py:43-45)."""
+    import copy
+    import json
+
+    from ice_crystal_phase_b200 import atlas as A
+
+    path = tmp_path / "plan.json"
+    path.write_text(json.dumps(SPECTRAL_PLAN))
+    A.read_spectrum_plan(path)
+    bad = []
+    for mutate in (lambda p: p.pop("composition"), lambda p: p["precompute"].pop("batch_rays"),
+                   lambda p: p["precompute"].update(theta=12.0), lambda p: p["precompute"].update(bogus=1),
+                   lambda p: p.update(wavelengths_nm=[550, 450]), lambda p: p.update(wavelengths_nm=[150]),
+                   lambda p: p.update(wavelengths_nm=[550, 550]),
+                   lambda p: p["composition"].update(inclinations_deg=[0, 0]),
+                   lambda p: p["composition"]["orientation"]["components"][0].update(fraction=.5)):
+        q = copy.deepcopy(SPECTRAL_PLAN)
+        mutate(q)
+        bad.append(q)
+    for k, q in enumerate(bad):
+        p = tmp_path / f"bad{k}.json"
+        p.write_text(json.dumps(q))
+        with pytest.raises(ValueError):
+            A.read_spectrum_plan(p)
+    args = ["spectrum", "--plan", str(path), "--atlas-root", str(tmp_path / "atlases"), "--out", str(tmp_path / "dry"),
+            "--dry-run"]
+    assert A.main(args) == 0
+    text = capsys.readouterr().out
+    assert "DRY RUN: no files were created" in text and text.count("precompute --material ice") == 3
+    assert "lambda_450_nm" in text
+    assert not (tmp_path / "atlases").exists() and not (tmp_path / "dry").exists()
+    p = tmp_path / "bad0.json"
+    assert A.main(["spectrum", "--plan", str(p), "--atlas-root", str(tmp_path / "a"), "--out", str(tmp_path / "o")]) == 2

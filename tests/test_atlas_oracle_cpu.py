@@ -127,3 +127,37 @@ def test_oracle_fold_covers_the_sphere():
             kc = (math.sin(t) * math.cos(p), math.cos(t), math.sin(t) * math.sin(p))
             qk = (c * kc[0] + s * sz * kc[2], sy * kc[1], -s * kc[0] + c * sz * kc[2])
             assert np.allclose(qk, b, atol=2e-14)
+
+
+def test_composed_record_meets_the_reader_contract(gold, tmp_path):
+    """A record written with atlas.record_metadata around the reference's composed masses and the
+    oracle's CDF passes the record reader's checks (python/rainbow_dataset/record.py:19-158)."""
+    import json
+    from types import SimpleNamespace
+
+    from record_check import validate_record
+    from ice_crystal_phase_b200 import atlas as A
+
+    key = "compose0_1"
+    mass = gold[key + "_mass"]
+    edges = gold["compose_edges"]
+    a, b, rep = AO.make_cdf(mass, edges)
+    frame = gold[key + "_frame"]
+    stub = SimpleNamespace(meta={"material": {"wavelength_nm": 550.0, "interior_index": 1.31, "exterior_index": 1.0},
+                                 "geometry": {"shape": "regular_hexagonal_prism", "circumradius_mm": .05,
+                                              "full_length_mm": .2}},
+                           hashes={}, it=6, ip=3, nt=16, np=32)
+    area, residual = gold[key + "_scalars"][:2]
+    meta = A.record_metadata(stub, float(area), float(residual),
+                             {"g_stored": rep["g"], "cdf_mass": rep["cdf_mass"], "l1_error": rep["l1"],
+                              "lost_mass": 0.0, "maximum_cell_error": 0.0}, frame, "0" * 64, {"config": RULES[0]},
+                             {"inclination_deg": 30.0}, {"method": "original_fixed_orientation_quadrature"}, "rainbow",
+                             float(mass.sum()))
+    d = tmp_path / "rec"
+    d.mkdir()
+    (d / "metadata.json").write_text(json.dumps(meta))
+    np.save(d / "phi_cdf.npy", a)
+    np.save(d / "theta_given_phi_cdf.npy", b)
+    np.save(d / "u_edges.npy", edges)
+    out = validate_record(d)
+    assert out["metadata"]["incident_inclination_degrees"] == pytest.approx(30.0, abs=1e-12)

@@ -205,3 +205,45 @@ def test_precompute_cli_matches_the_library(ctx, icp, tmp_path):
     assert np.array_equal(np.asarray(a.mass).view(np.uint64), np.asarray(b.mass).view(np.uint64))
     assert np.array_equal(a.area, b.area) and np.array_equal(a.edges, b.edges)
     assert a.meta["material"]["interior_index"] == b.meta["material"]["interior_index"]
+
+
+def test_spectral_runner_end_to_end(ctx, icp, tmp_path):
+    """Three dispersive-ice atlases and twelve records (hex_atlas/tests/spectral_cli_test.py):
+    the ice index per wavelength, different atlases per wavelength, the record contract, a
+    repeat with --reuse that leaves the cached atlases untouched and gives equal bytes, and the
+    refusal of a cache whose request changed."""
+    import copy
+
+    from record_check import validate_record
+    from test_atlas_cpu import SPECTRAL_PLAN
+    from ice_crystal_phase_b200 import atlas as A
+
+    plan = tmp_path / "plan.json"
+    plan.write_text(json.dumps(SPECTRAL_PLAN))
+    root = tmp_path / "atlases"
+    quiet = dict(log=lambda *_: None)
+    A.spectrum(plan, root, tmp_path / "dataset", **quiet)
+    arrays, times = [], []
+    for w, n in zip(SPECTRAL_PLAN["wavelengths_nm"], [1.3157, 1.3110, 1.3080]):
+        p = root / A.atlas_name(w)
+        m = json.loads((p / "metadata.json").read_text())
+        assert m["material"]["interior_index"] == n and m["material"]["automatic_ice_dispersion"] is True
+        arrays.append(np.load(p / "mass_mm2.npy"))
+        times.append((p / "mass_mm2.npy").stat().st_mtime_ns)
+    assert not np.array_equal(arrays[0], arrays[1]) and not np.array_equal(arrays[1], arrays[2])
+    index = json.loads((tmp_path / "dataset" / "batch_plan.json").read_text())
+    assert index["complete"] and len(index["records"]) == 12
+    for row in index["records"]:
+        validate_record(tmp_path / "dataset" / row["path"])
+    A.spectrum(plan, root, tmp_path / "repeat", reuse=True, **quiet)
+    for w, t in zip(SPECTRAL_PLAN["wavelengths_nm"], times):
+        assert (root / A.atlas_name(w) / "mass_mm2.npy").stat().st_mtime_ns == t
+    for row in index["records"]:
+        for f in ("phi_cdf.npy", "theta_given_phi_cdf.npy", "u_edges.npy"):
+            assert (tmp_path / "repeat" / row["path"] / f).read_bytes() == (tmp_path / "dataset" / row["path"] / f).read_bytes()
+    changed = copy.deepcopy(SPECTRAL_PLAN)
+    changed["precompute"]["length_mm"] = .3
+    plan.write_text(json.dumps(changed))
+    with pytest.raises(ValueError):
+        A.spectrum(plan, root, tmp_path / "reject", reuse=True, **quiet)
+    assert not (tmp_path / "reject").exists()
