@@ -3,7 +3,7 @@ composition (tests/golden/atlas_reference.npz).  The file sorts after the record
 suites.
 
 * atlas trace: every node of two reference atlases (the reference's own test setting and the
-  composition atlas); cell masses to 1e-12 of the node's flux, the ray-ordered escaped /
+  composition atlas); cell masses to L1 2e-11 with the same occupied cells, the ray-ordered escaped /
   unresolved sums, determinism, the index-matched delta and the failure gate of
   hex_atlas/tests/atlas_tests.cpp:43-72.
 * coupling: the reference's rotations through icp_atlas_coupling; the expected area, the
@@ -66,8 +66,9 @@ def test_atlas_nodes_match_reference(ctx, icp, gold, c):
         assert rep.escaped_mm2 == pytest.approx(head[n, 9], rel=1e-14)
         assert rep.unresolved_mm2 == pytest.approx(head[n, 10], rel=1e-9, abs=1e-30)
         assert rep.first_rejected == -1 and rep.invalid_bins == 0
-        assert np.all(mass >= 0)
-        assert np.max(np.abs(mass - ref)) <= 1e-12 * head[n, 9]
+        assert np.all(mass >= 0) and np.array_equal(mass > 0, ref > 0)
+        # L1 as the FP64 record-path tests (the reference's own CUDA/CPU atlas bar is 2e-9)
+        assert np.abs(mass - ref).sum() / ref.sum() <= 2e-11
         assert abs(mass.sum() / rep.escaped_mm2 - 1) < 1e-12
     assert icp.kernel_launches() - launches == 2 * (T + 1) * (P + 1)
 
