@@ -371,9 +371,66 @@ def run_training(ctx: I.Context, s: TrainSettings, cfg_over: dict | None = None,
     return sur, gate, held, report
 
 
+def profile(mode: str, records: int, steps: int, warmup: int = 2, device: int = 0, log=print) -> dict:
+    """A fixed surrogate workload for timing and kernel capture: the default network
+    (256 x 512 cells, 3 x 256 SiLU layers), He-initialised parameters (seed 0), `records` fresh
+    records of the batched distribution; `warmup` untimed steps, then `steps` timed steps of
+    `mode` (train: icp_surrogate_train_step against random cell distributions; predict:
+    icp_surrogate_predict; generate: icp_surrogate_generate at 64 x 128 storage).  Reports the
+    library's kernel-launch count before the timed steps (the `-s` of an ncu launch list) and
+    the launches per step (its `-c`)."""
+    torch = _torch()
+    cfg = I.surrogate_config(max_records=records)
+    specs = I.batched_record_specs(records, seed=7)
+    with I.Context(device) as ctx:
+        sur = I.Surrogate(ctx, cfg)
+        sur.set_parameters(init_parameters(cfg, 0))
+        n, cells = len(specs), sur.cells
+        gen = torch.Generator(device="cuda").manual_seed(0)
+        target = torch.rand((n, cells), generator=gen, device="cuda", dtype=torch.float32)
+        target /= target.sum(dim=1, keepdim=True)
+        y = torch.empty((n, cells), dtype=torch.float32, device="cuda")
+        ct, cp = 64, 128
+        phi = torch.empty(n * (cp + 1), dtype=torch.float64, device="cuda")
+        theta = torch.empty(n * cp * (ct + 1), dtype=torch.float64, device="cuda")
+        opt = I.Adam(1e-4, 0.9, 0.999, 1e-8, 0.0, 0)
+
+        def step():
+            if mode == "train":
+                opt.step += 1
+                sur.train_step(specs, target.data_ptr(), opt)
+            elif mode == "predict":
+                sur.predict(specs, y.data_ptr())
+            else:
+                sur.generate(specs, ct, cp, phi.data_ptr(), theta.data_ptr(), raise_on_audit=False)
+
+        for _ in range(warmup):
+            step()
+        torch.cuda.synchronize()
+        before = I.kernel_launches()
+        stream = torch.cuda.ExternalStream(I.LIB.icp_context_stream(ctx.handle))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out = {"mode": mode, "records": n, "cells": cells, "launches_before_timed_steps": before,
+               "launches_per_step": (I.kernel_launches() - before) // max(1, steps),
+               "ms_per_step": e0.elapsed_time(e1) / max(1, steps)}
+        sur.close()
+    log(json.dumps(out))
+    return out
+
+
 def main(argv=None) -> int:
     p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     sub = p.add_subparsers(dest="cmd", required=True)
+    q = sub.add_parser("profile", help="a fixed workload for timing and ncu launch lists")
+    q.add_argument("--mode", choices=["train", "predict", "generate"], required=True)
+    q.add_argument("--records", type=int, default=16)
+    q.add_argument("--steps", type=int, default=1)
+    q.add_argument("--warmup", type=int, default=2)
     t = sub.add_parser("train")
     t.add_argument("--out", required=True)
     for f in ("records", "heldout", "epochs", "batch", "seed", "max_internal_hits", "warmup_steps", "neighbours",
@@ -389,6 +446,9 @@ def main(argv=None) -> int:
     t.add_argument("--phi-frequencies", type=int, default=12)
     t.add_argument("--axis-harmonics", type=int, default=16)
     a = p.parse_args(argv)
+    if a.cmd == "profile":
+        profile(a.mode, a.records, a.steps, a.warmup)
+        return 0
     s = TrainSettings(**{k: getattr(a, k) for k in TrainSettings.__dataclass_fields__ if hasattr(a, k)})
     over = {"nt": a.nt, "np": a.np, "hidden": a.hidden, "input_width": a.input_width,
             "theta_frequencies": a.theta_frequencies, "phi_frequencies": a.phi_frequencies,
