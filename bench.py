@@ -700,6 +700,22 @@ def run_atlas(I, ctx, stream, a) -> dict:
         cpu = {"value": 1.0 / t_cpu, "unit": "compositions/s", "cores": 1, "kind": "port",
                "sample": f"{len(idx)} of {nnz[-1]} nonzero weights of one composition (28 nodes, 900x1800) as NumPy "
                          "rolls in the reference's order, scaled to all weights"}
+    # the reference's CPU precompute on a bounded sample: the 4 nodes of 1 x 1 intervals at the
+    # same grid (--batch-rays 16 keeps its per-ray columns within its 512 MiB default)
+    cpu_pre = None
+    ref_exe = ROOT / "oracle" / "_ref" / "ice_precompute_atlas_cpu"
+    if not a.no_cpu_baseline and ref_exe.exists():
+        with tempfile.TemporaryDirectory() as td:
+            t0 = time.perf_counter()
+            r = subprocess.run([str(ref_exe), "--out", str(Path(td) / "a"), "--radius-mm", "0.05", "--length-mm", "0.2",
+                                "--wavelength-nm", "550", "--incident-theta-intervals", "1",
+                                "--incident-phi-intervals", "1", "--theta", str(nt), "--phi", str(np_),
+                                "--area-subdivisions", "2", "--batch-rays", "16"], capture_output=True, text=True)
+            t_ref = time.perf_counter() - t0
+        if r.returncode == 0:
+            cpu_pre = {"value": 4 / t_ref, "unit": "atlas nodes/s", "cores": 1, "kind": "reference",
+                       "sample": "reference ice_precompute_atlas_cpu, 4 nodes (1 x 1 intervals), 900x1800, S = 2",
+                       "gpu_nodes_per_s": nodes / t_atlas}
     return {"workload": "hex_column_atlas_28_nodes_900x1800_horizontal_gaussian", "nodes": nodes,
             "cells": [nt, np_], "rotations": len(w), "incidences": incl, "atlas_trace_s": t_atlas,
             "ms_per_record": 1e3 * t_rec, "records_per_s": 1.0 / t_rec, "kernel_launches_per_record": launches,
@@ -708,7 +724,7 @@ def run_atlas(I, ctx, stream, a) -> dict:
                                  "peak": fp64_peak, "unit": "TFLOP/s", "frac": flops / min(ck) / 1e12 / fp64_peak,
                                  "kernel_ms": 1e3 * min(ck), "sms": sms,
                                  "peak_note": "nominal FP64 (separate mul and add; no measured FP64 peak)"},
-            "cpu_baseline": cpu}
+            "cpu_baseline": cpu, "cpu_baseline_precompute": cpu_pre}
 
 
 def _peaks() -> dict:

@@ -11,6 +11,7 @@
 #   oracle/_ref/ref_ice_harness          oracle/ref_ice_harness.cpp over hex_atlas/src/ice_optics.cpp
 #   oracle/_ref/ref_atlas_harness        oracle/ref_atlas_harness.cpp over hex_atlas/src/atlas.cpp and
 #                                        hex_trace/src/hex_trace.cpp (area rule, atlas nodes)
+#   oracle/_ref/ice_precompute_atlas_cpu reference CLI (hex_atlas/apps/precompute_atlas.cpp), CPU build
 #
 # Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
 set -euo pipefail
@@ -36,5 +37,8 @@ if [ -f "$ref/hex_atlas/src/ice_optics.cpp" ]; then
         "$ref/hex_atlas/src/ice_optics.cpp" -o "$out/ref_ice_harness"
     g++ "${flags[@]}" -I"$ref/hex_atlas/include" "$here/ref_atlas_harness.cpp" "$ref/hex_atlas/src/atlas.cpp" \
         "$ref/hex_trace/src/hex_trace.cpp" -o "$out/ref_atlas_harness"
+    g++ "${flags[@]}" -I"$ref/hex_atlas/include" "$ref/hex_atlas/apps/precompute_atlas.cpp" \
+        "$ref/hex_atlas/src/atlas.cpp" "$ref/hex_atlas/src/ice_optics.cpp" "$ref/hex_trace/src/hex_trace.cpp" \
+        "$ref/src/npy_writer.cpp" -o "$out/ice_precompute_atlas_cpu"
 fi
-echo "built $out/ice_generate_phase_cpu $out/ref_hex_harness $out/ref_drop_harness $out/ref_ice_harness $out/ref_atlas_harness"
+echo "built $out/ice_generate_phase_cpu $out/ref_hex_harness $out/ref_drop_harness $out/ref_ice_harness $out/ref_atlas_harness $out/ice_precompute_atlas_cpu"
