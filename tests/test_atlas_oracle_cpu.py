@@ -161,3 +161,123 @@ def test_composed_record_meets_the_reader_contract(gold, tmp_path):
     np.save(d / "u_edges.npy", edges)
     out = validate_record(d)
     assert out["metadata"]["incident_inclination_degrees"] == pytest.approx(30.0, abs=1e-12)
+
+
+# ---------------------------------------------------------------- the reference's composition properties
+def pattern_atlas():
+    """The reference's synthetic atlas (hex_atlas/tests/test_compose.py:13-21): 6 x 3 incident
+    intervals, 4 x 12 cells, every node the same normalised pattern times its projected area."""
+    from ice_crystal_phase_b200 import atlas as A
+
+    it, ip, nt, np_ = 6, 3, 4, 12
+    area = np.zeros((it + 1, ip + 1))
+    mass = np.zeros((it + 1, ip + 1, nt, np_))
+    pattern = np.arange(1, nt * np_ + 1, dtype=float).reshape(nt, np_)
+    pattern /= pattern.sum()
+    for i in range(it + 1):
+        for j in range(ip + 1):
+            area[i, j] = A.projected_area(.1, .2, A.canonical_frame(i * math.pi / 2 / it, j * math.pi / 6 / ip)[:, 2])
+            mass[i, j] = area[i, j] * pattern
+    return dict(it=it, ip=ip, nt=nt, np=np_, area=area, mass=mass, residual=np.zeros_like(area), R=.1, L=.2)
+
+
+def shift_cases():
+    """Rotations that bring node (2, 1) to ki = (1, 0, 0) with its frame turned by a chosen number
+    of phi cells, with and without a reflection (test_compose.py:76-94)."""
+    from ice_crystal_phase_b200 import atlas as A
+
+    f = A.canonical_frame(math.pi / 6, math.pi / 18)
+    fw = np.column_stack(_frame_of([1.0, 0.0, 0.0]))
+    for reflected in (False, True):
+        q = np.diag([1., 1., -1.]) if reflected else np.eye(3)
+        for shift in (0, 1, 2.3, -.7, 11.999):
+            d = 2 * math.pi * shift / 12
+            h = np.array([[math.cos(d), -math.sin(d), 0], [math.sin(d), math.cos(d), 0], [0, 0, 1.]])
+            if reflected:
+                h = h @ np.diag([1., -1., 1.])
+            yield reflected, shift, fw @ h @ f.T @ q.T
+
+
+def _frame_of(k):
+    e0, e1, kk = AO.output_frame(k)
+    return e0, e1, kk
+
+
+def expected_shift(a, reflected, shift):
+    original = a["mass"][2, 1]
+    if reflected:
+        original = original[:, ::-1]
+    lower = math.floor(shift)
+    fraction = shift - lower
+    return (1 - fraction) * np.roll(original, lower, axis=1) + fraction * np.roll(original, lower + 1, axis=1)
+
+
+def test_oracle_shift_and_reflection():
+    a = pattern_atlas()
+    for reflected, shift, r in shift_cases():
+        w, expected = AO.coupling(a["area"], 6, 3, 12, .1, .2, np.array([r]), np.ones(1), [1, 0, 0])
+        got = AO.compose(a["mass"].reshape(-1, 4, 12), w)
+        assert np.allclose(got, expected_shift(a, reflected, shift), atol=3e-17, rtol=1e-12), (reflected, shift)
+        assert got.sum() == pytest.approx(expected)
+
+
+def test_oracle_area_weighted_mixture_and_residual():
+    from ice_crystal_phase_b200 import atlas as A
+
+    a = pattern_atlas()
+    rot = np.array([np.eye(3), A._rz(np.array(math.pi / 2))])
+    w, area = AO.coupling(a["area"], 6, 3, 12, .1, .2, rot, np.array([.25, .75]), [1, 0, 0])
+    out = AO.compose(a["mass"].reshape(-1, 4, 12), w)
+    exact = .25 * A.projected_area(.1, .2, [1, 0, 0]) + .75 * A.projected_area(.1, .2, [0, -1, 0])
+    assert area == pytest.approx(exact) and out.sum() == pytest.approx(exact)
+    # a retained tail is propagated, not renormalised away (test_compose.py:103-108)
+    mass, residual = a["mass"] * .99, .01 * a["area"]
+    r = A._ry(np.array(.213)) @ A._rz(np.array(.7))
+    w, area = AO.coupling(a["area"], 6, 3, 12, .1, .2, np.array([r]), np.ones(1), [1, -.4, .3])
+    m = AO.compose(mass.reshape(-1, 4, 12), w)
+    tail = float(np.sum(w.sum(axis=(1, 2)) * residual.reshape(-1)))
+    assert m.sum() / area == pytest.approx(.99) and tail / area == pytest.approx(.01)
+
+
+def polar_rule(na=16):
+    return {"quadrature": {"azimuth": na, "tilt": 4, "spin": 3},
+            "components": [{"kind": "horizontal_gaussian", "sigma_deg": 10, "fraction": .9},
+                           {"kind": "isotropic", "fraction": .1}]}
+
+
+def oracle_vertical(a, rule, ki, mass):
+    """The vertical-incidence orbit average through the oracle (per component: one azimuth node,
+    row means), then the composition."""
+    from ice_crystal_phase_b200 import atlas as A
+
+    w = np.zeros(((a["it"] + 1) * (a["ip"] + 1), 2, a["np"]))
+    areas = []
+    for comp in rule["components"]:
+        analytic = comp["kind"] in ("isotropic", "horizontal_gaussian")
+        quad = dict(rule["quadrature"], azimuth=1) if analytic else rule["quadrature"]
+        r1, w1, _ = A.orientation_rule({"quadrature": quad, "components": [dict(comp, fraction=1.0)]})
+        _, ar = AO.coupling(a["area"], a["it"], a["ip"], a["np"], a["R"], a["L"], r1, w1, ki,
+                            fraction=comp["fraction"], orbit=analytic, out=w)
+        areas.append(comp["fraction"] * ar)
+    return AO.compose(mass.reshape(-1, a["nt"], a["np"]), w), math.fsum(areas)
+
+
+def test_oracle_poles_are_uniform_in_phi():
+    """At exact vertical incidence the analytic azimuth average equals the phi mean of the discrete
+    rule, row by row, at both poles; and it does not depend on the azimuth node count
+    (hex_atlas/tests/test_polar_azimuth.py:34-69)."""
+    from ice_crystal_phase_b200 import atlas as A
+
+    a = pattern_atlas()
+    mass = a["mass"] * .97
+    for sign in (-1, 1):
+        ki = [0, sign, 0]
+        rot, w, _ = A.orientation_rule(polar_rule())
+        wd, area_d = AO.coupling(a["area"], 6, 3, 12, .1, .2, rot, w, ki)
+        old = AO.compose(mass.reshape(-1, 4, 12), wd)
+        new, area = oracle_vertical(a, polar_rule(), ki, mass)
+        assert np.allclose(new, np.repeat(old.mean(axis=1, keepdims=True), 12, axis=1), rtol=1e-12, atol=2e-17)
+        assert area == pytest.approx(area_d, abs=1e-15)
+        first, _ = oracle_vertical(a, polar_rule(1), ki, mass)
+        for na in (2, 7, 23):
+            assert np.array_equal(oracle_vertical(a, polar_rule(na), ki, mass)[0], first)

@@ -248,3 +248,66 @@ def test_spectral_runner_end_to_end(ctx, icp, tmp_path):
     with pytest.raises(ValueError):
         A.spectrum(plan, root, tmp_path / "reject", reuse=True, **quiet)
     assert not (tmp_path / "reject").exists()
+
+
+def _pattern_stub():
+    from test_atlas_oracle_cpu import pattern_atlas
+
+    a = pattern_atlas()
+    return SimpleNamespace(it=a["it"], ip=a["ip"], nt=a["nt"], np=a["np"], radius=a["R"], length=a["L"],
+                           area=a["area"], residual=a["residual"], mass=a["mass"], nodes=(a["it"] + 1) * (a["ip"] + 1)), a
+
+
+def test_device_coupling_shift_reflection_and_mixture(ctx, icp):
+    """The reference's composition properties (hex_atlas/tests/test_compose.py:76-108) through
+    icp_atlas_coupling and icp_atlas_compose."""
+    from test_atlas_oracle_cpu import expected_shift, shift_cases
+    from ice_crystal_phase_b200 import atlas as A
+
+    stub, a = _pattern_stub()
+    comp = A.Composer(ctx, stub)
+
+    def run(rot, w, ki):
+        comp.coupling.zero()
+        area = comp.add_coupling(np.asarray(rot), np.asarray(w, float), np.asarray(ki, float), 1.0, False)
+        wts = comp.coupling.download().reshape(stub.nodes, 2, stub.np)
+        mass, _ = comp.compose(stub, wts)
+        return mass.download().reshape(stub.nt, stub.np), area, wts
+
+    for reflected, shift, r in shift_cases():
+        got, area, _ = run(np.array([r]), [1.0], [1, 0, 0])
+        assert np.allclose(got, expected_shift(a, reflected, shift), atol=3e-17, rtol=1e-12), (reflected, shift)
+        assert got.sum() == pytest.approx(area)
+    rot = np.array([np.eye(3), A._rz(np.array(math.pi / 2))])
+    out, area, _ = run(rot, [.25, .75], [1, 0, 0])
+    exact = .25 * A.projected_area(.1, .2, [1, 0, 0]) + .75 * A.projected_area(.1, .2, [0, -1, 0])
+    assert area == pytest.approx(exact) and out.sum() == pytest.approx(exact)
+
+
+def test_device_poles_are_uniform_in_phi(ctx, icp):
+    """Vertical incidence: the analytic azimuth average equals the phi mean of the discrete rule
+    and does not depend on the azimuth node count (hex_atlas/tests/test_polar_azimuth.py:34-69)."""
+    from test_atlas_oracle_cpu import polar_rule
+    from ice_crystal_phase_b200 import atlas as A
+
+    stub, a = _pattern_stub()
+    comp = A.Composer(ctx, stub)
+    for sign in (-1, 1):
+        ki = np.array([0.0, float(sign), 0.0])
+        rot, w, meta = A.orientation_rule(polar_rule())
+        comp.coupling.zero()
+        comp.add_coupling(rot, w, ki, 1.0, False)
+        wd = comp.coupling.download().reshape(stub.nodes, 2, stub.np)
+        old = comp.compose(stub, wd)[0].download().reshape(stub.nt, stub.np)
+        wts, area, _, info = comp.coupling_for_rule(rot, w, ki, meta)
+        new = comp.compose(stub, wts)[0].download().reshape(stub.nt, stub.np)
+        assert info["method"].startswith("analytic") and info["effective_pose_evaluations"] == 24
+        assert np.allclose(new, np.repeat(old.mean(axis=1, keepdims=True), stub.np, axis=1), rtol=1e-12, atol=2e-17)
+        first = None
+        for na in (1, 2, 7, 23):
+            r2, w2, m2 = A.orientation_rule(polar_rule(na))
+            wts, _, _, _ = comp.coupling_for_rule(r2, w2, ki, m2)
+            got = comp.compose(stub, wts)[0].download()
+            if first is None:
+                first = got
+            assert np.array_equal(got, first)
