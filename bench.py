@@ -910,7 +910,10 @@ def run_b200_drop(a) -> None:
         surrogate = run_surrogate(I, ctx, stream, a)
     atlas = None
     if world == 1 and a.atlas_incidents > 0:
-        atlas = run_atlas(I, ctx, stream, a)
+        try:
+            atlas = run_atlas(I, ctx, stream, a)
+        except (I.IcpError, RuntimeError, ValueError, OSError) as e:  # reported on the line, not fatal to it
+            atlas = {"error": f"{type(e).__name__}: {e}"}
 
     s0 = stats_all[-1]
     r0 = reps[-1]
