@@ -179,7 +179,7 @@ class AtlasRay(C.Structure):
 
 class AtlasIncident(C.Structure):
     _fields_ = [("theta", C.c_double), ("phi", C.c_double), ("ki", C.c_double * 3), ("e0", C.c_double * 3),
-                ("e1", C.c_double * 3)]
+                ("e1", C.c_double * 3), ("rule_ki", C.c_double * 3)]
 
 
 class AtlasSettings(C.Structure):

@@ -447,8 +447,9 @@ int icp_atlas_area_rule(double circumradius_mm, double length_mm, const double k
                         icp_atlas_ray* rays, uint64_t capacity, uint64_t* count)
 {
     if (!ki || !count) return fail(ICP_ERR_INVALID_ARGUMENT, "icp_atlas_area_rule: null argument");
-    H::V k;
-    if (!H::normalize(H::V{ki[0], ki[1], ki[2]}, k))
+    // a unit direction is used as given (make_area_rule requires one); any other is normalised
+    H::V k{ki[0], ki[1], ki[2]};
+    if (!H::is_unit(k) && !H::normalize(k, k))
         return fail(ICP_ERR_INVALID_ARGUMENT, "Incident direction must be finite and nonzero.");
     std::vector<H::AtlasRay> r;
     const int st = H::atlas_area_rule(circumradius_mm, length_mm, k, subdivisions, r);
@@ -477,7 +478,7 @@ int icp_atlas_incident_node(uint32_t theta_intervals, uint32_t phi_intervals, ui
     if (!H::atlas_incident(theta_intervals, phi_intervals, i, j, a))
         return fail(ICP_ERR_AUDIT, "Invalid incident spherical frame.");
     *out = icp_atlas_incident{a.theta, a.phi, {a.k.x, a.k.y, a.k.z}, {a.frame.e0.x, a.frame.e0.y, a.frame.e0.z},
-                              {a.frame.e1.x, a.frame.e1.y, a.frame.e1.z}};
+                              {a.frame.e1.x, a.frame.e1.y, a.frame.e1.z}, {a.k_rule.x, a.k_rule.y, a.k_rule.z}};
     return ok();
 }
 

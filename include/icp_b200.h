@@ -470,8 +470,8 @@ typedef struct {
     double weight_mm2;
 } icp_atlas_ray;
 
-/* Projected-area quadrature of the prism lit from unit direction ki (normalised as the
- * tracer does): S x S equal-area cells per lit side face and per end-cap sector, 2 x 3
+/* Projected-area quadrature of the prism lit from direction ki (used as given when it is a unit
+ * vector to 128 ulp, as make_area_rule requires; otherwise normalised first): S x S equal-area cells per lit side face and per end-cap sector, 2 x 3
  * Gauss-Legendre points per cell; replaces atlas::make_area_rule
  * (hex_atlas/include/ice_crystal/atlas.hpp:17, hex_atlas/src/atlas.cpp:11-51).  rays == NULL
  * returns the count only; otherwise capacity must hold it (ICP_ERR_CAPACITY).  Invalid
@@ -484,6 +484,8 @@ typedef struct {
     double theta, phi;  /* node angles (rad) */
     double ki[3];       /* incident propagation direction of the trace */
     double e0[3], e1[3];/* its spherical frame: e0 = (cos t cos p, -sin t, cos t sin p), e1 = ki x e0 */
+    double rule_ki[3];  /* the direction the area quadrature is built for (ki before its second
+                           normalisation, as atlas::make_node passes it to make_area_rule) */
 } icp_atlas_incident;
 
 /* Incident node (i, j) of theta_intervals x phi_intervals (end points included); replaces the

@@ -881,6 +881,132 @@ int icpo_hex_trace_rays(const double* node, uint64_t seed, uint64_t total, uint3
     return 0;
 }
 
+/*
+ * Deterministic atlas node (hex_atlas/src/atlas.cpp:140-153, atlas::trace_cpu): every quadrature
+ * ray traced from its given entry (trace_from_entry), its exits binned into a per-ray Kahan
+ * histogram by the atlas mass sink (hex_atlas/include/ice_crystal/atlas.hpp:51-72: weight x power
+ * per exit; an exit on a pole adds weight x power / np to every cell of the end row), then each
+ * touched cell of the ray added to the node's Kahan histogram, in ray order.
+ *
+ * k3, e03, e13: the trace direction and its frame (also the binning frame).  rays[5n]: face,
+ * x, y, z (units of the circumradius), weight (mm^2).  cells[nt*np] (out), stats[8] (out):
+ * escaped_mm2, unresolved_mm2 (weight x per-ray sums, Kahan in ray order), rays, outputs,
+ * max |balance|, max interface balance, first rejected ray (-1 none), its status.
+ * Returns 0, -1 invalid setup, -2 out of memory.
+ */
+int icpo_atlas_node(double R, double L, double n_ext, double n_int, double tail, uint32_t max_hits, const double* k3,
+                    const double* e03, const double* e13, const double* rays, uint64_t n, const double* edges,
+                    uint32_t nt, uint32_t np, double balance_tol, double* cells, double* stats);
+
+typedef struct {
+    grid_t grid;
+    ksum* ray_cells;
+    unsigned char* touched;
+    uint64_t* list;
+    uint64_t listed;
+    double weight;
+    int error;
+} atlas_sink_t;
+
+static void atlas_add(atlas_sink_t* s, uint64_t cell, double w)
+{
+    if (!s->touched[cell]) {
+        s->touched[cell] = 1;
+        s->list[s->listed++] = cell;
+    }
+    ks_add(&s->ray_cells[cell], w);
+}
+static void atlas_emit(void* user, v3 d, double power)
+{
+    atlas_sink_t* s = (atlas_sink_t*)user;
+    double w = s->weight * power;
+    bin_t b;
+    uint32_t row, j;
+    if (s->error) return;
+    if (!(w > 0) || !fin(w)) { s->error = 1; return; }
+    b = phase_bin(&s->grid, d);
+    if (!b.valid) { s->error = 2; return; }
+    if (!b.pole) { atlas_add(s, b.index, w); return; }
+    row = b.pole > 0 ? 0 : s->grid.nt - 1;
+    for (j = 0; j < s->grid.np; ++j) atlas_add(s, (uint64_t)row * s->grid.np + j, w / s->grid.np);
+}
+int icpo_atlas_node(double R, double L, double n_ext, double n_int, double tail, uint32_t max_hits, const double* k3,
+                    const double* e03, const double* e13, const double* rays, uint64_t n, const double* edges,
+                    uint32_t nt, uint32_t np, double balance_tol, double* cells, double* stats)
+{
+    trace_cfg_t c;
+    atlas_sink_t s;
+    ksum* acc;
+    ksum esc = {0, 0}, unres = {0, 0};
+    uint64_t r, q, C = (uint64_t)nt * np;
+    memset(&c, 0, sizeof c);
+    memset(&s, 0, sizeof s);
+    c.prism.R = R;
+    c.prism.L = L;
+    c.k.x = k3[0]; c.k.y = k3[1]; c.k.z = k3[2];
+    c.kf.e0.x = e03[0]; c.kf.e0.y = e03[1]; c.kf.e0.z = e03[2];
+    c.kf.e1.x = e13[0]; c.kf.e1.y = e13[1]; c.kf.e1.z = e13[2];
+    c.n_ext = n_ext;
+    c.n_int = n_int;
+    c.tail = tail;
+    c.total = n;
+    c.max_hits = max_hits;
+    if (!cfg_valid(&c) || !n || !nt || !np) return -1;
+    s.grid.edges = edges;
+    s.grid.ki = c.k;
+    s.grid.fr = c.kf;
+    s.grid.nt = nt;
+    s.grid.np = np;
+    acc = (ksum*)calloc(C, sizeof(ksum));
+    s.ray_cells = (ksum*)calloc(C, sizeof(ksum));
+    s.touched = (unsigned char*)calloc(C, 1);
+    s.list = (uint64_t*)malloc(C * sizeof(uint64_t));
+    if (!acc || !s.ray_cells || !s.touched || !s.list) {
+        free(acc); free(s.ray_cells); free(s.touched); free(s.list);
+        return -2;
+    }
+    stats[2] = (double)n;
+    stats[3] = 0;
+    stats[4] = stats[5] = 0;
+    stats[6] = -1;
+    stats[7] = 0;
+    for (r = 0; r < n; ++r) {
+        entry_t e;
+        ray_audit_t a;
+        const double* q5 = rays + 5 * r;
+        e.face = (unsigned)q5[0];
+        e.pos.x = q5[1]; e.pos.y = q5[2]; e.pos.z = q5[3];
+        e.valid = 1;
+        s.weight = q5[4];
+        s.listed = 0;
+        s.error = 0;
+        a = trace_from_entry(&c, r, e, atlas_emit, &s);
+        if (s.error) a.status = ST_OVERFLOW;
+        stats[3] += (double)a.outputs;
+        stats[4] = mx(stats[4], fabs(a.balance));
+        stats[5] = mx(stats[5], a.max_iface);
+        if (stats[6] < 0 && !((a.status == ST_EXHAUSTED || a.status == ST_TAIL) && fin(a.max_iface) &&
+                              a.max_iface <= balance_tol && fabs(a.balance) <= balance_tol)) {
+            stats[6] = (double)r;
+            stats[7] = (double)a.status;
+        }
+        ks_add(&esc, s.weight * a.escaped);
+        ks_add(&unres, s.weight * a.unresolved);
+        for (q = 0; q < s.listed; ++q) {
+            const uint64_t cell = s.list[q];
+            if (s.ray_cells[cell].value > 0) ks_add(&acc[cell], s.ray_cells[cell].value);
+            s.ray_cells[cell].value = 0;
+            s.ray_cells[cell].correction = 0;
+            s.touched[cell] = 0;
+        }
+    }
+    for (q = 0; q < C; ++q) cells[q] = acc[q].value;
+    stats[0] = esc.value;
+    stats[1] = unres.value;
+    free(acc); free(s.ray_cells); free(s.touched); free(s.list);
+    return 0;
+}
+
 /* PhaseMassAccumulator::masses (phase_table.cpp:63-76): pole mass spread uniformly
  * over the first / last row, added into the Kahan pair of each cell. */
 int icpo_masses(const double* cells, uint32_t nt, uint32_t np, const double* stats, double* out)

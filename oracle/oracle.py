@@ -59,6 +59,8 @@ def _lib() -> C.CDLL:
     lib.icpo_drop_trace_from.argtypes = [_D, _D, _D, _D, C.c_uint32, C.c_uint32, _D, _D]
     lib.icpo_drop_intersect.argtypes = [_D, _D, _D, C.c_int, _D]
     lib.icpo_drop_frame.argtypes = [C.c_double, _D, _D, _D]
+    lib.icpo_atlas_node.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint32, _D, _D,
+                                    _D, _D, C.c_uint64, _D, C.c_uint32, C.c_uint32, C.c_double, _D, _D]
     return lib
 
 
@@ -236,6 +238,24 @@ def build_cdf(mass: np.ndarray, nt: int, np_: int, ct: int | None = None, cp: in
 
 
 # ------------------------------------------------------------------ reference (_ref)
+def atlas_node(R: float, L: float, n_int: float, k, e0, e1, faces, points, weights, nt: int, np_: int,
+               n_ext: float = 1.0, tail: float = 1e-12, max_hits: int = 2048, balance_tol: float = 1e-10):
+    """One atlas node from its quadrature rays (atlas::trace_cpu, hex_atlas/src/atlas.cpp:140-153):
+    (cell masses [nt][np] in mm^2, stats: escaped_mm2, unresolved_mm2, rays, outputs, max balance,
+    max interface balance, first rejected ray or -1, its status)."""
+    rays = np.ascontiguousarray(np.column_stack([np.asarray(faces, float), np.asarray(points, float),
+                                                 np.asarray(weights, float)]))
+    edges = u_edges(nt)
+    cells = np.zeros(nt * np_)
+    stats = np.zeros(8)
+    k3, a3, b3 = (np.ascontiguousarray(v, dtype=np.float64) for v in (k, e0, e1))
+    st = lib().icpo_atlas_node(R, L, n_ext, n_int, tail, max_hits, _p(k3), _p(a3), _p(b3), _p(rays), len(rays),
+                               _p(edges), nt, np_, balance_tol, _p(cells), _p(stats))
+    if st:
+        raise RuntimeError(f"icpo_atlas_node failed ({st})")
+    return cells.reshape(nt, np_), stats
+
+
 def ref_available() -> bool:
     return (REF_DIR / "ref_hex_harness").exists()
 

@@ -281,3 +281,24 @@ def test_oracle_poles_are_uniform_in_phi():
         first, _ = oracle_vertical(a, polar_rule(1), ki, mass)
         for na in (2, 7, 23):
             assert np.array_equal(oracle_vertical(a, polar_rule(na), ki, mass)[0], first)
+
+
+def test_oracle_atlas_nodes_match_reference_bit_for_bit(icp, gold):
+    """The oracle's atlas node (C, the pinned prism tracer from given entries, per-ray Kahan
+    columns reduced in ray order) equals the reference's trace_cpu on every node of both
+    reference atlases, bit for bit."""
+    from oracle import oracle as O
+
+    for c in (0, 1):
+        R, L, n, ne, _, T, P, nt, np_, S, hits, tail = gold[f"nodes{c}_case"]
+        T, P, nt, np_, S = int(T), int(P), int(nt), int(np_), int(S)
+        head, want = gold[f"nodes{c}_head"], gold[f"nodes{c}_mass"]
+        for m in range((T + 1) * (P + 1)):
+            i, j = divmod(m, P + 1)
+            node = icp.atlas_incident_node(T, P, i, j)
+            faces, pts, w = icp.atlas_area_rule(R, L, list(node.rule_ki), S)
+            mass, st = O.atlas_node(R, L, n, list(node.ki), list(node.e0), list(node.e1), faces, pts, w, nt, np_,
+                                    n_ext=ne, tail=tail, max_hits=int(hits))
+            assert st[6] == -1 and st[2] == head[m, 12] and st[3] == head[m, 13]
+            assert st[0] == head[m, 9] and st[1] == head[m, 10]
+            assert np.array_equal(mass, want[i, j]), (c, i, j, np.abs(mass - want[i, j]).max())

@@ -311,3 +311,24 @@ def test_device_poles_are_uniform_in_phi(ctx, icp):
             if first is None:
                 first = got
             assert np.array_equal(got, first)
+
+
+def test_atlas_nodes_match_oracle_beyond_the_fixtures(ctx, icp):
+    """Settings outside the fixtures (S = 3, the ice index at 400 nm, 20 x 40 cells, a longer
+    column) against the oracle's atlas node, which equals the reference's trace_cpu bit for bit
+    on the fixtures."""
+    from oracle import oracle as O
+    from ice_crystal_phase_b200 import atlas as A
+
+    n = icp.evaluate_ice_optics(400.0).n
+    s = A.settings(0.08, 0.5, n, 2, 1, 20, 40, 3)
+    for m in range(6):
+        i, j = divmod(m, 2)
+        mass, rep = A.trace_node(ctx, s, i, j)
+        node = icp.atlas_incident_node(2, 1, i, j)
+        faces, pts, w = icp.atlas_area_rule(0.08, 0.5, list(node.rule_ki), 3)
+        ref, st = O.atlas_node(0.08, 0.5, n, list(node.ki), list(node.e0), list(node.e1), faces, pts, w, 20, 40)
+        assert rep.rays == st[2] and rep.outputs == st[3] and rep.first_rejected == -1 and st[6] == -1
+        assert rep.escaped_mm2 == pytest.approx(st[0], rel=1e-14)
+        assert np.array_equal(mass > 0, ref > 0)
+        assert np.abs(mass - ref).sum() / ref.sum() <= 2e-11
