@@ -205,6 +205,53 @@ def u_edges_ref(nt: int) -> np.ndarray:
     return np.array([float.fromhex(x) for x in r.stdout.split()])
 
 
+def compare_fixtures(td: Path) -> None:
+    """The reference's record-vs-record metric (tools/phase_analysis.py compare_tables) on two
+    records of one 64 x 128 grid: the TV judge of the learned surrogate's records."""
+    sys.path.insert(0, str(REF / "tools"))
+    sys.path.insert(0, str(REF / "python"))
+    sys.path.insert(0, str(ROOT))
+    import phase_analysis as pa  # noqa: E402  (reference module, test-fixture generation only)
+    from oracle import atlas_oracle as AO
+
+    nt, np_ = 64, 128
+    edges = u_edges_ref(nt)
+    rng = np.random.default_rng(44)
+    base = rng.gamma(0.5, size=(nt, np_)) * np.diff(edges)[:, None]
+    base[:, 7] = 0.0
+    other = base * np.exp(0.05 * rng.normal(size=base.shape))
+    other[3, :] *= 1.3
+    out = {}
+    for name, mass in (("a", base), ("b", other)):
+        phi, theta, rep = AO.make_cdf(mass, edges)
+        d = td / f"rec_{name}"
+        d.mkdir()
+        np.save(d / "phi_cdf.npy", phi)
+        np.save(d / "theta_given_phi_cdf.npy", theta)
+        np.save(d / "u_edges.npy", edges)
+        q = np.diff(phi)[:, None] * np.diff(theta, axis=1)
+        mu = 1.0 - (edges[:-1] + edges[1:])
+        g = float(np.sum(q * mu[None, :], dtype=np.longdouble) / np.sum(q, dtype=np.longdouble))
+        meta = {"schema": "rainbow.phase_cdf.numpy.v2", "complete": True, "dtype": "<f8", "order": "C",
+                "theta_count": nt, "phi_count": np_, "density_measure": "solid_angle_sr",
+                "cell_model": "constant_density_per_spherical_cell",
+                "coordinates": "u=(1-cos(theta))/2; v=(phi+pi)/(2*pi)", "cdf_axis_order": ["phi_cell", "theta_edge"],
+                "normalization": "integral_p_domega_equals_one", "input_polarization": "unpolarized",
+                "direction_convention": "physical_propagation", "theta_zero": "forward", "theta_pi": "backward",
+                "coordinate_contract_id": "rainbow.phase_cdf.coordinates.v1",
+                "sampling_frame_map": "local_column_to_particle_column",
+                "sampling_frame_columns": [[1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [0.0, 0.0, 1.0]],
+                "hg": {"g": g, "method": "first_moment_of_saved_cell_pdf", "target": "saved_cdf",
+                       "cosine_convention": "dot(incident_propagation,outgoing_propagation)"}}
+        (d / "metadata.json").write_text(json.dumps(meta))
+        out[f"phi_{name}"], out[f"theta_{name}"] = phi, theta
+    r = pa.compare_tables(pa.load_table(td / "rec_a"), pa.load_table(td / "rec_b"))
+    out["metrics"] = np.array([r["tv"], r["l1"], r["theta_marginal_tv"], r["hellinger"], r["jensen_shannon_nats"],
+                               r["g_a"], r["g_b"]])
+    out["edges"] = edges
+    np.savez_compressed(HERE / "compare_reference.npz", **out)
+
+
 def main() -> None:
     subprocess.run([str(ROOT / "oracle" / "build_ref.sh"), str(REF)], check=True)
     with tempfile.TemporaryDirectory() as t:
@@ -246,6 +293,8 @@ def main() -> None:
         ice_fixtures()
         # 6. deterministic atlas: area rule, traced nodes, orientation composition
         atlas_fixtures(td)
+        # 7. the reference's record-vs-record metric
+        compare_fixtures(td)
     for f in sorted(HERE.glob("*.npz")):
         print(f.name, f.stat().st_size)
 

@@ -135,3 +135,28 @@ def test_oracle_matches_reference_binary(oracle, tmp_path, ki, R, L, n, hits):
     rec = oracle.hex_record(R, L, ki, n, 1.0, 24, 48, oracle.parse_plan(plan), max_hits=hits, batch=333)
     assert np.array_equal(m, rec.masses)
     assert rec.escaped_area == d[5] and rec.unresolved_area == d[6]
+
+
+def _measure(oracle, edges, mass):
+    out = np.zeros(2)
+    nt, np_ = mass.shape
+    e = np.ascontiguousarray(edges, dtype=np.float64)
+    m = np.ascontiguousarray(mass, dtype=np.float64)
+    assert oracle.lib().icpo_measure_mass(oracle._p(e), nt, np_, oracle._p(m), oracle._p(out)) == 0
+    return out
+
+
+def test_cell_moment_known_answers(oracle):
+    """The saved-CDF first moment (tests/test_phase_storage_cpu.cpp:98-120): the mean cosine of a
+    u band is 1 - (u_lo + u_hi); a uniform sphere has g = 0 to 5e-16 on every saved grid, and the
+    two-column CDF of the reference's test has g = -0.40125 to 2e-16."""
+    for nt in (1, 2, 17, 900, 1800):
+        e = oracle.u_edges(nt)
+        total, axial = _measure(oracle, e, np.diff(e)[:, None] * np.ones((1, 3)) / 3)
+        assert abs(total - 1) < 4e-16 and abs(axial / total) < 5e-16
+    phi = [0, .25, 1]
+    c = [[0, .1, .5, 1], [0, 0, .25, 1]]
+    e = np.array([0, .1, .7, 1])
+    mass = np.array([[(phi[j + 1] - phi[j]) * (c[j][i + 1] - c[j][i]) for j in range(2)] for i in range(3)])
+    total, axial = _measure(oracle, e, mass)
+    assert abs(total - 1) < 2e-16 and abs(axial / total - (-0.40125)) < 2e-16

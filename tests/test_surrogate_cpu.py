@@ -174,3 +174,26 @@ def test_storage_grid_sums_and_tv():
     assert np.allclose(S.tv(pt, qt).numpy(), 0.5 * np.abs(p - q).sum(axis=1))
     # aggregation never raises the total variation
     assert np.all(S.tv(S.coarse(pt, 16, 32, 4, 8), S.coarse(qt, 16, 32, 4, 8)).numpy() <= S.tv(pt, qt).numpy() + 1e-15)
+
+
+def test_tv_is_the_reference_record_metric():
+    """On records of one grid the surrogate's TV judge equals the reference's record-vs-record TV
+    (tools/phase_analysis.py compare_tables, golden from the reference tool), and the record g
+    equals its g of the saved cells."""
+    import torch
+
+    import ice_crystal_phase_b200.surrogate as S
+    from conftest import GOLDEN
+
+    z = np.load(GOLDEN / "compare_reference.npz")
+    cells = {k: np.diff(z[f"phi_{k}"])[:, None] * np.diff(z[f"theta_{k}"], axis=1) for k in "ab"}
+    p = torch.from_numpy(cells["a"].reshape(1, -1))
+    q = torch.from_numpy(cells["b"].reshape(1, -1))
+    tv, l1, marginal_tv, _, _, ga, gb = z["metrics"]
+    assert float(S.tv(p, q)[0]) == pytest.approx(tv, rel=1e-12)
+    e = z["edges"]
+    mu = 1.0 - (e[:-1] + e[1:])
+    for c, g in ((cells["a"], ga), (cells["b"], gb)):
+        assert float((c * mu[None, :]).sum() / c.sum()) == pytest.approx(g, abs=1e-15)
+    # the theta marginal TV is the TV of the column sums
+    assert 0.5 * np.abs(cells["a"].sum(axis=0) - cells["b"].sum(axis=0)).sum() == pytest.approx(marginal_tv, rel=1e-12)
