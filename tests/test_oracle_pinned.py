@@ -160,3 +160,23 @@ def test_cell_moment_known_answers(oracle):
     mass = np.array([[(phi[j + 1] - phi[j]) * (c[j][i + 1] - c[j][i]) for j in range(2)] for i in range(3)])
     total, axial = _measure(oracle, e, mass)
     assert abs(total - 1) < 2e-16 and abs(axial / total - (-0.40125)) < 2e-16
+
+
+def _long_tir_case(oracle):
+    """The reference's long total-internal-reflection ray: condition 157 of its direction/aspect
+    sweep, sample 93 (hex_trace/tests/hex_trace_tests.cpp:282-300)."""
+    k = [2 * oracle.sample_uniform(119, 157, d) - 1 for d in range(3)]
+    length = 0.2 + 5 * oracle.sample_uniform(127, 157, 0)
+    return k, length
+
+
+def test_long_tir_known_answer(oracle):
+    """At 256 interactions the ray stops at the cap with more than 98 % of its power unresolved;
+    at 1024 it resolves (residual < 1e-12, balance 1e-10)."""
+    k, length = _long_tir_case(oracle)
+    info, _ = oracle.hex_trace_rays(1.0, length, k, 1.31, 1.0, 857, 100, 256, 1e-12, 93, 1)
+    status, outputs, escaped, unresolved, hits, _ = info[0]
+    assert status == 2 and hits == 256 and unresolved > 0.98
+    info, _ = oracle.hex_trace_rays(1.0, length, k, 1.31, 1.0, 857, 100, 1024, 1e-12, 93, 1)
+    status, outputs, escaped, unresolved, hits, _ = info[0]
+    assert status in (0, 1) and hits > 256 and unresolved < 1e-12 and abs(escaped + unresolved - 1) < 1e-10
