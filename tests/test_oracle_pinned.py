@@ -180,3 +180,33 @@ def test_long_tir_known_answer(oracle):
     info, _ = oracle.hex_trace_rays(1.0, length, k, 1.31, 1.0, 857, 100, 1024, 1e-12, 93, 1)
     status, outputs, escaped, unresolved, hits, _ = info[0]
     assert status in (0, 1) and hits > 256 and unresolved < 1e-12 and abs(escaped + unresolved - 1) < 1e-10
+
+
+def _sweep_case(oracle, condition):
+    k = [2 * oracle.sample_uniform(119, condition, d) - 1 for d in range(3)]
+    return k, 0.2 + 5 * oracle.sample_uniform(127, condition, 0)
+
+
+def test_direction_aspect_sweep(oracle):
+    """300 random directions and aspect ratios, 100 rays each, every ray accepted with balance
+    below 1e-10 and total internal reflection exercised (hex_trace/tests/hex_trace_tests.cpp:253-281)."""
+    worst, tir_rays = 0.0, 0
+    for condition in range(300):
+        k, length = _sweep_case(oracle, condition)
+        info, _ = oracle.hex_trace_rays(1.0, length, k, 1.31, 1.0, condition + 700, 100, 1024, 1e-12, 0, 100)
+        assert np.all((info[:, 0] == 0) | (info[:, 0] == 1)), condition
+        bal = np.abs(info[:, 2] + info[:, 3] - 1)
+        worst = max(worst, float(bal.max()))
+        tir_rays += int((info[:, 4] > 3).sum())
+    assert worst < 1e-10 and tir_rays > 0
+
+
+def test_scale_invariance(oracle):
+    """Scaling the prism leaves every exit's direction and power unchanged
+    (hex_trace/tests/hex_trace_tests.cpp:241-251)."""
+    k = [1, -0.4, 0.3]
+    base, ex0 = oracle.hex_trace_rays(0.1, 0.2, k, 1.31, 1.0, 43, 100, 1024, 1e-12, 0, 100)
+    for scale in (1e-6, 1e6):
+        info, ex = oracle.hex_trace_rays(0.1 * scale, 0.2 * scale, k, 1.31, 1.0, 43, 100, 1024, 1e-12, 0, 100)
+        assert np.array_equal(info[:, 1], base[:, 1])
+        assert np.allclose(ex, ex0, rtol=0, atol=1e-12)
