@@ -99,8 +99,9 @@ int icp_context_create(int device, icp_context** out)
                     device, major);
     auto* c = new icp_context();
     c->device = device;
-    cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
-    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    cudaError_t e = cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess && c->sms <= 0) e = cudaErrorInvalidDevice;
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev2);
