@@ -32,6 +32,7 @@
 #include "../../include/icp_b200.h"
 #include "../host/icp_atlas_host.hpp"
 #include "../host/icp_host_math.hpp"
+#include "icp_atlas_window.cuh"
 #include "icp_hex_kernel.cuh"
 #include "icp_internal.h"
 
@@ -355,6 +356,7 @@ __global__ void __launch_bounds__(kComposeThreads, 2) atlas_compose_kernel(const
     double* ws = sm + kTT * np;      // [np]
     const uint32_t t0 = blockIdx.x * kTT;
     const uint32_t p0 = (blockIdx.y * kComposeThreads + threadIdx.x) * kPT;
+    const uint32_t pm = p0 % np;
     double acc[kTT][kPT];
 #pragma unroll
     for (int t = 0; t < kTT; ++t)
@@ -370,9 +372,11 @@ __global__ void __launch_bounds__(kComposeThreads, 2) atlas_compose_kernel(const
             __syncthreads();
             for (uint32_t s = threadIdx.x; s < np; s += blockDim.x) ws[s] = w[((uint64_t)n * 2 + q) * np + s];
             __syncthreads();
-            // row index of output cell p at shift s: m = (p - s) mod np, reflected np-1-m when q = 1
+            // row index of output cell p0 + k at shift s: (p0 + k - s) mod np, reflected np-1-m when
+            // q = 1; m is that of the first cell, stepped down by one per shift
             double win[kTT][kPT];
             bool gap = true;
+            uint32_t m = 0;
             for (uint32_t s = 0; s < np; ++s) {
                 const double wv = ws[s];
                 if (wv == 0) {
@@ -380,17 +384,17 @@ __global__ void __launch_bounds__(kComposeThreads, 2) atlas_compose_kernel(const
                     continue;
                 }
                 if (gap) {
+                    m = phi_sub(pm, s, np);
 #pragma unroll
                     for (int k = 0; k < kPT; ++k) {
-                        const uint32_t m = (uint32_t)(((uint64_t)(p0 + k) % np + np - s) % np);
-                        const uint32_t idx = q ? np - 1 - m : m;
+                        const uint32_t idx = phi_cell(phi_add(m, (uint32_t)k, np), np, q);
 #pragma unroll
                         for (int t = 0; t < kTT; ++t) win[t][k] = rows[t * np + idx];
                     }
                     gap = false;
                 } else {
-                    const uint32_t m = (uint32_t)((p0 % np + np - s) % np);
-                    const uint32_t idx = q ? np - 1 - m : m;
+                    m = phi_prev(m, np);
+                    const uint32_t idx = phi_cell(m, np, q);
 #pragma unroll
                     for (int t = 0; t < kTT; ++t) {
 #pragma unroll
