@@ -19,7 +19,6 @@ batched, limited or resumed.  Records are written in rainbow_generate's format.
 from __future__ import annotations
 
 import argparse
-import ast
 import hashlib
 import json
 import math
@@ -42,23 +41,47 @@ B200_DEFAULTS = {"rays": 10_000_000, "seed": 12345, "precision": "fp32", "max_in
                  "diffraction": False, "batch_records": 32, "max_unresolved_fraction": 1e-4}
 
 
-# ------------------------------------------------------------------ config (reference semantics)
-def fail_constant(value: str) -> None:
-    raise ValueError(f"Nonfinite JSON constant: {value}")
+# ------------------------------------------------------------------ config contract
+# The accepted config file is the reference orchestrator's (generate_phase_dataset.py:33-152):
+# exact decimal parsing of every number, JSON NaN / Infinity refused, booleans only where a
+# flag is meant, the same ranges and the same condition grids.  Field tables drive the checks.
+TOP_KEYS = frozenset({"output_root", "generator", "radius_mm", "force_sphere", "temperature_c", "pressure_pa",
+                      "wavelengths", "inclinations", "solver", "reserve_gib"})
+TOP_FIELDS = {"radius_mm": ("real", 1e-9, 3), "force_sphere": ("bool",), "temperature_c": ("real", 0, 60),
+              "pressure_pa": ("real", 50000, 100000000)}
+SOLVER_FIELDS = {"grid": ("int", 2, 32767), "query_theta": ("int", 1, 32767), "query_phi": ("int", 1, 32767),
+                 "cdf_theta": ("int", 1, 32767), "cdf_phi": ("int", 1, 32767), "device": ("int", 0, 128),
+                 "allow_underresolved": ("bool",), "maximum_coarsening_tv": ("real", 0, 1),
+                 "cdf_max_l1": ("real", 0, 1), "cdf_max_lost_mass": ("real", 0, 1)}
+SOLVER_KEYS = frozenset(SOLVER_FIELDS) | {"stage", "focal_offsets"}
+B200_FIELDS = {"rays": ("int", 1, 10 ** 12), "seed": ("int", 0, 2 ** 62), "max_internal_hits": ("int", 1, 1 << 20),
+               "diffraction": ("bool",), "batch_records": ("int", 1, 4096),
+               "max_unresolved_fraction": ("real", 0, 0.999999)}
+STAGES = ("diffraction", "focal", "path", "incoherent")
+
+
+def _refuse_constant(name: str) -> None:
+    raise ValueError(f"Nonfinite JSON constant: {name}")
 
 
 def load_json(path: Path, limit: int = 8 << 20) -> dict[str, Any]:
+    """A JSON object from a file of at most `limit` bytes (a UTF-8 BOM allowed, NaN refused)."""
     if path.stat().st_size > limit:
         raise ValueError(f"JSON too large: {path}")
-    with path.open("r", encoding="utf-8-sig") as stream:
-        value = json.load(stream, parse_constant=fail_constant)
+    value = json.loads(path.read_text(encoding="utf-8-sig"), parse_constant=_refuse_constant)
     if not isinstance(value, dict):
         raise ValueError(f"Expected JSON object: {path}")
     return value
 
 
-def exact(value: Any) -> Decimal:
-    if isinstance(value, bool):
+def field(value: Any, kind: str, low: Any = None, high: Any = None) -> Any:
+    """One config value: "bool" (JSON true / false only), or a number read exactly as a decimal
+    -- "dec" (any finite), "int" (integral in [low, high]) or "real" ([low, high], as float)."""
+    if kind == "bool":
+        if type(value) is not bool:
+            raise ValueError("Expected JSON true or false")
+        return value
+    if type(value) is bool:
         raise ValueError("Boolean is not a numerical parameter")
     try:
         d = Decimal(str(value))
@@ -66,116 +89,95 @@ def exact(value: Any) -> Decimal:
         raise ValueError(f"Invalid decimal: {value}") from exc
     if not d.is_finite():
         raise ValueError("Nonfinite parameter")
-    return d
-
-
-def scalar(value: Any, low: float, high: float) -> float:
-    d = exact(value)
+    if kind == "dec":
+        return d
+    if kind == "int":
+        if d != d.to_integral_value() or not low <= d <= high:
+            raise ValueError(f"Expected integer in [{low}, {high}]")
+        return int(d)
     if not Decimal(str(low)) <= d <= Decimal(str(high)):
         raise ValueError(f"Parameter {value} is outside [{low}, {high}]")
     return float(d)
 
 
-def integer(value: Any, low: int, high: int) -> int:
-    d = exact(value)
-    if d != d.to_integral_value() or not low <= d <= high:
-        raise ValueError(f"Expected integer in [{low}, {high}]")
-    return int(d)
-
-
-def flag(value: Any) -> bool:
-    if type(value) is not bool:
-        raise ValueError("Expected JSON true or false")
-    return value
+def scalar(value: Any, low: float, high: float) -> float:
+    return field(value, "real", low, high)
 
 
 def fp32(x: float) -> float:
-    return struct.unpack("<f", struct.pack("<f", x))[0]
+    return float(np.float32(x))
 
 
 def wavelengths(spec: dict[str, Any]) -> list[str]:
-    """Inclusive exact-step wavelength list (generate_phase_dataset.py:83-99)."""
+    """Wavelengths start, start + step, ..., stop (stop reached exactly) as decimal strings; no
+    two may round to the same binary32 solver value (generate_phase_dataset.py:83-99)."""
     if set(spec) != {"start_nm", "stop_nm", "step_nm"}:
         raise ValueError("wavelengths needs start_nm, stop_nm, step_nm")
-    start, stop, step = (exact(spec[k]) for k in ("start_nm", "stop_nm", "step_nm"))
-    if not 380 <= start <= stop <= 830 or step <= 0:
+    start, stop, step = (field(spec[k], "dec") for k in ("start_nm", "stop_nm", "step_nm"))
+    if step <= 0 or not 380 <= start <= stop <= 830:
         raise ValueError("Require 380 <= start <= stop <= 830 and positive step")
-    intervals = (stop - start) / step
-    if intervals != intervals.to_integral_value():
+    steps, rest = divmod(stop - start, step)
+    if rest:
         raise ValueError("The wavelength range must contain an integer number of steps; no silent endpoint truncation")
-    count = int(intervals) + 1
-    if count > 100000:
+    if steps >= 100000:
         raise ValueError("Too many wavelengths")
-    values = [format(start + step * i, "f") for i in range(count)]
-    if len({fp32(float(v)) for v in values}) != len(values):
+    values = [format(start + step * i, "f") for i in range(int(steps) + 1)]
+    if np.unique(np.array([float(v) for v in values], dtype=np.float32)).size != len(values):
         raise ValueError("Distinct wavelengths collapse to the same FP32 solver value")
     return values
 
 
 def inclinations(spec: dict[str, Any]) -> list[str]:
-    """Cell-centred inclinations in [min, max] (generate_phase_dataset.py:102-111)."""
+    """Centres of `count` equal cells of [min, max] degrees as decimal strings, each computed as
+    min + (max - min) (i + 1/2) / count (generate_phase_dataset.py:102-111)."""
     if set(spec) != {"min_degrees", "max_degrees", "count", "placement"}:
         raise ValueError("inclinations needs min_degrees, max_degrees, count, placement")
     if spec["placement"] != "linear_angle_cell_centers":
         raise ValueError("Only explicit linear_angle_cell_centers is supported")
-    low, high = exact(spec["min_degrees"]), exact(spec["max_degrees"])
-    count = integer(spec["count"], 1, 100000)
+    low, high = field(spec["min_degrees"], "dec"), field(spec["max_degrees"], "dec")
+    count = field(spec["count"], "int", 1, 100000)
     if not -90 <= low < high <= 90:
         raise ValueError("Canonical inclination domain is [-90,90], NOT [0,180]")
-    return [format(low + (high - low) * (Decimal(i) + Decimal("0.5")) / count, "f") for i in range(count)]
+    half = Decimal("0.5")
+    return [format(low + (high - low) * (Decimal(i) + half) / count, "f") for i in range(count)]
 
 
 def normalized_config(raw: dict[str, Any]) -> dict[str, Any]:
-    """The reference's config contract (generate_phase_dataset.py:114-152) plus the optional
-    "b200" object.  Stages other than "incoherent" are the reference's wave-optics patch model,
-    which this build does not implement: they are rejected, as rainbow_generate rejects them."""
-    allowed = {"output_root", "generator", "radius_mm", "force_sphere", "temperature_c", "pressure_pa",
-               "wavelengths", "inclinations", "solver", "reserve_gib"}
-    if set(raw) - {"b200"} != allowed:
-        raise ValueError(f"Unexpected/missing config keys: {(set(raw) - {'b200'}) ^ allowed}")
-    s = raw["solver"]
-    sk = {"grid", "query_theta", "query_phi", "cdf_theta", "cdf_phi", "stage", "device", "focal_offsets",
-          "allow_underresolved", "maximum_coarsening_tv", "cdf_max_l1", "cdf_max_lost_mass"}
-    if not isinstance(s, dict) or set(s) != sk:
+    """The checked, normalised conditions of a config file.  Beyond the reference's keys an
+    optional "b200" object sets rays, seed, precision, max_internal_hits, diffraction and
+    batch_records.  Stages other than "incoherent" are the reference's wave-optics patch model,
+    which this build does not implement: they are refused, as rainbow_generate refuses them."""
+    keys = set(raw) - {"b200"}
+    if keys != TOP_KEYS:
+        raise ValueError(f"Unexpected/missing config keys: {keys ^ TOP_KEYS}")
+    solver = raw["solver"]
+    if not isinstance(solver, dict) or set(solver) != SOLVER_KEYS:
         raise ValueError("Invalid solver keys")
-    out = {k: integer(s[k], 2 if k == "grid" else 1, 32767)
-           for k in ("grid", "query_theta", "query_phi", "cdf_theta", "cdf_phi")}
-    if out["grid"] ** 2 * 4 > 0xFFFFFFFF:
+    out = {k: field(solver[k], *spec) for k, spec in SOLVER_FIELDS.items()}
+    if 4 * out["grid"] ** 2 > 0xFFFFFFFF:
         raise ValueError("Source index range exceeds the existing solver contract")
-    for axis in ("theta", "phi"):
-        if out["query_" + axis] % out["cdf_" + axis] or out["cdf_" + axis] > out["query_" + axis]:
-            raise ValueError("CDF grids must divide query grids")
-    if s["stage"] not in ("diffraction", "focal", "path", "incoherent"):
+    if any(out["cdf_" + a] > out["query_" + a] or out["query_" + a] % out["cdf_" + a] for a in ("theta", "phi")):
+        raise ValueError("CDF grids must divide query grids")
+    if solver["stage"] not in STAGES:
         raise ValueError("Unknown stage")
-    if s["stage"] != "incoherent":
-        raise ValueError(f"Stage {s['stage']} is the reference's wave-optics patch model, which this build does not "
+    if solver["stage"] != "incoherent":
+        raise ValueError(f"Stage {solver['stage']} is the reference's wave-optics patch model, which this build does not "
                          "implement; use stage incoherent (optionally with b200.diffraction)")
-    out["stage"] = s["stage"]
-    out["device"] = integer(s["device"], 0, 128)
-    out["allow_underresolved"] = flag(s["allow_underresolved"])
-    out["maximum_coarsening_tv"] = scalar(s["maximum_coarsening_tv"], 0, 1)
-    out["cdf_max_l1"] = scalar(s["cdf_max_l1"], 0, 1)
-    out["cdf_max_lost_mass"] = scalar(s["cdf_max_lost_mass"], 0, 1)
-    offsets = s["focal_offsets"]
+    out["stage"] = solver["stage"]
+    offsets = solver["focal_offsets"]
     if not isinstance(offsets, list) or len(offsets) != 4:
         raise ValueError("Four focal offsets required")
-    out["focal_offsets"] = [integer(v, 0, 3) for v in offsets]
-    b = dict(B200_DEFAULTS)
+    out["focal_offsets"] = [field(v, "int", 0, 3) for v in offsets]
     extra = raw.get("b200", {})
     if not isinstance(extra, dict) or not set(extra) <= set(B200_DEFAULTS):
         raise ValueError(f"b200 accepts only {sorted(B200_DEFAULTS)}")
-    b.update(extra)
-    b200 = {"rays": integer(b["rays"], 1, 10 ** 12), "seed": integer(b["seed"], 0, 2 ** 62),
-            "max_internal_hits": integer(b["max_internal_hits"], 1, 1 << 20), "diffraction": flag(b["diffraction"]),
-            "batch_records": integer(b["batch_records"], 1, 4096),
-            "max_unresolved_fraction": scalar(b["max_unresolved_fraction"], 0, 0.999999)}
+    b = {**B200_DEFAULTS, **extra}
+    b200 = {k: field(b[k], *spec) for k, spec in B200_FIELDS.items()}
     if b["precision"] not in ("fp32", "fp64"):
         raise ValueError("b200.precision must be fp32 or fp64")
     b200["precision"] = b["precision"]
-    return {"radius_mm": scalar(raw["radius_mm"], 1e-9, 3), "force_sphere": flag(raw["force_sphere"]),
-            "temperature_c": scalar(raw["temperature_c"], 0, 60),
-            "pressure_pa": scalar(raw["pressure_pa"], 50000, 100000000),
-            "wavelength_nm": wavelengths(raw["wavelengths"]),
+    top = {k: field(raw[k], *spec) for k, spec in TOP_FIELDS.items()}
+    return {**top, "wavelength_nm": wavelengths(raw["wavelengths"]),
             "inclination_degrees": inclinations(raw["inclinations"]),
             "inclination_placement": "linear_angle_cell_centers", "material": "water", "solver": out, "b200": b200}
 
@@ -212,13 +214,15 @@ def write_json(path: Path, value: Any) -> None:
 
 @contextmanager
 def batch_lock(root: Path) -> Iterator[None]:
+    """Exclusive writer lock of a dataset root (created with O_EXCL, removed on exit)."""
     lock = root / ".batch.lock"
     try:
-        with lock.open("x", encoding="ascii") as f:
-            f.write(f"pid={os.getpid()}\n")
+        fd = os.open(lock, os.O_CREAT | os.O_EXCL | os.O_WRONLY, 0o644)
     except FileExistsError as exc:
-        raise RuntimeError("Batch lock exists. Do not run two writers. After verifying that no batch is running, "
-                           "remove the stale .batch.lock manually.") from exc
+        raise RuntimeError("Batch lock exists: another writer may be running. Remove a stale .batch.lock by hand "
+                           "only after checking that no batch is running.") from exc
+    with os.fdopen(fd, "w", encoding="ascii") as f:
+        f.write(f"pid={os.getpid()}\n")
     try:
         yield
     finally:
@@ -237,110 +241,113 @@ def write_npy(path: Path, array: np.ndarray) -> None:
 
 
 def npy_size(path: Path, expected_shape: tuple[int, ...]) -> int:
-    """Header and length validation only (generate_phase_dataset.py:191-218)."""
+    """Byte size of a record array after checking its header (v1 or v2, <f8, C order, the
+    expected shape) and that the file holds exactly that many values (no trailing data)."""
+    fmt = np.lib.format
     with path.open("rb") as f:
-        if f.read(6) != b"\x93NUMPY":
-            raise ValueError(f"Not NPY: {path}")
-        ver = f.read(2)
-        if ver == b"\x01\x00":
-            raw = f.read(2)
-            if len(raw) != 2:
-                raise ValueError("Truncated NPY")
-            length = struct.unpack("<H", raw)[0]
-        elif ver == b"\x02\x00":
-            raw = f.read(4)
-            if len(raw) != 4:
-                raise ValueError("Truncated NPY")
-            length = struct.unpack("<I", raw)[0]
-        else:
+        try:
+            version = fmt.read_magic(f)
+        except ValueError as exc:
+            raise ValueError(f"Not NPY: {path}") from exc
+        if version not in ((1, 0), (2, 0)):
             raise ValueError("Unsupported NPY version")
-        if not 0 < length <= 65536:
-            raise ValueError("Invalid NPY header size")
-        text = f.read(length)
-        if len(text) != length:
-            raise ValueError("Truncated NPY header")
-        h = ast.literal_eval(text.decode("latin1"))
-        if h.get("descr") != "<f8" or h.get("fortran_order") is not False or h.get("shape") != expected_shape:
+        try:
+            shape, fortran, dtype = (fmt.read_array_header_1_0 if version == (1, 0) else fmt.read_array_header_2_0)(f)
+        except ValueError as exc:
+            raise ValueError(f"Invalid NPY header: {path}") from exc
+        if dtype.str != "<f8" or fortran or tuple(shape) != tuple(expected_shape):
             raise ValueError(f"Wrong NPY layout: {path}")
-        expected = f.tell() + 8 * math.prod(expected_shape)
-    if path.stat().st_size != expected:
+        end = f.tell() + 8 * math.prod(expected_shape)
+    if path.stat().st_size != end:
         raise ValueError(f"Truncated or trailing NPY data: {path}")
-    return expected
+    return end
 
 
 def close(a: Any, b: float, tol: float = 1e-12) -> bool:
     return type(a) in (int, float) and math.isfinite(a) and abs(a - b) <= tol * max(1.0, abs(b))
 
 
+def _is_number(x: Any) -> bool:
+    return type(x) in (int, float) and math.isfinite(x)
+
+
+def _frame_ok(rows: Any, alpha_deg: float) -> str | None:
+    """None, or what is wrong with sampling_frame_columns: a right-handed orthonormal 3x3 frame
+    (columns e0, e1, k to 2e-12) whose k is (cos a, -sin a, 0) to 2e-6."""
+    if not (isinstance(rows, list) and len(rows) == 3 and all(isinstance(r, list) and len(r) == 3 for r in rows)):
+        return "frame shape"
+    if not all(_is_number(v) for r in rows for v in r):
+        return "frame values"
+    cols = [[rows[r][j] for r in range(3)] for j in range(3)]
+    if not all(close(sum(x * y for x, y in zip(cols[j], cols[k])), float(j == k), 2e-12)
+               for j in range(3) for k in range(3)):
+        return "frame orthogonality"
+    e0, e1, kk = cols
+    det = sum(c * d for c, d in zip((e0[1] * e1[2] - e0[2] * e1[1], e0[2] * e1[0] - e0[0] * e1[2],
+                                     e0[0] * e1[1] - e0[1] * e1[0]), kk))
+    if not det > 1 - 2e-12:
+        return "frame handedness"
+    a = math.radians(alpha_deg)
+    if any(abs(v - w) >= 2e-6 for v, w in zip(kk, (math.cos(a), -math.sin(a), 0.0))):
+        return "incident direction/sign"
+    return None
+
+
 def verify_record(path: Path, plan: dict[str, Any], ii: int, ll: int) -> dict[str, Any]:
-    """The reference's record verification (generate_phase_dataset.py:227-287) for this
-    generator's records."""
+    """The record checks the reference's orchestrator makes before it trusts a record on resume
+    (generate_phase_dataset.py:227-287): the contract fields, the condition, the water model,
+    the frame, the area and cross sections, the quality and storage gates, the array files.
+    Returns the receipt digest of the record."""
     c, s = plan["conditions"], plan["conditions"]["solver"]
     m = load_json(path / "metadata.json", 1 << 20)
-
-    def require(ok: bool, message: str) -> None:
-        if not ok:
-            raise ValueError(f"{path}: {message}")
-
-    expected = {"complete": True, "schema": "rainbow.phase_cdf.numpy.v2", "generator_version": GENERATOR_VERSION,
-                "coordinate_contract_id": "rainbow.phase_cdf.coordinates.v1",
-                "direction_convention": "physical_propagation", "dtype": "<f8", "order": "C",
-                "density_measure": "solid_angle_sr", "cdf_axis_order": ["phi_cell", "theta_edge"],
-                "theta_count": s["cdf_theta"], "phi_count": s["cdf_phi"],
-                "query_grid": [s["query_theta"], s["query_phi"]], "incident_grid": [s["grid"], s["grid"]],
-                "stage": s["stage"], "force_sphere": c["force_sphere"], "focal_quarter_turn_offsets": s["focal_offsets"]}
-    for key, value in expected.items():
-        require(m.get(key) == value, f"mismatched {key}")
-    require(close(m.get("radius_mm"), fp32(c["radius_mm"])), "radius")
-    require(close(m.get("wavelength_nm"), fp32(float(c["wavelength_nm"][ll]))), "wavelength")
     alpha = float(c["inclination_degrees"][ii])
-    require(close(m.get("incident_inclination_degrees"), alpha), "inclination")
-    material = m.get("material", {})
-    require(material.get("model") == "water_iapws_r9_97", "material")
-    require(close(material.get("temperature_kelvin"), c["temperature_c"] + 273.15), "temperature")
-    require(close(material.get("pressure_pascal"), c["pressure_pa"]), "pressure")
-    mat = m.get("sampling_frame_columns", [])
-    require(isinstance(mat, list) and len(mat) == 3 and all(isinstance(r, list) and len(r) == 3 for r in mat),
-            "frame shape")
-    require(all(type(v) in (int, float) and math.isfinite(v) for r in mat for v in r), "frame values")
-    cols = [[mat[r][j] for r in range(3)] for j in range(3)]
-    for j in range(3):
-        for k in range(3):
-            require(close(sum(cols[j][r] * cols[k][r] for r in range(3)), float(j == k), 2e-12), "frame orthogonality")
-    cross = [cols[0][1] * cols[1][2] - cols[0][2] * cols[1][1], cols[0][2] * cols[1][0] - cols[0][0] * cols[1][2],
-             cols[0][0] * cols[1][1] - cols[0][1] * cols[1][0]]
-    require(sum(cross[r] * cols[2][r] for r in range(3)) > 1 - 2e-12, "frame handedness")
-    angle = math.radians(alpha)
-    ki = [math.cos(angle), -math.sin(angle), 0.0]
-    require(all(abs(cols[2][r] - ki[r]) < 2e-6 for r in range(3)), "incident direction/sign")
-    geometry, cs = m.get("geometry", {}), m.get("cross_sections", {})
+    geometry, cs, q = m.get("geometry", {}), m.get("cross_sections", {}), m.get("quality", {})
+    sp, hg, material = m.get("storage_processing", {}), m.get("hg", {}), m.get("material", {})
     area = geometry.get("projected_area_mm2")
-    require(type(area) in (int, float) and math.isfinite(area) and area > 0, "projected area")
-    require(geometry.get("projected_area_converged") is True and geometry.get("convexity_verified") is True,
-            "area validation")
-    require(cs.get("model") == "geometric_nonabsorbing" and cs.get("wave_scattering_cross_section_computed") is False,
-            "cross-section model")
-    require(cs.get("scattering_mm2") == area and cs.get("extinction_mm2") == area and cs.get("absorption_mm2") == 0,
-            "cross sections")
-    q = m.get("quality", {})
-    require(q.get("invalid_values") == 0 and q.get("incomplete_directions") == 0, "invalid optical data")
-    require(q.get("allow_underresolved") is s["allow_underresolved"], "underresolution policy")
-    require(s["allow_underresolved"] or q.get("underresolved_directions") == 0, "underresolution not authorized")
-    for key, cfg in (("cdf_l1_mass_error", "cdf_max_l1"), ("cdf_lost_probability_mass", "cdf_max_lost_mass")):
-        value = q.get(key)
-        require(type(value) in (int, float) and math.isfinite(value) and 0 <= value <= s[cfg], key)
-    sp = m.get("storage_processing", {})
-    require(sp.get("additional_filter") == "none", "unexpected global smoothing")
+    fields = {"complete": True, "schema": "rainbow.phase_cdf.numpy.v2", "generator_version": GENERATOR_VERSION,
+              "coordinate_contract_id": "rainbow.phase_cdf.coordinates.v1",
+              "direction_convention": "physical_propagation", "dtype": "<f8", "order": "C",
+              "density_measure": "solid_angle_sr", "cdf_axis_order": ["phi_cell", "theta_edge"],
+              "theta_count": s["cdf_theta"], "phi_count": s["cdf_phi"], "query_grid": [s["query_theta"], s["query_phi"]],
+              "incident_grid": [s["grid"], s["grid"]], "stage": s["stage"], "force_sphere": c["force_sphere"],
+              "focal_quarter_turn_offsets": s["focal_offsets"]}
+    checks = [(f"mismatched {k}", m.get(k) == v) for k, v in fields.items()]
+    checks += [("radius", close(m.get("radius_mm"), fp32(c["radius_mm"]))),
+               ("wavelength", close(m.get("wavelength_nm"), fp32(float(c["wavelength_nm"][ll])))),
+               ("inclination", close(m.get("incident_inclination_degrees"), alpha)),
+               ("material", material.get("model") == "water_iapws_r9_97"),
+               ("temperature", close(material.get("temperature_kelvin"), c["temperature_c"] + 273.15)),
+               ("pressure", close(material.get("pressure_pascal"), c["pressure_pa"]))]
+    for what, ok in checks:
+        if not ok:
+            raise ValueError(f"{path}: {what}")
+    bad_frame = _frame_ok(m.get("sampling_frame_columns", []), alpha)
+    lim = {"cdf_l1_mass_error": s["cdf_max_l1"], "cdf_lost_probability_mass": s["cdf_max_lost_mass"]}
     tv = sp.get("coarsening_tv")
-    require(type(tv) in (int, float) and math.isfinite(tv) and 0 <= tv <= s["maximum_coarsening_tv"],
-            "coarsening error")
-    hg = m.get("hg", {})
-    require(hg.get("target") == "saved_cdf" and type(hg.get("g")) in (float, int) and -1 < hg["g"] < 1, "HG target")
+    checks = [(bad_frame or "", bad_frame is None),
+              ("projected area", _is_number(area) and area > 0),
+              ("area validation", geometry.get("projected_area_converged") is True
+               and geometry.get("convexity_verified") is True),
+              ("cross-section model", cs.get("model") == "geometric_nonabsorbing"
+               and cs.get("wave_scattering_cross_section_computed") is False),
+              ("cross sections", cs.get("scattering_mm2") == area and cs.get("extinction_mm2") == area
+               and cs.get("absorption_mm2") == 0),
+              ("invalid optical data", q.get("invalid_values") == 0 and q.get("incomplete_directions") == 0),
+              ("underresolution policy", q.get("allow_underresolved") is s["allow_underresolved"]),
+              ("underresolution not authorized", s["allow_underresolved"] or q.get("underresolved_directions") == 0)]
+    checks += [(k, _is_number(q.get(k)) and 0 <= q.get(k) <= bound) for k, bound in lim.items()]
+    checks += [("unexpected global smoothing", sp.get("additional_filter") == "none"),
+               ("coarsening error", _is_number(tv) and 0 <= tv <= s["maximum_coarsening_tv"]),
+               ("HG target", hg.get("target") == "saved_cdf" and type(hg.get("g")) in (float, int)
+                and -1 < hg["g"] < 1)]
+    for what, ok in checks:
+        if not ok:
+            raise ValueError(f"{path}: {what}")
     nt, np_ = s["cdf_theta"], s["cdf_phi"]
-    sizes = {name: npy_size(path / name, shape)
-             for name, shape in zip(ARRAYS, ((np_ + 1,), (np_, nt + 1), (nt + 1,)))}
-    return {"metadata_sha256": sha256(path / "metadata.json"), "npy_sizes": sizes, "hg_g": hg["g"],
-            "projected_area_mm2": area, "underresolved_directions": q.get("underresolved_directions"),
+    shapes = ((np_ + 1,), (np_, nt + 1), (nt + 1,))
+    return {"metadata_sha256": sha256(path / "metadata.json"),
+            "npy_sizes": {name: npy_size(path / name, shape) for name, shape in zip(ARRAYS, shapes)},
+            "hg_g": hg["g"], "projected_area_mm2": area, "underresolved_directions": q.get("underresolved_directions"),
             "coarsening_tv": tv}
 
 
@@ -517,7 +524,7 @@ def generate(icp, ctx, c: dict, todo: list) -> list:
     return [(specs[i], waters[i], out.phi[i], out.theta[i], out.u_edges, out.reports[i]) for i in range(len(todo))]
 
 
-def run(argv: list[str] | None = None, backend=None) -> int:
+def _arguments(argv: list[str] | None) -> argparse.Namespace:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--config", type=Path, required=True)
     ap.add_argument("--out-root", type=Path)
@@ -534,106 +541,141 @@ def run(argv: list[str] | None = None, backend=None) -> int:
     args = ap.parse_args(argv)
     if args.limit is not None and args.limit <= 0:
         raise ValueError("limit must be positive")
-    raw = load_json(args.config)
-    if args.wavelength_range:
-        raw["wavelengths"] = dict(zip(("start_nm", "stop_nm", "step_nm"), args.wavelength_range))
-    if args.radius_mm is not None:
-        raw["radius_mm"] = args.radius_mm
-    if args.inclination_count is not None:
-        raw["inclinations"]["count"] = args.inclination_count
-    if args.allow_underresolved:
-        raw["solver"]["allow_underresolved"] = True
-    c = normalized_config(raw)
-    root = Path(args.out_root or raw["output_root"])
-    root = (root if root.is_absolute() else Path.cwd() / root).resolve()
-    reserve = int(scalar(raw["reserve_gib"], 0, 1000000) * (1 << 30))
-    nt, np_ = c["solver"]["cdf_theta"], c["solver"]["cdf_phi"]
-    payload = 8 * ((np_ + 1) + np_ * (nt + 1) + (nt + 1))
-    estimate_per_record = payload + (128 << 10)
-    ni, nl = len(c["inclination_degrees"]), len(c["wavelength_nm"])
-    print(f"conditions={ni} x {nl} = {ni * nl}; CDF={nt}x{np_}; array_bytes_per_record={payload}")
-    print(f"array_total_TB={payload * ni * nl / 1e12:.6f}; output={root}")
-    print(f"inclination_centers=[{c['inclination_degrees'][0]}, {c['inclination_degrees'][-1]}] degrees")
-    print(f"wavelengths=[{c['wavelength_nm'][0]}, {c['wavelength_nm'][-1]}] nm; inclusive exact-step endpoints")
-    print(f"Batches of {c['b200']['batch_records']} records per persistent GPU launch; "
-          f"{c['b200']['rays']} rays per record ({c['b200']['precision']}).")
-    if c["solver"]["maximum_coarsening_tv"] == 1:
-        print("WARNING: maximum_coarsening_tv=1 is not an accuracy acceptance threshold.")
-    if not args.execute:
-        print("DRY RUN: no simulations or files written. Add --execute to start.")
-        return 0
-    backend = backend or GpuBackend()
-    spec = {"version": VERSION, "conditions": c, "binary_sha256": {"libicp_b200": backend.library_sha256()}}
-    signature = object_hash(spec)
-    plan = {**spec, "signature": signature, "record_layout": "records/i{incident_index:04d}/w{wavelength_index:04d}"}
-    root.mkdir(parents=True, exist_ok=True)
-    with batch_lock(root):
-        manifest = root / "batch_plan.json"
+    return args
+
+
+class DatasetRun:
+    """One invocation over a dataset root: the plan (conditions + library hash, signed), the scan
+    of what exists (every existing record re-verified against its receipt), then the pending
+    conditions in GPU batches, each record written through .part, verified and receipted."""
+
+    def __init__(self, args: argparse.Namespace, backend=None):
+        raw = load_json(args.config)
+        overrides = {"radius_mm": args.radius_mm}
+        if args.wavelength_range:
+            raw["wavelengths"] = dict(zip(("start_nm", "stop_nm", "step_nm"), args.wavelength_range))
+        raw.update({k: v for k, v in overrides.items() if v is not None})
+        if args.inclination_count is not None:
+            raw["inclinations"]["count"] = args.inclination_count
+        if args.allow_underresolved:
+            raw["solver"]["allow_underresolved"] = True
+        self.args, self.backend = args, backend
+        self.c = normalized_config(raw)
+        root = Path(args.out_root or raw["output_root"])
+        self.root = (root if root.is_absolute() else Path.cwd() / root).resolve()
+        self.reserve = int(scalar(raw["reserve_gib"], 0, 1000000) * (1 << 30))
+        nt, np_ = self.c["solver"]["cdf_theta"], self.c["solver"]["cdf_phi"]
+        self.payload = 8 * ((np_ + 1) + np_ * (nt + 1) + (nt + 1))
+        self.per_record = self.payload + (128 << 10)  # arrays + metadata, receipt and progress allowance
+        self.ni, self.nl = len(self.c["inclination_degrees"]), len(self.c["wavelength_nm"])
+
+    def summary(self) -> None:
+        c, n = self.c, self.ni * self.nl
+        s, b = c["solver"], c["b200"]
+        print(f"conditions={self.ni} x {self.nl} = {n}; CDF={s['cdf_theta']}x{s['cdf_phi']}; "
+              f"array_bytes_per_record={self.payload}")
+        print(f"array_total_TB={self.payload * n / 1e12:.6f}; output={self.root}")
+        print(f"inclination_centers=[{c['inclination_degrees'][0]}, {c['inclination_degrees'][-1]}] degrees")
+        print(f"wavelengths=[{c['wavelength_nm'][0]}, {c['wavelength_nm'][-1]}] nm; inclusive exact-step endpoints")
+        print(f"Batches of {b['batch_records']} records per persistent GPU launch; {b['rays']} rays per record "
+              f"({b['precision']}).")
+        if s["maximum_coarsening_tv"] == 1:
+            print("WARNING: maximum_coarsening_tv=1 is not an accuracy acceptance threshold.")
+
+    def plan(self) -> tuple[dict, str]:
+        """The signed plan, written on first use and required to be identical on --resume."""
+        spec = {"version": VERSION, "conditions": self.c,
+                "binary_sha256": {"libicp_b200": self.backend.library_sha256()}}
+        signature = object_hash(spec)
+        plan = {**spec, "signature": signature, "record_layout": "records/i{incident_index:04d}/w{wavelength_index:04d}"}
+        manifest = self.root / "batch_plan.json"
         if manifest.exists():
-            if not args.resume:
+            if not self.args.resume:
                 raise FileExistsError("Dataset plan exists; use --resume with identical configuration and binaries")
             if load_json(manifest) != json.loads(json.dumps(plan)):
                 raise ValueError("Resume rejected: configuration/binaries differ from batch_plan.json")
         else:
-            if any(p.name != ".batch.lock" for p in root.iterdir()):
+            if any(p.name != ".batch.lock" for p in self.root.iterdir()):
                 raise ValueError("Refusing to adopt a nonempty directory without this batch plan")
             write_json(manifest, plan)
-        plan = load_json(manifest)
-        pending, skipped = [], 0
-        for ii in range(ni):
-            for ll in range(nl):
+        return load_json(manifest), signature
+
+    def scan(self, plan: dict, signature: str) -> tuple[list, int]:
+        """(pending conditions, number of existing records verified against their receipts)."""
+        pending, verified = [], 0
+        for ii in range(self.ni):
+            for ll in range(self.nl):
                 job = f"i{ii:04d}_w{ll:04d}"
-                path = root / f"records/i{ii:04d}/w{ll:04d}"
-                receipt = root / "receipts" / (job + ".json")
-                if Path(str(path) + ".part").exists():
+                path = self.root / "records" / f"i{ii:04d}" / f"w{ll:04d}"
+                receipt = self.root / "receipts" / f"{job}.json"
+                if path.with_name(path.name + ".part").exists():
                     raise ValueError(f"Incomplete .part exists: {path}.part; inspect and move it manually before retrying")
-                if path.exists():
-                    if not args.resume or not receipt.exists():
-                        raise ValueError(f"Existing record without authorized resume/receipt: {path}")
-                    saved = load_json(receipt)
-                    actual = verify_record(path, plan, ii, ll)
-                    if (saved.get("signature") != signature or saved.get("incident_index") != ii
-                            or saved.get("wavelength_index") != ll or saved.get("record") != actual):
-                        raise ValueError(f"Resume receipt/content mismatch: {path}")
-                    skipped += 1
-                else:
+                if not path.exists():
                     if receipt.exists():
                         raise ValueError(f"Receipt exists but record missing: {path}")
                     pending.append((ii, ll, job, path, receipt))
-        selected = pending if args.limit is None else pending[:args.limit]
-        needed = len(selected) * estimate_per_record + reserve
-        free = shutil.disk_usage(root).free
-        print(f"verified_existing={skipped}; pending={len(pending)}; this_run={len(selected)}; free_TB={free / 1e12:.3f}")
-        if needed > free:
-            raise RuntimeError(f"Insufficient free space: estimated {needed} bytes including reserve; available {free}")
-        start = time.monotonic()
-        done = 0
-        per = c["b200"]["batch_records"]
-        with backend.context(c["solver"]["device"]) as ctx:
-            for b0 in range(0, len(selected), per):
-                chunk = selected[b0:b0 + per]
-                free = shutil.disk_usage(root).free
-                if free < len(chunk) * estimate_per_record + reserve:
-                    raise RuntimeError("Free-space reserve reached; stopping without lowering precision")
-                results = backend.generate(ctx, c, [(ii, ll) for ii, ll, *_ in chunk])
-                for (ii, ll, job, path, receipt), (sp, water, phi, theta, u, rep) in zip(chunk, results):
-                    accept(rep, c)
-                    path.parent.mkdir(parents=True, exist_ok=True)
-                    write_record(path, phi, theta, u, record_metadata(c, ii, ll, sp, rep, water))
-                    checked = verify_record(path, plan, ii, ll)
-                    write_json(receipt, {"signature": signature, "incident_index": ii, "wavelength_index": ll,
-                                         "record": checked})
-                    done += 1
-                    write_json(root / "progress.json", {"completed": skipped + done, "total": ni * nl,
-                                                        "last_record": job,
-                                                        "elapsed_seconds_this_run": time.monotonic() - start})
-                    print(f"[{skipped + done}/{ni * nl}] {job}: alpha={c['inclination_degrees'][ii]} "
-                          f"lambda={c['wavelength_nm'][ll]} g={checked['hg_g']:.9g} "
-                          f"Aproj_mm2={checked['projected_area_mm2']:.9g}", flush=True)
-        complete = skipped + len(selected) == ni * nl
-        write_json(root / "progress.json", {"completed": skipped + len(selected), "total": ni * nl,
-                                            "complete": complete, "elapsed_seconds_this_run": time.monotonic() - start})
-        print("Dataset complete." if complete else "Requested subset finished. Repeat with --resume to continue the same plan.")
+                    continue
+                if not self.args.resume or not receipt.exists():
+                    raise ValueError(f"Existing record without authorized resume/receipt: {path}")
+                saved = load_json(receipt)
+                expected = {"signature": signature, "incident_index": ii, "wavelength_index": ll,
+                            "record": verify_record(path, plan, ii, ll)}
+                if any(saved.get(k) != v for k, v in expected.items()):
+                    raise ValueError(f"Resume receipt/content mismatch: {path}")
+                verified += 1
+        return pending, verified
+
+    def execute(self) -> None:
+        self.root.mkdir(parents=True, exist_ok=True)
+        with batch_lock(self.root):
+            plan, signature = self.plan()
+            pending, verified = self.scan(plan, signature)
+            todo = pending if self.args.limit is None else pending[:self.args.limit]
+            free = shutil.disk_usage(self.root).free
+            print(f"verified_existing={verified}; pending={len(pending)}; this_run={len(todo)}; "
+                  f"free_TB={free / 1e12:.3f}")
+            needed = len(todo) * self.per_record + self.reserve
+            if needed > free:
+                raise RuntimeError(f"Insufficient free space: estimated {needed} bytes including reserve; "
+                                   f"available {free}")
+            total, started, done = self.ni * self.nl, time.monotonic(), 0
+            per = self.c["b200"]["batch_records"]
+            with self.backend.context(self.c["solver"]["device"]) as ctx:
+                for batch in (todo[k:k + per] for k in range(0, len(todo), per)):
+                    if shutil.disk_usage(self.root).free < len(batch) * self.per_record + self.reserve:
+                        raise RuntimeError("Free-space reserve reached; stopping without lowering precision")
+                    results = self.backend.generate(ctx, self.c, [(ii, ll) for ii, ll, *_ in batch])
+                    for (ii, ll, job, path, receipt), (sp, water, phi, theta, u, rep) in zip(batch, results):
+                        accept(rep, self.c)
+                        path.parent.mkdir(parents=True, exist_ok=True)
+                        write_record(path, phi, theta, u, record_metadata(self.c, ii, ll, sp, rep, water))
+                        digest = verify_record(path, plan, ii, ll)
+                        write_json(receipt, {"signature": signature, "incident_index": ii, "wavelength_index": ll,
+                                             "record": digest})
+                        done += 1
+                        write_json(self.root / "progress.json",
+                                   {"completed": verified + done, "total": total, "last_record": job,
+                                    "elapsed_seconds_this_run": time.monotonic() - started})
+                        print(f"[{verified + done}/{total}] {job}: alpha={self.c['inclination_degrees'][ii]} "
+                              f"lambda={self.c['wavelength_nm'][ll]} g={digest['hg_g']:.9g} "
+                              f"Aproj_mm2={digest['projected_area_mm2']:.9g}", flush=True)
+            complete = verified + len(todo) == total
+            write_json(self.root / "progress.json", {"completed": verified + len(todo), "total": total,
+                                                     "complete": complete,
+                                                     "elapsed_seconds_this_run": time.monotonic() - started})
+            print("Dataset complete." if complete else
+                  "Requested subset finished. Repeat with --resume to continue the same plan.")
+
+
+def run(argv: list[str] | None = None, backend=None) -> int:
+    args = _arguments(argv)
+    job = DatasetRun(args, backend)
+    job.summary()
+    if not args.execute:
+        print("DRY RUN: no simulations or files written. Add --execute to start.")
+        return 0
+    job.backend = backend or GpuBackend()
+    job.execute()
     return 0
 
 
