@@ -1,7 +1,12 @@
-"""Record validation used by the tests: the checks of the reference's record reader
-(python/rainbow_dataset/record.py:19-158, PhaseRecord(validate=True)) restated, so that every
-record this repository writes is held to the consumer's contract on hosts without the
-reference checkout.
+"""Record validation for the tests: every record this repository writes is held to the contract
+the reference's record reader enforces (python/rainbow_dataset/record.py:19-158,
+PhaseRecord(validate=True)), on hosts without the reference checkout.
+
+The contract, as checked here: a complete v1/v2 record (not a .part directory); fixed layout
+strings; positive int32 grid sizes; three <f8 C-order arrays of the right shapes with no
+trailing bytes; a right-handed orthonormal sampling frame (2e-12); strictly increasing u edges
+from 0 to 1; a marginal CDF from 0 to 1, non-decreasing; conditional CDFs in [0, 1] from 0 to 1,
+non-decreasing; for v2, the HG label is the first moment of the saved cells (5e-12, mass 1e-10).
 """
 from __future__ import annotations
 
@@ -10,66 +15,66 @@ from pathlib import Path
 
 import numpy as np
 
-SCHEMAS = {"rainbow.phase_cdf.numpy.v1", "rainbow.phase_cdf.numpy.v2"}
+FIXED = {"dtype": "<f8", "order": "C", "density_measure": "solid_angle_sr",
+         "cell_model": "constant_density_per_spherical_cell", "coordinates": "u=(1-cos(theta))/2; v=(phi+pi)/(2*pi)",
+         "normalization": "integral_p_domega_equals_one", "input_polarization": "unpolarized",
+         "cdf_axis_order": ["phi_cell", "theta_edge"]}
+HG = {"method": "first_moment_of_saved_cell_pdf", "target": "saved_cdf",
+      "cosine_convention": "dot(incident_propagation,outgoing_propagation)"}
 
 
-def load_npy(path: Path, shape: tuple) -> np.ndarray:
+def _array(path: Path, shape: tuple) -> np.ndarray:
     a = np.load(path, mmap_mode="r", allow_pickle=False)
-    if a.dtype.str != "<f8" or a.shape != shape or not a.flags.c_contiguous:
-        raise ValueError(f"Unexpected shape/dtype/order in {path.name}")
-    if path.stat().st_size != a.offset + a.nbytes:
-        raise ValueError(f"Truncated or trailing data in {path.name}")
+    ok = a.dtype.str == "<f8" and a.shape == shape and a.flags.c_contiguous
+    if not ok or path.stat().st_size != a.offset + a.nbytes:
+        raise ValueError(f"{path.name}: layout or length differs from the record contract")
     return np.array(a)
+
+
+def _fail(what: str) -> None:
+    raise ValueError(f"record contract: {what}")
 
 
 def validate_record(directory: str | Path) -> dict:
     d = Path(directory)
     if d.name.endswith(".part"):
-        raise ValueError("An incomplete .part directory is not a dataset record")
+        _fail("a .part directory is incomplete")
     m = json.loads((d / "metadata.json").read_text(encoding="utf-8"))
-    if m.get("schema") not in SCHEMAS or m.get("complete") is not True:
-        raise ValueError("Unknown schema or incomplete record")
-    for key, expected in {"dtype": "<f8", "order": "C", "density_measure": "solid_angle_sr",
-                          "cell_model": "constant_density_per_spherical_cell",
-                          "coordinates": "u=(1-cos(theta))/2; v=(phi+pi)/(2*pi)",
-                          "normalization": "integral_p_domega_equals_one", "input_polarization": "unpolarized"}.items():
-        if m.get(key) != expected:
-            raise ValueError(f"Unsupported {key}: {m.get(key)!r}")
-    if m.get("cdf_axis_order") != ["phi_cell", "theta_edge"]:
-        raise ValueError("Conditional CDF axes are not phi_cell, theta_edge")
+    v2 = m.get("schema") == "rainbow.phase_cdf.numpy.v2"
+    if not (v2 or m.get("schema") == "rainbow.phase_cdf.numpy.v1") or m.get("complete") is not True:
+        _fail("schema / completeness")
+    for key in (k for k, v in FIXED.items() if m.get(k) != v):
+        _fail(f"field {key}")
     nt, np_ = m["theta_count"], m["phi_count"]
-    if type(nt) is not int or type(np_) is not int or not (1 <= nt <= 0x7FFFFFFF and 1 <= np_ <= 0x7FFFFFFF):
-        raise ValueError("Invalid angular dimension")
-    a = load_npy(d / "phi_cdf.npy", (np_ + 1,))
-    t = load_npy(d / "theta_given_phi_cdf.npy", (np_, nt + 1))
-    u = load_npy(d / "u_edges.npy", (nt + 1,))
-    frame = np.asarray(m["sampling_frame_columns"], dtype=np.float64)
-    if (frame.shape != (3, 3) or not np.isfinite(frame).all()
-            or not np.allclose(frame.T @ frame, np.eye(3), rtol=0, atol=2e-12)
-            or not np.isclose(np.linalg.det(frame), 1.0, rtol=0, atol=2e-12)):
-        raise ValueError("Sampling frame must be a right-handed orthonormal frame")
-    if not np.isfinite(u).all() or u[0] != 0 or u[-1] != 1 or not np.all(np.diff(u) > 0):
-        raise ValueError("u_edges are not strictly increasing from 0 to 1")
-    if not np.isfinite(a).all() or a[0] != 0 or a[-1] != 1 or not np.all(np.diff(a) >= 0):
-        raise ValueError("Marginal CDF is invalid")
-    if not np.isfinite(t).all() or np.any(t < 0) or np.any(t > 1):
-        raise ValueError("Conditional CDF contains nonfinite or out-of-range data")
-    if np.any(t[:, 0] != 0) or np.any(t[:, -1] != 1):
-        raise ValueError("Conditional CDF endpoints must be 0 and 1")
-    if np.any(np.diff(t, axis=1) < 0):
-        raise ValueError("Conditional CDF decreases; refusing to repair it")
-    if m["schema"].endswith(".v2"):
+    if not all(type(n) is int and 0 < n < 2 ** 31 for n in (nt, np_)):
+        _fail("grid size")
+    a = _array(d / "phi_cdf.npy", (np_ + 1,))
+    t = _array(d / "theta_given_phi_cdf.npy", (np_, nt + 1))
+    u = _array(d / "u_edges.npy", (nt + 1,))
+    f = np.asarray(m["sampling_frame_columns"], dtype=np.float64)
+    dt = np.diff(t, axis=1)
+    checks = {
+        "sampling frame": f.shape == (3, 3) and np.isfinite(f).all()
+        and np.max(np.abs(f.T @ f - np.eye(3))) <= 2e-12 and abs(np.linalg.det(f) - 1) <= 2e-12,
+        "u edges": np.isfinite(u).all() and u[0] == 0 and u[-1] == 1 and bool(np.all(np.diff(u) > 0)),
+        "marginal CDF": np.isfinite(a).all() and a[0] == 0 and a[-1] == 1 and bool(np.all(np.diff(a) >= 0)),
+        "conditional CDF range": np.isfinite(t).all() and bool(np.all((t >= 0) & (t <= 1))),
+        "conditional CDF ends": bool(np.all(t[:, 0] == 0) and np.all(t[:, -1] == 1)),
+        "conditional CDF order": bool(np.all(dt >= 0)),
+    }
+    for what in (k for k, ok in checks.items() if not ok):
+        _fail(what)
+    cells = np.diff(a)[:, None] * dt
+    if v2:
         hg = m.get("hg", {})
-        if (hg.get("method") != "first_moment_of_saved_cell_pdf" or hg.get("target") != "saved_cdf"
-                or hg.get("cosine_convention") != "dot(incident_propagation,outgoing_propagation)"):
-            raise ValueError("Unsupported HG moment convention")
+        if any(hg.get(k) != v for k, v in HG.items()):
+            _fail("HG convention")
         g = hg.get("g")
         if type(g) not in (int, float) or not np.isfinite(g) or not -1 < g < 1:
-            raise ValueError("Invalid HG first moment")
-        mean_mu = (1.0 - (u[:-1] + u[1:])).astype(np.longdouble)
-        q = np.diff(a).astype(np.longdouble)[:, None] * np.diff(t, axis=1).astype(np.longdouble)
-        mass = q.sum(dtype=np.longdouble)
-        axial = (q * mean_mu[None, :]).sum(dtype=np.longdouble)
-        if abs(float(mass) - 1.0) > 1e-10 or abs(float(axial / mass) - float(g)) > 5e-12:
-            raise ValueError("HG label is inconsistent with saved CDF")
-    return {"metadata": m, "phi": a, "theta": t, "u": u, "cell_probability": np.diff(a)[:, None] * np.diff(t, axis=1)}
+            _fail("HG value")
+        q = cells.astype(np.longdouble)
+        total = q.sum()
+        axial = (q * (1.0 - (u[:-1] + u[1:])).astype(np.longdouble)[None, :]).sum()
+        if abs(float(total) - 1.0) > 1e-10 or abs(float(axial / total) - float(g)) > 5e-12:
+            _fail("HG label differs from the saved CDF's first moment")
+    return {"metadata": m, "phi": a, "theta": t, "u": u, "cell_probability": cells}
