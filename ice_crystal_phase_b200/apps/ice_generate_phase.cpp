@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "icp_b200.h"
+#include "icp_cli_options.hpp"
 #include "icp_host_math.hpp"
 #include "icp_record_io.hpp"
 
@@ -54,45 +55,44 @@ template <class T> T number(std::string_view s)
 Options parse(int argc, char** argv)
 {
     Options o;
-    for (int i = 1; i < argc; ++i) {
-        const std::string key = argv[i];
-        if (!o.seen.insert(key).second) throw std::invalid_argument("Duplicate option: " + key);
-        auto next = [&]() -> std::string_view {
-            if (++i >= argc) throw std::invalid_argument("Missing value: " + key);
-            return argv[i];
-        };
-        if (key == "--out") o.out = next();
-        else if (key == "--orientations") o.orientations = next();
-        else if (key == "--modules") (void)next();
-        else if (key == "--radius-mm") o.R = number<double>(next());
-        else if (key == "--length-mm") o.L = number<double>(next());
-        else if (key == "--ki") { for (double& k : o.ki) k = number<double>(next()); }
-        else if (key == "--ior") o.ior = number<double>(next());
-        else if (key == "--external-ior") o.external_ior = number<double>(next());
-        else if (key == "--wavelength-nm") o.wavelength = number<double>(next());
-        else if (key == "--theta") o.nt = number<uint32_t>(next());
-        else if (key == "--phi") o.np = number<uint32_t>(next());
-        else if (key == "--cdf-theta") o.ct = number<uint32_t>(next());
-        else if (key == "--cdf-phi") o.cp = number<uint32_t>(next());
-        else if (key == "--batch-size") o.batch = number<uint64_t>(next());
-        else if (key == "--max-output-records") o.max_records = number<uint64_t>(next());
-        else if (key == "--max-internal-hits") o.max_hits = number<uint32_t>(next());
-        else if (key == "--tail-tolerance") o.tail = number<double>(next());
-        else if (key == "--max-unresolved-fraction") o.max_unresolved = number<double>(next());
-        else if (key == "--max-balance-error") o.max_balance = number<double>(next());
-        else if (key == "--max-histogram-relative-error") o.max_hist_err = number<double>(next());
-        else if (key == "--cdf-max-l1") o.max_l1 = number<double>(next());
-        else if (key == "--cdf-max-lost-mass") o.max_lost = number<double>(next());
-        else if (key == "--max-coarsening-tv") o.max_tv = number<double>(next());
-        else if (key == "--device") o.device = number<int>(next());
-        else if (key == "--trace-precision") {
-            const auto v = next();
-            if (v == "fp32") o.precision = ICP_FP32;
-            else if (v == "fp64") o.precision = ICP_FP64;
-            else throw std::invalid_argument("--trace-precision must be fp32 or fp64");
-        } else
-            throw std::invalid_argument("Unknown option: " + key);
-    }
+    using V = icp::cli::Values;
+    auto real = [](double& x) { return icp::cli::Flag{1, [&x](const V& v) { x = number<double>(v[0]); }}; };
+    auto u32 = [](uint32_t& x) { return icp::cli::Flag{1, [&x](const V& v) { x = number<uint32_t>(v[0]); }}; };
+    auto u64 = [](uint64_t& x) { return icp::cli::Flag{1, [&x](const V& v) { x = number<uint64_t>(v[0]); }}; };
+    const icp::cli::Table table = {
+        {"--out", {1, [&](const V& v) { o.out = std::string(v[0]); }}},
+        {"--orientations", {1, [&](const V& v) { o.orientations = std::string(v[0]); }}},
+        {"--modules", {1, [](const V&) {}}},
+        {"--radius-mm", real(o.R)},
+        {"--length-mm", real(o.L)},
+        {"--ki", {3, [&](const V& v) { for (int k = 0; k < 3; ++k) o.ki[k] = number<double>(v[k]); }}},
+        {"--ior", real(o.ior)},
+        {"--external-ior", real(o.external_ior)},
+        {"--wavelength-nm", real(o.wavelength)},
+        {"--theta", u32(o.nt)},
+        {"--phi", u32(o.np)},
+        {"--cdf-theta", u32(o.ct)},
+        {"--cdf-phi", u32(o.cp)},
+        {"--batch-size", u64(o.batch)},
+        {"--max-output-records", u64(o.max_records)},
+        {"--max-internal-hits", u32(o.max_hits)},
+        {"--tail-tolerance", real(o.tail)},
+        {"--max-unresolved-fraction", real(o.max_unresolved)},
+        {"--max-balance-error", real(o.max_balance)},
+        {"--max-histogram-relative-error", real(o.max_hist_err)},
+        {"--cdf-max-l1", real(o.max_l1)},
+        {"--cdf-max-lost-mass", real(o.max_lost)},
+        {"--max-coarsening-tv", real(o.max_tv)},
+        {"--device", {1, [&](const V& v) { o.device = number<int>(v[0]); }}},
+        {"--trace-precision", {1, [&](const V& v) {
+             if (v[0] == "fp32") o.precision = ICP_FP32;
+             else if (v[0] == "fp64") o.precision = ICP_FP64;
+             else throw std::invalid_argument("--trace-precision must be fp32 or fp64");
+         }}},
+    };
+    const icp::cli::Style style{true, false, [](const std::string& f) { return "Duplicate option: " + f; },
+                                [](const std::string& f) { return "Missing value: " + f; }};
+    o.seen = icp::cli::apply(argc, argv, table, style);
     for (const char* k : {"--out", "--orientations", "--radius-mm", "--length-mm", "--ki", "--ior", "--wavelength-nm",
                           "--theta", "--phi"})
         if (!o.seen.count(k)) throw std::invalid_argument(std::string("Required option: ") + k);

@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "icp_b200.h"
+#include "icp_cli_options.hpp"
 #include "icp_host_math.hpp"
 #include "icp_record_io.hpp"
 
@@ -65,37 +66,38 @@ void check(int status)
 Options parse(int argc, char** argv)
 {
     Options o;
-    std::set<std::string> seen;
-    for (int i = 1; i < argc; ++i) {
-        const std::string key = argv[i];
-        if (!seen.insert(key).second || i + 1 >= argc) throw std::invalid_argument("Duplicate option or missing argument.");
-        const std::string v = argv[++i];
-        auto& s = o.s;
-        if (key == "--out") o.out = v;
-        else if (key == "--modules") {}
-        else if (key == "--device") o.device = number<int>(v);
-        else if (key == "--radius-mm") s.circumradius_mm = number<double>(v);
-        else if (key == "--length-mm") s.length_mm = number<double>(v);
-        else if (key == "--material") {
-            if (v == "ice") o.ice = true;
-            else if (v == "constant") o.ice = false;
-            else throw std::invalid_argument("Material must be ice or constant.");
-        } else if (key == "--ior") s.interior_index = number<double>(v);
-        else if (key == "--exterior-ior") s.exterior_index = number<double>(v);
-        else if (key == "--wavelength-nm") o.wavelength = number<double>(v);
-        else if (key == "--incident-theta-intervals") s.theta_intervals = number<uint32_t>(v);
-        else if (key == "--incident-phi-intervals") s.phi_intervals = number<uint32_t>(v);
-        else if (key == "--theta") s.nt = number<uint32_t>(v);
-        else if (key == "--phi") s.np = number<uint32_t>(v);
-        else if (key == "--area-subdivisions") s.subdivisions = number<uint32_t>(v);
-        else if (key == "--batch-rays") o.batch_rays = number<uint32_t>(v);
-        else if (key == "--max-work-mib") o.max_work_mib = number<uint32_t>(v);
-        else if (key == "--max-internal-hits") s.max_internal_hits = number<uint32_t>(v);
-        else if (key == "--tail-tolerance") s.tail_tolerance = number<double>(v);
-        else if (key == "--max-unresolved-fraction") s.max_unresolved_fraction = number<double>(v);
-        else if (key == "--max-balance-error") s.max_balance_error = number<double>(v);
-        else throw std::invalid_argument("Unknown option: " + key);
-    }
+    auto& s = o.s;
+    using V = icp::cli::Values;
+    auto real = [](double& x) { return icp::cli::Flag{1, [&x](const V& v) { x = number<double>(v[0]); }}; };
+    auto u32 = [](uint32_t& x) { return icp::cli::Flag{1, [&x](const V& v) { x = number<uint32_t>(v[0]); }}; };
+    const icp::cli::Table table = {
+        {"--out", {1, [&](const V& v) { o.out = std::string(v[0]); }}},
+        {"--modules", {1, [](const V&) {}}},
+        {"--device", {1, [&](const V& v) { o.device = number<int>(v[0]); }}},
+        {"--radius-mm", real(s.circumradius_mm)},
+        {"--length-mm", real(s.length_mm)},
+        {"--material", {1, [&](const V& v) {
+             if (v[0] == "ice") o.ice = true;
+             else if (v[0] == "constant") o.ice = false;
+             else throw std::invalid_argument("Material must be ice or constant.");
+         }}},
+        {"--ior", real(s.interior_index)},
+        {"--exterior-ior", real(s.exterior_index)},
+        {"--wavelength-nm", real(o.wavelength)},
+        {"--incident-theta-intervals", u32(s.theta_intervals)},
+        {"--incident-phi-intervals", u32(s.phi_intervals)},
+        {"--theta", u32(s.nt)},
+        {"--phi", u32(s.np)},
+        {"--area-subdivisions", u32(s.subdivisions)},
+        {"--batch-rays", u32(o.batch_rays)},
+        {"--max-work-mib", u32(o.max_work_mib)},
+        {"--max-internal-hits", u32(s.max_internal_hits)},
+        {"--tail-tolerance", real(s.tail_tolerance)},
+        {"--max-unresolved-fraction", real(s.max_unresolved_fraction)},
+        {"--max-balance-error", real(s.max_balance_error)},
+    };
+    auto either = [](const std::string&) { return std::string("Duplicate option or missing argument."); };
+    const std::set<std::string> seen = icp::cli::apply(argc, argv, table, icp::cli::Style{true, true, either, either});
     if (o.out.empty()) throw std::invalid_argument("--out required.");
     if (!seen.count("--wavelength-nm")) throw std::invalid_argument("--wavelength-nm is required (vacuum nm).");
     if (o.device < 0) throw std::invalid_argument("Negative CUDA device ordinal.");

@@ -34,6 +34,7 @@
 #include <vector>
 
 #include "icp_b200.h"
+#include "icp_cli_options.hpp"
 #include "icp_host_math.hpp"
 #include "icp_record_io.hpp"
 
@@ -105,104 +106,121 @@ void print_help()
                  "  --max-unresolved-fraction E (1e-4) --max-balance-error E --max-histogram-relative-error E\n";
 }
 
-// Option parsing follows apps/generate_phase.cpp:84-223 (flag set, defaults, messages).
+// Flags, defaults and messages of apps/generate_phase.cpp:84-223: a repeated flag keeps its last
+// value (except --wavelength-nm), every flag other than the three switches carries one value.
+void focal_offsets(std::string_view value, unsigned out[4])
+{
+    size_t begin = 0;
+    for (unsigned k = 0; k < 4; ++k) {
+        const auto end = value.find(',', begin);
+        if ((k < 3 && end == std::string_view::npos) || (k == 3 && end != std::string_view::npos))
+            throw std::invalid_argument("Expected four focal offsets.");
+        const auto part = value.substr(begin, end == std::string_view::npos ? std::string_view::npos : end - begin);
+        const auto r = std::from_chars(part.data(), part.data() + part.size(), out[k]);
+        if (r.ec != std::errc{} || r.ptr != part.data() + part.size() || out[k] > 3)
+            throw std::invalid_argument("Focal offsets must be 0..3.");
+        begin = end == std::string_view::npos ? value.size() : end + 1;
+    }
+}
+unsigned shape_coefficients(std::string_view value, double out[8])
+{
+    unsigned k = 0;
+    for (size_t begin = 0;;) {
+        const auto end = value.find(',', begin);
+        if (k >= 8) throw std::invalid_argument("At most eight shape coefficients.");
+        out[k++] = number(value.substr(begin, end == std::string_view::npos ? std::string_view::npos : end - begin));
+        if (end == std::string_view::npos) return k;
+        begin = end + 1;
+    }
+}
+
 bool parse(int argc, char** argv, Command& c)
 {
+    using V = icp::cli::Values;
     std::string stage = "incoherent";
-    for (int i = 1; i < argc; ++i) {
-        const std::string option = argv[i];
-        if (option == "--sphere") { c.sphere = true; continue; }
-        if (option == "--allow-underresolved") { c.allow_underresolved = true; continue; }
-        if (option == "--help") { print_help(); return false; }
-        if (++i >= argc) throw std::invalid_argument("Missing option value.");
-        const std::string value = argv[i];
-        if (option == "--out") c.output = value;
-        else if (option == "--modules") {}
-        else if (option == "--radius-mm") c.radius_mm = static_cast<float>(number(value));
-        else if (option == "--wavelength-nm") {
-            if (c.wavelength_given) throw std::invalid_argument("Duplicate --wavelength-nm.");
-            c.wavelength_requested_nm = number(value);
-            c.wavelength_given = true;
-            if (!(c.wavelength_requested_nm > 0 && c.wavelength_requested_nm <= (std::numeric_limits<float>::max)()))
-                throw std::invalid_argument("Wavelength must be positive and representable by the solver.");
-            c.wavelength_nm = static_cast<float>(c.wavelength_requested_nm);
-            if (!(c.wavelength_nm > 0)) throw std::invalid_argument("Wavelength underflows solver precision.");
-        } else if (option == "--material") {
-            if (value == "water") c.material = Material::Water;
-            else if (value == "constant") c.material = Material::Constant;
-            else throw std::invalid_argument("Material must be water or constant.");
-        } else if (option == "--temperature-c") { c.temperature_c = number(value); c.state_given = true; }
-        else if (option == "--pressure-pa") { c.pressure_pa = number(value); c.state_given = true; }
-        else if (option == "--ior") { c.constant_index = number(value); c.index_given = true; }
-        else if (option == "--grid") c.grid = positive_integer<uint32_t>(value);
-        else if (option == "--query-theta") c.theta = positive_integer<uint32_t>(value);
-        else if (option == "--query-phi") c.phi = positive_integer<uint32_t>(value);
-        else if (option == "--inclination-deg") c.inclination_deg = number(value);
-        else if (option == "--cdf-theta") c.cdf_theta = positive_integer<uint32_t>(value);
-        else if (option == "--cdf-phi") c.cdf_phi = positive_integer<uint32_t>(value);
-        else if (option == "--storage-gaussian-sigma-deg" || option == "--storage-gaussian-support")
-            throw std::invalid_argument("Global storage blur has been removed from rainbow_generate. Remove this option; only local Table-II diffraction and cell-mass aggregation are applied.");
-        else if (option == "--max-coarsening-tv") c.max_tv = number(value);
-        else if (option == "--diffraction-sigma-deg")
-            throw std::invalid_argument("Manual diffraction width is not supported by rainbow_generate. Remove this option; Table II is selected automatically.");
-        else if (option == "--transition-contrast") c.transition_contrast = number(value);
-        else if (option == "--cdf-max-l1") c.max_l1 = number(value);
-        else if (option == "--cdf-max-lost-mass") c.max_lost = number(value);
-        else if (option == "--device") {
-            const auto r = std::from_chars(value.data(), value.data() + value.size(), c.device);
-            if (r.ec != std::errc{} || r.ptr != value.data() + value.size() || c.device < 0)
-                throw std::invalid_argument("Invalid device ordinal.");
-        } else if (option == "--stage") {
-            if (value != "incoherent" && value != "path" && value != "focal" && value != "diffraction")
-                throw std::invalid_argument("Unknown stage.");
-            stage = value;
-        } else if (option == "--focal-offsets") {
-            size_t begin = 0;
-            for (unsigned k = 0; k < 4; ++k) {
-                const auto end = value.find(',', begin);
-                if ((k < 3 && end == std::string::npos) || (k == 3 && end != std::string::npos))
-                    throw std::invalid_argument("Expected four focal offsets.");
-                const auto length = end == std::string::npos ? value.size() - begin : end - begin;
-                const auto part = std::string_view(value).substr(begin, length);
-                unsigned& x = c.focal_offsets[k];
-                const auto r = std::from_chars(part.data(), part.data() + part.size(), x);
-                if (r.ec != std::errc{} || r.ptr != part.data() + part.size() || x > 3)
-                    throw std::invalid_argument("Focal offsets must be 0..3.");
-                begin = end == std::string::npos ? value.size() : end + 1;
-            }
-        }
-        // ---- extensions
-        else if (option == "--rays") c.rays = positive_integer<uint64_t>(value);
-        else if (option == "--seed") {
-            const auto r = std::from_chars(value.data(), value.data() + value.size(), c.seed);
-            if (r.ec != std::errc{} || r.ptr != value.data() + value.size()) throw std::invalid_argument("Invalid seed.");
-        } else if (option == "--max-internal-hits") c.max_hits = positive_integer<uint32_t>(value);
-        else if (option == "--tail-tolerance") c.tail = number(value);
-        else if (option == "--max-unresolved-fraction") c.max_unresolved = number(value);
-        else if (option == "--max-balance-error") c.max_balance = number(value);
-        else if (option == "--max-histogram-relative-error") c.max_hist_err = number(value);
-        else if (option == "--trace-precision") {
-            if (value == "fp32") c.precision = ICP_FP32;
-            else if (value == "fp64") c.precision = ICP_FP64;
-            else throw std::invalid_argument("--trace-precision must be fp32 or fp64.");
-        } else if (option == "--diffraction") {
-            if (value == "none") c.analytic_diffraction = false;
-            else if (value == "analytic") c.analytic_diffraction = true;
-            else throw std::invalid_argument("--diffraction must be none or analytic.");
-        } else if (option == "--shape-coefficients") {
-            size_t begin = 0;
-            unsigned k = 0;
-            while (begin <= value.size()) {
-                const auto end = value.find(',', begin);
-                const auto part = value.substr(begin, end == std::string::npos ? std::string::npos : end - begin);
-                if (k >= 8) throw std::invalid_argument("At most eight shape coefficients.");
-                c.coefficients[k++] = number(part);
-                if (end == std::string::npos) break;
-                begin = end + 1;
-            }
-            c.custom_shape = true;
-        } else
-            throw std::invalid_argument("Unknown option: " + option);
+    bool help = false;
+    auto real = [](double& x) { return icp::cli::Flag{1, [&x](const V& v) { x = number(v[0]); }}; };
+    auto count32 = [](uint32_t& x) { return icp::cli::Flag{1, [&x](const V& v) { x = positive_integer<uint32_t>(v[0]); }}; };
+    auto refused = [](const char* why) { return icp::cli::Flag{1, [why](const V&) { throw std::invalid_argument(why); }}; };
+    const icp::cli::Table table = {
+        {"--sphere", {0, [&](const V&) { c.sphere = true; }}},
+        {"--allow-underresolved", {0, [&](const V&) { c.allow_underresolved = true; }}},
+        {"--help", {0, [&](const V&) { help = true; }, true}},
+        {"--out", {1, [&](const V& v) { c.output = std::string(v[0]); }}},
+        {"--modules", {1, [](const V&) {}}},
+        {"--radius-mm", {1, [&](const V& v) { c.radius_mm = static_cast<float>(number(v[0])); }}},
+        {"--wavelength-nm", {1, [&](const V& v) {
+             if (c.wavelength_given) throw std::invalid_argument("Duplicate --wavelength-nm.");
+             c.wavelength_requested_nm = number(v[0]);
+             c.wavelength_given = true;
+             if (!(c.wavelength_requested_nm > 0 && c.wavelength_requested_nm <= (std::numeric_limits<float>::max)()))
+                 throw std::invalid_argument("Wavelength must be positive and representable by the solver.");
+             c.wavelength_nm = static_cast<float>(c.wavelength_requested_nm);
+             if (!(c.wavelength_nm > 0)) throw std::invalid_argument("Wavelength underflows solver precision.");
+         }}},
+        {"--material", {1, [&](const V& v) {
+             if (v[0] == "water") c.material = Material::Water;
+             else if (v[0] == "constant") c.material = Material::Constant;
+             else throw std::invalid_argument("Material must be water or constant.");
+         }}},
+        {"--temperature-c", {1, [&](const V& v) { c.temperature_c = number(v[0]); c.state_given = true; }}},
+        {"--pressure-pa", {1, [&](const V& v) { c.pressure_pa = number(v[0]); c.state_given = true; }}},
+        {"--ior", {1, [&](const V& v) { c.constant_index = number(v[0]); c.index_given = true; }}},
+        {"--grid", count32(c.grid)},
+        {"--query-theta", count32(c.theta)},
+        {"--query-phi", count32(c.phi)},
+        {"--inclination-deg", real(c.inclination_deg)},
+        {"--cdf-theta", count32(c.cdf_theta)},
+        {"--cdf-phi", count32(c.cdf_phi)},
+        {"--storage-gaussian-sigma-deg", refused("Global storage blur has been removed from rainbow_generate. Remove this option; only local Table-II diffraction and cell-mass aggregation are applied.")},
+        {"--storage-gaussian-support", refused("Global storage blur has been removed from rainbow_generate. Remove this option; only local Table-II diffraction and cell-mass aggregation are applied.")},
+        {"--max-coarsening-tv", real(c.max_tv)},
+        {"--diffraction-sigma-deg", refused("Manual diffraction width is not supported by rainbow_generate. Remove this option; Table II is selected automatically.")},
+        {"--transition-contrast", real(c.transition_contrast)},
+        {"--cdf-max-l1", real(c.max_l1)},
+        {"--cdf-max-lost-mass", real(c.max_lost)},
+        {"--device", {1, [&](const V& v) {
+             const auto r = std::from_chars(v[0].data(), v[0].data() + v[0].size(), c.device);
+             if (r.ec != std::errc{} || r.ptr != v[0].data() + v[0].size() || c.device < 0)
+                 throw std::invalid_argument("Invalid device ordinal.");
+         }}},
+        {"--stage", {1, [&](const V& v) {
+             if (v[0] != "incoherent" && v[0] != "path" && v[0] != "focal" && v[0] != "diffraction")
+                 throw std::invalid_argument("Unknown stage.");
+             stage = std::string(v[0]);
+         }}},
+        {"--focal-offsets", {1, [&](const V& v) { focal_offsets(v[0], c.focal_offsets); }}},
+        // extensions
+        {"--rays", {1, [&](const V& v) { c.rays = positive_integer<uint64_t>(v[0]); }}},
+        {"--seed", {1, [&](const V& v) {
+             const auto r = std::from_chars(v[0].data(), v[0].data() + v[0].size(), c.seed);
+             if (r.ec != std::errc{} || r.ptr != v[0].data() + v[0].size()) throw std::invalid_argument("Invalid seed.");
+         }}},
+        {"--max-internal-hits", count32(c.max_hits)},
+        {"--tail-tolerance", real(c.tail)},
+        {"--max-unresolved-fraction", real(c.max_unresolved)},
+        {"--max-balance-error", real(c.max_balance)},
+        {"--max-histogram-relative-error", real(c.max_hist_err)},
+        {"--trace-precision", {1, [&](const V& v) {
+             if (v[0] == "fp32") c.precision = ICP_FP32;
+             else if (v[0] == "fp64") c.precision = ICP_FP64;
+             else throw std::invalid_argument("--trace-precision must be fp32 or fp64.");
+         }}},
+        {"--diffraction", {1, [&](const V& v) {
+             if (v[0] == "none") c.analytic_diffraction = false;
+             else if (v[0] == "analytic") c.analytic_diffraction = true;
+             else throw std::invalid_argument("--diffraction must be none or analytic.");
+         }}},
+        {"--shape-coefficients", {1, [&](const V& v) {
+             shape_coefficients(v[0], c.coefficients);
+             c.custom_shape = true;
+         }}},
+    };
+    const icp::cli::Style style{false, true, nullptr, [](const std::string&) { return std::string("Missing option value."); }};
+    icp::cli::apply(argc, argv, table, style);
+    if (help) {
+        print_help();
+        return false;
     }
     if (c.output.empty()) throw std::invalid_argument("--out is required.");
     if (!c.wavelength_given) throw std::invalid_argument("--wavelength-nm is required; there is no implicit wavelength.");
