@@ -64,7 +64,7 @@ def _refuse_constant(name: str) -> None:
     raise ValueError(f"Nonfinite JSON constant: {name}")
 
 
-def load_json(path: Path, limit: int = 8 << 20) -> dict[str, Any]:
+def read_json_object(path: Path, limit: int = 8 << 20) -> dict[str, Any]:
     """A JSON object from a file of at most `limit` bytes (a UTF-8 BOM allowed, NaN refused)."""
     if path.stat().st_size > limit:
         raise ValueError(f"JSON too large: {path}")
@@ -100,7 +100,7 @@ def field(value: Any, kind: str, low: Any = None, high: Any = None) -> Any:
     return float(d)
 
 
-def scalar(value: Any, low: float, high: float) -> float:
+def real_field(value: Any, low: float, high: float) -> float:
     return field(value, "real", low, high)
 
 
@@ -108,7 +108,7 @@ def fp32(x: float) -> float:
     return float(np.float32(x))
 
 
-def wavelengths(spec: dict[str, Any]) -> list[str]:
+def wavelength_grid(spec: dict[str, Any]) -> list[str]:
     """Wavelengths start, start + step, ..., stop (stop reached exactly) as decimal strings; no
     two may round to the same binary32 solver value (generate_phase_dataset.py:83-99)."""
     if set(spec) != {"start_nm", "stop_nm", "step_nm"}:
@@ -127,7 +127,7 @@ def wavelengths(spec: dict[str, Any]) -> list[str]:
     return values
 
 
-def inclinations(spec: dict[str, Any]) -> list[str]:
+def inclination_grid(spec: dict[str, Any]) -> list[str]:
     """Centres of `count` equal cells of [min, max] degrees as decimal strings, each computed as
     min + (max - min) (i + 1/2) / count (generate_phase_dataset.py:102-111)."""
     if set(spec) != {"min_degrees", "max_degrees", "count", "placement"}:
@@ -177,8 +177,8 @@ def normalized_config(raw: dict[str, Any]) -> dict[str, Any]:
         raise ValueError("b200.precision must be fp32 or fp64")
     b200["precision"] = b["precision"]
     top = {k: field(raw[k], *spec) for k, spec in TOP_FIELDS.items()}
-    return {**top, "wavelength_nm": wavelengths(raw["wavelengths"]),
-            "inclination_degrees": inclinations(raw["inclinations"]),
+    return {**top, "wavelength_nm": wavelength_grid(raw["wavelengths"]),
+            "inclination_degrees": inclination_grid(raw["inclinations"]),
             "inclination_placement": "linear_angle_cell_centers", "material": "water", "solver": out, "b200": b200}
 
 
@@ -263,7 +263,7 @@ def npy_size(path: Path, expected_shape: tuple[int, ...]) -> int:
     return end
 
 
-def close(a: Any, b: float, tol: float = 1e-12) -> bool:
+def near(a: Any, b: float, tol: float = 1e-12) -> bool:
     return type(a) in (int, float) and math.isfinite(a) and abs(a - b) <= tol * max(1.0, abs(b))
 
 
@@ -279,7 +279,7 @@ def _frame_ok(rows: Any, alpha_deg: float) -> str | None:
     if not all(_is_number(v) for r in rows for v in r):
         return "frame values"
     cols = [[rows[r][j] for r in range(3)] for j in range(3)]
-    if not all(close(sum(x * y for x, y in zip(cols[j], cols[k])), float(j == k), 2e-12)
+    if not all(near(sum(x * y for x, y in zip(cols[j], cols[k])), float(j == k), 2e-12)
                for j in range(3) for k in range(3)):
         return "frame orthogonality"
     e0, e1, kk = cols
@@ -299,7 +299,7 @@ def verify_record(path: Path, plan: dict[str, Any], ii: int, ll: int) -> dict[st
     the frame, the area and cross sections, the quality and storage gates, the array files.
     Returns the receipt digest of the record."""
     c, s = plan["conditions"], plan["conditions"]["solver"]
-    m = load_json(path / "metadata.json", 1 << 20)
+    m = read_json_object(path / "metadata.json", 1 << 20)
     alpha = float(c["inclination_degrees"][ii])
     geometry, cs, q = m.get("geometry", {}), m.get("cross_sections", {}), m.get("quality", {})
     sp, hg, material = m.get("storage_processing", {}), m.get("hg", {}), m.get("material", {})
@@ -312,12 +312,12 @@ def verify_record(path: Path, plan: dict[str, Any], ii: int, ll: int) -> dict[st
               "incident_grid": [s["grid"], s["grid"]], "stage": s["stage"], "force_sphere": c["force_sphere"],
               "focal_quarter_turn_offsets": s["focal_offsets"]}
     checks = [(f"mismatched {k}", m.get(k) == v) for k, v in fields.items()]
-    checks += [("radius", close(m.get("radius_mm"), fp32(c["radius_mm"]))),
-               ("wavelength", close(m.get("wavelength_nm"), fp32(float(c["wavelength_nm"][ll])))),
-               ("inclination", close(m.get("incident_inclination_degrees"), alpha)),
+    checks += [("radius", near(m.get("radius_mm"), fp32(c["radius_mm"]))),
+               ("wavelength", near(m.get("wavelength_nm"), fp32(float(c["wavelength_nm"][ll])))),
+               ("inclination", near(m.get("incident_inclination_degrees"), alpha)),
                ("material", material.get("model") == "water_iapws_r9_97"),
-               ("temperature", close(material.get("temperature_kelvin"), c["temperature_c"] + 273.15)),
-               ("pressure", close(material.get("pressure_pascal"), c["pressure_pa"]))]
+               ("temperature", near(material.get("temperature_kelvin"), c["temperature_c"] + 273.15)),
+               ("pressure", near(material.get("pressure_pascal"), c["pressure_pa"]))]
     for what, ok in checks:
         if not ok:
             raise ValueError(f"{path}: {what}")
@@ -550,7 +550,7 @@ class DatasetRun:
     conditions in GPU batches, each record written through .part, verified and receipted."""
 
     def __init__(self, args: argparse.Namespace, backend=None):
-        raw = load_json(args.config)
+        raw = read_json_object(args.config)
         overrides = {"radius_mm": args.radius_mm}
         if args.wavelength_range:
             raw["wavelengths"] = dict(zip(("start_nm", "stop_nm", "step_nm"), args.wavelength_range))
@@ -563,7 +563,7 @@ class DatasetRun:
         self.c = normalized_config(raw)
         root = Path(args.out_root or raw["output_root"])
         self.root = (root if root.is_absolute() else Path.cwd() / root).resolve()
-        self.reserve = int(scalar(raw["reserve_gib"], 0, 1000000) * (1 << 30))
+        self.reserve = int(real_field(raw["reserve_gib"], 0, 1000000) * (1 << 30))
         nt, np_ = self.c["solver"]["cdf_theta"], self.c["solver"]["cdf_phi"]
         self.payload = 8 * ((np_ + 1) + np_ * (nt + 1) + (nt + 1))
         self.per_record = self.payload + (128 << 10)  # arrays + metadata, receipt and progress allowance
@@ -592,13 +592,13 @@ class DatasetRun:
         if manifest.exists():
             if not self.args.resume:
                 raise FileExistsError("Dataset plan exists; use --resume with identical configuration and binaries")
-            if load_json(manifest) != json.loads(json.dumps(plan)):
+            if read_json_object(manifest) != json.loads(json.dumps(plan)):
                 raise ValueError("Resume rejected: configuration/binaries differ from batch_plan.json")
         else:
             if any(p.name != ".batch.lock" for p in self.root.iterdir()):
                 raise ValueError("Refusing to adopt a nonempty directory without this batch plan")
             write_json(manifest, plan)
-        return load_json(manifest), signature
+        return read_json_object(manifest), signature
 
     def scan(self, plan: dict, signature: str) -> tuple[list, int]:
         """(pending conditions, number of existing records verified against their receipts)."""
@@ -617,7 +617,7 @@ class DatasetRun:
                     continue
                 if not self.args.resume or not receipt.exists():
                     raise ValueError(f"Existing record without authorized resume/receipt: {path}")
-                saved = load_json(receipt)
+                saved = read_json_object(receipt)
                 expected = {"signature": signature, "incident_index": ii, "wavelength_index": ll,
                             "record": verify_record(path, plan, ii, ll)}
                 if any(saved.get(k) != v for k, v in expected.items()):
