@@ -50,17 +50,20 @@ GENERATOR = "icp_b200.deterministic_atlas.v1"
 
 
 # ------------------------------------------------------------------ orientation rule
-def positive_int(x: Any, name: str, maximum: int = 1_000_000) -> int:
-    if type(x) is not int or not 1 <= x <= maximum:
-        raise ValueError(f"{name} must be an integer in [1,{maximum}]")
-    return x
+def count_in(x: Any, name: str, top: int = 1_000_000) -> int:
+    """A JSON integer (not a bool, not a float) in 1..top."""
+    if type(x) is int and 0 < x <= top:
+        return x
+    raise ValueError(f"{name}: expected an integer from 1 to {top}, got {x!r}")
 
 
 def unit(v: Any) -> np.ndarray:
+    """v scaled by its largest component, then by its length (the tracer's normalisation)."""
     a = np.asarray(v, dtype=np.float64)
-    if a.shape != (3,) or not np.isfinite(a).all() or np.max(np.abs(a)) == 0:
+    big = float(np.max(np.abs(a))) if a.shape == (3,) and np.isfinite(a).all() else 0.0
+    if big == 0.0:
         raise ValueError("Expected finite nonzero three-vector")
-    a = a / np.max(np.abs(a))
+    a = a / big
     return a / math.sqrt(float(a @ a))
 
 
@@ -69,7 +72,7 @@ def gaussian_tilt_nodes(count: int, sigma_deg: float) -> np.ndarray:
     equal-probability strata of N(pi/2, sigma^2) truncated to [0, pi], density in d beta (no
     sin beta factor), found by 64 bisection steps of the erf CDF; sigma = 0 is an exact delta
     (atlas_math.py:75-106)."""
-    positive_int(count, "tilt count")
+    count_in(count, "tilt count")
     sigma = math.radians(float(sigma_deg))
     if not math.isfinite(sigma) or sigma < 0:
         raise ValueError("sigma_deg must be finite and nonnegative")
@@ -117,12 +120,16 @@ def quaternion_matrix(q: Any) -> np.ndarray:
 
 
 def validate_rotations(r: np.ndarray, w: np.ndarray) -> None:
-    if r.ndim != 3 or r.shape[1:] != (3, 3) or w.shape != (len(r),) or len(r) == 0:
+    """Proper rotations (R^T R = I and det R = 1 to 2e-12) with positive finite number weights
+    summing to one (2e-12)."""
+    shaped = r.ndim == 3 and r.shape[1:] == (3, 3) and len(r) > 0 and w.shape == (len(r),)
+    if not shaped:
         raise ValueError("Malformed orientation quadrature")
-    if not np.isfinite(r).all() or not np.isfinite(w).all() or np.any(w <= 0) or abs(math.fsum(w) - 1) > 2e-12:
+    finite = np.isfinite(r).all() and np.isfinite(w).all()
+    if not (finite and bool(np.all(w > 0)) and abs(math.fsum(w) - 1) <= 2e-12):
         raise ValueError("Nonfinite / nonpositive / unnormalized orientation weights")
-    rtr = np.swapaxes(r, 1, 2) @ r
-    if np.max(np.abs(rtr - np.eye(3))) > 2e-12 or np.max(np.abs(np.linalg.det(r) - 1)) > 2e-12:
+    gram_error = np.max(np.abs(np.einsum("nki,nkj->nij", r, r) - np.eye(3)))
+    if gram_error > 2e-12 or np.max(np.abs(np.linalg.det(r) - 1)) > 2e-12:
         raise ValueError("Orientation nodes must be proper orthogonal rotations")
 
 
@@ -137,7 +144,7 @@ def orientation_rule(config: dict[str, Any]) -> tuple[np.ndarray, np.ndarray, di
     q = config["quadrature"]
     if set(q) != {"azimuth", "tilt", "spin"}:
         raise ValueError("quadrature keys must be azimuth, tilt, spin")
-    na, nb, ng = (positive_int(q[k], k, 4096) for k in ("azimuth", "tilt", "spin"))
+    na, nb, ng = (count_in(q[k], k, 4096) for k in ("azimuth", "tilt", "spin"))
     comps = config["components"]
     if not isinstance(comps, list) or not comps:
         raise ValueError("Nonempty orientation components required")
@@ -179,25 +186,22 @@ def orientation_rule(config: dict[str, Any]) -> tuple[np.ndarray, np.ndarray, di
 
 
 def incidents(config: dict[str, Any]) -> list[tuple[np.ndarray, dict[str, Any]]]:
-    """Incident directions: inclinations alpha -> ki = (cos alpha, -sin alpha, 0), +-90 exactly
-    vertical; or explicit direction vectors (compose_atlas.py:38-59)."""
-    have = set(config) & {"inclinations_deg", "directions"}
-    if len(have) != 1:
+    """Incident directions: inclinations alpha -> ki = (cos alpha, -sin alpha, 0), exactly
+    (0, -+1, 0) at +-90; or explicit direction vectors (compose_atlas.py:38-59)."""
+    if ("inclinations_deg" in config) == ("directions" in config):
         raise ValueError("Specify exactly one of inclinations_deg or directions")
-    out = []
-    if "inclinations_deg" in config:
-        for value in config["inclinations_deg"]:
-            a = float(value)
-            if not math.isfinite(a) or not -90 <= a <= 90:
-                raise ValueError("Inclination must be in [-90,90] degrees")
-            k = np.array([math.cos(math.radians(a)), -math.sin(math.radians(a)), 0.0])
-            if abs(a) == 90:
-                k = np.array([0.0, -math.copysign(1, a), 0.0])
-            out.append((unit(k), {"inclination_deg": a}))
-    else:
-        for k in config["directions"]:
-            out.append((unit(k), {}))
-    if not out or len(out) > 10000:
+
+    def inclined(value: Any) -> tuple[np.ndarray, dict[str, Any]]:
+        a = float(value)
+        if not (math.isfinite(a) and abs(a) <= 90):
+            raise ValueError("Inclination must be in [-90,90] degrees")
+        r = math.radians(a)
+        k = [0.0, -math.copysign(1.0, a), 0.0] if abs(a) == 90 else [math.cos(r), -math.sin(r), 0.0]
+        return unit(k), {"inclination_deg": a}
+
+    out = ([inclined(v) for v in config["inclinations_deg"]] if "inclinations_deg" in config
+           else [(unit(k), {}) for k in config["directions"]])
+    if not 0 < len(out) <= 10000:
         raise ValueError("Require 1..10000 incident conditions")
     return out
 
@@ -350,53 +354,56 @@ class Atlas:
     """A complete atlas directory, validated as the reference's composer does (atlas_math.py:235-269)."""
 
     def __init__(self, directory: str | Path):
-        self.directory = Path(directory)
-        if self.directory.name.endswith(".part"):
+        self.directory = d = Path(directory)
+        if d.name.endswith(".part"):
             raise ValueError("Incomplete atlas directory")
-        with (self.directory / "metadata.json").open(encoding="utf-8") as f:
-            self.meta = m = json.load(f)
+        self.meta = m = json.loads((d / "metadata.json").read_text(encoding="utf-8"))
         if m.get("schema") != ATLAS_SCHEMA or m.get("complete") is not True:
             raise ValueError("Incomplete or unknown atlas schema")
-        if m.get("incident_reconstruction") != RECONSTRUCTION or m.get("symmetry") != SYMMETRY:
+        if (m.get("incident_reconstruction"), m.get("symmetry")) != (RECONSTRUCTION, SYMMETRY):
             raise ValueError("Unsupported atlas frame/interpolation/symmetry")
-        self.it, self.ip = (positive_int(m[k], k, 4096) for k in ("incident_theta_intervals", "incident_phi_intervals"))
-        self.nt, self.np = (positive_int(m[k], k) for k in ("theta_count", "phi_count"))
-        self.mass = np.load(self.directory / "mass_mm2.npy", mmap_mode="r", allow_pickle=False)
-        self.edges = np.load(self.directory / "u_edges.npy", allow_pickle=False)
-        if (self.mass.shape != (self.it + 1, self.ip + 1, self.nt, self.np) or self.mass.dtype.str != "<f8"
-                or not self.mass.flags.c_contiguous):
-            raise ValueError("Atlas mass layout does not match metadata")
-        e = self.edges
-        if (e.shape != (self.nt + 1,) or e.dtype.str != "<f8" or not np.isfinite(e).all() or e[0] != 0 or e[-1] != 1
-                or np.any(np.diff(e) <= 0)):
-            raise ValueError("Invalid atlas u edges")
-        if len(m["nodes"]) != (self.it + 1) * (self.ip + 1):
-            raise ValueError("Missing incident atlas nodes")
+        self.it = count_in(m["incident_theta_intervals"], "incident_theta_intervals", 4096)
+        self.ip = count_in(m["incident_phi_intervals"], "incident_phi_intervals", 4096)
+        self.nt, self.np = count_in(m["theta_count"], "theta_count"), count_in(m["phi_count"], "phi_count")
+        self.mass = np.load(d / "mass_mm2.npy", mmap_mode="r", allow_pickle=False)
+        self.edges = e = np.load(d / "u_edges.npy", allow_pickle=False)
         g = m["geometry"]
         self.radius, self.length = float(g["circumradius_mm"]), float(g["full_length_mm"])
-        if g["shape"] != "regular_hexagonal_prism" or not (self.radius > 0 and self.length > 0):
-            raise ValueError("Unsupported geometry")
-        self.area = np.zeros((self.it + 1, self.ip + 1))
-        self.residual = np.zeros_like(self.area)
-        for index, n in enumerate(m["nodes"]):
-            i, j = divmod(index, self.ip + 1)
-            if (n["i"], n["j"]) != (i, j):
-                raise ValueError("Node order mismatch")
+        grid = (self.it + 1, self.ip + 1)
+        layout = [
+            ("Atlas mass layout does not match metadata", self.mass.shape == (*grid, self.nt, self.np)
+             and self.mass.dtype.str == "<f8" and self.mass.flags.c_contiguous),
+            ("Invalid atlas u edges", e.shape == (self.nt + 1,) and e.dtype.str == "<f8" and np.isfinite(e).all()
+             and e[0] == 0 and e[-1] == 1 and bool(np.all(np.diff(e) > 0))),
+            ("Missing incident atlas nodes", len(m["nodes"]) == grid[0] * grid[1]),
+            ("Unsupported geometry", g["shape"] == "regular_hexagonal_prism" and self.radius > 0 and self.length > 0),
+        ]
+        for what, ok in layout:
+            if not ok:
+                raise ValueError(what)
+        nodes = m["nodes"]
+        if [(n["i"], n["j"]) for n in nodes] != [divmod(k, grid[1]) for k in range(len(nodes))]:
+            raise ValueError("Node order mismatch")
+        acct = np.array([[float(n[k]) for k in ("projected_area_mm2", "unresolved_mm2", "escaped_mm2")]
+                         for n in nodes])
+        area, residual, escaped = acct.T
+        for k, n in enumerate(nodes):
+            i, j = divmod(k, grid[1])
             f = canonical_frame(i * (PI / 2) / self.it, j * (PI / 6) / self.ip)
-            if (np.max(np.abs(np.array(n["ki"]) - f[:, 2])) > 2e-12 or
-                    np.max(np.abs(np.array(n["e0"]) - f[:, 0])) > 2e-12):
+            if max(np.max(np.abs(np.array(n["ki"]) - f[:, 2])), np.max(np.abs(np.array(n["e0"]) - f[:, 0]))) > 2e-12:
                 raise ValueError("Node frame mismatch")
             cell = self.mass[i, j]
-            if not np.isfinite(cell).all() or np.any(cell < 0):
+            if not (np.isfinite(cell).all() and bool(np.all(cell >= 0))):
                 raise ValueError("Invalid atlas cell mass")
-            area, residual, escaped = (float(n[k]) for k in ("projected_area_mm2", "unresolved_mm2", "escaped_mm2"))
-            if not all(math.isfinite(v) for v in (area, residual, escaped)) or area <= 0 or escaped <= 0 or residual < 0:
+            if not (np.isfinite(acct[k]).all() and area[k] > 0 and escaped[k] > 0 and residual[k] >= 0):
                 raise ValueError("Invalid node accounting")
-            if (abs((escaped + residual) / area - 1) > 2e-10 or abs(float(np.sum(cell)) / escaped - 1) > 2e-10 or
-                    abs(area / projected_area(self.radius, self.length, n["ki"]) - 1) > 2e-12):
+            audits = (abs((escaped[k] + residual[k]) / area[k] - 1) <= 2e-10,
+                      abs(float(np.sum(cell)) / escaped[k] - 1) <= 2e-10,
+                      abs(area[k] / projected_area(self.radius, self.length, n["ki"]) - 1) <= 2e-12)
+            if not all(audits):
                 raise ValueError("Node area / mass / residual audit failed")
-            self.area[i, j], self.residual[i, j] = area, residual
-        self.hashes = {n: sha256_file(self.directory / n) for n in ("metadata.json", "mass_mm2.npy", "u_edges.npy")}
+        self.area, self.residual = area.reshape(grid), residual.reshape(grid)
+        self.hashes = {n: sha256_file(d / n) for n in ("metadata.json", "mass_mm2.npy", "u_edges.npy")}
 
     @property
     def nodes(self) -> int:
