@@ -19,6 +19,10 @@ Mirrored reference interfaces (Somatic-Cell/ice-crystal-phase):
   PhaseMassAccumulatorCuda.add_drop  RaindropTracer::trace_unpolarized + patch stages, replaced by
                                    direct binning (include/rainbow/raindrop_tracer.hpp:32-36)
   generate_drop_record             apps/generate_phase.cpp:395-453 (rainbow_generate's record path)
+  rainbow_table_sigma              include/rainbow/rainbow_diffraction.hpp:16-28
+  diffraction_config               src/patch_optics.cpp:79-95 (the diffraction part of evaluate_wave_device)
+  rainbow_diffraction              PatchOptics::run_diffraction + its statistics, src/patch_optics.cpp:217-231,
+                                   334-348 (kernels device/patch_optics.cu:26-40)
 """
 from __future__ import annotations
 
@@ -201,6 +205,33 @@ class AtlasNodeReport(C.Structure):
         return {k: (list(getattr(self, k)) if k == "status" else getattr(self, k)) for k, _ in self._fields_}
 
 
+class DiffractionConfig(C.Structure):
+    _fields_ = [("primary_sigma_rad", C.c_double), ("support_sigma", C.c_double),
+                ("transition_contrast", C.c_double), ("inner_blend_sigma", C.c_double)]
+
+
+class DiffractionStats(C.Structure):
+    _fields_ = [(k, C.c_uint32) for k in ("primary_transitions", "secondary_transitions", "unknown_transitions",
+                                          "filtered_directions", "unavailable_directions",
+                                          "underresolved_directions")]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# One focal-stage query direction (icp_focal_sample = rainbow::FocalOpticalResult, 144 bytes) and
+# one diffraction result (icp_diffraction_result = rainbow::DiffractionResult, 40 bytes).
+FOCAL_DTYPE = np.dtype([("field", "<f8", 4), ("intensity_s", "<f8"), ("intensity_p", "<f8"),
+                        ("family_incoherent", "<f8", 4), ("family_hits", "<u4", 4), ("corrected_hits", "<u4"),
+                        ("extra_quarter_turn_hits", "<u4"), ("flags", "<u4"), ("first_problem_patch_id", "<u4"),
+                        ("field_second", "<f8", 4)])
+DIFFRACTION_DTYPE = np.dtype([("intensity_s", "<f8"), ("intensity_p", "<f8"), ("sigma_rad", "<f8"),
+                              ("blend", "<f8"), ("flags", "<u4"), ("transition_kind", "<u4")])
+TRANSITION_PRIMARY, TRANSITION_SECONDARY, TRANSITION_UNKNOWN = 1, 2, 4
+DIFFRACTION_FILTERED, DIFFRACTION_UNDERRESOLVED, DIFFRACTION_INPUT_UNAVAILABLE = 1, 2, 4
+DIFFRACTION_STENCIL_UNAVAILABLE, DIFFRACTION_DETECTION_UNAVAILABLE, DIFFRACTION_INVALID_DATA = 8, 16, 32
+
+
 class SurrogateConfig(C.Structure):
     _fields_ = [("nt", C.c_uint32), ("np", C.c_uint32), ("hidden", C.c_uint32), ("input_width", C.c_uint32),
                 ("theta_frequencies", C.c_uint32), ("phi_frequencies", C.c_uint32), ("max_records", C.c_uint32),
@@ -284,6 +315,12 @@ _FUNCS = {
     "icp_atlas_coupling": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_double, C.c_double, _D, _P, _P,
                                      C.c_uint64, _D, C.c_double, C.c_int, _P, _D]),
     "icp_atlas_compose": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, _P, _P, _P]),
+    "icp_rainbow_table_sigma": (C.c_int, [C.c_float, _D]),
+    "icp_rainbow_detect": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32, C.POINTER(DiffractionConfig), _P]),
+    "icp_rainbow_filter": (C.c_int, [_P, _P, _P, C.c_uint32, C.c_uint32, C.POINTER(DiffractionConfig), _P, _P,
+                                     C.POINTER(DiffractionStats)]),
+    "icp_rainbow_diffraction": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32, C.POINTER(DiffractionConfig), _P, _P, _P,
+                                          C.POINTER(DiffractionStats)]),
 }
 
 
@@ -1058,3 +1095,55 @@ class Surrogate:
     def targets(self, phi_ptr: int, theta_ptr: int, count: int, target_ptr: int) -> None:
         check(LIB.icp_surrogate_targets(self.handle, C.c_void_p(phi_ptr), C.c_void_p(theta_ptr), count,
                                         C.c_void_p(target_ptr)))
+
+
+# ------------------------------------------------------- Table-II rainbow diffraction
+def rainbow_table_sigma(radius_mm: float) -> float:
+    """Table-II primary width in degrees for a drop radius (mm, rounded to float32 first)."""
+    out = C.c_double(0.0)
+    check(LIB.icp_rainbow_table_sigma(float(np.float32(radius_mm)), C.byref(out)))
+    return out.value
+
+
+def diffraction_config(radius_mm: float, primary_sigma_deg: float = 0.0,
+                       transition_contrast: float = 0.25) -> DiffractionConfig:
+    """The diffraction settings PatchOptics derives from WaveOpticsSettings: a zero width
+    selects Table II at the drop's radius (outside 0.1 .. 1.0 mm rejected), a positive one
+    is an explicit extension; support 4 sigma, blend from 3 sigma."""
+    sigma = float(primary_sigma_deg)
+    if not (sigma >= 0.0 and math.isfinite(sigma)):
+        raise InvalidArgument(ICP_ERR_INVALID_ARGUMENT, "Invalid diffraction sigma.")
+    if sigma == 0.0:
+        sigma = rainbow_table_sigma(radius_mm)
+    return DiffractionConfig(sigma * math.pi / 180.0, 4.0, float(transition_contrast), 3.0)
+
+
+@dataclass
+class DiffractionOutput:
+    transitions: np.ndarray  # uint32 [nt * np]: edge labels below each direction
+    results: np.ndarray      # DIFFRACTION_DTYPE [nt * np]
+    density: np.ndarray      # float64 [nt * np]: intensity_s + intensity_p (the stage's CDF input)
+    stats: dict
+
+
+def rainbow_diffraction(ctx: Context, focal, nt: int, np_: int, config: DiffractionConfig,
+                        transitions=None) -> DiffractionOutput:
+    """Table-II diffraction of a focal grid (FOCAL_DTYPE [nt * np], host or DeviceArray): the
+    labels are detected unless given (uint32 [nt * np]), then every direction is filtered."""
+    n = nt * np_
+    if isinstance(focal, DeviceArray):
+        df = focal
+    else:
+        df = DeviceArray(ctx, n, FOCAL_DTYPE).upload(np.ascontiguousarray(focal, dtype=FOCAL_DTYPE).reshape(-1))
+    dt = DeviceArray(ctx, n, np.uint32)
+    dr = DeviceArray(ctx, n, DIFFRACTION_DTYPE)
+    dd = DeviceArray(ctx, n)
+    stats = DiffractionStats()
+    if transitions is None:
+        check(LIB.icp_rainbow_diffraction(ctx.handle, df.ptr, nt, np_, C.byref(config), dt.ptr, dr.ptr, dd.ptr,
+                                          C.byref(stats)))
+    else:
+        dt.upload(np.ascontiguousarray(transitions, dtype=np.uint32).reshape(-1))
+        check(LIB.icp_rainbow_filter(ctx.handle, df.ptr, dt.ptr, nt, np_, C.byref(config), dr.ptr, dd.ptr,
+                                     C.byref(stats)))
+    return DiffractionOutput(dt.download(), dr.download(), dd.download(), stats.as_dict())

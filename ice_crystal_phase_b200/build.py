@@ -50,6 +50,7 @@ UNITS = {
     "icp_capi_mlp.cu": ["-fmad=false"],
     "icp_cdf_static.cu": ["-fmad=false"],
     "icp_atlas.cu": ["-fmad=false"],
+    "icp_rainbow.cu": ["-fmad=false"],
 }
 
 HOST_SOURCES = ["icp_record_io.cpp"]

@@ -266,5 +266,7 @@ struct icp_context {
     icp::Scratch cdfb_partial, cdfb_colsum, cdfb_recs;
     // deterministic atlas: per-node trace scratch, coupling accumulators
     icp::Scratch atlas_trace, atlas_coupling;
+    // Table-II rainbow diffraction: packed samples, row marks, counters
+    icp::Scratch rainbow;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
 };

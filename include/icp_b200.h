@@ -20,6 +20,9 @@
  *   icp_drop_trace_bin    RaindropTracer::trace_unpolarized + patch/query/optics stages
  *                                                         include/rainbow/raindrop_tracer.hpp, apps/generate_phase.cpp:431-439
  *   icp_drop_generate     rainbow_generate's record path   apps/generate_phase.cpp:395-453
+ *   icp_rainbow_*         RainbowDiffraction + PatchOptics::run_diffraction
+ *                                                         include/rainbow/rainbow_diffraction.hpp,
+ *                                                         src/patch_optics.cpp:334-348
  */
 #ifndef ICP_B200_H
 #define ICP_B200_H
@@ -555,6 +558,88 @@ int icp_atlas_coupling(icp_context* ctx, uint32_t theta_intervals, uint32_t phi_
  * summation order per cell.  Replaces compose_mass (atlas_math.py:431-447). */
 int icp_atlas_compose(icp_context* ctx, uint32_t nodes, uint32_t nt, uint32_t np, const double* d_mass,
                       const double* d_coupling, double* d_out);
+
+/* -------------------------------------------------- Table-II rainbow diffraction */
+/* Local diffraction at the rainbows on a (theta, phi) query grid of the drop's focal stage:
+ * the reference's Sadeghi-2012 Table-II model (include/rainbow/rainbow_diffraction.hpp) run by
+ * PatchOptics::run_diffraction (src/patch_optics.cpp:334-348).  The query grid has nt theta
+ * rows (centre theta = (row + 1/2) pi / nt, theta = angle between the incident and outgoing
+ * propagation directions) of np phi cells, direction index = row * np + column.
+ *
+ * One direction of the focal stage, laid out as rainbow::FocalOpticalResult
+ * (include/rainbow/wave_optics_data.hpp:27-40, 144 bytes), so that the reference's
+ * focal-results buffer is passed unchanged.  The pass reads intensity_s, intensity_p,
+ * family_incoherent[2..3], family_hits[2..3] (families R, TT, TRT, TRRT) and flags
+ * (0 = valid). */
+typedef struct {
+    double field[4];                 /* column-0 field: s re, s im, p re, p im (unused)      */
+    double intensity_s, intensity_p; /* unpolarized focal intensities                         */
+    double family_incoherent[4];
+    uint32_t family_hits[4];
+    uint32_t corrected_hits, extra_quarter_turn_hits;
+    uint32_t flags, first_problem_patch_id;
+    double field_second[4];          /* column-1 field (unused)                               */
+} icp_focal_sample;
+
+/* rainbow::DiffractionConfig (wave_optics_data.hpp:48-54). */
+typedef struct {
+    double primary_sigma_rad;   /* Gaussian width at the primary bow; the secondary uses 2x   */
+    double support_sigma;       /* stencil radius in sigmas (4)                               */
+    double transition_contrast; /* minimum relative jump of the total intensity (0.25)        */
+    double inner_blend_sigma;   /* full blend inside, smoothstep taper to the support (3)     */
+} icp_diffraction_config;
+
+/* rainbow::DiffractionResult (wave_optics_data.hpp:66-78, 40 bytes). */
+typedef struct {
+    double intensity_s, intensity_p; /* NaN when unavailable                                  */
+    double sigma_rad, blend;
+    uint32_t flags, transition_kind;
+} icp_diffraction_result;
+
+/* Transition flags of the edge between row r and row r + 1 at one phi (RainbowTransitionFlags),
+ * and result flags (DiffractionFlags). */
+enum icp_transition_flags { ICP_TRANSITION_PRIMARY = 1, ICP_TRANSITION_SECONDARY = 2, ICP_TRANSITION_UNKNOWN = 4 };
+enum icp_diffraction_flags {
+    ICP_DIFFRACTION_FILTERED = 1,
+    ICP_DIFFRACTION_UNDERRESOLVED = 2,
+    ICP_DIFFRACTION_INPUT_UNAVAILABLE = 4,
+    ICP_DIFFRACTION_STENCIL_UNAVAILABLE = 8,
+    ICP_DIFFRACTION_DETECTION_UNAVAILABLE = 16,
+    ICP_DIFFRACTION_INVALID_DATA = 32
+};
+
+/* The diffraction counters of rainbow::WaveOpticsStatistics (src/patch_optics.cpp:224-229). */
+typedef struct {
+    uint32_t primary_transitions, secondary_transitions, unknown_transitions;
+    uint32_t filtered_directions, unavailable_directions, underresolved_directions;
+} icp_diffraction_stats;
+
+/* Table-II primary width in degrees for a drop radius in mm (0.1 .. 1.0 mm, linear between
+ * the table's radii; RainbowDiffraction::table_sigma_degrees, rainbow_diffraction.hpp:16-28).
+ * Host function.  Outside the table -> ICP_ERR_INVALID_ARGUMENT, *primary_sigma_deg untouched. */
+int icp_rainbow_table_sigma(float radius_mm, double* primary_sigma_deg);
+
+/* Transition labels d_transitions[nt*np] (device) of the focal grid d_focal[nt*np] (device):
+ * kernel detect_rainbow_transitions (device/patch_optics.cu:26-32).  An invalid configuration
+ * (RainbowDiffraction::valid_config) -> ICP_ERR_INVALID_ARGUMENT, as PatchOptics::evaluate
+ * rejects it (src/patch_optics.cpp:92-95). */
+int icp_rainbow_detect(icp_context* ctx, const icp_focal_sample* d_focal, uint32_t nt, uint32_t np,
+                       const icp_diffraction_config* config, uint32_t* d_transitions);
+
+/* Filtered directions d_results[nt*np] (device) from the focal grid and the given labels:
+ * kernel filter_rainbow_diffraction (device/patch_optics.cu:34-40).  d_density (device, may
+ * be NULL) receives intensity_s + intensity_p of every result, the density the reference's
+ * CDF builder reads for the diffraction stage (device/phase_cdf.cu:53-55), ready for
+ * icp_phase_cdf_build(ICP_CDF_DENSITY).  stats (host, may be NULL): the result counters
+ * (transition counters zero). */
+int icp_rainbow_filter(icp_context* ctx, const icp_focal_sample* d_focal, const uint32_t* d_transitions, uint32_t nt,
+                       uint32_t np, const icp_diffraction_config* config, icp_diffraction_result* d_results,
+                       double* d_density, icp_diffraction_stats* stats);
+
+/* Both passes and all counters, as PatchOptics::run_diffraction plus its statistics loop. */
+int icp_rainbow_diffraction(icp_context* ctx, const icp_focal_sample* d_focal, uint32_t nt, uint32_t np,
+                            const icp_diffraction_config* config, uint32_t* d_transitions,
+                            icp_diffraction_result* d_results, double* d_density, icp_diffraction_stats* stats);
 
 #ifdef __cplusplus
 }

@@ -12,6 +12,8 @@
 #   oracle/_ref/ref_atlas_harness        oracle/ref_atlas_harness.cpp over hex_atlas/src/atlas.cpp and
 #                                        hex_trace/src/hex_trace.cpp (area rule, atlas nodes)
 #   oracle/_ref/ice_precompute_atlas_cpu reference CLI (hex_atlas/apps/precompute_atlas.cpp), CPU build
+#   oracle/_ref/ref_rainbow_harness      oracle/ref_rainbow_harness.cpp over the header-only Table-II
+#                                        diffraction (include/rainbow/rainbow_diffraction.hpp)
 #
 # Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
 set -euo pipefail
@@ -32,6 +34,8 @@ g++ "${flags[@]}" "$ref/hex_phase/apps/generate_hex_phase.cpp" "${srcs[@]}" -o "
 g++ "${flags[@]}" "$here/ref_hex_harness.cpp" "${srcs[@]}" -o "$out/ref_hex_harness"
 g++ -std=c++20 -O2 -fno-fast-math -ffp-contract=off -I"$ref/include" "$here/ref_drop_harness.cpp" \
     "$ref/src/projected_area.cpp" "$ref/src/water_refractive_index.cpp" -o "$out/ref_drop_harness"
+g++ -std=c++20 -O2 -fno-fast-math -ffp-contract=off -I"$ref/include" "$here/ref_rainbow_harness.cpp" \
+    -o "$out/ref_rainbow_harness"
 if [ -f "$ref/hex_atlas/src/ice_optics.cpp" ]; then
     g++ -std=c++20 -O2 -fno-fast-math -ffp-contract=off -I"$ref/hex_atlas/include" "$here/ref_ice_harness.cpp" \
         "$ref/hex_atlas/src/ice_optics.cpp" -o "$out/ref_ice_harness"
@@ -41,4 +45,4 @@ if [ -f "$ref/hex_atlas/src/ice_optics.cpp" ]; then
         "$ref/hex_atlas/src/atlas.cpp" "$ref/hex_atlas/src/ice_optics.cpp" "$ref/hex_trace/src/hex_trace.cpp" \
         "$ref/src/npy_writer.cpp" -o "$out/ice_precompute_atlas_cpu"
 fi
-echo "built $out/ice_generate_phase_cpu $out/ref_hex_harness $out/ref_drop_harness $out/ref_ice_harness $out/ref_atlas_harness $out/ice_precompute_atlas_cpu"
+echo "built $out/ice_generate_phase_cpu $out/ref_hex_harness $out/ref_drop_harness $out/ref_ice_harness $out/ref_atlas_harness $out/ice_precompute_atlas_cpu $out/ref_rainbow_harness"

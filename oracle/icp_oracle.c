@@ -18,6 +18,7 @@
  *   CPU CDF builder        hex_phase/src/phase_table.cpp:104-187
  *   u edges                include/rainbow/phase_cdf_math.hpp:16-32
  *   quaternion rotation    hex_phase/src/phase_table.cpp:11-21
+ *   Table-II diffraction   include/rainbow/rainbow_diffraction.hpp:16-174
  * Parity is pinned: tests compare this restatement bit-for-bit with the
  * reference sources compiled from their own files into oracle/_ref
  * (oracle/build_ref.sh) and with fixtures under tests/golden/.
@@ -1624,4 +1625,246 @@ int icpo_drop_frame(double inclination_deg, double* k, double* e0, double* e1)
     e1[1] = k[2] * e0[0] - k[0] * e0[2];
     e1[2] = k[0] * e0[1] - k[1] * e0[0];
     return 0;
+}
+
+/* --------------------------------------------------- Table-II rainbow diffraction
+ * Restates RainbowDiffraction (include/rainbow/rainbow_diffraction.hpp): the Table-II width
+ * lookup (:16-28), the configuration check (:29-39), the transition labels of the edge below
+ * each query direction (:40-56), the local spherical Gaussian (:57-139), the haversine
+ * distance (:140-145) and the longitude window of a spherical cap (:166-174).  Binary64,
+ * the reference's operation order and the same libm calls, so the results equal the header's
+ * compiled on the same host bit for bit.  The focal records have the 144-byte layout of
+ * rainbow::FocalOpticalResult (include/rainbow/wave_optics_data.hpp:27-40). */
+typedef struct {
+    double field[4];
+    double s, p;
+    double fam_inc[4];
+    uint32_t fam_hits[4];
+    uint32_t corrected, extra;
+    uint32_t flags, first_problem;
+    double field2[4];
+} rb_focal;
+typedef struct {
+    double s, p, sigma, blend;
+    uint32_t flags, kind;
+} rb_result;
+typedef struct {
+    double s, c;
+} rb_sum;
+
+#define RB_TOL 0x1p-44 /* closed-cap cutoff slack (rainbow_diffraction.hpp:14) */
+enum { RB_PRIMARY = 1, RB_SECONDARY = 2, RB_UNKNOWN = 4 };
+enum { RB_FILTERED = 1, RB_UNDER = 2, RB_INPUT = 4, RB_STENCIL = 8, RB_DETECT = 16, RB_INVALID = 32 };
+
+int icpo_rainbow_table_sigma(float radius, double* out)
+{
+    static const float radii[10] = {0.1f, 0.2f, 0.3f, 0.4f, 0.5f, 0.6f, 0.7f, 0.8f, 0.9f, 1.0f};
+    static const double widths[10] = {0.70, 0.45, 0.30, 0.25, 0.22, 0.20, 0.18, 0.17, 0.16, 0.15};
+    if (!(radius >= radii[0] && radius <= radii[9])) return 0;
+    for (unsigned j = 0; j < 10; ++j) {
+        if (radius == radii[j]) {
+            *out = widths[j];
+            return 1;
+        }
+        if (j > 0 && radius < radii[j]) {
+            const double f = ((double)radius - radii[j - 1]) / ((double)radii[j] - radii[j - 1]);
+            *out = fma(f, widths[j] - widths[j - 1], widths[j - 1]);
+            return 1;
+        }
+    }
+    return 0;
+}
+
+/* cfg = {primary sigma (rad), support (sigmas), transition contrast, inner blend (sigmas)} */
+int icpo_rainbow_config_ok(uint32_t nt, uint32_t np, const double* cfg)
+{
+    return nt >= 2u && np >= 1u && nt <= 32767u && np <= 32767u && cfg[0] > 0 && fin(cfg[0]) && cfg[1] >= 2 &&
+           cfg[1] <= 8 && cfg[3] >= 0 && cfg[3] < cfg[1] && 2 * cfg[0] * cfg[1] < ICPO_PI && cfg[2] >= 0 && cfg[2] < 1;
+}
+
+static int rb_sample_ok(const rb_focal* r) { return r->flags == 0 && r->s >= 0 && r->p >= 0 && fin(r->s + r->p); }
+
+void icpo_rainbow_detect(const rb_focal* f, uint32_t nt, uint32_t np, const double* cfg, uint32_t* edges)
+{
+    const uint64_t n = (uint64_t)nt * np;
+    const int ok = icpo_rainbow_config_ok(nt, np, cfg);
+    for (uint64_t i = 0; i < n; ++i) {
+        uint32_t e = 0;
+        if (!ok)
+            e = RB_UNKNOWN;
+        else if (i / np + 1 != nt) { /* the last row has no edge below it */
+            const rb_focal* a = f + i;
+            const rb_focal* b = a + np;
+            if (!rb_sample_ok(a) || !rb_sample_ok(b))
+                e = RB_UNKNOWN;
+            else {
+                const double x = a->s + a->p, y = b->s + b->p, peak = fmax(x, y);
+                if (peak > 0 && fin(peak) && !(fabs(y - x) / peak < cfg[2])) {
+                    /* entering TRT support with increasing theta / leaving TRRT support */
+                    if (a->fam_hits[2] == 0 && b->fam_hits[2] > 0 && b->fam_inc[2] > 0) e |= RB_PRIMARY;
+                    if (a->fam_hits[3] > 0 && b->fam_hits[3] == 0 && a->fam_inc[3] > 0) e |= RB_SECONDARY;
+                }
+            }
+        }
+        edges[i] = e;
+    }
+}
+
+static int rb_wrap(int a, int n)
+{
+    const int r = a % n;
+    return r < 0 ? r + n : r;
+}
+double icpo_rainbow_distance(double a, double b, double phi)
+{
+    const double u = sin(0.5 * (a - b)), v = sin(0.5 * phi);
+    const double h = fma(sin(a) * sin(b), v * v, u * u);
+    return 2 * asin(sqrt(fmin(1.0, fmax(0.0, h))));
+}
+/* Half-width in columns of the longitude window of the cap of `radius` around colatitude t
+ * on row colatitude r; -1 when the row misses the cap, nc when the cap wraps the row. */
+static int rb_window(double t, double r, double radius, double dp, int nc)
+{
+    if (fabs(t - r) > radius + RB_TOL) return -1;
+    const double a = sin(t) * sin(r), b = cos(t) * cos(r);
+    if (!(a > 0)) return nc;
+    const double x = (cos(radius) - b) / a;
+    if (x <= -1) return nc;
+    if (x >= 1) return 1;
+    const int w = (int)ceil(acos(x) / dp) + 1;
+    return nc < w ? nc : w;
+}
+static void rb_add(rb_sum* z, double x)
+{
+    const double n = z->s + x;
+    z->c += fabs(z->s) >= fabs(x) ? (z->s - n) + x : (x - n) + z->s;
+    z->s = n;
+}
+static void rb_unavailable(rb_result* r) { r->s = r->p = NAN; }
+
+static rb_result rb_filter_one(const rb_focal* f, const uint32_t* edges, int nr, int nc, const double* cfg, int ok,
+                               uint32_t index)
+{
+    rb_result out = {0, 0, 0, 0, 0, 0};
+    if (!ok) {
+        out.flags = RB_INVALID;
+        rb_unavailable(&out);
+        return out;
+    }
+    const rb_focal* c0 = f + index;
+    if (!rb_sample_ok(c0)) {
+        out.flags = RB_INPUT;
+        rb_unavailable(&out);
+        return out;
+    }
+    out.s = c0->s;
+    out.p = c0->p;
+    const int row = (int)(index / (uint32_t)nc), col = (int)(index % (uint32_t)nc);
+    const double dt = ICPO_PI / (double)nr, dp = 2 * ICPO_PI / (double)nc, t = (row + 0.5) * dt;
+    const double support = cfg[1];
+    /* nearest labelled edge within twice the primary support, in units of its own sigma */
+    const double search = 2 * cfg[0] * support;
+    int lo = (int)floor((t - search) / dt) - 1, hi = (int)ceil((t + search) / dt);
+    if (lo < 0) lo = 0;
+    if (hi > nr - 2) hi = nr - 2;
+    double best = support + 1;
+    for (int rr = lo; rr <= hi; ++rr) {
+        const double tr = (rr + 1.0) * dt; /* the edge lies between rows rr and rr + 1 */
+        const int w = rb_window(t, tr, search, dp, nc);
+        if (w < 0) continue;
+        const int count = nc < 2 * w + 1 ? nc : 2 * w + 1, start = count == nc ? 0 : col - w;
+        for (int j = 0; j < count; ++j) {
+            const int cc = rb_wrap(start + j, nc);
+            const double d = icpo_rainbow_distance(t, tr, (cc - col) * dp);
+            if (d > search + RB_TOL) continue;
+            const uint32_t e = edges[(uint32_t)rr * (uint32_t)nc + (uint32_t)cc];
+            if (e & RB_UNKNOWN) out.flags |= RB_DETECT;
+            for (uint32_t kind = RB_PRIMARY; kind <= RB_SECONDARY; kind *= 2u) {
+                if (!(e & kind)) continue;
+                const double sigma = cfg[0] * (kind == RB_SECONDARY ? 2 : 1);
+                const double dist = d / sigma;
+                if (dist < support && (dist < best - 1e-12 || (fabs(dist - best) <= 1e-12 && kind < out.kind))) {
+                    best = dist;
+                    out.sigma = sigma;
+                    out.kind = kind;
+                }
+            }
+        }
+    }
+    if (out.flags & RB_DETECT) {
+        rb_unavailable(&out);
+        return out;
+    }
+    if (out.kind == 0) return out;
+    const double sigma = out.sigma;
+    if (dt > 0.5 * sigma || sin(t) * dp > 0.5 * sigma) out.flags |= RB_UNDER;
+    out.blend = 1;
+    if (best > cfg[3]) {
+        const double x = (best - cfg[3]) / (support - cfg[3]);
+        out.blend = 1 - x * x * (3 - 2 * x);
+    }
+    /* solid-angle weighted Gaussian over the cap of support x sigma, compensated sums */
+    const double radius = support * sigma;
+    int lower = (int)floor((t - radius) / dt) - 1, upper = (int)ceil((t + radius) / dt);
+    if (lower < 0) lower = 0;
+    if (upper > nr - 1) upper = nr - 1;
+    rb_sum ws = {0, 0}, ss = {0, 0}, sp = {0, 0};
+    for (int rr = lower; rr <= upper; ++rr) {
+        const double tr = (rr + 0.5) * dt;
+        const int w = rb_window(t, tr, radius, dp, nc);
+        if (w < 0) continue;
+        const int count = nc < 2 * w + 1 ? nc : 2 * w + 1, start = count == nc ? 0 : col - w;
+        const double area = 2 * sin(tr) * sin(0.5 * dt) * dp;
+        for (int j = 0; j < count; ++j) {
+            const int cc = rb_wrap(start + j, nc);
+            const double d = icpo_rainbow_distance(t, tr, (cc - col) * dp);
+            if (d > radius + RB_TOL) continue;
+            const rb_focal* q = f + (uint32_t)rr * (uint32_t)nc + (uint32_t)cc;
+            if (!rb_sample_ok(q)) {
+                out.flags |= RB_STENCIL;
+                continue;
+            }
+            const double weight = exp(-0.5 * (d / sigma) * (d / sigma)) * area;
+            rb_add(&ws, weight);
+            rb_add(&ss, weight * q->s);
+            rb_add(&sp, weight * q->p);
+        }
+    }
+    if (out.flags & RB_STENCIL) {
+        rb_unavailable(&out);
+        return out;
+    }
+    const double total = ws.s + ws.c;
+    if (!(total > 0) || !fin(total)) {
+        out.flags |= RB_INVALID;
+        rb_unavailable(&out);
+        return out;
+    }
+    /* constant-preserving local normalisation, blended toward the unfiltered value */
+    out.s = fma(out.blend, (ss.s + ss.c) / total - c0->s, c0->s);
+    out.p = fma(out.blend, (sp.s + sp.c) / total - c0->p, c0->p);
+    if (!(out.s >= 0 && out.p >= 0) || !fin(out.s + out.p)) {
+        out.flags |= RB_INVALID;
+        rb_unavailable(&out);
+        return out;
+    }
+    out.flags |= RB_FILTERED;
+    return out;
+}
+
+void icpo_rainbow_filter(const rb_focal* f, const uint32_t* edges, uint32_t nt, uint32_t np, const double* cfg,
+                         rb_result* out)
+{
+    const int ok = icpo_rainbow_config_ok(nt, np, cfg);
+    const uint64_t n = (uint64_t)nt * np;
+    for (uint64_t i = 0; i < n; ++i) out[i] = rb_filter_one(f, edges, (int)nt, (int)np, cfg, ok, (uint32_t)i);
+}
+
+/* The filter at `count` chosen directions only (bounded CPU time on large grids). */
+void icpo_rainbow_filter_at(const rb_focal* f, const uint32_t* edges, uint32_t nt, uint32_t np, const double* cfg,
+                            const uint64_t* index, uint64_t count, rb_result* out)
+{
+    const int ok = icpo_rainbow_config_ok(nt, np, cfg);
+    for (uint64_t k = 0; k < count; ++k)
+        out[k] = rb_filter_one(f, edges, (int)nt, (int)np, cfg, ok, (uint32_t)index[k]);
 }

@@ -59,6 +59,14 @@ def _lib() -> C.CDLL:
     lib.icpo_drop_trace_from.argtypes = [_D, _D, _D, _D, C.c_uint32, C.c_uint32, _D, _D]
     lib.icpo_drop_intersect.argtypes = [_D, _D, _D, C.c_int, _D]
     lib.icpo_drop_frame.argtypes = [C.c_double, _D, _D, _D]
+    lib.icpo_rainbow_table_sigma.argtypes = [C.c_float, _D]
+    lib.icpo_rainbow_config_ok.argtypes = [C.c_uint32, C.c_uint32, _D]
+    lib.icpo_rainbow_distance.restype = C.c_double
+    lib.icpo_rainbow_distance.argtypes = [C.c_double] * 3
+    lib.icpo_rainbow_detect.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, _D, C.c_void_p]
+    lib.icpo_rainbow_filter.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, _D, C.c_void_p]
+    lib.icpo_rainbow_filter_at.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, _D, C.c_void_p,
+                                           C.c_uint64, C.c_void_p]
     lib.icpo_atlas_node.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint32, _D, _D,
                                     _D, _D, C.c_uint64, _D, C.c_uint32, C.c_uint32, C.c_double, _D, _D]
     return lib
@@ -418,3 +426,97 @@ def ref_drop_families(radius_mm: float, sphere: bool, n_int: float, k, grid: int
     a = np.fromfile(out, dtype="<f8").reshape(-1, 41)
     out.unlink()
     return a
+
+
+# ------------------------------------------------------- Table-II rainbow diffraction
+# rainbow::FocalOpticalResult (include/rainbow/wave_optics_data.hpp:27-40) and
+# rainbow::DiffractionResult (:66-78) as numpy records.
+FOCAL_DTYPE = np.dtype([("field", "<f8", 4), ("intensity_s", "<f8"), ("intensity_p", "<f8"),
+                        ("family_incoherent", "<f8", 4), ("family_hits", "<u4", 4), ("corrected_hits", "<u4"),
+                        ("extra_quarter_turn_hits", "<u4"), ("flags", "<u4"), ("first_problem_patch_id", "<u4"),
+                        ("field_second", "<f8", 4)])
+RESULT_DTYPE = np.dtype([("intensity_s", "<f8"), ("intensity_p", "<f8"), ("sigma_rad", "<f8"), ("blend", "<f8"),
+                         ("flags", "<u4"), ("transition_kind", "<u4")])
+assert FOCAL_DTYPE.itemsize == 144 and RESULT_DTYPE.itemsize == 40
+
+
+def _cfg(config) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(config, dtype=np.float64).reshape(4))
+
+
+def rainbow_table_sigma(radius: float) -> float | None:
+    """Table-II primary width (degrees) of a float32 radius in mm, None outside the table."""
+    out = np.zeros(1)
+    return float(out[0]) if lib().icpo_rainbow_table_sigma(float(radius), _p(out)) else None
+
+
+def rainbow_config_ok(nt: int, np_: int, config) -> bool:
+    return bool(lib().icpo_rainbow_config_ok(nt, np_, _p(_cfg(config))))
+
+
+def rainbow_distance(a: float, b: float, phi: float) -> float:
+    return float(lib().icpo_rainbow_distance(a, b, phi))
+
+
+def rainbow_detect(focal: np.ndarray, nt: int, np_: int, config) -> np.ndarray:
+    """Transition labels (uint32 [nt*np]) of a focal grid (FOCAL_DTYPE [nt*np]); config =
+    (primary sigma rad, support sigma, transition contrast, inner blend sigma)."""
+    f = np.ascontiguousarray(focal, dtype=FOCAL_DTYPE).reshape(-1)
+    assert f.size == nt * np_
+    edges = np.zeros(nt * np_, dtype=np.uint32)
+    lib().icpo_rainbow_detect(f.ctypes.data, nt, np_, _p(_cfg(config)), edges.ctypes.data)
+    return edges
+
+
+def rainbow_filter(focal: np.ndarray, edges: np.ndarray, nt: int, np_: int, config) -> np.ndarray:
+    """Diffraction results (RESULT_DTYPE [nt*np]) of a focal grid under the given labels."""
+    f = np.ascontiguousarray(focal, dtype=FOCAL_DTYPE).reshape(-1)
+    e = np.ascontiguousarray(edges, dtype=np.uint32).reshape(-1)
+    assert f.size == e.size == nt * np_
+    out = np.zeros(nt * np_, dtype=RESULT_DTYPE)
+    lib().icpo_rainbow_filter(f.ctypes.data, e.ctypes.data, nt, np_, _p(_cfg(config)), out.ctypes.data)
+    return out
+
+
+def rainbow_filter_at(focal: np.ndarray, edges: np.ndarray, nt: int, np_: int, config, index) -> np.ndarray:
+    """The diffraction results at the given direction indices only."""
+    f = np.ascontiguousarray(focal, dtype=FOCAL_DTYPE).reshape(-1)
+    e = np.ascontiguousarray(edges, dtype=np.uint32).reshape(-1)
+    idx = np.ascontiguousarray(index, dtype=np.uint64).reshape(-1)
+    assert f.size == e.size == nt * np_ and (idx < nt * np_).all()
+    out = np.zeros(idx.size, dtype=RESULT_DTYPE)
+    lib().icpo_rainbow_filter_at(f.ctypes.data, e.ctypes.data, nt, np_, _p(_cfg(config)), idx.ctypes.data, idx.size,
+                                 out.ctypes.data)
+    return out
+
+
+def ref_rainbow_available() -> bool:
+    return (REF_DIR / "ref_rainbow_harness").exists()
+
+
+def ref_rainbow_table(radii) -> list[tuple[bool, float]]:
+    """The reference's table_sigma_degrees on float32 radii (given as decimal strings or floats)."""
+    text = "\n".join(repr(float(np.float32(r))) for r in radii) + "\n"
+    r = subprocess.run([str(REF_DIR / "ref_rainbow_harness"), "table"], input=text, capture_output=True, text=True,
+                       check=True)
+    return [(line.split()[0] == "1", float.fromhex(line.split()[1])) for line in r.stdout.splitlines()]
+
+
+def ref_rainbow_grid(focal: np.ndarray, nt: int, np_: int, config, edges: np.ndarray | None = None,
+                     workdir: Path | None = None) -> tuple[np.ndarray, np.ndarray]:
+    """The reference's detect (unless edges are given) and filter over a whole focal grid."""
+    f = np.ascontiguousarray(focal, dtype=FOCAL_DTYPE).reshape(-1)
+    base = Path(workdir or "/tmp") / f"ref_rainbow_{os.getpid()}"
+    src, dst = base.with_suffix(".in"), base.with_suffix(".out")
+    with open(src, "wb") as fh:
+        fh.write(np.array([nt, np_], dtype="<u4").tobytes() + _cfg(config).tobytes())
+        fh.write(np.array([0 if edges is None else 1, 0], dtype="<u4").tobytes() + f.tobytes())
+        if edges is not None:
+            fh.write(np.ascontiguousarray(edges, dtype="<u4").tobytes())
+    subprocess.run([str(REF_DIR / "ref_rainbow_harness"), "grid", str(src), str(dst)], check=True)
+    raw = dst.read_bytes()
+    src.unlink()
+    dst.unlink()
+    n = nt * np_
+    return (np.frombuffer(raw[: 4 * n], dtype="<u4").copy(),
+            np.frombuffer(raw[4 * n:], dtype=RESULT_DTYPE).copy())

@@ -252,6 +252,64 @@ def compare_fixtures(td: Path) -> None:
     np.savez_compressed(HERE / "compare_reference.npz", **out)
 
 
+RAINBOW_RADII = ["0.1", "0.2", "0.3", "0.4", "0.5", "0.6", "0.7", "0.8", "0.9", "1.0", "1.01", "0.01", "0.35", "0.15",
+                 "0.55", "0.95", "0.0999999", "0.1000001", "0.9999999", "1.0000001", "0.123456", "0.7777", "0.25",
+                 "0.45", "nan", "-0.5"]
+
+
+def rainbow_fixtures(td: Path) -> None:
+    """The reference's Table-II lookup on float32 radii and its detect + filter on the grids of
+    tests/rainbow_cases.py (every output field, bit for bit; the labels handed to the filter;
+    the SHA-256 of each input grid)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import rainbow_cases as RC  # noqa: E402
+    r = subprocess.run([str(REF_BIN / "ref_rainbow_harness"), "table"], input="\n".join(RAINBOW_RADII) + "\n",
+                       capture_output=True, text=True, check=True)
+    rows = [line.split() for line in r.stdout.splitlines()]
+    out = {"table_radius": np.array([np.float32(float(x)) for x in RAINBOW_RADII], dtype=np.float32),
+           "table_ok": np.array([int(a) for a, _ in rows], dtype=np.uint8),
+           "table_sigma": np.array([float.fromhex(b) for _, b in rows])}
+    n = len(RAINBOW_RADII)
+    assert len(rows) == n
+    for name, nt, np_, cfg, make, spec in RC.CASES:
+        f = make()
+        src, dst = td / "rb.in", td / "rb.out"
+        given = RC.labels_for(spec, lambda g: _ref_grid(src, dst, f if g is None else g, nt, np_, cfg, None)[0])
+        edges, res = _ref_grid(src, dst, f, nt, np_, cfg, given)
+        out[f"{name}.digest"] = np.array(RC.digest(f))
+        out[f"{name}.shape"] = np.array([nt, np_], dtype=np.uint32)
+        out[f"{name}.config"] = np.array(cfg, dtype=np.float64)
+        out[f"{name}.given"] = np.array(0 if given is None else 1, dtype=np.uint8)
+        out[f"{name}.edges"] = edges
+        # a direction without flags is returned unchanged (input intensities, zero width and
+        # blend, no kind): only the flagged ones are stored in full
+        changed = np.flatnonzero(res["flags"])
+        out[f"{name}.flags"] = res["flags"].copy()
+        out[f"{name}.changed"] = changed.astype(np.uint32)
+        for k in ("intensity_s", "intensity_p", "sigma_rad", "blend", "transition_kind"):
+            out[f"{name}.{k}"] = res[k][changed].copy()
+        quiet = res["flags"] == 0
+        assert (res["transition_kind"][quiet] == 0).all() and (res["sigma_rad"][quiet] == 0).all()
+        assert (res["blend"][quiet] == 0).all()
+        assert (res["intensity_s"][quiet] == f["intensity_s"][quiet]).all()
+        assert (res["intensity_p"][quiet] == f["intensity_p"][quiet]).all()
+    np.savez_compressed(HERE / "rainbow_reference.npz", **out)
+
+
+def _ref_grid(src: Path, dst: Path, f, nt, np_, cfg, edges):
+    import rainbow_cases as RC  # noqa: E402
+    with open(src, "wb") as fh:
+        fh.write(np.array([nt, np_], dtype="<u4").tobytes() + np.asarray(cfg, dtype="<f8").tobytes())
+        fh.write(np.array([0 if edges is None else 1, 0], dtype="<u4").tobytes())
+        fh.write(np.ascontiguousarray(f, dtype=RC.FOCAL_DTYPE).tobytes())
+        if edges is not None:
+            fh.write(np.ascontiguousarray(edges, dtype="<u4").tobytes())
+    run([REF_BIN / "ref_rainbow_harness", "grid", src, dst])
+    raw = dst.read_bytes()
+    n = nt * np_
+    return np.frombuffer(raw[:4 * n], "<u4").copy(), np.frombuffer(raw[4 * n:], RC.RESULT_DTYPE).copy()
+
+
 def main() -> None:
     subprocess.run([str(ROOT / "oracle" / "build_ref.sh"), str(REF)], check=True)
     with tempfile.TemporaryDirectory() as t:
@@ -295,6 +353,8 @@ def main() -> None:
         atlas_fixtures(td)
         # 7. the reference's record-vs-record metric
         compare_fixtures(td)
+        # 8. Table-II rainbow diffraction
+        rainbow_fixtures(td)
     for f in sorted(HERE.glob("*.npz")):
         print(f.name, f.stat().st_size)
 
