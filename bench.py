@@ -727,6 +727,77 @@ def run_atlas(I, ctx, stream, a) -> dict:
             "cpu_baseline": cpu, "cpu_baseline_precompute": cpu_pre}
 
 
+def run_rainbow(I, ctx, stream, a) -> dict:
+    """Table-II rainbow diffraction on the drop records' 1800 x 3600 query grid (0.1 degree
+    cells; a seeded synthetic focal grid with wobbling primary and secondary bows, radius
+    0.5 mm -> sigma 0.22 / 0.44 degrees): both passes through the C ABI, device-resident, timed
+    on the context's stream; the oracle's detect and a uniform sample of its filter as the CPU
+    baseline."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    sys.path.insert(0, str(ROOT / "tests"))
+    import rainbow_cases as RC
+
+    nt, np_ = 1800, 3600
+    n = nt * np_
+    focal = RC.bow_grid(nt, np_, 31, noise=0.2)
+    cfg = I.diffraction_config(0.5)
+    d_focal = I.DeviceArray(ctx, n, I.FOCAL_DTYPE).upload(focal)
+    d_edges = I.DeviceArray(ctx, n, np.uint32)
+    d_res = I.DeviceArray(ctx, n, I.DIFFRACTION_DTYPE)
+    d_den = I.DeviceArray(ctx, n)
+    stats = I.DiffractionStats()
+
+    def once() -> None:
+        I.check(I.LIB.icp_rainbow_diffraction(ctx.handle, d_focal.ptr, nt, np_, C.byref(cfg), d_edges.ptr, d_res.ptr,
+                                              d_den.ptr, C.byref(stats)))
+
+    for _ in range(3):
+        once()
+    launches0 = I.kernel_launches()
+    times = []
+    for _ in range(max(1, a.rainbow_steps)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        once()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1) / 1e3)
+    launches = (I.kernel_launches() - launches0) // max(1, a.rainbow_steps)
+    t = sorted(times)[len(times) // 2]
+    # algorithmic bytes per direction: the focal fields read (s, p, flags, TRT / TRRT hits and
+    # incoherent: 44 B), labels and packed samples written and read back (2 x 20 B), result and
+    # density written (48 B)
+    bytes_per_dir = 44 + 40 + 48
+    hbm = _peaks().get("hbm_gbs") or 6650.0
+    cpu = None
+    if not a.no_cpu_baseline:
+        from oracle import oracle as O
+
+        c4 = (cfg.primary_sigma_rad, cfg.support_sigma, cfg.transition_contrast, cfg.inner_blend_sigma)
+        t0 = time.perf_counter()
+        edges = O.rainbow_detect(focal, nt, np_, c4)
+        t_det = time.perf_counter() - t0
+        pick = np.random.default_rng(9).integers(0, n, 20000)
+        t0 = time.perf_counter()
+        O.rainbow_filter_at(focal, edges, nt, np_, c4, pick)
+        t_fil = (time.perf_counter() - t0) * n / pick.size
+        cpu = {"value": n / (t_det + t_fil), "unit": "directions/s", "cores": 1, "kind": "port",
+               "sample": "oracle detect over the whole grid + its filter at 20000 uniform random directions, "
+                         "scaled to the grid"}
+    return {"workload": "rainbow_table2_1800x3600_r0.5mm", "directions": n, "ms_per_pass": 1e3 * t,
+            "directions_per_s": n / t, "kernel_launches_per_pass": launches, "stats": {
+                k: getattr(stats, k) for k, _ in stats._fields_},
+            "roofline": {"bound": "hbm", "achieved": bytes_per_dir * n / t / 1e9, "peak": hbm, "unit": "GB/s",
+                         "frac": bytes_per_dir * n / t / 1e9 / hbm,
+                         "note": "whole pass (detect + filter + counters) against the algorithmic bytes; the "
+                                 "filtered band is FP64-bound (sin, asin, exp per neighbour)"},
+            "cpu_baseline": cpu}
+
+
 def _peaks() -> dict:
     try:
         return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
@@ -915,6 +986,13 @@ def run_b200_drop(a) -> None:
         except (I.IcpError, RuntimeError, ValueError, OSError) as e:  # reported on the line, not fatal to it
             atlas = {"error": f"{type(e).__name__}: {e}"}
 
+    rainbow = None
+    if world == 1 and a.rainbow_steps > 0:
+        try:
+            rainbow = run_rainbow(I, ctx, stream, a)
+        except (I.IcpError, RuntimeError, ValueError, OSError) as e:  # reported on the line, not fatal to it
+            rainbow = {"error": f"{type(e).__name__}: {e}"}
+
     s0 = stats_all[-1]
     r0 = reps[-1]
     line = {
@@ -949,6 +1027,8 @@ def run_b200_drop(a) -> None:
         line["surrogate"] = surrogate
     if atlas is not None:
         line["atlas"] = atlas
+    if rainbow is not None:
+        line["rainbow_diffraction"] = rainbow
     if r0 is not None:
         line["record"] = {"g": r0.cdf.g_stored, "projected_area_mm2": r0.projected_area_mm2,
                           "incident_area_mm2": r0.incident_area_mm2, "diffraction_mm2": r0.diffraction_area_mm2,
@@ -978,6 +1058,8 @@ def main() -> None:
     p.add_argument("--hash-slots", type=int, default=0, help="shared histogram slots (0 = default, 1 = none)")
     p.add_argument("--atlas-incidents", type=int, default=0,
                    help="incidences of the deterministic atlas composition measurement (0 = skip)")
+    p.add_argument("--rainbow-steps", type=int, default=0,
+                   help="timed passes of the Table-II rainbow diffraction measurement (0 = skip)")
     p.add_argument("--rays", type=float, default=1e8)
     p.add_argument("--ref-rays", type=float, default=1.6e6, help="reference rays per step (all processes)")
     p.add_argument("--no-cpu-baseline", action="store_true")
