@@ -19,6 +19,8 @@ Mirrored reference interfaces (Somatic-Cell/ice-crystal-phase):
   PhaseMassAccumulatorCuda.add_drop  RaindropTracer::trace_unpolarized + patch stages, replaced by
                                    direct binning (include/rainbow/raindrop_tracer.hpp:32-36)
   generate_drop_record             apps/generate_phase.cpp:395-453 (rainbow_generate's record path)
+  patch_optics                     PatchOptics::evaluate_device / evaluate_wave_device's kernels
+                                   evaluate_patch_optics / evaluate_focal_optics, device/patch_optics.cu:7-24
   rainbow_table_sigma              include/rainbow/rainbow_diffraction.hpp:16-28
   diffraction_config               src/patch_optics.cpp:79-95 (the diffraction part of evaluate_wave_device)
   rainbow_diffraction              PatchOptics::run_diffraction + its statistics, src/patch_optics.cpp:217-231,
@@ -232,6 +234,44 @@ DIFFRACTION_FILTERED, DIFFRACTION_UNDERRESOLVED, DIFFRACTION_INPUT_UNAVAILABLE =
 DIFFRACTION_STENCIL_UNAVAILABLE, DIFFRACTION_DETECTION_UNAVAILABLE, DIFFRACTION_INVALID_DATA = 8, 16, 32
 
 
+class Vec3f(C.Structure):
+    _fields_ = [("x", C.c_float), ("y", C.c_float), ("z", C.c_float)]
+
+
+class OpticsInput(C.Structure):
+    _fields_ = [("vertices", C.c_void_p), ("patches", C.c_void_p), ("directions", C.c_void_p),
+                ("offsets", C.c_void_p), ("summaries", C.c_void_p), ("hits", C.c_void_p),
+                ("second_input_fields", C.c_void_p), ("hit_storage_count", C.c_uint64),
+                ("vertex_count", C.c_uint32), ("patch_count", C.c_uint32), ("direction_count", C.c_uint32),
+                ("second_input_count", C.c_uint32), ("incident_direction", Vec3f), ("incident_basis_x", Vec3f),
+                ("input_polarization", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class FocalConfig(C.Structure):
+    _fields_ = [("grid_width", C.c_uint32), ("grid_height", C.c_uint32), ("grid_half_extent", C.c_float),
+                ("reserved", C.c_uint32), ("quarter_turn_offsets", C.c_uint32 * 4)]
+
+
+# The lattice, patch and query records of the drop's wave stages (icp_outgoing_vertex = 
+# rainbow::OutgoingVertex, icp_outgoing_patch, icp_query_hit, icp_query_summary) and the
+# per-direction optical result (icp_optical_result = rainbow::PatchOpticalResult).
+VERTEX_DTYPE = np.dtype([("position", "<f4", 3), ("direction", "<f4", 3), ("basis_x", "<f4", 3),
+                         ("field", "<f4", 4), ("turns", "<i4"), ("fraction", "<f4"), ("status", "<u4"),
+                         ("diagnostics", "<u4")])
+PATCH_DTYPE = np.dtype([("vertex_indices", "<u4", 4), ("patch_id", "<u4"), ("status", "<u4"),
+                        ("signed_solid_angle_sr", "<f4"), ("incident_area_drop2", "<f4")])
+HIT_DTYPE = np.dtype([("compact_index", "<u4"), ("patch_id", "<u4"), ("root_index", "<u4"), ("flags", "<u4"),
+                      ("u", "<f4"), ("v", "<f4"), ("t", "<f4"), ("residual", "<f4")])
+SUMMARY_DTYPE = np.dtype([(k, "<u4") for k in ("candidate_count", "hit_count", "regular_hits", "refinement_hits",
+                                               "boundary_hits", "flags", "first_problem_patch_id", "reserved")])
+OPTICAL_DTYPE = np.dtype([("path_field", "<f8", 4), ("incoherent_s", "<f8"), ("incoherent_p", "<f8"),
+                          ("path_s", "<f8"), ("path_p", "<f8")] +
+                         [(k, "<u4") for k in ("hit_count", "evaluated_hits", "rejected_hits", "refinement_hits",
+                                               "boundary_hits", "singular_hits", "flags", "query_flags",
+                                               "first_problem_patch_id", "folded_hits")] +
+                         [("path_field_second", "<f8", 4)])
+
+
 class SurrogateConfig(C.Structure):
     _fields_ = [("nt", C.c_uint32), ("np", C.c_uint32), ("hidden", C.c_uint32), ("input_width", C.c_uint32),
                 ("theta_frequencies", C.c_uint32), ("phi_frequencies", C.c_uint32), ("max_records", C.c_uint32),
@@ -315,6 +355,7 @@ _FUNCS = {
     "icp_atlas_coupling": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_double, C.c_double, _D, _P, _P,
                                      C.c_uint64, _D, C.c_double, C.c_int, _P, _D]),
     "icp_atlas_compose": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, _P, _P, _P]),
+    "icp_patch_optics": (C.c_int, [_P, C.POINTER(OpticsInput), _P, C.POINTER(FocalConfig), _P]),
     "icp_rainbow_table_sigma": (C.c_int, [C.c_float, _D]),
     "icp_rainbow_detect": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32, C.POINTER(DiffractionConfig), _P]),
     "icp_rainbow_filter": (C.c_int, [_P, _P, _P, C.c_uint32, C.c_uint32, C.POINTER(DiffractionConfig), _P, _P,
@@ -1147,3 +1188,37 @@ def rainbow_diffraction(ctx: Context, focal, nt: int, np_: int, config: Diffract
         check(LIB.icp_rainbow_filter(ctx.handle, df.ptr, dt.ptr, nt, np_, C.byref(config), dr.ptr, dd.ptr,
                                      C.byref(stats)))
     return DiffractionOutput(dt.download(), dr.download(), dd.download(), stats.as_dict())
+
+
+# ------------------------------------------------------------------ patch optics
+def patch_optics(ctx: Context, vertices, patches, directions, offsets, summaries, hits, incident, incident_basis,
+                 second=None, polarization: int | None = None, focal=None) -> tuple[np.ndarray, np.ndarray | None]:
+    """Per-direction optics of the drop's wave stages from host arrays (VERTEX_DTYPE, PATCH_DTYPE,
+    float32 [n, 3] directions, uint64 [n + 1] hit offsets, SUMMARY_DTYPE [n], HIT_DTYPE, optional
+    float32 [vertices, 4] second response column): the OPTICAL_DTYPE results and, with
+    focal = (grid_width, grid_height, grid_half_extent, quarter_turn_offsets[4]), the focal stage
+    (FOCAL_DTYPE, the input of rainbow_diffraction).  polarization defaults to unpolarized
+    exactly when a second column is given."""
+    n = len(directions)
+    arrays = [DeviceArray(ctx, len(a), dt).upload(np.ascontiguousarray(a, dtype=dt).reshape(-1))
+              for a, dt in ((vertices, VERTEX_DTYPE), (patches, PATCH_DTYPE), (summaries, SUMMARY_DTYPE),
+                            (hits, HIT_DTYPE))]
+    dv, dp, ds, dh = arrays
+    dd = DeviceArray(ctx, 3 * n, np.float32).upload(np.asarray(directions, dtype=np.float32).reshape(-1))
+    do = DeviceArray(ctx, n + 1, np.uint64).upload(np.asarray(offsets, dtype=np.uint64))
+    d2 = None
+    if second is not None:
+        d2 = DeviceArray(ctx, 4 * len(second), np.float32).upload(np.asarray(second, dtype=np.float32).reshape(-1))
+    pol = (1 if second is not None else 0) if polarization is None else int(polarization)
+    inp = OpticsInput(dv.ptr, dp.ptr, dd.ptr, do.ptr, ds.ptr, dh.ptr, d2.ptr if d2 else None, len(hits),
+                      len(vertices), len(patches), n, 0 if second is None else len(second),
+                      Vec3f(*map(float, incident)), Vec3f(*map(float, incident_basis)), pol, 0)
+    dr = DeviceArray(ctx, n, OPTICAL_DTYPE)
+    df = DeviceArray(ctx, n, FOCAL_DTYPE) if focal is not None else None
+    fc = None
+    if focal is not None:
+        w, h, e, q = focal
+        fc = FocalConfig(w, h, e, 0, (C.c_uint32 * 4)(*q))
+    check(LIB.icp_patch_optics(ctx.handle, C.byref(inp), dr.ptr, C.byref(fc) if fc is not None else None,
+                               df.ptr if df is not None else None))
+    return dr.download(), (df.download() if df is not None else None)

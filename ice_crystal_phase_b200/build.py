@@ -51,6 +51,7 @@ UNITS = {
     "icp_cdf_static.cu": ["-fmad=false"],
     "icp_atlas.cu": ["-fmad=false"],
     "icp_rainbow.cu": ["-fmad=false"],
+    "icp_optics.cu": ["-fmad=false"],
 }
 
 HOST_SOURCES = ["icp_record_io.cpp"]

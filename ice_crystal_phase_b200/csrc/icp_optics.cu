@@ -1,0 +1,595 @@
+// icp_optics.cu -- per-direction optics of the drop's wave stages on the device (sm_100a) and
+// its C ABI (include/icp_b200.h, "patch optics").  Built with -fmad=false: every binary32 and
+// binary64 product and sum rounds on its own and only the reference's explicit fmaf / fma
+// calls are fused, so the arithmetic is the reference's host build's operation for operation.
+//
+// patch_optics_kernel: one thread per query direction (grid-stride over the SMs).  The thread
+// walks the direction's sorted hit list (contiguous: consecutive directions read consecutive
+// hit ranges) and, per hit, gathers the four corner vertices of the hit patch (68-byte records;
+// the whole lattice -- 4 x 513^2 vertices, 72 MB -- stays resident in the 126 MB L2 across the
+// launch), carries each corner's Jones vector(s) to the query direction's scattering frame by
+// the minimum rotation, interpolates the optical path in cycles and the fields bilinearly at
+// the hit's (u, v), and adds the coherent path field, the incoherent intensities and -- for
+// the focal stage -- the quarter-turn-corrected field and the per-family counters into
+// compensated sums, in hit order.  The reference's PatchOpticalEvaluator
+// (include/rainbow/patch_optical_evaluator.hpp) defines every value and flag; folded-branch
+// records are not taken (hits on NeedsRefinement patches are refinement-pending).
+// Device libm (sqrt / sqrtf are correctly rounded; cosf, sinf, atan2 are CUDA's) is the only
+// source of difference from the reference's host results.
+#include <cfloat>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "../../include/icp_b200.h"
+#include "icp_internal.h"
+
+using namespace icp;
+
+namespace {
+
+thread_local char g_msg[512];
+
+int fail(int status, const char* fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_msg, sizeof g_msg, fmt, ap);
+    va_end(ap);
+    set_last_error(g_msg);
+    return status;
+}
+int ok()
+{
+    set_last_error("");
+    return ICP_OK;
+}
+#define ICP_CUDA(call)                                                                                  \
+    do {                                                                                                \
+        const cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess) return fail(ICP_ERR_DEVICE, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+constexpr unsigned kThreads = 128;
+
+// result flags (PatchOpticalFlags), query flags (PatchQueryFlags), focal flags (FocalOpticalFlags)
+enum : uint32_t { kQuery = 1, kInput = 2, kFrame = 4, kPhase = 8, kArith = 16, kRefine = 32, kBoundary = 64,
+                  kSingular = 128 };
+constexpr uint32_t kErrors = kQuery | kInput | kFrame | kPhase | kArith;
+constexpr uint32_t kPending = kRefine | kBoundary | kSingular;
+constexpr uint32_t kQueryErrors = 1u | 2u | 4u | 256u;
+enum : uint32_t { kQueryRefineHit = 8, kQueryBoundaryHit = 16, kQuerySingularHit = 128 };
+enum : uint32_t { kFocalInputError = 1, kFocalInputPending = 2, kFocalDerivative = 4, kFocalGeometry = 8,
+                  kFocalArith = 16 };
+constexpr float kFrameTol = 0x1p-10f;
+constexpr float kDegenerate = 0x1p-30f;
+
+struct F3 {
+    float x, y, z;
+};
+struct D3 {
+    double x, y, z;
+};
+struct Frame {
+    F3 e0, e1;
+};
+
+__device__ __forceinline__ F3 f3(const icp_vec3f& v) { return {v.x, v.y, v.z}; }
+__device__ __forceinline__ float dot(F3 a, F3 b) { return fmaf(a.x, b.x, fmaf(a.y, b.y, a.z * b.z)); }
+__device__ __forceinline__ double dot(D3 a, D3 b) { return fma(a.x, b.x, fma(a.y, b.y, a.z * b.z)); }
+__device__ __forceinline__ F3 cross(F3 a, F3 b)
+{
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ D3 cross(D3 a, D3 b)
+{
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ F3 scale(F3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ D3 scale(D3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ F3 divide(F3 a, float s) { return {a.x / s, a.y / s, a.z / s}; }
+__device__ __forceinline__ D3 divide(D3 a, double s) { return {a.x / s, a.y / s, a.z / s}; }
+__device__ __forceinline__ F3 minus(F3 a, F3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ D3 plus(D3 a, D3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ D3 wide(F3 a) { return {a.x, a.y, a.z}; }
+__device__ __forceinline__ F3 unit(F3 a) { return divide(a, sqrtf(dot(a, a))); }
+__device__ __forceinline__ D3 unit(D3 a) { return divide(a, sqrt(dot(a, a))); }
+__device__ __forceinline__ bool finite64(double x) { return x >= -DBL_MAX && x <= DBL_MAX; }
+__device__ __forceinline__ bool finite32(float x) { return x >= -FLT_MAX && x <= FLT_MAX; }
+__device__ __forceinline__ bool finite(F3 a) { return finite32(a.x) && finite32(a.y) && finite32(a.z); }
+__device__ __forceinline__ bool finite(const icp_field32& f)
+{
+    return finite32(f.x.real) && finite32(f.x.imag) && finite32(f.y.real) && finite32(f.y.imag);
+}
+__device__ __forceinline__ bool finite(const icp_field64& f)
+{
+    return finite64(f.s_real) && finite64(f.s_imag) && finite64(f.p_real) && finite64(f.p_imag);
+}
+__device__ __forceinline__ double nan64() { return __longlong_as_double(0x7ff8000000000000ll); }
+
+// ------------------------------------------------------------ frames and transport
+__device__ __forceinline__ bool is_unit(F3 a) { return finite(a) && fabsf(dot(a, a) - 1.0f) <= kFrameTol; }
+__device__ __forceinline__ bool is_frame(F3 d, const Frame& f)
+{
+    if (!is_unit(f.e0) || !is_unit(f.e1)) return false;
+    if (fabsf(dot(d, f.e0)) > kFrameTol || fabsf(dot(d, f.e1)) > kFrameTol || fabsf(dot(f.e0, f.e1)) > kFrameTol)
+        return false;
+    return dot(cross(f.e0, f.e1), d) >= 1.0f - 4.0f * kFrameTol;
+}
+// e0 normal to the scattering plane (the incident basis carried over at exact forward or
+// backward scattering), e1 = out x e0.
+__device__ bool scattering_frame(F3 inc, F3 basis, F3 out, Frame& frame)
+{
+    if (!is_unit(inc) || !is_unit(out) || !is_unit(basis) || fabsf(dot(inc, basis)) > kFrameTol) return false;
+    F3 e0 = cross(inc, out);
+    float n2 = dot(e0, e0);
+    if (n2 > kDegenerate)
+        e0 = divide(e0, sqrtf(n2));
+    else {
+        e0 = minus(basis, scale(out, dot(out, basis)));
+        n2 = dot(e0, e0);
+        if (!(n2 > kDegenerate)) return false;
+        e0 = divide(e0, sqrtf(n2));
+    }
+    F3 e1 = cross(out, e0);
+    const float m2 = dot(e1, e1);
+    if (!(m2 > kDegenerate)) return false;
+    e1 = divide(e1, sqrtf(m2));
+    const Frame f{e0, e1};
+    if (!is_frame(out, f)) return false;
+    frame = f;
+    return true;
+}
+// Rodrigues' formula for the minimum rotation taking a to b: v = a x b, c = a . b.
+__device__ __forceinline__ D3 rotate(D3 x, D3 v, double c)
+{
+    const D3 vx = cross(v, x);
+    return plus(plus(x, vx), divide(cross(v, vx), 1.0 + c));
+}
+__device__ __forceinline__ bool fits_float(double x) { return x >= -0x1.fffffep127 && x <= 0x1.fffffep127; }
+
+// Carries `columns` Jones vectors from the source ray's frame to the target frame.
+__device__ bool transport(F3 sdir, const Frame& sf, const icp_field32* src, unsigned columns, F3 tdir,
+                          const Frame& tf, icp_field32* out)
+{
+    if (columns == 2 && (!finite(src[0]) || !finite(src[1]))) return false;
+    if (!is_unit(sdir) || !is_unit(tdir) || !is_frame(sdir, sf) || !is_frame(tdir, tf)) return false;
+    const D3 sw = unit(wide(sdir)), tw = unit(wide(tdir));
+    const double c = dot(sw, tw);
+    if (!(1.0 + c > 0x1p-30)) return false; // no unique rotation between antipodes
+    const D3 v = cross(sw, tw);
+    const D3 se0 = wide(sf.e0), se1 = wide(sf.e1), te0 = wide(tf.e0), te1 = wide(tf.e1);
+    icp_field32 tmp[2];
+    for (unsigned j = 0; j < columns; ++j) {
+        const icp_field32& f = src[j];
+        const D3 re = plus(scale(se0, double(f.x.real)), scale(se1, double(f.y.real)));
+        const D3 im = plus(scale(se0, double(f.x.imag)), scale(se1, double(f.y.imag)));
+        const D3 rt = rotate(re, v, c), it = rotate(im, v, c);
+        const double xr = dot(rt, te0), xi = dot(it, te0), yr = dot(rt, te1), yi = dot(it, te1);
+        if (!fits_float(xr) || !fits_float(xi) || !fits_float(yr) || !fits_float(yi)) return false;
+        tmp[j] = {{float(xr), float(xi)}, {float(yr), float(yi)}};
+    }
+    for (unsigned j = 0; j < columns; ++j) out[j] = tmp[j];
+    return true;
+}
+
+// ------------------------------------------------------------ optical path in cycles
+__device__ __forceinline__ bool cycles_ok(const icp_phase_cycles& q) { return q.fraction >= 0.0f && q.fraction < 1.0f; }
+__device__ __forceinline__ double cycles_diff(const icp_phase_cycles& a, const icp_phase_cycles& b)
+{
+    const long long whole = (long long)a.turns - (long long)b.turns;
+    return double(whole) + (double(a.fraction) - double(b.fraction));
+}
+__device__ bool cycles_add(const icp_phase_cycles& anchor, double delta, icp_phase_cycles& out)
+{
+    if (!(delta > -0x1p33 && delta < 0x1p33)) return false;
+    const double whole = floor(delta);
+    double frac = double(anchor.fraction) + (delta - whole);
+    long long turns = (long long)anchor.turns + (long long)whole;
+    if (frac < 0.0) {
+        --turns;
+        frac += 1.0;
+    }
+    if (frac >= 1.0) {
+        ++turns;
+        frac -= 1.0;
+    }
+    constexpr long long lo = -2147483647LL - 1, hi = 2147483647LL;
+    if (turns < lo || turns > hi) return false;
+    float stored = float(frac);
+    if (stored >= 1.0f) {
+        ++turns;
+        stored = 0.0f;
+        if (turns > hi) return false;
+    } else if (stored < 0.0f) {
+        --turns;
+        stored += 1.0f;
+        if (turns < lo) return false;
+    }
+    out.turns = int(turns);
+    out.fraction = stored == 0.0f ? 0.0f : stored;
+    return cycles_ok(out);
+}
+// Bilinear optical path anchored at q00; the corners are returned exactly.
+__device__ bool cycles_bilinear(const icp_phase_cycles* q, float u, float v, icp_phase_cycles& out)
+{
+    if (!cycles_ok(q[0]) || !cycles_ok(q[1]) || !cycles_ok(q[2]) || !cycles_ok(q[3]) || !(u >= 0.0f && u <= 1.0f) ||
+        !(v >= 0.0f && v <= 1.0f))
+        return false;
+    if (u == 0.0f && v == 0.0f) { out = q[0]; return true; }
+    if (u == 1.0f && v == 0.0f) { out = q[1]; return true; }
+    if (u == 0.0f && v == 1.0f) { out = q[2]; return true; }
+    if (u == 1.0f && v == 1.0f) { out = q[3]; return true; }
+    const double du0 = cycles_diff(q[1], q[0]), du1 = cycles_diff(q[3], q[2]), dv0 = cycles_diff(q[2], q[0]);
+    const double ud = u, vd = v;
+    const double row = fma(ud, du1 - du0, dv0);
+    return cycles_add(q[0], fma(vd, row, ud * du0), out);
+}
+// exp(+i 2 pi fraction) in binary32, exact at quarter turns.
+__device__ bool unit_phasor(const icp_phase_cycles& q, float& re, float& im)
+{
+    if (!cycles_ok(q)) return false;
+    const float f = q.fraction;
+    if (f == 0.0f) { re = 1.0f; im = 0.0f; return true; }
+    if (f == 0.25f) { re = 0.0f; im = 1.0f; return true; }
+    if (f == 0.5f) { re = -1.0f; im = 0.0f; return true; }
+    if (f == 0.75f) { re = 0.0f; im = -1.0f; return true; }
+    const float angle = 0x1.921fb6p+2f * (f > 0.5f ? f - 1.0f : f);
+    re = cosf(angle);
+    im = sinf(angle);
+    return true;
+}
+
+// ------------------------------------------------------------ focal quarter turns
+__device__ __forceinline__ bool focal_layout_ok(const icp_focal_config& c)
+{
+    if (c.grid_width < 2 || c.grid_height < 2 || !(c.grid_half_extent > 0) || !(c.grid_half_extent <= FLT_MAX))
+        return false;
+    if ((unsigned long long)c.grid_width * c.grid_height > 0xffffffffull / 4u ||
+        (unsigned long long)(c.grid_width - 1u) * (c.grid_height - 1u) > 0xffffffffull / 4u)
+        return false;
+    for (unsigned j = 0; j < 4; ++j)
+        if (c.quarter_turn_offsets[j] > 3) return false;
+    return true;
+}
+// Sign of the radial derivative of the scattering angle over the emitting plane at the cell
+// centre: one extra quarter turn where it is positive (a focal line was crossed).
+__device__ uint32_t focal_estimate(const icp_outgoing_vertex* __restrict__ vertices, uint32_t vertex_count,
+                                   const icp_outgoing_patch& patch, F3 incident, const icp_focal_config& c,
+                                   uint32_t& family_out, uint32_t& extra_out, uint32_t& turns_out)
+{
+    if (!focal_layout_ok(c) || !finite(incident)) return kFocalGeometry;
+    const uint32_t n = c.grid_width * c.grid_height, nx = c.grid_width - 1u, cells = nx * (c.grid_height - 1u);
+    if (patch.patch_id >= 4u * cells || vertex_count < 4u * n) return kFocalGeometry;
+    const uint32_t family = patch.patch_id / cells, cell = patch.patch_id % cells;
+    const uint32_t ix = cell % nx, iy = cell / nx;
+    const uint32_t first = family * n + iy * c.grid_width + ix;
+    const uint32_t expected[4] = {first, first + 1u, first + c.grid_width, first + c.grid_width + 1u};
+    const D3 wi = wide(incident);
+    if (!(dot(wi, wi) > 0)) return kFocalGeometry;
+    double theta[4];
+    for (unsigned j = 0; j < 4; ++j) {
+        if (patch.vertex_indices[j] != expected[j]) return kFocalGeometry;
+        const icp_outgoing_vertex& a = vertices[expected[j]];
+        const F3 dir = f3(a.direction_drop);
+        if (a.status != 1u || !finite(dir)) return kFocalGeometry;
+        const D3 wo = wide(dir);
+        if (!(dot(wo, wo) > 0)) return kFocalGeometry;
+        const D3 x = cross(wi, wo);
+        theta[j] = atan2(sqrt(dot(x, x)), dot(wi, wo));
+        if (!finite64(theta[j])) return kFocalGeometry;
+    }
+    const double e = double(c.grid_half_extent);
+    const double du = 2 * e / double(c.grid_width - 1u), dv = 2 * e / double(c.grid_height - 1u);
+    const double U = (2 * (double(ix) + 0.5) / double(c.grid_width - 1u) - 1) * e;
+    const double V = (2 * (double(iy) + 0.5) / double(c.grid_height - 1u) - 1) * e;
+    const double r2 = fma(U, U, V * V);
+    if (!(r2 > 0)) return kFocalDerivative;
+    const double gu = ((theta[1] - theta[0]) + (theta[3] - theta[2])) / (2 * du);
+    const double gv = ((theta[2] - theta[0]) + (theta[3] - theta[1])) / (2 * dv);
+    const double num = fma(U, gu, V * gv);
+    const double guard = 0x1p-46 * (fabs(U * gu) + fabs(V * gv) + 1); // cancellation guard
+    if (!finite64(num) || !finite64(r2)) return kFocalGeometry;
+    if (fabs(num) <= guard) return kFocalDerivative;
+    if (!finite64(num / (2 * r2))) return kFocalGeometry;
+    family_out = family;
+    extra_out = num > 0 ? 1u : 0u;
+    turns_out = (c.quarter_turn_offsets[family] + extra_out) & 3u;
+    return 0;
+}
+__device__ __forceinline__ icp_field64 quarter_turns(const icp_field64& a, uint32_t q)
+{
+    switch (q & 3u) {
+    case 1: return {-a.s_imag, a.s_real, -a.p_imag, a.p_real};
+    case 2: return {-a.s_real, -a.s_imag, -a.p_real, -a.p_imag};
+    case 3: return {a.s_imag, -a.s_real, a.p_imag, -a.p_real};
+    default: return a;
+    }
+}
+
+// ------------------------------------------------------------ per hit, per direction
+struct Compensated {
+    double s = 0, c = 0;
+    __device__ __forceinline__ void add(double x)
+    {
+        const double n = s + x;
+        c += fabs(s) >= fabs(x) ? (s - n) + x : (x - n) + s;
+        s = n;
+    }
+    __device__ __forceinline__ double value() const { return s + c; }
+};
+struct FieldSum {
+    Compensated sr, si, pr, pi;
+    __device__ __forceinline__ void add(const icp_field64& f)
+    {
+        sr.add(f.s_real);
+        si.add(f.s_imag);
+        pr.add(f.p_real);
+        pi.add(f.p_imag);
+    }
+    __device__ __forceinline__ icp_field64 value() const { return {sr.value(), si.value(), pr.value(), pi.value()}; }
+};
+struct Contribution {
+    icp_field64 field[2];
+    double inc_s, inc_p;
+};
+__device__ __forceinline__ double lerp2(double a, double b, double c, double d, double u, double v)
+{
+    const double lower = fma(u, b - a, a), upper = fma(u, d - c, c);
+    return fma(v, upper - lower, lower);
+}
+
+__device__ uint32_t hit_optics(const icp_optics_input& in, const icp_outgoing_patch& patch, const icp_query_hit& hit,
+                               F3 dir, const Frame& target, Contribution& out)
+{
+    if (!in.vertices || (hit.flags & ~(1u | 2u | 4u)) != 0u || hit.patch_id != patch.patch_id || hit.root_index > 1u ||
+        !(hit.u >= 0.0f && hit.u <= 1.0f && hit.v >= 0.0f && hit.v <= 1.0f) || !(hit.t > 0.0f && finite32(hit.t)) ||
+        !(hit.residual >= 0.0f && finite32(hit.residual)))
+        return kInput;
+    uint32_t pending = 0;
+    if (patch.status == 3u)
+        pending |= kRefine; // no folded-branch records
+    else if (patch.status != 1u && patch.status != 2u)
+        return kInput;
+    if (hit.flags & 1u) pending |= kBoundary;
+    if (hit.flags & 2u) pending |= kSingular;
+    if (pending) return pending;
+    const double area = double(patch.incident_area_drop2), omega = fabs(double(patch.signed_solid_angle_sr));
+    if (!(area > 0.0 && finite64(area) && omega > 0.0 && finite64(omega))) return kInput;
+    const unsigned columns = in.second_input_fields ? 2u : 1u;
+    const double weight = in.second_input_fields ? 0.5 : 1.0;
+    icp_field32 moved[2][4];
+    icp_phase_cycles paths[4];
+    for (unsigned k = 0; k < 4; ++k) {
+        const uint32_t idx = patch.vertex_indices[k];
+        if (idx >= in.vertex_count) return kInput;
+        const icp_outgoing_vertex& vx = in.vertices[idx];
+        const F3 dirv = f3(vx.direction_drop), basis = f3(vx.basis_x);
+        if (vx.status != 1u || !finite(f3(vx.position_drop)) || !finite(dirv) || !finite(basis) || !finite(vx.field))
+            return kInput;
+        if (!cycles_ok(vx.optical_cycles)) return kPhase;
+        const F3 second = cross(dirv, basis);
+        const D3 s2 = wide(second);
+        const double len2 = dot(s2, s2);
+        if (!(len2 > 0.0 && finite64(len2))) return kFrame;
+        const Frame source{basis, unit(second)};
+        icp_field32 src[2] = {vx.field, vx.field};
+        if (in.second_input_fields) {
+            src[1] = in.second_input_fields[idx];
+            if (!finite(src[0]) || !finite(src[1])) return kInput;
+        }
+        icp_field32 got[2];
+        if (!transport(dirv, source, src, columns, dir, target, got)) return kFrame;
+        moved[0][k] = got[0];
+        moved[1][k] = columns == 2 ? got[1] : got[0];
+        paths[k] = vx.optical_cycles;
+    }
+    icp_phase_cycles path;
+    if (!cycles_bilinear(paths, hit.u, hit.v, path)) return kPhase;
+    float pre, pim;
+    if (!unit_phasor(path, pre, pim)) return kPhase;
+    const double amplitude = sqrt(area / omega);
+    const double c = pre, s = pim, u = hit.u, v = hit.v;
+    Contribution cand{};
+    for (unsigned j = 0; j < columns; ++j) {
+        const icp_field32* f = moved[j];
+        const double sr = amplitude * lerp2(f[0].x.real, f[1].x.real, f[2].x.real, f[3].x.real, u, v);
+        const double si = amplitude * lerp2(f[0].x.imag, f[1].x.imag, f[2].x.imag, f[3].x.imag, u, v);
+        const double pr = amplitude * lerp2(f[0].y.real, f[1].y.real, f[2].y.real, f[3].y.real, u, v);
+        const double pi = amplitude * lerp2(f[0].y.imag, f[1].y.imag, f[2].y.imag, f[3].y.imag, u, v);
+        cand.inc_s += weight * fma(sr, sr, si * si);
+        cand.inc_p += weight * fma(pr, pr, pi * pi);
+        cand.field[j] = {fma(sr, c, -si * s), fma(sr, s, si * c), fma(pr, c, -pi * s), fma(pr, s, pi * c)};
+    }
+    if (!finite64(cand.inc_s) || !finite64(cand.inc_p) || !finite(cand.field[0]) || !finite(cand.field[1]))
+        return kArith;
+    out = cand;
+    return 0;
+}
+
+__device__ __forceinline__ void unavailable(icp_optical_result& r)
+{
+    r.path_field = {nan64(), nan64(), nan64(), nan64()};
+    r.path_field_second = r.path_field;
+    r.incoherent_s = r.incoherent_p = r.path_s = r.path_p = nan64();
+}
+__device__ __forceinline__ void unavailable(icp_focal_sample& r)
+{
+    for (unsigned k = 0; k < 4; ++k) r.field[k] = r.field_second[k] = nan64();
+    r.intensity_s = r.intensity_p = nan64();
+}
+__device__ __forceinline__ bool hit_before(const icp_query_hit& a, const icp_query_hit& b)
+{
+    if (a.patch_id != b.patch_id) return a.patch_id < b.patch_id;
+    if (a.compact_index != b.compact_index) return a.compact_index < b.compact_index;
+    return a.root_index < b.root_index;
+}
+
+__device__ void direction_optics(const icp_optics_input& in, uint32_t index, const icp_focal_config* fc,
+                                 icp_optical_result& res, icp_focal_sample* focal_out)
+{
+    res = icp_optical_result{};
+    res.first_problem_patch_id = 0xffffffffu;
+    const bool dual = in.input_polarization == 1u;
+    const unsigned columns = dual ? 2u : 1u;
+    const double weight = dual ? 0.5 : 1.0;
+    if (focal_out) {
+        *focal_out = icp_focal_sample{};
+        focal_out->first_problem_patch_id = 0xffffffffu;
+        focal_out->flags = kFocalInputError;
+        unavailable(*focal_out);
+    }
+    if ((in.input_polarization != 0u && !dual) ||
+        (dual && (!in.second_input_fields || in.second_input_count != in.vertex_count)) ||
+        (!dual && (in.second_input_fields || in.second_input_count != 0u)) || index >= in.direction_count ||
+        !in.directions || !in.offsets || !in.summaries) {
+        res.flags = kInput;
+        unavailable(res);
+        return;
+    }
+    const icp_query_summary sm = in.summaries[index];
+    res.hit_count = sm.hit_count;
+    res.query_flags = sm.flags;
+    if (sm.flags & kQueryErrors) {
+        res.flags = kQuery;
+        res.first_problem_patch_id = sm.first_problem_patch_id;
+        res.rejected_hits = sm.hit_count;
+        unavailable(res);
+        return;
+    }
+    const uint64_t begin = in.offsets[index], end = in.offsets[index + 1u];
+    if (begin > end || end > in.hit_storage_count || uint64_t(sm.hit_count) > end - begin ||
+        uint64_t(sm.candidate_count) != end - begin || (sm.hit_count != 0u && (!in.hits || !in.patches || !in.vertices))) {
+        res.flags = kInput;
+        res.rejected_hits = sm.hit_count;
+        unavailable(res);
+        return;
+    }
+    if (sm.flags & kQueryRefineHit) res.flags |= kRefine;
+    if (sm.flags & kQueryBoundaryHit) res.flags |= kBoundary;
+    if (sm.flags & kQuerySingularHit) res.flags |= kSingular;
+    const F3 dir = f3(in.directions[index]);
+    Frame target;
+    if (!scattering_frame(f3(in.incident_direction), f3(in.incident_basis_x), dir, target)) {
+        res.flags |= kFrame;
+        res.rejected_hits = sm.hit_count;
+        unavailable(res);
+        return;
+    }
+    FieldSum path[2], turned[2];
+    Compensated inc_s, inc_p, envelope[4];
+    const bool with_focal = fc && focal_out;
+    icp_focal_sample focal{};
+    focal.first_problem_patch_id = 0xffffffffu;
+    if (with_focal && !focal_layout_ok(*fc)) focal.flags |= kFocalGeometry;
+    for (uint32_t i = 0; i < sm.hit_count; ++i) {
+        const icp_query_hit hit = in.hits[begin + i];
+        uint32_t flags;
+        Contribution ct{};
+        if (i != 0u && !hit_before(in.hits[begin + i - 1u], hit))
+            flags = kInput; // the query sorts its hits and removes duplicates
+        else if (hit.compact_index >= in.patch_count)
+            flags = kInput;
+        else
+            flags = hit_optics(in, in.patches[hit.compact_index], hit, dir, target, ct);
+        if (flags) {
+            res.flags |= flags;
+            ++res.rejected_hits;
+            res.refinement_hits += (flags & kRefine) != 0u;
+            res.boundary_hits += (flags & kBoundary) != 0u;
+            res.singular_hits += (flags & kSingular) != 0u;
+            if (hit.patch_id < res.first_problem_patch_id) res.first_problem_patch_id = hit.patch_id;
+            continue;
+        }
+        ++res.evaluated_hits;
+        for (unsigned j = 0; j < columns; ++j) path[j].add(ct.field[j]);
+        inc_s.add(ct.inc_s);
+        inc_p.add(ct.inc_p);
+        if (with_focal) {
+            uint32_t family = 0, extra = 0, turns = 0;
+            const uint32_t code = focal_estimate(in.vertices, in.vertex_count, in.patches[hit.compact_index],
+                                                 f3(in.incident_direction), *fc, family, extra, turns);
+            if (code) {
+                focal.flags |= code;
+                if (hit.patch_id < focal.first_problem_patch_id) focal.first_problem_patch_id = hit.patch_id;
+            } else {
+                for (unsigned j = 0; j < columns; ++j) turned[j].add(quarter_turns(ct.field[j], turns));
+                envelope[family].add(ct.inc_s + ct.inc_p);
+                ++focal.family_hits[family];
+                ++focal.corrected_hits;
+                focal.extra_quarter_turn_hits += extra;
+            }
+        }
+    }
+    res.path_field = path[0].value();
+    res.path_field_second = path[1].value();
+    res.incoherent_s = inc_s.value();
+    res.incoherent_p = inc_p.value();
+    for (unsigned j = 0; j < columns; ++j) {
+        const icp_field64 f = path[j].value();
+        res.path_s += weight * fma(f.s_real, f.s_real, f.s_imag * f.s_imag);
+        res.path_p += weight * fma(f.p_real, f.p_real, f.p_imag * f.p_imag);
+    }
+    if (!finite(res.path_field) || !finite(res.path_field_second) || !finite64(res.incoherent_s) ||
+        !finite64(res.incoherent_p) || !finite64(res.path_s) || !finite64(res.path_p))
+        res.flags |= kArith;
+    if (res.flags & kErrors) unavailable(res);
+    if (with_focal) {
+        if (res.flags & kErrors) focal.flags |= kFocalInputError;
+        if (res.flags & kPending) focal.flags |= kFocalInputPending;
+        if (res.first_problem_patch_id < focal.first_problem_patch_id)
+            focal.first_problem_patch_id = res.first_problem_patch_id;
+        const icp_field64 g0 = turned[0].value(), g1 = turned[1].value();
+        focal.field[0] = g0.s_real, focal.field[1] = g0.s_imag, focal.field[2] = g0.p_real, focal.field[3] = g0.p_imag;
+        focal.field_second[0] = g1.s_real, focal.field_second[1] = g1.s_imag;
+        focal.field_second[2] = g1.p_real, focal.field_second[3] = g1.p_imag;
+        for (unsigned j = 0; j < columns; ++j) {
+            const icp_field64& f = j == 0 ? g0 : g1;
+            focal.intensity_s += weight * fma(f.s_real, f.s_real, f.s_imag * f.s_imag);
+            focal.intensity_p += weight * fma(f.p_real, f.p_real, f.p_imag * f.p_imag);
+        }
+        for (unsigned k = 0; k < 4; ++k) focal.family_incoherent[k] = envelope[k].value();
+        if (!finite(g0) || !finite(g1) || !finite64(focal.intensity_s + focal.intensity_p)) focal.flags |= kFocalArith;
+        if (focal.flags) unavailable(focal);
+        *focal_out = focal;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) patch_optics_kernel(const icp_optics_input in, const icp_focal_config fc,
+                                                                int with_focal, icp_optical_result* __restrict__ results,
+                                                                icp_focal_sample* __restrict__ focal)
+{
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < in.direction_count; i += stride) {
+        icp_optical_result r;
+        if (with_focal) {
+            icp_focal_sample f;
+            direction_optics(in, i, &fc, r, &f);
+            focal[i] = f;
+        } else
+            direction_optics(in, i, nullptr, r, nullptr);
+        results[i] = r;
+    }
+}
+
+} // namespace
+
+extern "C" int icp_patch_optics(icp_context* ctx, const icp_optics_input* input, icp_optical_result* d_results,
+                                const icp_focal_config* focal, icp_focal_sample* d_focal)
+{
+    if (!ctx || !input || !d_results || (focal && !d_focal))
+        return fail(ICP_ERR_INVALID_ARGUMENT, "icp_patch_optics: null argument");
+    if (input->direction_count == 0) return ok();
+    if (input->direction_count > 0x7fffffffu) return fail(ICP_ERR_INVALID_ARGUMENT, "icp_patch_optics: too many directions");
+    ICP_CUDA(cudaSetDevice(ctx->device));
+    const uint64_t need = (uint64_t(input->direction_count) + kThreads - 1) / kThreads;
+    const uint64_t cap = uint64_t(ctx->sms > 0 ? ctx->sms : 148) * 16u;
+    const unsigned blocks = unsigned(need < cap ? need : cap);
+    const icp_focal_config fc = focal ? *focal : icp_focal_config{};
+    patch_optics_kernel<<<blocks, kThreads, 0, ctx->stream>>>(*input, fc, focal ? 1 : 0, d_results, d_focal);
+    ICP_CUDA(cudaGetLastError());
+    count_launch();
+    ICP_CUDA(cudaStreamSynchronize(ctx->stream));
+    return ok();
+}

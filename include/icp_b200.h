@@ -20,6 +20,7 @@
  *   icp_drop_trace_bin    RaindropTracer::trace_unpolarized + patch/query/optics stages
  *                                                         include/rainbow/raindrop_tracer.hpp, apps/generate_phase.cpp:431-439
  *   icp_drop_generate     rainbow_generate's record path   apps/generate_phase.cpp:395-453
+ *   icp_patch_optics      evaluate_patch_optics / evaluate_focal_optics  device/patch_optics.cu:7-24
  *   icp_rainbow_*         RainbowDiffraction + PatchOptics::run_diffraction
  *                                                         include/rainbow/rainbow_diffraction.hpp,
  *                                                         src/patch_optics.cpp:334-348
@@ -640,6 +641,84 @@ int icp_rainbow_filter(icp_context* ctx, const icp_focal_sample* d_focal, const 
 int icp_rainbow_diffraction(icp_context* ctx, const icp_focal_sample* d_focal, uint32_t nt, uint32_t np,
                             const icp_diffraction_config* config, uint32_t* d_transitions,
                             icp_diffraction_result* d_results, double* d_density, icp_diffraction_stats* stats);
+
+/* ----------------------------------------- patch optics (incoherent, path, focal stages) */
+/* Per-direction optics of the drop's wave stages from the outgoing-ray lattice, its patches
+ * and the query hits: the reference's PatchOpticalEvaluator
+ * (include/rainbow/patch_optical_evaluator.hpp) as launched by evaluate_patch_optics /
+ * evaluate_focal_optics (device/patch_optics.cu:7-24; src/patch_optics.cpp:150-175).  The
+ * records below have the reference's layouts (raindrop_trace_data.hpp, outgoing_patch.hpp,
+ * patch_query_data.hpp, patch_optics_data.hpp), so its device buffers pass unchanged.
+ * Folded-branch records are not taken: a hit on a NeedsRefinement patch is reported as
+ * refinement-pending, as the reference does without its folded view. */
+typedef struct { float x, y, z; } icp_vec3f;
+typedef struct { float real, imag; } icp_complex32;
+typedef struct { icp_complex32 x, y; } icp_field32;          /* Jones vector in a transverse frame */
+typedef struct { int32_t turns; float fraction; } icp_phase_cycles; /* optical path in cycles  */
+
+typedef struct {                                             /* rainbow::OutgoingVertex, 68 B     */
+    icp_vec3f position_drop, direction_drop, basis_x;
+    icp_field32 field;
+    icp_phase_cycles optical_cycles;
+    uint32_t status;                                         /* 1 = valid                         */
+    uint32_t diagnostics;
+} icp_outgoing_vertex;
+
+typedef struct {                                             /* rainbow::OutgoingPatch, 32 B      */
+    uint32_t vertex_indices[4];
+    uint32_t patch_id;                                       /* family x cells + iy (W-1) + ix    */
+    uint32_t status;                                         /* 1 / 2 regular, 3 needs refinement */
+    float signed_solid_angle_sr, incident_area_drop2;
+} icp_outgoing_patch;
+
+typedef struct {                                             /* rainbow::PatchQueryHit, 32 B      */
+    uint32_t compact_index, patch_id, root_index, flags;     /* flags: 1 boundary, 2 singular, 4 fp64 */
+    float u, v, t, residual;
+} icp_query_hit;
+
+typedef struct {                                             /* rainbow::PatchQuerySummary, 32 B  */
+    uint32_t candidate_count, hit_count, regular_hits, refinement_hits, boundary_hits, flags;
+    uint32_t first_problem_patch_id, reserved;
+} icp_query_summary;
+
+typedef struct { double s_real, s_imag, p_real, p_imag; } icp_field64;
+
+typedef struct {                                             /* rainbow::PatchOpticalResult, 136 B */
+    icp_field64 path_field;                                  /* input column 0                    */
+    double incoherent_s, incoherent_p, path_s, path_p;
+    uint32_t hit_count, evaluated_hits, rejected_hits, refinement_hits, boundary_hits, singular_hits;
+    uint32_t flags, query_flags, first_problem_patch_id, folded_hits;
+    icp_field64 path_field_second;                           /* input column 1 (unpolarized)      */
+} icp_optical_result;
+
+typedef struct {                                             /* rainbow::PatchOpticsParams        */
+    const icp_outgoing_vertex* vertices;                     /* device arrays                     */
+    const icp_outgoing_patch* patches;
+    const icp_vec3f* directions;                             /* direction_count query directions  */
+    const uint64_t* offsets;                                 /* direction_count + 1 hit offsets   */
+    const icp_query_summary* summaries;
+    const icp_query_hit* hits;
+    const icp_field32* second_input_fields;                  /* vertex_count, or NULL             */
+    uint64_t hit_storage_count;
+    uint32_t vertex_count, patch_count, direction_count, second_input_count;
+    icp_vec3f incident_direction, incident_basis_x;
+    uint32_t input_polarization;                             /* 0 single Jones, 1 unpolarized     */
+    uint32_t reserved;
+} icp_optics_input;
+
+typedef struct {                                             /* rainbow::FocalPhaseConfig, 32 B   */
+    uint32_t grid_width, grid_height;
+    float grid_half_extent;
+    uint32_t reserved;
+    uint32_t quarter_turn_offsets[4];                        /* per family, 0 .. 3                */
+} icp_focal_config;
+
+/* Optics of every query direction: d_results[direction_count] (device).  With focal != NULL
+ * also the focal stage d_focal[direction_count] (device; the input of icp_rainbow_diffraction).
+ * Malformed inputs are reported per direction in the result flags, as the reference does;
+ * only null pointers and sizes that overflow are rejected here. */
+int icp_patch_optics(icp_context* ctx, const icp_optics_input* input, icp_optical_result* d_results,
+                     const icp_focal_config* focal, icp_focal_sample* d_focal);
 
 #ifdef __cplusplus
 }

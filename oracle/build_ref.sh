@@ -14,6 +14,8 @@
 #   oracle/_ref/ice_precompute_atlas_cpu reference CLI (hex_atlas/apps/precompute_atlas.cpp), CPU build
 #   oracle/_ref/ref_rainbow_harness      oracle/ref_rainbow_harness.cpp over the header-only Table-II
 #                                        diffraction (include/rainbow/rainbow_diffraction.hpp)
+#   oracle/_ref/ref_optics_harness       oracle/ref_optics_harness.cpp over the header-only patch optics
+#                                        (include/rainbow/patch_optical_evaluator.hpp)
 #
 # Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
 set -euo pipefail
@@ -36,6 +38,8 @@ g++ -std=c++20 -O2 -fno-fast-math -ffp-contract=off -I"$ref/include" "$here/ref_
     "$ref/src/projected_area.cpp" "$ref/src/water_refractive_index.cpp" -o "$out/ref_drop_harness"
 g++ -std=c++20 -O2 -fno-fast-math -ffp-contract=off -I"$ref/include" "$here/ref_rainbow_harness.cpp" \
     -o "$out/ref_rainbow_harness"
+g++ -std=c++20 -O2 -fno-fast-math -ffp-contract=off -I"$ref/include" "$here/ref_optics_harness.cpp" \
+    -o "$out/ref_optics_harness"
 if [ -f "$ref/hex_atlas/src/ice_optics.cpp" ]; then
     g++ -std=c++20 -O2 -fno-fast-math -ffp-contract=off -I"$ref/hex_atlas/include" "$here/ref_ice_harness.cpp" \
         "$ref/hex_atlas/src/ice_optics.cpp" -o "$out/ref_ice_harness"
@@ -45,4 +49,4 @@ if [ -f "$ref/hex_atlas/src/ice_optics.cpp" ]; then
         "$ref/hex_atlas/src/atlas.cpp" "$ref/hex_atlas/src/ice_optics.cpp" "$ref/hex_trace/src/hex_trace.cpp" \
         "$ref/src/npy_writer.cpp" -o "$out/ice_precompute_atlas_cpu"
 fi
-echo "built $out/ice_generate_phase_cpu $out/ref_hex_harness $out/ref_drop_harness $out/ref_ice_harness $out/ref_atlas_harness $out/ice_precompute_atlas_cpu $out/ref_rainbow_harness"
+echo "built $out/ice_generate_phase_cpu $out/ref_hex_harness $out/ref_drop_harness $out/ref_ice_harness $out/ref_atlas_harness $out/ice_precompute_atlas_cpu $out/ref_rainbow_harness $out/ref_optics_harness"

@@ -1868,3 +1868,575 @@ void icpo_rainbow_filter_at(const rb_focal* f, const uint32_t* edges, uint32_t n
     for (uint64_t k = 0; k < count; ++k)
         out[k] = rb_filter_one(f, edges, (int)nt, (int)np, cfg, ok, (uint32_t)index[k]);
 }
+
+/* ------------------------------------------------------------- patch optics
+ * Restates the reference's per-direction optics of the drop's wave stages:
+ *   PatchOpticalEvaluator::evaluate_patch / evaluate_direction
+ *                          include/rainbow/patch_optical_evaluator.hpp:26-326 (no folded view)
+ *   scattering frame, minimum-rotation transport
+ *                          include/rainbow/polarization_transport.hpp:24-229
+ *   optical-path cycles    include/rainbow/phase_cycles.hpp:20-97, phase_interpolation.hpp:22-151
+ *   focal quarter turns    include/rainbow/focal_phase.hpp:18-104
+ *   float vectors          include/rainbow/vec3.hpp:11-66 (explicit fmaf dots, plain crosses)
+ * Binary32 and binary64 as the reference writes them, no contraction, same libm calls, so the
+ * results equal the reference's headers compiled on the same host bit for bit.  Record layouts
+ * are the reference's (OutgoingVertex 68 B, OutgoingPatch / PatchQueryHit / PatchQuerySummary
+ * 32 B, PatchOpticalResult 136 B, FocalOpticalResult 144 B). */
+typedef struct { float x, y, z; } pf3;
+typedef struct { double x, y, z; } pd3;
+typedef struct { float re, im; } pc32;
+typedef struct { pc32 x, y; } pfield;
+typedef struct { int32_t turns; float fraction; } pcycles;
+typedef struct {
+    pf3 position, direction, basis;
+    pfield field;
+    pcycles cycles;
+    uint32_t status, diagnostics;
+} pvertex;
+typedef struct {
+    uint32_t v[4];
+    uint32_t patch_id, status;
+    float solid_angle, area;
+} ppatch;
+typedef struct {
+    uint32_t compact, patch_id, root, flags;
+    float u, v, t, residual;
+} phit;
+typedef struct {
+    uint32_t candidates, hits, regular, refinement, boundary, flags, first_problem, reserved;
+} psummary;
+typedef struct { double sr, si, pr, pi; } pf64;
+typedef struct {
+    pf64 path;
+    double inc_s, inc_p, path_s, path_p;
+    uint32_t hits, evaluated, rejected, refinement, boundary, singular, flags, query_flags, first_problem, folded;
+    pf64 path2;
+} poptical;
+typedef struct { pf3 e0, e1; } pframe;
+typedef struct {
+    const pvertex* vertices;
+    const ppatch* patches;
+    const pf3* directions;
+    const uint64_t* offsets;
+    const psummary* summaries;
+    const phit* hits;
+    const pfield* second;
+    uint64_t hit_storage;
+    uint32_t vertex_count, patch_count, direction_count, second_count;
+    pf3 incident, incident_basis;
+    uint32_t polarization, reserved;
+} pinput;
+typedef struct {
+    uint32_t width, height;
+    float half_extent;
+    uint32_t reserved;
+    uint32_t offsets[4];
+} pfocal_cfg;
+
+enum { PO_QUERY = 1, PO_INPUT = 2, PO_FRAME = 4, PO_PHASE = 8, PO_ARITH = 16, PO_REFINE = 32, PO_BOUNDARY = 64,
+       PO_SINGULAR = 128 };
+#define PO_ERRORS (PO_QUERY | PO_INPUT | PO_FRAME | PO_PHASE | PO_ARITH)
+#define PO_PENDING (PO_REFINE | PO_BOUNDARY | PO_SINGULAR)
+enum { PQ_REFINE_HIT = 8, PQ_BOUNDARY_HIT = 16, PQ_SINGULAR_HIT = 128 };
+#define PQ_ERRORS (1u | 2u | 4u | 256u)
+enum { FO_INPUT_ERROR = 1, FO_INPUT_PENDING = 2, FO_DERIVATIVE = 4, FO_GEOMETRY = 8, FO_ARITH = 16 };
+#define PT_TOL 0x1p-10f   /* unit / orthogonality tolerance of frames */
+#define PT_DEGEN 0x1p-30f /* degenerate cross product                 */
+
+static float f3_dot(pf3 a, pf3 b) { return fmaf(a.x, b.x, fmaf(a.y, b.y, a.z * b.z)); }
+static pf3 f3_cross(pf3 a, pf3 b)
+{
+    pf3 r = {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+    return r;
+}
+static pf3 f3_scale(pf3 a, float s) { pf3 r = {a.x * s, a.y * s, a.z * s}; return r; }
+static pf3 f3_div(pf3 a, float s) { pf3 r = {a.x / s, a.y / s, a.z / s}; return r; }
+static pf3 f3_sub(pf3 a, pf3 b) { pf3 r = {a.x - b.x, a.y - b.y, a.z - b.z}; return r; }
+static int f3_fin(pf3 a)
+{
+    const float m = 0x1.fffffep127f;
+    return a.x >= -m && a.x <= m && a.y >= -m && a.y <= m && a.z >= -m && a.z <= m;
+}
+static pf3 f3_unit(pf3 a) { return f3_div(a, sqrtf(f3_dot(a, a))); }
+static pd3 f3_wide(pf3 a) { pd3 r = {a.x, a.y, a.z}; return r; }
+static double d3_dot(pd3 a, pd3 b) { return fma(a.x, b.x, fma(a.y, b.y, a.z * b.z)); }
+static pd3 d3_cross(pd3 a, pd3 b)
+{
+    pd3 r = {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+    return r;
+}
+static pd3 d3_scale(pd3 a, double s) { pd3 r = {a.x * s, a.y * s, a.z * s}; return r; }
+static pd3 d3_div(pd3 a, double s) { pd3 r = {a.x / s, a.y / s, a.z / s}; return r; }
+static pd3 d3_add(pd3 a, pd3 b) { pd3 r = {a.x + b.x, a.y + b.y, a.z + b.z}; return r; }
+static pd3 d3_unit(pd3 a) { return d3_div(a, sqrt(d3_dot(a, a))); }
+
+static int pt_unit(pf3 a) { return f3_fin(a) && fabsf(f3_dot(a, a) - 1.0f) <= PT_TOL; }
+static int pt_frame(pf3 d, pframe f)
+{
+    if (!pt_unit(f.e0) || !pt_unit(f.e1)) return 0;
+    if (fabsf(f3_dot(d, f.e0)) > PT_TOL || fabsf(f3_dot(d, f.e1)) > PT_TOL || fabsf(f3_dot(f.e0, f.e1)) > PT_TOL)
+        return 0;
+    return f3_dot(f3_cross(f.e0, f.e1), d) >= 1.0f - 4.0f * PT_TOL;
+}
+/* e0 normal to the scattering plane (or the incident basis carried over at exact forward /
+ * backward scattering), e1 = out x e0. */
+static int pt_scattering_frame(pf3 inc, pf3 basis, pf3 out, pframe* frame)
+{
+    if (!pt_unit(inc) || !pt_unit(out) || !pt_unit(basis) || fabsf(f3_dot(inc, basis)) > PT_TOL) return 0;
+    pf3 e0 = f3_cross(inc, out);
+    float n2 = f3_dot(e0, e0);
+    if (n2 > PT_DEGEN)
+        e0 = f3_div(e0, sqrtf(n2));
+    else {
+        e0 = f3_sub(basis, f3_scale(out, f3_dot(out, basis)));
+        n2 = f3_dot(e0, e0);
+        if (!(n2 > PT_DEGEN)) return 0;
+        e0 = f3_div(e0, sqrtf(n2));
+    }
+    pf3 e1 = f3_cross(out, e0);
+    const float m2 = f3_dot(e1, e1);
+    if (!(m2 > PT_DEGEN)) return 0;
+    e1 = f3_div(e1, sqrtf(m2));
+    const pframe f = {e0, e1};
+    if (!pt_frame(out, f)) return 0;
+    *frame = f;
+    return 1;
+}
+/* Rodrigues' rotation by the minimum rotation taking a to b (v = a x b, c = a.b). */
+static pd3 pt_rotate(pd3 x, pd3 a, pd3 b, double c)
+{
+    const pd3 v = d3_cross(a, b), vx = d3_cross(v, x);
+    return d3_add(d3_add(x, vx), d3_div(d3_cross(v, vx), 1.0 + c));
+}
+static int pt_fits(double x) { return x >= -0x1.fffffep127 && x <= 0x1.fffffep127; }
+static int pfield_fin(pfield f)
+{
+    return fin(f.x.re) && fin(f.x.im) && fin(f.y.re) && fin(f.y.im);
+}
+static int pfield_fin32(pfield f)
+{
+    const float m = 0x1.fffffep127f;
+    return f.x.re >= -m && f.x.re <= m && f.x.im >= -m && f.x.im <= m && f.y.re >= -m && f.y.re <= m &&
+           f.y.im >= -m && f.y.im <= m;
+}
+/* One Jones column carried from the source frame to the target frame (the shared geometry
+ * is set up by the caller). */
+static int pt_carry(pfield f, pd3 se0, pd3 se1, pd3 sw, pd3 tw, double c, pd3 te0, pd3 te1, pfield* out)
+{
+    const pd3 re = d3_add(d3_scale(se0, (double)f.x.re), d3_scale(se1, (double)f.y.re));
+    const pd3 im = d3_add(d3_scale(se0, (double)f.x.im), d3_scale(se1, (double)f.y.im));
+    const pd3 rt = pt_rotate(re, sw, tw, c), it = pt_rotate(im, sw, tw, c);
+    const double xr = d3_dot(rt, te0), xi = d3_dot(it, te0), yr = d3_dot(rt, te1), yi = d3_dot(it, te1);
+    if (!pt_fits(xr) || !pt_fits(xi) || !pt_fits(yr) || !pt_fits(yi)) return 0;
+    out->x.re = (float)xr;
+    out->x.im = (float)xi;
+    out->y.re = (float)yr;
+    out->y.im = (float)yi;
+    return 1;
+}
+/* try_transport (columns = 1) and try_transport_response (columns = 2). */
+static int pt_transport(pf3 sdir, pframe sf, const pfield* src, unsigned columns, pf3 tdir, pframe tf, pfield* out)
+{
+    if (columns == 2 && (!pfield_fin32(src[0]) || !pfield_fin32(src[1]))) return 0;
+    if (!pt_unit(sdir) || !pt_unit(tdir) || !pt_frame(sdir, sf) || !pt_frame(tdir, tf)) return 0;
+    const pd3 sw = d3_unit(f3_wide(sdir)), tw = d3_unit(f3_wide(tdir));
+    const double c = d3_dot(sw, tw);
+    if (!(1.0 + c > 0x1p-30)) return 0;
+    const pd3 se0 = f3_wide(sf.e0), se1 = f3_wide(sf.e1), te0 = f3_wide(tf.e0), te1 = f3_wide(tf.e1);
+    pfield tmp[2];
+    for (unsigned j = 0; j < columns; ++j)
+        if (!pt_carry(src[j], se0, se1, sw, tw, c, te0, te1, &tmp[j])) return 0;
+    for (unsigned j = 0; j < columns; ++j) out[j] = tmp[j];
+    return 1;
+}
+
+static int cyc_ok(pcycles q) { return q.fraction >= 0.0f && q.fraction < 1.0f; }
+static double cyc_diff(pcycles a, pcycles b)
+{
+    const int64_t whole = (int64_t)a.turns - (int64_t)b.turns;
+    return (double)whole + ((double)a.fraction - (double)b.fraction);
+}
+/* anchor + delta cycles, fraction carried into [0, 1) (phase_interpolation.hpp:96-151) */
+static int cyc_add(pcycles anchor, double delta, pcycles* out)
+{
+    if (!(delta > -0x1p33 && delta < 0x1p33)) return 0;
+    const double whole = floor(delta);
+    double frac = (double)anchor.fraction + (delta - whole);
+    int64_t turns = (int64_t)anchor.turns + (int64_t)whole;
+    if (frac < 0.0) {
+        --turns;
+        frac += 1.0;
+    }
+    if (frac >= 1.0) {
+        ++turns;
+        frac -= 1.0;
+    }
+    if (turns < -2147483647LL - 1 || turns > 2147483647LL) return 0;
+    float stored = (float)frac;
+    if (stored >= 1.0f) {
+        ++turns;
+        stored = 0.0f;
+        if (turns > 2147483647LL) return 0;
+    } else if (stored < 0.0f) {
+        --turns;
+        stored += 1.0f;
+        if (turns < -2147483647LL - 1) return 0;
+    }
+    out->turns = (int32_t)turns;
+    out->fraction = stored == 0.0f ? 0.0f : stored;
+    return cyc_ok(*out);
+}
+/* bilinear optical path from the four corners, anchored at q00 (corners returned exactly) */
+static int cyc_bilinear(pcycles q00, pcycles q10, pcycles q01, pcycles q11, float u, float v, pcycles* out)
+{
+    if (!cyc_ok(q00) || !cyc_ok(q10) || !cyc_ok(q01) || !cyc_ok(q11) || !(u >= 0.0f && u <= 1.0f) ||
+        !(v >= 0.0f && v <= 1.0f))
+        return 0;
+    if (u == 0.0f && v == 0.0f) { *out = q00; return 1; }
+    if (u == 1.0f && v == 0.0f) { *out = q10; return 1; }
+    if (u == 0.0f && v == 1.0f) { *out = q01; return 1; }
+    if (u == 1.0f && v == 1.0f) { *out = q11; return 1; }
+    const double du0 = cyc_diff(q10, q00), du1 = cyc_diff(q11, q01), dv0 = cyc_diff(q01, q00);
+    const double ud = (double)u, vd = (double)v;
+    const double row = fma(ud, du1 - du0, dv0);
+    return cyc_add(q00, fma(vd, row, ud * du0), out);
+}
+/* exp(+i 2 pi fraction) in binary32; exact quarter turns */
+static int cyc_phasor(pcycles q, pc32* out)
+{
+    if (!cyc_ok(q)) return 0;
+    const float f = q.fraction;
+    if (f == 0.0f) { out->re = 1.0f; out->im = 0.0f; return 1; }
+    if (f == 0.25f) { out->re = 0.0f; out->im = 1.0f; return 1; }
+    if (f == 0.5f) { out->re = -1.0f; out->im = 0.0f; return 1; }
+    if (f == 0.75f) { out->re = 0.0f; out->im = -1.0f; return 1; }
+    const float reduced = f > 0.5f ? f - 1.0f : f;
+    const float angle = 0x1.921fb6p+2f * reduced;
+    out->re = cosf(angle);
+    out->im = sinf(angle);
+    return 1;
+}
+
+static int focal_layout_ok(const pfocal_cfg* c)
+{
+    if (c->width < 2 || c->height < 2 || !(c->half_extent > 0) || !(c->half_extent <= 0x1.fffffep127f)) return 0;
+    if ((uint64_t)c->width * c->height > 0xffffffffull / 4u ||
+        (uint64_t)(c->width - 1u) * (c->height - 1u) > 0xffffffffull / 4u)
+        return 0;
+    for (unsigned j = 0; j < 4; ++j)
+        if (c->offsets[j] > 3) return 0;
+    return 1;
+}
+/* Sign of the radial derivative of the scattering angle at the cell centre, in emitting-plane
+ * coordinates (focal_phase.hpp:57-98, at_center): one extra quarter turn when it is positive. */
+static uint32_t focal_estimate(const pvertex* vertices, uint32_t vertex_count, const ppatch* patch, pf3 incident,
+                               const pfocal_cfg* c, uint32_t* family_out, uint32_t* extra_out, uint32_t* turns_out)
+{
+    if (!vertices || !focal_layout_ok(c) || !f3_fin(incident)) return FO_GEOMETRY;
+    const uint32_t n = c->width * c->height, nx = c->width - 1u, cells = nx * (c->height - 1u);
+    if (patch->patch_id >= 4u * cells || vertex_count < 4u * n) return FO_GEOMETRY;
+    const uint32_t family = patch->patch_id / cells, cell = patch->patch_id % cells;
+    const uint32_t ix = cell % nx, iy = cell / nx;
+    const uint32_t first = family * n + iy * c->width + ix;
+    const uint32_t expected[4] = {first, first + 1u, first + c->width, first + c->width + 1u};
+    const pd3 wi = f3_wide(incident);
+    if (!(d3_dot(wi, wi) > 0)) return FO_GEOMETRY;
+    double theta[4];
+    for (unsigned j = 0; j < 4; ++j) {
+        if (patch->v[j] != expected[j]) return FO_GEOMETRY;
+        const pvertex* a = vertices + expected[j];
+        if (a->status != 1u || !f3_fin(a->direction)) return FO_GEOMETRY;
+        const pd3 wo = f3_wide(a->direction);
+        if (!(d3_dot(wo, wo) > 0)) return FO_GEOMETRY;
+        const pd3 x = d3_cross(wi, wo);
+        theta[j] = atan2(sqrt(d3_dot(x, x)), d3_dot(wi, wo));
+        if (!fin(theta[j])) return FO_GEOMETRY;
+    }
+    const double e = (double)c->half_extent;
+    const double du = 2 * e / (double)(c->width - 1u), dv = 2 * e / (double)(c->height - 1u);
+    const double U = (2 * ((double)ix + 0.5) / (double)(c->width - 1u) - 1) * e;
+    const double V = (2 * ((double)iy + 0.5) / (double)(c->height - 1u) - 1) * e;
+    const double r2 = fma(U, U, V * V);
+    if (!(r2 > 0)) return FO_DERIVATIVE;
+    const double gu = ((theta[1] - theta[0]) + (theta[3] - theta[2])) / (2 * du);
+    const double gv = ((theta[2] - theta[0]) + (theta[3] - theta[1])) / (2 * dv);
+    const double num = fma(U, gu, V * gv);
+    const double guard = 0x1p-46 * (fabs(U * gu) + fabs(V * gv) + 1);
+    if (!fin(num) || !fin(r2)) return FO_GEOMETRY;
+    if (fabs(num) <= guard) return FO_DERIVATIVE;
+    if (!fin(num / (2 * r2))) return FO_GEOMETRY;
+    *family_out = family;
+    *extra_out = num > 0 ? 1u : 0u;
+    *turns_out = (c->offsets[family] + *extra_out) & 3u;
+    return 0;
+}
+static pf64 focal_turn(pf64 a, uint32_t q)
+{
+    pf64 r = a;
+    switch (q & 3u) {
+    case 1: r.sr = -a.si; r.si = a.sr; r.pr = -a.pi; r.pi = a.pr; break;
+    case 2: r.sr = -a.sr; r.si = -a.si; r.pr = -a.pr; r.pi = -a.pi; break;
+    case 3: r.sr = a.si; r.si = -a.sr; r.pr = a.pi; r.pi = -a.pr; break;
+    default: break;
+    }
+    return r;
+}
+
+typedef struct {
+    pf64 field[2];
+    double inc_s, inc_p;
+} pcontrib;
+static double lerp2(double a, double b, double c, double d, double u, double v)
+{
+    const double lower = fma(u, b - a, a), upper = fma(u, d - c, c);
+    return fma(v, upper - lower, lower);
+}
+static int pf64_fin(pf64 f) { return fin(f.sr) && fin(f.si) && fin(f.pr) && fin(f.pi); }
+
+static uint32_t optics_patch(const pinput* in, const ppatch* patch, const phit* hit, pf3 dir, pframe target,
+                             pcontrib* out)
+{
+    if (!in->vertices || (hit->flags & ~(1u | 2u | 4u)) != 0u || hit->patch_id != patch->patch_id || hit->root > 1u ||
+        !(hit->u >= 0.0f && hit->u <= 1.0f && hit->v >= 0.0f && hit->v <= 1.0f) || !(hit->t > 0.0f && fin(hit->t)) ||
+        !(hit->residual >= 0.0f && fin(hit->residual)))
+        return PO_INPUT;
+    uint32_t pending = 0;
+    if (patch->status == 3u)
+        pending |= PO_REFINE; /* no folded records */
+    else if (patch->status != 1u && patch->status != 2u)
+        return PO_INPUT;
+    if (hit->flags & 1u) pending |= PO_BOUNDARY;
+    if (hit->flags & 2u) pending |= PO_SINGULAR;
+    if (pending) return pending;
+    const double area = (double)patch->area, omega = fabs((double)patch->solid_angle);
+    if (!(area > 0.0 && fin(area) && omega > 0.0 && fin(omega))) return PO_INPUT;
+    const unsigned columns = in->second ? 2u : 1u;
+    const double weight = in->second ? 0.5 : 1.0;
+    pfield moved[2][4];
+    pcycles paths[4];
+    for (unsigned k = 0; k < 4; ++k) {
+        const uint32_t idx = patch->v[k];
+        if (idx >= in->vertex_count) return PO_INPUT;
+        const pvertex* vx = in->vertices + idx;
+        if (vx->status != 1u || !f3_fin(vx->position) || !f3_fin(vx->direction) || !f3_fin(vx->basis) ||
+            !pfield_fin(vx->field))
+            return PO_INPUT;
+        if (!cyc_ok(vx->cycles)) return PO_PHASE;
+        const pf3 second = f3_cross(vx->direction, vx->basis);
+        const pd3 s2 = f3_wide(second);
+        const double len2 = d3_dot(s2, s2);
+        if (!(len2 > 0.0 && fin(len2))) return PO_FRAME;
+        const pframe source = {vx->basis, f3_unit(second)};
+        pfield src[2] = {vx->field, vx->field};
+        pfield got[2];
+        if (in->second) {
+            src[1] = in->second[idx];
+            if (!pfield_fin32(src[0]) || !pfield_fin32(src[1])) return PO_INPUT;
+        }
+        if (!pt_transport(vx->direction, source, src, columns, dir, target, got)) return PO_FRAME;
+        moved[0][k] = got[0];
+        if (columns == 2) moved[1][k] = got[1];
+        paths[k] = vx->cycles;
+    }
+    pcycles path;
+    if (!cyc_bilinear(paths[0], paths[1], paths[2], paths[3], hit->u, hit->v, &path)) return PO_PHASE;
+    pc32 phasor;
+    if (!cyc_phasor(path, &phasor)) return PO_PHASE;
+    const double amplitude = sqrt(area / omega);
+    const double c = (double)phasor.re, s = (double)phasor.im;
+    pcontrib cand;
+    memset(&cand, 0, sizeof cand);
+    for (unsigned j = 0; j < columns; ++j) {
+        const pfield* f = moved[j];
+        const double u = hit->u, v = hit->v;
+        const double sr = amplitude * lerp2(f[0].x.re, f[1].x.re, f[2].x.re, f[3].x.re, u, v);
+        const double si = amplitude * lerp2(f[0].x.im, f[1].x.im, f[2].x.im, f[3].x.im, u, v);
+        const double pr = amplitude * lerp2(f[0].y.re, f[1].y.re, f[2].y.re, f[3].y.re, u, v);
+        const double pi = amplitude * lerp2(f[0].y.im, f[1].y.im, f[2].y.im, f[3].y.im, u, v);
+        cand.inc_s += weight * fma(sr, sr, si * si);
+        cand.inc_p += weight * fma(pr, pr, pi * pi);
+        cand.field[j].sr = fma(sr, c, -si * s);
+        cand.field[j].si = fma(sr, s, si * c);
+        cand.field[j].pr = fma(pr, c, -pi * s);
+        cand.field[j].pi = fma(pr, s, pi * c);
+    }
+    if (!fin(cand.inc_s) || !fin(cand.inc_p) || !pf64_fin(cand.field[0]) || !pf64_fin(cand.field[1]))
+        return PO_ARITH;
+    *out = cand;
+    return 0;
+}
+
+static void optical_nan(poptical* r)
+{
+    r->path.sr = r->path.si = r->path.pr = r->path.pi = NAN;
+    r->path2 = r->path;
+    r->inc_s = r->inc_p = r->path_s = r->path_p = NAN;
+}
+static void focal_nan(rb_focal* r)
+{
+    for (unsigned k = 0; k < 4; ++k) r->field[k] = r->field2[k] = NAN;
+    r->s = r->p = NAN;
+}
+static int hit_before(const phit* a, const phit* b)
+{
+    if (a->patch_id != b->patch_id) return a->patch_id < b->patch_id;
+    if (a->compact != b->compact) return a->compact < b->compact;
+    return a->root < b->root;
+}
+
+static poptical optics_direction(const pinput* in, uint32_t index, const pfocal_cfg* fc, rb_focal* focal_out)
+{
+    poptical res;
+    memset(&res, 0, sizeof res);
+    res.first_problem = 0xffffffffu;
+    const int dual = in->polarization == 1u;
+    const unsigned columns = dual ? 2u : 1u;
+    const double weight = dual ? 0.5 : 1.0;
+    if (focal_out) {
+        memset(focal_out, 0, sizeof *focal_out);
+        focal_out->first_problem = 0xffffffffu;
+        focal_out->flags = FO_INPUT_ERROR;
+        focal_nan(focal_out);
+    }
+    if ((in->polarization != 0u && !dual) || (dual && (!in->second || in->second_count != in->vertex_count)) ||
+        (!dual && (in->second || in->second_count != 0u)) || index >= in->direction_count || !in->directions ||
+        !in->offsets || !in->summaries) {
+        res.flags = PO_INPUT;
+        optical_nan(&res);
+        return res;
+    }
+    const psummary* sm = in->summaries + index;
+    res.hits = sm->hits;
+    res.query_flags = sm->flags;
+    if (sm->flags & PQ_ERRORS) {
+        res.flags = PO_QUERY;
+        res.first_problem = sm->first_problem;
+        res.rejected = sm->hits;
+        optical_nan(&res);
+        return res;
+    }
+    const uint64_t begin = in->offsets[index], end = in->offsets[index + 1u];
+    if (begin > end || end > in->hit_storage || (uint64_t)sm->hits > end - begin ||
+        (uint64_t)sm->candidates != end - begin || (sm->hits != 0u && (!in->hits || !in->patches || !in->vertices))) {
+        res.flags = PO_INPUT;
+        res.rejected = sm->hits;
+        optical_nan(&res);
+        return res;
+    }
+    if (sm->flags & PQ_REFINE_HIT) res.flags |= PO_REFINE;
+    if (sm->flags & PQ_BOUNDARY_HIT) res.flags |= PO_BOUNDARY;
+    if (sm->flags & PQ_SINGULAR_HIT) res.flags |= PO_SINGULAR;
+    pframe target;
+    if (!pt_scattering_frame(in->incident, in->incident_basis, in->directions[index], &target)) {
+        res.flags |= PO_FRAME;
+        res.rejected = sm->hits;
+        optical_nan(&res);
+        return res;
+    }
+    rb_sum sr[2], si[2], pr[2], pi[2], inc_s, inc_p, fsr[2], fsi[2], fpr[2], fpi[2], env[4];
+    memset(sr, 0, sizeof sr); memset(si, 0, sizeof si); memset(pr, 0, sizeof pr); memset(pi, 0, sizeof pi);
+    memset(fsr, 0, sizeof fsr); memset(fsi, 0, sizeof fsi); memset(fpr, 0, sizeof fpr); memset(fpi, 0, sizeof fpi);
+    memset(env, 0, sizeof env);
+    memset(&inc_s, 0, sizeof inc_s);
+    memset(&inc_p, 0, sizeof inc_p);
+    const int with_focal = fc && focal_out;
+    rb_focal focal;
+    memset(&focal, 0, sizeof focal);
+    focal.first_problem = 0xffffffffu;
+    if (with_focal && !focal_layout_ok(fc)) focal.flags |= FO_GEOMETRY;
+    for (uint32_t i = 0; i < sm->hits; ++i) {
+        const phit* hit = in->hits + begin + i;
+        uint32_t flags = 0;
+        pcontrib ct;
+        memset(&ct, 0, sizeof ct);
+        if (i != 0u && !hit_before(hit - 1, hit))
+            flags = PO_INPUT; /* the query sorts the hits and removes duplicates */
+        else if (hit->compact >= in->patch_count)
+            flags = PO_INPUT;
+        else
+            flags = optics_patch(in, in->patches + hit->compact, hit, in->directions[index], target, &ct);
+        if (flags) {
+            res.flags |= flags;
+            ++res.rejected;
+            res.refinement += (flags & PO_REFINE) != 0u;
+            res.boundary += (flags & PO_BOUNDARY) != 0u;
+            res.singular += (flags & PO_SINGULAR) != 0u;
+            if (hit->patch_id < res.first_problem) res.first_problem = hit->patch_id;
+            continue;
+        }
+        ++res.evaluated;
+        for (unsigned j = 0; j < columns; ++j) {
+            rb_add(&sr[j], ct.field[j].sr);
+            rb_add(&si[j], ct.field[j].si);
+            rb_add(&pr[j], ct.field[j].pr);
+            rb_add(&pi[j], ct.field[j].pi);
+        }
+        rb_add(&inc_s, ct.inc_s);
+        rb_add(&inc_p, ct.inc_p);
+        if (with_focal) {
+            uint32_t family = 0, extra = 0, turns = 0;
+            const uint32_t code = focal_estimate(in->vertices, in->vertex_count, in->patches + hit->compact,
+                                                 in->incident, fc, &family, &extra, &turns);
+            if (code) {
+                focal.flags |= code;
+                if (hit->patch_id < focal.first_problem) focal.first_problem = hit->patch_id;
+            } else {
+                for (unsigned j = 0; j < columns; ++j) {
+                    const pf64 f = focal_turn(ct.field[j], turns);
+                    rb_add(&fsr[j], f.sr);
+                    rb_add(&fsi[j], f.si);
+                    rb_add(&fpr[j], f.pr);
+                    rb_add(&fpi[j], f.pi);
+                }
+                rb_add(&env[family], ct.inc_s + ct.inc_p);
+                ++focal.fam_hits[family];
+                ++focal.corrected;
+                focal.extra += extra;
+            }
+        }
+    }
+    const pf64 f0 = {sr[0].s + sr[0].c, si[0].s + si[0].c, pr[0].s + pr[0].c, pi[0].s + pi[0].c};
+    const pf64 f1 = {sr[1].s + sr[1].c, si[1].s + si[1].c, pr[1].s + pr[1].c, pi[1].s + pi[1].c};
+    res.path = f0;
+    res.path2 = f1;
+    res.inc_s = inc_s.s + inc_s.c;
+    res.inc_p = inc_p.s + inc_p.c;
+    for (unsigned j = 0; j < columns; ++j) {
+        const pf64 f = j == 0 ? f0 : f1;
+        res.path_s += weight * fma(f.sr, f.sr, f.si * f.si);
+        res.path_p += weight * fma(f.pr, f.pr, f.pi * f.pi);
+    }
+    if (!pf64_fin(res.path) || !pf64_fin(res.path2) || !fin(res.inc_s) || !fin(res.inc_p) || !fin(res.path_s) ||
+        !fin(res.path_p))
+        res.flags |= PO_ARITH;
+    if (res.flags & PO_ERRORS) optical_nan(&res);
+    if (with_focal) {
+        if (res.flags & PO_ERRORS) focal.flags |= FO_INPUT_ERROR;
+        if (res.flags & PO_PENDING) focal.flags |= FO_INPUT_PENDING;
+        if (res.first_problem < focal.first_problem) focal.first_problem = res.first_problem;
+        const double g[2][4] = {{fsr[0].s + fsr[0].c, fsi[0].s + fsi[0].c, fpr[0].s + fpr[0].c, fpi[0].s + fpi[0].c},
+                                {fsr[1].s + fsr[1].c, fsi[1].s + fsi[1].c, fpr[1].s + fpr[1].c, fpi[1].s + fpi[1].c}};
+        for (unsigned k = 0; k < 4; ++k) {
+            focal.field[k] = g[0][k];
+            focal.field2[k] = g[1][k];
+        }
+        for (unsigned j = 0; j < columns; ++j) {
+            focal.s += weight * fma(g[j][0], g[j][0], g[j][1] * g[j][1]);
+            focal.p += weight * fma(g[j][2], g[j][2], g[j][3] * g[j][3]);
+        }
+        for (unsigned k = 0; k < 4; ++k) focal.fam_inc[k] = env[k].s + env[k].c;
+        if (!fin(g[0][0]) || !fin(g[0][1]) || !fin(g[0][2]) || !fin(g[0][3]) || !fin(g[1][0]) || !fin(g[1][1]) ||
+            !fin(g[1][2]) || !fin(g[1][3]) || !fin(focal.s + focal.p))
+            focal.flags |= FO_ARITH;
+        if (focal.flags) focal_nan(&focal);
+        *focal_out = focal;
+    }
+    return res;
+}
+
+/* Every direction of the input; focal results too when fc != NULL. */
+void icpo_patch_optics(const pinput* in, const pfocal_cfg* fc, poptical* results, rb_focal* focal)
+{
+    for (uint32_t i = 0; i < in->direction_count; ++i)
+        results[i] = optics_direction(in, i, fc, fc ? focal + i : NULL);
+}

@@ -67,6 +67,7 @@ def _lib() -> C.CDLL:
     lib.icpo_rainbow_filter.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, _D, C.c_void_p]
     lib.icpo_rainbow_filter_at.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, _D, C.c_void_p,
                                            C.c_uint64, C.c_void_p]
+    lib.icpo_patch_optics.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.icpo_atlas_node.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint32, _D, _D,
                                     _D, _D, C.c_uint64, _D, C.c_uint32, C.c_uint32, C.c_double, _D, _D]
     return lib
@@ -520,3 +521,77 @@ def ref_rainbow_grid(focal: np.ndarray, nt: int, np_: int, config, edges: np.nda
     n = nt * np_
     return (np.frombuffer(raw[: 4 * n], dtype="<u4").copy(),
             np.frombuffer(raw[4 * n:], dtype=RESULT_DTYPE).copy())
+
+
+# ----------------------------------------------------------------------- patch optics
+class _Vec3f(C.Structure):
+    _fields_ = [("x", C.c_float), ("y", C.c_float), ("z", C.c_float)]
+
+
+class _OpticsInput(C.Structure):
+    _fields_ = [("vertices", C.c_void_p), ("patches", C.c_void_p), ("directions", C.c_void_p),
+                ("offsets", C.c_void_p), ("summaries", C.c_void_p), ("hits", C.c_void_p), ("second", C.c_void_p),
+                ("hit_storage", C.c_uint64), ("vertex_count", C.c_uint32), ("patch_count", C.c_uint32),
+                ("direction_count", C.c_uint32), ("second_count", C.c_uint32), ("incident", _Vec3f),
+                ("incident_basis", _Vec3f), ("polarization", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class _FocalConfig(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("half_extent", C.c_float), ("reserved", C.c_uint32),
+                ("offsets", C.c_uint32 * 4)]
+
+
+OPTICAL_DTYPE = np.dtype([("path_field", "<f8", 4), ("incoherent_s", "<f8"), ("incoherent_p", "<f8"),
+                          ("path_s", "<f8"), ("path_p", "<f8")] +
+                         [(k, "<u4") for k in ("hit_count", "evaluated_hits", "rejected_hits", "refinement_hits",
+                                               "boundary_hits", "singular_hits", "flags", "query_flags",
+                                               "first_problem_patch_id", "folded_hits")] +
+                         [("path_field_second", "<f8", 4)])
+
+
+def patch_optics(case) -> tuple[np.ndarray, np.ndarray | None]:
+    """Per-direction optics of an optics input (tests/optics_cases.OpticsInput): the
+    PatchOpticalResult records, and the FocalOpticalResult records when it has a focal layout."""
+    keep = []
+
+    def ptr(a):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a)
+        keep.append(a)
+        return a.ctypes.data
+
+    n = case.count
+    inp = _OpticsInput(ptr(case.vertices), ptr(case.patches), ptr(np.asarray(case.directions, dtype=np.float32)),
+                       ptr(case.offsets.astype(np.uint64)), ptr(case.summaries), ptr(case.hits),
+                       ptr(None if case.second is None else np.asarray(case.second, dtype=np.float32)),
+                       len(case.hits), len(case.vertices), len(case.patches), n, case.second_len(),
+                       _Vec3f(*map(float, case.incident)), _Vec3f(*map(float, case.basis)), case.polarization, 0)
+    out = np.zeros(n, dtype=OPTICAL_DTYPE)
+    focal = np.zeros(n, dtype=FOCAL_DTYPE) if case.focal else None
+    cfg = None
+    if case.focal:
+        w, h, e, o = case.focal
+        cfg = _FocalConfig(w, h, e, 0, (C.c_uint32 * 4)(*o))
+    lib().icpo_patch_optics(C.addressof(inp), C.addressof(cfg) if cfg is not None else None, out.ctypes.data,
+                            focal.ctypes.data if focal is not None else None)
+    return out, focal
+
+
+def ref_optics_available() -> bool:
+    return (REF_DIR / "ref_optics_harness").exists()
+
+
+def ref_patch_optics(blob: bytes, count: int, with_focal: bool,
+                     workdir: Path | None = None) -> tuple[np.ndarray, np.ndarray | None]:
+    """The reference's evaluator over a serialized optics input (tests/optics_cases.serialize)."""
+    base = Path(workdir or "/tmp") / f"ref_optics_{os.getpid()}"
+    src, dst = base.with_suffix(".in"), base.with_suffix(".out")
+    src.write_bytes(blob)
+    subprocess.run([str(REF_DIR / "ref_optics_harness"), str(src), str(dst)], check=True)
+    raw = dst.read_bytes()
+    src.unlink()
+    dst.unlink()
+    out = np.frombuffer(raw[: 136 * count], dtype=OPTICAL_DTYPE).copy()
+    focal = np.frombuffer(raw[136 * count:], dtype=FOCAL_DTYPE).copy() if with_focal else None
+    return out, focal

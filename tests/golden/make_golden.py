@@ -310,6 +310,29 @@ def _ref_grid(src: Path, dst: Path, f, nt, np_, cfg, edges):
     return np.frombuffer(raw[:4 * n], "<u4").copy(), np.frombuffer(raw[4 * n:], RC.RESULT_DTYPE).copy()
 
 
+def optics_fixtures(td: Path) -> None:
+    """The reference's per-direction optics (PatchOpticalEvaluator::evaluate_direction, with and
+    without the focal stage) on the inputs of tests/optics_cases.py, with each input's SHA-256."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import optics_cases as OC  # noqa: E402
+    out = {}
+    for name, make in OC.CASES:
+        c = make()
+        blob = OC.serialize(c)
+        src, dst = td / "op.in", td / "op.out"
+        src.write_bytes(blob)
+        run([REF_BIN / "ref_optics_harness", src, dst])
+        raw = dst.read_bytes()
+        n = c.count
+        out[f"{name}.digest"] = np.array(OC.digest(c))
+        out[f"{name}.optical"] = np.frombuffer(raw[:136 * n], dtype=OC.OPTICAL_DTYPE).copy()
+        if c.focal:
+            sys.path.insert(0, str(ROOT / "tests"))
+            import rainbow_cases as RC  # noqa: E402
+            out[f"{name}.focal"] = np.frombuffer(raw[136 * n:], dtype=RC.FOCAL_DTYPE).copy()
+    np.savez_compressed(HERE / "optics_reference.npz", **out)
+
+
 def main() -> None:
     subprocess.run([str(ROOT / "oracle" / "build_ref.sh"), str(REF)], check=True)
     with tempfile.TemporaryDirectory() as t:
@@ -355,6 +378,8 @@ def main() -> None:
         compare_fixtures(td)
         # 8. Table-II rainbow diffraction
         rainbow_fixtures(td)
+        # 9. per-direction optics of the drop's wave stages
+        optics_fixtures(td)
     for f in sorted(HERE.glob("*.npz")):
         print(f.name, f.stat().st_size)
 

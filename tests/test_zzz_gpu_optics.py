@@ -1,0 +1,98 @@
+"""Per-direction optics of the drop's wave stages on the GPU, through the C ABI, against the
+reference's outputs (tests/golden/optics_reference.npz) and the oracle.
+
+Tolerances are the reference's own for its CUDA evaluator against its host build: flags,
+query flags and every hit counter exact; fields to 8e-6 x (1 + sqrt(incoherent) + |x|),
+intensities to 8e-6 relative (tests/patch_optics_test_cases.hpp:19-23, 227-243 of the
+reference); focal flags, counters and family hits exact, focal values to 2e-6 relative
+(tests/wave_optics_test_cases.hpp:10-25).  The differences come from CUDA's cosf / sinf /
+atan2 in the last ulps.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import optics_cases as OC
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+Z = np.load(GOLDEN / "optics_reference.npz")
+COUNTERS = ("flags", "query_flags", "hit_count", "evaluated_hits", "rejected_hits", "first_problem_patch_id",
+            "refinement_hits", "boundary_hits", "singular_hits", "folded_hits")
+
+
+def near(a, b, tol, scale=1.0):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return np.isfinite(a) & np.isfinite(b) & (np.abs(a - b) <= tol * (scale + np.abs(b)))
+
+
+def optics_mismatch(got, want) -> list[str]:
+    bad = [k for k in COUNTERS if not np.array_equal(got[k], want[k])]
+    ok = (want["flags"] & 31) == 0
+    if not np.isnan(got["path_s"][~ok]).all():
+        bad.append("unavailable not NaN")
+    g, w = got[ok], want[ok]
+    scale = 1.0 + np.sqrt(w["incoherent_s"] + w["incoherent_p"])
+    for k in ("path_field", "path_field_second"):
+        if not near(g[k], w[k], 8e-6, scale[:, None]).all():
+            bad.append(k)
+    for k in ("incoherent_s", "incoherent_p"):
+        if not near(g[k], w[k], 8e-6).all():
+            bad.append(k)
+    for k in ("path_s", "path_p"):
+        if not near(g[k], w[k], 8e-6, scale * scale).all():
+            bad.append(k)
+    return bad
+
+
+def focal_mismatch(got, want) -> list[str]:
+    bad = [k for k in ("flags", "corrected_hits", "extra_quarter_turn_hits", "first_problem_patch_id", "family_hits")
+           if not np.array_equal(got[k], want[k])]
+    ok = want["flags"] == 0
+    if not np.isnan(got["intensity_s"][~ok]).all():
+        bad.append("unavailable not NaN")
+    for k in ("family_incoherent", "intensity_s", "intensity_p", "field", "field_second"):
+        if not near(got[k][ok], want[k][ok], 2e-6).all():
+            bad.append(k)
+    return bad
+
+
+def run(icp, ctx, c):
+    return icp.patch_optics(ctx, c.vertices, c.patches, c.directions, c.offsets, c.summaries, c.hits, c.incident,
+                            c.basis, second=c.second, polarization=c.polarization, focal=c.focal)
+
+
+@pytest.mark.parametrize("name", [c[0] for c in OC.CASES])
+def test_fixture_cases_match_reference(icp, ctx, name):
+    c = dict(OC.CASES)[name]()
+    assert OC.digest(c) == str(Z[f"{name}.digest"])
+    before = icp.kernel_launches()
+    out, focal = run(icp, ctx, c)
+    assert icp.kernel_launches() - before == 1
+    bad = optics_mismatch(out, Z[f"{name}.optical"])
+    assert not bad, bad
+    if c.focal:
+        bad = focal_mismatch(focal, Z[f"{name}.focal"])
+        assert not bad, bad
+
+
+def test_large_lattice_against_oracle(icp, ctx, oracle):
+    """A 129 x 129 lattice (66 564 vertices, 65 536 patches) queried in 20 000 directions."""
+    c = OC.lattice_case(77, width=129, height=129, directions=20000)
+    out, focal = run(icp, ctx, c)
+    want, wfocal = oracle.patch_optics(c)
+    assert not optics_mismatch(out, want)
+    assert not focal_mismatch(focal, wfocal)
+    assert (out["flags"] == 0).sum() > 5000
+
+
+def test_focal_feeds_the_diffraction_pass(icp, ctx, oracle):
+    """The focal stage's output is the diffraction pass's input, unchanged (one query grid)."""
+    c = OC.lattice_case(9, directions=12 * 24, faults=False)
+    _, focal = run(icp, ctx, c)
+    cfg = icp.DiffractionConfig(3.0 * np.pi / 180, 4.0, 0.25, 3.0)
+    d = icp.rainbow_diffraction(ctx, focal, 12, 24, cfg)
+    edges = oracle.rainbow_detect(focal, 12, 24, (cfg.primary_sigma_rad, 4.0, 0.25, 3.0))
+    assert np.array_equal(d.transitions, edges)
