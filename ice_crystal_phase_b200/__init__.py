@@ -19,6 +19,7 @@ Mirrored reference interfaces (Somatic-Cell/ice-crystal-phase):
   PhaseMassAccumulatorCuda.add_drop  RaindropTracer::trace_unpolarized + patch stages, replaced by
                                    direct binning (include/rainbow/raindrop_tracer.hpp:32-36)
   generate_drop_record             apps/generate_phase.cpp:395-453 (rainbow_generate's record path)
+  patch_build                      PatchAccel::build's kernels, device/patch_build.cu:13-77
   patch_optics                     PatchOptics::evaluate_device / evaluate_wave_device's kernels
                                    evaluate_patch_optics / evaluate_focal_optics, device/patch_optics.cu:7-24
   rainbow_table_sigma              include/rainbow/rainbow_diffraction.hpp:16-28
@@ -270,6 +271,7 @@ OPTICAL_DTYPE = np.dtype([("path_field", "<f8", 4), ("incoherent_s", "<f8"), ("i
                                                "boundary_hits", "singular_hits", "flags", "query_flags",
                                                "first_problem_patch_id", "folded_hits")] +
                          [("path_field_second", "<f8", 4)])
+AABB_DTYPE = np.dtype([(k, "<f4") for k in ("min_x", "min_y", "min_z", "max_x", "max_y", "max_z")])
 
 
 class SurrogateConfig(C.Structure):
@@ -355,6 +357,8 @@ _FUNCS = {
     "icp_atlas_coupling": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_double, C.c_double, _D, _P, _P,
                                      C.c_uint64, _D, C.c_double, C.c_int, _P, _D]),
     "icp_atlas_compose": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, _P, _P, _P]),
+    "icp_patch_build": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32, C.c_float, _P, _P, _P, C.POINTER(C.c_uint32),
+                                  C.POINTER(C.c_uint64)]),
     "icp_patch_optics": (C.c_int, [_P, C.POINTER(OpticsInput), _P, C.POINTER(FocalConfig), _P]),
     "icp_rainbow_table_sigma": (C.c_int, [C.c_float, _D]),
     "icp_rainbow_detect": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32, C.POINTER(DiffractionConfig), _P]),
@@ -1222,3 +1226,29 @@ def patch_optics(ctx: Context, vertices, patches, directions, offsets, summaries
     check(LIB.icp_patch_optics(ctx.handle, C.byref(inp), dr.ptr, C.byref(fc) if fc is not None else None,
                                df.ptr if df is not None else None))
     return dr.download(), (df.download() if df is not None else None)
+
+
+@dataclass
+class PatchBuild:
+    patches: np.ndarray    # PATCH_DTYPE [count], patch_id order
+    aabbs: np.ndarray      # AABB_DTYPE [count]
+    statuses: np.ndarray   # uint32 [4 (W-1)(H-1)], per cell
+    histogram: list        # cells per status 0..7
+
+
+def patch_build(ctx: Context, vertices, grid_width: int, grid_height: int, grid_half_extent: float) -> PatchBuild:
+    """Patches of a four-family lattice (VERTEX_DTYPE [4 W H], host or DeviceArray)."""
+    cells = 4 * (grid_width - 1) * (grid_height - 1)
+    if isinstance(vertices, DeviceArray):
+        dv = vertices
+    else:
+        dv = DeviceArray(ctx, len(vertices), VERTEX_DTYPE).upload(np.ascontiguousarray(vertices, dtype=VERTEX_DTYPE))
+    dp = DeviceArray(ctx, cells, PATCH_DTYPE)
+    db = DeviceArray(ctx, cells, AABB_DTYPE)
+    ds = DeviceArray(ctx, cells, np.uint32)
+    count = C.c_uint32(0)
+    hist = (C.c_uint64 * 8)()
+    check(LIB.icp_patch_build(ctx.handle, dv.ptr, grid_width, grid_height, float(grid_half_extent), dp.ptr, db.ptr,
+                              ds.ptr, C.byref(count), hist))
+    n = count.value
+    return PatchBuild(dp.download()[:n], db.download()[:n], ds.download(), list(hist))

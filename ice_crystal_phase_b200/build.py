@@ -52,6 +52,7 @@ UNITS = {
     "icp_atlas.cu": ["-fmad=false"],
     "icp_rainbow.cu": ["-fmad=false"],
     "icp_optics.cu": ["-fmad=false"],
+    "icp_patches.cu": ["-fmad=false"],
 }
 
 HOST_SOURCES = ["icp_record_io.cpp"]

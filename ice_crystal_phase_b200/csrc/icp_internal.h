@@ -268,5 +268,7 @@ struct icp_context {
     icp::Scratch atlas_trace, atlas_coupling;
     // Table-II rainbow diffraction: packed samples, row marks, counters
     icp::Scratch rainbow;
+    // patch build: cell statuses, block counts, histogram
+    icp::Scratch patches;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
 };

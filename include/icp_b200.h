@@ -20,6 +20,7 @@
  *   icp_drop_trace_bin    RaindropTracer::trace_unpolarized + patch/query/optics stages
  *                                                         include/rainbow/raindrop_tracer.hpp, apps/generate_phase.cpp:431-439
  *   icp_drop_generate     rainbow_generate's record path   apps/generate_phase.cpp:395-453
+ *   icp_patch_build       PatchAccel::build's kernels    device/patch_build.cu:13-77
  *   icp_patch_optics      evaluate_patch_optics / evaluate_focal_optics  device/patch_optics.cu:7-24
  *   icp_rainbow_*         RainbowDiffraction + PatchOptics::run_diffraction
  *                                                         include/rainbow/rainbow_diffraction.hpp,
@@ -712,6 +713,22 @@ typedef struct {                                             /* rainbow::FocalPh
     uint32_t reserved;
     uint32_t quarter_turn_offsets[4];                        /* per family, 0 .. 3                */
 } icp_focal_config;
+
+/* Padded bounding box of a patch's four corner directions (rainbow::PatchAabb, 24 B). */
+typedef struct { float min_x, min_y, min_z, max_x, max_y, max_z; } icp_patch_aabb;
+
+/* Patches of a four-family outgoing-ray lattice d_vertices[4 * W * H] (device; family-major,
+ * row-major within a family, the layout of RaindropTracer's vertex buffer): every cell with
+ * four outgoing corner rays, certified regular (status 1 / 2, signed solid angle) or needing
+ * refinement (3), stored compactly in patch_id order in d_patches (device, capacity
+ * 4 (W-1)(H-1)) with its padded box in d_aabbs (device, may be NULL); each cell's status
+ * (0..7) in d_statuses[4 (W-1)(H-1)] (device, may be NULL).  *patch_count and histogram[8]
+ * (per status, may be NULL) on the host.  Replaces PatchAccel::build's kernels
+ * classify_outgoing_patches / compact_outgoing_patches (device/patch_build.cu:13-77) and their
+ * host-side scan; an invalid layout (PatchBuildLayout::try_make) -> ICP_ERR_INVALID_ARGUMENT. */
+int icp_patch_build(icp_context* ctx, const icp_outgoing_vertex* d_vertices, uint32_t grid_width, uint32_t grid_height,
+                    float grid_half_extent, icp_outgoing_patch* d_patches, icp_patch_aabb* d_aabbs, uint32_t* d_statuses,
+                    uint32_t* patch_count, uint64_t histogram[8]);
 
 /* Optics of every query direction: d_results[direction_count] (device).  With focal != NULL
  * also the focal stage d_focal[direction_count] (device; the input of icp_rainbow_diffraction).

@@ -16,6 +16,8 @@
 #                                        diffraction (include/rainbow/rainbow_diffraction.hpp)
 #   oracle/_ref/ref_optics_harness       oracle/ref_optics_harness.cpp over the header-only patch optics
 #                                        (include/rainbow/patch_optical_evaluator.hpp)
+#   oracle/_ref/ref_patch_harness        oracle/ref_patch_harness.cpp over the header-only patch
+#                                        construction (include/rainbow/patch_geometry.hpp)
 #
 # Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
 set -euo pipefail
@@ -40,6 +42,8 @@ g++ -std=c++20 -O2 -fno-fast-math -ffp-contract=off -I"$ref/include" "$here/ref_
     -o "$out/ref_rainbow_harness"
 g++ -std=c++20 -O2 -fno-fast-math -ffp-contract=off -I"$ref/include" "$here/ref_optics_harness.cpp" \
     -o "$out/ref_optics_harness"
+g++ -std=c++20 -O2 -fno-fast-math -ffp-contract=off -I"$ref/include" "$here/ref_patch_harness.cpp" \
+    -o "$out/ref_patch_harness"
 if [ -f "$ref/hex_atlas/src/ice_optics.cpp" ]; then
     g++ -std=c++20 -O2 -fno-fast-math -ffp-contract=off -I"$ref/hex_atlas/include" "$here/ref_ice_harness.cpp" \
         "$ref/hex_atlas/src/ice_optics.cpp" -o "$out/ref_ice_harness"
@@ -49,4 +53,4 @@ if [ -f "$ref/hex_atlas/src/ice_optics.cpp" ]; then
         "$ref/hex_atlas/src/atlas.cpp" "$ref/hex_atlas/src/ice_optics.cpp" "$ref/hex_trace/src/hex_trace.cpp" \
         "$ref/src/npy_writer.cpp" -o "$out/ice_precompute_atlas_cpu"
 fi
-echo "built $out/ice_generate_phase_cpu $out/ref_hex_harness $out/ref_drop_harness $out/ref_ice_harness $out/ref_atlas_harness $out/ice_precompute_atlas_cpu $out/ref_rainbow_harness $out/ref_optics_harness"
+echo "built $out/ice_generate_phase_cpu $out/ref_hex_harness $out/ref_drop_harness $out/ref_ice_harness $out/ref_atlas_harness $out/ice_precompute_atlas_cpu $out/ref_rainbow_harness $out/ref_optics_harness $out/ref_patch_harness"

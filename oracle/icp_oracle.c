@@ -2440,3 +2440,175 @@ void icpo_patch_optics(const pinput* in, const pfocal_cfg* fc, poptical* results
     for (uint32_t i = 0; i < in->direction_count; ++i)
         results[i] = optics_direction(in, i, fc, fc ? focal + i : NULL);
 }
+
+/* ---------------------------------------------------------------- patch build
+ * Restates the reference's patch construction (PatchConstruction::make,
+ * include/rainbow/patch_geometry.hpp:117-172; BilinearPatchGeometry :75-114 with its outward
+ * rounded interval orientation test and the two-triangle solid angle; the layout of
+ * include/rainbow/outgoing_patch.hpp:59-92) and its compaction in patch_id order
+ * (device/patch_build.cu:13-77).  Binary32 with the reference's explicit fmaf and nextafterf,
+ * no contraction: bit-identical to the reference's headers compiled on the host. */
+typedef struct { float lo, hi; } piv;
+typedef struct { piv x, y, z; } piv3;
+typedef struct { float min_x, min_y, min_z, max_x, max_y, max_z; } paabb;
+
+static piv iv_pt(float x) { piv r = {x, x}; return r; }
+static piv iv_add(piv a, piv b) { piv r = {nextafterf(a.lo + b.lo, -INFINITY), nextafterf(a.hi + b.hi, INFINITY)}; return r; }
+static piv iv_sub(piv a, piv b) { piv r = {nextafterf(a.lo - b.hi, -INFINITY), nextafterf(a.hi - b.lo, INFINITY)}; return r; }
+static piv iv_mul(piv a, piv b)
+{
+    const float p0 = a.lo * b.lo, p1 = a.lo * b.hi, p2 = a.hi * b.lo, p3 = a.hi * b.hi;
+    piv r = {nextafterf(fminf(fminf(p0, p1), fminf(p2, p3)), -INFINITY),
+             nextafterf(fmaxf(fmaxf(p0, p1), fmaxf(p2, p3)), INFINITY)};
+    return r;
+}
+static piv3 iv3_pt(pf3 p) { piv3 r = {iv_pt(p.x), iv_pt(p.y), iv_pt(p.z)}; return r; }
+static piv3 iv3_sub(piv3 a, piv3 b) { piv3 r = {iv_sub(a.x, b.x), iv_sub(a.y, b.y), iv_sub(a.z, b.z)}; return r; }
+static piv3 iv3_cross(piv3 a, piv3 b)
+{
+    piv3 r = {iv_sub(iv_mul(a.y, b.z), iv_mul(a.z, b.y)), iv_sub(iv_mul(a.z, b.x), iv_mul(a.x, b.z)),
+              iv_sub(iv_mul(a.x, b.y), iv_mul(a.y, b.x))};
+    return r;
+}
+static piv iv3_dot(piv3 a, piv3 b) { return iv_add(iv_add(iv_mul(a.x, b.x), iv_mul(a.y, b.y)), iv_mul(a.z, b.z)); }
+
+static float pb_dop(float x, float y, float z, float w)
+{
+    const float zw = z * w;
+    const float residual = fmaf(-z, w, zw);
+    return fmaf(x, y, -zw) + residual;
+}
+static float pb_det(pf3 a, pf3 b, pf3 c)
+{
+    const pf3 u = f3_sub(b, a), v = f3_sub(c, a);
+    return fmaf(a.x, pb_dop(u.y, v.z, u.z, v.y), fmaf(a.y, pb_dop(u.z, v.x, u.x, v.z), a.z * pb_dop(u.x, v.y, u.y, v.x)));
+}
+/* signed solid angle of the spherical triangle (Van Oosterom & Strackee) */
+static float pb_triangle(pf3 a, pf3 b, pf3 c)
+{
+    const float la = sqrtf(f3_dot(a, a)), lb = sqrtf(f3_dot(b, b)), lc = sqrtf(f3_dot(c, c));
+    const float den = fmaf(la, lb * lc, fmaf(f3_dot(a, b), lc, fmaf(f3_dot(b, c), la, f3_dot(c, a) * lb)));
+    return 2.0f * atan2f(pb_det(a, b, c), den);
+}
+static pf3 f3_add(pf3 a, pf3 b) { pf3 r = {a.x + b.x, a.y + b.y, a.z + b.z}; return r; }
+/* +1 / -1 when the corner Jacobians have one certified sign and all corners lie in the
+ * hemisphere of their mean direction; 0 otherwise */
+static int pb_orientation(const pf3* c)
+{
+    const piv3 p0 = iv3_pt(c[0]), p1 = iv3_pt(c[1]), p2 = iv3_pt(c[2]), p3 = iv3_pt(c[3]);
+    const piv d0 = iv3_dot(p0, iv3_cross(iv3_sub(p1, p0), iv3_sub(p2, p0)));
+    const piv d1 = iv3_dot(p1, iv3_cross(iv3_sub(p1, p0), iv3_sub(p3, p1)));
+    const piv d2 = iv3_dot(p2, iv3_cross(iv3_sub(p3, p2), iv3_sub(p2, p0)));
+    const piv d3 = iv3_dot(p3, iv3_cross(iv3_sub(p3, p2), iv3_sub(p3, p1)));
+    const int positive = d0.lo > 0 && d1.lo > 0 && d2.lo > 0 && d3.lo > 0;
+    const int negative = d0.hi < 0 && d1.hi < 0 && d2.hi < 0 && d3.hi < 0;
+    if (!positive && !negative) return 0;
+    const piv3 a = iv3_pt(f3_add(f3_add(c[0], c[1]), f3_add(c[2], c[3])));
+    if (!(iv3_dot(a, p0).lo > 0 && iv3_dot(a, p1).lo > 0 && iv3_dot(a, p2).lo > 0 && iv3_dot(a, p3).lo > 0)) return 0;
+    return positive ? 1 : -1;
+}
+static paabb pb_bounds(const pf3* c)
+{
+    pf3 lo = c[0], hi = c[0];
+    for (unsigned i = 1; i < 4; ++i) {
+        lo.x = fminf(lo.x, c[i].x); lo.y = fminf(lo.y, c[i].y); lo.z = fminf(lo.z, c[i].z);
+        hi.x = fmaxf(hi.x, c[i].x); hi.y = fmaxf(hi.y, c[i].y); hi.z = fmaxf(hi.z, c[i].z);
+    }
+    const float pad = 0x1p-19f;
+    paabb r = {nextafterf(lo.x - pad, -INFINITY), nextafterf(lo.y - pad, -INFINITY), nextafterf(lo.z - pad, -INFINITY),
+               nextafterf(hi.x + pad, INFINITY), nextafterf(hi.y + pad, INFINITY), nextafterf(hi.z + pad, INFINITY)};
+    return r;
+}
+static int pb_usable(const pvertex* v)
+{
+    const float n2 = f3_dot(v->direction, v->direction);
+    return f3_fin(v->position) && f3_fin(v->direction) && f3_fin(v->basis) && fabsf(n2 - 1.0f) <= 0x1p-16f &&
+           cyc_ok(v->cycles) && pfield_fin32(v->field);
+}
+typedef struct { uint32_t width, height, per_path, cells, cell_count; float area; } playout;
+/* PatchBuildLayout::try_make */
+int icpo_patch_layout(uint32_t width, uint32_t height, float half_extent, uint32_t* out /* 5 */, float* area)
+{
+    if (width < 2 || height < 2 || !(half_extent > 0.0f) || !(half_extent <= 0x1.fffffep127f)) return 0;
+    const uint64_t vertices = (uint64_t)width * height, cells = (uint64_t)(width - 1) * (height - 1);
+    if (vertices > 0xffffffffull / 4u || cells > 0xffffffffull / 4u) return 0;
+    const float du = 2.0f * half_extent / (float)(width - 1), dv = 2.0f * half_extent / (float)(height - 1);
+    const float a = du * dv;
+    if (!(a > 0.0f && a <= 0x1.fffffep127f)) return 0;
+    out[0] = width;
+    out[1] = height;
+    out[2] = (uint32_t)vertices;
+    out[3] = (uint32_t)cells;
+    out[4] = (uint32_t)(4 * cells);
+    *area = a;
+    return 1;
+}
+static void pb_make(const pvertex* vertices, const playout* L, uint32_t id, ppatch* patch, paabb* box)
+{
+    memset(patch, 0, sizeof *patch);
+    memset(box, 0, sizeof *box);
+    patch->patch_id = id;
+    patch->area = L->area;
+    patch->solid_angle = NAN;
+    const uint32_t family = id / L->cells, cell = id % L->cells;
+    const uint32_t ix = cell % (L->width - 1), iy = cell / (L->width - 1);
+    const uint32_t first = family * L->per_path + iy * L->width + ix;
+    patch->v[0] = first;
+    patch->v[1] = first + 1;
+    patch->v[2] = first + L->width;
+    patch->v[3] = first + L->width + 1;
+    unsigned valid = 0;
+    int bad_vertex = 0, bad_geometry = 0;
+    pf3 corners[4];
+    memset(corners, 0, sizeof corners);
+    for (unsigned i = 0; i < 4; ++i) {
+        const pvertex* v = vertices + patch->v[i];
+        if (v->status == 1u) {
+            ++valid;
+            bad_geometry |= !pb_usable(v);
+            corners[i] = v->direction;
+        } else if (v->status != 2u && v->status != 3u) /* neither a miss nor total internal reflection */
+            bad_vertex = 1;
+    }
+    if (bad_vertex) patch->status = 6;
+    else if (bad_geometry) patch->status = 7;
+    else if (valid == 0) patch->status = 5;
+    else if (valid < 4) patch->status = 4;
+    else {
+        *box = pb_bounds(corners);
+        const int orientation = pb_orientation(corners);
+        patch->status = 3; /* needs refinement unless certified regular */
+        if (orientation != 0) {
+            const float angle = pb_triangle(corners[0], corners[1], corners[3]) + pb_triangle(corners[0], corners[3], corners[2]);
+            if (angle >= -0x1.fffffep127f && angle <= 0x1.fffffep127f && angle * (float)orientation > 0.0f) {
+                patch->status = orientation > 0 ? 1u : 2u;
+                patch->solid_angle = angle;
+            }
+        }
+    }
+}
+/* Every cell's status (statuses[cell_count]), the patches with geometry (status 1..3) in
+ * patch_id order with their boxes, and the status histogram; returns the patch count. */
+uint32_t icpo_patch_build(const pvertex* vertices, uint32_t width, uint32_t height, float half_extent,
+                          uint32_t* statuses, ppatch* patches, paabb* boxes, uint32_t* histogram /* 8 */)
+{
+    uint32_t lay[5];
+    float area;
+    if (!icpo_patch_layout(width, height, half_extent, lay, &area)) return 0xffffffffu;
+    const playout L = {lay[0], lay[1], lay[2], lay[3], lay[4], area};
+    uint32_t count = 0;
+    for (unsigned k = 0; k < 8; ++k) histogram[k] = 0;
+    for (uint32_t id = 0; id < L.cell_count; ++id) {
+        ppatch p;
+        paabb b;
+        pb_make(vertices, &L, id, &p, &b);
+        statuses[id] = p.status;
+        ++histogram[p.status];
+        if (p.status >= 1u && p.status <= 3u) {
+            patches[count] = p;
+            boxes[count] = b;
+            ++count;
+        }
+    }
+    return count;
+}

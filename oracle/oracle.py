@@ -68,6 +68,9 @@ def _lib() -> C.CDLL:
     lib.icpo_rainbow_filter_at.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, _D, C.c_void_p,
                                            C.c_uint64, C.c_void_p]
     lib.icpo_patch_optics.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.icpo_patch_build.restype = C.c_uint32
+    lib.icpo_patch_build.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.c_void_p]
     lib.icpo_atlas_node.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint32, _D, _D,
                                     _D, _D, C.c_uint64, _D, C.c_uint32, C.c_uint32, C.c_double, _D, _D]
     return lib
@@ -595,3 +598,40 @@ def ref_patch_optics(blob: bytes, count: int, with_focal: bool,
     out = np.frombuffer(raw[: 136 * count], dtype=OPTICAL_DTYPE).copy()
     focal = np.frombuffer(raw[136 * count:], dtype=FOCAL_DTYPE).copy() if with_focal else None
     return out, focal
+
+
+PATCH_DTYPE = np.dtype([("vertex_indices", "<u4", 4), ("patch_id", "<u4"), ("status", "<u4"),
+                        ("signed_solid_angle_sr", "<f4"), ("incident_area_drop2", "<f4")])
+AABB_DTYPE = np.dtype([(k, "<f4") for k in ("min_x", "min_y", "min_z", "max_x", "max_y", "max_z")])
+
+
+def patch_build(vertices: np.ndarray, width: int, height: int, half_extent: float):
+    """(statuses [cells], patches with geometry in patch_id order, their boxes, status histogram)."""
+    cells = 4 * (width - 1) * (height - 1)
+    v = np.ascontiguousarray(vertices)
+    st = np.zeros(cells, dtype=np.uint32)
+    pa = np.zeros(cells, dtype=PATCH_DTYPE)
+    bx = np.zeros(cells, dtype=AABB_DTYPE)
+    hist = np.zeros(8, dtype=np.uint32)
+    n = lib().icpo_patch_build(v.ctypes.data, width, height, float(half_extent), st.ctypes.data, pa.ctypes.data,
+                               bx.ctypes.data, hist.ctypes.data)
+    if n == 0xFFFFFFFF:
+        raise ValueError("invalid patch layout")
+    return st, pa[:n].copy(), bx[:n].copy(), hist
+
+
+def ref_patch_build(blob: bytes, cells: int, workdir: Path | None = None):
+    base = Path(workdir or "/tmp") / f"ref_patch_{os.getpid()}"
+    src, dst = base.with_suffix(".in"), base.with_suffix(".out")
+    src.write_bytes(blob)
+    subprocess.run([str(REF_DIR / "ref_patch_harness"), str(src), str(dst)], check=True)
+    raw = dst.read_bytes()
+    src.unlink()
+    dst.unlink()
+    st = np.frombuffer(raw[:4 * cells], "<u4").copy()
+    n = int(np.frombuffer(raw[4 * cells:4 * cells + 4], "<u4")[0])
+    hist = np.frombuffer(raw[4 * cells + 4:4 * cells + 36], "<u4").copy()
+    off = 4 * cells + 36
+    pa = np.frombuffer(raw[off:off + 32 * n], PATCH_DTYPE).copy()
+    bx = np.frombuffer(raw[off + 32 * n:off + 56 * n], AABB_DTYPE).copy()
+    return st, pa, bx, hist

@@ -312,7 +312,8 @@ def _ref_grid(src: Path, dst: Path, f, nt, np_, cfg, edges):
 
 def optics_fixtures(td: Path) -> None:
     """The reference's per-direction optics (PatchOpticalEvaluator::evaluate_direction, with and
-    without the focal stage) on the inputs of tests/optics_cases.py, with each input's SHA-256."""
+    without the focal stage) and patch construction (PatchConstruction::make, patch_id order) on
+    the inputs of tests/optics_cases.py, with each input's SHA-256."""
     sys.path.insert(0, str(ROOT / "tests"))
     import optics_cases as OC  # noqa: E402
     out = {}
@@ -330,7 +331,26 @@ def optics_fixtures(td: Path) -> None:
             sys.path.insert(0, str(ROOT / "tests"))
             import rainbow_cases as RC  # noqa: E402
             out[f"{name}.focal"] = np.frombuffer(raw[136 * n:], dtype=RC.FOCAL_DTYPE).copy()
+    for name, make in OC.PATCH_CASES:
+        v, (w, h, e) = make()
+        src, dst = td / "pa.in", td / "pa.out"
+        src.write_bytes(OC.serialize_lattice(v, (w, h, e)))
+        run([REF_BIN / "ref_patch_harness", src, dst])
+        raw = dst.read_bytes()
+        cells = 4 * (w - 1) * (h - 1)
+        n = int(np.frombuffer(raw[4 * cells:4 * cells + 4], "<u4")[0])
+        off = 4 * cells + 36
+        out[f"patch.{name}.digest"] = np.array(hashlib_hex(OC.serialize_lattice(v, (w, h, e))))
+        out[f"patch.{name}.status"] = np.frombuffer(raw[:4 * cells], "<u4").astype(np.uint8)
+        out[f"patch.{name}.histogram"] = np.frombuffer(raw[4 * cells + 4:off], "<u4").copy()
+        out[f"patch.{name}.patches"] = np.frombuffer(raw[off:off + 32 * n], OC.PATCH_DTYPE).copy()
+        out[f"patch.{name}.aabbs"] = np.frombuffer(raw[off + 32 * n:off + 56 * n], OC.AABB_DTYPE).copy()
     np.savez_compressed(HERE / "optics_reference.npz", **out)
+
+
+def hashlib_hex(blob: bytes) -> str:
+    import hashlib
+    return hashlib.sha256(blob).hexdigest()
 
 
 def main() -> None:

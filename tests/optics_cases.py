@@ -34,6 +34,7 @@ OPTICAL_DTYPE = np.dtype([("path_field", "<f8", 4), ("incoherent_s", "<f8"), ("i
                                                "boundary_hits", "singular_hits", "flags", "query_flags",
                                                "first_problem_patch_id", "folded_hits")] +
                          [("path_field_second", "<f8", 4)])
+AABB_DTYPE = np.dtype([(k, "<f4") for k in ("min_x", "min_y", "min_z", "max_x", "max_y", "max_z")])
 assert (VERTEX_DTYPE.itemsize, PATCH_DTYPE.itemsize, HIT_DTYPE.itemsize, SUMMARY_DTYPE.itemsize,
         OPTICAL_DTYPE.itemsize) == (68, 32, 32, 32, 136)
 
@@ -225,3 +226,54 @@ def serialize(c: OpticsInput) -> bytes:
 
 def digest(c: OpticsInput) -> str:
     return hashlib.sha256(serialize(c)).hexdigest()
+
+
+# --------------------------------------------------------------- patch build lattices
+def patch_lattice(seed: int, width: int = 9, height: int = 8, faults: bool = True) -> tuple[np.ndarray, tuple]:
+    """A four-family lattice for the patch construction: smooth families, one whose scattering
+    angle folds over the emitting plane (cells of both orientations and uncertified cells at
+    the fold), misses and total internal reflections at the rim, and -- with faults -- invalid
+    vertices of each kind."""
+    c = lattice_case(seed, width=width, height=height, directions=1, dual=False, focal=False, faults=False)
+    v = c.vertices
+    rng = np.random.default_rng(seed + 1000)
+    n = width * height
+    half = 1.01
+    k, e0 = c.incident.astype(np.float64), c.basis.astype(np.float64)
+    e1 = np.cross(k, e0)
+    iy, ix = np.divmod(np.arange(n), width)
+    U = (2 * ix / (width - 1) - 1) * half
+    V = (2 * iy / (height - 1) - 1) * half
+    r2 = U * U + V * V
+    theta = 2.3 + 0.6 * r2 - 0.8 * r2 * r2          # folds at r^2 = 0.375
+    phi = np.arctan2(V, U)
+    d = np.cos(theta)[:, None] * k + np.sin(theta)[:, None] * (np.cos(phi)[:, None] * e0 + np.sin(phi)[:, None] * e1)
+    v["direction"][2 * n:3 * n] = _f32_unit(d)
+    rim = r2 > 0.98 * half * half
+    for f in range(4):
+        sl = slice(f * n, (f + 1) * n)
+        st = v["status"][sl]
+        st[rim] = 2 if f != 3 else 3                      # misses; TIR on the last family
+        v["status"][sl] = st
+    if faults:
+        pick = rng.choice(4 * n, 6, replace=False)
+        v["status"][pick[0]] = 4                          # unresolved intersection
+        v["status"][pick[1]] = 0                          # unwritten
+        v["direction"][pick[2]] *= np.float32(1.001)      # not unit to 2^-16
+        v["fraction"][pick[3]] = np.float32(np.nan)
+        v["position"][pick[4], 0] = np.inf
+        v["field"][pick[5], 2] = np.nan
+    return v, (width, height, half)
+
+
+PATCH_CASES = [
+    ("fold_9x8", lambda: patch_lattice(21)),
+    ("fold_17x13_clean", lambda: patch_lattice(22, width=17, height=13, faults=False)),
+    ("small_2x2", lambda: patch_lattice(23, width=2, height=2, faults=False)),
+    ("wide_33x5", lambda: patch_lattice(24, width=33, height=5)),
+]
+
+
+def serialize_lattice(vertices: np.ndarray, layout: tuple) -> bytes:
+    w, h, e = layout
+    return struct.pack("<IIf", w, h, e) + np.ascontiguousarray(vertices, dtype=VERTEX_DTYPE).tobytes()

@@ -106,3 +106,37 @@ def test_records_match_the_c_structs(icp, tmp_path):
                                        "icp_query_summary", "icp_optical_result", "icp_focal_config")] == \
         [68, 32, 32, 32, 136, 32]
     assert got[("icp_optics_input", "size")] == icp.C.sizeof(icp.OpticsInput)
+
+
+# ------------------------------------------------------------------------ patch build
+@pytest.mark.parametrize("name", [c[0] for c in OC.PATCH_CASES])
+def test_patch_build_oracle_bit_identical_to_reference(oracle, name):
+    import hashlib
+    v, (w, h, e) = dict(OC.PATCH_CASES)[name]()
+    blob = OC.serialize_lattice(v, (w, h, e))
+    assert hashlib.sha256(blob).hexdigest() == str(Z[f"patch.{name}.digest"])
+    st, pa, bx, hist = oracle.patch_build(v, w, h, e)
+    assert np.array_equal(st, Z[f"patch.{name}.status"]) and np.array_equal(hist, Z[f"patch.{name}.histogram"])
+    assert pa.tobytes() == Z[f"patch.{name}.patches"].tobytes() and bx.tobytes() == Z[f"patch.{name}.aabbs"].tobytes()
+
+
+def test_patch_build_covers_every_status_and_orders_by_id():
+    hist = sum(Z[f"patch.{n}.histogram"].astype(np.int64) for n, _ in OC.PATCH_CASES)
+    assert (hist[1:] > 0).all()  # regular +/-, refinement, missing, none, invalid vertex / geometry
+    for n, _ in OC.PATCH_CASES:
+        p = Z[f"patch.{n}.patches"]
+        assert (np.diff(p["patch_id"].astype(np.int64)) > 0).all()
+        reg = np.isin(p["status"], (1, 2))
+        assert np.isfinite(p["signed_solid_angle_sr"][reg]).all() and np.isnan(p["signed_solid_angle_sr"][~reg]).all()
+        assert (np.sign(p["signed_solid_angle_sr"][reg]) == np.where(p["status"][reg] == 1, 1, -1)).all()
+
+
+def test_patch_build_live_reference(oracle):
+    if not oracle.ref_optics_available() or not (oracle.REF_DIR / "ref_patch_harness").exists():
+        pytest.skip("reference harness not built")
+    for seed in (31, 32):
+        v, (w, h, e) = OC.patch_lattice(seed, width=6 + seed % 5, height=7)
+        cells = 4 * (w - 1) * (h - 1)
+        ref = oracle.ref_patch_build(OC.serialize_lattice(v, (w, h, e)), cells)
+        got = oracle.patch_build(v, w, h, e)
+        assert all(a.tobytes() == b.tobytes() for a, b in zip(got, ref))

@@ -96,3 +96,33 @@ def test_focal_feeds_the_diffraction_pass(icp, ctx, oracle):
     d = icp.rainbow_diffraction(ctx, focal, 12, 24, cfg)
     edges = oracle.rainbow_detect(focal, 12, 24, (cfg.primary_sigma_rad, 4.0, 0.25, 3.0))
     assert np.array_equal(d.transitions, edges)
+
+
+@pytest.mark.parametrize("name", [c[0] for c in OC.PATCH_CASES])
+def test_patch_build_matches_reference(icp, ctx, name):
+    """Statuses, order, corner indices, areas and boxes exact; the solid angle to 4 ulps
+    (CUDA's atan2f)."""
+    v, (w, h, e) = dict(OC.PATCH_CASES)[name]()
+    before = icp.kernel_launches()
+    got = icp.patch_build(ctx, v, w, h, e)
+    assert icp.kernel_launches() - before == 3
+    want = Z[f"patch.{name}.patches"]
+    assert np.array_equal(got.statuses.astype(np.uint8), Z[f"patch.{name}.status"])
+    assert got.histogram == [int(x) for x in Z[f"patch.{name}.histogram"]]
+    assert len(got.patches) == len(want)
+    for k in ("vertex_indices", "patch_id", "status", "incident_area_drop2"):
+        assert np.array_equal(got.patches[k], want[k]), k
+    a, b = got.patches["signed_solid_angle_sr"], want["signed_solid_angle_sr"]
+    reg = np.isfinite(b)
+    assert np.array_equal(np.isfinite(a), reg)
+    assert (np.abs(a[reg] - b[reg]) <= 4 * np.spacing(np.abs(b[reg]).astype(np.float32))).all()
+    assert got.aabbs.tobytes() == Z[f"patch.{name}.aabbs"].tobytes()
+
+
+def test_patch_build_large_lattice_against_oracle(icp, ctx, oracle):
+    """A 257 x 257 lattice (262 144 cells, 1024 blocks: a multi-chunk block-count scan)."""
+    v, (w, h, e) = OC.patch_lattice(41, width=257, height=257)
+    got = icp.patch_build(ctx, v, w, h, e)
+    st, pa, bx, hist = oracle.patch_build(v, w, h, e)
+    assert np.array_equal(got.statuses, st) and got.histogram == [int(x) for x in hist]
+    assert np.array_equal(got.patches["patch_id"], pa["patch_id"]) and got.aabbs.tobytes() == bx.tobytes()
