@@ -20,6 +20,8 @@ Mirrored reference interfaces (Somatic-Cell/ice-crystal-phase):
                                    direct binning (include/rainbow/raindrop_tracer.hpp:32-36)
   generate_drop_record             apps/generate_phase.cpp:395-453 (rainbow_generate's record path)
   patch_build                      PatchAccel::build's kernels, device/patch_build.cu:13-77
+  query_directions                 QueryDirectionGrid::directions, include/rainbow/query_direction_grid.hpp:14-58
+  patch_query                      PatchQuery::query_grid (OptiX all-hit query), src/patch_query.cpp
   patch_optics                     PatchOptics::evaluate_device / evaluate_wave_device's kernels
                                    evaluate_patch_optics / evaluate_focal_optics, device/patch_optics.cu:7-24
   rainbow_table_sigma              include/rainbow/rainbow_diffraction.hpp:16-28
@@ -358,6 +360,10 @@ _FUNCS = {
                                      C.c_uint64, _D, C.c_double, C.c_int, _P, _D]),
     "icp_atlas_compose": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, _P, _P, _P]),
     "icp_patch_build": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32, C.c_float, _P, _P, _P, C.POINTER(C.c_uint32),
+                                  C.POINTER(C.c_uint64)]),
+    "icp_query_directions": (C.c_int, [C.c_uint32, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                       C.POINTER(C.c_float)]),
+    "icp_patch_query": (C.c_int, [_P, _P, C.c_uint32, _P, _P, C.c_uint32, _P, C.c_uint32, _P, _P, _P, C.c_uint64,
                                   C.POINTER(C.c_uint64)]),
     "icp_patch_optics": (C.c_int, [_P, C.POINTER(OpticsInput), _P, C.POINTER(FocalConfig), _P]),
     "icp_rainbow_table_sigma": (C.c_int, [C.c_float, _D]),
@@ -1252,3 +1258,42 @@ def patch_build(ctx: Context, vertices, grid_width: int, grid_height: int, grid_
                               ds.ptr, C.byref(count), hist))
     n = count.value
     return PatchBuild(dp.download()[:n], db.download()[:n], ds.download(), list(hist))
+
+
+def query_directions(theta_count: int, phi_count: int, axis, e0) -> np.ndarray:
+    """The reference's query grid directions, float32 [theta_count * phi_count, 3]."""
+    out = np.empty((theta_count * phi_count, 3), dtype=np.float32)
+    a = (C.c_float * 3)(*map(float, axis))
+    b = (C.c_float * 3)(*map(float, e0))
+    check(LIB.icp_query_directions(theta_count, phi_count, a, b, out.ctypes.data_as(C.POINTER(C.c_float))))
+    return out
+
+
+@dataclass
+class PatchQueryResult:
+    offsets: np.ndarray    # uint64 [n + 1]
+    summaries: np.ndarray  # SUMMARY_DTYPE [n]
+    hits: np.ndarray       # HIT_DTYPE [offsets[n]]
+
+
+def patch_query(ctx: Context, vertices, patches, aabbs, directions) -> PatchQueryResult:
+    """All-hit query of patches (PATCH_DTYPE, AABB_DTYPE from patch_build) for float32 [n, 3]
+    directions: sized first, then filled, as the reference's two query passes."""
+    n = len(directions)
+    dv = DeviceArray(ctx, len(vertices), VERTEX_DTYPE).upload(np.ascontiguousarray(vertices, dtype=VERTEX_DTYPE))
+    dp = DeviceArray(ctx, max(1, len(patches)), PATCH_DTYPE)
+    db = DeviceArray(ctx, max(1, len(aabbs)), AABB_DTYPE)
+    if len(patches):
+        dp.upload(np.ascontiguousarray(patches, dtype=PATCH_DTYPE))
+        db.upload(np.ascontiguousarray(aabbs, dtype=AABB_DTYPE))
+    dd = DeviceArray(ctx, max(1, 3 * n), np.float32)
+    if n:
+        dd.upload(np.asarray(directions, dtype=np.float32).reshape(-1))
+    do = DeviceArray(ctx, n + 1, np.uint64)
+    total = C.c_uint64(0)
+    args = (ctx.handle, dv.ptr, len(vertices), dp.ptr, db.ptr, len(patches), dd.ptr, n, do.ptr)
+    check(LIB.icp_patch_query(*args, None, None, 0, C.byref(total)))
+    ds = DeviceArray(ctx, max(1, n), SUMMARY_DTYPE)
+    dh = DeviceArray(ctx, max(1, total.value), HIT_DTYPE)
+    check(LIB.icp_patch_query(*args, ds.ptr, dh.ptr, max(1, total.value), C.byref(total)))
+    return PatchQueryResult(do.download(), ds.download()[:n], dh.download()[:total.value])

@@ -53,6 +53,7 @@ UNITS = {
     "icp_rainbow.cu": ["-fmad=false"],
     "icp_optics.cu": ["-fmad=false"],
     "icp_patches.cu": ["-fmad=false"],
+    "icp_query.cu": ["-fmad=false"],
 }
 
 HOST_SOURCES = ["icp_record_io.cpp"]

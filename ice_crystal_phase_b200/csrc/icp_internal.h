@@ -270,5 +270,7 @@ struct icp_context {
     icp::Scratch rainbow;
     // patch build: cell statuses, block counts, histogram
     icp::Scratch patches;
+    // patch query: direction bins, scans, per-direction counts; the bins' patch lists
+    icp::Scratch query, query_list;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
 };

@@ -21,6 +21,7 @@
  *                                                         include/rainbow/raindrop_tracer.hpp, apps/generate_phase.cpp:431-439
  *   icp_drop_generate     rainbow_generate's record path   apps/generate_phase.cpp:395-453
  *   icp_patch_build       PatchAccel::build's kernels    device/patch_build.cu:13-77
+ *   icp_patch_query       PatchQuery::query_grid          src/patch_query.cpp, shaders/entry/patch_query.cu
  *   icp_patch_optics      evaluate_patch_optics / evaluate_focal_optics  device/patch_optics.cu:7-24
  *   icp_rainbow_*         RainbowDiffraction + PatchOptics::run_diffraction
  *                                                         include/rainbow/rainbow_diffraction.hpp,
@@ -729,6 +730,29 @@ typedef struct { float min_x, min_y, min_z, max_x, max_y, max_z; } icp_patch_aab
 int icp_patch_build(icp_context* ctx, const icp_outgoing_vertex* d_vertices, uint32_t grid_width, uint32_t grid_height,
                     float grid_half_extent, icp_outgoing_patch* d_patches, icp_patch_aabb* d_aabbs, uint32_t* d_statuses,
                     uint32_t* patch_count, uint64_t histogram[8]);
+
+/* The reference's query directions (QueryDirectionGrid, include/rainbow/query_direction_grid.hpp
+ * :14-58): theta_count x phi_count cell centres about `axis` (theta from the axis, phi from -pi
+ * at e0 toward axis x e0), normalised binary32, row-major, into directions[3 * nt * np] (host).
+ * A frame that is not orthonormal to 1e-5 -> ICP_ERR_INVALID_ARGUMENT.  Host function. */
+int icp_query_directions(uint32_t theta_count, uint32_t phi_count, const float axis[3], const float e0[3],
+                         float* directions);
+
+/* All-hit query of the patches (device arrays from icp_patch_build) for every direction:
+ * each patch whose padded box the ray t d (0 <= t <= 4) meets is intersected (binary32, and
+ * binary64 where binary32 is not conclusive: BilinearPatchIntersector, include/rainbow/
+ * bilinear_patch_intersection.hpp), and each direction's hits are stored sorted by
+ * (patch_id, compact index, root) with duplicates removed, as the reference's OptiX query and
+ * PatchHitCollector produce them (shaders/entry/patch_query.cu, include/rainbow/
+ * patch_query_data.hpp:43-128).  d_offsets[direction_count + 1] (device) always; *hit_count
+ * (host) = d_offsets[direction_count].  With d_hits == NULL or d_summaries == NULL the call only
+ * sizes; otherwise d_hits needs hit_capacity >= *hit_count (else ICP_ERR_CAPACITY) and
+ * d_summaries[direction_count] receives the summaries.  Replaces PatchQuery::query_grid's two
+ * OptiX launches (src/patch_query.cpp). */
+int icp_patch_query(icp_context* ctx, const icp_outgoing_vertex* d_vertices, uint32_t vertex_count,
+                    const icp_outgoing_patch* d_patches, const icp_patch_aabb* d_aabbs, uint32_t patch_count,
+                    const icp_vec3f* d_directions, uint32_t direction_count, uint64_t* d_offsets,
+                    icp_query_summary* d_summaries, icp_query_hit* d_hits, uint64_t hit_capacity, uint64_t* hit_count);
 
 /* Optics of every query direction: d_results[direction_count] (device).  With focal != NULL
  * also the focal stage d_focal[direction_count] (device; the input of icp_rainbow_diffraction).

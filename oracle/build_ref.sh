@@ -18,6 +18,8 @@
 #                                        (include/rainbow/patch_optical_evaluator.hpp)
 #   oracle/_ref/ref_patch_harness        oracle/ref_patch_harness.cpp over the header-only patch
 #                                        construction (include/rainbow/patch_geometry.hpp)
+#   oracle/_ref/ref_query_harness        oracle/ref_query_harness.cpp over the header-only ray / patch
+#                                        intersection and query direction grid
 #
 # Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
 set -euo pipefail
@@ -44,6 +46,8 @@ g++ -std=c++20 -O2 -fno-fast-math -ffp-contract=off -I"$ref/include" "$here/ref_
     -o "$out/ref_optics_harness"
 g++ -std=c++20 -O2 -fno-fast-math -ffp-contract=off -I"$ref/include" "$here/ref_patch_harness.cpp" \
     -o "$out/ref_patch_harness"
+g++ -std=c++20 -O2 -fno-fast-math -ffp-contract=off -I"$ref/include" "$here/ref_query_harness.cpp" \
+    -o "$out/ref_query_harness"
 if [ -f "$ref/hex_atlas/src/ice_optics.cpp" ]; then
     g++ -std=c++20 -O2 -fno-fast-math -ffp-contract=off -I"$ref/hex_atlas/include" "$here/ref_ice_harness.cpp" \
         "$ref/hex_atlas/src/ice_optics.cpp" -o "$out/ref_ice_harness"
@@ -53,4 +57,4 @@ if [ -f "$ref/hex_atlas/src/ice_optics.cpp" ]; then
         "$ref/hex_atlas/src/atlas.cpp" "$ref/hex_atlas/src/ice_optics.cpp" "$ref/hex_trace/src/hex_trace.cpp" \
         "$ref/src/npy_writer.cpp" -o "$out/ice_precompute_atlas_cpu"
 fi
-echo "built $out/ice_generate_phase_cpu $out/ref_hex_harness $out/ref_drop_harness $out/ref_ice_harness $out/ref_atlas_harness $out/ice_precompute_atlas_cpu $out/ref_rainbow_harness $out/ref_optics_harness $out/ref_patch_harness"
+echo "built $out/ice_generate_phase_cpu $out/ref_hex_harness $out/ref_drop_harness $out/ref_ice_harness $out/ref_atlas_harness $out/ice_precompute_atlas_cpu $out/ref_rainbow_harness $out/ref_optics_harness $out/ref_patch_harness $out/ref_query_harness"

@@ -2612,3 +2612,333 @@ uint32_t icpo_patch_build(const pvertex* vertices, uint32_t width, uint32_t heig
     }
     return count;
 }
+
+/* ------------------------------------------------ ray / bilinear patch intersection
+ * Restates BilinearPatchIntersector::intersect (include/rainbow/bilinear_patch_intersection.hpp
+ * :58-314): the patch and the ray projected along the ray's dominant axis, the quadratic in u
+ * with scaled coefficients, three Newton steps in (u, v), the acceptance tests, first in binary32
+ * and, when that is not conclusive, again in binary64.  One generic body instantiated for both
+ * types by the macro below; same operations and order as the reference's template. */
+typedef struct { float u, v, t, residual; uint32_t flags; } pbhit;
+typedef struct { pbhit hits[2]; uint32_t count, flags; } pbhits;
+enum { BH_BOUNDARY = 1, BH_SINGULAR = 2, BH_FP64 = 4 };
+enum { BQ_UNRESOLVED = 1, BQ_INVALID = 2, BQ_FP64 = 4 };
+
+#define PB_SOLVER(T, SUF, FMA, SQRT, COPYSIGN, EPS, IS_FLOAT)                                                       \
+    typedef struct { T x, y; } pb2##SUF;                                                                            \
+    typedef struct { T x, y, z; } pb3##SUF;                                                                         \
+    static T pb_abs_##SUF(T x) { return x < (T)0 ? -x : x; }                                                         \
+    static T pb_max_##SUF(T a, T b) { return a > b ? a : b; }                                                        \
+    static T pb_dop##SUF(T x, T y, T z, T w) { const T zw = z * w; return FMA(x, y, -zw) + FMA(-z, w, zw); }        \
+    static pb2##SUF pb2_add##SUF(pb2##SUF a, pb2##SUF b) { pb2##SUF r = {a.x + b.x, a.y + b.y}; return r; }          \
+    static pb2##SUF pb2_mul##SUF(pb2##SUF a, T s) { pb2##SUF r = {a.x * s, a.y * s}; return r; }                    \
+    static T pb2_big##SUF(pb2##SUF a) { return pb_max_##SUF(pb_abs_##SUF(a.x), pb_abs_##SUF(a.y)); }                   \
+    static T pb2_cross##SUF(pb2##SUF a, pb2##SUF b) { return pb_dop##SUF(a.x, b.y, a.y, b.x); }                     \
+    static T pb3_c##SUF(pb3##SUF p, unsigned k) { return k == 0 ? p.x : (k == 1 ? p.y : p.z); }                    \
+    static pb3##SUF pb3_sub##SUF(pb3##SUF a, pb3##SUF b) { pb3##SUF r = {a.x - b.x, a.y - b.y, a.z - b.z}; return r; } \
+    static pb3##SUF pb3_add##SUF(pb3##SUF a, pb3##SUF b) { pb3##SUF r = {a.x + b.x, a.y + b.y, a.z + b.z}; return r; } \
+    static pb3##SUF pb3_mul##SUF(pb3##SUF a, T s) { pb3##SUF r = {a.x * s, a.y * s, a.z * s}; return r; }           \
+    static pb2##SUF pb_project##SUF(pb3##SUF p, pb3##SUF w, unsigned kz)                                            \
+    {                                                                                                               \
+        const unsigned kx = (kz + 1) % 3, ky = (kz + 2) % 3;                                                        \
+        const T z = pb3_c##SUF(w, kz);                                                                              \
+        pb2##SUF r = {pb_dop##SUF(z, pb3_c##SUF(p, kx), pb3_c##SUF(w, kx), pb3_c##SUF(p, kz)),                       \
+                      pb_dop##SUF(z, pb3_c##SUF(p, ky), pb3_c##SUF(w, ky), pb3_c##SUF(p, kz))};                      \
+        return r;                                                                                                   \
+    }                                                                                                               \
+    static int pb_solve##SUF(const pf3* corner, pf3 dir, pbhits* out)                                               \
+    {                                                                                                               \
+        int retry = 0;                                                                                              \
+        memset(out, 0, sizeof *out);                                                                                \
+        const pb3##SUF w = {(T)dir.x, (T)dir.y, (T)dir.z};                                                          \
+        unsigned kz = 0;                                                                                            \
+        if (pb_abs_##SUF(w.y) > pb_abs_##SUF(w.x)) kz = 1;                                                            \
+        if (pb_abs_##SUF(w.z) > pb_abs_##SUF(pb3_c##SUF(w, kz))) kz = 2;                                              \
+        const pb3##SUF p0 = {(T)corner[0].x, (T)corner[0].y, (T)corner[0].z};                                       \
+        const pb3##SUF p1 = {(T)corner[1].x, (T)corner[1].y, (T)corner[1].z};                                       \
+        const pb3##SUF p2 = {(T)corner[2].x, (T)corner[2].y, (T)corner[2].z};                                       \
+        const pb3##SUF p3 = {(T)corner[3].x, (T)corner[3].y, (T)corner[3].z};                                       \
+        const pb3##SUF eu = pb3_sub##SUF(p1, p0), ev = pb3_sub##SUF(p2, p0);                                        \
+        const pb3##SUF tw = pb3_sub##SUF(pb3_sub##SUF(p3, p2), eu);                                                 \
+        pb2##SUF a = pb_project##SUF(p0, w, kz), b = pb_project##SUF(eu, w, kz);                                    \
+        pb2##SUF c = pb_project##SUF(ev, w, kz), d = pb_project##SUF(tw, w, kz);                                    \
+        const T scale = pb_max_##SUF(pb_max_##SUF(pb2_big##SUF(a), pb2_big##SUF(b)),                                  \
+                                    pb_max_##SUF(pb2_big##SUF(c), pb2_big##SUF(d)));                                 \
+        if (!(scale > (T)0)) return 1;                                                                              \
+        a = pb2_mul##SUF(a, (T)1 / scale); b = pb2_mul##SUF(b, (T)1 / scale);                                       \
+        c = pb2_mul##SUF(c, (T)1 / scale); d = pb2_mul##SUF(d, (T)1 / scale);                                       \
+        const T eps = EPS;                                                                                          \
+        const pb2##SUF cs[4] = {a, pb2_add##SUF(a, b), pb2_add##SUF(a, c),                                          \
+                                pb2_add##SUF(pb2_add##SUF(pb2_add##SUF(a, b), c), d)};                              \
+        T xlo = cs[0].x, xhi = xlo, ylo = cs[0].y, yhi = ylo;                                                       \
+        for (unsigned i = 1; i < 4; ++i) {                                                                          \
+            xlo = xlo < cs[i].x ? xlo : cs[i].x;                                                                    \
+            xhi = pb_max_##SUF(xhi, cs[i].x);                                                                        \
+            ylo = ylo < cs[i].y ? ylo : cs[i].y;                                                                    \
+            yhi = pb_max_##SUF(yhi, cs[i].y);                                                                        \
+        }                                                                                                           \
+        const T guard = (T)64 * eps;                                                                                \
+        if (xlo > guard || xhi < -guard || ylo > guard || yhi < -guard) return 0;                                   \
+        const T A = pb2_cross##SUF(b, d), B = pb2_cross##SUF(a, d) + pb2_cross##SUF(b, c), Cc = pb2_cross##SUF(a, c); \
+        const T mag = pb_max_##SUF(pb_abs_##SUF(A), pb_max_##SUF(pb_abs_##SUF(B), pb_abs_##SUF(Cc)));                    \
+        if (!(mag > (T)0)) return 1;                                                                                \
+        const T qa = A / mag, qb = B / mag, qc = Cc / mag;                                                          \
+        if (IS_FLOAT && A != (T)0 && pb_abs_##SUF(qa) < (T)64 * eps) return 1;                                       \
+        T roots[2] = {0, 0};                                                                                        \
+        unsigned nroot = 0;                                                                                         \
+        int repeated = 0;                                                                                           \
+        if (A == (T)0) {                                                                                            \
+            if (B == (T)0) return pb_abs_##SUF(qc) <= guard;                                                         \
+            roots[nroot++] = -qc / qb;                                                                              \
+        } else {                                                                                                    \
+            const T disc = pb_dop##SUF(qb, qb, (T)4 * qa, qc);                                                      \
+            const T err = (T)64 * eps * (qb * qb + pb_abs_##SUF((T)4 * qa * qc));                                    \
+            if (disc < (T)0) return disc >= -err;                                                                   \
+            if (disc == (T)0) {                                                                                     \
+                if (IS_FLOAT) return 1;                                                                             \
+                roots[nroot++] = -qb / ((T)2 * qa);                                                                 \
+                repeated = 1;                                                                                       \
+            } else {                                                                                                \
+                if (disc <= err) return 1;                                                                          \
+                const T q = -(T)0.5 * (qb + COPYSIGN(SQRT(disc), qb));                                              \
+                roots[0] = q / qa;                                                                                  \
+                roots[1] = qc / q;                                                                                  \
+                if (roots[1] < roots[0]) { const T tmp = roots[0]; roots[0] = roots[1]; roots[1] = tmp; }           \
+                nroot = 2;                                                                                          \
+            }                                                                                                       \
+        }                                                                                                           \
+        for (unsigned r = 0; r < nroot; ++r) {                                                                      \
+            T u = roots[r];                                                                                         \
+            if (!(u == u)) { retry = 1; continue; }                                                                 \
+            if (u < -guard || u > (T)1 + guard) continue;                                                           \
+            const pb2##SUF num = pb2_add##SUF(a, pb2_mul##SUF(b, u)), den = pb2_add##SUF(c, pb2_mul##SUF(d, u));    \
+            if (pb2_big##SUF(den) <= guard) { retry = 1; continue; }                                                \
+            T v = pb_abs_##SUF(den.x) >= pb_abs_##SUF(den.y) ? -num.x / den.x : -num.y / den.y;                       \
+            if (!(v == v)) { retry = 1; continue; }                                                                 \
+            if (v < -guard || v > (T)1 + guard) continue;                                                           \
+            T cond = (T)1;                                                                                          \
+            for (unsigned it = 0; it < 3; ++it) {                                                                   \
+                const pb2##SUF fu = pb2_add##SUF(b, pb2_mul##SUF(d, v)), fv = pb2_add##SUF(c, pb2_mul##SUF(d, u));  \
+                const T det = pb2_cross##SUF(fu, fv);                                                               \
+                const pb2##SUF res = pb2_add##SUF(pb2_add##SUF(pb2_add##SUF(a, pb2_mul##SUF(b, u)),                 \
+                                                               pb2_mul##SUF(c, v)), pb2_mul##SUF(d, u * v));        \
+                if (pb_abs_##SUF(det) <= (T)64 * eps * pb2_big##SUF(fu) * pb2_big##SUF(fv)) {                        \
+                    if (!repeated) retry = 1;                                                                       \
+                    break;                                                                                          \
+                }                                                                                                   \
+                cond = pb_max_##SUF((T)1, pb_max_##SUF(pb2_big##SUF(fu), pb2_big##SUF(fv)) / pb_abs_##SUF(det));       \
+                const T du = pb2_cross##SUF(res, fv) / det, dv = pb2_cross##SUF(fu, res) / det;                     \
+                u -= du;                                                                                            \
+                v -= dv;                                                                                            \
+            }                                                                                                       \
+            const T perr = (T)32 * eps * cond;                                                                      \
+            if (IS_FLOAT && (perr > (T)2e-5 || u <= perr || u >= (T)1 - perr || v <= perr || v >= (T)1 - perr)) {   \
+                retry = 1;                                                                                          \
+                continue;                                                                                           \
+            }                                                                                                       \
+            if (perr > (T)1e-5 && !repeated) { retry = 1; continue; }                                               \
+            if (u < -perr || u > (T)1 + perr || v < -perr || v > (T)1 + perr) continue;                             \
+            const int boundary = u <= perr || u >= (T)1 - perr || v <= perr || v >= (T)1 - perr;                    \
+            if (u < (T)0 || u > (T)1) u = u < (T)0 ? (T)0 : (T)1;                                                   \
+            if (v < (T)0 || v > (T)1) v = v < (T)0 ? (T)0 : (T)1;                                                   \
+            const pb2##SUF res = pb2_add##SUF(pb2_add##SUF(pb2_add##SUF(a, pb2_mul##SUF(b, u)), pb2_mul##SUF(c, v)), \
+                                              pb2_mul##SUF(d, u * v));                                              \
+            if (pb2_big##SUF(res) > (T)256 * eps) { retry = 1; continue; }                                          \
+            const pb3##SUF lower = pb3_add##SUF(pb3_mul##SUF(p0, (T)1 - u), pb3_mul##SUF(p1, u));                   \
+            const pb3##SUF upper = pb3_add##SUF(pb3_mul##SUF(p2, (T)1 - u), pb3_mul##SUF(p3, u));                   \
+            const pb3##SUF point = pb3_add##SUF(pb3_mul##SUF(lower, (T)1 - v), pb3_mul##SUF(upper, v));             \
+            const T t = pb3_c##SUF(point, kz) / pb3_c##SUF(w, kz);                                                  \
+            if (!(t > (T)0)) {                                                                                      \
+                if (pb_abs_##SUF(t) <= (T)64 * eps) retry = 1;                                                       \
+                continue;                                                                                           \
+            }                                                                                                       \
+            pbhit hit = {(float)u, (float)v, (float)t, 0.0f, 0};                                                    \
+            if (boundary) hit.flags |= BH_BOUNDARY;                                                                 \
+            if (repeated) hit.flags |= BH_SINGULAR;                                                                 \
+            if (!IS_FLOAT) hit.flags |= BH_FP64;                                                                    \
+            const pf3 e3 = f3_sub(pb_eval(corner, hit.u, hit.v), f3_scale(dir, hit.t));                             \
+            hit.residual = pb_max_f(pb_abs_f(e3.x), pb_max_f(pb_abs_f(e3.y), pb_abs_f(e3.z)));                             \
+            if (!(hit.residual <= 0x1p-21f && hit.t < 4.0f)) { retry = 1; continue; }                               \
+            if (out->count < 2) out->hits[out->count++] = hit;                                                      \
+            else retry = 1;                                                                                         \
+        }                                                                                                           \
+        return retry;                                                                                               \
+    }
+
+/* |x| and max are the reference's x < 0 ? -x : x and a > b ? a : b, not fabsf / fmaxf (the sign
+ * of a zero and the NaN rule differ); the float instances serve the residual. */
+static float pb_abs_f(float x);
+static float pb_max_f(float a, float b);
+/* BilinearPatchGeometry::evaluate in binary32 */
+static pf3 pb_eval(const pf3* c, float u, float v)
+{
+    const pf3 lower = f3_add(f3_scale(c[0], 1.0f - u), f3_scale(c[1], u));
+    const pf3 upper = f3_add(f3_scale(c[2], 1.0f - u), f3_scale(c[3], u));
+    return f3_add(f3_scale(lower, 1.0f - v), f3_scale(upper, v));
+}
+PB_SOLVER(float, f, fmaf, sqrtf, copysignf, 0x1p-23f, 1)
+PB_SOLVER(double, d, fma, sqrt, copysign, 0x1p-52, 0)
+
+void icpo_bilinear_intersect(const float* corners /* 12 */, const float* direction /* 3 */, void* out /* pbhits */)
+{
+    pbhits* r = (pbhits*)out;
+    memset(r, 0, sizeof *r);
+    const pf3 dir = {direction[0], direction[1], direction[2]};
+    pf3 c[4];
+    for (unsigned i = 0; i < 4; ++i) {
+        c[i].x = corners[3 * i];
+        c[i].y = corners[3 * i + 1];
+        c[i].z = corners[3 * i + 2];
+    }
+    const float n2 = f3_dot(dir, dir);
+    if (!f3_fin(dir) || !(n2 > 0.99f && n2 < 1.01f)) {
+        r->flags = BQ_INVALID;
+        return;
+    }
+    for (unsigned i = 0; i < 4; ++i)
+        if (!f3_fin(c[i]) || !(f3_dot(c[i], c[i]) <= 4.0f)) {
+            r->flags = BQ_INVALID;
+            return;
+        }
+    if (pb_solvef(c, dir, r)) {
+        const int unresolved = pb_solved(c, dir, r);
+        r->flags |= BQ_FP64;
+        if (unresolved) r->flags |= BQ_UNRESOLVED;
+    }
+    if (r->count == 2) {
+        pbhit* a = &r->hits[0];
+        pbhit* b = &r->hits[1];
+        if (b->u < a->u || (b->u == a->u && b->v < a->v)) {
+            const pbhit t = *a;
+            *a = *b;
+            *b = t;
+        }
+    }
+}
+
+/* --------------------------------------------------------------- all-hit patch query
+ * Restates the reference's per-direction query (shaders/entry/patch_query.cu: raygen,
+ * intersection and any-hit programs; PatchHitCollector, include/rainbow/patch_query_data.hpp
+ * :43-128): every patch whose padded box the ray t d (0 <= t <= 4) meets is intersected, its
+ * roots collected, then sorted by (patch_id, compact index, root), duplicates removed and the
+ * summary counted.  The box test is a plain binary32 slab test (the reference leaves it to the
+ * OptiX traversal); the oracle tests every patch, the device bins them by direction first. */
+typedef struct { uint32_t compact, patch_id, root, flags; float u, v, t, residual; } pqhit;
+enum { PQ_UNRESOLVED = 1, PQ_INVALID = 2, PQ_MISMATCH = 4, PQ_REFINE = 8, PQ_BOUNDARY = 16, PQ_FP64 = 32,
+       PQ_DUPLICATE = 64, PQ_SINGULAR = 128, PQ_OVERFLOW = 256 };
+
+int icpo_ray_box(const float* dir, const paabb* b)
+{
+    const float lo[3] = {b->min_x, b->min_y, b->min_z}, hi[3] = {b->max_x, b->max_y, b->max_z};
+    float tnear = 0.0f, tfar = 4.0f;
+    for (unsigned a = 0; a < 3; ++a) {
+        if (dir[a] == 0.0f) {
+            if (lo[a] > 0.0f || hi[a] < 0.0f) return 0;
+            continue;
+        }
+        const float t1 = lo[a] / dir[a], t2 = hi[a] / dir[a];
+        const float tmin = t1 < t2 ? t1 : t2, tmax = t1 < t2 ? t2 : t1;
+        if (tmin > tnear) tnear = tmin;
+        if (tmax < tfar) tfar = tmax;
+    }
+    return tnear <= tfar;
+}
+static int pq_less(const pqhit* a, const pqhit* b)
+{
+    if (a->patch_id != b->patch_id) return a->patch_id < b->patch_id;
+    if (a->compact != b->compact) return a->compact < b->compact;
+    return a->root < b->root;
+}
+/* One direction: hits into out[capacity] (pass 2) or only counted (out == NULL, pass 1). */
+static void pq_direction(const pvertex* vertices, uint32_t vertex_count, const ppatch* patches, const paabb* boxes,
+                         uint32_t patch_count, const float* dir, pqhit* out, uint32_t capacity, psummary* sm)
+{
+    uint32_t count = 0, flags = 0, first = 0xffffffffu;
+    const float n2 = fmaf(dir[0], dir[0], fmaf(dir[1], dir[1], dir[2] * dir[2]));
+    const int finite_dir = dir[0] >= -0x1.fffffep127f && dir[0] <= 0x1.fffffep127f && dir[1] >= -0x1.fffffep127f &&
+                           dir[1] <= 0x1.fffffep127f && dir[2] >= -0x1.fffffep127f && dir[2] <= 0x1.fffffep127f;
+    if (!finite_dir || !(n2 > 0.99f && n2 < 1.01f))
+        flags |= PQ_INVALID;
+    else
+        for (uint32_t k = 0; k < patch_count; ++k) {
+            if (!icpo_ray_box(dir, boxes + k)) continue;
+            const ppatch* p = patches + k;
+            float corners[12];
+            int bad = 0;
+            for (unsigned i = 0; i < 4 && !bad; ++i) {
+                if (p->v[i] >= vertex_count) { bad = 1; break; }
+                const pf3 c = vertices[p->v[i]].direction;
+                corners[3 * i] = c.x; corners[3 * i + 1] = c.y; corners[3 * i + 2] = c.z;
+            }
+            if (bad) { flags |= PQ_INVALID; continue; }
+            pbhits h;
+            icpo_bilinear_intersect(corners, dir, &h);
+            if ((h.flags & (BQ_UNRESOLVED | BQ_INVALID)) && p->patch_id < first) first = p->patch_id;
+            if (h.flags & BQ_UNRESOLVED) flags |= PQ_UNRESOLVED;
+            if (h.flags & BQ_INVALID) flags |= PQ_INVALID;
+            if (h.flags & BQ_FP64) flags |= PQ_FP64;
+            for (uint32_t r = 0; r < h.count; ++r) {
+                if (out) {
+                    if (count >= capacity) flags |= PQ_MISMATCH;
+                    else {
+                        pqhit x = {k, p->patch_id, r, h.hits[r].flags, h.hits[r].u, h.hits[r].v, h.hits[r].t,
+                                   h.hits[r].residual};
+                        out[count] = x;
+                    }
+                }
+                ++count;
+            }
+        }
+    memset(sm, 0, sizeof *sm);
+    if (!out) { /* count pass */
+        sm->candidates = count;
+        sm->flags = flags;
+        sm->first_problem = first;
+        return;
+    }
+    sm->candidates = capacity;
+    if (count != capacity) flags |= PQ_MISMATCH;
+    sm->flags = flags;
+    sm->first_problem = first;
+    if (count > capacity) return;
+    for (uint32_t i = 1; i < count; ++i) { /* insertion sort: stable, as the reference */
+        const pqhit x = out[i];
+        uint32_t j = i;
+        while (j != 0 && pq_less(&x, out + j - 1)) { out[j] = out[j - 1]; --j; }
+        out[j] = x;
+    }
+    uint32_t kept = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        const pqhit h = out[i];
+        if (kept != 0 && h.compact == out[kept - 1].compact && h.root == out[kept - 1].root) {
+            sm->flags |= PQ_DUPLICATE;
+            continue;
+        }
+        if (h.compact >= patch_count) { sm->flags |= PQ_INVALID; continue; }
+        out[kept++] = h;
+        const uint32_t st = patches[h.compact].status;
+        if (st == 3u) { ++sm->refinement; sm->flags |= PQ_REFINE; }
+        else if (st == 1u || st == 2u) ++sm->regular;
+        else sm->flags |= PQ_INVALID;
+        if (h.flags & BH_BOUNDARY) { ++sm->boundary; sm->flags |= PQ_BOUNDARY; }
+        if (h.flags & BH_SINGULAR) sm->flags |= PQ_SINGULAR;
+    }
+    sm->hits = kept;
+}
+/* Both passes over all directions: offsets[n + 1], summaries[n]; hits written when
+ * hits != NULL (capacity offsets[n]).  Returns the total candidate count. */
+uint64_t icpo_patch_query(const pvertex* vertices, uint32_t vertex_count, const ppatch* patches, const paabb* boxes,
+                          uint32_t patch_count, const float* directions, uint32_t n, uint64_t* offsets,
+                          psummary* summaries, pqhit* hits)
+{
+    offsets[0] = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        pq_direction(vertices, vertex_count, patches, boxes, patch_count, directions + 3 * i, NULL, 0, summaries + i);
+        offsets[i + 1] = offsets[i] + summaries[i].candidates;
+    }
+    if (hits)
+        for (uint32_t i = 0; i < n; ++i)
+            pq_direction(vertices, vertex_count, patches, boxes, patch_count, directions + 3 * i, hits + offsets[i],
+                         (uint32_t)(offsets[i + 1] - offsets[i]), summaries + i);
+    return offsets[n];
+}

@@ -68,6 +68,10 @@ def _lib() -> C.CDLL:
     lib.icpo_rainbow_filter_at.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, _D, C.c_void_p,
                                            C.c_uint64, C.c_void_p]
     lib.icpo_patch_optics.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.icpo_bilinear_intersect.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.icpo_patch_query.restype = C.c_uint64
+    lib.icpo_patch_query.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
+                                     C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.icpo_patch_build.restype = C.c_uint32
     lib.icpo_patch_build.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float, C.c_void_p, C.c_void_p,
                                      C.c_void_p, C.c_void_p]
@@ -635,3 +639,63 @@ def ref_patch_build(blob: bytes, cells: int, workdir: Path | None = None):
     pa = np.frombuffer(raw[off:off + 32 * n], PATCH_DTYPE).copy()
     bx = np.frombuffer(raw[off + 32 * n:off + 56 * n], AABB_DTYPE).copy()
     return st, pa, bx, hist
+
+
+BILINEAR_HITS_DTYPE = np.dtype([("hits", [("u", "<f4"), ("v", "<f4"), ("t", "<f4"), ("residual", "<f4"),
+                                          ("flags", "<u4")], 2), ("count", "<u4"), ("flags", "<u4")])
+assert BILINEAR_HITS_DTYPE.itemsize == 48
+
+
+def bilinear_intersect(corners: np.ndarray, directions: np.ndarray) -> np.ndarray:
+    """Ray / bilinear patch hits for rows of (corners [n, 4, 3], directions [n, 3]), float32."""
+    c = np.ascontiguousarray(corners, dtype=np.float32).reshape(-1, 12)
+    d = np.ascontiguousarray(directions, dtype=np.float32).reshape(-1, 3)
+    out = np.zeros(len(c), dtype=BILINEAR_HITS_DTYPE)
+    for i in range(len(c)):
+        lib().icpo_bilinear_intersect(c[i].ctypes.data, d[i].ctypes.data, out[i:i + 1].ctypes.data)
+    return out
+
+
+def ref_bilinear_intersect(corners: np.ndarray, directions: np.ndarray, workdir: Path | None = None) -> np.ndarray:
+    c = np.ascontiguousarray(corners, dtype=np.float32).reshape(-1, 12)
+    d = np.ascontiguousarray(directions, dtype=np.float32).reshape(-1, 3)
+    base = Path(workdir or "/tmp") / f"ref_isect_{os.getpid()}"
+    src, dst = base.with_suffix(".in"), base.with_suffix(".out")
+    src.write_bytes(np.array([len(c)], "<u4").tobytes() + np.hstack([c, d]).astype("<f4").tobytes())
+    subprocess.run([str(REF_DIR / "ref_query_harness"), "intersect", str(src), str(dst)], check=True)
+    out = np.frombuffer(dst.read_bytes(), dtype=BILINEAR_HITS_DTYPE).copy()
+    src.unlink()
+    dst.unlink()
+    return out
+
+
+SUMMARY_DTYPE = np.dtype([(k, "<u4") for k in ("candidate_count", "hit_count", "regular_hits", "refinement_hits",
+                                               "boundary_hits", "flags", "first_problem_patch_id", "reserved")])
+HIT_DTYPE = np.dtype([("compact_index", "<u4"), ("patch_id", "<u4"), ("root_index", "<u4"), ("flags", "<u4"),
+                      ("u", "<f4"), ("v", "<f4"), ("t", "<f4"), ("residual", "<f4")])
+
+
+def patch_query(vertices, patches, aabbs, directions):
+    """All-hit query by brute force over every patch: (offsets [n + 1], summaries [n], hits)."""
+    v = np.ascontiguousarray(vertices)
+    p = np.ascontiguousarray(patches, dtype=PATCH_DTYPE)
+    b = np.ascontiguousarray(aabbs, dtype=AABB_DTYPE)
+    d = np.ascontiguousarray(directions, dtype=np.float32).reshape(-1, 3)
+    n = len(d)
+    offsets = np.zeros(n + 1, dtype=np.uint64)
+    summaries = np.zeros(n, dtype=SUMMARY_DTYPE)
+    total = lib().icpo_patch_query(v.ctypes.data, len(v), p.ctypes.data, b.ctypes.data, len(p), d.ctypes.data, n,
+                                   offsets.ctypes.data, summaries.ctypes.data, None)
+    hits = np.zeros(max(1, total), dtype=HIT_DTYPE)
+    lib().icpo_patch_query(v.ctypes.data, len(v), p.ctypes.data, b.ctypes.data, len(p), d.ctypes.data, n,
+                           offsets.ctypes.data, summaries.ctypes.data, hits.ctypes.data)
+    return offsets, summaries, hits[:total]
+
+
+def ref_query_directions(nt: int, np_: int, axis, e0, workdir: Path | None = None) -> np.ndarray:
+    out = Path(workdir or "/tmp") / f"ref_qdirs_{os.getpid()}.bin"
+    subprocess.run([str(REF_DIR / "ref_query_harness"), "directions", str(nt), str(np_),
+                    *[repr(float(x)) for x in axis], *[repr(float(x)) for x in e0], str(out)], check=True)
+    d = np.frombuffer(out.read_bytes(), dtype="<f4").reshape(-1, 3).copy()
+    out.unlink()
+    return d

@@ -345,6 +345,17 @@ def optics_fixtures(td: Path) -> None:
         out[f"patch.{name}.histogram"] = np.frombuffer(raw[4 * cells + 4:off], "<u4").copy()
         out[f"patch.{name}.patches"] = np.frombuffer(raw[off:off + 32 * n], OC.PATCH_DTYPE).copy()
         out[f"patch.{name}.aabbs"] = np.frombuffer(raw[off + 32 * n:off + 56 * n], OC.AABB_DTYPE).copy()
+    # ray / bilinear patch intersections and the query direction grid
+    corners, dirs = OC.intersection_pairs()
+    src, dst = td / "is.in", td / "is.out"
+    src.write_bytes(np.array([len(corners)], "<u4").tobytes() +
+                    np.hstack([corners.reshape(-1, 12), dirs]).astype("<f4").tobytes())
+    run([REF_BIN / "ref_query_harness", "intersect", src, dst])
+    out["intersect.digest"] = np.array(hashlib_hex(corners.tobytes() + dirs.tobytes()))
+    out["intersect.hits"] = np.frombuffer(dst.read_bytes(), dtype=OC.BILINEAR_HITS_DTYPE).copy()
+    for nt, np_, axis, e0 in OC.DIRECTION_GRIDS:
+        run([REF_BIN / "ref_query_harness", "directions", nt, np_, *map(repr, axis), *map(repr, e0), dst])
+        out[f"directions.{nt}x{np_}"] = np.frombuffer(dst.read_bytes(), "<f4").reshape(-1, 3).copy()
     np.savez_compressed(HERE / "optics_reference.npz", **out)
 
 

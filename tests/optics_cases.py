@@ -277,3 +277,49 @@ PATCH_CASES = [
 def serialize_lattice(vertices: np.ndarray, layout: tuple) -> bytes:
     w, h, e = layout
     return struct.pack("<IIf", w, h, e) + np.ascontiguousarray(vertices, dtype=VERTEX_DTYPE).tobytes()
+
+
+# ------------------------------------------------------------- intersection pairs
+def intersection_pairs(seed: int = 51, count: int = 3000) -> tuple[np.ndarray, np.ndarray]:
+    """(corners [n, 4, 3], directions [n, 3]) float32: patches of a folding lattice queried at
+    interior points, at points on and just outside their edges and corners, through folded
+    cells, far outside, and with invalid inputs."""
+    rng = np.random.default_rng(seed)
+    v, (w, h, _) = patch_lattice(seed, width=12, height=11, faults=False)
+    n = w * h
+    corners, dirs = [], []
+    cells = [(f, iy, ix) for f in range(4) for iy in range(h - 1) for ix in range(w - 1)]
+    while len(corners) < count:
+        f, iy, ix = cells[rng.integers(len(cells))]
+        first = f * n + iy * w + ix
+        idx = [first, first + 1, first + w, first + w + 1]
+        if not (v["status"][idx] == 1).all():
+            continue
+        c = v["direction"][idx].astype(np.float32)
+        kind = rng.integers(0, 6)
+        if kind <= 1:
+            u, t = rng.random(2)
+        elif kind == 2:
+            u, t = rng.choice([0.0, 1.0, 1e-7, 1 - 1e-7, 0.5]), rng.random()
+        elif kind == 3:
+            u, t = rng.uniform(-0.05, 1.05, 2)
+        else:
+            u, t = rng.uniform(-3, 4, 2)
+        p = ((1 - u) * c[0] + u * c[1]) * (1 - t) + ((1 - u) * c[2] + u * c[3]) * t
+        d = p / np.linalg.norm(p)
+        corners.append(c)
+        dirs.append(d.astype(np.float32))
+    corners, dirs = np.array(corners, dtype=np.float32), np.array(dirs, dtype=np.float32)
+    dirs[0] = [np.nan, 0, 1]
+    dirs[1] = dirs[1] * np.float32(1.2)
+    corners[2, 1] = [3.0, 0.0, 0.0]
+    corners[3, :] = corners[3, 0]  # a degenerate patch
+    return corners, dirs
+
+
+BILINEAR_HITS_DTYPE = np.dtype([("hits", [("u", "<f4"), ("v", "<f4"), ("t", "<f4"), ("residual", "<f4"),
+                                          ("flags", "<u4")], 2), ("count", "<u4"), ("flags", "<u4")])
+_K20 = (0.9396926164627075, -0.3420201539993286, 0.0)  # float32 (cos 20, -sin 20, 0)
+# (theta_count, phi_count, axis, e0) of the query grids pinned to the reference's QueryDirectionGrid
+DIRECTION_GRIDS = [(36, 72, _K20, (0.0, 0.0, 1.0)), (7, 5, (0.0, 0.0, 1.0), (1.0, 0.0, 0.0)),
+                   (90, 180, (0.0, -1.0, 0.0), (0.0, 0.0, 1.0))]

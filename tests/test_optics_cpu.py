@@ -140,3 +140,68 @@ def test_patch_build_live_reference(oracle):
         ref = oracle.ref_patch_build(OC.serialize_lattice(v, (w, h, e)), cells)
         got = oracle.patch_build(v, w, h, e)
         assert all(a.tobytes() == b.tobytes() for a, b in zip(got, ref))
+
+
+# ----------------------------------------------------------------- patch query
+def test_intersection_oracle_bit_identical_to_reference(oracle):
+    import hashlib
+    corners, dirs = OC.intersection_pairs()
+    assert hashlib.sha256(corners.tobytes() + dirs.tobytes()).hexdigest() == str(Z["intersect.digest"])
+    got = oracle.bilinear_intersect(corners, dirs)
+    want = Z["intersect.hits"]
+    assert got.tobytes() == want.tobytes()
+    assert set(np.unique(want["count"])) == {0, 1, 2} and (want["flags"] & 2).any() and (want["flags"] & 4).any()
+
+
+@pytest.mark.parametrize("grid", OC.DIRECTION_GRIDS, ids=lambda g: f"{g[0]}x{g[1]}")
+def test_query_directions_bit_identical_to_reference(icp, grid):
+    nt, np_, axis, e0 = grid
+    got = icp.query_directions(nt, np_, np.float32(axis), np.float32(e0))
+    assert got.tobytes() == Z[f"directions.{nt}x{np_}"].tobytes()
+
+
+def test_query_directions_reject_a_bad_frame(icp):
+    with pytest.raises(icp.InvalidArgument):
+        icp.query_directions(4, 4, (0.0, 0.0, 1.0), (0.0, 0.1, 1.0))
+    with pytest.raises(icp.InvalidArgument):
+        icp.query_directions(0, 4, (0.0, 0.0, 1.0), (1.0, 0.0, 0.0))
+
+
+def test_oracle_query_is_sorted_and_consistent(oracle, icp):
+    v, (w, h, e) = OC.patch_lattice(21)
+    st, pa, bx, hist = oracle.patch_build(v, w, h, e)
+    dirs = icp.query_directions(36, 72, np.float32(OC._K20), np.float32((0, 0, 1)))
+    off, sm, hits = oracle.patch_query(v, pa, bx, dirs)
+    assert off[-1] == len(hits) and (sm["candidate_count"] == np.diff(off)).all()
+    for i in np.flatnonzero(sm["hit_count"]):
+        hs = hits[off[i]:off[i] + sm["hit_count"][i]]
+        key = list(zip(hs["patch_id"], hs["compact_index"], hs["root_index"]))
+        assert key == sorted(set(key))
+        assert (hs["residual"] <= 2.0 ** -21).all() and (hs["t"] > 0).all() and (hs["t"] < 4).all()
+        # every hit point lies on its patch: the bilinear point along the query direction
+        for hit in hs:
+            c = v["direction"][pa["vertex_indices"][hit["compact_index"]]].astype(np.float64)
+            u, t = float(hit["u"]), float(hit["v"])
+            p = ((1 - u) * c[0] + u * c[1]) * (1 - t) + ((1 - u) * c[2] + u * c[3]) * t
+            assert np.allclose(p / np.linalg.norm(p), dirs[i], atol=1e-5)
+    assert (sm["regular_hits"] + sm["refinement_hits"] == sm["hit_count"]).all()
+
+
+def test_oracle_chain_lattice_to_diffraction(oracle, icp):
+    """Lattice -> patches -> query -> optics (focal) -> Table-II diffraction, on the CPU."""
+    import rainbow_cases  # noqa: F401  (the focal record layout)
+    v, (w, h, e) = OC.patch_lattice(22, width=17, height=13, faults=False)
+    st, pa, bx, hist = oracle.patch_build(v, w, h, e)
+    k, e0 = np.float32(OC._K20), np.float32((0, 0, 1))
+    nt, np_ = 45, 90
+    dirs = icp.query_directions(nt, np_, k, e0)
+    off, sm, hits = oracle.patch_query(v, pa, bx, dirs)
+    case = OC.OpticsInput(v, pa, dirs, off, sm, hits, None, k, e0, 0, (w, h, e, (0, 0, 0, 0)))
+    out, focal = oracle.patch_optics(case)
+    lit = sm["hit_count"] > 0
+    assert lit.sum() > 50 and (out["evaluated_hits"][lit] > 0).any()
+    assert np.isfinite(out["incoherent_s"][out["flags"] == 0]).all()
+    cfg = (2.0 * np.pi / 180, 4.0, 0.25, 3.0)
+    edges = oracle.rainbow_detect(focal, nt, np_, cfg)
+    res = oracle.rainbow_filter(focal, edges, nt, np_, cfg)
+    assert len(res) == nt * np_

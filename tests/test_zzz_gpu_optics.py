@@ -126,3 +126,47 @@ def test_patch_build_large_lattice_against_oracle(icp, ctx, oracle):
     st, pa, bx, hist = oracle.patch_build(v, w, h, e)
     assert np.array_equal(got.statuses, st) and got.histogram == [int(x) for x in hist]
     assert np.array_equal(got.patches["patch_id"], pa["patch_id"]) and got.aabbs.tobytes() == bx.tobytes()
+
+
+def _query_case(seed, width, height, nt, np_):
+    import ice_crystal_phase_b200 as icp
+    v, (w, h, e) = OC.patch_lattice(seed, width=width, height=height)
+    dirs = icp.query_directions(nt, np_, np.float32(OC._K20), np.float32((0, 0, 1)))
+    return v, (w, h, e), dirs
+
+
+@pytest.mark.parametrize("seed,width,height,nt,np_", [(21, 9, 8, 36, 72), (24, 33, 5, 60, 120), (41, 65, 65, 90, 180)])
+def test_patch_query_bit_identical_to_oracle(icp, ctx, oracle, seed, width, height, nt, np_):
+    """The binned device query equals the brute-force oracle (every patch box tested) bit for
+    bit: offsets, summaries and hits."""
+    v, (w, h, e), dirs = _query_case(seed, width, height, nt, np_)
+    st, pa, bx, hist = oracle.patch_build(v, w, h, e)
+    got = icp.patch_query(ctx, v, pa, bx, dirs)
+    off, sm, hits = oracle.patch_query(v, pa, bx, dirs)
+    assert np.array_equal(got.offsets, off)
+    assert got.summaries.tobytes() == sm.tobytes()
+    assert got.hits.tobytes() == hits.tobytes()
+    assert len(hits) > 0
+
+
+def test_device_chain_lattice_to_diffraction(icp, ctx, oracle):
+    """Patch build, query, optics and diffraction chained on the device from one lattice,
+    against the same chain in the oracle."""
+    v, (w, h, e) = OC.patch_lattice(22, width=17, height=13, faults=False)
+    k, e0 = np.float32(OC._K20), np.float32((0, 0, 1))
+    nt, np_ = 45, 90
+    dirs = icp.query_directions(nt, np_, k, e0)
+    pb = icp.patch_build(ctx, v, w, h, e)
+    q = icp.patch_query(ctx, v, pb.patches, pb.aabbs, dirs)
+    out, focal = icp.patch_optics(ctx, v, pb.patches, dirs, q.offsets, q.summaries, q.hits, k, e0,
+                                  focal=(w, h, e, (0, 0, 0, 0)))
+    st, pa, bx, hist = oracle.patch_build(v, w, h, e)
+    off, sm, hits = oracle.patch_query(v, pa, bx, dirs)
+    assert q.hits.tobytes() == hits.tobytes()
+    case = OC.OpticsInput(v, pa, dirs, off, sm, hits, None, k, e0, 0, (w, h, e, (0, 0, 0, 0)))
+    want, wfocal = oracle.patch_optics(case)
+    assert not optics_mismatch(out, want)
+    assert not focal_mismatch(focal, wfocal)
+    cfg = icp.DiffractionConfig(2.0 * np.pi / 180, 4.0, 0.25, 3.0)
+    d = icp.rainbow_diffraction(ctx, focal, nt, np_, cfg)
+    assert np.array_equal(d.transitions, oracle.rainbow_detect(wfocal, nt, np_, (cfg.primary_sigma_rad, 4.0, 0.25, 3.0)))
