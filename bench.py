@@ -798,6 +798,82 @@ def run_rainbow(I, ctx, stream, a) -> dict:
             "cpu_baseline": cpu}
 
 
+def run_wave(I, ctx, stream, a) -> dict:
+    """The device chain of the drop's wave stages at the reference CLI's defaults (513 x 513
+    lattice of four families, 360 x 720 query grid): patch build, all-hit query (sizing and fill
+    passes), patch optics with the focal stage, Table-II diffraction, on a seeded synthetic
+    lattice with a folding family; each stage timed with CUDA events on the context's stream."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    sys.path.insert(0, str(ROOT / "tests"))
+    import optics_cases as OC
+
+    w = h = 513
+    nt, np_ = 360, 720
+    v, second, (_, _, e) = OC.bench_lattice(w, h)
+    k, e0 = np.float32(OC._K20), np.float32((0, 0, 1))
+    dirs = I.query_directions(nt, np_, k, e0)
+    n, cells = nt * np_, 4 * (w - 1) * (h - 1)
+    dv = I.DeviceArray(ctx, len(v), I.VERTEX_DTYPE).upload(v)
+    d2 = I.DeviceArray(ctx, 4 * len(second), np.float32).upload(second.reshape(-1))
+    dp, db = I.DeviceArray(ctx, cells, I.PATCH_DTYPE), I.DeviceArray(ctx, cells, I.AABB_DTYPE)
+    dd = I.DeviceArray(ctx, 3 * n, np.float32).upload(dirs.reshape(-1))
+    do, ds = I.DeviceArray(ctx, n + 1, np.uint64), I.DeviceArray(ctx, n, I.SUMMARY_DTYPE)
+    dr, df = I.DeviceArray(ctx, n, I.OPTICAL_DTYPE), I.DeviceArray(ctx, n, I.FOCAL_DTYPE)
+    dt, dres, dden = I.DeviceArray(ctx, n, np.uint32), I.DeviceArray(ctx, n, I.DIFFRACTION_DTYPE), I.DeviceArray(ctx, n)
+    npatch, hits = C.c_uint32(0), C.c_uint64(0)
+    hist = (C.c_uint64 * 8)()
+    cfg = I.diffraction_config(0.5)
+    fc = I.FocalConfig(w, h, e, 0, (C.c_uint32 * 4)(0, 0, 0, 0))
+    stats = I.DiffractionStats()
+    state = {}
+
+    def build():
+        I.check(I.LIB.icp_patch_build(ctx.handle, dv.ptr, w, h, e, dp.ptr, db.ptr, None, C.byref(npatch), hist))
+
+    def query():
+        args = (ctx.handle, dv.ptr, len(v), dp.ptr, db.ptr, npatch.value, dd.ptr, n, do.ptr)
+        I.check(I.LIB.icp_patch_query(*args, None, None, 0, C.byref(hits)))
+        if "dh" not in state or state["dh"].count < hits.value:
+            state["dh"] = I.DeviceArray(ctx, max(1, hits.value), I.HIT_DTYPE)
+        I.check(I.LIB.icp_patch_query(*args, ds.ptr, state["dh"].ptr, state["dh"].count, C.byref(hits)))
+
+    def optics():
+        inp = I.OpticsInput(dv.ptr, dp.ptr, dd.ptr, do.ptr, ds.ptr, state["dh"].ptr, d2.ptr, hits.value, len(v),
+                            npatch.value, n, len(second), I.Vec3f(*map(float, k)), I.Vec3f(*map(float, e0)), 1, 0)
+        I.check(I.LIB.icp_patch_optics(ctx.handle, C.byref(inp), dr.ptr, C.byref(fc), df.ptr))
+
+    def diffraction():
+        I.check(I.LIB.icp_rainbow_diffraction(ctx.handle, df.ptr, nt, np_, C.byref(cfg), dt.ptr, dres.ptr, dden.ptr,
+                                              C.byref(stats)))
+
+    stages = {"patch_build": build, "patch_query": query, "patch_optics": optics, "rainbow_diffraction": diffraction}
+    for _ in range(3):
+        for f in stages.values():
+            f()
+    ms = {}
+    for name, f in stages.items():
+        times = []
+        for _ in range(max(1, a.wave_steps)):
+            e0v, e1v = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0v.record(stream)
+            f()
+            e1v.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0v.elapsed_time(e1v))
+        ms[name] = sorted(times)[len(times) // 2]
+    summaries = ds.download()
+    total = sum(ms.values())
+    return {"workload": "drop_wave_stages_lattice_513x513_query_360x720_synthetic", "lattice": [w, h],
+            "query": [nt, np_], "patches": npatch.value, "patch_status_histogram": list(hist), "hits": hits.value,
+            "incomplete_directions": int(((summaries["flags"] & (8 | 16 | 128 | 1 | 2 | 4 | 256)) != 0).sum()),
+            "ms_per_stage": ms, "ms_per_chain": total, "directions_per_s": n / (total / 1e3),
+            "filtered_directions": stats.filtered_directions}
+
+
 def _peaks() -> dict:
     try:
         return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
@@ -993,6 +1069,13 @@ def run_b200_drop(a) -> None:
         except (I.IcpError, RuntimeError, ValueError, OSError) as e:  # reported on the line, not fatal to it
             rainbow = {"error": f"{type(e).__name__}: {e}"}
 
+    wave = None
+    if world == 1 and a.wave_steps > 0:
+        try:
+            wave = run_wave(I, ctx, stream, a)
+        except (I.IcpError, RuntimeError, ValueError, OSError) as e:  # reported on the line, not fatal to it
+            wave = {"error": f"{type(e).__name__}: {e}"}
+
     s0 = stats_all[-1]
     r0 = reps[-1]
     line = {
@@ -1029,6 +1112,8 @@ def run_b200_drop(a) -> None:
         line["atlas"] = atlas
     if rainbow is not None:
         line["rainbow_diffraction"] = rainbow
+    if wave is not None:
+        line["wave_stages"] = wave
     if r0 is not None:
         line["record"] = {"g": r0.cdf.g_stored, "projected_area_mm2": r0.projected_area_mm2,
                           "incident_area_mm2": r0.incident_area_mm2, "diffraction_mm2": r0.diffraction_area_mm2,
@@ -1060,6 +1145,8 @@ def main() -> None:
                    help="incidences of the deterministic atlas composition measurement (0 = skip)")
     p.add_argument("--rainbow-steps", type=int, default=0,
                    help="timed passes of the Table-II rainbow diffraction measurement (0 = skip)")
+    p.add_argument("--wave-steps", type=int, default=0,
+                   help="timed passes of each wave-stage kernel chain (patch build, query, optics, diffraction; 0 = skip)")
     p.add_argument("--rays", type=float, default=1e8)
     p.add_argument("--ref-rays", type=float, default=1.6e6, help="reference rays per step (all processes)")
     p.add_argument("--no-cpu-baseline", action="store_true")

@@ -323,3 +323,35 @@ _K20 = (0.9396926164627075, -0.3420201539993286, 0.0)  # float32 (cos 20, -sin 2
 # (theta_count, phi_count, axis, e0) of the query grids pinned to the reference's QueryDirectionGrid
 DIRECTION_GRIDS = [(36, 72, _K20, (0.0, 0.0, 1.0)), (7, 5, (0.0, 0.0, 1.0), (1.0, 0.0, 0.0)),
                    (90, 180, (0.0, -1.0, 0.0), (0.0, 0.0, 1.0))]
+
+
+def bench_lattice(width: int, height: int, seed: int = 61) -> tuple[np.ndarray, np.ndarray, tuple]:
+    """A large four-family lattice (vectorised; the bench's input): smooth families, one folding
+    at the rainbow angle, misses on the rim; second response column.  (vertices, second, layout)"""
+    rng = np.random.default_rng(seed)
+    half = 1.01
+    k = np.array([math.cos(math.radians(20)), -math.sin(math.radians(20)), 0.0])
+    e0 = np.array([0.0, 0.0, 1.0])
+    e1 = np.cross(k, e0)
+    n = width * height
+    iy, ix = np.divmod(np.arange(n), width)
+    U = (2 * ix / (width - 1) - 1) * half
+    V = (2 * iy / (height - 1) - 1) * half
+    r2 = U * U + V * V
+    phi = np.arctan2(V, U)
+    v = np.zeros(4 * n, dtype=VERTEX_DTYPE)
+    for f, theta in enumerate((0.05 + 0.15 * r2, 2.9 - 0.3 * r2, 2.3 + 0.6 * r2 - 0.8 * r2 * r2, 2.2 + 0.2 * r2)):
+        d = np.cos(theta)[:, None] * k + np.sin(theta)[:, None] * (np.cos(phi + 0.3 * f)[:, None] * e0 +
+                                                                    np.sin(phi + 0.3 * f)[:, None] * e1)
+        d = _f32_unit(d)
+        axis = np.where(np.abs(d[:, 2:3]) < 0.9, np.array([0, 0, 1.0]), np.array([1.0, 0, 0]))
+        sl = slice(f * n, (f + 1) * n)
+        v["position"][sl] = np.column_stack([U, V, np.ones(n)]).astype(np.float32)
+        v["direction"][sl] = d
+        v["basis_x"][sl] = _f32_unit(axis - d * (d * axis).sum(axis=1, keepdims=True))
+        v["field"][sl] = rng.standard_normal((n, 4)).astype(np.float32)
+        v["turns"][sl] = (1000 + 3000 * r2).astype(np.int32)
+        v["fraction"][sl] = rng.random(n).astype(np.float32)
+        v["status"][sl] = np.where(r2 > 0.98 * half * half, 2, 1)
+    second = rng.standard_normal((4 * n, 4)).astype(np.float32)
+    return v, second, (width, height, half)
