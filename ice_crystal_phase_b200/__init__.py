@@ -24,6 +24,8 @@ Mirrored reference interfaces (Somatic-Cell/ice-crystal-phase):
   patch_query                      PatchQuery::query_grid (OptiX all-hit query), src/patch_query.cpp
   patch_optics                     PatchOptics::evaluate_device / evaluate_wave_device's kernels
                                    evaluate_patch_optics / evaluate_focal_optics, device/patch_optics.cu:7-24
+  stage_density / stage_record     density() + phase_check_density (device/phase_cdf.cu:40-108) and
+                                   the CDF input gate (src/phase_cdf.cpp:325-328) before PhaseCdf::build
   rainbow_table_sigma              include/rainbow/rainbow_diffraction.hpp:16-28
   diffraction_config               src/patch_optics.cpp:79-95 (the diffraction part of evaluate_wave_device)
   rainbow_diffraction              PatchOptics::run_diffraction + its statistics, src/patch_optics.cpp:217-231,
@@ -276,6 +278,17 @@ OPTICAL_DTYPE = np.dtype([("path_field", "<f8", 4), ("incoherent_s", "<f8"), ("i
 AABB_DTYPE = np.dtype([(k, "<f4") for k in ("min_x", "min_y", "min_z", "max_x", "max_y", "max_z")])
 
 
+class DensityReport(C.Structure):
+    _fields_ = [("maximum", C.c_double), ("invalid_values", C.c_uint64), ("incomplete", C.c_uint64),
+                ("underresolved", C.c_uint64), ("first_problem", C.c_uint64)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+WAVE_STAGES = {"incoherent": 1, "path": 2, "focal": 3, "diffraction": 4}
+
+
 class SurrogateConfig(C.Structure):
     _fields_ = [("nt", C.c_uint32), ("np", C.c_uint32), ("hidden", C.c_uint32), ("input_width", C.c_uint32),
                 ("theta_frequencies", C.c_uint32), ("phi_frequencies", C.c_uint32), ("max_records", C.c_uint32),
@@ -366,6 +379,7 @@ _FUNCS = {
     "icp_patch_query": (C.c_int, [_P, _P, C.c_uint32, _P, _P, C.c_uint32, _P, C.c_uint32, _P, _P, _P, C.c_uint64,
                                   C.POINTER(C.c_uint64)]),
     "icp_patch_optics": (C.c_int, [_P, C.POINTER(OpticsInput), _P, C.POINTER(FocalConfig), _P]),
+    "icp_stage_density": (C.c_int, [_P, C.c_uint32, _P, _P, _P, C.c_uint64, _P, C.POINTER(DensityReport)]),
     "icp_rainbow_table_sigma": (C.c_int, [C.c_float, _D]),
     "icp_rainbow_detect": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32, C.POINTER(DiffractionConfig), _P]),
     "icp_rainbow_filter": (C.c_int, [_P, _P, _P, C.c_uint32, C.c_uint32, C.POINTER(DiffractionConfig), _P, _P,
@@ -1297,3 +1311,43 @@ def patch_query(ctx: Context, vertices, patches, aabbs, directions) -> PatchQuer
     dh = DeviceArray(ctx, max(1, total.value), HIT_DTYPE)
     check(LIB.icp_patch_query(*args, ds.ptr, dh.ptr, max(1, total.value), C.byref(total)))
     return PatchQueryResult(do.download(), ds.download()[:n], dh.download()[:total.value])
+
+
+# ----------------------------------------------------------- wave-stage CDF input
+def _device(ctx: Context, a, dtype):
+    if a is None or isinstance(a, DeviceArray):
+        return a
+    a = np.ascontiguousarray(a, dtype=dtype).reshape(-1)
+    return DeviceArray(ctx, len(a), dtype).upload(a)
+
+
+def stage_density(ctx: Context, stage: str, optical, focal=None, diffraction=None) -> tuple[DeviceArray, dict]:
+    """The density of a wave stage per query direction (device) and the CDF builder's input
+    audit (maximum, invalid values, incomplete and underresolved directions, first problem)."""
+    do = _device(ctx, optical, OPTICAL_DTYPE)
+    df = _device(ctx, focal, FOCAL_DTYPE)
+    dr = _device(ctx, diffraction, DIFFRACTION_DTYPE)
+    dd = DeviceArray(ctx, do.count)
+    rep = DensityReport()
+    check(LIB.icp_stage_density(ctx.handle, WAVE_STAGES[stage], do.ptr, df.ptr if df else None, dr.ptr if dr else None,
+                                do.count, dd.ptr, C.byref(rep)))
+    return dd, rep.as_dict()
+
+
+def density_gate(report: dict, allow_underresolved: bool = False) -> None:
+    """The reference's CDF input gate: raises AuditError on an invalid value, an incomplete
+    direction, no positive density, or (unless allowed) an underresolved direction."""
+    if (report["invalid_values"] or report["incomplete"] or not report["maximum"] > 0
+            or (not allow_underresolved and report["underresolved"])):
+        raise AuditError(ICP_ERR_AUDIT, "CDF input rejected: max_intensity={maximum}, invalid_values={invalid_values}, "
+                                        "incomplete={incomplete}, underresolved={underresolved}".format(**report))
+
+
+def stage_record(ctx: Context, stage: str, nt: int, np_: int, optical, focal=None, diffraction=None,
+                 ct: int | None = None, cp: int | None = None, allow_underresolved: bool = False,
+                 **policy) -> CdfResult:
+    """A record of one wave stage from its per-direction results on the nt x np query grid:
+    density, input gate, then the stored CDF (PhaseCdf.build with density input)."""
+    dd, rep = stage_density(ctx, stage, optical, focal, diffraction)
+    density_gate(rep, allow_underresolved)
+    return PhaseCdf(ctx).build(dd, nt, np_, ct, cp, density=True, **policy)

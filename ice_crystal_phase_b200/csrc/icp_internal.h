@@ -272,5 +272,7 @@ struct icp_context {
     icp::Scratch patches;
     // patch query: direction bins, scans, per-direction counts; the bins' patch lists
     icp::Scratch query, query_list;
+    // wave-stage density audit accumulators
+    icp::Scratch stage_audit;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
 };

@@ -573,7 +573,96 @@ __global__ void __launch_bounds__(kThreads) patch_optics_kernel(const icp_optics
     }
 }
 
+// ------------------------------------------------------------ stage density and audit
+__global__ void __launch_bounds__(256) stage_density_kernel(uint32_t stage, const icp_optical_result* __restrict__ optical,
+                                                            const icp_focal_sample* __restrict__ focal,
+                                                            const icp_diffraction_result* __restrict__ diffraction,
+                                                            uint64_t count, double* __restrict__ density,
+                                                            unsigned long long* __restrict__ acc)
+{
+    // acc: [0] max (bits of a non-negative double), [1] invalid, [2] incomplete, [3] underresolved,
+    //      [4] first problem
+    unsigned long long invalid = 0, incomplete_n = 0, under_n = 0, first = ~0ull, maxbits = 0;
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += stride) {
+        const icp_optical_result& o = optical[i];
+        bool incomplete = (o.flags & (kErrors | kPending)) != 0u || o.rejected_hits != 0u || o.evaluated_hits != o.hit_count;
+        bool under = false;
+        double d;
+        if (stage == ICP_STAGE_INCOHERENT)
+            d = o.incoherent_s + o.incoherent_p;
+        else if (stage == ICP_STAGE_PATH)
+            d = o.path_s + o.path_p;
+        else {
+            incomplete = incomplete || focal[i].flags != 0u;
+            if (stage == ICP_STAGE_FOCAL)
+                d = focal[i].intensity_s + focal[i].intensity_p;
+            else {
+                const icp_diffraction_result& r = diffraction[i];
+                incomplete = incomplete || (r.flags & (ICP_DIFFRACTION_INPUT_UNAVAILABLE | ICP_DIFFRACTION_STENCIL_UNAVAILABLE |
+                                                       ICP_DIFFRACTION_DETECTION_UNAVAILABLE | ICP_DIFFRACTION_INVALID_DATA)) != 0u;
+                under = (r.flags & ICP_DIFFRACTION_UNDERRESOLVED) != 0u;
+                d = r.intensity_s + r.intensity_p;
+            }
+        }
+        density[i] = d;
+        const bool bad = !finite64(d) || d < 0;
+        invalid += bad;
+        incomplete_n += incomplete;
+        under_n += under;
+        if ((bad || incomplete || under) && i < first) first = i;
+        if (!bad) {
+            const unsigned long long bits = (unsigned long long)__double_as_longlong(d + 0.0); // -0 -> +0
+            if (bits > maxbits) maxbits = bits;
+        }
+    }
+    for (unsigned off = 16; off; off >>= 1) {
+        invalid += __shfl_down_sync(0xffffffffu, invalid, off);
+        incomplete_n += __shfl_down_sync(0xffffffffu, incomplete_n, off);
+        under_n += __shfl_down_sync(0xffffffffu, under_n, off);
+        const unsigned long long f = __shfl_down_sync(0xffffffffu, first, off);
+        const unsigned long long m = __shfl_down_sync(0xffffffffu, maxbits, off);
+        first = f < first ? f : first;
+        maxbits = m > maxbits ? m : maxbits;
+    }
+    if ((threadIdx.x & 31u) == 0) {
+        if (maxbits) atomicMax(&acc[0], maxbits);
+        if (invalid) atomicAdd(&acc[1], invalid);
+        if (incomplete_n) atomicAdd(&acc[2], incomplete_n);
+        if (under_n) atomicAdd(&acc[3], under_n);
+        if (first != ~0ull) atomicMin(&acc[4], first);
+    }
+}
+
 } // namespace
+
+extern "C" int icp_stage_density(icp_context* ctx, uint32_t stage, const icp_optical_result* d_optical,
+                                 const icp_focal_sample* d_focal, const icp_diffraction_result* d_diffraction,
+                                 uint64_t count, double* d_density, icp_density_report* report)
+{
+    if (!ctx || !d_optical || !d_density || !report || stage < ICP_STAGE_INCOHERENT || stage > ICP_STAGE_DIFFRACTION ||
+        (stage >= ICP_STAGE_FOCAL && !d_focal) || (stage == ICP_STAGE_DIFFRACTION && !d_diffraction))
+        return fail(ICP_ERR_INVALID_ARGUMENT, "icp_stage_density: invalid stage or null argument");
+    ICP_CUDA(cudaSetDevice(ctx->device));
+    ICP_CUDA(ctx->stage_audit.ensure(5 * sizeof(unsigned long long)));
+    auto* acc = static_cast<unsigned long long*>(ctx->stage_audit.ptr);
+    const unsigned long long init[5] = {0ull, 0ull, 0ull, 0ull, ~0ull};
+    ICP_CUDA(cudaMemcpyAsync(acc, init, sizeof init, cudaMemcpyHostToDevice, ctx->stream));
+    if (count) {
+        const uint64_t need = (count + 255) / 256, cap = uint64_t(ctx->sms > 0 ? ctx->sms : 148) * 8u;
+        stage_density_kernel<<<unsigned(need < cap ? need : cap), 256, 0, ctx->stream>>>(stage, d_optical, d_focal,
+                                                                                        d_diffraction, count, d_density, acc);
+        ICP_CUDA(cudaGetLastError());
+        count_launch();
+    }
+    unsigned long long got[5];
+    ICP_CUDA(cudaMemcpyAsync(got, acc, sizeof got, cudaMemcpyDeviceToHost, ctx->stream));
+    ICP_CUDA(cudaStreamSynchronize(ctx->stream));
+    double m;
+    std::memcpy(&m, &got[0], sizeof m);
+    *report = {m, got[1], got[2], got[3], got[4]};
+    return ok();
+}
 
 extern "C" int icp_patch_optics(icp_context* ctx, const icp_optics_input* input, icp_optical_result* d_results,
                                 const icp_focal_config* focal, icp_focal_sample* d_focal)

@@ -23,6 +23,7 @@
  *   icp_patch_build       PatchAccel::build's kernels    device/patch_build.cu:13-77
  *   icp_patch_query       PatchQuery::query_grid          src/patch_query.cpp, shaders/entry/patch_query.cu
  *   icp_patch_optics      evaluate_patch_optics / evaluate_focal_optics  device/patch_optics.cu:7-24
+ *   icp_stage_density     density() + phase_check_density device/phase_cdf.cu:40-56, 93-108
  *   icp_rainbow_*         RainbowDiffraction + PatchOptics::run_diffraction
  *                                                         include/rainbow/rainbow_diffraction.hpp,
  *                                                         src/patch_optics.cpp:334-348
@@ -760,6 +761,31 @@ int icp_patch_query(icp_context* ctx, const icp_outgoing_vertex* d_vertices, uin
  * only null pointers and sizes that overflow are rejected here. */
 int icp_patch_optics(icp_context* ctx, const icp_optics_input* input, icp_optical_result* d_results,
                      const icp_focal_config* focal, icp_focal_sample* d_focal);
+
+/* ------------------------------------------------------- wave-stage CDF input */
+/* The density a wave stage hands to the CDF builder and the builder's input audit
+ * (device/phase_cdf.cu:40-56, 93-108: density() and phase_check_density).  Per direction:
+ *   incoherent   incoherent_s + incoherent_p of d_optical
+ *   path         path_s + path_p of d_optical
+ *   focal        intensity_s + intensity_p of d_focal
+ *   diffraction  intensity_s + intensity_p of d_diffraction (underresolved when flagged)
+ * incomplete: the optical result's known hits are not complete (flags with an error or pending
+ * bit, a rejected hit, or evaluated != hit_count), and for focal / diffraction also an invalid
+ * focal or an unavailable diffraction result.  The reference rejects a record whose input has
+ * an invalid value (non-finite or negative), an incomplete direction, no positive density, or an
+ * underresolved direction unless allowed (src/phase_cdf.cpp:325-328); the report carries the
+ * counts, the host applies that gate.  d_density[count] (device) feeds icp_phase_cdf_build with
+ * ICP_CDF_DENSITY. */
+enum icp_wave_stage { ICP_STAGE_INCOHERENT = 1, ICP_STAGE_PATH = 2, ICP_STAGE_FOCAL = 3, ICP_STAGE_DIFFRACTION = 4 };
+typedef struct {
+    double maximum;            /* largest valid density                                      */
+    uint64_t invalid_values, incomplete, underresolved;
+    uint64_t first_problem;    /* first direction that is invalid, incomplete or underresolved;
+                                  UINT64_MAX when none                                        */
+} icp_density_report;
+int icp_stage_density(icp_context* ctx, uint32_t stage, const icp_optical_result* d_optical,
+                      const icp_focal_sample* d_focal, const icp_diffraction_result* d_diffraction, uint64_t count,
+                      double* d_density, icp_density_report* report);
 
 #ifdef __cplusplus
 }

@@ -205,3 +205,13 @@ def test_oracle_chain_lattice_to_diffraction(oracle, icp):
     edges = oracle.rainbow_detect(focal, nt, np_, cfg)
     res = oracle.rainbow_filter(focal, edges, nt, np_, cfg)
     assert len(res) == nt * np_
+
+
+def test_density_gate_mirrors_the_reference(icp):
+    ok = {"maximum": 2.0, "invalid_values": 0, "incomplete": 0, "underresolved": 0, "first_problem": 2 ** 64 - 1}
+    icp.density_gate(ok)
+    for bad in ({"invalid_values": 1}, {"incomplete": 3}, {"maximum": 0.0}, {"underresolved": 1}):
+        with pytest.raises(icp.AuditError):
+            icp.density_gate({**ok, **bad})
+    icp.density_gate({**ok, "underresolved": 5}, allow_underresolved=True)
+    assert icp.C.sizeof(icp.DensityReport) == 40 and icp.WAVE_STAGES["diffraction"] == 4

@@ -170,3 +170,36 @@ def test_device_chain_lattice_to_diffraction(icp, ctx, oracle):
     cfg = icp.DiffractionConfig(2.0 * np.pi / 180, 4.0, 0.25, 3.0)
     d = icp.rainbow_diffraction(ctx, focal, nt, np_, cfg)
     assert np.array_equal(d.transitions, oracle.rainbow_detect(wfocal, nt, np_, (cfg.primary_sigma_rad, 4.0, 0.25, 3.0)))
+
+
+def test_stage_density_and_audit(icp, ctx):
+    """Densities and the CDF input audit of every stage against the predicates of the
+    reference's density() and phase_check_density, on a faulty case (incomplete directions)."""
+    c = OC.lattice_case(1)
+    out, focal = run(icp, ctx, c)
+    n = c.count
+    cfg = icp.DiffractionConfig(3.0 * np.pi / 180, 4.0, 0.25, 3.0)
+    d = icp.rainbow_diffraction(ctx, focal, 10, n // 10, cfg) if n % 10 == 0 else None
+    complete = ((out["flags"] & 255) == 0) & (out["rejected_hits"] == 0) & (out["evaluated_hits"] == out["hit_count"])
+    for stage in ("incoherent", "path", "focal") + (("diffraction",) if d else ()):
+        dens, rep = icp.stage_density(ctx, stage, out, focal, d.results if d else None)
+        got = dens.download()
+        if stage == "incoherent":
+            want, inc, under = out["incoherent_s"] + out["incoherent_p"], ~complete, np.zeros(n, bool)
+        elif stage == "path":
+            want, inc, under = out["path_s"] + out["path_p"], ~complete, np.zeros(n, bool)
+        elif stage == "focal":
+            want, inc, under = focal["intensity_s"] + focal["intensity_p"], ~complete | (focal["flags"] != 0), np.zeros(n, bool)
+        else:
+            r = d.results
+            want = r["intensity_s"] + r["intensity_p"]
+            inc = ~complete | (focal["flags"] != 0) | ((r["flags"] & 60) != 0)
+            under = (r["flags"] & 2) != 0
+        assert np.array_equal(np.isnan(got), np.isnan(want)) and np.array_equal(got[~np.isnan(want)], want[~np.isnan(want)])
+        bad = ~np.isfinite(want) | (want < 0)
+        assert rep["invalid_values"] == bad.sum() and rep["incomplete"] == inc.sum() and rep["underresolved"] == under.sum()
+        assert rep["maximum"] == (want[~bad].max() if (~bad).any() else 0.0)
+        probs = np.flatnonzero(bad | inc | under)
+        assert rep["first_problem"] == (probs[0] if probs.size else 2 ** 64 - 1)
+    with pytest.raises(icp.AuditError):
+        icp.stage_record(ctx, "path", 10, n // 10, out)
