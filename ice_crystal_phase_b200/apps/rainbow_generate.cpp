@@ -10,8 +10,10 @@
 //     accepted and recorded only;
 //   * the optical model is the geometric R/T chain with Fresnel/Stokes splitting and up to
 //     --max-internal-hits interactions (stage "incoherent", the default here).  The reference's
-//     wave-optics patch stages (path, focal and its Table-II "diffraction") are not part of this
-//     build and are rejected by name;
+//     wave-optics patch stages (path, focal and its Table-II "diffraction") are rejected by name:
+//     the library has their device stages from an outgoing-ray lattice on (icp_patch_build,
+//     icp_patch_query, icp_patch_optics, icp_rainbow_diffraction, icp_stage_density), but not the
+//     lattice trace and folded patches that a record of those stages needs;
 //   * --diffraction analytic adds a separately reported Fraunhofer stage of the circle of equal
 //     traced area (default none);
 //   * --shape-coefficients c0,...,c7 replaces the Table-I shape of --radius-mm (which then only
@@ -225,7 +227,7 @@ bool parse(int argc, char** argv, Command& c)
     if (c.output.empty()) throw std::invalid_argument("--out is required.");
     if (!c.wavelength_given) throw std::invalid_argument("--wavelength-nm is required; there is no implicit wavelength.");
     if (stage != "incoherent")
-        throw std::invalid_argument("Stage " + stage + " is the reference's wave-optics patch model, which this build does not implement; use --stage incoherent (optionally with --diffraction analytic).");
+        throw std::invalid_argument("Stage " + stage + " is the reference's wave-optics patch model; its lattice trace and folded patches are not available here (the later stages are, through the library's icp_patch_* and icp_rainbow_* calls); use --stage incoherent (optionally with --diffraction analytic).");
     if (c.material == Material::Water) {
         if (c.index_given)
             throw std::invalid_argument("Do not specify --ior for water. It is evaluated from wavelength and state; use --material constant only for explicit reference calculations.");
