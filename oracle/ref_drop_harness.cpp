@@ -16,6 +16,9 @@
 //             The tracer's Jones columns are amplitude responses; the flux power multiplies
 //             0.5 (|col0|^2 + |col1|^2) by n_t cos_t / (n_i cos_i) of both transmissions,
 //             taken from the logged boundary queries.
+//   vertices  radius sphere n_int kx ky kz grid out.bin: the same lattice trace as raw records
+//             (u32 width, height; f32 half_extent, incident[3], basis_x[3]; OutgoingVertex[4 n];
+//             Field32[4 n], the second response column)
 //   time      radius sphere n_int kx ky kz grid row0 rows [c0 .. c7]: traces lattice rows
 //             [row0, row0+rows) with RaindropPathTracer::trace_vertex_unpolarized and prints
 //             "vertices hits seconds" (the reference's CPU drop tracer; optional coefficients
@@ -117,6 +120,39 @@ int families(int argc, char** argv)
     return n == out.size() ? 0 : 1;
 }
 
+// The reference's unpolarized lattice trace as raw records: u32 width, height; f32 half_extent,
+// incident[3], basis_x[3]; OutgoingVertex[4 * count]; Field32[4 * count] (second column).
+int vertices(int argc, char** argv)
+{
+    if (argc != 10) {
+        std::fprintf(stderr, "vertices radius sphere n_int kx ky kz grid out.bin\n");
+        return 1;
+    }
+    RaindropSettings s;
+    s.radius_mm = std::strtof(argv[2], nullptr);
+    s.force_sphere = std::atoi(argv[3]) != 0;
+    s.interior_index = std::strtof(argv[4], nullptr);
+    s.incident_direction = {std::strtof(argv[5], nullptr), std::strtof(argv[6], nullptr), std::strtof(argv[7], nullptr)};
+    s.grid_width = s.grid_height = (std::uint32_t)std::atoi(argv[8]);
+    const RaindropTraceConfig cfg = s.make_config();
+    const std::uint32_t count = cfg.vertex_count();
+    std::vector<OutgoingVertex> v(4 * (size_t)count);
+    std::vector<Field32> second(4 * (size_t)count);
+    RaindropIntersector intersector{cfg.shape};
+    for (std::uint32_t idx = 0; idx < count; ++idx)
+        RaindropPathTracer::trace_vertex_unpolarized(cfg, idx, intersector, v.data(), second.data());
+    FILE* fp = std::fopen(argv[9], "wb");
+    if (!fp) return 1;
+    const std::uint32_t wh[2] = {cfg.grid_width, cfg.grid_height};
+    const float frame[7] = {cfg.grid_half_extent, cfg.incident_direction.x, cfg.incident_direction.y,
+                            cfg.incident_direction.z, cfg.incident_basis_x.x, cfg.incident_basis_x.y,
+                            cfg.incident_basis_x.z};
+    bool ok = std::fwrite(wh, 4, 2, fp) == 2 && std::fwrite(frame, 4, 7, fp) == 7;
+    ok = ok && std::fwrite(v.data(), sizeof(OutgoingVertex), v.size(), fp) == v.size();
+    ok = ok && std::fwrite(second.data(), sizeof(Field32), second.size(), fp) == second.size();
+    return std::fclose(fp) == 0 && ok ? 0 : 1;
+}
+
 int time_rows(int argc, char** argv)
 {
     if (argc != 11 && argc != 19) {
@@ -165,13 +201,14 @@ int time_rows(int argc, char** argv)
 int main(int argc, char** argv)
 {
     if (argc < 2) {
-        std::fprintf(stderr, "usage: ref_drop_harness water|shape|area|frame|families ...\n");
+        std::fprintf(stderr, "usage: ref_drop_harness water|shape|area|frame|families|vertices ...\n");
         return 1;
     }
     const std::string mode = argv[1];
     std::cout.precision(17);
     try {
         if (mode == "families") return families(argc, argv);
+        if (mode == "vertices") return vertices(argc, argv);
         if (mode == "time") return time_rows(argc, argv);
         std::string line;
         while (std::getline(std::cin, line)) {

@@ -357,6 +357,17 @@ def optics_fixtures(td: Path) -> None:
         run([REF_BIN / "ref_query_harness", "directions", nt, np_, *map(repr, axis), *map(repr, e0), dst])
         out[f"directions.{nt}x{np_}"] = np.frombuffer(dst.read_bytes(), "<f4").reshape(-1, 3).copy()
     np.savez_compressed(HERE / "optics_reference.npz", **out)
+    # the reference's own unpolarized lattice trace of a 0.5 mm sphere (25 x 25 vertices, four
+    # families), the real input of the device chain from patch build to the stage densities
+    lat = td / "lattice.bin"
+    run([REF_BIN / "ref_drop_harness", "vertices", "0.5", "1", "1.3317", "0.9396926", "-0.3420201", "0", "25", lat])
+    raw = lat.read_bytes()
+    w, h = np.frombuffer(raw[:8], "<u4")
+    n = 4 * int(w) * int(h)
+    np.savez_compressed(HERE / "drop_lattice_reference.npz", shape=np.array([w, h], dtype=np.uint32),
+                        frame=np.frombuffer(raw[8:36], "<f4").copy(),
+                        vertices=np.frombuffer(raw[36:36 + 68 * n], OC.VERTEX_DTYPE).copy(),
+                        second=np.frombuffer(raw[36 + 68 * n:], "<f4").reshape(-1, 4).copy())
 
 
 def hashlib_hex(blob: bytes) -> str:

@@ -215,3 +215,37 @@ def test_density_gate_mirrors_the_reference(icp):
             icp.density_gate({**ok, **bad})
     icp.density_gate({**ok, "underresolved": 5}, allow_underresolved=True)
     assert icp.C.sizeof(icp.DensityReport) == 40 and icp.WAVE_STAGES["diffraction"] == 4
+
+
+# ------------------------------------------------- the reference's own drop lattice
+def reference_lattice():
+    z = np.load(GOLDEN / "drop_lattice_reference.npz")
+    w, h = (int(x) for x in z["shape"])
+    f = z["frame"]
+    return z["vertices"], z["second"], (w, h, float(f[0])), np.float32(f[1:4]), np.float32(f[4:7])
+
+
+def oracle_chain(oracle, icp, nt=90, np_=180):
+    v, second, (w, h, e), k, e0 = reference_lattice()
+    st, pa, bx, hist = oracle.patch_build(v, w, h, e)
+    dirs = icp.query_directions(nt, np_, k, e0)
+    off, sm, hits = oracle.patch_query(v, pa, bx, dirs)
+    case = OC.OpticsInput(v, pa, dirs, off, sm, hits, second, k, e0, 1, (w, h, e, (0, 0, 0, 0)))
+    out, focal = oracle.patch_optics(case)
+    return dict(v=v, second=second, layout=(w, h, e), k=k, e0=e0, patches=pa, boxes=bx, hist=hist, dirs=dirs,
+                offsets=off, summaries=sm, hits=hits, out=out, focal=focal)
+
+
+def test_reference_lattice_chain_on_the_cpu(oracle, icp):
+    """The reference's unpolarized lattice trace of a 0.5 mm sphere through the oracle chain:
+    every query direction of the 90 x 180 grid sees patches, all but the caustic's are complete,
+    and the four families appear in the focal stage."""
+    c = oracle_chain(oracle, icp)
+    sm, out, focal = c["summaries"], c["out"], c["focal"]
+    assert (sm["hit_count"] > 0).all()
+    complete = ((out["flags"] & 255) == 0) & (out["rejected_hits"] == 0) & (out["evaluated_hits"] == out["hit_count"])
+    assert complete.sum() > 0.99 * len(out)
+    incomplete = np.flatnonzero(~complete)
+    assert incomplete.size > 0 and (out["flags"][incomplete] & 32).all()  # refinement-pending: the folds
+    assert (focal["family_hits"][complete].sum(axis=0) > 0).all()
+    assert np.isfinite(out["path_s"][complete]).all() and (out["incoherent_s"][complete] > 0).all()

@@ -203,3 +203,28 @@ def test_stage_density_and_audit(icp, ctx):
         assert rep["first_problem"] == (probs[0] if probs.size else 2 ** 64 - 1)
     with pytest.raises(icp.AuditError):
         icp.stage_record(ctx, "path", 10, n // 10, out)
+
+
+def test_reference_lattice_device_chain(icp, ctx, oracle):
+    """The reference's own lattice trace of a 0.5 mm sphere through the whole device chain --
+    patch build, query, optics with the focal stage, Table-II diffraction, stage densities --
+    against the oracle chain."""
+    import test_optics_cpu as T
+    c = T.oracle_chain(oracle, icp)
+    v, second, (w, h, e), k, e0 = T.reference_lattice()
+    pb = icp.patch_build(ctx, v, w, h, e)
+    assert list(pb.histogram) == [int(x) for x in c["hist"]]
+    assert np.array_equal(pb.patches["patch_id"], c["patches"]["patch_id"]) and pb.aabbs.tobytes() == c["boxes"].tobytes()
+    q = icp.patch_query(ctx, v, c["patches"], c["boxes"], c["dirs"])
+    assert q.hits.tobytes() == c["hits"].tobytes() and q.summaries.tobytes() == c["summaries"].tobytes()
+    out, focal = icp.patch_optics(ctx, v, c["patches"], c["dirs"], q.offsets, q.summaries, q.hits, k, e0,
+                                  second=second, focal=(w, h, e, (0, 0, 0, 0)))
+    assert not optics_mismatch(out, c["out"])
+    assert not focal_mismatch(focal, c["focal"])
+    cfg = icp.diffraction_config(0.5)
+    d = icp.rainbow_diffraction(ctx, focal, 90, 180, cfg)
+    c4 = (cfg.primary_sigma_rad, cfg.support_sigma, cfg.transition_contrast, cfg.inner_blend_sigma)
+    assert np.array_equal(d.transitions, oracle.rainbow_detect(c["focal"], 90, 180, c4))
+    for stage in ("incoherent", "path", "focal", "diffraction"):
+        _, rep = icp.stage_density(ctx, stage, out, focal, d.results)
+        assert rep["incomplete"] > 0  # the caustic's refinement-pending directions
