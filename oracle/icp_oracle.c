@@ -19,9 +19,15 @@
  *   u edges                include/rainbow/phase_cdf_math.hpp:16-32
  *   quaternion rotation    hex_phase/src/phase_table.cpp:11-21
  *   Table-II diffraction   include/rainbow/rainbow_diffraction.hpp:16-174
+ *   patch optics           include/rainbow/patch_optical_evaluator.hpp:26-326 (+ transport,
+ *                          phase cycles, focal phase)
+ *   patch construction     include/rainbow/patch_geometry.hpp:75-172
+ *   ray / patch hits       include/rainbow/bilinear_patch_intersection.hpp:58-314
+ *   all-hit query          shaders/entry/patch_query.cu, include/rainbow/patch_query_data.hpp:43-128
  * Parity is pinned: tests compare this restatement bit-for-bit with the
  * reference sources compiled from their own files into oracle/_ref
- * (oracle/build_ref.sh) and with fixtures under tests/golden/.
+ * (oracle/build_ref.sh) and with fixtures under tests/golden/.  The query's box test is
+ * the one part with no reference counterpart to pin (the reference leaves it to OptiX).
  *
  * Build: oracle/build_oracle.sh (gcc -O2 -ffp-contract=off -fno-fast-math).
  */
