@@ -204,27 +204,132 @@ inline double water_index_r9_97(double wavelength_nm, double temperature_k, doub
     const double x = r * rhs;
     return std::sqrt((1 + 2 * x) / (1 - x));
 }
-// Liquid density (kg m^-3) of air-free water.  At 1 atm: Tanaka et al. (2001, Metrologia 38,
-// 301) below 35 C, Kell (1975, J. Chem. Eng. Data 20, 97) above 45 C, blended linearly in
-// between; pressure through the secant bulk modulus of pure water of the UNESCO 1981
-// equation of state, rho(p) = rho(1 atm) / (1 - p/K(t, p)), p gauge in bar.  The reference
-// inverts the IAPWS-95 pressure equation of state instead; against it this stays within
-// 0.036 kg m^-3 over 0..60 C and 50 kPa..100 MPa, i.e. n within 2.5e-6 up to 10 MPa and
-// 1.2e-5 up to 100 MPa.
-inline double water_density(double temperature_c, double pressure_pa)
+// ---------------------------------------------------------------- IAPWS-95 liquid density
+// Density of liquid water from the IAPWS-95 equation of state (IAPWS R6-95(2018); Wagner & Pruss,
+// J. Phys. Chem. Ref. Data 31, 387 (2002)): p = rho R T (1 + delta dphi_r/ddelta), delta =
+// rho / 322 kg m^-3, tau = 647.096 K / T, R = 461.51805 J kg^-1 K^-1, with all 56 terms of the
+// residual Helmholtz energy (Table 2 of the release: 7 polynomial, 44 exponential, 3 Gaussian,
+// 2 non-analytic), inverted for rho on the liquid branch by bisection.  The reference solves
+// the same equation (src/water_refractive_index.cpp:84-187); the density it reports is a
+// function of its operation order, so this evaluation keeps that order: terms in table order,
+// each as ((n delta^d) tau^t) e^(-delta^c) times its delta-derivative factor, added with the
+// compensated (Neumaier) sum; bisection on [970, 1060] kg m^-3 until the bracket is at most
+// 2e-10 wide, then the end with the smaller pressure residual.
+namespace iapws95 {
+
+struct Term {
+    double n, t;
+    int d, c; // c = 0: polynomial term (no exponential)
+};
+// n_i, t_i, d_i, c_i of the polynomial and exponential terms (IAPWS R6-95 Table 2, i = 1..51)
+inline const Term* terms()
 {
-    const double t = temperature_c;
-    const double tanaka = 999.974950 * (1 - (t - 3.983035) * (t - 3.983035) * (t + 301.797) / (522528.9 * (t + 69.34881)));
-    const double kell = (999.83952 + 16.945176 * t - 7.9870401e-3 * t * t - 46.170461e-6 * t * t * t +
-                         105.56302e-9 * t * t * t * t - 280.54253e-12 * t * t * t * t * t) /
-                        (1 + 16.879850e-3 * t);
-    const double w = std::min(1.0, std::max(0.0, (t - 35.0) / 10.0));
-    const double rho0 = (1 - w) * tanaka + w * kell;
-    const double pb = (pressure_pa - 101325.0) * 1e-5;
-    const double k0 = 19652.21 + 148.4206 * t - 2.327105 * t * t + 1.360477e-2 * t * t * t - 5.155288e-5 * t * t * t * t;
-    const double ka = 3.239908 + 1.43713e-3 * t + 1.16092e-4 * t * t - 5.77905e-7 * t * t * t;
-    const double kb = 8.50935e-5 - 6.12293e-6 * t + 5.2787e-8 * t * t;
-    return rho0 / (1 - pb / (k0 + ka * pb + kb * pb * pb));
+    static const Term k[51] = {
+        {0.12533547935523e-1, -0.5, 1, 0},    {0.78957634722828e1, 0.875, 1, 0},   {-0.87803203303561e1, 1.0, 1, 0},
+        {0.31802509345418, 0.5, 2, 0},        {-0.26145533859358, 0.75, 2, 0},     {-0.78199751687981e-2, 0.375, 3, 0},
+        {0.88089493102134e-2, 1.0, 4, 0},     {-0.66856572307965, 4.0, 1, 1},      {0.20433810950965, 6.0, 1, 1},
+        {-0.66212605039687e-4, 12.0, 1, 1},   {-0.19232721156002, 1.0, 2, 1},      {-0.25709043003438, 5.0, 2, 1},
+        {0.16074868486251, 4.0, 3, 1},        {-0.40092828925807e-1, 2.0, 4, 1},   {0.39343422603254e-6, 13.0, 4, 1},
+        {-0.75941377088144e-5, 9.0, 5, 1},    {0.56250979351888e-3, 3.0, 7, 1},    {-0.15608652257135e-4, 4.0, 9, 1},
+        {0.11537996422951e-8, 11.0, 10, 1},   {0.36582165144204e-6, 4.0, 11, 1},   {-0.13251180074668e-11, 13.0, 13, 1},
+        {-0.62639586912454e-9, 1.0, 15, 1},   {-0.10793600908932, 7.0, 1, 2},      {0.17611491008752e-1, 1.0, 2, 2},
+        {0.22132295167546, 9.0, 2, 2},        {-0.40247669763528, 10.0, 2, 2},     {0.58083399985759, 10.0, 3, 2},
+        {0.49969146990806e-2, 3.0, 4, 2},     {-0.31358700712549e-1, 7.0, 4, 2},   {-0.74315929710341, 10.0, 4, 2},
+        {0.47807329915480, 10.0, 5, 2},       {0.20527940895948e-1, 6.0, 6, 2},    {-0.13636435110343, 10.0, 6, 2},
+        {0.14180634400617e-1, 10.0, 7, 2},    {0.83326504880713e-2, 1.0, 9, 2},    {-0.29052336009585e-1, 2.0, 9, 2},
+        {0.38615085574206e-1, 3.0, 9, 2},     {-0.20393486513704e-1, 4.0, 9, 2},   {-0.16554050063734e-2, 8.0, 9, 2},
+        {0.19955571979541e-2, 6.0, 10, 2},    {0.15870308324157e-3, 9.0, 10, 2},   {-0.16388568342530e-4, 8.0, 12, 2},
+        {0.43613615723811e-1, 16.0, 3, 3},    {0.34994005463765e-1, 22.0, 4, 3},   {-0.76788197844621e-1, 23.0, 4, 3},
+        {0.22446277332006e-1, 23.0, 5, 3},    {-0.62689710414685e-4, 10.0, 14, 4}, {-0.55711118565645e-9, 50.0, 3, 6},
+        {-0.19905718354408, 44.0, 6, 6},      {0.31777497330738, 46.0, 6, 6},      {-0.11841182425981, 50.0, 6, 6}};
+    return k;
+}
+
+// Compensated sum (Neumaier 1974): the rounding error of each addition is carried separately.
+struct NSum {
+    double s = 0.0, e = 0.0;
+    void add(double x)
+    {
+        const double t = s + x;
+        e += std::fabs(s) >= std::fabs(x) ? (s - t) + x : (x - t) + s;
+        s = t;
+    }
+    double value() const { return s + e; }
+};
+
+// delta * d(phi_r)/d(delta)
+inline double delta_phir_delta(double delta, double tau)
+{
+    NSum sum;
+    const Term* k = terms();
+    for (int i = 0; i < 51; ++i) {
+        const Term& a = k[i];
+        const double dc = a.c ? std::pow(delta, double(a.c)) : 0.0;
+        const double term = a.n * std::pow(delta, double(a.d)) * std::pow(tau, a.t) * (a.c ? std::exp(-dc) : 1.0);
+        sum.add(term * (double(a.d) - double(a.c) * dc));
+    }
+    // Gaussian bell terms i = 52..54: d = 3, epsilon = 1 (n, t, alpha, beta, gamma)
+    static const double gauss[3][5] = {{-0.31306260323435e2, 0.0, 20.0, 150.0, 1.21},
+                                       {0.31546140237781e2, 1.0, 20.0, 150.0, 1.21},
+                                       {-0.25213154341695e4, 4.0, 20.0, 250.0, 1.25}};
+    for (const auto& g : gauss) {
+        const double x = delta - 1.0, y = tau - g[4];
+        const double term = g[0] * delta * delta * delta * std::pow(tau, g[1]) * std::exp(-g[2] * x * x - g[3] * y * y);
+        sum.add(term * (3.0 - 2.0 * g[2] * delta * x));
+    }
+    // non-analytic terms i = 55, 56 (n, b, C, D) with a = 3.5, beta = 0.3, A = 0.32, B = 0.2; the
+    // liquid bracket stays far from delta = 1, where their derivatives need no special case
+    static const double crit[2][4] = {{-0.14874640856724, 0.85, 28.0, 700.0}, {0.31806110878444, 0.95, 32.0, 800.0}};
+    const double x = delta - 1.0, x2 = x * x;
+    const double A = 0.32, B = 0.2, ea = 3.5, eb = 0.3;
+    const double theta = 1.0 - tau + A * std::pow(x2, 1.0 / (2.0 * eb));
+    const double theta_d = A / eb * x * std::pow(x2, 1.0 / (2.0 * eb) - 1.0);
+    const double dist = theta * theta + B * std::pow(x2, ea);
+    const double dist_d = 2.0 * theta * theta_d + 2.0 * B * ea * x * std::pow(x2, ea - 1.0);
+    for (const auto& v : crit) {
+        const double psi = std::exp(-v[2] * x2 - v[3] * (tau - 1.0) * (tau - 1.0));
+        const double term = v[0] * delta * std::pow(dist, v[1]) * psi;
+        sum.add(term * (1.0 + delta * (v[1] * dist_d / dist - 2.0 * v[2] * x)));
+    }
+    return sum.value();
+}
+
+inline double pressure(double temperature_k, double density)
+{
+    const double R = 461.51805, Tc = 647.096, rhoc = 322.0; // the release's constants
+    return density * R * temperature_k * (1.0 + delta_phir_delta(density / rhoc, Tc / temperature_k));
+}
+
+} // namespace iapws95
+
+// Liquid density (kg m^-3) at T (K) and p (Pa); throws std::runtime_error where the reference's
+// solve fails (no bracket, nonfinite pressure, residual above 0.02 Pa, no convergence).
+inline double water_density(double temperature_k, double pressure_pa)
+{
+    double lo = 970.0, hi = 1060.0;
+    double flo = iapws95::pressure(temperature_k, lo) - pressure_pa;
+    double fhi = iapws95::pressure(temperature_k, hi) - pressure_pa;
+    if (!(std::isfinite(flo) && std::isfinite(fhi) && flo < 0.0 && fhi > 0.0))
+        throw std::runtime_error("IAPWS-95: liquid density bracket unavailable.");
+    for (int it = 0; it < 100; ++it) {
+        const double mid = (lo + hi) / 2; // std::midpoint of two finite doubles of this range
+        const double fm = iapws95::pressure(temperature_k, mid) - pressure_pa;
+        if (!std::isfinite(fm)) throw std::runtime_error("IAPWS-95: nonfinite pressure.");
+        if (fm < 0.0) {
+            lo = mid;
+            flo = fm;
+        } else {
+            hi = mid;
+            fhi = fm;
+        }
+        if (hi - lo <= 2e-10) {
+            const bool take_lo = std::fabs(flo) < std::fabs(fhi);
+            if (std::fabs(take_lo ? flo : fhi) > 0.02)
+                throw std::runtime_error("IAPWS-95: density pressure residual is too large.");
+            return take_lo ? lo : hi;
+        }
+    }
+    throw std::runtime_error("IAPWS-95: liquid density solve did not converge.");
 }
 struct WaterState {
     double index = 0, density = 0, temperature_k = 0, pressure_pa = 0;
@@ -239,7 +344,7 @@ inline WaterState water_optics(double wavelength_nm, double temperature_c = 20.0
     WaterState s;
     s.temperature_k = temperature_c + 273.15;
     s.pressure_pa = pressure_pa;
-    s.density = water_density(temperature_c, pressure_pa);
+    s.density = water_density(s.temperature_k, pressure_pa);
     s.index = water_index_r9_97(wavelength_nm, s.temperature_k, s.density);
     return s;
 }

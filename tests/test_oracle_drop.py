@@ -15,6 +15,7 @@ import numpy as np
 import pytest
 
 from conftest import GOLDEN
+from oracle import oracle as oracle_mod
 
 G = np.load(GOLDEN / "drop_reference.npz")
 
@@ -54,16 +55,28 @@ def test_drop_shape_matches_reference(icp):
 
 
 def test_water_index_matches_reference(icp):
-    # R9-97 evaluated identically; density from Tanaka/Kell + the UNESCO secant bulk modulus
-    # instead of IAPWS-95: n within 2.5e-6 up to 10 MPa, 1.2e-5 up to 100 MPa.
+    # IAPWS-95 liquid density (all 56 residual terms, the reference's bisection) and R9-97 index:
+    # bit for bit the reference's evaluate_water_optics on its golden grid
     for (lam, t, p), (n_ref, rho_ref) in zip(G["water_in"], G["water"]):
         w = icp.evaluate_water_optics(lam, t, p)
-        tol = 2.5e-6 if p <= 1e7 else 1.2e-5
-        assert abs(w.refractive_index - n_ref) <= tol, (lam, t, p)
-        assert abs(w.density_kg_m3 - rho_ref) <= 0.036, (lam, t, p)
+        assert w.refractive_index == n_ref, (lam, t, p)
+        assert w.density_kg_m3 == rho_ref, (lam, t, p)
     for bad in ((150.0, 20.0, 101325.0), (700.0, -1.0, 101325.0), (700.0, 61.0, 101325.0), (700.0, 20.0, 1e9)):
         with pytest.raises(icp.InvalidArgument):
             icp.evaluate_water_optics(*bad)
+
+
+@pytest.mark.skipif(not oracle_mod.ref_drop_available(), reason="reference drop harness not built")
+def test_water_index_matches_reference_on_random_states(icp):
+    # seeded states over the whole domain (200-1100 nm, 0-60 C, 50 kPa-100 MPa) through the
+    # reference's own evaluate_water_optics compiled here
+    rng = np.random.default_rng(20261204)
+    ins = [(float(lam), float(t), float(p)) for lam, t, p in
+           zip(rng.uniform(200, 1100, 300), rng.uniform(0, 60, 300), np.exp(rng.uniform(np.log(5e4), np.log(1e8), 300)))]
+    ref = oracle_mod.ref_drop_lines("water", [f"{lam!r} {t!r} {p!r}" for lam, t, p in ins])
+    for (lam, t, p), (n_ref, rho_ref) in zip(ins, ref):
+        w = icp.evaluate_water_optics(lam, t, p)
+        assert (w.refractive_index, w.density_kg_m3) == (n_ref, rho_ref), (lam, t, p)
 
 
 def test_projected_area_matches_reference(icp):
