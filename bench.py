@@ -132,7 +132,7 @@ def run_reference_hex(a) -> None:
     if rank != 0:
         return
     procs = os.cpu_count() or 1
-    per = max(1000, int(a.ref_rays) // procs)
+    per = max(1000, 5 * int(a.ref_rays) // procs)
     for _ in range(a.warmup):
         reference_sample(max(1000, per // 10), procs)
     vals = [reference_sample(per, procs) for _ in range(a.steps)]
@@ -149,9 +149,8 @@ def run_reference_hex(a) -> None:
 
 
 def _drop_reference_inputs() -> dict:
-    """Interior index (the reference's water model at 650 nm, 20 C, as binary32), the incident
-    direction the reference CLI builds, and this record's sampling hit fraction (the reference's
-    projected area over the bounding-disk area)."""
+    """Interior index (the reference's water model at 650 nm, 20 C, as binary32, from its own
+    evaluate_water_optics) and the incident direction the reference CLI builds."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import numpy as np
 
@@ -160,34 +159,33 @@ def _drop_reference_inputs() -> dict:
     d = DROP
     n = float(np.float32(oracle.ref_drop_lines("water", ["650.0 20.0 101325.0"])[0][0]))
     a = math.radians(d["incl"])
-    k = (float(np.float32(math.cos(a))), float(np.float32(-math.sin(a))), 0.0)
-    area = oracle.ref_drop_lines("area", [" ".join(repr(float(x)) for x in (*d["coefficients"], d["radius"],
-                                                                           *oracle.drop_frame(d["incl"])[0]))])[0][0]
-    disk = oracle.drop_geometry(d["coefficients"], d["radius"]).disk_area_mm2
-    return {"n": n, "k": k, "hit_fraction": area / disk}
+    return {"n": n, "k": (float(np.float32(math.cos(a))), float(np.float32(-math.sin(a))), 0.0)}
 
 
-def reference_drop_sample(grid: int, procs: int, inputs: dict) -> dict:
-    """The reference's CPU drop tracer (RaindropPathTracer: R, TT, TRT, TRRT per lattice vertex,
-    binary32, oracle/_ref/ref_drop_harness built from its sources) over a grid x grid lattice,
-    one process per core on disjoint row slices.  Rays/s are its hit rays per second divided by
-    this record's hit fraction, i.e. sampled rays of this record per second at the reference's
-    cost per hit (its misses are cheaper and its chain stops after three internal hits)."""
-    exe = ROOT / "oracle" / "_ref" / "ref_drop_harness"
+def reference_drop_sample(rays_per_proc: int, procs: int, inputs: dict, first: int = 0) -> dict:
+    """The record's work by the reference's own CPU code (oracle/_ref/ref_record_harness, built
+    from its sources): the same sampled ray ids of this record, at most 10 internal interactions
+    through its drop intersector and Fresnel split, every exit binned by its PhaseMassAccumulator,
+    and the stored CDF of the histogram by its build_host_cdf.  One process per core over
+    disjoint ray-id slices; the first process also builds the 900 x 1800 CDF (one record's CDF per
+    step).  Rays/s = rays of all processes / wall time of the step."""
+    exe = ROOT / "oracle" / "_ref" / "ref_record_harness"
     if not exe.exists():
         raise FileNotFoundError(exe)
     d = DROP
-    rows = (grid + procs - 1) // procs
-    args = [str(exe), "time", repr(d["radius"]), "0", repr(inputs["n"]), *map(repr, inputs["k"]), str(grid)]
+    base = [str(exe), "record", repr(d["radius"]), repr(inputs["n"]), *map(repr, inputs["k"]), str(d["nt"]),
+            str(d["np"]), str(d["hits"]), str(d["seed"]), str(int(1e8))]
     t0 = time.perf_counter()
-    ps = [subprocess.Popen(args + [str(i * rows), str(rows), *map(repr, d["coefficients"])], stdout=subprocess.PIPE,
-                           text=True) for i in range(procs) if i * rows < grid]
+    ps = [subprocess.Popen(base + [str(first + i * rays_per_proc), str(rays_per_proc), *map(repr, d["coefficients"]),
+                                   "1" if i == 0 else "0"], stdout=subprocess.PIPE, text=True) for i in range(procs)]
     outs = [p.communicate()[0].split() for p in ps]
     wall = time.perf_counter() - t0
-    vertices = sum(int(o[0]) for o in outs)
-    hits = sum(int(o[1]) for o in outs)
-    return {"vertices": vertices, "hits": hits, "seconds": wall, "procs": len(ps),
-            "rays_per_s": hits / wall / inputs["hit_fraction"]}
+    if any(p.returncode != 0 for p in ps):
+        raise RuntimeError("reference record harness failed")
+    rays = sum(int(o[0]) for o in outs)
+    return {"rays": rays, "hits": sum(int(o[1]) for o in outs), "exits": sum(int(o[2]) for o in outs),
+            "seconds": wall, "procs": procs, "rays_per_s": rays / wall, "cdf_seconds": float(outs[0][4]),
+            "trace_seconds_per_proc": sum(float(o[3]) for o in outs) / procs}
 
 
 def _drop_public() -> dict:
@@ -203,14 +201,15 @@ def run_reference_drop(a) -> None:
         return
     procs = os.cpu_count() or 1
     inputs = _drop_reference_inputs()
-    grid = int(a.ref_grid)
+    per = max(100, int(a.ref_rays) // procs)
     for _ in range(a.warmup):
-        reference_drop_sample(max(64, grid // 8), procs, inputs)
-    vals = [reference_drop_sample(grid, procs, inputs) for _ in range(a.steps)]
-    v = sum(x["rays_per_s"] * x["seconds"] for x in vals) / sum(x["seconds"] for x in vals)
-    sample = (f"{grid}x{grid} lattice per step ({vals[0]['hits']} hits), {vals[0]['procs']} processes; reference "
-              f"RaindropPathTracer (R, TT, TRT, TRRT, binary32) compiled from its sources; rays/s = hit rays/s / "
-              f"{inputs['hit_fraction']:.4f} (this record's hit fraction)")
+        reference_drop_sample(max(100, per // 10), procs, inputs)
+    vals = [reference_drop_sample(per, procs, inputs, first=i * per * procs) for i in range(a.steps)]
+    v = sum(x["rays"] for x in vals) / sum(x["seconds"] for x in vals)
+    sample = (f"{per} rays per process x {procs} processes per step (disjoint ray ids of this record), "
+              "<= 10 internal interactions, every exit binned, one 900x1800 stored CDF per step; the reference's "
+              "RaindropIntersector, DielectricInterface::split, PhaseMassAccumulator and build_host_cdf compiled from "
+              "its sources (oracle/_ref/ref_record_harness)")
     line = {"metric": METRIC, "value": v, "unit": "rays/s", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": 1e3 * sum(x["seconds"] for x in vals) / len(vals), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -406,7 +405,7 @@ def run_b200_hex(a) -> None:
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
             procs = os.cpu_count() or 1
-            rb = reference_sample(max(2000, int(a.ref_rays) // procs), procs)
+            rb = reference_sample(max(2000, 5 * int(a.ref_rays) // procs), procs)
             cpu = {"value": rb["rays_per_s"], "unit": "rays/s", "cores": procs, "kind": "reference",
                    "sample": f"{rb['rays']} rays of the same record (disjoint ray ids, {procs} processes), "
                              "reference hex tracer + PhaseMassAccumulator compiled from its sources"}
@@ -874,6 +873,62 @@ def run_wave(I, ctx, stream, a) -> dict:
             "filtered_directions": stats.filtered_directions}
 
 
+def _cpu_leg(kind: str, payload: dict) -> dict:
+    """Runs one CPU-side leg (the reference CPU baseline sample or the oracle parity check) in a
+    child process, so that the oracle library never loads into the process that measures the
+    device; returns its JSON result."""
+    r = subprocess.run([sys.executable, str(Path(__file__).resolve()), "--cpu-leg", kind, "--cpu-leg-args",
+                        json.dumps(payload)], capture_output=True, text=True, cwd=str(ROOT))
+    if r.returncode != 0:
+        raise RuntimeError(f"{kind} leg failed: {(r.stderr or r.stdout).strip().splitlines()[-1:]}")
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def run_cpu_leg(kind: str, payload: dict) -> None:
+    """Child side of _cpu_leg: the oracle and the reference binaries are used here only."""
+    if kind == "drop_reference":
+        inputs = _drop_reference_inputs()
+        out = reference_drop_sample(int(payload["rays_per_proc"]), int(payload["procs"]), inputs)
+    elif kind == "drop_parity":
+        import numpy as np
+
+        from oracle import parity
+
+        z = np.load(payload["npz"], allow_pickle=False)
+        out = parity.drop_parity(z["masses"], json.loads(str(z["cfg"])), json.loads(str(z["audit"])))
+    else:
+        raise ValueError(kind)
+    print(json.dumps(out), flush=True)
+
+
+def drop_parity_leg(I, ctx, rec, g, edges, mass, weight: float, count: int) -> dict:
+    """Same-seed parity of the timed record: the first `count` ray ids of the record traced again
+    by the FP32 kernel (outside the timed region) and checked against the FP64 oracle on the same
+    ray ids in a child process (TV of cell mass, g, energy, Monte Carlo noise floor)."""
+    import ctypes as C
+
+    import numpy as np
+
+    d = DROP
+    nt, np_ = d["nt"], d["np"]
+    mass.zero_()
+    s = I.TraceStats()
+    I.check(I.LIB.icp_drop_trace_bin(ctx.handle, C.byref(rec), 0, count, weight, C.byref(g),
+                                     C.c_void_p(edges.data_ptr()), C.c_void_p(mass.data_ptr()), C.byref(s)))
+    m = mass.cpu().numpy().reshape(nt, np_).copy()
+    m[0] += weight * s.forward_pole / np_
+    m[-1] += weight * s.backward_pole / np_
+    cfg = {"coefficients": list(d["coefficients"]), "radius_mm": d["radius"], "interior_index": rec.interior_index,
+           "inclination_deg": d["incl"], "nt": nt, "np": np_, "rays": int(rec.rays), "seed": d["seed"],
+           "max_internal_hits": d["hits"], "first": 0, "count": count}
+    audit = {"escaped": weight * s.escaped, "unresolved": weight * s.unresolved,
+             "incident": weight * (s.rays - s.missed), "missed": s.missed}
+    with tempfile.TemporaryDirectory() as td:
+        path = str(Path(td) / "slice.npz")
+        np.savez(path, masses=m.reshape(-1), cfg=json.dumps(cfg), audit=json.dumps(audit))
+        return _cpu_leg("drop_parity", {"npz": path})
+
+
 def _peaks() -> dict:
     try:
         return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
@@ -915,32 +970,27 @@ def run_b200_drop(a) -> None:
     theta = torch.empty(np_ * (nt + 1), dtype=torch.float64, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     weight = I.sampling_area(d["coefficients"], d["radius"]) / float(rays * world)
-    pole = torch.zeros(3, dtype=torch.float64, device="cuda")
     policy = rec.policy
+    from ice_crystal_phase_b200 import sharded
+
+    shard_trace, shard_finish, shard_sums, disk = sharded.device_record(ctx, rec, grid, edges, mass)
+    shard = sharded.shard_of(rays * world, rank, world, disk)
+    last_trace = {}
+
+    def traced(first: int, count: int):
+        t = shard_trace(first, count)
+        last_trace["t"] = t
+        return t
 
     def step():
-        """One record; returns (trace stats of this rank, record report or None)."""
+        """One record; returns (trace summary of this rank, record report or None)."""
         if world == 1:
             rep = I.DropReport()
             I.check(I.LIB.icp_drop_generate_device(ctx.handle, C.byref(rec), C.c_void_p(phi.data_ptr()),
                                                    C.c_void_p(theta.data_ptr()), None, C.byref(rep)))
             return rep.trace, rep
-        mass.zero_()
-        s = I.TraceStats()
-        I.check(I.LIB.icp_drop_trace_bin(ctx.handle, C.byref(rec), rank * rays, rays, weight, C.byref(g),
-                                         C.c_void_p(edges.data_ptr()), C.c_void_p(mass.data_ptr()), C.byref(s)))
-        pole[0], pole[1] = weight * s.forward_pole, weight * s.backward_pole
-        pole[2] = weight * (s.rays - s.missed)
-        dist.all_reduce(mass)
-        dist.all_reduce(pole)
-        if rank == 0:
-            rows = torch.from_numpy(I.diffraction_rows(grid.edges, float(pole[2]), d["wavelength"])).cuda()
-            mass.view(nt, np_).add_(rows[:, None] / np_)
-            crep = I.CdfReport()
-            I.check(I.LIB.icp_phase_cdf_build(ctx.handle, C.c_void_p(mass.data_ptr()), 0, nt, np_, float(pole[0]),
-                                              float(pole[1]), nt, np_, C.byref(policy), C.c_void_p(phi.data_ptr()),
-                                              C.c_void_p(theta.data_ptr()), C.byref(crep)))
-        return s, None
+        sharded.sharded_drop_record(shard, traced, dist.all_reduce, shard_finish, shard_sums)
+        return last_trace["t"], None
 
     def barrier():
         torch.cuda.synchronize()
@@ -1040,13 +1090,17 @@ def run_b200_drop(a) -> None:
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
             procs = os.cpu_count() or 1
-            inputs = _drop_reference_inputs()
-            rb = reference_drop_sample(int(a.ref_grid), procs, inputs)
+            per = max(100, int(a.ref_rays) // procs)
+            rb = _cpu_leg("drop_reference", {"rays_per_proc": per, "procs": procs})
+            r1 = _cpu_leg("drop_reference", {"rays_per_proc": per, "procs": 1})
             cpu = {"value": rb["rays_per_s"], "unit": "rays/s", "cores": rb["procs"], "kind": "reference",
-                   "sample": f"{a.ref_grid}x{a.ref_grid} lattice ({rb['hits']} hit rays, {rb['seconds']:.1f} s), "
-                             "reference RaindropPathTracer (R, TT, TRT, TRRT, binary32) compiled from its sources; "
-                             f"rays/s = hit rays/s / {inputs['hit_fraction']:.4f} (this record's hit fraction)"}
-        except (OSError, ValueError, IndexError) as e:
+                   "one_core": r1["rays_per_s"],
+                   "sample": f"{rb['rays']} rays of this record ({per} per process, {procs} processes, "
+                             f"{rb['seconds']:.1f} s; one core: {r1['rays']} rays in {r1['seconds']:.1f} s), <= 10 "
+                             "internal interactions, every exit binned, one 900x1800 stored CDF per sample; the "
+                             "reference's RaindropIntersector, DielectricInterface::split, PhaseMassAccumulator and "
+                             "build_host_cdf compiled from its sources"}
+        except (OSError, ValueError, IndexError, RuntimeError) as e:
             cpu = {"value": None, "unit": "rays/s", "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
 
     batched = None
@@ -1076,7 +1130,14 @@ def run_b200_drop(a) -> None:
         except (I.IcpError, RuntimeError, ValueError, OSError) as e:  # reported on the line, not fatal to it
             wave = {"error": f"{type(e).__name__}: {e}"}
 
-    s0 = stats_all[-1]
+    parity = None
+    if rank == 0 and world == 1 and a.parity_rays > 0:
+        try:
+            parity = drop_parity_leg(I, ctx, rec, g, edges, mass, weight, int(a.parity_rays))
+        except (I.IcpError, RuntimeError, ValueError, OSError) as e:  # reported on the line, not fatal to it
+            parity = {"error": f"{type(e).__name__}: {e}"}
+
+    s0 = stats_all[-1] if world == 1 else ks
     r0 = reps[-1]
     line = {
         "metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
@@ -1114,6 +1175,8 @@ def run_b200_drop(a) -> None:
         line["rainbow_diffraction"] = rainbow
     if wave is not None:
         line["wave_stages"] = wave
+    if parity is not None:
+        line["parity"] = parity
     if r0 is not None:
         line["record"] = {"g": r0.cdf.g_stored, "projected_area_mm2": r0.projected_area_mm2,
                           "incident_area_mm2": r0.incident_area_mm2, "diffraction_mm2": r0.diffraction_area_mm2,
@@ -1134,7 +1197,6 @@ def main() -> None:
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["b200", "reference"], default="b200")
     p.add_argument("--workload", choices=["drop", "hex"], default="drop")
-    p.add_argument("--ref-grid", type=int, default=1025, help="reference drop lattice size per step")
     p.add_argument("--block-threads", type=int, default=0, help="trace block size (0 = library default)")
     p.add_argument("--batch-records", type=int, default=256, help="records of the batched measurement (0 = skip)")
     p.add_argument("--batch-steps", type=int, default=3)
@@ -1148,9 +1210,17 @@ def main() -> None:
     p.add_argument("--wave-steps", type=int, default=0,
                    help="timed passes of each wave-stage kernel chain (patch build, query, optics, diffraction; 0 = skip)")
     p.add_argument("--rays", type=float, default=1e8)
-    p.add_argument("--ref-rays", type=float, default=1.6e6, help="reference rays per step (all processes)")
+    p.add_argument("--ref-rays", type=float, default=3.2e5,
+                   help="reference rays per step (all processes; the hex workload traces five times more)")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--parity-rays", type=float, default=4e6,
+                   help="first ray ids of the timed record checked against the FP64 oracle (0 = skip)")
+    p.add_argument("--cpu-leg", default=None, help=argparse.SUPPRESS)
+    p.add_argument("--cpu-leg-args", default="{}", help=argparse.SUPPRESS)
     a = p.parse_args()
+    if a.cpu_leg:
+        run_cpu_leg(a.cpu_leg, json.loads(a.cpu_leg_args))
+        return
     if a.warmup < 3:
         a.warmup = 3
     if a.impl == "reference":

@@ -8,6 +8,10 @@
 #   oracle/_ref/ref_hex_harness          oracle/ref_hex_harness.cpp over the same sources
 #   oracle/_ref/ref_drop_harness         oracle/ref_drop_harness.cpp over the header-only drop
 #                                        tracer, src/projected_area.cpp, src/water_refractive_index.cpp
+#   oracle/_ref/ref_record_harness       oracle/ref_record_harness.cpp: one drop record's trace, binning
+#                                        and stored CDF by the reference's drop intersector, Fresnel
+#                                        split, PhaseMassAccumulator and build_host_cdf (the timed
+#                                        reference arm)
 #   oracle/_ref/ref_ice_harness          oracle/ref_ice_harness.cpp over hex_atlas/src/ice_optics.cpp
 #   oracle/_ref/ref_atlas_harness        oracle/ref_atlas_harness.cpp over hex_atlas/src/atlas.cpp and
 #                                        hex_trace/src/hex_trace.cpp (area rule, atlas nodes)
@@ -21,10 +25,10 @@
 #   oracle/_ref/ref_query_harness        oracle/ref_query_harness.cpp over the header-only ray / patch
 #                                        intersection and query direction grid
 #
-# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default $ICP_REFERENCE_ROOT, else /root/reference)
 set -euo pipefail
 here="$(cd "$(dirname "$0")" && pwd)"
-ref="${1:-/root/reference}"
+ref="${1:-${ICP_REFERENCE_ROOT:-/root/reference}}"
 out="$here/_ref"
 if [ ! -d "$ref/hex_phase" ]; then
     echo "build_ref.sh: reference sources not found at $ref (prebuilt files in $out are used as-is)" >&2
@@ -40,6 +44,8 @@ g++ "${flags[@]}" "$ref/hex_phase/apps/generate_hex_phase.cpp" "${srcs[@]}" -o "
 g++ "${flags[@]}" "$here/ref_hex_harness.cpp" "${srcs[@]}" -o "$out/ref_hex_harness"
 g++ -std=c++20 -O2 -fno-fast-math -ffp-contract=off -I"$ref/include" "$here/ref_drop_harness.cpp" \
     "$ref/src/projected_area.cpp" "$ref/src/water_refractive_index.cpp" -o "$out/ref_drop_harness"
+g++ "${flags[@]}" "$here/ref_record_harness.cpp" "$ref/hex_phase/src/phase_table.cpp" "$ref/src/npy_writer.cpp" \
+    -o "$out/ref_record_harness"
 g++ -std=c++20 -O2 -fno-fast-math -ffp-contract=off -I"$ref/include" "$here/ref_rainbow_harness.cpp" \
     -o "$out/ref_rainbow_harness"
 g++ -std=c++20 -O2 -fno-fast-math -ffp-contract=off -I"$ref/include" "$here/ref_optics_harness.cpp" \
@@ -57,4 +63,4 @@ if [ -f "$ref/hex_atlas/src/ice_optics.cpp" ]; then
         "$ref/hex_atlas/src/atlas.cpp" "$ref/hex_atlas/src/ice_optics.cpp" "$ref/hex_trace/src/hex_trace.cpp" \
         "$ref/src/npy_writer.cpp" -o "$out/ice_precompute_atlas_cpu"
 fi
-echo "built $out/ice_generate_phase_cpu $out/ref_hex_harness $out/ref_drop_harness $out/ref_ice_harness $out/ref_atlas_harness $out/ice_precompute_atlas_cpu $out/ref_rainbow_harness $out/ref_optics_harness $out/ref_patch_harness $out/ref_query_harness"
+echo "built $out/ice_generate_phase_cpu $out/ref_hex_harness $out/ref_drop_harness $out/ref_record_harness $out/ref_ice_harness $out/ref_atlas_harness $out/ice_precompute_atlas_cpu $out/ref_rainbow_harness $out/ref_optics_harness $out/ref_patch_harness $out/ref_query_harness"

@@ -352,6 +352,7 @@ class DropRecord:
     max_balance: float
     max_iface: float
     counts: dict = field(default_factory=dict)
+    cells: np.ndarray | None = None  # cell masses before the pole caps are spread (mm^2)
 
 
 def drop_record(geo: DropGeometry, frame: np.ndarray, n_int: float, nt: int, np_: int, rays: int, seed: int,
@@ -378,7 +379,40 @@ def drop_record(geo: DropGeometry, frame: np.ndarray, n_int: float, nt: int, np_
     cnt = {k: int(v) for k, v in zip(names, counts)}
     hits = cnt["rays"] - cnt["missed"]
     return DropRecord(masses, stats[4], stats[6], scale * stats[8], scale * stats[10], scale * hits, stats[2],
-                      stats[12], stats[13], cnt)
+                      stats[12], stats[13], cnt, cells[0::2].copy())
+
+
+def drop_record_sharded(geo: DropGeometry, frame: np.ndarray, n_int: float, nt: int, np_: int, rays: int, seed: int,
+                        max_hits: int = 1024, tail: float = 1e-12, first: int = 0, count: int | None = None,
+                        workers: int | None = None) -> DropRecord:
+    """drop_record over rays [first, first + count) of a `rays`-ray record, cut into disjoint
+    ray-id slices traced on threads (the C oracle keeps no global state and ctypes releases the
+    GIL during the call).  The counter RNG makes every ray independent of the cut, so the merged
+    masses equal the single-call record's up to the order of the FP64 cell sums; counts are
+    exact."""
+    count = rays - first if count is None else count
+    workers = max(1, min(workers or os.cpu_count() or 1, max(1, count // 10000)))
+    bounds = [first + count * k // workers for k in range(workers + 1)]
+    from concurrent.futures import ThreadPoolExecutor
+
+    with ThreadPoolExecutor(max_workers=workers) as pool:
+        parts = list(pool.map(lambda k: drop_record(geo, frame, n_int, nt, np_, rays, seed, max_hits, tail,
+                                                    first=bounds[k], count=bounds[k + 1] - bounds[k]),
+                              range(workers)))
+    out = parts[0]
+    for p in parts[1:]:
+        out.masses = out.masses + p.masses
+        out.cells = out.cells + p.cells
+        out.forward += p.forward
+        out.backward += p.backward
+        out.escaped_area += p.escaped_area
+        out.unresolved_area += p.unresolved_area
+        out.incident_area += p.incident_area
+        out.point_axial += p.point_axial
+        out.max_balance = max(out.max_balance, p.max_balance)
+        out.max_iface = max(out.max_iface, p.max_iface)
+        out.counts = {k: out.counts[k] + p.counts[k] for k in out.counts}
+    return out
 
 
 def drop_trace_rays(geo: DropGeometry, frame, n_int, seed, total, first, count, max_hits=1024, tail=1e-12,

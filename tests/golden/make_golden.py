@@ -3,7 +3,8 @@
 Runs the reference's own CPU code, compiled from its sources by oracle/build_ref.sh into
 oracle/_ref/ (ice_generate_phase_cpu and the ref_*_harness drivers), imports the reference's
 Python atlas composition (hex_atlas/python/atlas_math.py),
-and stores its outputs as small .npz files.  Needs the reference checkout (default /root/reference);
+and stores its outputs as small .npz files.  Needs the reference checkout (the first argument, else
+$ICP_REFERENCE_ROOT, else /root/reference);
 the fixtures are committed so that tests never need it.
 
     python tests/golden/make_golden.py [REFERENCE_ROOT]
@@ -13,6 +14,7 @@ from __future__ import annotations
 import json
 import math
 import subprocess
+import os
 import sys
 import tempfile
 from pathlib import Path
@@ -21,7 +23,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
-REF = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+REF = Path(sys.argv[1]) if len(sys.argv) > 1 else Path(os.environ.get("ICP_REFERENCE_ROOT", "/root/reference"))
 REF_BIN = ROOT / "oracle" / "_ref"
 
 # The reference's CLI test plan (hex_phase/configs/two_orientations.csv), reproduced as data:

@@ -175,3 +175,62 @@ def test_invalid_drop_inputs_rejected(ctx, icp):
         icp.generate_drop_record(ctx, [0.0] * 8, 1.0, 1.33, 9, 16, 100, ct=4)
     with pytest.raises(icp.InvalidArgument):  # diffraction needs a wavelength
         icp.generate_drop_record(ctx, [0.0] * 8, 1.0, 1.33, 8, 16, 100, diffraction=True)
+
+
+# The record the headline measurement times: an oblate drop of equal-volume radius 1.5 mm with
+# r/a = 1 - 0.08 cos(chi) - 0.02 cos(2 chi) + 0.005 cos(3 chi), 650 nm with the water index at
+# 20 C held in binary32, inclination 20 deg, at most 10 internal interactions, 900 x 1800 cells,
+# seed 12345, 1e8 rays in the record.  Its first ray ids are traced here, exactly the rays the
+# timed record starts with (the counter RNG depends only on seed and ray id).
+BENCH_COEFF = (0.0, -0.08, -0.02, 0.005, 0.0, 0.0, 0.0, 0.0)
+BENCH_RAYS, BENCH_SEED, BENCH_HITS = 100_000_000, 12345, 10
+
+
+def _bench_index(icp):
+    return float(np.float32(icp.evaluate_water_optics(650.0).refractive_index))
+
+
+def test_benchmark_record_slice_parity(ctx, icp, oracle):
+    """FP32 device trace of the benchmark record's first 1e6 ray ids against the FP64 oracle on
+    the same ray ids: TV of cell mass <= 1e-3, |g - g_oracle| <= 1e-4, energy balance <= 1e-6 --
+    the tolerances the headline metric is quoted at."""
+    from oracle import parity
+
+    n_int, count = _bench_index(icp), 1_000_000
+    acc = icp.PhaseMassAccumulatorCuda(ctx, icp.make_drop_grid(900, 1800, 20.0))
+    acc.add_drop(BENCH_COEFF, 1.5, n_int, BENCH_RAYS, BENCH_SEED, 20.0, max_internal_hits=BENCH_HITS,
+                 precision=icp.ICP_FP32, first=0, count=count)
+    cfg = {"coefficients": list(BENCH_COEFF), "radius_mm": 1.5, "interior_index": n_int, "inclination_deg": 20.0,
+           "nt": 900, "np": 1800, "rays": BENCH_RAYS, "seed": BENCH_SEED, "max_internal_hits": BENCH_HITS, "first": 0,
+           "count": count}
+    audit = {"escaped": acc.escaped_area, "unresolved": acc.unresolved_area, "incident": acc.incident_area,
+             "missed": acc.stats.missed}
+    r = parity.drop_parity(acc.masses(), cfg, audit)
+    assert acc.stats.rays == count
+    assert r["tv"] <= 1e-3, r
+    assert r["g_abs_error"] <= 1e-4, r
+    assert r["energy_residual_device"] <= 1e-6, r
+    assert abs(r["missed_device"] - r["missed_oracle"]) <= 5, r
+
+
+def test_benchmark_record_stored_cdf_parity(ctx, icp, oracle):
+    """The benchmark record's whole pipeline at 1e6 rays (trace, analytic diffraction rows, stored
+    CDF) through the host-buffer entry against the oracle's record of the same rays plus the same
+    rows through the oracle's CDF build: TV of the stored cell probabilities <= 1e-3 and stored g
+    within 1e-4."""
+    n_int, rays = _bench_index(icp), 1_000_000
+    out = icp.generate_drop_record(ctx, BENCH_COEFF, 1.5, n_int, 900, 1800, rays, seed=BENCH_SEED,
+                                   max_internal_hits=BENCH_HITS, wavelength_nm=650.0, diffraction=True)
+    rep = out.report
+    geo = oracle.drop_geometry(BENCH_COEFF, 1.5)
+    rec = oracle.drop_record_sharded(geo, np.array(icp.drop_frame(20.0)), n_int, 900, 1800, rays, BENCH_SEED,
+                                     max_hits=BENCH_HITS)
+    rows = icp.diffraction_rows(icp.u_edges(900), rec.incident_area, 650.0)
+    cdf = oracle.build_cdf((rec.masses.reshape(900, 1800) + rows[:, None] / 1800).reshape(-1), 900, 1800)
+    p_gpu = np.diff(out.phi)[:, None] * np.diff(out.theta, axis=1)
+    p_ref = np.diff(cdf.phi)[:, None] * np.diff(cdf.theta, axis=1)
+    assert 0.5 * np.abs(p_gpu - p_ref).sum() <= 1e-3
+    assert abs(rep.cdf.g_stored - cdf.report["g_stored"]) <= 1e-4
+    assert abs((rep.escaped_area_mm2 + rep.unresolved_area_mm2) / rep.incident_area_mm2 - 1) <= 1e-6
+    assert abs(rep.diffraction_area_mm2 / rep.incident_area_mm2 - 1) <= 1e-12
+    assert rep.trace.rays == rays and rep.cdf.status == 0

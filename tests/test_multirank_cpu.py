@@ -1,8 +1,10 @@
-"""The N-rank record of bench.py --gpus N on the CPU: world size 2 over gloo, each rank traces
-its own contiguous ray-id shard of one drop record (here with the CPU oracle), the FP64
-histograms, pole sums and hit counts are summed with one all-reduce, and rank 0 adds the
-diffraction rows and builds the CDF.  The counter RNG makes the result partition-invariant:
-it must equal the one-rank record up to FP64 summation order."""
+"""The N-rank record of bench.py --gpus N on the CPU: world size 2 over gloo through the same
+package function bench.py runs (ice_crystal_phase_b200.sharded.sharded_drop_record), with the
+CPU oracle's trace and CDF build injected in place of the device's.  Each rank traces its own
+contiguous ray-id shard of one drop record, the FP64 histograms and the pole / hit sums cross one
+all-reduce each, and rank 0 adds the diffraction rows and builds the CDF.  The counter RNG makes
+the result partition-invariant: it must equal the one-rank record up to FP64 summation order,
+also for a ray count that does not divide by the world size."""
 from __future__ import annotations
 
 import os
@@ -14,7 +16,6 @@ import torch
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
-RAYS_PER_RANK = 3000
 NT, NP = 36, 72
 
 
@@ -34,33 +35,69 @@ def _record_inputs():
     return icp, oracle, geo, frame
 
 
-def _rank(rank: int, world: int, port: int, out: str) -> None:
+def _oracle_parts(total: int):
+    """Trace / finish callables of sharded_drop_record with the oracle in place of the device."""
+    icp, oracle, geo, frame = _record_inputs()
+
+    def trace(first: int, count: int):
+        from ice_crystal_phase_b200.sharded import ShardTrace
+
+        rec = oracle.drop_record(geo, frame, 1.3317, NT, NP, total, 77, max_hits=10, first=first, count=count)
+        w = geo.disk_area_mm2 / total  # the oracle's pole sums are in mm^2 already: back to ray units
+        return ShardTrace(torch.from_numpy(rec.cells.copy()), rec.forward / w, rec.backward / w,
+                          rec.counts["rays"] - rec.counts["missed"])
+
+    def finish(mass, forward, backward, incident):
+        rows = icp.diffraction_rows(icp.u_edges(NT), incident, 650.0)
+        m = mass.numpy().reshape(NT, NP).copy() + rows[:, None] / NP
+        m[0] += forward / NP
+        m[-1] += backward / NP
+        cdf = oracle.build_cdf(m.reshape(-1), NT, NP)
+        return mass.numpy().copy(), np.array([forward, backward, incident]), cdf
+
+    return trace, finish, geo
+
+
+def _rank(rank: int, world: int, port: int, total: int, out: str) -> None:
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        icp, oracle, geo, frame = _record_inputs()
-        total = RAYS_PER_RANK * world
-        rec = oracle.drop_record(geo, frame, 1.3317, NT, NP, total, 77, max_hits=10, first=rank * RAYS_PER_RANK,
-                                 count=RAYS_PER_RANK)
-        mass = torch.from_numpy(rec.masses.copy())
-        sums = torch.tensor([rec.incident_area, rec.escaped_area, rec.unresolved_area], dtype=torch.float64)
-        dist.all_reduce(mass)
-        dist.all_reduce(sums)
+        from ice_crystal_phase_b200.sharded import shard_of, sharded_drop_record
+
+        trace, finish, geo = _oracle_parts(total)
+        shard = shard_of(total, rank, world, geo.disk_area_mm2)
+        got = sharded_drop_record(shard, trace, dist.all_reduce, finish,
+                                  lambda v: torch.tensor(v, dtype=torch.float64))
         if rank == 0:
-            rows = icp.diffraction_rows(icp.u_edges(NT), float(sums[0]), 650.0)
-            m = mass.numpy().reshape(NT, NP) + rows[:, None] / NP
-            cdf = oracle.build_cdf(m.reshape(-1), NT, NP)
-            np.savez(out, mass=mass.numpy(), sums=sums.numpy(), phi=cdf.phi, theta=cdf.theta,
-                     g=cdf.report["g_stored"])
+            mass, sums, cdf = got
+            np.savez(out, mass=mass, sums=sums, phi=cdf.phi, theta=cdf.theta, g=cdf.report["g_stored"])
+        else:
+            assert got is None
     finally:
         dist.destroy_process_group()
 
 
-def test_two_rank_shards_equal_one_rank_record(tmp_path):
+def test_shard_bounds_cover_the_record_once():
+    from ice_crystal_phase_b200.sharded import shard_of
+
+    for total, world in ((10, 3), (6001, 2), (100_000_000, 8), (7, 7)):
+        shards = [shard_of(total, r, world, 1.0) for r in range(world)]
+        assert shards[0].first == 0 and sum(s.count for s in shards) == total
+        assert all(a.first + a.count == b.first for a, b in zip(shards, shards[1:]))
+        assert max(s.count for s in shards) - min(s.count for s in shards) <= 1
+        assert all(s.weight == 1.0 / total for s in shards)
+    with pytest.raises(ValueError):
+        shard_of(10, 2, 2, 1.0)
+    with pytest.raises(ValueError):
+        shard_of(1, 0, 2, 1.0)
+
+
+@pytest.mark.parametrize("total", [6000, 6001])
+def test_two_rank_shards_equal_one_rank_record(tmp_path, total):
     out = str(tmp_path / "r0.npz")
     ctx = mp.get_context("spawn")
     port = _free_port()
-    procs = [ctx.Process(target=_rank, args=(r, 2, port, out)) for r in range(2)]
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, total, out)) for r in range(2)]
     for p in procs:
         p.start()
     for p in procs:
@@ -68,10 +105,10 @@ def test_two_rank_shards_equal_one_rank_record(tmp_path):
         assert p.exitcode == 0
     got = np.load(out)
     icp, oracle, geo, frame = _record_inputs()
-    one = oracle.drop_record(geo, frame, 1.3317, NT, NP, 2 * RAYS_PER_RANK, 77, max_hits=10)
-    assert np.abs(got["mass"] - one.masses).sum() <= 1e-13 * one.masses.sum()
-    assert abs(got["sums"][0] - one.incident_area) <= 1e-14 * one.incident_area
-    assert abs(got["sums"][1] / one.escaped_area - 1) <= 1e-13
+    one = oracle.drop_record(geo, frame, 1.3317, NT, NP, total, 77, max_hits=10)
+    assert np.abs(got["mass"] - one.cells).sum() <= 1e-13 * one.cells.sum()
+    assert abs(got["sums"][2] - one.incident_area) <= 1e-14 * one.incident_area
+    assert abs(got["sums"][0] - one.forward) <= 1e-13 * max(one.forward, 1e-300)
     rows = icp.diffraction_rows(icp.u_edges(NT), one.incident_area, 650.0)
     cdf = oracle.build_cdf((one.masses.reshape(NT, NP) + rows[:, None] / NP).reshape(-1), NT, NP)
     p_one = np.diff(cdf.phi)[:, None] * np.diff(cdf.theta, axis=1)
