@@ -313,6 +313,7 @@ _FUNCS = {
     "icp_context_destroy": (C.c_int, [_P]),
     "icp_context_synchronize": (C.c_int, [_P]),
     "icp_context_stream": (_P, [_P]),
+    "icp_context_set_wait_limit": (C.c_int, [_P, C.c_uint32]),
     "icp_device_alloc": (C.c_int, [_P, C.c_size_t, C.POINTER(_P)]),
     "icp_device_free": (C.c_int, [_P, _P]),
     "icp_memcpy_h2d": (C.c_int, [_P, _P, _P, C.c_size_t]),
@@ -325,6 +326,9 @@ _FUNCS = {
                                     C.POINTER(Tuning)]),
     "icp_phase_cdf_build": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_uint32,
                                       C.c_uint32, C.POINTER(CdfPolicy), _P, _P, C.POINTER(CdfReport)]),
+    "icp_phase_cdf_enqueue": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_double, C.c_double,
+                                        C.c_uint32, C.c_uint32, _P, _P]),
+    "icp_phase_cdf_result": (C.c_int, [_P, C.POINTER(CdfPolicy), C.POINTER(CdfReport)]),
     "icp_phase_cdf_build_batch": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                             C.POINTER(CdfPolicy), _P, _P, C.POINTER(CdfReport)]),
     "icp_hex_generate": (C.c_int, [_P, C.POINTER(HexRecordArgs), C.POINTER(Orientation), C.c_uint32, _D, _D, _D,

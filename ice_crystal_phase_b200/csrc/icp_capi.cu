@@ -125,13 +125,20 @@ int icp_context_destroy(icp_context* c)
                       &c->b_reports,  &c->b_sync,     &c->b_phi,        &c->b_theta,     &c->mlp_error,
                       &c->cdfb_partial, &c->cdfb_colsum, &c->cdfb_recs, &c->atlas_trace, &c->atlas_coupling,
                       &c->rainbow,    &c->patches,
-                      &c->query,      &c->query_list, &c->stage_audit};
+                      &c->query,      &c->query_list, &c->stage_audit, &c->cdf_edges};
     for (Scratch* s : all) s->release();
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->ev2) cudaEventDestroy(c->ev2);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
+    return ok();
+}
+
+int icp_context_set_wait_limit(icp_context* c, uint32_t limit)
+{
+    if (!c) return fail(ICP_ERR_INVALID_ARGUMENT, "null context");
+    c->wait_limit = limit;
     return ok();
 }
 
@@ -149,7 +156,12 @@ int icp_device_alloc(icp_context* c, size_t bytes, void** out)
 {
     if (!c || !out) return fail(ICP_ERR_INVALID_ARGUMENT, "icp_device_alloc: null argument");
     ICP_CUDA(cudaSetDevice(c->device));
-    ICP_CUDA(cudaMalloc(out, bytes ? bytes : 1));
+    const cudaError_t e = cudaMalloc(out, bytes ? bytes : 1);
+    if (e != cudaSuccess) {
+        cudaGetLastError(); // a refused allocation leaves the context usable: clear the error
+        *out = nullptr;
+        return fail(ICP_ERR_DEVICE, "icp_device_alloc: cudaMalloc of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    }
     return ok();
 }
 int icp_device_free(icp_context* c, void* ptr)
@@ -406,17 +418,16 @@ namespace {
 
 int cdf_launch_common(icp_context* c, CdfLaunch& L, uint32_t ct, uint32_t cp)
 {
-    uint32_t cw = 0;
-    if (const int r = icp::choose_cdf_width(c, ct, cp, cw)) return r;
-    const uint32_t blocks = (cp + cw - 1) / cw;
+    const bool tma_ok = L.nt == ct && L.np == cp && L.np % 2 == 0 && ((uintptr_t)L.values % 16) == 0;
+    CdfShape sh{};
+    if (const int r = icp::cdf_shape(c, L.nt, L.np, ct, cp, tma_ok, sh)) return r;
+    const uint32_t blocks = (cp + sh.cw - 1) / sh.cw;
     ICP_CUDA(c->cdf_partial.ensure(cdf_partial_bytes() * blocks));
     ICP_CUDA(c->cdf_colsum.ensure(sizeof(double) * cp));
-    ICP_CUDA(cudaMemsetAsync(L.sync, 0, 2 * sizeof(unsigned), c->stream));
-    ICP_CUDA(cudaMemsetAsync(L.report, 0, sizeof(CdfDeviceReport), c->stream));
     L.colsum = (double*)c->cdf_colsum.ptr;
     L.partial = c->cdf_partial.ptr;
-    L.cw = cw;
-    const int e = launch_cdf_build(L, c->stream);
+    L.spin_limit = c->wait_limit;
+    const int e = launch_cdf_build(L, sh, c->stream);
     ++g_launches;
     if (e) return fail(ICP_ERR_DEVICE, "CDF launch failed: %s", cudaGetErrorString((cudaError_t)e));
     return ICP_OK;
@@ -440,7 +451,42 @@ int cdf_enqueue_kind(icp_context* c, const double* d_values, uint32_t kind, uint
     return cdf_launch_common(c, L, ct, cp);
 }
 
+// Arguments of icp_phase_cdf_enqueue / icp_phase_cdf_build (the reference's PhaseCdf::build
+// input checks, src/phase_cdf.cpp:285-310, and the host's pole split).
+int cdf_check_args(const icp_context* c, const double* d_values, uint32_t kind, uint32_t nt, uint32_t np, double fwd,
+                   double bwd, uint32_t ct, uint32_t cp, const double* d_phi, const double* d_theta, double& fa,
+                   double& ba)
+{
+    if (!c || !d_values || !d_phi || !d_theta) return fail(ICP_ERR_INVALID_ARGUMENT, "icp_phase_cdf_build: null argument");
+    if (kind > 1) return fail(ICP_ERR_INVALID_ARGUMENT, "Unknown CDF input kind.");
+    if (!nt || !np || (uint64_t)nt * np > 0xffffffffull)
+        return fail(ICP_ERR_INVALID_ARGUMENT, "Unsupported phase grid dimensions.");
+    if (!ct || !cp || ct > nt || cp > np || nt % ct || np % cp)
+        return fail(ICP_ERR_INVALID_ARGUMENT, "Storage dimensions must divide histogram dimensions.");
+    if (!(fwd >= 0) || !(bwd >= 0) || !H::finite(fwd) || !H::finite(bwd))
+        return fail(ICP_ERR_INVALID_ARGUMENT, "Invalid pole masses.");
+    fa = fwd / np;
+    ba = bwd / np;
+    if ((fwd > 0 && !(fa > 0)) || (bwd > 0 && !(ba > 0))) return fail(ICP_ERR_AUDIT, "Pole weight underflow.");
+    return ICP_OK;
+}
+
+bool policy_ok(const icp_cdf_policy& p)
+{
+    return H::finite(p.max_l1_error) && p.max_l1_error >= 0 && p.max_l1_error <= 2 && H::finite(p.max_lost_mass) &&
+           p.max_lost_mass >= 0 && p.max_lost_mass <= 1 && H::finite(p.max_coarsening_tv) &&
+           p.max_coarsening_tv >= 0 && p.max_coarsening_tv <= 1;
+}
+
 } // namespace
+
+int icp::cdf_clear(icp_context* c, void* d_reports, void* d_sync, uint32_t records)
+{
+    ICP_CUDA(cudaMemsetAsync(d_sync, 0, 2 * sizeof(unsigned) * records, c->stream));
+    ICP_CUDA(cudaMemsetAsync(d_reports, 0, sizeof(CdfDeviceReport) * records, c->stream));
+    ICP_CUDA(cudaStreamSynchronize(c->stream));
+    return ICP_OK;
+}
 
 int icp::cdf_enqueue(icp_context* c, const double* d_values, uint32_t nt, uint32_t np, uint32_t ct, uint32_t cp,
                      const double* d_edges, double fwd_add, double bwd_add, const unsigned long long* pole_fx,
@@ -468,11 +514,14 @@ int icp::cdf_enqueue_batch(icp_context* c, const CdfBatchInput* in, uint32_t cou
                            uint32_t ct, uint32_t cp, const double* d_edges, CdfDeviceReport* d_reports, unsigned* d_sync)
 {
     if (!count) return ICP_OK;
-    const uint32_t cw = std::max(1u, (cp + 15u) / 16u);
-    const uint32_t strips = (cp + cw - 1) / cw;
-    const size_t smem = cdf_smem_bytes(ct, cp, cw);
-    const int cap = smem <= 200 * 1024 ? cdf_max_coresident_blocks(smem, c->device) : 0;
-    const uint32_t per = (uint32_t)std::max(0, cap) / strips;
+    ICP_CUDA(cudaMemsetAsync(d_sync, 0, 2 * sizeof(unsigned) * count, c->stream));
+    ICP_CUDA(cudaMemsetAsync(d_reports, 0, sizeof(CdfDeviceReport) * count, c->stream));
+    // 16 strips per record, as many records per launch as stay co-resident
+    CdfShape sh{};
+    const bool fits = cdf_choose_shape(c->device, c->sms, nt, np, ct, cp, false, std::max(1u, (cp + 15u) / 16u),
+                                       0xffffffffu, sh) == 0;
+    const uint32_t strips = fits ? (cp + sh.cw - 1) / sh.cw : 0u;
+    const uint32_t per = fits ? (uint32_t)std::max(0, cdf_max_coresident_blocks(sh.smem, c->device)) / strips : 0u;
     if (!per) {
         // a record's strips alone do not fit: one launch per record, with its own strip width
         for (uint32_t r = 0; r < count; ++r)
@@ -486,8 +535,6 @@ int icp::cdf_enqueue_batch(icp_context* c, const CdfBatchInput* in, uint32_t cou
     ICP_CUDA(c->cdfb_partial.ensure(pb * count));
     ICP_CUDA(c->cdfb_colsum.ensure(sizeof(double) * cp * count));
     ICP_CUDA(c->cdfb_recs.ensure(sizeof(CdfBatchRecord) * count));
-    ICP_CUDA(cudaMemsetAsync(d_sync, 0, 2 * sizeof(unsigned) * count, c->stream));
-    ICP_CUDA(cudaMemsetAsync(d_reports, 0, sizeof(CdfDeviceReport) * count, c->stream));
     std::vector<CdfBatchRecord> recs(count);
     for (uint32_t r = 0; r < count; ++r) {
         CdfBatchRecord& b = recs[r];
@@ -513,30 +560,70 @@ int icp::cdf_enqueue_batch(icp_context* c, const CdfBatchInput* in, uint32_t cou
     L.np = np;
     L.ct = ct;
     L.cp = cp;
-    L.cw = cw;
+    L.spin_limit = c->wait_limit;
     for (uint32_t r0 = 0; r0 < count; r0 += per) {
         const uint32_t n = std::min(per, count - r0);
-        const int e = launch_cdf_build_batch(L, (const CdfBatchRecord*)c->cdfb_recs.ptr + r0, n, c->stream);
+        const int e = launch_cdf_build_batch(L, sh, (const CdfBatchRecord*)c->cdfb_recs.ptr + r0, n, c->stream);
         ++g_launches;
         if (e) return fail(ICP_ERR_DEVICE, "batched CDF launch failed: %s", cudaGetErrorString((cudaError_t)e));
     }
     return ICP_OK;
 }
 
-int icp::choose_cdf_width(icp_context* c, uint32_t ct, uint32_t cp, uint32_t& cw)
+int icp::cdf_shape(icp_context* c, uint32_t nt, uint32_t np, uint32_t ct, uint32_t cp, bool tma_ok, CdfShape& s)
 {
-    // smallest strip width whose grid fits co-resident, at least ceil(cp / SMs)
-    uint32_t w = std::max<uint32_t>(1u, (cp + c->sms - 1) / c->sms);
-    for (; w <= cp; ++w) {
-        const size_t smem = cdf_smem_bytes(ct, cp, w);
-        if (smem > 200 * 1024) break;
-        const uint32_t blocks = (cp + w - 1) / w;
-        if ((int)blocks <= cdf_max_coresident_blocks(smem, c->device)) {
-            cw = w;
+    for (const auto& k : c->cdf_shapes)
+        if (k.nt == nt && k.np == np && k.ct == ct && k.cp == cp && k.tma_ok == (uint32_t)tma_ok) {
+            s = k.shape;
             return ICP_OK;
         }
+    if (cdf_choose_shape(c->device, c->sms, nt, np, ct, cp, tma_ok, 1u, 0xffffffffu, s))
+        return fail(ICP_ERR_CAPACITY, "CDF strip for %u theta rows does not fit shared memory with a co-resident grid", ct);
+    c->cdf_shapes.push_back({nt, np, ct, cp, (uint32_t)tma_ok, s});
+    return ICP_OK;
+}
+
+extern "C" int icp_phase_cdf_enqueue(icp_context* c, const double* d_values, uint32_t kind, uint32_t nt, uint32_t np,
+                                     double fwd, double bwd, uint32_t ct, uint32_t cp, double* d_phi, double* d_theta)
+{
+    double fa = 0, ba = 0;
+    if (const int e = cdf_check_args(c, d_values, kind, nt, np, fwd, bwd, ct, cp, d_phi, d_theta, fa, ba)) return e;
+    ICP_CUDA(cudaSetDevice(c->device));
+    if (c->cdf_edges_nt != nt) {
+        std::vector<double> edges;
+        if (!H::u_edges(nt, edges))
+            return fail(ICP_ERR_INVALID_ARGUMENT, "Angular cells cannot be represented in binary64.");
+        ICP_CUDA(c->cdf_edges.ensure(sizeof(double) * (nt + 1)));
+        ICP_CUDA(cudaMemcpyAsync(c->cdf_edges.ptr, edges.data(), sizeof(double) * (nt + 1), cudaMemcpyHostToDevice,
+                                 c->stream));
+        ICP_CUDA(cudaStreamSynchronize(c->stream)); // the host vector goes out of scope
+        c->cdf_edges_nt = nt;
     }
-    return fail(ICP_ERR_CAPACITY, "CDF strip for %u theta rows does not fit shared memory with a co-resident grid", ct);
+    ICP_CUDA(c->cdf_report.ensure_zeroed(sizeof(CdfDeviceReport), c->stream));
+    ICP_CUDA(c->cdf_sync.ensure_zeroed(2 * sizeof(unsigned), c->stream));
+    const double* d_edges = (const double*)c->cdf_edges.ptr;
+    if (kind == 1) {
+        // density input: the kernel's mass conversion (kind 1) is only reached through here
+        if (const int e = cdf_enqueue_kind(c, d_values, kind, nt, np, ct, cp, d_edges, fa, ba, d_phi, d_theta)) return e;
+    } else if (const int e = cdf_enqueue(c, d_values, nt, np, ct, cp, d_edges, fa, ba, nullptr, 0.0, nullptr, d_phi,
+                                         d_theta, (CdfDeviceReport*)c->cdf_report.ptr, (unsigned*)c->cdf_sync.ptr))
+        return e;
+    return ok();
+}
+
+extern "C" int icp_phase_cdf_result(icp_context* c, const icp_cdf_policy* policy, icp_cdf_report* report)
+{
+    if (!c || !policy || !report) return fail(ICP_ERR_INVALID_ARGUMENT, "icp_phase_cdf_result: null argument");
+    std::memset(report, 0, sizeof *report);
+    if (!policy_ok(*policy)) return fail(ICP_ERR_INVALID_ARGUMENT, "Invalid CDF quality policy.");
+    if (!c->cdf_report.ptr) return fail(ICP_ERR_STATE, "icp_phase_cdf_result: no CDF build was enqueued");
+    ICP_CUDA(cudaSetDevice(c->device));
+    CdfDeviceReport r{};
+    ICP_CUDA(cudaMemcpyAsync(&r, c->cdf_report.ptr, sizeof r, cudaMemcpyDeviceToHost, c->stream));
+    ICP_CUDA(cudaStreamSynchronize(c->stream));
+    if (r.timeout)
+        if (const int e = cdf_clear(c, c->cdf_report.ptr, c->cdf_sync.ptr, 1)) return e;
+    return icp::cdf_finish(r, *policy, report);
 }
 
 extern "C" int icp_phase_cdf_build(icp_context* c, const double* d_values, uint32_t kind, uint32_t nt, uint32_t np,
@@ -546,40 +633,9 @@ extern "C" int icp_phase_cdf_build(icp_context* c, const double* d_values, uint3
     if (!c || !d_values || !d_phi || !d_theta || !report || !policy)
         return fail(ICP_ERR_INVALID_ARGUMENT, "icp_phase_cdf_build: null argument");
     std::memset(report, 0, sizeof *report);
-    const icp_cdf_policy& p = *policy;
-    if (!(H::finite(p.max_l1_error) && p.max_l1_error >= 0 && p.max_l1_error <= 2 && H::finite(p.max_lost_mass) &&
-          p.max_lost_mass >= 0 && p.max_lost_mass <= 1 && H::finite(p.max_coarsening_tv) && p.max_coarsening_tv >= 0 &&
-          p.max_coarsening_tv <= 1))
-        return fail(ICP_ERR_INVALID_ARGUMENT, "Invalid CDF quality policy.");
-    if (kind > 1) return fail(ICP_ERR_INVALID_ARGUMENT, "Unknown CDF input kind.");
-    if (!nt || !np || (uint64_t)nt * np > 0xffffffffull)
-        return fail(ICP_ERR_INVALID_ARGUMENT, "Unsupported phase grid dimensions.");
-    if (!ct || !cp || ct > nt || cp > np || nt % ct || np % cp)
-        return fail(ICP_ERR_INVALID_ARGUMENT, "Storage dimensions must divide histogram dimensions.");
-    if (!(fwd >= 0) || !(bwd >= 0) || !H::finite(fwd) || !H::finite(bwd))
-        return fail(ICP_ERR_INVALID_ARGUMENT, "Invalid pole masses.");
-    const double fa = fwd / np, ba = bwd / np;
-    if ((fwd > 0 && !(fa > 0)) || (bwd > 0 && !(ba > 0))) return fail(ICP_ERR_AUDIT, "Pole weight underflow.");
-    ICP_CUDA(cudaSetDevice(c->device));
-    std::vector<double> edges;
-    if (!H::u_edges(nt, edges)) return fail(ICP_ERR_INVALID_ARGUMENT, "Angular cells cannot be represented in binary64.");
-    ICP_CUDA(c->rec_edges.ensure(sizeof(double) * (nt + 1)));
-    ICP_CUDA(c->cdf_report.ensure(sizeof(CdfDeviceReport)));
-    ICP_CUDA(c->cdf_sync.ensure(2 * sizeof(unsigned)));
-    ICP_CUDA(cudaMemcpyAsync(c->rec_edges.ptr, edges.data(), sizeof(double) * (nt + 1), cudaMemcpyHostToDevice, c->stream));
-    if (kind == 1) {
-        // density input: the kernel's mass conversion (kind 1) is only reached through here
-        if (const int e = cdf_enqueue_kind(c, d_values, kind, nt, np, ct, cp, (const double*)c->rec_edges.ptr, fa, ba,
-                                           d_phi, d_theta))
-            return e;
-    } else if (const int e = cdf_enqueue(c, d_values, nt, np, ct, cp, (const double*)c->rec_edges.ptr, fa, ba, nullptr, 0.0,
-                                         nullptr, d_phi, d_theta, (CdfDeviceReport*)c->cdf_report.ptr,
-                                         (unsigned*)c->cdf_sync.ptr))
-        return e;
-    CdfDeviceReport r{};
-    ICP_CUDA(cudaMemcpyAsync(&r, c->cdf_report.ptr, sizeof r, cudaMemcpyDeviceToHost, c->stream));
-    ICP_CUDA(cudaStreamSynchronize(c->stream));
-    return icp::cdf_finish(r, p, report);
+    if (!policy_ok(*policy)) return fail(ICP_ERR_INVALID_ARGUMENT, "Invalid CDF quality policy.");
+    if (const int e = icp_phase_cdf_enqueue(c, d_values, kind, nt, np, fwd, bwd, ct, cp, d_phi, d_theta)) return e;
+    return icp_phase_cdf_result(c, policy, report);
 }
 
 extern "C" int icp_phase_cdf_build_batch(icp_context* c, const double* d_values, uint32_t count, uint32_t nt,
@@ -590,10 +646,7 @@ extern "C" int icp_phase_cdf_build_batch(icp_context* c, const double* d_values,
         return fail(ICP_ERR_INVALID_ARGUMENT, "icp_phase_cdf_build_batch: null argument");
     if (!count) return fail(ICP_ERR_INVALID_ARGUMENT, "icp_phase_cdf_build_batch: no records");
     const icp_cdf_policy& p = *policy;
-    if (!(H::finite(p.max_l1_error) && p.max_l1_error >= 0 && p.max_l1_error <= 2 && H::finite(p.max_lost_mass) &&
-          p.max_lost_mass >= 0 && p.max_lost_mass <= 1 && H::finite(p.max_coarsening_tv) && p.max_coarsening_tv >= 0 &&
-          p.max_coarsening_tv <= 1))
-        return fail(ICP_ERR_INVALID_ARGUMENT, "Invalid CDF quality policy.");
+    if (!policy_ok(p)) return fail(ICP_ERR_INVALID_ARGUMENT, "Invalid CDF quality policy.");
     if (!nt || !np || (uint64_t)nt * np > 0xffffffffull)
         return fail(ICP_ERR_INVALID_ARGUMENT, "Unsupported phase grid dimensions.");
     if (!ct || !cp || ct > nt || cp > np || nt % ct || np % cp)

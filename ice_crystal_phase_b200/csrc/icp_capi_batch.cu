@@ -188,8 +188,8 @@ int enqueue_finish(icp_context* c, const icp_drop_item* items, uint32_t count, c
     BatchState& B = c->batch;
     ICP_CUDA(c->b_rows.ensure(sizeof(double) * (s.nt + 1) * count));
     ICP_CUDA(c->b_dargs.ensure(sizeof(DiffractionArgs) * count));
-    ICP_CUDA(c->b_reports.ensure(sizeof(CdfDeviceReport) * count));
-    ICP_CUDA(c->b_sync.ensure(2 * sizeof(unsigned) * count));
+    ICP_CUDA(c->b_reports.ensure_zeroed(sizeof(CdfDeviceReport) * count, c->stream));
+    ICP_CUDA(c->b_sync.ensure_zeroed(2 * sizeof(unsigned) * count, c->stream));
     ICP_CUDA(B.h_dargs.ensure(sizeof(DiffractionArgs) * count));
     ICP_CUDA(B.h_stats.ensure(sb * count));
     ICP_CUDA(B.h_reports.ensure(sizeof(CdfDeviceReport) * count));
@@ -254,8 +254,8 @@ int prepare(icp_context* c, uint32_t count, const icp_batch_settings& s)
     ICP_CUDA(c->edges_f.ensure(sizeof(float) * (s.nt + 1)));
     ICP_CUDA(c->b_rows.ensure(sizeof(double) * (s.nt + 1) * count));
     ICP_CUDA(c->b_dargs.ensure(sizeof(DiffractionArgs) * count));
-    ICP_CUDA(c->b_reports.ensure(sizeof(CdfDeviceReport) * count));
-    ICP_CUDA(c->b_sync.ensure(2 * sizeof(unsigned) * count));
+    ICP_CUDA(c->b_reports.ensure_zeroed(sizeof(CdfDeviceReport) * count, c->stream));
+    ICP_CUDA(c->b_sync.ensure_zeroed(2 * sizeof(unsigned) * count, c->stream));
     ICP_CUDA(B.h_table.ensure(pb * count));
     ICP_CUDA(B.h_chunks.ensure(sizeof(unsigned long long) * (count + 1)));
     ICP_CUDA(B.h_edges.ensure(sizeof(double) * (s.nt + 1)));
@@ -263,9 +263,10 @@ int prepare(icp_context* c, uint32_t count, const icp_batch_settings& s)
     ICP_CUDA(B.h_stats.ensure(sb * count));
     ICP_CUDA(B.h_reports.ensure(sizeof(CdfDeviceReport) * count));
     ICP_CUDA(B.h_powers.ensure(sizeof(double) * count));
-    uint32_t cw = 0;
-    if (const int e = choose_cdf_width(c, s.ct, s.cp, cw)) return e;
-    ICP_CUDA(c->cdf_partial.ensure(cdf_partial_bytes() * ((s.cp + cw - 1) / cw)));
+    CdfShape sh{};
+    const bool tma_ok = s.nt == s.ct && s.np == s.cp && s.np % 2 == 0; // the record histograms are 256-byte aligned
+    if (const int e = cdf_shape(c, s.nt, s.np, s.ct, s.cp, tma_ok, sh)) return e;
+    ICP_CUDA(c->cdf_partial.ensure(cdf_partial_bytes() * ((s.cp + sh.cw - 1) / sh.cw)));
     ICP_CUDA(c->cdf_colsum.ensure(sizeof(double) * s.cp));
     return ICP_OK;
 }
@@ -405,6 +406,12 @@ int batch(icp_context* c, const icp_drop_item* items, uint32_t count, const icp_
         rep.cdf.status = (uint32_t)e;
         if (e && !first_error) first_error = e;
     }
+    for (uint32_t i = 0; i < count; ++i)
+        if (static_cast<const CdfDeviceReport*>(B.h_reports.ptr)[i].timeout) {
+            // a build gave up waiting: its counters stopped mid-way; clear every record's
+            if (const int e = cdf_clear(c, c->b_reports.ptr, c->b_sync.ptr, count)) return e;
+            break;
+        }
     if (first_error) return first_error; // the message of the first failing record stands
     return ok();
 }

@@ -366,8 +366,8 @@ int drop_record(icp_context* c, const icp_drop_record* r, double* phi_out, doubl
     ICP_CUDA(c->stats.ensure(sb));
     ICP_CUDA(c->rows.ensure(sizeof(double) * (r->nt + 1)));
     ICP_CUDA(c->dargs.ensure(sizeof(DiffractionArgs)));
-    ICP_CUDA(c->cdf_report.ensure(sizeof(CdfDeviceReport)));
-    ICP_CUDA(c->cdf_sync.ensure(2 * sizeof(unsigned)));
+    ICP_CUDA(c->cdf_report.ensure_zeroed(sizeof(CdfDeviceReport), c->stream));
+    ICP_CUDA(c->cdf_sync.ensure_zeroed(2 * sizeof(unsigned), c->stream));
     if (host) {
         ICP_CUDA(c->rec_phi.ensure(sizeof(double) * (r->cp + 1)));
         ICP_CUDA(c->rec_theta.ensure(sizeof(double) * (size_t)r->cp * (r->ct + 1)));
@@ -431,6 +431,8 @@ int drop_record(icp_context* c, const icp_drop_record* r, double* phi_out, doubl
     rep->seconds_trace = ms * 1e-3;
     cudaEventElapsedTime(&ms, c->ev1, c->ev2);
     rep->seconds_cdf = ms * 1e-3;
+    if (cdf.timeout)
+        if (const int e = cdf_clear(c, c->cdf_report.ptr, c->cdf_sync.ptr, 1)) return e;
     if (area_status) return area_status;
     const int st = finish_report(r, raw.data(), cdf, power, weight, rep);
     return st == ICP_OK ? ok() : st;

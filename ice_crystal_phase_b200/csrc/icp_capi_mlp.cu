@@ -736,6 +736,7 @@ int icp_mlp_gemm_bf16(icp_context* c, const void* d_a, const void* d_b, uint32_t
     g.ld_out = n;
     g.ld_t = m;
     g.error = (unsigned*)c->mlp_error.ptr;
+    g.wait_limit = c->wait_limit;
     const int e = mlp::gemm(d_a, d_b, g, accumulate ? mlp::kAtomicF32 : mlp::kStoreF32, split_k ? split_k : 1,
                             c->stream);
     count_launch();

@@ -3,29 +3,43 @@
 // Replaces the reference's eight host-synchronised stages (check density, reduce, measure,
 // coarsen, make weights / transpose, per-phi serial scan, 1-thread marginal, normalise,
 // audit, measure CDF: device/phase_cdf.cu:93-339 driven by src/phase_cdf.cpp:275-472) and
-// restates the CPU builder's arithmetic (hex_phase/src/phase_table.cpp:111-187):
-//   phase A  each block owns a strip of CW coarse phi columns: reads its fine strip once
-//            (coalesced), adds the pole caps to the end rows, aggregates conservatively
-//            (Kahan, row-major order), keeps the coarse strip in shared memory, and
-//            publishes fine / coarse moments and its maximum;
-//   barrier
-//   phase B  coarsening TV, the weights w = coarse / largest (parallel), then per column an
-//            ordered binary64 scan in ascending theta (exact plateaus, monotone prefixes) kept
-//            in shared memory, column sums published;
-//   barrier
-//   phase C  ordered marginal scan over all column sums (every block, identical result),
-//            normalisation (empty column -> the stored u edges), the phi marginal, and the
-//            L1 / lost-mass / malformed audit and stored moments from the written values;
-//   the last block to finish reduces the audits.
+// restates the CPU builder's arithmetic (hex_phase/src/phase_table.cpp:111-187).
+//
+// Each block owns a strip of CW stored phi columns and keeps it in shared memory for the whole
+// build: the coarse masses (array A) and the column prefixes (array B).
+//   phase A  without coarsening the fine strip arrives by 3-D TMA boxes (cp.async.bulk.tensor,
+//            one mbarrier per box; the rows of a box are processed as soon as it lands), else
+//            each thread aggregates its coarse cells from global memory (Kahan, row-major fine
+//            order).  Pole caps, per-row additions and the density conversion are applied in
+//            the same pass, which also publishes the fine / coarse moments and the maximum.
+//   barrier 1 (largest coarse mass, stored total)
+//   phase B  weights w = coarse / largest for the strip (all threads; the audit's p = coarse /
+//            stored total in the same pass), then one thread per column runs the reference's
+//            ordered ascending-theta binary64 scan (s += w) over shared memory and publishes its
+//            column sum.
+//   barrier 2 (all column sums)
+//   phase C  warp 0 runs the ordered marginal scan (phi[j+1] = phi[j] + colsum[j]) while the
+//            other warps normalise this strip's conditionals and write T (its rows are one
+//            contiguous range of the phi-major output, so the stores are coalesced); then every
+//            thread audits its cells (L1, lost mass, malformed, stored moments) from shared
+//            memory, and the last block to finish reduces the audits in a fixed order and
+//            resets the barrier counters for the next launch.
 // Grid barriers are counter spins with an iteration limit: on expiry the kernel records
-// ICP_ERR_TIMEOUT and returns without writing further output.
-#include <cooperative_groups.h>
+// ICP_ERR_TIMEOUT and returns without writing further output; the host then clears the
+// counters.  Where the two strip arrays do not fit in shared memory, phase C re-reads the coarse
+// masses from global memory instead of keeping them (`keep` = 0).
+#include <algorithm>
+#include <cfloat>
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "icp_internal.h"
+#include "icp_umma.cuh"
 
 namespace icp {
+
+namespace {
 
 struct KSum {
     double v, c;
@@ -37,11 +51,16 @@ struct KSum {
     }
 };
 
-struct BlockPartial {
-    double fine_mass, fine_axial, stored_mass, stored_axial, largest;
-    double tv, l1, lost, max_err, recovered, axial;
-    unsigned long long invalid, lost_cells, malformed, underflow;
+// Per-block partial results; doubles first (index constants below), then the counters.
+enum : uint32_t {
+    kFineMass, kFineAxial, kStoredMass, kStoredAxial, kLargest, kTv, kL1, kLost, kMaxErr, kRecovered, kAxial,
+    kInvalid, kLostCells, kMalformed, kUnderflow, kPartialWords
 };
+constexpr uint32_t kPartialDoubles = kInvalid;
+struct BlockPartial {
+    unsigned long long w[kPartialWords]; // doubles stored by their bits
+};
+static_assert(sizeof(BlockPartial) == kCdfPartialBytes, "partial slot size");
 
 struct CdfParams {
     const CdfBatchRecord* recs; // batched: block b builds strip b % strips of record b / strips
@@ -50,11 +69,12 @@ struct CdfParams {
     const double* edges; // fine edges, nt+1
     double* phi;
     double* theta;
-    double* colsum;       // cp
-    BlockPartial* partial; // gridDim.x
+    double* colsum;        // cp
+    BlockPartial* partial; // one per strip
     CdfDeviceReport* report;
-    unsigned* sync;       // [0] barrier arrivals, [1] finished-block ticket
+    unsigned* sync; // [0] barrier arrivals, [1] finished-block ticket; zero at launch, zero again at exit
     uint32_t kind, nt, np, ct, cp, dt, dp, cw;
+    uint32_t keep, tma, box_rows, boxes, rows_alloc, z0, spin_limit, pad;
     double fwd_add, bwd_add;
     const double* row_add;
     const unsigned long long* pole_fx;
@@ -83,22 +103,62 @@ __device__ __forceinline__ CdfAdds cdf_adds(const CdfParams& P, unsigned long lo
     return a;
 }
 
-constexpr unsigned kThreads = 256;
+constexpr unsigned kThreads = 512;
+constexpr unsigned kWarps = kThreads / 32;
+constexpr unsigned kMaxBoxes = 16;
 constexpr unsigned kSpinLimit = 1u << 22;
+constexpr unsigned kFull = 0xffffffffu;
 
-__device__ __forceinline__ bool grid_wait(unsigned* counter, unsigned target, unsigned* timeout_flag)
+// Shared-memory layout of one block (the same function sizes the launch on the host).
+struct Layout {
+    size_t a, b, e, s, phi, bar, total;
+};
+__host__ __device__ inline size_t take(size_t& off, size_t bytes)
+{
+    const size_t o = off;
+    off = (off + bytes + 127) / 128 * 128;
+    return o;
+}
+__host__ __device__ inline Layout layout_of(uint32_t ct, uint32_t cp, uint32_t cw, uint32_t rows_alloc, uint32_t keep)
+{
+    Layout L{};
+    size_t off = 0;
+    L.a = take(off, sizeof(double) * (size_t)rows_alloc * cw);
+    L.b = keep ? take(off, sizeof(double) * (size_t)ct * cw) : L.a;
+    L.e = take(off, sizeof(double) * (ct + 1));
+    L.s = take(off, sizeof(double) * cp);
+    L.phi = take(off, sizeof(double) * (cw + 1));
+    L.bar = take(off, sizeof(uint64_t) * kMaxBoxes);
+    L.total = off;
+    return L;
+}
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid barrier in two halves, so that independent work can run between arrival and wait.
+__device__ __forceinline__ void grid_arrive(unsigned* counter)
 {
     __syncthreads();
-    __shared__ int ok;
     if (threadIdx.x == 0) {
         __threadfence();
         atomicAdd(counter, 1u);
+    }
+}
+__device__ __forceinline__ bool grid_wait(unsigned* counter, unsigned target, unsigned limit, unsigned* timeout_flag)
+{
+    __shared__ int ok;
+    if (threadIdx.x == 0) {
         unsigned spins = 0;
-        while (*((volatile unsigned*)counter) < target && spins < kSpinLimit) {
-            __nanosleep(64);
+        while (ld_acquire(counter) < target && spins < limit) {
+            __nanosleep(32);
             ++spins;
         }
-        ok = spins < kSpinLimit;
+        ok = spins < limit;
         if (!ok) atomicExch(timeout_flag, 1u);
         __threadfence();
     }
@@ -106,14 +166,18 @@ __device__ __forceinline__ bool grid_wait(unsigned* counter, unsigned target, un
     return ok;
 }
 
-__device__ __forceinline__ double fine_mass_at(const CdfParams& P, const CdfAdds& A, uint32_t i, uint32_t j)
+__device__ __forceinline__ double adjust_fine(const CdfParams& P, const CdfAdds& A, double m, uint32_t i, double du)
 {
-    double m = P.values[(size_t)i * P.np + j];
-    if (P.kind == 1) m = m * (P.edges[i + 1] - P.edges[i]);
+    if (P.kind == 1) m = m * du;
     if (A.row) m += A.row[i];
     if (i == 0) m += A.fwd;
     if (i + 1 == P.nt) m += A.bwd;
     return m;
+}
+
+__device__ __forceinline__ double fine_mass_at(const CdfParams& P, const CdfAdds& A, uint32_t i, uint32_t j)
+{
+    return adjust_fine(P, A, P.values[(size_t)i * P.np + j], i, P.kind == 1 ? P.edges[i + 1] - P.edges[i] : 0.0);
 }
 
 // Conservative aggregate of one coarse cell: Kahan sum in row-major fine order
@@ -126,42 +190,90 @@ __device__ __forceinline__ double coarse_at(const CdfParams& P, const CdfAdds& A
     return acc.v;
 }
 
-template <class T> __device__ __forceinline__ T block_sum(T x, T* red)
+// Block sum (thread 0's result; warps added in order).
+template <class T> __device__ T block_sum(T x, T* red)
 {
-    for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
     __syncthreads();
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = x;
     __syncthreads();
     T s = T(0);
     if (threadIdx.x == 0)
-        for (unsigned w = 0; w < blockDim.x / 32; ++w) s += red[w];
-    return s; // valid in thread 0
+        for (unsigned w = 0; w < kWarps; ++w) s += red[w];
+    return s;
 }
-__device__ __forceinline__ double block_max(double x, double* red)
+__device__ double block_max(double x, double* red)
 {
-    for (int o = 16; o; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+    for (int o = 16; o; o >>= 1) x = fmax(x, __shfl_xor_sync(kFull, x, o));
     __syncthreads();
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = x;
     __syncthreads();
     double s = 0.0;
     if (threadIdx.x == 0)
-        for (unsigned w = 0; w < blockDim.x / 32; ++w) s = fmax(s, red[w]);
+        for (unsigned w = 0; w < kWarps; ++w) s = fmax(s, red[w]);
     return s;
 }
 
-__global__ void __launch_bounds__(kThreads) cdf_build_kernel(const CdfParams P0)
+// One partial word over all strips, reduced by one warp in a fixed order (lane l adds strips
+// l, l + 32, ... in order, then a shuffle tree); the result is lane 0's, broadcast, so every
+// block that runs this on the same partials obtains the same bits.
+__device__ __forceinline__ double warp_reduce_word(const BlockPartial* part, uint32_t strips, uint32_t word, bool is_max)
 {
-    extern __shared__ __align__(16) double strip[]; // ct x CW coarse strip, then phi strip (CW+1)
-    __shared__ double red_d[kThreads / 32];
-    __shared__ unsigned long long red_u[kThreads / 32];
-    __shared__ double s_glob[6];
+    const uint32_t lane = threadIdx.x & 31;
+    double v = 0.0;
+    for (uint32_t k = lane; k < strips; k += 32) {
+        const double x = __longlong_as_double((long long)__ldcg(&part[k].w[word]));
+        v = is_max ? fmax(v, x) : v + x;
+    }
+    for (int o = 16; o; o >>= 1) {
+        const double y = __shfl_down_sync(kFull, v, o);
+        v = is_max ? fmax(v, y) : v + y;
+    }
+    return __shfl_sync(kFull, v, 0);
+}
+__device__ __forceinline__ unsigned long long warp_reduce_count(const BlockPartial* part, uint32_t strips, uint32_t word)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    unsigned long long v = 0;
+    for (uint32_t k = lane; k < strips; k += 32) v += __ldcg(&part[k].w[word]);
+    for (int o = 16; o; o >>= 1) v += __shfl_down_sync(kFull, v, o);
+    return __shfl_sync(kFull, v, 0);
+}
+
+__device__ __forceinline__ void put(BlockPartial& p, uint32_t word, double x)
+{
+    p.w[word] = (unsigned long long)__double_as_longlong(x);
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int32_t x, int32_t y,
+                                            int32_t z)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::
+            "r"(umma::smem_u32(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(z), "r"(umma::smem_u32(bar))
+        : "memory");
+}
+
+__global__ void __launch_bounds__(kThreads, 2) cdf_build_kernel(const __grid_constant__ CUtensorMap map,
+                                                                 const CdfParams P0)
+{
+    extern __shared__ unsigned char smem_raw[];
+    // TMA box images start 128-byte aligned: align the base (the launch adds 128 bytes of slack)
+    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    __shared__ double red_d[kWarps];
+    __shared__ unsigned long long red_u[kWarps];
+    __shared__ double s_tot[4]; // fine total, stored total, largest, marginal total
+    __shared__ unsigned long long s_fin[kPartialWords];
     __shared__ int s_last;
 
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t strips = P0.strips ? P0.strips : gridDim.x;
+    const uint32_t rec = P0.strips ? blockIdx.x / strips : 0u;
     const uint32_t sb = P0.strips ? blockIdx.x % strips : blockIdx.x; // this block's strip of its record
     CdfParams P = P0;
     if (P0.recs) {
-        const CdfBatchRecord& R = P0.recs[blockIdx.x / strips];
+        const CdfBatchRecord& R = P0.recs[rec];
         P.values = R.values;
         P.phi = R.phi;
         P.theta = R.theta;
@@ -175,193 +287,237 @@ __global__ void __launch_bounds__(kThreads) cdf_build_kernel(const CdfParams P0)
         P.fwd_add = R.fwd_add;
         P.bwd_add = R.bwd_add;
     }
-    const uint32_t c0 = sb * P.cw;
-    const uint32_t c1 = min(P.cp, c0 + P.cw);
+    const uint32_t limit = P.spin_limit ? P.spin_limit : kSpinLimit;
+    const uint32_t CW = P.cw, ct = P.ct;
+    const uint32_t c0 = sb * CW;
+    const uint32_t c1 = min(P.cp, c0 + CW);
     const uint32_t w = c1 > c0 ? c1 - c0 : 0u; // columns in this strip
-    const uint32_t CW = P.cw;
-    double* sphi = strip + (size_t)P.ct * CW;
+    const Layout Lo = layout_of(ct, P.cp, CW, P.rows_alloc, P.keep);
+    double* A = reinterpret_cast<double*>(smem + Lo.a); // coarse masses, then p = coarse / stored total
+    double* B = reinterpret_cast<double*>(smem + Lo.b); // weights, prefixes, normalised conditionals
+    double* E = reinterpret_cast<double*>(smem + Lo.e); // coarse u edges
+    double* S = reinterpret_cast<double*>(smem + Lo.s); // all column sums
+    double* sphi = reinterpret_cast<double*>(smem + Lo.phi);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + Lo.bar);
+    // per-cell passes: thread -> (column my_cl, rows my_r, my_r + rstep, ...)
+    const uint32_t rstep = kThreads / CW;
+    const uint32_t my_cl = tid % CW, my_r = tid / CW;
+    const bool act = my_r < rstep && my_cl < w;
 
     // ------------------------------------------------------------ phase A
+    if (P.tma) {
+        if (tid == 0) {
+            for (uint32_t k = 0; k < P.boxes; ++k) umma::mbar_init(&bars[k], 1);
+            umma::mbar_fence_init();
+        }
+        __syncthreads();
+        if (tid == 0) {
+            const uint32_t box_bytes = P.box_rows * CW * (uint32_t)sizeof(double);
+            for (uint32_t k = 0; k < P.boxes; ++k) {
+                umma::mbar_arrive_expect_tx(&bars[k], box_bytes);
+                tma_load_3d(A + (size_t)k * P.box_rows * CW, &map, &bars[k], (int32_t)c0, (int32_t)(k * P.box_rows),
+                            (int32_t)(P.z0 + rec));
+            }
+        }
+    }
+    for (uint32_t i = tid; i <= ct; i += kThreads) E[i] = P.edges[(size_t)i * P.dt];
+    __syncthreads();
+
     KSum fm{0, 0}, fa{0, 0}, sm{0, 0}, sa{0, 0};
     double largest = 0.0;
     unsigned long long invalid = 0ull, pole_bad = 0ull;
     const CdfAdds adds = cdf_adds(P, &pole_bad);
-    if (threadIdx.x == 0) invalid += pole_bad;
-    const uint32_t cells = P.ct * w;
-    for (uint32_t q = threadIdx.x; q < cells; q += blockDim.x) {
-        const uint32_t ci = q / w, cl = q % w, cj = c0 + cl;
-        KSum acc{0, 0};
-        for (uint32_t i = ci * P.dt; i < (ci + 1) * P.dt; ++i) {
-            const double mu = 1.0 - P.edges[i] - P.edges[i + 1];
-            for (uint32_t j = cj * P.dp; j < (cj + 1) * P.dp; ++j) {
-                const double m = fine_mass_at(P, adds, i, j);
-                if (!(m >= 0.0) || !(m <= 1.7976931348623157e308)) ++invalid;
-                acc.add(m);
-                fm.add(m);
-                fa.add(m * mu);
-            }
+    if (tid == 0) invalid += pole_bad;
+    if (P.tma) {
+        // dt = dp = 1: coarse = fine; the stored moments equal the fine ones.  The box waits
+        // keep the default limit, so that no copy is still landing when the block leaves.
+        bool late = false;
+        for (uint32_t k = 0; k < P.boxes; ++k) {
+            if (!umma::mbar_wait(&bars[k], 0, kSpinLimit)) late = true;
+            const uint32_t r1 = min(ct, (k + 1) * P.box_rows);
+            if (act)
+                for (uint32_t i = k * P.box_rows + my_r; i < r1; i += rstep) {
+                    const double e0 = E[i], e1 = E[i + 1];
+                    const double m = adjust_fine(P, adds, A[(size_t)i * CW + my_cl], i, e1 - e0);
+                    if (!(m >= 0.0) || !(m <= DBL_MAX)) ++invalid;
+                    A[(size_t)i * CW + my_cl] = m;
+                    fm.add(m);
+                    fa.add(m * (1.0 - e0 - e1));
+                    largest = fmax(largest, m);
+                }
         }
-        const double c = acc.v;
-        strip[(size_t)ci * CW + cl] = c;
-        const double E0 = P.edges[(size_t)ci * P.dt], E1 = P.edges[(size_t)(ci + 1) * P.dt];
-        sm.add(c);
-        sa.add(c * (1.0 - E0 - E1));
-        largest = fmax(largest, c);
+        if (late) atomicExch(&P.report->timeout, 1u);
+    } else if (act) {
+        for (uint32_t ci = my_r; ci < ct; ci += rstep) {
+            const uint32_t cj = c0 + my_cl;
+            KSum acc{0, 0};
+            for (uint32_t i = ci * P.dt; i < (ci + 1) * P.dt; ++i) {
+                const double mu = 1.0 - P.edges[i] - P.edges[i + 1];
+                for (uint32_t j = cj * P.dp; j < (cj + 1) * P.dp; ++j) {
+                    const double m = fine_mass_at(P, adds, i, j);
+                    if (!(m >= 0.0) || !(m <= DBL_MAX)) ++invalid;
+                    acc.add(m);
+                    fm.add(m);
+                    fa.add(m * mu);
+                }
+            }
+            const double c = acc.v;
+            A[(size_t)ci * CW + my_cl] = c;
+            sm.add(c);
+            sa.add(c * (1.0 - E[ci] - E[ci + 1]));
+            largest = fmax(largest, c);
+        }
     }
     {
         const double a = block_sum(fm.v + fm.c, red_d);
         const double b = block_sum(fa.v + fa.c, red_d);
-        const double c = block_sum(sm.v + sm.c, red_d);
-        const double d = block_sum(sa.v + sa.c, red_d);
+        const double c = P.tma ? a : block_sum(sm.v + sm.c, red_d);
+        const double d = P.tma ? b : block_sum(sa.v + sa.c, red_d);
         const double e = block_max(largest, red_d);
         const unsigned long long f = block_sum(invalid, red_u);
-        if (threadIdx.x == 0) {
+        if (tid == 0) {
             BlockPartial& bp = P.partial[sb];
-            bp.fine_mass = a;
-            bp.fine_axial = b;
-            bp.stored_mass = c;
-            bp.stored_axial = d;
-            bp.largest = e;
-            bp.invalid = f;
+            put(bp, kFineMass, a);
+            put(bp, kFineAxial, b);
+            put(bp, kStoredMass, c);
+            put(bp, kStoredAxial, d);
+            put(bp, kLargest, e);
+            bp.w[kInvalid] = f;
         }
     }
-    if (!grid_wait(&P.sync[0], strips, &P.report->timeout)) return;
+    grid_arrive(&P.sync[0]);
+    if (!grid_wait(&P.sync[0], strips, limit, &P.report->timeout)) return;
 
     // ------------------------------------------------------------ phase B
-    // block partials staged through shared memory (L2 loads in parallel), then summed in
-    // block order by one thread so that every block derives identical totals
-    double* stage = sphi + CW + 1; // scratch: max(14 * strips, cp) doubles
-    for (unsigned k = threadIdx.x; k < strips; k += blockDim.x) {
-        const BlockPartial* bp = P.partial + k;
-        stage[5 * k + 0] = __ldcg(&bp->fine_mass);
-        stage[5 * k + 1] = __ldcg(&bp->fine_axial);
-        stage[5 * k + 2] = __ldcg(&bp->stored_mass);
-        stage[5 * k + 3] = __ldcg(&bp->stored_axial);
-        stage[5 * k + 4] = __ldcg(&bp->largest);
+    if (warp < 3) {
+        const double v = warp_reduce_word(P.partial, strips, warp == 0 ? kFineMass : warp == 1 ? kStoredMass : kLargest,
+                                          warp == 2);
+        if (lane == 0) s_tot[warp] = v;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double a = 0, b = 0, c = 0, d = 0, e = 0;
-        for (unsigned k = 0; k < strips; ++k) {
-            a += stage[5 * k + 0];
-            b += stage[5 * k + 1];
-            c += stage[5 * k + 2];
-            d += stage[5 * k + 3];
-            e = fmax(e, stage[5 * k + 4]);
-        }
-        s_glob[0] = a;
-        s_glob[1] = b;
-        s_glob[2] = c;
-        s_glob[3] = d;
-        s_glob[4] = e;
-    }
-    __syncthreads();
-    const double fine_total = s_glob[0], stored_total = s_glob[2], big = s_glob[4];
+    const double fine_total = s_tot[0], stored_total = s_tot[1], big = s_tot[2];
     KSum tv{0, 0};
     if (P.dt > 1 || P.dp > 1) {
         const uint32_t fw = w * P.dp;
-        for (uint32_t q = threadIdx.x; q < P.nt * fw; q += blockDim.x) {
+        for (uint32_t q = tid; q < P.nt * fw; q += kThreads) {
             const uint32_t i = q / fw, j = c0 * P.dp + q % fw;
             const uint32_t ci = i / P.dt, cl = j / P.dp - c0;
-            const double fraction = (P.edges[i + 1] - P.edges[i]) /
-                                    (P.edges[(size_t)(ci + 1) * P.dt] - P.edges[(size_t)ci * P.dt]) / P.dp;
-            tv.add(fabs(fine_mass_at(P, adds, i, j) / fine_total - strip[(size_t)ci * CW + cl] / stored_total * fraction));
+            const double fraction = (P.edges[i + 1] - P.edges[i]) / (E[ci + 1] - E[ci]) / P.dp;
+            tv.add(fabs(fine_mass_at(P, adds, i, j) / fine_total - A[(size_t)ci * CW + cl] / stored_total * fraction));
         }
+        __syncthreads();
     }
-    // weights w = coarse / largest for the whole strip in parallel (the ordered chains below
-    // then carry only additions); the coarse values are recomputed in phase C for the audit
-    unsigned long long underflow = 0ull;
-    for (uint32_t q = threadIdx.x; q < P.ct * w; q += blockDim.x) {
-        const uint32_t i = q / w, cl = q % w;
-        const double c = strip[(size_t)i * CW + cl];
-        const double x = c / big;
-        if (c > 0 && !(x > 0)) ++underflow;
-        strip[(size_t)i * CW + cl] = x;
-    }
+    // weights w = coarse / largest for the whole strip in parallel (the ordered chains below then
+    // carry only additions); with `keep`, the audit's p = coarse / stored total in the same pass
+    unsigned long long underflow = 0ull, malformed = 0ull;
+    if (act)
+        for (uint32_t i = my_r; i < ct; i += rstep) {
+            const size_t k = (size_t)i * CW + my_cl;
+            const double c = A[k];
+            const double x = c / big;
+            if (c > 0 && !(x > 0)) ++underflow;
+            if (P.keep) {
+                const double p = c / stored_total;
+                if (c > 0 && !(p > 0)) ++malformed;
+                A[k] = p;
+            }
+            B[k] = x;
+        }
     __syncthreads();
-    if (threadIdx.x < w) {
+    if (tid < w) {
         // ordered ascending-theta scan of one phi column; the unnormalised prefix of row i+1
         // replaces the weight of row i in place (each column belongs to one thread)
-        const uint32_t cl = threadIdx.x, j = c0 + cl;
+        const uint32_t cl = tid;
         double s = 0.0;
 #pragma unroll 8
-        for (uint32_t i = 0; i < P.ct; ++i) {
-            s += strip[(size_t)i * CW + cl];
-            strip[(size_t)i * CW + cl] = s;
+        for (uint32_t i = 0; i < ct; ++i) {
+            s += B[(size_t)i * CW + cl];
+            B[(size_t)i * CW + cl] = s;
         }
-        P.colsum[j] = s;
+        P.colsum[c0 + cl] = s;
     }
     {
         const double t = block_sum(tv.v + tv.c, red_d);
         const unsigned long long u = block_sum(underflow, red_u);
-        if (threadIdx.x == 0) {
-            P.partial[sb].tv = 0.5 * t;
-            P.partial[sb].underflow = u;
+        if (tid == 0) {
+            put(P.partial[sb], kTv, 0.5 * t);
+            P.partial[sb].w[kUnderflow] = u;
         }
     }
-    if (!grid_wait(&P.sync[0], 2u * strips, &P.report->timeout)) return;
+    grid_arrive(&P.sync[0]);
+    if (!grid_wait(&P.sync[0], 2u * strips, limit, &P.report->timeout)) return;
 
     // ------------------------------------------------------------ phase C
-    for (uint32_t j = threadIdx.x; j < P.cp; j += blockDim.x) stage[j] = __ldcg(P.colsum + j);
+    for (uint32_t j = tid; j < P.cp; j += kThreads) S[j] = __ldcg(P.colsum + j);
     __syncthreads();
-    if (threadIdx.x == 0) {
-        // ordered marginal scan (phase_table.cpp:154): phi[j+1] = phi[j] + colsum[j]
-        double a = 0.0;
-        for (uint32_t j = 0; j < c0; ++j) a += stage[j];
-        sphi[0] = a;
-        for (uint32_t cl = 0; cl < w; ++cl) {
-            a += stage[c0 + cl];
-            sphi[cl + 1] = a;
+    const uint32_t stride = ct + 1;
+    if (warp == 0) {
+        if (lane == 0) {
+            // ordered marginal scan (phase_table.cpp:154): phi[j+1] = phi[j] + colsum[j]
+            double a = 0.0;
+#pragma unroll 8
+            for (uint32_t j = 0; j < c0; ++j) a += S[j];
+            sphi[0] = a;
+            for (uint32_t cl = 0; cl < w; ++cl) {
+                a += S[c0 + cl];
+                sphi[cl + 1] = a;
+            }
+#pragma unroll 8
+            for (uint32_t j = c1; j < P.cp; ++j) a += S[j];
+            s_tot[3] = a;
         }
-        for (uint32_t j = c1; j < P.cp; ++j) a += stage[j];
-        s_glob[5] = a;
+    } else {
+        // normalised conditionals of this strip, written once each: its output rows are the
+        // contiguous range theta[c0*(ct+1) .. c1*(ct+1)); element (cl, i) from the prefix of row
+        // i kept at B[(i-1)*CW + cl], and kept normalised there for the audit
+        const uint32_t span = w * stride, step = kThreads - 32;
+        uint32_t q = tid - 32, cl = q / stride, i = q % stride;
+        double* out = P.theta + (size_t)c0 * stride;
+        for (; q < span; q += step) {
+            const double cs = S[c0 + cl];
+            double v;
+            if (i == 0) v = 0.0;
+            else if (i == ct) v = 1.0;
+            else v = cs > 0 ? B[(size_t)(i - 1) * CW + cl] / cs : E[i];
+            out[q] = v;
+            if (i > 0) B[(size_t)(i - 1) * CW + cl] = v;
+            i += step;
+            while (i >= stride) {
+                i -= stride;
+                ++cl;
+            }
+        }
     }
     __syncthreads();
-    const double total = s_glob[5];
-    // normalised marginal for this strip: phi[0] = 0, phi[cp] = 1, interior / total
-    if (threadIdx.x <= w) {
-        const uint32_t j = c0 + threadIdx.x;
-        if (threadIdx.x > 0 || c0 == 0) {
-            double v = sphi[threadIdx.x];
-            if (j == 0) v = 0.0;
-            else if (j == P.cp) v = 1.0;
-            else v = v / total;
-            P.phi[j] = v;
-        }
-    }
-    __syncthreads();
-    for (uint32_t cl = threadIdx.x; cl <= w; cl += blockDim.x) {
+    const double total = s_tot[3];
+    // normalised marginal for this strip: phi[0] = 0, phi[cp] = 1, interior / total; the boundary
+    // value j = c0 > 0 belongs to the previous strip's output
+    for (uint32_t cl = tid; cl <= w; cl += kThreads) {
         const uint32_t j = c0 + cl;
-        double v = sphi[cl];
-        sphi[cl] = (j == 0) ? 0.0 : (j == P.cp ? 1.0 : v / total);
+        const double v = j == 0 ? 0.0 : (j == P.cp ? 1.0 : sphi[cl] / total);
+        sphi[cl] = v;
+        if (cl > 0 || c0 == 0) P.phi[j] = v;
     }
     __syncthreads();
-    KSum l1{0, 0}, lost{0, 0}, rec{0, 0}, ax{0, 0};
+    KSum l1{0, 0}, lost{0, 0}, recv{0, 0}, ax{0, 0};
     double max_err = 0.0;
-    unsigned long long lost_cells = 0ull, malformed = 0ull;
-    const uint32_t stride = P.ct + 1;
-    // this strip's output rows are contiguous: theta[c0*(ct+1) .. c1*(ct+1)); every element is
-    // written once, from the prefixes kept in shared memory (prefix of row i at strip[i-1])
-    const uint32_t span = w * stride;
-#pragma unroll 2
-    for (uint32_t q = threadIdx.x; q < span; q += blockDim.x) {
-        const uint32_t cl = q / stride, i = q % stride, j = c0 + cl;
-        const double cs = stage[j];
-        auto norm = [&](uint32_t k) -> double {
-            if (k == 0) return 0.0;
-            if (k == P.ct) return 1.0;
-            return cs > 0 ? strip[(size_t)(k - 1) * CW + cl] / cs : P.edges[(size_t)k * P.dt];
-        };
-        const double b0 = norm(i);
-        if (i < P.ct) {
-            const double b1 = norm(i + 1);
-            const double a0 = sphi[cl], a1 = sphi[cl + 1];
+    unsigned long long lost_cells = 0ull;
+    if (act) {
+        const double a0 = sphi[my_cl], a1 = sphi[my_cl + 1];
+        for (uint32_t i = my_r; i < ct; i += rstep) {
+            const double b0 = i == 0 ? 0.0 : B[(size_t)(i - 1) * CW + my_cl];
+            const double b1 = B[(size_t)i * CW + my_cl]; // row ct - 1 holds 1
             const double qv = (a1 - a0) * (b1 - b0);
-            const double c = coarse_at(P, adds, i, j);
-            const double p = c / stored_total;
-            const bool bad = !(qv >= 0.0) || !(qv <= 1.7976931348623157e308) || a1 < a0 || b1 < b0;
+            double p;
+            if (P.keep) {
+                p = A[(size_t)i * CW + my_cl];
+            } else {
+                const double c = coarse_at(P, adds, i, c0 + my_cl);
+                p = c / stored_total;
+                if (c > 0 && !(p > 0)) ++malformed;
+            }
+            const bool bad = !(qv >= 0.0) || !(qv <= DBL_MAX) || a1 < a0 || b1 < b0;
             if (bad) ++malformed;
-            if (c > 0 && !(p > 0)) ++malformed;
             const double err = fabs(p - qv);
             l1.add(err);
             max_err = fmax(max_err, err);
@@ -369,29 +525,27 @@ __global__ void __launch_bounds__(kThreads) cdf_build_kernel(const CdfParams P0)
                 lost.add(p);
                 ++lost_cells;
             }
-            rec.add(qv);
-            const double E0 = P.edges[(size_t)i * P.dt], E1 = P.edges[(size_t)(i + 1) * P.dt];
-            ax.add(qv * (1.0 - E0 - E1));
+            recv.add(qv);
+            ax.add(qv * (1.0 - E[i] - E[i + 1]));
         }
-        P.theta[(size_t)c0 * stride + q] = b0;
     }
     {
         const double a = block_sum(l1.v + l1.c, red_d);
         const double b = block_sum(lost.v + lost.c, red_d);
-        const double c = block_sum(rec.v + rec.c, red_d);
+        const double c = block_sum(recv.v + recv.c, red_d);
         const double d = block_sum(ax.v + ax.c, red_d);
         const double e = block_max(max_err, red_d);
         const unsigned long long f = block_sum(lost_cells, red_u);
         const unsigned long long g = block_sum(malformed, red_u);
-        if (threadIdx.x == 0) {
+        if (tid == 0) {
             BlockPartial& bp = P.partial[sb];
-            bp.l1 = a;
-            bp.lost = b;
-            bp.recovered = c;
-            bp.axial = d;
-            bp.max_err = e;
-            bp.lost_cells = f;
-            bp.malformed = g;
+            put(bp, kL1, a);
+            put(bp, kLost, b);
+            put(bp, kRecovered, c);
+            put(bp, kAxial, d);
+            put(bp, kMaxErr, e);
+            bp.w[kLostCells] = f;
+            bp.w[kMalformed] = g;
             __threadfence();
             s_last = (atomicAdd(&P.sync[1], 1u) == strips - 1);
         }
@@ -399,54 +553,77 @@ __global__ void __launch_bounds__(kThreads) cdf_build_kernel(const CdfParams P0)
     __syncthreads();
     if (!s_last) return;
     __threadfence();
-    // last block: stage every block's audit partials (parallel L2 loads), sum in block order
-    constexpr unsigned kF = 14;
-    for (unsigned k = threadIdx.x; k < strips; k += blockDim.x) {
-        const BlockPartial* bp = P.partial + k;
-        double* o = stage + (size_t)kF * k;
-        o[0] = __ldcg(&bp->fine_mass);
-        o[1] = __ldcg(&bp->fine_axial);
-        o[2] = __ldcg(&bp->stored_mass);
-        o[3] = __ldcg(&bp->stored_axial);
-        o[4] = __ldcg(&bp->tv);
-        o[5] = __ldcg(&bp->l1);
-        o[6] = __ldcg(&bp->lost);
-        o[7] = __ldcg(&bp->recovered);
-        o[8] = __ldcg(&bp->axial);
-        o[9] = __ldcg(&bp->max_err);
-        o[10] = __longlong_as_double((long long)__ldcg(&bp->lost_cells));
-        o[13] = __longlong_as_double((long long)__ldcg(&bp->malformed));
-        o[11] = __longlong_as_double((long long)__ldcg(&bp->invalid));
-        o[12] = __longlong_as_double((long long)__ldcg(&bp->underflow));
+    // last block: warp f reduces partial word f over all strips in a fixed order
+    if (warp < kPartialWords) {
+        if (warp < kPartialDoubles) {
+            const double v = warp_reduce_word(P.partial, strips, warp, warp == kLargest || warp == kMaxErr);
+            if (lane == 0) s_fin[warp] = (unsigned long long)__double_as_longlong(v);
+        } else {
+            const unsigned long long v = warp_reduce_count(P.partial, strips, warp);
+            if (lane == 0) s_fin[warp] = v;
+        }
     }
     __syncthreads();
-    if (threadIdx.x != 0) return;
+    if (tid != 0) return;
+    auto d = [&](uint32_t k) { return __longlong_as_double((long long)s_fin[k]); };
     CdfDeviceReport r{};
-    for (unsigned k = 0; k < strips; ++k) {
-        const double* o = stage + (size_t)kF * k;
-        r.fine_mass += o[0];
-        r.fine_axial += o[1];
-        r.stored_mass += o[2];
-        r.stored_axial += o[3];
-        r.tv += o[4];
-        r.l1 += o[5];
-        r.lost += o[6];
-        r.recovered += o[7];
-        r.axial += o[8];
-        r.max_err = fmax(r.max_err, o[9]);
-        r.invalid += (unsigned long long)__double_as_longlong(o[11]);
-        r.underflow += (unsigned long long)__double_as_longlong(o[12]);
-        r.lost_cells += (unsigned long long)__double_as_longlong(o[10]);
-        r.malformed += (unsigned long long)__double_as_longlong(o[13]);
-    }
-    r.largest = s_glob[4];
+    r.fine_mass = d(kFineMass);
+    r.fine_axial = d(kFineAxial);
+    r.stored_mass = d(kStoredMass);
+    r.stored_axial = d(kStoredAxial);
+    r.tv = d(kTv);
+    r.l1 = d(kL1);
+    r.lost = d(kLost);
+    r.recovered = d(kRecovered);
+    r.axial = d(kAxial);
+    r.max_err = d(kMaxErr);
+    r.largest = d(kLargest);
     r.total = total;
-    r.timeout = P.report->timeout;
+    r.invalid = s_fin[kInvalid];
+    r.lost_cells = s_fin[kLostCells];
+    r.malformed = s_fin[kMalformed];
+    r.underflow = s_fin[kUnderflow];
+    r.timeout = *((volatile unsigned*)&P.report->timeout);
     *P.report = r;
+    // every block has passed both barriers and taken its ticket: the counters start the next launch at zero
+    P.sync[0] = 0u;
+    P.sync[1] = 0u;
 }
 
-// Fine-grid mass with pole caps for an FP64 histogram (used by the report path).
-int launch_cdf_build(const CdfLaunch& L, cudaStream_t stream)
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link-time libcuda).
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiled encode_tiled()
+{
+    static EncodeTiled fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<EncodeTiled>(p);
+    }();
+    return fn;
+}
+
+// FP64 histograms [records][nt][np], boxes of cw columns x box_rows rows x 1 record.
+int make_values_map(CUtensorMap* map, const double* values, uint32_t nt, uint32_t np, uint32_t records, uint32_t cw,
+                    uint32_t box_rows)
+{
+    const EncodeTiled encode = encode_tiled();
+    if (!encode) return (int)cudaErrorNotSupported;
+    const cuuint64_t dims[3] = {np, nt, records};
+    const cuuint64_t strides[2] = {(cuuint64_t)np * 8u, (cuuint64_t)np * nt * 8u};
+    const cuuint32_t box[3] = {cw, box_rows, 1u};
+    const cuuint32_t elem[3] = {1u, 1u, 1u};
+    const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double*>(values), dims, strides, box,
+                              elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? 0 : (int)cudaErrorInvalidValue;
+}
+
+CdfParams params_of(const CdfLaunch& L, const CdfShape& s)
 {
     CdfParams P{};
     P.values = L.values;
@@ -464,60 +641,125 @@ int launch_cdf_build(const CdfLaunch& L, cudaStream_t stream)
     P.cp = L.cp;
     P.dt = L.nt / L.ct;
     P.dp = L.np / L.cp;
-    P.cw = L.cw;
+    P.cw = s.cw;
+    P.keep = s.keep;
+    P.tma = s.tma;
+    P.box_rows = s.box_rows;
+    P.boxes = s.boxes;
+    P.rows_alloc = s.rows_alloc;
+    P.spin_limit = L.spin_limit;
     P.fwd_add = L.fwd_add;
     P.bwd_add = L.bwd_add;
     P.row_add = L.row_add;
     P.pole_fx = L.pole_fx;
     P.pole_weight = L.pole_weight;
-    const unsigned blocks = (L.cp + L.cw - 1) / L.cw;
-    const size_t smem = cdf_smem_bytes(L.ct, L.cp, L.cw);
+    return P;
+}
+
+int launch(const CdfParams& P, const CUtensorMap& map, uint32_t blocks, size_t smem, cudaStream_t stream)
+{
     cudaError_t e = cudaFuncSetAttribute(cdf_build_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return (int)e;
-    void* args[] = {&P};
+    void* args[] = {const_cast<CUtensorMap*>(&map), const_cast<CdfParams*>(&P)};
     e = cudaLaunchCooperativeKernel((const void*)cdf_build_kernel, dim3(blocks), dim3(kThreads), args, smem, stream);
     return (int)e;
 }
 
-size_t cdf_smem_bytes(uint32_t ct, uint32_t cp, uint32_t cw)
+// Rows per TMA box (at most the strip's rows): a box's shared-memory image must start 128-byte
+// aligned and at most kMaxBoxes boxes cover the strip; the fewest padded rows win (then the
+// larger box).
+bool box_rows_for(uint32_t ct, uint32_t cw, uint32_t& box_rows, uint32_t& boxes)
 {
-    const size_t blocks = (cp + cw - 1) / cw;
-    const size_t stage = blocks * 14 > cp ? blocks * 14 : cp;
-    return sizeof(double) * ((size_t)ct * cw + cw + 1 + stage);
+    uint32_t best = 0, best_rows = 0xffffffffu;
+    for (uint32_t r = std::min(256u, ct); r >= 1; --r) {
+        if ((r * cw * 8u) % 128u) continue;
+        const uint32_t n = (ct + r - 1) / r;
+        if (n > kMaxBoxes) continue;
+        if (n * r < best_rows) {
+            best_rows = n * r;
+            best = r;
+        }
+    }
+    if (!best) return false;
+    box_rows = best;
+    boxes = (ct + best - 1) / best;
+    return true;
 }
 
-int launch_cdf_build_batch(const CdfLaunch& L, const CdfBatchRecord* d_recs, uint32_t count, cudaStream_t stream)
-{
-    CdfParams P{};
-    P.recs = d_recs;
-    P.edges = L.edges;
-    P.kind = L.kind;
-    P.nt = L.nt;
-    P.np = L.np;
-    P.ct = L.ct;
-    P.cp = L.cp;
-    P.dt = L.nt / L.ct;
-    P.dp = L.np / L.cp;
-    P.cw = L.cw;
-    P.strips = (L.cp + L.cw - 1) / L.cw;
-    const size_t smem = cdf_smem_bytes(L.ct, L.cp, L.cw);
-    cudaError_t e = cudaFuncSetAttribute(cdf_build_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return (int)e;
-    void* args[] = {&P};
-    e = cudaLaunchCooperativeKernel((const void*)cdf_build_kernel, dim3(P.strips * count), dim3(kThreads), args, smem,
-                                    stream);
-    return (int)e;
-}
+} // namespace
 
 int cdf_max_coresident_blocks(size_t smem, int device)
 {
     int per_sm = 0, sms = 0;
-    cudaFuncSetAttribute(cdf_build_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (cudaFuncSetAttribute(cdf_build_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cdf_build_kernel, kThreads, smem) != cudaSuccess) return 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
     return per_sm * sms;
 }
 
 size_t cdf_partial_bytes() { return sizeof(BlockPartial); }
+
+size_t cdf_smem_bytes(const CdfShape& s, uint32_t ct, uint32_t cp)
+{
+    return layout_of(ct, cp, s.cw, s.rows_alloc, s.keep).total + 128; // + alignment slack of the base
+}
+
+int cdf_choose_shape(int device, int sms, uint32_t nt, uint32_t np, uint32_t ct, uint32_t cp, bool tma_ok,
+                     uint32_t min_width, uint32_t max_blocks, CdfShape& out)
+{
+    int max_smem = 0;
+    if (cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess) return -1;
+    // static shared memory of the kernel (reductions, totals) comes on top of the dynamic part
+    const size_t budget = (size_t)max_smem > 2048 ? (size_t)max_smem - 2048 : 0;
+    const bool fine = nt == ct && np == cp;
+    const uint32_t modes[3][2] = {{1u, 1u}, {1u, 0u}, {0u, 0u}}; // (keep, tma)
+    for (const auto& m : modes) {
+        const uint32_t keep = m[0], tma = m[1];
+        if (tma && !(tma_ok && fine)) continue;
+        uint32_t w = std::max<uint32_t>(min_width, (cp + (uint32_t)sms - 1) / (uint32_t)sms);
+        for (; w <= cp && w <= kThreads; ++w) {
+            CdfShape s{};
+            s.cw = w;
+            s.keep = keep;
+            s.tma = tma;
+            s.rows_alloc = ct;
+            if (tma) {
+                if (w % 2 || w > 256 || !box_rows_for(ct, w, s.box_rows, s.boxes)) continue;
+                s.rows_alloc = s.box_rows * s.boxes;
+            }
+            s.smem = cdf_smem_bytes(s, ct, cp);
+            if (s.smem > budget) break;
+            const uint32_t blocks = (cp + w - 1) / w;
+            if (blocks <= max_blocks && (int)blocks <= cdf_max_coresident_blocks(s.smem, device)) {
+                out = s;
+                return 0;
+            }
+        }
+    }
+    return 1;
+}
+
+int launch_cdf_build(const CdfLaunch& L, const CdfShape& s, cudaStream_t stream)
+{
+    const CdfParams P = params_of(L, s);
+    CUtensorMap map{};
+    if (s.tma)
+        if (const int e = make_values_map(&map, L.values, L.nt, L.np, 1u, s.cw, s.box_rows)) return e;
+    return launch(P, map, (L.cp + s.cw - 1) / s.cw, s.smem, stream);
+}
+
+int launch_cdf_build_batch(const CdfLaunch& L, const CdfShape& s, const CdfBatchRecord* d_recs, uint32_t count,
+                           cudaStream_t stream)
+{
+    CdfParams P = params_of(L, s);
+    P.recs = d_recs;
+    P.strips = (L.cp + s.cw - 1) / s.cw;
+    CUtensorMap map{};
+    if (s.tma) return (int)cudaErrorInvalidValue; // batched records are read without TMA
+    return launch(P, map, P.strips * count, s.smem, stream);
+}
 
 } // namespace icp

@@ -24,8 +24,9 @@ struct CdfLaunch {
     double* colsum;
     void* partial;
     CdfDeviceReport* report;
-    unsigned* sync; // two counters, zeroed before launch
-    uint32_t kind, nt, np, ct, cp, cw;
+    unsigned* sync; // two counters: zero before the first launch; every completed launch leaves them zero
+    uint32_t kind, nt, np, ct, cp;
+    uint32_t spin_limit; // grid-barrier iteration limit (0: the default)
     double fwd_add, bwd_add;
     // optional device-side inputs of a record launched without a host round trip:
     const double* row_add;             // nt values added to every cell of row i (or null)
@@ -33,7 +34,19 @@ struct CdfLaunch {
     double pole_weight;                // mm^2 per unit of pole power (with pole_fx)
 };
 
-int launch_cdf_build(const CdfLaunch& L, cudaStream_t stream);
+// Launch shape of one CDF build: strip width (stored phi columns per block), whether the coarse
+// strip stays in shared memory for the audit (keep), whether the fine strip arrives by TMA boxes
+// (tma; fine grid = stored grid only), the boxes' rows, and the dynamic shared memory.
+struct CdfShape {
+    uint32_t cw, keep, tma, box_rows, boxes, rows_alloc;
+    size_t smem;
+};
+// Widest-first search over (keep, tma) modes and the smallest strip width >= max(min_width,
+// ceil(cp / sms)) whose grid of ceil(cp / cw) blocks (at most max_blocks) is co-resident.
+// Returns 0 on success.
+int cdf_choose_shape(int device, int sms, uint32_t nt, uint32_t np, uint32_t ct, uint32_t cp, bool tma_ok,
+                     uint32_t min_width, uint32_t max_blocks, CdfShape& out);
+int launch_cdf_build(const CdfLaunch& L, const CdfShape& s, cudaStream_t stream);
 // One record of a batched CDF build (device array of these; scratch per record: `strips`
 // partials, cp column sums, two zeroed barrier counters, a zeroed report).
 struct CdfBatchRecord {
@@ -48,11 +61,14 @@ struct CdfBatchRecord {
     const unsigned long long* pole_fx;
     double pole_weight, fwd_add, bwd_add;
 };
-// Builds `count` records of one grid shape (L: edges, kind, nt, np, ct, cp, cw; its per-record
-// fields unused) in one cooperative launch of count x ceil(cp / cw) blocks.
-int launch_cdf_build_batch(const CdfLaunch& L, const CdfBatchRecord* d_recs, uint32_t count, cudaStream_t stream);
+// Builds `count` records of one grid shape (L: edges, kind, nt, np, ct, cp; its per-record
+// fields unused; s without tma) in one cooperative launch of count x ceil(cp / s.cw) blocks.
+int launch_cdf_build_batch(const CdfLaunch& L, const CdfShape& s, const CdfBatchRecord* d_recs, uint32_t count,
+                           cudaStream_t stream);
 int cdf_max_coresident_blocks(size_t smem, int device);
-size_t cdf_smem_bytes(uint32_t ct, uint32_t cp, uint32_t cw);
+// Bytes of one block's partial results in the CDF scratch (15 words).
+constexpr size_t kCdfPartialBytes = 120;
+size_t cdf_smem_bytes(const CdfShape& s, uint32_t ct, uint32_t cp);
 size_t cdf_partial_bytes();
 // Sets the calling thread's message returned by icp_last_error().
 void set_last_error(const char* message);
@@ -137,6 +153,14 @@ struct Scratch {
         if (e == cudaSuccess) bytes = n;
         return e;
     }
+    // As ensure; a buffer (re)allocated here is cleared on the stream (counters that kernels
+    // leave at zero after every completed launch start from zero this way).
+    cudaError_t ensure_zeroed(size_t n, cudaStream_t stream)
+    {
+        if (n <= bytes) return cudaSuccess;
+        const cudaError_t e = ensure(n);
+        return e == cudaSuccess ? cudaMemsetAsync(ptr, 0, bytes, stream) : e;
+    }
     void release()
     {
         if (ptr) cudaFree(ptr);
@@ -156,8 +180,11 @@ namespace icp {
 int ensure_float_edges(icp_context* c, const double* d_edges, uint32_t nt);
 // Adds one launch's device statistics (DevStats bytes) into the public stats struct.
 void stats_accumulate(const unsigned char* raw, icp_trace_stats* out);
-// Strip width of the cooperative CDF grid for a (ct, cp) storage grid.
-int choose_cdf_width(icp_context* c, uint32_t ct, uint32_t cp, uint32_t& cw);
+// Launch shape of the cooperative CDF grid for a (nt, np) -> (ct, cp) build (cached per context).
+int cdf_shape(icp_context* c, uint32_t nt, uint32_t np, uint32_t ct, uint32_t cp, bool tma_ok, CdfShape& s);
+// Clears `records` CDF reports and barrier-counter pairs after a build gave up waiting (a build
+// that completes leaves its counters at zero itself), then waits for the stream.
+int cdf_clear(icp_context* c, void* d_reports, void* d_sync, uint32_t records);
 // Public CDF report and quality gates (build_host_cdf) from the kernel's device report.
 int cdf_finish(const CdfDeviceReport& r, const icp_cdf_policy& p, icp_cdf_report* report);
 // Enqueues one cooperative CDF build (no host synchronisation); d_sync[2] and d_report are
@@ -275,4 +302,15 @@ struct icp_context {
     // wave-stage density audit accumulators
     icp::Scratch stage_audit;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+    // grid-barrier iteration limit handed to the CDF kernels (0: their default)
+    uint32_t wait_limit = 0;
+    // CDF launch shapes already chosen: (nt, np, ct, cp, tma allowed) -> shape
+    struct ShapeEntry {
+        uint32_t nt, np, ct, cp, tma_ok;
+        icp::CdfShape shape;
+    };
+    std::vector<ShapeEntry> cdf_shapes;
+    // u edges of the last icp_phase_cdf_enqueue grid (uploaded when nt changes)
+    icp::Scratch cdf_edges;
+    uint32_t cdf_edges_nt = 0;
 };

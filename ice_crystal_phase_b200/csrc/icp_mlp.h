@@ -41,6 +41,8 @@ struct GemmArgs {
     __nv_bfloat16* out_dzT;
     float* out_db;
     unsigned* error;        // set to 1 / 2 when a bounded wait expires
+    uint32_t wait_limit;    // tries of the split-K kernel's pipeline waits (0: the default); the waits
+                            // that drain loads in flight after an abort keep the default
 };
 
 // Enqueues D = A[M x K] * B[N x K]^T with the given epilogue; split-K (kAtomicF32 only) over

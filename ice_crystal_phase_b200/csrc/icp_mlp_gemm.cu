@@ -287,10 +287,11 @@ __global__ void __launch_bounds__(128, 1)
             umma::tma_load_2d(a + BOFF, &tmB, &full[s], (int32_t)((kc0 + kc) * 64u), 0);
         };
         uint32_t issued = nk < (uint32_t)S ? nk : (uint32_t)S, consumed = 0;
+        const uint32_t limit = g.wait_limit ? g.wait_limit : kWaitLimit;
         for (uint32_t s = 0; s < issued; ++s) load(s, s);
         for (uint32_t kc = 0; kc < nk && ok; ++kc) {
             const uint32_t s = kc % S, par = (kc / S) & 1u;
-            if (!umma::mbar_wait(&full[s], par, kWaitLimit)) {
+            if (!umma::mbar_wait(&full[s], par, limit)) {
                 ok = false;
                 break;
             }
@@ -305,7 +306,7 @@ __global__ void __launch_bounds__(128, 1)
                                    umma::smem_desc_sw128(b + 32u * k), idesc, kc > 0 || k > 0);
             umma::mma_commit(&empty[s]);
             if (kc + S < nk) {
-                if (!umma::mbar_wait(&empty[s], par, kWaitLimit)) {
+                if (!umma::mbar_wait(&empty[s], par, limit)) {
                     ok = false;
                     break;
                 }

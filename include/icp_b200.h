@@ -72,6 +72,12 @@ int icp_context_create(int device, icp_context** out);
 int icp_context_destroy(icp_context* ctx);
 /* Synchronises the context stream. */
 int icp_context_synchronize(icp_context* ctx);
+/* Iteration limit of the CDF kernels' grid-barrier waits and of the tensor-core pipeline waits
+ * of icp_mlp_gemm_bf16 on this context (0 = the library's default, about four million polls).
+ * A wait that runs out ends the call with ICP_ERR_TIMEOUT and leaves the context usable.  No
+ * reference counterpart: the reference's stages have no bounded device waits; this lets a host
+ * shorten them (and tests make them run out). */
+int icp_context_set_wait_limit(icp_context* ctx, uint32_t limit);
 /* The context's cudaStream_t, for callers that enqueue their own work. */
 void* icp_context_stream(icp_context* ctx);
 /* Device memory owned by the context's caller (thin wrappers for FFI users). */
@@ -199,6 +205,16 @@ enum icp_cdf_input { ICP_CDF_MASS = 0, ICP_CDF_DENSITY = 1 };
 int icp_phase_cdf_build(icp_context* ctx, const double* d_values, uint32_t input_kind, uint32_t nt,
                         uint32_t np, double forward_pole, double backward_pole, uint32_t ct, uint32_t cp,
                         const icp_cdf_policy* policy, double* d_phi, double* d_theta, icp_cdf_report* report);
+/* icp_phase_cdf_build in two halves, for device-resident callers that keep the build on the
+ * context's stream with other work (the reference's PhaseCdf::build waits before returning,
+ * src/phase_cdf.cpp:211-223): icp_phase_cdf_enqueue checks the arguments and enqueues the build
+ * (one cooperative kernel once the grid's u edges are on the device) without waiting;
+ * icp_phase_cdf_result waits for the stream, applies the quality gates and fills the report.
+ * One build in flight per context. */
+int icp_phase_cdf_enqueue(icp_context* ctx, const double* d_values, uint32_t input_kind, uint32_t nt, uint32_t np,
+                          double forward_pole, double backward_pole, uint32_t ct, uint32_t cp, double* d_phi,
+                          double* d_theta);
+int icp_phase_cdf_result(icp_context* ctx, const icp_cdf_policy* policy, icp_cdf_report* report);
 /* The same for `count` histograms of one shape (mass input, no pole caps) at d_values +
  * r*nt*np, built in few cooperative launches (no reference counterpart; the reference builds one
  * record per process): phi / theta of record r at d_phi + r*(cp+1), d_theta + r*cp*(ct+1), equal
@@ -211,15 +227,19 @@ int icp_phase_cdf_build_batch(icp_context* ctx, const double* d_values, uint32_t
  * allocate device memory themselves or through this library -- an embedding application
  * whose own allocator already owns the device, or a callback context where allocating is
  * not allowed.  Same inputs, outputs, gates and report as icp_phase_cdf_build, on the given
- * cudaStream_t (NULL = legacy default stream, current device), but every scratch buffer
+ * cudaStream_t (NULL = legacy default stream of the current device; a stream must belong to
+ * the current device and context, else ICP_ERR_INVALID_ARGUMENT), but every scratch buffer
  * (u edges, block partials, column sums, barrier counters, audit record) lives in one
- * file-scope device array of about 220 KiB that each GPU holds until the process exits.
- * Limits: nt <= ICP_STATIC_MAX_THETA, cp <= ICP_STATIC_MAX_PHI (ICP_ERR_CAPACITY beyond).
- * The first call on a device looks the array's address up (make it before any stream
- * capture); all calls share the array, so calls that overlap on the GPU race on it. */
+ * file-scope device array of ICP_STATIC_SCRATCH_BYTES (216.75 KiB) that each GPU holds until
+ * the process exits.  Limits: nt <= ICP_STATIC_MAX_THETA, cp <= ICP_STATIC_MAX_PHI
+ * (ICP_ERR_CAPACITY beyond).  The first call in a CUDA context looks the array's address up in
+ * that context (make it before any stream capture); the entry copies host memory and waits
+ * for the stream, so it is never called inside a stream capture.  All calls share the array,
+ * so calls that overlap on the GPU race on it. */
 #define ICP_STATIC_MAX_THETA 4096u
 #define ICP_STATIC_MAX_PHI 8192u
 #define ICP_STATIC_MAX_BLOCKS 1024u
+#define ICP_STATIC_SCRATCH_BYTES 221952u
 int icp_phase_cdf_build_static(void* stream, const double* d_values, uint32_t input_kind, uint32_t nt, uint32_t np,
                                double forward_pole, double backward_pole, uint32_t ct, uint32_t cp,
                                const icp_cdf_policy* policy, double* d_phi, double* d_theta, icp_cdf_report* report);

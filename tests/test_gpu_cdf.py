@@ -150,3 +150,59 @@ def test_batched_build_equals_single_records(ctx, icp, count, nt, np_, ct, cp):
         assert reps[r].status == 0
         assert abs(reps[r].g_stored - one.report["g_stored"]) <= 1e-13
         assert abs(reps[r].l1_error - one.report["l1_error"]) <= 1e-13
+
+
+def test_enqueue_and_result_equal_the_build(ctx, icp):
+    """icp_phase_cdf_enqueue + icp_phase_cdf_result (one kernel on the stream, report later) give
+    the bits and report of icp_phase_cdf_build, on repeated builds (the barrier counters are left
+    at zero by every completed build) and across grid shapes (the u edges follow nt)."""
+    import ctypes as C
+
+    rng = np.random.default_rng(77)
+    for nt, np_ in ((900, 1800), (64, 128), (900, 1800)):
+        m = rng.exponential(size=nt * np_) * (rng.random(nt * np_) < 0.5)
+        ref = icp.PhaseCdf(ctx).build(m, nt, np_)
+        d = icp.DeviceArray(ctx, nt * np_).upload(m)
+        phi, theta = icp.DeviceArray(ctx, np_ + 1), icp.DeviceArray(ctx, np_ * (nt + 1))
+        for _ in range(2):
+            icp.check(icp.LIB.icp_phase_cdf_enqueue(ctx.handle, d.ptr, 0, nt, np_, 0.0, 0.0, nt, np_, phi.ptr, theta.ptr))
+            rep = icp.CdfReport()
+            icp.check(icp.LIB.icp_phase_cdf_result(ctx.handle, C.byref(icp.CdfPolicy(1e-10, 1e-12, 1.0)), C.byref(rep)))
+            assert np.array_equal(phi.download(), ref.phi)
+            assert np.array_equal(theta.download().reshape(np_, nt + 1), ref.theta)
+            assert rep.status == 0 and rep.g_stored == ref.report["g_stored"] and rep.l1_error == ref.report["l1_error"]
+
+
+def test_grid_barrier_wait_that_runs_out_reports_timeout(ctx, icp):
+    """A grid-barrier wait limited to one poll runs out (129 cooperative blocks cannot all arrive
+    before the first ones poll): the build ends with ICP_ERR_TIMEOUT, and the same context then
+    builds the same record correctly once the default limit is back."""
+    rng = np.random.default_rng(12)
+    m = rng.exponential(size=900 * 1800)
+    ref = icp.PhaseCdf(ctx).build(m, 900, 1800)
+    icp.check(icp.LIB.icp_context_set_wait_limit(ctx.handle, 1))
+    try:
+        with pytest.raises(icp.IcpError) as err:
+            icp.PhaseCdf(ctx).build(m, 900, 1800)
+        assert err.value.status == icp.ICP_ERR_TIMEOUT
+        assert "gave up waiting" in icp.last_error()
+    finally:
+        icp.check(icp.LIB.icp_context_set_wait_limit(ctx.handle, 0))
+    again = icp.PhaseCdf(ctx).build(m, 900, 1800)
+    assert np.array_equal(again.phi, ref.phi) and np.array_equal(again.theta, ref.theta)
+    assert again.report["status"] == 0
+
+
+def test_refused_allocation_leaves_the_context_usable(ctx, icp):
+    """A device allocation the driver refuses (a petabyte) is reported as ICP_ERR_DEVICE with
+    the driver's message; the context then builds a record as before."""
+    import ctypes as C
+
+    p = C.c_void_p()
+    rc = icp.LIB.icp_device_alloc(ctx.handle, 1 << 50, C.byref(p))
+    assert rc == icp.ICP_ERR_DEVICE and not p.value
+    assert "cudaMalloc" in icp.last_error()
+    rng = np.random.default_rng(4)
+    m = rng.random(64 * 128)
+    out = icp.PhaseCdf(ctx).build(m, 64, 128)
+    assert out.report["status"] == 0 and out.phi[-1] == 1

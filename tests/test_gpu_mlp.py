@@ -54,3 +54,34 @@ def test_gemm_rejects_bad_shapes(ctx, icp):
     for m, n, k in [(100, 64, 64), (128, 96, 64), (128, 64, 100)]:
         with pytest.raises(icp.InvalidArgument):
             icp.mlp_gemm_bf16(ctx, d.data_ptr(), d.data_ptr(), m, n, k, c.data_ptr())
+
+
+def test_pipeline_wait_that_runs_out_reports_timeout(ctx, icp):
+    """The split-K GEMM's producer waits limited to one try (icp_context_set_wait_limit) give up
+    while the TMA loads of a 128-chunk K range are still landing: the call returns
+    ICP_ERR_TIMEOUT (the kernel drains the loads in flight with the default limit and frees its
+    tensor memory before it returns), and the same context then computes the product correctly
+    with the default limit."""
+    import ctypes as C
+
+    m, n, k = 256, 256, 8192
+    gen = torch.Generator().manual_seed(99)
+    a, b = _bf16((m, k), gen, 0.1), _bf16((n, k), gen, 0.1)
+    ref = a.double().numpy() @ b.double().numpy().T
+    da, db = a.cuda(), b.cuda()
+    dc = torch.zeros((m, n), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    codes = []
+    icp.check(icp.LIB.icp_context_set_wait_limit(ctx.handle, 1))
+    try:
+        for _ in range(3):
+            codes.append(icp.LIB.icp_mlp_gemm_bf16(ctx.handle, C.c_void_p(da.data_ptr()), C.c_void_p(db.data_ptr()), m,
+                                                   n, k, 1, C.c_void_p(dc.data_ptr()), 1))
+    finally:
+        icp.check(icp.LIB.icp_context_set_wait_limit(ctx.handle, 0))
+    assert icp.ICP_ERR_TIMEOUT in codes and set(codes) <= {icp.ICP_OK, icp.ICP_ERR_TIMEOUT}, codes
+    dc.zero_()
+    torch.cuda.synchronize()
+    icp.mlp_gemm_bf16(ctx, da.data_ptr(), db.data_ptr(), m, n, k, dc.data_ptr(), accumulate=True)
+    got = dc.cpu().double().numpy()
+    assert np.abs(got - ref).max() / np.abs(ref).max() <= 2e-5

@@ -4,8 +4,10 @@ That entry exists for callers that cannot allocate device memory (their own allo
 the device, or allocation is not allowed where they call from): it takes its scratch from a
 file-scope device array instead of cudaMalloc.  Its results must equal those of
 icp_phase_cdf_build bit for bit (the tolerance the CDF parity tests use for phi and theta),
-including on a second call that finds the previous call's contents still in the array.
-Collected last so that a run stopping at the first failure has run every other test.
+including on a second call that finds the previous call's contents still in the array, for
+mass and density input, and with the same status, message and report when an audit gate
+rejects the record.  Collected last so that a run stopping at the first failure has run every
+other test.
 """
 from __future__ import annotations
 
@@ -16,6 +18,9 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
+REPORT_FIELDS = ["g_source", "g_stored", "coarsening_tv", "cdf_mass", "l1_error", "lost_mass", "maximum_cell_error",
+                 "aggregation_relative_error", "fine_mass", "fine_axial", "lost_cells", "malformed", "status"]
+
 
 def _bind(icp):
     f = icp.LIB.icp_phase_cdf_build_static
@@ -25,20 +30,24 @@ def _bind(icp):
     return f
 
 
-def _regular(icp, ctx, dvals, nt, np_, ct, cp, fwd, bwd):
+def _regular(icp, ctx, dvals, kind, nt, np_, ct, cp, fwd, bwd, policy):
     phi, theta = icp.DeviceArray(ctx, cp + 1), icp.DeviceArray(ctx, cp * (ct + 1))
     rep = icp.CdfReport()
-    icp.check(icp.LIB.icp_phase_cdf_build(ctx.handle, dvals.ptr, 0, nt, np_, fwd, bwd, ct, cp,
-                                          C.byref(icp.CdfPolicy(1e-10, 1e-12, 1.0)), phi.ptr, theta.ptr, C.byref(rep)))
-    return phi.download(), theta.download(), rep
+    rc = icp.LIB.icp_phase_cdf_build(ctx.handle, dvals.ptr, kind, nt, np_, fwd, bwd, ct, cp, C.byref(policy), phi.ptr,
+                                     theta.ptr, C.byref(rep))
+    return rc, icp.last_error(), phi.download(), theta.download(), rep
 
 
-def _static(icp, ctx, fn, stream, dvals, nt, np_, ct, cp, fwd, bwd):
+def _static(icp, ctx, fn, stream, dvals, kind, nt, np_, ct, cp, fwd, bwd, policy):
     phi, theta = icp.DeviceArray(ctx, cp + 1), icp.DeviceArray(ctx, cp * (ct + 1))
     rep = icp.CdfReport()
-    icp.check(fn(stream, dvals.ptr, 0, nt, np_, fwd, bwd, ct, cp, C.byref(icp.CdfPolicy(1e-10, 1e-12, 1.0)), phi.ptr,
-                 theta.ptr, C.byref(rep)))
-    return phi.download(), theta.download(), rep
+    rc = fn(stream, dvals.ptr, kind, nt, np_, fwd, bwd, ct, cp, C.byref(policy), phi.ptr, theta.ptr, C.byref(rep))
+    return rc, icp.last_error(), phi.download(), theta.download(), rep
+
+
+def _same_report(a, b):
+    for k in REPORT_FIELDS:
+        assert getattr(a, k) == getattr(b, k), (k, getattr(a, k), getattr(b, k))
 
 
 def test_static_scratch_entry_matches_regular_entry_twice():
@@ -46,19 +55,47 @@ def test_static_scratch_entry_matches_regular_entry_twice():
 
     fn = _bind(icp)
     rng = np.random.default_rng(2024)
+    policy = icp.CdfPolicy(1e-10, 1e-12, 1.0)
     with icp.Context(0) as ctx:
-        cases = [(96, 192, 48, 64, 3.0, 1.0), (512, 1024, 512, 1024, 0.0, 0.0)]
-        streams = [None, icp.LIB.icp_context_stream(ctx.handle)]
-        for (nt, np_, ct, cp, fwd, bwd), stream in zip(cases, streams):
+        stream = icp.LIB.icp_context_stream(ctx.handle)
+        # (kind, nt, np, ct, cp, fwd, bwd): mass with coarsening and poles, mass at full size,
+        # density input -- each built twice in a row through the static entry
+        cases = [(0, 96, 192, 48, 64, 3.0, 1.0), (0, 512, 1024, 512, 1024, 0.0, 0.0), (1, 180, 360, 90, 120, 0.0, 0.0)]
+        for kind, nt, np_, ct, cp, fwd, bwd in cases:
             m = rng.exponential(size=nt * np_) * (rng.random(nt * np_) < 0.6)
             d = icp.DeviceArray(ctx, nt * np_).upload(m)
-            a_phi, a_theta, a_rep = _regular(icp, ctx, d, nt, np_, ct, cp, fwd, bwd)
-            b_phi, b_theta, b_rep = _static(icp, ctx, fn, stream, d, nt, np_, ct, cp, fwd, bwd)
-            assert np.array_equal(a_phi, b_phi)
-            assert np.array_equal(a_theta, b_theta)
-            assert abs(a_rep.g_stored - b_rep.g_stored) <= 2e-11
-            assert abs(a_rep.l1_error - b_rep.l1_error) <= 2e-10
-            assert b_rep.status == 0 and b_rep.lost_cells == a_rep.lost_cells
+            rc_a, _, a_phi, a_theta, a_rep = _regular(icp, ctx, d, kind, nt, np_, ct, cp, fwd, bwd, policy)
+            assert rc_a == 0
+            for s in (None, stream):
+                rc_b, _, b_phi, b_theta, b_rep = _static(icp, ctx, fn, s, d, kind, nt, np_, ct, cp, fwd, bwd, policy)
+                assert rc_b == 0
+                assert np.array_equal(a_phi, b_phi)
+                assert np.array_equal(a_theta, b_theta)
+                _same_report(a_rep, b_rep)
+
+
+def test_static_scratch_entry_rejects_like_regular_entry():
+    """A record that an audit gate rejects (an L1 bar below the CDF's own rounding) returns the
+    same status, message and report from both entries; the next call through the static entry,
+    which finds the rejected call's contents in the array, succeeds again."""
+    import ice_crystal_phase_b200 as icp
+
+    fn = _bind(icp)
+    rng = np.random.default_rng(7)
+    with icp.Context(0) as ctx:
+        nt, np_ = 128, 256
+        d = icp.DeviceArray(ctx, nt * np_).upload(rng.exponential(size=nt * np_))
+        tight = icp.CdfPolicy(1e-30, 1e-12, 1.0)
+        rc_a, msg_a, _, _, a_rep = _regular(icp, ctx, d, 0, nt, np_, nt, np_, 0.0, 0.0, tight)
+        rc_b, msg_b, _, _, b_rep = _static(icp, ctx, fn, None, d, 0, nt, np_, nt, np_, 0.0, 0.0, tight)
+        assert rc_a == rc_b == icp.ICP_ERR_AUDIT
+        assert msg_a == msg_b
+        _same_report(a_rep, b_rep)
+        ok = icp.CdfPolicy(1e-10, 1e-12, 1.0)
+        rc_c, _, c_phi, c_theta, _ = _static(icp, ctx, fn, None, d, 0, nt, np_, nt, np_, 0.0, 0.0, ok)
+        rc_d, _, d_phi, d_theta, _ = _regular(icp, ctx, d, 0, nt, np_, nt, np_, 0.0, 0.0, ok)
+        assert rc_c == rc_d == 0
+        assert np.array_equal(c_phi, d_phi) and np.array_equal(c_theta, d_theta)
 
 
 def test_static_scratch_rejects_sizes_beyond_its_maximum():
