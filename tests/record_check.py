@@ -1,6 +1,8 @@
 """Record validation for the tests: every record this repository writes is held to the contract
 the reference's record reader enforces (python/rainbow_dataset/record.py:19-158,
-PhaseRecord(validate=True)), on hosts without the reference checkout.
+PhaseRecord(validate=True)).  Where the reference checkout is present (ICP_REFERENCE_ROOT, by
+default the checkout this build was made against), validate_record also opens the record with
+that reader itself, unchanged; on hosts without it (the GPU box) the restatement below stands in.
 
 The contract, as checked here: a complete v1/v2 record (not a .part directory); fixed layout
 strings; positive int32 grid sizes; three <f8 C-order arrays of the right shapes with no
@@ -10,10 +12,29 @@ non-decreasing; for v2, the HG label is the first moment of the saved cells (5e-
 """
 from __future__ import annotations
 
+import importlib.util
 import json
+import os
 from pathlib import Path
 
 import numpy as np
+
+REFERENCE = Path(os.environ.get("ICP_REFERENCE_ROOT", "/root/reference"))
+_READER: list = []
+
+
+def reference_reader():
+    """The reference's PhaseRecord class, imported by path from its checkout, or None."""
+    if not _READER:
+        path = REFERENCE / "python" / "rainbow_dataset" / "record.py"
+        cls = None
+        if path.is_file():
+            spec = importlib.util.spec_from_file_location("reference_rainbow_record", path)
+            mod = importlib.util.module_from_spec(spec)
+            spec.loader.exec_module(mod)
+            cls = mod.PhaseRecord
+        _READER.append(cls)
+    return _READER[0]
 
 FIXED = {"dtype": "<f8", "order": "C", "density_measure": "solid_angle_sr",
          "cell_model": "constant_density_per_spherical_cell", "coordinates": "u=(1-cos(theta))/2; v=(phi+pi)/(2*pi)",
@@ -37,6 +58,12 @@ def _fail(what: str) -> None:
 
 def validate_record(directory: str | Path) -> dict:
     d = Path(directory)
+    reader = reference_reader()
+    if reader is not None:
+        rec = reader(d, validate=True)  # raises on any violation of its contract
+        close = getattr(rec, "close", None)
+        if close:
+            close()
     if d.name.endswith(".part"):
         _fail("a .part directory is incomplete")
     m = json.loads((d / "metadata.json").read_text(encoding="utf-8"))

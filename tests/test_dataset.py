@@ -195,6 +195,70 @@ def test_orchestration_refusals(ds, icp, tmp_path):
     assert not (root / ".batch.lock").exists()
 
 
+def test_io_failure_mid_record_stops_the_run(ds, icp, tmp_path, monkeypatch):
+    """Host-side fault injection: the disk fails while the third record's arrays are written (an
+    OSError from the NPY writer, as a full disk raises).  The run stops at that record with the
+    error, keeps its <record>.part for inspection (never reused), writes no receipt for it, keeps
+    the two completed records and their receipts, and releases the batch lock; a resume then
+    refuses until the .part is moved away by hand, and completes the plan after that."""
+    import shutil
+
+    cfg = copy.deepcopy(CONFIG)
+    root = tmp_path / "out"
+    cfg["output_root"] = str(root)
+    path = _write(tmp_path, cfg)
+    real = ds.write_npy
+    calls = {"n": 0}
+
+    def failing(p, a):
+        calls["n"] += 1
+        if calls["n"] == 8:  # second array of the third record
+            raise OSError(28, "No space left on device (injected)")
+        return real(p, a)
+
+    monkeypatch.setattr(ds, "write_npy", failing)
+    with pytest.raises(OSError, match="injected"):
+        ds.run(["--config", str(path), "--execute"], backend=FakeBackend(icp))
+    monkeypatch.setattr(ds, "write_npy", real)
+    assert not (root / ".batch.lock").exists()
+    assert sorted(p.name for p in (root / "receipts").iterdir()) == ["i0000_w0000.json", "i0000_w0001.json"]
+    part = root / "records/i0001/w0000.part"
+    assert part.is_dir() and not (root / "records/i0001/w0000").exists()
+    validate_record(root / "records/i0000/w0001")
+    with pytest.raises(ValueError, match="Incomplete .part exists"):
+        ds.run(["--config", str(path), "--execute", "--resume"], backend=FakeBackend(icp))
+    shutil.move(str(part), str(tmp_path / "inspected.part"))
+    fake = FakeBackend(icp)
+    assert ds.run(["--config", str(path), "--execute", "--resume"], backend=fake) == 0
+    assert fake.calls == [[(1, 0), (1, 1)]]
+    assert json.loads((root / "progress.json").read_text())["complete"] is True
+
+
+def test_device_allocation_failure_stops_the_run(ds, icp, tmp_path):
+    """Host-side fault injection: the device library fails a batch with its device error (an
+    allocation that cudaMalloc refused).  The run ends with that error before writing any record
+    of the batch, the lock is released, and a resume from the same plan completes every record."""
+    cfg = copy.deepcopy(CONFIG)
+    root = tmp_path / "out"
+    cfg["output_root"] = str(root)
+    path = _write(tmp_path, cfg)
+
+    class FailingBackend(FakeBackend):
+        def generate(self, ctx, c, todo):
+            self.calls.append(list(todo))
+            raise icp.IcpError(icp.ICP_ERR_DEVICE, "c->b_mass.ensure(...) failed: out of memory (injected)")
+
+    with pytest.raises(icp.IcpError, match="out of memory"):
+        ds.run(["--config", str(path), "--execute"], backend=FailingBackend(icp))
+    assert not (root / ".batch.lock").exists()
+    assert not (root / "receipts").exists() or not any((root / "receipts").iterdir())
+    if (root / "records").exists():
+        assert not list((root / "records").rglob("*.part"))
+    fake = FakeBackend(icp)
+    assert ds.run(["--config", str(path), "--execute", "--resume"], backend=fake) == 0
+    assert json.loads((root / "progress.json").read_text())["completed"] == 4
+
+
 @pytest.mark.gpu
 def test_batched_dataset_on_gpu(ds, icp, tmp_path):
     cfg = copy.deepcopy(CONFIG)
