@@ -48,7 +48,7 @@ __device__ __forceinline__ void warp_flush(const P_& P, unsigned* s_status, cons
 #pragma unroll
     for (int q = 0; q < 14; ++q)
         for (int o = 16; o; o >>= 1) w[q] += __shfl_xor_sync(kFull, w[q], o);
-    double ax = A.axial, mb = A.max_bal, mi = A.max_iface;
+    double ax = A.axial, mb = A.max_bal, mi = (double)A.max_iface;
     for (int o = 16; o; o >>= 1) {
         ax += __shfl_xor_sync(kFull, ax, o);
         mb = fmax(mb, __shfl_xor_sync(kFull, mb, o));

@@ -165,7 +165,7 @@ struct SmemHist {
 __device__ __forceinline__ uint32_t hash_cell(uint32_t k) { return (k * 0x9E3779B1u) >> 7; }
 
 __device__ __forceinline__ void hist_add(const SmemHist& h, double* global_mass, double to_mass, bool has,
-                                         uint32_t cell, uint64_t v, unsigned long long& fallback)
+                                         uint32_t cell, uint64_t v, uint32_t& fallback)
 {
     const unsigned act = __ballot_sync(kFull, has);
     if (!act) return;

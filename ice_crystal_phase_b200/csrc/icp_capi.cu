@@ -363,7 +363,7 @@ extern "C" int icp_hex_trace_bin(icp_context* c, const icp_hex_node* n, const ic
     // at least 64 rays per warp when the range is small; at most 2^16 per warp per launch
     uint64_t blocks = (uint64_t)per_sm * c->sms;
     blocks = std::max<uint64_t>(1, std::min<uint64_t>(blocks, (n->sample_count + 64ull * warps_per_block - 1) / (64ull * warps_per_block)));
-    const uint64_t piece = blocks * warps_per_block * 65536ull;
+    const uint64_t piece = blocks * warps_per_block * lane_rays_max(n->max_internal_hits);
 
     ICP_CUDA(c->stats.ensure(hex_stats_bytes()));
     ICP_CUDA(cudaMemsetAsync(c->stats.ptr, 0, hex_stats_bytes(), c->stream));

@@ -94,6 +94,8 @@ int launch_shape(icp_context* c, const icp_batch_settings& s, Shape& sh)
     if (sh.threads < 64 || sh.threads > 256 || sh.threads % 32)
         return fail(ICP_ERR_INVALID_ARGUMENT, "block_threads must be 64..256, multiple of 32");
     if (sh.chunk < 32) return fail(ICP_ERR_INVALID_ARGUMENT, "chunk_rays must be at least 32");
+    // a warp flushes its lanes' 32-bit counters once per chunk: keep a chunk within their range
+    sh.chunk = (uint32_t)std::max<uint64_t>(32u, std::min<uint64_t>(sh.chunk, lane_rays_max(s.max_internal_hits)));
     int per_sm = drop_batch_blocks_per_sm(s.precision, sh.threads, s.nt);
     if (per_sm <= 0) return fail(ICP_ERR_DEVICE, "batch trace kernel cannot be resident");
     if (s.blocks_per_sm) per_sm = std::min<int>(per_sm, (int)s.blocks_per_sm);

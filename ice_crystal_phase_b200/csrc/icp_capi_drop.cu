@@ -231,7 +231,7 @@ int drop_trace_enqueue(icp_context* c, const icp_drop_record* r, uint64_t first,
     const uint32_t wpb = threads / 32;
     uint64_t blocks = (uint64_t)per_sm * c->sms;
     blocks = std::max<uint64_t>(1, std::min<uint64_t>(blocks, (count + 64ull * wpb - 1) / (64ull * wpb)));
-    const uint64_t piece = blocks * wpb * 65536ull;
+    const uint64_t piece = blocks * wpb * lane_rays_max(r->max_internal_hits);
     if (f32)
         if (const int e = ensure_float_edges(c, d_edges, g->nt)) return e;
     HexLaunch L = drop_launch(r, g, d_edges, (const float*)c->edges_f.ptr, d_mass, d_stats, area_weight, slots);

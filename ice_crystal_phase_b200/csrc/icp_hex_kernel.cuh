@@ -245,11 +245,15 @@ template <class R> struct LaneRay {
     bool live;
 };
 
+// Per-lane accumulators, summed per warp when a block (or a batch chunk) ends.  The power sums are
+// exact 64-bit fixed-point integers; the counts are 32-bit: a lane traces at most
+// lane_rays_max(max_hits) rays between flushes (the launchers cut launches and chunks to that),
+// so that none of them can wrap.
 template <class R> struct LaneAcc {
-    unsigned long long esc_fx, unres_fx, fwd_fx, bwd_fx, outputs, rays, rejected, snapped, near_edge, fallback, invalid, encounters,
-        missed;
-    unsigned gauge_evals;
-    double axial, max_bal, max_iface;
+    unsigned long long esc_fx, unres_fx, fwd_fx, bwd_fx;
+    uint32_t outputs, rays, rejected, snapped, near_edge, fallback, invalid, encounters, missed, gauge_evals;
+    double axial, max_bal;
+    R max_iface;
     uint64_t cur_batch;
     uint32_t cur_batch_out;
 };
@@ -329,10 +333,11 @@ __device__ __forceinline__ BlockShared<R> block_setup(const P_& P, unsigned char
 
 template <class R> __device__ __forceinline__ void lane_acc_clear(LaneAcc<R>& A)
 {
-    A.esc_fx = A.unres_fx = A.fwd_fx = A.bwd_fx = A.outputs = A.rays = A.rejected = 0ull;
-    A.snapped = A.near_edge = A.fallback = A.invalid = A.encounters = A.missed = 0ull;
+    A.esc_fx = A.unres_fx = A.fwd_fx = A.bwd_fx = 0ull;
+    A.outputs = A.rays = A.rejected = A.snapped = A.near_edge = A.fallback = A.invalid = A.encounters = A.missed = 0u;
     A.gauge_evals = 0u;
-    A.axial = A.max_bal = A.max_iface = 0.0;
+    A.axial = A.max_bal = 0.0;
+    A.max_iface = R(0);
     A.cur_batch = ~0ull;
     A.cur_batch_out = 0u;
 }
@@ -456,7 +461,7 @@ __device__ __forceinline__ void trace_slice(const P_& P, const BlockShared<R>& B
             if (hs) {
                 finish_ray<R>(P, L, A, s_status, hs, sizeof(R) == 4 ? L.pfx : to_fix(L.S.I), L.S.I);
             } else {
-                A.near_edge += near_edge ? 1ull : 0ull;
+                A.near_edge += near_edge ? 1u : 0u;
                 ++L.hits;
                 ++A.encounters;
                 do_split = true;
@@ -469,7 +474,7 @@ __device__ __forceinline__ void trace_slice(const P_& P, const BlockShared<R>& B
         }
         if (do_split) {
             const Interface<R> sp = split(sd, se, sS, sn, *media);
-            A.max_iface = fmax(A.max_iface, (double)sp.balance);
+            A.max_iface = rmax(A.max_iface, sp.balance);
             // entry: exterior reflection exits, transmission continues;
             // internal: transmission exits, reflection continues
             unsigned long long cont_fx = 0ull;
@@ -524,7 +529,7 @@ __device__ __forceinline__ void trace_slice(const P_& P, const BlockShared<R>& B
                 v = efx;
                 A.esc_fx += v;
                 A.outputs += 1;
-                A.snapped += b.snapped ? 1ull : 0ull;
+                A.snapped += b.snapped ? 1u : 0u;
                 A.axial += (double)opow * b.mu;
                 if (b.pole > 0) A.fwd_fx += v;
                 else if (b.pole < 0) A.bwd_fx += v;
@@ -533,18 +538,22 @@ __device__ __forceinline__ void trace_slice(const P_& P, const BlockShared<R>& B
         }
         hist_add(B.H, P.mass, P.to_mass, to_table, cell, v, A.fallback);
 
-        // ---- per-batch exit counts (capacity audit), flushed when the lane's batch changes
-        if (P.batch_out && (has || fresh)) {
-            const uint64_t bidx = L.id / P.batch_size;
-            if (bidx != A.cur_batch) {
-                if (A.cur_batch != ~0ull && A.cur_batch_out) atomicAdd(&P.batch_out[A.cur_batch], A.cur_batch_out);
-                A.cur_batch = bidx;
-                A.cur_batch_out = 0u;
+        // ---- per-batch exit counts (the prism's capacity audit), flushed when the lane's batch
+        // changes
+        if constexpr (std::is_same_v<G, HexGeo<R>>) {
+            if (P.batch_out && (has || fresh)) {
+                const uint64_t bidx = L.id / P.batch_size;
+                if (bidx != A.cur_batch) {
+                    if (A.cur_batch != ~0ull && A.cur_batch_out) atomicAdd(&P.batch_out[A.cur_batch], A.cur_batch_out);
+                    A.cur_batch = bidx;
+                    A.cur_batch_out = 0u;
+                }
+                A.cur_batch_out += has ? 1u : 0u;
             }
-            A.cur_batch_out += has ? 1u : 0u;
         }
     }
-    if (P.batch_out && A.cur_batch != ~0ull && A.cur_batch_out) atomicAdd(&P.batch_out[A.cur_batch], A.cur_batch_out);
+    if constexpr (std::is_same_v<G, HexGeo<R>>)
+        if (P.batch_out && A.cur_batch != ~0ull && A.cur_batch_out) atomicAdd(&P.batch_out[A.cur_batch], A.cur_batch_out);
 }
 
 // Block epilogue (all threads): flush the table into P.mass and the lane accumulators and the
@@ -561,7 +570,7 @@ __device__ __forceinline__ void block_flush(const P_& P, const BlockShared<R>& B
 #pragma unroll
     for (int q = 0; q < 14; ++q)
         for (int o = 16; o; o >>= 1) w[q] += __shfl_xor_sync(kFull, w[q], o);
-    double ax = A.axial, mb = A.max_bal, mi = A.max_iface;
+    double ax = A.axial, mb = A.max_bal, mi = (double)A.max_iface;
     for (int o = 16; o; o >>= 1) {
         ax += __shfl_xor_sync(kFull, ax, o);
         mb = fmax(mb, __shfl_xor_sync(kFull, mb, o));

@@ -108,6 +108,16 @@ struct HexLaunch {
     uint32_t blocks;
 };
 
+// Most rays one lane may trace between two flushes of its 32-bit counters (icp_hex_kernel.cuh
+// LaneAcc): a ray adds at most max_hits + 1 outputs and encounters and 40 gauge evaluations per
+// intersection, so launch pieces (rays per warp) and batch chunks stay at or below this.
+inline uint64_t lane_rays_max(uint32_t max_hits)
+{
+    const uint64_t per_ray = 40ull * ((uint64_t)max_hits + 1ull);
+    const uint64_t n = 0xffffffffull / per_ray;
+    return n > 65536ull ? 65536ull : (n ? n : 1ull);
+}
+
 size_t hex_stats_bytes();
 int launch_hex_f32(const HexLaunch& L, cudaStream_t stream);
 int launch_hex_f64(const HexLaunch& L, cudaStream_t stream);
