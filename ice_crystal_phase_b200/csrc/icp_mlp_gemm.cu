@@ -164,10 +164,16 @@ __device__ __forceinline__ float epilogue_cols(const GemmArgs& g, uint32_t taddr
     constexpr bool kTrain = EPI == kHiddenTrain || EPI == kHeadTrain;
     constexpr bool kLayer = kHeadEpi || EPI == kHidden || EPI == kHiddenTrain;
     float yacc = 0.0f;
+    // columns in pairs of 32: both TMEM loads of a pair are in flight together (one wait per 64
+    // columns; c1 - c0 is a multiple of 64)
 #pragma unroll 1
-    for (uint32_t c = c0; c < c1; c += 32u) {
-        float v[32];
-        umma::tmem_ld32(taddr + c, v);
+    for (uint32_t c2 = c0; c2 < c1; c2 += 64u) {
+        float vv[2][32];
+        umma::tmem_ld32x2(taddr + c2, vv[0], vv[1]);
+#pragma unroll
+    for (uint32_t h = 0; h < 2; ++h) { // unrolled: vv[h] stays in registers
+        const uint32_t c = c2 + 32u * h;
+        float (&v)[32] = vv[h];
         if constexpr (EPI == kStoreF32) {
             float4* d = reinterpret_cast<float4*>(g.out_f32 + (size_t)m * g.ld_out + c);
 #pragma unroll
@@ -213,6 +219,7 @@ __device__ __forceinline__ float epilogue_cols(const GemmArgs& g, uint32_t taddr
             if (g.out_dzT) store_bf16x32_t(g.out_dzT + (size_t)c * g.ld_t + (m - lane), g.ld_t, v, tbuf, lane);
             if (g.out_db) atomicAdd(&colsum[c + lane], warp_column_sum(v, lane));
         }
+    }
     }
     return yacc;
 }
@@ -395,7 +402,7 @@ __global__ void __launch_bounds__(kPThreads, 1)
     constexpr uint32_t BB = (uint32_t)N * 128u;   // one 64-wide K chunk of B
     constexpr uint32_t W = (uint32_t)N / kSlices; // columns per epilogue warp
     static_assert(S >= 2, "ring too shallow");
-    static_assert(W % 32u == 0, "slice width");
+    static_assert(W % 64u == 0, "slice width: the epilogue takes columns in pairs of 32");
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* bres = smem;
