@@ -953,8 +953,9 @@ def cdf_kernel_times(I, ctx, stream, values, nt: int, np_: int, phi, theta, flus
     """Device time of the CDF kernel alone: icp_phase_cdf_enqueue puts one cooperative kernel on
     the library's stream (the grid's u edges are already on the device after the first build, and
     the barrier counters are left at zero by every build), bracketed by CUDA events on that
-    stream; the L2 is flushed before each launch.  The report is then checked through
-    icp_phase_cdf_result."""
+    stream; the L2 is flushed before each launch.  A short spin kernel ahead of the first event
+    keeps the stream busy while the host enqueues, so the events bracket the kernel and not the
+    host's launch latency.  The report is then checked through icp_phase_cdf_result."""
     import ctypes as C
 
     import torch
@@ -968,6 +969,8 @@ def cdf_kernel_times(I, ctx, stream, values, nt: int, np_: int, phi, theta, flus
         flush.fill_(1.0)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            torch.cuda._sleep(200_000)  # about 0.1 ms of device time
         e0.record(stream)
         I.check(I.LIB.icp_phase_cdf_enqueue(*args))
         e1.record(stream)

@@ -108,6 +108,7 @@ constexpr unsigned kWarps = kThreads / 32;
 constexpr unsigned kMaxBoxes = 16;
 constexpr unsigned kSpinLimit = 1u << 22;
 constexpr unsigned kFull = 0xffffffffu;
+constexpr uint32_t kChain = 8; // loads in flight ahead of an ordered chain of additions
 
 // Shared-memory layout of one block (the same function sizes the launch on the host).
 struct Layout {
@@ -426,15 +427,29 @@ __global__ void __launch_bounds__(kThreads, 2) cdf_build_kernel(const __grid_con
     __syncthreads();
     if (tid < w) {
         // ordered ascending-theta scan of one phi column; the unnormalised prefix of row i+1
-        // replaces the weight of row i in place (each column belongs to one thread)
-        const uint32_t cl = tid;
-        double s = 0.0;
-#pragma unroll 8
-        for (uint32_t i = 0; i < ct; ++i) {
-            s += B[(size_t)i * CW + cl];
-            B[(size_t)i * CW + cl] = s;
+        // replaces the weight of row i in place (each column belongs to one thread).  The next
+        // kChain weights are loaded before the current ones are added, so the shared-memory
+        // latency overlaps the dependent chain of additions.
+        double* col = B + tid;
+        double s = 0.0, nx[kChain];
+#pragma unroll
+        for (uint32_t k = 0; k < kChain; ++k) nx[k] = k < ct ? col[(size_t)k * CW] : 0.0;
+        for (uint32_t i = 0; i < ct; i += kChain) {
+            double cu[kChain];
+#pragma unroll
+            for (uint32_t k = 0; k < kChain; ++k) {
+                cu[k] = nx[k];
+                const uint32_t r = i + kChain + k;
+                nx[k] = r < ct ? col[(size_t)r * CW] : 0.0;
+            }
+#pragma unroll
+            for (uint32_t k = 0; k < kChain; ++k)
+                if (i + k < ct) {
+                    s += cu[k];
+                    col[(size_t)(i + k) * CW] = s;
+                }
         }
-        P.colsum[c0 + cl] = s;
+        P.colsum[c0 + tid] = s;
     }
     {
         const double t = block_sum(tv.v + tv.c, red_d);
@@ -453,17 +468,27 @@ __global__ void __launch_bounds__(kThreads, 2) cdf_build_kernel(const __grid_con
     const uint32_t stride = ct + 1;
     if (warp == 0) {
         if (lane == 0) {
-            // ordered marginal scan (phase_table.cpp:154): phi[j+1] = phi[j] + colsum[j]
-            double a = 0.0;
-#pragma unroll 8
-            for (uint32_t j = 0; j < c0; ++j) a += S[j];
-            sphi[0] = a;
-            for (uint32_t cl = 0; cl < w; ++cl) {
-                a += S[c0 + cl];
-                sphi[cl + 1] = a;
+            // ordered marginal scan (phase_table.cpp:154): phi[j+1] = phi[j] + colsum[j], the
+            // column sums read kChain ahead of the additions
+            double a = 0.0, nx[kChain];
+#pragma unroll
+            for (uint32_t k = 0; k < kChain; ++k) nx[k] = k < P.cp ? S[k] : 0.0;
+            for (uint32_t j = 0; j < P.cp; j += kChain) {
+                double cu[kChain];
+#pragma unroll
+                for (uint32_t k = 0; k < kChain; ++k) {
+                    cu[k] = nx[k];
+                    nx[k] = j + kChain + k < P.cp ? S[j + kChain + k] : 0.0;
+                }
+#pragma unroll
+                for (uint32_t k = 0; k < kChain; ++k) {
+                    const uint32_t jj = j + k;
+                    if (jj == c0) sphi[0] = a;
+                    if (jj < P.cp) a += cu[k];
+                    if (jj >= c0 && jj < c1) sphi[jj - c0 + 1] = a;
+                }
             }
-#pragma unroll 8
-            for (uint32_t j = c1; j < P.cp; ++j) a += S[j];
+            if (c0 >= P.cp) sphi[0] = a;
             s_tot[3] = a;
         }
     } else {

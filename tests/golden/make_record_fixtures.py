@@ -31,7 +31,8 @@ RECORDS = {
     "drop_oblate_1.5mm_650nm_90x180": ["rainbow_generate", "--wavelength-nm", "650", "--radius-mm", "1.5",
                                        "--shape-coefficients", "0,-0.08,-0.02,0.005", "--inclination-deg", "20",
                                        "--query-theta", "90", "--query-phi", "180", "--rays", "200000",
-                                       "--max-internal-hits", "10", "--diffraction", "analytic"],
+                                       "--max-internal-hits", "10", "--max-unresolved-fraction", "1e-3",
+                                       "--diffraction", "analytic"],
     # a Table-I drop, stored coarser than traced
     "drop_table1_0.5mm_550nm_72x144_36x72": ["rainbow_generate", "--wavelength-nm", "550", "--radius-mm", "0.5",
                                              "--query-theta", "72", "--query-phi", "144", "--cdf-theta", "36",
