@@ -252,6 +252,27 @@ class OpticsInput(C.Structure):
                 ("input_polarization", C.c_uint32), ("reserved", C.c_uint32)]
 
 
+class Field32(C.Structure):
+    _fields_ = [("x_real", C.c_float), ("x_imag", C.c_float), ("y_real", C.c_float), ("y_imag", C.c_float)]
+
+
+class RaindropConfig(C.Structure):
+    """icp_raindrop_config = rainbow::RaindropTraceConfig (116 B)."""
+    _fields_ = [("coefficients", C.c_float * 8), ("inner_radius", C.c_float), ("outer_radius", C.c_float),
+                ("incident_direction", Vec3f), ("incident_basis_x", Vec3f), ("incident_field", Field32),
+                ("radius_mm", C.c_float), ("wavelength_nm", C.c_float), ("exterior_index", C.c_float),
+                ("interior_index", C.c_float), ("grid_half_extent", C.c_float), ("reference_distance", C.c_float),
+                ("outgoing_reference_distance", C.c_float), ("grid_width", C.c_uint32), ("grid_height", C.c_uint32)]
+
+
+class LatticeStats(C.Structure):
+    _fields_ = [("status_counts", (C.c_uint64 * 8) * 4), ("intersection_fallbacks", C.c_uint64),
+                ("snell_fallbacks", C.c_uint64), ("incomplete", C.c_uint64), ("first_problem", C.c_uint64)]
+
+    def histogram(self) -> np.ndarray:
+        return np.array([[self.status_counts[f][s] for s in range(8)] for f in range(4)], dtype=np.uint64)
+
+
 class FocalConfig(C.Structure):
     _fields_ = [("grid_width", C.c_uint32), ("grid_height", C.c_uint32), ("grid_half_extent", C.c_float),
                 ("reserved", C.c_uint32), ("quarter_turn_offsets", C.c_uint32 * 4)]
@@ -378,6 +399,9 @@ _FUNCS = {
     "icp_atlas_compose": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, _P, _P, _P]),
     "icp_patch_build": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32, C.c_float, _P, _P, _P, C.POINTER(C.c_uint32),
                                   C.POINTER(C.c_uint64)]),
+    "icp_raindrop_config_make": (C.c_int, [C.c_float, C.c_int, C.POINTER(C.c_float), C.c_float, C.c_float,
+                                           C.POINTER(C.c_float), C.c_uint32, C.c_uint32, C.POINTER(RaindropConfig)]),
+    "icp_lattice_trace": (C.c_int, [_P, C.POINTER(RaindropConfig), _P, _P, C.POINTER(LatticeStats)]),
     "icp_query_directions": (C.c_int, [C.c_uint32, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float),
                                        C.POINTER(C.c_float)]),
     "icp_patch_query": (C.c_int, [_P, _P, C.c_uint32, _P, _P, C.c_uint32, _P, C.c_uint32, _P, _P, _P, C.c_uint64,
@@ -1276,6 +1300,37 @@ def patch_build(ctx: Context, vertices, grid_width: int, grid_height: int, grid_
                               ds.ptr, C.byref(count), hist))
     n = count.value
     return PatchBuild(dp.download()[:n], db.download()[:n], ds.download(), list(hist))
+
+
+def raindrop_config(radius_mm: float, wavelength_nm: float, interior_index: float, incident_direction, grid: int,
+                    sphere: bool = False, coefficients=None, grid_height: int | None = None) -> RaindropConfig:
+    """RaindropSettings::make_config of an unpolarised trace (icp_raindrop_config_make)."""
+    cfg = RaindropConfig()
+    d = (C.c_float * 3)(*map(float, incident_direction))
+    coef = None if coefficients is None else (C.c_float * 8)(*[float(x) for x in list(coefficients) + [0.0] * 8][:8])
+    check(LIB.icp_raindrop_config_make(C.c_float(radius_mm), int(bool(sphere)), coef, C.c_float(wavelength_nm),
+                                       C.c_float(interior_index), d, grid, grid if grid_height is None else grid_height,
+                                       C.byref(cfg)))
+    return cfg
+
+
+@dataclass
+class Lattice:
+    vertices: "DeviceArray"      # VERTEX_DTYPE [4 W H], family-major
+    second: "DeviceArray | None"  # float32 [4 W H, 4], the second response column
+    stats: LatticeStats
+    config: RaindropConfig
+
+
+def lattice_trace(ctx: Context, config: RaindropConfig, unpolarized: bool = True) -> Lattice:
+    """The four-family outgoing-ray lattice of one drop on the device (icp_lattice_trace)."""
+    n = 4 * config.grid_width * config.grid_height
+    dv = DeviceArray(ctx, n, VERTEX_DTYPE)
+    ds = DeviceArray(ctx, n * 4, np.float32) if unpolarized else None
+    st = LatticeStats()
+    check(LIB.icp_lattice_trace(ctx.handle, C.byref(config), dv.ptr, ds.ptr if ds is not None else None,
+                                C.byref(st)))
+    return Lattice(dv, ds, st, config)
 
 
 def query_directions(theta_count: int, phi_count: int, axis, e0) -> np.ndarray:

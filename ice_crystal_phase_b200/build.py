@@ -54,6 +54,7 @@ UNITS = {
     "icp_optics.cu": ["-fmad=false"],
     "icp_patches.cu": ["-fmad=false"],
     "icp_query.cu": ["-fmad=false"],
+    "icp_lattice.cu": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"],
 }
 
 HOST_SOURCES = ["icp_record_io.cpp"]

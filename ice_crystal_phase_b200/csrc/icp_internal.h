@@ -311,6 +311,8 @@ struct icp_context {
     icp::Scratch query, query_list;
     // wave-stage density audit accumulators
     icp::Scratch stage_audit;
+    // lattice trace tallies
+    icp::Scratch lattice;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
     // grid-barrier iteration limit handed to the CDF kernels (0: their default)
     uint32_t wait_limit = 0;

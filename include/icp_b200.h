@@ -736,6 +736,58 @@ typedef struct {                                             /* rainbow::FocalPh
     uint32_t quarter_turn_offsets[4];                        /* per family, 0 .. 3                */
 } icp_focal_config;
 
+/* ------------------------------------------------------- lattice trace (drop wave stages) */
+/* rainbow::RaindropTraceConfig, 116 B (include/rainbow/raindrop_trace_data.hpp:61-96): the drop
+ * shape (r/a = 1 + sum c_n cos(n chi), chi from -y, with conservative inner / outer radii), the
+ * incident direction and its transverse basis e0, the single-input field, the radius, vacuum
+ * wavelength and indices, and the incident lattice (grid_width x grid_height vertices spanning
+ * [-grid_half_extent, grid_half_extent]^2 about the drop, reference_distance before it). */
+typedef struct {
+    float coefficients[8];
+    float inner_radius, outer_radius;
+    icp_vec3f incident_direction, incident_basis_x;
+    icp_field32 incident_field;
+    float radius_mm, wavelength_nm, exterior_index, interior_index;
+    float grid_half_extent, reference_distance, outgoing_reference_distance;
+    uint32_t grid_width, grid_height;
+} icp_raindrop_config;
+
+/* RaindropSettings::make_config (include/rainbow/raindrop_settings.hpp:19-43) for an
+ * unpolarised trace: the Table-I shape of radius_mm (RaindropShape::try_make; sphere != 0 forces
+ * the sphere) or, with coefficients != NULL, those 8 coefficients with the same bounding radii;
+ * incident_direction normalised in binary32 and e0 from TransverseFrame::from_direction;
+ * exterior index 1, half extent 1.01 r_out, reference distances 2 r_out.  The reference's range
+ * checks and messages (radius (0,3], wavelength [380,830] nm, interior index [1,2], grid >= 2 with
+ * 4 W H < 2^32, finite nonzero direction) -> ICP_ERR_INVALID_ARGUMENT.  Host function. */
+int icp_raindrop_config_make(float radius_mm, int sphere, const float* coefficients, float wavelength_nm,
+                             float interior_index, const float incident_direction[3], uint32_t grid_width,
+                             uint32_t grid_height, icp_raindrop_config* out);
+
+/* Per-family vertex statuses of a lattice trace and the trace validation of
+ * PhaseCdf::validate_trace (src/phase_cdf.cpp:238-253). */
+typedef struct {
+    uint64_t status_counts[4][8];   /* [family R, TT, TRT, TRRT][VertexStatus 0..7]                 */
+    uint64_t intersection_fallbacks; /* records whose diagnostics carry IntersectionFallback (1)    */
+    uint64_t snell_fallbacks;        /* ... SnellFallback (2)                                        */
+    uint64_t incomplete;             /* records neither Valid, Miss nor TIR, or Valid with a
+                                        non-finite value or an invalid optical path                  */
+    uint64_t first_problem;          /* smallest such record index, or UINT64_MAX                    */
+} icp_lattice_stats;
+
+/* The four-family outgoing-ray lattice of one drop: per vertex (row-major, index iy W + ix) one
+ * incident ray traced through R, TT, TRT and TRRT into d_vertices[4 W H] (device, family-major:
+ * record f W H + index), exactly RaindropPathTracer::trace_vertex_unpolarized
+ * (include/rainbow/raindrop_paths.hpp:27-107) with the reference's intersector and interface,
+ * every record bit-identical to the reference's.  d_second_fields[4 W H] (device) receives the
+ * second response column (unpolarised trace: unit input states, RaindropTracer::
+ * trace_unpolarized); with d_second_fields == NULL the single-input trace of
+ * config->incident_field (RaindropTracer::trace).  stats (host, may be NULL) gets the status
+ * histogram and the trace validation.  Replaces RaindropTracer::trace_unpolarized's OptiX launch
+ * (src/raindrop_tracer.cpp:144-177, shaders/entry/raindrop_trace.cu:49-83) and
+ * PhaseCdf::validate_trace. */
+int icp_lattice_trace(icp_context* ctx, const icp_raindrop_config* config, icp_outgoing_vertex* d_vertices,
+                      icp_field32* d_second_fields, icp_lattice_stats* stats);
+
 /* Padded bounding box of a patch's four corner directions (rainbow::PatchAabb, 24 B). */
 typedef struct { float min_x, min_y, min_z, max_x, max_y, max_z; } icp_patch_aabb;
 

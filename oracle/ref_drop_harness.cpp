@@ -16,9 +16,14 @@
 //             The tracer's Jones columns are amplitude responses; the flux power multiplies
 //             0.5 (|col0|^2 + |col1|^2) by n_t cos_t / (n_i cos_i) of both transmissions,
 //             taken from the logged boundary queries.
-//   vertices  radius sphere n_int kx ky kz grid out.bin: the same lattice trace as raw records
-//             (u32 width, height; f32 half_extent, incident[3], basis_x[3]; OutgoingVertex[4 n];
-//             Field32[4 n], the second response column)
+//   vertices  radius sphere n_int kx ky kz grid out.bin [wavelength_nm [c0 .. c7]]: the same
+//             lattice trace as raw records (u32 width, height; f32 half_extent, incident[3],
+//             basis_x[3]; OutgoingVertex[4 n]; Field32[4 n], the second response column); an
+//             optional wavelength (default 700 nm) and explicit shape coefficients (with the
+//             bounding radii, half extent and reference distances derived from them as
+//             RaindropShape::try_make and make_config do)
+//   config    radius sphere n_int kx ky kz grid wavelength_nm [c0 .. c7]: the RaindropTraceConfig
+//             of those settings, its 116 bytes as hex
 //   time      radius sphere n_int kx ky kz grid row0 rows [c0 .. c7]: traces lattice rows
 //             [row0, row0+rows) with RaindropPathTracer::trace_vertex_unpolarized and prints
 //             "vertices hits seconds" (the reference's CPU drop tracer; optional coefficients
@@ -122,19 +127,52 @@ int families(int argc, char** argv)
 
 // The reference's unpolarized lattice trace as raw records: u32 width, height; f32 half_extent,
 // incident[3], basis_x[3]; OutgoingVertex[4 * count]; Field32[4 * count] (second column).
-int vertices(int argc, char** argv)
+// Settings from argv[2..8], an optional wavelength at argv[first] and optional coefficients
+// at argv[first + 1 .. first + 8].
+RaindropTraceConfig lattice_config(int argc, char** argv, int first)
 {
-    if (argc != 10) {
-        std::fprintf(stderr, "vertices radius sphere n_int kx ky kz grid out.bin\n");
-        return 1;
-    }
     RaindropSettings s;
     s.radius_mm = std::strtof(argv[2], nullptr);
     s.force_sphere = std::atoi(argv[3]) != 0;
     s.interior_index = std::strtof(argv[4], nullptr);
     s.incident_direction = {std::strtof(argv[5], nullptr), std::strtof(argv[6], nullptr), std::strtof(argv[7], nullptr)};
     s.grid_width = s.grid_height = (std::uint32_t)std::atoi(argv[8]);
-    const RaindropTraceConfig cfg = s.make_config();
+    if (argc > first) s.wavelength_nm = std::strtof(argv[first], nullptr);
+    RaindropTraceConfig cfg = s.make_config();
+    if (argc == first + 9) {
+        const float inf = std::numeric_limits<float>::infinity();
+        float sum = 0.0f;
+        for (int k = 0; k < 8; ++k) cfg.shape.coefficients[k] = std::strtof(argv[first + 1 + k], nullptr);
+        for (int k = 1; k < 8; ++k) sum = ::nextafterf(sum + ::fabsf(cfg.shape.coefficients[k]), inf);
+        const float center = 1.0f + cfg.shape.coefficients[0];
+        cfg.shape.inner_radius = ::nextafterf(center - sum - 0x1p-20f, -inf);
+        cfg.shape.outer_radius = ::nextafterf(center + sum + 0x1p-20f, inf);
+        cfg.grid_half_extent = cfg.shape.outer_radius * 1.01f;
+        cfg.reference_distance = cfg.outgoing_reference_distance = 2.0f * cfg.shape.outer_radius;
+    }
+    return cfg;
+}
+
+int config(int argc, char** argv)
+{
+    if (argc != 10 && argc != 18) {
+        std::fprintf(stderr, "config radius sphere n_int kx ky kz grid wavelength_nm [c0 .. c7]\n");
+        return 1;
+    }
+    const RaindropTraceConfig cfg = lattice_config(argc, argv, 9);
+    const unsigned char* b = reinterpret_cast<const unsigned char*>(&cfg);
+    for (size_t i = 0; i < sizeof cfg; ++i) std::printf("%02x", b[i]);
+    std::printf("\n");
+    return 0;
+}
+
+int vertices(int argc, char** argv)
+{
+    if (argc != 10 && argc != 11 && argc != 19) {
+        std::fprintf(stderr, "vertices radius sphere n_int kx ky kz grid out.bin [wavelength_nm [c0 .. c7]]\n");
+        return 1;
+    }
+    const RaindropTraceConfig cfg = lattice_config(argc, argv, 10);
     const std::uint32_t count = cfg.vertex_count();
     std::vector<OutgoingVertex> v(4 * (size_t)count);
     std::vector<Field32> second(4 * (size_t)count);
@@ -201,7 +239,7 @@ int time_rows(int argc, char** argv)
 int main(int argc, char** argv)
 {
     if (argc < 2) {
-        std::fprintf(stderr, "usage: ref_drop_harness water|shape|area|frame|families|vertices ...\n");
+        std::fprintf(stderr, "usage: ref_drop_harness water|shape|area|frame|families|vertices|config ...\n");
         return 1;
     }
     const std::string mode = argv[1];
@@ -209,6 +247,7 @@ int main(int argc, char** argv)
     try {
         if (mode == "families") return families(argc, argv);
         if (mode == "vertices") return vertices(argc, argv);
+        if (mode == "config") return config(argc, argv);
         if (mode == "time") return time_rows(argc, argv);
         std::string line;
         while (std::getline(std::cin, line)) {
