@@ -273,6 +273,24 @@ class LatticeStats(C.Structure):
         return np.array([[self.status_counts[f][s] for s in range(8)] for f in range(4)], dtype=np.uint64)
 
 
+class FoldedConfig(C.Structure):
+    _fields_ = [("relative_tolerance", C.c_double), ("maximum_panels", C.c_uint32), ("maximum_depth", C.c_uint32)]
+
+
+class FoldedView(C.Structure):
+    _fields_ = [("record_indices", C.c_void_p), ("records", C.c_void_p), ("patch_count", C.c_uint32),
+                ("record_count", C.c_uint32)]
+
+
+class FoldedStats(C.Structure):
+    _fields_ = [("candidates", C.c_uint32), ("prepared", C.c_uint32), ("unresolved", C.c_uint32),
+                ("branch_count", C.c_uint32), ("focal_pending_branches", C.c_uint32), ("reserved", C.c_uint32),
+                ("largest_estimated_relative_error", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
 class FocalConfig(C.Structure):
     _fields_ = [("grid_width", C.c_uint32), ("grid_height", C.c_uint32), ("grid_half_extent", C.c_float),
                 ("reserved", C.c_uint32), ("quarter_turn_offsets", C.c_uint32 * 4)]
@@ -297,6 +315,12 @@ OPTICAL_DTYPE = np.dtype([("path_field", "<f8", 4), ("incoherent_s", "<f8"), ("i
                                                "first_problem_patch_id", "folded_hits")] +
                          [("path_field_second", "<f8", 4)])
 AABB_DTYPE = np.dtype([(k, "<f4") for k in ("min_x", "min_y", "min_z", "max_x", "max_y", "max_z")])
+FOLDED_BRANCH_DTYPE = np.dtype([("u0", "<f8"), ("u1", "<f8"), ("area_fraction", "<f8"), ("solid_angle_sr", "<f8"),
+                                ("representative_u", "<f8"), ("representative_v", "<f8"), ("sign", "<i4"),
+                                ("focal_flags", "<u4"), ("quarter_turns", "<u4"), ("extra_quarter_turn", "<u4")])
+FOLDED_DTYPE = np.dtype([("compact_index", "<u4"), ("patch_id", "<u4"), ("flags", "<u4"), ("branch_count", "<u4"),
+                         ("jacobian", "<f8", 4), ("branches", FOLDED_BRANCH_DTYPE, 4),
+                         ("largest_estimated_relative_error", "<f8"), ("panels", "<u4"), ("reserved", "<u4")])
 
 
 class DensityReport(C.Structure):
@@ -358,6 +382,7 @@ _FUNCS = {
                                              C.c_uint32, C.c_uint32, C.POINTER(CdfPolicy), _P, _P,
                                              C.POINTER(CdfReport)]),
     "icp_water_index": (C.c_int, [C.c_double, C.c_double, C.c_double, _D, _D]),
+    "icp_water_state": (C.c_int, [C.c_double, C.c_double, C.c_double, _D]),
     "icp_drop_shape": (C.c_int, [C.c_double, C.c_int, _D, _D, _D]),
     "icp_drop_projected_area": (C.c_int, [_D, C.c_double, _D, _D]),
     "icp_drop_frame": (C.c_int, [C.c_double, _D, _D, _D]),
@@ -407,6 +432,11 @@ _FUNCS = {
     "icp_patch_query": (C.c_int, [_P, _P, C.c_uint32, _P, _P, C.c_uint32, _P, C.c_uint32, _P, _P, _P, C.c_uint64,
                                   C.POINTER(C.c_uint64)]),
     "icp_patch_optics": (C.c_int, [_P, C.POINTER(OpticsInput), _P, C.POINTER(FocalConfig), _P]),
+    "icp_patch_optics_folded": (C.c_int, [_P, C.POINTER(OpticsInput), _P, C.POINTER(FocalConfig), _P,
+                                          C.POINTER(FoldedView)]),
+    "icp_folded_prepare": (C.c_int, [_P, _P, C.c_uint32, _P, C.c_uint32, C.POINTER(C.c_float), C.POINTER(FocalConfig),
+                                     C.POINTER(FoldedConfig), _P, _P, C.c_uint32, C.POINTER(C.c_uint32),
+                                     C.POINTER(FoldedStats)]),
     "icp_stage_density": (C.c_int, [_P, C.c_uint32, _P, _P, _P, C.c_uint64, _P, C.POINTER(DensityReport)]),
     "icp_rainbow_table_sigma": (C.c_int, [C.c_float, _D]),
     "icp_rainbow_detect": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32, C.POINTER(DiffractionConfig), _P]),
@@ -827,14 +857,17 @@ class WaterOpticalState:
     density_kg_m3: float
     temperature_kelvin: float
     pressure_pascal: float
+    density_pressure_residual_pascal: float = 0.0
+    density_bracket_width_kg_m3: float = 0.0
 
 
 def evaluate_water_optics(vacuum_wavelength_nm: float, temperature_celsius: float = 20.0,
                           pressure_pascal: float = 101325.0) -> WaterOpticalState:
-    """IAPWS R9-97 real index of liquid water; bounded to 200..1100 nm, 0..60 C, 50 kPa..100 MPa."""
-    n, rho = C.c_double(), C.c_double()
-    check(LIB.icp_water_index(vacuum_wavelength_nm, temperature_celsius, pressure_pascal, C.byref(n), C.byref(rho)))
-    return WaterOpticalState(n.value, rho.value, temperature_celsius + 273.15, pressure_pascal)
+    """IAPWS R9-97 real index of liquid water with its IAPWS-95 density (evaluate_water_optics);
+    bounded to 200..1100 nm, 0..60 C, 50 kPa..100 MPa."""
+    w = (C.c_double * 6)()
+    check(LIB.icp_water_state(vacuum_wavelength_nm, temperature_celsius, pressure_pascal, w))
+    return WaterOpticalState(w[5], w[2], w[0], w[1], w[3], w[4])
 
 
 @dataclass
@@ -1243,14 +1276,47 @@ def rainbow_diffraction(ctx: Context, focal, nt: int, np_: int, config: Diffract
 
 
 # ------------------------------------------------------------------ patch optics
+@dataclass
+class FoldedRecords:
+    indices: np.ndarray    # uint32 [patch_count]: record of each compact patch, or 0xffffffff
+    records: np.ndarray    # FOLDED_DTYPE [count], compact-index order
+    stats: "FoldedStats"
+
+
+def folded_prepare(ctx: Context, vertices: "DeviceArray", patches: "DeviceArray", patch_count: int, incident,
+                   focal=None, config: "FoldedConfig | None" = None):
+    """Folded-patch records of every NeedsRefinement patch (icp_folded_prepare) from device arrays:
+    (device record indices, device records or None, count, FoldedStats)."""
+    di = DeviceArray(ctx, max(1, patch_count), np.uint32)
+    n = C.c_uint32(0)
+    st = FoldedStats()
+    k = (C.c_float * 3)(*map(float, incident))
+    fc = None
+    if focal is not None:
+        w, h, e, q = focal
+        fc = FocalConfig(w, h, e, 0, (C.c_uint32 * 4)(*q))
+    cfg = C.byref(config) if config is not None else None
+    args = (ctx.handle, vertices.ptr, vertices.count, patches.ptr, patch_count, k, C.byref(fc) if fc else None, cfg,
+            di.ptr)
+    rc = LIB.icp_folded_prepare(*args, None, 0, C.byref(n), C.byref(st))
+    if n.value == 0:
+        check(rc)
+        return di, None, 0, st
+    dr = DeviceArray(ctx, n.value, FOLDED_DTYPE)
+    check(LIB.icp_folded_prepare(*args, dr.ptr, n.value, C.byref(n), C.byref(st)))
+    return di, dr, n.value, st
+
+
 def patch_optics(ctx: Context, vertices, patches, directions, offsets, summaries, hits, incident, incident_basis,
-                 second=None, polarization: int | None = None, focal=None) -> tuple[np.ndarray, np.ndarray | None]:
+                 second=None, polarization: int | None = None, focal=None, folded: bool = False):
     """Per-direction optics of the drop's wave stages from host arrays (VERTEX_DTYPE, PATCH_DTYPE,
     float32 [n, 3] directions, uint64 [n + 1] hit offsets, SUMMARY_DTYPE [n], HIT_DTYPE, optional
     float32 [vertices, 4] second response column): the OPTICAL_DTYPE results and, with
     focal = (grid_width, grid_height, grid_half_extent, quarter_turn_offsets[4]), the focal stage
     (FOCAL_DTYPE, the input of rainbow_diffraction).  polarization defaults to unpolarized
-    exactly when a second column is given."""
+    exactly when a second column is given.  With folded=True the NeedsRefinement patches get
+    folded-patch records first (icp_folded_prepare) and the optics take them
+    (icp_patch_optics_folded); the records come back as a third value (FoldedRecords)."""
     n = len(directions)
     arrays = [DeviceArray(ctx, len(a), dt).upload(np.ascontiguousarray(a, dtype=dt).reshape(-1))
               for a, dt in ((vertices, VERTEX_DTYPE), (patches, PATCH_DTYPE), (summaries, SUMMARY_DTYPE),
@@ -1271,9 +1337,17 @@ def patch_optics(ctx: Context, vertices, patches, directions, offsets, summaries
     if focal is not None:
         w, h, e, q = focal
         fc = FocalConfig(w, h, e, 0, (C.c_uint32 * 4)(*q))
-    check(LIB.icp_patch_optics(ctx.handle, C.byref(inp), dr.ptr, C.byref(fc) if fc is not None else None,
-                               df.ptr if df is not None else None))
-    return dr.download(), (df.download() if df is not None else None)
+    if not folded:
+        check(LIB.icp_patch_optics(ctx.handle, C.byref(inp), dr.ptr, C.byref(fc) if fc is not None else None,
+                                   df.ptr if df is not None else None))
+        return dr.download(), (df.download() if df is not None else None)
+    di, drec, count, st = folded_prepare(ctx, dv, dp, len(patches), incident, focal)
+    view = FoldedView(di.ptr, drec.ptr if drec is not None else None, len(patches), count)
+    check(LIB.icp_patch_optics_folded(ctx.handle, C.byref(inp), dr.ptr, C.byref(fc) if fc is not None else None,
+                                      df.ptr if df is not None else None, C.byref(view) if drec is not None else None))
+    recs = FoldedRecords(di.download()[:len(patches)], drec.download() if drec is not None else
+                         np.zeros(0, FOLDED_DTYPE), st)
+    return dr.download(), (df.download() if df is not None else None), recs
 
 
 @dataclass

@@ -67,6 +67,18 @@ extern "C" int icp_water_index(double wavelength_nm, double temperature_c, doubl
     return ok();
 }
 
+extern "C" int icp_water_state(double wavelength_nm, double temperature_c, double pressure_pa, icp_water_optics* out)
+{
+    if (!out) return fail(ICP_ERR_INVALID_ARGUMENT, "icp_water_state: null output");
+    try {
+        const auto s = H::water_optics(wavelength_nm, temperature_c, pressure_pa);
+        *out = {s.temperature_k, s.pressure_pa, s.density, s.residual_pa, s.bracket_width, s.index};
+    } catch (const std::exception& e) {
+        return fail(ICP_ERR_INVALID_ARGUMENT, "%s", e.what());
+    }
+    return ok();
+}
+
 extern "C" int icp_drop_shape(double radius_mm, int sphere, double coefficients[8], double* inner, double* outer)
 {
     if (!coefficients) return fail(ICP_ERR_INVALID_ARGUMENT, "icp_drop_shape: null output");

@@ -313,6 +313,8 @@ struct icp_context {
     icp::Scratch stage_audit;
     // lattice trace tallies
     icp::Scratch lattice;
+    // folded-patch records: block counts, candidate list, statistics
+    icp::Scratch folded;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
     // grid-barrier iteration limit handed to the CDF kernels (0: their default)
     uint32_t wait_limit = 0;

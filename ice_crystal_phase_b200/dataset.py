@@ -388,9 +388,11 @@ def record_metadata(c: dict, ii: int, ll: int, spec, rep, water) -> dict:
                      "absorption_model": "ignored_k_equals_zero", "interior_index_evaluated_fp64": water.refractive_index,
                      "interior_index_solver_fp32": spec.interior_index, "exterior_index_solver": 1,
                      "refractive_index_release": "IAPWS R9-97",
-                     "density_model": "Tanaka2001/Kell1975 at 1 atm with UNESCO-1981 secant bulk modulus",
+                     "density_model": "IAPWS R6-95(2018) liquid pressure EOS inversion",
                      "temperature_kelvin": c["temperature_c"] + 273.15, "pressure_pascal": c["pressure_pa"],
-                     "density_kg_m3": water.density_kg_m3},
+                     "density_kg_m3": water.density_kg_m3,
+                     "density_pressure_residual_pascal": water.density_pressure_residual_pascal,
+                     "density_bracket_width_kg_m3": water.density_bracket_width_kg_m3},
         "diffraction_policy": {"name": "fraunhofer_equal_area_circle_v1" if spec.diffraction else "none",
                                "computed": bool(spec.diffraction),
                                "selected_output_includes_diffraction": bool(spec.diffraction),

@@ -303,8 +303,11 @@ inline double pressure(double temperature_k, double density)
 } // namespace iapws95
 
 // Liquid density (kg m^-3) at T (K) and p (Pa); throws std::runtime_error where the reference's
-// solve fails (no bracket, nonfinite pressure, residual above 0.02 Pa, no convergence).
-inline double water_density(double temperature_k, double pressure_pa)
+// solve fails (no bracket, nonfinite pressure, residual above 0.02 Pa, no convergence).  The
+// pressure residual of the returned density and the final bracket width go to *residual_pa and
+// *bracket_width when given.
+inline double water_density(double temperature_k, double pressure_pa, double* residual_pa = nullptr,
+                            double* bracket_width = nullptr)
 {
     double lo = 970.0, hi = 1060.0;
     double flo = iapws95::pressure(temperature_k, lo) - pressure_pa;
@@ -326,13 +329,15 @@ inline double water_density(double temperature_k, double pressure_pa)
             const bool take_lo = std::fabs(flo) < std::fabs(fhi);
             if (std::fabs(take_lo ? flo : fhi) > 0.02)
                 throw std::runtime_error("IAPWS-95: density pressure residual is too large.");
+            if (residual_pa) *residual_pa = take_lo ? flo : fhi;
+            if (bracket_width) *bracket_width = hi - lo;
             return take_lo ? lo : hi;
         }
     }
     throw std::runtime_error("IAPWS-95: liquid density solve did not converge.");
 }
 struct WaterState {
-    double index = 0, density = 0, temperature_k = 0, pressure_pa = 0;
+    double index = 0, density = 0, temperature_k = 0, pressure_pa = 0, residual_pa = 0, bracket_width = 0;
 };
 inline WaterState water_optics(double wavelength_nm, double temperature_c = 20.0, double pressure_pa = 101325.0)
 {
@@ -344,7 +349,7 @@ inline WaterState water_optics(double wavelength_nm, double temperature_c = 20.0
     WaterState s;
     s.temperature_k = temperature_c + 273.15;
     s.pressure_pa = pressure_pa;
-    s.density = water_density(s.temperature_k, pressure_pa);
+    s.density = water_density(s.temperature_k, pressure_pa, &s.residual_pa, &s.bracket_width);
     s.index = water_index_r9_97(wavelength_nm, s.temperature_k, s.density);
     return s;
 }

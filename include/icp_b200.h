@@ -286,8 +286,10 @@ int icp_hex_generate(icp_context* ctx, const icp_hex_record* record, const icp_o
 /* Host helpers for the drop record inputs (all binary64, CPU):
  *  icp_water_index      IAPWS R9-97 index at the drop's wavelength / temperature / pressure
  *                       (replaces evaluate_water_optics, src/water_refractive_index.cpp:157-187;
- *                       liquid density from the Tanaka / Kell correlations with the
- *                       UNESCO-1981 secant bulk modulus)
+ *                       liquid density by bisection of the IAPWS-95 pressure equation, all 56
+ *                       residual terms, in [970, 1060] kg m^-3)
+ *  icp_water_state      the same with the state, the density's pressure residual and the final
+ *                       bracket width (rainbow::WaterOptics, the fields metadata.json reports)
  *  icp_drop_shape       Table-I coefficients for an equal-volume radius
  *                       (RaindropShape::try_make, include/rainbow/raindrop_shape.hpp:22-67)
  *  icp_drop_projected_area  convex-surface projected area (compute_projected_area,
@@ -295,6 +297,12 @@ int icp_hex_generate(icp_context* ctx, const icp_hex_record* record, const icp_o
  *  icp_drop_frame       ki = (cos a, -sin a, 0) and its transverse frame (RaindropSettings,
  *                       include/rainbow/raindrop_settings.hpp:123-147) */
 int icp_water_index(double wavelength_nm, double temperature_c, double pressure_pa, double* index, double* density);
+typedef struct {
+    double temperature_kelvin, pressure_pascal, density_kg_m3;
+    double density_pressure_residual_pascal, density_bracket_width_kg_m3;
+    double refractive_index;
+} icp_water_optics;
+int icp_water_state(double wavelength_nm, double temperature_c, double pressure_pa, icp_water_optics* out);
 int icp_drop_shape(double radius_mm, int sphere, double coefficients[8], double* inner_radius, double* outer_radius);
 int icp_drop_projected_area(const double coefficients[8], double radius_mm, const double k[3], double* area_mm2);
 int icp_drop_frame(double inclination_deg, double k[3], double e0[3], double e1[3]);
@@ -830,9 +838,73 @@ int icp_patch_query(icp_context* ctx, const icp_outgoing_vertex* d_vertices, uin
 /* Optics of every query direction: d_results[direction_count] (device).  With focal != NULL
  * also the focal stage d_focal[direction_count] (device; the input of icp_rainbow_diffraction).
  * Malformed inputs are reported per direction in the result flags, as the reference does;
- * only null pointers and sizes that overflow are rejected here. */
+ * only null pointers and sizes that overflow are rejected here.  Without folded records: a hit
+ * on a NeedsRefinement patch is refinement-pending. */
 int icp_patch_optics(icp_context* ctx, const icp_optics_input* input, icp_optical_result* d_results,
                      const icp_focal_config* focal, icp_focal_sample* d_focal);
+
+/* --------------------------------------------------------------------- folded patches */
+/* A NeedsRefinement patch's direction map folds (its Jacobian changes sign inside the cell);
+ * the reference then evaluates each hit with the connected sign component ("branch") that
+ * contains it (include/rainbow/folded_patch_data.hpp, folded_patch_geometry.hpp,
+ * folded_patch_builder.hpp). */
+typedef struct {                                             /* rainbow::FoldedPatchConfig, 16 B */
+    double relative_tolerance;                               /* 1e-8 (1e-12 .. 1e-3)             */
+    uint32_t maximum_panels;                                 /* 2048 (1 .. 65536)                */
+    uint32_t maximum_depth;                                  /* 20 (1 .. 24)                     */
+} icp_folded_config;
+
+typedef struct {                                             /* rainbow::FoldedBranch, 64 B      */
+    double u0, u1;                                           /* u extent of the component        */
+    double area_fraction, solid_angle_sr;                    /* share of the cell, unsigned sr   */
+    double representative_u, representative_v;
+    int32_t sign;                                            /* sign of J on the component       */
+    uint32_t focal_flags, quarter_turns, extra_quarter_turn; /* focal estimate at the point      */
+} icp_folded_branch;
+
+typedef struct {                                             /* rainbow::FoldedPatchRecord, 320 B */
+    uint32_t compact_index, patch_id;
+    uint32_t flags;                                          /* 0 ready; FoldedPatchFlags bits   */
+    uint32_t branch_count;
+    double jacobian[4];                                      /* corners 00 10 01 11, scaled      */
+    icp_folded_branch branches[4];
+    double largest_estimated_relative_error;
+    uint32_t panels, reserved;
+} icp_folded_record;
+
+typedef struct {                                             /* rainbow::FoldedPatchView, 24 B   */
+    const uint32_t* record_indices;                          /* by compact patch index (device)  */
+    const icp_folded_record* records;                        /* device                           */
+    uint32_t patch_count, record_count;
+} icp_folded_view;
+
+typedef struct {                                             /* FoldedPatchStatistics (records)  */
+    uint32_t candidates, prepared, unresolved, branch_count, focal_pending_branches, reserved;
+    double largest_estimated_relative_error;
+} icp_folded_stats;
+
+/* The folded-patch record of every NeedsRefinement patch of d_patches[patch_count] (device,
+ * from icp_patch_build) over the lattice d_vertices[vertex_count] (device): records in
+ * compact-index order in d_records (device, capacity), d_record_indices[patch_count] (device)
+ * the record of each patch or 0xffffffff.  FoldedPatchBuilder::prepare per record (the
+ * reference's prepare_folded_patches, device/patch_optics.cu:46-60, which takes slots in
+ * completion order); with focal != NULL each ready branch also gets its focal quarter turns
+ * (FocalPhase::estimate_at).  config NULL = the reference's defaults.  *record_count (host)
+ * always; with d_records == NULL or capacity < count -> ICP_ERR_CAPACITY after the count.
+ * stats (host, may be NULL): PatchOptics::collect_folded_statistics. */
+int icp_folded_prepare(icp_context* ctx, const icp_outgoing_vertex* d_vertices, uint32_t vertex_count,
+                       const icp_outgoing_patch* d_patches, uint32_t patch_count, const float incident[3],
+                       const icp_focal_config* focal, const icp_folded_config* config, uint32_t* d_record_indices,
+                       icp_folded_record* d_records, uint32_t capacity, uint32_t* record_count,
+                       icp_folded_stats* stats);
+
+/* icp_patch_optics with folded records (folded may be NULL): the reference's
+ * evaluate_folded_optics (device/patch_optics.cu:62-68) -- a hit on a folded patch takes the
+ * area and solid angle of its branch and, for the focal stage, the branch's quarter turns; a
+ * direction whose refinement hits are not all accounted for by records stays pending or is
+ * flagged invalid (PatchOpticalEvaluator::evaluate_direction). */
+int icp_patch_optics_folded(icp_context* ctx, const icp_optics_input* input, icp_optical_result* d_results,
+                            const icp_focal_config* focal, icp_focal_sample* d_focal, const icp_folded_view* folded);
 
 /* ------------------------------------------------------- wave-stage CDF input */
 /* The density a wave stage hands to the CDF builder and the builder's input audit

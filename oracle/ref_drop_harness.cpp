@@ -5,6 +5,7 @@
 // path tracer, which pin the oracle restatement and the product's host helpers.
 //
 //   water     stdin "lambda_nm T_C p_Pa" lines -> "index density"  (evaluate_water_optics)
+//   water_state  the same -> "index density pressure_residual bracket_width"
 //   shape     stdin "radius_mm sphere" lines -> "c0..c7 inner outer" (RaindropShape::try_make)
 //   area      stdin "c0..c7 radius_mm kx ky kz" lines -> "area_mm2"  (compute_projected_area)
 //   frame     stdin "alpha_deg" lines -> float ki(3) and incident_basis_x(3) of the config the
@@ -261,6 +262,16 @@ int main(int argc, char** argv)
                     std::cout << w.refractive_index << ' ' << w.density_kg_m3 << '\n';
                 } catch (const std::exception&) {
                     std::cout << "nan nan\n";
+                }
+            } else if (mode == "water_state") {
+                double l, t, p;
+                in >> l >> t >> p;
+                try {
+                    const auto w = evaluate_water_optics(l, t, p);
+                    std::cout << w.refractive_index << ' ' << w.density_kg_m3 << ' ' << w.density_pressure_residual_pascal
+                              << ' ' << w.density_bracket_width_kg_m3 << '\n';
+                } catch (const std::exception&) {
+                    std::cout << "nan nan nan nan\n";
                 }
             } else if (mode == "shape") {
                 float r;

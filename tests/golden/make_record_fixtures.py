@@ -5,8 +5,9 @@ build:
 
     python tests/golden/make_record_fixtures.py [out_dir]
 
-The records (hex column through ice_generate_phase, water drops through rainbow_generate, at
-small grids so that they stay a few tens of KB) are the inputs of tests/test_record_reader_cpu.py,
+The records (hex column through ice_generate_phase, water drops through rainbow_generate -- the
+ray model and the reference's default patch-model diffraction stage -- at small grids so that
+they stay a few tens of KB) are the inputs of tests/test_record_reader_cpu.py,
 which checks them with the reference's own record reader where the reference checkout is present.
 """
 from __future__ import annotations
@@ -30,13 +31,18 @@ RECORDS = {
     # the benchmark drop's shape at a small grid, with the analytic diffraction stage
     "drop_oblate_1.5mm_650nm_90x180": ["rainbow_generate", "--wavelength-nm", "650", "--radius-mm", "1.5",
                                        "--shape-coefficients", "0,-0.08,-0.02,0.005", "--inclination-deg", "20",
-                                       "--query-theta", "90", "--query-phi", "180", "--rays", "200000",
+                                       "--query-theta", "90", "--query-phi", "180", "--stage", "incoherent",
+                                       "--rays", "200000",
                                        "--max-internal-hits", "10", "--max-unresolved-fraction", "1e-3",
                                        "--diffraction", "analytic"],
     # a Table-I drop, stored coarser than traced
     "drop_table1_0.5mm_550nm_72x144_36x72": ["rainbow_generate", "--wavelength-nm", "550", "--radius-mm", "0.5",
                                              "--query-theta", "72", "--query-phi", "144", "--cdf-theta", "36",
-                                             "--cdf-phi", "72", "--rays", "100000"],
+                                             "--cdf-phi", "72", "--stage", "incoherent", "--rays", "100000"],
+    # the reference's default stage: the patch model with Table-II diffraction, lattice 129 x 129
+    "drop_diffraction_0.5mm_650nm_grid129_90x180": ["rainbow_generate", "--wavelength-nm", "650", "--radius-mm",
+                                                    "0.5", "--grid", "129", "--query-theta", "90", "--query-phi",
+                                                    "180"],
 }
 
 

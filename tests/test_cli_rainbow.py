@@ -33,7 +33,10 @@ def run(args, code=0):
     (["--out", "X", "--wavelength-nm", "700", "--material", "constant", "--ior", "1.33", "--temperature-c", "5"],
      "Temperature/pressure do not define a constant-index material."),
     (["--out", "X", "--wavelength-nm", "700", "--material", "ice"], "Material must be water or constant."),
-    (["--out", "X", "--wavelength-nm", "700", "--radius-mm", "3.5"], "radius_mm must be in (0,3]"),
+    (["--out", "X", "--wavelength-nm", "700", "--radius-mm", "3.5", "--stage", "path"], "radius_mm must be in (0,3]"),
+    (["--out", "X", "--wavelength-nm", "700", "--radius-mm", "1.5"], "Table II covers radius 0.1..1.0 mm only."),
+    (["--out", "X", "--wavelength-nm", "700", "--radius-mm", "0.05", "--stage", "focal"],
+     "Table II covers radius 0.1..1.0 mm only."),
     (["--out", "X", "--wavelength-nm", "150"], "IAPWS R9-97: wavelength/state outside supported range."),
     (["--out", "X", "--wavelength-nm", "700", "--temperature-c", "70"], "Water material supports liquid branch"),
     (["--out", "X", "--wavelength-nm", "300"], "wavelength_nm must be in [380,830]"),
@@ -49,7 +52,12 @@ def run(args, code=0):
     (["--out", "X", "--wavelength-nm", "700", "--diffraction-sigma-deg", "1"], "Manual diffraction width is not supported"),
     (["--out", "X", "--wavelength-nm", "700", "--focal-offsets", "0,1,2"], "Expected four focal offsets."),
     (["--out", "X", "--wavelength-nm", "700", "--focal-offsets", "0,1,2,4"], "Focal offsets must be 0..3."),
-    (["--out", "X", "--wavelength-nm", "700", "--stage", "focal"], "Stage focal is the reference's wave-optics patch"),
+    (["--out", "X", "--wavelength-nm", "700", "--rays", "1000"], "apply to the ray model (--stage incoherent --optics rays)"),
+    (["--out", "X", "--wavelength-nm", "700", "--stage", "path", "--optics", "rays"],
+     "--optics rays applies to --stage incoherent only"),
+    (["--out", "X", "--wavelength-nm", "700", "--stage", "incoherent", "--optics", "lattice", "--seed", "3"],
+     "apply to the ray model"),
+    (["--out", "X", "--wavelength-nm", "700", "--optics", "mesh"], "--optics must be lattice or rays."),
     (["--out", "X", "--wavelength-nm", "700", "--stage", "bogus"], "Unknown stage."),
     (["--out", "X", "--wavelength-nm", "700", "--device", "-1"], "Invalid device ordinal."),
     (["--out", "X", "--wavelength-nm", "700", "--bogus", "1"], "Unknown option: --bogus"),
@@ -77,7 +85,7 @@ def test_help_and_existing_outputs(tmp_path):
 def test_record_contract(tmp_path, icp):
     out = tmp_path / "drop"
     r = run(["--out", out, "--wavelength-nm", "700", "--radius-mm", "1.5", "--query-theta", "180", "--query-phi",
-             "360", "--cdf-theta", "90", "--cdf-phi", "180", "--rays", "2000000"])
+             "360", "--cdf-theta", "90", "--cdf-phi", "180", "--stage", "incoherent", "--rays", "2000000"])
     assert "Saved NumPy CDF dataset" in r.stdout
     assert {p.name for p in out.iterdir()} == {"metadata.json", "phi_cdf.npy", "theta_given_phi_cdf.npy", "u_edges.npy"}
     rec = validate_record(out)
@@ -108,7 +116,7 @@ def test_record_contract(tmp_path, icp):
     assert 134 < theta_deg[back][np.argmax(rows[back])] < 142
     # a published record is not overwritten
     digest = {f.name: hashlib.sha256(f.read_bytes()).hexdigest() for f in out.iterdir()}
-    assert "Output already exists." in run(["--out", out, "--wavelength-nm", "700"], 1).stderr
+    assert "Output already exists." in run(["--out", out, "--wavelength-nm", "700", "--stage", "incoherent"], 1).stderr
     assert digest == {f.name: hashlib.sha256(f.read_bytes()).hexdigest() for f in out.iterdir()}
 
 
@@ -117,7 +125,8 @@ def test_fp64_record_matches_oracle(tmp_path, icp, oracle):
     """Four reference families only (3 internal hits): the FP64 record equals the oracle's CDF."""
     out = tmp_path / "fp64"
     run(["--out", out, "--wavelength-nm", "650", "--radius-mm", "1.0", "--inclination-deg", "35", "--query-theta", "72",
-         "--query-phi", "144", "--cdf-theta", "36", "--cdf-phi", "72", "--rays", "30000", "--seed", "5",
+         "--query-phi", "144", "--cdf-theta", "36", "--cdf-phi", "72", "--stage", "incoherent", "--rays", "30000",
+         "--seed", "5",
          "--trace-precision", "fp64", "--max-internal-hits", "3", "--max-unresolved-fraction", "0.5"])
     rec = validate_record(out)
     m = rec["metadata"]
@@ -134,7 +143,8 @@ def test_fp64_record_matches_oracle(tmp_path, icp, oracle):
 def test_extensions(tmp_path):
     out = tmp_path / "baseline_shape"
     run(["--out", out, "--wavelength-nm", "550", "--radius-mm", "0.5", "--shape-coefficients", "0,-0.08,-0.02,0.005",
-         "--diffraction", "analytic", "--query-theta", "90", "--query-phi", "180", "--rays", "200000"])
+         "--stage", "incoherent", "--diffraction", "analytic", "--query-theta", "90", "--query-phi", "180", "--rays",
+         "200000"])
     m = validate_record(out)["metadata"]
     assert m["shape_coefficients"] == [0, -0.08, -0.02, 0.005, 0, 0, 0, 0]
     assert m["shape_source"] == "command_line"
@@ -142,7 +152,58 @@ def test_extensions(tmp_path):
     assert d["computed"] is True and abs(d["power_mm2"] / m["transport_audit"]["incident_mm2"] - 1) < 1e-12
     sphere = tmp_path / "sphere"
     run(["--out", sphere, "--wavelength-nm", "550", "--radius-mm", "2.0", "--sphere", "--query-theta", "90",
-         "--query-phi", "180", "--rays", "100000", "--material", "constant", "--ior", "1.333"])
+         "--query-phi", "180", "--stage", "incoherent", "--rays", "100000", "--material", "constant", "--ior", "1.333"])
     m = validate_record(sphere)["metadata"]
     assert m["sampling"]["missed_rays"] == 0 and m["geometry"]["projected_area_method"] == "analytic_sphere"
     assert m["material"]["model"] == "constant"
+
+
+# ------------------------------------------------------------ the lattice (patch) model stages
+def _stage(tmp_path, stage, extra=()):
+    out = tmp_path / stage
+    r = run(["--out", out, "--wavelength-nm", "650", "--radius-mm", "0.5", "--grid", "129", "--query-theta", "180",
+             "--query-phi", "360", "--cdf-theta", "90", "--cdf-phi", "180", "--stage", stage, *extra])
+    assert "Saved NumPy CDF dataset" in r.stdout
+    return validate_record(out)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("stage", ["diffraction", "focal", "path"])
+def test_lattice_stage_records(tmp_path, icp, stage):
+    """rainbow_generate --stage path | focal | diffraction: the reference's patch model on the
+    device -- lattice trace, patches, query, folded records, optics, Table II, stored CDF --
+    written in the record contract the reference's reader accepts."""
+    rec = _stage(tmp_path, stage)
+    m, mass, u = rec["metadata"], rec["cell_probability"], rec["u"]
+    assert m["stage"] == stage and m["incident_grid"] == [129, 129]
+    assert abs(mass.sum() - 1) < 1e-12
+    assert m["diffraction_policy"]["computed"] is (stage != "path")
+    assert m["diffraction_policy"]["selected_output_includes_diffraction"] is (stage == "diffraction")
+    assert m["quality"]["incomplete_directions"] == 0 and m["quality"]["invalid_values"] == 0
+    assert m["patches"]["pending_directions"] == 0 and m["patches"]["error_directions"] == 0
+    assert m["patches"]["folded_candidates"] == m["patches"]["folded_prepared"] > 0
+    assert m["patches"]["folded_evaluated_hits"] > 0
+    assert m["material"]["density_model"] == "IAPWS R6-95(2018) liquid pressure EOS inversion"
+    cfg = icp.raindrop_config(0.5, 650.0, m["interior_index"], (np.cos(np.radians(20.0)), -np.sin(np.radians(20.0)), 0.0),
+                              129)
+    assert m["incident_grid_half_extent"] == float(np.float32(cfg.grid_half_extent))
+    # the primary bow near 138 degrees
+    rows = mass.sum(axis=0)
+    theta_deg = np.degrees(np.arccos(1 - (u[:-1] + u[1:])))
+    back = (theta_deg > 120) & (theta_deg < 160)
+    assert 134 < theta_deg[back][np.argmax(rows[back])] < 144
+
+
+@pytest.mark.gpu
+def test_lattice_incoherent_matches_ray_model(tmp_path):
+    """--stage incoherent with the reference's patch model and with the ray model describe the same
+    geometric optics: over the families both carry (R .. TRRT dominate the mass), their stored
+    phase functions agree in g to 1e-2 and in total variation to 0.15."""
+    lat = _stage(tmp_path, "incoherent", ["--optics", "lattice"])
+    out = tmp_path / "rays"
+    run(["--out", out, "--wavelength-nm", "650", "--radius-mm", "0.5", "--query-theta", "180", "--query-phi", "360",
+         "--cdf-theta", "90", "--cdf-phi", "180", "--stage", "incoherent", "--rays", "4000000",
+         "--max-internal-hits", "3", "--max-unresolved-fraction", "0.2"])
+    ray = validate_record(out)
+    assert abs(lat["metadata"]["hg"]["g"] - ray["metadata"]["hg"]["g"]) < 1e-2
+    assert 0.5 * np.abs(lat["cell_probability"] - ray["cell_probability"]).sum() < 0.15

@@ -73,10 +73,12 @@ def test_water_index_matches_reference_on_random_states(icp):
     rng = np.random.default_rng(20261204)
     ins = [(float(lam), float(t), float(p)) for lam, t, p in
            zip(rng.uniform(200, 1100, 300), rng.uniform(0, 60, 300), np.exp(rng.uniform(np.log(5e4), np.log(1e8), 300)))]
-    ref = oracle_mod.ref_drop_lines("water", [f"{lam!r} {t!r} {p!r}" for lam, t, p in ins])
-    for (lam, t, p), (n_ref, rho_ref) in zip(ins, ref):
+    ref = oracle_mod.ref_drop_lines("water_state", [f"{lam!r} {t!r} {p!r}" for lam, t, p in ins])
+    for (lam, t, p), (n_ref, rho_ref, res_ref, width_ref) in zip(ins, ref):
         w = icp.evaluate_water_optics(lam, t, p)
         assert (w.refractive_index, w.density_kg_m3) == (n_ref, rho_ref), (lam, t, p)
+        # the residual and bracket width metadata.json reports (rainbow::WaterOptics)
+        assert (w.density_pressure_residual_pascal, w.density_bracket_width_kg_m3) == (res_ref, width_ref), (lam, t, p)
 
 
 def test_projected_area_matches_reference(icp):
