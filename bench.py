@@ -46,6 +46,12 @@ from pathlib import Path
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of the drop record's two
+# kernels, from single-pass ncu captures of this workload: the 1e8-ray trace launch
+# (profiles/drop_trace_bin_kernel_dram_oblate_1e8.md) and the 900 x 1800 CDF launch
+# (profiles/cdf_build_kernel_900x1800.md)
+DROP_TRACE_TRAFFIC = 15.01e6 + 114.71e6
+DROP_CDF_TRAFFIC = 13.0885e6 + 0.0
 CFG = dict(R=0.05, L=0.2, ki=(0.8660254037844387, -0.5, 0.0), n=1.31, nt=512, np=1024, hits=12, seed=12345)
 DROP = dict(radius=1.5, coefficients=(0.0, -0.08, -0.02, 0.005, 0.0, 0.0, 0.0, 0.0), wavelength=650.0, incl=20.0,
             nt=900, np=1800, hits=10, seed=12345)
@@ -787,58 +793,89 @@ def run_rainbow(I, ctx, stream, a) -> dict:
 
 
 def run_wave(I, ctx, stream, a) -> dict:
-    """The device chain of the drop's wave stages at the reference CLI's defaults (513 x 513
-    lattice of four families, 360 x 720 query grid): patch build, all-hit query (sizing and fill
-    passes), patch optics with the focal stage, Table-II diffraction, on a seeded synthetic
-    lattice with a folding family; each stage timed with CUDA events on the context's stream."""
+    """One wave-stage record of a real drop at the reference CLI's defaults (1.0 mm Table-I drop,
+    650 nm water, inclination 20 deg, 513 x 513 lattice, 360 x 720 query grid, diffraction
+    stage): lattice trace, patch build, all-hit query (sizing and fill passes), folded-patch
+    records, patch optics with the focal stage, Table-II diffraction, stage density and the stored
+    CDF, every stage timed with CUDA events on the context's stream."""
     import ctypes as C
 
     import numpy as np
     import torch
 
-    sys.path.insert(0, str(ROOT / "tests"))
-    import optics_cases as OC
-
     w = h = 513
     nt, np_ = 360, 720
-    v, second, (_, _, e) = OC.bench_lattice(w, h)
-    k, e0 = np.float32(OC._K20), np.float32((0, 0, 1))
+    n_int = float(np.float32(I.evaluate_water_optics(650.0).refractive_index))
+    alpha = math.radians(20.0)
+    cfg = I.raindrop_config(1.0, 650.0, n_int, (math.cos(alpha), -math.sin(alpha), 0.0), w)
+    e = cfg.grid_half_extent
+    k = np.array([cfg.incident_direction.x, cfg.incident_direction.y, cfg.incident_direction.z], np.float32)
+    e0 = np.array([cfg.incident_basis_x.x, cfg.incident_basis_x.y, cfg.incident_basis_x.z], np.float32)
     dirs = I.query_directions(nt, np_, k, e0)
-    n, cells = nt * np_, 4 * (w - 1) * (h - 1)
-    dv = I.DeviceArray(ctx, len(v), I.VERTEX_DTYPE).upload(v)
-    d2 = I.DeviceArray(ctx, 4 * len(second), np.float32).upload(second.reshape(-1))
+    nv, n, cells = 4 * w * h, nt * np_, 4 * (w - 1) * (h - 1)
+    dv, d2 = I.DeviceArray(ctx, nv, I.VERTEX_DTYPE), I.DeviceArray(ctx, 4 * nv, np.float32)
     dp, db = I.DeviceArray(ctx, cells, I.PATCH_DTYPE), I.DeviceArray(ctx, cells, I.AABB_DTYPE)
     dd = I.DeviceArray(ctx, 3 * n, np.float32).upload(dirs.reshape(-1))
     do, ds = I.DeviceArray(ctx, n + 1, np.uint64), I.DeviceArray(ctx, n, I.SUMMARY_DTYPE)
     dr, df = I.DeviceArray(ctx, n, I.OPTICAL_DTYPE), I.DeviceArray(ctx, n, I.FOCAL_DTYPE)
     dt, dres, dden = I.DeviceArray(ctx, n, np.uint32), I.DeviceArray(ctx, n, I.DIFFRACTION_DTYPE), I.DeviceArray(ctx, n)
-    npatch, hits = C.c_uint32(0), C.c_uint64(0)
+    dphi, dth = I.DeviceArray(ctx, np_ + 1), I.DeviceArray(ctx, np_ * (nt + 1))
+    di = I.DeviceArray(ctx, cells, np.uint32)
+    npatch, hits, nrec = C.c_uint32(0), C.c_uint64(0), C.c_uint32(0)
     hist = (C.c_uint64 * 8)()
-    cfg = I.diffraction_config(0.5)
+    dcfg = I.diffraction_config(1.0)
     fc = I.FocalConfig(w, h, e, 0, (C.c_uint32 * 4)(0, 0, 0, 0))
-    stats = I.DiffractionStats()
+    lstats, fstats, dstats = I.LatticeStats(), I.FoldedStats(), I.DiffractionStats()
+    drep, crep = I.DensityReport(), I.CdfReport()
+    pol = I.CdfPolicy(1e-10, 1e-12, 1.0)
+    kin = (C.c_float * 3)(*map(float, k))
     state = {}
+
+    def trace():
+        I.check(I.LIB.icp_lattice_trace(ctx.handle, C.byref(cfg), dv.ptr, d2.ptr, C.byref(lstats)))
 
     def build():
         I.check(I.LIB.icp_patch_build(ctx.handle, dv.ptr, w, h, e, dp.ptr, db.ptr, None, C.byref(npatch), hist))
 
     def query():
-        args = (ctx.handle, dv.ptr, len(v), dp.ptr, db.ptr, npatch.value, dd.ptr, n, do.ptr)
-        I.check(I.LIB.icp_patch_query(*args, None, None, 0, C.byref(hits)))
-        if "dh" not in state or state["dh"].count < hits.value:
-            state["dh"] = I.DeviceArray(ctx, max(1, hits.value), I.HIT_DTYPE)
-        I.check(I.LIB.icp_patch_query(*args, ds.ptr, state["dh"].ptr, state["dh"].count, C.byref(hits)))
+        # one call counts and fills when the hits fit (four per direction to start with)
+        args = (ctx.handle, dv.ptr, nv, dp.ptr, db.ptr, npatch.value, dd.ptr, n, do.ptr)
+        if "dh" not in state:
+            state["dh"] = I.DeviceArray(ctx, 4 * n, I.HIT_DTYPE)
+        st = I.LIB.icp_patch_query(*args, ds.ptr, state["dh"].ptr, state["dh"].count, C.byref(hits))
+        if st == I.ICP_ERR_CAPACITY:
+            state["dh"] = I.DeviceArray(ctx, hits.value, I.HIT_DTYPE)
+            st = I.LIB.icp_patch_query(*args, ds.ptr, state["dh"].ptr, state["dh"].count, C.byref(hits))
+        I.check(st)
+
+    def folded():
+        args = (ctx.handle, dv.ptr, nv, dp.ptr, npatch.value, kin, C.byref(fc), None, di.ptr)
+        if "dfr" not in state:
+            I.LIB.icp_folded_prepare(*args, None, 0, C.byref(nrec), C.byref(fstats))
+            state["dfr"] = I.DeviceArray(ctx, max(1, nrec.value), I.FOLDED_DTYPE)
+        I.check(I.LIB.icp_folded_prepare(*args, state["dfr"].ptr, state["dfr"].count, C.byref(nrec), C.byref(fstats)))
 
     def optics():
-        inp = I.OpticsInput(dv.ptr, dp.ptr, dd.ptr, do.ptr, ds.ptr, state["dh"].ptr, d2.ptr, hits.value, len(v),
-                            npatch.value, n, len(second), I.Vec3f(*map(float, k)), I.Vec3f(*map(float, e0)), 1, 0)
-        I.check(I.LIB.icp_patch_optics(ctx.handle, C.byref(inp), dr.ptr, C.byref(fc), df.ptr))
+        inp = I.OpticsInput(dv.ptr, dp.ptr, dd.ptr, do.ptr, ds.ptr, state["dh"].ptr, d2.ptr, hits.value, nv,
+                            npatch.value, n, nv, I.Vec3f(*map(float, k)), I.Vec3f(*map(float, e0)), 1, 0)
+        view = I.FoldedView(di.ptr, state["dfr"].ptr, npatch.value, nrec.value)
+        I.check(I.LIB.icp_patch_optics_folded(ctx.handle, C.byref(inp), dr.ptr, C.byref(fc), df.ptr,
+                                              C.byref(view) if nrec.value else None))
 
     def diffraction():
-        I.check(I.LIB.icp_rainbow_diffraction(ctx.handle, df.ptr, nt, np_, C.byref(cfg), dt.ptr, dres.ptr, dden.ptr,
-                                              C.byref(stats)))
+        I.check(I.LIB.icp_rainbow_diffraction(ctx.handle, df.ptr, nt, np_, C.byref(dcfg), dt.ptr, dres.ptr, None,
+                                              C.byref(dstats)))
 
-    stages = {"patch_build": build, "patch_query": query, "patch_optics": optics, "rainbow_diffraction": diffraction}
+    def density():
+        I.check(I.LIB.icp_stage_density(ctx.handle, I.WAVE_STAGES["diffraction"], dr.ptr, df.ptr, dres.ptr, n,
+                                        dden.ptr, C.byref(drep)))
+
+    def cdf():
+        I.check(I.LIB.icp_phase_cdf_build(ctx.handle, dden.ptr, 1, nt, np_, 0.0, 0.0, nt, np_, C.byref(pol), dphi.ptr,
+                                          dth.ptr, C.byref(crep)))
+
+    stages = {"lattice_trace": trace, "patch_build": build, "patch_query": query, "folded_prepare": folded,
+              "patch_optics": optics, "rainbow_diffraction": diffraction, "stage_density": density, "cdf_build": cdf}
     for _ in range(3):
         for f in stages.values():
             f()
@@ -853,13 +890,52 @@ def run_wave(I, ctx, stream, a) -> dict:
             torch.cuda.synchronize()
             times.append(e0v.elapsed_time(e1v))
         ms[name] = sorted(times)[len(times) // 2]
-    summaries = ds.download()
     total = sum(ms.values())
-    return {"workload": "drop_wave_stages_lattice_513x513_query_360x720_synthetic", "lattice": [w, h],
-            "query": [nt, np_], "patches": npatch.value, "patch_status_histogram": list(hist), "hits": hits.value,
-            "incomplete_directions": int(((summaries["flags"] & (8 | 16 | 128 | 1 | 2 | 4 | 256)) != 0).sum()),
-            "ms_per_stage": ms, "ms_per_chain": total, "directions_per_s": n / (total / 1e3),
-            "filtered_directions": stats.filtered_directions}
+    # the reference's CDF input gate; the 1.0 mm drop's Table-II width (0.15 deg) is below twice the
+    # 0.5 deg cell, so its bow directions are underresolved and the record is the one written
+    # with --allow-underresolved
+    gate = drep.invalid_values == 0 and drep.incomplete == 0 and drep.maximum > 0
+    out = {"workload": "drop_diffraction_record_1.0mm_650nm_lattice_513x513_query_360x720", "lattice": [w, h],
+           "query": [nt, np_], "patches": npatch.value, "patch_status_histogram": list(hist), "hits": hits.value,
+           "folded_records": nrec.value, "folded": fstats.as_dict(), "trace_incomplete": lstats.incomplete,
+           "density_gate_passed_allowing_underresolved": bool(gate), "incomplete_directions": drep.incomplete,
+           "underresolved_directions": drep.underresolved,
+           "cdf_g": crep.g_stored, "cdf_l1": crep.l1_error,
+           "ms_per_stage": ms, "ms_per_record": total, "records_per_s": 1e3 / total,
+           "filtered_directions": dstats.filtered_directions}
+    # the reference's own CPU lattice trace (RaindropPathTracer, its only CPU stage of this chain)
+    # on a few rows of the same lattice, one process per core, beside the device trace
+    if not a.no_cpu_baseline and (ROOT / "oracle" / "_ref" / "ref_drop_harness").exists():
+        try:
+            out["cpu_baseline_lattice_trace"] = reference_lattice_rows(w, n_int)
+            out["cpu_baseline_lattice_trace"]["device_vertices_per_s"] = w * h / (ms["lattice_trace"] / 1e3)
+        except (OSError, ValueError, subprocess.SubprocessError) as ex:
+            out["cpu_baseline_lattice_trace"] = {"unavailable": f"{type(ex).__name__}: {ex}"}
+    return out
+
+
+def reference_lattice_rows(grid: int, n_int: float, rows_per_proc: int = 2) -> dict:
+    """The reference's CPU lattice trace (oracle/_ref/ref_drop_harness time: RaindropPathTracer::
+    trace_vertex_unpolarized with its RaindropIntersector) of `rows_per_proc` rows per process from
+    the middle of the same 1.0 mm drop's lattice, one process per core: vertices per second."""
+    import numpy as np
+
+    procs = os.cpu_count() or 1
+    alpha = math.radians(20.0)
+    k = (repr(float(np.float32(math.cos(alpha)))), repr(float(np.float32(-math.sin(alpha)))), "0")
+    base = grid // 2 - (procs * rows_per_proc) // 2
+    cmds = [[str(ROOT / "oracle" / "_ref" / "ref_drop_harness"), "time", "1.0", "0", repr(n_int), *k, str(grid),
+             str(max(0, base + p * rows_per_proc)), str(rows_per_proc)] for p in range(procs)]
+    t0 = time.perf_counter()
+    ps = [subprocess.Popen(c, stdout=subprocess.PIPE, text=True) for c in cmds]
+    outs = [p.communicate()[0].split() for p in ps]
+    wall = time.perf_counter() - t0
+    verts = sum(int(o[0]) for o in outs)
+    per_proc = [int(o[0]) / float(o[2]) for o in outs]
+    return {"value": verts / wall, "unit": "lattice vertices/s", "cores": procs, "kind": "reference",
+            "one_core": sum(per_proc) / len(per_proc),
+            "sample": f"{verts} vertices ({rows_per_proc} lattice rows per process, {procs} processes) of the "
+                      "513 x 513 lattice through the reference's RaindropPathTracer compiled from its sources"}
 
 
 def _cpu_leg(kind: str, payload: dict) -> dict:
@@ -1186,13 +1262,19 @@ def run_b200_drop(a) -> None:
         "records_per_s": 1.0 / t_step,
         "e2e": {"value": e2e_value, "unit": "rays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": {"kernel": "trace_bin_kernel<float, DropGeo<float>>", "bound": "fp32_simt", "achieved": achieved,
-                     "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+                     "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                     "traffic": DROP_TRACE_TRAFFIC if rays == 1e8 else None,
+                     "traffic_note": "DRAM bytes of one 1e8-ray launch (ncu, one pass): 15.0 MB read, 114.7 MB "
+                                     "written, against 13.0 MB algorithmic (the FP64 histogram)",
                      "peak_note": f"derived: {sms} SMs x 128 FP32 lanes x 2 x {mhz:.0f} MHz (median SM clock under load)",
                      "flops_per_ray": flops / max(1, ks.rays), "kernel_ms": 1e3 * t_kernel,
                      "interactions_per_hit": ks.encounters / max(1, hits),
                      "gauge_evaluations_per_hit": ks.gauge_evals / max(1, hits)},
         "roofline_cdf": ({"kernel": "cdf_build_kernel", "bound": "hbm", "achieved": cdf_bytes / statistics.mean(cdf_t) / 1e9,
-                          "peak": hbm, "unit": "GB/s", "frac": cdf_bytes / statistics.mean(cdf_t) / 1e9 / hbm, "traffic": None,
+                          "peak": hbm, "unit": "GB/s", "frac": cdf_bytes / statistics.mean(cdf_t) / 1e9 / hbm,
+                          "traffic": DROP_CDF_TRAFFIC if (nt, np_) == (900, 1800) else None,
+                          "traffic_note": "DRAM bytes of one launch (ncu): the 13.1 MB histogram read; the "
+                                          "13 MB of a / T output stay in L2 during the launch",
                           "algorithmic_bytes": cdf_bytes, "kernel_us": 1e6 * statistics.mean(cdf_t), "kernel_us_min": 1e6 * min(cdf_t),
                           "peak_note": "MEASURED_PEAKS.json hbm_gbs (of measured)"} if cdf_t else None),
         "cpu_baseline": cpu,
@@ -1245,7 +1327,8 @@ def main() -> None:
     p.add_argument("--rainbow-steps", type=int, default=5,
                    help="timed passes of the Table-II rainbow diffraction measurement (0 = skip)")
     p.add_argument("--wave-steps", type=int, default=5,
-                   help="timed passes of each wave-stage kernel chain (patch build, query, optics, diffraction; 0 = skip)")
+                   help="timed passes of each stage of a wave-stage (diffraction) record: lattice trace, patch build, "
+                        "query, folded records, optics, Table-II diffraction, density, CDF (0 = skip)")
     p.add_argument("--rays", type=float, default=1e8)
     p.add_argument("--ref-rays", type=float, default=3.2e5,
                    help="reference rays per step (all processes; the hex workload traces five times more)")

@@ -37,6 +37,7 @@
 #include <iostream>
 #include <limits>
 #include <locale>
+#include <memory>
 #include <sstream>
 #include <stdexcept>
 #include <string>
@@ -568,16 +569,24 @@ void lattice_record(const Command& c, LatticeRecord& R, std::vector<double>& phi
         check(icp_query_directions(c.theta, c.phi, axis, e0, dirs.data()));
         DeviceBuffer dd(ctx.ctx, sizeof(float) * dirs.size());
         check(icp_memcpy_h2d(ctx.ctx, dd.ptr, dirs.data(), sizeof(float) * dirs.size()));
-        // 4. all-hit query: sized, then filled
+        // 4. all-hit query: counted and filled in one call when the hits fit a first guess of
+        //    four per direction, else sized by that call and filled by a second
         DeviceBuffer doff(ctx.ctx, sizeof(uint64_t) * (n + 1)), dsum(ctx.ctx, sizeof(icp_query_summary) * n);
         const auto* vtx = dv.as<const icp_outgoing_vertex>();
-        check(icp_patch_query(ctx.ctx, vtx, uint32_t(vertices), dp.as<icp_outgoing_patch>(), db.as<icp_patch_aabb>(),
-                              R.patch_count, dd.as<icp_vec3f>(), uint32_t(n), doff.as<uint64_t>(), nullptr, nullptr, 0,
-                              &R.hits));
-        DeviceBuffer dh(ctx.ctx, sizeof(icp_query_hit) * (R.hits ? R.hits : 1));
-        check(icp_patch_query(ctx.ctx, vtx, uint32_t(vertices), dp.as<icp_outgoing_patch>(), db.as<icp_patch_aabb>(),
-                              R.patch_count, dd.as<icp_vec3f>(), uint32_t(n), doff.as<uint64_t>(),
-                              dsum.as<icp_query_summary>(), dh.as<icp_query_hit>(), R.hits ? R.hits : 1, &R.hits));
+        uint64_t capacity = 4 * n;
+        auto dh = std::make_unique<DeviceBuffer>(ctx.ctx, sizeof(icp_query_hit) * capacity);
+        int qs = icp_patch_query(ctx.ctx, vtx, uint32_t(vertices), dp.as<icp_outgoing_patch>(), db.as<icp_patch_aabb>(),
+                                 R.patch_count, dd.as<icp_vec3f>(), uint32_t(n), doff.as<uint64_t>(),
+                                 dsum.as<icp_query_summary>(), dh->as<icp_query_hit>(), capacity, &R.hits);
+        if (qs == ICP_ERR_CAPACITY) {
+            capacity = R.hits;
+            dh.reset();
+            dh = std::make_unique<DeviceBuffer>(ctx.ctx, sizeof(icp_query_hit) * capacity);
+            qs = icp_patch_query(ctx.ctx, vtx, uint32_t(vertices), dp.as<icp_outgoing_patch>(), db.as<icp_patch_aabb>(),
+                                 R.patch_count, dd.as<icp_vec3f>(), uint32_t(n), doff.as<uint64_t>(),
+                                 dsum.as<icp_query_summary>(), dh->as<icp_query_hit>(), capacity, &R.hits);
+        }
+        check(qs);
         {
             std::vector<icp_query_summary> sums(n);
             check(icp_memcpy_d2h(ctx.ctx, sums.data(), dsum.ptr, sizeof(icp_query_summary) * n));
@@ -609,7 +618,7 @@ void lattice_record(const Command& c, LatticeRecord& R, std::vector<double>& phi
         in.directions = dd.as<icp_vec3f>();
         in.offsets = doff.as<uint64_t>();
         in.summaries = dsum.as<icp_query_summary>();
-        in.hits = dh.as<icp_query_hit>();
+        in.hits = dh->as<icp_query_hit>();
         in.second_input_fields = d2.as<icp_field32>();
         in.hit_storage_count = R.hits;
         in.vertex_count = uint32_t(vertices);

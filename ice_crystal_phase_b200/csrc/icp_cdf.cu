@@ -108,7 +108,64 @@ constexpr unsigned kWarps = kThreads / 32;
 constexpr unsigned kMaxBoxes = 16;
 constexpr unsigned kSpinLimit = 1u << 22;
 constexpr unsigned kFull = 0xffffffffu;
-constexpr uint32_t kChain = 8; // loads in flight ahead of an ordered chain of additions
+
+// Ordered binary64 chains.  The sums must be the reference's sequential ones, so each addition
+// waits for the previous; the loads of the next eight operands are issued before the current
+// eight are added (plain registers, no arrays), so the chain runs at the latency of the
+// additions alone.  x[k * stride], k < n.
+__device__ __forceinline__ double chain_sum(const double* __restrict__ x, uint32_t n, uint32_t stride, double a)
+{
+    uint32_t i = 0;
+    if (n >= 8) {
+        double c0 = x[0], c1 = x[stride], c2 = x[2 * stride], c3 = x[3 * stride], c4 = x[4 * stride],
+               c5 = x[5 * stride], c6 = x[6 * stride], c7 = x[7 * stride];
+        for (i = 8; i + 8 <= n; i += 8) {
+            const double* y = x + (size_t)i * stride;
+            const double d0 = y[0], d1 = y[stride], d2 = y[2 * stride], d3 = y[3 * stride], d4 = y[4 * stride],
+                         d5 = y[5 * stride], d6 = y[6 * stride], d7 = y[7 * stride];
+            a += c0; a += c1; a += c2; a += c3; a += c4; a += c5; a += c6; a += c7;
+            c0 = d0; c1 = d1; c2 = d2; c3 = d3; c4 = d4; c5 = d5; c6 = d6; c7 = d7;
+        }
+        a += c0; a += c1; a += c2; a += c3; a += c4; a += c5; a += c6; a += c7;
+    }
+    for (; i < n; ++i) a += x[(size_t)i * stride];
+    return a;
+}
+// The same chain from zero, each prefix written over its operand: x[k] = x[0] + ... + x[k].  The
+// eight prefixes of a group are stored after the group's additions, so no store sits between
+// two dependent additions.
+__device__ __forceinline__ double chain_prefix(double* x, uint32_t n, uint32_t stride)
+{
+    double a = 0.0;
+    uint32_t i = 0;
+    if (n >= 8) {
+        double c0 = x[0], c1 = x[stride], c2 = x[2 * stride], c3 = x[3 * stride], c4 = x[4 * stride],
+               c5 = x[5 * stride], c6 = x[6 * stride], c7 = x[7 * stride];
+        for (i = 8; i + 8 <= n; i += 8) {
+            double* y = x + (size_t)i * stride;
+            const double d0 = y[0], d1 = y[stride], d2 = y[2 * stride], d3 = y[3 * stride], d4 = y[4 * stride],
+                         d5 = y[5 * stride], d6 = y[6 * stride], d7 = y[7 * stride];
+            const double p0 = a + c0, p1 = p0 + c1, p2 = p1 + c2, p3 = p2 + c3, p4 = p3 + c4, p5 = p4 + c5,
+                         p6 = p5 + c6, p7 = p6 + c7;
+            double* z = y - (size_t)8 * stride;
+            z[0] = p0; z[stride] = p1; z[2 * stride] = p2; z[3 * stride] = p3;
+            z[4 * stride] = p4; z[5 * stride] = p5; z[6 * stride] = p6; z[7 * stride] = p7;
+            a = p7;
+            c0 = d0; c1 = d1; c2 = d2; c3 = d3; c4 = d4; c5 = d5; c6 = d6; c7 = d7;
+        }
+        const double p0 = a + c0, p1 = p0 + c1, p2 = p1 + c2, p3 = p2 + c3, p4 = p3 + c4, p5 = p4 + c5,
+                     p6 = p5 + c6, p7 = p6 + c7;
+        double* z = x + (size_t)(i - 8) * stride;
+        z[0] = p0; z[stride] = p1; z[2 * stride] = p2; z[3 * stride] = p3;
+        z[4 * stride] = p4; z[5 * stride] = p5; z[6 * stride] = p6; z[7 * stride] = p7;
+        a = p7;
+    }
+    for (; i < n; ++i) {
+        a += x[(size_t)i * stride];
+        x[(size_t)i * stride] = a;
+    }
+    return a;
+}
 
 // Shared-memory layout of one block (the same function sizes the launch on the host).
 struct Layout {
@@ -125,7 +182,9 @@ __host__ __device__ inline Layout layout_of(uint32_t ct, uint32_t cp, uint32_t c
     Layout L{};
     size_t off = 0;
     L.a = take(off, sizeof(double) * (size_t)rows_alloc * cw);
-    L.b = keep ? take(off, sizeof(double) * (size_t)ct * cw) : L.a;
+    // with `keep`, B is column-major with an odd column stride (the chains read a column
+    // contiguously, the parallel passes hit distinct banks); otherwise it aliases A, row-major
+    L.b = keep ? take(off, sizeof(double) * (size_t)(ct | 1u) * cw) : L.a;
     L.e = take(off, sizeof(double) * (ct + 1));
     L.s = take(off, sizeof(double) * cp);
     L.phi = take(off, sizeof(double) * (cw + 1));
@@ -256,7 +315,7 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
         : "memory");
 }
 
-__global__ void __launch_bounds__(kThreads, 2) cdf_build_kernel(const __grid_constant__ CUtensorMap map,
+__global__ void __launch_bounds__(kThreads, 1) cdf_build_kernel(const __grid_constant__ CUtensorMap map,
                                                                  const CdfParams P0)
 {
     extern __shared__ unsigned char smem_raw[];
@@ -296,6 +355,8 @@ __global__ void __launch_bounds__(kThreads, 2) cdf_build_kernel(const __grid_con
     const Layout Lo = layout_of(ct, P.cp, CW, P.rows_alloc, P.keep);
     double* A = reinterpret_cast<double*>(smem + Lo.a); // coarse masses, then p = coarse / stored total
     double* B = reinterpret_cast<double*>(smem + Lo.b); // weights, prefixes, normalised conditionals
+    // element (row i, column cl) of B at i * b_row + cl * b_col
+    const uint32_t b_row = P.keep ? 1u : CW, b_col = P.keep ? (ct | 1u) : 1u;
     double* E = reinterpret_cast<double*>(smem + Lo.e); // coarse u edges
     double* S = reinterpret_cast<double*>(smem + Lo.s); // all column sums
     double* sphi = reinterpret_cast<double*>(smem + Lo.phi);
@@ -409,47 +470,29 @@ __global__ void __launch_bounds__(kThreads, 2) cdf_build_kernel(const __grid_con
         __syncthreads();
     }
     // weights w = coarse / largest for the whole strip in parallel (the ordered chains below then
-    // carry only additions); with `keep`, the audit's p = coarse / stored total in the same pass
+    // carry only additions)
     unsigned long long underflow = 0ull, malformed = 0ull;
     if (act)
         for (uint32_t i = my_r; i < ct; i += rstep) {
-            const size_t k = (size_t)i * CW + my_cl;
-            const double c = A[k];
+            const double c = A[(size_t)i * CW + my_cl];
             const double x = c / big;
             if (c > 0 && !(x > 0)) ++underflow;
-            if (P.keep) {
-                const double p = c / stored_total;
-                if (c > 0 && !(p > 0)) ++malformed;
-                A[k] = p;
-            }
-            B[k] = x;
+            B[(size_t)i * b_row + (size_t)my_cl * b_col] = x;
         }
     __syncthreads();
     if (tid < w) {
         // ordered ascending-theta scan of one phi column; the unnormalised prefix of row i+1
-        // replaces the weight of row i in place (each column belongs to one thread).  The next
-        // kChain weights are loaded before the current ones are added, so the shared-memory
-        // latency overlaps the dependent chain of additions.
-        double* col = B + tid;
-        double s = 0.0, nx[kChain];
-#pragma unroll
-        for (uint32_t k = 0; k < kChain; ++k) nx[k] = k < ct ? col[(size_t)k * CW] : 0.0;
-        for (uint32_t i = 0; i < ct; i += kChain) {
-            double cu[kChain];
-#pragma unroll
-            for (uint32_t k = 0; k < kChain; ++k) {
-                cu[k] = nx[k];
-                const uint32_t r = i + kChain + k;
-                nx[k] = r < ct ? col[(size_t)r * CW] : 0.0;
-            }
-#pragma unroll
-            for (uint32_t k = 0; k < kChain; ++k)
-                if (i + k < ct) {
-                    s += cu[k];
-                    col[(size_t)(i + k) * CW] = s;
-                }
+        // replaces the weight of row i in place (each column belongs to one thread)
+        P.colsum[c0 + tid] = chain_prefix(B + (size_t)tid * b_col, ct, b_row);
+    } else if (P.keep && tid >= 32) {
+        // meanwhile the other warps form the audit's p = coarse / stored total in A
+        for (uint32_t k = tid - 32; k < ct * w; k += kThreads - 32) {
+            const size_t a = (size_t)(k / w) * CW + k % w;
+            const double c = A[a];
+            const double pv = c / stored_total;
+            if (c > 0 && !(pv > 0)) ++malformed;
+            A[a] = pv;
         }
-        P.colsum[c0 + tid] = s;
     }
     {
         const double t = block_sum(tv.v + tv.c, red_d);
@@ -466,35 +509,21 @@ __global__ void __launch_bounds__(kThreads, 2) cdf_build_kernel(const __grid_con
     for (uint32_t j = tid; j < P.cp; j += kThreads) S[j] = __ldcg(P.colsum + j);
     __syncthreads();
     const uint32_t stride = ct + 1;
-    if (warp == 0) {
-        if (lane == 0) {
-            // ordered marginal scan (phase_table.cpp:154): phi[j+1] = phi[j] + colsum[j], the
-            // column sums read kChain ahead of the additions
-            double a = 0.0, nx[kChain];
-#pragma unroll
-            for (uint32_t k = 0; k < kChain; ++k) nx[k] = k < P.cp ? S[k] : 0.0;
-            for (uint32_t j = 0; j < P.cp; j += kChain) {
-                double cu[kChain];
-#pragma unroll
-                for (uint32_t k = 0; k < kChain; ++k) {
-                    cu[k] = nx[k];
-                    nx[k] = j + kChain + k < P.cp ? S[j + kChain + k] : 0.0;
-                }
-#pragma unroll
-                for (uint32_t k = 0; k < kChain; ++k) {
-                    const uint32_t jj = j + k;
-                    if (jj == c0) sphi[0] = a;
-                    if (jj < P.cp) a += cu[k];
-                    if (jj >= c0 && jj < c1) sphi[jj - c0 + 1] = a;
-                }
-            }
-            if (c0 >= P.cp) sphi[0] = a;
-            s_tot[3] = a;
+    if (tid == 0) {
+        // ordered marginal scan (phase_table.cpp:154): phi[j+1] = phi[j] + colsum[j]; this
+        // strip keeps the running values at its own columns
+        const uint32_t j0 = min(c0, P.cp), j1 = min(c1, P.cp);
+        double a = chain_sum(S, j0, 1u, 0.0);
+        sphi[0] = a;
+        for (uint32_t j = j0; j < j1; ++j) {
+            a += S[j];
+            sphi[j - j0 + 1] = a;
         }
-    } else {
-        // normalised conditionals of this strip, written once each: its output rows are the
-        // contiguous range theta[c0*(ct+1) .. c1*(ct+1)); element (cl, i) from the prefix of row
-        // i kept at B[(i-1)*CW + cl], and kept normalised there for the audit
+        s_tot[3] = chain_sum(S + j1, P.cp - j1, 1u, a);
+    } else if (tid >= 32) {
+        // meanwhile the normalised conditionals of this strip, written once each: its output
+        // rows are the contiguous range theta[c0*(ct+1) .. c1*(ct+1)); element (cl, i) comes from
+        // the prefix of row i kept at B(i-1, cl), which keeps the normalised value for the audit
         const uint32_t span = w * stride, step = kThreads - 32;
         uint32_t q = tid - 32, cl = q / stride, i = q % stride;
         double* out = P.theta + (size_t)c0 * stride;
@@ -503,9 +532,9 @@ __global__ void __launch_bounds__(kThreads, 2) cdf_build_kernel(const __grid_con
             double v;
             if (i == 0) v = 0.0;
             else if (i == ct) v = 1.0;
-            else v = cs > 0 ? B[(size_t)(i - 1) * CW + cl] / cs : E[i];
+            else v = cs > 0 ? B[(size_t)(i - 1) * b_row + (size_t)cl * b_col] / cs : E[i];
             out[q] = v;
-            if (i > 0) B[(size_t)(i - 1) * CW + cl] = v;
+            if (i > 0) B[(size_t)(i - 1) * b_row + (size_t)cl * b_col] = v;
             i += step;
             while (i >= stride) {
                 i -= stride;
@@ -530,8 +559,8 @@ __global__ void __launch_bounds__(kThreads, 2) cdf_build_kernel(const __grid_con
     if (act) {
         const double a0 = sphi[my_cl], a1 = sphi[my_cl + 1];
         for (uint32_t i = my_r; i < ct; i += rstep) {
-            const double b0 = i == 0 ? 0.0 : B[(size_t)(i - 1) * CW + my_cl];
-            const double b1 = B[(size_t)i * CW + my_cl]; // row ct - 1 holds 1
+            const double b0 = i == 0 ? 0.0 : B[(size_t)(i - 1) * b_row + (size_t)my_cl * b_col];
+            const double b1 = B[(size_t)i * b_row + (size_t)my_cl * b_col]; // row ct - 1 holds 1
             const double qv = (a1 - a0) * (b1 - b0);
             double p;
             if (P.keep) {

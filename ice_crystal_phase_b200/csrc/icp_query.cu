@@ -468,24 +468,48 @@ __device__ uint32_t collect(const QueryArgs& q, uint32_t i, icp_query_hit* out, 
     return count;
 }
 
-__global__ void __launch_bounds__(kThreads) query_count_kernel(QueryArgs q, unsigned long long* __restrict__ counts)
+// Roots a direction keeps from the counting pass for the fill pass (a direction with more is
+// intersected again there).
+constexpr uint32_t kCachedRoots = 8;
+struct RootCache {
+    icp_query_hit* hits; // kCachedRoots per direction, or null (sizing call: nothing kept)
+    uint32_t* flags;     // the collector's flags and first problem patch of the direction
+    uint32_t* first;
+};
+
+__global__ void __launch_bounds__(kThreads) query_count_kernel(QueryArgs q, unsigned long long* __restrict__ counts,
+                                                               RootCache cache)
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < q.direction_count; i += gridDim.x * blockDim.x) {
         uint32_t flags, first;
-        counts[i] = collect(q, i, nullptr, 0, flags, first);
+        if (cache.hits) {
+            const uint32_t n = collect(q, i, cache.hits + (size_t)i * kCachedRoots, kCachedRoots, flags, first);
+            cache.flags[i] = flags;
+            cache.first[i] = first;
+            counts[i] = n;
+        } else
+            counts[i] = collect(q, i, nullptr, 0, flags, first);
     }
 }
 
 __global__ void __launch_bounds__(kThreads) query_fill_kernel(QueryArgs q, const unsigned long long* __restrict__ offsets,
                                                               icp_query_summary* __restrict__ summaries,
-                                                              icp_query_hit* __restrict__ hits)
+                                                              icp_query_hit* __restrict__ hits, RootCache cache)
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < q.direction_count; i += gridDim.x * blockDim.x) {
         const unsigned long long begin = offsets[i], end = offsets[i + 1];
         const uint32_t capacity = uint32_t(end - begin);
         icp_query_hit* out = hits + begin;
-        uint32_t flags, first;
-        const uint32_t count = collect(q, i, out, capacity, flags, first);
+        uint32_t flags, first, count;
+        if (cache.hits && capacity <= kCachedRoots) {
+            // the counting pass kept every root of this direction, in the order it found them
+            const icp_query_hit* kept = cache.hits + (size_t)i * kCachedRoots;
+            for (uint32_t a = 0; a < capacity; ++a) out[a] = kept[a];
+            count = capacity;
+            flags = cache.flags[i];
+            first = cache.first[i];
+        } else
+            count = collect(q, i, out, capacity, flags, first);
         icp_query_summary sm{};
         sm.candidate_count = capacity;
         if (count != capacity) flags |= qMismatch;
@@ -670,14 +694,23 @@ extern "C" int icp_patch_query(icp_context* ctx, const icp_outgoing_vertex* d_ve
     const size_t o_counts = 0, o_offsets = align_up(o_counts + bins * 8), o_fill = align_up(o_offsets + (bins + 1) * 8);
     const size_t o_sums = align_up(o_fill + bins * 4), o_dir = align_up(o_sums + sum_blocks * 8);
     const size_t o_list = align_up(o_dir + (size_t(direction_count) + 1) * 8);
+    // a call that fills keeps up to kCachedRoots roots per direction from the counting pass
+    const bool keep = d_hits && d_summaries;
+    const size_t o_chits = o_list, o_cflags = align_up(o_chits + (keep ? sizeof(icp_query_hit) * kCachedRoots * direction_count : 0));
+    const size_t o_cfirst = align_up(o_cflags + (keep ? 4 * size_t(direction_count) : 0));
+    const size_t o_end = align_up(o_cfirst + (keep ? 4 * size_t(direction_count) : 0));
     ICP_CUDA(cudaSetDevice(ctx->device));
-    ICP_CUDA(ctx->query.ensure(o_list));
+    ICP_CUDA(ctx->query.ensure(o_end));
     char* base = static_cast<char*>(ctx->query.ptr);
     auto* bin_counts = reinterpret_cast<unsigned long long*>(base + o_counts);
     auto* bin_offsets = reinterpret_cast<unsigned long long*>(base + o_offsets);
     auto* bin_fill = reinterpret_cast<uint32_t*>(base + o_fill);
     auto* sums = reinterpret_cast<unsigned long long*>(base + o_sums);
     auto* dir_counts = reinterpret_cast<unsigned long long*>(base + o_dir);
+    RootCache cache{nullptr, nullptr, nullptr};
+    if (keep)
+        cache = {reinterpret_cast<icp_query_hit*>(base + o_chits), reinterpret_cast<uint32_t*>(base + o_cflags),
+                 reinterpret_cast<uint32_t*>(base + o_cfirst)};
     const unsigned pblocks = unsigned(patch_count ? (patch_count + kThreads - 1) / kThreads : 1);
     ICP_CUDA(cudaMemsetAsync(base, 0, o_sums, ctx->stream)); // counts, offsets, fill
     if (patch_count) {
@@ -702,7 +735,7 @@ extern "C" int icp_patch_query(icp_context* ctx, const icp_outgoing_vertex* d_ve
     const uint64_t cap = uint64_t(ctx->sms > 0 ? ctx->sms : 148) * 16u;
     const unsigned dblocks = unsigned(need ? (need < cap ? need : cap) : 1);
     if (direction_count) {
-        query_count_kernel<<<dblocks, kThreads, 0, ctx->stream>>>(q, dir_counts);
+        query_count_kernel<<<dblocks, kThreads, 0, ctx->stream>>>(q, dir_counts, cache);
         ICP_CUDA(cudaGetLastError());
         count_launch();
     }
@@ -717,7 +750,7 @@ extern "C" int icp_patch_query(icp_context* ctx, const icp_outgoing_vertex* d_ve
         return fail(ICP_ERR_CAPACITY, "icp_patch_query: %llu hits, capacity %llu", total,
                     (unsigned long long)hit_capacity);
     if (direction_count) {
-        query_fill_kernel<<<dblocks, kThreads, 0, ctx->stream>>>(q, offsets, d_summaries, d_hits);
+        query_fill_kernel<<<dblocks, kThreads, 0, ctx->stream>>>(q, offsets, d_summaries, d_hits, cache);
         ICP_CUDA(cudaGetLastError());
         count_launch();
     }

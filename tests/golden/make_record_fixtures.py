@@ -42,7 +42,7 @@ RECORDS = {
     # the reference's default stage: the patch model with Table-II diffraction, lattice 129 x 129
     "drop_diffraction_0.5mm_650nm_grid129_90x180": ["rainbow_generate", "--wavelength-nm", "650", "--radius-mm",
                                                     "0.5", "--grid", "129", "--query-theta", "90", "--query-phi",
-                                                    "180"],
+                                                    "180", "--allow-underresolved"],
 }
 
 

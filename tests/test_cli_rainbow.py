@@ -161,8 +161,12 @@ def test_extensions(tmp_path):
 # ------------------------------------------------------------ the lattice (patch) model stages
 def _stage(tmp_path, stage, extra=()):
     out = tmp_path / stage
+    # the 0.5 mm drop's Table-II width (0.22 deg) needs cells below 0.11 deg to be resolved; at
+    # this grid the diffraction stage is accepted only with --allow-underresolved, as in the
+    # reference (its defaults, 360 x 720 and 1.0 mm, are underresolved as well)
+    allow = ["--allow-underresolved"] if stage == "diffraction" else []
     r = run(["--out", out, "--wavelength-nm", "650", "--radius-mm", "0.5", "--grid", "129", "--query-theta", "180",
-             "--query-phi", "360", "--cdf-theta", "90", "--cdf-phi", "180", "--stage", stage, *extra])
+             "--query-phi", "360", "--cdf-theta", "90", "--cdf-phi", "180", "--stage", stage, *allow, *extra])
     assert "Saved NumPy CDF dataset" in r.stdout
     return validate_record(out)
 
@@ -207,3 +211,17 @@ def test_lattice_incoherent_matches_ray_model(tmp_path):
     ray = validate_record(out)
     assert abs(lat["metadata"]["hg"]["g"] - ray["metadata"]["hg"]["g"]) < 1e-2
     assert 0.5 * np.abs(lat["cell_probability"] - ray["cell_probability"]).sum() < 0.15
+
+
+@pytest.mark.gpu
+def test_lattice_diffraction_underresolved_gate(tmp_path):
+    """A query grid too coarse for the Table-II width leaves directions underresolved: the
+    reference's CDF input gate rejects the record unless --allow-underresolved is given."""
+    args = ["--wavelength-nm", "650", "--radius-mm", "0.5", "--grid", "129", "--query-theta", "180", "--query-phi",
+            "360", "--cdf-theta", "90", "--cdf-phi", "180"]
+    r = run(["--out", tmp_path / "rejected", *args], code=1)
+    assert "CDF input rejected" in r.stderr and "underresolved=" in r.stderr
+    assert not (tmp_path / "rejected").exists() and not (tmp_path / "rejected.part").exists()
+    run(["--out", tmp_path / "allowed", *args, "--allow-underresolved"])
+    m = validate_record(tmp_path / "allowed")["metadata"]
+    assert m["quality"]["underresolved_directions"] > 0 and m["quality"]["allow_underresolved"] is True
