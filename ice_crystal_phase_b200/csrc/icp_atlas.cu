@@ -15,10 +15,10 @@
 //                          the projected area), so the coupling does not depend on the order
 //                          in which threads run (atlas_math.py:186-310).
 //   atlas_compose_kernel   out[t][p] = sum_(n,q,s) w[n][q][s] * M_n[t][(p - s) mod np]
-//                          (phi reflected when q = 1): per thread a strip of PT consecutive
-//                          phi cells of TT rows; the shifted row window slides by one cell per
-//                          shift (one shared-memory load per row per shift), is reloaded
-//                          after a run of zero weights; products and sums are rounded
+//                          (phi reflected when q = 1) over the nonzero shifts only, compacted
+//                          per (node, parity) in shift order by atlas_weights_compact_kernel
+//                          (the couplings are ~4 % nonzero); kTT rows of a node in shared
+//                          memory, a thread per cell column; products and sums are rounded
 //                          separately in the order node, parity, shift -- the order of
 //                          compose_mass's elementwise `out += value * roll(cell)`
 //                          (atlas_math.py:431-447), so equal weights give equal bits.
@@ -343,25 +343,70 @@ __global__ void __launch_bounds__(256) atlas_coupling_finish_kernel(const unsign
 }
 
 // ------------------------------------------------------------------ compose
-constexpr int kTT = 2;   // rows per block
-constexpr int kPT = 8;   // phi cells per thread
-constexpr int kComposeThreads = 256;
+constexpr int kTT = 2;                 // rows per block
+constexpr int kComposeThreads = 256;   // cells per block row: threads x CPT >= np
+constexpr int kCompactThreads = 256;
 
-__global__ void __launch_bounds__(kComposeThreads, 2) atlas_compose_kernel(const double* mass, const double* w,
+// The nonzero shifts of one (node, parity) coupling row, ascending, with their weights: one
+// block per row, ballot ranks within each warp and the warps' counts in order, so the list's
+// order is the shift order (the composition's summation order depends on it).
+__global__ void __launch_bounds__(kCompactThreads) atlas_weights_compact_kernel(const double* __restrict__ w, uint32_t np,
+                                                                                uint32_t* __restrict__ counts,
+                                                                                uint32_t* __restrict__ shifts,
+                                                                                double* __restrict__ values)
+{
+    __shared__ uint32_t warp_count[kCompactThreads / 32];
+    __shared__ uint32_t base;
+    const uint32_t row = blockIdx.x, lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const double* wr = w + (uint64_t)row * np;
+    if (threadIdx.x == 0) base = 0;
+    __syncthreads();
+    for (uint32_t s0 = 0; s0 < np; s0 += kCompactThreads) {
+        const uint32_t sft = s0 + threadIdx.x;
+        const double v = sft < np ? wr[sft] : 0.0;
+        const bool nz = v != 0.0;
+        const unsigned ballot = __ballot_sync(0xffffffffu, nz);
+        if (lane == 0) warp_count[warp] = __popc(ballot);
+        __syncthreads();
+        uint32_t before = base;
+        for (uint32_t k = 0; k < warp; ++k) before += warp_count[k];
+        if (nz) {
+            const uint32_t slot = before + __popc(ballot & ((1u << lane) - 1u));
+            shifts[(uint64_t)row * np + slot] = sft;
+            values[(uint64_t)row * np + slot] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+            for (uint32_t k = 0; k < kCompactThreads / 32; ++k) base += warp_count[k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) counts[row] = base;
+}
+
+// out[t][p] = sum over nodes n, parities q and the nonzero shifts s of w[n][q][s] *
+// M_n[t][(p - s) mod np] (phi-reflected when q = 1).  A block holds kTT rows of one node in
+// shared memory and the (n, q) list of nonzero shifts; thread x owns the cells x + k T of its
+// rows (consecutive threads read consecutive cells).  Products and sums rounded separately,
+// in the order node, parity, ascending shift -- the order of compose_mass's elementwise
+// `out += value * roll(cell)` (atlas_math.py:431-447), so equal weights give equal bits.
+template <int CPT>
+__global__ void __launch_bounds__(kComposeThreads, 2) atlas_compose_kernel(const double* __restrict__ mass,
+                                                                           const uint32_t* __restrict__ counts,
+                                                                           const uint32_t* __restrict__ shifts,
+                                                                           const double* __restrict__ values,
                                                                            uint32_t nodes, uint32_t nt, uint32_t np,
-                                                                           double* out)
+                                                                           double* __restrict__ out)
 {
     extern __shared__ __align__(16) double sm[];
-    double* rows = sm;               // [kTT][np]
-    double* ws = sm + kTT * np;      // [np]
+    double* rows = sm;                                             // [kTT][np]
+    double* lw = sm + kTT * np;                                    // [np] weights of the list
+    uint32_t* ls = reinterpret_cast<uint32_t*>(lw + np);           // [np] shifts of the list
     const uint32_t t0 = blockIdx.x * kTT;
-    const uint32_t p0 = (blockIdx.y * kComposeThreads + threadIdx.x) * kPT;
-    const uint32_t pm = p0 % np;
-    double acc[kTT][kPT];
+    double acc[kTT][CPT];
 #pragma unroll
     for (int t = 0; t < kTT; ++t)
 #pragma unroll
-        for (int k = 0; k < kPT; ++k) acc[t][k] = 0.0;
+        for (int k = 0; k < CPT; ++k) acc[t][k] = 0.0;
     for (uint32_t n = 0; n < nodes; ++n) {
         __syncthreads();
         for (uint32_t e = threadIdx.x; e < kTT * np; e += blockDim.x) {
@@ -369,52 +414,41 @@ __global__ void __launch_bounds__(kComposeThreads, 2) atlas_compose_kernel(const
             rows[e] = t < nt ? mass[((uint64_t)n * nt + t) * np + e % np] : 0.0;
         }
         for (int q = 0; q < 2; ++q) {
+            const uint64_t r = (uint64_t)n * 2 + q;
+            const uint32_t cnt = counts[r];
             __syncthreads();
-            for (uint32_t s = threadIdx.x; s < np; s += blockDim.x) ws[s] = w[((uint64_t)n * 2 + q) * np + s];
-            __syncthreads();
-            // row index of output cell p0 + k at shift s: (p0 + k - s) mod np, reflected np-1-m when
-            // q = 1; m is that of the first cell, stepped down by one per shift
-            double win[kTT][kPT];
-            bool gap = true;
-            uint32_t m = 0;
-            for (uint32_t s = 0; s < np; ++s) {
-                const double wv = ws[s];
-                if (wv == 0) {
-                    gap = true;
-                    continue;
-                }
-                if (gap) {
-                    m = phi_sub(pm, s, np);
-#pragma unroll
-                    for (int k = 0; k < kPT; ++k) {
-                        const uint32_t idx = phi_cell(phi_add(m, (uint32_t)k, np), np, q);
-#pragma unroll
-                        for (int t = 0; t < kTT; ++t) win[t][k] = rows[t * np + idx];
-                    }
-                    gap = false;
-                } else {
-                    m = phi_prev(m, np);
-                    const uint32_t idx = phi_cell(m, np, q);
-#pragma unroll
-                    for (int t = 0; t < kTT; ++t) {
-#pragma unroll
-                        for (int k = kPT - 1; k > 0; --k) win[t][k] = win[t][k - 1];
-                        win[t][0] = rows[t * np + idx];
-                    }
-                }
-#pragma unroll
-                for (int t = 0; t < kTT; ++t)
-#pragma unroll
-                    for (int k = 0; k < kPT; ++k) acc[t][k] = acc[t][k] + wv * win[t][k];
+            for (uint32_t e = threadIdx.x; e < cnt; e += blockDim.x) {
+                lw[e] = values[r * np + e];
+                ls[e] = shifts[r * np + e];
             }
+            __syncthreads();
+            if (threadIdx.x < np)
+                for (uint32_t e = 0; e < cnt; ++e) {
+                    const double wv = lw[e];
+                    // m = (p - s) mod np for p = x + k T, stepped by T per cell (T < np when CPT > 1)
+                    uint32_t m = phi_sub(threadIdx.x, ls[e], np);
+#pragma unroll
+                    for (int k = 0; k < CPT; ++k) {
+                        if (k > 0) {
+                            if (threadIdx.x + (uint32_t)k * kComposeThreads >= np) break;
+                            m += kComposeThreads;
+                            if (m >= np) m -= np;
+                        }
+                        const uint32_t idx = phi_cell(m, np, q);
+#pragma unroll
+                        for (int t = 0; t < kTT; ++t) acc[t][k] = acc[t][k] + wv * rows[t * np + idx];
+                    }
+                }
         }
     }
 #pragma unroll
     for (int t = 0; t < kTT; ++t) {
         if (t0 + t >= nt) continue;
 #pragma unroll
-        for (int k = 0; k < kPT; ++k)
-            if (p0 + k < np) out[(uint64_t)(t0 + t) * np + p0 + k] = acc[t][k];
+        for (int k = 0; k < CPT; ++k) {
+            const uint32_t p = threadIdx.x + (uint32_t)k * kComposeThreads;
+            if (p < np) out[(uint64_t)(t0 + t) * np + p] = acc[t][k];
+        }
     }
 }
 
@@ -696,15 +730,38 @@ int icp_atlas_compose(icp_context* ctx, uint32_t nodes, uint32_t nt, uint32_t np
     if (!ctx || !d_mass || !d_coupling || !d_out) return fail(ICP_ERR_INVALID_ARGUMENT, "icp_atlas_compose: null argument");
     if (nodes == 0 || nt == 0 || np == 0 || uint64_t(nt) * np > 100000000ull)
         return fail(ICP_ERR_INVALID_ARGUMENT, "icp_atlas_compose: invalid shape");
-    const size_t smem = (size_t(kTT) + 1) * np * sizeof(double);
-    if (smem > 227u * 1024u)
-        return fail(ICP_ERR_CAPACITY, "icp_atlas_compose: %u phi cells need %zu bytes of shared memory (limit 227 KiB)",
-                    np, smem);
+    const size_t smem = (size_t(kTT) + 1) * np * sizeof(double) + np * sizeof(uint32_t);
+    if (smem > 227u * 1024u || np > 16u * kComposeThreads)
+        return fail(ICP_ERR_CAPACITY, "icp_atlas_compose: %u phi cells need %zu bytes of shared memory (limit 227 KiB) "
+                    "or more than %u cells per row", np, smem, 16u * kComposeThreads);
     ICP_CUDA(cudaSetDevice(ctx->device));
-    ICP_CUDA(cudaFuncSetAttribute(atlas_compose_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const dim3 grid((nt + kTT - 1) / kTT, (np + kComposeThreads * kPT - 1) / (kComposeThreads * kPT));
-    atlas_compose_kernel<<<grid, kComposeThreads, smem, ctx->stream>>>(d_mass, d_coupling, nodes, nt, np, d_out);
+    // the nonzero coupling shifts of every (node, parity) row, compacted in shift order
+    const uint64_t rowsw = uint64_t(nodes) * 2;
+    const size_t o_shifts = (rowsw * 4 + 255) / 256 * 256, o_values = o_shifts + (rowsw * np * 4 + 255) / 256 * 256;
+    ICP_CUDA(ctx->atlas_list.ensure(o_values + rowsw * np * 8));
+    char* base = static_cast<char*>(ctx->atlas_list.ptr);
+    auto* counts = reinterpret_cast<uint32_t*>(base);
+    auto* shifts = reinterpret_cast<uint32_t*>(base + o_shifts);
+    auto* values = reinterpret_cast<double*>(base + o_values);
+    atlas_weights_compact_kernel<<<(unsigned)rowsw, kCompactThreads, 0, ctx->stream>>>(d_coupling, np, counts, shifts,
+                                                                                      values);
     ICP_CUDA(cudaGetLastError());
+    count_launch();
+    const uint32_t cpt = (np + kComposeThreads - 1) / kComposeThreads;
+    const dim3 grid((nt + kTT - 1) / kTT);
+    auto run = [&](auto kernel) -> cudaError_t {
+        cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        kernel<<<grid, kComposeThreads, smem, ctx->stream>>>(d_mass, counts, shifts, values, nodes, nt, np, d_out);
+        return cudaGetLastError();
+    };
+    cudaError_t e;
+    if (cpt <= 1) e = run(atlas_compose_kernel<1>);
+    else if (cpt <= 2) e = run(atlas_compose_kernel<2>);
+    else if (cpt <= 4) e = run(atlas_compose_kernel<4>);
+    else if (cpt <= 8) e = run(atlas_compose_kernel<8>);
+    else e = run(atlas_compose_kernel<16>);
+    ICP_CUDA(e);
     count_launch();
     ICP_CUDA(cudaStreamSynchronize(ctx->stream));
     return ok();

@@ -1,7 +1,7 @@
 // icp_atlas_window.cuh -- phi-index arithmetic of the cyclic composition (atlas_compose_kernel):
-// the cell of row m that output cell p reads at shift s is m = (p - s) mod np.  A thread keeps
-// the index of its first cell and steps it by one per shift, so the inner loop needs no integer
-// division.  Host and device code alike (the host test compiles it with g++).
+// the cell of row m that output cell p reads at shift s is m = (p - s) mod np, reflected to
+// np - 1 - m for the mirrored parity; no integer division in the inner loop.  Host and device
+// code alike (the host test compiles it with g++).
 #pragma once
 #include <cstdint>
 

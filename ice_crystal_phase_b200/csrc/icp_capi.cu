@@ -125,7 +125,7 @@ int icp_context_destroy(icp_context* c)
                       &c->b_reports,  &c->b_sync,     &c->b_phi,        &c->b_theta,     &c->mlp_error,
                       &c->cdfb_partial, &c->cdfb_colsum, &c->cdfb_recs, &c->atlas_trace, &c->atlas_coupling,
                       &c->rainbow,    &c->patches,
-                      &c->query,      &c->query_list, &c->stage_audit, &c->cdf_edges, &c->lattice, &c->folded};
+                      &c->query,      &c->query_list, &c->stage_audit, &c->cdf_edges, &c->lattice, &c->folded, &c->atlas_list};
     for (Scratch* s : all) s->release();
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);

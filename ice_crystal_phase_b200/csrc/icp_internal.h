@@ -315,6 +315,8 @@ struct icp_context {
     icp::Scratch lattice;
     // folded-patch records: block counts, candidate list, statistics
     icp::Scratch folded;
+    // atlas composition: the compacted nonzero coupling shifts
+    icp::Scratch atlas_list;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
     // grid-barrier iteration limit handed to the CDF kernels (0: their default)
     uint32_t wait_limit = 0;

@@ -9,10 +9,12 @@ contract -- batch_plan.json with a signature, a .batch.lock, records/i####/w####
 reserve -- and the same refusal to lower precision, skip or delete anything on failure.
 
 What changes: the reference runs one rainbow_generate process per condition, one at a time
-(generate_phase_dataset.py:296-311).  Here the pending conditions go to the GPU in batches of
-`batch_records` through one persistent launch (icp_drop_batch_generate); every record keeps its
-own seed (derived from the condition indices), so a record does not depend on how the run was
-batched, limited or resumed.  Records are written in rainbow_generate's format.
+(generate_phase_dataset.py:296-311).  Here the ray-model records (stage "incoherent") go to the
+GPU in batches of `batch_records` through one persistent launch (icp_drop_batch_generate); every
+record keeps its own seed (derived from the condition indices), so a record does not depend on
+how the run was batched, limited or resumed.  The patch-model stages (path, focal, diffraction)
+run rainbow_generate once per record with the reference's options, as the reference does.
+Records are written in rainbow_generate's format.
 
     python -m ice_crystal_phase_b200.dataset --config CONFIG.json [--execute] [--resume] [--limit N]
 """
@@ -25,6 +27,7 @@ import math
 import os
 import shutil
 import struct
+import subprocess
 import sys
 import time
 from contextlib import contextmanager
@@ -35,7 +38,8 @@ from typing import Any, Iterator
 import numpy as np
 
 VERSION = "rainbow.condition_batch.v1"
-GENERATOR_VERSION = "icp_b200.rainbow.v1"
+GENERATOR_VERSION = "icp_b200.rainbow.v1"                # ray-model records (the batched library)
+LATTICE_GENERATOR_VERSION = "icp_b200.rainbow.lattice.v1"  # patch-model records (rainbow_generate)
 ARRAYS = ("phi_cdf.npy", "theta_given_phi_cdf.npy", "u_edges.npy")
 B200_DEFAULTS = {"rays": 10_000_000, "seed": 12345, "precision": "fp32", "max_internal_hits": 1024,
                  "diffraction": False, "batch_records": 32, "max_unresolved_fraction": 1e-4}
@@ -145,8 +149,9 @@ def inclination_grid(spec: dict[str, Any]) -> list[str]:
 def normalized_config(raw: dict[str, Any]) -> dict[str, Any]:
     """The checked, normalised conditions of a config file.  Beyond the reference's keys an
     optional "b200" object sets rays, seed, precision, max_internal_hits, diffraction and
-    batch_records.  Stages other than "incoherent" are the reference's wave-optics patch model,
-    which this build does not implement: they are refused, as rainbow_generate refuses them."""
+    batch_records: the ray model of stage "incoherent".  The other stages (path, focal,
+    diffraction) are the reference's patch model, one rainbow_generate process per record as in
+    the reference; the "b200" settings do not apply to them."""
     keys = set(raw) - {"b200"}
     if keys != TOP_KEYS:
         raise ValueError(f"Unexpected/missing config keys: {keys ^ TOP_KEYS}")
@@ -160,9 +165,6 @@ def normalized_config(raw: dict[str, Any]) -> dict[str, Any]:
         raise ValueError("CDF grids must divide query grids")
     if solver["stage"] not in STAGES:
         raise ValueError("Unknown stage")
-    if solver["stage"] != "incoherent":
-        raise ValueError(f"Stage {solver['stage']} is the reference's wave-optics patch model, which this build does not "
-                         "implement; use stage incoherent (optionally with b200.diffraction)")
     out["stage"] = solver["stage"]
     offsets = solver["focal_offsets"]
     if not isinstance(offsets, list) or len(offsets) != 4:
@@ -304,7 +306,8 @@ def verify_record(path: Path, plan: dict[str, Any], ii: int, ll: int) -> dict[st
     geometry, cs, q = m.get("geometry", {}), m.get("cross_sections", {}), m.get("quality", {})
     sp, hg, material = m.get("storage_processing", {}), m.get("hg", {}), m.get("material", {})
     area = geometry.get("projected_area_mm2")
-    fields = {"complete": True, "schema": "rainbow.phase_cdf.numpy.v2", "generator_version": GENERATOR_VERSION,
+    version = GENERATOR_VERSION if s["stage"] == "incoherent" else LATTICE_GENERATOR_VERSION
+    fields = {"complete": True, "schema": "rainbow.phase_cdf.numpy.v2", "generator_version": version,
               "coordinate_contract_id": "rainbow.phase_cdf.coordinates.v1",
               "direction_convention": "physical_propagation", "dtype": "<f8", "order": "C",
               "density_measure": "solid_angle_sr", "cdf_axis_order": ["phi_cell", "theta_edge"],
@@ -483,16 +486,49 @@ def write_record(path: Path, phi, theta, u, metadata: dict) -> None:
     part.rename(path)
 
 
-class GpuBackend:
-    """The batched device library: a context for the run and one persistent launch per batch."""
+def lattice_command(exe: Path, out: Path, c: dict, ii: int, ll: int) -> list[str]:
+    """The rainbow_generate command of one patch-model record: the options the reference's
+    orchestrator passes (tools/generate_phase_dataset.py:296-311), so a record is the CLI's."""
+    s = c["solver"]
+    values = {"out": str(out), "material": "water", "radius-mm": str(c["radius_mm"]),
+              "wavelength-nm": c["wavelength_nm"][ll], "inclination-deg": c["inclination_degrees"][ii],
+              "temperature-c": str(c["temperature_c"]), "pressure-pa": str(c["pressure_pa"]),
+              "grid": s["grid"], "query-theta": s["query_theta"], "query-phi": s["query_phi"],
+              "cdf-theta": s["cdf_theta"], "cdf-phi": s["cdf_phi"], "stage": s["stage"],
+              "device": s["device"], "max-coarsening-tv": s["maximum_coarsening_tv"],
+              "cdf-max-l1": s["cdf_max_l1"], "cdf-max-lost-mass": s["cdf_max_lost_mass"],
+              "focal-offsets": ",".join(map(str, s["focal_offsets"]))}
+    args = [str(exe)]
+    for k, v in values.items():
+        args += ["--" + k, str(v)]
+    if c["force_sphere"]:
+        args.append("--sphere")
+    if s["allow_underresolved"]:
+        args.append("--allow-underresolved")
+    return args
 
-    def __init__(self):
+
+class GpuBackend:
+    """The batched device library (a context for the run and one persistent launch per batch of
+    ray-model records) and rainbow_generate for the patch-model stages."""
+
+    def __init__(self, generator: Path | None = None):
         import ice_crystal_phase_b200 as icp  # noqa: PLC0415 (only needed to execute)
 
         self.icp = icp
+        self.generator = Path(generator) if generator else Path(icp.__file__).resolve().parent / "bin" / "rainbow_generate"
 
     def library_sha256(self) -> str:
         return sha256(self.icp.LIB_PATH)
+
+    def generator_sha256(self) -> str:
+        return sha256(self.generator)
+
+    def lattice_record(self, c: dict, ii: int, ll: int, path: Path) -> None:
+        """One patch-model record written by rainbow_generate (through its own .part directory)."""
+        r = subprocess.run(lattice_command(self.generator, path, c, ii, ll), capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"rainbow_generate failed for {path}: {(r.stderr or r.stdout).strip()[-2000:]}")
 
     def context(self, device: int):
         return self.icp.Context(device)
@@ -530,7 +566,8 @@ def _arguments(argv: list[str] | None) -> argparse.Namespace:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--config", type=Path, required=True)
     ap.add_argument("--out-root", type=Path)
-    ap.add_argument("--generator", type=Path, help="accepted for compatibility; the batched library generates")
+    ap.add_argument("--generator", type=Path, help="rainbow_generate for the patch-model stages (default: the "
+                    "package's bin/rainbow_generate); ray-model records come from the batched library")
     ap.add_argument("--wavelength-range", nargs=3, metavar=("START_NM", "STOP_NM", "STEP_NM"))
     ap.add_argument("--radius-mm")
     ap.add_argument("--inclination-count", type=int)
@@ -579,15 +616,21 @@ class DatasetRun:
         print(f"array_total_TB={self.payload * n / 1e12:.6f}; output={self.root}")
         print(f"inclination_centers=[{c['inclination_degrees'][0]}, {c['inclination_degrees'][-1]}] degrees")
         print(f"wavelengths=[{c['wavelength_nm'][0]}, {c['wavelength_nm'][-1]}] nm; inclusive exact-step endpoints")
-        print(f"Batches of {b['batch_records']} records per persistent GPU launch; {b['rays']} rays per record "
-              f"({b['precision']}).")
+        if s["stage"] == "incoherent":
+            print(f"Batches of {b['batch_records']} records per persistent GPU launch; {b['rays']} rays per record "
+                  f"({b['precision']}).")
+        else:
+            print(f"Stage {s['stage']}: one rainbow_generate process per record (lattice {s['grid']} x {s['grid']}, "
+                  f"query {s['query_theta']} x {s['query_phi']}).")
         if s["maximum_coarsening_tv"] == 1:
             print("WARNING: maximum_coarsening_tv=1 is not an accuracy acceptance threshold.")
 
     def plan(self) -> tuple[dict, str]:
         """The signed plan, written on first use and required to be identical on --resume."""
-        spec = {"version": VERSION, "conditions": self.c,
-                "binary_sha256": {"libicp_b200": self.backend.library_sha256()}}
+        binaries = {"libicp_b200": self.backend.library_sha256()}
+        if self.c["solver"]["stage"] != "incoherent":
+            binaries["rainbow_generate"] = self.backend.generator_sha256()
+        spec = {"version": VERSION, "conditions": self.c, "binary_sha256": binaries}
         signature = object_hash(spec)
         plan = {**spec, "signature": signature, "record_layout": "records/i{incident_index:04d}/w{wavelength_index:04d}"}
         manifest = self.root / "batch_plan.json"
@@ -641,16 +684,24 @@ class DatasetRun:
                 raise RuntimeError(f"Insufficient free space: estimated {needed} bytes including reserve; "
                                    f"available {free}")
             total, started, done = self.ni * self.nl, time.monotonic(), 0
-            per = self.c["b200"]["batch_records"]
+            lattice = self.c["solver"]["stage"] != "incoherent"
+            per = 1 if lattice else self.c["b200"]["batch_records"]
             with self.backend.context(self.c["solver"]["device"]) as ctx:
                 for batch in (todo[k:k + per] for k in range(0, len(todo), per)):
                     if shutil.disk_usage(self.root).free < len(batch) * self.per_record + self.reserve:
                         raise RuntimeError("Free-space reserve reached; stopping without lowering precision")
-                    results = self.backend.generate(ctx, self.c, [(ii, ll) for ii, ll, *_ in batch])
-                    for (ii, ll, job, path, receipt), (sp, water, phi, theta, u, rep) in zip(batch, results):
-                        accept(rep, self.c)
+                    if lattice:
+                        results = [None] * len(batch)
+                    else:
+                        results = self.backend.generate(ctx, self.c, [(ii, ll) for ii, ll, *_ in batch])
+                    for (ii, ll, job, path, receipt), result in zip(batch, results):
                         path.parent.mkdir(parents=True, exist_ok=True)
-                        write_record(path, phi, theta, u, record_metadata(self.c, ii, ll, sp, rep, water))
+                        if lattice:
+                            self.backend.lattice_record(self.c, ii, ll, path)
+                        else:
+                            sp, water, phi, theta, u, rep = result
+                            accept(rep, self.c)
+                            write_record(path, phi, theta, u, record_metadata(self.c, ii, ll, sp, rep, water))
                         digest = verify_record(path, plan, ii, ll)
                         write_json(receipt, {"signature": signature, "incident_index": ii, "wavelength_index": ll,
                                              "record": digest})
@@ -676,7 +727,7 @@ def run(argv: list[str] | None = None, backend=None) -> int:
     if not args.execute:
         print("DRY RUN: no simulations or files written. Add --execute to start.")
         return 0
-    job.backend = backend or GpuBackend()
+    job.backend = backend or GpuBackend(args.generator)
     job.execute()
     return 0
 

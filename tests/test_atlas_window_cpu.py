@@ -1,8 +1,9 @@
-"""The composition kernel's phi-window arithmetic on the CPU (no GPU): the helpers of
-csrc/icp_atlas_window.cuh, compiled with g++, driven through the kernel's per-thread loop (the
-first cell's index set after a run of zero weights, stepped down by one per shift), give the
-cell (p0 + k - s) mod np, phi-reflected when q = 1, for every output cell, shift and weight
-pattern -- including thread strips past the row end and rows narrower than a strip."""
+"""The composition's phi-index arithmetic on the CPU (no GPU): the helpers of
+csrc/icp_atlas_window.cuh, compiled with g++ -- driven both directly (phi_sub, phi_cell per cell
+and shift, as atlas_compose_kernel uses them) and through a sliding window (the first cell's
+index set after a run of zero weights, stepped down by one per shift) -- give the cell
+(p0 + k - s) mod np, phi-reflected when q = 1, for every output cell, shift and weight
+pattern -- including strips past the row end and rows narrower than a strip."""
 from __future__ import annotations
 
 import subprocess
@@ -46,7 +47,8 @@ int main()
                         for (unsigned k = 0; k < kPT; ++k) {
                             const long long r = (((long long)p0 + k - (long long)s) % (long long)np + np) % np;
                             const unsigned want = q ? np - 1 - (unsigned)r : (unsigned)r;
-                            if (idx[k] != want || idx[k] >= np) {
+                            const unsigned direct = phi_cell(phi_sub((p0 + k) % np, s, np), np, q);
+                            if (idx[k] != want || idx[k] >= np || direct != want) {
                                 printf("MISMATCH np=%u p0=%u q=%d s=%u k=%u got=%u want=%u\n", np, p0, q, s, k, idx[k], want);
                                 return 1;
                             }

@@ -48,7 +48,6 @@ def ds():
     (lambda c: c["inclinations"].update(min_degrees=0, max_degrees=180), "Canonical inclination domain"),
     (lambda c: c["inclinations"].update(placement="edges"), "linear_angle_cell_centers"),
     (lambda c: c["solver"].update(cdf_theta=50), "CDF grids must divide query grids"),
-    (lambda c: c["solver"].update(stage="diffraction"), "Stage diffraction is the reference's wave-optics"),
     (lambda c: c["solver"].update(stage="bogus"), "Unknown stage"),
     (lambda c: c.update(radius_mm=4), "outside"),
     (lambda c: c["solver"].update(allow_underresolved=1), "Expected JSON true or false"),
@@ -280,3 +279,37 @@ def test_batched_dataset_on_gpu(ds, icp, tmp_path):
             t = m["transport_audit"]
             assert abs((t["escaped_mm2"] + t["unresolved_mm2"]) / t["incident_mm2"] - 1) <= 1e-12
     assert ds.run(["--config", str(_write(tmp_path, cfg)), "--execute", "--resume"]) == 0
+
+
+def test_lattice_stage_command_is_the_reference_orchestrators(ds, tmp_path):
+    """A patch-model record is one rainbow_generate process with the options the reference's
+    orchestrator passes (tools/generate_phase_dataset.py:296-311)."""
+    cfg = copy.deepcopy(CONFIG)
+    cfg["solver"].update(stage="diffraction", allow_underresolved=True)
+    c = ds.normalized_config(cfg)
+    args = ds.lattice_command("gen", tmp_path / "rec", c, 1, 0)
+    assert args[0] == "gen" and "--allow-underresolved" in args and "--sphere" not in args
+    pairs = dict(zip(args[1:-1:2], args[2:-1:2]))
+    assert pairs["--stage"] == "diffraction" and pairs["--grid"] == "129" and pairs["--material"] == "water"
+    assert pairs["--wavelength-nm"] == c["wavelength_nm"][0] and pairs["--inclination-deg"] == c["inclination_degrees"][1]
+    assert pairs["--focal-offsets"] == "0,0,0,0" and pairs["--out"] == str(tmp_path / "rec")
+
+
+@pytest.mark.gpu
+def test_lattice_stage_dataset_on_gpu(ds, tmp_path):
+    """Stage path through the orchestrator: one rainbow_generate per record, every record verified,
+    receipted and re-verified on --resume."""
+    cfg = copy.deepcopy(CONFIG)
+    cfg["radius_mm"] = 0.5
+    cfg["solver"].update(stage="path", grid=33, query_theta=36, query_phi=72, cdf_theta=18, cdf_phi=36)
+    cfg["output_root"] = str(tmp_path / "out")
+    path = _write(tmp_path, cfg)
+    assert ds.run(["--config", str(path), "--execute"]) == 0
+    recs = sorted((tmp_path / "out" / "records").glob("i*/w*"))
+    assert len(recs) == 4
+    for r in recs:
+        m = validate_record(r)["metadata"]
+        assert m["stage"] == "path" and m["generator_version"] == "icp_b200.rainbow.lattice.v1"
+    plan = json.loads((tmp_path / "out" / "batch_plan.json").read_text())
+    assert "rainbow_generate" in plan["binary_sha256"]
+    assert ds.run(["--config", str(path), "--execute", "--resume"]) == 0
