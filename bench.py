@@ -593,7 +593,7 @@ def run_surrogate(I, ctx, stream, a) -> dict:
                     "served_out_of_tolerance": served_bad,
                     "served_out_of_tolerance_fraction": served_bad / max(1, len(served_tv)),
                     "served_tv_storage_max": max(served_tv) if served_tv else None},
-        "roofline_forward": {"kernel": "gemm_persistent_kernel x3 (forward pass)", "bound": "tensor",
+        "roofline_forward": {"kernel": "features_kernel + mlp_fused_kernel (forward pass: input rows, three layers and head in one kernel)", "bound": "tensor",
                              "achieved": flops / t_fwd / 1e12, "peak": bf16, "unit": "TFLOP/s",
                              "frac": flops / t_fwd / 1e12 / bf16, "records": nf, "ms": 1e3 * t_fwd,
                              "peak_note": "MEASURED_PEAKS.json bf16_tflops (of measured)"},

@@ -223,6 +223,26 @@ int enqueue_forward(icp_surrogate* s, uint32_t count, bool training, float* y_ou
 {
     const uint64_t M = (uint64_t)count * s->C;
     const uint32_t Hn = s->H;
+    if (!training && mlp::fused_shape(s->K0, Hn)) {
+        // inference: the three layers and the head in one kernel, activations kept on chip
+        mlp::FusedArgs f{};
+        f.M = (uint32_t)M;
+        f.K0 = s->K0;
+        f.b1 = s->P(s->o_b1);
+        f.b2 = s->P(s->o_b2);
+        f.b3 = s->P(s->o_b3);
+        f.head_w = s->P(s->o_w4);
+        f.head_b = s->head_b;
+        f.out_y = y_out;
+        f.out_mass = mass_out;
+        f.out_mass_sum = mass_sum;
+        f.record_rows = s->C;
+        f.error = (unsigned*)s->c->mlp_error.ptr;
+        const int e = mlp::forward_fused(s->X.ptr, s->w1b(), s->w2b(), s->w3b(), f, s->c->stream);
+        count_launch();
+        if (e) return fail(ICP_ERR_DEVICE, "surrogate forward launch failed (%d)", e);
+        return ICP_OK;
+    }
     const size_t act = 2 * M * Hn;
     ICP_CUDA(s->h1.ensure(act));
     ICP_CUDA(s->h2.ensure(act));

@@ -49,6 +49,24 @@ struct GemmArgs {
 // `splits` CTAs per row tile.  Returns 0 or a negative / CUDA error code.
 int gemm(const void* A, const void* B, GemmArgs g, int epi, uint32_t splits, cudaStream_t stream);
 
+// The whole inference pass of the 3-hidden-layer network in one persistent kernel (the
+// activations of a 128-row tile never leave the SM): X [M x K0] BF16 with K0 in {64, 128},
+// W1 [256 x K0], W2, W3 [256 x 256] BF16 (row n = output unit, K contiguous), biases and head in
+// FP32.  Writes y and / or exp(y) with the per-record sums as the kHead epilogue does.
+struct FusedArgs {
+    uint32_t M, K0;
+    const float *b1, *b2, *b3, *head_w;
+    float head_b;
+    float* out_y;
+    double* out_mass;
+    double* out_mass_sum;
+    uint32_t record_rows;
+    unsigned* error;
+};
+bool fused_shape(uint32_t K0, uint32_t H);
+int forward_fused(const void* X, const void* W1, const void* W2, const void* W3, const FusedArgs& f,
+                  cudaStream_t stream);
+
 // ---------------------------------------------------------------- icp_mlp.cu
 // X[m][k] (BF16, [R*C x K0]) and optionally XT[k][m]: record features in columns [0, 16), the
 // cell table (C x (K0-16), row-major) after them; record r owns rows [r*C, (r+1)*C).  The last P

@@ -48,16 +48,27 @@ template <int N, int MT = 1> constexpr size_t smem_bytes()
 // Logistic function 1 / (1 + exp(-z)) with the exponential on the special-function unit and
 // the reciprocal on the FMA pipe, so that the two pipes share the epilogue's activation work
 // (one SiLU per output element is the MLP's largest non-tensor cost).  Reciprocal of d >= 1:
-// the exponent-negation seed y0 = 2 bits(1.0) - bits(d) (relative error at most 1/8), then three
-// Newton steps y <- y (2 - d y) (error squares each step: 1/8 -> 1.6e-2 -> 2.4e-4 -> 6e-8).
-// z is clamped at -80 so that d stays finite; the result then is below 2e-35.
+// the integer seed y0 = bits(0x7EF311C0) - bits(d), a line in log2 space whose offset minimises
+// the largest relative error over a binade (0.0505, found by a search over the offsets), then
+// one Newton step y <- y (1 + e), e = 1 - d y (error squared: 2.6e-3) and one third-order step
+// y <- y (1 + e + e^2) (error cubed: 1.7e-8; 1.1e-7 after the binary32 roundings, measured over
+// a binade) -- five FMA-pipe operations.  z is clamped at -80 so that d stays finite; the
+// result then is below 2e-35.
+// 2^x on the special-function unit with subnormal results flushed (one instruction; the
+// exponential here is only ever added to 1).
+__device__ __forceinline__ float ex2_ftz(float x)
+{
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
 __device__ __forceinline__ float logistic(float z)
 {
-    const float d = 1.0f + __expf(-fmaxf(z, -80.0f));
-    float y = __int_as_float(0x7F000000 - __float_as_int(d));
-#pragma unroll
-    for (int k = 0; k < 3; ++k) y = fmaf(y, fmaf(-d, y, 1.0f), y);
-    return y;
+    const float d = 1.0f + ex2_ftz(fmaxf(z, -80.0f) * -1.44269504088896341f);
+    float y = __int_as_float(0x7EF311C0 - __float_as_int(d));
+    y = fmaf(y, fmaf(-d, y, 1.0f), y);
+    const float e = fmaf(-d, y, 1.0f);
+    return fmaf(y, fmaf(e, e, e), y);
 }
 // The training epilogues (more stores per element, MUFU pipe not the limit) use the
 // special-function reciprocal instead: both forms agree to ~1e-7 relative.
@@ -681,6 +692,328 @@ bool persistent_shape(const GemmArgs& g)
     return (g.N == 128 || g.N == 256) && (kc == 1 || kc == 2 || kc == 4);
 }
 
+// ---------------------------------------------------------------- fused inference pass
+// One persistent CTA per SM walks the 128-row tiles t = blockIdx.x, blockIdx.x + gridDim.x, ...
+// and takes each through the three hidden layers and the head without leaving the SM:
+//   * the tile's input rows X (KC1 chunks of 64 columns) arrive by TMA into their own buffer;
+//   * the weights (W1, then W2, then W3, 32 KB chunks of 64 input columns x 256 units, read from
+//     L2) stream through a kFStages-deep ring, the same sequence for every tile;
+//   * a layer's accumulator (128 x 256 FP32) lives in one of two TMEM regions; layers alternate
+//     between them (layer counter j, region j & 1), so a layer's epilogue drains one region
+//     while the next layer's MMAs fill the other;
+//   * the epilogue writes the layer's activations as BF16 into the H buffer (128 rows x 256, the
+//     K-major 128-byte-swizzled layout a TMA load would have written, four 16 KB chunks) and
+//     signals each 64-column chunk on its own mbarrier, so the next layer's MMAs start on a chunk
+//     as soon as it is written.  Epilogue slice s (four warps, one per TMEM lane quarter) owns
+//     chunk s; four slices keep four epilogue warps on each SM sub-partition, enough to cover
+//     the TMEM-load and special-function latencies of the epilogue.
+// H is rewritten only by a layer's epilogue, after that layer's MMAs (the last readers of the
+// previous activations) have completed.  The head epilogue forms y = silu(z3) . w4 + b as the
+// kHead epilogue does.  Barriers: x_full / x_empty, w_full / w_empty per ring stage, acc_full /
+// acc_empty per TMEM region, h_ready per H chunk, drain.  Every wait is bounded as in
+// gemm_persistent_kernel.
+constexpr uint32_t kFStages = 3;
+constexpr uint32_t kFEpiWarps = 16; // four per TMEM lane quarter, one 64-column chunk each
+constexpr uint32_t kFThreads = 64 + 32 * kFEpiWarps;
+constexpr uint32_t kWChunk = 256u * 128u; // 64 input columns x 256 units, BF16
+constexpr uint32_t kHChunk = 128u * 128u; // 128 rows x 64 columns, BF16
+constexpr uint32_t kFExtra = 8192;        // barriers, TMEM slot, abort flag, biases, head, partial sums
+template <int KC1> constexpr size_t fsmem_bytes()
+{
+    return 1024 + (size_t)KC1 * kHChunk + 4 * kHChunk + kFStages * kWChunk + kFExtra;
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+
+// One 64-column chunk of this thread's accumulator row through bias + SiLU into BF16, stored in
+// row `row` of a swizzled H chunk: 16-byte piece p of the row at ((p ^ (row & 7)) << 4).
+// 32 columns per TMEM load keep the epilogue within the 96 registers that 18 warps per SM allow.
+__device__ __forceinline__ void hidden_chunk(uint32_t taddr, const float* bias, uint8_t* hrow, uint32_t row)
+{
+#pragma unroll
+    for (uint32_t h = 0; h < 2; ++h) {
+        float v[32];
+        umma::tmem_ld32(taddr + 32u * h, v);
+#pragma unroll
+        for (uint32_t q = 0; q < 4; ++q) {
+            const float4 b0 = *reinterpret_cast<const float4*>(bias + 32u * h + 8u * q);
+            const float4 b1 = *reinterpret_cast<const float4*>(bias + 32u * h + 8u * q + 4u);
+            const float bb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+            uint32_t w[4];
+#pragma unroll
+            for (uint32_t i = 0; i < 4; ++i) {
+                const float a = silu<true>(v[8 * q + 2 * i] + bb[2 * i]);
+                const float c = silu<true>(v[8 * q + 2 * i + 1] + bb[2 * i + 1]);
+                const __nv_bfloat162 p = __floats2bfloat162_rn(a, c);
+                w[i] = *reinterpret_cast<const uint32_t*>(&p);
+            }
+            const uint32_t piece = 4u * h + q;
+            *reinterpret_cast<uint4*>(hrow + ((piece ^ (row & 7u)) << 4)) = make_uint4(w[0], w[1], w[2], w[3]);
+        }
+    }
+}
+
+// Partial head sum of one 64-column chunk: sum silu(acc + bias) * head_w.
+__device__ __forceinline__ float head_chunk(uint32_t taddr, const float* bias, const float* head_w, float y)
+{
+#pragma unroll
+    for (uint32_t h = 0; h < 2; ++h) {
+        float vv[32];
+        umma::tmem_ld32(taddr + 32u * h, vv);
+#pragma unroll
+        for (uint32_t q = 0; q < 8; ++q) {
+            const float4 b = *reinterpret_cast<const float4*>(bias + 32u * h + 4u * q);
+            const float4 w = *reinterpret_cast<const float4*>(head_w + 32u * h + 4u * q);
+            y = fmaf(silu<true>(vv[4 * q] + b.x), w.x, y);
+            y = fmaf(silu<true>(vv[4 * q + 1] + b.y), w.y, y);
+            y = fmaf(silu<true>(vv[4 * q + 2] + b.z), w.z, y);
+            y = fmaf(silu<true>(vv[4 * q + 3] + b.w), w.w, y);
+        }
+    }
+    return y;
+}
+
+__device__ __forceinline__ void fused_head_store(const FusedArgs& f, uint32_t m, float yacc)
+{
+    const float y = yacc + f.head_b;
+    if (f.out_y) f.out_y[m] = y;
+    if (f.out_mass) {
+        double e = exp((double)y);
+        f.out_mass[m] = e;
+        if (f.out_mass_sum) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+            if ((threadIdx.x & 31u) == 0) atomicAdd(&f.out_mass_sum[m / f.record_rows], e);
+        }
+    }
+}
+
+template <int KC1>
+__global__ void __launch_bounds__(kFThreads, 1)
+    mlp_fused_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmW1,
+                     const __grid_constant__ CUtensorMap tmW2, const __grid_constant__ CUtensorMap tmW3,
+                     const FusedArgs f)
+{
+    constexpr uint32_t S = kFStages;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* xbuf = smem;
+    uint8_t* hbuf = xbuf + KC1 * kHChunk;
+    uint8_t* ring = hbuf + 4 * kHChunk;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(ring + S * kWChunk);
+    uint64_t* x_full = bars;
+    uint64_t* x_empty = bars + 1;
+    uint64_t* w_full = bars + 2;
+    uint64_t* w_empty = w_full + S;
+    uint64_t* acc_full = w_empty + S;
+    uint64_t* acc_empty = acc_full + 2;
+    uint64_t* h_ready = acc_empty + 2;
+    uint64_t* drain = h_ready + 4;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(drain + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
+    float* sb = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(bars) + 1024); // b1, b2, b3, head_w
+    float* ypart = sb + 4 * 256;                                                     // [3][128]
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t tiles = f.M / 128u;
+
+    if (threadIdx.x == 0) {
+        umma::mbar_init(x_full, 1);
+        umma::mbar_init(x_empty, 1);
+        for (uint32_t s = 0; s < S; ++s) {
+            umma::mbar_init(&w_full[s], 1);
+            umma::mbar_init(&w_empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            umma::mbar_init(&acc_full[b], 1);
+            umma::mbar_init(&acc_empty[b], kFEpiWarps);
+        }
+        for (int c = 0; c < 4; ++c) umma::mbar_init(&h_ready[c], 4);
+        umma::mbar_init(drain, 1);
+        *abort_flag = 0;
+        umma::mbar_fence_init();
+    }
+    for (uint32_t i = threadIdx.x; i < 256u; i += blockDim.x) {
+        sb[i] = f.b1[i];
+        sb[256 + i] = f.b2[i];
+        sb[512 + i] = f.b3[i];
+        sb[768 + i] = f.head_w[i];
+    }
+    if (warp == 1) umma::tmem_alloc(tslot, 512u);
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = *tslot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // producer: per tile the input rows, then the weight chunks of the three layers
+            bool ok = true;
+            uint32_t it = 0, xi = 0; // weight chunks and input tiles issued
+#pragma unroll 1
+            for (uint32_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+                if (xi >= 1 && !umma::mbar_wait(x_empty, (xi - 1u) & 1u, kWaitLimit)) {
+                    ok = false;
+                    break;
+                }
+                ++xi;
+                umma::mbar_arrive_expect_tx(x_full, KC1 * kHChunk);
+                for (int kc = 0; kc < KC1; ++kc)
+                    umma::tma_load_2d(xbuf + kc * kHChunk, &tmX, x_full, kc * 64, (int32_t)(t * 128u));
+#pragma unroll 1
+                for (uint32_t l = 0; l < 3 && ok; ++l) {
+                    const uint32_t n = l == 0 ? (uint32_t)KC1 : 4u;
+                    for (uint32_t jj = 0; jj < n; ++jj, ++it) {
+                        const uint32_t kc = jj;
+                        const uint32_t s = it % S;
+                        if (it >= S && !umma::mbar_wait(&w_empty[s], ((it / S) & 1u) ^ 1u, kWaitLimit)) {
+                            ok = false;
+                            break;
+                        }
+                        if (*abort_flag) {
+                            ok = false;
+                            break;
+                        }
+                        const CUtensorMap* map = l == 0 ? &tmW1 : (l == 1 ? &tmW2 : &tmW3);
+                        umma::mbar_arrive_expect_tx(&w_full[s], kWChunk);
+                        umma::tma_load_2d(ring + s * kWChunk, map, &w_full[s], (int32_t)(kc * 64u), 0);
+                    }
+                }
+            }
+            if (!ok) {
+                *abort_flag = 1;
+                atomicExch(f.error, 3u);
+            }
+            // every issued load lands before the CTA's shared memory is released (at most one
+            // input tile is in flight: the next is loaded only after the last was consumed)
+            for (uint32_t j = it > S ? it - S : 0u; j < it; ++j) umma::mbar_wait(&w_full[j % S], (j / S) & 1u, kWaitLimit);
+            if (xi) umma::mbar_wait(x_full, (xi - 1u) & 1u, kWaitLimit);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // MMA issuer
+            const uint32_t idesc = umma::instr_desc_bf16_f32(128, 256);
+            bool ok = true;
+            uint32_t it = 0, i = 0, j = 0;
+#pragma unroll 1
+            for (uint32_t t = blockIdx.x; t < tiles && ok; t += gridDim.x, ++i) {
+#pragma unroll 1
+                for (uint32_t l = 0; l < 3 && ok; ++l, ++j) {
+                    const uint32_t r = j & 1u;
+                    if (j >= 2 && !umma::mbar_wait(&acc_empty[r], ((j >> 1) - 1u) & 1u, kWaitLimit)) {
+                        ok = false;
+                        break;
+                    }
+                    if (l == 0 && !umma::mbar_wait(x_full, i & 1u, kWaitLimit)) {
+                        ok = false;
+                        break;
+                    }
+                    umma::fence_after_sync();
+                    const uint32_t d = tmem + r * 256u;
+                    const uint32_t n = l == 0 ? (uint32_t)KC1 : 4u;
+                    for (uint32_t jj = 0; jj < n; ++jj, ++it) {
+                        const uint32_t kc = jj;
+                        const uint32_t s = it % S;
+                        // layer l > 0 reads H chunk kc of the previous layer: phase 2 i + l - 1
+                        if (l > 0 && !umma::mbar_wait(&h_ready[kc], (2u * i + l - 1u) & 1u, kWaitLimit)) {
+                            ok = false;
+                            break;
+                        }
+                        if (!umma::mbar_wait(&w_full[s], (it / S) & 1u, kWaitLimit) || *abort_flag) {
+                            ok = false;
+                            break;
+                        }
+                        umma::fence_after_sync();
+                        const uint32_t a = umma::smem_u32((l == 0 ? xbuf : hbuf) + kc * kHChunk);
+                        const uint32_t b = umma::smem_u32(ring + s * kWChunk);
+#pragma unroll
+                        for (uint32_t k = 0; k < 4; ++k)
+                            umma::mma_bf16(d, umma::smem_desc_sw128(a + 32u * k), umma::smem_desc_sw128(b + 32u * k),
+                                           idesc, jj > 0 || k > 0);
+                        umma::mma_commit(&w_empty[s]);
+                    }
+                    if (!ok) break;
+                    if (l == 0) umma::mma_commit(x_empty);
+                    umma::mma_commit(&acc_full[r]);
+                }
+            }
+            if (!ok) {
+                *abort_flag = 1;
+                atomicExch(f.error, 4u);
+            }
+            umma::mma_commit(drain);
+            if (!umma::mbar_wait(drain, 0, kWaitLimit)) atomicExch(f.error, 6u);
+        }
+    } else {
+        // epilogue warps: lane quarter q (TMEM lanes 32 q ..), 64-column chunk `slice`
+        const uint32_t q = warp & 3u, slice = (warp - 2u) >> 2;
+        const uint32_t row = 32u * q + lane;
+        uint32_t j = 0;
+        bool live = true;
+#pragma unroll 1
+        for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+#pragma unroll 1
+            for (uint32_t l = 0; l < 3; ++l, ++j) {
+                const uint32_t r = j & 1u;
+                const bool mine = live && umma::mbar_wait(&acc_full[r], (j >> 1) & 1u, kWaitLimit);
+                if (!__all_sync(0xffffffffu, mine && !*abort_flag)) {
+                    if (lane == 0 && live) {
+                        *abort_flag = 1;
+                        atomicExch(f.error, 5u);
+                    }
+                    live = false;
+                }
+                const uint32_t taddr = tmem + ((32u * q) << 16) + r * 256u;
+                float y = 0.0f;
+                if (live) {
+                    umma::fence_after_sync();
+                    const uint32_t c = 64u * slice;
+                    if (l < 2) {
+                        hidden_chunk(taddr + c, sb + 256u * l + c, hbuf + slice * kHChunk + row * 128u, row);
+                        fence_proxy_async_smem();
+                        __syncwarp();
+                        if (lane == 0) umma::mbar_arrive(&h_ready[slice]);
+                    } else {
+                        y = head_chunk(taddr + c, sb + 512u + c, sb + 768u + c, y);
+                    }
+                    umma::fence_before_sync();
+                    __syncwarp();
+                    if (lane == 0) umma::mbar_arrive(&acc_empty[r]);
+                }
+                if (l == 2) {
+                    // the four slices of a lane quarter meet here every tile (also after an abort,
+                    // so that the named barrier never waits for a warp that has left the loop)
+                    if (slice) ypart[(slice - 1u) * 128u + row] = y;
+                    named_sync(1u + q, 128u);
+                    if (slice == 0 && live)
+                        fused_head_store(f, t * 128u + row, ((y + ypart[row]) + ypart[128u + row]) + ypart[256u + row]);
+                    named_sync(1u + q, 128u);
+                }
+            }
+        }
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 1) umma::tmem_dealloc(tmem, 512u);
+}
+
+template <int KC1>
+int launch_fused(const void* X, const void* W1, const void* W2, const void* W3, const FusedArgs& f, cudaStream_t st)
+{
+    CUtensorMap tx, t1, t2, t3;
+    if (make_map(&tx, X, f.M, f.K0, 128u) || make_map(&t1, W1, 256u, f.K0, 256u) || make_map(&t2, W2, 256u, 256u, 256u) ||
+        make_map(&t3, W3, 256u, 256u, 256u))
+        return -1;
+    const size_t smem = fsmem_bytes<KC1>();
+    cudaError_t e =
+        cudaFuncSetAttribute(mlp_fused_kernel<KC1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return (int)e;
+    const uint32_t tiles = f.M / 128u;
+    const uint32_t grid = tiles < (uint32_t)sm_count() ? tiles : (uint32_t)sm_count();
+    mlp_fused_kernel<KC1><<<grid, kFThreads, smem, st>>>(tx, t1, t2, t3, f);
+    return (int)cudaGetLastError();
+}
+
 } // namespace
 
 int gemm(const void* A, const void* B, GemmArgs g, int epi, uint32_t splits, cudaStream_t st)
@@ -711,6 +1044,15 @@ int gemm(const void* A, const void* B, GemmArgs g, int epi, uint32_t splits, cud
     case kBackprop: return launch_epi<kBackprop>(A, B, g, 1, st);
     default: return -4;
     }
+}
+
+bool fused_shape(uint32_t K0, uint32_t H) { return H == 256u && (K0 == 64u || K0 == 128u); }
+
+int forward_fused(const void* X, const void* W1, const void* W2, const void* W3, const FusedArgs& f,
+                  cudaStream_t st)
+{
+    if (f.M == 0 || f.M % 128u || !fused_shape(f.K0, 256u)) return -3;
+    return f.K0 == 64u ? launch_fused<1>(X, W1, W2, W3, f, st) : launch_fused<2>(X, W1, W2, W3, f, st);
 }
 
 } // namespace icp::mlp
