@@ -693,26 +693,25 @@ bool persistent_shape(const GemmArgs& g)
 }
 
 // ---------------------------------------------------------------- fused inference pass
-// One persistent CTA per SM walks the 128-row tiles t = blockIdx.x, blockIdx.x + gridDim.x, ...
-// and takes each through the three hidden layers and the head without leaving the SM:
-//   * the tile's input rows X (KC1 chunks of 64 columns) arrive by TMA into their own buffer;
-//   * the weights (W1, then W2, then W3, 32 KB chunks of 64 input columns x 256 units, read from
-//     L2) stream through a kFStages-deep ring, the same sequence for every tile;
-//   * a layer's accumulator (128 x 256 FP32) lives in one of two TMEM regions; layers alternate
-//     between them (layer counter j, region j & 1), so a layer's epilogue drains one region
-//     while the next layer's MMAs fill the other;
-//   * the epilogue writes the layer's activations as BF16 into the H buffer (128 rows x 256, the
-//     K-major 128-byte-swizzled layout a TMA load would have written, four 16 KB chunks) and
-//     signals each 64-column chunk on its own mbarrier, so the next layer's MMAs start on a chunk
-//     as soon as it is written.  Epilogue slice s (four warps, one per TMEM lane quarter) owns
-//     chunk s; four slices keep four epilogue warps on each SM sub-partition, enough to cover
-//     the TMEM-load and special-function latencies of the epilogue.
-// H is rewritten only by a layer's epilogue, after that layer's MMAs (the last readers of the
-// previous activations) have completed.  The head epilogue forms y = silu(z3) . w4 + b as the
-// kHead epilogue does.  Barriers: x_full / x_empty, w_full / w_empty per ring stage, acc_full /
-// acc_empty per TMEM region, h_ready per H chunk, drain.  Every wait is bounded as in
-// gemm_persistent_kernel.
-constexpr uint32_t kFStages = 3;
+// One persistent CTA per SM takes its 128-row tiles (t = blockIdx.x, blockIdx.x + gridDim.x, ...)
+// two at a time, in slots 0 and 1, through the three hidden layers and the head without leaving
+// the SM.  Each slot owns a TMEM region (its 128 x 256 FP32 accumulator) and an H buffer (its
+// activations as BF16, 128 rows x 256 in the K-major 128-byte-swizzled layout a TMA load would
+// have written, four 16 KB chunks).  The MMA thread issues (layer, slot) in the order
+// (0, 0), (0, 1), (1, 0), (1, 1), (2, 0), (2, 1), so the tensor pipe computes one slot's layer while
+// the epilogue warps drain the other slot's previous layer: a tile's own layers are serial (each
+// needs the previous one's activations), the two tiles of a pair overlap.
+//   * A tile's input rows X (KC1 chunks of 64 columns) arrive by TMA in the first chunks of its
+//     slot's H buffer, once the slot's previous tile has finished its last layer (h_free).
+//   * The weights (W1, W2, W3 in 32 KB chunks of 64 input columns x 256 units, read from L2) go
+//     through a kFStages-deep ring in the MMA order, once per (layer, slot).
+//   * The epilogue (sixteen warps: lane quarter q, 64-column chunk s) writes a layer's activations
+//     into the slot's H buffer, fences them for the tensor core's reads and arrives on the slot's
+//     acc_empty: the slot's next layer may then overwrite the accumulator and read H.  The head
+//     epilogue forms y = silu(z3) . w4 + b as the kHead epilogue does.
+// Barriers per slot: x_full, h_free, acc_full, acc_empty; per ring stage: w_full, w_empty; drain.
+// Every wait is bounded as in gemm_persistent_kernel.
+constexpr uint32_t kFStages = 2;
 constexpr uint32_t kFEpiWarps = 16; // four per TMEM lane quarter, one 64-column chunk each
 constexpr uint32_t kFThreads = 64 + 32 * kFEpiWarps;
 constexpr uint32_t kWChunk = 256u * 128u; // 64 input columns x 256 units, BF16
@@ -720,7 +719,7 @@ constexpr uint32_t kHChunk = 128u * 128u; // 128 rows x 64 columns, BF16
 constexpr uint32_t kFExtra = 8192;        // barriers, TMEM slot, abort flag, biases, head, partial sums
 template <int KC1> constexpr size_t fsmem_bytes()
 {
-    return 1024 + (size_t)KC1 * kHChunk + 4 * kHChunk + kFStages * kWChunk + kFExtra;
+    return 1024 + 2 * 4 * kHChunk + kFStages * kWChunk + kFExtra;
 }
 
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
@@ -798,37 +797,38 @@ __global__ void __launch_bounds__(kFThreads, 1)
     constexpr uint32_t S = kFStages;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint8_t* xbuf = smem;
-    uint8_t* hbuf = xbuf + KC1 * kHChunk;
-    uint8_t* ring = hbuf + 4 * kHChunk;
+    uint8_t* hbuf = smem; // slot s at hbuf + s * 4 kHChunk; its input rows in chunks [0, KC1)
+    uint8_t* ring = hbuf + 2 * 4 * kHChunk;
     uint64_t* bars = reinterpret_cast<uint64_t*>(ring + S * kWChunk);
-    uint64_t* x_full = bars;
-    uint64_t* x_empty = bars + 1;
-    uint64_t* w_full = bars + 2;
-    uint64_t* w_empty = w_full + S;
-    uint64_t* acc_full = w_empty + S;
-    uint64_t* acc_empty = acc_full + 2;
-    uint64_t* h_ready = acc_empty + 2;
-    uint64_t* drain = h_ready + 4;
+    uint64_t* x_full = bars;         // [2]
+    uint64_t* h_free = bars + 2;     // [2]
+    uint64_t* acc_full = bars + 4;   // [2]
+    uint64_t* acc_empty = bars + 6;  // [2]
+    uint64_t* w_full = bars + 8;     // [S]
+    uint64_t* w_empty = w_full + S;  // [S]
+    uint64_t* drain = w_empty + S;
     uint32_t* tslot = reinterpret_cast<uint32_t*>(drain + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
     float* sb = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(bars) + 1024); // b1, b2, b3, head_w
     float* ypart = sb + 4 * 256;                                                     // [3][128]
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t tiles = f.M / 128u;
+    // this CTA's tiles: t_k = blockIdx.x + k gridDim.x, k < mine; pair p holds k = 2p (slot 0)
+    // and k = 2p + 1 (slot 1, absent in a last pair of an odd count)
+    const uint32_t mine = blockIdx.x < tiles ? (tiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0u;
+    const uint32_t pairs = (mine + 1u) / 2u;
 
     if (threadIdx.x == 0) {
-        umma::mbar_init(x_full, 1);
-        umma::mbar_init(x_empty, 1);
+        for (int s = 0; s < 2; ++s) {
+            umma::mbar_init(&x_full[s], 1);
+            umma::mbar_init(&h_free[s], 1);
+            umma::mbar_init(&acc_full[s], 1);
+            umma::mbar_init(&acc_empty[s], kFEpiWarps);
+        }
         for (uint32_t s = 0; s < S; ++s) {
             umma::mbar_init(&w_full[s], 1);
             umma::mbar_init(&w_empty[s], 1);
         }
-        for (int b = 0; b < 2; ++b) {
-            umma::mbar_init(&acc_full[b], 1);
-            umma::mbar_init(&acc_empty[b], kFEpiWarps);
-        }
-        for (int c = 0; c < 4; ++c) umma::mbar_init(&h_ready[c], 4);
         umma::mbar_init(drain, 1);
         *abort_flag = 0;
         umma::mbar_fence_init();
@@ -847,36 +847,45 @@ __global__ void __launch_bounds__(kFThreads, 1)
 
     if (warp == 0) {
         if (lane == 0) {
-            // producer: per tile the input rows, then the weight chunks of the three layers
+            // producer, in the MMA order: per (layer, slot) the slot's input rows (layer 0) and
+            // the layer's weight chunks
             bool ok = true;
-            uint32_t it = 0, xi = 0; // weight chunks and input tiles issued
+            uint32_t it = 0, xi[2] = {0u, 0u}; // weight chunks and input tiles per slot issued
 #pragma unroll 1
-            for (uint32_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
-                if (xi >= 1 && !umma::mbar_wait(x_empty, (xi - 1u) & 1u, kWaitLimit)) {
-                    ok = false;
-                    break;
-                }
-                ++xi;
-                umma::mbar_arrive_expect_tx(x_full, KC1 * kHChunk);
-                for (int kc = 0; kc < KC1; ++kc)
-                    umma::tma_load_2d(xbuf + kc * kHChunk, &tmX, x_full, kc * 64, (int32_t)(t * 128u));
+            for (uint32_t p = 0; p < pairs && ok; ++p) {
 #pragma unroll 1
                 for (uint32_t l = 0; l < 3 && ok; ++l) {
-                    const uint32_t n = l == 0 ? (uint32_t)KC1 : 4u;
-                    for (uint32_t jj = 0; jj < n; ++jj, ++it) {
-                        const uint32_t kc = jj;
-                        const uint32_t s = it % S;
-                        if (it >= S && !umma::mbar_wait(&w_empty[s], ((it / S) & 1u) ^ 1u, kWaitLimit)) {
-                            ok = false;
-                            break;
+#pragma unroll 1
+                    for (uint32_t sl = 0; sl < 2 && ok; ++sl) {
+                        const uint32_t k = 2u * p + sl;
+                        if (k >= mine) break;
+                        if (l == 0) {
+                            if (xi[sl] >= 1 && !umma::mbar_wait(&h_free[sl], (xi[sl] - 1u) & 1u, kWaitLimit)) {
+                                ok = false;
+                                break;
+                            }
+                            ++xi[sl];
+                            const uint32_t t = blockIdx.x + k * gridDim.x;
+                            umma::mbar_arrive_expect_tx(&x_full[sl], KC1 * kHChunk);
+                            for (int kc = 0; kc < KC1; ++kc)
+                                umma::tma_load_2d(hbuf + (sl * 4u + kc) * kHChunk, &tmX, &x_full[sl], kc * 64,
+                                                  (int32_t)(t * 128u));
                         }
-                        if (*abort_flag) {
-                            ok = false;
-                            break;
-                        }
+                        const uint32_t n = l == 0 ? (uint32_t)KC1 : 4u;
                         const CUtensorMap* map = l == 0 ? &tmW1 : (l == 1 ? &tmW2 : &tmW3);
-                        umma::mbar_arrive_expect_tx(&w_full[s], kWChunk);
-                        umma::tma_load_2d(ring + s * kWChunk, map, &w_full[s], (int32_t)(kc * 64u), 0);
+                        for (uint32_t kc = 0; kc < n; ++kc, ++it) {
+                            const uint32_t s = it % S;
+                            if (it >= S && !umma::mbar_wait(&w_empty[s], ((it / S) & 1u) ^ 1u, kWaitLimit)) {
+                                ok = false;
+                                break;
+                            }
+                            if (*abort_flag) {
+                                ok = false;
+                                break;
+                            }
+                            umma::mbar_arrive_expect_tx(&w_full[s], kWChunk);
+                            umma::tma_load_2d(ring + s * kWChunk, map, &w_full[s], (int32_t)(kc * 64u), 0);
+                        }
                     }
                 }
             }
@@ -885,56 +894,58 @@ __global__ void __launch_bounds__(kFThreads, 1)
                 atomicExch(f.error, 3u);
             }
             // every issued load lands before the CTA's shared memory is released (at most one
-            // input tile is in flight: the next is loaded only after the last was consumed)
+            // input tile per slot is in flight)
             for (uint32_t j = it > S ? it - S : 0u; j < it; ++j) umma::mbar_wait(&w_full[j % S], (j / S) & 1u, kWaitLimit);
-            if (xi) umma::mbar_wait(x_full, (xi - 1u) & 1u, kWaitLimit);
+            for (int sl = 0; sl < 2; ++sl)
+                if (xi[sl]) umma::mbar_wait(&x_full[sl], (xi[sl] - 1u) & 1u, kWaitLimit);
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            // MMA issuer
+            // MMA issuer: (layer, slot) in the order above.  Layer l of a slot's tile n waits for
+            // completion 3 n + l - 1 of the slot's acc_empty (its previous layer drained and its
+            // activations written; for l = 0 the previous tile's head), and layer 0 for the rows.
             const uint32_t idesc = umma::instr_desc_bf16_f32(128, 256);
             bool ok = true;
-            uint32_t it = 0, i = 0, j = 0;
+            uint32_t it = 0;
 #pragma unroll 1
-            for (uint32_t t = blockIdx.x; t < tiles && ok; t += gridDim.x, ++i) {
+            for (uint32_t p = 0; p < pairs && ok; ++p) {
 #pragma unroll 1
-                for (uint32_t l = 0; l < 3 && ok; ++l, ++j) {
-                    const uint32_t r = j & 1u;
-                    if (j >= 2 && !umma::mbar_wait(&acc_empty[r], ((j >> 1) - 1u) & 1u, kWaitLimit)) {
-                        ok = false;
-                        break;
-                    }
-                    if (l == 0 && !umma::mbar_wait(x_full, i & 1u, kWaitLimit)) {
-                        ok = false;
-                        break;
-                    }
-                    umma::fence_after_sync();
-                    const uint32_t d = tmem + r * 256u;
-                    const uint32_t n = l == 0 ? (uint32_t)KC1 : 4u;
-                    for (uint32_t jj = 0; jj < n; ++jj, ++it) {
-                        const uint32_t kc = jj;
-                        const uint32_t s = it % S;
-                        // layer l > 0 reads H chunk kc of the previous layer: phase 2 i + l - 1
-                        if (l > 0 && !umma::mbar_wait(&h_ready[kc], (2u * i + l - 1u) & 1u, kWaitLimit)) {
+                for (uint32_t l = 0; l < 3 && ok; ++l) {
+#pragma unroll 1
+                    for (uint32_t sl = 0; sl < 2 && ok; ++sl) {
+                        const uint32_t k = 2u * p + sl;
+                        if (k >= mine) break;
+                        const uint32_t c = 3u * p + l; // this layer's index among the slot's layers
+                        if (c >= 1 && !umma::mbar_wait(&acc_empty[sl], (c - 1u) & 1u, kWaitLimit)) {
                             ok = false;
                             break;
                         }
-                        if (!umma::mbar_wait(&w_full[s], (it / S) & 1u, kWaitLimit) || *abort_flag) {
+                        if (l == 0 && !umma::mbar_wait(&x_full[sl], p & 1u, kWaitLimit)) {
                             ok = false;
                             break;
                         }
                         umma::fence_after_sync();
-                        const uint32_t a = umma::smem_u32((l == 0 ? xbuf : hbuf) + kc * kHChunk);
-                        const uint32_t b = umma::smem_u32(ring + s * kWChunk);
+                        const uint32_t d = tmem + sl * 256u;
+                        const uint32_t n = l == 0 ? (uint32_t)KC1 : 4u;
+                        for (uint32_t kc = 0; kc < n; ++kc, ++it) {
+                            const uint32_t s = it % S;
+                            if (!umma::mbar_wait(&w_full[s], (it / S) & 1u, kWaitLimit) || *abort_flag) {
+                                ok = false;
+                                break;
+                            }
+                            umma::fence_after_sync();
+                            const uint32_t a = umma::smem_u32(hbuf + (sl * 4u + kc) * kHChunk);
+                            const uint32_t b = umma::smem_u32(ring + s * kWChunk);
 #pragma unroll
-                        for (uint32_t k = 0; k < 4; ++k)
-                            umma::mma_bf16(d, umma::smem_desc_sw128(a + 32u * k), umma::smem_desc_sw128(b + 32u * k),
-                                           idesc, jj > 0 || k > 0);
-                        umma::mma_commit(&w_empty[s]);
+                            for (uint32_t q = 0; q < 4; ++q)
+                                umma::mma_bf16(d, umma::smem_desc_sw128(a + 32u * q), umma::smem_desc_sw128(b + 32u * q),
+                                               idesc, kc > 0 || q > 0);
+                            umma::mma_commit(&w_empty[s]);
+                        }
+                        if (!ok) break;
+                        if (l == 2) umma::mma_commit(&h_free[sl]);
+                        umma::mma_commit(&acc_full[sl]);
                     }
-                    if (!ok) break;
-                    if (l == 0) umma::mma_commit(x_empty);
-                    umma::mma_commit(&acc_full[r]);
                 }
             }
             if (!ok) {
@@ -947,47 +958,49 @@ __global__ void __launch_bounds__(kFThreads, 1)
     } else {
         // epilogue warps: lane quarter q (TMEM lanes 32 q ..), 64-column chunk `slice`
         const uint32_t q = warp & 3u, slice = (warp - 2u) >> 2;
-        const uint32_t row = 32u * q + lane;
-        uint32_t j = 0;
+        const uint32_t row = 32u * q + lane, c = 64u * slice;
         bool live = true;
 #pragma unroll 1
-        for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+        for (uint32_t p = 0; p < pairs; ++p) {
 #pragma unroll 1
-            for (uint32_t l = 0; l < 3; ++l, ++j) {
-                const uint32_t r = j & 1u;
-                const bool mine = live && umma::mbar_wait(&acc_full[r], (j >> 1) & 1u, kWaitLimit);
-                if (!__all_sync(0xffffffffu, mine && !*abort_flag)) {
-                    if (lane == 0 && live) {
-                        *abort_flag = 1;
-                        atomicExch(f.error, 5u);
+            for (uint32_t l = 0; l < 3; ++l) {
+#pragma unroll 1
+                for (uint32_t sl = 0; sl < 2; ++sl) {
+                    const uint32_t k = 2u * p + sl;
+                    if (k >= mine) break;
+                    const uint32_t n = 3u * p + l;
+                    const bool ready = live && umma::mbar_wait(&acc_full[sl], n & 1u, kWaitLimit);
+                    if (!__all_sync(0xffffffffu, ready && !*abort_flag)) {
+                        if (lane == 0 && live) {
+                            *abort_flag = 1;
+                            atomicExch(f.error, 5u);
+                        }
+                        live = false;
                     }
-                    live = false;
-                }
-                const uint32_t taddr = tmem + ((32u * q) << 16) + r * 256u;
-                float y = 0.0f;
-                if (live) {
-                    umma::fence_after_sync();
-                    const uint32_t c = 64u * slice;
-                    if (l < 2) {
-                        hidden_chunk(taddr + c, sb + 256u * l + c, hbuf + slice * kHChunk + row * 128u, row);
-                        fence_proxy_async_smem();
+                    const uint32_t taddr = tmem + ((32u * q) << 16) + sl * 256u + c;
+                    float y = 0.0f;
+                    if (live) {
+                        umma::fence_after_sync();
+                        if (l < 2) {
+                            hidden_chunk(taddr, sb + 256u * l + c, hbuf + (sl * 4u + slice) * kHChunk + row * 128u, row);
+                            fence_proxy_async_smem();
+                        } else {
+                            y = head_chunk(taddr, sb + 512u + c, sb + 768u + c, y);
+                        }
+                        umma::fence_before_sync();
                         __syncwarp();
-                        if (lane == 0) umma::mbar_arrive(&h_ready[slice]);
-                    } else {
-                        y = head_chunk(taddr + c, sb + 512u + c, sb + 768u + c, y);
+                        if (lane == 0) umma::mbar_arrive(&acc_empty[sl]);
                     }
-                    umma::fence_before_sync();
-                    __syncwarp();
-                    if (lane == 0) umma::mbar_arrive(&acc_empty[r]);
-                }
-                if (l == 2) {
-                    // the four slices of a lane quarter meet here every tile (also after an abort,
-                    // so that the named barrier never waits for a warp that has left the loop)
-                    if (slice) ypart[(slice - 1u) * 128u + row] = y;
-                    named_sync(1u + q, 128u);
-                    if (slice == 0 && live)
-                        fused_head_store(f, t * 128u + row, ((y + ypart[row]) + ypart[128u + row]) + ypart[256u + row]);
-                    named_sync(1u + q, 128u);
+                    if (l == 2) {
+                        // the four slices of a lane quarter meet here every tile (also after an
+                        // abort, so that the named barrier never waits for a warp that has left)
+                        if (slice) ypart[(slice - 1u) * 128u + row] = y;
+                        named_sync(1u + q, 128u);
+                        if (slice == 0 && live)
+                            fused_head_store(f, (blockIdx.x + k * gridDim.x) * 128u + row,
+                                             ((y + ypart[row]) + ypart[128u + row]) + ypart[256u + row]);
+                        named_sync(1u + q, 128u);
+                    }
                 }
             }
         }
