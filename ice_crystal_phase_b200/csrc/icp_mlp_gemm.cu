@@ -724,6 +724,53 @@ template <int KC1> constexpr size_t fsmem_bytes()
 
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
+// Packed FP32 pairs (sm_100 add / mul / fma .f32x2: one instruction for two lanes of work).
+__device__ __forceinline__ uint64_t pk2(float a, float b)
+{
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void upk2(uint64_t r, float& a, float& b) { asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r)); }
+__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b)
+{
+    uint64_t r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b)
+{
+    uint64_t r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c)
+{
+    uint64_t r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+// silu(a + ba), silu(b + bb) with the arithmetic of logistic() done in pairs, bit for bit: the
+// negated denominator -d = ex2 * -1 - 1 is exact, its seed 0xFEF311C0 - bits(-d) equals
+// 0x7EF311C0 - bits(d), and fma(-d, y, 1) is the same rounding as before.
+__device__ __forceinline__ void silu_pair(float& a, float& b, float ba, float bb)
+{
+    constexpr float kNegLog2e = -1.44269504088896341f;
+    float va, vb;
+    upk2(add2(pk2(a, b), pk2(ba, bb)), va, vb);
+    float xa, xb;
+    upk2(mul2(pk2(fmaxf(va, -80.0f), fmaxf(vb, -80.0f)), pk2(kNegLog2e, kNegLog2e)), xa, xb);
+    const uint64_t m1 = pk2(-1.0f, -1.0f), one = pk2(1.0f, 1.0f);
+    const uint64_t nd = fma2(pk2(ex2_ftz(xa), ex2_ftz(xb)), m1, m1);
+    float da, db;
+    upk2(nd, da, db);
+    uint64_t y = pk2(__int_as_float((int)(0xFEF311C0u - (uint32_t)__float_as_int(da))),
+                     __int_as_float((int)(0xFEF311C0u - (uint32_t)__float_as_int(db))));
+    y = fma2(y, fma2(nd, y, one), y);
+    const uint64_t e = fma2(nd, y, one);
+    upk2(mul2(pk2(va, vb), fma2(y, fma2(e, e, e), y)), a, b);
+}
+
 
 // One 64-column chunk of this thread's accumulator row through bias + SiLU into BF16, stored in
 // row `row` of a swizzled H chunk: 16-byte piece p of the row at ((p ^ (row & 7)) << 4).
@@ -742,8 +789,8 @@ __device__ __forceinline__ void hidden_chunk(uint32_t taddr, const float* bias, 
             uint32_t w[4];
 #pragma unroll
             for (uint32_t i = 0; i < 4; ++i) {
-                const float a = silu<true>(v[8 * q + 2 * i] + bb[2 * i]);
-                const float c = silu<true>(v[8 * q + 2 * i + 1] + bb[2 * i + 1]);
+                float a = v[8 * q + 2 * i], c = v[8 * q + 2 * i + 1];
+                silu_pair(a, c, bb[2 * i], bb[2 * i + 1]);
                 const __nv_bfloat162 p = __floats2bfloat162_rn(a, c);
                 w[i] = *reinterpret_cast<const uint32_t*>(&p);
             }
@@ -764,10 +811,13 @@ __device__ __forceinline__ float head_chunk(uint32_t taddr, const float* bias, c
         for (uint32_t q = 0; q < 8; ++q) {
             const float4 b = *reinterpret_cast<const float4*>(bias + 32u * h + 4u * q);
             const float4 w = *reinterpret_cast<const float4*>(head_w + 32u * h + 4u * q);
-            y = fmaf(silu<true>(vv[4 * q] + b.x), w.x, y);
-            y = fmaf(silu<true>(vv[4 * q + 1] + b.y), w.y, y);
-            y = fmaf(silu<true>(vv[4 * q + 2] + b.z), w.z, y);
-            y = fmaf(silu<true>(vv[4 * q + 3] + b.w), w.w, y);
+            float s0 = vv[4 * q], s1 = vv[4 * q + 1], s2 = vv[4 * q + 2], s3 = vv[4 * q + 3];
+            silu_pair(s0, s1, b.x, b.y);
+            silu_pair(s2, s3, b.z, b.w);
+            y = fmaf(s0, w.x, y);
+            y = fmaf(s1, w.y, y);
+            y = fmaf(s2, w.z, y);
+            y = fmaf(s3, w.w, y);
         }
     }
     return y;
