@@ -135,7 +135,7 @@ struct icp_surrogate {
     uint32_t o_w1 = 0, o_b1 = 0, o_w2 = 0, o_b2 = 0, o_w3 = 0, o_b3 = 0, o_w4 = 0, o_hb = 0;
     Scratch params, grads, adam_m, adam_v, wbf, cells, edges, rec16, loss;
     Scratch X, XT, z1, h1, h1T, z2, h2, h2T, z3, y, dy, dz3, dz3T, dz2, dz2T, dz1T, mass, reports, sync;
-    Scratch mass_sum, dfrac, drows, cellgeo, recgeo;
+    Scratch mass_sum, dfrac, drows, cellgeo, recgeo, xcells;
     std::vector<double> h_edges;
     std::vector<uint16_t> h_rec;
     std::vector<double> h_recgeo;
@@ -143,7 +143,7 @@ struct icp_surrogate {
     {
         Scratch* all[] = {&params, &grads, &adam_m, &adam_v, &wbf, &cells, &edges, &rec16, &loss, &X, &XT, &z1, &h1,
                           &h1T, &z2, &h2, &h2T, &z3, &y, &dy, &dz3, &dz3T, &dz2, &dz2T, &dz1T, &mass, &reports, &sync,
-                          &mass_sum, &dfrac, &drows, &cellgeo, &recgeo};
+                          &mass_sum, &dfrac, &drows, &cellgeo, &recgeo, &xcells};
         for (Scratch* s : all) s->release();
     }
     float* P(uint32_t o) const { return (float*)params.ptr + o; }
@@ -168,8 +168,12 @@ int check_call(icp_surrogate* s, const icp_drop_item* items, uint32_t count)
     return ICP_OK;
 }
 
-// Record feature rows to the device and the feature matrix (XT too when training).
-int enqueue_features(icp_surrogate* s, const icp_drop_item* items, uint32_t count, bool training)
+// Inference runs as one fused kernel that builds its own input rows (mlp::forward_fused).
+bool fused_inference(const icp_surrogate* s) { return mlp::fused_shape(s->K0, s->H); }
+
+// Record feature rows to the device and the feature matrix (XT too when training; no matrix
+// when `rows` is false: the fused inference pass builds the rows itself).
+int enqueue_features(icp_surrogate* s, const icp_drop_item* items, uint32_t count, bool training, bool rows = true)
 {
     icp_context* c = s->c;
     s->h_rec.resize((size_t)16 * count);
@@ -183,10 +187,11 @@ int enqueue_features(icp_surrogate* s, const icp_drop_item* items, uint32_t coun
     const uint64_t M = (uint64_t)count * s->C;
     ICP_CUDA(s->rec16.ensure(32u * s->R));
     ICP_CUDA(s->recgeo.ensure(16u * s->R));
-    ICP_CUDA(s->X.ensure(2 * M * s->K0));
-    if (training) ICP_CUDA(s->XT.ensure(2 * M * s->K0));
     ICP_CUDA(cudaMemcpyAsync(s->rec16.ptr, s->h_rec.data(), 32u * count, cudaMemcpyHostToDevice, c->stream));
     ICP_CUDA(cudaMemcpyAsync(s->recgeo.ptr, s->h_recgeo.data(), 16u * count, cudaMemcpyHostToDevice, c->stream));
+    if (!rows) return ICP_OK;
+    ICP_CUDA(s->X.ensure(2 * M * s->K0));
+    if (training) ICP_CUDA(s->XT.ensure(2 * M * s->K0));
     const int e = mlp::launch_features(as<__nv_bfloat16>(s->rec16), as<__nv_bfloat16>(s->cells), count, s->C, s->K0,
                                        s->cfg.axis_harmonics, as<double>(s->recgeo), as<double>(s->cellgeo),
                                        as<__nv_bfloat16>(s->X), training ? as<__nv_bfloat16>(s->XT) : nullptr,
@@ -223,11 +228,16 @@ int enqueue_forward(icp_surrogate* s, uint32_t count, bool training, float* y_ou
 {
     const uint64_t M = (uint64_t)count * s->C;
     const uint32_t Hn = s->H;
-    if (!training && mlp::fused_shape(s->K0, Hn)) {
-        // inference: the three layers and the head in one kernel, activations kept on chip
+    if (!training && fused_inference(s)) {
+        // inference: input rows, the three layers and the head in one kernel, all kept on chip
         mlp::FusedArgs f{};
         f.M = (uint32_t)M;
         f.K0 = s->K0;
+        f.P = s->cfg.axis_harmonics;
+        f.rec16 = as<__nv_bfloat16>(s->rec16);
+        f.xcells = as<__nv_bfloat16>(s->xcells);
+        f.recgeo = as<double>(s->recgeo);
+        f.cellgeo = as<double>(s->cellgeo);
         f.b1 = s->P(s->o_b1);
         f.b2 = s->P(s->o_b2);
         f.b3 = s->P(s->o_b3);
@@ -238,7 +248,7 @@ int enqueue_forward(icp_surrogate* s, uint32_t count, bool training, float* y_ou
         f.out_mass_sum = mass_sum;
         f.record_rows = s->C;
         f.error = (unsigned*)s->c->mlp_error.ptr;
-        const int e = mlp::forward_fused(s->X.ptr, s->w1b(), s->w2b(), s->w3b(), f, s->c->stream);
+        const int e = mlp::forward_fused(s->w1b(), s->w2b(), s->w3b(), f, s->c->stream);
         count_launch();
         if (e) return fail(ICP_ERR_DEVICE, "surrogate forward launch failed (%d)", e);
         return ICP_OK;
@@ -526,6 +536,14 @@ int icp_surrogate_create(icp_context* c, const icp_surrogate_config* g, icp_surr
     if (e == cudaSuccess) e = s->edges.ensure(sizeof(double) * edges.size());
     if (e == cudaSuccess) e = s->loss.ensure(sizeof(double) * s->R);
     if (e == cudaSuccess) e = cudaMemcpy(s->cells.ptr, both.data(), 2 * both.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && mlp::fused_shape(s->K0, Hn)) {
+        // the cell table in the layout of the input rows (record columns zero), which the fused
+        // inference pass loads by TMA before it writes each row's record and axis columns
+        std::vector<uint16_t> rows((size_t)s->C * s->K0, 0);
+        for (size_t m = 0; m < s->C; ++m) std::memcpy(&rows[m * s->K0 + 16], &cells[m * kc], 2 * kc);
+        e = s->xcells.ensure(2 * rows.size());
+        if (e == cudaSuccess) e = cudaMemcpy(s->xcells.ptr, rows.data(), 2 * rows.size(), cudaMemcpyHostToDevice);
+    }
     if (e == cudaSuccess) e = cudaMemcpy(s->edges.ptr, edges.data(), sizeof(double) * edges.size(), cudaMemcpyHostToDevice);
     s->h_edges = edges;
     // cell geometry of the axis harmonics: cos(theta) and sin(theta) sin(phi), phi the column's
@@ -633,7 +651,7 @@ int icp_surrogate_predict(icp_surrogate* s, const icp_drop_item* items, uint32_t
     ICP_TRY(check_call(s, items, count));
     if (!d_logits) return fail(ICP_ERR_INVALID_ARGUMENT, "surrogate: null output");
     ICP_TRY(begin(s));
-    ICP_TRY(enqueue_features(s, items, count, false));
+    ICP_TRY(enqueue_features(s, items, count, false, !fused_inference(s)));
     ICP_TRY(enqueue_forward(s, count, false, d_logits, nullptr));
     return finish(s->c, "icp_surrogate_predict");
 }
@@ -660,7 +678,7 @@ int icp_surrogate_generate(icp_surrogate* s, const icp_drop_item* items, uint32_
     ICP_CUDA(s->dfrac.ensure(sizeof(double) * s->R * g.nt));
     ICP_CUDA(s->drows.ensure(sizeof(double) * s->R * g.nt));
     ICP_CUDA(cudaMemsetAsync(s->mass_sum.ptr, 0, sizeof(double) * count, c->stream));
-    ICP_TRY(enqueue_features(s, items, count, false));
+    ICP_TRY(enqueue_features(s, items, count, false, !fused_inference(s)));
     ICP_TRY(enqueue_forward(s, count, false, nullptr, as<double>(s->mass), as<double>(s->mass_sum)));
     // the analytic diffraction rows on host threads while the device runs the network
     std::vector<double> frac((size_t)count * g.nt);

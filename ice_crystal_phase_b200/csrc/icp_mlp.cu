@@ -8,6 +8,7 @@
 #include <cstdint>
 
 #include "icp_mlp.h"
+#include "icp_mlp_features.cuh"
 
 namespace icp::mlp {
 
@@ -21,29 +22,6 @@ __device__ __forceinline__ float silu_grad_of(float z)
 {
     const float s = sigmoid_of(z);
     return s * (1.0f + z * (1.0f - s));
-}
-
-// cos psi of one (record, cell) and the Chebyshev values T_k(cos psi), k = k0 .. k0+7, rounded
-// to FP32 then BF16.  Uncontracted FP64 arithmetic (the host restatement repeats it exactly).
-__device__ __forceinline__ double cos_psi(const double* recgeo, const double* cellgeo, uint32_t r, uint32_t c)
-{
-    return __dsub_rn(-__dmul_rn(recgeo[2 * r], cellgeo[2 * c]), __dmul_rn(recgeo[2 * r + 1], cellgeo[2 * c + 1]));
-}
-__device__ __forceinline__ void axis_harmonics8(double x, uint32_t k0, __nv_bfloat16 (&out)[8])
-{
-    double tm = 1.0, t = x; // T_0, T_1
-    for (uint32_t k = 1; k < k0; ++k) {
-        const double tn = __dsub_rn(__dmul_rn(__dmul_rn(2.0, x), t), tm);
-        tm = t;
-        t = tn;
-    }
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        out[i] = __float2bfloat16_rn(__double2float_rn(t));
-        const double tn = __dsub_rn(__dmul_rn(__dmul_rn(2.0, x), t), tm);
-        tm = t;
-        t = tn;
-    }
 }
 
 // X rows: thread per 8 BF16 (one uint4) of a row.

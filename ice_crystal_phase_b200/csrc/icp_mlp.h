@@ -49,12 +49,18 @@ struct GemmArgs {
 // `splits` CTAs per row tile.  Returns 0 or a negative / CUDA error code.
 int gemm(const void* A, const void* B, GemmArgs g, int epi, uint32_t splits, cudaStream_t stream);
 
-// The whole inference pass of the 3-hidden-layer network in one persistent kernel (the
-// activations of a 128-row tile never leave the SM): X [M x K0] BF16 with K0 in {64, 128},
-// W1 [256 x K0], W2, W3 [256 x 256] BF16 (row n = output unit, K contiguous), biases and head in
-// FP32.  Writes y and / or exp(y) with the per-record sums as the kHead epilogue does.
+// The whole inference pass of the 3-hidden-layer network in one persistent kernel (the input
+// rows and activations of a 128-row tile never leave the SM): the input rows as launch_features
+// defines them (K0 in {64, 128}; rec16, recgeo, cellgeo, P as there, record_rows = C), built from
+// xcells, the cell table in the row layout ([C x K0], record columns zero), W1 [256 x K0], W2, W3
+// [256 x 256] BF16 (row n = output unit, K contiguous), biases and head in FP32.  Writes y and / or
+// exp(y) with the per-record sums as the kHead epilogue does.
 struct FusedArgs {
-    uint32_t M, K0;
+    uint32_t M, K0, P;
+    const __nv_bfloat16* rec16;
+    const __nv_bfloat16* xcells;
+    const double* recgeo;
+    const double* cellgeo;
     const float *b1, *b2, *b3, *head_w;
     float head_b;
     float* out_y;
@@ -64,8 +70,7 @@ struct FusedArgs {
     unsigned* error;
 };
 bool fused_shape(uint32_t K0, uint32_t H);
-int forward_fused(const void* X, const void* W1, const void* W2, const void* W3, const FusedArgs& f,
-                  cudaStream_t stream);
+int forward_fused(const void* W1, const void* W2, const void* W3, const FusedArgs& f, cudaStream_t stream);
 
 // ---------------------------------------------------------------- icp_mlp.cu
 // X[m][k] (BF16, [R*C x K0]) and optionally XT[k][m]: record features in columns [0, 16), the

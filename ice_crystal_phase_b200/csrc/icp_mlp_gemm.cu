@@ -23,6 +23,7 @@
 
 #include "icp_internal.h"
 #include "icp_mlp.h"
+#include "icp_mlp_features.cuh"
 #include "icp_umma.cuh"
 
 namespace icp::mlp {
@@ -701,19 +702,24 @@ bool persistent_shape(const GemmArgs& g)
 // (0, 0), (0, 1), (1, 0), (1, 1), (2, 0), (2, 1), so the tensor pipe computes one slot's layer while
 // the epilogue warps drain the other slot's previous layer: a tile's own layers are serial (each
 // needs the previous one's activations), the two tiles of a pair overlap.
-//   * A tile's input rows X (KC1 chunks of 64 columns) arrive by TMA in the first chunks of its
-//     slot's H buffer, once the slot's previous tile has finished its last layer (h_free).
+//   * A tile's input rows X (KC1 chunks of 64 columns: record features, the cell table, the axis
+//     harmonics, as launch_features defines them) are built in the first chunks of its slot's H
+//     buffer once the slot's previous tile has finished its last layer (h_free): the slot's
+//     feature warp loads the tile's 128 cells from the row-layout cell table by TMA (x_land),
+//     then writes the record and axis-harmonic columns (x_full).  The rows never exist in
+//     global memory.
 //   * The weights (W1, W2, W3 in 32 KB chunks of 64 input columns x 256 units, read from L2) go
 //     through a kFStages-deep ring in the MMA order, once per (layer, slot).
 //   * The epilogue (sixteen warps: lane quarter q, 64-column chunk s) writes a layer's activations
 //     into the slot's H buffer, fences them for the tensor core's reads and arrives on the slot's
 //     acc_empty: the slot's next layer may then overwrite the accumulator and read H.  The head
 //     epilogue forms y = silu(z3) . w4 + b as the kHead epilogue does.
-// Barriers per slot: x_full, h_free, acc_full, acc_empty; per ring stage: w_full, w_empty; drain.
+// Barriers per slot: x_land, x_full, h_free, acc_full, acc_empty; per ring stage: w_full, w_empty;
+// drain.
 // Every wait is bounded as in gemm_persistent_kernel.
 constexpr uint32_t kFStages = 2;
 constexpr uint32_t kFEpiWarps = 16; // four per TMEM lane quarter, one 64-column chunk each
-constexpr uint32_t kFThreads = 64 + 32 * kFEpiWarps;
+constexpr uint32_t kFThreads = 128 + 32 * kFEpiWarps; // producer, MMA, two feature warps, epilogue
 constexpr uint32_t kWChunk = 256u * 128u; // 64 input columns x 256 units, BF16
 constexpr uint32_t kHChunk = 128u * 128u; // 128 rows x 64 columns, BF16
 constexpr uint32_t kFExtra = 8192;        // barriers, TMEM slot, abort flag, biases, head, partial sums
@@ -840,7 +846,7 @@ __device__ __forceinline__ void fused_head_store(const FusedArgs& f, uint32_t m,
 
 template <int KC1>
 __global__ void __launch_bounds__(kFThreads, 1)
-    mlp_fused_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmW1,
+    mlp_fused_kernel(const __grid_constant__ CUtensorMap tmXC, const __grid_constant__ CUtensorMap tmW1,
                      const __grid_constant__ CUtensorMap tmW2, const __grid_constant__ CUtensorMap tmW3,
                      const FusedArgs f)
 {
@@ -854,7 +860,8 @@ __global__ void __launch_bounds__(kFThreads, 1)
     uint64_t* h_free = bars + 2;     // [2]
     uint64_t* acc_full = bars + 4;   // [2]
     uint64_t* acc_empty = bars + 6;  // [2]
-    uint64_t* w_full = bars + 8;     // [S]
+    uint64_t* x_land = bars + 8;     // [2]
+    uint64_t* w_full = bars + 10;    // [S]
     uint64_t* w_empty = w_full + S;  // [S]
     uint64_t* drain = w_empty + S;
     uint32_t* tslot = reinterpret_cast<uint32_t*>(drain + 1);
@@ -874,6 +881,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
             umma::mbar_init(&h_free[s], 1);
             umma::mbar_init(&acc_full[s], 1);
             umma::mbar_init(&acc_empty[s], kFEpiWarps);
+            umma::mbar_init(&x_land[s], 1);
         }
         for (uint32_t s = 0; s < S; ++s) {
             umma::mbar_init(&w_full[s], 1);
@@ -897,10 +905,9 @@ __global__ void __launch_bounds__(kFThreads, 1)
 
     if (warp == 0) {
         if (lane == 0) {
-            // producer, in the MMA order: per (layer, slot) the slot's input rows (layer 0) and
-            // the layer's weight chunks
+            // producer: the weight chunks of every (layer, slot) in the MMA order
             bool ok = true;
-            uint32_t it = 0, xi[2] = {0u, 0u}; // weight chunks and input tiles per slot issued
+            uint32_t it = 0; // weight chunks issued
 #pragma unroll 1
             for (uint32_t p = 0; p < pairs && ok; ++p) {
 #pragma unroll 1
@@ -909,18 +916,6 @@ __global__ void __launch_bounds__(kFThreads, 1)
                     for (uint32_t sl = 0; sl < 2 && ok; ++sl) {
                         const uint32_t k = 2u * p + sl;
                         if (k >= mine) break;
-                        if (l == 0) {
-                            if (xi[sl] >= 1 && !umma::mbar_wait(&h_free[sl], (xi[sl] - 1u) & 1u, kWaitLimit)) {
-                                ok = false;
-                                break;
-                            }
-                            ++xi[sl];
-                            const uint32_t t = blockIdx.x + k * gridDim.x;
-                            umma::mbar_arrive_expect_tx(&x_full[sl], KC1 * kHChunk);
-                            for (int kc = 0; kc < KC1; ++kc)
-                                umma::tma_load_2d(hbuf + (sl * 4u + kc) * kHChunk, &tmX, &x_full[sl], kc * 64,
-                                                  (int32_t)(t * 128u));
-                        }
                         const uint32_t n = l == 0 ? (uint32_t)KC1 : 4u;
                         const CUtensorMap* map = l == 0 ? &tmW1 : (l == 1 ? &tmW2 : &tmW3);
                         for (uint32_t kc = 0; kc < n; ++kc, ++it) {
@@ -943,11 +938,8 @@ __global__ void __launch_bounds__(kFThreads, 1)
                 *abort_flag = 1;
                 atomicExch(f.error, 3u);
             }
-            // every issued load lands before the CTA's shared memory is released (at most one
-            // input tile per slot is in flight)
+            // every issued load lands before the CTA's shared memory is released
             for (uint32_t j = it > S ? it - S : 0u; j < it; ++j) umma::mbar_wait(&w_full[j % S], (j / S) & 1u, kWaitLimit);
-            for (int sl = 0; sl < 2; ++sl)
-                if (xi[sl]) umma::mbar_wait(&x_full[sl], (xi[sl] - 1u) & 1u, kWaitLimit);
         }
     } else if (warp == 1) {
         if (lane == 0) {
@@ -1005,9 +997,70 @@ __global__ void __launch_bounds__(kFThreads, 1)
             umma::mma_commit(drain);
             if (!umma::mbar_wait(drain, 0, kWaitLimit)) atomicExch(f.error, 6u);
         }
+    } else if (warp < 4) {
+        // feature warp of slot sl: the input rows of each of the slot's tiles into its H buffer,
+        // bit for bit as features_kernel writes them (16-byte pieces: q < 2 the record features,
+        // q < qaxis the cell table, then the axis harmonics).  A tile's rows belong to one record
+        // (the record's cell count is a multiple of 128) and to 128 consecutive cells.
+        const uint32_t sl = warp - 2u;
+        const uint32_t qrow = f.K0 / 8u, qaxis = qrow - f.P / 8u, C = f.record_rows;
+        const uint4* rec16 = reinterpret_cast<const uint4*>(f.rec16);
+        uint8_t* h = hbuf + sl * 4u * kHChunk;
+#pragma unroll 1
+        for (uint32_t p = 0; p < pairs; ++p) {
+            const uint32_t k = 2u * p + sl;
+            if (k >= mine) break;
+            const bool ready = p == 0 || umma::mbar_wait(&h_free[sl], (p - 1u) & 1u, kWaitLimit);
+            if (!__all_sync(0xffffffffu, ready && !*abort_flag)) {
+                if (lane == 0) {
+                    *abort_flag = 1;
+                    atomicExch(f.error, 7u);
+                }
+                break;
+            }
+            const uint32_t row0 = (blockIdx.x + k * gridDim.x) * 128u;
+            const uint32_t rec = row0 / C, c0 = row0 - rec * C;
+            if (lane == 0) {
+                umma::mbar_arrive_expect_tx(&x_land[sl], KC1 * kHChunk);
+                for (int kc = 0; kc < KC1; ++kc)
+                    umma::tma_load_2d(h + kc * kHChunk, &tmXC, &x_land[sl], kc * 64, (int32_t)c0);
+            }
+            const bool landed = umma::mbar_wait(&x_land[sl], p & 1u, kWaitLimit);
+            if (!__all_sync(0xffffffffu, landed)) {
+                if (lane == 0) {
+                    *abort_flag = 1;
+                    atomicExch(f.error, 7u);
+                    umma::mbar_wait(&x_land[sl], p & 1u, kWaitLimit); // the load lands before the CTA ends
+                }
+                break;
+            }
+            const uint4 ra = rec16[2u * rec], rb = rec16[2u * rec + 1u];
+            for (uint32_t r = lane; r < 128u; r += 32u) {
+                // record columns: pieces 0 and 1 of chunk 0
+                *reinterpret_cast<uint4*>(h + r * 128u + ((0u ^ (r & 7u)) << 4)) = ra;
+                *reinterpret_cast<uint4*>(h + r * 128u + ((1u ^ (r & 7u)) << 4)) = rb;
+                const double x = cos_psi(f.recgeo, f.cellgeo, rec, c0 + r);
+                double tm = 1.0, t = x; // T_0, T_1: the same recurrence as axis_harmonics8
+                for (uint32_t q = qaxis; q < qrow; ++q) {
+                    __align__(16) __nv_bfloat16 hv[8];
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        hv[i] = __float2bfloat16_rn(__double2float_rn(t));
+                        const double tn = __dsub_rn(__dmul_rn(__dmul_rn(2.0, x), t), tm);
+                        tm = t;
+                        t = tn;
+                    }
+                    *reinterpret_cast<uint4*>(h + (q >> 3) * kHChunk + r * 128u + (((q & 7u) ^ (r & 7u)) << 4)) =
+                        *reinterpret_cast<const uint4*>(hv);
+                }
+            }
+            fence_proxy_async_smem();
+            __syncwarp();
+            if (lane == 0) umma::mbar_arrive(&x_full[sl]);
+        }
     } else {
         // epilogue warps: lane quarter q (TMEM lanes 32 q ..), 64-column chunk `slice`
-        const uint32_t q = warp & 3u, slice = (warp - 2u) >> 2;
+        const uint32_t q = warp & 3u, slice = (warp - 4u) >> 2;
         const uint32_t row = 32u * q + lane, c = 64u * slice;
         bool live = true;
 #pragma unroll 1
@@ -1061,11 +1114,11 @@ __global__ void __launch_bounds__(kFThreads, 1)
 }
 
 template <int KC1>
-int launch_fused(const void* X, const void* W1, const void* W2, const void* W3, const FusedArgs& f, cudaStream_t st)
+int launch_fused(const void* W1, const void* W2, const void* W3, const FusedArgs& f, cudaStream_t st)
 {
-    CUtensorMap tx, t1, t2, t3;
-    if (make_map(&tx, X, f.M, f.K0, 128u) || make_map(&t1, W1, 256u, f.K0, 256u) || make_map(&t2, W2, 256u, 256u, 256u) ||
-        make_map(&t3, W3, 256u, 256u, 256u))
+    CUtensorMap tc, t1, t2, t3;
+    if (make_map(&tc, f.xcells, f.record_rows, f.K0, 128u) || make_map(&t1, W1, 256u, f.K0, 256u) ||
+        make_map(&t2, W2, 256u, 256u, 256u) || make_map(&t3, W3, 256u, 256u, 256u))
         return -1;
     const size_t smem = fsmem_bytes<KC1>();
     cudaError_t e =
@@ -1073,7 +1126,7 @@ int launch_fused(const void* X, const void* W1, const void* W2, const void* W3, 
     if (e != cudaSuccess) return (int)e;
     const uint32_t tiles = f.M / 128u;
     const uint32_t grid = tiles < (uint32_t)sm_count() ? tiles : (uint32_t)sm_count();
-    mlp_fused_kernel<KC1><<<grid, kFThreads, smem, st>>>(tx, t1, t2, t3, f);
+    mlp_fused_kernel<KC1><<<grid, kFThreads, smem, st>>>(tc, t1, t2, t3, f);
     return (int)cudaGetLastError();
 }
 
@@ -1111,11 +1164,12 @@ int gemm(const void* A, const void* B, GemmArgs g, int epi, uint32_t splits, cud
 
 bool fused_shape(uint32_t K0, uint32_t H) { return H == 256u && (K0 == 64u || K0 == 128u); }
 
-int forward_fused(const void* X, const void* W1, const void* W2, const void* W3, const FusedArgs& f,
-                  cudaStream_t st)
+int forward_fused(const void* W1, const void* W2, const void* W3, const FusedArgs& f, cudaStream_t st)
 {
-    if (f.M == 0 || f.M % 128u || !fused_shape(f.K0, 256u)) return -3;
-    return f.K0 == 64u ? launch_fused<1>(X, W1, W2, W3, f, st) : launch_fused<2>(X, W1, W2, W3, f, st);
+    if (f.M == 0 || f.M % 128u || !fused_shape(f.K0, 256u) || f.P % 8u || f.P + 16u > f.K0 || !f.record_rows ||
+        f.record_rows % 128u)
+        return -3;
+    return f.K0 == 64u ? launch_fused<1>(W1, W2, W3, f, st) : launch_fused<2>(W1, W2, W3, f, st);
 }
 
 } // namespace icp::mlp
