@@ -516,9 +516,11 @@ int icp::cdf_enqueue_batch(icp_context* c, const CdfBatchInput* in, uint32_t cou
     if (!count) return ICP_OK;
     ICP_CUDA(cudaMemsetAsync(d_sync, 0, 2 * sizeof(unsigned) * count, c->stream));
     ICP_CUDA(cudaMemsetAsync(d_reports, 0, sizeof(CdfDeviceReport) * count, c->stream));
-    // 16 strips per record, as many records per launch as stay co-resident
+    // 2 strips per record, as many records per launch as stay co-resident (the chains of a
+    // strip's columns run side by side, so wider strips cost little and let more records share
+    // one launch)
     CdfShape sh{};
-    const bool fits = cdf_choose_shape(c->device, c->sms, nt, np, ct, cp, false, std::max(1u, (cp + 15u) / 16u),
+    const bool fits = cdf_choose_shape(c->device, c->sms, nt, np, ct, cp, false, std::max(1u, (cp + 1u) / 2u),
                                        0xffffffffu, sh) == 0;
     const uint32_t strips = fits ? (cp + sh.cw - 1) / sh.cw : 0u;
     const uint32_t per = fits ? (uint32_t)std::max(0, cdf_max_coresident_blocks(sh.smem, c->device)) / strips : 0u;

@@ -124,6 +124,28 @@ void record_row(const icp_surrogate_config& g, const icp_drop_item& it, uint16_t
     for (int k = 0; k < 16; ++k) out[k] = feature(f[k]);
 }
 
+// Page-locked host staging: copies from it are asynchronous, so a call enqueues its work after
+// the forward pass without waiting for it.
+struct PinnedHost {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t n)
+    {
+        if (n <= bytes) return cudaSuccess;
+        release();
+        const cudaError_t e = cudaHostAlloc(&ptr, n, cudaHostAllocDefault);
+        if (e == cudaSuccess) bytes = n;
+        else ptr = nullptr;
+        return e;
+    }
+    void release()
+    {
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
+
 } // namespace
 
 struct icp_surrogate {
@@ -139,8 +161,11 @@ struct icp_surrogate {
     std::vector<double> h_edges;
     std::vector<uint16_t> h_rec;
     std::vector<double> h_recgeo;
+    PinnedHost h_frac, h_reports; // diffraction fractions and CDF reports of a generate call
     ~icp_surrogate()
     {
+        h_frac.release();
+        h_reports.release();
         Scratch* all[] = {&params, &grads, &adam_m, &adam_v, &wbf, &cells, &edges, &rec16, &loss, &X, &XT, &z1, &h1,
                           &h1T, &z2, &h2, &h2T, &z3, &y, &dy, &dz3, &dz3T, &dz2, &dz2T, &dz1T, &mass, &reports, &sync,
                           &mass_sum, &dfrac, &drows, &cellgeo, &recgeo, &xcells};
@@ -680,8 +705,12 @@ int icp_surrogate_generate(icp_surrogate* s, const icp_drop_item* items, uint32_
     ICP_CUDA(cudaMemsetAsync(s->mass_sum.ptr, 0, sizeof(double) * count, c->stream));
     ICP_TRY(enqueue_features(s, items, count, false, !fused_inference(s)));
     ICP_TRY(enqueue_forward(s, count, false, nullptr, as<double>(s->mass), as<double>(s->mass_sum)));
-    // the analytic diffraction rows on host threads while the device runs the network
-    std::vector<double> frac((size_t)count * g.nt);
+    // the analytic diffraction rows on host threads while the device runs the network, into
+    // page-locked staging so that the copy, the row scaling, the CDF build and the reports are
+    // all enqueued behind the network without waiting for it
+    ICP_CUDA(s->h_frac.ensure(sizeof(double) * (size_t)count * g.nt));
+    ICP_CUDA(s->h_reports.ensure(sizeof(CdfDeviceReport) * count));
+    double* frac = static_cast<double*>(s->h_frac.ptr);
     std::vector<int> fst(count, ICP_OK);
     {
         const unsigned workers = std::max(1u, std::min<unsigned>(count, std::thread::hardware_concurrency()));
@@ -689,7 +718,7 @@ int icp_surrogate_generate(icp_surrogate* s, const icp_drop_item* items, uint32_
         for (unsigned w = 0; w < workers; ++w)
             jobs.push_back(std::async(std::launch::async, [&, w]() {
                 for (uint32_t r = w; r < count; r += workers)
-                    fst[r] = diffraction_fractions(s, items[r], frac.data() + (size_t)r * g.nt);
+                    fst[r] = diffraction_fractions(s, items[r], frac + (size_t)r * g.nt);
             }));
         for (auto& j : jobs) j.get();
     }
@@ -698,7 +727,8 @@ int icp_surrogate_generate(icp_surrogate* s, const icp_drop_item* items, uint32_
             cudaStreamSynchronize(c->stream);
             return fail(fst[r], "surrogate: record %u: diffraction rows failed", r);
         }
-    ICP_CUDA(cudaMemcpyAsync(s->dfrac.ptr, frac.data(), sizeof(double) * frac.size(), cudaMemcpyHostToDevice, c->stream));
+    ICP_CUDA(cudaMemcpyAsync(s->dfrac.ptr, frac, sizeof(double) * (size_t)count * g.nt, cudaMemcpyHostToDevice,
+                             c->stream));
     {
         const int e = mlp::launch_scale_rows(as<double>(s->dfrac), as<double>(s->mass_sum), count, g.nt,
                                              as<double>(s->drows), c->stream);
@@ -715,8 +745,8 @@ int icp_surrogate_generate(icp_surrogate* s, const icp_drop_item* items, uint32_
     }
     ICP_TRY(cdf_enqueue_batch(c, in.data(), count, g.nt, g.np, ct, cp, as<double>(s->edges),
                               as<CdfDeviceReport>(s->reports), as<unsigned>(s->sync)));
-    std::vector<CdfDeviceReport> dev(count);
-    ICP_CUDA(cudaMemcpyAsync(dev.data(), s->reports.ptr, sizeof(CdfDeviceReport) * count, cudaMemcpyDeviceToHost,
+    CdfDeviceReport* dev = static_cast<CdfDeviceReport*>(s->h_reports.ptr);
+    ICP_CUDA(cudaMemcpyAsync(dev, s->reports.ptr, sizeof(CdfDeviceReport) * count, cudaMemcpyDeviceToHost,
                              c->stream));
     ICP_TRY(finish(c, "icp_surrogate_generate"));
     int first = ICP_OK;

@@ -480,13 +480,15 @@ __global__ void __launch_bounds__(kThreads, 1) cdf_build_kernel(const __grid_con
             B[(size_t)i * b_row + (size_t)my_cl * b_col] = x;
         }
     __syncthreads();
+    // the warps that hold a column chain (threads tid < w) sit out the audit pass below
+    const uint32_t aw = (w + 31u) & ~31u;
     if (tid < w) {
         // ordered ascending-theta scan of one phi column; the unnormalised prefix of row i+1
         // replaces the weight of row i in place (each column belongs to one thread)
         P.colsum[c0 + tid] = chain_prefix(B + (size_t)tid * b_col, ct, b_row);
-    } else if (P.keep && tid >= 32) {
+    } else if (P.keep && tid >= aw) {
         // meanwhile the other warps form the audit's p = coarse / stored total in A
-        for (uint32_t k = tid - 32; k < ct * w; k += kThreads - 32) {
+        for (uint32_t k = tid - aw; k < ct * w; k += kThreads - aw) {
             const size_t a = (size_t)(k / w) * CW + k % w;
             const double c = A[a];
             const double pv = c / stored_total;
@@ -774,7 +776,7 @@ int cdf_choose_shape(int device, int sms, uint32_t nt, uint32_t np, uint32_t ct,
         const uint32_t keep = m[0], tma = m[1];
         if (tma && !(tma_ok && fine)) continue;
         uint32_t w = std::max<uint32_t>(min_width, (cp + (uint32_t)sms - 1) / (uint32_t)sms);
-        for (; w <= cp && w <= kThreads; ++w) {
+        for (; w <= cp && w <= kThreads - 32u; ++w) { // at least one warp besides the column chains
             CdfShape s{};
             s.cw = w;
             s.keep = keep;
