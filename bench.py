@@ -513,7 +513,7 @@ def run_surrogate(I, ctx, stream, a) -> dict:
 
     if not S.DEFAULT_MODEL.exists():
         return {"unavailable": f"{S.DEFAULT_MODEL.name} missing"}
-    R = 64  # records per surrogate call (the serving batch)
+    R = 128  # records per surrogate call: the serving batch where records/s saturates
     sur, extra = S.load(ctx, S.DEFAULT_MODEL, max_records=R)
     gate = S.FallbackGate.from_dict(extra["gate"])
     ct, cp = extra["storage"]

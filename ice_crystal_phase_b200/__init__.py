@@ -1040,14 +1040,34 @@ def batch_settings(nt: int, np_: int, ct: int | None = None, cp: int | None = No
     return s
 
 
+# icp_drop_item as a NumPy record with the ctypes structure's own offsets, so that a batch of
+# items is filled column by column rather than one ctypes field at a time
+_DROP_ITEM_DTYPE = np.dtype({
+    "names": ["radius_mm", "coefficients", "inclination_deg", "interior_index", "wavelength_nm", "rays", "seed",
+              "diffraction"],
+    "formats": ["<f8", ("<f8", 8), "<f8", "<f8", "<f8", "<u8", "<u8", "<u4"],
+    "offsets": [getattr(DropItem, f).offset for f in ("radius_mm", "coefficients", "inclination_deg", "interior_index",
+                                                      "wavelength_nm", "rays", "seed", "diffraction")],
+    "itemsize": C.sizeof(DropItem)})
+
+
 def _items(specs) -> C.Array:
-    arr = (DropItem * len(specs))()
-    for i, sp in enumerate(specs):
-        arr[i].radius_mm = sp.radius_mm
-        arr[i].coefficients = _c8(sp.coefficients)
-        arr[i].inclination_deg, arr[i].interior_index = sp.inclination_deg, sp.interior_index
-        arr[i].wavelength_nm, arr[i].rays, arr[i].seed = sp.wavelength_nm, sp.rays, sp.seed
-        arr[i].diffraction = int(bool(sp.diffraction))
+    n = len(specs)
+    arr = (DropItem * n)()
+    if not n:
+        return arr
+    v = np.frombuffer(arr, dtype=_DROP_ITEM_DTYPE, count=n)
+    coeffs = [[float(x) for x in sp.coefficients] for sp in specs]
+    if any(len(c) > 8 for c in coeffs):
+        raise ValueError("At most eight shape coefficients.")
+    v["coefficients"] = [c + [0.0] * (8 - len(c)) for c in coeffs]
+    v["radius_mm"] = [sp.radius_mm for sp in specs]
+    v["inclination_deg"] = [sp.inclination_deg for sp in specs]
+    v["interior_index"] = [sp.interior_index for sp in specs]
+    v["wavelength_nm"] = [sp.wavelength_nm for sp in specs]
+    v["rays"] = [int(sp.rays) for sp in specs]
+    v["seed"] = [int(sp.seed) for sp in specs]
+    v["diffraction"] = [int(bool(sp.diffraction)) for sp in specs]
     return arr
 
 

@@ -806,9 +806,11 @@ __device__ __forceinline__ void hidden_chunk(uint32_t taddr, const float* bias, 
     }
 }
 
-// Partial head sum of one 64-column chunk: sum silu(acc + bias) * head_w.
+// Partial head sum of one 64-column chunk: sum silu(acc + bias) * head_w (four interleaved
+// partial sums, so that the products do not wait on one another).
 __device__ __forceinline__ float head_chunk(uint32_t taddr, const float* bias, const float* head_w, float y)
 {
+    float y0 = 0.0f, y1 = 0.0f, y2 = 0.0f, y3 = 0.0f;
 #pragma unroll
     for (uint32_t h = 0; h < 2; ++h) {
         float vv[32];
@@ -820,13 +822,13 @@ __device__ __forceinline__ float head_chunk(uint32_t taddr, const float* bias, c
             float s0 = vv[4 * q], s1 = vv[4 * q + 1], s2 = vv[4 * q + 2], s3 = vv[4 * q + 3];
             silu_pair(s0, s1, b.x, b.y);
             silu_pair(s2, s3, b.z, b.w);
-            y = fmaf(s0, w.x, y);
-            y = fmaf(s1, w.y, y);
-            y = fmaf(s2, w.z, y);
-            y = fmaf(s3, w.w, y);
+            y0 = fmaf(s0, w.x, y0);
+            y1 = fmaf(s1, w.y, y1);
+            y2 = fmaf(s2, w.z, y2);
+            y3 = fmaf(s3, w.w, y3);
         }
     }
-    return y;
+    return y + ((y0 + y1) + (y2 + y3));
 }
 
 __device__ __forceinline__ void fused_head_store(const FusedArgs& f, uint32_t m, float yacc)

@@ -197,3 +197,24 @@ def test_tv_is_the_reference_record_metric():
         assert float((c * mu[None, :]).sum() / c.sum()) == pytest.approx(g, abs=1e-15)
     # the theta marginal TV is the TV of the column sums
     assert 0.5 * np.abs(cells["a"].sum(axis=0) - cells["b"].sum(axis=0)).sum() == pytest.approx(marginal_tv, rel=1e-12)
+
+
+def test_drop_items_carry_every_field(icp):
+    """The C array of icp_drop_item that batch and surrogate calls pass is filled column by column;
+    every field equals the record description's, short coefficient lists are zero-padded and more
+    than eight are refused."""
+    specs = icp.batched_record_specs(9, seed=3)
+    specs[0].coefficients = [0.0, -0.05]
+    specs[1].diffraction = False
+    arr = icp._items(specs)
+    for i, sp in enumerate(specs):
+        c = [float(x) for x in sp.coefficients] + [0.0] * (8 - len(sp.coefficients))
+        assert list(arr[i].coefficients) == c
+        assert (arr[i].radius_mm, arr[i].inclination_deg, arr[i].interior_index, arr[i].wavelength_nm) == \
+            (sp.radius_mm, sp.inclination_deg, sp.interior_index, sp.wavelength_nm)
+        assert (arr[i].rays, arr[i].seed, arr[i].diffraction, arr[i].reserved) == \
+            (sp.rays, sp.seed, int(bool(sp.diffraction)), 0)
+    assert len(icp._items([])) == 0
+    specs[2].coefficients = [0.0] * 9
+    with pytest.raises(ValueError):
+        icp._items(specs)
