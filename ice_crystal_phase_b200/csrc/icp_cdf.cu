@@ -315,6 +315,26 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
         : "memory");
 }
 
+// The ordered chains (column prefixes in phase B, the marginal scan in phase C) are dependent
+// FP64 additions on warps 0 .. chain_warps - 1; warps on the same SM sub-partition (warp mod 4)
+// that run FP64 divisions meanwhile slow each addition.  The side work of those phases therefore
+// goes to the warps of the other sub-partitions (all non-chain warps when the chains occupy all
+// four), numbered densely: this thread's index and the number of side threads.
+__device__ __forceinline__ bool side_worker(uint32_t warp, uint32_t lane, uint32_t chain_warps, uint32_t& idx,
+                                            uint32_t& count)
+{
+    const uint32_t busy = chain_warps < 4u ? chain_warps : 0u; // sub-partitions 0 .. busy - 1 hold a chain
+    uint32_t before = 0, total = 0;
+    for (uint32_t u = chain_warps; u < kWarps; ++u)
+        if ((u & 3u) >= busy) {
+            before += u < warp ? 1u : 0u;
+            ++total;
+        }
+    idx = before * 32u + lane;
+    count = total * 32u;
+    return warp >= chain_warps && (warp & 3u) >= busy;
+}
+
 __global__ void __launch_bounds__(kThreads, 1) cdf_build_kernel(const __grid_constant__ CUtensorMap map,
                                                                  const CdfParams P0)
 {
@@ -480,15 +500,17 @@ __global__ void __launch_bounds__(kThreads, 1) cdf_build_kernel(const __grid_con
             B[(size_t)i * b_row + (size_t)my_cl * b_col] = x;
         }
     __syncthreads();
-    // the warps that hold a column chain (threads tid < w) sit out the audit pass below
-    const uint32_t aw = (w + 31u) & ~31u;
+    // the warps that hold a column chain (threads tid < w) sit out the audit pass below, and so
+    // do the warps that share their sub-partitions
+    uint32_t side_b = 0, sides_b = 0;
+    const bool side_in_b = side_worker(warp, lane, (w + 31u) >> 5, side_b, sides_b);
     if (tid < w) {
         // ordered ascending-theta scan of one phi column; the unnormalised prefix of row i+1
         // replaces the weight of row i in place (each column belongs to one thread)
         P.colsum[c0 + tid] = chain_prefix(B + (size_t)tid * b_col, ct, b_row);
-    } else if (P.keep && tid >= aw) {
+    } else if (P.keep && side_in_b) {
         // meanwhile the other warps form the audit's p = coarse / stored total in A
-        for (uint32_t k = tid - aw; k < ct * w; k += kThreads - aw) {
+        for (uint32_t k = side_b; k < ct * w; k += sides_b) {
             const size_t a = (size_t)(k / w) * CW + k % w;
             const double c = A[a];
             const double pv = c / stored_total;
@@ -511,6 +533,8 @@ __global__ void __launch_bounds__(kThreads, 1) cdf_build_kernel(const __grid_con
     for (uint32_t j = tid; j < P.cp; j += kThreads) S[j] = __ldcg(P.colsum + j);
     __syncthreads();
     const uint32_t stride = ct + 1;
+    uint32_t side_c = 0, sides_c = 0;
+    const bool side_in_c = side_worker(warp, lane, 1u, side_c, sides_c);
     if (tid == 0) {
         // ordered marginal scan (phase_table.cpp:154): phi[j+1] = phi[j] + colsum[j]; this
         // strip keeps the running values at its own columns
@@ -522,12 +546,12 @@ __global__ void __launch_bounds__(kThreads, 1) cdf_build_kernel(const __grid_con
             sphi[j - j0 + 1] = a;
         }
         s_tot[3] = chain_sum(S + j1, P.cp - j1, 1u, a);
-    } else if (tid >= 32) {
+    } else if (side_in_c) {
         // meanwhile the normalised conditionals of this strip, written once each: its output
         // rows are the contiguous range theta[c0*(ct+1) .. c1*(ct+1)); element (cl, i) comes from
         // the prefix of row i kept at B(i-1, cl), which keeps the normalised value for the audit
-        const uint32_t span = w * stride, step = kThreads - 32;
-        uint32_t q = tid - 32, cl = q / stride, i = q % stride;
+        const uint32_t span = w * stride, step = sides_c;
+        uint32_t q = side_c, cl = q / stride, i = q % stride;
         double* out = P.theta + (size_t)c0 * stride;
         for (; q < span; q += step) {
             const double cs = S[c0 + cl];
