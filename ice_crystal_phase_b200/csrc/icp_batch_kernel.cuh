@@ -28,7 +28,7 @@ template <class R, class G> struct BatchParams {
     const double* edges_d;
 };
 
-// Dynamic shared memory: per-warp parameter slots, per-warp status counts, the u edges.
+// Dynamic shared memory: per-warp parameter slots, per-warp tallies, the u edges.
 template <class R, class G> __host__ __device__ constexpr size_t batch_slot_bytes()
 {
     return (sizeof(TraceParams<R, G>) + 15) / 16 * 16;
@@ -36,46 +36,7 @@ template <class R, class G> __host__ __device__ constexpr size_t batch_slot_byte
 template <class R, class G> size_t batch_smem_bytes(uint32_t threads, uint32_t nt, bool smem_edges)
 {
     const uint32_t warps = threads / 32;
-    return warps * batch_slot_bytes<R, G>() + warps * 8 * sizeof(unsigned) + (smem_edges ? (nt + 1) * sizeof(R) : 0);
-}
-
-// Counters of one warp's chunk into its record (lane 0), status counts of the warp cleared.
-template <class R, class P_>
-__device__ __forceinline__ void warp_flush(const P_& P, unsigned* s_status, const LaneAcc<R>& A)
-{
-    unsigned long long w[14] = {A.esc_fx, A.unres_fx, A.fwd_fx, A.bwd_fx, A.rays, A.outputs, A.rejected,
-                                A.snapped, A.near_edge, A.fallback, A.invalid, A.encounters, A.missed, A.gauge_evals};
-#pragma unroll
-    for (int q = 0; q < 14; ++q)
-        for (int o = 16; o; o >>= 1) w[q] += __shfl_xor_sync(kFull, w[q], o);
-    double ax = A.axial, mb = A.max_bal, mi = (double)A.max_iface;
-    for (int o = 16; o; o >>= 1) {
-        ax += __shfl_xor_sync(kFull, ax, o);
-        mb = fmax(mb, __shfl_xor_sync(kFull, mb, o));
-        mi = fmax(mi, __shfl_xor_sync(kFull, mi, o));
-    }
-    __syncwarp();
-    const unsigned lane = threadIdx.x & 31u;
-    DevStats* Gs = P.stats;
-    if (lane == 0) {
-        add128(Gs->esc, w[0]);
-        add128(Gs->unres, w[1]);
-        add128(Gs->fwd, w[2]);
-        add128(Gs->bwd, w[3]);
-        unsigned long long* counters[10] = {&Gs->rays, &Gs->outputs, &Gs->rejected, &Gs->snapped, &Gs->near_edge,
-                                            &Gs->fallback, &Gs->invalid, &Gs->encounters, &Gs->missed, &Gs->gauge_evals};
-#pragma unroll
-        for (int q = 0; q < 10; ++q)
-            if (w[4 + q]) atomicAdd(counters[q], w[4 + q]);
-        if (ax != 0.0) atomicAdd(&Gs->axial, ax);
-        atomicMax(&Gs->max_bal_bits, (unsigned long long)__double_as_longlong(mb));
-        atomicMax(&Gs->max_iface_bits, (unsigned long long)__double_as_longlong(mi));
-    }
-    if (lane < 8) {
-        if (s_status[lane]) atomicAdd(&Gs->status[lane], (unsigned long long)s_status[lane]);
-        s_status[lane] = 0u;
-    }
-    __syncwarp();
+    return warps * batch_slot_bytes<R, G>() + warps * kTallyBytes + (smem_edges ? (nt + 1) * sizeof(R) : 0);
 }
 
 template <class R, class G>
@@ -84,9 +45,9 @@ __global__ void __launch_bounds__(256, (sizeof(R) == 4 ? 4 : 1)) batch_trace_ker
     extern __shared__ __align__(16) unsigned char smem[];
     const unsigned warps = blockDim.x >> 5, wib = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     unsigned char* slots = smem;
-    unsigned* s_status_all = reinterpret_cast<unsigned*>(slots + warps * batch_slot_bytes<R, G>());
-    R* s_edges = reinterpret_cast<R*>(s_status_all + 8 * warps);
-    for (unsigned i = threadIdx.x; i < 8 * warps; i += blockDim.x) s_status_all[i] = 0u;
+    Tally* tallies = reinterpret_cast<Tally*>(slots + warps * batch_slot_bytes<R, G>());
+    R* s_edges = reinterpret_cast<R*>(tallies + warps);
+    for (unsigned i = threadIdx.x; i < warps * kTallyBytes / 4; i += blockDim.x) reinterpret_cast<unsigned*>(tallies)[i] = 0u;
     const R* gedges;
     if constexpr (sizeof(R) == 4) gedges = Q.edges_f;
     else gedges = Q.edges_d;
@@ -97,7 +58,7 @@ __global__ void __launch_bounds__(256, (sizeof(R) == 4 ? 4 : 1)) batch_trace_ker
     TraceParams<R, G>& P = *reinterpret_cast<TraceParams<R, G>*>(slots + wib * batch_slot_bytes<R, G>());
     BlockShared<R> B;
     B.H = SmemHist{nullptr, nullptr, 0u};
-    B.s_status = s_status_all + 8 * wib;
+    B.T = tallies + wib;
     B.edges = Q.smem_edges ? s_edges : gedges;
     uint32_t cur = 0xffffffffu;
     while (true) {
@@ -131,7 +92,7 @@ __global__ void __launch_bounds__(256, (sizeof(R) == 4 ? 4 : 1)) batch_trace_ker
         LaneAcc<R> A;
         lane_acc_clear(A);
         trace_slice<R, G>(P, B, first, end, A);
-        warp_flush<R>(P, B.s_status, A);
+        warp_stats_flush<R>(P.stats, A, B.T);
     }
 }
 

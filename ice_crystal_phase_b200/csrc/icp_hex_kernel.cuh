@@ -245,22 +245,52 @@ template <class R> struct LaneRay {
     bool live;
 };
 
-// Per-lane accumulators, summed per warp when a block (or a batch chunk) ends.  The power sums are
-// exact 64-bit fixed-point integers; the counts are 32-bit: a lane traces at most
-// lane_rays_max(max_hits) rays between flushes (the launchers cut launches and chunks to that),
-// so that none of them can wrap.
+// Per-lane accumulators of what changes every step or every ray, summed per warp when a block (or
+// a batch chunk) ends.  The power sums are exact 64-bit fixed-point integers; the counts are
+// 32-bit: a
+// lane traces at most lane_rays_max(max_hits) rays between flushes (the launchers cut launches
+// and chunks to that), so that none of them can wrap.
 template <class R> struct LaneAcc {
     unsigned long long esc_fx, unres_fx, fwd_fx, bwd_fx;
-    uint32_t outputs, rays, rejected, snapped, near_edge, fallback, invalid, encounters, missed, gauge_evals;
-    double axial, max_bal;
+    uint32_t outputs, fallback, encounters, gauge_evals, snapped, near_edge;
+    double axial;
     R max_iface;
     uint64_t cur_batch;
     uint32_t cur_batch_out;
 };
 
+// Per-warp tally in shared memory of what changes once per ray or more rarely (the rays per
+// status, misses, rejections, invalid exits, the largest energy residual and, for the drop, the
+// unresolved and pole powers), added with shared atomics.  Kept out of the lanes' registers, which
+// the FP32 kernels need for the ray state at 64 registers; without them the drop kernel's spills
+// halve and its DRAM traffic falls from 130 MB to 17 MB per 1e8-ray launch.  The warp's ray count
+// is the status counts plus the misses; its power sums stay below 2^60 (lane_rays_max).  The
+// prism keeps snapped exits, near-edge hits and the power sums per lane: its symmetric directions
+// make them frequent (forward exits through parallel faces), and contended 64-bit shared atomics
+// cost it 7 %.
+struct Tally {
+    unsigned status[8];
+    unsigned missed, rejected, invalid, pad;
+    unsigned long long unres_fx, fwd_fx, bwd_fx, max_bal_bits;
+};
+constexpr uint32_t kTallyWarps = 8; // blocks of 64..256 threads
+constexpr size_t kTallyBytes = 80;
+// whether a trace's power sums go to the tally (the drop) or stay per lane (the prism)
+template <class P_> __host__ __device__ constexpr bool power_in_tally()
+{
+    return !std::is_same_v<std::remove_cv_t<decltype(P_::geo)>, HexGeo<std::remove_cv_t<decltype(P_::tail)>>>;
+}
+static_assert(sizeof(Tally) == kTallyBytes, "tally layout");
+// Byte offset of the tallies in the trace kernel's shared memory (after the histogram table's
+// values and keys, 16-byte aligned); the u edges follow the kTallyWarps tallies.
+__host__ __device__ constexpr size_t trace_tally_offset(uint32_t hash_slots)
+{
+    return ((size_t)hash_slots * 12u + 15u) / 16u * 16u;
+}
+
 template <class R, class P_>
-__device__ __forceinline__ void finish_ray(const P_& P, LaneRay<R>& L, LaneAcc<R>& A, unsigned* s_status,
-                                           int status, unsigned long long residual_fx, R residual)
+__device__ __forceinline__ void finish_ray(const P_& P, LaneRay<R>& L, LaneAcc<R>& A, Tally* T, int status,
+                                           unsigned long long residual_fx, R residual)
 {
     L.live = false;
     double bal;
@@ -272,37 +302,40 @@ __device__ __forceinline__ void finish_ray(const P_& P, LaneRay<R>& L, LaneAcc<R
     } else {
         bal = fabs((double)L.esc + (double)residual - 1.0);
     }
-    A.unres_fx += residual_fx;
-    A.max_bal = fmax(A.max_bal, bal);
-    A.rays += 1;
-    atomicAdd(&s_status[status], 1u);
+    if constexpr (power_in_tally<P_>()) {
+        if (residual_fx) atomicAdd(&T->unres_fx, residual_fx);
+    } else {
+        A.unres_fx += residual_fx;
+    }
+    if (bal > 0.0) atomicMax(&T->max_bal_bits, (unsigned long long)__double_as_longlong(bal));
+    atomicAdd(&T->status[status], 1u);
     const bool ok = (status == 0 || status == 1) && bal <= P.bal_tol;
-    if (!ok) A.rejected += 1;
+    if (!ok) atomicAdd(&T->rejected, 1u);
 }
 
 // Ends the ray if the continuing branch is exhausted / below the tail / out of encounters
 // (the top-of-loop and after-loop tests of hex_trace_core.hpp:217-251, applied eagerly).
 template <class R, class P_>
-__device__ __forceinline__ void settle(const P_& P, LaneRay<R>& L, LaneAcc<R>& A, unsigned* s_status)
+__device__ __forceinline__ void settle(const P_& P, LaneRay<R>& L, LaneAcc<R>& A, Tally* T)
 {
     if constexpr (sizeof(R) == 4) {
         const unsigned long long p = L.pfx;
-        if (p == 0ull) finish_ray<R>(P, L, A, s_status, 0, 0ull, R(0));
-        else if (p <= P.tail_fx) finish_ray<R>(P, L, A, s_status, 1, p, R(0));
-        else if (L.hits >= P.max_hits) finish_ray<R>(P, L, A, s_status, 2, p, R(0));
+        if (p == 0ull) finish_ray<R>(P, L, A, T, 0, 0ull, R(0));
+        else if (p <= P.tail_fx) finish_ray<R>(P, L, A, T, 1, p, R(0));
+        else if (L.hits >= P.max_hits) finish_ray<R>(P, L, A, T, 2, p, R(0));
     } else {
         const R power = L.S.I;
-        if (power == R(0)) finish_ray<R>(P, L, A, s_status, 0, 0ull, R(0));
-        else if (power <= P.tail) finish_ray<R>(P, L, A, s_status, 1, to_fix(power), power);
-        else if (L.hits >= P.max_hits) finish_ray<R>(P, L, A, s_status, 2, to_fix(power), power);
+        if (power == R(0)) finish_ray<R>(P, L, A, T, 0, 0ull, R(0));
+        else if (power <= P.tail) finish_ray<R>(P, L, A, T, 1, to_fix(power), power);
+        else if (L.hits >= P.max_hits) finish_ray<R>(P, L, A, T, 2, to_fix(power), power);
     }
 }
 
-// Per-block shared state: the privatised histogram table, the per-status ray counts of the
-// block and (optionally) the u edges.
+// Per-block shared state: the privatised histogram table, this warp's tally and (optionally) the
+// u edges.
 template <class R> struct BlockShared {
     SmemHist H;
-    unsigned* s_status;
+    Tally* T;
     const R* edges;
 };
 
@@ -312,11 +345,13 @@ __device__ __forceinline__ BlockShared<R> block_setup(const P_& P, unsigned char
     BlockShared<R> B;
     unsigned long long* s_vals = reinterpret_cast<unsigned long long*>(smem);
     uint32_t* s_keys = reinterpret_cast<uint32_t*>(s_vals + P.hash_slots);
-    B.s_status = reinterpret_cast<unsigned*>(s_keys + P.hash_slots);
-    R* s_edges = reinterpret_cast<R*>(B.s_status + 8);
+    Tally* tallies = reinterpret_cast<Tally*>(smem + trace_tally_offset(P.hash_slots));
+    B.T = tallies + (threadIdx.x >> 5);
+    R* s_edges = reinterpret_cast<R*>(tallies + kTallyWarps);
     const uint32_t nt = P.gf.nt;
     for (uint32_t s = threadIdx.x; s < P.hash_slots; s += blockDim.x) { s_keys[s] = 0u; s_vals[s] = 0ull; }
-    if (threadIdx.x < 8) B.s_status[threadIdx.x] = 0u;
+    for (uint32_t i = threadIdx.x; i < kTallyWarps * kTallyBytes / 4; i += blockDim.x)
+        reinterpret_cast<unsigned*>(tallies)[i] = 0u;
     if (P.smem_edges) {
         for (uint32_t i = threadIdx.x; i <= nt; i += blockDim.x) {
             if constexpr (sizeof(R) == 4) s_edges[i] = P.edges_f[i];
@@ -334,9 +369,8 @@ __device__ __forceinline__ BlockShared<R> block_setup(const P_& P, unsigned char
 template <class R> __device__ __forceinline__ void lane_acc_clear(LaneAcc<R>& A)
 {
     A.esc_fx = A.unres_fx = A.fwd_fx = A.bwd_fx = 0ull;
-    A.outputs = A.rays = A.rejected = A.snapped = A.near_edge = A.fallback = A.invalid = A.encounters = A.missed = 0u;
-    A.gauge_evals = 0u;
-    A.axial = A.max_bal = 0.0;
+    A.outputs = A.fallback = A.encounters = A.gauge_evals = A.snapped = A.near_edge = 0u;
+    A.axial = 0.0;
     A.max_iface = R(0);
     A.cur_batch = ~0ull;
     A.cur_batch_out = 0u;
@@ -350,7 +384,7 @@ __device__ __forceinline__ void trace_slice(const P_& P, const BlockShared<R>& B
 {
     const unsigned lane = threadIdx.x & 31u;
     const unsigned lt_mask = (1u << lane) - 1u;
-    unsigned* s_status = B.s_status;
+    Tally* T = B.T;
     LaneRay<R> L;
     L.live = false;
     while (true) {
@@ -397,8 +431,7 @@ __device__ __forceinline__ void trace_slice(const P_& P, const BlockShared<R>& B
             if (fresh) {
                 if (!hit) {
                     // a sampled ray that misses the particle carries no incident power
-                    ++A.missed;
-                    ++A.rays;
+                    atomicAdd(&T->missed, 1u);
                 } else {
                     L.live = true;
                     L.esc = R(0);
@@ -432,8 +465,7 @@ __device__ __forceinline__ void trace_slice(const P_& P, const BlockShared<R>& B
             const int es = geo_entry(P.geo, P.seed, L.id, pos, n, face);
             if (es < 0) {
                 // a sampled ray that misses the particle carries no incident power
-                ++A.missed;
-                ++A.rays;
+                atomicAdd(&T->missed, 1u);
             } else {
                 L.live = true;
                 L.esc = R(0);
@@ -444,7 +476,7 @@ __device__ __forceinline__ void trace_slice(const P_& P, const BlockShared<R>& B
                 L.face = face;
                 do_split = true;
                 if (es) {
-                    finish_ray<R>(P, L, A, s_status, es, 1ull << kFixBits, R(1));
+                    finish_ray<R>(P, L, A, T, es, 1ull << kFixBits, R(1));
                     do_split = false;
                 }
                 sd = P.k;
@@ -459,7 +491,7 @@ __device__ __forceinline__ void trace_slice(const P_& P, const BlockShared<R>& B
             bool near_edge = false;
             const int hs = geo_next(P.geo, L.p, L.d, L.face, n, near_edge);
             if (hs) {
-                finish_ray<R>(P, L, A, s_status, hs, sizeof(R) == 4 ? L.pfx : to_fix(L.S.I), L.S.I);
+                finish_ray<R>(P, L, A, T, hs, sizeof(R) == 4 ? L.pfx : to_fix(L.S.I), L.S.I);
             } else {
                 A.near_edge += near_edge ? 1u : 0u;
                 ++L.hits;
@@ -502,7 +534,7 @@ __device__ __forceinline__ void trace_slice(const P_& P, const BlockShared<R>& B
                 }
             }
             if (fresh && !sp.has_t) {
-                finish_ray<R>(P, L, A, s_status, 0, 0ull, R(0));
+                finish_ray<R>(P, L, A, T, 0, 0ull, R(0));
             } else {
                 L.d = fresh ? sp.dt : sp.dr;
                 L.e = sp.s;
@@ -511,7 +543,7 @@ __device__ __forceinline__ void trace_slice(const P_& P, const BlockShared<R>& B
                     L.pfx = cont_fx;
                     L.S.I = (R)cont_fx * R(kFixUnit);
                 }
-                settle<R>(P, L, A, s_status);
+                settle<R>(P, L, A, T);
             }
         }
 
@@ -524,16 +556,23 @@ __device__ __forceinline__ void trace_slice(const P_& P, const BlockShared<R>& B
             if constexpr (sizeof(R) == 4) b = bin_f32(P.gf, B.edges, od);
             else b = bin_f64(P.gd, B.edges, od);
             if (!b.valid) {
-                A.invalid += 1;
+                atomicAdd(&T->invalid, 1u);
             } else {
                 v = efx;
                 A.esc_fx += v;
                 A.outputs += 1;
                 A.snapped += b.snapped ? 1u : 0u;
                 A.axial += (double)opow * b.mu;
-                if (b.pole > 0) A.fwd_fx += v;
-                else if (b.pole < 0) A.bwd_fx += v;
-                else { to_table = true; cell = b.cell; }
+                if (b.pole > 0) {
+                    if constexpr (power_in_tally<P_>()) atomicAdd(&T->fwd_fx, (unsigned long long)v);
+                    else A.fwd_fx += v;
+                } else if (b.pole < 0) {
+                    if constexpr (power_in_tally<P_>()) atomicAdd(&T->bwd_fx, (unsigned long long)v);
+                    else A.bwd_fx += v;
+                } else {
+                    to_table = true;
+                    cell = b.cell;
+                }
             }
         }
         hist_add(B.H, P.mass, P.to_mass, to_table, cell, v, A.fallback);
@@ -556,45 +595,56 @@ __device__ __forceinline__ void trace_slice(const P_& P, const BlockShared<R>& B
         if (P.batch_out && A.cur_batch != ~0ull && A.cur_batch_out) atomicAdd(&P.batch_out[A.cur_batch], A.cur_batch_out);
 }
 
-// Block epilogue (all threads): flush the table into P.mass and the lane accumulators and the
-// block's status counts into P.stats; leaves the table and the status counts cleared.
+// The warp's sums into the record's statistics: its lanes' accumulators (shuffled) and its tally
+// (lane 0 adds, then clears the tally).  Called by whole warps after the lanes' last update.
+template <class R>
+__device__ __forceinline__ void warp_stats_flush(DevStats* Gs, const LaneAcc<R>& A, Tally* T)
+{
+    unsigned long long w[10] = {A.esc_fx, A.outputs, A.fallback, A.encounters, A.gauge_evals, A.snapped, A.near_edge,
+                                A.unres_fx, A.fwd_fx, A.bwd_fx};
+#pragma unroll
+    for (int q = 0; q < 10; ++q)
+        for (int o = 16; o; o >>= 1) w[q] += __shfl_xor_sync(kFull, w[q], o);
+    double ax = A.axial, mi = (double)A.max_iface;
+    for (int o = 16; o; o >>= 1) {
+        ax += __shfl_xor_sync(kFull, ax, o);
+        mi = fmax(mi, __shfl_xor_sync(kFull, mi, o));
+    }
+    __syncwarp();
+    if ((threadIdx.x & 31u) == 0) {
+        add128(Gs->esc, w[0]);
+        // one of each pair is zero: the sums sit per lane (the prism) or in the tally (the drop)
+        add128(Gs->unres, w[7] + T->unres_fx);
+        add128(Gs->fwd, w[8] + T->fwd_fx);
+        add128(Gs->bwd, w[9] + T->bwd_fx);
+        unsigned long long rays = T->missed;
+#pragma unroll
+        for (int s = 0; s < 8; ++s) {
+            rays += T->status[s];
+            if (T->status[s]) atomicAdd(&Gs->status[s], (unsigned long long)T->status[s]);
+        }
+        const unsigned long long c[10] = {rays, w[1], T->rejected, w[5], w[6], w[2], T->invalid, w[3], T->missed, w[4]};
+        unsigned long long* counters[10] = {&Gs->rays, &Gs->outputs, &Gs->rejected, &Gs->snapped, &Gs->near_edge,
+                                            &Gs->fallback, &Gs->invalid, &Gs->encounters, &Gs->missed, &Gs->gauge_evals};
+#pragma unroll
+        for (int q = 0; q < 10; ++q)
+            if (c[q]) atomicAdd(counters[q], c[q]);
+        if (ax != 0.0) atomicAdd(&Gs->axial, ax);
+        atomicMax(&Gs->max_bal_bits, T->max_bal_bits);
+        atomicMax(&Gs->max_iface_bits, (unsigned long long)__double_as_longlong(mi));
+        *T = Tally{};
+    }
+    __syncwarp();
+}
+
+// Block epilogue (all threads): flush the table into P.mass and every warp's sums into P.stats;
+// leaves the table and the tallies cleared.
 template <class R, class P_>
 __device__ __forceinline__ void block_flush(const P_& P, const BlockShared<R>& B, const LaneAcc<R>& A)
 {
     __syncthreads();
     hist_flush(B.H, P.mass, P.to_mass);
-    DevStats* Gs = P.stats;
-    // Per-warp sums stay below 2^60 (a warp slice holds at most 2^16 rays of power <= 1).
-    unsigned long long w[14] = {A.esc_fx, A.unres_fx, A.fwd_fx, A.bwd_fx, A.rays, A.outputs, A.rejected,
-                                A.snapped, A.near_edge, A.fallback, A.invalid, A.encounters, A.missed, A.gauge_evals};
-#pragma unroll
-    for (int q = 0; q < 14; ++q)
-        for (int o = 16; o; o >>= 1) w[q] += __shfl_xor_sync(kFull, w[q], o);
-    double ax = A.axial, mb = A.max_bal, mi = (double)A.max_iface;
-    for (int o = 16; o; o >>= 1) {
-        ax += __shfl_xor_sync(kFull, ax, o);
-        mb = fmax(mb, __shfl_xor_sync(kFull, mb, o));
-        mi = fmax(mi, __shfl_xor_sync(kFull, mi, o));
-    }
-    if ((threadIdx.x & 31u) == 0) {
-        add128(Gs->esc, w[0]);
-        add128(Gs->unres, w[1]);
-        add128(Gs->fwd, w[2]);
-        add128(Gs->bwd, w[3]);
-        unsigned long long* counters[10] = {&Gs->rays, &Gs->outputs, &Gs->rejected, &Gs->snapped, &Gs->near_edge,
-                                            &Gs->fallback, &Gs->invalid, &Gs->encounters, &Gs->missed, &Gs->gauge_evals};
-#pragma unroll
-        for (int q = 0; q < 10; ++q)
-            if (w[4 + q]) atomicAdd(counters[q], w[4 + q]);
-        if (ax != 0.0) atomicAdd(&Gs->axial, ax);
-        atomicMax(&Gs->max_bal_bits, (unsigned long long)__double_as_longlong(mb));
-        atomicMax(&Gs->max_iface_bits, (unsigned long long)__double_as_longlong(mi));
-    }
-    __syncthreads();
-    if (threadIdx.x < 8) {
-        if (B.s_status[threadIdx.x]) atomicAdd(&Gs->status[threadIdx.x], (unsigned long long)B.s_status[threadIdx.x]);
-        B.s_status[threadIdx.x] = 0u;
-    }
+    warp_stats_flush<R>(P.stats, A, B.T);
 }
 
 // One record: the ray range [first, first+count) split into contiguous per-warp slices.

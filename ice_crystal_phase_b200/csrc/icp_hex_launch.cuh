@@ -14,7 +14,7 @@ constexpr uint32_t kEdgeSmemMax = 4097; // stage u edges in shared memory up to 
 
 template <class R> size_t trace_smem_bytes(uint32_t hash_slots, uint32_t nt)
 {
-    size_t b = (size_t)hash_slots * (8 + 4) + 8 * 4;
+    size_t b = trace_tally_offset(hash_slots) + kTallyWarps * kTallyBytes;
     if (nt + 1 <= kEdgeSmemMax) b += sizeof(R) * (nt + 1);
     return b;
 }
