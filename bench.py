@@ -50,7 +50,7 @@ sys.path.insert(0, str(ROOT))
 # kernels, from single-pass ncu captures of this workload: the 1e8-ray trace launch
 # (profiles/drop_trace_bin_kernel_dram_oblate_1e8.md) and the 900 x 1800 CDF launch
 # (profiles/cdf_build_kernel_900x1800.md)
-DROP_TRACE_TRAFFIC = 15.01e6 + 114.71e6
+DROP_TRACE_TRAFFIC = 14.249e6 + 2.328e6
 DROP_CDF_TRAFFIC = 13.0885e6 + 0.0
 CFG = dict(R=0.05, L=0.2, ki=(0.8660254037844387, -0.5, 0.0), n=1.31, nt=512, np=1024, hits=12, seed=12345)
 DROP = dict(radius=1.5, coefficients=(0.0, -0.08, -0.02, 0.005, 0.0, 0.0, 0.0, 0.0), wavelength=650.0, incl=20.0,
@@ -1264,7 +1264,7 @@ def run_b200_drop(a) -> None:
         "roofline": {"kernel": "trace_bin_kernel<float, DropGeo<float>>", "bound": "fp32_simt", "achieved": achieved,
                      "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
                      "traffic": DROP_TRACE_TRAFFIC if rays == 1e8 else None,
-                     "traffic_note": "DRAM bytes of one 1e8-ray launch (ncu, one pass): 15.0 MB read, 114.7 MB "
+                     "traffic_note": "DRAM bytes of one 1e8-ray launch (ncu, one pass): 14.2 MB read, 2.3 MB "
                                      "written, against 13.0 MB algorithmic (the FP64 histogram)",
                      "peak_note": f"derived: {sms} SMs x 128 FP32 lanes x 2 x {mhz:.0f} MHz (median SM clock under load)",
                      "flops_per_ray": flops / max(1, ks.rays), "kernel_ms": 1e3 * t_kernel,
