@@ -513,7 +513,7 @@ def run_surrogate(I, ctx, stream, a) -> dict:
 
     if not S.DEFAULT_MODEL.exists():
         return {"unavailable": f"{S.DEFAULT_MODEL.name} missing"}
-    R = 128  # records per surrogate call: the serving batch where records/s saturates
+    R = a.surrogate_batch  # records per surrogate call
     sur, extra = S.load(ctx, S.DEFAULT_MODEL, max_records=R)
     gate = S.FallbackGate.from_dict(extra["gate"])
     ct, cp = extra["storage"]
@@ -577,7 +577,8 @@ def run_surrogate(I, ctx, stream, a) -> dict:
     served_tv = [t for ok, t in zip(trusted, tv) if ok]
     served_bad = sum(1 for t in served_tv if t > 5e-3)
     return {
-        "workload": "learned_surrogate_256x512", "model": S.DEFAULT_MODEL.name, "records": n, "cells": [nt, np_],
+        "workload": "learned_surrogate_256x512", "model": S.DEFAULT_MODEL.name, "records": n, "records_per_call": R,
+        "cells": [nt, np_],
         "storage": [ct, cp], "network": {"hidden": H, "layers": 4, "input_width": K0, "dtype": "bf16 weights and "
                                          "activations, fp32 accumulation (tcgen05, TMEM)"},
         "surrogate_records_per_s": n / t_sur, "served_records_per_s": n / t_serve,
@@ -1321,6 +1322,8 @@ def main() -> None:
     p.add_argument("--batch-steps", type=int, default=3)
     p.add_argument("--surrogate-records", type=int, default=256, help="records of the surrogate measurement (0 = skip)")
     p.add_argument("--surrogate-checked", type=int, default=64, help="fresh records checked by 1e8-ray tracer records")
+    p.add_argument("--surrogate-batch", type=int, default=256,
+                   help="records per surrogate call (records/s grows with it up to ~128 and flattens)")
     p.add_argument("--hash-slots", type=int, default=0, help="shared histogram slots (0 = default, 1 = none)")
     p.add_argument("--atlas-incidents", type=int, default=3,
                    help="incidences of the deterministic atlas composition measurement (0 = skip)")
