@@ -57,6 +57,10 @@ int ok()
     } while (0)
 
 constexpr unsigned kThreads = 128;
+// The counting and filling passes wait on candidate gathers; six blocks per SM (80 registers, a
+// few bytes of spills) keep more of them in flight than the four that 128 registers allowed:
+// 3.77 -> 3.47 ms for the 513 x 513 lattice at 360 x 720 directions.
+constexpr unsigned kQueryBlocksPerSm = 6;
 constexpr unsigned kScanThreads = 1024;
 constexpr int kBinRows = 256, kBinCols = 512;
 constexpr double kPi = 3.141592653589793238462643383279502884;
@@ -477,7 +481,7 @@ struct RootCache {
     uint32_t* first;
 };
 
-__global__ void __launch_bounds__(kThreads) query_count_kernel(QueryArgs q, unsigned long long* __restrict__ counts,
+__global__ void __launch_bounds__(kThreads, kQueryBlocksPerSm) query_count_kernel(QueryArgs q, unsigned long long* __restrict__ counts,
                                                                RootCache cache)
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < q.direction_count; i += gridDim.x * blockDim.x) {
@@ -492,7 +496,7 @@ __global__ void __launch_bounds__(kThreads) query_count_kernel(QueryArgs q, unsi
     }
 }
 
-__global__ void __launch_bounds__(kThreads) query_fill_kernel(QueryArgs q, const unsigned long long* __restrict__ offsets,
+__global__ void __launch_bounds__(kThreads, kQueryBlocksPerSm) query_fill_kernel(QueryArgs q, const unsigned long long* __restrict__ offsets,
                                                               icp_query_summary* __restrict__ summaries,
                                                               icp_query_hit* __restrict__ hits, RootCache cache)
 {
