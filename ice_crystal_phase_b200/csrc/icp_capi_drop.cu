@@ -233,8 +233,10 @@ int drop_trace_enqueue(icp_context* c, const icp_drop_record* r, uint64_t first,
                        const icp_grid* g, const double* d_edges, double* d_mass, void* d_stats)
 {
     const bool f32 = r->precision == ICP_FP32;
-    const uint32_t threads = r->tuning.block_threads ? r->tuning.block_threads : 256u;
-    if (threads < 64 || threads > 256 || threads % 32) return fail(ICP_ERR_INVALID_ARGUMENT, "block_threads must be 64..256, multiple of 32");
+    const uint32_t max_threads = f32 ? drop_trace_threads_f32() : drop_trace_threads_f64();
+    const uint32_t threads = r->tuning.block_threads ? r->tuning.block_threads : max_threads;
+    if (threads < 64 || threads > max_threads || threads % 32)
+        return fail(ICP_ERR_INVALID_ARGUMENT, "block_threads must be 64..%u, multiple of 32", max_threads);
     uint32_t slots;
     if (const int e = table_slots(r->tuning, slots)) return e;
     int per_sm = f32 ? drop_blocks_per_sm_f32(slots, g->nt, threads) : drop_blocks_per_sm_f64(slots, g->nt, threads);

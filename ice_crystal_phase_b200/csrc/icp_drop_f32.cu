@@ -7,6 +7,7 @@ int drop_blocks_per_sm_f32(uint32_t slots, uint32_t nt, uint32_t threads)
 {
     return trace_blocks_per_sm<float, DropGeo<float>>(slots, nt, threads);
 }
+uint32_t drop_trace_threads_f32() { return TraceShape<float, DropGeo<float>>::threads; }
 int launch_drop_batch_f32(const BatchLaunch& B, cudaStream_t s) { return launch_drop_batch<float>(B, s); }
 int drop_batch_blocks_f32(uint32_t threads, uint32_t nt) { return drop_batch_blocks<float>(threads, nt); }
 size_t drop_batch_param_bytes_f32() { return sizeof(TraceParams<float, DropGeo<float>>); }

@@ -127,6 +127,9 @@ int hex_blocks_per_sm_f32(uint32_t slots, uint32_t nt, uint32_t threads);
 int hex_blocks_per_sm_f64(uint32_t slots, uint32_t nt, uint32_t threads);
 int drop_blocks_per_sm_f32(uint32_t slots, uint32_t nt, uint32_t threads);
 int drop_blocks_per_sm_f64(uint32_t slots, uint32_t nt, uint32_t threads);
+// the drop trace kernels' block size: the default, and the most threads a block may have
+uint32_t drop_trace_threads_f32();
+uint32_t drop_trace_threads_f64();
 
 // One persistent launch over many drop records (icp_batch_kernel.cuh).  recs[r] describes
 // record r exactly as for a single-record launch (first = 0, count = total = its rays, its

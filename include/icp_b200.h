@@ -138,7 +138,8 @@ typedef struct {
 
 /* Histogram privatisation / launch tuning (all zero = autotuned defaults). */
 typedef struct {
-    uint32_t block_threads;  /* 128..1024, multiple of 32                                     */
+    uint32_t block_threads;  /* 0 = the kernel's size (FP32 drop 128, others 256), else 64 up
+                              * to that size, a multiple of 32                               */
     uint32_t blocks_per_sm;  /* resident blocks per SM requested                              */
     uint32_t hash_slots;     /* shared-memory table slots (power of two; 0 = default; 1 = off) */
     uint32_t reserved;
