@@ -3,8 +3,11 @@
 //
 //   D[M x N] = A[M x K] * B[N x K]^T      A, B: BF16, K-major (row-major with K contiguous)
 //
-// Two kernels.  The layer GEMMs (K, N = layer widths <= 256, M = the rows of a batch) run
-// persistent and warp-specialised (gemm_persistent_kernel, below).  The weight gradients (M, N =
+// Three kernels.  Inference of the default network shape runs as one persistent kernel that takes
+// each 128-row tile from its input row to y with the activations on chip (mlp_fused_kernel,
+// below).  The layer GEMMs of training and of other shapes (K, N = layer widths <= 256, M = the
+// rows of a batch) run persistent and warp-specialised (gemm_persistent_kernel).  The weight
+// gradients (M, N =
 // layer widths, K = rows of a batch) run split-K (gemm_kernel): one CTA of 128 threads computes a
 // 128 x N tile (N in {64, 128, 256}) over a range of K chunks of 64: thread 0 streams A and B
 // chunks through a STAGES-deep ring with 2-D TMA loads (128-byte swizzle, completion counted on a
